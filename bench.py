@@ -1,0 +1,389 @@
+"""Benchmark of the fixed-grid Mie ensemble (the batched configuration: 1024 wavelengths x 64
+lognormal distributions x 512 radius nodes, 360 Gauss cosines, Greek order 64, FP64).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A step is one pass of the hot path over the whole batch (33,554,432 size nodes). ``value`` is
+node throughput with the inputs resident in HBM, timed with CUDA events on the launching
+stream, L2 flushed between steps (a 512 MiB write outside the timed events), max over ranks.
+``e2e`` is the same metric through the C ABI with host buffers (pinned), the host-device copies
+of the inputs and outputs inside the timed region. For N > 1 every rank runs its own batch
+(seed = rank): weak scaling, no collective on the data path.
+
+``--impl reference`` times the reference's algorithm on the host cores: the reference itself
+(Rust) cannot be built in this image, so its CPU restatement (the oracle, OpenMP over units,
+all host threads) runs on a bounded random sample of the same batch's units.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mie ensemble nodes/s on 1 B200, batched vs plain FP64, at 1e-10 rel err vs FP64"
+UNIT = "nodes/s"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--scale", type=float, default=1.0, help="fraction of the batch (tests)")
+    p.add_argument("--cpu-seconds", type=float, default=15.0)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def workload_config(w, args):
+    return {"workload": "config2: 1024 wavelengths x 64 lognormal distributions x 512 ln-r Gauss "
+                        "nodes, m per (distribution, wavelength), 360 Gauss cosines, Greek L=64",
+            "n_dist": int(w.dists.size), "n_wl": int(w.wavelengths.size),
+            "n_nodes": int(w.n_nodes), "n_mu": int(w.mu.size), "greek_order": int(w.greek_order),
+            "nodes_per_step": int(w.n_nodes_total), "scale": args.scale,
+            "l2": "flushed between steps (512 MiB write outside the timed events)",
+            "parallelism": "replicas (weak): each rank its own batch"}
+
+
+# ---------------------------------------------------------------------------------------------
+# CPU leg: the oracle on a bounded random sample of the batch's units.
+# ---------------------------------------------------------------------------------------------
+def cpu_sample(w, seconds: float, seed: int = 12345):
+    from oracle import oracle as O
+
+    threads = os.cpu_count() or 1
+    rng = np.random.default_rng(seed)
+    units = rng.permutation(w.n_units)
+    d = np.zeros(w.dists.size, dtype=O.DIST_DTYPE)
+    d["kind"], d["p"] = w.dists["kind"], w.dists["param"]
+    d["r_lo"], d["r_hi"] = w.dists["r_lo"], w.dists["r_hi"]
+    nodes = 0
+    t_total = 0.0
+    k = 0
+    batch = max(threads, 8)
+    while t_total < seconds and k < units.size:
+        sel = units[k:k + batch]
+        k += sel.size
+        t0 = time.perf_counter()
+        for u in sel:
+            di, wi = divmod(int(u), w.wavelengths.size)
+            O.ensemble_fixed(d[di:di + 1], w.wavelengths[wi:wi + 1], w.m[di:di + 1, wi:wi + 1],
+                             w.n_nodes, w.mu, w.greek_order, True, threads=threads)
+        t_total += time.perf_counter() - t0
+        nodes += sel.size * w.n_nodes
+    return {"value": nodes / t_total, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{k} random units ({nodes} nodes) of the batch, {t_total:.1f} s, "
+                      f"oracle (f64 restatement of the reference) with OpenMP over each "
+                      f"unit's... one unit at a time, {threads} threads"}
+
+
+def reference_arm(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from scatrs_b200 import workloads as W
+
+    w = W.config2(seed=0, scale=args.scale, mu=None)
+    vals = []
+    base = None
+    for s in range(args.warmup + args.steps):
+        base = cpu_sample(w, args.cpu_seconds / 3, seed=1000 + s)
+        if s >= args.warmup:
+            vals.append(base["value"])
+    v = float(np.mean(vals))
+    base["value"] = v
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": w.n_nodes_total / v * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)", "config": workload_config(w, args),
+            "cpu_baseline": base,
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "the reference (Rust) cannot be built here; its CPU restatement is timed"}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------------------------
+# GPU legs.
+# ---------------------------------------------------------------------------------------------
+class Clocks:
+    """nvidia-smi samples of the SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def algorithmic_flops(w, user_rows: int):
+    """FP64 flops of K-b per step: 16 N_j (h_u + h_b) for node j (2 GEMMs x 4 real columns x 2
+    flops per order and table row; h_u the requested cosines' table rows, h_b the rows of the
+    band of the node's chunk) -- the per-node figure of the angle sums."""
+    r = np.empty((w.dists.size, w.n_nodes))
+    from scatrs_b200 import _native
+
+    xi, om = _native.gauss_legendre(w.n_nodes)
+    for d in range(w.dists.size):
+        a, b = np.log(w.dists["r_lo"][d]), np.log(w.dists["r_hi"][d])
+        r[d] = np.exp(0.5 * (a + b) + 0.5 * (b - a) * xi)
+    total = 0.0
+    L = w.greek_order
+    cpu = (w.n_nodes + 31) // 32
+    pad = cpu * 32 - w.n_nodes
+    for i, lam in enumerate(w.wavelengths):
+        x = 2.0 * np.pi * r / lam
+        n = np.ceil(x + 6.0 * np.cbrt(x) + 3.0)
+        npad = np.pad(n, ((0, 0), (0, pad)))
+        nc = npad.reshape(w.dists.size, cpu, 32).max(axis=2)
+        hb = np.zeros_like(nc)
+        if L >= 0:
+            u = np.ones_like(nc)
+            while np.any(u < nc):
+                u = np.where(u < nc, np.ceil(u * 1.25), u)
+            order = np.minimum(L, 2 * u)
+            nq = u + np.floor((order + 2) / 2)
+            hb = nq - np.floor(nq / 2)
+        hrow = np.repeat(hb, 32, axis=1)[:, : w.n_nodes]
+        total += float(np.sum(16.0 * n * (user_rows + hrow)))
+    return total
+
+
+def fp64_peak_tflops(torch):
+    """cuBLAS DGEMM (FP64) throughput, best of 5, as the FP64 roofline denominator."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        torch.matmul(a, b)
+    best = 1e30
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        torch.cuda.synchronize()
+        best = min(best, s.elapsed_time(e))
+    del a, b
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def ours(args):
+    import torch
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    from scatrs_b200 import _native
+    from scatrs_b200 import workloads as W
+
+    _native.require_device()
+    w = W.config2(seed=rank, scale=args.scale)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    wl_d = torch.tensor(w.wavelengths, dtype=torch.float64, device=dev)
+    m_d = torch.tensor(w.m.view(np.float64).reshape(-1), dtype=torch.float64, device=dev)
+    n = w.n_units
+    values_d = torch.empty(11 * n, dtype=torch.float64, device=dev)
+    phase_d = torch.empty(6 * n * w.mu.size, dtype=torch.float64, device=dev)
+    greek_d = torch.empty(6 * n * (w.greek_order + 1), dtype=torch.float64, device=dev)
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)
+
+    def step():
+        _native.ensemble_fixed_device(w.dists, wl_d.data_ptr(), w.wavelengths.size,
+                                      m_d.data_ptr(), w.mu, w.n_nodes, w.greek_order, True,
+                                      values_d.data_ptr(), phase_d.data_ptr(),
+                                      greek_d.data_ptr(), stream.cuda_stream)
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        step()
+    _native.check_errors(stream.cuda_stream)
+    barrier()
+    launches0 = _native.launch_count()
+    times = []
+    with Clocks(local) as clk:
+        for _ in range(args.steps):
+            flush.random_(0, 255)
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            step()
+            e.record(stream)
+            e.synchronize()
+            times.append(s.elapsed_time(e))
+        barrier()
+    _native.check_errors(stream.cuda_stream)
+    launches = _native.launch_count() - launches0
+    ms = float(np.sum(times))
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * w.n_nodes_total * args.steps / (ms * 1e-3)
+
+    # e2e: the host-buffer entry point, pinned buffers, copies inside the timed region.
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
+    wl_h = pin(w.wavelengths)
+    m_h = pin(w.m.view(np.float64).reshape(-1))
+    v_h = torch.empty(11 * n, dtype=torch.float64).pin_memory()
+    p_h = torch.empty(6 * n * w.mu.size, dtype=torch.float64).pin_memory()
+    g_h = torch.empty(6 * n * (w.greek_order + 1), dtype=torch.float64).pin_memory()
+    import ctypes
+
+    opts = _native.FixedOptions(w.n_nodes, w.greek_order, 1, 0)
+    err = ctypes.create_string_buffer(1024)
+    mu = np.ascontiguousarray(w.mu)
+    pd = lambda t: ctypes.cast(t.data_ptr(), _native._PD)  # noqa: E731
+
+    def e2e_step():
+        st = _native.load().scatrs_ensemble_fixed(
+            w.dists.ctypes.data, w.dists.size, pd(wl_h), w.wavelengths.size, pd(m_h),
+            _native._p(mu), mu.size, ctypes.byref(opts), pd(v_h), pd(p_h), pd(g_h), err, 1024)
+        _native._check(st, err)
+
+    e2e_step()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    barrier()
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * w.n_nodes_total * args.steps / e2e_s
+    h2d = 8 * w.wavelengths.size + 16 * n + 16 * w.dists.size * w.n_nodes
+    d2h = 8 * (11 * n + 6 * n * w.mu.size + 6 * n * (w.greek_order + 1)) + 4 * n * (
+        (w.n_nodes + 31) // 32)
+
+    # Kernel times of one profiled step (events around each launch on its stream).
+    _native.set_profiling(True)
+    step()
+    kt = _native.kernel_times()
+    _native.set_profiling(False)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    fp64 = fp64_peak_tflops(torch)
+    user_rows = int(np.unique(np.abs(w.mu)).size)
+    flops = algorithmic_flops(w, user_rows)
+    unit_ms, unit_n = kt["unit_kernel"]
+    mie_ms, mie_n = kt["mie_fixed_kernel"]
+    achieved = flops / (unit_ms * 1e-3) / 1e12
+    total_k = sum(v[0] for v in kt.values())
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": workload_config(w, args),
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "fp64", "kernel": "unit_kernel (K-b/c/d)", "achieved": achieved,
+                     "peak": fp64, "unit": "TFLOP/s", "frac": achieved / fp64,
+                     "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (no FP64 entry "
+                                    "in MEASURED_PEAKS.json)",
+                     "traffic": None, "launches": unit_n, "avg_launch_ms": unit_ms / max(unit_n, 1),
+                     "algorithmic_flop_per_step": flops},
+        "kernels_ms_per_step": {k: v[0] for k, v in kt.items()},
+        "kernel_share": {k: (v[0] / total_k if total_k else None) for k, v in kt.items()},
+        "hbm_peak_gbs": peaks.get("hbm_gbs"),
+    }
+    line["clocks"] = clk.summary()
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_sample(w, args.cpu_seconds)
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        ours(args)
+
+
+if __name__ == "__main__":
+    main()

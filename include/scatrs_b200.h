@@ -1,0 +1,151 @@
+/*
+ * scatrs_b200: the size-distribution ensemble path of usask-arg/scatrs on NVIDIA B200
+ * (sm_100a), behind a C ABI.
+ *
+ * Every entry point takes plain pointers and sizes, returns a status code, and (on failure)
+ * writes a message into a caller-owned buffer. The status codes mirror the reference's error
+ * enum (scatrs/src/error.rs:17-32), as its Python binding maps them
+ * (scatrs-py/src/errors.rs:14-45):
+ *   0 OK, 1 INVALID_INPUT, 2 NOT_CONVERGED, 3 OUTSIDE_VALIDATED_DOMAIN,
+ *   4 CUDA (a CUDA runtime error or a device-side wait that gave up), 5 NO_DEVICE.
+ *
+ * Units are distribution-major, like the reference's batch (scatrs-py/src/ensemble.rs:452-454):
+ * unit u = d * n_wavelengths + i for distribution d and wavelength i.
+ */
+#ifndef SCATRS_B200_H
+#define SCATRS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum scatrs_status {
+  SCATRS_OK = 0,
+  SCATRS_INVALID_INPUT = 1,
+  SCATRS_NOT_CONVERGED = 2,
+  SCATRS_OUTSIDE_VALIDATED_DOMAIN = 3,
+  SCATRS_CUDA = 4,
+  SCATRS_NO_DEVICE = 5
+};
+
+/* Distribution kinds, with the parameters in the order of the reference's tagged tuples
+ * (scatrs-py/src/ensemble.rs:38-57; SizeDistribution, scatrs/src/ensemble/distribution.rs:15-66):
+ *   LOGNORMAL (median_radius, width), GAMMA (effective_radius, effective_variance),
+ *   MODIFIED_GAMMA (alpha, b, gamma), POWER_LAW (exponent, min_radius, max_radius). */
+enum scatrs_distribution_kind {
+  SCATRS_LOGNORMAL = 1,
+  SCATRS_GAMMA = 2,
+  SCATRS_MODIFIED_GAMMA = 3,
+  SCATRS_POWER_LAW = 4
+};
+
+/* One size distribution on a fixed grid: n_nodes Gauss-Legendre nodes in t = ln r over
+ * [ln r_lo, ln r_hi] (the radius of a sphere). */
+typedef struct scatrs_distribution {
+  int32_t kind;
+  int32_t reserved;
+  double param[3];
+  double r_lo;
+  double r_hi;
+} scatrs_distribution;
+
+/* Options of the fixed-grid ensemble. The reference's EnsembleOptions
+ * (scatrs/src/ensemble/mod.rs:342-382) minus the adaptive controls (rtol, max_panels,
+ * refine_*), which the fixed grid does not have. */
+typedef struct scatrs_fixed_options {
+  int32_t n_nodes;           /* radius nodes per distribution, >= 1 */
+  int32_t greek_order;       /* highest Greek order L, or -1 for none */
+  int32_t normalized;        /* 1: normalized phase matrix and Greek coefficients */
+  int32_t allow_unvalidated; /* 1: compute outside the Mie validated domain */
+} scatrs_fixed_options;
+
+/* Sizes of the outputs of scatrs_ensemble_fixed for n_units units: the reference dict's arrays
+ * (scatrs-py/src/ensemble.rs:289-294): values (11, n_units), phase (6, n_units, n_mu) and
+ * greek (6, n_units, L + 1), in doubles. */
+void scatrs_ensemble_fixed_sizes(int64_t n_units, int64_t n_mu, int32_t greek_order,
+                                 int64_t* values_len, int64_t* phase_len, int64_t* greek_len);
+
+/*
+ * The fixed-grid ensemble of every (distribution, wavelength) unit, from HOST buffers into HOST
+ * buffers (host-device copies included).
+ *
+ * Replaces compute_batch_with_particle (scatrs/src/ensemble/mod.rs:654-686), reached from Python
+ * as _scatrs.ensemble_compute_batch (scatrs-py/src/ensemble.rs:455-504), for spheres, extended
+ * to a refractive index per (distribution, wavelength) and to a fixed size grid: the pass-2
+ * sums of scatrs/src/ensemble/engine.rs:1423-1766 on fixed nodes, the averages (1782-1836), the
+ * band projection (2310-2355) and the assembly (2396-2497).
+ *
+ *   dists[n_dist], wavelengths[n_wl], m[2 * n_dist * n_wl] (complex128: re, im, unit-major),
+ *   mu[n_mu] (cosines for the phase matrix; may be NULL with n_mu = 0),
+ *   values[11 * n_units] (c_ext, c_sca, c_abs, c_back, ssa, g, lidar_ratio, depolarization,
+ *   effective_radius, mean_area, mean_volume per unit), phase[6 * n_units * n_mu] (F11, F12,
+ *   F22, F33, F34, F44) or NULL, greek[6 * n_units * (L + 1)] (alpha1..4, beta1, beta2) or NULL.
+ */
+int scatrs_ensemble_fixed(const scatrs_distribution* dists, int64_t n_dist,
+                          const double* wavelengths, int64_t n_wl, const double* m,
+                          const double* mu, int64_t n_mu, const scatrs_fixed_options* options,
+                          double* values, double* phase, double* greek, char* err,
+                          size_t err_len);
+
+/*
+ * As scatrs_ensemble_fixed, with every array in DEVICE memory of the current device, launched
+ * on `stream` (a cudaStream_t, or NULL for the default stream). Returns after the work is
+ * enqueued and the launch checks passed; input errors found on the device (a size node outside
+ * the accepted or validated range) are reported by the NEXT call of scatrs_check_errors, which
+ * synchronizes the stream.
+ */
+int scatrs_ensemble_fixed_device(const scatrs_distribution* dists_host, int64_t n_dist,
+                                 const double* wavelengths_dev, int64_t n_wl,
+                                 const double* m_dev, const double* mu_host, int64_t n_mu,
+                                 const scatrs_fixed_options* options, double* values_dev,
+                                 double* phase_dev, double* greek_dev, void* stream, char* err,
+                                 size_t err_len);
+
+/* Synchronizes `stream` and returns the first device-side input error of the last
+ * scatrs_ensemble_fixed_device call on it (in wavelength, distribution, radius order). */
+int scatrs_check_errors(void* stream, char* err, size_t err_len);
+
+/*
+ * Mie coefficients of independent spheres, from HOST buffers: the batched Mie::compute
+ * (scatrs/src/mie/mod.rs:227-271; State::prepare and State::finish,
+ * scatrs/src/mie/kernel.rs:249-559) and MieSolution::efficiencies
+ * (scatrs/src/mie/efficiencies.rs:164-187).
+ *
+ *   x[n], m[2 * n]; n_terms[n] receives the number of terms N of each sphere (the default
+ *   truncation ceil(x + 6 x^(1/3) + 3)); coeffs (may be NULL) receives, for sphere s, a_1..a_N
+ *   then b_1..b_N as complex pairs from offset 4 * coeff_offset[s] doubles, where coeff_offset is
+ *   the caller's exclusive prefix sum of the n_terms of the first call (call once with
+ *   coeffs = NULL to size it); eff[5 * n] (may be NULL) receives Q_ext, Q_sca, Q_abs, Q_back, g.
+ */
+int scatrs_mie(const double* x, const double* m, int64_t n, int32_t allow_unvalidated,
+               int64_t* n_terms, const int64_t* coeff_offset, double* coeffs, double* eff,
+               char* err, size_t err_len);
+
+/* The CUDA device count, or -1 when the runtime is unusable. */
+int scatrs_device_count(void);
+
+/* Kernel launches made by this library since load (for the benchmark's launch count). */
+int64_t scatrs_launch_count(void);
+
+/* Per-kernel timing for profiling runs: with on = 1, every launch is bracketed by CUDA events on
+ * its stream; scatrs_kernel_times synchronizes and returns, for the kernels 0 plan_chunks,
+ * 1 mie_fixed (K-a), 2 unit (K-b/c/d), 3 mie_nodes, the total milliseconds and launch counts
+ * since the last scatrs_set_profiling call, and the number of kernels. */
+void scatrs_set_profiling(int32_t on);
+int scatrs_kernel_times(double* ms, int64_t* launches, int32_t n);
+
+/* Gauss-Legendre rule of n points on [-1, 1] (ascending nodes), as the host tables use it
+ * (scatrs/src/special/gauss_legendre.rs:188-260). */
+void scatrs_gauss_legendre(int64_t n, double* nodes, double* weights);
+
+/* Frees the cached tables and buffers of the current device. */
+void scatrs_release(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SCATRS_B200_H */

@@ -1,0 +1,181 @@
+"""ctypes binding of the CPU oracle (liboracle.so).
+
+TEST INFRASTRUCTURE ONLY. The oracle is a plain double-precision restatement of the reference
+(usask-arg/scatrs) algorithms on the size-distribution ensemble path; the parity tests, the
+smoke check and the CPU-baseline leg of the benchmark use it as the checker. Nothing in the
+product package imports this module.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(_HERE, "liboracle.so")
+_lib = None
+
+_D = ctypes.c_double
+_I64 = ctypes.c_int64
+_PD = ctypes.POINTER(ctypes.c_double)
+
+
+def build() -> str:
+    """Compiles liboracle.so if it is missing or older than its sources."""
+    srcs = [os.path.join(_HERE, f) for f in ("oracle_capi.cpp", "oracle_core.hpp", "Makefile")]
+    if not os.path.exists(_LIB) or any(os.path.getmtime(s) > os.path.getmtime(_LIB) for s in srcs):
+        subprocess.run(["make", "-C", _HERE, "CXX=g++"], check=True, capture_output=True)
+    return _LIB
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        _lib = ctypes.CDLL(_LIB)
+        _lib.orc_mie.argtypes = [_D, _D, _D, _I64, ctypes.c_int, ctypes.c_int,
+                                 ctypes.POINTER(_I64), _PD, _PD, _PD, _PD, _PD, _PD, _PD, _PD,
+                                 _PD]
+        _lib.orc_amplitudes.argtypes = [_D, _D, _D, _I64, _PD, _I64, _PD, _PD]
+        _lib.orc_gauss_legendre.argtypes = [_I64, _PD, _PD]
+        _lib.orc_gauss_legendre.restype = None
+        _lib.orc_wigner_d.argtypes = [ctypes.c_int, ctypes.c_int, _D, _I64, _PD]
+        _lib.orc_wigner_d.restype = None
+        _lib.orc_mie_greek.argtypes = [_D, _D, _D, _I64, ctypes.c_int, _PD]
+        _lib.orc_density.argtypes = [ctypes.c_int, _D, _D, _D, _D, _PD]
+        _lib.orc_density.restype = _D
+        _lib.orc_bucket.argtypes = [_I64]
+        _lib.orc_bucket.restype = _I64
+        _lib.orc_default_n_max.argtypes = [_D]
+        _lib.orc_ensemble_fixed.argtypes = [ctypes.c_void_p, _I64, _PD, _I64, _PD, _I64, _PD,
+                                            _I64, _I64, ctypes.c_int, ctypes.c_int,
+                                            ctypes.c_int, _PD, _PD, _PD, ctypes.c_char_p, _I64]
+    return _lib
+
+
+def _p(a: np.ndarray | None):
+    if a is None:
+        return None
+    return a.ctypes.data_as(_PD)
+
+
+class OracleError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"status {status}: {message}")
+        self.status = status
+
+
+def mie(x: float, m: complex, n_max: int = 0, allow_unvalidated: bool = True,
+        derivatives: bool = False) -> dict:
+    """a_n, b_n (n = 1..N), efficiencies and the absorption sum of one sphere."""
+    L = lib()
+    n = _I64(0)
+    st = L.orc_mie(x, m.real, m.imag, n_max, int(allow_unvalidated), 0, ctypes.byref(n), None,
+                   None, None, None, None, None, None, None, None)
+    if st != 0:
+        raise OracleError(st, f"mie({x}, {m})")
+    N = n.value
+    a = np.zeros(2 * N)
+    b = np.zeros(2 * N)
+    eff = np.zeros(5)
+    asum = np.zeros(1)
+    d = [np.zeros(2 * N) for _ in range(4)] if derivatives else [None] * 4
+    jac = np.zeros(3)
+    L.orc_mie(x, m.real, m.imag, n_max, int(allow_unvalidated), int(derivatives),
+              ctypes.byref(n), _p(a), _p(b), _p(eff), _p(asum), _p(d[0]), _p(d[1]), _p(d[2]),
+              _p(d[3]), _p(jac))
+    out = {
+        "a": a.view(np.complex128), "b": b.view(np.complex128),
+        "q_ext": eff[0], "q_sca": eff[1], "q_abs": eff[2], "q_back": eff[3], "g": eff[4],
+        "abs_sum": asum[0], "n": N,
+    }
+    if derivatives:
+        out.update(da_dx=d[0].view(np.complex128), da_dm=d[1].view(np.complex128),
+                   db_dx=d[2].view(np.complex128), db_dm=d[3].view(np.complex128),
+                   abs_jac=jac)
+    return out
+
+
+def amplitudes(x: float, m: complex, mu, n_max: int = 0):
+    mu = np.ascontiguousarray(mu, dtype=np.float64)
+    s1 = np.zeros(2 * mu.size)
+    s2 = np.zeros(2 * mu.size)
+    st = lib().orc_amplitudes(x, m.real, m.imag, n_max, _p(mu), mu.size, _p(s1), _p(s2))
+    if st != 0:
+        raise OracleError(st, "amplitudes")
+    return s1.view(np.complex128), s2.view(np.complex128)
+
+
+def gauss_legendre(n: int):
+    x = np.zeros(n)
+    w = np.zeros(n)
+    lib().orc_gauss_legendre(n, _p(x), _p(w))
+    return x, w
+
+
+def wigner_d(m: int, n: int, x: float, l_max: int):
+    out = np.zeros(l_max + 1)
+    lib().orc_wigner_d(m, n, x, l_max + 1, _p(out))
+    return out
+
+
+def mie_greek(x: float, m: complex, order: int, normalized: bool = True):
+    out = np.zeros(6 * (order + 1))
+    st = lib().orc_mie_greek(x, m.real, m.imag, order, int(normalized), _p(out))
+    if st != 0:
+        raise OracleError(st, "greek")
+    return out.reshape(6, order + 1)
+
+
+def density(kind: int, params, r: float):
+    p = list(params) + [0.0] * (3 - len(params))
+    g = np.zeros(3)
+    u = lib().orc_density(kind, p[0], p[1], p[2], r, _p(g))
+    return u, g
+
+
+def bucket(n: int) -> int:
+    return lib().orc_bucket(n)
+
+
+def default_n_max(x: float) -> int:
+    return lib().orc_default_n_max(x)
+
+
+DIST_DTYPE = np.dtype([("kind", np.int32), ("pad", np.int32), ("p", np.float64, 3),
+                       ("r_lo", np.float64), ("r_hi", np.float64)])
+
+
+def ensemble_fixed(dists: np.ndarray, wavelengths, m, n_nodes: int, mu=None,
+                   greek_order: int | None = None, normalized: bool = True,
+                   allow_unvalidated: bool = False, threads: int = 0) -> dict:
+    """The fixed-grid ensemble of every (distribution, wavelength) unit, distribution-major.
+
+    ``dists`` is a structured array of ``DIST_DTYPE``; ``m`` has shape (n_dist, n_wl)."""
+    dists = np.ascontiguousarray(dists, dtype=DIST_DTYPE)
+    wl = np.ascontiguousarray(wavelengths, dtype=np.float64).reshape(-1)
+    m = np.ascontiguousarray(np.broadcast_to(np.asarray(m, dtype=np.complex128),
+                                             (dists.size, wl.size)))
+    mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
+    n_units = dists.size * wl.size
+    values = np.zeros((11, n_units))
+    phase = np.zeros((6, n_units, mu.size)) if mu.size else None
+    L = -1 if greek_order is None else int(greek_order)
+    greek = np.zeros((6, n_units, L + 1)) if L >= 0 else None
+    err = ctypes.create_string_buffer(512)
+    mv = m.view(np.float64).reshape(-1)
+    st = lib().orc_ensemble_fixed(dists.ctypes.data, dists.size, _p(wl), wl.size, _p(mv),
+                                  n_nodes, _p(mu), mu.size, L, int(normalized),
+                                  int(allow_unvalidated), threads, _p(values), _p(phase),
+                                  _p(greek), err, 512)
+    if st != 0:
+        raise OracleError(st, err.value.decode())
+    out = {"values": values}
+    if phase is not None:
+        out["phase"] = phase
+    if greek is not None:
+        out["greek"] = greek
+    return out

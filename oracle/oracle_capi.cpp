@@ -1,0 +1,412 @@
+// C entry points of the CPU oracle, for the tests (ctypes) and the CPU baseline of the
+// benchmark. TEST INFRASTRUCTURE ONLY: never linked into the product library.
+#include "oracle_core.hpp"
+
+#include <cstdio>
+#include <omp.h>
+
+using namespace orc;
+
+extern "C" {
+
+int orc_default_n_max(double x) { return (int)default_n_max(x); }
+
+// Mie::compute / compute_with_derivatives (mie/mod.rs:227-271) for one sphere: with a == NULL
+// only the number of terms is returned in *n_terms. eff receives Q_ext, Q_sca, Q_abs, Q_back, g.
+int orc_mie(double x, double m_re, double m_im, int64_t n_max, int allow_unvalidated,
+            int derivatives, int64_t* n_terms, double* a, double* b, double* eff,
+            double* abs_sum, double* da_dx, double* da_dm, double* db_dx, double* db_dm,
+            double* abs_jac) {
+  int64_t n = 0;
+  std::string msg;
+  int st = check_inputs(x, m_re, m_im, n_max, allow_unvalidated != 0, &n, &msg);
+  if (st != OK) return st;
+  *n_terms = n;
+  if (!a) return OK;
+  MieState s;
+  s.solve(x, C(m_re, m_im), n, derivatives != 0);
+  for (int64_t k = 0; k < n; ++k) {
+    a[2 * k] = s.a[k].re;
+    a[2 * k + 1] = s.a[k].im;
+    b[2 * k] = s.b[k].re;
+    b[2 * k + 1] = s.b[k].im;
+    if (derivatives) {
+      da_dx[2 * k] = s.da_dx[k].re;
+      da_dx[2 * k + 1] = s.da_dx[k].im;
+      da_dm[2 * k] = s.da_dm[k].re;
+      da_dm[2 * k + 1] = s.da_dm[k].im;
+      db_dx[2 * k] = s.db_dx[k].re;
+      db_dx[2 * k + 1] = s.db_dx[k].im;
+      db_dm[2 * k] = s.db_dm[k].re;
+      db_dm[2 * k + 1] = s.db_dm[k].im;
+    }
+  }
+  Efficiencies q = efficiencies(s);
+  eff[0] = q.q_ext;
+  eff[1] = q.q_sca;
+  eff[2] = q.q_abs;
+  eff[3] = q.q_back;
+  eff[4] = q.g;
+  *abs_sum = s.abs_sum;
+  if (derivatives && abs_jac) {
+    abs_jac[0] = s.abs_sum_jacobian[0];
+    abs_jac[1] = s.abs_sum_jacobian[1];
+    abs_jac[2] = s.abs_sum_jacobian[2];
+  }
+  return OK;
+}
+
+// MieSolution::amplitudes (mie/amplitudes.rs:328-344) of the sphere (x, m) with the default
+// truncation (or n_max terms): s1, s2 interleaved re/im, one pair per cosine.
+int orc_amplitudes(double x, double m_re, double m_im, int64_t n_max, const double* mu,
+                   int64_t n_mu, double* s1, double* s2) {
+  int64_t n = 0;
+  int st = check_inputs(x, m_re, m_im, n_max, true, &n, nullptr);
+  if (st != OK) return st;
+  MieState s;
+  s.solve(x, C(m_re, m_im), n, false);
+  for (int64_t j = 0; j < n_mu; ++j) {
+    cplx a1, a2;
+    amplitudes(s.a.data(), s.b.data(), n, mu[j], &a1, &a2);
+    s1[2 * j] = a1.re;
+    s1[2 * j + 1] = a1.im;
+    s2[2 * j] = a2.re;
+    s2[2 * j + 1] = a2.im;
+  }
+  return OK;
+}
+
+void orc_gauss_legendre(int64_t n, double* nodes, double* weights) {
+  gauss_legendre(n, nodes, weights);
+}
+
+void orc_wigner_d(int m, int n, double x, int64_t len, double* out) {
+  wigner_d(m, n, x, out, len);
+}
+
+// MieSolution::greek (mie/greek.rs:386-447, 501-509): out holds alpha1..beta2, each order+1.
+int orc_mie_greek(double x, double m_re, double m_im, int64_t order, int normalized,
+                  double* out) {
+  int64_t n = 0;
+  int st = check_inputs(x, m_re, m_im, 0, true, &n, nullptr);
+  if (st != OK) return st;
+  MieState s;
+  s.solve(x, C(m_re, m_im), n, false);
+  int64_t projected = std::min(order, 2 * n);
+  int64_t nodes = n + (projected + 2) / 2;
+  std::vector<double> mu(nodes), w(nodes);
+  gauss_legendre(nodes, mu.data(), w.data());
+  std::vector<double> f(4 * nodes);
+  double c = 4.0 / (x * x);
+  for (int64_t k = 0; k < nodes; ++k) {
+    cplx a1, a2;
+    amplitudes(s.a.data(), s.b.data(), n, mu[k], &a1, &a2);
+    double e[4];
+    elements(a1, a2, e);
+    for (int i = 0; i < 4; ++i) f[i * nodes + k] = c * e[i];
+  }
+  Greek g = project(mu.data(), w.data(), nodes, projected, f.data(), f.data() + nodes,
+                    f.data() + 2 * nodes, f.data() + 3 * nodes);
+  double r0 = g.c[0][0];
+  for (auto& v : g.c)
+    for (auto& e : v) e = e / r0;
+  g.c[0][0] = 1.0;
+  if (!normalized) {
+    double q = efficiencies(s).q_sca;
+    for (auto& v : g.c)
+      for (auto& e : v) e = e * q;
+  }
+  for (int i = 0; i < 6; ++i)
+    for (int64_t l = 0; l <= order; ++l) out[i * (order + 1) + l] = l <= projected ? g.c[i][l] : 0.0;
+  return OK;
+}
+
+// Number density u(r) of a distribution (distribution.rs:370-441), with its gradient.
+double orc_density(int kind, double p0, double p1, double p2, double r, double* grad) {
+  Density d = prepare(kind, p0, p1, p2);
+  return density_eval(d, r, grad);
+}
+
+int64_t orc_bucket(int64_t n) { return bucket(n); }
+
+// ---------------------------------------------------------------------------------------
+// The fixed-grid ensemble (an extension of the reference's pass 2, engine.rs:1025-1202,
+// 1423-1766, averages 1782-1836, project 2310-2355 and assemble 2396-2497): every
+// (distribution, wavelength) unit is integrated on the same n_nodes Gauss-Legendre nodes in
+// t = ln r over [ln r_lo, ln r_hi], weights w_j u(r_j) r_j as in the reference's panels, and
+// normalized by the sum of the weights on those nodes. Nodes group into chunks of 32 in
+// ascending radius; a chunk's largest number of terms chooses its projector band, as a panel's
+// does in the reference. Units are distribution-major: unit = d * n_wl + i.
+// ---------------------------------------------------------------------------------------
+struct FixedDist {
+  int32_t kind;
+  int32_t pad;
+  double p[3];
+  double r_lo, r_hi;
+};
+
+static constexpr int NODES_PER_CHUNK = 32;
+
+struct BandData {
+  int64_t upper;
+  int64_t order;  // L_b
+  int64_t n_q;
+  std::vector<double> nodes, weights;
+  std::vector<double> ge, go;  // h x upper, row-major
+  std::vector<double> dmat[4];  // n_q x (L_b+1): (2l+1)/2 w_k d_l(mu_k)
+};
+
+static BandData make_band(int64_t upper, int64_t order) {
+  BandData b;
+  b.upper = upper;
+  b.order = std::min(order, 2 * upper);
+  b.n_q = upper + (b.order + 2) / 2;
+  b.nodes.resize(b.n_q);
+  b.weights.resize(b.n_q);
+  gauss_legendre(b.n_q, b.nodes.data(), b.weights.data());
+  int64_t lo = b.n_q / 2, h = b.n_q - lo;
+  b.ge.assign(h * upper, 0.0);
+  b.go.assign(h * upper, 0.0);
+  for (int64_t i = 0; i < h; ++i) {
+    for_each_order(b.nodes[lo + i], upper, [&](int64_t k, double pi, double tau) {
+      bool odd = k % 2 == 1;
+      b.ge[i * upper + (k - 1)] = odd ? pi : tau;
+      b.go[i * upper + (k - 1)] = odd ? tau : pi;
+    });
+  }
+  int64_t len = b.order + 1;
+  std::vector<double> buf(len);
+  const int mn[4][2] = {{0, 0}, {2, 2}, {2, -2}, {0, 2}};
+  for (int i = 0; i < 4; ++i) b.dmat[i].assign(b.n_q * len, 0.0);
+  for (int64_t k = 0; k < b.n_q; ++k) {
+    for (int i = 0; i < 4; ++i) {
+      wigner_d(mn[i][0], mn[i][1], b.nodes[k], buf.data(), len);
+      for (int64_t l = 0; l < len; ++l)
+        b.dmat[i][k * len + l] = (double)(2 * l + 1) * 0.5 * b.weights[k] * buf[l];
+    }
+  }
+  return b;
+}
+
+int orc_ensemble_fixed(const FixedDist* dists, int64_t n_dist, const double* wl, int64_t n_wl,
+                       const double* m, int64_t n_nodes, const double* mu, int64_t n_mu,
+                       int64_t greek_order, int normalized, int allow_unvalidated,
+                       int n_threads, double* values, double* phase, double* greek,
+                       char* err, int64_t err_len) {
+  const int64_t n_units = n_dist * n_wl;
+  std::vector<double> xi(n_nodes), om(n_nodes);
+  gauss_legendre(n_nodes, xi.data(), om.data());
+  // Node radii and weights per distribution.
+  std::vector<double> radius(n_dist * n_nodes), weight(n_dist * n_nodes);
+  for (int64_t d = 0; d < n_dist; ++d) {
+    Density den = prepare(dists[d].kind, dists[d].p[0], dists[d].p[1], dists[d].p[2]);
+    double a = std::log(dists[d].r_lo), b = std::log(dists[d].r_hi);
+    double c = 0.5 * (a + b), h = 0.5 * (b - a);
+    for (int64_t j = 0; j < n_nodes; ++j) {
+      double t = c + h * xi[j];
+      double w = h * om[j];
+      double r = std::exp(t);
+      double u = density_eval(den, r, nullptr);
+      radius[d * n_nodes + j] = r;
+      weight[d * n_nodes + j] = w * (u * r);
+    }
+  }
+  // Bands: every band up to the largest number of terms.
+  bool want_greek = greek_order >= 0;
+  int64_t n_max_all = 0;
+  for (int64_t d = 0; d < n_dist; ++d)
+    for (int64_t i = 0; i < n_wl; ++i) {
+      double r = radius[d * n_nodes + n_nodes - 1];
+      double x = 2.0 * PI * r / wl[i];
+      n_max_all = std::max(n_max_all, default_n_max(x));
+    }
+  std::vector<BandData> bands;
+  if (want_greek) {
+    for (int64_t u = 1;; u = (int64_t)std::ceil((double)u * 1.25)) {
+      bands.push_back(make_band(u, greek_order));
+      if (u >= n_max_all) break;
+    }
+  }
+  auto band_index = [&](int64_t n) {
+    int64_t u = bucket(n);
+    for (size_t i = 0; i < bands.size(); ++i)
+      if (bands[i].upper == u) return (int64_t)i;
+    return (int64_t)-1;
+  };
+  int64_t L = want_greek ? greek_order : 0;
+  int first_status = OK;
+  int64_t first_unit = n_units;
+  std::string first_msg;
+  if (n_threads > 0) omp_set_num_threads(n_threads);
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int64_t unit = 0; unit < n_units; ++unit) {
+    int64_t d = unit / n_wl, i = unit % n_wl;
+    double lambda = wl[i];
+    cplx mv = C(m[2 * unit], m[2 * unit + 1]);
+    std::vector<double> S(9, 0.0), Smu(4 * n_mu, 0.0);
+    std::vector<std::vector<double>> Sband(bands.size());
+    MieState st;
+    std::string msg;
+    int status = OK;
+    for (int64_t c0 = 0; c0 < n_nodes && status == OK; c0 += NODES_PER_CHUNK) {
+      int64_t c1 = std::min(n_nodes, c0 + NODES_PER_CHUNK);
+      // The chunk's band: its largest number of terms.
+      int64_t n_chunk = 0;
+      for (int64_t j = c0; j < c1; ++j) {
+        double x = 2.0 * PI * radius[d * n_nodes + j] / lambda;
+        n_chunk = std::max(n_chunk, default_n_max(x));
+      }
+      int64_t bi = want_greek ? band_index(n_chunk) : -1;
+      for (int64_t j = c0; j < c1; ++j) {
+        double r = radius[d * n_nodes + j];
+        double W = weight[d * n_nodes + j];
+        double x = 2.0 * PI * r / lambda;
+        int64_t n = 0;
+        status = check_inputs(x, mv.re, mv.im, 0, allow_unvalidated != 0, &n, &msg);
+        if (status != OK) {
+          char buf[160];
+          snprintf(buf, sizeof buf, "at wavelength %e, radius %e: ", lambda, r);
+          msg = buf + msg;
+          break;
+        }
+        st.solve(x, mv, n, false);
+        Efficiencies q = efficiencies(st);
+        double area = PI * r * r;
+        double qv[9] = {1.0,          area * q.q_ext, area * q.q_sca, area * q.q_sca * q.g,
+                        area * q.q_abs, area * q.q_back, r * r,       r * r * r,
+                        0.0};
+        for (int k = 0; k < 9; ++k) S[k] += W * qv[k];
+        double cph = 4.0 / (x * x);
+        for (int64_t k = 0; k < n_mu; ++k) {
+          cplx s1, s2;
+          amplitudes(st.a.data(), st.b.data(), n, mu[k], &s1, &s2);
+          double e[4];
+          elements(s1, s2, e);
+          for (int t = 0; t < 4; ++t) Smu[t * n_mu + k] += W * (cph * e[t] * area);
+        }
+        if (bi >= 0) {
+          BandData& B = bands[bi];
+          std::vector<double>& sb = Sband[bi];
+          if (sb.empty()) sb.assign(4 * B.n_q, 0.0);
+          int64_t q = B.n_q, lo = q / 2, h = q - lo;
+          int64_t terms = std::min(n_chunk, B.upper);
+          double scl = 4.0 / (x * x) * (PI * r * r);
+          for (int64_t ii = 0; ii < h; ++ii) {
+            // ce = G_E X and co = G_O X for this sphere's 4 columns (fast.rs:141-145), X
+            // zero beyond the sphere's own terms.
+            double ce[4] = {0, 0, 0, 0}, co[4] = {0, 0, 0, 0};
+            for (int64_t k = 0; k < terms; ++k) {
+              double xr[4] = {0, 0, 0, 0};
+              if (k < n) {
+                cplx uu = (k % 2 == 0) ? st.a[k] : st.b[k];
+                cplx vv = (k % 2 == 0) ? st.b[k] : st.a[k];
+                xr[0] = uu.re;
+                xr[1] = uu.im;
+                xr[2] = vv.re;
+                xr[3] = vv.im;
+              }
+              double ge = B.ge[ii * B.upper + k], go = B.go[ii * B.upper + k];
+              for (int t = 0; t < 4; ++t) {
+                ce[t] += ge * xr[t];
+                co[t] += go * xr[t];
+              }
+            }
+            cplx eu = C(ce[0], ce[1]), ev = C(ce[2], ce[3]);
+            cplx ou = C(co[0], co[1]), ov = C(co[2], co[3]);
+            int64_t jn = lo + ii;
+            auto write = [&](int64_t node, double sign) {
+              cplx s1 = eu + scale(ov, sign), s2 = ev + scale(ou, sign);
+              double e[4];
+              elements(s1, s2, e);
+              for (int t = 0; t < 4; ++t) sb[t * q + node] += W * (scl * e[t]);
+            };
+            write(jn, 1.0);
+            int64_t mirror = q - 1 - jn;
+            if (mirror != jn) write(mirror, -1.0);
+          }
+        }
+      }
+    }
+    double* vrow = values;  // (11, n_units)
+    if (status == OK) {
+      double z = S[0];
+      double v[9];
+      for (int k = 0; k < 9; ++k) v[k] = S[k] / z;
+      double ext = v[1], sca = v[2], scag = v[3], ab = v[4], back = v[5], r2 = v[6], r3 = v[7];
+      const char* bad = nullptr;
+      if (!(std::isfinite(ext) && ext != 0.0)) bad = "<C_ext>";
+      else if (!(std::isfinite(sca) && sca != 0.0)) bad = "<C_sca>";
+      else if (!(std::isfinite(back) && back != 0.0)) bad = "<C_back>";
+      if (bad) {
+        status = INVALID_INPUT;
+        msg = std::string("the ensemble's ") + bad + " is 0 or not finite, so its ratios are undefined (does m = 1?)";
+      } else {
+        double out[11] = {ext,       sca,        ab,       back,     sca / ext,
+                          scag / sca, (4.0 * PI) * (ext / back), 0.0, r3 / r2,
+                          PI * r2,   (4.0 * PI / 3.0) * r3};
+        for (int k = 0; k < 11; ++k) vrow[k * n_units + unit] = out[k];
+        if (phase && n_mu > 0) {
+          const int src[6] = {0, 1, 0, 2, 3, 2};
+          for (int e = 0; e < 6; ++e)
+            for (int64_t k = 0; k < n_mu; ++k) {
+              double f = Smu[src[e] * n_mu + k] / z;
+              phase[(e * n_units + unit) * n_mu + k] = normalized ? f / sca : f;
+            }
+        }
+        if (greek && want_greek) {
+          std::vector<double> g(6 * (L + 1), 0.0);
+          for (size_t bi = 0; bi < bands.size(); ++bi) {
+            if (Sband[bi].empty()) continue;
+            BandData& B = bands[bi];
+            int64_t q = B.n_q, len = B.order + 1;
+            std::vector<double> f(4 * q);
+            for (int64_t k = 0; k < 4 * q; ++k) f[k] = Sband[bi][k] / z;
+            const double* f11 = f.data();
+            const double* f12 = f.data() + q;
+            const double* f33 = f.data() + 2 * q;
+            const double* f34 = f.data() + 3 * q;
+            for (int64_t l = 0; l < len; ++l) {
+              double a1 = 0, a4 = 0, p = 0, mi = 0, b1 = 0, b2 = 0;
+              for (int64_t k = 0; k < q; ++k) {
+                double d00 = B.dmat[0][k * len + l], d22 = B.dmat[1][k * len + l];
+                double d2m2 = B.dmat[2][k * len + l], d02 = B.dmat[3][k * len + l];
+                a1 += f11[k] * d00;
+                a4 += f33[k] * d00;
+                p += (f11[k] + f33[k]) * d22;
+                mi += (f11[k] - f33[k]) * d2m2;
+                b1 += f12[k] * d02;
+                b2 += f34[k] * d02;
+              }
+              double c6[6] = {a1, (p + mi) * 0.5, (p - mi) * 0.5, a4, b1, b2};
+              for (int e = 0; e < 6; ++e) g[e * (L + 1) + l] += c6[e];
+            }
+          }
+          if (normalized) {
+            double a0 = g[0];
+            for (auto& e : g) e = e / a0;
+            g[0] = 1.0;
+          }
+          for (int e = 0; e < 6; ++e)
+            for (int64_t l = 0; l <= L; ++l)
+              greek[(e * n_units + unit) * (L + 1) + l] = g[e * (L + 1) + l];
+        }
+      }
+    }
+    if (status != OK) {
+#pragma omp critical
+      {
+        if (unit < first_unit) {
+          first_unit = unit;
+          first_status = status;
+          first_msg = msg;
+        }
+      }
+    }
+  }
+  if (first_status != OK && err && err_len > 0) {
+    snprintf(err, err_len, "%s", first_msg.c_str());
+  }
+  return first_status;
+}
+
+}  // extern "C"

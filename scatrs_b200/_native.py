@@ -1,0 +1,184 @@
+"""ctypes binding of libscatrs_b200.so (the C ABI of include/scatrs_b200.h).
+
+The library is the only compute path: if it is missing, or no CUDA device is usable, the calls
+raise instead of falling back to anything else.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from .errors import DeviceError, raise_for
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libscatrs_b200.so")
+
+_D = ctypes.c_double
+_I32 = ctypes.c_int32
+_I64 = ctypes.c_int64
+_PD = ctypes.POINTER(ctypes.c_double)
+_PI64 = ctypes.POINTER(ctypes.c_int64)
+_VP = ctypes.c_void_p
+_CP = ctypes.c_char_p
+_SZ = ctypes.c_size_t
+
+DIST_DTYPE = np.dtype([("kind", np.int32), ("reserved", np.int32), ("param", np.float64, 3),
+                       ("r_lo", np.float64), ("r_hi", np.float64)])
+KINDS = {"lognormal": 1, "gamma": 2, "modified_gamma": 3, "power_law": 4}
+
+
+class FixedOptions(ctypes.Structure):
+    _fields_ = [("n_nodes", _I32), ("greek_order", _I32), ("normalized", _I32),
+                ("allow_unvalidated", _I32)]
+
+
+# Every symbol the header declares, with (restype, argtypes).
+SYMBOLS = {
+    "scatrs_ensemble_fixed_sizes": (None, [_I64, _I64, _I32, _PI64, _PI64, _PI64]),
+    "scatrs_ensemble_fixed": (ctypes.c_int, [_VP, _I64, _PD, _I64, _PD, _PD, _I64,
+                                             ctypes.POINTER(FixedOptions), _PD, _PD, _PD, _CP,
+                                             _SZ]),
+    "scatrs_ensemble_fixed_device": (ctypes.c_int, [_VP, _I64, _VP, _I64, _VP, _PD, _I64,
+                                                    ctypes.POINTER(FixedOptions), _VP, _VP, _VP,
+                                                    _VP, _CP, _SZ]),
+    "scatrs_check_errors": (ctypes.c_int, [_VP, _CP, _SZ]),
+    "scatrs_mie": (ctypes.c_int, [_PD, _PD, _I64, _I32, _PI64, _PI64, _PD, _PD, _CP, _SZ]),
+    "scatrs_device_count": (ctypes.c_int, []),
+    "scatrs_launch_count": (_I64, []),
+    "scatrs_gauss_legendre": (None, [_I64, _PD, _PD]),
+    "scatrs_release": (None, []),
+    "scatrs_set_profiling": (None, [_I32]),
+    "scatrs_kernel_times": (ctypes.c_int, [_PD, _PI64, _I32]),
+}
+
+KERNEL_NAMES = ("plan_chunks_kernel", "mie_fixed_kernel", "unit_kernel", "mie_nodes_kernel")
+
+_lib = None
+
+
+def load() -> ctypes.CDLL:
+    """The library (loaded once); raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise DeviceError(f"{LIB_PATH} is missing: build it with python -m scatrs_b200.build")
+        lib = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SYMBOLS.items():
+            f = getattr(lib, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def require_device() -> None:
+    n = load().scatrs_device_count()
+    if n <= 0:
+        raise DeviceError("no usable CUDA device: the ensemble path runs on the GPU only")
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(_PD)
+
+
+def _check(status: int, buf) -> None:
+    raise_for(status, buf.value.decode(errors="replace"))
+
+
+def gauss_legendre(n: int):
+    x = np.zeros(n)
+    w = np.zeros(n)
+    load().scatrs_gauss_legendre(n, _p(x), _p(w))
+    return x, w
+
+
+def launch_count() -> int:
+    return int(load().scatrs_launch_count())
+
+
+def set_profiling(on: bool) -> None:
+    load().scatrs_set_profiling(int(on))
+
+
+def kernel_times() -> dict:
+    """{kernel: (total ms, launches)} since set_profiling (synchronizes)."""
+    ms = np.zeros(8)
+    n = np.zeros(8, dtype=np.int64)
+    k = load().scatrs_kernel_times(_p(ms), n.ctypes.data_as(_PI64), 8)
+    return {KERNEL_NAMES[i]: (float(ms[i]), int(n[i])) for i in range(k)}
+
+
+def mie(x, m, allow_unvalidated: bool = False):
+    """Coefficients and efficiencies of independent spheres on the GPU (batched Mie::compute):
+    a list of (a, b) complex arrays and an (n, 5) array of Q_ext, Q_sca, Q_abs, Q_back, g."""
+    require_device()
+    x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1)
+    m = np.ascontiguousarray(np.broadcast_to(np.asarray(m, dtype=np.complex128), x.shape))
+    n = x.size
+    nt = np.zeros(n, dtype=np.int64)
+    err = ctypes.create_string_buffer(512)
+    mv = m.view(np.float64)
+    st = load().scatrs_mie(_p(x), _p(mv), n, int(allow_unvalidated), nt.ctypes.data_as(_PI64),
+                           None, None, None, err, 512)
+    _check(st, err)
+    off = np.zeros(n, dtype=np.int64)
+    off[1:] = np.cumsum(nt)[:-1]
+    coeffs = np.zeros(4 * int(nt.sum()))
+    eff = np.zeros(5 * n)
+    st = load().scatrs_mie(_p(x), _p(mv), n, int(allow_unvalidated), nt.ctypes.data_as(_PI64),
+                           off.ctypes.data_as(_PI64), _p(coeffs), _p(eff), err, 512)
+    _check(st, err)
+    c = coeffs.view(np.complex128)
+    out = []
+    for i in range(n):
+        o, k = 2 * off[i], nt[i]
+        out.append((c[o:o + k], c[o + k:o + 2 * k]))
+    return out, eff.reshape(n, 5)
+
+
+def ensemble_fixed(dists: np.ndarray, wavelengths, m, mu, n_nodes: int, greek_order: int = -1,
+                   normalized: bool = True, allow_unvalidated: bool = False):
+    """The fixed-grid ensemble from host arrays; returns (values, phase or None, greek or None)
+    shaped (11, n), (6, n, n_mu), (6, n, L + 1) with n = n_dist * n_wl, distribution-major."""
+    require_device()
+    dists = np.ascontiguousarray(dists, dtype=DIST_DTYPE)
+    wl = np.ascontiguousarray(wavelengths, dtype=np.float64).reshape(-1)
+    m = np.ascontiguousarray(np.broadcast_to(np.asarray(m, dtype=np.complex128),
+                                             (dists.size, wl.size)))
+    mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
+    n = dists.size * wl.size
+    opts = FixedOptions(int(n_nodes), int(greek_order), int(normalized), int(allow_unvalidated))
+    values = np.zeros((11, n))
+    phase = np.zeros((6, n, mu.size)) if mu.size else None
+    greek = np.zeros((6, n, greek_order + 1)) if greek_order >= 0 else None
+    err = ctypes.create_string_buffer(1024)
+    st = load().scatrs_ensemble_fixed(dists.ctypes.data, dists.size, _p(wl), wl.size,
+                                      _p(m.view(np.float64)), _p(mu), mu.size,
+                                      ctypes.byref(opts), _p(values), _p(phase), _p(greek), err,
+                                      1024)
+    _check(st, err)
+    return values, phase, greek
+
+
+def ensemble_fixed_device(dists: np.ndarray, wl_ptr: int, n_wl: int, m_ptr: int, mu, n_nodes: int,
+                          greek_order: int, normalized: bool, values_ptr: int, phase_ptr: int,
+                          greek_ptr: int, stream: int = 0, allow_unvalidated: bool = False):
+    """The fixed-grid ensemble on device arrays (raw pointers, e.g. torch's data_ptr()),
+    enqueued on `stream`; device-side input errors surface in check_errors(stream)."""
+    dists = np.ascontiguousarray(dists, dtype=DIST_DTYPE)
+    mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
+    opts = FixedOptions(int(n_nodes), int(greek_order), int(normalized), int(allow_unvalidated))
+    err = ctypes.create_string_buffer(1024)
+    st = load().scatrs_ensemble_fixed_device(dists.ctypes.data, dists.size, wl_ptr, n_wl, m_ptr,
+                                             _p(mu), mu.size, ctypes.byref(opts), values_ptr,
+                                             phase_ptr or None, greek_ptr or None, stream or None,
+                                             err, 1024)
+    _check(st, err)
+
+
+def check_errors(stream: int = 0) -> None:
+    err = ctypes.create_string_buffer(1024)
+    _check(load().scatrs_check_errors(stream or None, err, 1024), err)

@@ -1,0 +1,120 @@
+"""The reference's binding surface for the ensemble path (scatrs-py/src/ensemble.rs), backed by
+the GPU library.
+
+* ``ensemble_parameters(items, mixture)``: the parameter names of ensemble.rs:172-188.
+* ``ensemble_compute_fixed(specs, particle_spec, wavelengths, greek, all_orders, mu,
+  normalized, n_nodes, spread, allow_unvalidated)``: the batch call of ensemble.rs:455-504 on a
+  fixed size grid, returning the same dict (values/errors (11, n), d/d_errors (0, 11, n),
+  greek* (6, n, L + 1), phase* (6, n, n_mu), converged (n), panels (n)), rows
+  distribution-major. The particle spec is ("sphere", m) with m of shape (n_wl,) as in the
+  reference, or (n_dist, n_wl) for a refractive index per distribution and wavelength.
+
+Errors are those of the reference's Python package (scatrs_b200.errors).
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+from . import _native
+from .errors import InvalidInputError
+
+_PARAMS = {
+    "lognormal": ("median_radius", "width"),
+    "gamma": ("effective_radius", "effective_variance"),
+    "modified_gamma": ("alpha", "b", "gamma"),
+    "power_law": ("exponent",),
+    "monodisperse": ("radius",),
+    "tabulated": (),
+}
+
+
+def ensemble_parameters(items, mixture: bool) -> list[str]:
+    """Parameter names in the order ensemble_compute indexes them (scatrs/src/ensemble/mod.rs:
+    254-337): the distribution's, then the particle's, then the weight in a mixture."""
+    if not items:
+        return []
+    if not mixture and len(items) != 1:
+        raise InvalidInputError(
+            f"a single distribution needs exactly one component, got {len(items)}")
+    out = []
+    for ci, (spec, particle, _w) in enumerate(items):
+        prefix = f"c{ci}." if mixture else ""
+        kind = spec[0]
+        if kind == "multimodal":
+            for j, (_v, mode) in enumerate(spec[1]):
+                out += [f"{prefix}mode{j}.{n}" for n in _PARAMS[mode[0]]]
+                out.append(f"{prefix}mode{j}.weight")
+        elif kind in _PARAMS:
+            out += [prefix + n for n in _PARAMS[kind]]
+        else:
+            raise TypeError(f"unknown distribution kind {kind!r}")
+        pk = particle[0]
+        if pk == "sphere":
+            out += [prefix + "m_real", prefix + "m_imag"]
+        elif pk == "spheroid":
+            out += [prefix + "m_real", prefix + "m_imag", prefix + "aspect_ratio"]
+        elif pk == "layered":
+            layers = np.asarray(particle[2]).shape[0]
+            for layer in range(layers):
+                out += [f"{prefix}layer{layer}.m_real", f"{prefix}layer{layer}.m_imag"]
+            for layer in range(np.asarray(particle[1]).size):
+                out.append(f"{prefix}layer{layer}.radius_fraction")
+        else:
+            raise TypeError(f"unknown particle kind {pk!r}")
+        if mixture:
+            out.append(prefix + "weight")
+    return out
+
+
+def _dist_array(specs, spread: float, ranges=None) -> np.ndarray:
+    d = np.zeros(len(specs), dtype=_native.DIST_DTYPE)
+    for k, spec in enumerate(specs):
+        if not isinstance(spec, tuple):
+            raise TypeError("a distribution spec must be a tuple")
+        kind = spec[0]
+        if kind not in _native.KINDS:
+            raise TypeError(f"unknown distribution kind {kind!r}")
+        p = [float(v) for v in spec[1:]]
+        d[k]["kind"] = _native.KINDS[kind]
+        d[k]["param"][: len(p)] = p
+        if ranges is not None:
+            d[k]["r_lo"], d[k]["r_hi"] = ranges[k]
+        elif kind == "lognormal":
+            d[k]["r_lo"] = p[0] * p[1] ** (-spread)
+            d[k]["r_hi"] = p[0] * p[1] ** spread
+        elif kind == "power_law":
+            d[k]["r_lo"], d[k]["r_hi"] = p[1], p[2]
+        else:
+            raise InvalidInputError(f"a {kind} distribution needs an explicit grid range")
+    return d
+
+
+def ensemble_compute_fixed(specs, particle_spec, wavelengths, greek, all_orders, mu, normalized,
+                           n_nodes: int = 256, spread: float = 5.0, allow_unvalidated=False,
+                           ranges=None) -> dict:
+    if not isinstance(particle_spec, tuple) or particle_spec[0] != "sphere":
+        raise TypeError("the fixed-grid ensemble takes ('sphere', m)")
+    if all_orders:
+        raise InvalidInputError("the fixed-grid ensemble needs a finite Greek order")
+    wl = np.ascontiguousarray(wavelengths, dtype=np.float64).reshape(-1)
+    dists = _dist_array(specs, spread, ranges)
+    m = np.asarray(particle_spec[1], dtype=np.complex128)
+    if m.ndim == 1:
+        m = np.broadcast_to(m, (dists.size, wl.size))
+    mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
+    L = -1 if greek is None else int(greek)
+    values, phase, g = _native.ensemble_fixed(dists, wl, m, mu, n_nodes, L, bool(normalized),
+                                              bool(allow_unvalidated))
+    n = values.shape[1]
+    out = {"values": values, "errors": np.zeros_like(values), "d": np.zeros((0, 11, n)),
+           "d_errors": np.zeros((0, 11, n))}
+    for prefix, arr in (("greek", g), ("phase", phase)):
+        if arr is not None:
+            out[prefix] = arr
+            out[f"{prefix}_errors"] = np.zeros_like(arr)
+            out[f"{prefix}_d"] = np.zeros((0,) + arr.shape)
+            out[f"{prefix}_d_errors"] = np.zeros((0,) + arr.shape)
+    out["converged"] = np.ones(n, dtype=bool)
+    out["panels"] = np.zeros(n, dtype=np.uint64)
+    return out

@@ -1,0 +1,785 @@
+// The C ABI of include/scatrs_b200.h: input checks, the cached tables, slab planning and the
+// launches of K-a (mie_kernels.cu) and K-b/c/d (unit_kernel.cu).
+//
+// A call of the fixed-grid ensemble runs, per device and in one stream:
+//   1. the node table (radii and weights w_j u(r_j) r_j per distribution) on the host;
+//   2. plan_chunks: each chunk's largest number of terms N_c, copied back to the host, which
+//      picks the projector bands, grows the tables if needed, and cuts the units into slabs
+//      whose coefficient rows fit the arena;
+//   3. per slab, K-a (one warp per chunk) then the unit kernel (one persistent CTA per SM slot).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/scatrs_b200.h"
+#include "kernels.h"
+#include "tables.h"
+
+namespace sb {
+
+static std::atomic<int64_t> g_launches{0};
+
+// Optional per-kernel timing: CUDA events recorded around each launch on its stream, read back
+// by scatrs_kernel_times (which synchronizes). Off unless scatrs_set_profiling(1).
+enum KernelId { K_PLAN = 0, K_MIE = 1, K_UNITS = 2, K_NODES = 3, K_COUNT = 4 };
+static bool g_profiling = false;
+struct Timed {
+  int id;
+  cudaEvent_t a, b;
+};
+static std::vector<Timed> g_timed;
+static double g_kernel_ms[K_COUNT];
+static int64_t g_kernel_launches[K_COUNT];
+
+template <class F>
+static void timed_launch(int id, cudaStream_t s, F f) {
+  if (!g_profiling) {
+    f();
+    g_launches++;
+    return;
+  }
+  Timed t{id, nullptr, nullptr};
+  cudaEventCreate(&t.a);
+  cudaEventCreate(&t.b);
+  cudaEventRecord(t.a, s);
+  f();
+  cudaEventRecord(t.b, s);
+  g_timed.push_back(t);
+  g_launches++;
+}
+
+namespace {
+
+constexpr int64_t kMaxGreekOrder = 1 << 21;        // MAX_GREEK_ORDER (mie/greek.rs:344)
+constexpr int64_t kMaxMieValues = 1 << 27;         // scatrs-py/src/mie.rs:30
+constexpr int64_t kArenaRows = 1 << 20;            // coefficient rows per slab (1 KiB each)
+constexpr int64_t kMaxSlabChunks = 1 << 16;        // chunks per slab
+
+struct Failure {
+  int status;
+  std::string msg;
+};
+
+void set_err(char* err, size_t len, const std::string& msg) {
+  if (err && len > 0) {
+    size_t n = std::min(len - 1, msg.size());
+    memcpy(err, msg.data(), n);
+    err[n] = 0;
+  }
+}
+
+#define SB_CUDA(call)                                                                        \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess)                                                                   \
+      throw Failure{SCATRS_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)};        \
+  } while (0)
+
+int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
+
+// A grow-only device buffer.
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+  void* get(size_t bytes) {
+    if (bytes > cap) {
+      if (p) cudaFree(p);
+      p = nullptr;
+      cap = 0;
+      size_t want = std::max<size_t>(bytes, 256);
+      SB_CUDA(cudaMalloc(&p, want));
+      cap = want;
+    }
+    return p;
+  }
+  template <class T>
+  T* as(size_t count) {
+    return static_cast<T*>(get(count * sizeof(T)));
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+};
+
+// Tables of the requested cosines: one row per cosine c (or per pair c, -c), G_E and G_O of
+// orders 1..ld.
+struct UserTables {
+  std::vector<double> mu;
+  int64_t n_orders = 0;
+  int h = 0, h_pad = 0, ld = 0;
+  DevBuf ge, go, map;
+};
+
+struct BandTables {
+  int order = -1;
+  int n_bands = 0;
+  int nq_max = 0;
+  std::vector<BandDesc> desc;
+  std::vector<double> ge, go, d;  // host copies, appended band by band
+  DevBuf ge_d, go_d, d_d, desc_d;
+};
+
+struct Context {
+  int device = -1;
+  int sms = 0;
+  int unit_bps = 1;
+  std::mutex mtx;
+  UserTables user;
+  std::map<int, BandTables> bands;  // by Greek order
+  std::map<int64_t, std::pair<std::vector<double>, std::vector<double>>> rules;
+  DevBuf radius, weight, wl, m, chunk_n, chunk_row, chunk_order, unit_order, X, uz, ux,
+      chunk_sums, err, acc, counter, values, phase, greek;
+  std::vector<int> chunk_n_host;
+  int* pinned_chunk_n = nullptr;
+  size_t pinned_cap = 0;
+};
+
+std::mutex g_ctx_mtx;
+std::vector<std::unique_ptr<Context>> g_ctx;
+
+Context& context() {
+  int dev = 0;
+  SB_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(g_ctx_mtx);
+  if ((int)g_ctx.size() <= dev) g_ctx.resize(dev + 1);
+  if (!g_ctx[dev]) {
+    auto c = std::make_unique<Context>();
+    c->device = dev;
+    cudaDeviceProp prop;
+    SB_CUDA(cudaGetDeviceProperties(&prop, dev));
+    c->sms = prop.multiProcessorCount;
+    c->unit_bps = unit_kernel_blocks_per_sm();
+    g_ctx[dev] = std::move(c);
+  }
+  return *g_ctx[dev];
+}
+
+const std::pair<std::vector<double>, std::vector<double>>& rule(Context& c, int64_t n) {
+  auto it = c.rules.find(n);
+  if (it != c.rules.end()) return it->second;
+  std::vector<double> x(n), w(n);
+  gauss_legendre(n, x.data(), w.data());
+  return c.rules.emplace(n, std::make_pair(std::move(x), std::move(w))).first->second;
+}
+
+// The tables of the requested cosines, for orders 1..n_orders at least.
+void ensure_user(Context& c, const double* mu, int64_t n_mu, int64_t n_orders, cudaStream_t s) {
+  UserTables& u = c.user;
+  bool same = (int64_t)u.mu.size() == n_mu && u.n_orders >= n_orders &&
+              (n_mu == 0 || memcmp(u.mu.data(), mu, n_mu * sizeof(double)) == 0);
+  if (same) return;
+  u.mu.assign(mu, mu + n_mu);
+  u.n_orders = std::max<int64_t>(round_up(std::max<int64_t>(n_orders, 1), 16), u.n_orders);
+  // Pair each cosine with its exact negative where the list has one.
+  std::unordered_multimap<uint64_t, int> by_bits;
+  for (int j = 0; j < n_mu; ++j) {
+    uint64_t b;
+    memcpy(&b, &mu[j], 8);
+    by_bits.emplace(b, j);
+  }
+  std::vector<char> used(n_mu, 0);
+  std::vector<double> cosines;
+  std::vector<int2> map;
+  for (int j = 0; j < n_mu; ++j) {
+    if (used[j]) continue;
+    used[j] = 1;
+    int partner = -1;
+    double neg = -mu[j];
+    uint64_t nb;
+    memcpy(&nb, &neg, 8);
+    auto range = by_bits.equal_range(nb);
+    for (auto it = range.first; it != range.second; ++it)
+      if (!used[it->second]) {
+        partner = it->second;
+        break;
+      }
+    if (mu[j] == 0.0 && partner < 0) {
+      // +0 and -0 are the same cosine.
+      for (int k = j + 1; k < n_mu; ++k)
+        if (!used[k] && mu[k] == 0.0) {
+          partner = k;
+          break;
+        }
+    }
+    if (partner >= 0) used[partner] = 1;
+    cosines.push_back(mu[j]);
+    map.push_back(make_int2(j, partner));
+  }
+  u.h = (int)cosines.size();
+  u.h_pad = (int)round_up(std::max(u.h, 1), 32);
+  u.ld = (int)u.n_orders;
+  std::vector<double> ge((size_t)u.h_pad * u.ld, 0.0), go((size_t)u.h_pad * u.ld, 0.0);
+  for (int r = 0; r < u.h; ++r)
+    pi_tau_row(cosines[r], u.n_orders, &ge[(size_t)r * u.ld], &go[(size_t)r * u.ld]);
+  SB_CUDA(cudaMemcpyAsync(u.ge.get(ge.size() * 8), ge.data(), ge.size() * 8,
+                          cudaMemcpyHostToDevice, s));
+  SB_CUDA(cudaMemcpyAsync(u.go.get(go.size() * 8), go.data(), go.size() * 8,
+                          cudaMemcpyHostToDevice, s));
+  if (!map.empty())
+    SB_CUDA(cudaMemcpyAsync(u.map.get(map.size() * sizeof(int2)), map.data(),
+                            map.size() * sizeof(int2), cudaMemcpyHostToDevice, s));
+  SB_CUDA(cudaStreamSynchronize(s));
+}
+
+// Bands 0..last_band for Greek order L (engine.rs:2034-2072).
+BandTables& ensure_bands(Context& c, int L, int last_band, cudaStream_t s) {
+  BandTables& bt = c.bands[L];
+  bt.order = L;
+  if (bt.n_bands > last_band) return bt;
+  for (int b = bt.n_bands; b <= last_band; ++b) {
+    int64_t upper = band_upper(b);
+    int64_t order = std::min<int64_t>(L, 2 * upper);
+    int64_t n_q = upper + (order + 2) / 2;
+    const auto& r = rule(c, n_q);
+    BandDesc d;
+    d.upper = (int)upper;
+    d.order = (int)order;
+    d.n_q = (int)n_q;
+    int64_t lo = n_q / 2;
+    d.h = (int)(n_q - lo);
+    d.h_pad = (int)round_up(d.h, 32);
+    d.ld = (int)round_up(upper, 16);
+    d.g_off = (int64_t)bt.ge.size();
+    d.d_off = (int64_t)bt.d.size();
+    bt.ge.resize(bt.ge.size() + (size_t)d.h_pad * d.ld, 0.0);
+    bt.go.resize(bt.go.size() + (size_t)d.h_pad * d.ld, 0.0);
+    for (int i = 0; i < d.h; ++i)
+      pi_tau_row(r.first[lo + i], upper, &bt.ge[d.g_off + (size_t)i * d.ld],
+                 &bt.go[d.g_off + (size_t)i * d.ld]);
+    int64_t len = order + 1;
+    bt.d.resize(bt.d.size() + 4 * (size_t)n_q * len);
+    std::vector<double> buf(len);
+    const int mn[4][2] = {{0, 0}, {2, 2}, {2, -2}, {0, 2}};
+    for (int f = 0; f < 4; ++f)
+      for (int64_t k = 0; k < n_q; ++k) {
+        wigner_d(mn[f][0], mn[f][1], r.first[k], buf.data(), len);
+        double* dst = &bt.d[d.d_off + ((size_t)f * n_q + k) * len];
+        for (int64_t l = 0; l < len; ++l) dst[l] = (double)(2 * l + 1) * 0.5 * r.second[k] * buf[l];
+      }
+    bt.desc.push_back(d);
+    bt.nq_max = std::max(bt.nq_max, d.n_q);
+  }
+  bt.n_bands = last_band + 1;
+  SB_CUDA(cudaMemcpyAsync(bt.ge_d.get(bt.ge.size() * 8), bt.ge.data(), bt.ge.size() * 8,
+                          cudaMemcpyHostToDevice, s));
+  SB_CUDA(cudaMemcpyAsync(bt.go_d.get(bt.go.size() * 8), bt.go.data(), bt.go.size() * 8,
+                          cudaMemcpyHostToDevice, s));
+  SB_CUDA(cudaMemcpyAsync(bt.d_d.get(bt.d.size() * 8), bt.d.data(), bt.d.size() * 8,
+                          cudaMemcpyHostToDevice, s));
+  SB_CUDA(cudaMemcpyAsync(bt.desc_d.get(bt.desc.size() * sizeof(BandDesc)), bt.desc.data(),
+                          bt.desc.size() * sizeof(BandDesc), cudaMemcpyHostToDevice, s));
+  SB_CUDA(cudaStreamSynchronize(s));
+  return bt;
+}
+
+void check_options(const scatrs_fixed_options* o, int64_t n_units, int64_t n_mu,
+                   const double* mu) {
+  if (!o) throw Failure{SCATRS_INVALID_INPUT, "options must not be NULL"};
+  if (o->n_nodes < 1) throw Failure{SCATRS_INVALID_INPUT, "n_nodes must be >= 1"};
+  if (o->greek_order < -1 || o->greek_order > kMaxGreekOrder)
+    throw Failure{SCATRS_INVALID_INPUT, "the Greek order must be at most 2097152"};
+  if (n_mu < 0) throw Failure{SCATRS_INVALID_INPUT, "n_mu must be >= 0"};
+  for (int64_t j = 0; j < n_mu; ++j)
+    if (!(std::isfinite(mu[j]) && mu[j] >= -1.0 && mu[j] <= 1.0))
+      throw Failure{SCATRS_INVALID_INPUT,
+                    "a cosine of the scattering angle must be finite and in [-1, 1]"};
+  // The output bound of scatrs-py/src/ensemble.rs:388-399.
+  int64_t per = 11 + 4 * n_mu + (o->greek_order >= 0 ? 6 * ((int64_t)o->greek_order + 1) : 0);
+  if ((double)n_units * (double)per * 2.0 > 2.0 * (double)kMaxMieValues)
+    throw Failure{SCATRS_INVALID_INPUT,
+                  "the ensemble outputs would exceed 2 * MAX_MIE_VALUES = 268435456 real values"};
+}
+
+std::string node_message(int status, double lambda, double r) {
+  char buf[256];
+  snprintf(buf, sizeof buf, "at wavelength %e, radius %e: %s", lambda, r,
+           status == 3 ? "the size parameter and refractive index are outside the validated "
+                         "domain x in [1e-06, 2e4], 0 < Re m <= 10, 0 <= Im m <= 10, |m| >= 0.1"
+                       : "the size parameter x must be in [1e-30, 1e6] and the refractive "
+                         "index finite with Re m >= 0, Im m >= 0 and |m| in [1e-6, 1e3]");
+  return buf;
+}
+
+struct FixedCall {
+  // Host copies needed for error messages.
+  std::vector<double> radius;  // [n_dist][n_nodes]
+  std::vector<double> wl_host;
+  int64_t n_dist = 0, n_wl = 0, n_nodes = 0;
+};
+
+// The device pipeline; wl_dev and m_dev are device arrays, outputs device arrays.
+void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, const double* wl_dev,
+               int64_t n_wl, const double* m_dev, const double* mu, int64_t n_mu,
+               const scatrs_fixed_options* opt, double* values, double* phase, double* greek,
+               cudaStream_t s, FixedCall* call) {
+  const int64_t n_units = n_dist * n_wl;
+  check_options(opt, n_units, n_mu, mu);
+  if (n_units == 0) return;
+  const int64_t n_nodes = opt->n_nodes;
+  const int cpu = (int)((n_nodes + 31) / 32);
+  const int64_t n_chunks = n_units * cpu;
+  if (n_chunks > (int64_t)INT32_MAX / 32)
+    throw Failure{SCATRS_INVALID_INPUT, "too many (distribution, wavelength, node) triples"};
+  // 1. Node table.
+  const auto& gl = rule(c, n_nodes);
+  std::vector<double> radius(n_dist * n_nodes), weight(n_dist * n_nodes);
+  for (int64_t d = 0; d < n_dist; ++d) {
+    std::string msg;
+    if (!validate_distribution(dists[d].kind, dists[d].param, &msg))
+      throw Failure{SCATRS_INVALID_INPUT, "distribution " + std::to_string(d) + ": " + msg};
+    if (!(dists[d].r_lo > 0.0 && dists[d].r_hi > dists[d].r_lo && std::isfinite(dists[d].r_hi)))
+      throw Failure{SCATRS_INVALID_INPUT, "distribution " + std::to_string(d) +
+                                              ": the grid needs 0 < r_lo < r_hi < inf"};
+    double a = std::log(dists[d].r_lo), b = std::log(dists[d].r_hi);
+    double ctr = 0.5 * (a + b), h = 0.5 * (b - a);
+    for (int64_t j = 0; j < n_nodes; ++j) {
+      double t = ctr + h * gl.first[j];
+      double r = std::exp(t);
+      double u = density(dists[d].kind, dists[d].param, r);
+      radius[d * n_nodes + j] = r;
+      weight[d * n_nodes + j] = h * gl.second[j] * (u * r);
+    }
+  }
+  SB_CUDA(cudaMemcpyAsync(c.radius.get(radius.size() * 8), radius.data(), radius.size() * 8,
+                          cudaMemcpyHostToDevice, s));
+  SB_CUDA(cudaMemcpyAsync(c.weight.get(weight.size() * 8), weight.data(), weight.size() * 8,
+                          cudaMemcpyHostToDevice, s));
+  unsigned long long* err = c.err.as<unsigned long long>(2);
+  SB_CUDA(cudaMemsetAsync(err, 0xff, 2 * sizeof(unsigned long long), s));
+  // 2. Plan.
+  MieFixedArgs ka{};
+  ka.radius = c.radius.as<double>(0);
+  ka.weight = c.weight.as<double>(0);
+  ka.wl = wl_dev;
+  ka.m = reinterpret_cast<const double2*>(m_dev);
+  ka.n_dist = (int)n_dist;
+  ka.n_wl = (int)n_wl;
+  ka.n_nodes = (int)n_nodes;
+  ka.cpu = cpu;
+  ka.unit0 = 0;
+  ka.n_chunks = (int)n_chunks;
+  int* chunk_n = c.chunk_n.as<int>(n_chunks);
+  ka.chunk_n = chunk_n;
+  ka.err = err;
+  ka.allow_unvalidated = opt->allow_unvalidated;
+  timed_launch(K_PLAN, s, [&] { launch_plan_chunks(ka, s); });
+  SB_CUDA(cudaGetLastError());
+  if (c.pinned_cap < (size_t)n_chunks) {
+    if (c.pinned_chunk_n) cudaFreeHost(c.pinned_chunk_n);
+    c.pinned_chunk_n = nullptr;
+    c.pinned_cap = 0;
+    SB_CUDA(cudaMallocHost(&c.pinned_chunk_n, n_chunks * sizeof(int)));
+    c.pinned_cap = n_chunks;
+  }
+  int* cn = c.pinned_chunk_n;
+  SB_CUDA(cudaMemcpyAsync(cn, chunk_n, n_chunks * sizeof(int), cudaMemcpyDeviceToHost, s));
+  SB_CUDA(cudaStreamSynchronize(s));
+  int n_max = 0;
+  for (int64_t k = 0; k < n_chunks; ++k) n_max = std::max(n_max, cn[k]);
+  // Tables.
+  const int L = opt->greek_order;
+  ensure_user(c, mu, n_mu, std::max(n_max, 1), s);
+  BandTables* bt = nullptr;
+  if (L >= 0) bt = &ensure_bands(c, L, band_index(std::max(n_max, 1)), s);
+  // 3. Slabs of whole units whose coefficient rows fit the arena.
+  std::vector<int64_t> rows(n_chunks);
+  const int64_t arena = std::max<int64_t>(kArenaRows, (int64_t)cpu * n_max);
+  double* X = c.X.as<double>((size_t)arena * 128);
+  // Scratch rows of a chunk: its N_c + 2 orders of u_k(mx) and u_k(x).
+  const int64_t max_slab_chunks = std::max<int64_t>(kMaxSlabChunks, cpu);
+  double2* uz = c.uz.as<double2>((size_t)(arena + 2 * max_slab_chunks) * 32);
+  double* ux = c.ux.as<double>((size_t)(arena + 2 * max_slab_chunks) * 32);
+  int64_t* chunk_row = c.chunk_row.as<int64_t>(n_chunks);
+  double* chunk_sums = c.chunk_sums.as<double>((size_t)n_chunks * 8);
+  std::vector<int64_t> slab_begin;  // unit index
+  {
+    int64_t used = 0;
+    slab_begin.push_back(0);
+    for (int64_t u = 0; u < n_units; ++u) {
+      int64_t need = 0;
+      for (int k = 0; k < cpu; ++k) need += cn[u * cpu + k];
+      int64_t slab_units = u - slab_begin.back();
+      int64_t slab_chunks = (slab_units + 1) * cpu;
+      if (slab_units > 0 && (used + need > arena || slab_chunks > max_slab_chunks)) {
+        slab_begin.push_back(u);
+        used = 0;
+      }
+      int64_t base = used;
+      for (int k = 0; k < cpu; ++k) {
+        rows[u * cpu + k] = base;
+        base += cn[u * cpu + k];
+      }
+      used += need;
+    }
+    slab_begin.push_back(n_units);
+  }
+  SB_CUDA(cudaMemcpyAsync(chunk_row, rows.data(), n_chunks * 8, cudaMemcpyHostToDevice, s));
+  // Per-CTA accumulators of the unit kernel.
+  const int grid_max = c.sms * c.unit_bps;
+  const int nq_max = bt ? bt->nq_max : 0;
+  const int64_t acc_stride = round_up(4 * n_mu + 4 * (int64_t)nq_max + (L >= 0 ? 6 * (L + 1) : 0), 32);
+  double* acc = c.acc.as<double>((size_t)grid_max * std::max<int64_t>(acc_stride, 1));
+  int* counter = c.counter.as<int>(64);
+  // Processing order inside a slab: units with the most work first.
+  std::vector<int> order;
+  int* unit_order_d = c.unit_order.as<int>(n_units);
+  {
+    std::vector<int> all(n_units);
+    for (size_t si = 0; si + 1 < slab_begin.size(); ++si) {
+      int64_t u0 = slab_begin[si], u1 = slab_begin[si + 1];
+      std::vector<std::pair<int64_t, int>> cost;
+      cost.reserve(u1 - u0);
+      for (int64_t u = u0; u < u1; ++u) {
+        int64_t w = 0;
+        for (int k = 0; k < cpu; ++k) {
+          int64_t nc = cn[u * cpu + k];
+          w += nc * ((int64_t)c.user.h + (L >= 0 ? (nc + L / 2) / 2 : 0)) + 64;
+        }
+        cost.emplace_back(-w, (int)(u - u0));
+      }
+      std::sort(cost.begin(), cost.end());
+      for (int64_t k = 0; k < u1 - u0; ++k) all[u0 + k] = cost[k].second;
+    }
+    SB_CUDA(cudaMemcpyAsync(unit_order_d, all.data(), n_units * sizeof(int),
+                            cudaMemcpyHostToDevice, s));
+    SB_CUDA(cudaStreamSynchronize(s));
+  }
+  UnitArgs ua{};
+  ua.radius = ka.radius;
+  ua.weight = ka.weight;
+  ua.wl = wl_dev;
+  ua.n_dist = (int)n_dist;
+  ua.n_wl = (int)n_wl;
+  ua.n_nodes = (int)n_nodes;
+  ua.cpu = cpu;
+  ua.X = X;
+  ua.n_mu = (int)n_mu;
+  ua.h_u = c.user.h;
+  ua.h_u_pad = c.user.h_pad;
+  ua.ld_u = c.user.ld;
+  ua.ge_u = c.user.ge.as<double>(0);
+  ua.go_u = c.user.go.as<double>(0);
+  ua.user_map = c.user.map.as<int2>(0);
+  ua.greek_order = L;
+  if (bt) {
+    ua.n_bands = bt->n_bands;
+    ua.bands = bt->desc_d.as<BandDesc>(0);
+    ua.band_ge = bt->ge_d.as<double>(0);
+    ua.band_go = bt->go_d.as<double>(0);
+    ua.band_d = bt->d_d.as<double>(0);
+  }
+  ua.nq_max = nq_max;
+  ua.n_units_total = n_units;
+  ua.values = values;
+  ua.phase = n_mu > 0 ? phase : nullptr;
+  ua.greek = L >= 0 ? greek : nullptr;
+  ua.normalized = opt->normalized;
+  ua.acc = acc;
+  ua.acc_stride = acc_stride;
+  ua.work_counter = counter;
+  ua.err = err;
+  for (size_t si = 0; si + 1 < slab_begin.size(); ++si) {
+    int64_t u0 = slab_begin[si], u1 = slab_begin[si + 1];
+    int64_t nu = u1 - u0;
+    ka.unit0 = u0;
+    ka.n_chunks = (int)(nu * cpu);
+    ka.chunk_order = nullptr;
+    ka.chunk_n = chunk_n + u0 * cpu;
+    ka.chunk_row = chunk_row + u0 * cpu;
+    ka.X = X;
+    ka.uz = uz;
+    ka.ux = ux;
+    ka.chunk_sums = chunk_sums + u0 * cpu * 8;
+    timed_launch(K_MIE, s, [&] { launch_mie_fixed(ka, s); });
+    SB_CUDA(cudaGetLastError());
+    SB_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), s));
+    ua.unit0 = u0;
+    ua.n_units = (int)nu;
+    ua.unit_order = unit_order_d + u0;
+    ua.chunk_n = ka.chunk_n;
+    ua.chunk_row = ka.chunk_row;
+    ua.chunk_sums = ka.chunk_sums;
+    int grid = (int)std::min<int64_t>(grid_max, nu);
+    timed_launch(K_UNITS, s, [&] { launch_units(ua, grid, s); });
+    SB_CUDA(cudaGetLastError());
+  }
+  if (call) {
+    call->radius = std::move(radius);
+    call->n_dist = n_dist;
+    call->n_wl = n_wl;
+    call->n_nodes = n_nodes;
+  }
+}
+
+// Reads the error words of the last call (synchronizes the stream).
+void check_device_errors(Context& c, cudaStream_t s, const FixedCall* call) {
+  unsigned long long h[2];
+  SB_CUDA(cudaMemcpyAsync(h, c.err.as<unsigned long long>(2), sizeof h, cudaMemcpyDeviceToHost, s));
+  SB_CUDA(cudaStreamSynchronize(s));
+  if (h[0] != ~0ull) {
+    int status = (int)(h[0] & 3);
+    unsigned long long key = h[0] >> 2;
+    std::string msg = "a size node's inputs are invalid";
+    if (call && call->n_nodes > 0) {
+      int64_t j = key % call->n_nodes;
+      int64_t d = (key / call->n_nodes) % call->n_dist;
+      int64_t i = key / call->n_nodes / call->n_dist;
+      double lam = i < (int64_t)call->wl_host.size() ? call->wl_host[i] : NAN;
+      msg = node_message(status, lam, call->radius[d * call->n_nodes + j]);
+    }
+    throw Failure{status, msg};
+  }
+  if (h[1] != ~0ull) {
+    int which = (int)(h[1] & 3);
+    const char* what = which == 1 ? "<C_ext>" : which == 2 ? "<C_sca>" : "<C_back>";
+    throw Failure{SCATRS_INVALID_INPUT,
+                  std::string("the ensemble's ") + what +
+                      " is 0 or not finite, so its ratios (albedo, asymmetry parameter, lidar "
+                      "ratio) are undefined (does m = 1?)"};
+  }
+}
+
+FixedCall g_last_call;  // for scatrs_check_errors
+
+template <class F>
+int guarded(char* err, size_t err_len, F f) {
+  try {
+    f();
+    return SCATRS_OK;
+  } catch (const Failure& e) {
+    set_err(err, err_len, e.msg);
+    return e.status;
+  } catch (const std::bad_alloc&) {
+    set_err(err, err_len, "host allocation failed");
+    return SCATRS_INVALID_INPUT;
+  }
+}
+
+}  // namespace
+}  // namespace sb
+
+using namespace sb;
+
+extern "C" {
+
+void scatrs_ensemble_fixed_sizes(int64_t n_units, int64_t n_mu, int32_t greek_order,
+                                 int64_t* values_len, int64_t* phase_len, int64_t* greek_len) {
+  if (values_len) *values_len = 11 * n_units;
+  if (phase_len) *phase_len = 6 * n_units * n_mu;
+  if (greek_len) *greek_len = greek_order >= 0 ? 6 * n_units * ((int64_t)greek_order + 1) : 0;
+}
+
+int scatrs_ensemble_fixed(const scatrs_distribution* dists, int64_t n_dist,
+                          const double* wavelengths, int64_t n_wl, const double* m,
+                          const double* mu, int64_t n_mu, const scatrs_fixed_options* options,
+                          double* values, double* phase, double* greek, char* err,
+                          size_t err_len) {
+  return guarded(err, err_len, [&] {
+    if (n_dist < 0 || n_wl < 0) throw Failure{SCATRS_INVALID_INPUT, "negative sizes"};
+    for (int64_t i = 0; i < n_wl; ++i)
+      if (!(std::isfinite(wavelengths[i]) && wavelengths[i] > 0.0))
+        throw Failure{SCATRS_INVALID_INPUT, "wavelengths must be finite and > 0"};
+    Context& c = context();
+    std::lock_guard<std::mutex> lk(c.mtx);
+    cudaStream_t s = 0;
+    const int64_t n_units = n_dist * n_wl;
+    check_options(options, n_units, n_mu, mu);
+    if (n_units == 0) return;
+    double* wl_d = c.wl.as<double>(n_wl);
+    double* m_d = c.m.as<double>(2 * n_units);
+    SB_CUDA(cudaMemcpyAsync(wl_d, wavelengths, n_wl * 8, cudaMemcpyHostToDevice, s));
+    SB_CUDA(cudaMemcpyAsync(m_d, m, 2 * n_units * 8, cudaMemcpyHostToDevice, s));
+    int64_t vl, pl, gl;
+    scatrs_ensemble_fixed_sizes(n_units, n_mu, options->greek_order, &vl, &pl, &gl);
+    double* v_d = c.values.as<double>(vl);
+    double* p_d = pl > 0 ? c.phase.as<double>(pl) : nullptr;
+    double* g_d = gl > 0 ? c.greek.as<double>(gl) : nullptr;
+    FixedCall call;
+    call.wl_host.assign(wavelengths, wavelengths + n_wl);
+    run_fixed(c, dists, n_dist, wl_d, n_wl, m_d, mu, n_mu, options, v_d, p_d, g_d, s, &call);
+    check_device_errors(c, s, &call);
+    SB_CUDA(cudaMemcpyAsync(values, v_d, vl * 8, cudaMemcpyDeviceToHost, s));
+    if (pl > 0 && phase) SB_CUDA(cudaMemcpyAsync(phase, p_d, pl * 8, cudaMemcpyDeviceToHost, s));
+    if (gl > 0 && greek) SB_CUDA(cudaMemcpyAsync(greek, g_d, gl * 8, cudaMemcpyDeviceToHost, s));
+    SB_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+int scatrs_ensemble_fixed_device(const scatrs_distribution* dists_host, int64_t n_dist,
+                                 const double* wavelengths_dev, int64_t n_wl,
+                                 const double* m_dev, const double* mu_host, int64_t n_mu,
+                                 const scatrs_fixed_options* options, double* values_dev,
+                                 double* phase_dev, double* greek_dev, void* stream, char* err,
+                                 size_t err_len) {
+  return guarded(err, err_len, [&] {
+    if (n_dist < 0 || n_wl < 0) throw Failure{SCATRS_INVALID_INPUT, "negative sizes"};
+    Context& c = context();
+    std::lock_guard<std::mutex> lk(c.mtx);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    FixedCall call;
+    call.wl_host.resize(n_wl);
+    if (n_wl > 0)
+      SB_CUDA(cudaMemcpyAsync(call.wl_host.data(), wavelengths_dev, n_wl * 8,
+                              cudaMemcpyDeviceToHost, s));
+    run_fixed(c, dists_host, n_dist, wavelengths_dev, n_wl, m_dev, mu_host, n_mu, options,
+              values_dev, phase_dev, greek_dev, s, &call);
+    g_last_call = std::move(call);
+  });
+}
+
+int scatrs_check_errors(void* stream, char* err, size_t err_len) {
+  return guarded(err, err_len, [&] {
+    Context& c = context();
+    std::lock_guard<std::mutex> lk(c.mtx);
+    check_device_errors(c, static_cast<cudaStream_t>(stream), &g_last_call);
+  });
+}
+
+int scatrs_mie(const double* x, const double* m, int64_t n, int32_t allow_unvalidated,
+               int64_t* n_terms, const int64_t* coeff_offset, double* coeffs, double* eff,
+               char* err, size_t err_len) {
+  return guarded(err, err_len, [&] {
+    if (n <= 0) return;
+    Context& c = context();
+    std::lock_guard<std::mutex> lk(c.mtx);
+    cudaStream_t s = 0;
+    DevBuf xb, mb, nb, ob, cb, eb, uzb, uxb;
+    struct Free {
+      DevBuf* b[8];
+      ~Free() {
+        for (auto* p : b) p->release();
+      }
+    } guard{{&xb, &mb, &nb, &ob, &cb, &eb, &uzb, &uxb}};
+    double* xd = xb.as<double>(n);
+    double2* md = mb.as<double2>(n);
+    int64_t* nd = nb.as<int64_t>(n);
+    SB_CUDA(cudaMemcpyAsync(xd, x, n * 8, cudaMemcpyHostToDevice, s));
+    SB_CUDA(cudaMemcpyAsync(md, m, n * 16, cudaMemcpyHostToDevice, s));
+    unsigned long long* errw = c.err.as<unsigned long long>(2);
+    SB_CUDA(cudaMemsetAsync(errw, 0xff, 16, s));
+    MieNodesArgs a{};
+    a.x = xd;
+    a.m = md;
+    a.n = n;
+    a.n_terms = nd;
+    a.err = errw;
+    a.allow_unvalidated = allow_unvalidated;
+    int64_t bound = 0;
+    if (coeffs) {
+      // Sized from the default truncation of the largest sphere; the exact total follows
+      // from the terms the kernel reports.
+      double xmax = 0.0;
+      int64_t off_max = 0;
+      for (int64_t i = 0; i < n; ++i) {
+        xmax = std::max(xmax, x[i]);
+        off_max = std::max(off_max, coeff_offset[i]);
+      }
+      bound = off_max + (int64_t)std::ceil(xmax + 6.0 * std::cbrt(xmax) + 3.0);
+      int64_t* od = ob.as<int64_t>(n);
+      SB_CUDA(cudaMemcpyAsync(od, coeff_offset, n * 8, cudaMemcpyHostToDevice, s));
+      a.coeff_offset = od;
+      a.coeffs = cb.as<double>(4 * bound);
+      a.uz = uzb.as<double2>(bound + 2 * n);
+      a.ux = uxb.as<double>(bound + 2 * n);
+    }
+    if (eff) a.eff = eb.as<double>(5 * n);
+    timed_launch(K_NODES, s, [&] { launch_mie_nodes(a, s); });
+    SB_CUDA(cudaGetLastError());
+    unsigned long long h[2];
+    SB_CUDA(cudaMemcpyAsync(h, errw, 16, cudaMemcpyDeviceToHost, s));
+    SB_CUDA(cudaStreamSynchronize(s));
+    if (h[0] != ~0ull) {
+      int64_t t = (int64_t)(h[0] >> 2);
+      char buf[200];
+      snprintf(buf, sizeof buf, "sphere %lld (x = %e): %s", (long long)t, x[t],
+               (h[0] & 3) == 3 ? "outside the validated domain" : "invalid input");
+      throw Failure{(int)(h[0] & 3), buf};
+    }
+    SB_CUDA(cudaMemcpyAsync(n_terms, nd, n * 8, cudaMemcpyDeviceToHost, s));
+    SB_CUDA(cudaStreamSynchronize(s));
+    if (coeffs) {
+      int64_t total = 0;
+      for (int64_t i = 0; i < n; ++i) total = std::max(total, coeff_offset[i] + n_terms[i]);
+      if (total > bound) throw Failure{SCATRS_INVALID_INPUT, "coeff_offset is not the prefix sum of n_terms"};
+      SB_CUDA(cudaMemcpyAsync(coeffs, a.coeffs, 4 * total * 8, cudaMemcpyDeviceToHost, s));
+    }
+    if (eff) SB_CUDA(cudaMemcpyAsync(eff, a.eff, 5 * n * 8, cudaMemcpyDeviceToHost, s));
+    SB_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+int scatrs_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) return -1;
+  return n;
+}
+
+int64_t scatrs_launch_count(void) { return g_launches.load(); }
+
+void scatrs_gauss_legendre(int64_t n, double* nodes, double* weights) {
+  sb::gauss_legendre(n, nodes, weights);
+}
+
+void scatrs_set_profiling(int32_t on) {
+  sb::g_profiling = on != 0;
+  for (auto& t : sb::g_timed) {
+    cudaEventDestroy(t.a);
+    cudaEventDestroy(t.b);
+  }
+  sb::g_timed.clear();
+  for (int k = 0; k < sb::K_COUNT; ++k) {
+    sb::g_kernel_ms[k] = 0.0;
+    sb::g_kernel_launches[k] = 0;
+  }
+}
+
+int scatrs_kernel_times(double* ms, int64_t* launches, int32_t n) {
+  for (auto& t : sb::g_timed) {
+    float v = 0.0f;
+    if (cudaEventSynchronize(t.b) == cudaSuccess && cudaEventElapsedTime(&v, t.a, t.b) == cudaSuccess) {
+      sb::g_kernel_ms[t.id] += v;
+      sb::g_kernel_launches[t.id] += 1;
+    }
+    cudaEventDestroy(t.a);
+    cudaEventDestroy(t.b);
+  }
+  sb::g_timed.clear();
+  for (int k = 0; k < n && k < sb::K_COUNT; ++k) {
+    ms[k] = sb::g_kernel_ms[k];
+    launches[k] = sb::g_kernel_launches[k];
+  }
+  return sb::K_COUNT;
+}
+
+void scatrs_release(void) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return;
+  std::lock_guard<std::mutex> lk(g_ctx_mtx);
+  if (dev < (int)g_ctx.size() && g_ctx[dev]) {
+    Context& c = *g_ctx[dev];
+    for (DevBuf* b : {&c.radius, &c.weight, &c.wl, &c.m, &c.chunk_n, &c.chunk_row, &c.chunk_order,
+                      &c.unit_order, &c.X, &c.uz, &c.ux, &c.chunk_sums, &c.err, &c.acc,
+                      &c.counter, &c.values, &c.phase, &c.greek, &c.user.ge, &c.user.go,
+                      &c.user.map})
+      b->release();
+    for (auto& kv : c.bands)
+      for (DevBuf* b : {&kv.second.ge_d, &kv.second.go_d, &kv.second.d_d, &kv.second.desc_d})
+        b->release();
+    if (c.pinned_chunk_n) cudaFreeHost(c.pinned_chunk_n);
+    g_ctx[dev].reset();
+  }
+}
+
+}  // extern "C"

@@ -1,0 +1,298 @@
+// Device-side Mie arithmetic for one size node per thread: complex numbers in num-complex's
+// operation order, the reference's complex reciprocal, the start index of the downward
+// recurrences and the truncation rule. Translation units including this header are compiled
+// with -fmad=false, so every a*b+c rounds twice as the reference's Rust does; the coefficients
+// then match the reference's bit for bit wherever the device's sin, cos, cbrt, log2 and pow
+// return the same doubles as the host's libm.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace sb {
+
+constexpr double kPi = 3.14159265358979323846264338327950288;
+constexpr double kEps = 2.220446049250313e-16;  // 2^-52
+
+struct cplx {
+  double re, im;
+};
+__device__ __forceinline__ cplx mk(double r, double i) { return {r, i}; }
+__device__ __forceinline__ cplx rl(double v) { return {v, 0.0}; }
+__device__ __forceinline__ cplx operator+(cplx a, cplx b) { return {a.re + b.re, a.im + b.im}; }
+__device__ __forceinline__ cplx operator-(cplx a, cplx b) { return {a.re - b.re, a.im - b.im}; }
+__device__ __forceinline__ cplx operator-(cplx a) { return {-a.re, -a.im}; }
+__device__ __forceinline__ cplx operator*(cplx a, cplx b) {
+  return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+}
+__device__ __forceinline__ cplx scl(cplx a, double t) { return {a.re * t, a.im * t}; }
+__device__ __forceinline__ double nsq(cplx a) { return a.re * a.re + a.im * a.im; }
+__device__ __forceinline__ double cabs_(cplx a) { return hypot(a.re, a.im); }
+__device__ __forceinline__ double re_mul_conj(cplx u, cplx v) { return u.re * v.re + u.im * v.im; }
+
+// 1/z as scatrs/src/complex.rs:21-38: one division where 1e-300 < |z|^2 < 1e300 and
+// Im z != 0, Smith's algorithm otherwise.
+__device__ __forceinline__ cplx cinv(cplx z) {
+  double c = z.re, d = z.im;
+  double s = c * c + d * d;
+  if (s > 1e-300 && s < 1e300 && d != 0.0) {
+    double t = 1.0 / s;
+    return {c * t, -(d * t)};
+  }
+  if (fabs(d) <= fabs(c)) {
+    double r = d / c;
+    double t = 1.0 / (c + d * r);
+    return {t, -(r * t)};
+  }
+  double r = c / d;
+  double t = 1.0 / (c * r + d);
+  return {r * t, -t};
+}
+
+// ceil(x + 6 x^(1/3) + 3), the f64 truncation (scatrs/src/mie/mod.rs:122-145).
+__device__ __forceinline__ int64_t default_n_max(double x) {
+  double n = ceil(x + 6.0 * cbrt(x) + 3.0);
+  if (isfinite(n) && n < 9007199254740992.0) return (int64_t)n;
+  return INT64_MAX;
+}
+
+// The start of a downward ratio recurrence that reaches n_top with its start value forgotten
+// to rounding level (scatrs/src/mie/kernel.rs:99-112), 52 bits, margin 30.
+__device__ __forceinline__ int64_t start_index(int64_t n_top, double rho_abs) {
+  const double bits = 52.0;
+  double c15 = ceil(1.5 * rho_abs);
+  int64_t k0 = n_top > (int64_t)c15 ? n_top : (int64_t)c15;
+  double q = (double)(2 * k0 + 1) / rho_abs - 0.5;
+  int64_t enclosed = k0 + (int64_t)ceil(bits / (2.0 * log2(q))) + 2;
+  if ((double)n_top >= 1.5 * rho_abs) return enclosed;
+  double s0 = (double)n_top - rho_abs;
+  double s0_32 = s0 > 0.0 ? s0 * sqrt(s0) : 0.0;
+  double s = pow(s0_32 + 1.4 * 0.37 * bits * sqrt(rho_abs), 2.0 / 3.0);
+  int64_t asymptotic = (int64_t)ceil(rho_abs + s) + 30;
+  return asymptotic < enclosed ? asymptotic : enclosed;
+}
+
+// One downward step u_k = 1/((2k+1)/z - u_{k+1}) (kernel.rs:116-125).
+__device__ __forceinline__ cplx step_complex(int64_t k, cplx inv_z, cplx u) {
+  cplx c = scl(inv_z, (double)(2 * k + 1));
+  cplx den = c - u;
+  if (den.re == 0.0 && den.im == 0.0) den = rl(kEps * (cabs_(c) + cabs_(u)));
+  return cinv(den);
+}
+
+// The real form (kernel.rs:129-136).
+__device__ __forceinline__ double step_real(int64_t k, double inv_rho, double u) {
+  double c = inv_rho * (double)(2 * k + 1);
+  double den = c - u;
+  if (den == 0.0) den = kEps * (fabs(c) + fabs(u));
+  return 1.0 / den;
+}
+
+// The last order of the upward psi/chi recurrences (kernel.rs:208-215).
+__device__ __forceinline__ int64_t upward_orders(double x, int64_t n) {
+  if (x >= 1.0) {
+    int64_t f = (int64_t)floor(x);
+    return f < n ? f : n;
+  }
+  return 0;
+}
+
+// Input checks of Mie::compute (scatrs/src/mie/mod.rs:274-320) with the default truncation:
+// 0 when accepted, else the status (1 invalid input, 3 outside the validated domain).
+__device__ __forceinline__ int check_node(double x, cplx m, int64_t n, bool allow_unvalidated) {
+  if (!(x >= 1e-30 && x <= 1e6)) return 1;
+  if (!(isfinite(m.re) && isfinite(m.im))) return 1;
+  if (m.re < 0.0 || m.im < 0.0) return 1;
+  double abs_m = hypot(m.re, m.im);
+  if (!(abs_m >= 1e-6 && abs_m <= 1e3)) return 1;
+  if (n == 0 || n > (1 << 20)) return 1;
+  if (!allow_unvalidated) {
+    bool in = x >= 1e-6 && x <= 2e4 && m.re > 0.0 && m.re <= 10.0 && m.im >= 0.0 &&
+              m.im <= 10.0 && abs_m >= 0.1;
+    if (!in) return 3;
+  }
+  return 0;
+}
+
+// Per-node scratch of the downward recurrences: u_k(mx) and u_k(x) at order k, strided so that
+// the lanes of a warp touch consecutive addresses.
+struct Scratch {
+  double2* uz;
+  double* ux;
+  int stride;  // lanes sharing the rows
+  __device__ __forceinline__ void put_z(int64_t k, cplx v) const {
+    uz[k * stride] = make_double2(v.re, v.im);
+  }
+  __device__ __forceinline__ cplx get_z(int64_t k) const {
+    double2 v = uz[k * stride];
+    return {v.x, v.y};
+  }
+  __device__ __forceinline__ void put_x(int64_t k, double v) const { ux[k * stride] = v; }
+  __device__ __forceinline__ double get_x(int64_t k) const { return ux[k * stride]; }
+};
+
+// State::prepare (kernel.rs:249-313): u_k(mx) for k = 1..n+1 and u_k(x) for the orders above
+// the upward recurrences. The two recurrences are independent; they run one after the other.
+__device__ __forceinline__ void mie_prepare(double x, cplx m, int64_t n, const Scratch& s) {
+  int64_t n_s = upward_orders(x, n);
+  int64_t top = n + 1;
+  if (n_s < n) {
+    int64_t start = start_index(top, fabs(x));
+    int64_t lo = n_s + 1 > 1 ? n_s + 1 : 1;
+    double inv_x = 1.0 / x;
+    double ux = 0.0;
+    for (int64_t k = start; k >= lo; --k) {
+      ux = step_real(k, inv_x, ux);
+      if (k <= top) s.put_x(k, ux);
+    }
+  }
+  cplx z = scl(m, x);
+  if (m.im == 0.0) {
+    double inv_rho = 1.0 / z.re;
+    double u = 0.0;
+    int64_t start = start_index(top, fabs(z.re));
+    for (int64_t k = start; k >= 1; --k) {
+      u = step_real(k, inv_rho, u);
+      if (k <= top) s.put_z(k, rl(u));
+    }
+  } else {
+    cplx inv_z = cinv(z);
+    cplx u = rl(0.0);
+    int64_t start = start_index(top, cabs_(z));
+    for (int64_t k = start; k >= 1; --k) {
+      u = step_complex(k, inv_z, u);
+      if (k <= top) s.put_z(k, u);
+    }
+  }
+}
+
+// Running sums of value_sums (scatrs/src/mie/efficiencies.rs:64-84), fed one order at a time
+// in the reference's order of operations.
+struct ValueSums {
+  double sca = 0.0, g = 0.0;
+  cplx back = {0.0, 0.0};
+  cplx a_prev = {0.0, 0.0}, b_prev = {0.0, 0.0};
+  // Order k's coefficients arrive; the pair and own terms of order k-1 follow.
+  __device__ __forceinline__ void add(int64_t k, cplx ak, cplx bk) {
+    if (k > 1) {
+      double kf = (double)(k - 1);
+      double w1 = (double)(2 * (k - 1) + 1);
+      g += kf * (kf + 2.0) / (kf + 1.0) * (re_mul_conj(a_prev, ak) + re_mul_conj(b_prev, bk));
+      g += w1 / (kf * (kf + 1.0)) * re_mul_conj(a_prev, b_prev);
+    }
+    double w = (double)(2 * k + 1);
+    sca += w * (nsq(ak) + nsq(bk));
+    cplx t = scl(ak - bk, w);
+    back = (k % 2 == 0) ? back + t : back - t;
+    a_prev = ak;
+    b_prev = bk;
+  }
+  // After the last order n: its own term.
+  __device__ __forceinline__ void close(int64_t n) {
+    if (n >= 1) {
+      double kf = (double)n;
+      double w = (double)(2 * n + 1);
+      g += w / (kf * (kf + 1.0)) * re_mul_conj(a_prev, b_prev);
+    }
+  }
+};
+
+struct Eff {
+  double q_ext, q_sca, q_abs, q_back, g;
+};
+
+// efficiencies_from (efficiencies.rs:169-187).
+__device__ __forceinline__ Eff efficiencies_from(double x, double abs_sum, const ValueSums& s) {
+  double inv_x = 1.0 / x;
+  double inv_x2 = inv_x * inv_x;
+  double two_x2 = 2.0 * inv_x2;
+  double q_sca = two_x2 * s.sca;
+  double q_abs = two_x2 * abs_sum;
+  double g = s.sca == 0.0 ? 0.0 : 2.0 * s.g / s.sca;
+  return {q_sca + q_abs, q_sca, q_abs, nsq(s.back) * inv_x2, g};
+}
+
+// State::finish (kernel.rs:324-559) for a homogeneous sphere without derivatives: calls
+// emit(k, a_k, b_k) for k = 1..n and returns the absorption sum (x^2/2) Q_abs, feeding the
+// value sums on the way.
+template <class Emit>
+__device__ __forceinline__ double mie_finish(double x, cplx m, int64_t n, const Scratch& s,
+                                             ValueSums& vs, Emit emit) {
+  const double one = 1.0;
+  cplx z = scl(m, x);
+  int64_t n_s = upward_orders(x, n);
+  double inv_x = 1.0 / x;
+  cplx inv_z = cinv(z);
+  cplx inv_m = cinv(m);
+  cplx inv_m2 = inv_m * inv_m;
+  cplx m2_minus_1 = (m - rl(one)) * (m + rl(one));
+  cplx c_a = -(m2_minus_1 * inv_m2);
+  double sin_x, cos_x;
+  sincos(x, &sin_x, &cos_x);
+  double psi_prev = cos_x, psi = sin_x;
+  double chi_prev = -sin_x, chi = cos_x;
+  cplx t = rl(0.0), inv_xi = rl(0.0), r = rl(0.0);
+  if (n_s == 0) {
+    cplx xi0 = mk(sin_x, -cos_x);
+    t = rl(sin_x) * cinv(xi0);
+    inv_xi = mk(sin_x, cos_x);
+    r = mk(0.0, one);
+  }
+  double asum = 0.0;
+  cplx u_next = s.get_z(1 + 1);
+  for (int64_t k = 1; k <= n; ++k) {
+    double kf = (double)k;
+    double k_x = kf * inv_x;
+    cplx u_z1 = u_next;
+    if (k < n) u_next = s.get_z(k + 2);
+    cplx d = scl(inv_z, (double)(k + 1)) - u_z1;
+    cplx d_m = d * inv_m;
+    cplx md = d * m;
+    cplx big_a = d_m + rl(k_x);
+    cplx big_b = md + rl(k_x);
+    cplx an, bn, inv_da, inv_db;
+    if (k <= n_s) {
+      double c = (double)(2 * k - 1) * inv_x;
+      double psi_next = c * psi - psi_prev;
+      psi_prev = psi;
+      psi = psi_next;
+      double chi_next = c * chi - chi_prev;
+      chi_prev = chi;
+      chi = chi_next;
+      cplx xi = mk(psi, -chi);
+      cplx xi_prev = mk(psi_prev, -chi_prev);
+      inv_da = cinv(big_a * xi - xi_prev);
+      inv_db = cinv(big_b * xi - xi_prev);
+      an = (scl(big_a, psi) - rl(psi_prev)) * inv_da;
+      bn = (scl(big_b, psi) - rl(psi_prev)) * inv_db;
+      if (k == n_s) {
+        inv_xi = cinv(xi);
+        t = rl(psi) * inv_xi;
+        r = xi_prev * inv_xi;
+      }
+    } else {
+      r = cinv(rl((double)(2 * k - 1) * inv_x) - r);
+      t = scl(t * r, s.get_x(k));
+      inv_xi = inv_xi * r;
+      cplx u_x1 = rl(s.get_x(k + 1));
+      cplx num_a = scl(c_a, (double)(k + 1) * inv_x) + u_x1 - u_z1 * inv_m;
+      cplx num_b = u_x1 - m * u_z1;
+      cplx ia = cinv(big_a - r);
+      cplx ib = cinv(big_b - r);
+      an = t * num_a * ia;
+      bn = t * num_b * ib;
+      inv_da = inv_xi * ia;
+      inv_db = inv_xi * ib;
+    }
+    emit(k, an, bn);
+    vs.add(k, an, bn);
+    double na = nsq(inv_da);
+    double nb = nsq(inv_db);
+    double weight = (double)(2 * k + 1);
+    asum += weight * (-(d_m.im * na) - md.im * nb);
+  }
+  vs.close(n);
+  return asum;
+}
+
+}  // namespace sb

@@ -1,0 +1,158 @@
+// K-a: the Mie recurrences of every size node, one thread per node, one warp per chunk of 32
+// consecutive nodes of a (distribution, wavelength) unit. Compiled with -fmad=false (see
+// mie_device.cuh). The coefficients leave in the layout the angle GEMM reads: for each chunk a
+// row per order n (n = 1..N_c, N_c the chunk's largest number of terms) of 128 doubles,
+// 4 per lane: u.re, u.im, v.re, v.im with (u, v) = (a_n, b_n) for odd n and (b_n, a_n) for even
+// n (scatrs/src/ensemble/fast.rs:95-137), zero above the node's own N.
+#include "kernels.h"
+#include "mie_device.cuh"
+
+namespace sb {
+
+// Error word: the smallest (wavelength, distribution, radius) key of a node whose inputs fail,
+// with its status in the low 2 bits.
+__device__ __forceinline__ void record_error(unsigned long long* err, long long i_wl,
+                                             long long d, long long j, long long n_dist,
+                                             long long n_nodes, int status) {
+  unsigned long long key = (unsigned long long)(((i_wl * n_dist + d) * n_nodes + j) << 2) |
+                           (unsigned long long)status;
+  atomicMin(err, key);
+}
+
+// Each chunk's largest number of terms (the band selector, engine.rs:961-978).
+__global__ void plan_chunks_kernel(MieFixedArgs a) {
+  int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (warp >= a.n_chunks) return;
+  int64_t unit = a.unit0 + warp / a.cpu;
+  int c = warp % a.cpu;
+  int64_t d = unit / a.n_wl, i = unit % a.n_wl;
+  int j = c * 32 + lane;
+  int64_t n = 0;
+  if (j < a.n_nodes) {
+    double r = a.radius[d * a.n_nodes + j];
+    double x = 2.0 * kPi * r / a.wl[i];
+    n = default_n_max(x);
+    if (n > (1 << 20)) n = 1 << 20;
+  }
+  int nn = (int)n;
+  for (int off = 16; off > 0; off >>= 1) {
+    int o = __shfl_xor_sync(0xffffffffu, nn, off);
+    nn = o > nn ? o : nn;
+  }
+  if (lane == 0) a.chunk_n[warp] = nn;
+}
+
+__global__ void __launch_bounds__(128) mie_fixed_kernel(MieFixedArgs a) {
+  int wslot = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (wslot >= a.n_chunks) return;
+  int chunk = a.chunk_order ? a.chunk_order[wslot] : wslot;
+  int64_t unit = a.unit0 + chunk / a.cpu;
+  int c = chunk % a.cpu;
+  int64_t d = unit / a.n_wl, i = unit % a.n_wl;
+  int j = c * 32 + lane;
+  int nc = a.chunk_n[chunk];
+  int64_t row0 = a.chunk_row[chunk];
+  double* X = a.X + row0 * 128 + lane * 4;
+  Scratch s;
+  s.uz = a.uz + (row0 + 2 * (int64_t)chunk) * 32 + lane;
+  s.ux = a.ux + (row0 + 2 * (int64_t)chunk) * 32 + lane;
+  s.stride = 32;
+  double q[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  int64_t n = 0;
+  if (j < a.n_nodes) {
+    double r = a.radius[d * a.n_nodes + j];
+    double w = a.weight[d * a.n_nodes + j];
+    double x = 2.0 * kPi * r / a.wl[i];
+    double2 mv = a.m[unit];
+    cplx m = mk(mv.x, mv.y);
+    n = default_n_max(x);
+    int st = check_node(x, m, n, a.allow_unvalidated != 0);
+    if (st != 0 || n > nc) {
+      record_error(a.err, i, d, j, a.n_dist, a.n_nodes, st != 0 ? st : 1);
+      n = 0;
+    } else {
+      mie_prepare(x, m, n, s);
+      ValueSums vs;
+      double asum = mie_finish(x, m, n, s, vs, [&](int64_t k, cplx an, cplx bn) {
+        bool odd = (k & 1) != 0;
+        cplx u = odd ? an : bn, v = odd ? bn : an;
+        *reinterpret_cast<double4*>(X + (k - 1) * 128) = make_double4(u.re, u.im, v.re, v.im);
+      });
+      Eff e = efficiencies_from(x, asum, vs);
+      // The per-particle quantities of pass 2 (engine.rs:1047-1057), weighted.
+      double area = kPi * r * r;
+      double qv[8] = {1.0,           area * e.q_ext, area * e.q_sca, area * e.q_sca * e.g,
+                      area * e.q_abs, area * e.q_back, r * r,         r * r * r};
+      for (int k = 0; k < 8; ++k) q[k] = w * qv[k];
+    }
+  }
+  // Orders above the node's own N are zero up to the chunk's.
+  for (int64_t k = n + 1; k <= nc; ++k)
+    *reinterpret_cast<double4*>(X + (k - 1) * 128) = make_double4(0.0, 0.0, 0.0, 0.0);
+  // The chunk's weighted sums, in a fixed tree order.
+  for (int k = 0; k < 8; ++k) {
+    double v = q[k];
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+    if (lane == 0) a.chunk_sums[(int64_t)chunk * 8 + k] = v;
+  }
+}
+
+// Independent spheres, one per thread (the batched Mie::compute): coefficients a_1..a_N then
+// b_1..b_N per sphere, and the efficiencies.
+__global__ void __launch_bounds__(128) mie_nodes_kernel(MieNodesArgs a) {
+  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.n) return;
+  double x = a.x[t];
+  cplx m = mk(a.m[t].x, a.m[t].y);
+  int64_t n = default_n_max(x);
+  int st = check_node(x, m, n, a.allow_unvalidated != 0);
+  if (st != 0) {
+    unsigned long long key = ((unsigned long long)t << 2) | (unsigned long long)st;
+    atomicMin(a.err, key);
+    return;
+  }
+  if (a.n_terms) a.n_terms[t] = n;
+  if (!a.coeffs) return;
+  int64_t off = a.coeff_offset[t];
+  Scratch s;
+  s.uz = a.uz + off + 2 * t;
+  s.ux = a.ux + off + 2 * t;
+  s.stride = 1;
+  mie_prepare(x, m, n, s);
+  ValueSums vs;
+  double2* out = reinterpret_cast<double2*>(a.coeffs) + 2 * off;
+  double asum = mie_finish(x, m, n, s, vs, [&](int64_t k, cplx an, cplx bn) {
+    out[k - 1] = make_double2(an.re, an.im);
+    out[n + k - 1] = make_double2(bn.re, bn.im);
+  });
+  Eff e = efficiencies_from(x, asum, vs);
+  if (a.eff) {
+    a.eff[5 * t] = e.q_ext;
+    a.eff[5 * t + 1] = e.q_sca;
+    a.eff[5 * t + 2] = e.q_abs;
+    a.eff[5 * t + 3] = e.q_back;
+    a.eff[5 * t + 4] = e.g;
+  }
+}
+
+void launch_plan_chunks(const MieFixedArgs& a, cudaStream_t s) {
+  int threads = 128;
+  int blocks = (a.n_chunks * 32 + threads - 1) / threads;
+  plan_chunks_kernel<<<blocks, threads, 0, s>>>(a);
+}
+
+void launch_mie_fixed(const MieFixedArgs& a, cudaStream_t s) {
+  int threads = 128;
+  int blocks = (a.n_chunks * 32 + threads - 1) / threads;
+  mie_fixed_kernel<<<blocks, threads, 0, s>>>(a);
+}
+
+void launch_mie_nodes(const MieNodesArgs& a, cudaStream_t s) {
+  int threads = 128;
+  int blocks = (int)((a.n + threads - 1) / threads);
+  mie_nodes_kernel<<<blocks, threads, 0, s>>>(a);
+}
+
+}  // namespace sb

@@ -1,0 +1,36 @@
+// Host-side tables shared by every launch: Gauss-Legendre rules, the generalized spherical
+// functions of the projection, the pi/tau tables of the angle GEMMs, and the size
+// distributions' densities. Compiled with -ffp-contract=off so that the tables hold the
+// reference's doubles.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace sb {
+
+// n-point Gauss-Legendre rule on [-1, 1], nodes ascending, exactly symmetric
+// (scatrs/src/special/gauss_legendre.rs:188-260).
+void gauss_legendre(int64_t n, double* nodes, double* weights);
+
+// d^l_{mn}(x) for l = 0..len-1 and |m|, |n| <= 2 (scatrs/src/special/wigner.rs:152-184).
+void wigner_d(int m, int n, double x, double* out, int64_t len);
+
+// (w pi_n, w tau_n) at cosine mu for n = 1..n_max into ge/go split by parity: G_E holds w pi_n
+// for odd n and w tau_n for even n, G_O the other (scatrs/src/ensemble/fast.rs:31-45 with
+// scatrs/src/mie/amplitudes.rs:52-65).
+void pi_tau_row(double mu, int64_t n_max, double* ge, double* go);
+
+// The number of terms of the band containing n (engine.rs:951-957) and its index in the
+// sequence 1, 2, 3, 4, 5, 7, 9, ...
+int64_t bucket(int64_t n);
+int band_index(int64_t n);
+int64_t band_upper(int index);
+
+// Size distributions (scatrs/src/ensemble/distribution.rs): validation and the unnormalized
+// density u(r).
+bool validate_distribution(int kind, const double* p, std::string* msg);
+double density(int kind, const double* p, double r);
+
+}  // namespace sb

@@ -1,0 +1,84 @@
+"""Seeded synthetic inputs of the benchmark configurations (no dataset is involved: every
+input is drawn from numpy's default_rng with a recorded seed).
+
+* ``config1``: spheres m = 1.43 + 1e-8 i; lognormal r_g = 0.08, sigma_g = 1.6; wavelengths
+  0.35, 0.55, 1.0; 256 Gauss nodes in ln r over r_g sigma_g^(+-5); 180 Gauss cosines; L = 32.
+* ``config2``: 1024 wavelengths log-spaced over 0.3-2.5; 64 lognormals (median log-uniform
+  0.05-5, width uniform 1.2-2.2); m per (distribution, wavelength) with Re uniform 1.33-1.60 and
+  Im log-uniform 1e-8-1e-1; 512 Gauss nodes over median width^(+-4); 360 Gauss cosines; L = 64.
+  ``scale`` keeps the first fraction of the wavelengths and distributions for smaller cases of
+  the same shape.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from ._native import DIST_DTYPE, KINDS
+
+
+@dataclass
+class Workload:
+    name: str
+    dists: np.ndarray       # DIST_DTYPE, (n_dist,)
+    wavelengths: np.ndarray  # (n_wl,)
+    m: np.ndarray            # complex128 (n_dist, n_wl)
+    mu: np.ndarray           # cosines
+    n_nodes: int
+    greek_order: int
+
+    @property
+    def n_units(self) -> int:
+        return self.dists.size * self.wavelengths.size
+
+    @property
+    def n_nodes_total(self) -> int:
+        return self.n_units * self.n_nodes
+
+
+def gauss_legendre(n: int) -> np.ndarray:
+    """Gauss-Legendre cosines from the library's own rule (the same on every machine)."""
+    from ._native import gauss_legendre as gl
+
+    return gl(n)[0]
+
+
+def lognormals(median, width, spread) -> np.ndarray:
+    median = np.atleast_1d(np.asarray(median, dtype=np.float64))
+    width = np.broadcast_to(np.asarray(width, dtype=np.float64), median.shape)
+    d = np.zeros(median.size, dtype=DIST_DTYPE)
+    d["kind"] = KINDS["lognormal"]
+    d["param"][:, 0] = median
+    d["param"][:, 1] = width
+    d["r_lo"] = median * width ** (-float(spread))
+    d["r_hi"] = median * width ** float(spread)
+    return d
+
+
+def config1(mu: np.ndarray | None = None) -> Workload:
+    wl = np.array([0.35, 0.55, 1.0])
+    d = lognormals(0.08, 1.6, 5)
+    m = np.full((1, wl.size), 1.43 + 1e-8j)
+    mu = gauss_legendre(180) if mu is None else mu
+    return Workload("config1", d, wl, m, mu, 256, 32)
+
+
+def config2(seed: int = 0, scale: float = 1.0, mu: np.ndarray | None = None) -> Workload:
+    rng = np.random.default_rng(seed)
+    n_dist, n_wl = 64, 1024
+    wl = np.geomspace(0.3, 2.5, n_wl)
+    med = np.exp(rng.uniform(np.log(0.05), np.log(5.0), n_dist))
+    wid = rng.uniform(1.2, 2.2, n_dist)
+    m_re = rng.uniform(1.33, 1.60, (n_dist, n_wl))
+    m_im = np.exp(rng.uniform(np.log(1e-8), np.log(1e-1), (n_dist, n_wl)))
+    m = m_re + 1j * m_im
+    if scale < 1.0:
+        kd = max(1, int(round(n_dist * scale)))
+        kw = max(1, int(round(n_wl * scale)))
+        med, wid, m = med[:kd], wid[:kd], m[:kd, :kw]
+        wl = wl[:kw]
+    mu = gauss_legendre(360) if mu is None else mu
+    return Workload(f"config2(seed={seed},scale={scale})", lognormals(med, wid, 4), wl, m, mu,
+                    512, 64)
