@@ -89,9 +89,10 @@ def cpu_sample(w, seconds: float, seed: int = 12345):
         t_total += time.perf_counter() - t0
         nodes += sel.size * w.n_nodes
     return {"value": nodes / t_total, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{k} random units ({nodes} nodes) of the batch, {t_total:.1f} s, "
-                      f"oracle (f64 restatement of the reference) with OpenMP over each "
-                      f"unit's... one unit at a time, {threads} threads"}
+            "sample": f"{k} random (distribution, wavelength) units of the batch ({nodes} "
+                      f"nodes) in {t_total:.1f} s: the oracle (f64 restatement of the "
+                      f"reference), one unit per call, OpenMP inside each call, {threads} "
+                      f"threads"}
 
 
 def reference_arm(args):

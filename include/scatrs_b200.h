@@ -132,8 +132,9 @@ int64_t scatrs_launch_count(void);
 
 /* Per-kernel timing for profiling runs: with on = 1, every launch is bracketed by CUDA events on
  * its stream; scatrs_kernel_times synchronizes and returns, for the kernels 0 plan_chunks,
- * 1 mie_fixed (K-a), 2 unit (K-b/c/d), 3 mie_nodes, the total milliseconds and launch counts
- * since the last scatrs_set_profiling call, and the number of kernels. */
+ * 1 mie_fixed (K-a), 2 unit (K-b/c), 3 mie_nodes, 4 final (the outputs), 5 proj (K-d), the total
+ * milliseconds and launch counts since the last scatrs_set_profiling call, and the number of
+ * kernels. */
 void scatrs_set_profiling(int32_t on);
 int scatrs_kernel_times(double* ms, int64_t* launches, int32_t n);
 

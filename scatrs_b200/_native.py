@@ -54,7 +54,8 @@ SYMBOLS = {
     "scatrs_kernel_times": (ctypes.c_int, [_PD, _PI64, _I32]),
 }
 
-KERNEL_NAMES = ("plan_chunks_kernel", "mie_fixed_kernel", "unit_kernel", "mie_nodes_kernel")
+KERNEL_NAMES = ("plan_chunks_kernel", "mie_fixed_kernel", "unit_kernel", "mie_nodes_kernel",
+                "final_kernel", "proj_kernel")
 
 _lib = None
 

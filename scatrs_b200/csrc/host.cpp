@@ -31,7 +31,7 @@ static std::atomic<int64_t> g_launches{0};
 
 // Optional per-kernel timing: CUDA events recorded around each launch on its stream, read back
 // by scatrs_kernel_times (which synchronizes). Off unless scatrs_set_profiling(1).
-enum KernelId { K_PLAN = 0, K_MIE = 1, K_UNITS = 2, K_NODES = 3, K_COUNT = 4 };
+enum KernelId { K_PLAN = 0, K_MIE = 1, K_UNITS = 2, K_NODES = 3, K_FINAL = 4, K_PROJ = 5, K_COUNT = 6 };
 static bool g_profiling = false;
 struct Timed {
   int id;
@@ -62,8 +62,8 @@ namespace {
 
 constexpr int64_t kMaxGreekOrder = 1 << 21;        // MAX_GREEK_ORDER (mie/greek.rs:344)
 constexpr int64_t kMaxMieValues = 1 << 27;         // scatrs-py/src/mie.rs:30
-constexpr int64_t kArenaRows = 1 << 20;            // coefficient rows per slab (1 KiB each)
-constexpr int64_t kMaxSlabChunks = 1 << 16;        // chunks per slab
+constexpr int64_t kArenaRows = 1 << 22;            // coefficient rows per slab (1 KiB each)
+constexpr int64_t kMaxSlabChunks = 1 << 18;        // chunks per slab
 
 struct Failure {
   int status;
@@ -139,7 +139,8 @@ struct Context {
   UserTables user;
   std::map<int, BandTables> bands;  // by Greek order
   std::map<int64_t, std::pair<std::vector<double>, std::vector<double>>> rules;
-  DevBuf radius, weight, wl, m, chunk_n, chunk_row, chunk_order, unit_order, X, uz, ux,
+  DevBuf radius, weight, wl, m, chunk_n, chunk_n_slab, chunk_row, chunk_acc, plan_units,
+      unit_acc, unit_slots, slots, items, proj_items, slot_index, slot_greek, X, uz, ux,
       chunk_sums, err, acc, counter, values, phase, greek;
   std::vector<int> chunk_n_host;
   int* pinned_chunk_n = nullptr;
@@ -220,9 +221,17 @@ void ensure_user(Context& c, const double* mu, int64_t n_mu, int64_t n_orders, c
   u.h = (int)cosines.size();
   u.h_pad = (int)round_up(std::max(u.h, 1), 32);
   u.ld = (int)u.n_orders;
+  // Order-major (transposed) tables: element (row, order k) at k * h_pad + row, so that one
+  // order of a 32-row tile is 256 contiguous bytes.
   std::vector<double> ge((size_t)u.h_pad * u.ld, 0.0), go((size_t)u.h_pad * u.ld, 0.0);
-  for (int r = 0; r < u.h; ++r)
-    pi_tau_row(cosines[r], u.n_orders, &ge[(size_t)r * u.ld], &go[(size_t)r * u.ld]);
+  std::vector<double> re(u.ld), ro(u.ld);
+  for (int r = 0; r < u.h; ++r) {
+    pi_tau_row(cosines[r], u.n_orders, re.data(), ro.data());
+    for (int k = 0; k < u.ld; ++k) {
+      ge[(size_t)k * u.h_pad + r] = re[k];
+      go[(size_t)k * u.h_pad + r] = ro[k];
+    }
+  }
   SB_CUDA(cudaMemcpyAsync(u.ge.get(ge.size() * 8), ge.data(), ge.size() * 8,
                           cudaMemcpyHostToDevice, s));
   SB_CUDA(cudaMemcpyAsync(u.go.get(go.size() * 8), go.data(), go.size() * 8,
@@ -255,9 +264,17 @@ BandTables& ensure_bands(Context& c, int L, int last_band, cudaStream_t s) {
     d.d_off = (int64_t)bt.d.size();
     bt.ge.resize(bt.ge.size() + (size_t)d.h_pad * d.ld, 0.0);
     bt.go.resize(bt.go.size() + (size_t)d.h_pad * d.ld, 0.0);
-    for (int i = 0; i < d.h; ++i)
-      pi_tau_row(r.first[lo + i], upper, &bt.ge[d.g_off + (size_t)i * d.ld],
-                 &bt.go[d.g_off + (size_t)i * d.ld]);
+    {
+      // Order-major, as the requested cosines' tables.
+      std::vector<double> re(upper), ro(upper);
+      for (int i = 0; i < d.h; ++i) {
+        pi_tau_row(r.first[lo + i], upper, re.data(), ro.data());
+        for (int64_t k = 0; k < upper; ++k) {
+          bt.ge[d.g_off + (size_t)k * d.h_pad + i] = re[k];
+          bt.go[d.g_off + (size_t)k * d.h_pad + i] = ro[k];
+        }
+      }
+    }
     int64_t len = order + 1;
     bt.d.resize(bt.d.size() + 4 * (size_t)n_q * len);
     std::vector<double> buf(len);
@@ -358,7 +375,261 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
                           cudaMemcpyHostToDevice, s));
   unsigned long long* err = c.err.as<unsigned long long>(2);
   SB_CUDA(cudaMemsetAsync(err, 0xff, 2 * sizeof(unsigned long long), s));
-  // 2. Plan.
+  // 2. Plan: every chunk's largest number of terms.
+  PlanArgs pa{};
+  pa.radius = c.radius.as<double>(0);
+  pa.wl = wl_dev;
+  pa.n_dist = (int)n_dist;
+  pa.n_wl = (int)n_wl;
+  pa.n_nodes = (int)n_nodes;
+  pa.cpu = cpu;
+  pa.n_chunks = n_chunks;
+  int* chunk_n_all = c.chunk_n.as<int>(n_chunks);
+  pa.chunk_n = chunk_n_all;
+  timed_launch(K_PLAN, s, [&] { launch_plan_chunks(pa, s); });
+  SB_CUDA(cudaGetLastError());
+  if (c.pinned_cap < (size_t)n_chunks) {
+    if (c.pinned_chunk_n) cudaFreeHost(c.pinned_chunk_n);
+    c.pinned_chunk_n = nullptr;
+    c.pinned_cap = 0;
+    SB_CUDA(cudaMallocHost(&c.pinned_chunk_n, n_chunks * sizeof(int)));
+    c.pinned_cap = n_chunks;
+  }
+  const int* cn = c.pinned_chunk_n;
+  SB_CUDA(cudaMemcpyAsync(c.pinned_chunk_n, chunk_n_all, n_chunks * sizeof(int),
+                          cudaMemcpyDeviceToHost, s));
+  SB_CUDA(cudaStreamSynchronize(s));
+  int n_max = 1;
+  for (int64_t k = 0; k < n_chunks; ++k) n_max = std::max(n_max, cn[k]);
+  // Tables.
+  const int L = opt->greek_order;
+  ensure_user(c, mu, n_mu, n_max, s);
+  BandTables* bt = nullptr;
+  if (L >= 0) bt = &ensure_bands(c, L, band_index(n_max), s);
+  // 3. Slabs. Each unit's work: its chunks' rows times the table rows they meet.
+  std::vector<int> band_of_n(n_max + 1, -1);
+  if (bt) {
+    int b = 0;
+    for (int n = 1; n <= n_max; ++n) {
+      while (bt->desc[b].upper < n) ++b;
+      band_of_n[n] = b;
+    }
+  }
+  const int t_user = (c.user.h + 31) / 32;
+  const int64_t acc_head = 4 * n_mu;
+  std::vector<int64_t> urows(n_units), uacc(n_units);
+  std::vector<double> ucost(n_units);
+  int64_t total_rows = 0;
+  for (int64_t u = 0; u < n_units; ++u) {
+    int64_t rows = 0, acc = acc_head;
+    double cost = 0.0;
+    int prev = -1;
+    for (int k = 0; k < cpu; ++k) {
+      int nc = cn[u * cpu + k];
+      rows += nc;
+      int tiles = t_user;
+      if (bt && nc > 0) {
+        int b = band_of_n[nc];
+        tiles += (bt->desc[b].h + 31) / 32;
+        if (b != prev) acc += 4 * (int64_t)bt->desc[b].n_q;
+        prev = b;
+      }
+      cost += (double)tiles * ((double)nc + 24.0);
+    }
+    urows[u] = rows;
+    uacc[u] = acc;
+    ucost[u] = cost;
+    total_rows += rows;
+  }
+  const int64_t max_urows = *std::max_element(urows.begin(), urows.end());
+  const int64_t arena = std::max<int64_t>(kArenaRows, 2 * max_urows);
+  std::vector<int> by_cost(n_units);
+  for (int64_t u = 0; u < n_units; ++u) by_cost[u] = (int)u;
+  std::sort(by_cost.begin(), by_cost.end(), [&](int x, int y) {
+    return ucost[x] != ucost[y] ? ucost[x] > ucost[y] : x < y;
+  });
+  // Deal the units, largest first, in snake order over n_slabs slabs: every slab gets the same
+  // mix of large and small units. More slabs while one overflows the arena.
+  int64_t n_slabs = std::max<int64_t>(1, (total_rows + arena - 1) / arena);
+  n_slabs = std::max<int64_t>(n_slabs, (n_chunks + kMaxSlabChunks - 1) / kMaxSlabChunks);
+  std::vector<int> slab_of(n_units);
+  for (;;) {
+    std::vector<int64_t> rows(n_slabs, 0), chunks(n_slabs, 0);
+    bool fits = true;
+    for (int64_t k = 0; k < n_units; ++k) {
+      int64_t round = k / n_slabs, pos = k % n_slabs;
+      int64_t sl = (round & 1) ? n_slabs - 1 - pos : pos;
+      slab_of[by_cost[k]] = (int)sl;
+      rows[sl] += urows[by_cost[k]];
+      chunks[sl] += cpu;
+      if (rows[sl] > arena || chunks[sl] > kMaxSlabChunks) fits = false;
+    }
+    if (fits) break;
+    ++n_slabs;
+  }
+  // Per slab: units (largest first), chunk tables, accumulator layout, work items.
+  const int grid_max = c.sms * c.unit_bps;
+  double total_cost = 0.0;
+  for (double v : ucost) total_cost += v;
+  const double item_target = std::max(1.0, total_cost / (double)n_slabs / (4.0 * grid_max));
+  struct Slab {
+    int64_t u0, nu;        // into the flat unit list
+    int64_t ch0;           // into the flat chunk tables
+    int64_t it0, n_items;  // into the flat item list
+    int64_t sl0;           // into the flat band-slot list
+    int64_t n_slots;
+    int64_t pi0, n_proj;   // into the flat projection items
+    int64_t si0;           // into the flat slot-index list
+    int64_t acc_len;
+  };
+  std::vector<Slab> slabs(n_slabs);
+  std::vector<int> units_flat;
+  units_flat.reserve(n_units);
+  {
+    std::vector<std::vector<int>> members(n_slabs);
+    for (int64_t k = 0; k < n_units; ++k) members[slab_of[by_cost[k]]].push_back(by_cost[k]);
+    int64_t u0 = 0;
+    for (int64_t sl = 0; sl < n_slabs; ++sl) {
+      slabs[sl].u0 = u0;
+      slabs[sl].nu = (int64_t)members[sl].size();
+      for (int u : members[sl]) units_flat.push_back(u);
+      u0 += slabs[sl].nu;
+    }
+  }
+  std::vector<int> chunk_n_flat(n_chunks);
+  std::vector<int64_t> chunk_row_flat(n_chunks), chunk_acc_flat(n_chunks);
+  std::vector<int64_t> unit_acc_flat(n_units);
+  std::vector<int2> unit_slots_flat(n_units);
+  std::vector<BandSlot> slots_flat;
+  std::vector<WorkItem> items_flat;
+  std::vector<int> slot_index_flat;   // per slab: slab-local slots grouped by band
+  std::vector<ProjItem> proj_flat;
+  int64_t slots_max = 1;
+  int64_t acc_max = 1;
+  for (int64_t sl = 0; sl < n_slabs; ++sl) {
+    Slab& S = slabs[sl];
+    S.ch0 = S.u0 * cpu;
+    S.it0 = (int64_t)items_flat.size();
+    S.sl0 = (int64_t)slots_flat.size();
+    int64_t row = 0, acc = 0;
+    std::vector<std::pair<double, WorkItem>> items;
+    for (int64_t lu = 0; lu < S.nu; ++lu) {
+      const int u = units_flat[S.u0 + lu];
+      unit_acc_flat[S.u0 + lu] = acc;
+      int64_t band_acc = acc + acc_head;
+      int2 us = make_int2((int)(slots_flat.size() - S.sl0), 0);
+      int prev = -1;
+      int max_tiles = 0;
+      for (int k = 0; k < cpu; ++k) {
+        const int64_t g = S.ch0 + lu * cpu + k;
+        const int nc = cn[(int64_t)u * cpu + k];
+        chunk_n_flat[g] = nc;
+        chunk_row_flat[g] = row;
+        row += nc;
+        chunk_acc_flat[g] = -1;
+        int tiles = t_user;
+        if (bt && nc > 0) {
+          const int b = band_of_n[nc];
+          if (b != prev) {
+            BandSlot bs;
+            bs.band = b;
+            bs.unit = (int)lu;
+            bs.off = band_acc;
+            slots_flat.push_back(bs);
+            us.y += 1;
+            band_acc += 4 * (int64_t)bt->desc[b].n_q;
+            prev = b;
+          }
+          chunk_acc_flat[g] = slots_flat.back().off;
+          tiles += (bt->desc[b].h + 31) / 32;
+        }
+        max_tiles = std::max(max_tiles, tiles);
+      }
+      unit_slots_flat[S.u0 + lu] = us;
+      acc += uacc[u];
+      int groups = (int)std::min<double>(std::max(1.0, std::ceil(ucost[u] / item_target)),
+                                         (double)std::max(max_tiles, 1));
+      for (int gi = 0; gi < groups; ++gi) {
+        WorkItem w;
+        w.unit = (int)lu;
+        w.group = gi;
+        w.n_groups = groups;
+        w.pad = 0;
+        items.emplace_back(ucost[u] / groups, w);
+      }
+    }
+    std::stable_sort(items.begin(), items.end(),
+                     [](const std::pair<double, WorkItem>& x,
+                        const std::pair<double, WorkItem>& y) { return x.first > y.first; });
+    for (auto& it : items) items_flat.push_back(it.second);
+    S.n_items = (int64_t)items.size();
+    S.acc_len = acc;
+    acc_max = std::max(acc_max, acc);
+    // Projection tiles: the slab's slots grouped by band, 32 at a time.
+    S.n_slots = (int64_t)slots_flat.size() - S.sl0;
+    slots_max = std::max(slots_max, S.n_slots);
+    S.pi0 = (int64_t)proj_flat.size();
+    S.si0 = (int64_t)slot_index_flat.size();
+    if (bt && S.n_slots > 0) {
+      std::vector<std::vector<int>> by_band(bt->n_bands);
+      for (int64_t k = 0; k < S.n_slots; ++k) by_band[slots_flat[S.sl0 + k].band].push_back((int)k);
+      const int64_t base = S.si0;
+      for (int b = bt->n_bands - 1; b >= 0; --b) {
+        for (size_t k0 = 0; k0 < by_band[b].size(); k0 += 32) {
+          ProjItem pi;
+          pi.band = b;
+          pi.count = (int)std::min<size_t>(32, by_band[b].size() - k0);
+          pi.first = (int64_t)slot_index_flat.size() - base + (int64_t)k0;
+          proj_flat.push_back(pi);
+        }
+        slot_index_flat.insert(slot_index_flat.end(), by_band[b].begin(), by_band[b].end());
+      }
+    }
+    S.n_proj = (int64_t)proj_flat.size() - S.pi0;
+  }
+  // Upload the plan once.
+  const size_t bytes_units = units_flat.size() * sizeof(int);
+  int* units_d = c.plan_units.as<int>(units_flat.size());
+  int* chunk_n_d = c.chunk_n_slab.as<int>(n_chunks);
+  int64_t* chunk_row_d = c.chunk_row.as<int64_t>(n_chunks);
+  int64_t* chunk_acc_d = c.chunk_acc.as<int64_t>(n_chunks);
+  int64_t* unit_acc_d = c.unit_acc.as<int64_t>(n_units);
+  int2* unit_slots_d = c.unit_slots.as<int2>(n_units);
+  BandSlot* slots_d = c.slots.as<BandSlot>(std::max<size_t>(slots_flat.size(), 1));
+  WorkItem* items_d = c.items.as<WorkItem>(items_flat.size());
+  ProjItem* proj_d = c.proj_items.as<ProjItem>(std::max<size_t>(proj_flat.size(), 1));
+  int* slot_index_d = c.slot_index.as<int>(std::max<size_t>(slot_index_flat.size(), 1));
+  if (!proj_flat.empty()) {
+    SB_CUDA(cudaMemcpyAsync(proj_d, proj_flat.data(), proj_flat.size() * sizeof(ProjItem),
+                            cudaMemcpyHostToDevice, s));
+    SB_CUDA(cudaMemcpyAsync(slot_index_d, slot_index_flat.data(),
+                            slot_index_flat.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+  }
+  SB_CUDA(cudaMemcpyAsync(units_d, units_flat.data(), bytes_units, cudaMemcpyHostToDevice, s));
+  SB_CUDA(cudaMemcpyAsync(chunk_n_d, chunk_n_flat.data(), n_chunks * sizeof(int),
+                          cudaMemcpyHostToDevice, s));
+  SB_CUDA(cudaMemcpyAsync(chunk_row_d, chunk_row_flat.data(), n_chunks * 8,
+                          cudaMemcpyHostToDevice, s));
+  SB_CUDA(cudaMemcpyAsync(chunk_acc_d, chunk_acc_flat.data(), n_chunks * 8,
+                          cudaMemcpyHostToDevice, s));
+  SB_CUDA(cudaMemcpyAsync(unit_acc_d, unit_acc_flat.data(), n_units * 8, cudaMemcpyHostToDevice,
+                          s));
+  SB_CUDA(cudaMemcpyAsync(unit_slots_d, unit_slots_flat.data(), n_units * sizeof(int2),
+                          cudaMemcpyHostToDevice, s));
+  if (!slots_flat.empty())
+    SB_CUDA(cudaMemcpyAsync(slots_d, slots_flat.data(), slots_flat.size() * sizeof(BandSlot),
+                            cudaMemcpyHostToDevice, s));
+  SB_CUDA(cudaMemcpyAsync(items_d, items_flat.data(), items_flat.size() * sizeof(WorkItem),
+                          cudaMemcpyHostToDevice, s));
+  // Buffers.
+  double* X = c.X.as<double>((size_t)arena * 128);
+  double2* uz = c.uz.as<double2>((size_t)(arena + 2 * kMaxSlabChunks) * 32);
+  double* ux = c.ux.as<double>((size_t)(arena + 2 * kMaxSlabChunks) * 32);
+  double* chunk_sums = c.chunk_sums.as<double>((size_t)kMaxSlabChunks * 8);
+  double* acc = c.acc.as<double>((size_t)acc_max);
+  double* slot_greek = L >= 0 ? c.slot_greek.as<double>((size_t)slots_max * 6 * (L + 1)) : nullptr;
+  int* counter = c.counter.as<int>(64);
+  // 4. Launches, slab by slab.
   MieFixedArgs ka{};
   ka.radius = c.radius.as<double>(0);
   ka.weight = c.weight.as<double>(0);
@@ -368,94 +639,12 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
   ka.n_wl = (int)n_wl;
   ka.n_nodes = (int)n_nodes;
   ka.cpu = cpu;
-  ka.unit0 = 0;
-  ka.n_chunks = (int)n_chunks;
-  int* chunk_n = c.chunk_n.as<int>(n_chunks);
-  ka.chunk_n = chunk_n;
+  ka.X = X;
+  ka.uz = uz;
+  ka.ux = ux;
+  ka.chunk_sums = chunk_sums;
   ka.err = err;
   ka.allow_unvalidated = opt->allow_unvalidated;
-  timed_launch(K_PLAN, s, [&] { launch_plan_chunks(ka, s); });
-  SB_CUDA(cudaGetLastError());
-  if (c.pinned_cap < (size_t)n_chunks) {
-    if (c.pinned_chunk_n) cudaFreeHost(c.pinned_chunk_n);
-    c.pinned_chunk_n = nullptr;
-    c.pinned_cap = 0;
-    SB_CUDA(cudaMallocHost(&c.pinned_chunk_n, n_chunks * sizeof(int)));
-    c.pinned_cap = n_chunks;
-  }
-  int* cn = c.pinned_chunk_n;
-  SB_CUDA(cudaMemcpyAsync(cn, chunk_n, n_chunks * sizeof(int), cudaMemcpyDeviceToHost, s));
-  SB_CUDA(cudaStreamSynchronize(s));
-  int n_max = 0;
-  for (int64_t k = 0; k < n_chunks; ++k) n_max = std::max(n_max, cn[k]);
-  // Tables.
-  const int L = opt->greek_order;
-  ensure_user(c, mu, n_mu, std::max(n_max, 1), s);
-  BandTables* bt = nullptr;
-  if (L >= 0) bt = &ensure_bands(c, L, band_index(std::max(n_max, 1)), s);
-  // 3. Slabs of whole units whose coefficient rows fit the arena.
-  std::vector<int64_t> rows(n_chunks);
-  const int64_t arena = std::max<int64_t>(kArenaRows, (int64_t)cpu * n_max);
-  double* X = c.X.as<double>((size_t)arena * 128);
-  // Scratch rows of a chunk: its N_c + 2 orders of u_k(mx) and u_k(x).
-  const int64_t max_slab_chunks = std::max<int64_t>(kMaxSlabChunks, cpu);
-  double2* uz = c.uz.as<double2>((size_t)(arena + 2 * max_slab_chunks) * 32);
-  double* ux = c.ux.as<double>((size_t)(arena + 2 * max_slab_chunks) * 32);
-  int64_t* chunk_row = c.chunk_row.as<int64_t>(n_chunks);
-  double* chunk_sums = c.chunk_sums.as<double>((size_t)n_chunks * 8);
-  std::vector<int64_t> slab_begin;  // unit index
-  {
-    int64_t used = 0;
-    slab_begin.push_back(0);
-    for (int64_t u = 0; u < n_units; ++u) {
-      int64_t need = 0;
-      for (int k = 0; k < cpu; ++k) need += cn[u * cpu + k];
-      int64_t slab_units = u - slab_begin.back();
-      int64_t slab_chunks = (slab_units + 1) * cpu;
-      if (slab_units > 0 && (used + need > arena || slab_chunks > max_slab_chunks)) {
-        slab_begin.push_back(u);
-        used = 0;
-      }
-      int64_t base = used;
-      for (int k = 0; k < cpu; ++k) {
-        rows[u * cpu + k] = base;
-        base += cn[u * cpu + k];
-      }
-      used += need;
-    }
-    slab_begin.push_back(n_units);
-  }
-  SB_CUDA(cudaMemcpyAsync(chunk_row, rows.data(), n_chunks * 8, cudaMemcpyHostToDevice, s));
-  // Per-CTA accumulators of the unit kernel.
-  const int grid_max = c.sms * c.unit_bps;
-  const int nq_max = bt ? bt->nq_max : 0;
-  const int64_t acc_stride = round_up(4 * n_mu + 4 * (int64_t)nq_max + (L >= 0 ? 6 * (L + 1) : 0), 32);
-  double* acc = c.acc.as<double>((size_t)grid_max * std::max<int64_t>(acc_stride, 1));
-  int* counter = c.counter.as<int>(64);
-  // Processing order inside a slab: units with the most work first.
-  std::vector<int> order;
-  int* unit_order_d = c.unit_order.as<int>(n_units);
-  {
-    std::vector<int> all(n_units);
-    for (size_t si = 0; si + 1 < slab_begin.size(); ++si) {
-      int64_t u0 = slab_begin[si], u1 = slab_begin[si + 1];
-      std::vector<std::pair<int64_t, int>> cost;
-      cost.reserve(u1 - u0);
-      for (int64_t u = u0; u < u1; ++u) {
-        int64_t w = 0;
-        for (int k = 0; k < cpu; ++k) {
-          int64_t nc = cn[u * cpu + k];
-          w += nc * ((int64_t)c.user.h + (L >= 0 ? (nc + L / 2) / 2 : 0)) + 64;
-        }
-        cost.emplace_back(-w, (int)(u - u0));
-      }
-      std::sort(cost.begin(), cost.end());
-      for (int64_t k = 0; k < u1 - u0; ++k) all[u0 + k] = cost[k].second;
-    }
-    SB_CUDA(cudaMemcpyAsync(unit_order_d, all.data(), n_units * sizeof(int),
-                            cudaMemcpyHostToDevice, s));
-    SB_CUDA(cudaStreamSynchronize(s));
-  }
   UnitArgs ua{};
   ua.radius = ka.radius;
   ua.weight = ka.weight;
@@ -468,51 +657,79 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
   ua.n_mu = (int)n_mu;
   ua.h_u = c.user.h;
   ua.h_u_pad = c.user.h_pad;
-  ua.ld_u = c.user.ld;
   ua.ge_u = c.user.ge.as<double>(0);
   ua.go_u = c.user.go.as<double>(0);
   ua.user_map = c.user.map.as<int2>(0);
   ua.greek_order = L;
   if (bt) {
-    ua.n_bands = bt->n_bands;
     ua.bands = bt->desc_d.as<BandDesc>(0);
     ua.band_ge = bt->ge_d.as<double>(0);
     ua.band_go = bt->go_d.as<double>(0);
-    ua.band_d = bt->d_d.as<double>(0);
   }
-  ua.nq_max = nq_max;
-  ua.n_units_total = n_units;
-  ua.values = values;
-  ua.phase = n_mu > 0 ? phase : nullptr;
-  ua.greek = L >= 0 ? greek : nullptr;
-  ua.normalized = opt->normalized;
   ua.acc = acc;
-  ua.acc_stride = acc_stride;
   ua.work_counter = counter;
-  ua.err = err;
-  for (size_t si = 0; si + 1 < slab_begin.size(); ++si) {
-    int64_t u0 = slab_begin[si], u1 = slab_begin[si + 1];
-    int64_t nu = u1 - u0;
-    ka.unit0 = u0;
-    ka.n_chunks = (int)(nu * cpu);
-    ka.chunk_order = nullptr;
-    ka.chunk_n = chunk_n + u0 * cpu;
-    ka.chunk_row = chunk_row + u0 * cpu;
-    ka.X = X;
-    ka.uz = uz;
-    ka.ux = ux;
-    ka.chunk_sums = chunk_sums + u0 * cpu * 8;
+  ProjArgs pj{};
+  pj.cpu = cpu;
+  pj.greek_order = L;
+  pj.acc = acc;
+  pj.chunk_sums = chunk_sums;
+  pj.slot_greek = slot_greek;
+  if (bt) {
+    pj.bands = bt->desc_d.as<BandDesc>(0);
+    pj.band_d = bt->d_d.as<double>(0);
+  }
+  FinalArgs fa{};
+  fa.cpu = cpu;
+  fa.n_dist = (int)n_dist;
+  fa.n_wl = (int)n_wl;
+  fa.chunk_sums = chunk_sums;
+  fa.n_mu = (int)n_mu;
+  fa.greek_order = L;
+  if (bt) fa.bands = ua.bands;
+  fa.slot_greek = slot_greek;
+  fa.acc = acc;
+  fa.n_units_total = n_units;
+  fa.values = values;
+  fa.phase = n_mu > 0 ? phase : nullptr;
+  fa.greek = L >= 0 ? greek : nullptr;
+  fa.normalized = opt->normalized;
+  fa.err = err;
+  for (int64_t sl = 0; sl < n_slabs; ++sl) {
+    const Slab& S = slabs[sl];
+    if (S.nu == 0) continue;
+    ka.units = units_d + S.u0;
+    ka.n_chunks = (int)(S.nu * cpu);
+    ka.chunk_n = chunk_n_d + S.ch0;
+    ka.chunk_row = chunk_row_d + S.ch0;
     timed_launch(K_MIE, s, [&] { launch_mie_fixed(ka, s); });
     SB_CUDA(cudaGetLastError());
+    SB_CUDA(cudaMemsetAsync(acc, 0, (size_t)S.acc_len * 8, s));
     SB_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), s));
-    ua.unit0 = u0;
-    ua.n_units = (int)nu;
-    ua.unit_order = unit_order_d + u0;
+    ua.units = ka.units;
+    ua.n_items = (int)S.n_items;
+    ua.items = items_d + S.it0;
     ua.chunk_n = ka.chunk_n;
     ua.chunk_row = ka.chunk_row;
-    ua.chunk_sums = ka.chunk_sums;
-    int grid = (int)std::min<int64_t>(grid_max, nu);
+    ua.chunk_acc = chunk_acc_d + S.ch0;
+    ua.unit_acc = unit_acc_d + S.u0;
+    const int grid = (int)std::min<int64_t>(grid_max, S.n_items);
     timed_launch(K_UNITS, s, [&] { launch_units(ua, grid, s); });
+    SB_CUDA(cudaGetLastError());
+    if (bt && S.n_proj > 0) {
+      pj.items = proj_d + S.pi0;
+      pj.n_items = (int)S.n_proj;
+      // slot_index holds slab-local slot numbers; the slab's slot list starts at sl0.
+      pj.slot_index = slot_index_d + S.si0;
+      pj.slots = slots_d + S.sl0;
+      timed_launch(K_PROJ, s, [&] { launch_proj(pj, s); });
+      SB_CUDA(cudaGetLastError());
+    }
+    fa.units = ka.units;
+    fa.n_units = (int)S.nu;
+    fa.unit_acc = ua.unit_acc;
+    fa.unit_slots = unit_slots_d + S.u0;
+    fa.slots = slots_d + S.sl0;
+    timed_launch(K_FINAL, s, [&] { launch_final(fa, s); });
     SB_CUDA(cudaGetLastError());
   }
   if (call) {
@@ -769,8 +986,10 @@ void scatrs_release(void) {
   std::lock_guard<std::mutex> lk(g_ctx_mtx);
   if (dev < (int)g_ctx.size() && g_ctx[dev]) {
     Context& c = *g_ctx[dev];
-    for (DevBuf* b : {&c.radius, &c.weight, &c.wl, &c.m, &c.chunk_n, &c.chunk_row, &c.chunk_order,
-                      &c.unit_order, &c.X, &c.uz, &c.ux, &c.chunk_sums, &c.err, &c.acc,
+    for (DevBuf* b : {&c.radius, &c.weight, &c.wl, &c.m, &c.chunk_n, &c.chunk_n_slab,
+                      &c.chunk_row, &c.chunk_acc, &c.plan_units, &c.unit_acc, &c.unit_slots,
+                      &c.slots, &c.items, &c.proj_items, &c.slot_index, &c.slot_greek,
+                      &c.X, &c.uz, &c.ux, &c.chunk_sums, &c.err, &c.acc,
                       &c.counter, &c.values, &c.phase, &c.greek, &c.user.ge, &c.user.go,
                       &c.user.map})
       b->release();

@@ -7,17 +7,25 @@
 
 namespace sb {
 
-// K-a over one slab of units (consecutive units unit0 .. unit0 + n_chunks / cpu - 1).
+// The largest number of terms of every chunk of every unit (unit = chunk / cpu).
+struct PlanArgs {
+  const double* radius;  // [n_dist][n_nodes]
+  const double* wl;      // [n_wl]
+  int n_dist, n_wl, n_nodes, cpu;
+  int64_t n_chunks;
+  int* chunk_n;
+};
+
+// K-a over one slab: its units (global indices), each with cpu chunks of 32 nodes.
 struct MieFixedArgs {
   const double* radius;  // [n_dist][n_nodes]
   const double* weight;  // [n_dist][n_nodes]: w_j u(r_j) r_j
   const double* wl;      // [n_wl]
   const double2* m;      // [n_units_total]
   int n_dist, n_wl, n_nodes, cpu;
-  int64_t unit0;
-  int n_chunks;             // chunks of the slab
-  const int* chunk_order;   // slab-local launch order of the chunks, or null
-  int* chunk_n;             // slab-local: each chunk's largest number of terms
+  const int* units;         // slab-local unit -> global unit
+  int n_chunks;             // chunks of the slab (units x cpu)
+  const int* chunk_n;       // slab-local: each chunk's largest number of terms
   const int64_t* chunk_row; // slab-local: first coefficient row of each chunk
   double* X;                // coefficient rows, 128 doubles each
   double2* uz;              // scratch rows of u_k(mx), 32 lanes each
@@ -42,8 +50,8 @@ struct MieNodesArgs {
 };
 
 // One projector band (engine.rs:2034-2072): orders up to `order` on n_q Gauss nodes, the
-// pi/tau tables G_E, G_O of its h = ceil(n_q/2) non-negative nodes (h_pad rows of ld columns)
-// and the projection matrices (2l+1)/2 w_k d_l(mu_k) of d00, d22, d2-2, d02.
+// pi/tau tables G_E, G_O of its h = ceil(n_q/2) non-negative nodes (order-major: ld orders of
+// h_pad rows) and the projection matrices (2l+1)/2 w_k d_l(mu_k) of d00, d22, d2-2, d02.
 struct BandDesc {
   int upper;
   int order;
@@ -55,50 +63,102 @@ struct BandDesc {
   int64_t d_off;  // into band_d: 4 matrices of n_q x (order + 1)
 };
 
-// K-b, K-c and K-d over one slab of units.
+// A share of one unit's angle GEMMs: row tiles t (over the requested cosines' tiles, then the
+// chunk's band tiles) with t % n_groups == group, for every chunk of the unit.
+struct WorkItem {
+  int unit;  // slab-local
+  int group;
+  int n_groups;
+  int pad;
+};
+
+// One band accumulator of a unit: the band, the unit (slab-local) and the offset of its
+// 4 n_q doubles.
+struct BandSlot {
+  int band;
+  int unit;
+  int64_t off;
+};
+
+// A tile of up to 32 band slots of one band, projected together (they share the band's
+// projection matrices).
+struct ProjItem {
+  int band;
+  int count;
+  int64_t first;  // into ProjArgs::slot_index
+};
+
+// K-d over one slab: each band slot's averaged tables projected onto its Greek coefficients,
+// 6 (L + 1) doubles per slot at slot_greek + slot * 6 (L + 1).
+struct ProjArgs {
+  const ProjItem* items;
+  int n_items;
+  const int* slot_index;     // slab-local slots, grouped by band
+  const BandSlot* slots;
+  const BandDesc* bands;
+  const double* band_d;
+  const double* acc;
+  const double* chunk_sums;  // for each unit's Z
+  int cpu;
+  int greek_order;
+  double* slot_greek;
+};
+
+// K-b and K-c over one slab: the work items write the per-unit accumulators (zeroed before).
 struct UnitArgs {
   const double* radius;
   const double* weight;
   const double* wl;
   int n_dist, n_wl, n_nodes, cpu;
-  int64_t unit0;
-  int n_units;              // units of the slab
-  const int* unit_order;    // slab-local processing order, or null
-  const int* chunk_n;       // slab-local
-  const int64_t* chunk_row; // slab-local
+  const int* units;
+  int n_items;
+  const WorkItem* items;
+  const int* chunk_n;
+  const int64_t* chunk_row;
+  const int64_t* chunk_acc;  // offset of each chunk's band accumulator, or -1
+  const int64_t* unit_acc;   // offset of each unit's cosine accumulator (4 n_mu doubles)
   const double* X;
-  const double* chunk_sums;
-  // Phase matrix at the requested cosines: table rows (G_E, G_O of h_u rows, padded to
-  // h_u_pad, ld_u columns) and each row's output cosines (plus side, minus side or -1).
-  int n_mu, h_u, h_u_pad, ld_u;
+  // Phase matrix at the requested cosines: tables G_E, G_O of h_u rows (order-major: ld_u
+  // orders of h_u_pad rows) and each row's output cosines (plus side, minus side or -1).
+  int n_mu, h_u, h_u_pad;
   const double* ge_u;
   const double* go_u;
   const int2* user_map;
-  // Greek coefficients by bands (greek_order < 0: none).
   int greek_order;
-  int n_bands;
   const BandDesc* bands;
   const double* band_ge;
   const double* band_go;
-  const double* band_d;
-  int nq_max;
-  // Outputs over all units.
+  double* acc;
+  int* work_counter;
+};
+
+// K-d and the outputs over one slab: averages, band projections, assembly.
+struct FinalArgs {
+  const int* units;
+  int n_units;
+  int cpu, n_dist, n_wl;
+  const double* chunk_sums;
+  const int64_t* unit_acc;   // per unit: 4 n_mu cosine sums, then 6 (L + 1) Greek sums
+  const int2* unit_slots;    // per unit: first band slot and count
+  const BandSlot* slots;
+  const double* slot_greek;  // each slot's projected coefficients
+  int n_mu, greek_order;
+  const BandDesc* bands;
+  double* acc;
   int64_t n_units_total;
   double* values;
   double* phase;
   double* greek;
   int normalized;
-  // Per-CTA scratch: 4 n_mu + 4 nq_max + 6 (L + 1) doubles each.
-  double* acc;
-  int64_t acc_stride;
-  int* work_counter;
   unsigned long long* err;
 };
 
-void launch_plan_chunks(const MieFixedArgs& a, cudaStream_t s);
+void launch_plan_chunks(const PlanArgs& a, cudaStream_t s);
 void launch_mie_fixed(const MieFixedArgs& a, cudaStream_t s);
 void launch_mie_nodes(const MieNodesArgs& a, cudaStream_t s);
 int unit_kernel_blocks_per_sm();
 void launch_units(const UnitArgs& a, int grid, cudaStream_t s);
+void launch_proj(const ProjArgs& a, cudaStream_t s);
+void launch_final(const FinalArgs& a, cudaStream_t s);
 
 }  // namespace sb

@@ -20,11 +20,11 @@ __device__ __forceinline__ void record_error(unsigned long long* err, long long 
 }
 
 // Each chunk's largest number of terms (the band selector, engine.rs:961-978).
-__global__ void plan_chunks_kernel(MieFixedArgs a) {
-  int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+__global__ void plan_chunks_kernel(PlanArgs a) {
+  int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   int lane = threadIdx.x & 31;
   if (warp >= a.n_chunks) return;
-  int64_t unit = a.unit0 + warp / a.cpu;
+  int64_t unit = warp / a.cpu;
   int c = warp % a.cpu;
   int64_t d = unit / a.n_wl, i = unit % a.n_wl;
   int j = c * 32 + lane;
@@ -47,8 +47,8 @@ __global__ void __launch_bounds__(128) mie_fixed_kernel(MieFixedArgs a) {
   int wslot = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   int lane = threadIdx.x & 31;
   if (wslot >= a.n_chunks) return;
-  int chunk = a.chunk_order ? a.chunk_order[wslot] : wslot;
-  int64_t unit = a.unit0 + chunk / a.cpu;
+  int chunk = wslot;
+  int64_t unit = a.units[chunk / a.cpu];
   int c = chunk % a.cpu;
   int64_t d = unit / a.n_wl, i = unit % a.n_wl;
   int j = c * 32 + lane;
@@ -137,9 +137,9 @@ __global__ void __launch_bounds__(128) mie_nodes_kernel(MieNodesArgs a) {
   }
 }
 
-void launch_plan_chunks(const MieFixedArgs& a, cudaStream_t s) {
+void launch_plan_chunks(const PlanArgs& a, cudaStream_t s) {
   int threads = 128;
-  int blocks = (a.n_chunks * 32 + threads - 1) / threads;
+  int blocks = (int)((a.n_chunks * 32 + threads - 1) / threads);
   plan_chunks_kernel<<<blocks, threads, 0, s>>>(a);
 }
 

@@ -18,9 +18,9 @@ namespace sb {
 namespace {
 
 constexpr double kPi = 3.14159265358979323846264338327950288;
-constexpr int KB = 16;   // orders per GEMM stage
-constexpr int TR = 32;   // table rows per tile
-constexpr int NT = 128;  // threads: 8 row groups of 4 rows x 16 node groups of 2 nodes
+constexpr int KB = 8;     // orders per GEMM stage
+constexpr int TR = 32;    // table rows per tile
+constexpr int NT = 128;   // threads: 8 row groups of 4 rows x 16 node groups of 2 nodes
 
 __device__ __forceinline__ void elements4(double s1r, double s1i, double s2r, double s2i,
                                           double e[4]) {
@@ -44,17 +44,47 @@ __device__ __forceinline__ int band_of(int n) {
 }
 
 struct Smem {
-  double ae[KB][TR];
-  double ao[KB][TR];
-  double xs[KB][128];
+  double a[2][2][KB][TR];  // [stage][G_E, G_O][order][row]
+  double xs[2][KB][128];   // [stage][order][4 columns x 32 nodes]
   double w[32], cu[32], area[32], sc[32];
   double S[8];
   int slot;
 };
 
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src));
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::); }
+
+// One stage: orders k0 .. k0+KB-1 (those below nc) of the 32 table rows and of the chunk's
+// coefficient rows, copied asynchronously into stage buffer st. The tables are stored
+// transposed (order-major, ldr doubles per order) so that each order's 32 rows are contiguous.
+__device__ __forceinline__ void load_stage(Smem& sm, int st, const double* __restrict__ ge,
+                                           const double* __restrict__ go, int ldr, int r0,
+                                           int k0, int nc, const double* __restrict__ xc) {
+  const int t = threadIdx.x;
+  {
+    const int kk = t >> 4, c = t & 15;
+    if (k0 + kk < nc) {
+      const int64_t off = (int64_t)(k0 + kk) * ldr + r0 + 2 * c;
+      cp_async16(&sm.a[st][0][kk][2 * c], ge + off);
+      cp_async16(&sm.a[st][1][kk][2 * c], go + off);
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int idx = t + q * NT;
+    const int kk = idx >> 6, c = idx & 63;
+    if (k0 + kk < nc) cp_async16(&sm.xs[st][kk][2 * c], xc + (int64_t)(k0 + kk) * 128 + 2 * c);
+  }
+  cp_commit();
+}
+
 // accE/accO[r][c] = sum_k G[r0 + 4 rg + r][k] X[k][4 ng + c (+ 64 for c >= 4)] for k < nc.
 __device__ __forceinline__ void gemm_tile(Smem& sm, const double* __restrict__ ge,
-                                          const double* __restrict__ go, int ld, int r0, int nc,
+                                          const double* __restrict__ go, int ldr, int r0, int nc,
                                           const double* __restrict__ xc, double accE[4][8],
                                           double accO[4][8]) {
   const int t = threadIdx.x, rg = t >> 4, ng = t & 15;
@@ -65,76 +95,51 @@ __device__ __forceinline__ void gemm_tile(Smem& sm, const double* __restrict__ g
       accE[r][c] = 0.0;
       accO[r][c] = 0.0;
     }
-  for (int k0 = 0; k0 < nc; k0 += KB) {
-#pragma unroll
-    for (int q = 0; q < 2; ++q) {
-      int idx = t + q * NT;
-      int row = idx >> 3, kp = (idx & 7) * 2;
-      int k = k0 + kp;
-      double2 e = make_double2(0.0, 0.0), o = make_double2(0.0, 0.0);
-      if (k < nc) {
-        int64_t off = (int64_t)(r0 + row) * ld + k;
-        e = *reinterpret_cast<const double2*>(ge + off);
-        o = *reinterpret_cast<const double2*>(go + off);
-        if (k + 1 >= nc) {
-          e.y = 0.0;
-          o.y = 0.0;
-        }
-      }
-      sm.ae[kp][row] = e.x;
-      sm.ae[kp + 1][row] = e.y;
-      sm.ao[kp][row] = o.x;
-      sm.ao[kp + 1][row] = o.y;
-    }
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      int idx = t + q * NT;
-      int kr = idx >> 6, cp = (idx & 63) * 2;
-      int k = k0 + kr;
-      double2 v = make_double2(0.0, 0.0);
-      if (k < nc) v = *reinterpret_cast<const double2*>(xc + (int64_t)k * 128 + cp);
-      *reinterpret_cast<double2*>(&sm.xs[kr][cp]) = v;
-    }
+  load_stage(sm, 0, ge, go, ldr, r0, 0, nc, xc);
+  int st = 0;
+  for (int k0 = 0; k0 < nc; k0 += KB, st ^= 1) {
+    cp_wait_all();
     __syncthreads();
+    if (k0 + KB < nc) load_stage(sm, st ^ 1, ge, go, ldr, r0, k0 + KB, nc, xc);
+    const int kend = nc - k0 < KB ? nc - k0 : KB;
 #pragma unroll
     for (int kk = 0; kk < KB; ++kk) {
-      double2 e01 = *reinterpret_cast<const double2*>(&sm.ae[kk][rg * 4]);
-      double2 e23 = *reinterpret_cast<const double2*>(&sm.ae[kk][rg * 4 + 2]);
-      double2 o01 = *reinterpret_cast<const double2*>(&sm.ao[kk][rg * 4]);
-      double2 o23 = *reinterpret_cast<const double2*>(&sm.ao[kk][rg * 4 + 2]);
-      double2 x0 = *reinterpret_cast<const double2*>(&sm.xs[kk][ng * 4]);
-      double2 x1 = *reinterpret_cast<const double2*>(&sm.xs[kk][ng * 4 + 2]);
-      double2 y0 = *reinterpret_cast<const double2*>(&sm.xs[kk][(ng + 16) * 4]);
-      double2 y1 = *reinterpret_cast<const double2*>(&sm.xs[kk][(ng + 16) * 4 + 2]);
-      const double ae[4] = {e01.x, e01.y, e23.x, e23.y};
-      const double ao[4] = {o01.x, o01.y, o23.x, o23.y};
-      const double xv[8] = {x0.x, x0.y, x1.x, x1.y, y0.x, y0.y, y1.x, y1.y};
+      if (kk < kend) {
+        const double2 e01 = *reinterpret_cast<const double2*>(&sm.a[st][0][kk][rg * 4]);
+        const double2 e23 = *reinterpret_cast<const double2*>(&sm.a[st][0][kk][rg * 4 + 2]);
+        const double2 o01 = *reinterpret_cast<const double2*>(&sm.a[st][1][kk][rg * 4]);
+        const double2 o23 = *reinterpret_cast<const double2*>(&sm.a[st][1][kk][rg * 4 + 2]);
+        const double2 x0 = *reinterpret_cast<const double2*>(&sm.xs[st][kk][ng * 4]);
+        const double2 x1 = *reinterpret_cast<const double2*>(&sm.xs[st][kk][ng * 4 + 2]);
+        const double2 y0 = *reinterpret_cast<const double2*>(&sm.xs[st][kk][(ng + 16) * 4]);
+        const double2 y1 = *reinterpret_cast<const double2*>(&sm.xs[st][kk][(ng + 16) * 4 + 2]);
+        const double ae[4] = {e01.x, e01.y, e23.x, e23.y};
+        const double ao[4] = {o01.x, o01.y, o23.x, o23.y};
+        const double xv[8] = {x0.x, x0.y, x1.x, x1.y, y0.x, y0.y, y1.x, y1.y};
 #pragma unroll
-      for (int r = 0; r < 4; ++r)
+        for (int r = 0; r < 4; ++r)
 #pragma unroll
-        for (int c = 0; c < 8; ++c) {
-          accE[r][c] = fma(ae[r], xv[c], accE[r][c]);
-          accO[r][c] = fma(ao[r], xv[c], accO[r][c]);
-        }
+          for (int c = 0; c < 8; ++c) {
+            accE[r][c] = fma(ae[r], xv[c], accE[r][c]);
+            accO[r][c] = fma(ao[r], xv[c], accO[r][c]);
+          }
+      }
     }
-    __syncthreads();
   }
+  __syncthreads();  // the stage buffers are free for the next tile
 }
 
-// The elements at +mu (P) and -mu (M) of this thread's 4 rows, scaled and weighted per sphere
-// and summed over the chunk's 32 spheres; returned in the threads with ng == 0.
+// The elements at +mu and -mu of this thread's 4 rows for its 2 spheres, scaled and weighted,
+// summed over the chunk's 32 spheres by a reduce-scatter over the 16 threads sharing the rows:
+// thread ng ends with v[0], v[1] of side ng >> 3 (0: +mu, 1: -mu), row (ng >> 1) & 3 and
+// elements 2 (ng & 1) and 2 (ng & 1) + 1.
 template <bool kUser>
 __device__ __forceinline__ void chunk_elements(const Smem& sm, const double accE[4][8],
-                                               const double accO[4][8], double P[4][4],
-                                               double M[4][4]) {
+                                               const double accO[4][8], double v[2]) {
   const int ng = threadIdx.x & 15;
+  double p[32];
 #pragma unroll
-  for (int r = 0; r < 4; ++r)
-#pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      P[r][e] = 0.0;
-      M[r][e] = 0.0;
-    }
+  for (int i = 0; i < 32; ++i) p[i] = 0.0;
 #pragma unroll
   for (int nd = 0; nd < 2; ++nd) {
     const int node = ng + 16 * nd;
@@ -153,100 +158,63 @@ __device__ __forceinline__ void chunk_elements(const Smem& sm, const double accE
         // Requested cosines: W (4/x^2 F) pi r^2 (phase.rs:204-219, engine.rs:1075); band
         // tables: W (4/x^2 pi r^2) F (engine.rs:1655-1660).
         if (kUser) {
-          P[r][e] += w * ((cu * ep[e]) * ar);
-          M[r][e] += w * ((cu * em[e]) * ar);
+          p[r * 4 + e] += w * ((cu * ep[e]) * ar);
+          p[16 + r * 4 + e] += w * ((cu * em[e]) * ar);
         } else {
-          P[r][e] += w * (sc * ep[e]);
-          M[r][e] += w * (sc * em[e]);
+          p[r * 4 + e] += w * (sc * ep[e]);
+          p[16 + r * 4 + e] += w * (sc * em[e]);
         }
       }
     }
   }
+  // Reduce-scatter: at offset o the lane keeps the lower half of its values if (ng & o) == 0.
 #pragma unroll
-  for (int off = 8; off > 0; off >>= 1)
+  for (int lvl = 0, o = 8, h = 16; lvl < 4; ++lvl, o >>= 1, h >>= 1) {
+    const bool lower = (ng & o) == 0;
 #pragma unroll
-    for (int r = 0; r < 4; ++r)
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        P[r][e] += __shfl_xor_sync(0xffffffffu, P[r][e], off);
-        M[r][e] += __shfl_xor_sync(0xffffffffu, M[r][e], off);
+    for (int i = 0; i < 16; ++i) {
+      if (i < h) {
+        const double mine = lower ? p[i] : p[i + h];
+        const double other = lower ? p[i + h] : p[i];
+        p[i] = mine + __shfl_xor_sync(0xffffffffu, other, o);
       }
-}
-
-// K-d: the band's averaged tables projected and added to the Greek accumulators; the band
-// accumulator is cleared for the next band.
-__device__ void flush_band(const UnitArgs& a, int b, double z, double* acc_band,
-                           double* acc_greek, int glen) {
-  __syncthreads();
-  const BandDesc B = a.bands[b];
-  const int q = B.n_q, len = B.order + 1;
-  for (int k = threadIdx.x; k < 4 * q; k += NT) acc_band[k] = acc_band[k] / z;
-  __syncthreads();
-  const double* D = a.band_d + B.d_off;
-  for (int l = threadIdx.x; l < len; l += NT) {
-    double a1 = 0.0, a4 = 0.0, p = 0.0, mi = 0.0, b1 = 0.0, b2 = 0.0;
-    for (int k = 0; k < q; ++k) {
-      const double f11 = acc_band[k], f12 = acc_band[q + k];
-      const double f33 = acc_band[2 * q + k], f34 = acc_band[3 * q + k];
-      const double d00 = D[(int64_t)k * len + l];
-      const double d22 = D[(int64_t)(q + k) * len + l];
-      const double d2m2 = D[(int64_t)(2 * q + k) * len + l];
-      const double d02 = D[(int64_t)(3 * q + k) * len + l];
-      a1 = fma(f11, d00, a1);
-      a4 = fma(f33, d00, a4);
-      p = fma(f11 + f33, d22, p);
-      mi = fma(f11 - f33, d2m2, mi);
-      b1 = fma(f12, d02, b1);
-      b2 = fma(f34, d02, b2);
     }
-    acc_greek[l] += a1;
-    acc_greek[glen + l] += (p + mi) * 0.5;
-    acc_greek[2 * glen + l] += (p - mi) * 0.5;
-    acc_greek[3 * glen + l] += a4;
-    acc_greek[4 * glen + l] += b1;
-    acc_greek[5 * glen + l] += b2;
   }
-  __syncthreads();
-  for (int k = threadIdx.x; k < 4 * q; k += NT) acc_band[k] = 0.0;
-  __syncthreads();
+  v[0] = p[0];
+  v[1] = p[1];
 }
 
 }  // namespace
 
+// K-b and K-c: each work item runs its row tiles of every chunk of its unit and adds the
+// reduced tiles into the unit's accumulators. Every output sum is owned by one thread of one
+// work item and runs over the chunks in order, so the results do not depend on how a unit's
+// tiles are split into work items.
 __global__ void __launch_bounds__(NT) unit_kernel(UnitArgs a) {
   __shared__ __align__(16) Smem sm;
   const int t = threadIdx.x, rg = t >> 4, ng = t & 15;
-  double* acc_user = a.acc + (int64_t)blockIdx.x * a.acc_stride;
-  double* acc_band = acc_user + 4 * a.n_mu;
-  double* acc_greek = acc_band + 4 * a.nq_max;
-  const int L = a.greek_order;
-  const int glen = L >= 0 ? L + 1 : 0;
+  // This thread's share of a reduced tile: side (+mu, -mu), row, two elements.
+  const int side = ng >> 3, rr = (ng >> 1) & 3, e0 = 2 * (ng & 1);
+  const int t_user = (a.h_u + TR - 1) / TR;
   for (;;) {
     if (t == 0) sm.slot = atomicAdd(a.work_counter, 1);
     __syncthreads();
     const int slot = sm.slot;
-    if (slot >= a.n_units) break;
-    const int ul = a.unit_order ? a.unit_order[slot] : slot;
-    const int64_t unit = a.unit0 + ul;
+    __syncthreads();
+    if (slot >= a.n_items) break;
+    const WorkItem it = a.items[slot];
+    const int ul = it.unit;
+    const int64_t unit = a.units[ul];
     const int64_t d = unit / a.n_wl, i = unit % a.n_wl;
     const double lam = a.wl[i];
-    for (int k = t; k < 4 * a.n_mu; k += NT) acc_user[k] = 0.0;
-    for (int k = t; k < 4 * a.nq_max; k += NT) acc_band[k] = 0.0;
-    for (int k = t; k < 6 * glen; k += NT) acc_greek[k] = 0.0;
-    if (t < 8) {
-      double s = 0.0;
-      for (int c = 0; c < a.cpu; ++c) s += a.chunk_sums[((int64_t)ul * a.cpu + c) * 8 + t];
-      sm.S[t] = s;
-    }
-    __syncthreads();
-    const double z = sm.S[0];
-    int prev = -1;
+    double* acc_user = a.acc + a.unit_acc[ul];
     for (int c = 0; c < a.cpu; ++c) {
-      const int nc = a.chunk_n[ul * a.cpu + c];
+      const int64_t ci = (int64_t)ul * a.cpu + c;
+      const int nc = a.chunk_n[ci];
       if (nc == 0) continue;
-      const int b = L >= 0 ? band_of(nc) : -1;
-      if (b != prev && prev >= 0) flush_band(a, prev, z, acc_band, acc_greek, glen);
-      prev = b;
+      const int b = a.greek_order >= 0 ? band_of(nc) : -1;
+      const int t_band = b >= 0 ? (a.bands[b].h + TR - 1) / TR : 0;
+      if (it.group >= t_user + t_band) continue;
       if (t < 32) {
         const int j = c * 32 + t;
         double w = 0.0, cu = 0.0, ar = 0.0, sc = 0.0;
@@ -264,66 +232,178 @@ __global__ void __launch_bounds__(NT) unit_kernel(UnitArgs a) {
         sm.sc[t] = sc;
       }
       __syncthreads();
-      const double* xc = a.X + a.chunk_row[ul * a.cpu + c] * 128;
-      double accE[4][8], accO[4][8], P[4][4], M[4][4];
-      for (int r0 = 0; r0 < a.h_u; r0 += TR) {
-        gemm_tile(sm, a.ge_u, a.go_u, a.ld_u, r0, nc, xc, accE, accO);
-        chunk_elements<true>(sm, accE, accO, P, M);
-        if (ng == 0) {
-#pragma unroll
-          for (int r = 0; r < 4; ++r) {
-            const int row = r0 + rg * 4 + r;
-            if (row < a.h_u) {
-              const int2 mp = a.user_map[row];
-#pragma unroll
-              for (int e = 0; e < 4; ++e) {
-                acc_user[e * a.n_mu + mp.x] += P[r][e];
-                if (mp.y >= 0) acc_user[e * a.n_mu + mp.y] += M[r][e];
-              }
+      const double* xc = a.X + a.chunk_row[ci] * 128;
+      double accE[4][8], accO[4][8], v[2];
+      for (int tile = it.group; tile < t_user + t_band; tile += it.n_groups) {
+        if (tile < t_user) {
+          const int r0 = tile * TR;
+          gemm_tile(sm, a.ge_u, a.go_u, a.h_u_pad, r0, nc, xc, accE, accO);
+          chunk_elements<true>(sm, accE, accO, v);
+          const int row = r0 + rg * 4 + rr;
+          if (row < a.h_u) {
+            const int2 mp = a.user_map[row];
+            const int j = side ? mp.y : mp.x;
+            if (j >= 0) {
+              acc_user[e0 * a.n_mu + j] += v[0];
+              acc_user[(e0 + 1) * a.n_mu + j] += v[1];
             }
           }
-        }
-      }
-      if (b >= 0) {
-        const BandDesc B = a.bands[b];
-        const int q = B.n_q, lo = q / 2;
-        for (int r0 = 0; r0 < B.h; r0 += TR) {
-          gemm_tile(sm, a.band_ge + B.g_off, a.band_go + B.g_off, B.ld, r0, nc, xc, accE, accO);
-          chunk_elements<false>(sm, accE, accO, P, M);
-          if (ng == 0) {
-#pragma unroll
-            for (int r = 0; r < 4; ++r) {
-              const int row = r0 + rg * 4 + r;
-              if (row < B.h) {
-                const int jn = lo + row, mirror = q - 1 - jn;
-#pragma unroll
-                for (int e = 0; e < 4; ++e) {
-                  acc_band[e * q + jn] += P[r][e];
-                  if (mirror != jn) acc_band[e * q + mirror] += M[r][e];
-                }
-              }
+        } else {
+          const BandDesc B = a.bands[b];
+          const int q = B.n_q, lo = q / 2;
+          const int r0 = (tile - t_user) * TR;
+          double* acc_band = a.acc + a.chunk_acc[ci];
+          gemm_tile(sm, a.band_ge + B.g_off, a.band_go + B.g_off, B.h_pad, r0, nc, xc, accE,
+                    accO);
+          chunk_elements<false>(sm, accE, accO, v);
+          const int row = r0 + rg * 4 + rr;
+          if (row < B.h) {
+            const int jn = lo + row, mirror = q - 1 - jn;
+            const int j = side ? mirror : jn;
+            if (side == 0 || mirror != jn) {
+              acc_band[e0 * q + j] += v[0];
+              acc_band[(e0 + 1) * q + j] += v[1];
             }
           }
         }
       }
       __syncthreads();
     }
-    if (prev >= 0) flush_band(a, prev, z, acc_band, acc_greek, glen);
+  }
+}
+
+// K-d: the Greek coefficients of each band slot, (2l+1)/2 sum_k w_k F(mu_k) d_l(mu_k) with F
+// the slot's averaged tables (fast.rs:238-253): a contraction over the band's n_q nodes shared
+// by a tile of up to 32 slots. Lane s of each warp holds slot s; warp w the orders
+// l0 + w + 4 j (j < 8) of each block of 32 orders. The sums over k run in node order.
+namespace {
+constexpr int PQ = 16;  // nodes per stage
+}
+
+__global__ void __launch_bounds__(NT) proj_kernel(ProjArgs a) {
+  __shared__ double fs[6][PQ][32];  // F11, F12, F33, F34, F11 + F33, F11 - F33 per slot
+  __shared__ double ds[4][PQ][32];  // d00, d22, d2-2, d02 (scaled) per node and order
+  __shared__ double zs[32];
+  __shared__ int64_t offs[32];
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  const int glen = a.greek_order + 1;
+  for (int item = blockIdx.x; item < a.n_items; item += gridDim.x) {
+    const ProjItem it = a.items[item];
+    const BandDesc B = a.bands[it.band];
+    const int q = B.n_q, len = B.order + 1;
+    if (t < 32) {
+      double z = 1.0;
+      int64_t off = -1;
+      if (t < it.count) {
+        const BandSlot bs = a.slots[a.slot_index[it.first + t]];
+        z = 0.0;
+        for (int c = 0; c < a.cpu; ++c) z += a.chunk_sums[((int64_t)bs.unit * a.cpu + c) * 8];
+        off = bs.off;
+      }
+      zs[t] = z;
+      offs[t] = off;
+    }
     __syncthreads();
-    // Averages and outputs (engine.rs:1782-1836, 2396-2497).
+    const double* D = a.band_d + B.d_off;
+    for (int l0 = 0; l0 < len; l0 += 32) {
+      double acc[8][6];
+#pragma unroll
+      for (int j = 0; j < 8; ++j)
+#pragma unroll
+        for (int e = 0; e < 6; ++e) acc[j][e] = 0.0;
+      for (int k0 = 0; k0 < q; k0 += PQ) {
+        const int kn = q - k0 < PQ ? q - k0 : PQ;
+        // Tables of the 32 slots at nodes k0..k0+kn-1, divided by Z (the averages).
+        for (int idx = t; idx < 4 * PQ * 32; idx += NT) {
+          const int s = idx & 31, kk = (idx >> 5) % PQ, e = idx / (32 * PQ);
+          double v = 0.0;
+          if (kk < kn && offs[s] >= 0) v = a.acc[offs[s] + (int64_t)e * q + k0 + kk] / zs[s];
+          fs[e][kk][s] = v;
+        }
+        for (int idx = t; idx < 4 * PQ * 32; idx += NT) {
+          const int l = idx & 31, kk = (idx >> 5) % PQ, m = idx / (32 * PQ);
+          double v = 0.0;
+          if (kk < kn && l0 + l < len) v = D[((int64_t)m * q + k0 + kk) * len + l0 + l];
+          ds[m][kk][l] = v;
+        }
+        __syncthreads();
+        for (int idx = t; idx < PQ * 32; idx += NT) {
+          const int s = idx & 31, kk = idx >> 5;
+          fs[4][kk][s] = fs[0][kk][s] + fs[2][kk][s];
+          fs[5][kk][s] = fs[0][kk][s] - fs[2][kk][s];
+        }
+        __syncthreads();
+        for (int kk = 0; kk < kn; ++kk) {
+          const double f11 = fs[0][kk][lane], f12 = fs[1][kk][lane], f33 = fs[2][kk][lane];
+          const double f34 = fs[3][kk][lane], fp = fs[4][kk][lane], fm = fs[5][kk][lane];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            const int l = w + 4 * j;
+            const double d00 = ds[0][kk][l], d22 = ds[1][kk][l];
+            const double d2m2 = ds[2][kk][l], d02 = ds[3][kk][l];
+            acc[j][0] = fma(f11, d00, acc[j][0]);
+            acc[j][1] = fma(f33, d00, acc[j][1]);
+            acc[j][2] = fma(fp, d22, acc[j][2]);
+            acc[j][3] = fma(fm, d2m2, acc[j][3]);
+            acc[j][4] = fma(f12, d02, acc[j][4]);
+            acc[j][5] = fma(f34, d02, acc[j][5]);
+          }
+        }
+        __syncthreads();
+      }
+      if (lane < it.count) {
+        double* out = a.slot_greek + (int64_t)a.slot_index[it.first + lane] * 6 * glen;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const int l = l0 + w + 4 * j;
+          if (l < len) {
+            const double p = acc[j][2], mi = acc[j][3];
+            out[l] = acc[j][0];
+            out[glen + l] = (p + mi) * 0.5;
+            out[2 * glen + l] = (p - mi) * 0.5;
+            out[3 * glen + l] = acc[j][1];
+            out[4 * glen + l] = acc[j][4];
+            out[5 * glen + l] = acc[j][5];
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// The outputs per unit: the averages S/Z (engine.rs:1782-1836), the Greek coefficients summed
+// over the unit's band slots in increasing band order (engine.rs:2310-2355), and the assembly
+// of engine.rs:2396-2497.
+__global__ void __launch_bounds__(NT) final_kernel(FinalArgs a) {
+  __shared__ double S[8];
+  __shared__ double a0s;
+  const int t = threadIdx.x;
+  const int L = a.greek_order;
+  const int glen = L >= 0 ? L + 1 : 0;
+  const int64_t nu = a.n_units_total;
+  for (int ul = blockIdx.x; ul < a.n_units; ul += gridDim.x) {
+    const int64_t unit = a.units[ul];
+    const int64_t d = unit / a.n_wl, i = unit % a.n_wl;
+    if (t < 8) {
+      double s = 0.0;
+      for (int c = 0; c < a.cpu; ++c) s += a.chunk_sums[((int64_t)ul * a.cpu + c) * 8 + t];
+      S[t] = s;
+    }
+    __syncthreads();
+    const double z = S[0];
+    const double* acc_user = a.acc + a.unit_acc[ul];
     double v[8];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) v[k] = sm.S[k] / z;
+    for (int k = 0; k < 8; ++k) v[k] = S[k] / z;
     const double ext = v[1], sca = v[2], scag = v[3], ab = v[4], back = v[5], r2 = v[6],
                  r3 = v[7];
-    const int64_t nu = a.n_units_total;
     if (t == 0) {
-      bool bad = !(isfinite(ext) && ext != 0.0) || !(isfinite(sca) && sca != 0.0) ||
-                 !(isfinite(back) && back != 0.0);
-      if (bad) {
-        unsigned long long key =
-            ((unsigned long long)(i * a.n_dist + d) << 2) |
-            (unsigned long long)(!(isfinite(ext) && ext != 0.0) ? 1 : (!(isfinite(sca) && sca != 0.0) ? 2 : 3));
+      const bool bext = !(isfinite(ext) && ext != 0.0), bsca = !(isfinite(sca) && sca != 0.0);
+      const bool bback = !(isfinite(back) && back != 0.0);
+      if (bext || bsca || bback) {
+        unsigned long long key = ((unsigned long long)(i * a.n_dist + d) << 2) |
+                                 (unsigned long long)(bext ? 1 : (bsca ? 2 : 3));
         atomicMin(a.err + 1, key);
       }
       const double out[11] = {ext,         sca,        ab,  back,    sca / ext,
@@ -345,11 +425,24 @@ __global__ void __launch_bounds__(NT) unit_kernel(UnitArgs a) {
         for (int e = 0; e < 6; ++e) a.phase[((int64_t)e * nu + unit) * a.n_mu + j] = o6[e];
       }
     }
-    if (a.greek && glen > 0) {
-      const double a0 = acc_greek[0];
+    if (glen > 0 && a.greek) {
+      const int2 sl = a.unit_slots[ul];
+      auto sum = [&](int idx) {
+        const int e = idx / glen, l = idx % glen;
+        double g = 0.0;
+        for (int k = 0; k < sl.y; ++k) {
+          const BandSlot bs = a.slots[sl.x + k];
+          if (l <= a.bands[bs.band].order)
+            g += a.slot_greek[(int64_t)(sl.x + k) * 6 * glen + (int64_t)e * glen + l];
+        }
+        return g;
+      };
+      if (t == 0) a0s = sum(0);
+      __syncthreads();
+      const double a0 = a0s;
       for (int idx = t; idx < 6 * glen; idx += NT) {
         const int e = idx / glen, l = idx % glen;
-        double g = acc_greek[idx];
+        double g = sum(idx);
         if (a.normalized) g = idx == 0 ? 1.0 : g / a0;
         a.greek[((int64_t)e * nu + unit) * glen + l] = g;
       }
@@ -366,6 +459,16 @@ int unit_kernel_blocks_per_sm() {
 
 void launch_units(const UnitArgs& a, int grid, cudaStream_t s) {
   unit_kernel<<<grid, NT, 0, s>>>(a);
+}
+
+void launch_proj(const ProjArgs& a, cudaStream_t s) {
+  int grid = a.n_items < 8192 ? a.n_items : 8192;
+  if (grid > 0) proj_kernel<<<grid, NT, 0, s>>>(a);
+}
+
+void launch_final(const FinalArgs& a, cudaStream_t s) {
+  int grid = a.n_units < 4096 ? a.n_units : 4096;
+  final_kernel<<<grid, NT, 0, s>>>(a);
 }
 
 }  // namespace sb
