@@ -124,6 +124,26 @@ int scatrs_mie(const double* x, const double* m, int64_t n, int32_t allow_unvali
                int64_t* n_terms, const int64_t* coeff_offset, double* coeffs, double* eff,
                char* err, size_t err_len);
 
+/*
+ * The batched Mie solve of scatrs_mie without any allocation, for callers that cannot call
+ * cudaMalloc (a plugin inside a host process whose pool owns every device allocation, or a
+ * loop that must not risk an allocation failure or the implicit synchronization of
+ * cudaMalloc/cudaFree). This entry point has no counterpart in the reference.
+ *
+ * Every array is in DEVICE memory of the current device and is the caller's: x[n], m[2 * n],
+ * coeff_offset[n] (the exclusive prefix sum of the terms N_s = ceil(x_s + 6 x_s^(1/3) + 3)),
+ * n_terms[n], coeffs[4 * total_terms] (laid out as in scatrs_mie), eff[5 * n] or NULL;
+ * total_terms is the sum of the N_s. The recurrences' scratch is a fixed 12 MiB array compiled
+ * into the library (every GPU that loads it holds the array until exit): calls needing more than
+ * its 524288 rows (total_terms + 2 n) are rejected with SCATRS_INVALID_INPUT. The first call on a
+ * device resolves the array's address with that device current, so make it before any stream
+ * capture. All calls on a device share the array: calls that overlap on the GPU race on it.
+ * Runs on `stream` (a cudaStream_t, or NULL) and synchronizes it before returning.
+ */
+int scatrs_mie_static(const double* x, const double* m, int64_t n, int32_t allow_unvalidated,
+                      int64_t total_terms, int64_t* n_terms, const int64_t* coeff_offset,
+                      double* coeffs, double* eff, void* stream, char* err, size_t err_len);
+
 /* The CUDA device count, or -1 when the runtime is unusable. */
 int scatrs_device_count(void);
 

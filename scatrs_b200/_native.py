@@ -46,6 +46,8 @@ SYMBOLS = {
                                                     _VP, _CP, _SZ]),
     "scatrs_check_errors": (ctypes.c_int, [_VP, _CP, _SZ]),
     "scatrs_mie": (ctypes.c_int, [_PD, _PD, _I64, _I32, _PI64, _PI64, _PD, _PD, _CP, _SZ]),
+    "scatrs_mie_static": (ctypes.c_int, [_VP, _VP, _I64, _I32, _I64, _VP, _VP, _VP, _VP, _VP,
+                                         _CP, _SZ]),
     "scatrs_device_count": (ctypes.c_int, []),
     "scatrs_launch_count": (_I64, []),
     "scatrs_gauss_legendre": (None, [_I64, _PD, _PD]),
