@@ -52,6 +52,23 @@ def dist_env():
     return rank, world, local
 
 
+def max_over_ranks(value: float, device="cuda") -> float:
+    """The maximum of a per-rank time over the ranks (identity on one process)."""
+    import torch
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()):
+        return value
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def total_nodes(world: int, nodes_per_rank: int) -> int:
+    """Weak scaling: every rank processes its own batch of nodes_per_rank nodes."""
+    return world * nodes_per_rank
+
+
 def workload_config(w, args):
     return {"workload": "config2: 1024 wavelengths x 64 lognormal distributions x 512 ln-r Gauss "
                         "nodes, m per (distribution, wavelength), 360 Gauss cosines, Greek L=64",
@@ -282,14 +299,8 @@ def ours(args):
         barrier()
     _native.check_errors(stream.cuda_stream)
     launches = _native.launch_count() - launches0
-    ms = float(np.sum(times))
-    if world > 1:
-        import torch.distributed as dist
-
-        t = torch.tensor([ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * w.n_nodes_total * args.steps / (ms * 1e-3)
+    ms = max_over_ranks(float(np.sum(times)), device=dev)
+    value = total_nodes(world, w.n_nodes_total) * args.steps / (ms * 1e-3)
 
     # e2e: the host-buffer entry point, pinned buffers, copies inside the timed region.
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
@@ -317,14 +328,8 @@ def ours(args):
     for _ in range(args.steps):
         e2e_step()
     barrier()
-    e2e_s = time.perf_counter() - t0
-    if world > 1:
-        import torch.distributed as dist
-
-        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = world * w.n_nodes_total * args.steps / e2e_s
+    e2e_s = max_over_ranks(time.perf_counter() - t0, device=dev)
+    e2e_value = total_nodes(world, w.n_nodes_total) * args.steps / e2e_s
     h2d = 8 * w.wavelengths.size + 16 * n + 16 * w.dists.size * w.n_nodes
     d2h = 8 * (11 * n + 6 * n * w.mu.size + 6 * n * (w.greek_order + 1)) + 4 * n * (
         (w.n_nodes + 31) // 32)

@@ -1,0 +1,107 @@
+"""Host logic without a GPU: the binding surface's parameter names and specs, the seeded
+workloads, and ensemble identities of the reference's tests (scatrs/tests/ensemble.rs) on the
+oracle's fixed-grid restatement."""
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from scatrs_b200 import _scatrs, workloads as W
+from scatrs_b200.errors import InvalidInputError
+
+
+def test_parameter_names_follow_the_reference():
+    m = np.array([1.5 + 0j])
+    assert _scatrs.ensemble_parameters([(("lognormal", 0.1, 1.5), ("sphere", m), 1.0)], False) \
+        == ["median_radius", "width", "m_real", "m_imag"]
+    names = _scatrs.ensemble_parameters(
+        [(("gamma", 1.0, 0.1), ("sphere", m), 1.0),
+         (("multimodal", [(1.0, ("lognormal", 0.1, 1.5)), (2.0, ("lognormal", 1.0, 2.0))]),
+          ("layered", np.array([0.5]), np.ones((2, 1), complex)), 2.0)], True)
+    assert names == ["c0.effective_radius", "c0.effective_variance", "c0.m_real", "c0.m_imag",
+                     "c0.weight", "c1.mode0.median_radius", "c1.mode0.width", "c1.mode0.weight",
+                     "c1.mode1.median_radius", "c1.mode1.width", "c1.mode1.weight",
+                     "c1.layer0.m_real", "c1.layer0.m_imag", "c1.layer1.m_real",
+                     "c1.layer1.m_imag", "c1.layer0.radius_fraction", "c1.weight"]
+    with pytest.raises(InvalidInputError):
+        _scatrs.ensemble_parameters([(("lognormal", 0.1, 1.5), ("sphere", m), 1.0)] * 2, False)
+    with pytest.raises(TypeError):
+        _scatrs.ensemble_parameters([(("weibull", 1.0), ("sphere", m), 1.0)], False)
+
+
+def test_distribution_specs_and_ranges():
+    d = _scatrs._dist_array([("lognormal", 0.2, 1.5), ("power_law", 3.0, 0.1, 2.0)], 4.0)
+    assert d["kind"].tolist() == [1, 4]
+    assert np.isclose(d["r_lo"][0], 0.2 * 1.5 ** -4) and np.isclose(d["r_hi"][0], 0.2 * 1.5 ** 4)
+    assert (d["r_lo"][1], d["r_hi"][1]) == (0.1, 2.0)
+    with pytest.raises(InvalidInputError):
+        _scatrs._dist_array([("gamma", 1.0, 0.1)], 4.0)
+    with pytest.raises(TypeError):
+        _scatrs._dist_array([("bogus", 1.0)], 4.0)
+
+
+def test_workloads_are_seeded_and_shaped():
+    a, b = W.config2(seed=5), W.config2(seed=5)
+    assert np.array_equal(a.m, b.m) and np.array_equal(a.dists, b.dists)
+    assert a.n_nodes_total == 33554432 and a.mu.size == 360 and a.greek_order == 64
+    assert not np.array_equal(W.config2(seed=6).m, a.m)
+    assert 1.33 <= a.m.real.min() and a.m.real.max() <= 1.60
+    assert 1e-8 <= a.m.imag.min() and a.m.imag.max() <= 1e-1
+    c = W.config1()
+    assert c.n_nodes_total == 768 and c.greek_order == 32
+
+
+def test_bands_follow_the_reference_sequence():
+    seq = [O.bucket(n) for n in range(1, 40)]
+    assert seq[:12] == [1, 2, 3, 4, 5, 7, 7, 9, 9, 12, 12, 12]
+    assert O.bucket(2198) == 2712 and O.bucket(2169) == 2169
+
+
+def _fixed(w, **kw):
+    d = np.zeros(w.dists.size, dtype=O.DIST_DTYPE)
+    d["kind"], d["p"] = w.dists["kind"], w.dists["param"]
+    d["r_lo"], d["r_hi"] = w.dists["r_lo"], w.dists["r_hi"]
+    return O.ensemble_fixed(d, w.wavelengths, w.m, w.n_nodes, w.mu, w.greek_order, **kw)
+
+
+def test_narrow_distribution_is_the_single_sphere():
+    """A lognormal narrow enough is one sphere: the averages are its cross sections
+    (scatrs/tests/ensemble.rs:61-112, monodisperse = single sphere)."""
+    r0, lam, m = 0.3, 0.55, 1.5 + 0.01j
+    w = W.Workload("narrow", W.lognormals(r0, 1.0 + 1e-9, 1.0), np.array([lam]),
+                   np.full((1, 1), m), np.array([1.0, 0.5, -0.2, -1.0]), 64, 8)
+    out = _fixed(w)
+    s = O.mie(2 * np.pi * r0 / lam, m)
+    area = np.pi * r0 * r0
+    assert np.isclose(out["values"][0, 0], area * s["q_ext"], rtol=1e-7)
+    assert np.isclose(out["values"][5, 0], s["g"], rtol=1e-7)
+    g = O.mie_greek(2 * np.pi * r0 / lam, m, 8)
+    assert np.allclose(out["greek"][:, 0, :], g, rtol=1e-6, atol=1e-9)
+
+
+def test_normalized_phase_integrates_to_one_and_alpha1_is_3g():
+    w = W.config1()
+    mu, wt = O.gauss_legendre(200)
+    w.mu = mu
+    out = _fixed(w)
+    norm = 0.5 * (out["phase"][0] * wt[None]).sum(axis=1)
+    assert np.allclose(norm, 1.0, rtol=1e-12)
+    assert np.allclose(out["greek"][0, :, 1], 3 * out["values"][5], rtol=1e-11)
+    assert np.all(out["greek"][0, :, 0] == 1.0)
+
+
+def test_rayleigh_limit():
+    """Small spheres: Q_sca ~ (8/3) x^4 |(m^2-1)/(m^2+2)|^2 (scatrs/tests/ensemble.rs:158-174)."""
+    r, lam, m = 1e-3, 1.0, 1.5 + 0j
+    x = 2 * np.pi * r / lam
+    s = O.mie(x, m)
+    k = abs((m * m - 1) / (m * m + 2)) ** 2
+    assert np.isclose(s["q_sca"], 8.0 / 3.0 * x ** 4 * k, rtol=1e-4)
+
+
+def test_errors_are_the_reference_classes():
+    w = W.config1()
+    w.m = np.full_like(w.m, 1.5 + 11j)
+    with pytest.raises(O.OracleError) as e:
+        _fixed(w)
+    assert e.value.status == 3 and "at wavelength" in str(e.value)
