@@ -145,6 +145,37 @@ struct Context {
   std::vector<int> chunk_n_host;
   int* pinned_chunk_n = nullptr;
   size_t pinned_cap = 0;
+  // Two halves of pinned staging for the slabs' plans, each with the event of its last upload.
+  unsigned char* staging = nullptr;
+  size_t staging_cap = 0;  // bytes per half
+  cudaEvent_t staged[2] = {nullptr, nullptr};
+  bool staged_pending[2] = {false, false};
+
+  void ensure_staging(size_t bytes) {
+    if (!staged[0]) {
+      SB_CUDA(cudaEventCreateWithFlags(&staged[0], cudaEventDisableTiming));
+      SB_CUDA(cudaEventCreateWithFlags(&staged[1], cudaEventDisableTiming));
+    }
+    if (bytes <= staging_cap) return;
+    for (int h = 0; h < 2; ++h)
+      if (staged_pending[h]) SB_CUDA(cudaEventSynchronize(staged[h]));
+    staged_pending[0] = staged_pending[1] = false;
+    if (staging) cudaFreeHost(staging);
+    staging = nullptr;
+    staging_cap = 0;
+    SB_CUDA(cudaMallocHost(&staging, 2 * bytes));
+    staging_cap = bytes;
+  }
+  // Half h, once the device has read what was last uploaded from it.
+  unsigned char* staging_half(int h) {
+    if (staged_pending[h]) SB_CUDA(cudaEventSynchronize(staged[h]));
+    staged_pending[h] = false;
+    return staging + (size_t)h * staging_cap;
+  }
+  void staging_uploaded(int h, cudaStream_t s) {
+    SB_CUDA(cudaEventRecord(staged[h], s));
+    staged_pending[h] = true;
+  }
 };
 
 std::mutex g_ctx_mtx;
@@ -407,39 +438,54 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
   BandTables* bt = nullptr;
   if (L >= 0) bt = &ensure_bands(c, L, band_index(n_max), s);
   // 3. Slabs. Each unit's work: its chunks' rows times the table rows they meet.
-  std::vector<int> band_of_n(n_max + 1, -1);
+  const int nb = bt ? bt->n_bands : 0;
+  std::vector<int> band_of_n(n_max + 1, -1), band_tiles(nb), band_nq(nb);
   if (bt) {
     int b = 0;
     for (int n = 1; n <= n_max; ++n) {
       while (bt->desc[b].upper < n) ++b;
       band_of_n[n] = b;
     }
+    for (int k = 0; k < nb; ++k) {
+      band_tiles[k] = (bt->desc[k].h + 31) / 32;
+      band_nq[k] = bt->desc[k].n_q;
+    }
   }
   const int t_user = (c.user.h + 31) / 32;
   const int64_t acc_head = 4 * n_mu;
   std::vector<int64_t> urows(n_units), uacc(n_units);
+  std::vector<int> uslots(n_units), utiles(n_units);
   std::vector<double> ucost(n_units);
   int64_t total_rows = 0;
+  double total_cost = 0.0;
   for (int64_t u = 0; u < n_units; ++u) {
+    const int* cu = cn + u * cpu;
     int64_t rows = 0, acc = acc_head;
     double cost = 0.0;
-    int prev = -1;
+    int prev = -1, slots = 0, max_tiles = 1;
     for (int k = 0; k < cpu; ++k) {
-      int nc = cn[u * cpu + k];
+      const int nc = cu[k];
       rows += nc;
       int tiles = t_user;
       if (bt && nc > 0) {
-        int b = band_of_n[nc];
-        tiles += (bt->desc[b].h + 31) / 32;
-        if (b != prev) acc += 4 * (int64_t)bt->desc[b].n_q;
-        prev = b;
+        const int b = band_of_n[nc];
+        tiles += band_tiles[b];
+        if (b != prev) {
+          acc += 4 * (int64_t)band_nq[b];
+          ++slots;
+          prev = b;
+        }
       }
       cost += (double)tiles * ((double)nc + 24.0);
+      max_tiles = std::max(max_tiles, tiles);
     }
     urows[u] = rows;
     uacc[u] = acc;
+    uslots[u] = slots;
+    utiles[u] = max_tiles;
     ucost[u] = cost;
     total_rows += rows;
+    total_cost += cost;
   }
   const int64_t max_urows = *std::max_element(urows.begin(), urows.end());
   const int64_t arena = std::max<int64_t>(kArenaRows, 2 * max_urows);
@@ -457,8 +503,8 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
     std::vector<int64_t> rows(n_slabs, 0), chunks(n_slabs, 0);
     bool fits = true;
     for (int64_t k = 0; k < n_units; ++k) {
-      int64_t round = k / n_slabs, pos = k % n_slabs;
-      int64_t sl = (round & 1) ? n_slabs - 1 - pos : pos;
+      const int64_t round = k / n_slabs, pos = k % n_slabs;
+      const int64_t sl = (round & 1) ? n_slabs - 1 - pos : pos;
       slab_of[by_cost[k]] = (int)sl;
       rows[sl] += urows[by_cost[k]];
       chunks[sl] += cpu;
@@ -467,169 +513,92 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
     if (fits) break;
     ++n_slabs;
   }
-  // Per slab: units (largest first), chunk tables, accumulator layout, work items.
+  // A large unit's row tiles split into work items of about item_target work each.
   const int grid_max = c.sms * c.unit_bps;
-  double total_cost = 0.0;
-  for (double v : ucost) total_cost += v;
   const double item_target = std::max(1.0, total_cost / (double)n_slabs / (4.0 * grid_max));
+  std::vector<int> ugroups(n_units);
+  for (int64_t u = 0; u < n_units; ++u)
+    ugroups[u] = (int)std::min<double>(std::max(1.0, std::ceil(ucost[u] / item_target)),
+                                       (double)utiles[u]);
   struct Slab {
-    int64_t u0, nu;        // into the flat unit list
-    int64_t ch0;           // into the flat chunk tables
-    int64_t it0, n_items;  // into the flat item list
-    int64_t sl0;           // into the flat band-slot list
-    int64_t n_slots;
-    int64_t pi0, n_proj;   // into the flat projection items
-    int64_t si0;           // into the flat slot-index list
-    int64_t acc_len;
+    int64_t u0 = 0, nu = 0;      // units (flat list, slab-major)
+    int64_t sl0 = 0, n_slots = 0;
+    int64_t pi0 = 0, pi_cap = 0;  // projection items: nb + n_slots / 32 at most
+    int64_t it0 = 0, n_items = 0;
+    int64_t acc_len = 0;
+    int64_t n_proj = 0;
   };
   std::vector<Slab> slabs(n_slabs);
-  std::vector<int> units_flat;
-  units_flat.reserve(n_units);
+  std::vector<int> members(n_units);
   {
-    std::vector<std::vector<int>> members(n_slabs);
-    for (int64_t k = 0; k < n_units; ++k) members[slab_of[by_cost[k]]].push_back(by_cost[k]);
-    int64_t u0 = 0;
+    std::vector<int64_t> count(n_slabs, 0);
+    for (int64_t u = 0; u < n_units; ++u) {
+      Slab& S = slabs[slab_of[u]];
+      count[slab_of[u]]++;
+      S.n_slots += uslots[u];
+      S.n_items += ugroups[u];
+      S.acc_len += uacc[u];
+    }
+    int64_t u0 = 0, sl0 = 0, pi0 = 0, it0 = 0;
     for (int64_t sl = 0; sl < n_slabs; ++sl) {
-      slabs[sl].u0 = u0;
-      slabs[sl].nu = (int64_t)members[sl].size();
-      for (int u : members[sl]) units_flat.push_back(u);
-      u0 += slabs[sl].nu;
+      Slab& S = slabs[sl];
+      S.u0 = u0;
+      S.nu = count[sl];
+      S.sl0 = sl0;
+      S.pi0 = pi0;
+      S.pi_cap = nb + S.n_slots / 32 + 1;
+      S.it0 = it0;
+      u0 += S.nu;
+      sl0 += S.n_slots;
+      pi0 += S.pi_cap;
+      it0 += S.n_items;
+    }
+    // by_cost order within each slab: the largest units first.
+    std::vector<int64_t> fill(n_slabs, 0);
+    for (int64_t k = 0; k < n_units; ++k) {
+      const int u = by_cost[k];
+      const int sl = slab_of[u];
+      members[slabs[sl].u0 + fill[sl]++] = u;
     }
   }
-  std::vector<int> chunk_n_flat(n_chunks);
-  std::vector<int64_t> chunk_row_flat(n_chunks), chunk_acc_flat(n_chunks);
-  std::vector<int64_t> unit_acc_flat(n_units);
-  std::vector<int2> unit_slots_flat(n_units);
-  std::vector<BandSlot> slots_flat;
-  std::vector<WorkItem> items_flat;
-  std::vector<int> slot_index_flat;   // per slab: slab-local slots grouped by band
-  std::vector<ProjItem> proj_flat;
-  int64_t slots_max = 1;
-  int64_t acc_max = 1;
-  for (int64_t sl = 0; sl < n_slabs; ++sl) {
-    Slab& S = slabs[sl];
-    S.ch0 = S.u0 * cpu;
-    S.it0 = (int64_t)items_flat.size();
-    S.sl0 = (int64_t)slots_flat.size();
-    int64_t row = 0, acc = 0;
-    std::vector<std::pair<double, WorkItem>> items;
-    for (int64_t lu = 0; lu < S.nu; ++lu) {
-      const int u = units_flat[S.u0 + lu];
-      unit_acc_flat[S.u0 + lu] = acc;
-      int64_t band_acc = acc + acc_head;
-      int2 us = make_int2((int)(slots_flat.size() - S.sl0), 0);
-      int prev = -1;
-      int max_tiles = 0;
-      for (int k = 0; k < cpu; ++k) {
-        const int64_t g = S.ch0 + lu * cpu + k;
-        const int nc = cn[(int64_t)u * cpu + k];
-        chunk_n_flat[g] = nc;
-        chunk_row_flat[g] = row;
-        row += nc;
-        chunk_acc_flat[g] = -1;
-        int tiles = t_user;
-        if (bt && nc > 0) {
-          const int b = band_of_n[nc];
-          if (b != prev) {
-            BandSlot bs;
-            bs.band = b;
-            bs.unit = (int)lu;
-            bs.off = band_acc;
-            slots_flat.push_back(bs);
-            us.y += 1;
-            band_acc += 4 * (int64_t)bt->desc[b].n_q;
-            prev = b;
-          }
-          chunk_acc_flat[g] = slots_flat.back().off;
-          tiles += (bt->desc[b].h + 31) / 32;
-        }
-        max_tiles = std::max(max_tiles, tiles);
-      }
-      unit_slots_flat[S.u0 + lu] = us;
-      acc += uacc[u];
-      int groups = (int)std::min<double>(std::max(1.0, std::ceil(ucost[u] / item_target)),
-                                         (double)std::max(max_tiles, 1));
-      for (int gi = 0; gi < groups; ++gi) {
-        WorkItem w;
-        w.unit = (int)lu;
-        w.group = gi;
-        w.n_groups = groups;
-        w.pad = 0;
-        items.emplace_back(ucost[u] / groups, w);
-      }
-    }
-    std::stable_sort(items.begin(), items.end(),
-                     [](const std::pair<double, WorkItem>& x,
-                        const std::pair<double, WorkItem>& y) { return x.first > y.first; });
-    for (auto& it : items) items_flat.push_back(it.second);
-    S.n_items = (int64_t)items.size();
-    S.acc_len = acc;
-    acc_max = std::max(acc_max, acc);
-    // Projection tiles: the slab's slots grouped by band, 32 at a time.
-    S.n_slots = (int64_t)slots_flat.size() - S.sl0;
+  int64_t acc_max = 1, slots_max = 1, stage_max = 0, n_slots_all = 0, n_proj_all = 0,
+          n_items_all = 0;
+  auto stage_bytes = [&](const Slab& S) {
+    return S.nu * (int64_t)(sizeof(int) + 8 + sizeof(int2)) +
+           S.nu * cpu * (int64_t)(sizeof(int) + 16) +
+           S.n_slots * (int64_t)(sizeof(BandSlot) + sizeof(int)) +
+           S.pi_cap * (int64_t)sizeof(ProjItem) + S.n_items * (int64_t)sizeof(WorkItem) + 256;
+  };
+  for (const Slab& S : slabs) {
+    acc_max = std::max(acc_max, S.acc_len);
     slots_max = std::max(slots_max, S.n_slots);
-    S.pi0 = (int64_t)proj_flat.size();
-    S.si0 = (int64_t)slot_index_flat.size();
-    if (bt && S.n_slots > 0) {
-      std::vector<std::vector<int>> by_band(bt->n_bands);
-      for (int64_t k = 0; k < S.n_slots; ++k) by_band[slots_flat[S.sl0 + k].band].push_back((int)k);
-      const int64_t base = S.si0;
-      for (int b = bt->n_bands - 1; b >= 0; --b) {
-        for (size_t k0 = 0; k0 < by_band[b].size(); k0 += 32) {
-          ProjItem pi;
-          pi.band = b;
-          pi.count = (int)std::min<size_t>(32, by_band[b].size() - k0);
-          pi.first = (int64_t)slot_index_flat.size() - base + (int64_t)k0;
-          proj_flat.push_back(pi);
-        }
-        slot_index_flat.insert(slot_index_flat.end(), by_band[b].begin(), by_band[b].end());
-      }
-    }
-    S.n_proj = (int64_t)proj_flat.size() - S.pi0;
+    stage_max = std::max(stage_max, stage_bytes(S));
+    n_slots_all += S.n_slots;
+    n_proj_all += S.pi_cap;
+    n_items_all += S.n_items;
   }
-  // Upload the plan once.
-  const size_t bytes_units = units_flat.size() * sizeof(int);
-  int* units_d = c.plan_units.as<int>(units_flat.size());
+  // Device buffers: the plan's flat arrays (every slab its own segment), arena, scratch, sums.
+  int* units_d = c.plan_units.as<int>(n_units);
   int* chunk_n_d = c.chunk_n_slab.as<int>(n_chunks);
   int64_t* chunk_row_d = c.chunk_row.as<int64_t>(n_chunks);
   int64_t* chunk_acc_d = c.chunk_acc.as<int64_t>(n_chunks);
   int64_t* unit_acc_d = c.unit_acc.as<int64_t>(n_units);
   int2* unit_slots_d = c.unit_slots.as<int2>(n_units);
-  BandSlot* slots_d = c.slots.as<BandSlot>(std::max<size_t>(slots_flat.size(), 1));
-  WorkItem* items_d = c.items.as<WorkItem>(items_flat.size());
-  ProjItem* proj_d = c.proj_items.as<ProjItem>(std::max<size_t>(proj_flat.size(), 1));
-  int* slot_index_d = c.slot_index.as<int>(std::max<size_t>(slot_index_flat.size(), 1));
-  if (!proj_flat.empty()) {
-    SB_CUDA(cudaMemcpyAsync(proj_d, proj_flat.data(), proj_flat.size() * sizeof(ProjItem),
-                            cudaMemcpyHostToDevice, s));
-    SB_CUDA(cudaMemcpyAsync(slot_index_d, slot_index_flat.data(),
-                            slot_index_flat.size() * sizeof(int), cudaMemcpyHostToDevice, s));
-  }
-  SB_CUDA(cudaMemcpyAsync(units_d, units_flat.data(), bytes_units, cudaMemcpyHostToDevice, s));
-  SB_CUDA(cudaMemcpyAsync(chunk_n_d, chunk_n_flat.data(), n_chunks * sizeof(int),
-                          cudaMemcpyHostToDevice, s));
-  SB_CUDA(cudaMemcpyAsync(chunk_row_d, chunk_row_flat.data(), n_chunks * 8,
-                          cudaMemcpyHostToDevice, s));
-  SB_CUDA(cudaMemcpyAsync(chunk_acc_d, chunk_acc_flat.data(), n_chunks * 8,
-                          cudaMemcpyHostToDevice, s));
-  SB_CUDA(cudaMemcpyAsync(unit_acc_d, unit_acc_flat.data(), n_units * 8, cudaMemcpyHostToDevice,
-                          s));
-  SB_CUDA(cudaMemcpyAsync(unit_slots_d, unit_slots_flat.data(), n_units * sizeof(int2),
-                          cudaMemcpyHostToDevice, s));
-  if (!slots_flat.empty())
-    SB_CUDA(cudaMemcpyAsync(slots_d, slots_flat.data(), slots_flat.size() * sizeof(BandSlot),
-                            cudaMemcpyHostToDevice, s));
-  SB_CUDA(cudaMemcpyAsync(items_d, items_flat.data(), items_flat.size() * sizeof(WorkItem),
-                          cudaMemcpyHostToDevice, s));
-  // Buffers.
+  BandSlot* slots_d = c.slots.as<BandSlot>(std::max<int64_t>(n_slots_all, 1));
+  int* slot_index_d = c.slot_index.as<int>(std::max<int64_t>(n_slots_all, 1));
+  ProjItem* proj_d = c.proj_items.as<ProjItem>(std::max<int64_t>(n_proj_all, 1));
+  WorkItem* items_d = c.items.as<WorkItem>(std::max<int64_t>(n_items_all, 1));
   double* X = c.X.as<double>((size_t)arena * 128);
   double2* uz = c.uz.as<double2>((size_t)(arena + 2 * kMaxSlabChunks) * 32);
   double* ux = c.ux.as<double>((size_t)(arena + 2 * kMaxSlabChunks) * 32);
   double* chunk_sums = c.chunk_sums.as<double>((size_t)kMaxSlabChunks * 8);
   double* acc = c.acc.as<double>((size_t)acc_max);
-  double* slot_greek = L >= 0 ? c.slot_greek.as<double>((size_t)slots_max * 6 * (L + 1)) : nullptr;
+  double* slot_greek =
+      L >= 0 ? c.slot_greek.as<double>((size_t)slots_max * 6 * (L + 1)) : nullptr;
   int* counter = c.counter.as<int>(64);
-  // 4. Launches, slab by slab.
+  c.ensure_staging((size_t)stage_max);
+  // 4. Per slab: build its plan into pinned staging, upload it, launch its kernels. The host
+  // builds the next slab while the device runs this one.
   MieFixedArgs ka{};
   ka.radius = c.radius.as<double>(0);
   ka.weight = c.weight.as<double>(0);
@@ -694,13 +663,125 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
   fa.greek = L >= 0 ? greek : nullptr;
   fa.normalized = opt->normalized;
   fa.err = err;
+  std::vector<std::pair<double, int64_t>> order;  // work items by cost
+  std::vector<int> per_band;
   for (int64_t sl = 0; sl < n_slabs; ++sl) {
-    const Slab& S = slabs[sl];
+    Slab& S = slabs[sl];
     if (S.nu == 0) continue;
+    const int64_t nch = S.nu * cpu;
+    // Staging layout of this slab.
+    unsigned char* base = c.staging_half(sl & 1);
+    auto take = [&](size_t bytes) {
+      unsigned char* p = base;
+      base += (bytes + 15) / 16 * 16;
+      return p;
+    };
+    int* P_units = (int*)take(S.nu * sizeof(int));
+    int64_t* P_uacc = (int64_t*)take(S.nu * 8);
+    int2* P_uslots = (int2*)take(S.nu * sizeof(int2));
+    int* P_cn = (int*)take(nch * sizeof(int));
+    int64_t* P_row = (int64_t*)take(nch * 8);
+    int64_t* P_cacc = (int64_t*)take(nch * 8);
+    BandSlot* P_slots = (BandSlot*)take(S.n_slots * sizeof(BandSlot));
+    int* P_sidx = (int*)take(S.n_slots * sizeof(int));
+    ProjItem* P_proj = (ProjItem*)take(S.pi_cap * sizeof(ProjItem));
+    WorkItem* P_items = (WorkItem*)take(S.n_items * sizeof(WorkItem));
+    const size_t used = (size_t)(base - c.staging_half(sl & 1));
+    int64_t row = 0, accpos = 0, nslot = 0;
+    order.clear();
+    for (int64_t lu = 0; lu < S.nu; ++lu) {
+      const int u = members[S.u0 + lu];
+      P_units[lu] = u;
+      P_uacc[lu] = accpos;
+      int64_t band_acc = accpos + acc_head;
+      int2 us = make_int2((int)nslot, 0);
+      int prev = -1;
+      for (int k = 0; k < cpu; ++k) {
+        const int64_t ci = lu * cpu + k;
+        const int nc = cn[(int64_t)u * cpu + k];
+        P_cn[ci] = nc;
+        P_row[ci] = row;
+        row += nc;
+        P_cacc[ci] = -1;
+        if (bt && nc > 0) {
+          const int b = band_of_n[nc];
+          if (b != prev) {
+            P_slots[nslot].band = b;
+            P_slots[nslot].unit = (int)lu;
+            P_slots[nslot].off = band_acc;
+            band_acc += 4 * (int64_t)band_nq[b];
+            ++nslot;
+            us.y += 1;
+            prev = b;
+          }
+          P_cacc[ci] = P_slots[nslot - 1].off;
+        }
+      }
+      P_uslots[lu] = us;
+      accpos += uacc[u];
+      const int G = ugroups[u];
+      for (int g = 0; g < G; ++g) order.emplace_back(-ucost[u] / G, lu * 65536 + g);
+    }
+    std::stable_sort(order.begin(), order.end(),
+                     [](const std::pair<double, int64_t>& x, const std::pair<double, int64_t>& y) {
+                       return x.first < y.first;
+                     });
+    for (size_t k = 0; k < order.size(); ++k) {
+      const int64_t lu = order[k].second / 65536;
+      P_items[k].unit = (int)lu;
+      P_items[k].group = (int)(order[k].second % 65536);
+      P_items[k].n_groups = ugroups[P_units[lu]];
+      P_items[k].pad = 0;
+    }
+    // Projection tiles: the slab's slots grouped by band (largest bands first), 32 at a time.
+    S.n_proj = 0;
+    if (bt && S.n_slots > 0) {
+      per_band.assign(nb + 1, 0);
+      for (int64_t k = 0; k < S.n_slots; ++k) per_band[P_slots[k].band + 1]++;
+      std::vector<int64_t> start(nb + 1, 0), cursor(nb, 0);
+      // Bands in descending order occupy the slot-index list from the front.
+      int64_t pos = 0;
+      for (int b = nb - 1; b >= 0; --b) {
+        start[b] = pos;
+        pos += per_band[b + 1];
+      }
+      for (int b = 0; b < nb; ++b) cursor[b] = start[b];
+      for (int64_t k = 0; k < S.n_slots; ++k) P_sidx[cursor[P_slots[k].band]++] = (int)k;
+      for (int b = nb - 1; b >= 0; --b)
+        for (int64_t k0 = 0; k0 < per_band[b + 1]; k0 += 32) {
+          ProjItem& pi = P_proj[S.n_proj++];
+          pi.band = b;
+          pi.count = (int)std::min<int64_t>(32, per_band[b + 1] - k0);
+          pi.first = start[b] + k0;
+        }
+    }
+    // Upload (pinned source: asynchronous) once the staging half's previous upload is done.
+    (void)used;
+    SB_CUDA(cudaMemcpyAsync(units_d + S.u0, P_units, S.nu * sizeof(int), cudaMemcpyHostToDevice, s));
+    SB_CUDA(cudaMemcpyAsync(unit_acc_d + S.u0, P_uacc, S.nu * 8, cudaMemcpyHostToDevice, s));
+    SB_CUDA(cudaMemcpyAsync(unit_slots_d + S.u0, P_uslots, S.nu * sizeof(int2),
+                            cudaMemcpyHostToDevice, s));
+    const int64_t ch0 = S.u0 * cpu;
+    SB_CUDA(cudaMemcpyAsync(chunk_n_d + ch0, P_cn, nch * sizeof(int), cudaMemcpyHostToDevice, s));
+    SB_CUDA(cudaMemcpyAsync(chunk_row_d + ch0, P_row, nch * 8, cudaMemcpyHostToDevice, s));
+    SB_CUDA(cudaMemcpyAsync(chunk_acc_d + ch0, P_cacc, nch * 8, cudaMemcpyHostToDevice, s));
+    if (S.n_slots > 0) {
+      SB_CUDA(cudaMemcpyAsync(slots_d + S.sl0, P_slots, S.n_slots * sizeof(BandSlot),
+                              cudaMemcpyHostToDevice, s));
+      SB_CUDA(cudaMemcpyAsync(slot_index_d + S.sl0, P_sidx, S.n_slots * sizeof(int),
+                              cudaMemcpyHostToDevice, s));
+    }
+    if (S.n_proj > 0)
+      SB_CUDA(cudaMemcpyAsync(proj_d + S.pi0, P_proj, S.n_proj * sizeof(ProjItem),
+                              cudaMemcpyHostToDevice, s));
+    SB_CUDA(cudaMemcpyAsync(items_d + S.it0, P_items, S.n_items * sizeof(WorkItem),
+                            cudaMemcpyHostToDevice, s));
+    c.staging_uploaded(sl & 1, s);
+    // Launches.
     ka.units = units_d + S.u0;
-    ka.n_chunks = (int)(S.nu * cpu);
-    ka.chunk_n = chunk_n_d + S.ch0;
-    ka.chunk_row = chunk_row_d + S.ch0;
+    ka.n_chunks = (int)nch;
+    ka.chunk_n = chunk_n_d + ch0;
+    ka.chunk_row = chunk_row_d + ch0;
     timed_launch(K_MIE, s, [&] { launch_mie_fixed(ka, s); });
     SB_CUDA(cudaGetLastError());
     SB_CUDA(cudaMemsetAsync(acc, 0, (size_t)S.acc_len * 8, s));
@@ -710,7 +791,7 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
     ua.items = items_d + S.it0;
     ua.chunk_n = ka.chunk_n;
     ua.chunk_row = ka.chunk_row;
-    ua.chunk_acc = chunk_acc_d + S.ch0;
+    ua.chunk_acc = chunk_acc_d + ch0;
     ua.unit_acc = unit_acc_d + S.u0;
     const int grid = (int)std::min<int64_t>(grid_max, S.n_items);
     timed_launch(K_UNITS, s, [&] { launch_units(ua, grid, s); });
@@ -718,8 +799,7 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
     if (bt && S.n_proj > 0) {
       pj.items = proj_d + S.pi0;
       pj.n_items = (int)S.n_proj;
-      // slot_index holds slab-local slot numbers; the slab's slot list starts at sl0.
-      pj.slot_index = slot_index_d + S.si0;
+      pj.slot_index = slot_index_d + S.sl0;
       pj.slots = slots_d + S.sl0;
       timed_launch(K_PROJ, s, [&] { launch_proj(pj, s); });
       SB_CUDA(cudaGetLastError());
@@ -997,6 +1077,12 @@ void scatrs_release(void) {
       for (DevBuf* b : {&kv.second.ge_d, &kv.second.go_d, &kv.second.d_d, &kv.second.desc_d})
         b->release();
     if (c.pinned_chunk_n) cudaFreeHost(c.pinned_chunk_n);
+    for (int h = 0; h < 2; ++h)
+      if (c.staged[h]) {
+        cudaEventSynchronize(c.staged[h]);
+        cudaEventDestroy(c.staged[h]);
+      }
+    if (c.staging) cudaFreeHost(c.staging);
     g_ctx[dev].reset();
   }
 }

@@ -275,16 +275,22 @@ __global__ void __launch_bounds__(NT) unit_kernel(UnitArgs a) {
 // K-d: the Greek coefficients of each band slot, (2l+1)/2 sum_k w_k F(mu_k) d_l(mu_k) with F
 // the slot's averaged tables (fast.rs:238-253): a contraction over the band's n_q nodes shared
 // by a tile of up to 32 slots. Lane s of each warp holds slot s; warp w the orders
-// l0 + w + 4 j (j < 8) of each block of 32 orders. The sums over k run in node order.
+// l0 + 9w + j (j < 9) of each block of 72 orders. The sums over k run in node order.
 namespace {
-constexpr int PQ = 16;  // nodes per stage
-}
+constexpr int PQ = 32;   // nodes per stage
+constexpr int PT = 256;  // threads
+constexpr int PL = 72;   // orders per pass: 8 warps x 9
+struct ProjSmem {
+  double fs[4][PQ][33];  // F11, F12, F33, F34 per node and slot (padded against conflicts)
+  double ds[4][PQ][PL];  // d00, d22, d2-2, d02 (scaled) per node and order
+  double rz[32];         // 1/Z per slot
+  int64_t offs[32];
+};
+}  // namespace
 
-__global__ void __launch_bounds__(NT) proj_kernel(ProjArgs a) {
-  __shared__ double fs[6][PQ][32];  // F11, F12, F33, F34, F11 + F33, F11 - F33 per slot
-  __shared__ double ds[4][PQ][32];  // d00, d22, d2-2, d02 (scaled) per node and order
-  __shared__ double zs[32];
-  __shared__ int64_t offs[32];
+__global__ void __launch_bounds__(PT) proj_kernel(ProjArgs a) {
+  extern __shared__ __align__(16) unsigned char proj_raw[];
+  ProjSmem& sm = *reinterpret_cast<ProjSmem*>(proj_raw);
   const int t = threadIdx.x, lane = t & 31, w = t >> 5;
   const int glen = a.greek_order + 1;
   for (int item = blockIdx.x; item < a.n_items; item += gridDim.x) {
@@ -292,55 +298,53 @@ __global__ void __launch_bounds__(NT) proj_kernel(ProjArgs a) {
     const BandDesc B = a.bands[it.band];
     const int q = B.n_q, len = B.order + 1;
     if (t < 32) {
-      double z = 1.0;
+      double rz = 0.0;
       int64_t off = -1;
       if (t < it.count) {
         const BandSlot bs = a.slots[a.slot_index[it.first + t]];
-        z = 0.0;
+        double z = 0.0;
         for (int c = 0; c < a.cpu; ++c) z += a.chunk_sums[((int64_t)bs.unit * a.cpu + c) * 8];
+        rz = 1.0 / z;
         off = bs.off;
       }
-      zs[t] = z;
-      offs[t] = off;
+      sm.rz[t] = rz;
+      sm.offs[t] = off;
     }
     __syncthreads();
     const double* D = a.band_d + B.d_off;
-    for (int l0 = 0; l0 < len; l0 += 32) {
-      double acc[8][6];
+    for (int l0 = 0; l0 < len; l0 += PL) {
+      double acc[9][6];
 #pragma unroll
-      for (int j = 0; j < 8; ++j)
+      for (int j = 0; j < 9; ++j)
 #pragma unroll
         for (int e = 0; e < 6; ++e) acc[j][e] = 0.0;
       for (int k0 = 0; k0 < q; k0 += PQ) {
         const int kn = q - k0 < PQ ? q - k0 : PQ;
-        // Tables of the 32 slots at nodes k0..k0+kn-1, divided by Z (the averages).
-        for (int idx = t; idx < 4 * PQ * 32; idx += NT) {
-          const int s = idx & 31, kk = (idx >> 5) % PQ, e = idx / (32 * PQ);
+        // The averaged tables (S/Z) of the 32 slots at nodes k0..k0+kn-1; node fastest, so
+        // each slot's run is one coalesced read.
+        for (int idx = t; idx < 4 * 32 * PQ; idx += PT) {
+          const int kk = idx % PQ, s = (idx / PQ) & 31, e = idx / (32 * PQ);
           double v = 0.0;
-          if (kk < kn && offs[s] >= 0) v = a.acc[offs[s] + (int64_t)e * q + k0 + kk] / zs[s];
-          fs[e][kk][s] = v;
+          const int64_t off = sm.offs[s];
+          if (kk < kn && off >= 0) v = a.acc[off + (int64_t)e * q + k0 + kk] * sm.rz[s];
+          sm.fs[e][kk][s] = v;
         }
-        for (int idx = t; idx < 4 * PQ * 32; idx += NT) {
-          const int l = idx & 31, kk = (idx >> 5) % PQ, m = idx / (32 * PQ);
+        for (int idx = t; idx < 4 * PQ * PL; idx += PT) {
+          const int l = idx % PL, kk = (idx / PL) % PQ, m = idx / (PL * PQ);
           double v = 0.0;
           if (kk < kn && l0 + l < len) v = D[((int64_t)m * q + k0 + kk) * len + l0 + l];
-          ds[m][kk][l] = v;
-        }
-        __syncthreads();
-        for (int idx = t; idx < PQ * 32; idx += NT) {
-          const int s = idx & 31, kk = idx >> 5;
-          fs[4][kk][s] = fs[0][kk][s] + fs[2][kk][s];
-          fs[5][kk][s] = fs[0][kk][s] - fs[2][kk][s];
+          sm.ds[m][kk][l] = v;
         }
         __syncthreads();
         for (int kk = 0; kk < kn; ++kk) {
-          const double f11 = fs[0][kk][lane], f12 = fs[1][kk][lane], f33 = fs[2][kk][lane];
-          const double f34 = fs[3][kk][lane], fp = fs[4][kk][lane], fm = fs[5][kk][lane];
+          const double f11 = sm.fs[0][kk][lane], f12 = sm.fs[1][kk][lane];
+          const double f33 = sm.fs[2][kk][lane], f34 = sm.fs[3][kk][lane];
+          const double fp = f11 + f33, fm = f11 - f33;
 #pragma unroll
-          for (int j = 0; j < 8; ++j) {
-            const int l = w + 4 * j;
-            const double d00 = ds[0][kk][l], d22 = ds[1][kk][l];
-            const double d2m2 = ds[2][kk][l], d02 = ds[3][kk][l];
+          for (int j = 0; j < 9; ++j) {
+            const int l = 9 * w + j;
+            const double d00 = sm.ds[0][kk][l], d22 = sm.ds[1][kk][l];
+            const double d2m2 = sm.ds[2][kk][l], d02 = sm.ds[3][kk][l];
             acc[j][0] = fma(f11, d00, acc[j][0]);
             acc[j][1] = fma(f33, d00, acc[j][1]);
             acc[j][2] = fma(fp, d22, acc[j][2]);
@@ -354,8 +358,8 @@ __global__ void __launch_bounds__(NT) proj_kernel(ProjArgs a) {
       if (lane < it.count) {
         double* out = a.slot_greek + (int64_t)a.slot_index[it.first + lane] * 6 * glen;
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          const int l = l0 + w + 4 * j;
+        for (int j = 0; j < 9; ++j) {
+          const int l = l0 + 9 * w + j;
           if (l < len) {
             const double p = acc[j][2], mi = acc[j][3];
             out[l] = acc[j][0];
@@ -462,8 +466,17 @@ void launch_units(const UnitArgs& a, int grid, cudaStream_t s) {
 }
 
 void launch_proj(const ProjArgs& a, cudaStream_t s) {
+  // The attribute is per device: set it once on each.
+  static bool configured[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev >= 0 && dev < 64 && !configured[dev]) {
+    cudaFuncSetAttribute(proj_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(ProjSmem));
+    configured[dev] = true;
+  }
   int grid = a.n_items < 8192 ? a.n_items : 8192;
-  if (grid > 0) proj_kernel<<<grid, NT, 0, s>>>(a);
+  if (grid > 0) proj_kernel<<<grid, PT, sizeof(ProjSmem), s>>>(a);
 }
 
 void launch_final(const FinalArgs& a, cudaStream_t s) {
