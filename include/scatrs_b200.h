@@ -90,6 +90,29 @@ int scatrs_ensemble_fixed(const scatrs_distribution* dists, int64_t n_dist,
                           double* values, double* phase, double* greek, char* err,
                           size_t err_len);
 
+/* Layered spheres (scatrs/src/layered/mod.rs; Particle::LayeredSphere,
+ * scatrs/src/ensemble/mod.rs:58-65): n_layers layers, the core first; per distribution the
+ * n_layers - 1 outer radii of layers 0..L-2 as fractions of the particle's radius (nondecreasing
+ * in (0, 1]), and each layer's index per distribution and wavelength. One layer is a
+ * homogeneous sphere (m then as in scatrs_ensemble_fixed). */
+typedef struct scatrs_layers {
+  int32_t n_layers;
+  int32_t reserved;
+  const double* fractions; /* [n_dist][n_layers - 1] */
+  const double* m;         /* complex128 [n_dist][n_layers][n_wl] */
+} scatrs_layers;
+
+/*
+ * scatrs_ensemble_fixed for layered spheres (at most 16 layers): the per-node solve is
+ * Layered::compute (scatrs/src/layered/mod.rs:137-160, kernel.rs:308-465) at x_l = f_l x
+ * (scatrs/src/ensemble/particle.rs:186-195); everything after the coefficients is the sphere's.
+ */
+int scatrs_ensemble_fixed_layered(const scatrs_distribution* dists, int64_t n_dist,
+                                  const double* wavelengths, int64_t n_wl,
+                                  const scatrs_layers* layers, const double* mu, int64_t n_mu,
+                                  const scatrs_fixed_options* options, double* values,
+                                  double* phase, double* greek, char* err, size_t err_len);
+
 /*
  * As scatrs_ensemble_fixed, with every array in DEVICE memory of the current device, launched
  * on `stream` (a cudaStream_t, or NULL for the default stream). Returns after the work is

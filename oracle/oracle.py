@@ -179,3 +179,53 @@ def ensemble_fixed(dists: np.ndarray, wavelengths, m, n_nodes: int, mu=None,
     if greek is not None:
         out["greek"] = greek
     return out
+
+
+def layered(x, m):
+    """A layered sphere: x the interface size parameters (outer last), m the layers' indices."""
+    L = lib()
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    mv = np.ascontiguousarray(np.asarray(m, dtype=np.complex128)).view(np.float64)
+    f = L.orc_layered
+    f.argtypes = [_PD, _PD, _I64, ctypes.POINTER(_I64), _PD, _PD, _PD]
+    n = _I64(0)
+    f(_p(x), _p(mv), x.size, ctypes.byref(n), None, None, None)
+    N = n.value
+    a, b, eff = np.zeros(2 * N), np.zeros(2 * N), np.zeros(5)
+    f(_p(x), _p(mv), x.size, ctypes.byref(n), _p(a), _p(b), _p(eff))
+    return {"a": a.view(np.complex128), "b": b.view(np.complex128), "q_ext": eff[0],
+            "q_sca": eff[1], "q_abs": eff[2], "q_back": eff[3], "g": eff[4], "n": N}
+
+
+def ensemble_fixed_layered(dists: np.ndarray, wavelengths, fractions, m_layers, n_nodes: int,
+                           mu=None, greek_order: int | None = None, normalized: bool = True,
+                           allow_unvalidated: bool = False, threads: int = 0) -> dict:
+    """As ensemble_fixed for layered spheres: fractions (n_dist, L - 1), m_layers complex
+    (n_dist, L, n_wl)."""
+    dists = np.ascontiguousarray(dists, dtype=DIST_DTYPE)
+    wl = np.ascontiguousarray(wavelengths, dtype=np.float64).reshape(-1)
+    ml = np.ascontiguousarray(m_layers, dtype=np.complex128)
+    L = ml.shape[1]
+    fr = np.ascontiguousarray(fractions, dtype=np.float64).reshape(dists.size, L - 1)
+    mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
+    n_units = dists.size * wl.size
+    values = np.zeros((11, n_units))
+    phase = np.zeros((6, n_units, mu.size)) if mu.size else None
+    G = -1 if greek_order is None else int(greek_order)
+    greek = np.zeros((6, n_units, G + 1)) if G >= 0 else None
+    err = ctypes.create_string_buffer(512)
+    f = lib().orc_ensemble_fixed_layered
+    f.argtypes = [ctypes.c_void_p, _I64, _PD, _I64, ctypes.c_int, _PD, _PD, _I64, _PD, _I64,
+                  _I64, ctypes.c_int, ctypes.c_int, ctypes.c_int, _PD, _PD, _PD,
+                  ctypes.c_char_p, _I64]
+    st = f(dists.ctypes.data, dists.size, _p(wl), wl.size, L, _p(fr),
+           _p(ml.view(np.float64).reshape(-1)), n_nodes, _p(mu), mu.size, G, int(normalized),
+           int(allow_unvalidated), threads, _p(values), _p(phase), _p(greek), err, 512)
+    if st != 0:
+        raise OracleError(st, err.value.decode())
+    out = {"values": values}
+    if phase is not None:
+        out["phase"] = phase
+    if greek is not None:
+        out["greek"] = greek
+    return out

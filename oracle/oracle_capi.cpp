@@ -56,6 +56,34 @@ int orc_mie(double x, double m_re, double m_im, int64_t n_max, int allow_unvalid
   return OK;
 }
 
+// Layered::compute (layered/mod.rs:137-160): interface size parameters x[0..layers) (the outer
+// last) and indices m (re, im pairs); a, b (N complex pairs each) and eff as orc_mie's.
+int orc_layered(const double* x, const double* m, int64_t layers, int64_t* n_terms, double* a,
+                double* b, double* eff) {
+  std::vector<double> xs(x, x + layers);
+  std::vector<cplx> ms(layers);
+  for (int64_t l = 0; l < layers; ++l) ms[l] = C(m[2 * l], m[2 * l + 1]);
+  int64_t n = default_n_max(xs[layers - 1]);
+  *n_terms = n;
+  if (!a) return OK;
+  MieState s;
+  layered_solve(xs, ms, n, s);
+  for (int64_t k = 0; k < n; ++k) {
+    a[2 * k] = s.a[k].re;
+    a[2 * k + 1] = s.a[k].im;
+    b[2 * k] = s.b[k].re;
+    b[2 * k + 1] = s.b[k].im;
+  }
+  s.x = xs[layers - 1];
+  Efficiencies q = efficiencies(s);
+  eff[0] = q.q_ext;
+  eff[1] = q.q_sca;
+  eff[2] = q.q_abs;
+  eff[3] = q.q_back;
+  eff[4] = q.g;
+  return OK;
+}
+
 // MieSolution::amplitudes (mie/amplitudes.rs:328-344) of the sphere (x, m) with the default
 // truncation (or n_max terms): s1, s2 interleaved re/im, one pair per cosine.
 int orc_amplitudes(double x, double m_re, double m_im, int64_t n_max, const double* mu,
@@ -188,11 +216,76 @@ static BandData make_band(int64_t upper, int64_t order) {
   return b;
 }
 
+// Layered::check_inputs (layered/mod.rs:233-305) with the default truncation.
+static int check_layered(const std::vector<double>& x, const std::vector<cplx>& m,
+                         bool allow_unvalidated, std::string* msg) {
+  const size_t L = x.size();
+  for (size_t l = 0; l < L; ++l)
+    if (!std::isfinite(x[l]) || (l > 0 && x[l] < x[l - 1])) {
+      *msg = "the size parameters must be finite and nondecreasing from the core out";
+      return INVALID_INPUT;
+    }
+  const double outer = x[L - 1];
+  if (x[0] < MIN_SIZE_PARAMETER || outer > MAX_SIZE_PARAMETER) {
+    *msg = "the size parameters must be in [1e-30, 1e6]";
+    return INVALID_INPUT;
+  }
+  for (auto& v : m) {
+    if (!(std::isfinite(v.re) && std::isfinite(v.im)) || v.re < 0.0 || v.im < 0.0 ||
+        !(cnorm(v) >= MIN_REFRACTIVE_INDEX && cnorm(v) <= MAX_REFRACTIVE_INDEX)) {
+      *msg = "invalid refractive index of a layer";
+      return INVALID_INPUT;
+    }
+  }
+  if (!allow_unvalidated) {
+    bool in = L <= 16 && outer >= 1e-6 && outer <= 1e4;
+    for (auto& v : m)
+      in = in && cnorm(v) * outer <= 3e4 && v.re > 0.0 && v.re <= 10.0 && v.im >= 0.0 &&
+           v.im <= 10.0 && cnorm(v) >= 0.1;
+    if (!in) {
+      *msg = "outside the validated domain of layered spheres";
+      return OUTSIDE_VALIDATED_DOMAIN;
+    }
+  }
+  return OK;
+}
+
+static int ensemble_impl(const FixedDist* dists, int64_t n_dist, const double* wl, int64_t n_wl,
+                         const double* m, int n_layers, const double* fractions,
+                         const double* m_layers, int64_t n_nodes, const double* mu,
+                         int64_t n_mu, int64_t greek_order, int normalized,
+                         int allow_unvalidated, int n_threads, double* values, double* phase,
+                         double* greek, char* err, int64_t err_len);
+
 int orc_ensemble_fixed(const FixedDist* dists, int64_t n_dist, const double* wl, int64_t n_wl,
                        const double* m, int64_t n_nodes, const double* mu, int64_t n_mu,
                        int64_t greek_order, int normalized, int allow_unvalidated,
                        int n_threads, double* values, double* phase, double* greek,
                        char* err, int64_t err_len) {
+  return ensemble_impl(dists, n_dist, wl, n_wl, m, 1, nullptr, nullptr, n_nodes, mu, n_mu,
+                       greek_order, normalized, allow_unvalidated, n_threads, values, phase,
+                       greek, err, err_len);
+}
+
+// The fixed-grid ensemble of layered spheres: fractions [n_dist][n_layers - 1], m_layers
+// complex [n_dist][n_layers][n_wl].
+int orc_ensemble_fixed_layered(const FixedDist* dists, int64_t n_dist, const double* wl,
+                               int64_t n_wl, int n_layers, const double* fractions,
+                               const double* m_layers, int64_t n_nodes, const double* mu,
+                               int64_t n_mu, int64_t greek_order, int normalized,
+                               int allow_unvalidated, int n_threads, double* values,
+                               double* phase, double* greek, char* err, int64_t err_len) {
+  return ensemble_impl(dists, n_dist, wl, n_wl, nullptr, n_layers, fractions, m_layers, n_nodes,
+                       mu, n_mu, greek_order, normalized, allow_unvalidated, n_threads, values,
+                       phase, greek, err, err_len);
+}
+
+static int ensemble_impl(const FixedDist* dists, int64_t n_dist, const double* wl, int64_t n_wl,
+                         const double* m, int n_layers, const double* fractions,
+                         const double* m_layers, int64_t n_nodes, const double* mu,
+                         int64_t n_mu, int64_t greek_order, int normalized,
+                         int allow_unvalidated, int n_threads, double* values, double* phase,
+                         double* greek, char* err, int64_t err_len) {
   const int64_t n_units = n_dist * n_wl;
   std::vector<double> xi(n_nodes), om(n_nodes);
   gauss_legendre(n_nodes, xi.data(), om.data());
@@ -242,7 +335,12 @@ int orc_ensemble_fixed(const FixedDist* dists, int64_t n_dist, const double* wl,
   for (int64_t unit = 0; unit < n_units; ++unit) {
     int64_t d = unit / n_wl, i = unit % n_wl;
     double lambda = wl[i];
-    cplx mv = C(m[2 * unit], m[2 * unit + 1]);
+    cplx mv = n_layers > 1 ? C(0.0, 0.0) : C(m[2 * unit], m[2 * unit + 1]);
+    std::vector<cplx> mls(n_layers);
+    for (int l = 0; n_layers > 1 && l < n_layers; ++l) {
+      const double* p = m_layers + 2 * ((d * n_layers + l) * n_wl + i);
+      mls[l] = C(p[0], p[1]);
+    }
     std::vector<double> S(9, 0.0), Smu(4 * n_mu, 0.0);
     std::vector<std::vector<double>> Sband(bands.size());
     MieState st;
@@ -262,14 +360,26 @@ int orc_ensemble_fixed(const FixedDist* dists, int64_t n_dist, const double* wl,
         double W = weight[d * n_nodes + j];
         double x = 2.0 * PI * r / lambda;
         int64_t n = 0;
-        status = check_inputs(x, mv.re, mv.im, 0, allow_unvalidated != 0, &n, &msg);
+        if (n_layers <= 1) {
+          status = check_inputs(x, mv.re, mv.im, 0, allow_unvalidated != 0, &n, &msg);
+        } else {
+          std::vector<double> xs(n_layers);
+          for (int l = 0; l < n_layers - 1; ++l) xs[l] = fractions[d * (n_layers - 1) + l] * x;
+          xs[n_layers - 1] = x;
+          status = check_layered(xs, mls, allow_unvalidated != 0, &msg);
+          n = default_n_max(x);
+          if (status == OK) {
+            layered_solve(xs, mls, n, st);
+            st.x = x;
+          }
+        }
         if (status != OK) {
           char buf[160];
           snprintf(buf, sizeof buf, "at wavelength %e, radius %e: ", lambda, r);
           msg = buf + msg;
           break;
         }
-        st.solve(x, mv, n, false);
+        if (n_layers <= 1) st.solve(x, mv, n, false);
         Efficiencies q = efficiencies(st);
         double area = PI * r * r;
         double qv[9] = {1.0,          area * q.q_ext, area * q.q_sca, area * q.q_sca * q.g,

@@ -170,6 +170,17 @@ inline int64_t upward_orders(double x, int64_t n) {
   return 0;
 }
 
+// One coefficient's effective log-derivative H at a layered sphere's outer surface at one order
+// (mie/kernel.rs:16-24): as the correction delta = H - D_n(mx), or as H itself near the poles.
+enum SideKind { SIDE_DELTA = 0, SIDE_DIRECT = 1 };
+struct Side {
+  int kind;
+  cplx v;
+};
+struct Outer {
+  Side a, b;
+};
+
 struct MieState {
   double x = 0;
   cplx m{0, 0};
@@ -219,7 +230,7 @@ struct MieState {
   }
 
   // State::finish (kernel.rs:324-559), homogeneous sphere (no layered outer hooks).
-  void finish(double xv, cplx mv, int64_t n, bool derivs) {
+  void finish(double xv, cplx mv, int64_t n, bool derivs, const Outer* outer = nullptr) {
     const double one = 1.0, two = 2.0;
     x = xv;
     m = mv;
@@ -255,7 +266,13 @@ struct MieState {
       double kf = (double)k;
       double k_x = kf * inv_x;
       cplx d = scale(inv_z, (double)(k + 1)) - u_z[k + 1];
-      cplx hh_a = d, hh_b = d;
+      // H of a layered sphere in place of D_n(mx) (kernel.rs:382-388).
+      auto hsel = [&](const Side* sd) {
+        if (!sd) return d;
+        return sd->kind == SIDE_DELTA ? d + sd->v : sd->v;
+      };
+      const Outer* side = outer ? &outer[k - 1] : nullptr;
+      cplx hh_a = hsel(side ? &side->a : nullptr), hh_b = hsel(side ? &side->b : nullptr);
       cplx d_m = hh_a * inv_m;
       cplx md = hh_b * mv;
       cplx big_a = d_m + real(k_x);
@@ -273,8 +290,21 @@ struct MieState {
         cplx xi_prev = C(psi_prev, -chi_prev);
         inv_da = inv(big_a * xi - xi_prev);
         inv_db = inv(big_b * xi - xi_prev);
-        an = (scale(big_a, psi) - real(psi_prev)) * inv_da;
-        bn = (scale(big_b, psi) - real(psi_prev)) * inv_db;
+        if (!side) {
+          an = (scale(big_a, psi) - real(psi_prev)) * inv_da;
+          bn = (scale(big_b, psi) - real(psi_prev)) * inv_db;
+        } else {
+          // kernel.rs:412-435: the outer layer's own numerator plus delta/m psi_n, m delta psi_n.
+          auto own = [&](cplx f) {
+            if (mv.re == 1.0 && mv.im == 0.0) return real(0.0);
+            return scale(f + real(k_x), psi) - real(psi_prev);
+          };
+          an = side->a.kind == SIDE_DELTA
+                   ? (own(d * inv_m) + scale(side->a.v * inv_m, psi)) * inv_da
+                   : (scale(big_a, psi) - real(psi_prev)) * inv_da;
+          bn = side->b.kind == SIDE_DELTA ? (own(d * mv) + scale(mv * side->b.v, psi)) * inv_db
+                                          : (scale(big_b, psi) - real(psi_prev)) * inv_db;
+        }
         g_a = xi * inv_da;
         g_b = xi * inv_db;
         h_a = xi_prev * inv_da;
@@ -292,6 +322,12 @@ struct MieState {
         cplx u_x1 = real(u_x[k + 1]);
         cplx num_a = scale(c_a, (double)(k + 1) * inv_x) + u_x1 - u_z1 * inv_m;
         cplx num_b = u_x1 - mv * u_z1;
+        if (side) {
+          // kernel.rs:456-466.
+          cplx d_x = real((double)(k + 1) * inv_x) - u_x1;
+          num_a = side->a.kind == SIDE_DELTA ? num_a + side->a.v * inv_m : d_m - d_x;
+          num_b = side->b.kind == SIDE_DELTA ? num_b + mv * side->b.v : md - d_x;
+        }
         cplx ia = inv(big_a - r);
         cplx ib = inv(big_b - r);
         an = t * num_a * ia;
@@ -309,7 +345,7 @@ struct MieState {
       double nb = norm_sqr(inv_db);
       double weight = (double)(2 * k + 1);
       asum += weight * (-(d_m.im * na) - md.im * nb);
-      if (derivs) {
+      if (derivs && !outer) {
         cplx u = u_z[k + 1];
         cplx one_u2 = real(one) + u * u;
         cplx dp = scale(scale(u, two) * inv_z - inv_z * inv_z, (double)(k + 1)) - one_u2;
@@ -349,6 +385,183 @@ struct MieState {
     finish(xv, mv, n, derivs);
   }
 };
+
+// ---------------------------------------------------------------------------------------
+// Layered spheres (scatrs/src/layered/kernel.rs), values only.
+// ---------------------------------------------------------------------------------------
+// num-complex's sin, cos: sin(a+ib) = sin a cosh b + i cos a sinh b, cos(a+ib) = cos a cosh b
+// - i sin a sinh b.
+inline cplx csin(cplx z) { return {std::sin(z.re) * std::cosh(z.im), std::cos(z.re) * std::sinh(z.im)}; }
+inline cplx ccos(cplx z) { return {std::cos(z.re) * std::cosh(z.im), -std::sin(z.re) * std::sinh(z.im)}; }
+// complex::exp_m1 (complex.rs:51-56).
+inline cplx cexp_m1(cplx w) {
+  double a = w.re, b = w.im;
+  double sb = std::sin(b), cb = std::cos(b);
+  double h = std::sin(b * 0.5);
+  return {std::expm1(a) * cb - h * h * 2.0, std::exp(a) * sb};
+}
+// 2iz (layered/kernel.rs:45-47).
+inline cplx two_i(cplx z) { return {-(z.im * 2.0), z.re * 2.0}; }
+
+// ratios (mie/kernel.rs:159-205): u_k(mx) for k = 1..n+1.
+inline std::vector<cplx> ratios(cplx m, double x, int64_t n) {
+  std::vector<cplx> out(n + 2, real(0.0));
+  cplx z = scale(m, x);
+  if (m.im == 0.0) {
+    double inv_rho = 1.0 / z.re, u = 0.0;
+    int64_t start = start_index(n + 1, std::fabs(z.re));
+    for (int64_t k = start; k >= 1; --k) {
+      u = step_real(k, inv_rho, u);
+      if (k <= n + 1) out[k] = real(u);
+    }
+  } else {
+    cplx inv_z = inv(z), u = real(0.0);
+    int64_t start = start_index(n + 1, cnorm(z));
+    for (int64_t k = start; k >= 1; --k) {
+      u = step_complex(k, inv_z, u);
+      if (k <= n + 1) out[k] = u;
+    }
+  }
+  return out;
+}
+
+// Arg (layered/kernel.rs:33-103): Pi_n(z) and w_{n+1}(z), advanced order by order.
+struct Arg {
+  cplx z, inv_z, pi, w, w_n;
+  Arg() = default;
+  Arg(cplx zz, bool chi) {
+    z = zz;
+    inv_z = inv(z);
+    if (chi) {
+      cplx sz = csin(z), cz = ccos(z);
+      pi = sz * cz;
+      w = inv_z + sz * inv(cz);
+    } else {
+      pi = -scale(cexp_m1(two_i(z)), 0.5);
+      w = inv_z - C(0.0, 1.0);
+    }
+    w_n = real(0.0);
+  }
+  void step(int64_t n, cplx u_n) {
+    w_n = w;
+    pi = pi * u_n * w;
+    w = scale(inv_z, (double)(2 * n + 1)) - inv(w);
+  }
+  cplx d1(int64_t n, cplx u_next) const { return scale(inv_z, (double)(n + 1)) - u_next; }
+  cplx d3(int64_t n) const { return scale(inv_z, (double)(n + 1)) - w; }
+};
+
+inline double norm1(cplx z) { return std::fabs(z.re) + std::fabs(z.im); }
+
+struct LayerStep {
+  cplx u_prev, u1, d1i, d3i, d1o, d3o, pio, p, w;
+};
+
+// side (layered/kernel.rs:158-183) without the derivatives' sensitivities.
+inline Side layer_side(cplx mi, cplx mo, Side prev, cplx h, cplx lead, const LayerStep& s,
+                       cplx* h_out) {
+  cplx mh = mi * h;
+  cplx g1 = prev.kind == SIDE_DELTA ? lead - mi * s.u_prev + mo * s.u1 + mi * prev.v
+                                    : mh - mo * s.d1i;
+  cplx g2 = mh - mo * s.d3i;
+  cplx inv_den = inv(s.pio * g2 - s.p * g1);
+  cplx delta = -(s.w * s.p * g1 * inv_den * inv(s.pio));
+  cplx hd = s.d1o + delta;
+  if (norm1(hd) * 4.0 >= std::max(norm1(s.d1o), norm1(delta))) {
+    *h_out = hd;
+    return {SIDE_DELTA, delta};
+  }
+  cplx hp = s.d3o - s.w * g2 * inv_den;
+  *h_out = hp;
+  return {SIDE_DIRECT, hp};
+}
+
+// Kernel::solve (layered/kernel.rs:308-465) for values: x[l] the interface size parameters (the
+// outer one last), m[l] the layers' indices; a_n, b_n and the absorption sum into `mie`.
+inline void layered_solve(const std::vector<double>& x, const std::vector<cplx>& m, int64_t n,
+                          MieState& mie) {
+  const size_t layers = x.size(), last = layers - 1;
+  if (last == 0) {
+    mie.solve(x[0], m[0], n, false);
+    return;
+  }
+  mie.prepare(x[last], m[last], n);
+  std::vector<std::vector<cplx>> u(2 * last);
+  u[0] = ratios(m[0], x[0], n);
+  for (size_t l = 1; l < layers; ++l) {
+    u[2 * l - 1] = ratios(m[l], x[l - 1], n);
+    if (l < last) u[2 * l] = ratios(m[l], x[l], n);
+  }
+  std::vector<Arg> inner, outer_args;
+  std::vector<cplx> p, lead;
+  std::vector<bool> chi;
+  for (size_t l = 1; l < layers; ++l) {
+    bool c = m[l].im * x[l] < 0.5;
+    chi.push_back(c);
+    cplx a = m[l], b = m[l - 1];
+    lead.push_back((a - b) * (a + b) * inv(a * b));
+    cplx z1 = scale(m[l], x[l - 1]), z2 = scale(m[l], x[l]);
+    inner.emplace_back(z1, c);
+    outer_args.emplace_back(z2, c);
+    cplx p0;
+    if (c) {
+      cplx c2 = ccos(z2);
+      p0 = csin(z1) * inv(ccos(z1)) * c2 * c2;
+    } else {
+      double dx = x[l] - x[l - 1];
+      double ea = -(m[l].im * dx * 2.0), eb = m[l].re * dx * 2.0;
+      double sb = std::sin(eb), cb = std::cos(eb);
+      cplx e = scale(C(cb, sb), std::exp(ea));
+      p0 = -scale(e * cexp_m1(two_i(z1)), 0.5);
+    }
+    p.push_back(p0);
+  }
+  Arg core(scale(m[0], x[0]), false);
+  std::vector<Outer> outer(n);
+  for (int64_t k = 1; k <= n; ++k) {
+    auto u_of = [&](size_t l) -> const std::vector<cplx>& {
+      return l == last ? mie.u_z : u[2 * l];
+    };
+    for (size_t l = 1; l < layers; ++l) {
+      Arg& ai = inner[l - 1];
+      Arg& ao = outer_args[l - 1];
+      ai.step(k, u[2 * l - 1][k]);
+      ao.step(k, u_of(l)[k]);
+      p[l - 1] = p[l - 1] * u[2 * l - 1][k] * inv(ai.w_n) * ao.w_n * ao.w_n;
+    }
+    cplx ha = core.d1(k, u[0][k + 1]);
+    cplx hb = ha;
+    Side sa{SIDE_DELTA, real(0.0)}, sb{SIDE_DELTA, real(0.0)};
+    for (size_t l = 1; l < layers; ++l) {
+      const Arg& ai = inner[l - 1];
+      const Arg& ao = outer_args[l - 1];
+      const std::vector<cplx>& up = l == 1 ? u[0] : u[2 * (l - 1)];
+      LayerStep st;
+      st.u_prev = up[k + 1];
+      st.u1 = u[2 * l - 1][k + 1];
+      st.d1i = ai.d1(k, u[2 * l - 1][k + 1]);
+      st.d3i = ai.d3(k);
+      st.d1o = ao.d1(k, u_of(l)[k + 1]);
+      st.d3o = ao.d3(k);
+      st.pio = ao.pi;
+      st.p = p[l - 1];
+      st.w = chi[l - 1] ? real(-1.0) : C(0.0, 1.0);
+      cplx ld = scale(lead[l - 1], (double)(k + 1) / x[l - 1]);
+      cplx na, nb;
+      Side a2 = layer_side(m[l], m[l - 1], sa, ha, ld, st, &na);
+      Side b2 = layer_side(m[l - 1], m[l], sb, hb, real(0.0), st, &nb);
+      ha = na;
+      hb = nb;
+      sa = a2;
+      sb = b2;
+    }
+    outer[k - 1] = {sa, sb};
+  }
+  mie.finish(x[last], m[last], n, false, outer.data());
+  bool lossless = true;
+  for (auto& v : m) lossless = lossless && v.im == 0.0;
+  if (lossless) mie.abs_sum = 0.0;
+}
 
 // ---------------------------------------------------------------------------------------
 // Efficiencies (scatrs/src/mie/efficiencies.rs:64-84, 169-187).

@@ -30,6 +30,10 @@ DIST_DTYPE = np.dtype([("kind", np.int32), ("reserved", np.int32), ("param", np.
 KINDS = {"lognormal": 1, "gamma": 2, "modified_gamma": 3, "power_law": 4}
 
 
+class Layers(ctypes.Structure):
+    _fields_ = [("n_layers", _I32), ("reserved", _I32), ("fractions", _PD), ("m", _PD)]
+
+
 class FixedOptions(ctypes.Structure):
     _fields_ = [("n_nodes", _I32), ("greek_order", _I32), ("normalized", _I32),
                 ("allow_unvalidated", _I32)]
@@ -41,6 +45,9 @@ SYMBOLS = {
     "scatrs_ensemble_fixed": (ctypes.c_int, [_VP, _I64, _PD, _I64, _PD, _PD, _I64,
                                              ctypes.POINTER(FixedOptions), _PD, _PD, _PD, _CP,
                                              _SZ]),
+    "scatrs_ensemble_fixed_layered": (ctypes.c_int, [_VP, _I64, _PD, _I64, ctypes.POINTER(Layers),
+                                                     _PD, _I64, ctypes.POINTER(FixedOptions), _PD,
+                                                     _PD, _PD, _CP, _SZ]),
     "scatrs_ensemble_fixed_device": (ctypes.c_int, [_VP, _I64, _VP, _I64, _VP, _PD, _I64,
                                                     ctypes.POINTER(FixedOptions), _VP, _VP, _VP,
                                                     _VP, _CP, _SZ]),
@@ -162,6 +169,33 @@ def ensemble_fixed(dists: np.ndarray, wavelengths, m, mu, n_nodes: int, greek_or
                                       _p(m.view(np.float64)), _p(mu), mu.size,
                                       ctypes.byref(opts), _p(values), _p(phase), _p(greek), err,
                                       1024)
+    _check(st, err)
+    return values, phase, greek
+
+
+def ensemble_fixed_layered(dists: np.ndarray, wavelengths, fractions, m_layers, mu,
+                           n_nodes: int, greek_order: int = -1, normalized: bool = True,
+                           allow_unvalidated: bool = False):
+    """The fixed-grid ensemble of layered spheres: fractions (n_dist, L - 1), m_layers complex
+    (n_dist, L, n_wl); outputs as ensemble_fixed."""
+    require_device()
+    dists = np.ascontiguousarray(dists, dtype=DIST_DTYPE)
+    wl = np.ascontiguousarray(wavelengths, dtype=np.float64).reshape(-1)
+    ml = np.ascontiguousarray(m_layers, dtype=np.complex128)
+    n_layers = ml.shape[1]
+    fr = np.ascontiguousarray(fractions, dtype=np.float64).reshape(dists.size, n_layers - 1)
+    mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
+    n = dists.size * wl.size
+    lay = Layers(n_layers, 0, _p(fr), _p(ml.view(np.float64).reshape(-1)))
+    opts = FixedOptions(int(n_nodes), int(greek_order), int(normalized), int(allow_unvalidated))
+    values = np.zeros((11, n))
+    phase = np.zeros((6, n, mu.size)) if mu.size else None
+    greek = np.zeros((6, n, greek_order + 1)) if greek_order >= 0 else None
+    err = ctypes.create_string_buffer(1024)
+    st = load().scatrs_ensemble_fixed_layered(dists.ctypes.data, dists.size, _p(wl), wl.size,
+                                              ctypes.byref(lay), _p(mu), mu.size,
+                                              ctypes.byref(opts), _p(values), _p(phase),
+                                              _p(greek), err, 1024)
     _check(st, err)
     return values, phase, greek
 

@@ -139,7 +139,7 @@ struct Context {
   UserTables user;
   std::map<int, BandTables> bands;  // by Greek order
   std::map<int64_t, std::pair<std::vector<double>, std::vector<double>>> rules;
-  DevBuf radius, weight, wl, m, chunk_n, chunk_n_slab, chunk_row, chunk_acc, plan_units,
+  DevBuf radius, weight, wl, m, fractions, chunk_n, chunk_n_slab, chunk_row, chunk_acc, plan_units,
       unit_acc, unit_slots, slots, items, proj_items, slot_index, slot_greek, X, uz, ux,
       chunk_sums, err, acc, counter, values, phase, greek;
   std::vector<int> chunk_n_host;
@@ -368,10 +368,18 @@ struct FixedCall {
 };
 
 // The device pipeline; wl_dev and m_dev are device arrays, outputs device arrays.
+// Layered spheres: L layers, per distribution the L - 1 radius fractions (host) and the
+// layers' indices per wavelength (device, [n_dist][L][n_wl] complex).
+struct LayerInput {
+  int n_layers = 1;
+  const double* fractions = nullptr;
+  const double* m_dev = nullptr;
+};
+
 void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, const double* wl_dev,
                int64_t n_wl, const double* m_dev, const double* mu, int64_t n_mu,
                const scatrs_fixed_options* opt, double* values, double* phase, double* greek,
-               cudaStream_t s, FixedCall* call) {
+               cudaStream_t s, FixedCall* call, const LayerInput& layers = LayerInput()) {
   const int64_t n_units = n_dist * n_wl;
   check_options(opt, n_units, n_mu, mu);
   if (n_units == 0) return;
@@ -399,6 +407,22 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
       radius[d * n_nodes + j] = r;
       weight[d * n_nodes + j] = h * gl.second[j] * (u * r);
     }
+  }
+  const int L_layers = layers.n_layers;
+  if (L_layers < 1 || L_layers > 16)
+    throw Failure{SCATRS_INVALID_INPUT, "the GPU path takes 1 to 16 layers"};
+  if (L_layers > 1) {
+    for (int64_t d = 0; d < n_dist; ++d)
+      for (int l = 0; l < L_layers - 1; ++l) {
+        const double f = layers.fractions[d * (L_layers - 1) + l];
+        const double prev = l > 0 ? layers.fractions[d * (L_layers - 1) + l - 1] : 0.0;
+        if (!(f > 0.0 && f <= 1.0 && f >= prev))
+          throw Failure{SCATRS_INVALID_INPUT,
+                        "distribution " + std::to_string(d) +
+                            ": radius fractions must be nondecreasing in (0, 1]"};
+      }
+    SB_CUDA(cudaMemcpyAsync(c.fractions.get(n_dist * (L_layers - 1) * 8), layers.fractions,
+                            n_dist * (L_layers - 1) * 8, cudaMemcpyHostToDevice, s));
   }
   SB_CUDA(cudaMemcpyAsync(c.radius.get(radius.size() * 8), radius.data(), radius.size() * 8,
                           cudaMemcpyHostToDevice, s));
@@ -589,7 +613,8 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
   ProjItem* proj_d = c.proj_items.as<ProjItem>(std::max<int64_t>(n_proj_all, 1));
   WorkItem* items_d = c.items.as<WorkItem>(std::max<int64_t>(n_items_all, 1));
   double* X = c.X.as<double>((size_t)arena * 128);
-  double2* uz = c.uz.as<double2>((size_t)(arena + 2 * kMaxSlabChunks) * 32);
+  const int n_arr = L_layers > 1 ? 2 * L_layers - 1 : 1;
+  double2* uz = c.uz.as<double2>((size_t)(arena + 2 * kMaxSlabChunks) * 32 * n_arr);
   double* ux = c.ux.as<double>((size_t)(arena + 2 * kMaxSlabChunks) * 32);
   double* chunk_sums = c.chunk_sums.as<double>((size_t)kMaxSlabChunks * 8);
   double* acc = c.acc.as<double>((size_t)acc_max);
@@ -608,6 +633,11 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
   ka.n_wl = (int)n_wl;
   ka.n_nodes = (int)n_nodes;
   ka.cpu = cpu;
+  ka.n_layers = L_layers;
+  if (L_layers > 1) {
+    ka.fractions = c.fractions.as<double>(0);
+    ka.m_layers = reinterpret_cast<const double2*>(layers.m_dev);
+  }
   ka.X = X;
   ka.uz = uz;
   ka.ux = ux;
@@ -914,6 +944,57 @@ int scatrs_ensemble_fixed(const scatrs_distribution* dists, int64_t n_dist,
   });
 }
 
+int scatrs_ensemble_fixed_layered(const scatrs_distribution* dists, int64_t n_dist,
+                                  const double* wavelengths, int64_t n_wl,
+                                  const scatrs_layers* layers, const double* mu, int64_t n_mu,
+                                  const scatrs_fixed_options* options, double* values,
+                                  double* phase, double* greek, char* err, size_t err_len) {
+  return guarded(err, err_len, [&] {
+    if (n_dist < 0 || n_wl < 0) throw Failure{SCATRS_INVALID_INPUT, "negative sizes"};
+    if (!layers || layers->n_layers < 1 || (layers->n_layers > 1 && !layers->fractions) ||
+        !layers->m)
+      throw Failure{SCATRS_INVALID_INPUT, "layers must give n_layers >= 1, fractions and m"};
+    for (int64_t i = 0; i < n_wl; ++i)
+      if (!(std::isfinite(wavelengths[i]) && wavelengths[i] > 0.0))
+        throw Failure{SCATRS_INVALID_INPUT, "wavelengths must be finite and > 0"};
+    Context& c = context();
+    std::lock_guard<std::mutex> lk(c.mtx);
+    cudaStream_t s = 0;
+    const int64_t n_units = n_dist * n_wl;
+    check_options(options, n_units, n_mu, mu);
+    if (n_units == 0) return;
+    const int L = layers->n_layers;
+    double* wl_d = c.wl.as<double>(n_wl);
+    SB_CUDA(cudaMemcpyAsync(wl_d, wavelengths, n_wl * 8, cudaMemcpyHostToDevice, s));
+    LayerInput li;
+    li.n_layers = L;
+    li.fractions = layers->fractions;
+    double* m_d;
+    if (L == 1) {
+      m_d = c.m.as<double>(2 * n_units);
+      SB_CUDA(cudaMemcpyAsync(m_d, layers->m, 2 * n_units * 8, cudaMemcpyHostToDevice, s));
+    } else {
+      m_d = c.m.as<double>(2 * n_dist * L * n_wl);
+      SB_CUDA(cudaMemcpyAsync(m_d, layers->m, 2 * n_dist * L * n_wl * 8, cudaMemcpyHostToDevice,
+                              s));
+      li.m_dev = m_d;
+    }
+    int64_t vl, pl, gl;
+    scatrs_ensemble_fixed_sizes(n_units, n_mu, options->greek_order, &vl, &pl, &gl);
+    double* v_d = c.values.as<double>(vl);
+    double* p_d = pl > 0 ? c.phase.as<double>(pl) : nullptr;
+    double* g_d = gl > 0 ? c.greek.as<double>(gl) : nullptr;
+    FixedCall call;
+    call.wl_host.assign(wavelengths, wavelengths + n_wl);
+    run_fixed(c, dists, n_dist, wl_d, n_wl, m_d, mu, n_mu, options, v_d, p_d, g_d, s, &call, li);
+    check_device_errors(c, s, &call);
+    SB_CUDA(cudaMemcpyAsync(values, v_d, vl * 8, cudaMemcpyDeviceToHost, s));
+    if (pl > 0 && phase) SB_CUDA(cudaMemcpyAsync(phase, p_d, pl * 8, cudaMemcpyDeviceToHost, s));
+    if (gl > 0 && greek) SB_CUDA(cudaMemcpyAsync(greek, g_d, gl * 8, cudaMemcpyDeviceToHost, s));
+    SB_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
 int scatrs_ensemble_fixed_device(const scatrs_distribution* dists_host, int64_t n_dist,
                                  const double* wavelengths_dev, int64_t n_wl,
                                  const double* m_dev, const double* mu_host, int64_t n_mu,
@@ -1066,7 +1147,7 @@ void scatrs_release(void) {
   std::lock_guard<std::mutex> lk(g_ctx_mtx);
   if (dev < (int)g_ctx.size() && g_ctx[dev]) {
     Context& c = *g_ctx[dev];
-    for (DevBuf* b : {&c.radius, &c.weight, &c.wl, &c.m, &c.chunk_n, &c.chunk_n_slab,
+    for (DevBuf* b : {&c.radius, &c.weight, &c.wl, &c.m, &c.fractions, &c.chunk_n, &c.chunk_n_slab,
                       &c.chunk_row, &c.chunk_acc, &c.plan_units, &c.unit_acc, &c.unit_slots,
                       &c.slots, &c.items, &c.proj_items, &c.slot_index, &c.slot_greek,
                       &c.X, &c.uz, &c.ux, &c.chunk_sums, &c.err, &c.acc,

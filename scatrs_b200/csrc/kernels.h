@@ -21,8 +21,13 @@ struct MieFixedArgs {
   const double* radius;  // [n_dist][n_nodes]
   const double* weight;  // [n_dist][n_nodes]: w_j u(r_j) r_j
   const double* wl;      // [n_wl]
-  const double2* m;      // [n_units_total]
+  const double2* m;      // [n_units_total] (homogeneous spheres)
   int n_dist, n_wl, n_nodes, cpu;
+  // Layered spheres (n_layers > 1): layer l's outer radius over the particle's (l < L - 1) per
+  // distribution, and each layer's index per distribution and wavelength.
+  int n_layers;
+  const double* fractions;  // [n_dist][n_layers - 1]
+  const double2* m_layers;  // [n_dist][n_layers][n_wl]
   const int* units;         // slab-local unit -> global unit
   int n_chunks;             // chunks of the slab (units x cpu)
   const int* chunk_n;       // slab-local: each chunk's largest number of terms

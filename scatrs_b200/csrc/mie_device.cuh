@@ -212,12 +212,26 @@ __device__ __forceinline__ Eff efficiencies_from(double x, double abs_sum, const
   return {q_sca + q_abs, q_sca, q_abs, nsq(s.back) * inv_x2, g};
 }
 
-// State::finish (kernel.rs:324-559) for a homogeneous sphere without derivatives: calls
-// emit(k, a_k, b_k) for k = 1..n and returns the absorption sum (x^2/2) Q_abs, feeding the
-// value sums on the way.
-template <class Emit>
+// One coefficient's effective log-derivative H at a layered sphere's outer surface at one order
+// (kernel.rs:16-24): the correction delta = H - D_n(mx), or H itself near D_n's poles.
+struct Side {
+  bool direct;
+  cplx v;
+};
+
+// No layers: D_n(mx) itself.
+struct NoLayers {
+  static constexpr bool kLayered = false;
+  __device__ __forceinline__ void order(int64_t, Side&, Side&) {}
+};
+
+// State::finish (kernel.rs:324-559) without derivatives: calls emit(k, a_k, b_k) for k = 1..n
+// and returns the absorption sum (x^2/2) Q_abs, feeding the value sums on the way. With a
+// layered sphere's `layers`, its H_a, H_b replace D_n(mx) at each order (kernel.rs:382-476);
+// they are computed order by order in the same upward loop.
+template <class Emit, class Layers>
 __device__ __forceinline__ double mie_finish(double x, cplx m, int64_t n, const Scratch& s,
-                                             ValueSums& vs, Emit emit) {
+                                             ValueSums& vs, Emit emit, Layers& layers) {
   const double one = 1.0;
   cplx z = scl(m, x);
   int64_t n_s = upward_orders(x, n);
@@ -246,8 +260,15 @@ __device__ __forceinline__ double mie_finish(double x, cplx m, int64_t n, const 
     cplx u_z1 = u_next;
     if (k < n) u_next = s.get_z(k + 2);
     cplx d = scl(inv_z, (double)(k + 1)) - u_z1;
-    cplx d_m = d * inv_m;
-    cplx md = d * m;
+    Side sa{false, rl(0.0)}, sb{false, rl(0.0)};
+    cplx hh_a = d, hh_b = d;
+    if (Layers::kLayered) {
+      layers.order(k, sa, sb);
+      hh_a = sa.direct ? sa.v : d + sa.v;
+      hh_b = sb.direct ? sb.v : d + sb.v;
+    }
+    cplx d_m = hh_a * inv_m;
+    cplx md = hh_b * m;
     cplx big_a = d_m + rl(k_x);
     cplx big_b = md + rl(k_x);
     cplx an, bn, inv_da, inv_db;
@@ -263,8 +284,20 @@ __device__ __forceinline__ double mie_finish(double x, cplx m, int64_t n, const 
       cplx xi_prev = mk(psi_prev, -chi_prev);
       inv_da = cinv(big_a * xi - xi_prev);
       inv_db = cinv(big_b * xi - xi_prev);
-      an = (scl(big_a, psi) - rl(psi_prev)) * inv_da;
-      bn = (scl(big_b, psi) - rl(psi_prev)) * inv_db;
+      if (!Layers::kLayered) {
+        an = (scl(big_a, psi) - rl(psi_prev)) * inv_da;
+        bn = (scl(big_b, psi) - rl(psi_prev)) * inv_db;
+      } else {
+        // The outer layer's own numerator plus delta/m psi_n and m delta psi_n
+        // (kernel.rs:412-435); the own numerator is exactly 0 for m = 1.
+        const bool unit_m = m.re == 1.0 && m.im == 0.0;
+        cplx own_a = unit_m ? rl(0.0) : scl(d * inv_m + rl(k_x), psi) - rl(psi_prev);
+        cplx own_b = unit_m ? rl(0.0) : scl(d * m + rl(k_x), psi) - rl(psi_prev);
+        an = sa.direct ? (scl(big_a, psi) - rl(psi_prev)) * inv_da
+                       : (own_a + scl(sa.v * inv_m, psi)) * inv_da;
+        bn = sb.direct ? (scl(big_b, psi) - rl(psi_prev)) * inv_db
+                       : (own_b + scl(m * sb.v, psi)) * inv_db;
+      }
       if (k == n_s) {
         inv_xi = cinv(xi);
         t = rl(psi) * inv_xi;
@@ -277,6 +310,12 @@ __device__ __forceinline__ double mie_finish(double x, cplx m, int64_t n, const 
       cplx u_x1 = rl(s.get_x(k + 1));
       cplx num_a = scl(c_a, (double)(k + 1) * inv_x) + u_x1 - u_z1 * inv_m;
       cplx num_b = u_x1 - m * u_z1;
+      if (Layers::kLayered) {
+        // kernel.rs:456-466.
+        cplx d_x = rl((double)(k + 1) * inv_x) - u_x1;
+        num_a = sa.direct ? d_m - d_x : num_a + sa.v * inv_m;
+        num_b = sb.direct ? md - d_x : num_b + m * sb.v;
+      }
       cplx ia = cinv(big_a - r);
       cplx ib = cinv(big_b - r);
       an = t * num_a * ia;
@@ -293,6 +332,232 @@ __device__ __forceinline__ double mie_finish(double x, cplx m, int64_t n, const 
   }
   vs.close(n);
   return asum;
+}
+
+template <class Emit>
+__device__ __forceinline__ double mie_finish(double x, cplx m, int64_t n, const Scratch& s,
+                                             ValueSums& vs, Emit emit) {
+  NoLayers none;
+  return mie_finish(x, m, n, s, vs, emit, none);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Layered spheres (scatrs/src/layered/kernel.rs), values only.
+// ---------------------------------------------------------------------------------------------
+constexpr int kMaxLayers = 16;
+
+// num-complex's sin, cos, and complex::exp_m1 (scatrs/src/complex.rs:51-56).
+__device__ __forceinline__ cplx csin(cplx z) {
+  return {sin(z.re) * cosh(z.im), cos(z.re) * sinh(z.im)};
+}
+__device__ __forceinline__ cplx ccos(cplx z) {
+  return {cos(z.re) * cosh(z.im), -sin(z.re) * sinh(z.im)};
+}
+__device__ __forceinline__ cplx cexp_m1(cplx w) {
+  double sb, cb;
+  sincos(w.im, &sb, &cb);
+  double h = sin(w.im * 0.5);
+  return {expm1(w.re) * cb - h * h * 2.0, exp(w.re) * sb};
+}
+__device__ __forceinline__ cplx two_i(cplx z) { return {-(z.im * 2.0), z.re * 2.0}; }
+__device__ __forceinline__ double norm1(cplx z) { return fabs(z.re) + fabs(z.im); }
+
+// Pi_n(z) and w_{n+1}(z) of one argument (layered/kernel.rs:33-103).
+struct LArg {
+  cplx z, inv_z, pi, w, w_n;
+  __device__ __forceinline__ void init(cplx zz, bool chi) {
+    z = zz;
+    inv_z = cinv(z);
+    if (chi) {
+      cplx sz = csin(z), cz = ccos(z);
+      pi = sz * cz;
+      w = inv_z + sz * cinv(cz);
+    } else {
+      pi = -scl(cexp_m1(two_i(z)), 0.5);
+      w = inv_z - mk(0.0, 1.0);
+    }
+    w_n = rl(0.0);
+  }
+  __device__ __forceinline__ void step(int64_t n, cplx u_n) {
+    w_n = w;
+    pi = pi * u_n * w;
+    w = scl(inv_z, (double)(2 * n + 1)) - cinv(w);
+  }
+  __device__ __forceinline__ cplx d1(int64_t n, cplx u_next) const {
+    return scl(inv_z, (double)(n + 1)) - u_next;
+  }
+  __device__ __forceinline__ cplx d3(int64_t n) const {
+    return scl(inv_z, (double)(n + 1)) - w;
+  }
+};
+
+// Ratio arrays of one lane: array 0 is the outer layer's u_k(m x) (the sphere's u_z), then the
+// core's, then per layer l >= 1 those of m_l x_{l-1} and (but for the outermost) m_l x_l.
+struct LayerArrays {
+  double2* base;
+  int64_t astride;  // elements between arrays
+  int stride;       // lanes
+  __device__ __forceinline__ cplx get(int a, int64_t k) const {
+    double2 v = base[a * astride + k * stride];
+    return {v.x, v.y};
+  }
+  __device__ __forceinline__ void put(int a, int64_t k, cplx v) const {
+    base[a * astride + k * stride] = make_double2(v.re, v.im);
+  }
+};
+
+// ratios (kernel.rs:159-205): u_k(m x) for k = 1..n+1 into array a.
+__device__ __forceinline__ void ratios_into(cplx m, double x, int64_t n, const LayerArrays& L,
+                                            int a) {
+  cplx z = scl(m, x);
+  int64_t top = n + 1;
+  if (m.im == 0.0) {
+    double inv_rho = 1.0 / z.re, u = 0.0;
+    int64_t start = start_index(top, fabs(z.re));
+    for (int64_t k = start; k >= 1; --k) {
+      u = step_real(k, inv_rho, u);
+      if (k <= top) L.put(a, k, rl(u));
+    }
+  } else {
+    cplx inv_z = cinv(z), u = rl(0.0);
+    int64_t start = start_index(top, cabs_(z));
+    for (int64_t k = start; k >= 1; --k) {
+      u = step_complex(k, inv_z, u);
+      if (k <= top) L.put(a, k, u);
+    }
+  }
+}
+
+// side (layered/kernel.rs:158-183) for the values.
+__device__ __forceinline__ Side layer_side(cplx mi, cplx mo, Side prev, cplx h, cplx lead,
+                                           cplx u_prev, cplx u1, cplx d1i, cplx d3i, cplx d1o,
+                                           cplx d3o, cplx pio, cplx p, cplx w, cplx* h_out) {
+  cplx mh = mi * h;
+  cplx g1 = prev.direct ? mh - mo * d1i : lead - mi * u_prev + mo * u1 + mi * prev.v;
+  cplx g2 = mh - mo * d3i;
+  cplx inv_den = cinv(pio * g2 - p * g1);
+  cplx delta = -(w * p * g1 * inv_den * cinv(pio));
+  cplx hd = d1o + delta;
+  if (norm1(hd) * 4.0 >= fmax(norm1(d1o), norm1(delta))) {
+    *h_out = hd;
+    return {false, delta};
+  }
+  cplx hp = d3o - w * g2 * inv_den;
+  *h_out = hp;
+  return {true, hp};
+}
+
+// Kernel::solve's recursion (layered/kernel.rs:308-465) for `layers` layers of interface size
+// parameters x[0..layers) and indices m, its H_a, H_b produced one order at a time.
+struct Layered {
+  static constexpr bool kLayered = true;
+  int layers;
+  const double* x;
+  const cplx* m;
+  LayerArrays arr;
+  LArg inner[kMaxLayers - 1], outer[kMaxLayers - 1], core;
+  cplx p[kMaxLayers - 1], lead[kMaxLayers - 1];
+  bool chi[kMaxLayers - 1];
+
+  // Array index of the ratios of layer l's outer argument (l < layers - 1), of m_l x_{l-1}, and
+  // of the core.
+  __device__ __forceinline__ int a_outer(int l) const { return l == layers - 1 ? 0 : 2 * l + 1; }
+  __device__ __forceinline__ int a_inner(int l) const { return 2 * l; }
+  static constexpr int kCore = 1;
+
+  // The ratio arrays and the initial state; the outer argument's own ratios (array 0) come from
+  // mie_prepare.
+  __device__ void prepare(int64_t n) {
+    const int last = layers - 1;
+    ratios_into(m[0], x[0], n, arr, kCore);
+    for (int l = 1; l < layers; ++l) {
+      ratios_into(m[l], x[l - 1], n, arr, a_inner(l));
+      if (l < last) ratios_into(m[l], x[l], n, arr, a_outer(l));
+    }
+    for (int l = 1; l < layers; ++l) {
+      const bool c = m[l].im * x[l] < 0.5;
+      chi[l - 1] = c;
+      const cplx a = m[l], b = m[l - 1];
+      lead[l - 1] = (a - b) * (a + b) * cinv(a * b);
+      const cplx z1 = scl(m[l], x[l - 1]), z2 = scl(m[l], x[l]);
+      inner[l - 1].init(z1, c);
+      outer[l - 1].init(z2, c);
+      if (c) {
+        const cplx c2 = ccos(z2);
+        p[l - 1] = csin(z1) * cinv(ccos(z1)) * c2 * c2;
+      } else {
+        const double dx = x[l] - x[l - 1];
+        const double ea = -(m[l].im * dx * 2.0), eb = m[l].re * dx * 2.0;
+        double sb, cb;
+        sincos(eb, &sb, &cb);
+        const cplx e = scl(mk(cb, sb), exp(ea));
+        p[l - 1] = -scl(e * cexp_m1(two_i(z1)), 0.5);
+      }
+    }
+    core.init(scl(m[0], x[0]), false);
+  }
+
+  __device__ __forceinline__ void order(int64_t k, Side& sa, Side& sb) {
+    for (int l = 1; l < layers; ++l) {
+      LArg& ai = inner[l - 1];
+      LArg& ao = outer[l - 1];
+      const cplx u1k = arr.get(a_inner(l), k);
+      ai.step(k, u1k);
+      ao.step(k, arr.get(a_outer(l), k));
+      p[l - 1] = p[l - 1] * u1k * cinv(ai.w_n) * ao.w_n * ao.w_n;
+    }
+    cplx ha = core.d1(k, arr.get(kCore, k + 1));
+    cplx hb = ha;
+    Side a{false, rl(0.0)}, b{false, rl(0.0)};
+    for (int l = 1; l < layers; ++l) {
+      const LArg& ai = inner[l - 1];
+      const LArg& ao = outer[l - 1];
+      const cplx u_prev = arr.get(l == 1 ? kCore : a_outer(l - 1), k + 1);
+      const cplx u1 = arr.get(a_inner(l), k + 1);
+      const cplx u2 = arr.get(a_outer(l), k + 1);
+      const cplx d1i = ai.d1(k, u1), d3i = ai.d3(k);
+      const cplx d1o = ao.d1(k, u2), d3o = ao.d3(k);
+      const cplx w = chi[l - 1] ? rl(-1.0) : mk(0.0, 1.0);
+      const cplx ld = scl(lead[l - 1], (double)(k + 1) / x[l - 1]);
+      cplx na, nb;
+      const Side a2 = layer_side(m[l], m[l - 1], a, ha, ld, u_prev, u1, d1i, d3i, d1o, d3o,
+                                 ao.pi, p[l - 1], w, &na);
+      const Side b2 = layer_side(m[l - 1], m[l], b, hb, rl(0.0), u_prev, u1, d1i, d3i, d1o, d3o,
+                                 ao.pi, p[l - 1], w, &nb);
+      ha = na;
+      hb = nb;
+      a = a2;
+      b = b2;
+    }
+    sa = a;
+    sb = b;
+  }
+};
+
+// Layered::check_inputs (layered/mod.rs:233-305) with the default truncation: 0 when accepted,
+// else the status (1 invalid input, 3 outside the validated domain, layered/domain.rs:76-92).
+__device__ __forceinline__ int check_layered(const double* x, const cplx* m, int layers,
+                                             int64_t n, bool allow_unvalidated) {
+  for (int l = 0; l < layers; ++l)
+    if (!isfinite(x[l]) || (l > 0 && x[l] < x[l - 1])) return 1;
+  const double outer = x[layers - 1];
+  if (x[0] < 1e-30 || outer > 1e6) return 1;
+  for (int l = 0; l < layers; ++l) {
+    if (!(isfinite(m[l].re) && isfinite(m[l].im)) || m[l].re < 0.0 || m[l].im < 0.0) return 1;
+    const double a = hypot(m[l].re, m[l].im);
+    if (!(a >= 1e-6 && a <= 1e3)) return 1;
+  }
+  if (n == 0 || n > (1 << 20)) return 1;
+  if (!allow_unvalidated) {
+    if (layers > 16 || !(outer >= 1e-6 && outer <= 1e4)) return 3;
+    for (int l = 0; l < layers; ++l) {
+      const double a = hypot(m[l].re, m[l].im);
+      if (!(a * outer <= 3e4 && m[l].re > 0.0 && m[l].re <= 10.0 && m[l].im >= 0.0 &&
+            m[l].im <= 10.0 && a >= 0.1))
+        return 3;
+    }
+  }
+  return 0;
 }
 
 }  // namespace sb

@@ -43,7 +43,8 @@ __global__ void plan_chunks_kernel(PlanArgs a) {
   if (lane == 0) a.chunk_n[warp] = nn;
 }
 
-__global__ void __launch_bounds__(128) mie_fixed_kernel(MieFixedArgs a) {
+template <bool kLayered>
+__device__ __forceinline__ void mie_chunk(const MieFixedArgs& a) {
   int wslot = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   int lane = threadIdx.x & 31;
   if (wslot >= a.n_chunks) return;
@@ -55,36 +56,72 @@ __global__ void __launch_bounds__(128) mie_fixed_kernel(MieFixedArgs a) {
   int nc = a.chunk_n[chunk];
   int64_t row0 = a.chunk_row[chunk];
   double* X = a.X + row0 * 128 + lane * 4;
+  // Scratch: 2L - 1 complex ratio arrays (one for a sphere) of nc + 2 rows, and u_k(x).
+  const int n_arr = kLayered ? 2 * a.n_layers - 1 : 1;
   Scratch s;
-  s.uz = a.uz + (row0 + 2 * (int64_t)chunk) * 32 + lane;
+  s.uz = a.uz + (row0 + 2 * (int64_t)chunk) * n_arr * 32 + lane;
   s.ux = a.ux + (row0 + 2 * (int64_t)chunk) * 32 + lane;
   s.stride = 32;
   double q[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   int64_t n = 0;
   if (j < a.n_nodes) {
-    double r = a.radius[d * a.n_nodes + j];
-    double w = a.weight[d * a.n_nodes + j];
-    double x = 2.0 * kPi * r / a.wl[i];
-    double2 mv = a.m[unit];
-    cplx m = mk(mv.x, mv.y);
+    const double r = a.radius[d * a.n_nodes + j];
+    const double w = a.weight[d * a.n_nodes + j];
+    const double x = 2.0 * kPi * r / a.wl[i];
     n = default_n_max(x);
-    int st = check_node(x, m, n, a.allow_unvalidated != 0);
+    auto emit = [&](int64_t k, cplx an, cplx bn) {
+      const bool odd = (k & 1) != 0;
+      const cplx u = odd ? an : bn, v = odd ? bn : an;
+      *reinterpret_cast<double4*>(X + (k - 1) * 128) = make_double4(u.re, u.im, v.re, v.im);
+    };
+    ValueSums vs;
+    double asum = 0.0;
+    int st;
+    if (!kLayered) {
+      const double2 mv = a.m[unit];
+      const cplx m = mk(mv.x, mv.y);
+      st = check_node(x, m, n, a.allow_unvalidated != 0);
+      if (st == 0 && n <= nc) {
+        mie_prepare(x, m, n, s);
+        asum = mie_finish(x, m, n, s, vs, emit);
+      }
+    } else {
+      // A layered sphere: x_l = f_l x, the outer surface's x last (ensemble/particle.rs:186-195).
+      const int L = a.n_layers;
+      double xs[kMaxLayers];
+      cplx ms[kMaxLayers];
+      bool lossless = true;
+      for (int l = 0; l < L; ++l) {
+        xs[l] = l < L - 1 ? a.fractions[d * (L - 1) + l] * x : x;
+        const double2 mv = a.m_layers[(d * L + l) * a.n_wl + i];
+        ms[l] = mk(mv.x, mv.y);
+        lossless = lossless && mv.y == 0.0;
+      }
+      st = check_layered(xs, ms, L, n, a.allow_unvalidated != 0);
+      if (st == 0 && n <= nc) {
+        mie_prepare(x, ms[L - 1], n, s);
+        Layered lay;
+        lay.layers = L;
+        lay.x = xs;
+        lay.m = ms;
+        lay.arr.base = s.uz;
+        lay.arr.astride = (int64_t)(nc + 2) * 32;
+        lay.arr.stride = 32;
+        lay.prepare(n);
+        asum = mie_finish(x, ms[L - 1], n, s, vs, emit, lay);
+        // A lossless particle absorbs nothing (layered/kernel.rs:455-464).
+        if (lossless) asum = 0.0;
+      }
+    }
     if (st != 0 || n > nc) {
       record_error(a.err, i, d, j, a.n_dist, a.n_nodes, st != 0 ? st : 1);
       n = 0;
     } else {
-      mie_prepare(x, m, n, s);
-      ValueSums vs;
-      double asum = mie_finish(x, m, n, s, vs, [&](int64_t k, cplx an, cplx bn) {
-        bool odd = (k & 1) != 0;
-        cplx u = odd ? an : bn, v = odd ? bn : an;
-        *reinterpret_cast<double4*>(X + (k - 1) * 128) = make_double4(u.re, u.im, v.re, v.im);
-      });
-      Eff e = efficiencies_from(x, asum, vs);
+      const Eff e = efficiencies_from(x, asum, vs);
       // The per-particle quantities of pass 2 (engine.rs:1047-1057), weighted.
-      double area = kPi * r * r;
-      double qv[8] = {1.0,           area * e.q_ext, area * e.q_sca, area * e.q_sca * e.g,
-                      area * e.q_abs, area * e.q_back, r * r,         r * r * r};
+      const double area = kPi * r * r;
+      const double qv[8] = {1.0,           area * e.q_ext, area * e.q_sca, area * e.q_sca * e.g,
+                            area * e.q_abs, area * e.q_back, r * r,         r * r * r};
       for (int k = 0; k < 8; ++k) q[k] = w * qv[k];
     }
   }
@@ -98,6 +135,12 @@ __global__ void __launch_bounds__(128) mie_fixed_kernel(MieFixedArgs a) {
     if (lane == 0) a.chunk_sums[(int64_t)chunk * 8 + k] = v;
   }
 }
+
+// Homogeneous spheres.
+__global__ void __launch_bounds__(128) mie_fixed_kernel(MieFixedArgs a) { mie_chunk<false>(a); }
+
+// Layered spheres (their per-layer state lives in local memory).
+__global__ void __launch_bounds__(128) mie_layered_kernel(MieFixedArgs a) { mie_chunk<true>(a); }
 
 // Independent spheres, one per thread (the batched Mie::compute): coefficients a_1..a_N then
 // b_1..b_N per sphere, and the efficiencies.
@@ -146,7 +189,10 @@ void launch_plan_chunks(const PlanArgs& a, cudaStream_t s) {
 void launch_mie_fixed(const MieFixedArgs& a, cudaStream_t s) {
   int threads = 128;
   int blocks = (a.n_chunks * 32 + threads - 1) / threads;
-  mie_fixed_kernel<<<blocks, threads, 0, s>>>(a);
+  if (a.n_layers > 1)
+    mie_layered_kernel<<<blocks, threads, 0, s>>>(a);
+  else
+    mie_fixed_kernel<<<blocks, threads, 0, s>>>(a);
 }
 
 void launch_mie_nodes(const MieNodesArgs& a, cudaStream_t s) {

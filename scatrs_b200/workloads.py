@@ -20,6 +20,22 @@ from ._native import DIST_DTYPE, KINDS
 
 
 @dataclass
+class LayeredWorkload:
+    name: str
+    dists: np.ndarray
+    wavelengths: np.ndarray
+    fractions: np.ndarray  # (n_dist, L - 1)
+    m_layers: np.ndarray   # complex (n_dist, L, n_wl)
+    mu: np.ndarray
+    n_nodes: int
+    greek_order: int
+
+    @property
+    def n_units(self) -> int:
+        return self.dists.size * self.wavelengths.size
+
+
+@dataclass
 class Workload:
     name: str
     dists: np.ndarray       # DIST_DTYPE, (n_dist,)
@@ -82,3 +98,27 @@ def config2(seed: int = 0, scale: float = 1.0, mu: np.ndarray | None = None) -> 
     mu = gauss_legendre(360) if mu is None else mu
     return Workload(f"config2(seed={seed},scale={scale})", lognormals(med, wid, 4), wl, m, mu,
                     512, 64)
+
+
+def config4(seed: int = 0, scale: float = 1.0, mu: np.ndarray | None = None) -> LayeredWorkload:
+    """Three-layer spheres (a core and two shells): core fraction uniform 0.3-0.9, inner shell
+    boundary uniform 0.9-0.99; each layer's index Re uniform 1.3-2.0, Im log-uniform 1e-6-0.5
+    (per distribution and layer, the same at every wavelength); lognormal median uniform
+    0.05-1, width uniform 1.3-2.0; 256 distributions x 128 wavelengths log-spaced over 0.3-1.6;
+    256 Gauss nodes in ln r over median width^(+-4); Greek order 32."""
+    rng = np.random.default_rng(seed)
+    n_dist, n_wl = 256, 128
+    wl = np.geomspace(0.3, 1.6, n_wl)
+    med = rng.uniform(0.05, 1.0, n_dist)
+    wid = rng.uniform(1.3, 2.0, n_dist)
+    f = np.stack([rng.uniform(0.3, 0.9, n_dist), rng.uniform(0.9, 0.99, n_dist)], axis=1)
+    m_re = rng.uniform(1.3, 2.0, (n_dist, 3))
+    m_im = np.exp(rng.uniform(np.log(1e-6), np.log(0.5), (n_dist, 3)))
+    ml = np.repeat((m_re + 1j * m_im)[:, :, None], n_wl, axis=2)
+    if scale < 1.0:
+        kd = max(1, int(round(n_dist * scale)))
+        kw = max(1, int(round(n_wl * scale)))
+        med, wid, f, ml, wl = med[:kd], wid[:kd], f[:kd], ml[:kd, :, :kw], wl[:kw]
+    mu = gauss_legendre(180) if mu is None else mu
+    return LayeredWorkload(f"config4(seed={seed},scale={scale})", lognormals(med, wid, 4), wl, f,
+                           ml, mu, 256, 32)

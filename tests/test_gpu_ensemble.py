@@ -129,3 +129,30 @@ def test_deterministic_and_empty(gpu):
         assert np.array_equal(x, y)
     v, p, g = gpu.ensemble_fixed(w.dists[:0], w.wavelengths, w.m[:0], w.mu, w.n_nodes, 16)
     assert v.shape == (11, 0) and p.shape == (6, 0, w.mu.size) and g.shape == (6, 0, 17)
+
+
+def _oracle_layered(w, **kw):
+    d = np.zeros(w.dists.size, dtype=O.DIST_DTYPE)
+    d["kind"], d["p"] = w.dists["kind"], w.dists["param"]
+    d["r_lo"], d["r_hi"] = w.dists["r_lo"], w.dists["r_hi"]
+    return O.ensemble_fixed_layered(d, w.wavelengths, w.fractions, w.m_layers, w.n_nodes, w.mu,
+                                    w.greek_order, **kw)
+
+
+def test_layered_matches_oracle(gpu):
+    w = W.config4(seed=2, scale=0.03)  # 8 distributions x 4 wavelengths of three-layer spheres
+    got = gpu.ensemble_fixed_layered(w.dists, w.wavelengths, w.fractions, w.m_layers, w.mu,
+                                     w.n_nodes, w.greek_order)
+    _compare(got, _oracle_layered(w), tol=1e-11)
+
+
+def test_layered_with_equal_indices_is_the_sphere(gpu):
+    """One index in every layer: the sphere's results bit for bit (tests/ensemble_layered.rs:
+    62-116 of the reference)."""
+    w = W.config1()
+    ml = np.repeat(w.m[:, None, :], 3, axis=1)
+    fr = np.array([[0.4, 0.8]])
+    got = gpu.ensemble_fixed_layered(w.dists, w.wavelengths, fr, ml, w.mu, w.n_nodes, 16)
+    ref = gpu.ensemble_fixed(w.dists, w.wavelengths, w.m, w.mu, w.n_nodes, 16)
+    for a, b in zip(got, ref):
+        assert np.array_equal(a, b)

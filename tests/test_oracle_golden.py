@@ -144,3 +144,67 @@ def test_phase_matrix_matches_arb():
             ref = np.array([val(r[name], j) for j in range(mu.size)])
             assert np.all(np.abs(got - ref) / scale <= 32.0 * kappa(x, m) * EPS * 16), \
                 (r["case"], name)
+
+
+def kappa_layered(x_outer, ms):
+    """layered condition_factor (layered/domain.rs:95-110): the largest index and the largest
+    near-unity factor of any layer whose index is not exactly 1."""
+    big = max([1.0] + [abs(m) for m in ms])
+    near = max([1.0] + [abs(m) / abs(m - 1) for m in ms if m != 1])
+    return (1.0 + big * x_outer) * near
+
+
+def test_layered_within_declared_tolerance():
+    for r in load("layered_coefficients"):
+        x = np.array(r["x"])
+        ms = np.array(r["m_re"]) + 1j * np.array(r["m_im"])
+        s = O.layered(x, ms)
+        orders = np.array(r["orders"])
+        if orders.max() > s["n"]:
+            continue
+        tol = 16.0 * kappa_layered(x[-1], ms) * EPS * 4  # cond not tabulated: slack 4
+        for stem in "ab":
+            ref = np.array([complex(val(r[stem + "_re"], i), val(r[stem + "_im"], i))
+                            for i in range(orders.size)])
+            scale = np.abs(ref).max()
+            if scale == 0.0:
+                continue
+            assert np.abs(s[stem][orders - 1] - ref).max() / scale <= tol, (r["case"], stem)
+    for r in load("layered_series"):
+        x = np.array(r["x"])
+        ms = np.array(r["m_re"]) + 1j * np.array(r["m_im"])
+        s = O.layered(x, ms)
+        names = ("q_ext", "q_sca", "q_abs", "q_back", "g")
+        q = np.array([s[k] for k in names])
+        # cond by central differences in every layer's x, Re m and Im m (relative step 1e-6)
+        cond_num = np.zeros(5)
+        h = 1e-6
+        for l in range(x.size):
+            for kind in ("x", "re", "im"):
+                if kind == "x" and l > 0 and x[l] == x[l - 1]:
+                    continue
+                xp, xm, mp, mm = x.copy(), x.copy(), ms.copy(), ms.copy()
+                if kind == "x":
+                    xp[l] *= 1 + h
+                    xm[l] *= 1 - h
+                    if (l + 1 < x.size and xp[l] > x[l + 1]) or (l > 0 and xm[l] < x[l - 1]):
+                        continue
+                elif kind == "re":
+                    mp[l] += h * ms[l].real
+                    mm[l] -= h * ms[l].real
+                else:
+                    if ms[l].imag == 0.0:
+                        continue
+                    mp[l] += 1j * h * ms[l].imag
+                    mm[l] -= 1j * h * ms[l].imag
+                sp, sm = O.layered(xp, mp), O.layered(xm, mm)
+                cond_num += np.abs(np.array([sp[k] - sm[k] for k in names])) / (2 * h)
+        for i, k in enumerate(names):
+            ref = val(r[k], 0)
+            if ref == 0.0:
+                continue
+            scale = max(abs(ref), s["q_sca"]) if k == "q_back" else abs(ref)
+            if k == "q_abs":
+                scale = max(abs(ref), 1e-3 * s["q_ext"])
+            tol = 16.0 * (kappa_layered(x[-1], ms) + cond_num[i] / scale) * EPS * 4
+            assert abs(q[i] - ref) / scale <= tol, (r["case"], k, q[i], ref)
