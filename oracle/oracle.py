@@ -229,3 +229,42 @@ def ensemble_fixed_layered(dists: np.ndarray, wavelengths, fractions, m_layers, 
     if greek is not None:
         out["greek"] = greek
     return out
+
+
+def ensemble_fixed_d(dists: np.ndarray, wavelengths, m, n_nodes: int, mu=None,
+                     greek_order: int | None = None, normalized: bool = True,
+                     allow_unvalidated: bool = False, threads: int = 0) -> dict:
+    """ensemble_fixed with the derivatives of every output along the distribution's parameters
+    and then Re m and Im m (P directions, every distribution of one kind): d_values (P, 11, n),
+    d_phase (P, 6, n, n_mu), d_greek (P, 6, n, L + 1)."""
+    dists = np.ascontiguousarray(dists, dtype=DIST_DTYPE)
+    wl = np.ascontiguousarray(wavelengths, dtype=np.float64).reshape(-1)
+    m = np.ascontiguousarray(np.broadcast_to(np.asarray(m, dtype=np.complex128),
+                                             (dists.size, wl.size)))
+    mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
+    kinds = set(int(k) for k in dists["kind"])
+    P = 2 + ({3: 3, 4: 1}.get(kinds.pop(), 2) if len(kinds) == 1 else 2)
+    n_units = dists.size * wl.size
+    L = -1 if greek_order is None else int(greek_order)
+    values = np.zeros((11, n_units))
+    d_values = np.zeros((P, 11, n_units))
+    phase = np.zeros((6, n_units, mu.size)) if mu.size else None
+    d_phase = np.zeros((P, 6, n_units, mu.size)) if mu.size else None
+    greek = np.zeros((6, n_units, L + 1)) if L >= 0 else None
+    d_greek = np.zeros((P, 6, n_units, L + 1)) if L >= 0 else None
+    err = ctypes.create_string_buffer(512)
+    f = lib().orc_ensemble_fixed_d
+    f.argtypes = [ctypes.c_void_p, _I64, _PD, _I64, _PD, _I64, _PD, _I64, _I64, ctypes.c_int,
+                  ctypes.c_int, ctypes.c_int, _PD, _PD, _PD, _PD, _PD, _PD, ctypes.c_char_p,
+                  _I64]
+    st = f(dists.ctypes.data, dists.size, _p(wl), wl.size, _p(m.view(np.float64).reshape(-1)),
+           n_nodes, _p(mu), mu.size, L, int(normalized), int(allow_unvalidated), threads,
+           _p(values), _p(phase), _p(greek), _p(d_values), _p(d_phase), _p(d_greek), err, 512)
+    if st != 0:
+        raise OracleError(st, err.value.decode())
+    out = {"values": values, "d_values": d_values}
+    if phase is not None:
+        out["phase"], out["d_phase"] = phase, d_phase
+    if greek is not None:
+        out["greek"], out["d_greek"] = greek, d_greek
+    return out

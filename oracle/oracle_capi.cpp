@@ -255,7 +255,9 @@ static int ensemble_impl(const FixedDist* dists, int64_t n_dist, const double* w
                          const double* m_layers, int64_t n_nodes, const double* mu,
                          int64_t n_mu, int64_t greek_order, int normalized,
                          int allow_unvalidated, int n_threads, double* values, double* phase,
-                         double* greek, char* err, int64_t err_len);
+                         double* greek, char* err, int64_t err_len, int derivs = 0,
+                         double* d_values = nullptr, double* d_phase = nullptr,
+                         double* d_greek = nullptr);
 
 int orc_ensemble_fixed(const FixedDist* dists, int64_t n_dist, const double* wl, int64_t n_wl,
                        const double* m, int64_t n_nodes, const double* mu, int64_t n_mu,
@@ -280,17 +282,64 @@ int orc_ensemble_fixed_layered(const FixedDist* dists, int64_t n_dist, const dou
                        phase, greek, err, err_len);
 }
 
+// A value with derivatives along P parameters (ensemble/lin.rs:7-68, errors dropped: the fixed
+// grid has no error estimates).
+struct LinV {
+  double v;
+  std::vector<double> d;
+};
+static LinV lin_div(const LinV& a, const LinV& b) {
+  LinV o{a.v / b.v, std::vector<double>(a.d.size())};
+  for (size_t k = 0; k < a.d.size(); ++k) o.d[k] = (a.d[k] - o.v * b.d[k]) / b.v;
+  return o;
+}
+static LinV lin_scale(const LinV& a, double c) {
+  LinV o{c * a.v, std::vector<double>(a.d.size())};
+  for (size_t k = 0; k < a.d.size(); ++k) o.d[k] = c * a.d[k];
+  return o;
+}
+
+// element_derivatives (mie/phase.rs:62-73).
+static void element_derivs(cplx s1, cplx s2, cplx d1, cplx d2, double out[4]) {
+  double r1 = (conj(s1) * d1).re;
+  double r2 = (conj(s2) * d2).re;
+  cplx p = d2 * conj(s1) + s2 * conj(d1);
+  out[0] = r1 + r2;
+  out[1] = r2 - r1;
+  out[2] = p.re;
+  out[3] = p.im;
+}
+
+static int theta_count(int kind) { return kind == MODIFIED_GAMMA ? 3 : kind == POWER_LAW ? 1 : 2; }
+
 static int ensemble_impl(const FixedDist* dists, int64_t n_dist, const double* wl, int64_t n_wl,
                          const double* m, int n_layers, const double* fractions,
                          const double* m_layers, int64_t n_nodes, const double* mu,
                          int64_t n_mu, int64_t greek_order, int normalized,
                          int allow_unvalidated, int n_threads, double* values, double* phase,
-                         double* greek, char* err, int64_t err_len) {
+                         double* greek, char* err, int64_t err_len, int derivs,
+                         double* d_values, double* d_phase, double* d_greek) {
   const int64_t n_units = n_dist * n_wl;
   std::vector<double> xi(n_nodes), om(n_nodes);
   gauss_legendre(n_nodes, xi.data(), om.data());
-  // Node radii and weights per distribution.
+  int P_th = 0;
+  if (derivs) {
+    if (n_layers > 1) {
+      if (err && err_len > 0) snprintf(err, err_len, "derivatives of layered spheres: not here");
+      return INVALID_INPUT;
+    }
+    P_th = n_dist > 0 ? theta_count(dists[0].kind) : 0;
+    for (int64_t d = 1; d < n_dist; ++d)
+      if (theta_count(dists[d].kind) != P_th) {
+        if (err && err_len > 0) snprintf(err, err_len, "derivatives need one distribution kind");
+        return INVALID_INPUT;
+      }
+  }
+  const int P = derivs ? P_th + 2 : 0;  // theta parameters, then Re m and Im m
+  const int B = 1 + P;                  // blocks: values, then one per parameter
+  // Node radii and weights per distribution: w u r, and w (du/dtheta) r.
   std::vector<double> radius(n_dist * n_nodes), weight(n_dist * n_nodes);
+  std::vector<double> wth(n_dist * n_nodes * 3, 0.0);
   for (int64_t d = 0; d < n_dist; ++d) {
     Density den = prepare(dists[d].kind, dists[d].p[0], dists[d].p[1], dists[d].p[2]);
     double a = std::log(dists[d].r_lo), b = std::log(dists[d].r_hi);
@@ -299,12 +348,13 @@ static int ensemble_impl(const FixedDist* dists, int64_t n_dist, const double* w
       double t = c + h * xi[j];
       double w = h * om[j];
       double r = std::exp(t);
-      double u = density_eval(den, r, nullptr);
+      double grad[3];
+      double u = density_eval(den, r, grad);
       radius[d * n_nodes + j] = r;
       weight[d * n_nodes + j] = w * (u * r);
+      for (int p = 0; p < 3; ++p) wth[(d * n_nodes + j) * 3 + p] = w * (grad[p] * r);
     }
   }
-  // Bands: every band up to the largest number of terms.
   bool want_greek = greek_order >= 0;
   int64_t n_max_all = 0;
   for (int64_t d = 0; d < n_dist; ++d)
@@ -341,14 +391,14 @@ static int ensemble_impl(const FixedDist* dists, int64_t n_dist, const double* w
       const double* p = m_layers + 2 * ((d * n_layers + l) * n_wl + i);
       mls[l] = C(p[0], p[1]);
     }
-    std::vector<double> S(9, 0.0), Smu(4 * n_mu, 0.0);
+    // Sums per block: 8 per-particle quantities, the cosine tables, each band's tables.
+    std::vector<double> S(B * 8, 0.0), Smu(B * 4 * n_mu, 0.0);
     std::vector<std::vector<double>> Sband(bands.size());
     MieState st;
     std::string msg;
     int status = OK;
     for (int64_t c0 = 0; c0 < n_nodes && status == OK; c0 += NODES_PER_CHUNK) {
       int64_t c1 = std::min(n_nodes, c0 + NODES_PER_CHUNK);
-      // The chunk's band: its largest number of terms.
       int64_t n_chunk = 0;
       for (int64_t j = c0; j < c1; ++j) {
         double x = 2.0 * PI * radius[d * n_nodes + j] / lambda;
@@ -358,6 +408,10 @@ static int ensemble_impl(const FixedDist* dists, int64_t n_dist, const double* w
       for (int64_t j = c0; j < c1; ++j) {
         double r = radius[d * n_nodes + j];
         double W = weight[d * n_nodes + j];
+        double Wb[8];  // the weight of each block
+        Wb[0] = W;
+        for (int p = 0; p < P_th; ++p) Wb[1 + p] = wth[(d * n_nodes + j) * 3 + p];
+        for (int k = 0; k < 2 && derivs; ++k) Wb[1 + P_th + k] = W;
         double x = 2.0 * PI * r / lambda;
         int64_t n = 0;
         if (n_layers <= 1) {
@@ -379,34 +433,96 @@ static int ensemble_impl(const FixedDist* dists, int64_t n_dist, const double* w
           msg = buf + msg;
           break;
         }
-        if (n_layers <= 1) st.solve(x, mv, n, false);
+        if (n_layers <= 1) st.solve(x, mv, n, derivs != 0);
         Efficiencies q = efficiencies(st);
         double area = PI * r * r;
-        double qv[9] = {1.0,          area * q.q_ext, area * q.q_sca, area * q.q_sca * q.g,
-                        area * q.q_abs, area * q.q_back, r * r,       r * r * r,
-                        0.0};
-        for (int k = 0; k < 9; ++k) S[k] += W * qv[k];
+        // Per-block per-particle quantities (engine.rs:1047-1085).
+        double qb[8][8] = {};
+        {
+          double qv[8] = {1.0,            area * q.q_ext, area * q.q_sca, area * q.q_sca * q.g,
+                          area * q.q_abs, area * q.q_back, r * r,       r * r * r};
+          for (int b = 0; b < 1 + P_th; ++b)
+            for (int k = 0; k < 8; ++k) qb[b][k] = qv[k];
+        }
+        if (derivs) {
+          // derivative_sums (efficiencies.rs:89-146) along Re m and Im m, and
+          // efficiencies_jacobian (192-230) for those directions.
+          Sums vs = value_sums(st.a.data(), st.b.data(), n);
+          for (int p = 0; p < 2; ++p) {
+            double sca = 0.0, g = 0.0;
+            cplx back = real(0.0);
+            auto dA = [&](int64_t i2) { return p == 0 ? st.da_dm[i2] : times_i(st.da_dm[i2]); };
+            auto dB = [&](int64_t i2) { return p == 0 ? st.db_dm[i2] : times_i(st.db_dm[i2]); };
+            for (int64_t k = 1; k <= n; ++k) {
+              cplx ak = st.a[k - 1], bk = st.b[k - 1], dak = dA(k - 1), dbk = dB(k - 1);
+              double w = (double)(2 * k + 1), kf = (double)k;
+              double pair = kf * (kf + 2.0) / (kf + 1.0);
+              double own = w / (kf * (kf + 1.0));
+              sca += w * 2.0 * (re_mul_conj(dak, ak) + re_mul_conj(dbk, bk));
+              cplx t = scale(dak - dbk, w);
+              back = (k % 2 == 0) ? back + t : back - t;
+              if (k < n) {
+                cplx a1 = st.a[k], b1 = st.b[k], da1 = dA(k), db1 = dB(k);
+                g += pair * (re_mul_conj(dak, a1) + re_mul_conj(ak, da1) + re_mul_conj(dbk, b1) +
+                             re_mul_conj(bk, db1));
+              }
+              g += own * (re_mul_conj(dak, bk) + re_mul_conj(ak, dbk));
+            }
+            double inv_x = 1.0 / x, inv_x2 = inv_x * inv_x, two_x2 = 2.0 * inv_x2;
+            double dsca = two_x2 * sca;
+            double dabs = two_x2 * st.abs_sum_jacobian[1 + p];
+            double dback = 2.0 * re_mul_conj(back, vs.back) * inv_x2;
+            double dg = vs.sca == 0.0 ? 0.0 : (2.0 * g - q.g * sca) / vs.sca;
+            double dext = dsca + dabs;
+            double qd[8] = {0.0,          area * dext, area * dsca, area * (dsca * q.g + q.q_sca * dg),
+                            area * dabs, area * dback, 0.0,        0.0};
+            for (int k = 0; k < 8; ++k) qb[1 + P_th + p][k] = qd[k];
+          }
+        }
+        for (int b = 0; b < B; ++b)
+          for (int k = 0; k < 8; ++k) S[b * 8 + k] += Wb[b] * qb[b][k];
+        // The requested cosines: phase_matrix(_with_derivatives) at each cosine
+        // (phase.rs:204-219, 289-341; amplitudes.rs:347-381), times the area.
         double cph = 4.0 / (x * x);
-        for (int64_t k = 0; k < n_mu; ++k) {
-          cplx s1, s2;
-          amplitudes(st.a.data(), st.b.data(), n, mu[k], &s1, &s2);
+        for (int64_t kk = 0; kk < n_mu; ++kk) {
+          cplx s1 = real(0.0), s2 = real(0.0), d1 = real(0.0), d2 = real(0.0);
+          for_each_order(mu[kk], n, [&](int64_t k, double pi, double tau) {
+            cplx an = st.a[k - 1], bn = st.b[k - 1];
+            s1 = s1 + scale(an, pi) + scale(bn, tau);
+            s2 = s2 + scale(an, tau) + scale(bn, pi);
+            if (derivs) {
+              cplx da = st.da_dm[k - 1], db = st.db_dm[k - 1];
+              d1 = d1 + scale(da, pi) + scale(db, tau);
+              d2 = d2 + scale(da, tau) + scale(db, pi);
+            }
+          });
           double e[4];
           elements(s1, s2, e);
-          for (int t = 0; t < 4; ++t) Smu[t * n_mu + k] += W * (cph * e[t] * area);
+          for (int b = 0; b < 1 + P_th; ++b)
+            for (int t = 0; t < 4; ++t) Smu[(b * 4 + t) * n_mu + kk] += Wb[b] * (cph * e[t] * area);
+          if (derivs) {
+            double fr[4], fi[4];
+            element_derivs(s1, s2, d1, d2, fr);
+            element_derivs(s1, s2, times_i(d1), times_i(d2), fi);
+            for (int t = 0; t < 4; ++t) {
+              Smu[((1 + P_th) * 4 + t) * n_mu + kk] += W * (area * (cph * fr[t] + 0.0 * e[t]));
+              Smu[((2 + P_th) * 4 + t) * n_mu + kk] += W * (area * (cph * fi[t] + 0.0 * e[t]));
+            }
+          }
         }
         if (bi >= 0) {
-          BandData& B = bands[bi];
+          BandData& Bd = bands[bi];
           std::vector<double>& sb = Sband[bi];
-          if (sb.empty()) sb.assign(4 * B.n_q, 0.0);
-          int64_t q = B.n_q, lo = q / 2, h = q - lo;
-          int64_t terms = std::min(n_chunk, B.upper);
+          if (sb.empty()) sb.assign(B * 4 * Bd.n_q, 0.0);
+          int64_t qn = Bd.n_q, lo = qn / 2, h = qn - lo;
+          int64_t terms = std::min(n_chunk, Bd.upper);
           double scl = 4.0 / (x * x) * (PI * r * r);
           for (int64_t ii = 0; ii < h; ++ii) {
-            // ce = G_E X and co = G_O X for this sphere's 4 columns (fast.rs:141-145), X
-            // zero beyond the sphere's own terms.
-            double ce[4] = {0, 0, 0, 0}, co[4] = {0, 0, 0, 0};
+            // ce = G_E X and co = G_O X over the sphere's 4 columns and, with derivatives, its
+            // 4 derivative columns (fast.rs:98-145).
+            double ce[8] = {0}, co[8] = {0};
             for (int64_t k = 0; k < terms; ++k) {
-              double xr[4] = {0, 0, 0, 0};
+              double xr[8] = {0};
               if (k < n) {
                 cplx uu = (k % 2 == 0) ? st.a[k] : st.b[k];
                 cplx vv = (k % 2 == 0) ? st.b[k] : st.a[k];
@@ -414,91 +530,157 @@ static int ensemble_impl(const FixedDist* dists, int64_t n_dist, const double* w
                 xr[1] = uu.im;
                 xr[2] = vv.re;
                 xr[3] = vv.im;
+                if (derivs) {
+                  cplx du = (k % 2 == 0) ? st.da_dm[k] : st.db_dm[k];
+                  cplx dv = (k % 2 == 0) ? st.db_dm[k] : st.da_dm[k];
+                  xr[4] = du.re;
+                  xr[5] = du.im;
+                  xr[6] = dv.re;
+                  xr[7] = dv.im;
+                }
               }
-              double ge = B.ge[ii * B.upper + k], go = B.go[ii * B.upper + k];
-              for (int t = 0; t < 4; ++t) {
+              double ge = Bd.ge[ii * Bd.upper + k], go = Bd.go[ii * Bd.upper + k];
+              for (int t = 0; t < 8; ++t) {
                 ce[t] += ge * xr[t];
                 co[t] += go * xr[t];
               }
             }
             cplx eu = C(ce[0], ce[1]), ev = C(ce[2], ce[3]);
             cplx ou = C(co[0], co[1]), ov = C(co[2], co[3]);
+            cplx deu = C(ce[4], ce[5]), dev = C(ce[6], ce[7]);
+            cplx dou = C(co[4], co[5]), dov = C(co[6], co[7]);
             int64_t jn = lo + ii;
             auto write = [&](int64_t node, double sign) {
               cplx s1 = eu + scale(ov, sign), s2 = ev + scale(ou, sign);
               double e[4];
               elements(s1, s2, e);
-              for (int t = 0; t < 4; ++t) sb[t * q + node] += W * (scl * e[t]);
+              for (int b = 0; b < 1 + P_th; ++b)
+                for (int t = 0; t < 4; ++t) sb[(b * 4 + t) * qn + node] += Wb[b] * (scl * e[t]);
+              if (derivs) {
+                cplx d1 = deu + scale(dov, sign), d2 = dev + scale(dou, sign);
+                double fr[4], fi[4];
+                element_derivs(s1, s2, d1, d2, fr);
+                element_derivs(s1, s2, times_i(d1), times_i(d2), fi);
+                for (int t = 0; t < 4; ++t) {
+                  sb[((1 + P_th) * 4 + t) * qn + node] += W * (scl * fr[t]);
+                  sb[((2 + P_th) * 4 + t) * qn + node] += W * (scl * fi[t]);
+                }
+              }
             };
             write(jn, 1.0);
-            int64_t mirror = q - 1 - jn;
+            int64_t mirror = qn - 1 - jn;
             if (mirror != jn) write(mirror, -1.0);
           }
         }
       }
     }
-    double* vrow = values;  // (11, n_units)
     if (status == OK) {
-      double z = S[0];
-      double v[9];
-      for (int k = 0; k < 9; ++k) v[k] = S[k] / z;
-      double ext = v[1], sca = v[2], scag = v[3], ab = v[4], back = v[5], r2 = v[6], r3 = v[7];
+      // averages (engine.rs:1782-1836): v = S/Z; theta: (S_t - v dZ)/Z; m: S_m/Z.
+      const double z = S[0];
+      auto average = [&](std::vector<double>& blk, int64_t len) {
+        for (int64_t k = 0; k < len; ++k) blk[k] = blk[k] / z;
+        for (int p = 0; p < P_th; ++p) {
+          const double dz = S[(1 + p) * 8];
+          for (int64_t k = 0; k < len; ++k)
+            blk[(1 + p) * len + k] = (blk[(1 + p) * len + k] - blk[k] * dz) / z;
+        }
+        for (int p = 1 + P_th; p < B; ++p)
+          for (int64_t k = 0; k < len; ++k) blk[p * len + k] = blk[p * len + k] / z;
+      };
+      std::vector<double> Sv = S;
+      average(Sv, 8);
+      average(Smu, 4 * n_mu);
+      for (size_t b2 = 0; b2 < bands.size(); ++b2)
+        if (!Sband[b2].empty()) average(Sband[b2], 4 * bands[b2].n_q);
+      auto lin = [&](int k) {
+        LinV o{Sv[k], std::vector<double>(P)};
+        for (int p = 0; p < P; ++p) o.d[p] = Sv[(1 + p) * 8 + k];
+        return o;
+      };
+      LinV ext = lin(1), sca = lin(2), scag = lin(3), ab = lin(4), back = lin(5), r2 = lin(6),
+           r3 = lin(7);
       const char* bad = nullptr;
-      if (!(std::isfinite(ext) && ext != 0.0)) bad = "<C_ext>";
-      else if (!(std::isfinite(sca) && sca != 0.0)) bad = "<C_sca>";
-      else if (!(std::isfinite(back) && back != 0.0)) bad = "<C_back>";
+      if (!(std::isfinite(ext.v) && ext.v != 0.0)) bad = "<C_ext>";
+      else if (!(std::isfinite(sca.v) && sca.v != 0.0)) bad = "<C_sca>";
+      else if (!(std::isfinite(back.v) && back.v != 0.0)) bad = "<C_back>";
       if (bad) {
         status = INVALID_INPUT;
         msg = std::string("the ensemble's ") + bad + " is 0 or not finite, so its ratios are undefined (does m = 1?)";
       } else {
-        double out[11] = {ext,       sca,        ab,       back,     sca / ext,
-                          scag / sca, (4.0 * PI) * (ext / back), 0.0, r3 / r2,
-                          PI * r2,   (4.0 * PI / 3.0) * r3};
-        for (int k = 0; k < 11; ++k) vrow[k * n_units + unit] = out[k];
+        LinV zero{0.0, std::vector<double>(P, 0.0)};
+        LinV out[11] = {ext,
+                        sca,
+                        ab,
+                        back,
+                        lin_div(sca, ext),
+                        lin_div(scag, sca),
+                        lin_scale(lin_div(ext, back), 4.0 * PI),
+                        zero,
+                        lin_div(r3, r2),
+                        lin_scale(r2, PI),
+                        lin_scale(r3, 4.0 * PI / 3.0)};
+        for (int k = 0; k < 11; ++k) {
+          values[k * n_units + unit] = out[k].v;
+          for (int p = 0; p < P; ++p) d_values[(p * 11 + k) * n_units + unit] = out[k].d[p];
+        }
         if (phase && n_mu > 0) {
           const int src[6] = {0, 1, 0, 2, 3, 2};
           for (int e = 0; e < 6; ++e)
             for (int64_t k = 0; k < n_mu; ++k) {
-              double f = Smu[src[e] * n_mu + k] / z;
-              phase[(e * n_units + unit) * n_mu + k] = normalized ? f / sca : f;
+              LinV f{Smu[src[e] * n_mu + k], std::vector<double>(P)};
+              for (int p = 0; p < P; ++p) f.d[p] = Smu[((1 + p) * 4 + src[e]) * n_mu + k];
+              if (normalized) f = lin_div(f, sca);
+              phase[(e * n_units + unit) * n_mu + k] = f.v;
+              for (int p = 0; p < P; ++p)
+                d_phase[((p * 6 + e) * n_units + unit) * n_mu + k] = f.d[p];
             }
         }
         if (greek && want_greek) {
-          std::vector<double> g(6 * (L + 1), 0.0);
-          for (size_t bi = 0; bi < bands.size(); ++bi) {
-            if (Sband[bi].empty()) continue;
-            BandData& B = bands[bi];
-            int64_t q = B.n_q, len = B.order + 1;
-            std::vector<double> f(4 * q);
-            for (int64_t k = 0; k < 4 * q; ++k) f[k] = Sband[bi][k] / z;
-            const double* f11 = f.data();
-            const double* f12 = f.data() + q;
-            const double* f33 = f.data() + 2 * q;
-            const double* f34 = f.data() + 3 * q;
-            for (int64_t l = 0; l < len; ++l) {
-              double a1 = 0, a4 = 0, p = 0, mi = 0, b1 = 0, b2 = 0;
-              for (int64_t k = 0; k < q; ++k) {
-                double d00 = B.dmat[0][k * len + l], d22 = B.dmat[1][k * len + l];
-                double d2m2 = B.dmat[2][k * len + l], d02 = B.dmat[3][k * len + l];
-                a1 += f11[k] * d00;
-                a4 += f33[k] * d00;
-                p += (f11[k] + f33[k]) * d22;
-                mi += (f11[k] - f33[k]) * d2m2;
-                b1 += f12[k] * d02;
-                b2 += f34[k] * d02;
+          // project (engine.rs:2310-2355) every block of every band, summed over the bands.
+          std::vector<double> g(B * 6 * (L + 1), 0.0);
+          for (size_t b2 = 0; b2 < bands.size(); ++b2) {
+            if (Sband[b2].empty()) continue;
+            BandData& Bd = bands[b2];
+            int64_t qn = Bd.n_q, len = Bd.order + 1;
+            for (int blk = 0; blk < B; ++blk) {
+              const double* f = Sband[b2].data() + (int64_t)blk * 4 * qn;
+              const double* f11 = f;
+              const double* f12 = f + qn;
+              const double* f33 = f + 2 * qn;
+              const double* f34 = f + 3 * qn;
+              for (int64_t l = 0; l < len; ++l) {
+                double a1 = 0, a4 = 0, pp = 0, mi = 0, b1 = 0, b2v = 0;
+                for (int64_t k = 0; k < qn; ++k) {
+                  double d00 = Bd.dmat[0][k * len + l], d22 = Bd.dmat[1][k * len + l];
+                  double d2m2 = Bd.dmat[2][k * len + l], d02 = Bd.dmat[3][k * len + l];
+                  a1 += f11[k] * d00;
+                  a4 += f33[k] * d00;
+                  pp += (f11[k] + f33[k]) * d22;
+                  mi += (f11[k] - f33[k]) * d2m2;
+                  b1 += f12[k] * d02;
+                  b2v += f34[k] * d02;
+                }
+                double c6[6] = {a1, (pp + mi) * 0.5, (pp - mi) * 0.5, a4, b1, b2v};
+                for (int e = 0; e < 6; ++e) g[(blk * 6 + e) * (L + 1) + l] += c6[e];
               }
-              double c6[6] = {a1, (p + mi) * 0.5, (p - mi) * 0.5, a4, b1, b2};
-              for (int e = 0; e < 6; ++e) g[e * (L + 1) + l] += c6[e];
             }
           }
-          if (normalized) {
-            double a0 = g[0];
-            for (auto& e : g) e = e / a0;
-            g[0] = 1.0;
-          }
+          LinV a0{g[0], std::vector<double>(P)};
+          for (int p = 0; p < P; ++p) a0.d[p] = g[((1 + p) * 6) * (L + 1)];
           for (int e = 0; e < 6; ++e)
-            for (int64_t l = 0; l <= L; ++l)
-              greek[(e * n_units + unit) * (L + 1) + l] = g[e * (L + 1) + l];
+            for (int64_t l = 0; l <= L; ++l) {
+              LinV c{g[e * (L + 1) + l], std::vector<double>(P)};
+              for (int p = 0; p < P; ++p) c.d[p] = g[((1 + p) * 6 + e) * (L + 1) + l];
+              if (normalized) {
+                if (e == 0 && l == 0)
+                  c = LinV{1.0, std::vector<double>(P, 0.0)};
+                else
+                  c = lin_div(c, a0);
+              }
+              greek[(e * n_units + unit) * (L + 1) + l] = c.v;
+              for (int p = 0; p < P; ++p)
+                d_greek[((p * 6 + e) * n_units + unit) * (L + 1) + l] = c.d[p];
+            }
         }
       }
     }
@@ -517,6 +699,20 @@ static int ensemble_impl(const FixedDist* dists, int64_t n_dist, const double* w
     snprintf(err, err_len, "%s", first_msg.c_str());
   }
   return first_status;
+}
+
+// The fixed-grid ensemble with the derivatives of every output along the distribution's
+// parameters, then Re m and Im m (P of them): d_values (P, 11, n), d_phase (P, 6, n, n_mu),
+// d_greek (P, 6, n, L + 1).
+int orc_ensemble_fixed_d(const FixedDist* dists, int64_t n_dist, const double* wl, int64_t n_wl,
+                         const double* m, int64_t n_nodes, const double* mu, int64_t n_mu,
+                         int64_t greek_order, int normalized, int allow_unvalidated,
+                         int n_threads, double* values, double* phase, double* greek,
+                         double* d_values, double* d_phase, double* d_greek, char* err,
+                         int64_t err_len) {
+  return ensemble_impl(dists, n_dist, wl, n_wl, m, 1, nullptr, nullptr, n_nodes, mu, n_mu,
+                       greek_order, normalized, allow_unvalidated, n_threads, values, phase,
+                       greek, err, err_len, 1, d_values, d_phase, d_greek);
 }
 
 }  // extern "C"
