@@ -90,6 +90,26 @@ int scatrs_ensemble_fixed(const scatrs_distribution* dists, int64_t n_dist,
                           double* values, double* phase, double* greek, char* err,
                           size_t err_len);
 
+/*
+ * scatrs_ensemble_fixed with the derivatives of every output (the reference's
+ * `derivatives=True` of Ensemble.compute: compute_with_particle with derivative parameters,
+ * scatrs/src/ensemble/mod.rs:254-337 for their order, engine.rs:1047-1200 per node,
+ * 1782-1836 for the averages, ensemble/lin.rs for the ratios), for homogeneous spheres with
+ * every distribution of one kind. The P = n_theta + 2 directions are the distribution's
+ * parameters in ensemble_parameters order (lognormal: median_radius, width; gamma:
+ * effective_radius, effective_variance; modified gamma: alpha, b, gamma; power law: exponent),
+ * then Re m and Im m of the unit's own index. The size grid [r_lo, r_hi] is held fixed.
+ *
+ *   d_values[P * 11 * n_units], d_phase[P * 6 * n_units * n_mu] or NULL,
+ *   d_greek[P * 6 * n_units * (L + 1)] or NULL: direction-major, each block laid out as the
+ *   value arrays.
+ */
+int scatrs_ensemble_fixed_d(const scatrs_distribution* dists, int64_t n_dist,
+                            const double* wavelengths, int64_t n_wl, const double* m,
+                            const double* mu, int64_t n_mu, const scatrs_fixed_options* options,
+                            double* values, double* phase, double* greek, double* d_values,
+                            double* d_phase, double* d_greek, char* err, size_t err_len);
+
 /* Layered spheres (scatrs/src/layered/mod.rs; Particle::LayeredSphere,
  * scatrs/src/ensemble/mod.rs:58-65): n_layers layers, the core first; per distribution the
  * n_layers - 1 outer radii of layers 0..L-2 as fractions of the particle's radius (nondecreasing

@@ -45,6 +45,9 @@ SYMBOLS = {
     "scatrs_ensemble_fixed": (ctypes.c_int, [_VP, _I64, _PD, _I64, _PD, _PD, _I64,
                                              ctypes.POINTER(FixedOptions), _PD, _PD, _PD, _CP,
                                              _SZ]),
+    "scatrs_ensemble_fixed_d": (ctypes.c_int, [_VP, _I64, _PD, _I64, _PD, _PD, _I64,
+                                               ctypes.POINTER(FixedOptions), _PD, _PD, _PD, _PD,
+                                               _PD, _PD, _CP, _SZ]),
     "scatrs_ensemble_fixed_layered": (ctypes.c_int, [_VP, _I64, _PD, _I64, ctypes.POINTER(Layers),
                                                      _PD, _I64, ctypes.POINTER(FixedOptions), _PD,
                                                      _PD, _PD, _CP, _SZ]),
@@ -65,6 +68,8 @@ SYMBOLS = {
 
 KERNEL_NAMES = ("plan_chunks_kernel", "mie_fixed_kernel", "unit_kernel", "mie_nodes_kernel",
                 "final_kernel", "proj_kernel")
+# The kernels each id covers: K-a also as mie_layered_kernel / mie_deriv_kernel, the unit kernel
+# as unit_deriv_kernel, the final kernel as final_deriv_kernel.
 
 _lib = None
 
@@ -171,6 +176,35 @@ def ensemble_fixed(dists: np.ndarray, wavelengths, m, mu, n_nodes: int, greek_or
                                       1024)
     _check(st, err)
     return values, phase, greek
+
+
+def ensemble_fixed_d(dists: np.ndarray, wavelengths, m, mu, n_nodes: int, greek_order: int = -1,
+                     normalized: bool = True, allow_unvalidated: bool = False):
+    """ensemble_fixed with the derivatives along the distribution's parameters, then Re m and
+    Im m (P of them; every distribution of one kind): returns (values, phase, greek, d_values,
+    d_phase, d_greek), the derivative arrays shaped (P,) + the value array's shape."""
+    require_device()
+    dists = np.ascontiguousarray(dists, dtype=DIST_DTYPE)
+    wl = np.ascontiguousarray(wavelengths, dtype=np.float64).reshape(-1)
+    m = np.ascontiguousarray(np.broadcast_to(np.asarray(m, dtype=np.complex128),
+                                             (dists.size, wl.size)))
+    mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
+    n = dists.size * wl.size
+    kind = int(dists["kind"][0]) if dists.size else KINDS["lognormal"]
+    P = {3: 3, 4: 1}.get(kind, 2) + 2
+    opts = FixedOptions(int(n_nodes), int(greek_order), int(normalized), int(allow_unvalidated))
+    values, d_values = np.zeros((11, n)), np.zeros((P, 11, n))
+    phase = np.zeros((6, n, mu.size)) if mu.size else None
+    d_phase = np.zeros((P, 6, n, mu.size)) if mu.size else None
+    greek = np.zeros((6, n, greek_order + 1)) if greek_order >= 0 else None
+    d_greek = np.zeros((P, 6, n, greek_order + 1)) if greek_order >= 0 else None
+    err = ctypes.create_string_buffer(1024)
+    st = load().scatrs_ensemble_fixed_d(dists.ctypes.data, dists.size, _p(wl), wl.size,
+                                        _p(m.view(np.float64)), _p(mu), mu.size,
+                                        ctypes.byref(opts), _p(values), _p(phase), _p(greek),
+                                        _p(d_values), _p(d_phase), _p(d_greek), err, 1024)
+    _check(st, err)
+    return values, phase, greek, d_values, d_phase, d_greek
 
 
 def ensemble_fixed_layered(dists: np.ndarray, wavelengths, fractions, m_layers, mu,

@@ -139,7 +139,7 @@ struct Context {
   UserTables user;
   std::map<int, BandTables> bands;  // by Greek order
   std::map<int64_t, std::pair<std::vector<double>, std::vector<double>>> rules;
-  DevBuf radius, weight, wl, m, fractions, chunk_n, chunk_n_slab, chunk_row, chunk_acc, plan_units,
+  DevBuf radius, weight, wtheta, wl, m, fractions, chunk_n, chunk_n_slab, chunk_row, chunk_acc, plan_units,
       unit_acc, unit_slots, slots, items, proj_items, slot_index, slot_greek, X, uz, ux,
       chunk_sums, err, acc, counter, values, phase, greek;
   std::vector<int> chunk_n_host;
@@ -333,7 +333,7 @@ BandTables& ensure_bands(Context& c, int L, int last_band, cudaStream_t s) {
 }
 
 void check_options(const scatrs_fixed_options* o, int64_t n_units, int64_t n_mu,
-                   const double* mu) {
+                   const double* mu, int n_derivs = 0) {
   if (!o) throw Failure{SCATRS_INVALID_INPUT, "options must not be NULL"};
   if (o->n_nodes < 1) throw Failure{SCATRS_INVALID_INPUT, "n_nodes must be >= 1"};
   if (o->greek_order < -1 || o->greek_order > kMaxGreekOrder)
@@ -345,6 +345,7 @@ void check_options(const scatrs_fixed_options* o, int64_t n_units, int64_t n_mu,
                     "a cosine of the scattering angle must be finite and in [-1, 1]"};
   // The output bound of scatrs-py/src/ensemble.rs:388-399.
   int64_t per = 11 + 4 * n_mu + (o->greek_order >= 0 ? 6 * ((int64_t)o->greek_order + 1) : 0);
+  per *= 1 + n_derivs;
   if ((double)n_units * (double)per * 2.0 > 2.0 * (double)kMaxMieValues)
     throw Failure{SCATRS_INVALID_INPUT,
                   "the ensemble outputs would exceed 2 * MAX_MIE_VALUES = 268435456 real values"};
@@ -376,12 +377,24 @@ struct LayerInput {
   const double* m_dev = nullptr;
 };
 
+// Derivative outputs (homogeneous spheres, every distribution of one kind): along the
+// distribution's n_theta parameters, then Re m and Im m; device arrays d_values [P][11][n],
+// d_phase [P][6][n][n_mu], d_greek [P][6][n][L + 1].
+struct DerivOutput {
+  bool on = false;
+  int n_theta = 0;
+  double* d_values = nullptr;
+  double* d_phase = nullptr;
+  double* d_greek = nullptr;
+};
+
 void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, const double* wl_dev,
                int64_t n_wl, const double* m_dev, const double* mu, int64_t n_mu,
                const scatrs_fixed_options* opt, double* values, double* phase, double* greek,
-               cudaStream_t s, FixedCall* call, const LayerInput& layers = LayerInput()) {
+               cudaStream_t s, FixedCall* call, const LayerInput& layers = LayerInput(),
+               const DerivOutput& dv = DerivOutput()) {
   const int64_t n_units = n_dist * n_wl;
-  check_options(opt, n_units, n_mu, mu);
+  check_options(opt, n_units, n_mu, mu, dv.on ? dv.n_theta + 2 : 0);
   if (n_units == 0) return;
   const int64_t n_nodes = opt->n_nodes;
   const int cpu = (int)((n_nodes + 31) / 32);
@@ -391,6 +404,16 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
   // 1. Node table.
   const auto& gl = rule(c, n_nodes);
   std::vector<double> radius(n_dist * n_nodes), weight(n_dist * n_nodes);
+  std::vector<double> wtheta(dv.on ? n_dist * n_nodes * 3 : 0);
+  if (dv.on) {
+    if (layers.n_layers > 1)
+      throw Failure{SCATRS_INVALID_INPUT, "derivatives are for homogeneous spheres"};
+    for (int64_t d = 0; d < n_dist; ++d)
+      if (parameter_count(dists[d].kind) != dv.n_theta)
+        throw Failure{SCATRS_INVALID_INPUT,
+                      "derivatives need every distribution of one kind (distribution " +
+                          std::to_string(d) + " differs)"};
+  }
   for (int64_t d = 0; d < n_dist; ++d) {
     std::string msg;
     if (!validate_distribution(dists[d].kind, dists[d].param, &msg))
@@ -403,9 +426,17 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
     for (int64_t j = 0; j < n_nodes; ++j) {
       double t = ctr + h * gl.first[j];
       double r = std::exp(t);
-      double u = density(dists[d].kind, dists[d].param, r);
+      const double w = h * gl.second[j];
+      double u;
+      if (dv.on) {
+        double g[3];
+        u = density_gradient(dists[d].kind, dists[d].param, r, g);
+        for (int p = 0; p < 3; ++p) wtheta[(d * n_nodes + j) * 3 + p] = w * (g[p] * r);
+      } else {
+        u = density(dists[d].kind, dists[d].param, r);
+      }
       radius[d * n_nodes + j] = r;
-      weight[d * n_nodes + j] = h * gl.second[j] * (u * r);
+      weight[d * n_nodes + j] = w * (u * r);
     }
   }
   const int L_layers = layers.n_layers;
@@ -428,7 +459,13 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
                           cudaMemcpyHostToDevice, s));
   SB_CUDA(cudaMemcpyAsync(c.weight.get(weight.size() * 8), weight.data(), weight.size() * 8,
                           cudaMemcpyHostToDevice, s));
-  unsigned long long* err = c.err.as<unsigned long long>(2);
+  if (dv.on)
+    SB_CUDA(cudaMemcpyAsync(c.wtheta.get(wtheta.size() * 8), wtheta.data(), wtheta.size() * 8,
+                            cudaMemcpyHostToDevice, s));
+  // Blocks of sums per quantity (values, then each derivative) and coefficient rows per term
+  // of a chunk (two 16-node halves with derivatives).
+  const int n_blk = dv.on ? 3 + dv.n_theta : 1;
+  const int rows_per_term = dv.on ? 2 : 1;  unsigned long long* err = c.err.as<unsigned long long>(2);
   SB_CUDA(cudaMemsetAsync(err, 0xff, 2 * sizeof(unsigned long long), s));
   // 2. Plan: every chunk's largest number of terms.
   PlanArgs pa{};
@@ -476,7 +513,7 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
     }
   }
   const int t_user = (c.user.h + 31) / 32;
-  const int64_t acc_head = 4 * n_mu;
+  const int64_t acc_head = 4 * n_mu * n_blk;
   std::vector<int64_t> urows(n_units), uacc(n_units);
   std::vector<int> uslots(n_units), utiles(n_units);
   std::vector<double> ucost(n_units);
@@ -489,18 +526,18 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
     int prev = -1, slots = 0, max_tiles = 1;
     for (int k = 0; k < cpu; ++k) {
       const int nc = cu[k];
-      rows += nc;
+      rows += (int64_t)rows_per_term * nc;
       int tiles = t_user;
       if (bt && nc > 0) {
         const int b = band_of_n[nc];
         tiles += band_tiles[b];
         if (b != prev) {
-          acc += 4 * (int64_t)band_nq[b];
-          ++slots;
+          acc += 4 * (int64_t)band_nq[b] * n_blk;
+          slots += n_blk;
           prev = b;
         }
       }
-      cost += (double)tiles * ((double)nc + 24.0);
+      cost += (double)tiles * ((double)nc + 24.0) * rows_per_term * (dv.on ? 1.5 : 1.0);
       max_tiles = std::max(max_tiles, tiles);
     }
     urows[u] = rows;
@@ -616,7 +653,7 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
   const int n_arr = L_layers > 1 ? 2 * L_layers - 1 : 1;
   double2* uz = c.uz.as<double2>((size_t)(arena + 2 * kMaxSlabChunks) * 32 * n_arr);
   double* ux = c.ux.as<double>((size_t)(arena + 2 * kMaxSlabChunks) * 32);
-  double* chunk_sums = c.chunk_sums.as<double>((size_t)kMaxSlabChunks * 8);
+  double* chunk_sums = c.chunk_sums.as<double>((size_t)kMaxSlabChunks * 8 * n_blk);
   double* acc = c.acc.as<double>((size_t)acc_max);
   double* slot_greek =
       L >= 0 ? c.slot_greek.as<double>((size_t)slots_max * 6 * (L + 1)) : nullptr;
@@ -644,6 +681,11 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
   ka.chunk_sums = chunk_sums;
   ka.err = err;
   ka.allow_unvalidated = opt->allow_unvalidated;
+  if (dv.on) {
+    ka.deriv = 1;
+    ka.n_theta = dv.n_theta;
+    ka.wtheta = c.wtheta.as<double>(0);
+  }
   UnitArgs ua{};
   ua.radius = ka.radius;
   ua.weight = ka.weight;
@@ -667,12 +709,16 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
   }
   ua.acc = acc;
   ua.work_counter = counter;
+  ua.deriv = ka.deriv;
+  ua.n_theta = ka.n_theta;
+  ua.wtheta = ka.wtheta;
   ProjArgs pj{};
   pj.cpu = cpu;
   pj.greek_order = L;
   pj.acc = acc;
   pj.chunk_sums = chunk_sums;
   pj.slot_greek = slot_greek;
+  pj.raw = dv.on ? 1 : 0;
   if (bt) {
     pj.bands = bt->desc_d.as<BandDesc>(0);
     pj.band_d = bt->d_d.as<double>(0);
@@ -693,6 +739,12 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
   fa.greek = L >= 0 ? greek : nullptr;
   fa.normalized = opt->normalized;
   fa.err = err;
+  if (dv.on) {
+    fa.n_theta = dv.n_theta;
+    fa.d_values = dv.d_values;
+    fa.d_phase = n_mu > 0 ? dv.d_phase : nullptr;
+    fa.d_greek = L >= 0 ? dv.d_greek : nullptr;
+  }
   std::vector<std::pair<double, int64_t>> order;  // work items by cost
   std::vector<int> per_band;
   for (int64_t sl = 0; sl < n_slabs; ++sl) {
@@ -731,20 +783,23 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
         const int nc = cn[(int64_t)u * cpu + k];
         P_cn[ci] = nc;
         P_row[ci] = row;
-        row += nc;
+        row += (int64_t)rows_per_term * nc;
         P_cacc[ci] = -1;
         if (bt && nc > 0) {
           const int b = band_of_n[nc];
           if (b != prev) {
-            P_slots[nslot].band = b;
-            P_slots[nslot].unit = (int)lu;
-            P_slots[nslot].off = band_acc;
-            band_acc += 4 * (int64_t)band_nq[b];
-            ++nslot;
-            us.y += 1;
+            // One slot per block of sums, their tables 4 n_q doubles apart.
+            for (int blk = 0; blk < n_blk; ++blk) {
+              P_slots[nslot].band = b;
+              P_slots[nslot].unit = (int)lu;
+              P_slots[nslot].off = band_acc;
+              band_acc += 4 * (int64_t)band_nq[b];
+              ++nslot;
+            }
+            us.y += n_blk;
             prev = b;
           }
-          P_cacc[ci] = P_slots[nslot - 1].off;
+          P_cacc[ci] = P_slots[nslot - n_blk].off;
         }
       }
       P_uslots[lu] = us;
@@ -940,6 +995,56 @@ int scatrs_ensemble_fixed(const scatrs_distribution* dists, int64_t n_dist,
     SB_CUDA(cudaMemcpyAsync(values, v_d, vl * 8, cudaMemcpyDeviceToHost, s));
     if (pl > 0 && phase) SB_CUDA(cudaMemcpyAsync(phase, p_d, pl * 8, cudaMemcpyDeviceToHost, s));
     if (gl > 0 && greek) SB_CUDA(cudaMemcpyAsync(greek, g_d, gl * 8, cudaMemcpyDeviceToHost, s));
+    SB_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+int scatrs_ensemble_fixed_d(const scatrs_distribution* dists, int64_t n_dist,
+                            const double* wavelengths, int64_t n_wl, const double* m,
+                            const double* mu, int64_t n_mu, const scatrs_fixed_options* options,
+                            double* values, double* phase, double* greek, double* d_values,
+                            double* d_phase, double* d_greek, char* err, size_t err_len) {
+  return guarded(err, err_len, [&] {
+    if (n_dist < 0 || n_wl < 0) throw Failure{SCATRS_INVALID_INPUT, "negative sizes"};
+    for (int64_t i = 0; i < n_wl; ++i)
+      if (!(std::isfinite(wavelengths[i]) && wavelengths[i] > 0.0))
+        throw Failure{SCATRS_INVALID_INPUT, "wavelengths must be finite and > 0"};
+    DerivOutput dv;
+    dv.on = true;
+    dv.n_theta = n_dist > 0 ? parameter_count(dists[0].kind) : 2;
+    const int P = dv.n_theta + 2;
+    Context& c = context();
+    std::lock_guard<std::mutex> lk(c.mtx);
+    cudaStream_t s = 0;
+    const int64_t n_units = n_dist * n_wl;
+    check_options(options, n_units, n_mu, mu, P);
+    if (n_units == 0) return;
+    double* wl_d = c.wl.as<double>(n_wl);
+    double* m_d = c.m.as<double>(2 * n_units);
+    SB_CUDA(cudaMemcpyAsync(wl_d, wavelengths, n_wl * 8, cudaMemcpyHostToDevice, s));
+    SB_CUDA(cudaMemcpyAsync(m_d, m, 2 * n_units * 8, cudaMemcpyHostToDevice, s));
+    int64_t vl, pl, gl;
+    scatrs_ensemble_fixed_sizes(n_units, n_mu, options->greek_order, &vl, &pl, &gl);
+    // One allocation per output kind: the values, then the P derivative blocks.
+    double* v_d = c.values.as<double>(vl * (1 + P));
+    double* p_d = pl > 0 ? c.phase.as<double>(pl * (1 + P)) : nullptr;
+    double* g_d = gl > 0 ? c.greek.as<double>(gl * (1 + P)) : nullptr;
+    dv.d_values = v_d + vl;
+    dv.d_phase = p_d ? p_d + pl : nullptr;
+    dv.d_greek = g_d ? g_d + gl : nullptr;
+    FixedCall call;
+    call.wl_host.assign(wavelengths, wavelengths + n_wl);
+    run_fixed(c, dists, n_dist, wl_d, n_wl, m_d, mu, n_mu, options, v_d, p_d, g_d, s, &call,
+              LayerInput(), dv);
+    check_device_errors(c, s, &call);
+    SB_CUDA(cudaMemcpyAsync(values, v_d, vl * 8, cudaMemcpyDeviceToHost, s));
+    if (d_values) SB_CUDA(cudaMemcpyAsync(d_values, dv.d_values, P * vl * 8, cudaMemcpyDeviceToHost, s));
+    if (pl > 0 && phase) SB_CUDA(cudaMemcpyAsync(phase, p_d, pl * 8, cudaMemcpyDeviceToHost, s));
+    if (pl > 0 && d_phase)
+      SB_CUDA(cudaMemcpyAsync(d_phase, dv.d_phase, P * pl * 8, cudaMemcpyDeviceToHost, s));
+    if (gl > 0 && greek) SB_CUDA(cudaMemcpyAsync(greek, g_d, gl * 8, cudaMemcpyDeviceToHost, s));
+    if (gl > 0 && d_greek)
+      SB_CUDA(cudaMemcpyAsync(d_greek, dv.d_greek, P * gl * 8, cudaMemcpyDeviceToHost, s));
     SB_CUDA(cudaStreamSynchronize(s));
   });
 }
@@ -1147,7 +1252,7 @@ void scatrs_release(void) {
   std::lock_guard<std::mutex> lk(g_ctx_mtx);
   if (dev < (int)g_ctx.size() && g_ctx[dev]) {
     Context& c = *g_ctx[dev];
-    for (DevBuf* b : {&c.radius, &c.weight, &c.wl, &c.m, &c.fractions, &c.chunk_n, &c.chunk_n_slab,
+    for (DevBuf* b : {&c.radius, &c.weight, &c.wtheta, &c.wl, &c.m, &c.fractions, &c.chunk_n, &c.chunk_n_slab,
                       &c.chunk_row, &c.chunk_acc, &c.plan_units, &c.unit_acc, &c.unit_slots,
                       &c.slots, &c.items, &c.proj_items, &c.slot_index, &c.slot_greek,
                       &c.X, &c.uz, &c.ux, &c.chunk_sums, &c.err, &c.acc,

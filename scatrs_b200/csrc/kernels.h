@@ -38,6 +38,11 @@ struct MieFixedArgs {
   double* chunk_sums;       // [n_chunks][8] weighted per-particle quantities
   unsigned long long* err;
   int allow_unvalidated;
+  // Derivatives (homogeneous spheres): chunk rows of two 16-node halves, chunk_sums
+  // [n_chunks][3 + n_theta][8], and the parameter weights w_j (du/dtheta_p)(r_j) r_j.
+  int deriv;
+  int n_theta;
+  const double* wtheta;  // [n_dist][n_nodes][3]
 };
 
 struct MieNodesArgs {
@@ -107,6 +112,7 @@ struct ProjArgs {
   int cpu;
   int greek_order;
   double* slot_greek;
+  int raw;  // project the raw sums (derivatives: averaged after the projection)
 };
 
 // K-b and K-c over one slab: the work items write the per-unit accumulators (zeroed before).
@@ -135,6 +141,11 @@ struct UnitArgs {
   const double* band_go;
   double* acc;
   int* work_counter;
+  // Derivatives (deriv != 0): n_theta distribution parameters, their node weights in wtheta
+  // ([n_dist][n_nodes][3]).
+  int deriv;
+  int n_theta;
+  const double* wtheta;
 };
 
 // K-d and the outputs over one slab: averages, band projections, assembly.
@@ -156,6 +167,13 @@ struct FinalArgs {
   double* greek;
   int normalized;
   unsigned long long* err;
+  // Derivatives (d_values != nullptr): n_theta distribution parameters, then Re m and Im m;
+  // chunk_sums [chunk][3 + n_theta][8], each unit's cosine sums and slots one block after
+  // another; d_values [P][11][n], d_phase [P][6][n][n_mu], d_greek [P][6][n][L + 1].
+  int n_theta;
+  double* d_values;
+  double* d_phase;
+  double* d_greek;
 };
 
 void launch_plan_chunks(const PlanArgs& a, cudaStream_t s);

@@ -26,6 +26,8 @@ __device__ __forceinline__ cplx operator*(cplx a, cplx b) {
   return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
 }
 __device__ __forceinline__ cplx scl(cplx a, double t) { return {a.re * t, a.im * t}; }
+// i u (complex.rs:43-45).
+__device__ __forceinline__ cplx cti(cplx u) { return {-u.im, u.re}; }
 __device__ __forceinline__ double nsq(cplx a) { return a.re * a.re + a.im * a.im; }
 __device__ __forceinline__ double cabs_(cplx a) { return hypot(a.re, a.im); }
 __device__ __forceinline__ double re_mul_conj(cplx u, cplx v) { return u.re * v.re + u.im * v.im; }
@@ -201,6 +203,50 @@ struct Eff {
   double q_ext, q_sca, q_abs, q_back, g;
 };
 
+// Running sums of derivative_sums (efficiencies.rs:89-146) along Re m (p = 0) and Im m (p = 1,
+// where d/d(Im m) = i d/dm), fed one order at a time like ValueSums.
+struct DerivSums {
+  double sca[2] = {0.0, 0.0}, g[2] = {0.0, 0.0};
+  cplx back[2] = {{0.0, 0.0}, {0.0, 0.0}};
+  cplx a_prev = {0.0, 0.0}, b_prev = {0.0, 0.0}, da_prev = {0.0, 0.0}, db_prev = {0.0, 0.0};
+  __device__ __forceinline__ void add(int64_t k, cplx ak, cplx bk, cplx dak, cplx dbk) {
+    const cplx dA[2] = {dak, cti(dak)}, dB[2] = {dbk, cti(dbk)};
+    if (k > 1) {
+      const double kf = (double)(k - 1);
+      const double pair = kf * (kf + 2.0) / (kf + 1.0);
+      const double own = (double)(2 * (k - 1) + 1) / (kf * (kf + 1.0));
+      const cplx pA[2] = {da_prev, cti(da_prev)}, pB[2] = {db_prev, cti(db_prev)};
+#pragma unroll
+      for (int p = 0; p < 2; ++p) {
+        g[p] += pair * (re_mul_conj(pA[p], ak) + re_mul_conj(a_prev, dA[p]) +
+                        re_mul_conj(pB[p], bk) + re_mul_conj(b_prev, dB[p]));
+        g[p] += own * (re_mul_conj(pA[p], b_prev) + re_mul_conj(a_prev, pB[p]));
+      }
+    }
+    const double w = (double)(2 * k + 1);
+#pragma unroll
+    for (int p = 0; p < 2; ++p) {
+      sca[p] += w * 2.0 * (re_mul_conj(dA[p], ak) + re_mul_conj(dB[p], bk));
+      const cplx t = scl(dA[p] - dB[p], w);
+      back[p] = (k % 2 == 0) ? back[p] + t : back[p] - t;
+    }
+    a_prev = ak;
+    b_prev = bk;
+    da_prev = dak;
+    db_prev = dbk;
+  }
+  __device__ __forceinline__ void close(int64_t n) {
+    if (n >= 1) {
+      const double kf = (double)n;
+      const double own = (double)(2 * n + 1) / (kf * (kf + 1.0));
+      const cplx pA[2] = {da_prev, cti(da_prev)}, pB[2] = {db_prev, cti(db_prev)};
+#pragma unroll
+      for (int p = 0; p < 2; ++p)
+        g[p] += own * (re_mul_conj(pA[p], b_prev) + re_mul_conj(a_prev, pB[p]));
+    }
+  }
+};
+
 // efficiencies_from (efficiencies.rs:169-187).
 __device__ __forceinline__ Eff efficiencies_from(double x, double abs_sum, const ValueSums& s) {
   double inv_x = 1.0 / x;
@@ -210,6 +256,20 @@ __device__ __forceinline__ Eff efficiencies_from(double x, double abs_sum, const
   double q_abs = two_x2 * abs_sum;
   double g = s.sca == 0.0 ? 0.0 : 2.0 * s.g / s.sca;
   return {q_sca + q_abs, q_sca, q_abs, nsq(s.back) * inv_x2, g};
+}
+
+// The efficiencies' derivatives along Re m (p = 0) or Im m (p = 1) of a homogeneous sphere
+// (efficiencies_jacobian, efficiencies.rs:192-230; no x term along m).
+__device__ __forceinline__ Eff efficiency_derivs(double x, const ValueSums& vs, const Eff& q,
+                                                 const DerivSums& ds, int p, double abs_d) {
+  double inv_x = 1.0 / x;
+  double inv_x2 = inv_x * inv_x;
+  double two_x2 = 2.0 * inv_x2;
+  double q_sca = two_x2 * ds.sca[p];
+  double q_abs = two_x2 * abs_d;
+  double q_back = 2.0 * re_mul_conj(ds.back[p], vs.back) * inv_x2;
+  double g = vs.sca == 0.0 ? 0.0 : (2.0 * ds.g[p] - q.g * ds.sca[p]) / vs.sca;
+  return {q_sca + q_abs, q_sca, q_abs, q_back, g};
 }
 
 // One coefficient's effective log-derivative H at a layered sphere's outer surface at one order
@@ -225,13 +285,28 @@ struct NoLayers {
   __device__ __forceinline__ void order(int64_t, Side&, Side&) {}
 };
 
-// State::finish (kernel.rs:324-559) without derivatives: calls emit(k, a_k, b_k) for k = 1..n
-// and returns the absorption sum (x^2/2) Q_abs, feeding the value sums on the way. With a
-// layered sphere's `layers`, its H_a, H_b replace D_n(mx) at each order (kernel.rs:382-476);
-// they are computed order by order in the same upward loop.
-template <class Emit, class Layers>
+// No derivatives.
+struct NoDeriv {
+  static constexpr bool kOn = false;
+};
+
+// The derivatives along the refractive index of a homogeneous sphere (kernel.rs:486-532):
+// da/dm, db/dm per order go to emit(k, a_k, b_k, da_k/dm, db_k/dm), and the absorption sum's
+// derivatives along Re m and Im m (d/d(Im m) = i d/dm) accumulate here.
+struct MDeriv {
+  static constexpr bool kOn = true;
+  double abs_re = 0.0, abs_im = 0.0;
+};
+
+// State::finish (kernel.rs:324-559): calls emit(k, a_k, b_k) for k = 1..n and returns the
+// absorption sum (x^2/2) Q_abs, feeding the value sums on the way. With a layered sphere's
+// `layers`, its H_a, H_b replace D_n(mx) at each order (kernel.rs:382-476); they are computed
+// order by order in the same upward loop. With MDeriv (homogeneous spheres only) emit also
+// receives the coefficients' derivatives along m.
+template <class Emit, class Layers, class Deriv = NoDeriv>
 __device__ __forceinline__ double mie_finish(double x, cplx m, int64_t n, const Scratch& s,
-                                             ValueSums& vs, Emit emit, Layers& layers) {
+                                             ValueSums& vs, Emit emit, Layers& layers,
+                                             Deriv* deriv = nullptr) {
   const double one = 1.0;
   cplx z = scl(m, x);
   int64_t n_s = upward_orders(x, n);
@@ -271,7 +346,7 @@ __device__ __forceinline__ double mie_finish(double x, cplx m, int64_t n, const 
     cplx md = hh_b * m;
     cplx big_a = d_m + rl(k_x);
     cplx big_b = md + rl(k_x);
-    cplx an, bn, inv_da, inv_db;
+    cplx an, bn, inv_da, inv_db, g_a, g_b;
     if (k <= n_s) {
       double c = (double)(2 * k - 1) * inv_x;
       double psi_next = c * psi - psi_prev;
@@ -298,6 +373,10 @@ __device__ __forceinline__ double mie_finish(double x, cplx m, int64_t n, const 
         bn = sb.direct ? (scl(big_b, psi) - rl(psi_prev)) * inv_db
                        : (own_b + scl(m * sb.v, psi)) * inv_db;
       }
+      if (Deriv::kOn) {
+        g_a = xi * inv_da;
+        g_b = xi * inv_db;
+      }
       if (k == n_s) {
         inv_xi = cinv(xi);
         t = rl(psi) * inv_xi;
@@ -322,13 +401,39 @@ __device__ __forceinline__ double mie_finish(double x, cplx m, int64_t n, const 
       bn = t * num_b * ib;
       inv_da = inv_xi * ia;
       inv_db = inv_xi * ib;
+      g_a = ia;
+      g_b = ib;
     }
-    emit(k, an, bn);
     vs.add(k, an, bn);
     double na = nsq(inv_da);
     double nb = nsq(inv_db);
     double weight = (double)(2 * k + 1);
     asum += weight * (-(d_m.im * na) - md.im * nb);
+    if constexpr (Deriv::kOn) {
+      // d_plus = D + z D' and d_minus = D - z D' in terms of u = u_{k+1}(mx) (kernel.rs:
+      // 490-500); d(D/m)/dm and d(mD)/dm and the absorption terms (kernel.rs:507-532).
+      const double two = 2.0;
+      cplx one_u2 = rl(one) + u_z1 * u_z1;
+      cplx d_plus = scl(u_z1, weight) - z * one_u2;
+      cplx d_minus = scl(d, two) - d_plus;
+      cplx ida2 = inv_da * inv_da;
+      cplx idb2 = inv_db * inv_db;
+      cplx dan = cti(d_minus) * inv_m2 * ida2;
+      cplx dbn = -(cti(d_plus) * idb2);
+      emit(k, an, bn, dan, dbn);
+      cplx fa_m = -(d_minus * inv_m2);
+      cplx fb_m = d_plus;
+      cplx la_m = fa_m * g_a;
+      cplx lb_m = fb_m * g_b;
+      auto term = [&](cplx f, cplx df, cplx l, double n2) {
+        return -((df.im - two * f.im * l.re) * n2);
+      };
+      deriv->abs_re += weight * (term(d_m, fa_m, la_m, na) + term(md, fb_m, lb_m, nb));
+      deriv->abs_im += weight * (term(d_m, cti(fa_m), cti(la_m), na) +
+                                 term(md, cti(fb_m), cti(lb_m), nb));
+    } else {
+      emit(k, an, bn);
+    }
   }
   vs.close(n);
   return asum;

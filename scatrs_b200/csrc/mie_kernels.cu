@@ -136,8 +136,109 @@ __device__ __forceinline__ void mie_chunk(const MieFixedArgs& a) {
   }
 }
 
+// Homogeneous spheres with the derivatives along the distribution's parameters and m. The
+// chunk's coefficient rows are two halves of 16 nodes, nc rows each (lanes 0-15, then 16-31);
+// a row holds the 16 nodes' (u, v) in its first 64 doubles and their derivatives along m,
+// (du/dm, dv/dm), in the last 64, so that one 128-column GEMM tile carries both. The chunk's
+// sums are per block: values, then each parameter of the distribution (weights
+// w_j (du/dtheta)(r_j) r_j), then Re m and Im m (engine.rs:1047-1109).
+__device__ __forceinline__ void mie_chunk_deriv(const MieFixedArgs& a) {
+  int wslot = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (wslot >= a.n_chunks) return;
+  int chunk = wslot;
+  int64_t unit = a.units[chunk / a.cpu];
+  int c = chunk % a.cpu;
+  int64_t d = unit / a.n_wl, i = unit % a.n_wl;
+  int j = c * 32 + lane;
+  int nc = a.chunk_n[chunk];
+  int64_t row0 = a.chunk_row[chunk];
+  double* X = a.X + (row0 + (int64_t)(lane >> 4) * nc) * 128 + (lane & 15) * 4;
+  Scratch s;
+  s.uz = a.uz + (row0 + 2 * (int64_t)chunk) * 32 + lane;
+  s.ux = a.ux + (row0 + 2 * (int64_t)chunk) * 32 + lane;
+  s.stride = 32;
+  const int P = a.n_theta;
+  const int B = 3 + P;
+  double q[6][8];
+#pragma unroll
+  for (int b = 0; b < 6; ++b)
+#pragma unroll
+    for (int k = 0; k < 8; ++k) q[b][k] = 0.0;
+  int64_t n = 0;
+  if (j < a.n_nodes) {
+    const double r = a.radius[d * a.n_nodes + j];
+    const double w = a.weight[d * a.n_nodes + j];
+    const double x = 2.0 * kPi * r / a.wl[i];
+    n = default_n_max(x);
+    ValueSums vs;
+    DerivSums ds;
+    MDeriv md;
+    const double2 mv = a.m[unit];
+    const cplx m = mk(mv.x, mv.y);
+    const int st = check_node(x, m, n, a.allow_unvalidated != 0);
+    double asum = 0.0;
+    if (st == 0 && n <= nc) {
+      mie_prepare(x, m, n, s);
+      NoLayers none;
+      auto emit = [&](int64_t k, cplx an, cplx bn, cplx dan, cplx dbn) {
+        const bool odd = (k & 1) != 0;
+        const cplx u = odd ? an : bn, v = odd ? bn : an;
+        const cplx du = odd ? dan : dbn, dv = odd ? dbn : dan;
+        *reinterpret_cast<double4*>(X + (k - 1) * 128) = make_double4(u.re, u.im, v.re, v.im);
+        *reinterpret_cast<double4*>(X + (k - 1) * 128 + 64) =
+            make_double4(du.re, du.im, dv.re, dv.im);
+        ds.add(k, an, bn, dan, dbn);
+      };
+      asum = mie_finish(x, m, n, s, vs, emit, none, &md);
+      ds.close(n);
+    }
+    if (st != 0 || n > nc) {
+      record_error(a.err, i, d, j, a.n_dist, a.n_nodes, st != 0 ? st : 1);
+      n = 0;
+    } else {
+      const Eff e = efficiencies_from(x, asum, vs);
+      const double area = kPi * r * r;
+      const double qv[8] = {1.0,           area * e.q_ext, area * e.q_sca, area * e.q_sca * e.g,
+                            area * e.q_abs, area * e.q_back, r * r,         r * r * r};
+      for (int k = 0; k < 8; ++k) q[0][k] = w * qv[k];
+      for (int p = 0; p < P; ++p) {
+        const double wt = a.wtheta[(d * a.n_nodes + j) * 3 + p];
+        for (int k = 0; k < 8; ++k) q[1 + p][k] = wt * qv[k];
+      }
+      for (int p = 0; p < 2; ++p) {
+        const Eff de = efficiency_derivs(x, vs, e, ds, p, p == 0 ? md.abs_re : md.abs_im);
+        const double qd[8] = {0.0,
+                              area * de.q_ext,
+                              area * de.q_sca,
+                              area * (de.q_sca * e.g + e.q_sca * de.g),
+                              area * de.q_abs,
+                              area * de.q_back,
+                              0.0,
+                              0.0};
+        for (int k = 0; k < 8; ++k) q[1 + P + p][k] = w * qd[k];
+      }
+    }
+  }
+  for (int64_t k = n + 1; k <= nc; ++k) {
+    *reinterpret_cast<double4*>(X + (k - 1) * 128) = make_double4(0.0, 0.0, 0.0, 0.0);
+    *reinterpret_cast<double4*>(X + (k - 1) * 128 + 64) = make_double4(0.0, 0.0, 0.0, 0.0);
+  }
+  for (int b = 0; b < 6; ++b) {
+    if (b >= B) break;
+    for (int k = 0; k < 8; ++k) {
+      double v = q[b][k];
+      for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+      if (lane == 0) a.chunk_sums[((int64_t)chunk * B + b) * 8 + k] = v;
+    }
+  }
+}
+
 // Homogeneous spheres.
 __global__ void __launch_bounds__(128) mie_fixed_kernel(MieFixedArgs a) { mie_chunk<false>(a); }
+
+// Homogeneous spheres with derivatives.
+__global__ void __launch_bounds__(128) mie_deriv_kernel(MieFixedArgs a) { mie_chunk_deriv(a); }
 
 // Layered spheres (their per-layer state lives in local memory).
 __global__ void __launch_bounds__(128) mie_layered_kernel(MieFixedArgs a) { mie_chunk<true>(a); }
@@ -189,7 +290,9 @@ void launch_plan_chunks(const PlanArgs& a, cudaStream_t s) {
 void launch_mie_fixed(const MieFixedArgs& a, cudaStream_t s) {
   int threads = 128;
   int blocks = (a.n_chunks * 32 + threads - 1) / threads;
-  if (a.n_layers > 1)
+  if (a.deriv)
+    mie_deriv_kernel<<<blocks, threads, 0, s>>>(a);
+  else if (a.n_layers > 1)
     mie_layered_kernel<<<blocks, threads, 0, s>>>(a);
   else
     mie_fixed_kernel<<<blocks, threads, 0, s>>>(a);

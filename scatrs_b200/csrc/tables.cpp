@@ -281,4 +281,49 @@ double density(int kind, const double* p, double r) {
   return std::exp(ln_u);
 }
 
+int parameter_count(int kind) { return kind == 3 ? 3 : kind == 4 ? 1 : 2; }
+
+double density_gradient(int kind, const double* p, double r, double grad[3]) {
+  const double u = density(kind, p, r);
+  double dln[3] = {0.0, 0.0, 0.0};
+  switch (kind) {
+    case 1: {
+      // ln u = -z^2 / (2 s^2) - ln s - ln(r/r0), z = ln r - ln median, s = ln width.
+      const double s = std::log(p[1]);
+      const double z = std::log(r) - std::log(p[0]);
+      dln[0] = z / (s * s * p[0]);
+      dln[1] = (z * z / (s * s * s) - 1.0 / s) / p[1];
+      break;
+    }
+    case 2: {
+      // ln u = alpha ln(r/r0) - (r - r0)/(a b), alpha = (1 - 3b)/b.
+      const double a = p[0], b = p[1];
+      const double alpha = (1.0 - 3.0 * b) / b;
+      const double r0 = alpha > 0.0 ? alpha * a * b : a;
+      const double sc = a * b;
+      dln[0] = (r - r0) * b / (sc * sc);
+      dln[1] = -std::log(r / r0) / (b * b) + (r - r0) * a / (sc * sc);
+      break;
+    }
+    case 3: {
+      // ln u = alpha ln(r/r0) - b (r^gamma - r0^gamma).
+      const double alpha = p[0], b = p[1], g = p[2];
+      const double r0 = std::pow(std::max(alpha, 1.0) / (b * g), 1.0 / g);
+      const double rg = std::pow(r, g), r0g = std::pow(r0, g);
+      dln[0] = std::log(r / r0);
+      dln[1] = -(rg - r0g);
+      dln[2] = -b * (rg * std::log(r) - r0g * std::log(r0));
+      break;
+    }
+    case 4: {
+      // ln u = -exponent ln(r/r0) on [min, max], 0 outside.
+      const double r0 = p[0] >= 0.0 ? p[1] : p[2];
+      if (r >= p[1] && r <= p[2]) dln[0] = -std::log(r / r0);
+      break;
+    }
+  }
+  for (int k = 0; k < 3; ++k) grad[k] = u * dln[k];
+  return u;
+}
+
 }  // namespace sb

@@ -33,4 +33,10 @@ int64_t band_upper(int index);
 bool validate_distribution(int kind, const double* p, std::string* msg);
 double density(int kind, const double* p, double r);
 
+// The number of a distribution kind's parameters (ensemble/mod.rs:254-337) and the gradient of
+// u(r) along them at a fixed reference radius (distribution.rs:370-441); the reference radius'
+// own dependence cancels in every average. Returns u(r).
+int parameter_count(int kind);
+double density_gradient(int kind, const double* p, double r, double grad[3]);
+
 }  // namespace sb

@@ -32,6 +32,19 @@ __device__ __forceinline__ void elements4(double s1r, double s1i, double s2r, do
   e[3] = s2i * s1r - s2r * s1i;
 }
 
+// element_derivatives (scatrs/src/mie/phase.rs:62-73): the elements' derivatives for amplitude
+// derivatives (D1, D2).
+__device__ __forceinline__ void element_derivs4(double s1r, double s1i, double s2r, double s2i,
+                                                double d1r, double d1i, double d2r, double d2i,
+                                                double e[4]) {
+  const double r1 = s1r * d1r + s1i * d1i;
+  const double r2 = s2r * d2r + s2i * d2i;
+  e[0] = r1 + r2;
+  e[1] = r2 - r1;
+  e[2] = (d2r * s1r + d2i * s1i) + (s2r * d1r + s2i * d1i);
+  e[3] = (d2i * s1r - d2r * s1i) + (s2i * d1r - s2r * d1i);
+}
+
 // The band of a chunk with n terms: the index of bucket(n) in 1, 2, 3, 4, 5, 7, ... (each the
 // ceiling of 1.25 times the last; engine.rs:951-957).
 __device__ __forceinline__ int band_of(int n) {
@@ -47,6 +60,7 @@ struct Smem {
   double a[2][2][KB][TR];  // [stage][G_E, G_O][order][row]
   double xs[2][KB][128];   // [stage][order][4 columns x 32 nodes]
   double w[32], cu[32], area[32], sc[32];
+  double wth[3][32];  // the distribution parameters' weights (derivatives only)
   double S[8];
   int slot;
 };
@@ -129,6 +143,27 @@ __device__ __forceinline__ void gemm_tile(Smem& sm, const double* __restrict__ g
   __syncthreads();  // the stage buffers are free for the next tile
 }
 
+// Sums of p[32] over the 16 threads sharing a row group, scattered: thread ng ends with the
+// sums of entries 2 ng and 2 ng + 1 in v. At offset o a lane keeps the lower half of its values
+// if (ng & o) == 0.
+__device__ __forceinline__ void reduce_scatter16(double p[32], double v[2]) {
+  const int ng = threadIdx.x & 15;
+#pragma unroll
+  for (int lvl = 0, o = 8, h = 16; lvl < 4; ++lvl, o >>= 1, h >>= 1) {
+    const bool lower = (ng & o) == 0;
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      if (i < h) {
+        const double mine = lower ? p[i] : p[i + h];
+        const double other = lower ? p[i + h] : p[i];
+        p[i] = mine + __shfl_xor_sync(0xffffffffu, other, o);
+      }
+    }
+  }
+  v[0] = p[0];
+  v[1] = p[1];
+}
+
 // The elements at +mu and -mu of this thread's 4 rows for its 2 spheres, scaled and weighted,
 // summed over the chunk's 32 spheres by a reduce-scatter over the 16 threads sharing the rows:
 // thread ng ends with v[0], v[1] of side ng >> 3 (0: +mu, 1: -mu), row (ng >> 1) & 3 and
@@ -167,35 +202,68 @@ __device__ __forceinline__ void chunk_elements(const Smem& sm, const double accE
       }
     }
   }
-  // Reduce-scatter: at offset o the lane keeps the lower half of its values if (ng & o) == 0.
+  reduce_scatter16(p, v);
+}
+
+// The derivative blocks' elements of this thread's 4 rows for its one sphere (node
+// 16 half + ng; accumulator columns 0-3 its (u, v) sums, 4-7 those of (du/dm, dv/dm)), for
+// block blk: values (weight w), the distribution's parameters (their weights), Re m and Im m
+// (weight w, the element derivatives along dS/dm and i dS/dm; phase.rs:322-335), reduced over
+// the 16 spheres as chunk_elements does.
+template <bool kUser>
+__device__ __forceinline__ void chunk_elements_d(const Smem& sm, const double accE[4][8],
+                                                 const double accO[4][8], int half, int blk,
+                                                 int n_theta, double v[2]) {
+  const int ng = threadIdx.x & 15;
+  const int node = 16 * half + ng;
+  const int kind = blk == 0 ? 0 : (blk <= n_theta ? 0 : blk - n_theta);  // 0 f, 1 Re m, 2 Im m
+  const double wt = (blk >= 1 && blk <= n_theta) ? sm.wth[blk - 1][node] : sm.w[node];
+  const double cu = sm.cu[node], ar = sm.area[node], sc = sm.sc[node];
+  double p[32];
 #pragma unroll
-  for (int lvl = 0, o = 8, h = 16; lvl < 4; ++lvl, o >>= 1, h >>= 1) {
-    const bool lower = (ng & o) == 0;
+  for (int r = 0; r < 4; ++r) {
 #pragma unroll
-    for (int i = 0; i < 16; ++i) {
-      if (i < h) {
-        const double mine = lower ? p[i] : p[i + h];
-        const double other = lower ? p[i + h] : p[i];
-        p[i] = mine + __shfl_xor_sync(0xffffffffu, other, o);
+    for (int sd = 0; sd < 2; ++sd) {
+      const double sg = sd == 0 ? 1.0 : -1.0;
+      const double s1r = accE[r][0] + sg * accO[r][2], s1i = accE[r][1] + sg * accO[r][3];
+      const double s2r = accE[r][2] + sg * accO[r][0], s2i = accE[r][3] + sg * accO[r][1];
+      double e[4];
+      if (kind == 0) {
+        elements4(s1r, s1i, s2r, s2i, e);
+      } else {
+        double d1r = accE[r][4] + sg * accO[r][6], d1i = accE[r][5] + sg * accO[r][7];
+        double d2r = accE[r][6] + sg * accO[r][4], d2i = accE[r][7] + sg * accO[r][5];
+        if (kind == 2) {
+          const double t1 = d1r, t2 = d2r;
+          d1r = -d1i;
+          d1i = t1;
+          d2r = -d2i;
+          d2i = t2;
+        }
+        element_derivs4(s1r, s1i, s2r, s2i, d1r, d1i, d2r, d2i, e);
       }
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        p[sd * 16 + r * 4 + k] = kUser ? wt * ((cu * e[k]) * ar) : wt * (sc * e[k]);
     }
   }
-  v[0] = p[0];
-  v[1] = p[1];
+  reduce_scatter16(p, v);
 }
 
 }  // namespace
 
-// K-b and K-c: each work item runs its row tiles of every chunk of its unit and adds the
-// reduced tiles into the unit's accumulators. Every output sum is owned by one thread of one
-// work item and runs over the chunks in order, so the results do not depend on how a unit's
-// tiles are split into work items.
-__global__ void __launch_bounds__(NT) unit_kernel(UnitArgs a) {
+template <bool kDeriv>
+__device__ __forceinline__ void unit_body(const UnitArgs& a) {
   __shared__ __align__(16) Smem sm;
   const int t = threadIdx.x, rg = t >> 4, ng = t & 15;
   // This thread's share of a reduced tile: side (+mu, -mu), row, two elements.
   const int side = ng >> 3, rr = (ng >> 1) & 3, e0 = 2 * (ng & 1);
   const int t_user = (a.h_u + TR - 1) / TR;
+  // Blocks of sums: the values, then (with derivatives) each distribution parameter, Re m and
+  // Im m; halves: a chunk's coefficient rows are one 32-node tile, or two of 16 nodes with
+  // their derivative columns.
+  const int n_blk = kDeriv ? 3 + a.n_theta : 1;
+  constexpr int kHalves = kDeriv ? 2 : 1;
   for (;;) {
     if (t == 0) sm.slot = atomicAdd(a.work_counter, 1);
     __syncthreads();
@@ -218,6 +286,7 @@ __global__ void __launch_bounds__(NT) unit_kernel(UnitArgs a) {
       if (t < 32) {
         const int j = c * 32 + t;
         double w = 0.0, cu = 0.0, ar = 0.0, sc = 0.0;
+        double wth[3] = {0.0, 0.0, 0.0};
         if (j < a.n_nodes) {
           const double r = a.radius[d * a.n_nodes + j];
           const double x = 2.0 * kPi * r / lam;
@@ -225,44 +294,64 @@ __global__ void __launch_bounds__(NT) unit_kernel(UnitArgs a) {
           cu = 4.0 / (x * x);
           ar = kPi * r * r;
           sc = 4.0 / (x * x) * (kPi * r * r);
+          if (kDeriv)
+            for (int p = 0; p < a.n_theta; ++p) wth[p] = a.wtheta[(d * a.n_nodes + j) * 3 + p];
         }
         sm.w[t] = w;
         sm.cu[t] = cu;
         sm.area[t] = ar;
         sm.sc[t] = sc;
+        if (kDeriv)
+          for (int p = 0; p < 3; ++p) sm.wth[p][t] = wth[p];
       }
       __syncthreads();
-      const double* xc = a.X + a.chunk_row[ci] * 128;
-      double accE[4][8], accO[4][8], v[2];
-      for (int tile = it.group; tile < t_user + t_band; tile += it.n_groups) {
-        if (tile < t_user) {
-          const int r0 = tile * TR;
-          gemm_tile(sm, a.ge_u, a.go_u, a.h_u_pad, r0, nc, xc, accE, accO);
-          chunk_elements<true>(sm, accE, accO, v);
-          const int row = r0 + rg * 4 + rr;
-          if (row < a.h_u) {
-            const int2 mp = a.user_map[row];
-            const int j = side ? mp.y : mp.x;
-            if (j >= 0) {
-              acc_user[e0 * a.n_mu + j] += v[0];
-              acc_user[(e0 + 1) * a.n_mu + j] += v[1];
+      for (int half = 0; half < kHalves; ++half) {
+        const double* xc = a.X + (a.chunk_row[ci] + (int64_t)half * nc) * 128;
+        double accE[4][8], accO[4][8], v[2];
+        for (int tile = it.group; tile < t_user + t_band; tile += it.n_groups) {
+          if (tile < t_user) {
+            const int r0 = tile * TR;
+            gemm_tile(sm, a.ge_u, a.go_u, a.h_u_pad, r0, nc, xc, accE, accO);
+            const int row = r0 + rg * 4 + rr;
+            int j = -1;
+            if (row < a.h_u) {
+              const int2 mp = a.user_map[row];
+              j = side ? mp.y : mp.x;
             }
-          }
-        } else {
-          const BandDesc B = a.bands[b];
-          const int q = B.n_q, lo = q / 2;
-          const int r0 = (tile - t_user) * TR;
-          double* acc_band = a.acc + a.chunk_acc[ci];
-          gemm_tile(sm, a.band_ge + B.g_off, a.band_go + B.g_off, B.h_pad, r0, nc, xc, accE,
-                    accO);
-          chunk_elements<false>(sm, accE, accO, v);
-          const int row = r0 + rg * 4 + rr;
-          if (row < B.h) {
-            const int jn = lo + row, mirror = q - 1 - jn;
-            const int j = side ? mirror : jn;
-            if (side == 0 || mirror != jn) {
-              acc_band[e0 * q + j] += v[0];
-              acc_band[(e0 + 1) * q + j] += v[1];
+            for (int blk = 0; blk < n_blk; ++blk) {
+              if (kDeriv)
+                chunk_elements_d<true>(sm, accE, accO, half, blk, a.n_theta, v);
+              else
+                chunk_elements<true>(sm, accE, accO, v);
+              if (j >= 0) {
+                double* au = acc_user + (int64_t)blk * 4 * a.n_mu;
+                au[e0 * a.n_mu + j] += v[0];
+                au[(e0 + 1) * a.n_mu + j] += v[1];
+              }
+            }
+          } else {
+            const BandDesc B = a.bands[b];
+            const int q = B.n_q, lo = q / 2;
+            const int r0 = (tile - t_user) * TR;
+            double* acc_band = a.acc + a.chunk_acc[ci];
+            gemm_tile(sm, a.band_ge + B.g_off, a.band_go + B.g_off, B.h_pad, r0, nc, xc, accE,
+                      accO);
+            const int row = r0 + rg * 4 + rr;
+            int j = -1;
+            if (row < B.h) {
+              const int jn = lo + row, mirror = q - 1 - jn;
+              if (side == 0 || mirror != jn) j = side ? mirror : jn;
+            }
+            for (int blk = 0; blk < n_blk; ++blk) {
+              if (kDeriv)
+                chunk_elements_d<false>(sm, accE, accO, half, blk, a.n_theta, v);
+              else
+                chunk_elements<false>(sm, accE, accO, v);
+              if (j >= 0) {
+                double* ab = acc_band + (int64_t)blk * 4 * q;
+                ab[e0 * q + j] += v[0];
+                ab[(e0 + 1) * q + j] += v[1];
+              }
             }
           }
         }
@@ -271,6 +360,17 @@ __global__ void __launch_bounds__(NT) unit_kernel(UnitArgs a) {
     }
   }
 }
+
+// K-b and K-c: each work item runs its row tiles of every chunk of its unit and adds the
+// reduced tiles into the unit's accumulators. Every output sum is owned by one thread of one
+// work item and runs over the chunks in order, so the results do not depend on how a unit's
+// tiles are split into work items.
+__global__ void __launch_bounds__(NT) unit_kernel(UnitArgs a) { unit_body<false>(a); }
+
+// The same with the derivative blocks: per chunk, its two 16-node halves in order; per tile,
+// every block's sums (values, distribution parameters, Re m, Im m), each into its own
+// accumulator (4 n_mu or 4 n_q doubles apart).
+__global__ void __launch_bounds__(NT) unit_deriv_kernel(UnitArgs a) { unit_body<true>(a); }
 
 // K-d: the Greek coefficients of each band slot, (2l+1)/2 sum_k w_k F(mu_k) d_l(mu_k) with F
 // the slot's averaged tables (fast.rs:238-253): a contraction over the band's n_q nodes shared
@@ -302,9 +402,13 @@ __global__ void __launch_bounds__(PT) proj_kernel(ProjArgs a) {
       int64_t off = -1;
       if (t < it.count) {
         const BandSlot bs = a.slots[a.slot_index[it.first + t]];
-        double z = 0.0;
-        for (int c = 0; c < a.cpu; ++c) z += a.chunk_sums[((int64_t)bs.unit * a.cpu + c) * 8];
-        rz = 1.0 / z;
+        if (a.raw) {
+          rz = 1.0;
+        } else {
+          double z = 0.0;
+          for (int c = 0; c < a.cpu; ++c) z += a.chunk_sums[((int64_t)bs.unit * a.cpu + c) * 8];
+          rz = 1.0 / z;
+        }
         off = bs.off;
       }
       sm.rz[t] = rz;
@@ -455,6 +559,147 @@ __global__ void __launch_bounds__(NT) final_kernel(FinalArgs a) {
   }
 }
 
+// The outputs and their derivatives per unit. Blocks b of the sums S_b (b = 0 the values,
+// 1..P_theta the distribution's parameters, then Re m and Im m): the averages v = S_0/Z, along a
+// parameter (S_p - v Z_p)/Z, along m S_m/Z (engine.rs:1782-1836); the ratios and the
+// normalizations with the quotient rule of ensemble/lin.rs; the Greek coefficients from each
+// block's projected raw sums, averaged the same way (the projection is linear).
+__global__ void __launch_bounds__(NT) final_deriv_kernel(FinalArgs a) {
+  __shared__ double S[6][8];
+  __shared__ double a0s[6];
+  const int t = threadIdx.x;
+  const int L = a.greek_order;
+  const int glen = L >= 0 ? L + 1 : 0;
+  const int64_t nu = a.n_units_total;
+  const int P = a.n_theta + 2, B = 1 + P, nth = a.n_theta;
+  for (int ul = blockIdx.x; ul < a.n_units; ul += gridDim.x) {
+    const int64_t unit = a.units[ul];
+    const int64_t d = unit / a.n_wl, i = unit % a.n_wl;
+    if (t < 8 * B) {
+      const int b = t / 8, k = t % 8;
+      double s = 0.0;
+      for (int c = 0; c < a.cpu; ++c)
+        s += a.chunk_sums[(((int64_t)ul * a.cpu + c) * B + b) * 8 + k];
+      S[b][k] = s;
+    }
+    __syncthreads();
+    const double z = S[0][0];
+    // An average and its derivatives from the raw sums s_b of one quantity.
+    auto avg = [&](const double* sb, int stride, double* out) {
+      const double v = sb[0] / z;
+      out[0] = v;
+      for (int p = 0; p < P; ++p) {
+        const double sp = sb[(1 + p) * stride];
+        out[1 + p] = p < nth ? (sp - v * S[1 + p][0]) / z : sp / z;
+      }
+    };
+    // x / y with derivatives (lin.rs Lin::div).
+    auto ldiv = [&](const double* x, const double* y, double* out) {
+      const double v = x[0] / y[0];
+      out[0] = v;
+      for (int p = 0; p < P; ++p) out[1 + p] = (x[1 + p] - v * y[1 + p]) / y[0];
+    };
+    const double* acc_user = a.acc + a.unit_acc[ul];
+    if (t == 0) {
+      double v[8][6];
+      for (int k = 0; k < 8; ++k) avg(&S[0][k], 8, v[k]);
+      const double ext = v[1][0], sca = v[2][0], back = v[5][0];
+      const bool bext = !(isfinite(ext) && ext != 0.0), bsca = !(isfinite(sca) && sca != 0.0);
+      const bool bback = !(isfinite(back) && back != 0.0);
+      if (bext || bsca || bback) {
+        unsigned long long key = ((unsigned long long)(i * a.n_dist + d) << 2) |
+                                 (unsigned long long)(bext ? 1 : (bsca ? 2 : 3));
+        atomicMin(a.err + 1, key);
+      }
+      double out[11][6];
+      for (int p = 0; p <= P; ++p) {
+        out[0][p] = v[1][p];
+        out[1][p] = v[2][p];
+        out[2][p] = v[4][p];
+        out[3][p] = v[5][p];
+        out[7][p] = 0.0;
+        out[9][p] = kPi * v[6][p];
+        out[10][p] = (4.0 * kPi / 3.0) * v[7][p];
+      }
+      ldiv(v[2], v[1], out[4]);
+      ldiv(v[3], v[2], out[5]);
+      ldiv(v[1], v[5], out[6]);
+      for (int p = 0; p <= P; ++p) out[6][p] *= 4.0 * kPi;
+      ldiv(v[7], v[6], out[8]);
+      for (int k = 0; k < 11; ++k) {
+        a.values[k * nu + unit] = out[k][0];
+        for (int p = 0; p < P; ++p) a.d_values[((int64_t)p * 11 + k) * nu + unit] = out[k][1 + p];
+      }
+    }
+    double sca[6];
+    {
+      double v[6];
+      avg(&S[0][2], 8, v);
+      for (int p = 0; p <= P; ++p) sca[p] = v[p];
+    }
+    if (a.phase) {
+      const int64_t blk = 4 * (int64_t)a.n_mu;
+      for (int j = t; j < a.n_mu; j += NT) {
+        double f[4][6];
+        for (int e = 0; e < 4; ++e) {
+          avg(acc_user + e * a.n_mu + j, (int)blk, f[e]);
+          if (a.normalized) {
+            double o[6];
+            ldiv(f[e], sca, o);
+            for (int p = 0; p <= P; ++p) f[e][p] = o[p];
+          }
+        }
+        const int src[6] = {0, 1, 0, 2, 3, 2};
+        for (int e = 0; e < 6; ++e) {
+          a.phase[((int64_t)e * nu + unit) * a.n_mu + j] = f[src[e]][0];
+          for (int p = 0; p < P; ++p)
+            a.d_phase[(((int64_t)p * 6 + e) * nu + unit) * a.n_mu + j] = f[src[e]][1 + p];
+        }
+      }
+    }
+    if (glen > 0 && a.greek) {
+      // The unit's slots are B consecutive entries (one per block) per band, bands ascending.
+      const int2 sl = a.unit_slots[ul];
+      auto sum = [&](int b, int idx) {
+        const int e = idx / glen, l = idx % glen;
+        double g = 0.0;
+        for (int k = b; k < sl.y; k += B) {
+          const BandSlot bs = a.slots[sl.x + k];
+          if (l <= a.bands[bs.band].order)
+            g += a.slot_greek[(int64_t)(sl.x + k) * 6 * glen + (int64_t)e * glen + l];
+        }
+        return g;
+      };
+      auto coeff = [&](int idx, double* out) {
+        double raw[6];
+        for (int b = 0; b < B; ++b) raw[b] = sum(b, idx);
+        avg(raw, 1, out);
+      };
+      if (t == 0) coeff(0, a0s);
+      __syncthreads();
+      for (int idx = t; idx < 6 * glen; idx += NT) {
+        const int e = idx / glen, l = idx % glen;
+        double c[6];
+        coeff(idx, c);
+        if (a.normalized) {
+          if (idx == 0) {
+            c[0] = 1.0;
+            for (int p = 0; p < P; ++p) c[1 + p] = 0.0;
+          } else {
+            double o[6];
+            ldiv(c, a0s, o);
+            for (int p = 0; p <= P; ++p) c[p] = o[p];
+          }
+        }
+        a.greek[((int64_t)e * nu + unit) * glen + l] = c[0];
+        for (int p = 0; p < P; ++p)
+          a.d_greek[(((int64_t)p * 6 + e) * nu + unit) * glen + l] = c[1 + p];
+      }
+    }
+    __syncthreads();
+  }
+}
+
 int unit_kernel_blocks_per_sm() {
   int n = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, unit_kernel, NT, 0);
@@ -462,7 +707,10 @@ int unit_kernel_blocks_per_sm() {
 }
 
 void launch_units(const UnitArgs& a, int grid, cudaStream_t s) {
-  unit_kernel<<<grid, NT, 0, s>>>(a);
+  if (a.deriv)
+    unit_deriv_kernel<<<grid, NT, 0, s>>>(a);
+  else
+    unit_kernel<<<grid, NT, 0, s>>>(a);
 }
 
 void launch_proj(const ProjArgs& a, cudaStream_t s) {
@@ -481,7 +729,10 @@ void launch_proj(const ProjArgs& a, cudaStream_t s) {
 
 void launch_final(const FinalArgs& a, cudaStream_t s) {
   int grid = a.n_units < 4096 ? a.n_units : 4096;
-  final_kernel<<<grid, NT, 0, s>>>(a);
+  if (a.d_values)
+    final_deriv_kernel<<<grid, NT, 0, s>>>(a);
+  else
+    final_kernel<<<grid, NT, 0, s>>>(a);
 }
 
 }  // namespace sb
