@@ -3,11 +3,15 @@ the GPU library.
 
 * ``ensemble_parameters(items, mixture)``: the parameter names of ensemble.rs:172-188.
 * ``ensemble_compute_fixed(specs, particle_spec, wavelengths, greek, all_orders, mu,
-  normalized, n_nodes, spread, allow_unvalidated)``: the batch call of ensemble.rs:455-504 on a
-  fixed size grid, returning the same dict (values/errors (11, n), d/d_errors (0, 11, n),
-  greek* (6, n, L + 1), phase* (6, n, n_mu), converged (n), panels (n)), rows
-  distribution-major. The particle spec is ("sphere", m) with m of shape (n_wl,) as in the
-  reference, or (n_dist, n_wl) for a refractive index per distribution and wavelength.
+  normalized, n_nodes, spread, allow_unvalidated, ranges, derivatives)``: the batch call of
+  ensemble.rs:455-504 on a fixed size grid, returning the same dict (values/errors (11, n),
+  d/d_errors (k, 11, n), greek* (6, n, L + 1) and (k, 6, n, L + 1), phase* (6, n, n_mu) and
+  (k, 6, n, n_mu), converged (n), panels (n)), rows distribution-major. The particle spec is
+  ("sphere", m) with m of shape (n_wl,) as in the reference, or (n_dist, n_wl) for a
+  refractive index per distribution and wavelength; or ("layered", fractions, m) with
+  fractions (L - 1,) and m (L, n_wl) as in the reference, or per distribution (n_dist, L - 1)
+  and (n_dist, L, n_wl). ``derivatives`` are indices into ensemble_parameters (the
+  reference's deriv_idx, ensemble.rs:295-311), computed in forward mode like the reference's.
 
 Errors are those of the reference's Python package (scatrs_b200.errors).
 """
@@ -92,29 +96,57 @@ def _dist_array(specs, spread: float, ranges=None) -> np.ndarray:
 
 def ensemble_compute_fixed(specs, particle_spec, wavelengths, greek, all_orders, mu, normalized,
                            n_nodes: int = 256, spread: float = 5.0, allow_unvalidated=False,
-                           ranges=None) -> dict:
-    if not isinstance(particle_spec, tuple) or particle_spec[0] != "sphere":
-        raise TypeError("the fixed-grid ensemble takes ('sphere', m)")
+                           ranges=None, derivatives=()) -> dict:
+    """The batch dict on a fixed grid. ``derivatives`` selects parameters by their index in
+    ``ensemble_parameters([(specs[0], particle_spec, 1.0)], False)`` (the reference's
+    ``deriv_idx``); they need homogeneous spheres and every distribution of one kind."""
+    if not isinstance(particle_spec, tuple) or particle_spec[0] not in ("sphere", "layered"):
+        raise TypeError("the fixed-grid ensemble takes ('sphere', m) or ('layered', fractions, m)")
     if all_orders:
         raise InvalidInputError("the fixed-grid ensemble needs a finite Greek order")
     wl = np.ascontiguousarray(wavelengths, dtype=np.float64).reshape(-1)
     dists = _dist_array(specs, spread, ranges)
-    m = np.asarray(particle_spec[1], dtype=np.complex128)
-    if m.ndim == 1:
-        m = np.broadcast_to(m, (dists.size, wl.size))
     mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
     L = -1 if greek is None else int(greek)
-    values, phase, g = _native.ensemble_fixed(dists, wl, m, mu, n_nodes, L, bool(normalized),
-                                              bool(allow_unvalidated))
+    derivatives = [int(k) for k in derivatives]
+    d = dp = dg = None
+    if particle_spec[0] == "layered":
+        if derivatives:
+            raise InvalidInputError("derivatives of layered spheres are not on the fixed grid")
+        fr = np.asarray(particle_spec[1], dtype=np.float64).reshape(-1)
+        ml = np.asarray(particle_spec[2], dtype=np.complex128)
+        if ml.ndim == 2:  # (L, n_wl): the same particle for every distribution
+            ml = np.broadcast_to(ml, (dists.size,) + ml.shape)
+            fr = np.broadcast_to(fr, (dists.size, fr.size))
+        values, phase, g = _native.ensemble_fixed_layered(dists, wl, fr, ml, mu, n_nodes, L,
+                                                          bool(normalized),
+                                                          bool(allow_unvalidated))
+    else:
+        m = np.asarray(particle_spec[1], dtype=np.complex128)
+        if m.ndim == 1:
+            m = np.broadcast_to(m, (dists.size, wl.size))
+        if derivatives:
+            names = ensemble_parameters([(specs[0], particle_spec, 1.0)], False)
+            for k in derivatives:
+                if not 0 <= k < len(names):
+                    raise InvalidInputError(f"derivative index {k} out of range of {names}")
+            values, phase, g, d, dp, dg = _native.ensemble_fixed_d(
+                dists, wl, m, mu, n_nodes, L, bool(normalized), bool(allow_unvalidated))
+            d, dp, dg = (None if a is None else np.ascontiguousarray(a[derivatives])
+                         for a in (d, dp, dg))
+        else:
+            values, phase, g = _native.ensemble_fixed(dists, wl, m, mu, n_nodes, L,
+                                                      bool(normalized), bool(allow_unvalidated))
     n = values.shape[1]
-    out = {"values": values, "errors": np.zeros_like(values), "d": np.zeros((0, 11, n)),
-           "d_errors": np.zeros((0, 11, n))}
-    for prefix, arr in (("greek", g), ("phase", phase)):
+    k = len(derivatives)
+    out = {"values": values, "errors": np.zeros_like(values),
+           "d": d if d is not None else np.zeros((0, 11, n)), "d_errors": np.zeros((k, 11, n))}
+    for prefix, arr, darr in (("greek", g, dg), ("phase", phase, dp)):
         if arr is not None:
             out[prefix] = arr
             out[f"{prefix}_errors"] = np.zeros_like(arr)
-            out[f"{prefix}_d"] = np.zeros((0,) + arr.shape)
-            out[f"{prefix}_d_errors"] = np.zeros((0,) + arr.shape)
+            out[f"{prefix}_d"] = darr if darr is not None else np.zeros((0,) + arr.shape)
+            out[f"{prefix}_d_errors"] = np.zeros((k,) + arr.shape)
     out["converged"] = np.ones(n, dtype=bool)
     out["panels"] = np.zeros(n, dtype=np.uint64)
     return out

@@ -105,3 +105,41 @@ def test_errors_are_the_reference_classes():
     with pytest.raises(O.OracleError) as e:
         _fixed(w)
     assert e.value.status == 3 and "at wavelength" in str(e.value)
+
+
+def test_autograd_backward_contracts_the_jacobian(monkeypatch):
+    """The torch wrapper's backward pass is J^T g over every output of each unit, summed over
+    the wavelengths for the distribution parameters (a fake forward with a known Jacobian)."""
+    import torch
+
+    from scatrs_b200 import _native, autograd
+
+    rng = np.random.default_rng(3)
+    n_dist, n_wl, n_mu, L = 2, 3, 4, 5
+    n = n_dist * n_wl
+    P = 4
+    jv, jp, jg = (rng.normal(size=s) for s in ((P, 11, n), (P, 6, n, n_mu), (P, 6, n, L + 1)))
+
+    def fake(dists, wl, m, mu, n_nodes, greek_order, normalized, allow):
+        th = dists["param"][:, :2]
+        x = np.concatenate([np.repeat(th, n_wl, axis=0).T, m.real.reshape(1, -1),
+                            m.imag.reshape(1, -1)])  # (P, n)
+        v = np.einsum("pkn,pn->kn", jv, x)
+        ph = np.einsum("pknj,pn->knj", jp, x)
+        g = np.einsum("pknj,pn->knj", jg, x)
+        return v, ph, g, jv, jp, jg
+
+    monkeypatch.setattr(_native, "ensemble_fixed_d", fake)
+    theta = torch.tensor(rng.uniform(0.1, 2, (n_dist, 2)), requires_grad=True)
+    m_re = torch.tensor(rng.uniform(1.3, 1.6, (n_dist, n_wl)), requires_grad=True)
+    m_im = torch.tensor(rng.uniform(0, 0.1, (n_dist, n_wl)), requires_grad=True)
+    v, ph, g = autograd.ensemble_fixed(theta, m_re, m_im, kind="lognormal",
+                                       ranges=[[0.01, 1.0]] * n_dist, wavelengths=[0.4, 0.5, 0.6],
+                                       mu=np.zeros(n_mu), greek_order=L)
+    wv, wp, wg = (torch.tensor(rng.normal(size=t.shape)) for t in (v, ph, g))
+    ((v * wv).sum() + (ph * wp).sum() + (g * wg).sum()).backward()
+    tot = (np.einsum("pkn,kn->pn", jv, wv.numpy()) + np.einsum("pknj,knj->pn", jp, wp.numpy())
+           + np.einsum("pknj,knj->pn", jg, wg.numpy())).reshape(P, n_dist, n_wl)
+    assert np.allclose(theta.grad.numpy(), tot[:2].sum(axis=2).T)
+    assert np.allclose(m_re.grad.numpy(), tot[2])
+    assert np.allclose(m_im.grad.numpy(), tot[3])
