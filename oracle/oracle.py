@@ -268,3 +268,55 @@ def ensemble_fixed_d(dists: np.ndarray, wavelengths, m, n_nodes: int, mu=None,
     if greek is not None:
         out["greek"], out["d_greek"] = greek, d_greek
     return out
+
+
+MONODISPERSE = 5
+
+
+def ensemble_adaptive(dists: np.ndarray, wavelengths, m, mu=None, greek_order=None,
+                      normalized: bool = True, rtol: float = 1e-6, max_panels: int = 4096,
+                      allow_unvalidated: bool = False, refine_backscatter: bool = False,
+                      batch: bool = False, threads: int = 0) -> dict:
+    """The reference's adaptive ensemble of spheres (m per wavelength): every distribution on
+    its own (batch=False) or as one batch sharing panels (batch=True). Distribution kinds as
+    DIST_DTYPE, plus MONODISPERSE (p[0] the radius); r_lo, r_hi unused. Returns values,
+    errors, phase(_err), greek(_err), converged, panels; units distribution-major."""
+    dists = np.ascontiguousarray(dists, dtype=DIST_DTYPE)
+    wl = np.ascontiguousarray(wavelengths, dtype=np.float64).reshape(-1)
+    m = np.ascontiguousarray(np.broadcast_to(np.asarray(m, dtype=np.complex128), wl.shape))
+    mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
+    n = dists.size * wl.size
+    L = -1 if greek_order is None else int(greek_order)
+    out = {"values": np.zeros((11, n)), "errors": np.zeros((11, n)),
+           "converged": np.zeros(n, dtype=np.int8), "panels": np.zeros(n, dtype=np.int64)}
+    ph = pe = g = ge = None
+    if mu.size:
+        ph, pe = np.zeros((6, n, mu.size)), np.zeros((6, n, mu.size))
+    if L >= 0:
+        g, ge = np.zeros((6, n, L + 1)), np.zeros((6, n, L + 1))
+    err = ctypes.create_string_buffer(512)
+    f = lib().orc_ensemble_adaptive
+    f.argtypes = [ctypes.c_void_p, _I64, ctypes.c_int, _PD, _I64, _PD, _PD, _I64, _I64,
+                  ctypes.c_int, _D, _I64, ctypes.c_int, ctypes.c_int, ctypes.c_int, _PD, _PD,
+                  _PD, _PD, _PD, _PD, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_char_p, _I64]
+    st = f(dists.ctypes.data, dists.size, int(batch), _p(wl), wl.size,
+           _p(m.view(np.float64).reshape(-1)), _p(mu), mu.size, L, int(normalized), rtol,
+           max_panels, int(allow_unvalidated), int(refine_backscatter), threads,
+           _p(out["values"]), _p(out["errors"]), _p(ph), _p(pe), _p(g), _p(ge),
+           out["converged"].ctypes.data, out["panels"].ctypes.data, err, 512)
+    if st != 0:
+        raise OracleError(st, err.value.decode())
+    out["converged"] = out["converged"].astype(bool)
+    if ph is not None:
+        out["phase"], out["phase_err"] = ph, pe
+    if g is not None:
+        out["greek"], out["greek_err"] = g, ge
+    return out
+
+
+def dist(kind: int, *params) -> np.ndarray:
+    """One distribution record (kind as DIST_DTYPE's, or MONODISPERSE)."""
+    d = np.zeros(1, dtype=DIST_DTYPE)
+    d["kind"] = kind
+    d["p"][0, :len(params)] = params
+    return d

@@ -1,0 +1,1020 @@
+// TEST INFRASTRUCTURE ONLY: the reference's adaptive ensemble engine restated on the CPU, the
+// oracle of the GPU adaptive path. Spheres; distributions with unbounded support (lognormal,
+// gamma, modified gamma), finite support (power law) or a single radius (monodisperse); one
+// distribution per call (`compute`, ensemble/mod.rs:548-606) or a batch sharing panels
+// (`compute_batch`, mod.rs:613-686). Values and error estimates; no derivatives.
+//
+//   ensemble/kronrod.rs   GK15 panels                     (gk_panel)
+//   ensemble/range.rs     tail cut-offs                   (masses, cutoffs)
+//   ensemble/moments.rs   Z, <r^2>, <r^3>                 (moments)
+//   ensemble/engine.rs    parts 141-233, initial_panels 301-354, quantities1/panel1 369-560,
+//                         status 620-720, pass1 724-924, panel_terms 961-978, pass2 1363-1766,
+//                         averages 1782-1836, monodisperse 1838-1890, wavelength 1964-2250,
+//                         project 2310-2355, assemble 2396-2497
+//   ensemble/lin.rs       error propagation through the ratios (Lin)
+#include "oracle_core.hpp"
+
+#include <omp.h>
+
+#include <algorithm>
+#include <array>
+#include <cstdio>
+#include <cstring>
+#include <functional>
+#include <limits>
+#include <set>
+#include <string>
+#include <vector>
+
+using namespace orc;
+
+namespace {
+
+constexpr double STEP = 0.5;
+constexpr int MAX_STEPS = 400;
+constexpr int MAX_EXTENSIONS = 100;
+constexpr double MIN_WIDTH = 1e-10;
+constexpr double MAX_DX = 20.0;
+constexpr size_t MOMENT_MAX_PANELS = 100000;
+constexpr int MONODISPERSE = 5;
+constexpr double INF = std::numeric_limits<double>::infinity();
+
+// Pass-1 quantities (engine.rs:43-54): 1, C_ext, C_sca, C_sca g, C_back, C_abs.
+constexpr int N_BASE = 6;
+constexpr int P1_ONE = 0, P1_EXT = 1, P1_SCA = 2, P1_SCAG = 3, P1_BACK = 4, P1_ABS = 5;
+// Pass-2 scalars (engine.rs:31-41).
+constexpr int S_ONE = 0, S_EXT = 1, S_SCA = 2, S_SCAG = 3, S_ABS = 4, S_BACK = 5, S_R2 = 6,
+              S_R3 = 7, SCALARS = 9;
+
+struct Failure {
+  int status;
+  std::string msg;
+};
+
+std::string at(double lambda, double r) {
+  char buf[160];
+  snprintf(buf, sizeof buf, "at wavelength %e, radius %e: ", lambda, r);
+  return buf;
+}
+
+// kronrod.rs:5-52.
+const double KN[8] = {0.9914553711208126, 0.9491079123427585, 0.8648644233597691,
+                      0.7415311855993944, 0.5860872354676911, 0.4058451513773972,
+                      0.20778495500789847, 0.0};
+const double KW[8] = {0.022935322010529225, 0.06309209262997855, 0.10479001032225018,
+                      0.14065325971552592,  0.1690047266392679,  0.1903505780647854,
+                      0.2044329400752989,   0.20948214108472783};
+const double GW[4] = {0.1294849661688697, 0.2797053914892767, 0.3818300505051189,
+                      0.4179591836734694};
+struct Node {
+  double t, wk, wg;
+};
+void gk_panel(double a, double b, Node out[15]) {
+  const double c = 0.5 * (a + b), h = 0.5 * (b - a);
+  for (int i = 0; i < 7; ++i) {
+    const double gauss = i % 2 == 1 ? h * GW[i / 2] : 0.0;
+    const double k = h * KW[i];
+    out[i] = {c - h * KN[i], k, gauss};
+    out[14 - i] = {c + h * KN[i], k, gauss};
+  }
+  out[7] = {c, h * KW[7], h * GW[3]};
+}
+
+double powk(double r, int k) { return k == 0 ? 1.0 : k == 2 ? r * r : r * r * r; }
+
+double max_step(const Density& d, double step) { return std::min(step, 0.5 * d.log_width); }
+
+// range.rs:25-36.
+void masses(const Density& d, double t0, double t1, const int* powers, int np, double* out) {
+  Node nd[15];
+  gk_panel(t0, t1, nd);
+  for (int k = 0; k < np; ++k) out[k] = 0.0;
+  for (auto& n : nd) {
+    const double r = std::exp(n.t);
+    const double wu = n.wk * r * density_eval(d, r, nullptr);
+    for (int k = 0; k < np; ++k) out[k] += wu * powk(r, powers[k]);
+  }
+}
+
+// range.rs:48-93.
+std::pair<double, double> cutoffs(const Density& d, double center, double eps,
+                                  std::vector<int> powers) {
+  const double t0 = std::log(center);
+  const double step = max_step(d, STEP);
+  const int np = (int)powers.size();
+  std::vector<double> total(np, 0.0);
+  double ends[2] = {t0, t0};
+  std::vector<double> last[2] = {std::vector<double>(np, INF), std::vector<double>(np, INF)};
+  bool done[2] = {false, false};
+  std::vector<double> mass(np);
+  for (int i = 0; i < MAX_STEPS; ++i) {
+    for (int side = 0; side < 2; ++side) {
+      if (done[side]) continue;
+      const double sign = side == 0 ? -1.0 : 1.0;
+      const double a = ends[side], b = a + sign * step;
+      masses(d, std::min(a, b), std::max(a, b), powers.data(), np, mass.data());
+      for (double m : mass)
+        if (!std::isfinite(m)) {
+          char buf[160];
+          snprintf(buf, sizeof buf,
+                   "the size distribution's density is not finite near r = %e", std::exp(b));
+          throw Failure{INVALID_INPUT, buf};
+        }
+      ends[side] = b;
+      bool small = i >= 1;
+      for (int k = 0; k < np; ++k) {
+        total[k] += mass[k];
+        const double q = mass[k] / last[side][k];
+        last[side][k] = mass[k];
+        small = small && (mass[k] == 0.0 || (q < 1.0 && mass[k] / (1.0 - q) <= eps * total[k]));
+      }
+      done[side] = small;
+    }
+    if (done[0] && done[1]) return {std::exp(ends[0]), std::exp(ends[1])};
+  }
+  throw Failure{INVALID_INPUT, "the size distribution is too broad: its tails do not decay"};
+}
+
+struct Moments {
+  double v[2], e[2], z, ez;
+};
+
+// moments.rs:62-167 (no derivative parameters).
+Moments moments(const Density& d, std::pair<double, double> range, double rtol,
+                double truncation) {
+  const double step = max_step(d, STEP);
+  const double t_lo = std::log(range.first), t_hi = std::log(range.second);
+  std::vector<std::pair<double, double>> panels;
+  {
+    const size_t n = (size_t)std::max(1.0, std::ceil((t_hi - t_lo) / step));
+    const double h = (t_hi - t_lo) / (double)n;
+    for (size_t i = 0; i < n; ++i) panels.push_back({t_lo + i * h, t_lo + (i + 1) * h});
+  }
+  auto finish = [&](const std::vector<std::array<double, 6>>& sums) {
+    double s[3] = {0, 0, 0}, e[3] = {0, 0, 0};
+    for (int j = 0; j < 3; ++j)
+      for (auto& p : sums) {
+        s[j] += p[j];
+        e[j] += p[3 + j];
+      }
+    const double z = s[0], ez = e[0];
+    if (!(std::isfinite(z) && z > 0.0))
+      throw Failure{INVALID_INPUT, "the size distribution has no finite positive mass on its range"};
+    Moments m;
+    m.z = z;
+    m.ez = ez;
+    for (int k = 0; k < 2; ++k) {
+      m.v[k] = s[1 + k] / z;
+      m.e[k] = (e[1 + k] + std::fabs(m.v[k]) * ez) / z + truncation * std::fabs(m.v[k]);
+    }
+    return m;
+  };
+  for (;;) {
+    std::vector<std::array<double, 6>> sums;  // Kronrod sums of 1, r^2, r^3, then |K - G|
+    for (auto& p : panels) {
+      Node nd[15];
+      gk_panel(p.first, p.second, nd);
+      double k[3] = {0, 0, 0}, g[3] = {0, 0, 0};
+      for (auto& n : nd) {
+        const double r = std::exp(n.t);
+        const double u = density_eval(d, r, nullptr);
+        const double q[3] = {1.0, r * r, r * r * r};
+        for (int j = 0; j < 3; ++j) {
+          k[j] += n.wk * u * r * q[j];
+          g[j] += n.wg * u * r * q[j];
+        }
+      }
+      sums.push_back({k[0], k[1], k[2], std::fabs(k[0] - g[0]), std::fabs(k[1] - g[1]),
+                      std::fabs(k[2] - g[2])});
+    }
+    double total[3] = {0, 0, 0}, terr[3] = {0, 0, 0}, target[3];
+    for (auto& s : sums)
+      for (int j = 0; j < 3; ++j) {
+        total[j] += s[j];
+        terr[j] += s[3 + j];
+      }
+    bool met = true;
+    for (int j = 0; j < 3; ++j) {
+      target[j] = rtol * std::fabs(total[j]);
+      met = met && terr[j] <= target[j];
+    }
+    const size_t n = panels.size();
+    if (met || n >= MOMENT_MAX_PANELS) return finish(sums);
+    std::vector<std::pair<double, double>> next;
+    for (size_t i = 0; i < n; ++i) {
+      bool bad = false;
+      for (int j = 0; j < 3; ++j)
+        bad = bad || (sums[i][3 + j] * (double)n > target[j] && terr[j] > target[j]);
+      const auto& p = panels[i];
+      if (bad && p.second - p.first > 1e-10) {
+        const double mid = 0.5 * (p.first + p.second);
+        next.push_back({p.first, mid});
+        next.push_back({mid, p.second});
+      } else {
+        next.push_back(p);
+      }
+    }
+    if (next.size() == n) return finish(sums);
+    panels.swap(next);
+  }
+}
+
+enum SupportKind { UNBOUNDED, FINITE, POINT };
+
+struct Part {
+  FixedDist dist;
+  Density den;
+  SupportKind support;
+  double s_a = 0, s_b = 0;  // center (unbounded), [lo, hi] (finite), radius (point)
+  std::pair<double, double> cut;
+  Moments mom{};
+};
+
+Part make_part(const FixedDist& d, double rtol) {
+  Part p;
+  p.dist = d;
+  if (d.kind == MONODISPERSE) {
+    p.den = prepare(LOGNORMAL, 1.0, 2.0, 0.0);  // unused
+    p.support = POINT;
+    p.s_a = d.p[0];
+    p.cut = {d.p[0], d.p[0]};
+    return p;
+  }
+  p.den = prepare(d.kind, d.p[0], d.p[1], d.p[2]);
+  if (d.kind == POWER_LAW) {
+    p.support = FINITE;
+    p.s_a = d.p[1];
+    p.s_b = d.p[2];
+    p.mom = moments(p.den, {p.s_a, p.s_b}, rtol, 0.0);
+    p.cut = {p.s_a, p.s_b};
+    return p;
+  }
+  // distribution.rs:272-290: lognormal about its median, gamma its effective radius,
+  // modified gamma its reference radius.
+  p.support = UNBOUNDED;
+  p.s_a = d.kind == LOGNORMAL ? d.p[0] : d.kind == GAMMA ? d.p[0] : p.den.reference;
+  p.cut = cutoffs(p.den, p.s_a, rtol / 10.0, {2});
+  const double eps = std::max(1e-3 * rtol, 1e-16);
+  auto wide = cutoffs(p.den, p.s_a, eps, {0, 2, 3});
+  p.mom = moments(p.den, wide, rtol, 0.2 * rtol);
+  return p;
+}
+
+double size_param(double r, double lambda) { return 2.0 * PI * r / lambda; }
+
+// engine.rs:301-354.
+std::vector<std::pair<double, double>> initial_panels(double t_lo, double t_hi, double lambda,
+                                                      const std::vector<double>& breaks,
+                                                      const std::function<double(double)>& step_of,
+                                                      size_t budget) {
+  std::vector<double> edges{t_lo};
+  for (double r : breaks) {
+    const double t = std::log(r);
+    if (t > t_lo && t < t_hi) edges.push_back(t);
+  }
+  edges.push_back(t_hi);
+  std::vector<std::pair<double, double>> out;
+  for (size_t e = 0; e + 1 < edges.size() && out.size() <= budget; ++e) {
+    double a = edges[e];
+    const double b = edges[e + 1];
+    while (a < b) {
+      const double x = size_param(std::exp(a), lambda);
+      const double step = std::min(step_of(a), std::log(1.0 + MAX_DX / x));
+      const double n = std::max(1.0, std::ceil((b - a) / step));
+      const double h = (b - a) / n;
+      const double next = (n <= 1.0 || a + h <= a) ? b : a + h;
+      out.push_back({a, next});
+      a = next;
+      if (out.size() > budget) break;
+    }
+  }
+  if (out.size() <= budget) return out;
+  const double width = t_hi - t_lo;
+  std::vector<std::pair<double, double>> equal;
+  for (size_t e = 0; e + 1 < edges.size(); ++e) {
+    const size_t n =
+        (size_t)std::max(1.0, std::floor((edges[e + 1] - edges[e]) / width * (double)budget));
+    const double h = (edges[e + 1] - edges[e]) / (double)n;
+    for (size_t i = 0; i < n; ++i)
+      equal.push_back({edges[e] + (double)i * h, edges[e] + (double)(i + 1) * h});
+  }
+  return equal;
+}
+
+struct Options {
+  double rtol;
+  size_t max_panels;
+  bool allow_unvalidated, refine_backscatter;
+};
+
+// A solved sphere at radius r, or a Failure with the node's context.
+void solve(double r, double lambda, cplx m, bool allow, MieState& st, int64_t* n_terms) {
+  const double x = size_param(r, lambda);
+  std::string msg;
+  int64_t n = 0;
+  const int s = check_inputs(x, m.re, m.im, 0, allow, &n, &msg);
+  if (s != OK) throw Failure{s, at(lambda, r) + msg};
+  st.solve(x, m, n, false);
+  *n_terms = n;
+}
+
+struct Sums1 {
+  double k[N_BASE], err[N_BASE], absv[N_BASE];
+  int64_t n_terms;
+  double edge[2][N_BASE];
+};
+
+// quantities1 + panel1 (engine.rs:369-560) for every part of a group.
+std::vector<Sums1> panel1(const std::vector<const Part*>& group, double a, double b,
+                          double lambda, cplx m, const Options& o) {
+  Node nd[15];
+  gk_panel(a, b, nd);
+  double q[15][N_BASE];
+  int64_t n_max = 0;
+  MieState st;
+  for (int i = 0; i < 15; ++i) {
+    const double r = std::exp(nd[i].t);
+    int64_t n;
+    solve(r, lambda, m, o.allow_unvalidated, st, &n);
+    n_max = std::max(n_max, n);
+    const Efficiencies e = efficiencies(st);
+    const double area = PI * r * r;
+    const double v[N_BASE] = {1.0,           area * e.q_ext,  area * e.q_sca,
+                              area * e.q_sca * e.g, area * e.q_back, area * e.q_abs};
+    for (int j = 0; j < N_BASE; ++j) q[i][j] = v[j];
+  }
+  std::vector<Sums1> out;
+  for (const Part* p : group) {
+    Sums1 s{};
+    double g[N_BASE] = {};
+    for (int i = 0; i < 15; ++i) {
+      const double r = std::exp(nd[i].t);
+      const double u = density_eval(p->den, r, nullptr);
+      const double base = u * r;
+      for (int j = 0; j < N_BASE; ++j) {
+        s.k[j] += nd[i].wk * base * q[i][j];
+        g[j] += nd[i].wg * base * q[i][j];
+        s.absv[j] += nd[i].wk * std::fabs(base * q[i][j]);
+        if (i == 0) s.edge[0][j] = base * q[i][j];
+        if (i == 14) s.edge[1][j] = base * q[i][j];
+      }
+    }
+    for (int j = 0; j < N_BASE; ++j) s.err[j] = std::fabs(s.k[j] - g[j]);
+    s.n_terms = n_max;
+    out.push_back(s);
+  }
+  return out;
+}
+
+struct Status {
+  double target[N_BASE], errors[N_BASE];
+  bool met;
+  bool small[2];
+};
+
+// engine.rs:620-720 (no Greek refinement, no derivatives).
+Status status(const std::vector<const Sums1*>& sums, const Options& o, double ext) {
+  Status s;
+  auto total = [&](int j) {
+    double t = 0.0;
+    for (auto* x : sums) t += x->k[j];
+    return t;
+  };
+  auto err = [&](int j) {
+    double t = 0.0;
+    for (auto* x : sums) t += x->err[j];
+    return t;
+  };
+  auto scale_of = [](int j) { return j == P1_ABS ? P1_EXT : j; };
+  const double c_sca = std::fabs(total(P1_SCA));
+  for (int j = 0; j < N_BASE; ++j) {
+    double scale;
+    if (j == P1_SCAG)
+      scale = c_sca;
+    else if (j == P1_BACK)
+      scale = std::max(std::fabs(total(P1_BACK)), c_sca);
+    else
+      scale = std::fabs(total(scale_of(j)));
+    s.target[j] = o.rtol * scale;
+  }
+  s.target[P1_ONE] = INF;
+  if (!o.refine_backscatter) s.target[P1_BACK] = INF;
+  s.met = true;
+  for (int j = 0; j < N_BASE; ++j) {
+    s.errors[j] = err(j);
+    s.met = s.met && s.errors[j] <= s.target[j];
+  }
+  auto small = [&](const double* density) {
+    for (int j = 0; j < N_BASE; ++j)
+      if (!(std::fabs(density[j]) * (ext / STEP) <= 0.1 * s.target[j])) return false;
+    return true;
+  };
+  s.small[0] = small(sums.front()->edge[0]);
+  s.small[1] = small(sums.back()->edge[1]);
+  return s;
+}
+
+struct Pass1 {
+  std::vector<std::pair<double, double>> panels;
+  std::vector<bool> converged;
+  int64_t n_terms = 0;
+};
+
+// engine.rs:724-924.
+Pass1 pass1(const std::vector<const Part*>& group, double lambda, cplx m, const Options& o) {
+  std::vector<double> breaks;
+  for (auto* p : group)
+    if (p->support == FINITE) {
+      breaks.push_back(p->s_a);
+      breaks.push_back(p->s_b);
+    }
+  std::sort(breaks.begin(), breaks.end());
+  breaks.erase(std::unique(breaks.begin(), breaks.end()), breaks.end());
+  double lo = INF, hi = 0.0;
+  for (auto* p : group) {
+    lo = std::min(lo, p->cut.first);
+    hi = std::max(hi, p->cut.second);
+  }
+  double t_lo = std::log(lo), t_hi = std::log(hi);
+  const double x_hi = size_param(hi, lambda);
+  if (x_hi > MAX_SIZE_PARAMETER) {
+    char buf[200];
+    snprintf(buf, sizeof buf,
+             "the integration range reaches size parameter %e, above the accepted %e", x_hi,
+             MAX_SIZE_PARAMETER);
+    throw Failure{INVALID_INPUT, at(lambda, hi) + buf};
+  }
+  const size_t np = group.size();
+  std::vector<bool> extendable(np);
+  std::vector<std::array<double, 3>> steps(np);
+  std::vector<double> exts(np);
+  for (size_t p = 0; p < np; ++p) {
+    extendable[p] = group[p]->support == UNBOUNDED;
+    steps[p] = {std::log(group[p]->cut.first), std::log(group[p]->cut.second),
+                max_step(group[p]->den, STEP)};
+    exts[p] = std::min(STEP, group[p]->den.log_width);
+  }
+  auto step_of = [&](double t) {
+    double s = STEP;
+    for (auto& st : steps)
+      if (st[0] <= t && t < st[1]) s = std::min(s, st[2]);
+    return s;
+  };
+  struct Panel {
+    std::pair<double, double> ab;
+    bool done = false;
+    std::vector<Sums1> sums;
+  };
+  std::vector<Panel> panels;
+  for (auto& ab : initial_panels(t_lo, t_hi, lambda, breaks, step_of, o.max_panels))
+    panels.push_back({ab, false, {}});
+  int extensions[2] = {0, 0};
+  for (;;) {
+    // Every panel, then the first error in order.
+    const int64_t n_pan = (int64_t)panels.size();
+    std::vector<Failure> fails(n_pan, Failure{OK, ""});
+    for (int64_t i = 0; i < n_pan; ++i) {
+      if (panels[i].done) continue;
+      try {
+        panels[i].sums = panel1(group, panels[i].ab.first, panels[i].ab.second, lambda, m, o);
+        panels[i].done = true;
+      } catch (const Failure& f) {
+        fails[i] = f;
+      }
+    }
+    for (auto& f : fails)
+      if (f.status != OK) throw f;
+    const size_t n = panels.size();
+    std::vector<Status> statuses;
+    for (size_t p = 0; p < np; ++p) {
+      std::vector<const Sums1*> sums;
+      for (auto& pn : panels) sums.push_back(&pn.sums[p]);
+      statuses.push_back(status(sums, o, exts[p]));
+    }
+    auto finish = [&]() {
+      Pass1 r;
+      for (auto& pn : panels) {
+        r.panels.push_back(pn.ab);
+        r.n_terms = std::max(r.n_terms, pn.sums.front().n_terms);
+      }
+      for (size_t p = 0; p < np; ++p)
+        r.converged.push_back(statuses[p].met &&
+                              (!extendable[p] || (statuses[p].small[0] && statuses[p].small[1])));
+      return r;
+    };
+    bool all_met = true;
+    for (auto& s : statuses) all_met = all_met && s.met;
+    if (all_met) {
+      auto wanting = [&](int end, double* ext, double* step) {
+        if (extensions[end] >= MAX_EXTENSIONS) return false;
+        bool any = false;
+        for (size_t p = 0; p < np; ++p)
+          if (extendable[p] && !statuses[p].small[end]) {
+            if (!any) {
+              *ext = exts[p];
+              *step = steps[p][2];
+            } else {
+              *ext = std::min(*ext, exts[p]);
+              *step = std::min(*step, steps[p][2]);
+            }
+            any = true;
+          }
+        return any;
+      };
+      double e0 = 0, s0 = 0, e1 = 0, s1 = 0;
+      const bool w0 = wanting(0, &e0, &s0), w1 = wanting(1, &e1, &s1);
+      bool extended = false;
+      if (w0) {
+        auto fresh = initial_panels(t_lo - e0, t_lo, lambda, {}, [&](double) { return s0; },
+                                    o.max_panels);
+        if (panels.size() + fresh.size() > o.max_panels) return finish();
+        t_lo -= e0;
+        extensions[0] += 1;
+        std::vector<Panel> nw;
+        for (auto& ab : fresh) nw.push_back({ab, false, {}});
+        for (auto& pn : panels) nw.push_back(std::move(pn));
+        panels.swap(nw);
+        extended = true;
+      }
+      if (w1) {
+        auto fresh = initial_panels(t_hi, t_hi + e1, lambda, {}, [&](double) { return s1; },
+                                    o.max_panels);
+        if (panels.size() + fresh.size() > o.max_panels) return finish();
+        t_hi += e1;
+        extensions[1] += 1;
+        for (auto& ab : fresh) panels.push_back({ab, false, {}});
+        extended = true;
+      }
+      if (!extended) return finish();
+      continue;
+    }
+    std::vector<std::pair<double, size_t>> cand;
+    for (size_t i = 0; i < n; ++i) {
+      if (!(panels[i].ab.second - panels[i].ab.first > MIN_WIDTH)) continue;
+      double bad = 0.0;
+      for (size_t p = 0; p < np; ++p)
+        for (int j = 0; j < N_BASE; ++j) {
+          if (!(statuses[p].errors[j] > statuses[p].target[j])) continue;
+          const double t = std::max(statuses[p].target[j], std::numeric_limits<double>::min());
+          bad = std::max(bad, panels[i].sums[p].err[j] * (double)n / t);
+        }
+      if (bad > 1.0) cand.push_back({bad, i});
+    }
+    const size_t budget = o.max_panels > n ? o.max_panels - n : 0;
+    if (cand.empty() || budget == 0) return finish();
+    std::sort(cand.begin(), cand.end(), [](const auto& x, const auto& y) {
+      return x.first != y.first ? x.first > y.first : x.second < y.second;
+    });
+    if (cand.size() > budget) cand.resize(budget);
+    std::vector<char> split(n, 0);
+    for (auto& c : cand) split[c.second] = 1;
+    std::vector<Panel> next;
+    for (size_t i = 0; i < n; ++i) {
+      if (split[i]) {
+        const double a = panels[i].ab.first, b = panels[i].ab.second, mid = 0.5 * (a + b);
+        next.push_back({{a, mid}, false, {}});
+        next.push_back({{mid, b}, false, {}});
+      } else {
+        next.push_back(std::move(panels[i]));
+      }
+    }
+    panels.swap(next);
+  }
+}
+
+// panel_terms (engine.rs:961-978).
+int64_t panel_terms(double a, double b, double lambda, cplx m, bool allow) {
+  Node nd[15];
+  gk_panel(a, b, nd);
+  int64_t most = 0;
+  for (auto& n : nd) {
+    const double r = std::exp(n.t);
+    std::string msg;
+    int64_t nt = 0;
+    const int s = check_inputs(size_param(r, lambda), m.re, m.im, 0, allow, &nt, &msg);
+    if (s != OK) throw Failure{s, at(lambda, r) + msg};
+    most = std::max(most, nt);
+  }
+  return most;
+}
+
+struct Layout {
+  int64_t n_mu = 0;
+  std::vector<BandData> bands;
+  std::vector<int64_t> start;
+  int64_t len = 0;
+  int band_of(int64_t n) const {
+    const int64_t u = bucket(n);
+    for (size_t b = 0; b < bands.size(); ++b)
+      if (bands[b].upper == u) return (int)b;
+    return -1;
+  }
+};
+
+// quantities2 (engine.rs:1025-1202) without derivatives: the scalars, the requested cosines'
+// tables (times the area) and the band's tables (fast.rs:95-205) of one solved sphere.
+void quantities2(const MieState& st, int64_t n, double r, double lambda, const Layout& L,
+                 const double* mu, int band, int64_t band_terms, double* g) {
+  const double x = size_param(r, lambda);
+  const Efficiencies q = efficiencies(st);
+  const double area = PI * r * r;
+  const double sc[SCALARS] = {1.0,           area * q.q_ext, area * q.q_sca, area * q.q_sca * q.g,
+                              area * q.q_abs, area * q.q_back, r * r,         r * r * r,
+                              0.0};
+  for (int k = 0; k < SCALARS; ++k) g[k] = sc[k];
+  const double cph = 4.0 / (x * x);
+  for (int64_t j = 0; j < L.n_mu; ++j) {
+    cplx s1 = real(0.0), s2 = real(0.0);
+    for_each_order(mu[j], n, [&](int64_t k, double pi, double tau) {
+      s1 = s1 + scale(st.a[k - 1], pi) + scale(st.b[k - 1], tau);
+      s2 = s2 + scale(st.a[k - 1], tau) + scale(st.b[k - 1], pi);
+    });
+    double e[4];
+    elements(s1, s2, e);
+    for (int t = 0; t < 4; ++t) g[SCALARS + t * L.n_mu + j] = cph * e[t] * area;
+  }
+  if (band < 0) return;
+  const BandData& B = L.bands[band];
+  double* out = g + L.start[band];
+  const int64_t qn = B.n_q, lo = qn / 2, h = qn - lo;
+  const int64_t terms = std::min(band_terms, B.upper);
+  const double scl = 4.0 / (x * x) * (PI * r * r);
+  for (int64_t ii = 0; ii < h; ++ii) {
+    double ce[4] = {0, 0, 0, 0}, co[4] = {0, 0, 0, 0};
+    for (int64_t k = 0; k < terms; ++k) {
+      double xr[4] = {0, 0, 0, 0};
+      if (k < n) {
+        const cplx uu = (k % 2 == 0) ? st.a[k] : st.b[k];
+        const cplx vv = (k % 2 == 0) ? st.b[k] : st.a[k];
+        xr[0] = uu.re;
+        xr[1] = uu.im;
+        xr[2] = vv.re;
+        xr[3] = vv.im;
+      }
+      const double ge = B.ge[ii * B.upper + k], go = B.go[ii * B.upper + k];
+      for (int t = 0; t < 4; ++t) {
+        ce[t] += ge * xr[t];
+        co[t] += go * xr[t];
+      }
+    }
+    const cplx eu = C(ce[0], ce[1]), ev = C(ce[2], ce[3]);
+    const cplx ou = C(co[0], co[1]), ov = C(co[2], co[3]);
+    const int64_t jn = lo + ii;
+    auto write = [&](int64_t node, double sign) {
+      double e[4];
+      elements(eu + scale(ov, sign), ev + scale(ou, sign), e);
+      for (int t = 0; t < 4; ++t) out[t * qn + node] = scl * e[t];
+    };
+    write(jn, 1.0);
+    const int64_t mirror = qn - 1 - jn;
+    if (mirror != jn) write(mirror, -1.0);
+  }
+}
+
+struct Lin {
+  double v, e;
+};
+Lin ldiv(Lin a, Lin b) {
+  const double v = a.v / b.v;
+  return {v, (a.e + std::fabs(v) * b.e) / std::fabs(b.v)};
+}
+Lin lscale(Lin a, double c) { return {c * a.v, std::fabs(c) * a.e}; }
+
+struct UnitOut {
+  double values[11], errors[11];
+  std::vector<double> phase, phase_err;  // 6 x n_mu
+  std::vector<double> greek, greek_err;  // 6 x (L + 1)
+  bool converged = true;
+  int64_t panels = 0;
+};
+
+// One wavelength (engine.rs:1964-2250): pass 1 per group, bands, pass 2, averages, a unit per
+// entry of `units` (each a list of parts with weight 1), the projection and the assembly.
+std::vector<UnitOut> wavelength(const std::vector<Part>& parts,
+                                const std::vector<std::vector<int>>& groups,
+                                const std::vector<std::vector<int>>& units, double lambda,
+                                cplx m, const double* mu, int64_t n_mu, int64_t order,
+                                bool normalized, const Options& o) {
+  std::vector<Pass1> firsts;
+  int64_t n_max = 0;
+  for (auto& g : groups) {
+    std::vector<const Part*> mem;
+    for (int p : g) mem.push_back(&parts[p]);
+    Pass1 p1;
+    if (mem[0]->support == POINT) {
+      const double r = mem[0]->s_a;
+      std::string msg;
+      int64_t nt = 0;
+      const int s = check_inputs(size_param(r, lambda), m.re, m.im, 0, o.allow_unvalidated,
+                                 &nt, &msg);
+      if (s != OK) throw Failure{s, at(lambda, r) + msg};
+      p1.converged = {true};
+      p1.n_terms = nt;
+    } else {
+      p1 = pass1(mem, lambda, m, o);
+    }
+    n_max = std::max(n_max, p1.n_terms);
+    firsts.push_back(std::move(p1));
+  }
+  std::vector<int> group_of(parts.size()), place(parts.size());
+  for (size_t gi = 0; gi < groups.size(); ++gi)
+    for (size_t k = 0; k < groups[gi].size(); ++k) {
+      group_of[groups[gi][k]] = (int)gi;
+      place[groups[gi][k]] = (int)k;
+    }
+  Layout L;
+  L.n_mu = n_mu;
+  L.len = SCALARS + 4 * n_mu;
+  if (order >= 0) {
+    std::set<int64_t> uppers;
+    for (size_t gi = 0; gi < groups.size(); ++gi) {
+      if (parts[groups[gi][0]].support == POINT) {
+        uppers.insert(bucket(firsts[gi].n_terms));
+        continue;
+      }
+      for (auto& ab : firsts[gi].panels)
+        uppers.insert(bucket(panel_terms(ab.first, ab.second, lambda, m, o.allow_unvalidated)));
+    }
+    for (int64_t u : uppers) {
+      L.bands.push_back(make_band(u, order));
+      L.start.push_back(L.len);
+      L.len += 4 * L.bands.back().n_q;
+    }
+  }
+  const int64_t len = L.len;
+  // Pass 2 and the averages of every part.
+  std::vector<std::vector<double>> av(parts.size()), ae(parts.size());
+  std::vector<double> g(len);
+  MieState st;
+  for (size_t gi = 0; gi < groups.size(); ++gi) {
+    const auto& grp = groups[gi];
+    if (parts[grp[0]].support == POINT) {
+      const double r = parts[grp[0]].s_a;
+      int64_t n;
+      solve(r, lambda, m, o.allow_unvalidated, st, &n);
+      std::fill(g.begin(), g.end(), 0.0);
+      const int band = order >= 0 ? L.band_of(n) : -1;
+      quantities2(st, n, r, lambda, L, mu, band, n, g.data());
+      av[grp[0]] = g;
+      ae[grp[0]].assign(len, 0.0);
+      continue;
+    }
+    const size_t np = grp.size();
+    std::vector<std::vector<double>> s(np, std::vector<double>(len, 0.0)),
+        e(np, std::vector<double>(len, 0.0));
+    for (auto& ab : firsts[gi].panels) {
+      const int64_t bt = order >= 0 ? panel_terms(ab.first, ab.second, lambda, m,
+                                                  o.allow_unvalidated)
+                                    : 0;
+      const int band = order >= 0 ? L.band_of(bt) : -1;
+      Node nd[15];
+      gk_panel(ab.first, ab.second, nd);
+      std::vector<std::vector<double>> vals(15, std::vector<double>(len, 0.0));
+      for (int i = 0; i < 15; ++i) {
+        const double r = std::exp(nd[i].t);
+        int64_t n;
+        solve(r, lambda, m, o.allow_unvalidated, st, &n);
+        quantities2(st, n, r, lambda, L, mu, band, bt, vals[i].data());
+      }
+      // The ranges the panel touches: the common part and its band's tables.
+      const int64_t common = SCALARS + 4 * n_mu;
+      const int64_t b_lo = band >= 0 ? L.start[band] : 0;
+      const int64_t b_hi = band >= 0 ? b_lo + 4 * L.bands[band].n_q : 0;
+      for (size_t p = 0; p < np; ++p) {
+        const Part& part = parts[grp[p]];
+        double wk[15], wg[15];
+        for (int i = 0; i < 15; ++i) {
+          const double r = std::exp(nd[i].t);
+          const double u = density_eval(part.den, r, nullptr);
+          wk[i] = nd[i].wk * (u * r);
+          wg[i] = nd[i].wg * (u * r);
+        }
+        auto add = [&](int64_t a, int64_t b) {
+          for (int64_t idx = a; idx < b; ++idx) {
+            double K = 0.0, G = 0.0;
+            for (int i = 0; i < 15; ++i) {
+              K += wk[i] * vals[i][idx];
+              G += wg[i] * vals[i][idx];
+            }
+            s[p][idx] += K;
+            e[p][idx] += std::fabs(K - G);
+          }
+        };
+        add(0, common);
+        add(b_lo, b_hi);
+      }
+    }
+    for (size_t p = 0; p < np; ++p) {
+      const Part& part = parts[grp[p]];
+      const double trunc = part.support == UNBOUNDED ? 0.2 * o.rtol : 0.0;
+      const double z = part.mom.z, ez = part.mom.ez;
+      std::vector<double> v(len), er(len);
+      for (int64_t i = 0; i < len; ++i) {
+        v[i] = s[p][i] / z;
+        er[i] = (e[p][i] + std::fabs(v[i]) * ez) / z + trunc * std::fabs(v[i]);
+      }
+      for (int k = 0; k < 2; ++k) {
+        v[S_R2 + k] = part.mom.v[k];
+        er[S_R2 + k] = part.mom.e[k];
+      }
+      av[grp[p]] = std::move(v);
+      ae[grp[p]] = std::move(er);
+    }
+  }
+  // Units: the mixture of their parts with number fractions 1/count (one part per unit here).
+  std::vector<UnitOut> out;
+  for (auto& un : units) {
+    std::vector<double> v(len, 0.0), e(len, 0.0);
+    const double f = 1.0 / (double)un.size();
+    for (int p : un)
+      for (int64_t i = 0; i < len; ++i) {
+        v[i] += f * av[p][i];
+        e[i] += f * ae[p][i];
+      }
+    UnitOut u;
+    auto lin = [&](int i) { return Lin{v[i], e[i]}; };
+    Lin ext = lin(S_EXT), sca = lin(S_SCA), scag = lin(S_SCAG), ab = lin(S_ABS),
+        back = lin(S_BACK), r2 = lin(S_R2), r3 = lin(S_R3);
+    for (Lin* l : {&ext, &sca, &back})
+      if (!(std::isfinite(l->v) && l->v != 0.0))
+        throw Failure{INVALID_INPUT,
+                      "a ratio's denominator (<C_ext>, <C_sca> or <C_back>) is 0 or not finite"};
+    const Lin sc[11] = {ext, sca, ab, back, ldiv(sca, ext), ldiv(scag, sca),
+                        lscale(ldiv(ext, back), 4.0 * PI), Lin{0.0, 0.0}, ldiv(r3, r2),
+                        lscale(r2, PI), lscale(r3, 4.0 * PI / 3.0)};
+    for (int k = 0; k < 11; ++k) {
+      u.values[k] = sc[k].v;
+      u.errors[k] = sc[k].e;
+    }
+    if (n_mu > 0) {
+      u.phase.assign(6 * n_mu, 0.0);
+      u.phase_err.assign(6 * n_mu, 0.0);
+      const int src[6] = {0, 1, 0, 2, 3, 2};
+      for (int el = 0; el < 6; ++el)
+        for (int64_t j = 0; j < n_mu; ++j) {
+          Lin f = lin((int)(SCALARS + src[el] * n_mu + j));
+          if (normalized) f = ldiv(f, sca);
+          u.phase[el * n_mu + j] = f.v;
+          u.phase_err[el * n_mu + j] = f.e;
+        }
+    }
+    if (order >= 0) {
+      int64_t top = 0;
+      for (auto& B : L.bands) top = std::max(top, std::min(order, 2 * B.upper));
+      std::vector<Lin> gk(6 * (top + 1), Lin{0.0, 0.0});
+      for (size_t b = 0; b < L.bands.size(); ++b) {
+        const BandData& B = L.bands[b];
+        const int64_t qn = B.n_q, blen = B.order + 1;
+        const double* f = v.data() + L.start[b];
+        const double* fe = e.data() + L.start[b];
+        for (int64_t l = 0; l < blen; ++l) {
+          double c[6] = {0, 0, 0, 0, 0, 0}, pp = 0, mi = 0;
+          double ce[4] = {0, 0, 0, 0}, bp = 0, bm = 0;
+          for (int64_t k = 0; k < qn; ++k) {
+            const double d00 = B.dmat[0][k * blen + l], d22 = B.dmat[1][k * blen + l];
+            const double d2m2 = B.dmat[2][k * blen + l], d02 = B.dmat[3][k * blen + l];
+            c[0] += f[k] * d00;
+            c[3] += f[2 * qn + k] * d00;
+            pp += (f[k] + f[2 * qn + k]) * d22;
+            mi += (f[k] - f[2 * qn + k]) * d2m2;
+            c[4] += f[qn + k] * d02;
+            c[5] += f[3 * qn + k] * d02;
+            const double es = fe[k] + fe[2 * qn + k];
+            ce[0] += fe[k] * std::fabs(d00);
+            ce[1] += fe[2 * qn + k] * std::fabs(d00);
+            ce[2] += fe[qn + k] * std::fabs(d02);
+            ce[3] += fe[3 * qn + k] * std::fabs(d02);
+            bp += es * std::fabs(d22);
+            bm += es * std::fabs(d2m2);
+          }
+          c[1] = (pp + mi) * 0.5;
+          c[2] = (pp - mi) * 0.5;
+          const double both = (bp + bm) * 0.5;
+          const double cerr[6] = {ce[0], both, both, ce[1], ce[2], ce[3]};
+          for (int el = 0; el < 6; ++el) {
+            gk[el * (top + 1) + l].v += c[el];
+            gk[el * (top + 1) + l].e += cerr[el];
+          }
+        }
+      }
+      if (normalized) {
+        const Lin a0 = gk[0];
+        for (auto& x : gk) x = ldiv(x, a0);
+        gk[0] = Lin{1.0, 0.0};
+      }
+      u.greek.assign(6 * (order + 1), 0.0);
+      u.greek_err.assign(6 * (order + 1), 0.0);
+      for (int el = 0; el < 6; ++el)
+        for (int64_t l = 0; l <= std::min(top, order); ++l) {
+          u.greek[el * (order + 1) + l] = gk[el * (top + 1) + l].v;
+          u.greek_err[el * (order + 1) + l] = gk[el * (top + 1) + l].e;
+        }
+    }
+    std::set<int> ug;
+    for (int p : un) {
+      u.converged = u.converged && firsts[group_of[p]].converged[place[p]];
+      ug.insert(group_of[p]);
+    }
+    for (int gi : ug) u.panels += (int64_t)firsts[gi].panels.size();
+    out.push_back(std::move(u));
+  }
+  return out;
+}
+
+}  // namespace
+
+extern "C" {
+
+// The adaptive ensemble of spheres with m per wavelength (complex, n_wl). batch = 0: every
+// distribution on its own (`compute` per distribution); batch = 1: one `compute_batch` over
+// all (shared panels per wavelength). Outputs distribution-major (unit = d * n_wl + i): values
+// and errors (11, n), phase and phase_err (6, n, n_mu), greek and greek_err (6, n, L + 1),
+// converged (n) as bytes, panels (n). Returns a status, the first error in wavelength order.
+int orc_ensemble_adaptive(const FixedDist* dists, int64_t n_dist, int batch, const double* wl,
+                          int64_t n_wl, const double* m, const double* mu, int64_t n_mu,
+                          int64_t greek_order, int normalized, double rtol, int64_t max_panels,
+                          int allow_unvalidated, int refine_backscatter, int n_threads,
+                          double* values, double* errors, double* phase, double* phase_err,
+                          double* greek, double* greek_err, int8_t* converged, int64_t* panels,
+                          char* err, int64_t err_len) {
+  const int64_t n_units = n_dist * n_wl;
+  Options o{rtol, (size_t)max_panels, allow_unvalidated != 0, refine_backscatter != 0};
+  auto fail = [&](const Failure& f) {
+    if (err && err_len > 0) snprintf(err, err_len, "%s", f.msg.c_str());
+    return f.status;
+  };
+  if (!(rtol >= 1e-13 && rtol <= 0.1)) return fail({INVALID_INPUT, "rtol must be in [1e-13, 0.1]"});
+  if (max_panels < 1) return fail({INVALID_INPUT, "max_panels must be at least 1"});
+  std::vector<Part> parts;
+  try {
+    for (int64_t d = 0; d < n_dist; ++d) parts.push_back(make_part(dists[d], rtol));
+  } catch (const Failure& f) {
+    return fail(f);
+  }
+  // Groups and units: a batch shares one group (point parts alone); single calls are one
+  // part per group and unit.
+  std::vector<std::vector<std::vector<int>>> groups_of, units_of;  // per call
+  if (batch) {
+    std::vector<std::vector<int>> groups, units;
+    std::vector<int> shared;
+    for (int64_t d = 0; d < n_dist; ++d) {
+      if (parts[d].support == POINT)
+        groups.push_back({(int)d});
+      else
+        shared.push_back((int)d);
+      units.push_back({(int)d});
+    }
+    if (!shared.empty()) groups.push_back(shared);
+    groups_of.push_back(groups);
+    units_of.push_back(units);
+  } else {
+    for (int64_t d = 0; d < n_dist; ++d) {
+      groups_of.push_back({{(int)d}});
+      units_of.push_back({{(int)d}});
+    }
+  }
+  const int64_t n_calls = (int64_t)groups_of.size();
+  const int64_t glen = greek_order >= 0 ? greek_order + 1 : 0;
+  std::vector<Failure> fails(n_calls * n_wl, Failure{OK, ""});
+  if (n_threads > 0) omp_set_num_threads(n_threads);
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int64_t job = 0; job < n_calls * n_wl; ++job) {
+    const int64_t c = job / n_wl, i = job % n_wl;
+    try {
+      auto res = wavelength(parts, groups_of[c], units_of[c], wl[i], C(m[2 * i], m[2 * i + 1]),
+                            mu, n_mu, greek_order, normalized != 0, o);
+      for (size_t k = 0; k < units_of[c].size(); ++k) {
+        const int64_t d = units_of[c][k][0];
+        const int64_t unit = d * n_wl + i;
+        const UnitOut& u = res[k];
+        for (int q = 0; q < 11; ++q) {
+          values[q * n_units + unit] = u.values[q];
+          errors[q * n_units + unit] = u.errors[q];
+        }
+        if (phase && n_mu > 0)
+          for (int el = 0; el < 6; ++el)
+            for (int64_t j = 0; j < n_mu; ++j) {
+              phase[(el * n_units + unit) * n_mu + j] = u.phase[el * n_mu + j];
+              phase_err[(el * n_units + unit) * n_mu + j] = u.phase_err[el * n_mu + j];
+            }
+        if (greek && glen > 0)
+          for (int el = 0; el < 6; ++el)
+            for (int64_t l = 0; l < glen; ++l) {
+              greek[(el * n_units + unit) * glen + l] = u.greek[el * glen + l];
+              greek_err[(el * n_units + unit) * glen + l] = u.greek_err[el * glen + l];
+            }
+        converged[unit] = u.converged ? 1 : 0;
+        panels[unit] = u.panels;
+      }
+    } catch (const Failure& f) {
+      fails[job] = f;
+    }
+  }
+  // The first error in (wavelength, call) order, as the reference reports the first in order.
+  for (int64_t i = 0; i < n_wl; ++i)
+    for (int64_t c = 0; c < n_calls; ++c)
+      if (fails[c * n_wl + i].status != OK) return fail(fails[c * n_wl + i]);
+  return OK;
+}
+
+}  // extern "C"

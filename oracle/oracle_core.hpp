@@ -998,4 +998,58 @@ inline int64_t bucket(int64_t n) {
   return u;
 }
 
+// ---------------------------------------------------------------------------------------
+// Distributions as the C ABI passes them, and a projector band's tables (engine.rs:2034-2072,
+// fast.rs:22-50, 210-235).
+// ---------------------------------------------------------------------------------------
+struct FixedDist {
+  int32_t kind;
+  int32_t pad;
+  double p[3];
+  double r_lo, r_hi;
+};
+
+constexpr int NODES_PER_CHUNK = 32;
+
+struct BandData {
+  int64_t upper;
+  int64_t order;  // L_b
+  int64_t n_q;
+  std::vector<double> nodes, weights;
+  std::vector<double> ge, go;  // h x upper, row-major
+  std::vector<double> dmat[4];  // n_q x (L_b+1): (2l+1)/2 w_k d_l(mu_k)
+};
+
+inline BandData make_band(int64_t upper, int64_t order) {
+  BandData b;
+  b.upper = upper;
+  b.order = std::min(order, 2 * upper);
+  b.n_q = upper + (b.order + 2) / 2;
+  b.nodes.resize(b.n_q);
+  b.weights.resize(b.n_q);
+  gauss_legendre(b.n_q, b.nodes.data(), b.weights.data());
+  int64_t lo = b.n_q / 2, h = b.n_q - lo;
+  b.ge.assign(h * upper, 0.0);
+  b.go.assign(h * upper, 0.0);
+  for (int64_t i = 0; i < h; ++i) {
+    for_each_order(b.nodes[lo + i], upper, [&](int64_t k, double pi, double tau) {
+      bool odd = k % 2 == 1;
+      b.ge[i * upper + (k - 1)] = odd ? pi : tau;
+      b.go[i * upper + (k - 1)] = odd ? tau : pi;
+    });
+  }
+  int64_t len = b.order + 1;
+  std::vector<double> buf(len);
+  const int mn[4][2] = {{0, 0}, {2, 2}, {2, -2}, {0, 2}};
+  for (int i = 0; i < 4; ++i) b.dmat[i].assign(b.n_q * len, 0.0);
+  for (int64_t k = 0; k < b.n_q; ++k) {
+    for (int i = 0; i < 4; ++i) {
+      wigner_d(mn[i][0], mn[i][1], b.nodes[k], buf.data(), len);
+      for (int64_t l = 0; l < len; ++l)
+        b.dmat[i][k * len + l] = (double)(2 * l + 1) * 0.5 * b.weights[k] * buf[l];
+    }
+  }
+  return b;
+}
+
 }  // namespace orc
