@@ -110,6 +110,41 @@ int scatrs_ensemble_fixed_d(const scatrs_distribution* dists, int64_t n_dist,
                             double* values, double* phase, double* greek, double* d_values,
                             double* d_phase, double* d_greek, char* err, size_t err_len);
 
+/* A single radius (SizeDistribution::Monodisperse, distribution.rs:50-53): param[0] the
+ * radius. Adaptive calls only. */
+#define SCATRS_MONODISPERSE 5
+
+/* Options of the adaptive ensemble: the reference's EnsembleOptions (scatrs/src/ensemble/
+ * mod.rs:342-382; defaults rtol 1e-6, max_panels 4096). */
+typedef struct scatrs_adaptive_options {
+  double rtol;                /* relative tolerance of the size integration, in [1e-13, 0.1] */
+  int64_t max_panels;         /* panels per part and wavelength, >= 1 */
+  int32_t greek_order;        /* highest Greek order L, or -1 for none */
+  int32_t normalized;         /* 1: normalized phase matrix and Greek coefficients */
+  int32_t allow_unvalidated;  /* 1: compute outside the Mie validated domain */
+  int32_t refine_backscatter; /* 1: also refine on <C_back> */
+} scatrs_adaptive_options;
+
+/*
+ * The adaptive ensemble of spheres, the reference's default integration: per distribution
+ * (batch = 0: `compute`, scatrs/src/ensemble/mod.rs:548-606) or as one batch sharing panels per
+ * wavelength (batch = 1: `compute_batch`, mod.rs:613-686), with the reference's tail cut-offs
+ * (range.rs), moments (moments.rs), GK15 pass 1 refined on C_ext, C_sca, C_sca g, C_abs (and
+ * C_back if asked) with range extensions, and pass 2 on the final panels with Kronrod sums and
+ * |Kronrod - Gauss| error estimates (engine.rs:724-1836, 2310-2497). m is complex128 per
+ * wavelength (one particle, as the reference's). Distributions as scatrs_distribution (r_lo,
+ * r_hi unused) or SCATRS_MONODISPERSE. Outputs as scatrs_ensemble_fixed, each with its error
+ * estimate in the *_err / errors array of the same layout; converged[n_units] (0/1) and
+ * panels[n_units] (the shared panels of a batch; 0 for a single radius).
+ */
+int scatrs_ensemble_adaptive(const scatrs_distribution* dists, int64_t n_dist, int32_t batch,
+                             const double* wavelengths, int64_t n_wl, const double* m,
+                             const double* mu, int64_t n_mu,
+                             const scatrs_adaptive_options* options, double* values,
+                             double* errors, double* phase, double* phase_err, double* greek,
+                             double* greek_err, int8_t* converged, int64_t* panels, char* err,
+                             size_t err_len);
+
 /* Layered spheres (scatrs/src/layered/mod.rs; Particle::LayeredSphere,
  * scatrs/src/ensemble/mod.rs:58-65): n_layers layers, the core first; per distribution the
  * n_layers - 1 outer radii of layers 0..L-2 as fractions of the particle's radius (nondecreasing

@@ -28,10 +28,16 @@ _SZ = ctypes.c_size_t
 DIST_DTYPE = np.dtype([("kind", np.int32), ("reserved", np.int32), ("param", np.float64, 3),
                        ("r_lo", np.float64), ("r_hi", np.float64)])
 KINDS = {"lognormal": 1, "gamma": 2, "modified_gamma": 3, "power_law": 4}
+MONODISPERSE = 5  # adaptive calls only: param[0] the radius
 
 
 class Layers(ctypes.Structure):
     _fields_ = [("n_layers", _I32), ("reserved", _I32), ("fractions", _PD), ("m", _PD)]
+
+
+class AdaptiveOptions(ctypes.Structure):
+    _fields_ = [("rtol", _D), ("max_panels", _I64), ("greek_order", _I32), ("normalized", _I32),
+                ("allow_unvalidated", _I32), ("refine_backscatter", _I32)]
 
 
 class FixedOptions(ctypes.Structure):
@@ -54,6 +60,9 @@ SYMBOLS = {
     "scatrs_ensemble_fixed_device": (ctypes.c_int, [_VP, _I64, _VP, _I64, _VP, _PD, _I64,
                                                     ctypes.POINTER(FixedOptions), _VP, _VP, _VP,
                                                     _VP, _CP, _SZ]),
+    "scatrs_ensemble_adaptive": (ctypes.c_int, [_VP, _I64, _I32, _PD, _I64, _PD, _PD, _I64,
+                                                ctypes.POINTER(AdaptiveOptions), _PD, _PD, _PD,
+                                                _PD, _PD, _PD, _VP, _VP, _CP, _SZ]),
     "scatrs_check_errors": (ctypes.c_int, [_VP, _CP, _SZ]),
     "scatrs_mie": (ctypes.c_int, [_PD, _PD, _I64, _I32, _PI64, _PI64, _PD, _PD, _CP, _SZ]),
     "scatrs_mie_static": (ctypes.c_int, [_VP, _VP, _I64, _I32, _I64, _VP, _VP, _VP, _VP, _VP,
@@ -205,6 +214,46 @@ def ensemble_fixed_d(dists: np.ndarray, wavelengths, m, mu, n_nodes: int, greek_
                                         _p(d_values), _p(d_phase), _p(d_greek), err, 1024)
     _check(st, err)
     return values, phase, greek, d_values, d_phase, d_greek
+
+
+def ensemble_adaptive(dists: np.ndarray, wavelengths, m, mu=None, greek_order: int = -1,
+                      normalized: bool = True, rtol: float = 1e-6, max_panels: int = 4096,
+                      allow_unvalidated: bool = False, refine_backscatter: bool = False,
+                      batch: bool = False) -> dict:
+    """The adaptive ensemble of spheres (the reference's default integration) with m per
+    wavelength: each distribution on its own, or one batch sharing panels. Returns values,
+    errors (11, n), phase/phase_err (6, n, n_mu), greek/greek_err (6, n, L + 1), converged,
+    panels (n), units distribution-major."""
+    require_device()
+    dists = np.ascontiguousarray(dists, dtype=DIST_DTYPE)
+    wl = np.ascontiguousarray(wavelengths, dtype=np.float64).reshape(-1)
+    m = np.ascontiguousarray(np.broadcast_to(np.asarray(m, dtype=np.complex128), wl.shape))
+    mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
+    n = dists.size * wl.size
+    L = int(greek_order)
+    opts = AdaptiveOptions(float(rtol), int(max_panels), L, int(normalized),
+                           int(allow_unvalidated), int(refine_backscatter))
+    out = {"values": np.zeros((11, n)), "errors": np.zeros((11, n)),
+           "converged": np.zeros(n, dtype=np.int8), "panels": np.zeros(n, dtype=np.int64)}
+    ph = pe = g = ge = None
+    if mu.size:
+        ph, pe = np.zeros((6, n, mu.size)), np.zeros((6, n, mu.size))
+    if L >= 0:
+        g, ge = np.zeros((6, n, L + 1)), np.zeros((6, n, L + 1))
+    err = ctypes.create_string_buffer(1024)
+    st = load().scatrs_ensemble_adaptive(dists.ctypes.data, dists.size, int(batch), _p(wl),
+                                         wl.size, _p(m.view(np.float64)), _p(mu), mu.size,
+                                         ctypes.byref(opts), _p(out["values"]),
+                                         _p(out["errors"]), _p(ph), _p(pe), _p(g), _p(ge),
+                                         out["converged"].ctypes.data, out["panels"].ctypes.data,
+                                         err, 1024)
+    _check(st, err)
+    out["converged"] = out["converged"].astype(bool)
+    if ph is not None:
+        out["phase"], out["phase_err"] = ph, pe
+    if g is not None:
+        out["greek"], out["greek_err"] = g, ge
+    return out
 
 
 def ensemble_fixed_layered(dists: np.ndarray, wavelengths, fractions, m_layers, mu,

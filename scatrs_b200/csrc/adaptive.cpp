@@ -1,0 +1,591 @@
+// The adaptive ensemble's host logic: see adaptive.h. Each function cites the reference code
+// whose decisions it makes; the numbers it decides on (the pass-1 sums) come from the device.
+#include "adaptive.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <limits>
+
+#include "tables.h"
+
+namespace sb {
+namespace adaptive {
+
+namespace {
+
+constexpr double kStep = 0.5;          // range.rs:8
+constexpr int kMaxSteps = 400;         // range.rs:11
+constexpr int kMaxExtensions = 100;    // engine.rs:60
+constexpr double kMinWidth = 1e-10;    // engine.rs:63
+constexpr double kMaxDx = 20.0;        // engine.rs:67
+constexpr size_t kMomentPanels = 100000;  // moments.rs:10
+constexpr double kInf = std::numeric_limits<double>::infinity();
+constexpr double kPi = 3.14159265358979323846264338327950288;
+constexpr double kMaxSizeParameter = 1e6;  // mie/mod.rs MAX_SIZE_PARAMETER
+
+// Pass-1 indices (engine.rs:43-54).
+constexpr int ONE = 0, EXT = 1, SCA = 2, SCAG = 3, BACK = 4, ABS = 5;
+
+double max_step(const Part& p, double step) { return std::min(step, 0.5 * p.log_width); }
+
+std::string at(double lambda, double r) {
+  char buf[128];
+  snprintf(buf, sizeof buf, "at wavelength %e, radius %e: ", lambda, r);
+  return buf;
+}
+
+// The masses of r^k u over [t0, t1] for k in {0, 2, 3} as selected (range.rs:25-36).
+void masses(const Part& p, double t0, double t1, const std::vector<int>& pw, double* out) {
+  Node nd[15];
+  gk15(t0, t1, nd);
+  for (size_t k = 0; k < pw.size(); ++k) out[k] = 0.0;
+  for (const Node& n : nd) {
+    const double r = std::exp(n.t);
+    const double wu = n.wk * r * p.u(r);
+    for (size_t k = 0; k < pw.size(); ++k)
+      out[k] += wu * (pw[k] == 0 ? 1.0 : pw[k] == 2 ? r * r : r * r * r);
+  }
+}
+
+// range.rs:48-93: march outward in steps of ln r until each side's tail, bounded
+// geometrically, holds at most eps of every moment.
+std::pair<double, double> cutoffs(const Part& p, double center, double eps,
+                                  const std::vector<int>& pw) {
+  const double t0 = std::log(center), step = max_step(p, kStep);
+  const size_t np = pw.size();
+  std::vector<double> total(np, 0.0), mass(np);
+  std::vector<double> last[2] = {std::vector<double>(np, kInf), std::vector<double>(np, kInf)};
+  double ends[2] = {t0, t0};
+  bool done[2] = {false, false};
+  for (int i = 0; i < kMaxSteps; ++i) {
+    for (int side = 0; side < 2; ++side) {
+      if (done[side]) continue;
+      const double a = ends[side], b = a + (side == 0 ? -1.0 : 1.0) * step;
+      masses(p, std::min(a, b), std::max(a, b), pw, mass.data());
+      for (double m : mass)
+        if (!std::isfinite(m)) {
+          char buf[128];
+          snprintf(buf, sizeof buf, "the size distribution's density is not finite near r = %e",
+                   std::exp(b));
+          throw Error{1, buf};
+        }
+      ends[side] = b;
+      bool small = i >= 1;
+      for (size_t k = 0; k < np; ++k) {
+        total[k] += mass[k];
+        const double q = mass[k] / last[side][k];
+        last[side][k] = mass[k];
+        small = small && (mass[k] == 0.0 || (q < 1.0 && mass[k] / (1.0 - q) <= eps * total[k]));
+      }
+      done[side] = small;
+    }
+    if (done[0] && done[1]) return {std::exp(ends[0]), std::exp(ends[1])};
+  }
+  char buf[160];
+  snprintf(buf, sizeof buf,
+           "the size distribution is too broad: its tails do not decay within e^%g of r = %e",
+           kMaxSteps * step, center);
+  throw Error{1, buf};
+}
+
+// moments.rs:62-167 without derivative parameters: GK15 panels of at most max_step, split
+// where their |Kronrod - Gauss| is above their share, until Z, <r^2 u>, <r^3 u> meet rtol.
+Moments moments(const Part& p, double lo, double hi, double rtol, double truncation) {
+  const double step = max_step(p, kStep);
+  const double t_lo = std::log(lo), t_hi = std::log(hi);
+  std::vector<std::pair<double, double>> panels;
+  {
+    const size_t n = (size_t)std::max(1.0, std::ceil((t_hi - t_lo) / step));
+    const double h = (t_hi - t_lo) / (double)n;
+    for (size_t i = 0; i < n; ++i) panels.push_back({t_lo + i * h, t_lo + (i + 1) * h});
+  }
+  std::vector<double> sums;  // per panel: K0, K2, K3, |K-G| x 3
+  auto result = [&]() {
+    double s[3] = {0, 0, 0}, e[3] = {0, 0, 0};
+    for (int j = 0; j < 3; ++j)
+      for (size_t i = 0; i < panels.size(); ++i) {
+        s[j] += sums[6 * i + j];
+        e[j] += sums[6 * i + 3 + j];
+      }
+    if (!(std::isfinite(s[0]) && s[0] > 0.0)) {
+      char buf[128];
+      snprintf(buf, sizeof buf,
+               "the size distribution has no finite positive mass on its range (got %e)", s[0]);
+      throw Error{1, buf};
+    }
+    Moments m;
+    m.z = s[0];
+    m.ez = e[0];
+    for (int k = 0; k < 2; ++k) {
+      m.v[k] = s[1 + k] / m.z;
+      m.e[k] = (e[1 + k] + std::fabs(m.v[k]) * m.ez) / m.z + truncation * std::fabs(m.v[k]);
+    }
+    return m;
+  };
+  for (;;) {
+    sums.assign(6 * panels.size(), 0.0);
+    for (size_t i = 0; i < panels.size(); ++i) {
+      Node nd[15];
+      gk15(panels[i].first, panels[i].second, nd);
+      double k[3] = {0, 0, 0}, g[3] = {0, 0, 0};
+      for (const Node& n : nd) {
+        const double r = std::exp(n.t), u = p.u(r);
+        const double q[3] = {1.0, r * r, r * r * r};
+        for (int j = 0; j < 3; ++j) {
+          k[j] += n.wk * u * r * q[j];
+          g[j] += n.wg * u * r * q[j];
+        }
+      }
+      for (int j = 0; j < 3; ++j) {
+        sums[6 * i + j] = k[j];
+        sums[6 * i + 3 + j] = std::fabs(k[j] - g[j]);
+      }
+    }
+    double total[3] = {0, 0, 0}, terr[3] = {0, 0, 0}, target[3];
+    for (size_t i = 0; i < panels.size(); ++i)
+      for (int j = 0; j < 3; ++j) {
+        total[j] += sums[6 * i + j];
+        terr[j] += sums[6 * i + 3 + j];
+      }
+    bool met = true;
+    for (int j = 0; j < 3; ++j) {
+      target[j] = rtol * std::fabs(total[j]);
+      met = met && terr[j] <= target[j];
+    }
+    const size_t n = panels.size();
+    if (met || n >= kMomentPanels) return result();
+    std::vector<std::pair<double, double>> next;
+    for (size_t i = 0; i < n; ++i) {
+      bool bad = false;
+      for (int j = 0; j < 3; ++j)
+        bad = bad || (sums[6 * i + 3 + j] * (double)n > target[j] && terr[j] > target[j]);
+      if (bad && panels[i].second - panels[i].first > 1e-10) {
+        const double mid = 0.5 * (panels[i].first + panels[i].second);
+        next.push_back({panels[i].first, mid});
+        next.push_back({mid, panels[i].second});
+      } else {
+        next.push_back(panels[i]);
+      }
+    }
+    if (next.size() == n) return result();
+    panels.swap(next);
+  }
+}
+
+double size_param(double r, double lambda) { return 2.0 * kPi * r / lambda; }
+
+// engine.rs:301-354.
+std::vector<std::pair<double, double>> initial_panels(double t_lo, double t_hi, double lambda,
+                                                      const std::vector<double>& breaks,
+                                                      const std::function<double(double)>& step_of,
+                                                      size_t budget) {
+  std::vector<double> edges{t_lo};
+  for (double r : breaks) {
+    const double t = std::log(r);
+    if (t > t_lo && t < t_hi) edges.push_back(t);
+  }
+  edges.push_back(t_hi);
+  std::vector<std::pair<double, double>> out;
+  for (size_t e = 0; e + 1 < edges.size() && out.size() <= budget; ++e) {
+    double a = edges[e];
+    const double b = edges[e + 1];
+    while (a < b) {
+      const double x = size_param(std::exp(a), lambda);
+      const double step = std::min(step_of(a), std::log(1.0 + kMaxDx / x));
+      const double n = std::max(1.0, std::ceil((b - a) / step));
+      const double h = (b - a) / n;
+      const double next = (n <= 1.0 || a + h <= a) ? b : a + h;
+      out.push_back({a, next});
+      a = next;
+      if (out.size() > budget) break;
+    }
+  }
+  if (out.size() <= budget) return out;
+  const double width = t_hi - t_lo;
+  std::vector<std::pair<double, double>> equal;
+  for (size_t e = 0; e + 1 < edges.size(); ++e) {
+    const size_t n =
+        (size_t)std::max(1.0, std::floor((edges[e + 1] - edges[e]) / width * (double)budget));
+    const double h = (edges[e + 1] - edges[e]) / (double)n;
+    for (size_t i = 0; i < n; ++i)
+      equal.push_back({edges[e] + (double)i * h, edges[e] + (double)(i + 1) * h});
+  }
+  return equal;
+}
+
+// One panel's pass-1 sums for one part (engine.rs:482-549).
+struct Sums1 {
+  double k[kPass1], err[kPass1], edge[2][kPass1];
+};
+
+// The targets, errors and ends of a part (engine.rs:620-720, no Greek refinement, no
+// derivatives).
+struct Status {
+  double target[kPass1], errors[kPass1];
+  bool met, small[2];
+};
+
+Status status_of(const std::vector<const Sums1*>& s, const Options& o, double ext) {
+  Status st;
+  auto total = [&](int j) {
+    double t = 0.0;
+    for (auto* x : s) t += x->k[j];
+    return t;
+  };
+  const double c_sca = std::fabs(total(SCA));
+  for (int j = 0; j < kPass1; ++j) {
+    double scale;
+    if (j == SCAG)
+      scale = c_sca;
+    else if (j == BACK)
+      scale = std::max(std::fabs(total(BACK)), c_sca);
+    else
+      scale = std::fabs(total(j == ABS ? EXT : j));  // C_abs to rtol of C_ext
+    st.target[j] = o.rtol * scale;
+  }
+  st.target[ONE] = kInf;
+  if (!o.refine_backscatter) st.target[BACK] = kInf;
+  st.met = true;
+  for (int j = 0; j < kPass1; ++j) {
+    double e = 0.0;
+    for (auto* x : s) e += x->err[j];
+    st.errors[j] = e;
+    st.met = st.met && e <= st.target[j];
+  }
+  auto small = [&](const double* d) {
+    for (int j = 0; j < kPass1; ++j)
+      if (!(std::fabs(d[j]) * (ext / kStep) <= 0.1 * st.target[j])) return false;
+    return true;
+  };
+  st.small[0] = small(s.front()->edge[0]);
+  st.small[1] = small(s.back()->edge[1]);
+  return st;
+}
+
+struct Panel {
+  double a, b;
+  bool done = false;
+  int64_t n_terms = 0;
+  std::vector<Sums1> sums;  // per part of the job
+};
+
+struct State {
+  std::vector<Panel> panels;
+  double t_lo = 0, t_hi = 0;
+  int extensions[2] = {0, 0};
+  std::vector<double> exts;                     // per part
+  std::vector<std::array<double, 3>> steps;     // per part: ln lo, ln hi, step
+  bool finished = false;
+};
+
+}  // namespace
+
+double Part::u(double r) const {
+  if (support == POINT) return 0.0;
+  return density(kind, p, r);
+}
+
+void gk15(double a, double b, Node out[15]) {
+  // kronrod.rs:5-52 (QUADPACK's qk15 abscissae and weights).
+  static const double kn[8] = {0.991455371120812639206854697526329,
+                               0.949107912342758524526189684047851,
+                               0.864864423359769072789712788640926,
+                               0.741531185599394439863864773280788,
+                               0.586087235467691130294144845693013,
+                               0.405845151377397166906606412076961,
+                               0.207784955007898467600689403773245,
+                               0.0};
+  static const double kw[8] = {0.022935322010529224963732008058970,
+                               0.063092092629978553290700663189204,
+                               0.104790010322250183839876322541518,
+                               0.140653259715525918745189590510238,
+                               0.169004726639267902826583426598550,
+                               0.190350578064785409913256402421014,
+                               0.204432940075298892414161999234649,
+                               0.209482141084727828012999174891714};
+  static const double gw[4] = {0.129484966168869693270611432679082,
+                               0.279705391489276667901467771423780,
+                               0.381830050505118944950369775488975,
+                               0.417959183673469387755102040816327};
+  const double c = 0.5 * (a + b), h = 0.5 * (b - a);
+  for (int i = 0; i < 7; ++i) {
+    const double g = i % 2 == 1 ? h * gw[i / 2] : 0.0;
+    const double k = h * kw[i];
+    out[i] = {c - h * kn[i], k, g};
+    out[14 - i] = {c + h * kn[i], k, g};
+  }
+  out[7] = {c, h * kw[7], h * gw[3]};
+}
+
+Part make_part(int kind, const double* p, double rtol) {
+  Part part;
+  part.kind = kind;
+  for (int k = 0; k < 3; ++k) part.p[k] = p[k];
+  if (kind == kMonodisperse) {
+    if (!(std::isfinite(p[0]) && p[0] > 0.0)) throw Error{1, "radius must be finite and > 0"};
+    part.support = POINT;
+    part.lo = part.hi = p[0];
+    return part;
+  }
+  std::string msg;
+  if (!validate_distribution(kind, p, &msg)) throw Error{1, msg};
+  const DensityInfo info = density_info(kind, p);
+  part.reference = info.reference;
+  part.log_width = info.log_width;
+  if (kind == 4) {  // finite support [min_radius, max_radius]
+    part.support = FINITE;
+    part.lo = p[1];
+    part.hi = p[2];
+    part.mom = moments(part, p[1], p[2], rtol, 0.0);
+    return part;
+  }
+  // Unbounded (distribution.rs:272-290): about the median, the effective radius or the
+  // reference radius; the Mie range bounds the area's tails to rtol/10, the moments' range
+  // every tail to 1e-3 rtol (engine.rs:190-205).
+  part.support = UNBOUNDED;
+  const double center = kind == 3 ? part.reference : p[0];
+  auto mie = cutoffs(part, center, rtol / 10.0, {2});
+  part.lo = mie.first;
+  part.hi = mie.second;
+  auto wide = cutoffs(part, center, std::max(1e-3 * rtol, 1e-16), {0, 2, 3});
+  part.mom = moments(part, wide.first, wide.second, rtol, 0.2 * rtol);
+  return part;
+}
+
+// engine.rs:724-924, every job at once: a round evaluates the unevaluated panels of every
+// unfinished job, then each job refines (splits worst first), extends its range or finishes.
+void pass1(std::vector<Job>& jobs, const std::vector<Part>& parts, const double* wavelengths,
+           const Options& o, const Evaluate& eval) {
+  const size_t budget_max = (size_t)o.max_panels;
+  std::vector<State> states(jobs.size());
+  for (size_t ji = 0; ji < jobs.size(); ++ji) {
+    Job& job = jobs[ji];
+    State& st = states[ji];
+    const double lambda = wavelengths[job.wl];
+    std::vector<double> breaks;
+    double lo = kInf, hi = 0.0;
+    for (int pi : job.parts) {
+      const Part& p = parts[pi];
+      if (p.support == FINITE) {
+        breaks.push_back(p.lo);
+        breaks.push_back(p.hi);
+      }
+      lo = std::min(lo, p.lo);
+      hi = std::max(hi, p.hi);
+      st.exts.push_back(std::min(kStep, p.log_width));
+      st.steps.push_back({std::log(p.lo), std::log(p.hi), max_step(p, kStep)});
+    }
+    std::sort(breaks.begin(), breaks.end());
+    breaks.erase(std::unique(breaks.begin(), breaks.end()), breaks.end());
+    const double x_hi = size_param(hi, lambda);
+    if (x_hi > kMaxSizeParameter) {
+      char buf[200];
+      snprintf(buf, sizeof buf,
+               "the integration range reaches size parameter %e, above the accepted %e", x_hi,
+               kMaxSizeParameter);
+      job.status = 1;
+      job.msg = at(lambda, hi) + buf;
+      st.finished = true;
+      continue;
+    }
+    st.t_lo = std::log(lo);
+    st.t_hi = std::log(hi);
+    auto step_of = [&st](double t) {
+      double s = kStep;
+      for (auto& x : st.steps)
+        if (x[0] <= t && t < x[1]) s = std::min(s, x[2]);
+      return s;
+    };
+    for (auto& ab : initial_panels(st.t_lo, st.t_hi, lambda, breaks, step_of, budget_max))
+      st.panels.push_back({ab.first, ab.second});
+  }
+  for (;;) {
+    // Gather this round's nodes.
+    std::vector<Query> qs;
+    std::vector<std::pair<size_t, size_t>> owner;  // (job, panel) per 15 nodes
+    for (size_t ji = 0; ji < jobs.size(); ++ji) {
+      if (states[ji].finished) continue;
+      for (size_t pi = 0; pi < states[ji].panels.size(); ++pi) {
+        Panel& pn = states[ji].panels[pi];
+        if (pn.done) continue;
+        Node nd[15];
+        gk15(pn.a, pn.b, nd);
+        for (const Node& n : nd) qs.push_back({std::exp(n.t), jobs[ji].wl});
+        owner.push_back({ji, pi});
+      }
+    }
+    if (owner.empty()) break;
+    std::vector<NodeResult> res(qs.size());
+    eval(qs, res);
+    // Panel sums, and each job's first failing node in panel order.
+    std::vector<int> first_fail(jobs.size(), -1);
+    for (size_t k = 0; k < owner.size(); ++k) {
+      const size_t ji = owner[k].first, pi = owner[k].second;
+      Panel& pn = states[ji].panels[pi];
+      Node nd[15];
+      gk15(pn.a, pn.b, nd);
+      bool ok = true;
+      for (int i = 0; i < 15 && ok; ++i)
+        if (res[15 * k + i].status != 0) {
+          ok = false;
+          if (first_fail[ji] < 0 || (int)pi < first_fail[ji]) {
+            first_fail[ji] = (int)pi;
+            jobs[ji].status = res[15 * k + i].status;
+            jobs[ji].msg = at(wavelengths[jobs[ji].wl], qs[15 * k + i].r) +
+                           (jobs[ji].status == 3
+                                ? "the size parameter and refractive index are outside the "
+                                  "validated domain x in [1e-06, 2e4], 0 < Re m <= 10, "
+                                  "0 <= Im m <= 10, |m| >= 0.1"
+                                : "the size parameter x must be in [1e-30, 1e6] and the "
+                                  "refractive index finite with Re m >= 0, Im m >= 0 and |m| in "
+                                  "[1e-6, 1e3]");
+          }
+        }
+      if (!ok) continue;
+      pn.done = true;
+      pn.n_terms = 0;
+      for (int i = 0; i < 15; ++i) pn.n_terms = std::max(pn.n_terms, res[15 * k + i].n);
+      pn.sums.assign(jobs[ji].parts.size(), Sums1{});
+      for (size_t p = 0; p < jobs[ji].parts.size(); ++p) {
+        const Part& part = parts[jobs[ji].parts[p]];
+        Sums1& s = pn.sums[p];
+        double g[kPass1] = {0, 0, 0, 0, 0, 0};
+        for (int j = 0; j < kPass1; ++j) s.k[j] = 0.0;
+        for (int i = 0; i < 15; ++i) {
+          const double r = qs[15 * k + i].r;
+          const double base = part.u(r) * r;
+          const double* q = res[15 * k + i].q;
+          for (int j = 0; j < kPass1; ++j) {
+            s.k[j] += nd[i].wk * base * q[j];
+            g[j] += nd[i].wg * base * q[j];
+            if (i == 0) s.edge[0][j] = base * q[j];
+            if (i == 14) s.edge[1][j] = base * q[j];
+          }
+        }
+        for (int j = 0; j < kPass1; ++j) s.err[j] = std::fabs(s.k[j] - g[j]);
+      }
+    }
+    for (size_t ji = 0; ji < jobs.size(); ++ji) {
+      State& st = states[ji];
+      Job& job = jobs[ji];
+      if (st.finished) continue;
+      if (first_fail[ji] >= 0) {
+        st.finished = true;
+        continue;
+      }
+      const double lambda = wavelengths[job.wl];
+      const size_t np = job.parts.size();
+      std::vector<Status> stat;
+      for (size_t p = 0; p < np; ++p) {
+        std::vector<const Sums1*> s;
+        for (auto& pn : st.panels) s.push_back(&pn.sums[p]);
+        stat.push_back(status_of(s, o, st.exts[p]));
+      }
+      auto finish = [&]() {
+        job.panels.clear();
+        job.panel_terms.clear();
+        job.n_terms = 0;
+        for (auto& pn : st.panels) {
+          job.panels.push_back({pn.a, pn.b});
+          job.panel_terms.push_back(pn.n_terms);
+          job.n_terms = std::max(job.n_terms, pn.n_terms);
+        }
+        job.converged.assign(np, false);
+        for (size_t p = 0; p < np; ++p) {
+          const bool ext = parts[job.parts[p]].support == UNBOUNDED;
+          job.converged[p] = stat[p].met && (!ext || (stat[p].small[0] && stat[p].small[1]));
+        }
+        st.finished = true;
+      };
+      bool all_met = true;
+      for (auto& s : stat) all_met = all_met && s.met;
+      const size_t n = st.panels.size();
+      if (all_met) {
+        // Extend at an end where an unbounded part's integrand is not negligible.
+        auto wanting = [&](int end, double* ext, double* step) {
+          if (st.extensions[end] >= kMaxExtensions) return false;
+          bool any = false;
+          for (size_t p = 0; p < np; ++p)
+            if (parts[job.parts[p]].support == UNBOUNDED && !stat[p].small[end]) {
+              *ext = any ? std::min(*ext, st.exts[p]) : st.exts[p];
+              *step = any ? std::min(*step, st.steps[p][2]) : st.steps[p][2];
+              any = true;
+            }
+          return any;
+        };
+        double e0 = 0, s0 = 0, e1 = 0, s1 = 0;
+        const bool w0 = wanting(0, &e0, &s0), w1 = wanting(1, &e1, &s1);
+        bool extended = false, stop = false;
+        if (w0) {
+          auto fresh = initial_panels(st.t_lo - e0, st.t_lo, lambda, {},
+                                      [s0](double) { return s0; }, budget_max);
+          if (st.panels.size() + fresh.size() > budget_max) {
+            stop = true;
+          } else {
+            st.t_lo -= e0;
+            st.extensions[0] += 1;
+            std::vector<Panel> nw;
+            for (auto& ab : fresh) nw.push_back({ab.first, ab.second});
+            for (auto& pn : st.panels) nw.push_back(std::move(pn));
+            st.panels.swap(nw);
+            extended = true;
+          }
+        }
+        if (!stop && w1) {
+          auto fresh = initial_panels(st.t_hi, st.t_hi + e1, lambda, {},
+                                      [s1](double) { return s1; }, budget_max);
+          if (st.panels.size() + fresh.size() > budget_max) {
+            stop = true;
+          } else {
+            st.t_hi += e1;
+            st.extensions[1] += 1;
+            for (auto& ab : fresh) st.panels.push_back({ab.first, ab.second});
+            extended = true;
+          }
+        }
+        if (stop || !extended) finish();
+        continue;
+      }
+      // Split every panel above its share of a target still missed, worst first.
+      std::vector<std::pair<double, size_t>> cand;
+      for (size_t i = 0; i < n; ++i) {
+        if (!(st.panels[i].b - st.panels[i].a > kMinWidth)) continue;
+        double bad = 0.0;
+        for (size_t p = 0; p < np; ++p)
+          for (int j = 0; j < kPass1; ++j) {
+            if (!(stat[p].errors[j] > stat[p].target[j])) continue;
+            const double t = std::max(stat[p].target[j], std::numeric_limits<double>::min());
+            bad = std::max(bad, st.panels[i].sums[p].err[j] * (double)n / t);
+          }
+        if (bad > 1.0) cand.push_back({bad, i});
+      }
+      const size_t budget = budget_max > n ? budget_max - n : 0;
+      if (cand.empty() || budget == 0) {
+        finish();
+        continue;
+      }
+      std::sort(cand.begin(), cand.end(), [](const auto& x, const auto& y) {
+        return x.first != y.first ? x.first > y.first : x.second < y.second;
+      });
+      if (cand.size() > budget) cand.resize(budget);
+      std::vector<char> split(n, 0);
+      for (auto& c : cand) split[c.second] = 1;
+      std::vector<Panel> next;
+      next.reserve(n + cand.size());
+      for (size_t i = 0; i < n; ++i) {
+        if (split[i]) {
+          const double a = st.panels[i].a, b = st.panels[i].b, mid = 0.5 * (a + b);
+          next.push_back({a, mid});
+          next.push_back({mid, b});
+        } else {
+          next.push_back(std::move(st.panels[i]));
+        }
+      }
+      st.panels.swap(next);
+    }
+  }
+}
+
+}  // namespace adaptive
+}  // namespace sb

@@ -1,0 +1,93 @@
+// Host side of the adaptive ensemble (the reference's default integration,
+// scatrs/src/ensemble/engine.rs pass 1 with range.rs, moments.rs and kronrod.rs): the parts of
+// a call, their cut-offs and moments, and pass 1's panels, refined round by round. The node
+// evaluations of every round of every (group, wavelength) job go to the device in one batch
+// through the `Evaluate` callback; pass 2 then runs on the final panels' nodes.
+#pragma once
+
+#include <array>
+#include <cstdint>
+#include <functional>
+#include <string>
+#include <utility>
+#include <vector>
+
+namespace sb {
+namespace adaptive {
+
+constexpr int kMonodisperse = 5;  // a single radius (param[0])
+constexpr int kPass1 = 6;         // 1, C_ext, C_sca, C_sca g, C_back, C_abs (engine.rs:43-54)
+
+struct Error {
+  int status;
+  std::string msg;
+};
+
+enum Support { UNBOUNDED, FINITE, POINT };
+
+struct Moments {
+  double v[2] = {0, 0}, e[2] = {0, 0};  // <r^2>, <r^3> and their error estimates
+  double z = 1.0, ez = 0.0;             // the normalization Z = integral of u dr
+};
+
+// One distribution of a call (engine.rs:78-112 Part, without modes or derivatives).
+struct Part {
+  int kind = 0;
+  double p[3] = {0, 0, 0};
+  double reference = 1.0, log_width = 0.0;  // distribution.rs:292-336
+  Support support = UNBOUNDED;
+  double lo = 0.0, hi = 0.0;  // the Mie range before extensions (a point: r, r)
+  Moments mom;
+  double u(double r) const;  // the unnormalized density
+};
+
+// Parses and prepares a part: validation, support, cut-offs (range.rs) and moments
+// (moments.rs). Throws Error.
+Part make_part(int kind, const double* p, double rtol);
+
+struct Options {
+  double rtol = 1e-6;
+  int64_t max_panels = 4096;
+  bool allow_unvalidated = false;
+  bool refine_backscatter = false;
+};
+
+// A node to evaluate: radius and wavelength index; the result: the pass-1 quantities, the
+// number of terms, and a status (0 or the node's error).
+struct Query {
+  double r;
+  int wl;
+};
+struct NodeResult {
+  double q[kPass1];
+  int64_t n;
+  int status;
+};
+using Evaluate = std::function<void(const std::vector<Query>&, std::vector<NodeResult>&)>;
+
+// Pass 1 of one group of parts sharing panels at one wavelength.
+struct Job {
+  std::vector<int> parts;  // indices into the call's parts (none a point)
+  int wl = 0;
+  // results
+  std::vector<std::pair<double, double>> panels;  // final panels in t = ln r
+  std::vector<int64_t> panel_terms;               // each panel's largest number of terms
+  std::vector<bool> converged;                    // per part
+  int64_t n_terms = 0;
+  int status = 0;  // the first node error in panel order, if any
+  std::string msg;
+};
+
+// Runs pass 1 of every job in rounds; each round evaluates all jobs' new panels (15 GK nodes
+// each) with one eval call.
+void pass1(std::vector<Job>& jobs, const std::vector<Part>& parts, const double* wavelengths,
+           const Options& o, const Evaluate& eval);
+
+// The GK15 rule on [a, b] in t: nodes ascending with Kronrod and Gauss weights (kronrod.rs).
+struct Node {
+  double t, wk, wg;
+};
+void gk15(double a, double b, Node out[15]);
+
+}  // namespace adaptive
+}  // namespace sb

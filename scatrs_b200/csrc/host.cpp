@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "../../include/scatrs_b200.h"
+#include "adaptive.h"
 #include "kernels.h"
 #include "tables.h"
 
@@ -139,9 +140,11 @@ struct Context {
   UserTables user;
   std::map<int, BandTables> bands;  // by Greek order
   std::map<int64_t, std::pair<std::vector<double>, std::vector<double>>> rules;
-  DevBuf radius, weight, wtheta, wl, m, fractions, chunk_n, chunk_n_slab, chunk_row, chunk_acc, plan_units,
+  DevBuf radius, weight, wtheta, wdiff, unit_norm, wl, m, fractions, chunk_n, chunk_n_slab, chunk_row, chunk_acc, plan_units,
       unit_acc, unit_slots, slots, items, proj_items, slot_index, slot_greek, X, uz, ux,
       chunk_sums, err, acc, counter, values, phase, greek;
+  // Pass 1 of the adaptive ensemble.
+  DevBuf p1_radius, p1_wl, p1_scratch, p1_uz, p1_ux, p1_q, p1_n, p1_status;
   std::vector<int> chunk_n_host;
   int* pinned_chunk_n = nullptr;
   size_t pinned_cap = 0;
@@ -363,9 +366,10 @@ std::string node_message(int status, double lambda, double r) {
 
 struct FixedCall {
   // Host copies needed for error messages.
-  std::vector<double> radius;  // [n_dist][n_nodes]
+  std::vector<double> radius;  // [n_dist][n_nodes], or [n_units][n_nodes] with per_unit
   std::vector<double> wl_host;
   int64_t n_dist = 0, n_wl = 0, n_nodes = 0;
+  bool per_unit = false;
 };
 
 // The device pipeline; wl_dev and m_dev are device arrays, outputs device arrays.
@@ -388,11 +392,26 @@ struct DerivOutput {
   double* d_greek = nullptr;
 };
 
+// Adaptive panels (pass 2 of the adaptive ensemble): each unit's own nodes, two GK15 panels per
+// chunk of 32 (host arrays [n_units][n_nodes], radius 0 for padding), the error weights, the
+// per-unit normalization (8 doubles, see FinalArgs) and the device error outputs.
+struct AdaptiveInput {
+  bool on = false;
+  const double* radius = nullptr;
+  const double* weight = nullptr;
+  const double* wdiff = nullptr;
+  const double* unit_norm = nullptr;
+  double* errors = nullptr;
+  double* phase_err = nullptr;
+  double* greek_err = nullptr;
+};
+
 void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, const double* wl_dev,
                int64_t n_wl, const double* m_dev, const double* mu, int64_t n_mu,
                const scatrs_fixed_options* opt, double* values, double* phase, double* greek,
                cudaStream_t s, FixedCall* call, const LayerInput& layers = LayerInput(),
-               const DerivOutput& dv = DerivOutput()) {
+               const DerivOutput& dv = DerivOutput(),
+               const AdaptiveInput& ad = AdaptiveInput()) {
   const int64_t n_units = n_dist * n_wl;
   check_options(opt, n_units, n_mu, mu, dv.on ? dv.n_theta + 2 : 0);
   if (n_units == 0) return;
@@ -414,7 +433,7 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
                       "derivatives need every distribution of one kind (distribution " +
                           std::to_string(d) + " differs)"};
   }
-  for (int64_t d = 0; d < n_dist; ++d) {
+  for (int64_t d = 0; d < n_dist && !ad.on; ++d) {
     std::string msg;
     if (!validate_distribution(dists[d].kind, dists[d].param, &msg))
       throw Failure{SCATRS_INVALID_INPUT, "distribution " + std::to_string(d) + ": " + msg};
@@ -455,16 +474,26 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
     SB_CUDA(cudaMemcpyAsync(c.fractions.get(n_dist * (L_layers - 1) * 8), layers.fractions,
                             n_dist * (L_layers - 1) * 8, cudaMemcpyHostToDevice, s));
   }
-  SB_CUDA(cudaMemcpyAsync(c.radius.get(radius.size() * 8), radius.data(), radius.size() * 8,
-                          cudaMemcpyHostToDevice, s));
-  SB_CUDA(cudaMemcpyAsync(c.weight.get(weight.size() * 8), weight.data(), weight.size() * 8,
-                          cudaMemcpyHostToDevice, s));
+  if (ad.on) {
+    // Nodes per unit.
+    const size_t cnt = (size_t)n_units * n_nodes;
+    SB_CUDA(cudaMemcpyAsync(c.radius.get(cnt * 8), ad.radius, cnt * 8, cudaMemcpyHostToDevice, s));
+    SB_CUDA(cudaMemcpyAsync(c.weight.get(cnt * 8), ad.weight, cnt * 8, cudaMemcpyHostToDevice, s));
+    SB_CUDA(cudaMemcpyAsync(c.wdiff.get(cnt * 8), ad.wdiff, cnt * 8, cudaMemcpyHostToDevice, s));
+    SB_CUDA(cudaMemcpyAsync(c.unit_norm.get((size_t)n_units * 64), ad.unit_norm,
+                            (size_t)n_units * 64, cudaMemcpyHostToDevice, s));
+  } else {
+    SB_CUDA(cudaMemcpyAsync(c.radius.get(radius.size() * 8), radius.data(), radius.size() * 8,
+                            cudaMemcpyHostToDevice, s));
+    SB_CUDA(cudaMemcpyAsync(c.weight.get(weight.size() * 8), weight.data(), weight.size() * 8,
+                            cudaMemcpyHostToDevice, s));
+  }
   if (dv.on)
     SB_CUDA(cudaMemcpyAsync(c.wtheta.get(wtheta.size() * 8), wtheta.data(), wtheta.size() * 8,
                             cudaMemcpyHostToDevice, s));
   // Blocks of sums per quantity (values, then each derivative) and coefficient rows per term
   // of a chunk (two 16-node halves with derivatives).
-  const int n_blk = dv.on ? 3 + dv.n_theta : 1;
+  const int n_blk = dv.on ? 3 + dv.n_theta : (ad.on ? 2 : 1);
   const int rows_per_term = dv.on ? 2 : 1;  unsigned long long* err = c.err.as<unsigned long long>(2);
   SB_CUDA(cudaMemsetAsync(err, 0xff, 2 * sizeof(unsigned long long), s));
   // 2. Plan: every chunk's largest number of terms.
@@ -478,6 +507,7 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
   pa.n_chunks = n_chunks;
   int* chunk_n_all = c.chunk_n.as<int>(n_chunks);
   pa.chunk_n = chunk_n_all;
+  pa.per_unit = ad.on ? 1 : 0;
   timed_launch(K_PLAN, s, [&] { launch_plan_chunks(pa, s); });
   SB_CUDA(cudaGetLastError());
   if (c.pinned_cap < (size_t)n_chunks) {
@@ -607,7 +637,7 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
       S.nu = count[sl];
       S.sl0 = sl0;
       S.pi0 = pi0;
-      S.pi_cap = nb + S.n_slots / 32 + 1;
+      S.pi_cap = 2 * nb + S.n_slots / 32 + 1;
       S.it0 = it0;
       u0 += S.nu;
       sl0 += S.n_slots;
@@ -686,6 +716,10 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
     ka.n_theta = dv.n_theta;
     ka.wtheta = c.wtheta.as<double>(0);
   }
+  if (ad.on) {
+    ka.per_unit = 1;
+    ka.wdiff = c.wdiff.as<double>(0);
+  }
   UnitArgs ua{};
   ua.radius = ka.radius;
   ua.weight = ka.weight;
@@ -712,6 +746,8 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
   ua.deriv = ka.deriv;
   ua.n_theta = ka.n_theta;
   ua.wtheta = ka.wtheta;
+  ua.per_unit = ka.per_unit;
+  ua.wdiff = ka.wdiff;
   ProjArgs pj{};
   pj.cpu = cpu;
   pj.greek_order = L;
@@ -719,6 +755,7 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
   pj.chunk_sums = chunk_sums;
   pj.slot_greek = slot_greek;
   pj.raw = dv.on ? 1 : 0;
+  if (ad.on) pj.unit_norm = c.unit_norm.as<double>(0);
   if (bt) {
     pj.bands = bt->desc_d.as<BandDesc>(0);
     pj.band_d = bt->d_d.as<double>(0);
@@ -744,6 +781,12 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
     fa.d_values = dv.d_values;
     fa.d_phase = n_mu > 0 ? dv.d_phase : nullptr;
     fa.d_greek = L >= 0 ? dv.d_greek : nullptr;
+  }
+  if (ad.on) {
+    fa.unit_norm = c.unit_norm.as<double>(0);
+    fa.errors = ad.errors;
+    fa.phase_err = n_mu > 0 ? ad.phase_err : nullptr;
+    fa.greek_err = L >= 0 ? ad.greek_err : nullptr;
   }
   std::vector<std::pair<double, int64_t>> order;  // work items by cost
   std::vector<int> per_band;
@@ -793,6 +836,8 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
               P_slots[nslot].band = b;
               P_slots[nslot].unit = (int)lu;
               P_slots[nslot].off = band_acc;
+              P_slots[nslot].kind = ad.on ? blk : 0;
+              P_slots[nslot].pad = 0;
               band_acc += 4 * (int64_t)band_nq[b];
               ++nslot;
             }
@@ -821,23 +866,29 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
     // Projection tiles: the slab's slots grouped by band (largest bands first), 32 at a time.
     S.n_proj = 0;
     if (bt && S.n_slots > 0) {
-      per_band.assign(nb + 1, 0);
-      for (int64_t k = 0; k < S.n_slots; ++k) per_band[P_slots[k].band + 1]++;
-      std::vector<int64_t> start(nb + 1, 0), cursor(nb, 0);
+      // Slots grouped by (band, kind): a tile's slots share the band's matrices and the kind
+      // (values or bounds) of its projection.
+      const int nk = ad.on ? 2 : 1, ng = nb * nk;
+      per_band.assign(ng + 1, 0);
+      auto key = [&](const BandSlot& x) { return x.band * nk + (nk > 1 ? x.kind : 0); };
+      for (int64_t k = 0; k < S.n_slots; ++k) per_band[key(P_slots[k]) + 1]++;
+      std::vector<int64_t> start(ng + 1, 0), cursor(ng, 0);
       // Bands in descending order occupy the slot-index list from the front.
       int64_t pos = 0;
-      for (int b = nb - 1; b >= 0; --b) {
-        start[b] = pos;
-        pos += per_band[b + 1];
+      for (int g = ng - 1; g >= 0; --g) {
+        start[g] = pos;
+        pos += per_band[g + 1];
       }
-      for (int b = 0; b < nb; ++b) cursor[b] = start[b];
-      for (int64_t k = 0; k < S.n_slots; ++k) P_sidx[cursor[P_slots[k].band]++] = (int)k;
-      for (int b = nb - 1; b >= 0; --b)
-        for (int64_t k0 = 0; k0 < per_band[b + 1]; k0 += 32) {
+      for (int g = 0; g < ng; ++g) cursor[g] = start[g];
+      for (int64_t k = 0; k < S.n_slots; ++k) P_sidx[cursor[key(P_slots[k])]++] = (int)k;
+      for (int g = ng - 1; g >= 0; --g)
+        for (int64_t k0 = 0; k0 < per_band[g + 1]; k0 += 32) {
           ProjItem& pi = P_proj[S.n_proj++];
-          pi.band = b;
-          pi.count = (int)std::min<int64_t>(32, per_band[b + 1] - k0);
-          pi.first = start[b] + k0;
+          pi.band = g / nk;
+          pi.kind = g % nk;
+          pi.pad = 0;
+          pi.count = (int)std::min<int64_t>(32, per_band[g + 1] - k0);
+          pi.first = start[g] + k0;
         }
     }
     // Upload (pinned source: asynchronous) once the staging half's previous upload is done.
@@ -886,6 +937,7 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
       pj.n_items = (int)S.n_proj;
       pj.slot_index = slot_index_d + S.sl0;
       pj.slots = slots_d + S.sl0;
+      pj.units = ka.units;
       timed_launch(K_PROJ, s, [&] { launch_proj(pj, s); });
       SB_CUDA(cudaGetLastError());
     }
@@ -897,7 +949,7 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
     timed_launch(K_FINAL, s, [&] { launch_final(fa, s); });
     SB_CUDA(cudaGetLastError());
   }
-  if (call) {
+  if (call && !ad.on) {
     call->radius = std::move(radius);
     call->n_dist = n_dist;
     call->n_wl = n_wl;
@@ -919,7 +971,9 @@ void check_device_errors(Context& c, cudaStream_t s, const FixedCall* call) {
       int64_t d = (key / call->n_nodes) % call->n_dist;
       int64_t i = key / call->n_nodes / call->n_dist;
       double lam = i < (int64_t)call->wl_host.size() ? call->wl_host[i] : NAN;
-      msg = node_message(status, lam, call->radius[d * call->n_nodes + j]);
+      const int64_t row = call->per_unit ? d * call->n_wl + i : d;
+      const size_t at = (size_t)(row * call->n_nodes + j);
+      msg = node_message(status, lam, at < call->radius.size() ? call->radius[at] : NAN);
     }
     throw Failure{status, msg};
   }
@@ -1045,6 +1099,270 @@ int scatrs_ensemble_fixed_d(const scatrs_distribution* dists, int64_t n_dist,
     if (gl > 0 && greek) SB_CUDA(cudaMemcpyAsync(greek, g_d, gl * 8, cudaMemcpyDeviceToHost, s));
     if (gl > 0 && d_greek)
       SB_CUDA(cudaMemcpyAsync(d_greek, dv.d_greek, P * gl * 8, cudaMemcpyDeviceToHost, s));
+    SB_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+int scatrs_ensemble_adaptive(const scatrs_distribution* dists, int64_t n_dist, int32_t batch,
+                             const double* wavelengths, int64_t n_wl, const double* m,
+                             const double* mu, int64_t n_mu,
+                             const scatrs_adaptive_options* options, double* values,
+                             double* errors, double* phase, double* phase_err, double* greek,
+                             double* greek_err, int8_t* converged, int64_t* panels, char* err,
+                             size_t err_len) {
+  return guarded(err, err_len, [&] {
+    if (!options) throw Failure{SCATRS_INVALID_INPUT, "options must not be NULL"};
+    if (n_dist < 0 || n_wl < 0) throw Failure{SCATRS_INVALID_INPUT, "negative sizes"};
+    const adaptive::Options o{options->rtol, options->max_panels,
+                              options->allow_unvalidated != 0, options->refine_backscatter != 0};
+    // ensemble/mod.rs:688-720.
+    if (!(o.rtol >= 1e-13 && o.rtol <= 0.1)) {
+      char buf[80];
+      snprintf(buf, sizeof buf, "rtol must be in [1e-13, 0.1], got %g", o.rtol);
+      throw Failure{SCATRS_INVALID_INPUT, buf};
+    }
+    if (o.max_panels < 1) throw Failure{SCATRS_INVALID_INPUT, "max_panels must be at least 1"};
+    for (int64_t i = 0; i < n_wl; ++i)
+      if (!(std::isfinite(wavelengths[i]) && wavelengths[i] > 0.0))
+        throw Failure{SCATRS_INVALID_INPUT, "wavelength " + std::to_string(i) +
+                                                " must be finite and > 0"};
+    scatrs_fixed_options fo{32, options->greek_order, options->normalized,
+                            options->allow_unvalidated};
+    const int64_t n_units = n_dist * n_wl;
+    check_options(&fo, n_units, n_mu, mu);
+    if (n_units == 0) return;
+    std::vector<adaptive::Part> parts;
+    for (int64_t d = 0; d < n_dist; ++d) {
+      try {
+        parts.push_back(adaptive::make_part(dists[d].kind, dists[d].param, o.rtol));
+      } catch (const adaptive::Error& e) {
+        throw Failure{e.status, "distribution " + std::to_string(d) + ": " + e.msg};
+      }
+    }
+    Context& c = context();
+    std::lock_guard<std::mutex> lk(c.mtx);
+    cudaStream_t s = 0;
+    double* wl_d = c.wl.as<double>(n_wl);
+    SB_CUDA(cudaMemcpyAsync(wl_d, wavelengths, n_wl * 8, cudaMemcpyHostToDevice, s));
+    double2* m_wl = c.fractions.as<double2>(n_wl);  // the index per wavelength, for pass 1
+    SB_CUDA(cudaMemcpyAsync(m_wl, m, n_wl * 16, cudaMemcpyHostToDevice, s));
+    // Node evaluations on the device, in batches of at most kRows scratch rows.
+    constexpr int64_t kRows = int64_t(1) << 26;
+    auto eval = [&](const std::vector<adaptive::Query>& qs,
+                    std::vector<adaptive::NodeResult>& res) {
+      size_t k0 = 0;
+      std::vector<double> r;
+      std::vector<int> wi;
+      std::vector<int64_t> off;
+      while (k0 < qs.size()) {
+        r.clear();
+        wi.clear();
+        off.assign(1, 0);
+        size_t k1 = k0;
+        while (k1 < qs.size()) {
+          const double x = 2.0 * 3.14159265358979323846 * qs[k1].r / wavelengths[qs[k1].wl];
+          const int64_t cap = (std::isfinite(x) && x > 0.0 && x <= 1e6)
+                                  ? (int64_t)std::ceil(x + 6.0 * std::cbrt(x) + 3.0) + 4
+                                  : 0;
+          if (k1 > k0 && off.back() + cap > kRows) break;
+          r.push_back(qs[k1].r);
+          wi.push_back(qs[k1].wl);
+          off.push_back(off.back() + cap);
+          ++k1;
+        }
+        const int64_t n = (int64_t)r.size(), rows = std::max<int64_t>(off.back(), 1);
+        Pass1Args a{};
+        a.radius = c.p1_radius.as<double>(n);
+        a.wl_index = c.p1_wl.as<int>(n);
+        a.scratch = c.p1_scratch.as<int64_t>(n + 1);
+        a.uz = c.p1_uz.as<double2>(rows);
+        a.ux = c.p1_ux.as<double>(rows);
+        a.q = c.p1_q.as<double>(6 * n);
+        a.n_terms = c.p1_n.as<int64_t>(n);
+        a.status = c.p1_status.as<int>(n);
+        a.wl = wl_d;
+        a.m = m_wl;
+        a.n = n;
+        a.allow_unvalidated = o.allow_unvalidated ? 1 : 0;
+        SB_CUDA(cudaMemcpyAsync((void*)a.radius, r.data(), n * 8, cudaMemcpyHostToDevice, s));
+        SB_CUDA(cudaMemcpyAsync((void*)a.wl_index, wi.data(), n * 4, cudaMemcpyHostToDevice, s));
+        SB_CUDA(cudaMemcpyAsync((void*)a.scratch, off.data(), (n + 1) * 8,
+                                cudaMemcpyHostToDevice, s));
+        timed_launch(K_NODES, s, [&] { launch_pass1(a, s); });
+        SB_CUDA(cudaGetLastError());
+        std::vector<double> q(6 * n);
+        std::vector<int64_t> nt(n);
+        std::vector<int> st(n);
+        SB_CUDA(cudaMemcpyAsync(q.data(), a.q, 6 * n * 8, cudaMemcpyDeviceToHost, s));
+        SB_CUDA(cudaMemcpyAsync(nt.data(), a.n_terms, n * 8, cudaMemcpyDeviceToHost, s));
+        SB_CUDA(cudaMemcpyAsync(st.data(), a.status, n * 4, cudaMemcpyDeviceToHost, s));
+        SB_CUDA(cudaStreamSynchronize(s));
+        for (int64_t k = 0; k < n; ++k) {
+          adaptive::NodeResult& x = res[k0 + k];
+          for (int j = 0; j < 6; ++j) x.q[j] = q[6 * k + j];
+          x.n = nt[k];
+          x.status = st[k];
+        }
+        k0 = k1;
+      }
+    };
+    // Jobs: a batch shares one group per wavelength (single radii alone); otherwise every
+    // distribution is its own call (engine.rs:236-296).
+    std::vector<adaptive::Job> jobs;
+    std::vector<int> job_of(n_units, -1);
+    std::vector<int> place(n_units, 0);
+    for (int64_t i = 0; i < n_wl; ++i) {
+      if (batch) {
+        adaptive::Job jb;
+        jb.wl = (int)i;
+        for (int64_t d = 0; d < n_dist; ++d)
+          if (parts[d].support != adaptive::POINT) {
+            place[d * n_wl + i] = (int)jb.parts.size();
+            job_of[d * n_wl + i] = (int)jobs.size();
+            jb.parts.push_back((int)d);
+          }
+        if (!jb.parts.empty()) jobs.push_back(jb);
+      } else {
+        for (int64_t d = 0; d < n_dist; ++d)
+          if (parts[d].support != adaptive::POINT) {
+            job_of[d * n_wl + i] = (int)jobs.size();
+            adaptive::Job jb;
+            jb.wl = (int)i;
+            jb.parts = {(int)d};
+            jobs.push_back(jb);
+          }
+      }
+    }
+    // Single radii: their node checked once.
+    std::vector<adaptive::Query> points;
+    std::vector<int64_t> point_unit;
+    for (int64_t d = 0; d < n_dist; ++d)
+      if (parts[d].support == adaptive::POINT)
+        for (int64_t i = 0; i < n_wl; ++i) {
+          points.push_back({parts[d].lo, (int)i});
+          point_unit.push_back(d * n_wl + i);
+        }
+    std::vector<adaptive::NodeResult> point_res(points.size());
+    if (!points.empty()) eval(points, point_res);
+    adaptive::pass1(jobs, parts, wavelengths, o, eval);
+    // The first error in (wavelength, distribution) order.
+    {
+      int64_t first = n_units;
+      int status = 0;
+      std::string msg;
+      for (int64_t u = 0; u < n_units; ++u) {
+        const int64_t key = (u % n_wl) * n_dist + u / n_wl;
+        if (job_of[u] >= 0 && jobs[job_of[u]].status != 0 && key < first) {
+          first = key;
+          status = jobs[job_of[u]].status;
+          msg = jobs[job_of[u]].msg;
+        }
+      }
+      for (size_t k = 0; k < points.size(); ++k) {
+        const int64_t u = point_unit[k], key = (u % n_wl) * n_dist + u / n_wl;
+        if (point_res[k].status != 0 && key < first) {
+          first = key;
+          status = point_res[k].status;
+          msg = node_message(point_res[k].status, wavelengths[u % n_wl], points[k].r);
+        }
+      }
+      if (status != 0) throw Failure{status, msg};
+    }
+    // Pass 2: every unit's nodes, up to two panels per chunk of 32 (nodes 0-14 and 16-30),
+    // two only when their projector bands agree, so that each panel's tables go to its own
+    // band (engine.rs:1530-1543).
+    std::vector<std::vector<int64_t>> slot_of(jobs.size());
+    int64_t n_nodes = 32;
+    for (size_t k = 0; k < jobs.size(); ++k) {
+      const auto& jb = jobs[k];
+      int64_t next = 0;  // the next free half-chunk (16 nodes)
+      for (size_t pi = 0; pi < jb.panels.size(); ++pi) {
+        if (next % 2 == 1 && bucket(jb.panel_terms[pi]) != bucket(jb.panel_terms[pi - 1])) ++next;
+        slot_of[k].push_back(16 * next);
+        ++next;
+      }
+      n_nodes = std::max<int64_t>(n_nodes, 32 * ((next + 1) / 2));
+    }
+    if ((double)n_units * (double)n_nodes > 4e9)
+      throw Failure{SCATRS_INVALID_INPUT, "too many (unit, node) pairs for one call"};
+    std::vector<double> radius((size_t)n_units * n_nodes, 0.0), weight(radius.size(), 0.0),
+        wdiff(radius.size(), 0.0), norm((size_t)n_units * 8, 0.0);
+    std::vector<double> m_unit(2 * n_units);
+    for (int64_t u = 0; u < n_units; ++u) {
+      const int64_t d = u / n_wl, i = u % n_wl;
+      m_unit[2 * u] = m[2 * i];
+      m_unit[2 * u + 1] = m[2 * i + 1];
+      const adaptive::Part& p = parts[d];
+      double* nr = &radius[(size_t)u * n_nodes];
+      double* nw = &weight[(size_t)u * n_nodes];
+      double* nd = &wdiff[(size_t)u * n_nodes];
+      double* un = &norm[(size_t)u * 8];
+      if (p.support == adaptive::POINT) {
+        nr[0] = p.lo;
+        nw[0] = 1.0;
+        un[0] = 1.0;
+        un[3] = 1.0;
+        converged[u] = 1;
+        panels[u] = 0;
+        continue;
+      }
+      const adaptive::Job& jb = jobs[job_of[u]];
+      for (size_t pi = 0; pi < jb.panels.size(); ++pi) {
+        adaptive::Node g[15];
+        adaptive::gk15(jb.panels[pi].first, jb.panels[pi].second, g);
+        const size_t base = (size_t)slot_of[job_of[u]][pi];
+        for (int k = 0; k < 15; ++k) {
+          const double r = std::exp(g[k].t), ur = p.u(r) * r;
+          nr[base + k] = r;
+          nw[base + k] = g[k].wk * ur;
+          nd[base + k] = g[k].wk * ur - g[k].wg * ur;
+        }
+      }
+      un[0] = p.mom.z;
+      un[1] = p.mom.ez;
+      un[2] = p.support == adaptive::UNBOUNDED ? 0.2 * o.rtol : 0.0;
+      un[4] = p.mom.v[0];
+      un[5] = p.mom.e[0];
+      un[6] = p.mom.v[1];
+      un[7] = p.mom.e[1];
+      converged[u] = jb.converged[place[u]] ? 1 : 0;
+      panels[u] = (int64_t)jb.panels.size();
+    }
+    double* m_d = c.m.as<double>(2 * n_units);
+    SB_CUDA(cudaMemcpyAsync(m_d, m_unit.data(), 2 * n_units * 8, cudaMemcpyHostToDevice, s));
+    fo.n_nodes = (int32_t)n_nodes;
+    int64_t vl, pl, gl;
+    scatrs_ensemble_fixed_sizes(n_units, n_mu, options->greek_order, &vl, &pl, &gl);
+    double* v_d = c.values.as<double>(2 * vl);
+    double* p_d = pl > 0 ? c.phase.as<double>(2 * pl) : nullptr;
+    double* g_d = gl > 0 ? c.greek.as<double>(2 * gl) : nullptr;
+    AdaptiveInput ad;
+    ad.on = true;
+    ad.radius = radius.data();
+    ad.weight = weight.data();
+    ad.wdiff = wdiff.data();
+    ad.unit_norm = norm.data();
+    ad.errors = v_d + vl;
+    ad.phase_err = p_d ? p_d + pl : nullptr;
+    ad.greek_err = g_d ? g_d + gl : nullptr;
+    FixedCall call;
+    call.wl_host.assign(wavelengths, wavelengths + n_wl);
+    call.per_unit = true;
+    call.n_dist = n_dist;
+    call.n_wl = n_wl;
+    call.n_nodes = n_nodes;
+    run_fixed(c, dists, n_dist, wl_d, n_wl, m_d, mu, n_mu, &fo, v_d, p_d, g_d, s, &call,
+              LayerInput(), DerivOutput(), ad);
+    call.radius = std::move(radius);
+    check_device_errors(c, s, &call);
+    SB_CUDA(cudaMemcpyAsync(values, v_d, vl * 8, cudaMemcpyDeviceToHost, s));
+    if (errors) SB_CUDA(cudaMemcpyAsync(errors, ad.errors, vl * 8, cudaMemcpyDeviceToHost, s));
+    if (pl > 0 && phase) SB_CUDA(cudaMemcpyAsync(phase, p_d, pl * 8, cudaMemcpyDeviceToHost, s));
+    if (pl > 0 && phase_err)
+      SB_CUDA(cudaMemcpyAsync(phase_err, ad.phase_err, pl * 8, cudaMemcpyDeviceToHost, s));
+    if (gl > 0 && greek) SB_CUDA(cudaMemcpyAsync(greek, g_d, gl * 8, cudaMemcpyDeviceToHost, s));
+    if (gl > 0 && greek_err)
+      SB_CUDA(cudaMemcpyAsync(greek_err, ad.greek_err, gl * 8, cudaMemcpyDeviceToHost, s));
     SB_CUDA(cudaStreamSynchronize(s));
   });
 }
@@ -1252,7 +1570,7 @@ void scatrs_release(void) {
   std::lock_guard<std::mutex> lk(g_ctx_mtx);
   if (dev < (int)g_ctx.size() && g_ctx[dev]) {
     Context& c = *g_ctx[dev];
-    for (DevBuf* b : {&c.radius, &c.weight, &c.wtheta, &c.wl, &c.m, &c.fractions, &c.chunk_n, &c.chunk_n_slab,
+    for (DevBuf* b : {&c.radius, &c.weight, &c.wtheta, &c.wdiff, &c.unit_norm, &c.wl, &c.m, &c.fractions, &c.chunk_n, &c.chunk_n_slab,
                       &c.chunk_row, &c.chunk_acc, &c.plan_units, &c.unit_acc, &c.unit_slots,
                       &c.slots, &c.items, &c.proj_items, &c.slot_index, &c.slot_greek,
                       &c.X, &c.uz, &c.ux, &c.chunk_sums, &c.err, &c.acc,

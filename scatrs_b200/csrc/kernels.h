@@ -14,6 +14,7 @@ struct PlanArgs {
   int n_dist, n_wl, n_nodes, cpu;
   int64_t n_chunks;
   int* chunk_n;
+  int per_unit;  // nodes per unit ([n_units][n_nodes]) rather than per distribution
 };
 
 // K-a over one slab: its units (global indices), each with cpu chunks of 32 nodes.
@@ -43,6 +44,11 @@ struct MieFixedArgs {
   int deriv;
   int n_theta;
   const double* wtheta;  // [n_dist][n_nodes][3]
+  // Adaptive panels: nodes per unit ([n_units][n_nodes], radius 0 for padding), two GK15 panels
+  // per chunk (lanes 0-15 and 16-31), the error weights (w_K - w_G) u r in wdiff, and
+  // chunk_sums [n_chunks][2][8]: the Kronrod sums, then the sums of |Kronrod - Gauss| per panel.
+  int per_unit;
+  const double* wdiff;
 };
 
 struct MieNodesArgs {
@@ -83,11 +89,14 @@ struct WorkItem {
 };
 
 // One band accumulator of a unit: the band, the unit (slab-local) and the offset of its
-// 4 n_q doubles.
+// 4 n_q doubles; kind 1 marks the error sums of an adaptive call (the values' slot precedes
+// it).
 struct BandSlot {
   int band;
   int unit;
   int64_t off;
+  int kind;
+  int pad;
 };
 
 // A tile of up to 32 band slots of one band, projected together (they share the band's
@@ -96,6 +105,8 @@ struct ProjItem {
   int band;
   int count;
   int64_t first;  // into ProjArgs::slot_index
+  int kind;       // the slots' kind: 0 values, 1 error bounds (projected with |d|)
+  int pad;
 };
 
 // K-d over one slab: each band slot's averaged tables projected onto its Greek coefficients,
@@ -113,6 +124,10 @@ struct ProjArgs {
   int greek_order;
   double* slot_greek;
   int raw;  // project the raw sums (derivatives: averaged after the projection)
+  // Adaptive: per unit (z, ez, truncation, ...; see FinalArgs): values averaged as s / z, error
+  // sums as (e + |s/z| ez) / z + truncation |s/z| (engine.rs:1782-1800), then bounded with |d|.
+  const double* unit_norm;
+  const int* units;  // slab-local unit -> unit
 };
 
 // K-b and K-c over one slab: the work items write the per-unit accumulators (zeroed before).
@@ -141,6 +156,8 @@ struct UnitArgs {
   const double* band_go;
   double* acc;
   int* work_counter;
+  int per_unit;
+  const double* wdiff;  // adaptive: the error weights (see MieFixedArgs)
   // Derivatives (deriv != 0): n_theta distribution parameters, their node weights in wtheta
   // ([n_dist][n_nodes][3]).
   int deriv;
@@ -174,6 +191,29 @@ struct FinalArgs {
   double* d_values;
   double* d_phase;
   double* d_greek;
+  // Adaptive: per unit 8 doubles (z, ez, truncation, point, <r^2>, its error, <r^3>, its
+  // error), and the error outputs laid out as the values.
+  const double* unit_norm;
+  double* errors;
+  double* phase_err;
+  double* greek_err;
+};
+
+// Pass 1 of the adaptive ensemble: each node's per-particle quantities 1, pi r^2 Q_ext,
+// pi r^2 Q_sca, pi r^2 Q_sca g, pi r^2 Q_back, pi r^2 Q_abs and its number of terms.
+struct Pass1Args {
+  const double* radius;
+  const int* wl_index;
+  const double* wl;
+  const double2* m;          // per wavelength
+  int64_t n;
+  const int64_t* scratch;    // each node's first scratch row; rows scratch[i]..scratch[i+1]-1
+  double2* uz;
+  double* ux;
+  double* q;                 // [n][6]
+  int64_t* n_terms;
+  int* status;
+  int allow_unvalidated;
 };
 
 void launch_plan_chunks(const PlanArgs& a, cudaStream_t s);
@@ -183,5 +223,6 @@ int unit_kernel_blocks_per_sm();
 void launch_units(const UnitArgs& a, int grid, cudaStream_t s);
 void launch_proj(const ProjArgs& a, cudaStream_t s);
 void launch_final(const FinalArgs& a, cudaStream_t s);
+void launch_pass1(const Pass1Args& a, cudaStream_t s);
 
 }  // namespace sb

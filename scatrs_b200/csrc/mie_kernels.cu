@@ -30,10 +30,12 @@ __global__ void plan_chunks_kernel(PlanArgs a) {
   int j = c * 32 + lane;
   int64_t n = 0;
   if (j < a.n_nodes) {
-    double r = a.radius[d * a.n_nodes + j];
-    double x = 2.0 * kPi * r / a.wl[i];
-    n = default_n_max(x);
-    if (n > (1 << 20)) n = 1 << 20;
+    double r = a.radius[(a.per_unit ? unit : d) * a.n_nodes + j];
+    if (r > 0.0) {
+      double x = 2.0 * kPi * r / a.wl[i];
+      n = default_n_max(x);
+      if (n > (1 << 20)) n = 1 << 20;
+    }
   }
   int nn = (int)n;
   for (int off = 16; off > 0; off >>= 1) {
@@ -63,10 +65,12 @@ __device__ __forceinline__ void mie_chunk(const MieFixedArgs& a) {
   s.ux = a.ux + (row0 + 2 * (int64_t)chunk) * 32 + lane;
   s.stride = 32;
   double q[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  double qe[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // adaptive: weighted by w_K - w_G
   int64_t n = 0;
-  if (j < a.n_nodes) {
-    const double r = a.radius[d * a.n_nodes + j];
-    const double w = a.weight[d * a.n_nodes + j];
+  const int64_t node = (a.per_unit ? unit : d) * a.n_nodes + j;
+  if (j < a.n_nodes && a.radius[node] > 0.0) {
+    const double r = a.radius[node];
+    const double w = a.weight[node];
     const double x = 2.0 * kPi * r / a.wl[i];
     n = default_n_max(x);
     auto emit = [&](int64_t k, cplx an, cplx bn) {
@@ -123,16 +127,30 @@ __device__ __forceinline__ void mie_chunk(const MieFixedArgs& a) {
       const double qv[8] = {1.0,           area * e.q_ext, area * e.q_sca, area * e.q_sca * e.g,
                             area * e.q_abs, area * e.q_back, r * r,         r * r * r};
       for (int k = 0; k < 8; ++k) q[k] = w * qv[k];
+      if (a.wdiff) {
+        const double wd = a.wdiff[node];
+        for (int k = 0; k < 8; ++k) qe[k] = wd * qv[k];
+      }
     }
   }
   // Orders above the node's own N are zero up to the chunk's.
   for (int64_t k = n + 1; k <= nc; ++k)
     *reinterpret_cast<double4*>(X + (k - 1) * 128) = make_double4(0.0, 0.0, 0.0, 0.0);
   // The chunk's weighted sums, in a fixed tree order.
+  const int stride = a.wdiff ? 16 : 8;
   for (int k = 0; k < 8; ++k) {
     double v = q[k];
     for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-    if (lane == 0) a.chunk_sums[(int64_t)chunk * 8 + k] = v;
+    if (lane == 0) a.chunk_sums[(int64_t)chunk * stride + k] = v;
+  }
+  if (a.wdiff) {
+    // |Kronrod - Gauss| of each of the chunk's two panels (lanes 0-15, 16-31), then added.
+    for (int k = 0; k < 8; ++k) {
+      double v = qe[k];
+      for (int off = 8; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+      const double other = __shfl_sync(0xffffffffu, v, 16);
+      if (lane == 0) a.chunk_sums[(int64_t)chunk * 16 + 8 + k] = fabs(v) + fabs(other);
+    }
   }
 }
 
@@ -279,6 +297,51 @@ __global__ void __launch_bounds__(128) mie_nodes_kernel(MieNodesArgs a) {
     a.eff[5 * t + 3] = e.q_back;
     a.eff[5 * t + 4] = e.g;
   }
+}
+
+// Pass 1 of the adaptive ensemble: one thread per node (engine.rs:369-449 quantities1 for
+// spheres). Scratch rows scratch[t]..scratch[t+1]-1 hold u_k(mx) and u_k(x); a node whose
+// number of terms does not fit them reports status 1 (the host sizes them from the same
+// truncation rule with a margin).
+__global__ void __launch_bounds__(128) pass1_kernel(Pass1Args a) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.n) return;
+  const double r = a.radius[t];
+  const int wi = a.wl_index[t];
+  const double x = 2.0 * kPi * r / a.wl[wi];
+  const cplx m = mk(a.m[wi].x, a.m[wi].y);
+  int64_t n = default_n_max(x);
+  int st = check_node(x, m, n, a.allow_unvalidated != 0);
+  const int64_t off = a.scratch[t], cap = a.scratch[t + 1] - off;
+  if (st == 0 && n + 2 > cap) st = 1;
+  a.status[t] = st;
+  a.n_terms[t] = st == 0 ? n : 0;
+  double* q = a.q + 6 * t;
+  if (st != 0) {
+    for (int k = 0; k < 6; ++k) q[k] = 0.0;
+    return;
+  }
+  Scratch s;
+  s.uz = a.uz + off;
+  s.ux = a.ux + off;
+  s.stride = 1;
+  mie_prepare(x, m, n, s);
+  ValueSums vs;
+  const double asum = mie_finish(x, m, n, s, vs, [](int64_t, cplx, cplx) {});
+  const Eff e = efficiencies_from(x, asum, vs);
+  const double area = kPi * r * r;
+  q[0] = 1.0;
+  q[1] = area * e.q_ext;
+  q[2] = area * e.q_sca;
+  q[3] = area * e.q_sca * e.g;
+  q[4] = area * e.q_back;
+  q[5] = area * e.q_abs;
+}
+
+void launch_pass1(const Pass1Args& a, cudaStream_t s) {
+  const int threads = 128;
+  const int64_t blocks = (a.n + threads - 1) / threads;
+  if (blocks > 0) pass1_kernel<<<(unsigned)blocks, threads, 0, s>>>(a);
 }
 
 void launch_plan_chunks(const PlanArgs& a, cudaStream_t s) {

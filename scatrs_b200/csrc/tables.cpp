@@ -326,4 +326,30 @@ double density_gradient(int kind, const double* p, double r, double grad[3]) {
   return u;
 }
 
+DensityInfo density_info(int kind, const double* p) {
+  DensityInfo d{1.0, std::numeric_limits<double>::infinity()};
+  switch (kind) {
+    case 1:
+      d.reference = p[0];
+      d.log_width = std::log(p[1]);
+      break;
+    case 2: {
+      const double b = p[1], alpha = (1.0 - 3.0 * b) / b;
+      d.reference = alpha > 0.0 ? alpha * p[0] * b : p[0];
+      d.log_width = std::sqrt(b / (1.0 - 2.0 * b));
+      break;
+    }
+    case 3: {
+      const double alpha = p[0], b = p[1], g = p[2];
+      d.reference = std::pow(std::max(alpha, 1.0) / (b * g), 1.0 / g);
+      d.log_width = alpha > 0.0 ? 1.0 / std::sqrt(alpha * g) : 1.0 / g;
+      break;
+    }
+    case 4:
+      d.reference = p[0] >= 0.0 ? p[1] : p[2];
+      break;
+  }
+  return d;
+}
+
 }  // namespace sb

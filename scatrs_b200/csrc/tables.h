@@ -37,6 +37,13 @@ double density(int kind, const double* p, double r);
 // u(r) along them at a fixed reference radius (distribution.rs:370-441); the reference radius'
 // own dependence cancels in every average. Returns u(r).
 int parameter_count(int kind);
+
+// The reference radius, where the density is about 1, and the width of its peak in ln r
+// (infinite for a power law): Density of distribution.rs:292-336.
+struct DensityInfo {
+  double reference, log_width;
+};
+DensityInfo density_info(int kind, const double* p);
 double density_gradient(int kind, const double* p, double r, double grad[3]);
 
 }  // namespace sb

@@ -252,8 +252,47 @@ __device__ __forceinline__ void chunk_elements_d(const Smem& sm, const double ac
 
 }  // namespace
 
-template <bool kDeriv>
+// The error block of an adaptive call: |sum over panel A| + |sum over panel B| of the elements
+// weighted by w_K - w_G (sm.wth[0]), the chunk's panels being nodes 0-15 (this thread's node
+// ng) and 16-31 (node ng + 16); each panel reduced over its 16 nodes like chunk_elements.
+template <bool kUser>
+__device__ __forceinline__ void chunk_errors(const Smem& sm, const double accE[4][8],
+                                             const double accO[4][8], double v[2]) {
+  const int ng = threadIdx.x & 15;
+  double out[2] = {0.0, 0.0};
+#pragma unroll 1
+  for (int nd = 0; nd < 2; ++nd) {
+    const int node = ng + 16 * nd;
+    const double w = sm.wth[0][node], cu = sm.cu[node], ar = sm.area[node], sc = sm.sc[node];
+    double p[32];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      double eu_r = nd ? accE[r][4] : accE[r][0], eu_i = nd ? accE[r][5] : accE[r][1];
+      double ev_r = nd ? accE[r][6] : accE[r][2], ev_i = nd ? accE[r][7] : accE[r][3];
+      double ou_r = nd ? accO[r][4] : accO[r][0], ou_i = nd ? accO[r][5] : accO[r][1];
+      double ov_r = nd ? accO[r][6] : accO[r][2], ov_i = nd ? accO[r][7] : accO[r][3];
+      double ep[4], em[4];
+      elements4(eu_r + ov_r, eu_i + ov_i, ev_r + ou_r, ev_i + ou_i, ep);
+      elements4(eu_r - ov_r, eu_i - ov_i, ev_r - ou_r, ev_i - ou_i, em);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        p[r * 4 + e] = kUser ? w * ((cu * ep[e]) * ar) : w * (sc * ep[e]);
+        p[16 + r * 4 + e] = kUser ? w * ((cu * em[e]) * ar) : w * (sc * em[e]);
+      }
+    }
+    double vv[2];
+    reduce_scatter16(p, vv);
+    out[0] += fabs(vv[0]);
+    out[1] += fabs(vv[1]);
+  }
+  v[0] = out[0];
+  v[1] = out[1];
+}
+
+// kMode 0: values; 1: with the derivative blocks; 2: adaptive panels (values and errors).
+template <int kMode>
 __device__ __forceinline__ void unit_body(const UnitArgs& a) {
+  constexpr bool kDeriv = kMode == 1;
   __shared__ __align__(16) Smem sm;
   const int t = threadIdx.x, rg = t >> 4, ng = t & 15;
   // This thread's share of a reduced tile: side (+mu, -mu), row, two elements.
@@ -262,7 +301,7 @@ __device__ __forceinline__ void unit_body(const UnitArgs& a) {
   // Blocks of sums: the values, then (with derivatives) each distribution parameter, Re m and
   // Im m; halves: a chunk's coefficient rows are one 32-node tile, or two of 16 nodes with
   // their derivative columns.
-  const int n_blk = kDeriv ? 3 + a.n_theta : 1;
+  const int n_blk = kDeriv ? 3 + a.n_theta : (kMode == 2 ? 2 : 1);
   constexpr int kHalves = kDeriv ? 2 : 1;
   for (;;) {
     if (t == 0) sm.slot = atomicAdd(a.work_counter, 1);
@@ -287,21 +326,23 @@ __device__ __forceinline__ void unit_body(const UnitArgs& a) {
         const int j = c * 32 + t;
         double w = 0.0, cu = 0.0, ar = 0.0, sc = 0.0;
         double wth[3] = {0.0, 0.0, 0.0};
-        if (j < a.n_nodes) {
-          const double r = a.radius[d * a.n_nodes + j];
+        const int64_t node = (a.per_unit ? unit : d) * a.n_nodes + j;
+        if (j < a.n_nodes && a.radius[node] > 0.0) {
+          const double r = a.radius[node];
           const double x = 2.0 * kPi * r / lam;
-          w = a.weight[d * a.n_nodes + j];  // w_j u(r_j) r_j
+          w = a.weight[node];  // w_j u(r_j) r_j
           cu = 4.0 / (x * x);
           ar = kPi * r * r;
           sc = 4.0 / (x * x) * (kPi * r * r);
           if (kDeriv)
-            for (int p = 0; p < a.n_theta; ++p) wth[p] = a.wtheta[(d * a.n_nodes + j) * 3 + p];
+            for (int p = 0; p < a.n_theta; ++p) wth[p] = a.wtheta[node * 3 + p];
+          if (kMode == 2) wth[0] = a.wdiff[node];
         }
         sm.w[t] = w;
         sm.cu[t] = cu;
         sm.area[t] = ar;
         sm.sc[t] = sc;
-        if (kDeriv)
+        if (kDeriv || kMode == 2)
           for (int p = 0; p < 3; ++p) sm.wth[p][t] = wth[p];
       }
       __syncthreads();
@@ -321,6 +362,8 @@ __device__ __forceinline__ void unit_body(const UnitArgs& a) {
             for (int blk = 0; blk < n_blk; ++blk) {
               if (kDeriv)
                 chunk_elements_d<true>(sm, accE, accO, half, blk, a.n_theta, v);
+              else if (kMode == 2 && blk == 1)
+                chunk_errors<true>(sm, accE, accO, v);
               else
                 chunk_elements<true>(sm, accE, accO, v);
               if (j >= 0) {
@@ -345,6 +388,8 @@ __device__ __forceinline__ void unit_body(const UnitArgs& a) {
             for (int blk = 0; blk < n_blk; ++blk) {
               if (kDeriv)
                 chunk_elements_d<false>(sm, accE, accO, half, blk, a.n_theta, v);
+              else if (kMode == 2 && blk == 1)
+                chunk_errors<false>(sm, accE, accO, v);
               else
                 chunk_elements<false>(sm, accE, accO, v);
               if (j >= 0) {
@@ -365,12 +410,15 @@ __device__ __forceinline__ void unit_body(const UnitArgs& a) {
 // reduced tiles into the unit's accumulators. Every output sum is owned by one thread of one
 // work item and runs over the chunks in order, so the results do not depend on how a unit's
 // tiles are split into work items.
-__global__ void __launch_bounds__(NT) unit_kernel(UnitArgs a) { unit_body<false>(a); }
+__global__ void __launch_bounds__(NT) unit_kernel(UnitArgs a) { unit_body<0>(a); }
 
 // The same with the derivative blocks: per chunk, its two 16-node halves in order; per tile,
 // every block's sums (values, distribution parameters, Re m, Im m), each into its own
 // accumulator (4 n_mu or 4 n_q doubles apart).
-__global__ void __launch_bounds__(NT) unit_deriv_kernel(UnitArgs a) { unit_body<true>(a); }
+__global__ void __launch_bounds__(NT) unit_deriv_kernel(UnitArgs a) { unit_body<1>(a); }
+
+// Adaptive panels: per tile the values' sums and the sums of |Kronrod - Gauss| per panel.
+__global__ void __launch_bounds__(NT) unit_adaptive_kernel(UnitArgs a) { unit_body<2>(a); }
 
 // K-d: the Greek coefficients of each band slot, (2l+1)/2 sum_k w_k F(mu_k) d_l(mu_k) with F
 // the slot's averaged tables (fast.rs:238-253): a contraction over the band's n_q nodes shared
@@ -384,6 +432,7 @@ struct ProjSmem {
   double fs[4][PQ][33];  // F11, F12, F33, F34 per node and slot (padded against conflicts)
   double ds[4][PQ][PL];  // d00, d22, d2-2, d02 (scaled) per node and order
   double rz[32];         // 1/Z per slot
+  double z[32], ez[32], tr[32];  // adaptive: Z, its error, the truncation term
   int64_t offs[32];
 };
 }  // namespace
@@ -397,12 +446,18 @@ __global__ void __launch_bounds__(PT) proj_kernel(ProjArgs a) {
     const ProjItem it = a.items[item];
     const BandDesc B = a.bands[it.band];
     const int q = B.n_q, len = B.order + 1;
+    const bool bounds = it.kind == 1;
     if (t < 32) {
       double rz = 0.0;
       int64_t off = -1;
       if (t < it.count) {
         const BandSlot bs = a.slots[a.slot_index[it.first + t]];
-        if (a.raw) {
+        if (a.unit_norm) {
+          const double* un = a.unit_norm + 8 * (int64_t)a.units[bs.unit];
+          sm.z[t] = un[0];
+          sm.ez[t] = un[1];
+          sm.tr[t] = un[2];
+        } else if (a.raw) {
           rz = 1.0;
         } else {
           double z = 0.0;
@@ -430,20 +485,33 @@ __global__ void __launch_bounds__(PT) proj_kernel(ProjArgs a) {
           const int kk = idx % PQ, s = (idx / PQ) & 31, e = idx / (32 * PQ);
           double v = 0.0;
           const int64_t off = sm.offs[s];
-          if (kk < kn && off >= 0) v = a.acc[off + (int64_t)e * q + k0 + kk] * sm.rz[s];
+          if (kk < kn && off >= 0) {
+            const int64_t o = off + (int64_t)e * q + k0 + kk;
+            if (!a.unit_norm) {
+              v = a.acc[o] * sm.rz[s];
+            } else if (!bounds) {
+              v = a.acc[o] / sm.z[s];
+            } else {
+              // The error sums of the slot after the values' (engine.rs:1782-1800).
+              const double av = fabs(a.acc[o - 4 * (int64_t)q] / sm.z[s]);
+              v = (a.acc[o] + av * sm.ez[s]) / sm.z[s] + sm.tr[s] * av;
+            }
+          }
           sm.fs[e][kk][s] = v;
         }
         for (int idx = t; idx < 4 * PQ * PL; idx += PT) {
           const int l = idx % PL, kk = (idx / PL) % PQ, m = idx / (PL * PQ);
           double v = 0.0;
           if (kk < kn && l0 + l < len) v = D[((int64_t)m * q + k0 + kk) * len + l0 + l];
-          sm.ds[m][kk][l] = v;
+          sm.ds[m][kk][l] = bounds ? fabs(v) : v;
         }
         __syncthreads();
         for (int kk = 0; kk < kn; ++kk) {
           const double f11 = sm.fs[0][kk][lane], f12 = sm.fs[1][kk][lane];
           const double f33 = sm.fs[2][kk][lane], f34 = sm.fs[3][kk][lane];
-          const double fp = f11 + f33, fm = f11 - f33;
+          // Bounds: alpha2 and alpha3 share the half sum of the bounds of alpha2 +- alpha3
+          // (fast.rs:256-271).
+          const double fp = f11 + f33, fm = bounds ? fp : f11 - f33;
 #pragma unroll
           for (int j = 0; j < 9; ++j) {
             const int l = 9 * w + j;
@@ -468,7 +536,7 @@ __global__ void __launch_bounds__(PT) proj_kernel(ProjArgs a) {
             const double p = acc[j][2], mi = acc[j][3];
             out[l] = acc[j][0];
             out[glen + l] = (p + mi) * 0.5;
-            out[2 * glen + l] = (p - mi) * 0.5;
+            out[2 * glen + l] = bounds ? (p + mi) * 0.5 : (p - mi) * 0.5;
             out[3 * glen + l] = acc[j][1];
             out[4 * glen + l] = acc[j][4];
             out[5 * glen + l] = acc[j][5];
@@ -700,6 +768,122 @@ __global__ void __launch_bounds__(NT) final_deriv_kernel(FinalArgs a) {
   }
 }
 
+// The outputs of adaptive panels per unit with their error estimates: averages from the
+// Kronrod sums and the moments' Z, errors (e + |v| e_Z)/Z + truncation |v| (engine.rs:
+// 1782-1836), <r^2>, <r^3> from the moments (a single radius keeps its own), the ratios and
+// normalizations with the first-order bounds of ensemble/lin.rs (Lin::div, Lin::scale), and the
+// Greek coefficients summed over the bands, values and bounds (engine.rs:2310-2355).
+namespace {
+struct LinE {
+  double v, e;
+};
+__device__ __forceinline__ LinE ldiv(LinE a, LinE b) {
+  const double v = a.v / b.v;
+  return {v, (a.e + fabs(v) * b.e) / fabs(b.v)};
+}
+__device__ __forceinline__ LinE lscale(LinE a, double c) { return {c * a.v, fabs(c) * a.e}; }
+}  // namespace
+
+__global__ void __launch_bounds__(NT) final_adaptive_kernel(FinalArgs a) {
+  __shared__ double S[2][8];
+  __shared__ LinE a0s;
+  const int t = threadIdx.x;
+  const int L = a.greek_order;
+  const int glen = L >= 0 ? L + 1 : 0;
+  const int64_t nu = a.n_units_total;
+  for (int ul = blockIdx.x; ul < a.n_units; ul += gridDim.x) {
+    const int64_t unit = a.units[ul];
+    const int64_t d = unit / a.n_wl, i = unit % a.n_wl;
+    if (t < 16) {
+      double s = 0.0;
+      for (int c = 0; c < a.cpu; ++c) s += a.chunk_sums[((int64_t)ul * a.cpu + c) * 16 + t];
+      S[t / 8][t % 8] = s;
+    }
+    __syncthreads();
+    const double* un = a.unit_norm + 8 * unit;
+    const double z = un[0], ez = un[1], tr = un[2];
+    const bool point = un[3] != 0.0;
+    auto avg = [&](double s, double e) {
+      const double v = s / z;
+      return LinE{v, (e + fabs(v) * ez) / z + tr * fabs(v)};
+    };
+    LinE v[8];
+    for (int k = 0; k < 8; ++k) v[k] = avg(S[0][k], S[1][k]);
+    if (!point) {
+      v[6] = LinE{un[4], un[5]};
+      v[7] = LinE{un[6], un[7]};
+    }
+    const LinE ext = v[1], sca = v[2], scag = v[3], ab = v[4], back = v[5], r2 = v[6], r3 = v[7];
+    if (t == 0) {
+      const bool bext = !(isfinite(ext.v) && ext.v != 0.0);
+      const bool bsca = !(isfinite(sca.v) && sca.v != 0.0);
+      const bool bback = !(isfinite(back.v) && back.v != 0.0);
+      if (bext || bsca || bback) {
+        unsigned long long key = ((unsigned long long)(i * a.n_dist + d) << 2) |
+                                 (unsigned long long)(bext ? 1 : (bsca ? 2 : 3));
+        atomicMin(a.err + 1, key);
+      }
+      const LinE out[11] = {ext,
+                            sca,
+                            ab,
+                            back,
+                            ldiv(sca, ext),
+                            ldiv(scag, sca),
+                            lscale(ldiv(ext, back), 4.0 * kPi),
+                            LinE{0.0, 0.0},
+                            ldiv(r3, r2),
+                            lscale(r2, kPi),
+                            lscale(r3, 4.0 * kPi / 3.0)};
+      for (int k = 0; k < 11; ++k) {
+        a.values[k * nu + unit] = out[k].v;
+        a.errors[k * nu + unit] = out[k].e;
+      }
+    }
+    const double* acc_user = a.acc + a.unit_acc[ul];
+    if (a.phase) {
+      for (int j = t; j < a.n_mu; j += NT) {
+        LinE f[4];
+        for (int e = 0; e < 4; ++e) {
+          f[e] = avg(acc_user[e * a.n_mu + j], acc_user[(4 + e) * a.n_mu + j]);
+          if (a.normalized) f[e] = ldiv(f[e], sca);
+        }
+        const int src[6] = {0, 1, 0, 2, 3, 2};
+        for (int e = 0; e < 6; ++e) {
+          a.phase[((int64_t)e * nu + unit) * a.n_mu + j] = f[src[e]].v;
+          a.phase_err[((int64_t)e * nu + unit) * a.n_mu + j] = f[src[e]].e;
+        }
+      }
+    }
+    if (glen > 0 && a.greek) {
+      // The unit's slots: per band a values slot, then its bounds slot.
+      const int2 sl = a.unit_slots[ul];
+      auto sum = [&](int idx) {
+        const int e = idx / glen, l = idx % glen;
+        LinE g{0.0, 0.0};
+        for (int k = 0; k + 1 < sl.y; k += 2) {
+          const BandSlot bs = a.slots[sl.x + k];
+          if (l <= a.bands[bs.band].order) {
+            g.v += a.slot_greek[(int64_t)(sl.x + k) * 6 * glen + (int64_t)e * glen + l];
+            g.e += a.slot_greek[(int64_t)(sl.x + k + 1) * 6 * glen + (int64_t)e * glen + l];
+          }
+        }
+        return g;
+      };
+      if (t == 0) a0s = sum(0);
+      __syncthreads();
+      const LinE a0 = a0s;
+      for (int idx = t; idx < 6 * glen; idx += NT) {
+        const int e = idx / glen, l = idx % glen;
+        LinE g = sum(idx);
+        if (a.normalized) g = idx == 0 ? LinE{1.0, 0.0} : ldiv(g, a0);
+        a.greek[((int64_t)e * nu + unit) * glen + l] = g.v;
+        a.greek_err[((int64_t)e * nu + unit) * glen + l] = g.e;
+      }
+    }
+    __syncthreads();
+  }
+}
+
 int unit_kernel_blocks_per_sm() {
   int n = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, unit_kernel, NT, 0);
@@ -709,6 +893,8 @@ int unit_kernel_blocks_per_sm() {
 void launch_units(const UnitArgs& a, int grid, cudaStream_t s) {
   if (a.deriv)
     unit_deriv_kernel<<<grid, NT, 0, s>>>(a);
+  else if (a.wdiff)
+    unit_adaptive_kernel<<<grid, NT, 0, s>>>(a);
   else
     unit_kernel<<<grid, NT, 0, s>>>(a);
 }
@@ -731,6 +917,8 @@ void launch_final(const FinalArgs& a, cudaStream_t s) {
   int grid = a.n_units < 4096 ? a.n_units : 4096;
   if (a.d_values)
     final_deriv_kernel<<<grid, NT, 0, s>>>(a);
+  else if (a.unit_norm)
+    final_adaptive_kernel<<<grid, NT, 0, s>>>(a);
   else
     final_kernel<<<grid, NT, 0, s>>>(a);
 }
