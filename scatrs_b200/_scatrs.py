@@ -13,6 +13,14 @@ the GPU library.
   and (n_dist, L, n_wl). ``derivatives`` are indices into ensemble_parameters (the
   reference's deriv_idx, ensemble.rs:295-311), computed in forward mode like the reference's.
 
+* ``ensemble_compute(items, wavelengths, mixture, greek, all_orders, mu, normalized,
+  derivatives, rtol, max_panels, allow_unvalidated, refine_backscatter)`` and
+  ``ensemble_compute_batch(specs, particle_spec, wavelengths, greek, all_orders, mu,
+  normalized, rtol, max_panels, allow_unvalidated, refine_backscatter)``: the reference's
+  calls (ensemble.rs:295-349, 455-504) on the adaptive GPU engine, for one sphere component
+  (lognormal, gamma, modified gamma, power law or monodisperse distributions), values and error
+  estimates.
+
 Errors are those of the reference's Python package (scatrs_b200.errors).
 """
 
@@ -92,6 +100,96 @@ def _dist_array(specs, spread: float, ranges=None) -> np.ndarray:
         else:
             raise InvalidInputError(f"a {kind} distribution needs an explicit grid range")
     return d
+
+
+def _adaptive_dists(specs) -> np.ndarray:
+    d = np.zeros(len(specs), dtype=_native.DIST_DTYPE)
+    for k, spec in enumerate(specs):
+        if not isinstance(spec, tuple):
+            raise TypeError("a distribution spec must be a tuple")
+        kind = spec[0]
+        p = [float(v) for v in spec[1:]]
+        if kind == "monodisperse":
+            d[k]["kind"] = _native.MONODISPERSE
+        elif kind in _native.KINDS:
+            d[k]["kind"] = _native.KINDS[kind]
+        elif kind in ("tabulated", "multimodal"):
+            raise InvalidInputError(f"{kind} distributions are not on the GPU path")
+        else:
+            raise TypeError(f"unknown distribution kind {kind!r}")
+        d[k]["param"][: len(p)] = p
+    return d
+
+
+def _adaptive_dict(out: dict, mu_size: int, k: int) -> dict:
+    n = out["values"].shape[1]
+    raw = {"values": out["values"], "errors": out["errors"], "d": np.zeros((k, 11, n)),
+           "d_errors": np.zeros((k, 11, n))}
+    for prefix in ("greek", "phase"):
+        if prefix in out:
+            arr = out[prefix]
+            raw[prefix] = arr
+            raw[f"{prefix}_errors"] = out[f"{prefix}_err"]
+            raw[f"{prefix}_d"] = np.zeros((k,) + arr.shape)
+            raw[f"{prefix}_d_errors"] = np.zeros((k,) + arr.shape)
+    raw["converged"] = out["converged"]
+    raw["panels"] = out["panels"].astype(np.uint64)
+    return raw
+
+
+def _sphere_m(particle_spec, n_wl: int) -> np.ndarray:
+    if not isinstance(particle_spec, tuple):
+        raise TypeError("a particle spec must be a tuple")
+    if particle_spec[0] != "sphere":
+        if particle_spec[0] in ("layered", "spheroid"):
+            raise InvalidInputError(
+                f"{particle_spec[0]} particles are not on the adaptive GPU path")
+        raise TypeError(f"unknown particle kind {particle_spec[0]!r}")
+    m = np.asarray(particle_spec[1], dtype=np.complex128).reshape(-1)
+    if m.size != n_wl:
+        raise InvalidInputError(f"{m.size} refractive indices for {n_wl} wavelengths")
+    return m
+
+
+def ensemble_compute(items, wavelengths, mixture, greek, all_orders, mu, normalized, derivatives,
+                     rtol, max_panels, allow_unvalidated, refine_backscatter) -> dict:
+    """The reference's ``_scatrs.ensemble_compute`` (one component) on the GPU."""
+    if not items:
+        raise InvalidInputError("a mixture needs a component")
+    if len(items) != 1:
+        raise InvalidInputError("mixtures of several components are not on the GPU path")
+    if list(derivatives):
+        raise InvalidInputError(
+            "derivatives of the adaptive ensemble are not on the GPU path: use the fixed grid")
+    if all_orders:
+        raise InvalidInputError("greek='all' is not on the GPU path: give an order")
+    spec, particle, _w = items[0]
+    wl = np.ascontiguousarray(wavelengths, dtype=np.float64).reshape(-1)
+    m = _sphere_m(particle, wl.size)
+    mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
+    out = _native.ensemble_adaptive(_adaptive_dists([spec]), wl, m, mu,
+                                    -1 if greek is None else int(greek), bool(normalized),
+                                    float(rtol), int(max_panels), bool(allow_unvalidated),
+                                    bool(refine_backscatter))
+    return _adaptive_dict(out, mu.size, 0)
+
+
+def ensemble_compute_batch(specs, particle_spec, wavelengths, greek, all_orders, mu, normalized,
+                           rtol, max_panels, allow_unvalidated, refine_backscatter) -> dict:
+    """The reference's ``_scatrs.ensemble_compute_batch`` on the GPU: every distribution of
+    one sphere material on shared panels per wavelength, rows distribution-major."""
+    if not specs:
+        raise InvalidInputError("a batch needs a distribution")
+    if all_orders:
+        raise InvalidInputError("greek='all' is not on the GPU path: give an order")
+    wl = np.ascontiguousarray(wavelengths, dtype=np.float64).reshape(-1)
+    m = _sphere_m(particle_spec, wl.size)
+    mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
+    out = _native.ensemble_adaptive(_adaptive_dists(list(specs)), wl, m, mu,
+                                    -1 if greek is None else int(greek), bool(normalized),
+                                    float(rtol), int(max_panels), bool(allow_unvalidated),
+                                    bool(refine_backscatter), batch=True)
+    return _adaptive_dict(out, mu.size, 0)
 
 
 def ensemble_compute_fixed(specs, particle_spec, wavelengths, greek, all_orders, mu, normalized,

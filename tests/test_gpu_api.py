@@ -41,3 +41,23 @@ def test_layered_spec(gpu):
     v, _, g = _native.ensemble_fixed_layered(_scatrs._dist_array(specs, 4.0), wl, [[0.5, 0.9]],
                                              ml[None], None, 64, 8)
     assert np.array_equal(raw["values"], v) and np.array_equal(raw["greek"], g)
+
+
+def test_adaptive_calls_mirror_the_reference(gpu):
+    """ensemble_compute / ensemble_compute_batch: the reference dict from the adaptive engine,
+    equal to the raw binding's arrays."""
+    wl = np.array([0.4, 0.7])
+    m = np.array([1.45 + 0.01j, 1.40 + 1e-4j])
+    mu = np.array([1.0, -0.3])
+    items = [(("gamma", 0.4, 0.1), ("sphere", m), 1.0)]
+    raw = _scatrs.ensemble_compute(items, wl, False, 12, False, mu, True, [], 1e-6, 4096, False,
+                                   False)
+    ref = _native.ensemble_adaptive(_scatrs._adaptive_dists([items[0][0]]), wl, m, mu, 12)
+    assert np.array_equal(raw["values"], ref["values"])
+    assert np.array_equal(raw["greek_errors"], ref["greek_err"])
+    assert raw["d"].shape == (0, 11, 2) and raw["panels"].dtype == np.uint64
+    specs = [("lognormal", 0.1, 1.5), ("monodisperse", 0.3)]
+    b = _scatrs.ensemble_compute_batch(specs, ("sphere", m), wl, None, False, mu, True, 1e-6,
+                                       4096, False, False)
+    assert b["values"].shape == (11, 4) and "greek" not in b and b["phase"].shape == (6, 4, 2)
+    assert np.all(b["panels"][2:] == 0) and np.all(b["converged"])
