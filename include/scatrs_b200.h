@@ -145,6 +145,34 @@ int scatrs_ensemble_adaptive(const scatrs_distribution* dists, int64_t n_dist, i
                              double* greek_err, int8_t* converged, int64_t* panels, char* err,
                              size_t err_len);
 
+/* One component of a mixture (scatrs::ensemble::Component, ensemble/mod.rs:136-160): its
+ * distribution, or the modes of a multimodal one (SizeDistribution::MultiModal,
+ * distribution.rs:60-66) with their weights, its weight w in the mixture, and its sphere's
+ * index per wavelength. */
+typedef struct scatrs_component {
+  const scatrs_distribution* modes; /* n_modes distributions (one for a plain distribution) */
+  const double* mode_weights;       /* n_modes weights v_j of a multimodal one, or NULL */
+  int32_t n_modes;
+  int32_t reserved;
+  double weight;                    /* w */
+  const double* m;                  /* complex128 per wavelength */
+} scatrs_component;
+
+/*
+ * The adaptive ensemble of an external mixture of sphere components (`compute_mixture`,
+ * scatrs/src/ensemble/mod.rs:609-625; a multimodal distribution alone is a mixture of one
+ * component): every mode of every component integrated on its own panels, the averages mixed
+ * with the number fractions (w / sum w) (v_j / sum v) (engine.rs:2121-2176) before the ratios,
+ * normalizations and the Greek projection. Outputs per wavelength as scatrs_ensemble_adaptive
+ * with n_units = n_wl; converged when every part converged, panels summed over the parts.
+ */
+int scatrs_ensemble_mixture(const scatrs_component* components, int64_t n_comp,
+                            const double* wavelengths, int64_t n_wl, const double* mu,
+                            int64_t n_mu, const scatrs_adaptive_options* options, double* values,
+                            double* errors, double* phase, double* phase_err, double* greek,
+                            double* greek_err, int8_t* converged, int64_t* panels, char* err,
+                            size_t err_len);
+
 /* Layered spheres (scatrs/src/layered/mod.rs; Particle::LayeredSphere,
  * scatrs/src/ensemble/mod.rs:58-65): n_layers layers, the core first; per distribution the
  * n_layers - 1 outer radii of layers 0..L-2 as fractions of the particle's radius (nondecreasing

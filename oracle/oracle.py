@@ -320,3 +320,56 @@ def dist(kind: int, *params) -> np.ndarray:
     d["kind"] = kind
     d["p"][0, :len(params)] = params
     return d
+
+
+def _mixture_arrays(components, n_wl):
+    """(modes, mode weights, n_modes, w, m) arrays from [(dists, mode_weights or None, w, m)]."""
+    modes, mw, nm, w, ms = [], [], [], [], []
+    for dists, mode_w, weight, m in components:
+        dists = np.atleast_1d(np.asarray(dists, dtype=DIST_DTYPE))
+        modes.append(dists)
+        mw.extend(list(mode_w) if mode_w is not None else [1.0] * dists.size)
+        nm.append(dists.size)
+        w.append(float(weight))
+        ms.append(np.broadcast_to(np.asarray(m, dtype=np.complex128), (n_wl,)))
+    return (np.ascontiguousarray(np.concatenate(modes)), np.ascontiguousarray(mw, dtype=np.float64),
+            np.ascontiguousarray(nm, dtype=np.int32), np.ascontiguousarray(w, dtype=np.float64),
+            np.ascontiguousarray(np.concatenate(ms)))
+
+
+def ensemble_mixture(components, wavelengths, mu=None, greek_order=None, normalized=True,
+                     rtol=1e-6, max_panels=4096, allow_unvalidated=False,
+                     refine_backscatter=False) -> dict:
+    """The adaptive ensemble of a mixture: components [(dists, mode_weights or None, w, m)],
+    a component's dists one distribution or the modes of a multimodal one; m per wavelength.
+    Outputs per wavelength (n = n_wl)."""
+    wl = np.ascontiguousarray(wavelengths, dtype=np.float64).reshape(-1)
+    modes, mw, nm, w, ms = _mixture_arrays(components, wl.size)
+    mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
+    n = wl.size
+    L = -1 if greek_order is None else int(greek_order)
+    out = {"values": np.zeros((11, n)), "errors": np.zeros((11, n)),
+           "converged": np.zeros(n, dtype=np.int8), "panels": np.zeros(n, dtype=np.int64)}
+    ph = pe = g = ge = None
+    if mu.size:
+        ph, pe = np.zeros((6, n, mu.size)), np.zeros((6, n, mu.size))
+    if L >= 0:
+        g, ge = np.zeros((6, n, L + 1)), np.zeros((6, n, L + 1))
+    err = ctypes.create_string_buffer(512)
+    f = lib().orc_ensemble_mixture
+    f.argtypes = [ctypes.c_void_p, _PD, ctypes.c_void_p, _PD, _PD, _I64, _PD, _I64, _PD, _I64,
+                  _I64, ctypes.c_int, _D, _I64, ctypes.c_int, ctypes.c_int, _PD, _PD, _PD, _PD,
+                  _PD, _PD, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_char_p, _I64]
+    st = f(modes.ctypes.data, _p(mw), nm.ctypes.data, _p(w), _p(ms.view(np.float64)), nm.size,
+           _p(wl), wl.size, _p(mu), mu.size, L, int(normalized), rtol, max_panels,
+           int(allow_unvalidated), int(refine_backscatter), _p(out["values"]),
+           _p(out["errors"]), _p(ph), _p(pe), _p(g), _p(ge), out["converged"].ctypes.data,
+           out["panels"].ctypes.data, err, 512)
+    if st != 0:
+        raise OracleError(st, err.value.decode())
+    out["converged"] = out["converged"].astype(bool)
+    if ph is not None:
+        out["phase"], out["phase_err"] = ph, pe
+    if g is not None:
+        out["greek"], out["greek_err"] = g, ge
+    return out

@@ -223,6 +223,8 @@ enum SupportKind { UNBOUNDED, FINITE, POINT };
 
 struct Part {
   FixedDist dist;
+  const double* m = nullptr;  // complex per wavelength: the part's sphere
+  double f = 1.0;             // the number fraction in its unit (engine.rs:2131)
   Density den;
   SupportKind support;
   double s_a = 0, s_b = 0;  // center (unbounded), [lo, hi] (finite), radius (point)
@@ -693,13 +695,15 @@ struct UnitOut {
 std::vector<UnitOut> wavelength(const std::vector<Part>& parts,
                                 const std::vector<std::vector<int>>& groups,
                                 const std::vector<std::vector<int>>& units, double lambda,
-                                cplx m, const double* mu, int64_t n_mu, int64_t order,
+                                int64_t wi, const double* mu, int64_t n_mu, int64_t order,
                                 bool normalized, const Options& o) {
+  auto m_of = [&](int p) { return C(parts[p].m[2 * wi], parts[p].m[2 * wi + 1]); };
   std::vector<Pass1> firsts;
   int64_t n_max = 0;
   for (auto& g : groups) {
     std::vector<const Part*> mem;
     for (int p : g) mem.push_back(&parts[p]);
+    const cplx m = m_of(g[0]);  // a group shares its particle
     Pass1 p1;
     if (mem[0]->support == POINT) {
       const double r = mem[0]->s_a;
@@ -728,6 +732,7 @@ std::vector<UnitOut> wavelength(const std::vector<Part>& parts,
   if (order >= 0) {
     std::set<int64_t> uppers;
     for (size_t gi = 0; gi < groups.size(); ++gi) {
+      const cplx m = m_of(groups[gi][0]);
       if (parts[groups[gi][0]].support == POINT) {
         uppers.insert(bucket(firsts[gi].n_terms));
         continue;
@@ -748,6 +753,7 @@ std::vector<UnitOut> wavelength(const std::vector<Part>& parts,
   MieState st;
   for (size_t gi = 0; gi < groups.size(); ++gi) {
     const auto& grp = groups[gi];
+    const cplx m = m_of(grp[0]);
     if (parts[grp[0]].support == POINT) {
       const double r = parts[grp[0]].s_a;
       int64_t n;
@@ -821,16 +827,17 @@ std::vector<UnitOut> wavelength(const std::vector<Part>& parts,
       ae[grp[p]] = std::move(er);
     }
   }
-  // Units: the mixture of their parts with number fractions 1/count (one part per unit here).
+  // Units: the mixture of their parts with their number fractions (engine.rs:2121-2176).
   std::vector<UnitOut> out;
   for (auto& un : units) {
     std::vector<double> v(len, 0.0), e(len, 0.0);
-    const double f = 1.0 / (double)un.size();
-    for (int p : un)
+    for (int p : un) {
+      const double f = parts[p].f;
       for (int64_t i = 0; i < len; ++i) {
         v[i] += f * av[p][i];
         e[i] += f * ae[p][i];
       }
+    }
     UnitOut u;
     auto lin = [&](int i) { return Lin{v[i], e[i]}; };
     Lin ext = lin(S_EXT), sca = lin(S_SCA), scag = lin(S_SCAG), ab = lin(S_ABS),
@@ -947,7 +954,10 @@ int orc_ensemble_adaptive(const FixedDist* dists, int64_t n_dist, int batch, con
   if (max_panels < 1) return fail({INVALID_INPUT, "max_panels must be at least 1"});
   std::vector<Part> parts;
   try {
-    for (int64_t d = 0; d < n_dist; ++d) parts.push_back(make_part(dists[d], rtol));
+    for (int64_t d = 0; d < n_dist; ++d) {
+      parts.push_back(make_part(dists[d], rtol));
+      parts.back().m = m;
+    }
   } catch (const Failure& f) {
     return fail(f);
   }
@@ -981,8 +991,8 @@ int orc_ensemble_adaptive(const FixedDist* dists, int64_t n_dist, int batch, con
   for (int64_t job = 0; job < n_calls * n_wl; ++job) {
     const int64_t c = job / n_wl, i = job % n_wl;
     try {
-      auto res = wavelength(parts, groups_of[c], units_of[c], wl[i], C(m[2 * i], m[2 * i + 1]),
-                            mu, n_mu, greek_order, normalized != 0, o);
+      auto res = wavelength(parts, groups_of[c], units_of[c], wl[i], i, mu, n_mu, greek_order,
+                            normalized != 0, o);
       for (size_t k = 0; k < units_of[c].size(); ++k) {
         const int64_t d = units_of[c][k][0];
         const int64_t unit = d * n_wl + i;
@@ -1014,6 +1024,83 @@ int orc_ensemble_adaptive(const FixedDist* dists, int64_t n_dist, int batch, con
   for (int64_t i = 0; i < n_wl; ++i)
     for (int64_t c = 0; c < n_calls; ++c)
       if (fails[c * n_wl + i].status != OK) return fail(fails[c * n_wl + i]);
+  return OK;
+}
+
+// The adaptive ensemble of a mixture (compute_mixture, ensemble/mod.rs:609-625): n_comp
+// components, component c with n_modes[c] modes (its distributions, consecutive in `modes`,
+// with weights mode_w, ignored for one mode), weight w[c] and m of its own (complex per
+// wavelength, consecutive n_wl per component). Each mode is a part on its own panels; the
+// outputs per wavelength as orc_ensemble_adaptive with n_units = n_wl.
+int orc_ensemble_mixture(const FixedDist* modes, const double* mode_w, const int32_t* n_modes,
+                         const double* w, const double* m, int64_t n_comp, const double* wl,
+                         int64_t n_wl, const double* mu, int64_t n_mu, int64_t greek_order,
+                         int normalized, double rtol, int64_t max_panels, int allow_unvalidated,
+                         int refine_backscatter, double* values, double* errors, double* phase,
+                         double* phase_err, double* greek, double* greek_err, int8_t* converged,
+                         int64_t* panels, char* err, int64_t err_len) {
+  Options o{rtol, (size_t)max_panels, allow_unvalidated != 0, refine_backscatter != 0};
+  auto fail = [&](const Failure& f) {
+    if (err && err_len > 0) snprintf(err, err_len, "%s", f.msg.c_str());
+    return f.status;
+  };
+  if (!(rtol >= 1e-13 && rtol <= 0.1)) return fail({INVALID_INPUT, "rtol must be in [1e-13, 0.1]"});
+  double w_total = 0.0;
+  for (int64_t c = 0; c < n_comp; ++c) w_total += w[c];
+  std::vector<Part> parts;
+  std::vector<int> unit;
+  try {
+    int64_t k = 0;
+    for (int64_t c = 0; c < n_comp; ++c) {
+      double v_total = 0.0;
+      for (int j = 0; j < n_modes[c]; ++j) v_total += n_modes[c] > 1 ? mode_w[k + j] : 1.0;
+      for (int j = 0; j < n_modes[c]; ++j) {
+        const double v = n_modes[c] > 1 ? mode_w[k + j] : 1.0;
+        parts.push_back(make_part(modes[k + j], rtol));
+        parts.back().m = m + 2 * n_wl * c;
+        parts.back().f = w[c] / w_total * v / v_total;
+        unit.push_back((int)parts.size() - 1);
+      }
+      k += n_modes[c];
+    }
+  } catch (const Failure& f) {
+    return fail(f);
+  }
+  std::vector<std::vector<int>> groups;
+  for (size_t p = 0; p < parts.size(); ++p) groups.push_back({(int)p});
+  std::vector<std::vector<int>> units{unit};
+  const int64_t glen = greek_order >= 0 ? greek_order + 1 : 0;
+  std::vector<Failure> fails(n_wl, Failure{OK, ""});
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int64_t i = 0; i < n_wl; ++i) {
+    try {
+      auto res = wavelength(parts, groups, units, wl[i], i, mu, n_mu, greek_order,
+                            normalized != 0, o);
+      const UnitOut& u = res[0];
+      for (int q = 0; q < 11; ++q) {
+        values[q * n_wl + i] = u.values[q];
+        errors[q * n_wl + i] = u.errors[q];
+      }
+      if (phase && n_mu > 0)
+        for (int el = 0; el < 6; ++el)
+          for (int64_t j = 0; j < n_mu; ++j) {
+            phase[(el * n_wl + i) * n_mu + j] = u.phase[el * n_mu + j];
+            phase_err[(el * n_wl + i) * n_mu + j] = u.phase_err[el * n_mu + j];
+          }
+      if (greek && glen > 0)
+        for (int el = 0; el < 6; ++el)
+          for (int64_t l = 0; l < glen; ++l) {
+            greek[(el * n_wl + i) * glen + l] = u.greek[el * glen + l];
+            greek_err[(el * n_wl + i) * glen + l] = u.greek_err[el * glen + l];
+          }
+      converged[i] = u.converged ? 1 : 0;
+      panels[i] = u.panels;
+    } catch (const Failure& f) {
+      fails[i] = f;
+    }
+  }
+  for (auto& f : fails)
+    if (f.status != OK) return fail(f);
   return OK;
 }
 

@@ -40,6 +40,11 @@ class AdaptiveOptions(ctypes.Structure):
                 ("allow_unvalidated", _I32), ("refine_backscatter", _I32)]
 
 
+class Component(ctypes.Structure):
+    _fields_ = [("modes", _VP), ("mode_weights", _PD), ("n_modes", _I32), ("reserved", _I32),
+                ("weight", _D), ("m", _PD)]
+
+
 class FixedOptions(ctypes.Structure):
     _fields_ = [("n_nodes", _I32), ("greek_order", _I32), ("normalized", _I32),
                 ("allow_unvalidated", _I32)]
@@ -63,6 +68,9 @@ SYMBOLS = {
     "scatrs_ensemble_adaptive": (ctypes.c_int, [_VP, _I64, _I32, _PD, _I64, _PD, _PD, _I64,
                                                 ctypes.POINTER(AdaptiveOptions), _PD, _PD, _PD,
                                                 _PD, _PD, _PD, _VP, _VP, _CP, _SZ]),
+    "scatrs_ensemble_mixture": (ctypes.c_int, [ctypes.POINTER(Component), _I64, _PD, _I64, _PD,
+                                               _I64, ctypes.POINTER(AdaptiveOptions), _PD, _PD,
+                                               _PD, _PD, _PD, _PD, _VP, _VP, _CP, _SZ]),
     "scatrs_check_errors": (ctypes.c_int, [_VP, _CP, _SZ]),
     "scatrs_mie": (ctypes.c_int, [_PD, _PD, _I64, _I32, _PI64, _PI64, _PD, _PD, _CP, _SZ]),
     "scatrs_mie_static": (ctypes.c_int, [_VP, _VP, _I64, _I32, _I64, _VP, _VP, _VP, _VP, _VP,
@@ -247,6 +255,50 @@ def ensemble_adaptive(dists: np.ndarray, wavelengths, m, mu=None, greek_order: i
                                          _p(out["errors"]), _p(ph), _p(pe), _p(g), _p(ge),
                                          out["converged"].ctypes.data, out["panels"].ctypes.data,
                                          err, 1024)
+    _check(st, err)
+    out["converged"] = out["converged"].astype(bool)
+    if ph is not None:
+        out["phase"], out["phase_err"] = ph, pe
+    if g is not None:
+        out["greek"], out["greek_err"] = g, ge
+    return out
+
+
+def ensemble_mixture(components, wavelengths, mu=None, greek_order: int = -1,
+                     normalized: bool = True, rtol: float = 1e-6, max_panels: int = 4096,
+                     allow_unvalidated: bool = False, refine_backscatter: bool = False) -> dict:
+    """The adaptive ensemble of a mixture of sphere components [(dists, mode_weights or None,
+    weight, m)], dists a DIST_DTYPE array (one distribution, or a multimodal one's modes), m per
+    wavelength. Outputs per wavelength, as ensemble_adaptive."""
+    require_device()
+    wl = np.ascontiguousarray(wavelengths, dtype=np.float64).reshape(-1)
+    keep = []
+    comps = (Component * max(len(components), 1))()
+    for k, (dists, mode_w, weight, m) in enumerate(components):
+        d = np.ascontiguousarray(np.atleast_1d(dists), dtype=DIST_DTYPE)
+        mw = None if mode_w is None else np.ascontiguousarray(mode_w, dtype=np.float64)
+        mm = np.ascontiguousarray(np.broadcast_to(np.asarray(m, dtype=np.complex128), wl.shape))
+        keep += [d, mw, mm]
+        comps[k] = Component(d.ctypes.data, _p(mw), d.size, 0, float(weight),
+                             _p(mm.view(np.float64)))
+    mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
+    n = wl.size
+    L = int(greek_order)
+    opts = AdaptiveOptions(float(rtol), int(max_panels), L, int(normalized),
+                           int(allow_unvalidated), int(refine_backscatter))
+    out = {"values": np.zeros((11, n)), "errors": np.zeros((11, n)),
+           "converged": np.zeros(n, dtype=np.int8), "panels": np.zeros(n, dtype=np.int64)}
+    ph = pe = g = ge = None
+    if mu.size:
+        ph, pe = np.zeros((6, n, mu.size)), np.zeros((6, n, mu.size))
+    if L >= 0:
+        g, ge = np.zeros((6, n, L + 1)), np.zeros((6, n, L + 1))
+    err = ctypes.create_string_buffer(1024)
+    st = load().scatrs_ensemble_mixture(comps, len(components), _p(wl), wl.size, _p(mu), mu.size,
+                                        ctypes.byref(opts), _p(out["values"]), _p(out["errors"]),
+                                        _p(ph), _p(pe), _p(g), _p(ge),
+                                        out["converged"].ctypes.data, out["panels"].ctypes.data,
+                                        err, 1024)
     _check(st, err)
     out["converged"] = out["converged"].astype(bool)
     if ph is not None:

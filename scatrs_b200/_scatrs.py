@@ -17,9 +17,9 @@ the GPU library.
   derivatives, rtol, max_panels, allow_unvalidated, refine_backscatter)`` and
   ``ensemble_compute_batch(specs, particle_spec, wavelengths, greek, all_orders, mu,
   normalized, rtol, max_panels, allow_unvalidated, refine_backscatter)``: the reference's
-  calls (ensemble.rs:295-349, 455-504) on the adaptive GPU engine, for one sphere component
-  (lognormal, gamma, modified gamma, power law or monodisperse distributions), values and error
-  estimates.
+  calls (ensemble.rs:295-349, 455-504) on the adaptive GPU engine: sphere components (a
+  mixture), each a lognormal, gamma, modified gamma, power law, monodisperse or multimodal
+  distribution; values and error estimates.
 
 Errors are those of the reference's Python package (scatrs_b200.errors).
 """
@@ -113,8 +113,10 @@ def _adaptive_dists(specs) -> np.ndarray:
             d[k]["kind"] = _native.MONODISPERSE
         elif kind in _native.KINDS:
             d[k]["kind"] = _native.KINDS[kind]
-        elif kind in ("tabulated", "multimodal"):
-            raise InvalidInputError(f"{kind} distributions are not on the GPU path")
+        elif kind == "tabulated":
+            raise InvalidInputError("tabulated distributions are not on the GPU path")
+        elif kind == "multimodal":
+            raise InvalidInputError("a multimodal distribution is not one distribution here")
         else:
             raise TypeError(f"unknown distribution kind {kind!r}")
         d[k]["param"][: len(p)] = p
@@ -151,26 +153,40 @@ def _sphere_m(particle_spec, n_wl: int) -> np.ndarray:
     return m
 
 
+def _modes(spec):
+    """(DIST_DTYPE modes, mode weights or None) of a spec; multimodal specs list (v, spec)."""
+    if isinstance(spec, tuple) and spec and spec[0] == "multimodal":
+        modes = list(spec[1])
+        if not modes:
+            raise InvalidInputError("a multimodal distribution needs a mode")
+        for _v, mode in modes:
+            if isinstance(mode, tuple) and mode and mode[0] == "multimodal":
+                raise InvalidInputError(
+                    "the modes of a multimodal distribution cannot be multimodal")
+        return _adaptive_dists([mode for _v, mode in modes]), [float(v) for v, _m in modes]
+    return _adaptive_dists([spec]), None
+
+
 def ensemble_compute(items, wavelengths, mixture, greek, all_orders, mu, normalized, derivatives,
                      rtol, max_panels, allow_unvalidated, refine_backscatter) -> dict:
-    """The reference's ``_scatrs.ensemble_compute`` (one component) on the GPU."""
+    """The reference's ``_scatrs.ensemble_compute`` on the GPU: one or more sphere components
+    (a mixture), each a distribution or a multimodal one, one output per wavelength."""
     if not items:
         raise InvalidInputError("a mixture needs a component")
-    if len(items) != 1:
-        raise InvalidInputError("mixtures of several components are not on the GPU path")
     if list(derivatives):
         raise InvalidInputError(
             "derivatives of the adaptive ensemble are not on the GPU path: use the fixed grid")
     if all_orders:
         raise InvalidInputError("greek='all' is not on the GPU path: give an order")
-    spec, particle, _w = items[0]
     wl = np.ascontiguousarray(wavelengths, dtype=np.float64).reshape(-1)
-    m = _sphere_m(particle, wl.size)
+    comps = []
+    for spec, particle, weight in items:
+        dists, mode_w = _modes(spec)
+        comps.append((dists, mode_w, float(weight), _sphere_m(particle, wl.size)))
     mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
-    out = _native.ensemble_adaptive(_adaptive_dists([spec]), wl, m, mu,
-                                    -1 if greek is None else int(greek), bool(normalized),
-                                    float(rtol), int(max_panels), bool(allow_unvalidated),
-                                    bool(refine_backscatter))
+    out = _native.ensemble_mixture(comps, wl, mu, -1 if greek is None else int(greek),
+                                   bool(normalized), float(rtol), int(max_panels),
+                                   bool(allow_unvalidated), bool(refine_backscatter))
     return _adaptive_dict(out, mu.size, 0)
 
 

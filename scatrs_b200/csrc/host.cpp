@@ -144,7 +144,8 @@ struct Context {
       unit_acc, unit_slots, slots, items, proj_items, slot_index, slot_greek, X, uz, ux,
       chunk_sums, err, acc, counter, values, phase, greek;
   // Pass 1 of the adaptive ensemble.
-  DevBuf p1_radius, p1_wl, p1_scratch, p1_uz, p1_ux, p1_q, p1_n, p1_status;
+  DevBuf p1_radius, p1_wl, p1_wlu, p1_scratch, p1_uz, p1_ux, p1_q, p1_n, p1_status;
+  DevBuf avg, mix_first, mix_part, mix_frac;
   std::vector<int> chunk_n_host;
   int* pinned_chunk_n = nullptr;
   size_t pinned_cap = 0;
@@ -401,9 +402,7 @@ struct AdaptiveInput {
   const double* weight = nullptr;
   const double* wdiff = nullptr;
   const double* unit_norm = nullptr;
-  double* errors = nullptr;
-  double* phase_err = nullptr;
-  double* greek_err = nullptr;
+  double* avg = nullptr;  // the units' averages, mixed and assembled by mix_assemble_kernel
 };
 
 void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, const double* wl_dev,
@@ -784,9 +783,7 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
   }
   if (ad.on) {
     fa.unit_norm = c.unit_norm.as<double>(0);
-    fa.errors = ad.errors;
-    fa.phase_err = n_mu > 0 ? ad.phase_err : nullptr;
-    fa.greek_err = L >= 0 ? ad.greek_err : nullptr;
+    fa.avg = ad.avg;
   }
   std::vector<std::pair<double, int64_t>> order;  // work items by cost
   std::vector<int> per_band;
@@ -987,6 +984,360 @@ void check_device_errors(Context& c, cudaStream_t s, const FixedCall* call) {
   }
 }
 
+// One part of an adaptive call (engine.rs:78-112): a distribution (or a mode of one), its
+// sphere's m per wavelength (host), its number fraction in its output unit, that unit, and the
+// prefix of its validation errors.
+struct AdPart {
+  int kind;
+  double p[3];
+  const double* m;
+  double f;
+  int out;
+  std::string who;
+};
+
+struct AdOutputs {
+  double *values, *errors, *phase, *phase_err, *greek, *greek_err;
+  int8_t* converged;
+  int64_t* panels;
+};
+
+// The adaptive ensemble of `parts` mixed into n_out output units (engine.rs:236-296 run and
+// run_batch, 1964-2250 wavelength): the parts' cut-offs and moments; pass 1 with each part on its
+// own panels, or (batch) every part with a range on one shared group per wavelength; pass 2 on
+// the final panels; each part's averages; the mixing and the outputs per (output unit,
+// wavelength), unit-major.
+void adaptive_call(const std::vector<AdPart>& in, int n_out, bool batch, const double* wavelengths,
+                   int64_t n_wl, const double* mu, int64_t n_mu,
+                   const scatrs_adaptive_options* options, const AdOutputs& res) {
+  if (!options) throw Failure{SCATRS_INVALID_INPUT, "options must not be NULL"};
+  if (n_wl < 0) throw Failure{SCATRS_INVALID_INPUT, "negative sizes"};
+  const adaptive::Options o{options->rtol, options->max_panels, options->allow_unvalidated != 0,
+                            options->refine_backscatter != 0};
+  // ensemble/mod.rs:688-720.
+  if (!(o.rtol >= 1e-13 && o.rtol <= 0.1)) {
+    char buf[80];
+    snprintf(buf, sizeof buf, "rtol must be in [1e-13, 0.1], got %g", o.rtol);
+    throw Failure{SCATRS_INVALID_INPUT, buf};
+  }
+  if (o.max_panels < 1) throw Failure{SCATRS_INVALID_INPUT, "max_panels must be at least 1"};
+  for (int64_t i = 0; i < n_wl; ++i)
+    if (!(std::isfinite(wavelengths[i]) && wavelengths[i] > 0.0))
+      throw Failure{SCATRS_INVALID_INPUT,
+                    "wavelength " + std::to_string(i) + " must be finite and > 0"};
+  scatrs_fixed_options fo{32, options->greek_order, options->normalized,
+                          options->allow_unvalidated};
+  const int64_t n_parts = (int64_t)in.size();
+  const int64_t n_units = n_parts * n_wl;  // pipeline units: (part, wavelength)
+  check_options(&fo, (int64_t)n_out * n_wl, n_mu, mu);
+  if (n_units == 0 || n_out == 0) return;
+  std::vector<adaptive::Part> parts;
+  for (const AdPart& p : in) {
+    try {
+      parts.push_back(adaptive::make_part(p.kind, p.p, o.rtol));
+    } catch (const adaptive::Error& e) {
+      throw Failure{e.status, p.who + e.msg};
+    }
+  }
+  Context& c = context();
+  std::lock_guard<std::mutex> lk(c.mtx);
+  cudaStream_t s = 0;
+  double* wl_d = c.wl.as<double>(n_wl);
+  SB_CUDA(cudaMemcpyAsync(wl_d, wavelengths, n_wl * 8, cudaMemcpyHostToDevice, s));
+  // Each pipeline unit's m, and a distinct index per (part, wavelength) for pass 1.
+  std::vector<double> m_unit(2 * n_units);
+  for (int64_t u = 0; u < n_units; ++u) {
+    const int64_t p = u / n_wl, i = u % n_wl;
+    m_unit[2 * u] = in[p].m[2 * i];
+    m_unit[2 * u + 1] = in[p].m[2 * i + 1];
+  }
+  double* m_d = c.m.as<double>(2 * n_units);
+  SB_CUDA(cudaMemcpyAsync(m_d, m_unit.data(), 2 * n_units * 8, cudaMemcpyHostToDevice, s));
+  // Node evaluations on the device (queries carry the pipeline unit in `wl`), in batches of at
+  // most kRows scratch rows.
+  constexpr int64_t kRows = int64_t(1) << 26;
+  double* wl_unit_d = c.p1_wlu.as<double>(n_units);
+  {
+    std::vector<double> wlu(n_units);
+    for (int64_t u = 0; u < n_units; ++u) wlu[u] = wavelengths[u % n_wl];
+    SB_CUDA(cudaMemcpyAsync(wl_unit_d, wlu.data(), n_units * 8, cudaMemcpyHostToDevice, s));
+  }
+  auto eval = [&](const std::vector<adaptive::Query>& qs, std::vector<adaptive::NodeResult>& out) {
+    size_t k0 = 0;
+    std::vector<double> r;
+    std::vector<int> wi;
+    std::vector<int64_t> off;
+    while (k0 < qs.size()) {
+      r.clear();
+      wi.clear();
+      off.assign(1, 0);
+      size_t k1 = k0;
+      while (k1 < qs.size()) {
+        const double x =
+            2.0 * 3.14159265358979323846 * qs[k1].r / wavelengths[qs[k1].wl % n_wl];
+        const int64_t cap = (std::isfinite(x) && x > 0.0 && x <= 1e6)
+                                ? (int64_t)std::ceil(x + 6.0 * std::cbrt(x) + 3.0) + 4
+                                : 0;
+        if (k1 > k0 && off.back() + cap > kRows) break;
+        r.push_back(qs[k1].r);
+        wi.push_back(qs[k1].wl);
+        off.push_back(off.back() + cap);
+        ++k1;
+      }
+      const int64_t n = (int64_t)r.size(), rows = std::max<int64_t>(off.back(), 1);
+      Pass1Args a{};
+      a.radius = c.p1_radius.as<double>(n);
+      a.wl_index = c.p1_wl.as<int>(n);
+      a.scratch = c.p1_scratch.as<int64_t>(n + 1);
+      a.uz = c.p1_uz.as<double2>(rows);
+      a.ux = c.p1_ux.as<double>(rows);
+      a.q = c.p1_q.as<double>(6 * n);
+      a.n_terms = c.p1_n.as<int64_t>(n);
+      a.status = c.p1_status.as<int>(n);
+      a.wl = wl_unit_d;
+      a.m = reinterpret_cast<const double2*>(m_d);
+      a.n = n;
+      a.allow_unvalidated = o.allow_unvalidated ? 1 : 0;
+      SB_CUDA(cudaMemcpyAsync((void*)a.radius, r.data(), n * 8, cudaMemcpyHostToDevice, s));
+      SB_CUDA(cudaMemcpyAsync((void*)a.wl_index, wi.data(), n * 4, cudaMemcpyHostToDevice, s));
+      SB_CUDA(cudaMemcpyAsync((void*)a.scratch, off.data(), (n + 1) * 8, cudaMemcpyHostToDevice,
+                              s));
+      timed_launch(K_NODES, s, [&] { launch_pass1(a, s); });
+      SB_CUDA(cudaGetLastError());
+      std::vector<double> q(6 * n);
+      std::vector<int64_t> nt(n);
+      std::vector<int> st(n);
+      SB_CUDA(cudaMemcpyAsync(q.data(), a.q, 6 * n * 8, cudaMemcpyDeviceToHost, s));
+      SB_CUDA(cudaMemcpyAsync(nt.data(), a.n_terms, n * 8, cudaMemcpyDeviceToHost, s));
+      SB_CUDA(cudaMemcpyAsync(st.data(), a.status, n * 4, cudaMemcpyDeviceToHost, s));
+      SB_CUDA(cudaStreamSynchronize(s));
+      for (int64_t k = 0; k < n; ++k) {
+        adaptive::NodeResult& x = out[k0 + k];
+        for (int j = 0; j < 6; ++j) x.q[j] = q[6 * k + j];
+        x.n = nt[k];
+        x.status = st[k];
+      }
+      k0 = k1;
+    }
+  };
+  // Jobs: pass-1 groups per wavelength. The pass-1 callback's `wl` is the pipeline unit of the
+  // group's first part (its m and wavelength serve every part of a batch: one particle).
+  std::vector<adaptive::Job> jobs;
+  std::vector<int> job_of(n_units, -1), place(n_units, 0);
+  std::vector<double> wl_of_job;
+  for (int64_t i = 0; i < n_wl; ++i) {
+    if (batch) {
+      adaptive::Job jb;
+      for (int64_t p = 0; p < n_parts; ++p)
+        if (parts[p].support != adaptive::POINT) {
+          if (jb.parts.empty()) jb.wl = (int)(p * n_wl + i);
+          place[p * n_wl + i] = (int)jb.parts.size();
+          job_of[p * n_wl + i] = (int)jobs.size();
+          jb.parts.push_back((int)p);
+        }
+      if (!jb.parts.empty()) jobs.push_back(jb);
+    } else {
+      for (int64_t p = 0; p < n_parts; ++p)
+        if (parts[p].support != adaptive::POINT) {
+          job_of[p * n_wl + i] = (int)jobs.size();
+          adaptive::Job jb;
+          jb.wl = (int)(p * n_wl + i);
+          jb.parts = {(int)p};
+          jobs.push_back(jb);
+        }
+    }
+  }
+  // Pass 1 sees the wavelength of each job's unit.
+  std::vector<double> wl_units(n_units);
+  for (int64_t u = 0; u < n_units; ++u) wl_units[u] = wavelengths[u % n_wl];
+  // Single radii: their node checked once.
+  std::vector<adaptive::Query> points;
+  std::vector<int64_t> point_unit;
+  for (int64_t p = 0; p < n_parts; ++p)
+    if (parts[p].support == adaptive::POINT)
+      for (int64_t i = 0; i < n_wl; ++i) {
+        points.push_back({parts[p].lo, (int)(p * n_wl + i)});
+        point_unit.push_back(p * n_wl + i);
+      }
+  std::vector<adaptive::NodeResult> point_res(points.size());
+  if (!points.empty()) eval(points, point_res);
+  adaptive::pass1(jobs, parts, wl_units.data(), o, eval);
+  // The first error in (wavelength, part) order.
+  {
+    int64_t first = n_units;
+    int status = 0;
+    std::string msg;
+    for (int64_t u = 0; u < n_units; ++u) {
+      const int64_t key = (u % n_wl) * n_parts + u / n_wl;
+      if (job_of[u] >= 0 && jobs[job_of[u]].status != 0 && key < first) {
+        first = key;
+        status = jobs[job_of[u]].status;
+        msg = jobs[job_of[u]].msg;
+      }
+    }
+    for (size_t k = 0; k < points.size(); ++k) {
+      const int64_t u = point_unit[k], key = (u % n_wl) * n_parts + u / n_wl;
+      if (point_res[k].status != 0 && key < first) {
+        first = key;
+        status = point_res[k].status;
+        msg = node_message(point_res[k].status, wavelengths[u % n_wl], points[k].r);
+      }
+    }
+    if (status != 0) throw Failure{status, msg};
+  }
+  // Pass 2: every unit's nodes, up to two panels per chunk of 32 (nodes 0-14 and 16-30), two
+  // only when their projector bands agree, so that each panel's tables go to its own band
+  // (engine.rs:1530-1543).
+  std::vector<std::vector<int64_t>> slot_of(jobs.size());
+  int64_t n_nodes = 32;
+  for (size_t k = 0; k < jobs.size(); ++k) {
+    const auto& jb = jobs[k];
+    int64_t next = 0;  // the next free half-chunk (16 nodes)
+    for (size_t pi = 0; pi < jb.panels.size(); ++pi) {
+      if (next % 2 == 1 && bucket(jb.panel_terms[pi]) != bucket(jb.panel_terms[pi - 1])) ++next;
+      slot_of[k].push_back(16 * next);
+      ++next;
+    }
+    n_nodes = std::max<int64_t>(n_nodes, 32 * ((next + 1) / 2));
+  }
+  if ((double)n_units * (double)n_nodes > 4e9)
+    throw Failure{SCATRS_INVALID_INPUT, "too many (unit, node) pairs for one call"};
+  std::vector<double> radius((size_t)n_units * n_nodes, 0.0), weight(radius.size(), 0.0),
+      wdiff(radius.size(), 0.0), norm((size_t)n_units * 8, 0.0);
+  std::vector<char> unit_converged(n_units, 1);
+  std::vector<int64_t> unit_panels(n_units, 0);
+  for (int64_t u = 0; u < n_units; ++u) {
+    const int64_t p = u / n_wl;
+    const adaptive::Part& part = parts[p];
+    double* nr = &radius[(size_t)u * n_nodes];
+    double* nw = &weight[(size_t)u * n_nodes];
+    double* nd = &wdiff[(size_t)u * n_nodes];
+    double* un = &norm[(size_t)u * 8];
+    if (part.support == adaptive::POINT) {
+      nr[0] = part.lo;
+      nw[0] = 1.0;
+      un[0] = 1.0;
+      un[3] = 1.0;
+      continue;
+    }
+    const adaptive::Job& jb = jobs[job_of[u]];
+    for (size_t pi = 0; pi < jb.panels.size(); ++pi) {
+      adaptive::Node g[15];
+      adaptive::gk15(jb.panels[pi].first, jb.panels[pi].second, g);
+      const size_t base = (size_t)slot_of[job_of[u]][pi];
+      for (int k = 0; k < 15; ++k) {
+        const double r = std::exp(g[k].t), ur = part.u(r) * r;
+        nr[base + k] = r;
+        nw[base + k] = g[k].wk * ur;
+        nd[base + k] = g[k].wk * ur - g[k].wg * ur;
+      }
+    }
+    un[0] = part.mom.z;
+    un[1] = part.mom.ez;
+    un[2] = part.support == adaptive::UNBOUNDED ? 0.2 * o.rtol : 0.0;
+    un[4] = part.mom.v[0];
+    un[5] = part.mom.e[0];
+    un[6] = part.mom.v[1];
+    un[7] = part.mom.e[1];
+    unit_converged[u] = jb.converged[place[u]] ? 1 : 0;
+    unit_panels[u] = (int64_t)jb.panels.size();
+  }
+  fo.n_nodes = (int32_t)n_nodes;
+  const int glen = options->greek_order >= 0 ? options->greek_order + 1 : 0;
+  const int64_t stride = 16 + 8 * n_mu + 12 * (int64_t)glen;
+  double* avg = c.avg.as<double>((size_t)n_units * stride);
+  AdaptiveInput ad;
+  ad.on = true;
+  ad.radius = radius.data();
+  ad.weight = weight.data();
+  ad.wdiff = wdiff.data();
+  ad.unit_norm = norm.data();
+  ad.avg = avg;
+  FixedCall call;
+  call.wl_host.assign(wavelengths, wavelengths + n_wl);
+  call.per_unit = true;
+  call.n_dist = n_parts;
+  call.n_wl = n_wl;
+  call.n_nodes = n_nodes;
+  std::vector<scatrs_distribution> dummy(n_parts);
+  run_fixed(c, dummy.data(), n_parts, wl_d, n_wl, m_d, mu, n_mu, &fo, nullptr, nullptr, nullptr,
+            s, &call, LayerInput(), DerivOutput(), ad);
+  // Mixing and outputs.
+  const int64_t n_outs = (int64_t)n_out * n_wl;
+  int64_t vl, pl, gl;
+  scatrs_ensemble_fixed_sizes(n_outs, n_mu, options->greek_order, &vl, &pl, &gl);
+  double* v_d = c.values.as<double>(2 * vl);
+  double* p_d = pl > 0 ? c.phase.as<double>(2 * pl) : nullptr;
+  double* g_d = gl > 0 ? c.greek.as<double>(2 * gl) : nullptr;
+  std::vector<int> first(n_out + 1, 0), member;
+  std::vector<double> frac;
+  for (int ou = 0; ou < n_out; ++ou) {
+    for (int64_t p = 0; p < n_parts; ++p)
+      if (in[p].out == ou) {
+        member.push_back((int)p);
+        frac.push_back(in[p].f);
+      }
+    first[ou + 1] = (int)member.size();
+  }
+  int* first_d = c.mix_first.as<int>(first.size());
+  int* member_d = c.mix_part.as<int>(std::max<size_t>(member.size(), 1));
+  double* frac_d = c.mix_frac.as<double>(std::max<size_t>(frac.size(), 1));
+  SB_CUDA(cudaMemcpyAsync(first_d, first.data(), first.size() * 4, cudaMemcpyHostToDevice, s));
+  SB_CUDA(cudaMemcpyAsync(member_d, member.data(), member.size() * 4, cudaMemcpyHostToDevice, s));
+  SB_CUDA(cudaMemcpyAsync(frac_d, frac.data(), frac.size() * 8, cudaMemcpyHostToDevice, s));
+  MixArgs mx{};
+  mx.n_out = n_out;
+  mx.n_wl = (int)n_wl;
+  mx.n_mu = (int)n_mu;
+  mx.greek_order = options->greek_order;
+  mx.normalized = options->normalized;
+  mx.first = first_d;
+  mx.part = member_d;
+  mx.fraction = frac_d;
+  mx.avg = avg;
+  mx.values = v_d;
+  mx.errors = v_d + vl;
+  mx.phase = p_d;
+  mx.phase_err = p_d ? p_d + pl : nullptr;
+  mx.greek = g_d;
+  mx.greek_err = g_d ? g_d + gl : nullptr;
+  mx.err = c.err.as<unsigned long long>(2);
+  timed_launch(K_FINAL, s, [&] { launch_mix(mx, s); });
+  SB_CUDA(cudaGetLastError());
+  call.radius = std::move(radius);
+  check_device_errors(c, s, &call);
+  SB_CUDA(cudaMemcpyAsync(res.values, v_d, vl * 8, cudaMemcpyDeviceToHost, s));
+  if (res.errors) SB_CUDA(cudaMemcpyAsync(res.errors, v_d + vl, vl * 8, cudaMemcpyDeviceToHost, s));
+  if (pl > 0 && res.phase)
+    SB_CUDA(cudaMemcpyAsync(res.phase, p_d, pl * 8, cudaMemcpyDeviceToHost, s));
+  if (pl > 0 && res.phase_err)
+    SB_CUDA(cudaMemcpyAsync(res.phase_err, p_d + pl, pl * 8, cudaMemcpyDeviceToHost, s));
+  if (gl > 0 && res.greek)
+    SB_CUDA(cudaMemcpyAsync(res.greek, g_d, gl * 8, cudaMemcpyDeviceToHost, s));
+  if (gl > 0 && res.greek_err)
+    SB_CUDA(cudaMemcpyAsync(res.greek_err, g_d + gl, gl * 8, cudaMemcpyDeviceToHost, s));
+  SB_CUDA(cudaStreamSynchronize(s));
+  // converged: every part of the output unit; panels: the sum over its distinct groups
+  // (engine.rs:2228-2236).
+  for (int ou = 0; ou < n_out; ++ou)
+    for (int64_t i = 0; i < n_wl; ++i) {
+      bool conv = true;
+      int64_t pan = 0;
+      std::vector<int> seen;
+      for (int k = first[ou]; k < first[ou + 1]; ++k) {
+        const int64_t u = (int64_t)member[k] * n_wl + i;
+        conv = conv && unit_converged[u];
+        const int g = job_of[u];
+        if (g >= 0 && std::find(seen.begin(), seen.end(), g) == seen.end()) {
+          seen.push_back(g);
+          pan += unit_panels[u];
+        }
+      }
+      if (res.converged) res.converged[ou * n_wl + i] = conv ? 1 : 0;
+      if (res.panels) res.panels[ou * n_wl + i] = pan;
+    }
+}
+
 FixedCall g_last_call;  // for scatrs_check_errors
 
 template <class F>
@@ -1111,259 +1462,62 @@ int scatrs_ensemble_adaptive(const scatrs_distribution* dists, int64_t n_dist, i
                              double* greek_err, int8_t* converged, int64_t* panels, char* err,
                              size_t err_len) {
   return guarded(err, err_len, [&] {
-    if (!options) throw Failure{SCATRS_INVALID_INPUT, "options must not be NULL"};
-    if (n_dist < 0 || n_wl < 0) throw Failure{SCATRS_INVALID_INPUT, "negative sizes"};
-    const adaptive::Options o{options->rtol, options->max_panels,
-                              options->allow_unvalidated != 0, options->refine_backscatter != 0};
-    // ensemble/mod.rs:688-720.
-    if (!(o.rtol >= 1e-13 && o.rtol <= 0.1)) {
-      char buf[80];
-      snprintf(buf, sizeof buf, "rtol must be in [1e-13, 0.1], got %g", o.rtol);
-      throw Failure{SCATRS_INVALID_INPUT, buf};
-    }
-    if (o.max_panels < 1) throw Failure{SCATRS_INVALID_INPUT, "max_panels must be at least 1"};
-    for (int64_t i = 0; i < n_wl; ++i)
-      if (!(std::isfinite(wavelengths[i]) && wavelengths[i] > 0.0))
-        throw Failure{SCATRS_INVALID_INPUT, "wavelength " + std::to_string(i) +
-                                                " must be finite and > 0"};
-    scatrs_fixed_options fo{32, options->greek_order, options->normalized,
-                            options->allow_unvalidated};
-    const int64_t n_units = n_dist * n_wl;
-    check_options(&fo, n_units, n_mu, mu);
-    if (n_units == 0) return;
-    std::vector<adaptive::Part> parts;
-    for (int64_t d = 0; d < n_dist; ++d) {
-      try {
-        parts.push_back(adaptive::make_part(dists[d].kind, dists[d].param, o.rtol));
-      } catch (const adaptive::Error& e) {
-        throw Failure{e.status, "distribution " + std::to_string(d) + ": " + e.msg};
-      }
-    }
-    Context& c = context();
-    std::lock_guard<std::mutex> lk(c.mtx);
-    cudaStream_t s = 0;
-    double* wl_d = c.wl.as<double>(n_wl);
-    SB_CUDA(cudaMemcpyAsync(wl_d, wavelengths, n_wl * 8, cudaMemcpyHostToDevice, s));
-    double2* m_wl = c.fractions.as<double2>(n_wl);  // the index per wavelength, for pass 1
-    SB_CUDA(cudaMemcpyAsync(m_wl, m, n_wl * 16, cudaMemcpyHostToDevice, s));
-    // Node evaluations on the device, in batches of at most kRows scratch rows.
-    constexpr int64_t kRows = int64_t(1) << 26;
-    auto eval = [&](const std::vector<adaptive::Query>& qs,
-                    std::vector<adaptive::NodeResult>& res) {
-      size_t k0 = 0;
-      std::vector<double> r;
-      std::vector<int> wi;
-      std::vector<int64_t> off;
-      while (k0 < qs.size()) {
-        r.clear();
-        wi.clear();
-        off.assign(1, 0);
-        size_t k1 = k0;
-        while (k1 < qs.size()) {
-          const double x = 2.0 * 3.14159265358979323846 * qs[k1].r / wavelengths[qs[k1].wl];
-          const int64_t cap = (std::isfinite(x) && x > 0.0 && x <= 1e6)
-                                  ? (int64_t)std::ceil(x + 6.0 * std::cbrt(x) + 3.0) + 4
-                                  : 0;
-          if (k1 > k0 && off.back() + cap > kRows) break;
-          r.push_back(qs[k1].r);
-          wi.push_back(qs[k1].wl);
-          off.push_back(off.back() + cap);
-          ++k1;
-        }
-        const int64_t n = (int64_t)r.size(), rows = std::max<int64_t>(off.back(), 1);
-        Pass1Args a{};
-        a.radius = c.p1_radius.as<double>(n);
-        a.wl_index = c.p1_wl.as<int>(n);
-        a.scratch = c.p1_scratch.as<int64_t>(n + 1);
-        a.uz = c.p1_uz.as<double2>(rows);
-        a.ux = c.p1_ux.as<double>(rows);
-        a.q = c.p1_q.as<double>(6 * n);
-        a.n_terms = c.p1_n.as<int64_t>(n);
-        a.status = c.p1_status.as<int>(n);
-        a.wl = wl_d;
-        a.m = m_wl;
-        a.n = n;
-        a.allow_unvalidated = o.allow_unvalidated ? 1 : 0;
-        SB_CUDA(cudaMemcpyAsync((void*)a.radius, r.data(), n * 8, cudaMemcpyHostToDevice, s));
-        SB_CUDA(cudaMemcpyAsync((void*)a.wl_index, wi.data(), n * 4, cudaMemcpyHostToDevice, s));
-        SB_CUDA(cudaMemcpyAsync((void*)a.scratch, off.data(), (n + 1) * 8,
-                                cudaMemcpyHostToDevice, s));
-        timed_launch(K_NODES, s, [&] { launch_pass1(a, s); });
-        SB_CUDA(cudaGetLastError());
-        std::vector<double> q(6 * n);
-        std::vector<int64_t> nt(n);
-        std::vector<int> st(n);
-        SB_CUDA(cudaMemcpyAsync(q.data(), a.q, 6 * n * 8, cudaMemcpyDeviceToHost, s));
-        SB_CUDA(cudaMemcpyAsync(nt.data(), a.n_terms, n * 8, cudaMemcpyDeviceToHost, s));
-        SB_CUDA(cudaMemcpyAsync(st.data(), a.status, n * 4, cudaMemcpyDeviceToHost, s));
-        SB_CUDA(cudaStreamSynchronize(s));
-        for (int64_t k = 0; k < n; ++k) {
-          adaptive::NodeResult& x = res[k0 + k];
-          for (int j = 0; j < 6; ++j) x.q[j] = q[6 * k + j];
-          x.n = nt[k];
-          x.status = st[k];
-        }
-        k0 = k1;
-      }
-    };
-    // Jobs: a batch shares one group per wavelength (single radii alone); otherwise every
-    // distribution is its own call (engine.rs:236-296).
-    std::vector<adaptive::Job> jobs;
-    std::vector<int> job_of(n_units, -1);
-    std::vector<int> place(n_units, 0);
-    for (int64_t i = 0; i < n_wl; ++i) {
-      if (batch) {
-        adaptive::Job jb;
-        jb.wl = (int)i;
-        for (int64_t d = 0; d < n_dist; ++d)
-          if (parts[d].support != adaptive::POINT) {
-            place[d * n_wl + i] = (int)jb.parts.size();
-            job_of[d * n_wl + i] = (int)jobs.size();
-            jb.parts.push_back((int)d);
-          }
-        if (!jb.parts.empty()) jobs.push_back(jb);
-      } else {
-        for (int64_t d = 0; d < n_dist; ++d)
-          if (parts[d].support != adaptive::POINT) {
-            job_of[d * n_wl + i] = (int)jobs.size();
-            adaptive::Job jb;
-            jb.wl = (int)i;
-            jb.parts = {(int)d};
-            jobs.push_back(jb);
-          }
-      }
-    }
-    // Single radii: their node checked once.
-    std::vector<adaptive::Query> points;
-    std::vector<int64_t> point_unit;
+    if (n_dist < 0) throw Failure{SCATRS_INVALID_INPUT, "negative sizes"};
+    std::vector<AdPart> parts;
     for (int64_t d = 0; d < n_dist; ++d)
-      if (parts[d].support == adaptive::POINT)
-        for (int64_t i = 0; i < n_wl; ++i) {
-          points.push_back({parts[d].lo, (int)i});
-          point_unit.push_back(d * n_wl + i);
-        }
-    std::vector<adaptive::NodeResult> point_res(points.size());
-    if (!points.empty()) eval(points, point_res);
-    adaptive::pass1(jobs, parts, wavelengths, o, eval);
-    // The first error in (wavelength, distribution) order.
-    {
-      int64_t first = n_units;
-      int status = 0;
-      std::string msg;
-      for (int64_t u = 0; u < n_units; ++u) {
-        const int64_t key = (u % n_wl) * n_dist + u / n_wl;
-        if (job_of[u] >= 0 && jobs[job_of[u]].status != 0 && key < first) {
-          first = key;
-          status = jobs[job_of[u]].status;
-          msg = jobs[job_of[u]].msg;
-        }
+      parts.push_back(AdPart{dists[d].kind, {dists[d].param[0], dists[d].param[1],
+                                             dists[d].param[2]},
+                             m, 1.0, (int)d, "distribution " + std::to_string(d) + ": "});
+    AdOutputs out{values, errors, phase, phase_err, greek, greek_err, converged, panels};
+    adaptive_call(parts, (int)n_dist, batch != 0, wavelengths, n_wl, mu, n_mu, options, out);
+  });
+}
+
+int scatrs_ensemble_mixture(const scatrs_component* components, int64_t n_comp,
+                            const double* wavelengths, int64_t n_wl, const double* mu,
+                            int64_t n_mu, const scatrs_adaptive_options* options, double* values,
+                            double* errors, double* phase, double* phase_err, double* greek,
+                            double* greek_err, int8_t* converged, int64_t* panels, char* err,
+                            size_t err_len) {
+  return guarded(err, err_len, [&] {
+    // ensemble/mod.rs:609-625, 688-780: the components' weights and modes.
+    if (n_comp < 1) throw Failure{SCATRS_INVALID_INPUT, "a mixture needs a component"};
+    double total = 0.0;
+    for (int64_t c = 0; c < n_comp; ++c) {
+      const scatrs_component& k = components[c];
+      const std::string who = "component " + std::to_string(c);
+      if (!(std::isfinite(k.weight) && k.weight >= 0.0))
+        throw Failure{SCATRS_INVALID_INPUT, "the weight of " + who + " must be finite and >= 0"};
+      if (k.n_modes < 1 || !k.modes || !k.m)
+        throw Failure{SCATRS_INVALID_INPUT, who + ": needs a distribution and m"};
+      if (k.n_modes > 1) {
+        if (!k.mode_weights) throw Failure{SCATRS_INVALID_INPUT, who + ": needs mode weights"};
+        double sum = 0.0;
+        for (int j = 0; j < k.n_modes; ++j) sum += k.mode_weights[j];
+        if (!std::isfinite(sum))
+          throw Failure{SCATRS_INVALID_INPUT, who + ": the mode weights must have a finite sum"};
       }
-      for (size_t k = 0; k < points.size(); ++k) {
-        const int64_t u = point_unit[k], key = (u % n_wl) * n_dist + u / n_wl;
-        if (point_res[k].status != 0 && key < first) {
-          first = key;
-          status = point_res[k].status;
-          msg = node_message(point_res[k].status, wavelengths[u % n_wl], points[k].r);
-        }
-      }
-      if (status != 0) throw Failure{status, msg};
+      total += k.weight;
     }
-    // Pass 2: every unit's nodes, up to two panels per chunk of 32 (nodes 0-14 and 16-30),
-    // two only when their projector bands agree, so that each panel's tables go to its own
-    // band (engine.rs:1530-1543).
-    std::vector<std::vector<int64_t>> slot_of(jobs.size());
-    int64_t n_nodes = 32;
-    for (size_t k = 0; k < jobs.size(); ++k) {
-      const auto& jb = jobs[k];
-      int64_t next = 0;  // the next free half-chunk (16 nodes)
-      for (size_t pi = 0; pi < jb.panels.size(); ++pi) {
-        if (next % 2 == 1 && bucket(jb.panel_terms[pi]) != bucket(jb.panel_terms[pi - 1])) ++next;
-        slot_of[k].push_back(16 * next);
-        ++next;
+    if (!(std::isfinite(total) && total > 0.0))
+      throw Failure{SCATRS_INVALID_INPUT,
+                    "the mixture weights must have a finite, positive sum"};
+    std::vector<AdPart> parts;
+    for (int64_t c = 0; c < n_comp; ++c) {
+      const scatrs_component& k = components[c];
+      double v_total = 0.0;
+      for (int j = 0; j < k.n_modes; ++j) v_total += k.n_modes > 1 ? k.mode_weights[j] : 1.0;
+      for (int j = 0; j < k.n_modes; ++j) {
+        const double v = k.n_modes > 1 ? k.mode_weights[j] : 1.0;
+        const scatrs_distribution& d = k.modes[j];
+        // The number fraction of engine.rs:2131: w / w_total * v / v_total.
+        parts.push_back(AdPart{d.kind, {d.param[0], d.param[1], d.param[2]}, k.m,
+                               k.weight / total * v / v_total, 0,
+                               "component " + std::to_string(c) + ": "});
       }
-      n_nodes = std::max<int64_t>(n_nodes, 32 * ((next + 1) / 2));
     }
-    if ((double)n_units * (double)n_nodes > 4e9)
-      throw Failure{SCATRS_INVALID_INPUT, "too many (unit, node) pairs for one call"};
-    std::vector<double> radius((size_t)n_units * n_nodes, 0.0), weight(radius.size(), 0.0),
-        wdiff(radius.size(), 0.0), norm((size_t)n_units * 8, 0.0);
-    std::vector<double> m_unit(2 * n_units);
-    for (int64_t u = 0; u < n_units; ++u) {
-      const int64_t d = u / n_wl, i = u % n_wl;
-      m_unit[2 * u] = m[2 * i];
-      m_unit[2 * u + 1] = m[2 * i + 1];
-      const adaptive::Part& p = parts[d];
-      double* nr = &radius[(size_t)u * n_nodes];
-      double* nw = &weight[(size_t)u * n_nodes];
-      double* nd = &wdiff[(size_t)u * n_nodes];
-      double* un = &norm[(size_t)u * 8];
-      if (p.support == adaptive::POINT) {
-        nr[0] = p.lo;
-        nw[0] = 1.0;
-        un[0] = 1.0;
-        un[3] = 1.0;
-        converged[u] = 1;
-        panels[u] = 0;
-        continue;
-      }
-      const adaptive::Job& jb = jobs[job_of[u]];
-      for (size_t pi = 0; pi < jb.panels.size(); ++pi) {
-        adaptive::Node g[15];
-        adaptive::gk15(jb.panels[pi].first, jb.panels[pi].second, g);
-        const size_t base = (size_t)slot_of[job_of[u]][pi];
-        for (int k = 0; k < 15; ++k) {
-          const double r = std::exp(g[k].t), ur = p.u(r) * r;
-          nr[base + k] = r;
-          nw[base + k] = g[k].wk * ur;
-          nd[base + k] = g[k].wk * ur - g[k].wg * ur;
-        }
-      }
-      un[0] = p.mom.z;
-      un[1] = p.mom.ez;
-      un[2] = p.support == adaptive::UNBOUNDED ? 0.2 * o.rtol : 0.0;
-      un[4] = p.mom.v[0];
-      un[5] = p.mom.e[0];
-      un[6] = p.mom.v[1];
-      un[7] = p.mom.e[1];
-      converged[u] = jb.converged[place[u]] ? 1 : 0;
-      panels[u] = (int64_t)jb.panels.size();
-    }
-    double* m_d = c.m.as<double>(2 * n_units);
-    SB_CUDA(cudaMemcpyAsync(m_d, m_unit.data(), 2 * n_units * 8, cudaMemcpyHostToDevice, s));
-    fo.n_nodes = (int32_t)n_nodes;
-    int64_t vl, pl, gl;
-    scatrs_ensemble_fixed_sizes(n_units, n_mu, options->greek_order, &vl, &pl, &gl);
-    double* v_d = c.values.as<double>(2 * vl);
-    double* p_d = pl > 0 ? c.phase.as<double>(2 * pl) : nullptr;
-    double* g_d = gl > 0 ? c.greek.as<double>(2 * gl) : nullptr;
-    AdaptiveInput ad;
-    ad.on = true;
-    ad.radius = radius.data();
-    ad.weight = weight.data();
-    ad.wdiff = wdiff.data();
-    ad.unit_norm = norm.data();
-    ad.errors = v_d + vl;
-    ad.phase_err = p_d ? p_d + pl : nullptr;
-    ad.greek_err = g_d ? g_d + gl : nullptr;
-    FixedCall call;
-    call.wl_host.assign(wavelengths, wavelengths + n_wl);
-    call.per_unit = true;
-    call.n_dist = n_dist;
-    call.n_wl = n_wl;
-    call.n_nodes = n_nodes;
-    run_fixed(c, dists, n_dist, wl_d, n_wl, m_d, mu, n_mu, &fo, v_d, p_d, g_d, s, &call,
-              LayerInput(), DerivOutput(), ad);
-    call.radius = std::move(radius);
-    check_device_errors(c, s, &call);
-    SB_CUDA(cudaMemcpyAsync(values, v_d, vl * 8, cudaMemcpyDeviceToHost, s));
-    if (errors) SB_CUDA(cudaMemcpyAsync(errors, ad.errors, vl * 8, cudaMemcpyDeviceToHost, s));
-    if (pl > 0 && phase) SB_CUDA(cudaMemcpyAsync(phase, p_d, pl * 8, cudaMemcpyDeviceToHost, s));
-    if (pl > 0 && phase_err)
-      SB_CUDA(cudaMemcpyAsync(phase_err, ad.phase_err, pl * 8, cudaMemcpyDeviceToHost, s));
-    if (gl > 0 && greek) SB_CUDA(cudaMemcpyAsync(greek, g_d, gl * 8, cudaMemcpyDeviceToHost, s));
-    if (gl > 0 && greek_err)
-      SB_CUDA(cudaMemcpyAsync(greek_err, ad.greek_err, gl * 8, cudaMemcpyDeviceToHost, s));
-    SB_CUDA(cudaStreamSynchronize(s));
+    AdOutputs out{values, errors, phase, phase_err, greek, greek_err, converged, panels};
+    adaptive_call(parts, 1, false, wavelengths, n_wl, mu, n_mu, options, out);
   });
 }
 

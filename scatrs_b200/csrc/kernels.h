@@ -192,11 +192,26 @@ struct FinalArgs {
   double* d_phase;
   double* d_greek;
   // Adaptive: per unit 8 doubles (z, ez, truncation, point, <r^2>, its error, <r^3>, its
-  // error), and the error outputs laid out as the values.
+  // error); the averages go to avg (per unit 16 + 8 n_mu + 12 (L + 1) doubles) for the mixing.
   const double* unit_norm;
+  double* avg;
+};
+
+// The mixing and the outputs of adaptive calls: output unit (o, wavelength i) is
+// sum_k fraction[k] * averages of part part[k] at i, for k in first[o] .. first[o + 1] - 1.
+struct MixArgs {
+  int n_out, n_wl, n_mu, greek_order, normalized;
+  const int* first;
+  const int* part;
+  const double* fraction;
+  const double* avg;
+  double* values;
   double* errors;
+  double* phase;
   double* phase_err;
+  double* greek;
   double* greek_err;
+  unsigned long long* err;
 };
 
 // Pass 1 of the adaptive ensemble: each node's per-particle quantities 1, pi r^2 Q_ext,
@@ -224,5 +239,6 @@ void launch_units(const UnitArgs& a, int grid, cudaStream_t s);
 void launch_proj(const ProjArgs& a, cudaStream_t s);
 void launch_final(const FinalArgs& a, cudaStream_t s);
 void launch_pass1(const Pass1Args& a, cudaStream_t s);
+void launch_mix(const MixArgs& a, cudaStream_t s);
 
 }  // namespace sb

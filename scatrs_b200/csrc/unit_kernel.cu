@@ -784,16 +784,18 @@ __device__ __forceinline__ LinE ldiv(LinE a, LinE b) {
 __device__ __forceinline__ LinE lscale(LinE a, double c) { return {c * a.v, fabs(c) * a.e}; }
 }  // namespace
 
+// Stage 1 of the adaptive outputs: each (part, wavelength) unit's averages with their error
+// estimates into `avg` (per unit: the 8 scalars, the 4 n_mu cosine tables, the 6 (L + 1) Greek
+// sums, each as values then errors). The Greek sums are projected per part and mixed after
+// (the projection is linear and its bounds are linear in the errors).
 __global__ void __launch_bounds__(NT) final_adaptive_kernel(FinalArgs a) {
   __shared__ double S[2][8];
-  __shared__ LinE a0s;
   const int t = threadIdx.x;
   const int L = a.greek_order;
   const int glen = L >= 0 ? L + 1 : 0;
-  const int64_t nu = a.n_units_total;
+  const int64_t stride = 16 + 8 * (int64_t)a.n_mu + 12 * (int64_t)glen;
   for (int ul = blockIdx.x; ul < a.n_units; ul += gridDim.x) {
     const int64_t unit = a.units[ul];
-    const int64_t d = unit / a.n_wl, i = unit % a.n_wl;
     if (t < 16) {
       double s = 0.0;
       for (int c = 0; c < a.cpu; ++c) s += a.chunk_sums[((int64_t)ul * a.cpu + c) * 16 + t];
@@ -807,19 +809,72 @@ __global__ void __launch_bounds__(NT) final_adaptive_kernel(FinalArgs a) {
       const double v = s / z;
       return LinE{v, (e + fabs(v) * ez) / z + tr * fabs(v)};
     };
-    LinE v[8];
-    for (int k = 0; k < 8; ++k) v[k] = avg(S[0][k], S[1][k]);
-    if (!point) {
-      v[6] = LinE{un[4], un[5]};
-      v[7] = LinE{un[6], un[7]};
+    double* out = a.avg + stride * unit;
+    if (t < 8) {
+      LinE v = avg(S[0][t], S[1][t]);
+      // <r^2>, <r^3> from the moment integration (a single radius keeps its own).
+      if (!point && t >= 6) v = LinE{un[4 + 2 * (t - 6)], un[5 + 2 * (t - 6)]};
+      out[t] = v.v;
+      out[8 + t] = v.e;
     }
-    const LinE ext = v[1], sca = v[2], scag = v[3], ab = v[4], back = v[5], r2 = v[6], r3 = v[7];
+    const double* acc_user = a.acc + a.unit_acc[ul];
+    for (int j = t; j < 4 * a.n_mu; j += NT) {
+      const LinE f = avg(acc_user[j], acc_user[4 * a.n_mu + j]);
+      out[16 + j] = f.v;
+      out[16 + 4 * a.n_mu + j] = f.e;
+    }
+    if (glen > 0) {
+      // The unit's slots: per band a values slot, then its bounds slot.
+      const int2 sl = a.unit_slots[ul];
+      double* og = out + 16 + 8 * (int64_t)a.n_mu;
+      for (int idx = t; idx < 6 * glen; idx += NT) {
+        const int e = idx / glen, l = idx % glen;
+        double gv = 0.0, ge = 0.0;
+        for (int k = 0; k + 1 < sl.y; k += 2) {
+          const BandSlot bs = a.slots[sl.x + k];
+          if (l <= a.bands[bs.band].order) {
+            gv += a.slot_greek[(int64_t)(sl.x + k) * 6 * glen + (int64_t)e * glen + l];
+            ge += a.slot_greek[(int64_t)(sl.x + k + 1) * 6 * glen + (int64_t)e * glen + l];
+          }
+        }
+        og[idx] = gv;
+        og[6 * glen + idx] = ge;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Stage 2: each output unit (o, wavelength i) mixes its parts' averages with their number
+// fractions f (engine.rs:2121-2176: values and errors alike, in part order) and assembles the
+// outputs: ratios, normalizations and bounds of ensemble/lin.rs, Greek normalized by the
+// mixture's alpha1_0 (engine.rs:2396-2497).
+__global__ void __launch_bounds__(NT) mix_assemble_kernel(MixArgs a) {
+  __shared__ double V[16];
+  __shared__ LinE a0s;
+  const int t = threadIdx.x;
+  const int glen = a.greek_order >= 0 ? a.greek_order + 1 : 0;
+  const int64_t stride = 16 + 8 * (int64_t)a.n_mu + 12 * (int64_t)glen;
+  const int64_t n_out = (int64_t)a.n_out * a.n_wl;
+  auto mixed = [&](int64_t o, int64_t i, int64_t off) {
+    double v = 0.0;
+    for (int k = a.first[o]; k < a.first[o + 1]; ++k)
+      v += a.fraction[k] * a.avg[stride * ((int64_t)a.part[k] * a.n_wl + i) + off];
+    return v;
+  };
+  for (int64_t ou = blockIdx.x; ou < n_out; ou += gridDim.x) {
+    const int64_t o = ou / a.n_wl, i = ou % a.n_wl;
+    if (t < 16) V[t] = mixed(o, i, t);
+    __syncthreads();
+    auto lin = [&](int k) { return LinE{V[k], V[8 + k]}; };
+    const LinE ext = lin(1), sca = lin(2), scag = lin(3), ab = lin(4), back = lin(5), r2 = lin(6),
+               r3 = lin(7);
     if (t == 0) {
       const bool bext = !(isfinite(ext.v) && ext.v != 0.0);
       const bool bsca = !(isfinite(sca.v) && sca.v != 0.0);
       const bool bback = !(isfinite(back.v) && back.v != 0.0);
       if (bext || bsca || bback) {
-        unsigned long long key = ((unsigned long long)(i * a.n_dist + d) << 2) |
+        unsigned long long key = ((unsigned long long)(i * a.n_out + o) << 2) |
                                  (unsigned long long)(bext ? 1 : (bsca ? 2 : 3));
         atomicMin(a.err + 1, key);
       }
@@ -835,53 +890,46 @@ __global__ void __launch_bounds__(NT) final_adaptive_kernel(FinalArgs a) {
                             lscale(r2, kPi),
                             lscale(r3, 4.0 * kPi / 3.0)};
       for (int k = 0; k < 11; ++k) {
-        a.values[k * nu + unit] = out[k].v;
-        a.errors[k * nu + unit] = out[k].e;
+        a.values[k * n_out + ou] = out[k].v;
+        a.errors[k * n_out + ou] = out[k].e;
       }
     }
-    const double* acc_user = a.acc + a.unit_acc[ul];
     if (a.phase) {
       for (int j = t; j < a.n_mu; j += NT) {
         LinE f[4];
         for (int e = 0; e < 4; ++e) {
-          f[e] = avg(acc_user[e * a.n_mu + j], acc_user[(4 + e) * a.n_mu + j]);
+          f[e] = LinE{mixed(o, i, 16 + e * a.n_mu + j),
+                      mixed(o, i, 16 + (4 + e) * (int64_t)a.n_mu + j)};
           if (a.normalized) f[e] = ldiv(f[e], sca);
         }
         const int src[6] = {0, 1, 0, 2, 3, 2};
         for (int e = 0; e < 6; ++e) {
-          a.phase[((int64_t)e * nu + unit) * a.n_mu + j] = f[src[e]].v;
-          a.phase_err[((int64_t)e * nu + unit) * a.n_mu + j] = f[src[e]].e;
+          a.phase[((int64_t)e * n_out + ou) * a.n_mu + j] = f[src[e]].v;
+          a.phase_err[((int64_t)e * n_out + ou) * a.n_mu + j] = f[src[e]].e;
         }
       }
     }
     if (glen > 0 && a.greek) {
-      // The unit's slots: per band a values slot, then its bounds slot.
-      const int2 sl = a.unit_slots[ul];
-      auto sum = [&](int idx) {
-        const int e = idx / glen, l = idx % glen;
-        LinE g{0.0, 0.0};
-        for (int k = 0; k + 1 < sl.y; k += 2) {
-          const BandSlot bs = a.slots[sl.x + k];
-          if (l <= a.bands[bs.band].order) {
-            g.v += a.slot_greek[(int64_t)(sl.x + k) * 6 * glen + (int64_t)e * glen + l];
-            g.e += a.slot_greek[(int64_t)(sl.x + k + 1) * 6 * glen + (int64_t)e * glen + l];
-          }
-        }
-        return g;
-      };
-      if (t == 0) a0s = sum(0);
+      const int64_t g0 = 16 + 8 * (int64_t)a.n_mu;
+      if (t == 0) a0s = LinE{mixed(o, i, g0), mixed(o, i, g0 + 6 * glen)};
       __syncthreads();
       const LinE a0 = a0s;
       for (int idx = t; idx < 6 * glen; idx += NT) {
         const int e = idx / glen, l = idx % glen;
-        LinE g = sum(idx);
+        LinE g{mixed(o, i, g0 + idx), mixed(o, i, g0 + 6 * glen + idx)};
         if (a.normalized) g = idx == 0 ? LinE{1.0, 0.0} : ldiv(g, a0);
-        a.greek[((int64_t)e * nu + unit) * glen + l] = g.v;
-        a.greek_err[((int64_t)e * nu + unit) * glen + l] = g.e;
+        a.greek[((int64_t)e * n_out + ou) * glen + l] = g.v;
+        a.greek_err[((int64_t)e * n_out + ou) * glen + l] = g.e;
       }
     }
     __syncthreads();
   }
+}
+
+void launch_mix(const MixArgs& a, cudaStream_t s) {
+  const int64_t n = (int64_t)a.n_out * a.n_wl;
+  const int grid = (int)(n < 4096 ? n : 4096);
+  if (grid > 0) mix_assemble_kernel<<<grid, NT, 0, s>>>(a);
 }
 
 int unit_kernel_blocks_per_sm() {

@@ -83,3 +83,15 @@ def test_errors_name_the_node(gpu):
         gpu.ensemble_adaptive(d, [0.5], 1.5, rtol=0.5)
     with pytest.raises(InvalidInputError, match="distribution 0"):
         gpu.ensemble_adaptive(_dists((1, -0.1, 1.5)), [0.5], 1.5)
+
+
+def test_mixture_and_multimodal_match_the_oracle(gpu):
+    wl = np.array([0.45, 0.8])
+    comps = [(_dists((1, 0.1, 1.5)), None, 2.0, np.array([1.45 + 0j, 1.44 + 1e-5j])),
+             (_dists((1, 1.0, 1.3), (2, 0.4, 0.1)), [3.0, 1.0], 0.5,
+              np.array([1.53 + 0.01j, 1.50 + 0.02j])),
+             (_dists((5, 0.35)), None, 0.25, np.array([1.6 + 0.1j, 1.6 + 0.1j]))]
+    got = gpu.ensemble_mixture(comps, wl, MU, 14)
+    ref = O.ensemble_mixture([(_odist(d), mw, w, m) for d, mw, w, m in comps], wl, mu=MU,
+                             greek_order=14)
+    _compare(got, ref)

@@ -61,3 +61,20 @@ def test_adaptive_calls_mirror_the_reference(gpu):
                                        4096, False, False)
     assert b["values"].shape == (11, 4) and "greek" not in b and b["phase"].shape == (6, 4, 2)
     assert np.all(b["panels"][2:] == 0) and np.all(b["converged"])
+
+
+def test_mixture_call_mirrors_the_reference(gpu):
+    wl = np.array([0.5])
+    m1, m2 = np.array([1.45 + 0j]), np.array([1.53 + 0.01j])
+    items = [(("multimodal", [(2.0, ("lognormal", 0.1, 1.5)), (0.5, ("lognormal", 1.0, 1.3))]),
+              ("sphere", m1), 1.0)]
+    bi = _scatrs.ensemble_compute(items, wl, False, 10, False, None, True, [], 1e-6, 4096, False,
+                                  False)
+    both = _scatrs.ensemble_compute([(("lognormal", 0.1, 1.5), ("sphere", m1), 2.0),
+                                     (("lognormal", 1.0, 1.3), ("sphere", m1), 0.5)], wl, True,
+                                    10, False, None, True, [], 1e-6, 4096, False, False)
+    assert np.array_equal(bi["values"], both["values"])
+    mix = _scatrs.ensemble_compute([(("lognormal", 0.1, 1.5), ("sphere", m1), 2.0),
+                                    (("lognormal", 1.0, 1.3), ("sphere", m2), 0.5)], wl, True,
+                                   10, False, None, True, [], 1e-6, 4096, False, False)
+    assert mix["values"].shape == (11, 1) and mix["greek"].shape == (6, 1, 11)

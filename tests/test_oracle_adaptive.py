@@ -126,3 +126,30 @@ def test_bad_inputs_are_rejected():
         O.ensemble_adaptive(O.dist(1, 0.1, 1.5), [0.5], 1.5, rtol=0.5)
     with pytest.raises(O.OracleError, match="outside|validated"):
         O.ensemble_adaptive(O.dist(1, 0.1, 1.5), [0.5], 1.5 + 20j)
+
+
+def test_mixtures_average_with_the_number_weights():
+    """scatrs/tests/ensemble.rs:205-262."""
+    lam, mu = 0.6, np.array([0.5])
+    d1, m1, w1 = O.dist(1, 0.1, 1.5), 1.45 + 0j, 2.0
+    d2, m2, w2 = O.dist(1, 1.0, 1.3), 1.53 + 0.01j, 0.5
+    mix = O.ensemble_mixture([(d1, None, w1, m1), (d2, None, w2, m2)], [lam], mu=mu,
+                             greek_order=10)
+    a = O.ensemble_adaptive(d1, [lam], m1, mu=mu, greek_order=10)
+    b = O.ensemble_adaptive(d2, [lam], m2, mu=mu, greek_order=10)
+    fa, fb = w1 / (w1 + w2), w2 / (w1 + w2)
+    va, vb, vm = a["values"][:, 0], b["values"][:, 0], mix["values"][:, 0]
+    assert abs(vm[0] - (fa * va[0] + fb * vb[0])) <= 1e-12 * vm[0]
+    assert abs(vm[10] - (fa * va[10] + fb * vb[10])) <= 1e-12 * vm[10]
+    sca = fa * va[1] + fb * vb[1]
+    want = (fa * va[1] * a["phase"][0, 0, 0] + fb * vb[1] * b["phase"][0, 0, 0]) / sca
+    assert abs(mix["phase"][0, 0, 0] - want) < 1e-10 * want
+    want = (fa * va[1] * a["greek"][4, 0, 4] + fb * vb[1] * b["greek"][4, 0, 4]) / sca
+    assert abs(mix["greek"][4, 0, 4] - want) < 1e-10 * max(abs(want), 1e-6)
+    # A bimodal distribution is a mixture of its modes with one refractive index.
+    bi = O.ensemble_mixture([(np.concatenate([d1, d2]), [w1, w2], 1.0, m1)], [lam], mu=mu,
+                            greek_order=10)
+    both = O.ensemble_mixture([(d1, None, w1, m1), (d2, None, w2, m1)], [lam], mu=mu,
+                              greek_order=10)
+    assert np.array_equal(bi["values"], both["values"])
+    assert bi["panels"][0] == both["panels"][0]
