@@ -96,6 +96,150 @@ __device__ __forceinline__ void load_stage(Smem& sm, int st, const double* __res
   cp_commit();
 }
 
+// As load_stage, with the rows at or above nc zero-filled (cp.async with a zero source size), so
+// that whole 4-order steps of the FP64 MMA can run past the chunk's last order.
+__device__ __forceinline__ void cp_async16_zfill(void* dst, const void* src, bool valid) {
+  unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  const int n = valid ? 16 : 0;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(n));
+}
+__device__ __forceinline__ void load_stage_z(Smem& sm, int st, const double* __restrict__ ge,
+                                             const double* __restrict__ go, int ldr, int r0,
+                                             int k0, int nc, const double* __restrict__ xc) {
+  const int t = threadIdx.x;
+  {
+    const int kk = t >> 4, c = t & 15;
+    const bool valid = k0 + kk < nc;
+    const int64_t off = valid ? (int64_t)(k0 + kk) * ldr + r0 + 2 * c : 0;
+    cp_async16_zfill(&sm.a[st][0][kk][2 * c], ge + off, valid);
+    cp_async16_zfill(&sm.a[st][1][kk][2 * c], go + off, valid);
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int idx = t + q * NT;
+    const int kk = idx >> 6, c = idx & 63;
+    const bool valid = k0 + kk < nc;
+    cp_async16_zfill(&sm.xs[st][kk][2 * c], xc + (valid ? (int64_t)(k0 + kk) * 128 + 2 * c : 0),
+                     valid);
+  }
+  cp_commit();
+}
+
+// D (8x8) += A (8x4, row) B (4x8, col) in FP64 on the tensor cores (PTX mma.sync m8n8k4):
+// lane l holds A[l/4][l%4], B[l%4][l/4] and D[l/4][2 (l%4) + {0, 1}].
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+// The tile C_E = G_E X, C_O = G_O X (32 rows x 128 columns) on the FP64 tensor path: warp w
+// computes columns 32w .. 32w + 31 of all 32 rows as 4 x 4 MMA tiles of 8 x 8 each for E and O;
+// cE[mt][nt] is D of rows 8 mt .., columns 32 w + 8 nt ...
+__device__ __forceinline__ void gemm_tile_mma(Smem& sm, const double* __restrict__ ge,
+                                              const double* __restrict__ go, int ldr, int r0,
+                                              int nc, const double* __restrict__ xc,
+                                              double cE[4][4][2], double cO[4][4][2]) {
+  const int t = threadIdx.x, w = t >> 5, lane = t & 31, q = lane & 3, g = lane >> 2;
+#pragma unroll
+  for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt) {
+      cE[mt][nt][0] = cE[mt][nt][1] = 0.0;
+      cO[mt][nt][0] = cO[mt][nt][1] = 0.0;
+    }
+  load_stage_z(sm, 0, ge, go, ldr, r0, 0, nc, xc);
+  int st = 0;
+  for (int k0 = 0; k0 < nc; k0 += KB, st ^= 1) {
+    cp_wait_all();
+    __syncthreads();
+    if (k0 + KB < nc) load_stage_z(sm, st ^ 1, ge, go, ldr, r0, k0 + KB, nc, xc);
+    const int kend = nc - k0 < KB ? nc - k0 : KB;
+#pragma unroll
+    for (int k4 = 0; k4 < KB; k4 += 4) {
+      if (k4 < kend) {
+        const int kk = k4 + q;
+        double aE[4], aO[4], b[4];
+#pragma unroll
+        for (int mt = 0; mt < 4; ++mt) {
+          aE[mt] = sm.a[st][0][kk][8 * mt + g];
+          aO[mt] = sm.a[st][1][kk][8 * mt + g];
+        }
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) b[nt] = sm.xs[st][kk][32 * w + 8 * nt + g];
+#pragma unroll
+        for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+          for (int nt = 0; nt < 4; ++nt) {
+            dmma(cE[mt][nt][0], cE[mt][nt][1], aE[mt], b[nt]);
+            dmma(cO[mt][nt][0], cO[mt][nt][1], aO[mt], b[nt]);
+          }
+      }
+    }
+  }
+  __syncthreads();  // the stage buffers are free for the reduction and the next tile
+}
+
+// The elements of an MMA tile, scaled, weighted and summed over the chunk's 32 spheres. Lane
+// pairs (q, q ^ 1) hold a node's (u) and (v) columns; after exchanging them the even lane forms
+// the elements at +mu and the odd lane those at -mu, of its 4 rows (8 mt + g) and of its 4 nodes
+// (8 w + 2 nt + q / 2); the 4 nodes add in the thread, node pairs across lanes q, q ^ 2, and the
+// 4 warps in a fixed order through shared memory. Thread t ends with v[0], v[1] of row t / 4,
+// side (t / 2) & 1 and elements 2 (t & 1), 2 (t & 1) + 1.
+template <bool kUser>
+__device__ __forceinline__ void chunk_elements_mma(Smem& sm, const double cE[4][4][2],
+                                                   const double cO[4][4][2], double v[2]) {
+  const int t = threadIdx.x, w = t >> 5, lane = t & 31, q = lane & 3, g = lane >> 2;
+  const int side = q & 1;
+  const double sg = side ? -1.0 : 1.0;
+  double p[4][4];
+#pragma unroll
+  for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+    for (int k = 0; k < 4; ++k) p[mt][k] = 0.0;
+#pragma unroll
+  for (int nt = 0; nt < 4; ++nt) {
+    const int node = 8 * w + 2 * nt + (q >> 1);
+    const double wt = sm.w[node], cu = sm.cu[node], ar = sm.area[node], sc = sm.sc[node];
+#pragma unroll
+    for (int mt = 0; mt < 4; ++mt) {
+      const double e0 = cE[mt][nt][0], e1 = cE[mt][nt][1];
+      const double o0 = cO[mt][nt][0], o1 = cO[mt][nt][1];
+      const double pe0 = __shfl_xor_sync(0xffffffffu, e0, 1);
+      const double pe1 = __shfl_xor_sync(0xffffffffu, e1, 1);
+      const double po0 = __shfl_xor_sync(0xffffffffu, o0, 1);
+      const double po1 = __shfl_xor_sync(0xffffffffu, o1, 1);
+      // The even lane of a pair holds u (re, im), the odd one v.
+      const double eur = side ? pe0 : e0, eui = side ? pe1 : e1;
+      const double evr = side ? e0 : pe0, evi = side ? e1 : pe1;
+      const double our = side ? po0 : o0, oui = side ? po1 : o1;
+      const double ovr = side ? o0 : po0, ovi = side ? o1 : po1;
+      double e[4];
+      elements4(eur + sg * ovr, eui + sg * ovi, evr + sg * our, evi + sg * oui, e);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) p[mt][k] += kUser ? wt * ((cu * e[k]) * ar) : wt * (sc * e[k]);
+    }
+  }
+#pragma unroll
+  for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+    for (int k = 0; k < 4; ++k) p[mt][k] += __shfl_xor_sync(0xffffffffu, p[mt][k], 2);
+  double* red = &sm.xs[0][0][0];  // 4 warps x 256 partial sums
+  if (q < 2) {
+#pragma unroll
+    for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) red[w * 256 + ((8 * mt + g) * 2 + side) * 4 + k] = p[mt][k];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    const int o = 2 * t + j;
+    v[j] = ((red[o] + red[256 + o]) + red[512 + o]) + red[768 + o];
+  }
+  __syncthreads();
+}
+
 // accE/accO[r][c] = sum_k G[r0 + 4 rg + r][k] X[k][4 ng + c (+ 64 for c >= 4)] for k < nc.
 __device__ __forceinline__ void gemm_tile(Smem& sm, const double* __restrict__ ge,
                                           const double* __restrict__ go, int ldr, int r0, int nc,
@@ -348,54 +492,66 @@ __device__ __forceinline__ void unit_body(const UnitArgs& a) {
       __syncthreads();
       for (int half = 0; half < kHalves; ++half) {
         const double* xc = a.X + (a.chunk_row[ci] + (int64_t)half * nc) * 128;
-        double accE[4][8], accO[4][8], v[2];
+        double v[2];
+        // This thread's output of a reduced tile (kMode 0, the MMA tile, owns row t / 4).
+        const int o_row = kMode == 0 ? (t >> 2) : rg * 4 + rr;
+        const int o_side = kMode == 0 ? ((t >> 1) & 1) : side;
+        const int o_e0 = kMode == 0 ? 2 * (t & 1) : e0;
         for (int tile = it.group; tile < t_user + t_band; tile += it.n_groups) {
-          if (tile < t_user) {
-            const int r0 = tile * TR;
-            gemm_tile(sm, a.ge_u, a.go_u, a.h_u_pad, r0, nc, xc, accE, accO);
-            const int row = r0 + rg * 4 + rr;
-            int j = -1;
+          const bool user = tile < t_user;
+          const BandDesc B = user ? BandDesc{} : a.bands[b];
+          const int r0 = (user ? tile : tile - t_user) * TR;
+          const double* ge = user ? a.ge_u : a.band_ge + B.g_off;
+          const double* go = user ? a.go_u : a.band_go + B.g_off;
+          const int ldr = user ? a.h_u_pad : B.h_pad;
+          // The output index of this thread's sums, or -1.
+          const int row = r0 + o_row;
+          int j = -1;
+          if (user) {
             if (row < a.h_u) {
               const int2 mp = a.user_map[row];
-              j = side ? mp.y : mp.x;
+              j = o_side ? mp.y : mp.x;
             }
-            for (int blk = 0; blk < n_blk; ++blk) {
-              if (kDeriv)
-                chunk_elements_d<true>(sm, accE, accO, half, blk, a.n_theta, v);
-              else if (kMode == 2 && blk == 1)
-                chunk_errors<true>(sm, accE, accO, v);
-              else
-                chunk_elements<true>(sm, accE, accO, v);
-              if (j >= 0) {
-                double* au = acc_user + (int64_t)blk * 4 * a.n_mu;
-                au[e0 * a.n_mu + j] += v[0];
-                au[(e0 + 1) * a.n_mu + j] += v[1];
-              }
+          } else if (row < B.h) {
+            const int q = B.n_q, jn = q / 2 + row, mirror = q - 1 - jn;
+            if (o_side == 0 || mirror != jn) j = o_side ? mirror : jn;
+          }
+          const int64_t len = user ? a.n_mu : B.n_q;
+          double* base = user ? acc_user : a.acc + a.chunk_acc[ci];
+          if constexpr (kMode == 0) {
+            double cE[4][4][2], cO[4][4][2];
+            gemm_tile_mma(sm, ge, go, ldr, r0, nc, xc, cE, cO);
+            if (user)
+              chunk_elements_mma<true>(sm, cE, cO, v);
+            else
+              chunk_elements_mma<false>(sm, cE, cO, v);
+            if (j >= 0) {
+              base[o_e0 * len + j] += v[0];
+              base[(o_e0 + 1) * len + j] += v[1];
             }
           } else {
-            const BandDesc B = a.bands[b];
-            const int q = B.n_q, lo = q / 2;
-            const int r0 = (tile - t_user) * TR;
-            double* acc_band = a.acc + a.chunk_acc[ci];
-            gemm_tile(sm, a.band_ge + B.g_off, a.band_go + B.g_off, B.h_pad, r0, nc, xc, accE,
-                      accO);
-            const int row = r0 + rg * 4 + rr;
-            int j = -1;
-            if (row < B.h) {
-              const int jn = lo + row, mirror = q - 1 - jn;
-              if (side == 0 || mirror != jn) j = side ? mirror : jn;
-            }
+            double accE[4][8], accO[4][8];
+            gemm_tile(sm, ge, go, ldr, r0, nc, xc, accE, accO);
             for (int blk = 0; blk < n_blk; ++blk) {
-              if (kDeriv)
-                chunk_elements_d<false>(sm, accE, accO, half, blk, a.n_theta, v);
-              else if (kMode == 2 && blk == 1)
-                chunk_errors<false>(sm, accE, accO, v);
-              else
-                chunk_elements<false>(sm, accE, accO, v);
+              if (user) {
+                if (kDeriv)
+                  chunk_elements_d<true>(sm, accE, accO, half, blk, a.n_theta, v);
+                else if (kMode == 2 && blk == 1)
+                  chunk_errors<true>(sm, accE, accO, v);
+                else
+                  chunk_elements<true>(sm, accE, accO, v);
+              } else {
+                if (kDeriv)
+                  chunk_elements_d<false>(sm, accE, accO, half, blk, a.n_theta, v);
+                else if (kMode == 2 && blk == 1)
+                  chunk_errors<false>(sm, accE, accO, v);
+                else
+                  chunk_elements<false>(sm, accE, accO, v);
+              }
               if (j >= 0) {
-                double* ab = acc_band + (int64_t)blk * 4 * q;
-                ab[e0 * q + j] += v[0];
-                ab[(e0 + 1) * q + j] += v[1];
+                double* ab = base + (int64_t)blk * 4 * len;
+                ab[o_e0 * len + j] += v[0];
+                ab[(o_e0 + 1) * len + j] += v[1];
               }
             }
           }
@@ -410,7 +566,7 @@ __device__ __forceinline__ void unit_body(const UnitArgs& a) {
 // reduced tiles into the unit's accumulators. Every output sum is owned by one thread of one
 // work item and runs over the chunks in order, so the results do not depend on how a unit's
 // tiles are split into work items.
-__global__ void __launch_bounds__(NT) unit_kernel(UnitArgs a) { unit_body<0>(a); }
+__global__ void __launch_bounds__(NT, 3) unit_kernel(UnitArgs a) { unit_body<0>(a); }
 
 // The same with the derivative blocks: per chunk, its two 16-node halves in order; per tile,
 // every block's sums (values, distribution parameters, Re m, Im m), each into its own
