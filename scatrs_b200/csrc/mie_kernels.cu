@@ -45,7 +45,7 @@ __global__ void plan_chunks_kernel(PlanArgs a) {
   if (lane == 0) a.chunk_n[warp] = nn;
 }
 
-template <bool kLayered>
+template <bool kLayered, bool kAdaptive>
 __device__ __forceinline__ void mie_chunk(const MieFixedArgs& a) {
   int wslot = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   int lane = threadIdx.x & 31;
@@ -65,7 +65,7 @@ __device__ __forceinline__ void mie_chunk(const MieFixedArgs& a) {
   s.ux = a.ux + (row0 + 2 * (int64_t)chunk) * 32 + lane;
   s.stride = 32;
   double q[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  double qe[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // adaptive: weighted by w_K - w_G
+  double qe[kAdaptive ? 8 : 1] = {};  // adaptive: weighted by w_K - w_G
   int64_t n = 0;
   const int64_t node = (a.per_unit ? unit : d) * a.n_nodes + j;
   if (j < a.n_nodes && a.radius[node] > 0.0) {
@@ -127,7 +127,7 @@ __device__ __forceinline__ void mie_chunk(const MieFixedArgs& a) {
       const double qv[8] = {1.0,           area * e.q_ext, area * e.q_sca, area * e.q_sca * e.g,
                             area * e.q_abs, area * e.q_back, r * r,         r * r * r};
       for (int k = 0; k < 8; ++k) q[k] = w * qv[k];
-      if (a.wdiff) {
+      if constexpr (kAdaptive) {
         const double wd = a.wdiff[node];
         for (int k = 0; k < 8; ++k) qe[k] = wd * qv[k];
       }
@@ -137,13 +137,13 @@ __device__ __forceinline__ void mie_chunk(const MieFixedArgs& a) {
   for (int64_t k = n + 1; k <= nc; ++k)
     *reinterpret_cast<double4*>(X + (k - 1) * 128) = make_double4(0.0, 0.0, 0.0, 0.0);
   // The chunk's weighted sums, in a fixed tree order.
-  const int stride = a.wdiff ? 16 : 8;
+  const int stride = kAdaptive ? 16 : 8;
   for (int k = 0; k < 8; ++k) {
     double v = q[k];
     for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
     if (lane == 0) a.chunk_sums[(int64_t)chunk * stride + k] = v;
   }
-  if (a.wdiff) {
+  if constexpr (kAdaptive) {
     // |Kronrod - Gauss| of each of the chunk's two panels (lanes 0-15, 16-31), then added.
     for (int k = 0; k < 8; ++k) {
       double v = qe[k];
@@ -253,13 +253,22 @@ __device__ __forceinline__ void mie_chunk_deriv(const MieFixedArgs& a) {
 }
 
 // Homogeneous spheres.
-__global__ void __launch_bounds__(128) mie_fixed_kernel(MieFixedArgs a) { mie_chunk<false>(a); }
+__global__ void __launch_bounds__(128) mie_fixed_kernel(MieFixedArgs a) {
+  mie_chunk<false, false>(a);
+}
+
+// Homogeneous spheres on adaptive panels (with the chunk's |Kronrod - Gauss| sums).
+__global__ void __launch_bounds__(128) mie_adaptive_kernel(MieFixedArgs a) {
+  mie_chunk<false, true>(a);
+}
 
 // Homogeneous spheres with derivatives.
 __global__ void __launch_bounds__(128) mie_deriv_kernel(MieFixedArgs a) { mie_chunk_deriv(a); }
 
 // Layered spheres (their per-layer state lives in local memory).
-__global__ void __launch_bounds__(128) mie_layered_kernel(MieFixedArgs a) { mie_chunk<true>(a); }
+__global__ void __launch_bounds__(128) mie_layered_kernel(MieFixedArgs a) {
+  mie_chunk<true, false>(a);
+}
 
 // Independent spheres, one per thread (the batched Mie::compute): coefficients a_1..a_N then
 // b_1..b_N per sphere, and the efficiencies.
@@ -357,6 +366,8 @@ void launch_mie_fixed(const MieFixedArgs& a, cudaStream_t s) {
     mie_deriv_kernel<<<blocks, threads, 0, s>>>(a);
   else if (a.n_layers > 1)
     mie_layered_kernel<<<blocks, threads, 0, s>>>(a);
+  else if (a.wdiff)
+    mie_adaptive_kernel<<<blocks, threads, 0, s>>>(a);
   else
     mie_fixed_kernel<<<blocks, threads, 0, s>>>(a);
 }
