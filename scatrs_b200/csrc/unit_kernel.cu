@@ -79,8 +79,9 @@ __device__ __forceinline__ void load_stage(Smem& sm, int st, const double* __res
                                            const double* __restrict__ go, int ldr, int r0,
                                            int k0, int nc, const double* __restrict__ xc) {
   const int t = threadIdx.x;
-  {
-    const int kk = t >> 4, c = t & 15;
+#pragma unroll
+  for (int i = t; i < KB * 16; i += NT) {
+    const int kk = i >> 4, c = i & 15;
     if (k0 + kk < nc) {
       const int64_t off = (int64_t)(k0 + kk) * ldr + r0 + 2 * c;
       cp_async16(&sm.a[st][0][kk][2 * c], ge + off);
@@ -88,9 +89,8 @@ __device__ __forceinline__ void load_stage(Smem& sm, int st, const double* __res
     }
   }
 #pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    const int idx = t + q * NT;
-    const int kk = idx >> 6, c = idx & 63;
+  for (int i = t; i < KB * 64; i += NT) {
+    const int kk = i >> 6, c = i & 63;
     if (k0 + kk < nc) cp_async16(&sm.xs[st][kk][2 * c], xc + (int64_t)(k0 + kk) * 128 + 2 * c);
   }
   cp_commit();
@@ -107,17 +107,17 @@ __device__ __forceinline__ void load_stage_z(Smem& sm, int st, const double* __r
                                              const double* __restrict__ go, int ldr, int r0,
                                              int k0, int nc, const double* __restrict__ xc) {
   const int t = threadIdx.x;
-  {
-    const int kk = t >> 4, c = t & 15;
+#pragma unroll
+  for (int i = t; i < KB * 16; i += NT) {
+    const int kk = i >> 4, c = i & 15;
     const bool valid = k0 + kk < nc;
     const int64_t off = valid ? (int64_t)(k0 + kk) * ldr + r0 + 2 * c : 0;
     cp_async16_zfill(&sm.a[st][0][kk][2 * c], ge + off, valid);
     cp_async16_zfill(&sm.a[st][1][kk][2 * c], go + off, valid);
   }
 #pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    const int idx = t + q * NT;
-    const int kk = idx >> 6, c = idx & 63;
+  for (int i = t; i < KB * 64; i += NT) {
+    const int kk = i >> 6, c = i & 63;
     const bool valid = k0 + kk < nc;
     cp_async16_zfill(&sm.xs[st][kk][2 * c], xc + (valid ? (int64_t)(k0 + kk) * 128 + 2 * c : 0),
                      valid);
@@ -260,7 +260,7 @@ __device__ __forceinline__ void gemm_tile(Smem& sm, const double* __restrict__ g
     __syncthreads();
     if (k0 + KB < nc) load_stage(sm, st ^ 1, ge, go, ldr, r0, k0 + KB, nc, xc);
     const int kend = nc - k0 < KB ? nc - k0 : KB;
-#pragma unroll
+#pragma unroll 8
     for (int kk = 0; kk < KB; ++kk) {
       if (kk < kend) {
         const double2 e01 = *reinterpret_cast<const double2*>(&sm.a[st][0][kk][rg * 4]);
@@ -437,7 +437,8 @@ __device__ __forceinline__ void chunk_errors(const Smem& sm, const double accE[4
 template <int kMode>
 __device__ __forceinline__ void unit_body(const UnitArgs& a) {
   constexpr bool kDeriv = kMode == 1;
-  __shared__ __align__(16) Smem sm;
+  extern __shared__ __align__(16) unsigned char unit_raw[];
+  Smem& sm = *reinterpret_cast<Smem*>(unit_raw);
   const int t = threadIdx.x, rg = t >> 4, ng = t & 15;
   // This thread's share of a reduced tile: side (+mu, -mu), row, two elements.
   const int side = ng >> 3, rr = (ng >> 1) & 3, e0 = 2 * (ng & 1);
@@ -1088,19 +1089,34 @@ void launch_mix(const MixArgs& a, cudaStream_t s) {
   if (grid > 0) mix_assemble_kernel<<<grid, NT, 0, s>>>(a);
 }
 
+// The unit kernels' stage buffers are dynamic shared memory (above the 48 KB static limit);
+// the attribute is per device: set it once on each.
+static void configure_units() {
+  static bool configured[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev >= 0 && dev < 64 && !configured[dev]) {
+    for (auto f : {unit_kernel, unit_deriv_kernel, unit_adaptive_kernel})
+      cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Smem));
+    configured[dev] = true;
+  }
+}
+
 int unit_kernel_blocks_per_sm() {
+  configure_units();
   int n = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, unit_kernel, NT, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, unit_kernel, NT, sizeof(Smem));
   return n > 0 ? n : 1;
 }
 
 void launch_units(const UnitArgs& a, int grid, cudaStream_t s) {
+  configure_units();
   if (a.deriv)
-    unit_deriv_kernel<<<grid, NT, 0, s>>>(a);
+    unit_deriv_kernel<<<grid, NT, sizeof(Smem), s>>>(a);
   else if (a.wdiff)
-    unit_adaptive_kernel<<<grid, NT, 0, s>>>(a);
+    unit_adaptive_kernel<<<grid, NT, sizeof(Smem), s>>>(a);
   else
-    unit_kernel<<<grid, NT, 0, s>>>(a);
+    unit_kernel<<<grid, NT, sizeof(Smem), s>>>(a);
 }
 
 void launch_proj(const ProjArgs& a, cudaStream_t s) {
