@@ -29,6 +29,10 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+# DRAM bytes per node of the unit kernel: (805.47 MB read + 27.56 MB written) / 313,344 nodes in
+# one ncu capture of the 0.1-scale batched workload (the traffic grows with the nodes).
+UNIT_DRAM_BYTES_PER_NODE = (805.469952e6 + 27.562752e6) / 313344
+
 METRIC = "Mie ensemble nodes/s on 1 B200, batched vs plain FP64, at 1e-10 rel err vs FP64"
 UNIT = "nodes/s"
 
@@ -371,7 +375,11 @@ def ours(args):
                      "peak": fp64, "unit": "TFLOP/s", "frac": achieved / fp64,
                      "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (no FP64 entry "
                                     "in MEASURED_PEAKS.json)",
-                     "traffic": None, "launches": unit_n, "avg_launch_ms": unit_ms / max(unit_n, 1),
+                     "traffic": UNIT_DRAM_BYTES_PER_NODE * w.n_nodes_total / max(unit_n, 1),
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
+                                       "launch on the 0.1-scale workload, scaled by nodes per "
+                                       "launch (profiles/unit_kernel_config2_scale0.1.md)",
+                     "launches": unit_n, "avg_launch_ms": unit_ms / max(unit_n, 1),
                      "algorithmic_flop_per_step": flops},
         "kernels_ms_per_step": {k: v[0] for k, v in kt.items()},
         "kernel_share": {k: (v[0] / total_k if total_k else None) for k, v in kt.items()},
