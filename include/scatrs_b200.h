@@ -173,6 +173,21 @@ int scatrs_ensemble_mixture(const scatrs_component* components, int64_t n_comp,
                             double* greek_err, int8_t* converged, int64_t* panels, char* err,
                             size_t err_len);
 
+/*
+ * The Greek coefficients of phase matrices tabulated at the n_q Gauss-Legendre cosines
+ * (ascending, the rule of scatrs_gauss_legendre), projected with the reference's projector
+ * (2l+1)/2 w_k d_l(mu_k) (scatrs/src/mie/greek.rs:131-335; the band projection of
+ * scatrs/src/ensemble/fast.rs:210-271 on one rule): exact for tables of polynomial degree up to
+ * 2 n_q - 1 - order. phase_dev [6][n_units][n_q] as scatrs_ensemble_fixed_device writes it
+ * (F11, F12, F22, F33, F34, F44), greek_dev [6][n_units][order + 1]; DEVICE pointers, enqueued
+ * on `stream`. precision 0: FP64; 1: 3xTF32 on the tensor cores (each operand a TF32 head and
+ * tail, FP32 accumulation: about 1e-6 of the largest coefficient). Returns after the FP64 form
+ * is enqueued, or after the tensor-core form completed (it checks its pipeline).
+ */
+int scatrs_project_greek_device(const double* phase_dev, int64_t n_units, int64_t n_q,
+                                int32_t order, int32_t precision, double* greek_dev,
+                                void* stream, char* err, size_t err_len);
+
 /* Layered spheres (scatrs/src/layered/mod.rs; Particle::LayeredSphere,
  * scatrs/src/ensemble/mod.rs:58-65): n_layers layers, the core first; per distribution the
  * n_layers - 1 outer radii of layers 0..L-2 as fractions of the particle's radius (nondecreasing

@@ -71,6 +71,8 @@ SYMBOLS = {
     "scatrs_ensemble_mixture": (ctypes.c_int, [ctypes.POINTER(Component), _I64, _PD, _I64, _PD,
                                                _I64, ctypes.POINTER(AdaptiveOptions), _PD, _PD,
                                                _PD, _PD, _PD, _PD, _VP, _VP, _CP, _SZ]),
+    "scatrs_project_greek_device": (ctypes.c_int, [_VP, _I64, _I64, _I32, _I32, _VP, _VP, _CP,
+                                                   _SZ]),
     "scatrs_check_errors": (ctypes.c_int, [_VP, _CP, _SZ]),
     "scatrs_mie": (ctypes.c_int, [_PD, _PD, _I64, _I32, _PI64, _PI64, _PD, _PD, _CP, _SZ]),
     "scatrs_mie_static": (ctypes.c_int, [_VP, _VP, _I64, _I32, _I64, _VP, _VP, _VP, _VP, _VP,
@@ -349,6 +351,16 @@ def ensemble_fixed_device(dists: np.ndarray, wl_ptr: int, n_wl: int, m_ptr: int,
                                              phase_ptr or None, greek_ptr or None, stream or None,
                                              err, 1024)
     _check(st, err)
+
+
+def project_greek_device(phase_ptr: int, n_units: int, n_q: int, order: int, precision: int,
+                         greek_ptr: int, stream: int = 0) -> None:
+    """Greek coefficients of device tables at the n_q Gauss cosines (raw device pointers):
+    precision 0 FP64, 1 3xTF32 on the tensor cores."""
+    err = ctypes.create_string_buffer(1024)
+    _check(load().scatrs_project_greek_device(phase_ptr, int(n_units), int(n_q), int(order),
+                                              int(precision), greek_ptr, stream or None, err,
+                                              1024), err)
 
 
 def check_errors(stream: int = 0) -> None:

@@ -7,7 +7,9 @@
 //      picks the projector bands, grows the tables if needed, and cuts the units into slabs
 //      whose coefficient rows fit the arena;
 //   3. per slab, K-a (one warp per chunk) then the unit kernel (one persistent CTA per SM slot).
+#include <cuda.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <atomic>
@@ -146,6 +148,13 @@ struct Context {
   // Pass 1 of the adaptive ensemble.
   DevBuf p1_radius, p1_wl, p1_wlu, p1_scratch, p1_uz, p1_ux, p1_q, p1_n, p1_status;
   DevBuf avg, mix_first, mix_part, mix_frac;
+  // The Greek projection of tables at Gauss cosines: per (n_q, L) the matrices (FP64 and their
+  // TF32 heads and tails), and the workspaces of the tensor-core form.
+  struct Projector {
+    DevBuf d, d_hi, d_lo;
+  };
+  std::map<std::pair<int64_t, int>, Projector> projectors;
+  DevBuf tc_a_hi, tc_a_lo, tc_prod, tc_err;
   std::vector<int> chunk_n_host;
   int* pinned_chunk_n = nullptr;
   size_t pinned_cap = 0;
@@ -1338,6 +1347,67 @@ void adaptive_call(const std::vector<AdPart>& in, int n_out, bool batch, const d
     }
 }
 
+// The driver's tensor-map encoder, found once through the runtime.
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    cudaDriverEntryPointQueryResult q;
+    void* p = nullptr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  if (!fn) throw Failure{SCATRS_CUDA, "cuTensorMapEncodeTiled is not available"};
+  return fn;
+}
+
+// A 2-D FP32 tensor map over rows of n_q_pad values, boxes of 32 x box_rows, 128-byte swizzle,
+// zero fill outside.
+CUtensorMap tensor_map_2d(float* base, int64_t n_q_pad, int64_t rows, int box_rows) {
+  CUtensorMap m;
+  const cuuint64_t dims[2] = {(cuuint64_t)n_q_pad, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)n_q_pad * 4};
+  const cuuint32_t box[2] = {32, (cuuint32_t)box_rows};
+  const cuuint32_t estr[2] = {1, 1};
+  CUresult r = tensor_map_encoder()(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims, strides,
+                                    box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                    CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS)
+    throw Failure{SCATRS_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")"};
+  return m;
+}
+
+// The projection matrices (2l+1)/2 w_k d_l(mu_k) of d00, d22, d2-2, d02 ([4][n_q][L + 1]) on the
+// n_q-point Gauss rule (greek.rs:131-335), and their TF32 heads and tails transposed.
+Context::Projector& projector(Context& c, int64_t n_q, int L, cudaStream_t s) {
+  auto key = std::make_pair(n_q, L);
+  auto it = c.projectors.find(key);
+  if (it != c.projectors.end()) return it->second;
+  Context::Projector& p = c.projectors[key];
+  const auto& r = rule(c, n_q);
+  const int64_t len = L + 1;
+  std::vector<double> d(4 * (size_t)n_q * len), buf(len);
+  const int mn[4][2] = {{0, 0}, {2, 2}, {2, -2}, {0, 2}};
+  for (int f = 0; f < 4; ++f)
+    for (int64_t k = 0; k < n_q; ++k) {
+      wigner_d(mn[f][0], mn[f][1], r.first[k], buf.data(), len);
+      for (int64_t l = 0; l < len; ++l)
+        d[((size_t)f * n_q + k) * len + l] = (double)(2 * l + 1) * 0.5 * r.second[k] * buf[l];
+    }
+  double* dd = p.d.as<double>(d.size());
+  SB_CUDA(cudaMemcpyAsync(dd, d.data(), d.size() * 8, cudaMemcpyHostToDevice, s));
+  const int64_t n_q_pad = round_up(n_q, 4);
+  float* hi = p.d_hi.as<float>(4 * (size_t)len * n_q_pad);
+  float* lo = p.d_lo.as<float>(4 * (size_t)len * n_q_pad);
+  launch_greek_split_d(dd, (int)n_q, (int)n_q_pad, (int)len, hi, lo, s);
+  SB_CUDA(cudaGetLastError());
+  SB_CUDA(cudaStreamSynchronize(s));
+  return p;
+}
+
 FixedCall g_last_call;  // for scatrs_check_errors
 
 template <class F>
@@ -1518,6 +1588,55 @@ int scatrs_ensemble_mixture(const scatrs_component* components, int64_t n_comp,
     }
     AdOutputs out{values, errors, phase, phase_err, greek, greek_err, converged, panels};
     adaptive_call(parts, 1, false, wavelengths, n_wl, mu, n_mu, options, out);
+  });
+}
+
+int scatrs_project_greek_device(const double* phase_dev, int64_t n_units, int64_t n_q,
+                                int32_t order, int32_t precision, double* greek_dev,
+                                void* stream, char* err, size_t err_len) {
+  return guarded(err, err_len, [&] {
+    if (n_units < 0 || n_q < 1 || order < 0 || order > (1 << 21))
+      throw Failure{SCATRS_INVALID_INPUT, "needs n_units >= 0, n_q >= 1 and 0 <= order"};
+    if (precision != 0 && precision != 1)
+      throw Failure{SCATRS_INVALID_INPUT, "precision must be 0 (FP64) or 1 (3xTF32)"};
+    if (n_units == 0) return;
+    Context& c = context();
+    std::lock_guard<std::mutex> lk(c.mtx);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    Context::Projector& p = projector(c, n_q, order, s);
+    const int len = order + 1;
+    if (precision == 0) {
+      timed_launch(K_PROJ, s, [&] {
+        launch_greek_fp64(phase_dev, n_units, (int)n_q, len, p.d.as<double>(0), greek_dev, s);
+      });
+      SB_CUDA(cudaGetLastError());
+      return;
+    }
+    if (n_units > (int64_t)INT32_MAX / 6)
+      throw Failure{SCATRS_INVALID_INPUT, "too many tables for one tensor-core projection"};
+    const int64_t n_q_pad = round_up(n_q, 4);
+    float* a_hi = c.tc_a_hi.as<float>(6 * (size_t)n_units * n_q_pad);
+    float* a_lo = c.tc_a_lo.as<float>(6 * (size_t)n_units * n_q_pad);
+    float* prod = c.tc_prod.as<float>(6 * (size_t)n_units * len);
+    unsigned* flag = c.tc_err.as<unsigned>(1);
+    SB_CUDA(cudaMemsetAsync(flag, 0, sizeof(unsigned), s));
+    launch_greek_split(phase_dev, n_units, (int)n_q, (int)n_q_pad, a_hi, a_lo, s);
+    SB_CUDA(cudaGetLastError());
+    const CUtensorMap maps[4] = {
+        tensor_map_2d(a_hi, n_q_pad, 6 * n_units, 128), tensor_map_2d(a_lo, n_q_pad, 6 * n_units, 128),
+        tensor_map_2d(p.d_hi.as<float>(0), n_q_pad, 4 * (int64_t)len, 256),
+        tensor_map_2d(p.d_lo.as<float>(0), n_q_pad, 4 * (int64_t)len, 256)};
+    TcArgs ta{(int)n_units, (int)n_q_pad, len, prod, flag};
+    cudaError_t e = cudaSuccess;
+    timed_launch(K_PROJ, s, [&] { e = launch_greek_tc(maps, ta, s); });
+    if (e != cudaSuccess)
+      throw Failure{SCATRS_CUDA, std::string("greek_tc_kernel: ") + cudaGetErrorString(e)};
+    launch_greek_assemble(prod, n_units, len, greek_dev, s);
+    SB_CUDA(cudaGetLastError());
+    unsigned h = 0;
+    SB_CUDA(cudaMemcpyAsync(&h, flag, sizeof h, cudaMemcpyDeviceToHost, s));
+    SB_CUDA(cudaStreamSynchronize(s));
+    if (h) throw Failure{SCATRS_CUDA, "the tensor-core projection's pipeline timed out"};
   });
 }
 

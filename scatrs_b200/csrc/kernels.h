@@ -239,6 +239,26 @@ void launch_units(const UnitArgs& a, int grid, cudaStream_t s);
 void launch_proj(const ProjArgs& a, cudaStream_t s);
 void launch_final(const FinalArgs& a, cudaStream_t s);
 void launch_pass1(const Pass1Args& a, cudaStream_t s);
+
+// The Greek projection of tables at Gauss cosines (greek_tc.cu): the 3xTF32 tensor-core GEMM's
+// arguments (products [6][n_units][len] in FP32, an error word for its bounded waits).
+struct TcArgs {
+  int n_units;
+  int n_q_pad;
+  int len;
+  float* out;
+  unsigned* err;
+};
+size_t greek_tc_smem();
+void launch_greek_split(const double* phase, int64_t n_units, int n_q, int n_q_pad, float* hi,
+                        float* lo, cudaStream_t s);
+void launch_greek_split_d(const double* d, int n_q, int n_q_pad, int len, float* hi, float* lo,
+                          cudaStream_t s);
+cudaError_t launch_greek_tc(const struct CUtensorMap_st* maps, const TcArgs& a, cudaStream_t s);
+void launch_greek_assemble(const float* prod, int64_t n_units, int len, double* greek,
+                           cudaStream_t s);
+void launch_greek_fp64(const double* phase, int64_t n_units, int n_q, int len, const double* d,
+                       double* greek, cudaStream_t s);
 void launch_mix(const MixArgs& a, cudaStream_t s);
 
 }  // namespace sb

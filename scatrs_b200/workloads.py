@@ -100,6 +100,41 @@ def config2(seed: int = 0, scale: float = 1.0, mu: np.ndarray | None = None) -> 
                     512, 64)
 
 
+def gammas(r_eff, v_eff) -> np.ndarray:
+    """Gamma distributions on grids wide enough for their tails: [max(0.01, 1 - 8 sqrt(b)) a,
+    (1 + 12 sqrt(b)) a] for effective radius a and variance b."""
+    a = np.atleast_1d(np.asarray(r_eff, dtype=np.float64))
+    b = np.broadcast_to(np.asarray(v_eff, dtype=np.float64), a.shape)
+    d = np.zeros(a.size, dtype=DIST_DTYPE)
+    d["kind"] = KINDS["gamma"]
+    d["param"][:, 0] = a
+    d["param"][:, 1] = b
+    d["r_lo"] = a * np.maximum(0.01, 1.0 - 8.0 * np.sqrt(b))
+    d["r_hi"] = a * (1.0 + 12.0 * np.sqrt(b))
+    return d
+
+
+def config3(seed: int = 0, scale: float = 1.0, n_q: int = 4096) -> Workload:
+    """Large droplets: 128 gamma distributions (effective radius uniform 5-20, effective
+    variance uniform 0.05-0.2) x 256 wavelengths log-spaced over 0.4-2.2, m = 1.33 + k i with k
+    log-uniform 1e-9-1e-3 per (distribution, wavelength), 256 nodes in ln r, the phase matrix at
+    n_q = 4096 Gauss cosines, Greek order 1024 (projected from those tables). ``scale`` keeps the
+    first fraction of the distributions and wavelengths."""
+    rng = np.random.default_rng(seed)
+    n_dist, n_wl = 128, 256
+    wl = np.geomspace(0.4, 2.2, n_wl)
+    a = rng.uniform(5.0, 20.0, n_dist)
+    b = rng.uniform(0.05, 0.2, n_dist)
+    k = np.exp(rng.uniform(np.log(1e-9), np.log(1e-3), (n_dist, n_wl)))
+    m = 1.33 + 1j * k
+    if scale < 1.0:
+        kd = max(1, int(round(n_dist * scale)))
+        kw = max(1, int(round(n_wl * scale)))
+        a, b, m, wl = a[:kd], b[:kd], m[:kd, :kw], wl[:kw]
+    return Workload(f"config3(seed={seed},scale={scale})", gammas(a, b), wl, m,
+                    gauss_legendre(n_q), 256, 1024)
+
+
 def config4(seed: int = 0, scale: float = 1.0, mu: np.ndarray | None = None) -> LayeredWorkload:
     """Three-layer spheres (a core and two shells): core fraction uniform 0.3-0.9, inner shell
     boundary uniform 0.9-0.99; each layer's index Re uniform 1.3-2.0, Im log-uniform 1e-6-0.5
