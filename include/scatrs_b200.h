@@ -181,7 +181,8 @@ int scatrs_ensemble_mixture(const scatrs_component* components, int64_t n_comp,
  * 2 n_q - 1 - order. phase_dev [6][n_units][n_q] as scatrs_ensemble_fixed_device writes it
  * (F11, F12, F22, F33, F34, F44), greek_dev [6][n_units][order + 1]; DEVICE pointers, enqueued
  * on `stream`. precision 0: FP64; 1: 3xTF32 on the tensor cores (each operand a TF32 head and
- * tail, FP32 accumulation: about 1e-6 of the largest coefficient). Returns after the FP64 form
+ * tail, FP32 accumulation over the cosines: about 1e-5 of the largest coefficient at order
+ * 1000 and 4096 cosines, less at lower orders). Returns after the FP64 form
  * is enqueued, or after the tensor-core form completed (it checks its pipeline).
  */
 int scatrs_project_greek_device(const double* phase_dev, int64_t n_units, int64_t n_q,
