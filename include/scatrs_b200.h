@@ -189,6 +189,28 @@ int scatrs_project_greek_device(const double* phase_dev, int64_t n_units, int64_
                                 int32_t order, int32_t precision, double* greek_dev,
                                 void* stream, char* err, size_t err_len);
 
+/*
+ * Spheroids by the extended boundary condition method (scatrs/src/tmatrix; Shape::Spheroid,
+ * aspect ratio eps = a/c > 1 oblate; x the equal-volume sphere's size parameter; m complex128).
+ *
+ * scatrs_spheroid_tmatrix: the T-matrix of azimuthal mode `mode` at truncation n_terms and
+ * n_theta Gauss nodes in 0 < theta < pi/2 (TMatrix::compute with fixed N and n_theta,
+ * tmatrix/mod.rs:221-362, kernel.rs:516-563): t[2 (2K)^2], row-major complex (2K)^2 with
+ * K = n_terms - max(mode, 1) + 1 and blocks [T11 T12; T21 T22].
+ *
+ * scatrs_spheroid_efficiencies: the orientation-averaged Q_ext, Q_sca, Q_abs of n spheroids
+ * (q[3 n]), converged in N and n_theta to rtol as driver.rs:343-420 converges them on mode 0,
+ * then every mode at the final N (n_terms[n], n_theta[n] the values used; either may be NULL).
+ * Status 2 when N reaches its cap. The FP64 formulation is the classical one; see the accuracy
+ * limits stated with the library.
+ */
+int scatrs_spheroid_tmatrix(double x, double aspect_ratio, const double* m, int32_t mode,
+                            int32_t n_terms, int32_t n_theta, double* t, char* err,
+                            size_t err_len);
+int scatrs_spheroid_efficiencies(int64_t n, const double* x, const double* aspect_ratio,
+                                 const double* m, double rtol, double* q, int32_t* n_terms,
+                                 int32_t* n_theta, char* err, size_t err_len);
+
 /* Layered spheres (scatrs/src/layered/mod.rs; Particle::LayeredSphere,
  * scatrs/src/ensemble/mod.rs:58-65): n_layers layers, the core first; per distribution the
  * n_layers - 1 outer radii of layers 0..L-2 as fractions of the particle's radius (nondecreasing

@@ -373,3 +373,39 @@ def ensemble_mixture(components, wavelengths, mu=None, greek_order=None, normali
     if g is not None:
         out["greek"], out["greek_err"] = g, ge
     return out
+
+
+def tmatrix_mode(x: float, eps: float, s: complex, m: int, n: int, n_theta: int) -> np.ndarray:
+    """One azimuthal mode's T-matrix of a spheroid (2K x 2K complex, K = n - max(m, 1) + 1)."""
+    k = n - max(m, 1) + 1
+    t = np.zeros(2 * (2 * k) ** 2)
+    f = lib().orc_tmatrix_mode
+    f.argtypes = [_D, _D, _D, _D, ctypes.c_int, ctypes.c_int, ctypes.c_int, _PD]
+    st = f(x, eps, s.real, s.imag, m, n, n_theta, _p(t))
+    if st != 0:
+        raise OracleError(st, "tmatrix_mode")
+    return t.view(np.complex128).reshape(2 * k, 2 * k)
+
+
+def spheroid_q(x: float, eps: float, s: complex, n: int, n_theta: int):
+    """Orientation-averaged (Q_ext, Q_sca) of a spheroid at truncation n and n_theta nodes."""
+    q = np.zeros(2)
+    f = lib().orc_spheroid_q
+    f.argtypes = [_D, _D, _D, _D, ctypes.c_int, ctypes.c_int, _PD]
+    st = f(x, eps, s.real, s.imag, n, n_theta, _p(q))
+    if st != 0:
+        raise OracleError(st, "spheroid_q")
+    return q[0], q[1]
+
+
+def spheroid_converged(x: float, eps: float, s: complex, rtol: float = 1e-8):
+    """Converged orientation-averaged (Q_ext, Q_sca, Q_abs), N and n_theta of a spheroid."""
+    q = np.zeros(3)
+    n, nth = ctypes.c_int(0), ctypes.c_int(0)
+    f = lib().orc_spheroid_converged
+    f.argtypes = [_D, _D, _D, _D, _D, _PD, ctypes.POINTER(ctypes.c_int),
+                  ctypes.POINTER(ctypes.c_int)]
+    st = f(x, eps, s.real, s.imag, rtol, _p(q), ctypes.byref(n), ctypes.byref(nth))
+    if st != 0:
+        raise OracleError(st, "spheroid_converged")
+    return q, n.value, nth.value

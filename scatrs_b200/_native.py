@@ -73,6 +73,9 @@ SYMBOLS = {
                                                _PD, _PD, _PD, _PD, _VP, _VP, _CP, _SZ]),
     "scatrs_project_greek_device": (ctypes.c_int, [_VP, _I64, _I64, _I32, _I32, _VP, _VP, _CP,
                                                    _SZ]),
+    "scatrs_spheroid_tmatrix": (ctypes.c_int, [_D, _D, _PD, _I32, _I32, _I32, _PD, _CP, _SZ]),
+    "scatrs_spheroid_efficiencies": (ctypes.c_int, [_I64, _PD, _PD, _PD, _D, _PD, _VP, _VP, _CP,
+                                                    _SZ]),
     "scatrs_check_errors": (ctypes.c_int, [_VP, _CP, _SZ]),
     "scatrs_mie": (ctypes.c_int, [_PD, _PD, _I64, _I32, _PI64, _PI64, _PD, _PD, _CP, _SZ]),
     "scatrs_mie_static": (ctypes.c_int, [_VP, _VP, _I64, _I32, _I64, _VP, _VP, _VP, _VP, _VP,
@@ -361,6 +364,36 @@ def project_greek_device(phase_ptr: int, n_units: int, n_q: int, order: int, pre
     _check(load().scatrs_project_greek_device(phase_ptr, int(n_units), int(n_q), int(order),
                                               int(precision), greek_ptr, stream or None, err,
                                               1024), err)
+
+
+def spheroid_tmatrix(x: float, aspect_ratio: float, m: complex, mode: int, n_terms: int,
+                     n_theta: int) -> np.ndarray:
+    """The T-matrix of one azimuthal mode of a spheroid: (2K, 2K) complex."""
+    require_device()
+    k = n_terms - max(mode, 1) + 1
+    t = np.zeros(2 * (2 * k) ** 2)
+    mm = np.array([complex(m).real, complex(m).imag])
+    err = ctypes.create_string_buffer(1024)
+    _check(load().scatrs_spheroid_tmatrix(float(x), float(aspect_ratio), _p(mm), int(mode),
+                                          int(n_terms), int(n_theta), _p(t), err, 1024), err)
+    return t.view(np.complex128).reshape(2 * k, 2 * k)
+
+
+def spheroid_efficiencies(x, aspect_ratio, m, rtol: float = 1e-8):
+    """Orientation-averaged (Q_ext, Q_sca, Q_abs) of spheroids ((n, 3)), with the N and n_theta
+    each converged at."""
+    require_device()
+    x = np.ascontiguousarray(np.atleast_1d(x), dtype=np.float64)
+    eps = np.ascontiguousarray(np.broadcast_to(np.asarray(aspect_ratio, dtype=np.float64), x.shape))
+    mm = np.ascontiguousarray(np.broadcast_to(np.asarray(m, dtype=np.complex128), x.shape))
+    q = np.zeros((x.size, 3))
+    n_terms = np.zeros(x.size, dtype=np.int32)
+    n_theta = np.zeros(x.size, dtype=np.int32)
+    err = ctypes.create_string_buffer(1024)
+    _check(load().scatrs_spheroid_efficiencies(x.size, _p(x), _p(eps), _p(mm.view(np.float64)),
+                                               float(rtol), _p(q), n_terms.ctypes.data,
+                                               n_theta.ctypes.data, err, 1024), err)
+    return q, n_terms, n_theta
 
 
 def check_errors(stream: int = 0) -> None:

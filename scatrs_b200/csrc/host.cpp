@@ -155,6 +155,8 @@ struct Context {
   };
   std::map<std::pair<int64_t, int>, Projector> projectors;
   DevBuf tc_a_hi, tc_a_lo, tc_prod, tc_err;
+  // Spheroid T-matrices.
+  DevBuf tm_jobs, tm_rules_x, tm_rules_w, tm_node, tm_fun, tm_J, tm_work, tm_T, tm_sums, tm_err;
   std::vector<int> chunk_n_host;
   int* pinned_chunk_n = nullptr;
   size_t pinned_cap = 0;
@@ -1408,6 +1410,134 @@ Context::Projector& projector(Context& c, int64_t n_q, int L, cudaStream_t s) {
   return p;
 }
 
+// ---------------------------------------------------------------------------------------
+// Spheroid T-matrices (tmatrix.cu) and the convergence in N and n_theta (driver.rs).
+// ---------------------------------------------------------------------------------------
+struct TmSpec {
+  double x, eps, s_re, s_im;
+  int m, N, n_theta;
+};
+
+void check_tm_spec(const TmSpec& t) {
+  if (!(std::isfinite(t.x) && t.x > 0.0 && t.x <= 1e4))
+    throw Failure{SCATRS_INVALID_INPUT, "the size parameter must be finite and in (0, 1e4]"};
+  if (!(std::isfinite(t.eps) && t.eps > 0.0))
+    throw Failure{SCATRS_INVALID_INPUT, "the aspect ratio must be finite and > 0"};
+  if (!(std::isfinite(t.s_re) && std::isfinite(t.s_im) && t.s_re > 0.0 && t.s_im >= 0.0))
+    throw Failure{SCATRS_INVALID_INPUT, "the refractive index needs Re m > 0 and Im m >= 0"};
+  if (t.N < 1 || t.N > 400 || t.m < 0 || t.m > t.N || t.n_theta < 2 || t.n_theta > 4000)
+    throw Failure{SCATRS_INVALID_INPUT,
+                  "a T-matrix needs 1 <= N <= 400, 0 <= m <= N and 2 <= n_theta <= 4000"};
+}
+
+// Runs the jobs in batches of bounded memory; sums[2 j] = -Re tr T, sums[2 j + 1] = sum |T|^2 of
+// job j, and each job's T (row-major (2K)^2 complex) into t_out if given.
+void run_tmatrices(Context& c, const std::vector<TmSpec>& specs, std::vector<double>& sums,
+                   std::vector<std::vector<double>>* t_out, cudaStream_t s) {
+  sums.assign(2 * specs.size(), 0.0);
+  if (t_out) t_out->assign(specs.size(), {});
+  constexpr double kBudget = 2.0e9;  // bytes of device workspace per batch
+  size_t j0 = 0;
+  while (j0 < specs.size()) {
+    std::vector<TmJob> jobs;
+    std::map<int, int64_t> rule_at;
+    std::vector<double> rx, rw;
+    int64_t nodes = 0, pairs = 0, fun = 0, J = 0, W = 0, T = 0;
+    double bytes = 0.0;
+    size_t j1 = j0;
+    for (; j1 < specs.size(); ++j1) {
+      const TmSpec& t = specs[j1];
+      check_tm_spec(t);
+      const int K = t.N - std::max(t.m, 1) + 1, n2 = 2 * K, nq = 2 * t.n_theta;
+      const double b = 8.0 * ((double)nq * (t.N + 1) * 13 + 5.0 * nq + 16.0 * K * K +
+                              4.0 * n2 * n2 + (t_out ? 2.0 * n2 * n2 : 0.0));
+      if (j1 > j0 && bytes + b > kBudget) break;
+      bytes += b;
+      if (!rule_at.count(nq)) {
+        rule_at[nq] = (int64_t)rx.size();
+        const auto& r = rule(c, nq);
+        rx.insert(rx.end(), r.first.begin(), r.first.end());
+        rw.insert(rw.end(), r.second.begin(), r.second.end());
+      }
+      TmJob jb{};
+      jb.x = t.x;
+      jb.eps = t.eps;
+      jb.s_re = t.s_re;
+      jb.s_im = t.s_im;
+      jb.m = t.m;
+      jb.N = t.N;
+      jb.n_theta = t.n_theta;
+      jb.node0 = nodes;
+      jb.pair0 = pairs;
+      jb.fun0 = fun;
+      jb.J0 = J;
+      jb.W0 = W;
+      jb.T0 = T;
+      jb.rule = rule_at[nq];
+      nodes += nq;
+      pairs += (int64_t)K * K;
+      fun += (int64_t)nq * (t.N + 1) * 13;
+      J += 8 * (int64_t)K * K;
+      W += 2 * (int64_t)n2 * n2;
+      T += (int64_t)n2 * n2;
+      jobs.push_back(jb);
+    }
+    TmArgs a{};
+    a.n_jobs = (int)jobs.size();
+    a.n_node_total = nodes;
+    a.n_pair_total = pairs;
+    a.jobs = c.tm_jobs.as<TmJob>(jobs.size());
+    double* gx = c.tm_rules_x.as<double>(rx.size());
+    double* gw = c.tm_rules_w.as<double>(rw.size());
+    a.gl_nodes = gx;
+    a.gl_weights = gw;
+    a.node = c.tm_node.as<double>(5 * (size_t)nodes);
+    a.fun = c.tm_fun.as<double>((size_t)fun);
+    a.J = c.tm_J.as<double>(2 * (size_t)J);
+    a.work = c.tm_work.as<double>(2 * (size_t)W);
+    a.T = t_out ? c.tm_T.as<double>(2 * (size_t)T) : nullptr;
+    a.sums = c.tm_sums.as<double>(2 * jobs.size());
+    a.err = c.tm_err.as<unsigned>(1);
+    SB_CUDA(cudaMemcpyAsync((void*)a.jobs, jobs.data(), jobs.size() * sizeof(TmJob),
+                            cudaMemcpyHostToDevice, s));
+    SB_CUDA(cudaMemcpyAsync(gx, rx.data(), rx.size() * 8, cudaMemcpyHostToDevice, s));
+    SB_CUDA(cudaMemcpyAsync(gw, rw.data(), rw.size() * 8, cudaMemcpyHostToDevice, s));
+    SB_CUDA(cudaMemsetAsync(a.err, 0, sizeof(unsigned), s));
+    timed_launch(K_UNITS, s, [&] { launch_tmatrix(a, s); });
+    SB_CUDA(cudaGetLastError());
+    unsigned flag = 0;
+    SB_CUDA(cudaMemcpyAsync(sums.data() + 2 * j0, a.sums, 2 * jobs.size() * 8,
+                            cudaMemcpyDeviceToHost, s));
+    SB_CUDA(cudaMemcpyAsync(&flag, a.err, sizeof flag, cudaMemcpyDeviceToHost, s));
+    if (t_out) {
+      std::vector<double> all(2 * (size_t)T);
+      SB_CUDA(cudaMemcpyAsync(all.data(), a.T, all.size() * 8, cudaMemcpyDeviceToHost, s));
+      SB_CUDA(cudaStreamSynchronize(s));
+      for (size_t k = 0; k < jobs.size(); ++k) {
+        const int K = jobs[k].N - std::max(jobs[k].m, 1) + 1, n2 = 2 * K;
+        (*t_out)[j0 + k].assign(all.begin() + 2 * jobs[k].T0,
+                                all.begin() + 2 * jobs[k].T0 + 2 * (int64_t)n2 * n2);
+      }
+    }
+    SB_CUDA(cudaStreamSynchronize(s));
+    if (flag) throw Failure{SCATRS_INVALID_INPUT, "a spheroid's Q matrix is singular"};
+    j0 = j1;
+  }
+}
+
+// driver.rs:166-214.
+double tm_x_max(double x, double eps) {
+  const double a = x * std::cbrt(eps);
+  return std::max(a, a / eps);
+}
+int tm_wiscombe(double xm) { return std::max((int)std::ceil(xm + 4.0 * std::cbrt(xm)) + 2, 4); }
+int tm_theta_of(int n, double eps, double rtol) {
+  const double h = std::max(eps, 1.0 / eps);
+  const int shape =
+      h <= 1.0 ? 0 : (int)std::ceil(std::log(1e4 / rtol) / (2.0 * std::log((h + 1.0) / (h - 1.0))));
+  return std::max(2 * n, shape);
+}
+
 FixedCall g_last_call;  // for scatrs_check_errors
 
 template <class F>
@@ -1637,6 +1767,124 @@ int scatrs_project_greek_device(const double* phase_dev, int64_t n_units, int64_
     SB_CUDA(cudaMemcpyAsync(&h, flag, sizeof h, cudaMemcpyDeviceToHost, s));
     SB_CUDA(cudaStreamSynchronize(s));
     if (h) throw Failure{SCATRS_CUDA, "the tensor-core projection's pipeline timed out"};
+  });
+}
+
+int scatrs_spheroid_tmatrix(double x, double aspect_ratio, const double* m, int32_t mode,
+                            int32_t n_terms, int32_t n_theta, double* t, char* err,
+                            size_t err_len) {
+  return guarded(err, err_len, [&] {
+    if (!m || !t) throw Failure{SCATRS_INVALID_INPUT, "m and t are required"};
+    Context& c = context();
+    std::lock_guard<std::mutex> lk(c.mtx);
+    std::vector<double> sums;
+    std::vector<std::vector<double>> ts;
+    run_tmatrices(c, {TmSpec{x, aspect_ratio, m[0], m[1], mode, n_terms, n_theta}}, sums, &ts, 0);
+    std::copy(ts[0].begin(), ts[0].end(), t);
+  });
+}
+
+int scatrs_spheroid_efficiencies(int64_t n, const double* x, const double* aspect_ratio,
+                                 const double* m, double rtol, double* q, int32_t* n_terms,
+                                 int32_t* n_theta, char* err, size_t err_len) {
+  return guarded(err, err_len, [&] {
+    if (n < 0) throw Failure{SCATRS_INVALID_INPUT, "negative sizes"};
+    if (!(rtol >= 1e-13 && rtol <= 0.1))
+      throw Failure{SCATRS_INVALID_INPUT, "rtol must be in [1e-13, 0.1]"};
+    if (n == 0) return;
+    if (!x || !aspect_ratio || !m || !q)
+      throw Failure{SCATRS_INVALID_INPUT, "x, aspect_ratio, m and q are required"};
+    for (int64_t i = 0; i < n; ++i)
+      check_tm_spec({x[i], aspect_ratio[i], m[2 * i], m[2 * i + 1], 0, 1, 2});
+    Context& c = context();
+    std::lock_guard<std::mutex> lk(c.mtx);
+    cudaStream_t s = 0;
+    // Per spheroid: the loop in N on mode 0, then in n_theta (driver.rs:343-420).
+    struct St {
+      int n, nth, cap, th_cap, stage;  // stage 0: N, 1: n_theta, 2: done
+      double e, sc;
+    };
+    std::vector<St> st(n);
+    std::vector<TmSpec> specs;
+    auto theta = [&](int64_t i, int nn) {
+      return std::min(tm_theta_of(nn, aspect_ratio[i], rtol), st[i].th_cap);
+    };
+    for (int64_t i = 0; i < n; ++i) {
+      const double mag = std::hypot(m[2 * i], m[2 * i + 1]);
+      st[i].cap = 2 * tm_wiscombe(tm_x_max(x[i], aspect_ratio[i]) * std::max(mag, 1.0)) + 20;
+      st[i].n = std::min(tm_wiscombe(tm_x_max(x[i], aspect_ratio[i])), st[i].cap);
+      // mod.rs:293-300: n_theta's cap is 4 theta(start) + 40.
+      st[i].th_cap = 4 * tm_theta_of(st[i].n, aspect_ratio[i], rtol) + 40;
+      st[i].nth = theta(i, st[i].n);
+      st[i].stage = 0;
+      specs.push_back({x[i], aspect_ratio[i], m[2 * i], m[2 * i + 1], 0, st[i].n, st[i].nth});
+    }
+    std::vector<double> sums;
+    run_tmatrices(c, specs, sums, nullptr, s);
+    for (int64_t i = 0; i < n; ++i) {
+      st[i].e = sums[2 * i];
+      st[i].sc = sums[2 * i + 1];
+    }
+    for (;;) {
+      std::vector<int64_t> who;
+      specs.clear();
+      for (int64_t i = 0; i < n; ++i) {
+        St& z = st[i];
+        if (z.stage == 2) continue;
+        if ((z.stage == 0 && z.n >= z.cap) || (z.stage == 1 && z.nth >= z.th_cap)) {
+          char buf[200];
+          snprintf(buf, sizeof buf,
+                   "spheroid %lld: the cross sections did not settle to %g within N = %d, "
+                   "n_theta = %d",
+                   (long long)i, rtol, z.cap, z.th_cap);
+          throw Failure{SCATRS_NOT_CONVERGED, buf};
+        }
+        int nn = z.n, nt = z.nth;
+        if (z.stage == 0) {
+          nn = std::min(z.n + std::max(z.n / 8, 2), z.cap);
+          nt = theta(i, nn);
+        } else {
+          nt = std::min(z.nth + std::max(z.nth / 10, 2), z.th_cap);
+        }
+        specs.push_back({x[i], aspect_ratio[i], m[2 * i], m[2 * i + 1], 0, nn, nt});
+        who.push_back(i);
+      }
+      if (who.empty()) break;
+      run_tmatrices(c, specs, sums, nullptr, s);
+      for (size_t k = 0; k < who.size(); ++k) {
+        St& z = st[who[k]];
+        const double e1 = sums[2 * k], s1 = sums[2 * k + 1];
+        const double ch = std::max(std::fabs(e1 - z.e) / std::fabs(e1), std::fabs(s1 - z.sc) / std::fabs(s1));
+        z.n = specs[k].N;
+        z.nth = specs[k].n_theta;
+        z.e = e1;
+        z.sc = s1;
+        if (ch < rtol) z.stage += 1;
+      }
+    }
+    // Every mode at the final N and n_theta.
+    specs.clear();
+    std::vector<int64_t> owner;
+    for (int64_t i = 0; i < n; ++i)
+      for (int mm = 0; mm <= st[i].n; ++mm) {
+        specs.push_back({x[i], aspect_ratio[i], m[2 * i], m[2 * i + 1], mm, st[i].n, st[i].nth});
+        owner.push_back(i);
+      }
+    run_tmatrices(c, specs, sums, nullptr, s);
+    std::vector<double> ext(n, 0.0), sca(n, 0.0);
+    for (size_t k = 0; k < specs.size(); ++k) {
+      const double w = specs[k].m == 0 ? 1.0 : 2.0;
+      ext[owner[k]] += w * sums[2 * k];
+      sca[owner[k]] += w * sums[2 * k + 1];
+    }
+    for (int64_t i = 0; i < n; ++i) {
+      const double area = 3.14159265358979323846 * x[i] * x[i];
+      q[3 * i] = 2.0 * 3.14159265358979323846 * ext[i] / area;
+      q[3 * i + 1] = 2.0 * 3.14159265358979323846 * sca[i] / area;
+      q[3 * i + 2] = q[3 * i] - q[3 * i + 1];
+      if (n_terms) n_terms[i] = st[i].n;
+      if (n_theta) n_theta[i] = st[i].nth;
+    }
   });
 }
 

@@ -257,6 +257,31 @@ void launch_greek_split_d(const double* d, int n_q, int n_q_pad, int len, float*
 cudaError_t launch_greek_tc(const struct CUtensorMap_st* maps, const TcArgs& a, cudaStream_t s);
 void launch_greek_assemble(const float* prod, int64_t n_units, int len, double* greek,
                            cudaStream_t s);
+// Spheroid T-matrices (tmatrix.cu): one job per (spheroid, azimuthal mode m) at truncation N
+// and n_theta nodes in 0 < theta < pi/2 (the 2 n_theta-point Gauss rule on [-1, 1], at
+// gl_nodes + rule); offsets into the flat arrays (nodes, functions, surface integrals J,
+// workspace, T) per job.
+struct TmJob {
+  double x, eps, s_re, s_im;
+  int m, N, n_theta, pad;
+  int64_t node0, pair0, fun0, J0, W0, T0, rule;
+};
+struct TmArgs {
+  const TmJob* jobs;
+  int n_jobs;
+  int64_t n_node_total, n_pair_total;
+  const double* gl_nodes;
+  const double* gl_weights;
+  double* node;  // [nodes][5]
+  double* fun;   // per job [2 n_theta][N + 1][13]
+  double* J;     // per job 8 K^2 complex
+  double* work;  // per job 2 (2K)^2 complex
+  double* T;     // per job (2K)^2 complex, or null
+  double* sums;  // per job: -Re tr T, sum |T|^2
+  unsigned* err;
+};
+void launch_tmatrix(const TmArgs& a, cudaStream_t s);
+
 void launch_greek_fp64(const double* phase, int64_t n_units, int n_q, int len, const double* d,
                        double* greek, cudaStream_t s);
 void launch_mix(const MixArgs& a, cudaStream_t s);

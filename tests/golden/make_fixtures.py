@@ -4,7 +4,7 @@ The reference (usask-arg/scatrs) ships certified or high-precision values comput
 ball arithmetic in ``reference/data/*.jsonl`` (each value as hi + lo + lo2 plus an error bound).
 This script keeps the records on the ensemble path (homogeneous spheres, their Greek
 coefficients, Gauss-Legendre rules, the Wigner d functions the projection uses, layered
-spheres) as hi + lo pairs in compact JSON, so that the tests run without the reference tree.
+spheres, spheroids' T-matrices) as hi + lo pairs in compact JSON, so that the tests run without the reference tree.
 
 Run from the repository root:  python tests/golden/make_fixtures.py [path/to/reference]
 """
@@ -84,6 +84,14 @@ def main(ref: str) -> None:
          "m_im": r["inputs"]["m_im"],
          **{k: pairs(r["outputs"][k]) for k in r["outputs"] if k.startswith("q_") or k == "g"}}
         for r in layered if r["case"].endswith(",series")
+    ]
+    sph = load(ref, "spheroid.jsonl")
+    out["spheroid"] = [
+        {"case": r["case"], "x": r["inputs"]["x"], "eps": r["inputs"]["aspect_ratio"],
+         "m": [r["inputs"]["m_re"], r["inputs"]["m_im"]],
+         "n_terms": r["inputs"].get("n_terms"), "n_theta": r["inputs"].get("n_theta"),
+         **{k: pairs(v) for k, v in r["outputs"].items()}}
+        for r in sph
     ]
     for name, recs in out.items():
         with open(os.path.join(HERE, f"{name}.json"), "w") as f:
