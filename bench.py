@@ -271,7 +271,7 @@ def tf32_peak_tflops(torch):
     return 2.0 * n ** 3 / (best * 1e-3) / 1e12
 
 
-def projection_c3(torch, steps: int = 3):
+def projection_c3(torch, steps: int = 3, scale: float = 1.0):
     """The Greek projection of the large-droplet configuration's shape (128 distributions x
     256 wavelengths = 32,768 tables at 4096 Gauss cosines, order 1024) on the tensor cores
     (3xTF32, FP32 accumulation) against the FP64 projection of the same tables: throughput of
@@ -280,7 +280,7 @@ def projection_c3(torch, steps: int = 3):
     from scatrs_b200 import _native
     from scatrs_b200 import workloads as W
 
-    n_units, n_q, L = 128 * 256, 4096, 1024
+    n_units, n_q, L = max(1, round(128 * 256 * min(scale, 1.0))), 4096, 1024
     g = torch.Generator(device="cuda").manual_seed(3)
     mu = torch.tensor(W.gauss_legendre(n_q), device="cuda")
     # F = sum of a few Legendre-like smooth lobes per table.
@@ -317,8 +317,8 @@ def projection_c3(torch, steps: int = 3):
     achieved = tf32_flops / (gemm_ms * 1e-3) / 1e12
     del phase, out_tc, out_64
     torch.cuda.empty_cache()
-    return {"workload": "32768 tables x 4096 Gauss cosines -> Greek order 1024 (large-droplet "
-                        "shape, seeded synthetic tables)",
+    return {"workload": f"{n_units} tables x 4096 Gauss cosines -> Greek order 1024 "
+                        "(large-droplet shape, seeded synthetic tables)",
             "kernel": "greek_tc_kernel (tcgen05.mma kind::tf32, 3 products)",
             "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
             "frac": achieved / peak,
@@ -468,7 +468,7 @@ def ours(args):
     }
     line["clocks"] = clk.summary()
     if world == 1 and not args.no_projection:
-        line["projection_tc"] = projection_c3(torch)
+        line["projection_tc"] = projection_c3(torch, scale=args.scale)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_sample(w, args.cpu_seconds)
     print(json.dumps(line), flush=True)
