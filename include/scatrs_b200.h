@@ -201,8 +201,13 @@ int scatrs_project_greek_device(const double* phase_dev, int64_t n_units, int64_
  * scatrs_spheroid_efficiencies: the orientation-averaged Q_ext, Q_sca, Q_abs of n spheroids
  * (q[3 n]), converged in N and n_theta to rtol as driver.rs:343-420 converges them on mode 0,
  * then every mode at the final N (n_terms[n], n_theta[n] the values used; either may be NULL).
- * Status 2 when N reaches its cap. The FP64 formulation is the classical one; see the accuracy
- * limits stated with the library.
+ * Status 2 when N reaches its cap, or n_theta its cap 4 theta(start) + 40 (mod.rs:293-300).
+ * The surface integrals are the classical ones from the definition, assembled in double-double
+ * (about 106 bits) against their cancellation, then solved in FP64 with double-double residual
+ * refinement (the last sweep's relative correction is below 2^-54 on return): T agrees with a
+ * quadruple-precision EBCM to about 1e-26 of its largest element on the reference's records.
+ * Where the cancellation exceeds double-double's reach (about 1e28: aspect ratios near 0.4 or 3
+ * at size parameters above about 17), the N loop does not settle and status 2 is returned.
  */
 int scatrs_spheroid_tmatrix(double x, double aspect_ratio, const double* m, int32_t mode,
                             int32_t n_terms, int32_t n_theta, double* t, char* err,

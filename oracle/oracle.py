@@ -375,11 +375,13 @@ def ensemble_mixture(components, wavelengths, mu=None, greek_order=None, normali
     return out
 
 
-def tmatrix_mode(x: float, eps: float, s: complex, m: int, n: int, n_theta: int) -> np.ndarray:
-    """One azimuthal mode's T-matrix of a spheroid (2K x 2K complex, K = n - max(m, 1) + 1)."""
+def tmatrix_mode(x: float, eps: float, s: complex, m: int, n: int, n_theta: int,
+                 quad: bool = False) -> np.ndarray:
+    """One azimuthal mode's T-matrix of a spheroid (2K x 2K complex, K = n - max(m, 1) + 1); in
+    quadruple precision with `quad`."""
     k = n - max(m, 1) + 1
     t = np.zeros(2 * (2 * k) ** 2)
-    f = lib().orc_tmatrix_mode
+    f = lib().orc_tmatrix_mode_q if quad else lib().orc_tmatrix_mode
     f.argtypes = [_D, _D, _D, _D, ctypes.c_int, ctypes.c_int, ctypes.c_int, _PD]
     st = f(x, eps, s.real, s.imag, m, n, n_theta, _p(t))
     if st != 0:
@@ -387,10 +389,11 @@ def tmatrix_mode(x: float, eps: float, s: complex, m: int, n: int, n_theta: int)
     return t.view(np.complex128).reshape(2 * k, 2 * k)
 
 
-def spheroid_q(x: float, eps: float, s: complex, n: int, n_theta: int):
-    """Orientation-averaged (Q_ext, Q_sca) of a spheroid at truncation n and n_theta nodes."""
+def spheroid_q(x: float, eps: float, s: complex, n: int, n_theta: int, quad: bool = False):
+    """Orientation-averaged (Q_ext, Q_sca) of a spheroid at truncation n and n_theta nodes; in
+    quadruple precision with `quad`."""
     q = np.zeros(2)
-    f = lib().orc_spheroid_q
+    f = lib().orc_spheroid_q_q if quad else lib().orc_spheroid_q
     f.argtypes = [_D, _D, _D, _D, ctypes.c_int, ctypes.c_int, _PD]
     st = f(x, eps, s.real, s.imag, n, n_theta, _p(q))
     if st != 0:

@@ -25,6 +25,7 @@
 
 #include "../../include/scatrs_b200.h"
 #include "adaptive.h"
+#include "dd.cuh"
 #include "kernels.h"
 #include "tables.h"
 
@@ -156,7 +157,9 @@ struct Context {
   std::map<std::pair<int64_t, int>, Projector> projectors;
   DevBuf tc_a_hi, tc_a_lo, tc_prod, tc_err;
   // Spheroid T-matrices.
-  DevBuf tm_jobs, tm_rules_x, tm_rules_w, tm_node, tm_fun, tm_J, tm_work, tm_T, tm_sums, tm_err;
+  DevBuf tm_geoms, tm_jobs, tm_rules, tm_node, tm_rad, tm_ang, tm_J, tm_work, tm_piv, tm_T, tm_sums,
+      tm_err;
+  std::map<int64_t, std::vector<double>> dd_rules;  // n -> per node x (hi, lo), w (hi, lo)
   std::vector<int> chunk_n_host;
   int* pinned_chunk_n = nullptr;
   size_t pinned_cap = 0;
@@ -1425,102 +1428,164 @@ void check_tm_spec(const TmSpec& t) {
     throw Failure{SCATRS_INVALID_INPUT, "the aspect ratio must be finite and > 0"};
   if (!(std::isfinite(t.s_re) && std::isfinite(t.s_im) && t.s_re > 0.0 && t.s_im >= 0.0))
     throw Failure{SCATRS_INVALID_INPUT, "the refractive index needs Re m > 0 and Im m >= 0"};
-  if (t.N < 1 || t.N > 400 || t.m < 0 || t.m > t.N || t.n_theta < 2 || t.n_theta > 4000)
+  if (t.N < 1 || t.N > 500 || t.m < 0 || t.m > t.N || t.n_theta < 2 || t.n_theta > 4000)
     throw Failure{SCATRS_INVALID_INPUT,
-                  "a T-matrix needs 1 <= N <= 400, 0 <= m <= N and 2 <= n_theta <= 4000"};
+                  "a T-matrix needs 1 <= N <= 500, 0 <= m <= N and 2 <= n_theta <= 4000"};
 }
 
-// Runs the jobs in batches of bounded memory; sums[2 j] = -Re tr T, sums[2 j + 1] = sum |T|^2 of
-// job j, and each job's T (row-major (2K)^2 complex) into t_out if given.
+// The n-point Gauss-Legendre rule on [-1, 1] in double-double: the double rule's nodes refined
+// by Newton's method on P_n (three-term recurrence) in the host's 113-bit __float128
+// arithmetic, the weights 2 / ((1 - x^2) P_n'(x)^2), each rounded to a double-double pair.
+const std::vector<double>& dd_rule(Context& c, int64_t n) {
+  auto it = c.dd_rules.find(n);
+  if (it != c.dd_rules.end()) return it->second;
+  typedef __float128 q128;
+  const auto& r = rule(c, n);
+  std::vector<double> out(4 * (size_t)n);
+  auto legendre = [&](q128 t, q128* p, q128* dp) {
+    q128 p0 = 1, p1 = t;
+    for (int64_t k = 2; k <= n; ++k) {
+      const q128 p2 = ((2 * k - 1) * t * p1 - (k - 1) * p0) / k;
+      p0 = p1;
+      p1 = p2;
+    }
+    *p = p1;
+    *dp = n * (p0 - t * p1) / ((1 - t) * (1 + t));
+  };
+  auto split = [](q128 v, double* o) {
+    o[0] = (double)v;
+    o[1] = (double)(v - (q128)o[0]);
+  };
+  for (int64_t i = 0; i < n; ++i) {
+    q128 t = r.first[i], p, dp;
+    for (int it2 = 0; it2 < 3; ++it2) {
+      legendre(t, &p, &dp);
+      t -= p / dp;
+    }
+    legendre(t, &p, &dp);
+    split(t, &out[4 * i]);
+    split(2 / ((1 - t) * (1 + t) * dp * dp), &out[4 * i + 2]);
+  }
+  return c.dd_rules.emplace(n, std::move(out)).first->second;
+}
+
+// Runs the T-matrices of specs in batches of bounded memory. Consecutive specs of the same
+// spheroid at the same N and n_theta share one geometry (nodes and radial functions). Per
+// spec j: sums[3 j] = -Re tr T, sums[3 j + 1] = sum |T|^2, sums[3 j + 2] = the refinement's
+// last relative correction; each T (row-major (2K)^2 complex) into t_out if given.
 void run_tmatrices(Context& c, const std::vector<TmSpec>& specs, std::vector<double>& sums,
                    std::vector<std::vector<double>>* t_out, cudaStream_t s) {
-  sums.assign(2 * specs.size(), 0.0);
+  sums.assign(3 * specs.size(), 0.0);
   if (t_out) t_out->assign(specs.size(), {});
-  constexpr double kBudget = 2.0e9;  // bytes of device workspace per batch
+  constexpr double kBudget = 8.0e9;  // bytes of device workspace per batch
+  auto same_geom = [](const TmSpec& p, const TmSpec& q) {
+    return p.x == q.x && p.eps == q.eps && p.s_re == q.s_re && p.s_im == q.s_im && p.N == q.N &&
+           p.n_theta == q.n_theta;
+  };
   size_t j0 = 0;
   while (j0 < specs.size()) {
+    std::vector<TmGeom> geoms;
     std::vector<TmJob> jobs;
-    std::map<int, int64_t> rule_at;
-    std::vector<double> rx, rw;
-    int64_t nodes = 0, pairs = 0, fun = 0, J = 0, W = 0, T = 0;
+    std::map<int64_t, int64_t> rule_at;
+    std::vector<double> rules;
+    int64_t nodes = 0, rad = 0, ang_nodes = 0, ang = 0, pairs = 0, J = 0, W = 0, P = 0, T = 0;
     double bytes = 0.0;
     size_t j1 = j0;
     for (; j1 < specs.size(); ++j1) {
       const TmSpec& t = specs[j1];
       check_tm_spec(t);
+      const bool new_geom = j1 == j0 || !same_geom(specs[j1 - 1], t);
       const int K = t.N - std::max(t.m, 1) + 1, n2 = 2 * K, nq = 2 * t.n_theta;
-      const double b = 8.0 * ((double)nq * (t.N + 1) * 13 + 5.0 * nq + 16.0 * K * K +
-                              4.0 * n2 * n2 + (t_out ? 2.0 * n2 * n2 : 0.0));
+      double b = 8.0 * ((double)nq * (t.N + 1) * 6 + 32.0 * K * K + 14.0 * n2 * n2 +
+                        (t_out ? 2.0 * n2 * n2 : 0.0)) + 4.0 * n2;
+      if (new_geom) b += 8.0 * ((double)nq * 16 + (double)nq * (t.N + 1) * 20);
       if (j1 > j0 && bytes + b > kBudget) break;
       bytes += b;
-      if (!rule_at.count(nq)) {
-        rule_at[nq] = (int64_t)rx.size();
-        const auto& r = rule(c, nq);
-        rx.insert(rx.end(), r.first.begin(), r.first.end());
-        rw.insert(rw.end(), r.second.begin(), r.second.end());
+      if (new_geom) {
+        if (!rule_at.count(nq)) {
+          rule_at[nq] = (int64_t)rules.size() / 4;
+          const auto& r = dd_rule(c, nq);
+          rules.insert(rules.end(), r.begin(), r.end());
+        }
+        TmGeom g{};
+        g.a = t.x * std::cbrt(t.eps);
+        g.c = g.a / t.eps;
+        g.s_re = t.s_re;
+        g.s_im = t.s_im;
+        g.N = t.N;
+        g.n_theta = t.n_theta;
+        g.node0 = nodes;
+        g.rule = rule_at[nq];
+        g.rad0 = rad;
+        nodes += nq;
+        rad += (int64_t)nq * (t.N + 1) * 20;
+        geoms.push_back(g);
       }
       TmJob jb{};
-      jb.x = t.x;
-      jb.eps = t.eps;
-      jb.s_re = t.s_re;
-      jb.s_im = t.s_im;
+      jb.geom = (int)geoms.size() - 1;
       jb.m = t.m;
-      jb.N = t.N;
-      jb.n_theta = t.n_theta;
-      jb.node0 = nodes;
+      jb.K = K;
+      jb.ang_node0 = ang_nodes;
+      jb.ang0 = ang;
       jb.pair0 = pairs;
-      jb.fun0 = fun;
       jb.J0 = J;
       jb.W0 = W;
+      jb.piv0 = P;
       jb.T0 = T;
-      jb.rule = rule_at[nq];
-      nodes += nq;
+      ang_nodes += nq;
+      ang += (int64_t)nq * (t.N + 1) * 6;
       pairs += (int64_t)K * K;
-      fun += (int64_t)nq * (t.N + 1) * 13;
       J += 8 * (int64_t)K * K;
-      W += 2 * (int64_t)n2 * n2;
+      W += 14 * (int64_t)n2 * n2;
+      P += n2;
       T += (int64_t)n2 * n2;
       jobs.push_back(jb);
     }
     TmArgs a{};
+    a.n_geoms = (int)geoms.size();
     a.n_jobs = (int)jobs.size();
     a.n_node_total = nodes;
+    a.n_ang_total = ang_nodes;
     a.n_pair_total = pairs;
+    a.geoms = c.tm_geoms.as<TmGeom>(geoms.size());
     a.jobs = c.tm_jobs.as<TmJob>(jobs.size());
-    double* gx = c.tm_rules_x.as<double>(rx.size());
-    double* gw = c.tm_rules_w.as<double>(rw.size());
-    a.gl_nodes = gx;
-    a.gl_weights = gw;
-    a.node = c.tm_node.as<double>(5 * (size_t)nodes);
-    a.fun = c.tm_fun.as<double>((size_t)fun);
-    a.J = c.tm_J.as<double>(2 * (size_t)J);
-    a.work = c.tm_work.as<double>(2 * (size_t)W);
+    double* rl = c.tm_rules.as<double>(rules.size());
+    a.rule = rl;
+    a.node = c.tm_node.as<double>(16 * (size_t)nodes);
+    a.rad = c.tm_rad.as<double>((size_t)rad);
+    a.ang = c.tm_ang.as<double>((size_t)ang);
+    a.J = c.tm_J.as<double>(4 * (size_t)J);
+    a.work = c.tm_work.as<double>((size_t)W);
+    a.piv = c.tm_piv.as<int>((size_t)P);
     a.T = t_out ? c.tm_T.as<double>(2 * (size_t)T) : nullptr;
-    a.sums = c.tm_sums.as<double>(2 * jobs.size());
+    a.sums = c.tm_sums.as<double>(3 * jobs.size());
     a.err = c.tm_err.as<unsigned>(1);
+    a.max_sweeps = 4;
+    SB_CUDA(cudaMemcpyAsync((void*)a.geoms, geoms.data(), geoms.size() * sizeof(TmGeom),
+                            cudaMemcpyHostToDevice, s));
     SB_CUDA(cudaMemcpyAsync((void*)a.jobs, jobs.data(), jobs.size() * sizeof(TmJob),
                             cudaMemcpyHostToDevice, s));
-    SB_CUDA(cudaMemcpyAsync(gx, rx.data(), rx.size() * 8, cudaMemcpyHostToDevice, s));
-    SB_CUDA(cudaMemcpyAsync(gw, rw.data(), rw.size() * 8, cudaMemcpyHostToDevice, s));
+    SB_CUDA(cudaMemcpyAsync(rl, rules.data(), rules.size() * 8, cudaMemcpyHostToDevice, s));
     SB_CUDA(cudaMemsetAsync(a.err, 0, sizeof(unsigned), s));
     timed_launch(K_UNITS, s, [&] { launch_tmatrix(a, s); });
     SB_CUDA(cudaGetLastError());
     unsigned flag = 0;
-    SB_CUDA(cudaMemcpyAsync(sums.data() + 2 * j0, a.sums, 2 * jobs.size() * 8,
+    SB_CUDA(cudaMemcpyAsync(sums.data() + 3 * j0, a.sums, 3 * jobs.size() * 8,
                             cudaMemcpyDeviceToHost, s));
     SB_CUDA(cudaMemcpyAsync(&flag, a.err, sizeof flag, cudaMemcpyDeviceToHost, s));
+    std::vector<double> all;
     if (t_out) {
-      std::vector<double> all(2 * (size_t)T);
+      all.resize(2 * (size_t)T);
       SB_CUDA(cudaMemcpyAsync(all.data(), a.T, all.size() * 8, cudaMemcpyDeviceToHost, s));
-      SB_CUDA(cudaStreamSynchronize(s));
-      for (size_t k = 0; k < jobs.size(); ++k) {
-        const int K = jobs[k].N - std::max(jobs[k].m, 1) + 1, n2 = 2 * K;
-        (*t_out)[j0 + k].assign(all.begin() + 2 * jobs[k].T0,
-                                all.begin() + 2 * jobs[k].T0 + 2 * (int64_t)n2 * n2);
-      }
     }
     SB_CUDA(cudaStreamSynchronize(s));
     if (flag) throw Failure{SCATRS_INVALID_INPUT, "a spheroid's Q matrix is singular"};
+    if (t_out)
+      for (size_t k = 0; k < jobs.size(); ++k) {
+        const int n2 = 2 * jobs[k].K;
+        (*t_out)[j0 + k].assign(all.begin() + 2 * jobs[k].T0,
+                                all.begin() + 2 * jobs[k].T0 + 2 * (int64_t)n2 * n2);
+      }
     j0 = j1;
   }
 }
@@ -1822,8 +1887,8 @@ int scatrs_spheroid_efficiencies(int64_t n, const double* x, const double* aspec
     std::vector<double> sums;
     run_tmatrices(c, specs, sums, nullptr, s);
     for (int64_t i = 0; i < n; ++i) {
-      st[i].e = sums[2 * i];
-      st[i].sc = sums[2 * i + 1];
+      st[i].e = sums[3 * i];
+      st[i].sc = sums[3 * i + 1];
     }
     for (;;) {
       std::vector<int64_t> who;
@@ -1853,7 +1918,7 @@ int scatrs_spheroid_efficiencies(int64_t n, const double* x, const double* aspec
       run_tmatrices(c, specs, sums, nullptr, s);
       for (size_t k = 0; k < who.size(); ++k) {
         St& z = st[who[k]];
-        const double e1 = sums[2 * k], s1 = sums[2 * k + 1];
+        const double e1 = sums[3 * k], s1 = sums[3 * k + 1];
         const double ch = std::max(std::fabs(e1 - z.e) / std::fabs(e1), std::fabs(s1 - z.sc) / std::fabs(s1));
         z.n = specs[k].N;
         z.nth = specs[k].n_theta;
@@ -1874,8 +1939,8 @@ int scatrs_spheroid_efficiencies(int64_t n, const double* x, const double* aspec
     std::vector<double> ext(n, 0.0), sca(n, 0.0);
     for (size_t k = 0; k < specs.size(); ++k) {
       const double w = specs[k].m == 0 ? 1.0 : 2.0;
-      ext[owner[k]] += w * sums[2 * k];
-      sca[owner[k]] += w * sums[2 * k + 1];
+      ext[owner[k]] += w * sums[3 * k];
+      sca[owner[k]] += w * sums[3 * k + 1];
     }
     for (int64_t i = 0; i < n; ++i) {
       const double area = 3.14159265358979323846 * x[i] * x[i];

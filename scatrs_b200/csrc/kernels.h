@@ -261,24 +261,42 @@ void launch_greek_assemble(const float* prod, int64_t n_units, int len, double* 
 // and n_theta nodes in 0 < theta < pi/2 (the 2 n_theta-point Gauss rule on [-1, 1], at
 // gl_nodes + rule); offsets into the flat arrays (nodes, functions, surface integrals J,
 // workspace, T) per job.
+// One spheroid at one truncation N and n_theta (the shared node and radial tables), and one
+// azimuthal mode of it (a job). Offsets are in doubles unless stated.
+struct TmGeom {
+  double a, c, s_re, s_im;  // semi-axes (size parameters) and the relative index
+  int N, n_theta;
+  int64_t node0;  // first node (of 2 n_theta) in the node table
+  int64_t rule;   // first node of its Gauss-Legendre rule in the rule table
+  int64_t rad0;   // radial table [node][order 0..N][20]
+};
 struct TmJob {
-  double x, eps, s_re, s_im;
-  int m, N, n_theta, pad;
-  int64_t node0, pair0, fun0, J0, W0, T0, rule;
+  int geom, m, K, pad;
+  int64_t ang_node0;  // first (job, node) index of the angular table
+  int64_t ang0;       // angular table [node][order 0..N][6]
+  int64_t pair0;      // first (i, k) pair
+  int64_t J0;         // surface integrals: 8 K^2 complex double-doubles (4 doubles each)
+  int64_t W0;         // workspace: 14 (2K)^2 doubles
+  int64_t piv0;       // pivots: 2K ints
+  int64_t T0;         // T: (2K)^2 complex doubles (2 each), if kept
 };
 struct TmArgs {
+  const TmGeom* geoms;
+  int n_geoms;
   const TmJob* jobs;
   int n_jobs;
-  int64_t n_node_total, n_pair_total;
-  const double* gl_nodes;
-  const double* gl_weights;
-  double* node;  // [nodes][5]
-  double* fun;   // per job [2 n_theta][N + 1][13]
-  double* J;     // per job 8 K^2 complex
-  double* work;  // per job 2 (2K)^2 complex
-  double* T;     // per job (2K)^2 complex, or null
-  double* sums;  // per job: -Re tr T, sum |T|^2
-  unsigned* err;
+  int64_t n_node_total, n_ang_total, n_pair_total;
+  const double* rule;  // per rule node: x (hi, lo), w (hi, lo)
+  double* node;        // [node][16]: r, 1/r, nu_theta, weight factor (dd), s r (cdd), cos, sin (dd)
+  double* rad;
+  double* ang;
+  double* J;
+  double* work;
+  int* piv;
+  double* T;      // or null
+  double* sums;   // per job: -Re tr T, sum |T|^2, the refinement's last relative correction
+  unsigned* err;  // 1: a singular Q
+  int max_sweeps;
 };
 void launch_tmatrix(const TmArgs& a, cudaStream_t s);
 

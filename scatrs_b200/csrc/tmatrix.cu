@@ -1,260 +1,374 @@
 // The T-matrix of spheroids by the extended boundary condition method on the GPU
 // (scatrs/src/tmatrix: kernel.rs for Q and P = RgQ of each azimuthal mode by Gauss-Legendre
-// quadrature over the surface, solve.rs for T = -RgQ Q^{-1}, kernel.rs:985-1010 for the
-// orientation-averaged cross sections), batched over (spheroid, mode) jobs in three kernels:
+// quadrature over the surface, solve.rs for T = -P Q^{-1} with residual refinement,
+// kernel.rs:985-1010 for the orientation-averaged cross sections), batched over spheroids
+// (geometries) and their modes (jobs) in four kernels:
 //
-//   tm_functions_kernel  one thread per (job, node): the node's r(theta), the normal, the
-//                        weight, the angular functions d, pi, tau and the radial functions
-//                        h_n(r), j_n(r), j_n(s r) with their [z z_n]'/z, orders 0..N;
-//   tm_surface_kernel    one thread per (job, i, k): the eight surface integrals
-//                        J[out][a][b]_{ik} = sum_nodes w r^2 2 pi n . (A_i x B_k) of the outgoing
-//                        (h or j) and inner vector spherical wave functions;
-//   tm_solve_kernel      one block per job: Q and RgQ from J, the LU factorization of Q^T with
-//                        partial pivoting and the solve for T (in global memory, L2-resident),
-//                        and the mode's -Re tr T and sum |T|^2.
+//   tm_geom_kernel     one thread per (spheroid, node): r(theta), 1/r, the normal's
+//                      theta-component, the weight factor, s r, and the radial functions
+//                      j_n(r), y_n(r), j_n(s r) with their [z z_n]'/z, orders 0..N;
+//   tm_angular_kernel  one thread per (mode, node): the normalized d, pi, tau, orders 0..N;
+//   tm_surface_kernel  one thread per (mode, i, k): the eight surface integrals
+//                      J[out][a][b]_{ik} = sum_nodes w r^2 2 pi n . (A_i x B_k) of the outgoing
+//                      (j or h) and inner vector spherical wave functions;
+//   tm_solve_kernel    one block per mode: Q^T and -P^T from J, an FP64 LU factorization of Q^T
+//                      with partial pivoting, the solve, and residual sweeps X += LU^{-1}
+//                      (-P^T - Q^T X) with the residual in double-double; then the mode's
+//                      -Re tr T and sum |T|^2.
 //
-// The formulation is the classical one from the definition (Mishchenko, Travis & Lacis 2002,
-// section 5.8; as research/tmatrix/ebcm.py states it), in FP64. It is accurate where the EBCM's
-// own cancellation in the outgoing integrals is mild (moderate aspect ratios and sizes); the
-// reference's cancellation-free forms and double-double refinement are not restated here.
+// Everything before the factorization is double-double (dd.cuh): the EBCM's outgoing integrals
+// cancel exactly in their singular (electrostatic) terms, by up to 1e16 and more at the sizes
+// and aspect ratios of the spheroid workloads (research/tmatrix/README.md, findings 1-3), and
+// any pointwise error of the sampled functions or the rule is amplified by that factor.
+// Carrying the functions, the Gauss-Legendre rule and the sums in about 106 bits leaves the
+// elements accurate to about 1e-32 times the cancellation; the residual refinement then
+// removes the FP64 factorization's floor (Skeel(Q) 2^-53, finding 4), which is what the
+// reference's refinement (solve.rs:249-385) does with its own cancellation-free integrands.
+// The formulation of the integrands is the classical one from the definition (Mishchenko,
+// Travis & Lacis 2002, section 5.8; research/tmatrix/ebcm.py).
 #include <cuda_runtime.h>
 
 #include <cstdint>
 
+#include "dd.cuh"
 #include "kernels.h"
-#include "mie_device.cuh"
 
 namespace sb {
 
+using ddm::cdd;
+using ddm::dd;
+using ddm::mkc;
+using ddm::mkdd;
+
 namespace {
 
-constexpr int kFun = 13;  // doubles per (node, order): d, pi, tau, h (2), h' (2), j, j', w (2), w' (2)
-constexpr int kNode = 5;  // doubles per node: r, nu_theta, fac, (s r) (2)
+constexpr int kNodeD = 16;  // doubles per node
+constexpr int kRadD = 20;   // doubles per (node, order): j, j', y, y' (dd), w, w', w/(s r) (cdd)
+constexpr int kAngD = 6;    // doubles per (node, order): d, pi, tau (dd)
+constexpr double kPiHi = 3.141592653589793, kPiLo = 1.2246467991473532e-16;
 
-__device__ __forceinline__ cplx csin_(cplx z) {
-  return mk(sin(z.re) * cosh(z.im), cos(z.re) * sinh(z.im));
+__device__ __forceinline__ dd ld(const double* p) { return dd{p[0], p[1]}; }
+__device__ __forceinline__ void st(double* p, dd v) {
+  p[0] = v.hi;
+  p[1] = v.lo;
 }
-__device__ __forceinline__ cplx ccos_(cplx z) {
-  return mk(cos(z.re) * cosh(z.im), -(sin(z.re) * sinh(z.im)));
+__device__ __forceinline__ cdd ldc(const double* p) { return cdd{dd{p[0], p[1]}, dd{p[2], p[3]}}; }
+__device__ __forceinline__ void stc(double* p, cdd v) {
+  p[0] = v.re.hi;
+  p[1] = v.re.lo;
+  p[2] = v.im.hi;
+  p[3] = v.im.lo;
+}
+
+// The largest index i in [0, n) with first(i) <= t (first ascending, first(0) = 0).
+template <class F>
+__device__ __forceinline__ int owner(int n, int64_t t, F first) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) / 2;
+    if (first(mid) <= t) lo = mid; else hi = mid - 1;
+  }
+  return lo;
 }
 
 }  // namespace
 
-__global__ void __launch_bounds__(128) tm_functions_kernel(TmArgs a) {
+__global__ void __launch_bounds__(128) tm_geom_kernel(TmArgs a) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= a.n_node_total) return;
-  // The job of this node: the largest job whose first node is <= t.
-  int lo = 0, hi = a.n_jobs - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) / 2;
-    if (a.jobs[mid].node0 <= t) lo = mid; else hi = mid - 1;
-  }
-  const TmJob jb = a.jobs[lo];
-  const int q = (int)(t - jb.node0);
-  const int N = jb.N, m = jb.m;
-  const double ct = a.gl_nodes[jb.rule + q], wq = a.gl_weights[jb.rule + q];
-  const double st = sqrt(1.0 - ct * ct);
-  // r(theta), dr/dtheta of the spheroid x eps^(1/3) (a), a / eps (c) (ebcm.py:53-65).
-  const double ax = jb.x * cbrt(jb.eps), cx = ax / jb.eps;
-  const double den = cx * cx * st * st + ax * ax * ct * ct;
-  const double r = ax * cx / sqrt(den);
-  const double dr = -ax * cx * (cx * cx - ax * ax) * st * ct / (den * sqrt(den));
-  double* ns = a.node + t * kNode;
-  const cplx s = mk(jb.s_re, jb.s_im);
-  const cplx sr = scl(s, r);
-  ns[0] = r;
-  ns[1] = -dr / r;
-  ns[2] = wq * r * r * 2.0 * kPi;
-  ns[3] = sr.re;
-  ns[4] = sr.im;
-  double* f = a.fun + jb.fun0 + (int64_t)q * (N + 1) * kFun;
-  // Angular functions (ebcm.py:68-100), normalized, m >= 0.
+  const int gi = owner(a.n_geoms, t, [&](int i) { return a.geoms[i].node0; });
+  const TmGeom g = a.geoms[gi];
+  const int q = (int)(t - g.node0), N = g.N;
+  const double* rl = a.rule + 4 * (g.rule + q);
+  const dd ct = ld(rl), wq = ld(rl + 2);
+  const dd stt = ddm::dd_sqrt(mkdd(1.0) - ct * ct);
+  // r(theta) and dr/dtheta of the spheroid with semi-axes a (equatorial) and c (ebcm.py:53-65).
+  const dd A = mkdd(g.a), Cc = mkdd(g.c);
+  const dd den = Cc * Cc * (stt * stt) + A * A * (ct * ct);
+  const dd sden = ddm::dd_sqrt(den);
+  const dd r = (A * Cc) / sden;
+  const dd dr = -((A * Cc) * (Cc * Cc - A * A) * stt * ct) / (den * sden);
+  const dd ir = mkdd(1.0) / r;
+  double* ns = a.node + t * kNodeD;
+  st(ns + 0, r);
+  st(ns + 2, ir);
+  st(ns + 4, -(dr * ir));
+  st(ns + 6, wq * (r * r) * dd{2.0 * kPiHi, 2.0 * kPiLo});
+  const cdd s = mkc(g.s_re, g.s_im);
+  const cdd sr = s * r;
+  stc(ns + 8, sr);
+  st(ns + 12, ct);
+  st(ns + 14, stt);
+  double* f = a.rad + g.rad0 + (int64_t)q * (N + 1) * kRadD;
+  // j_n(r): ratios rho_n = j_n / j_{n-1} = r / (2n + 1 - r rho_{n+1}) downward from far above
+  // N (kept in the j slots), then values upward from j_0 = sin r / r, j_{-1} = cos r / r;
+  // der_n = j_{n-1} - n j_n / r.
+  dd sn, cs;
+  ddm::dd_sincos(r, &sn, &cs);
   {
-    double am = 1.0;
-    for (int k = 1; k <= m; ++k) am *= sqrt((double)(2 * k - 1) / (2 * k));
-    double dprev = 0.0, dcur = 0.0;
-    for (int n = 0; n <= N; ++n) {
-      double dn;
-      if (n < m) dn = 0.0;
-      else if (n == m) dn = am * pow(st, (double)m);
-      else if (n == m + 1) dn = sqrt(2.0 * m + 1) * ct * dcur;
-      else
-        dn = ((2 * (n - 1) + 1) * ct * dcur - sqrt((double)(n - 1) * (n - 1) - (double)m * m) * dprev) /
-             sqrt((double)n * n - (double)m * m);
-      double tau = 0.0, pi = 0.0;
-      if (n >= (m > 1 ? m : 1)) {
-        const double prev = n - 1 >= m ? dcur : 0.0;
-        tau = (n * ct * dn - sqrt((double)n * n - (double)m * m) * prev) / st;
-        pi = m * dn / st;
-      }
-      f[n * kFun + 0] = dn;
-      f[n * kFun + 1] = pi;
-      f[n * kFun + 2] = tau;
-      dprev = dcur;
-      dcur = dn;
-    }
-  }
-  // j_n(z) by downward ratios rho_n = j_n / j_{n-1} = z / (2n + 1 - z rho_{n+1}) from far above
-  // N; the ratios of orders <= N are kept in the output slots, then turned into values upward
-  // from j_0 = sin z / z, j_{-1} = cos z / z. der_n = z_{n-1} - n z_n / z.
-  auto bessel_j = [&](cplx z, int slot_re, int slot_im, int dslot_re, int dslot_im) {
-    const int start = N + 40 + (int)(2.0 * cabs_(z));
-    cplx rho = rl(0.0);
+    const int start = N + 60 + (int)(2.0 * r.hi);
+    dd rho = mkdd(0.0);
     for (int n = start; n >= 1; --n) {
-      rho = z * cinv(rl(2.0 * n + 1) - z * rho);
-      if (n <= N) {
-        f[n * kFun + slot_re] = rho.re;
-        if (slot_im >= 0) f[n * kFun + slot_im] = rho.im;
-      }
+      rho = r / (mkdd(2.0 * n + 1) - r * rho);
+      if (n <= N) st(f + n * kRadD + 0, rho);
     }
-    const cplx iz = cinv(z);
-    cplx jm1 = ccos_(z) * iz, j = csin_(z) * iz;
+    dd jm1 = cs * ir, j = sn * ir;
     for (int n = 0; n <= N; ++n) {
       if (n > 0) {
-        const cplx rn = mk(f[n * kFun + slot_re], slot_im >= 0 ? f[n * kFun + slot_im] : 0.0);
+        const dd rn = ld(f + n * kRadD + 0);
         jm1 = j;
         j = rn * j;
       }
-      const cplx der = jm1 - scl(j * iz, (double)n);
-      f[n * kFun + slot_re] = j.re;
-      if (slot_im >= 0) f[n * kFun + slot_im] = j.im;
-      f[n * kFun + dslot_re] = der.re;
-      if (dslot_im >= 0) f[n * kFun + dslot_im] = der.im;
+      st(f + n * kRadD + 0, j);
+      st(f + n * kRadD + 2, jm1 - (j * ir) * (double)n);
     }
-  };
-  bessel_j(rl(r), 7, -1, 8, -1);  // j_n(r), real
-  bessel_j(sr, 9, 10, 11, 12);    // j_n(s r)
-  // h_n(r) = j_n(r) + i y_n(r), y_n by the upward recurrence (y_{-1} = sin r / r).
+  }
+  // y_n(r) upward from y_{-1} = sin r / r, y_0 = -cos r / r.
   {
-    const double ir = 1.0 / r;
-    double ym1 = sin(r) * ir, y = -cos(r) * ir;
+    dd ym1 = sn * ir, y = -(cs * ir);
     for (int n = 0; n <= N; ++n) {
       if (n > 0) {
-        const double yn = (2 * (n - 1) + 1) * ir * y - ym1;
+        const dd yn = (y * ir) * (double)(2 * n - 1) - ym1;
         ym1 = y;
         y = yn;
       }
-      const double jn = f[n * kFun + 7], jd = f[n * kFun + 8];
-      const double yd = ym1 - n * y * ir;
-      f[n * kFun + 3] = jn;
-      f[n * kFun + 4] = y;
-      f[n * kFun + 5] = jd;
-      f[n * kFun + 6] = yd;
+      st(f + n * kRadD + 4, y);
+      st(f + n * kRadD + 6, ym1 - (y * ir) * (double)n);
+    }
+  }
+  // j_n(s r), its derivative term, and j_n(s r) / (s r).
+  {
+    const cdd isr = ddm::inv(sr);
+    const double mag = fmax(fabs(sr.re.hi), fabs(sr.im.hi));
+    const int start = N + 60 + (int)(2.0 * mag);
+    cdd rho = mkc(0.0);
+    for (int n = start; n >= 1; --n) {
+      rho = sr * ddm::inv(mkc(2.0 * n + 1) - sr * rho);
+      if (n <= N) stc(f + n * kRadD + 8, rho);
+    }
+    cdd sz, cz;
+    ddm::c_sincos(sr, &sz, &cz);
+    cdd jm1 = cz * isr, j = sz * isr;
+    for (int n = 0; n <= N; ++n) {
+      if (n > 0) {
+        const cdd rn = ldc(f + n * kRadD + 8);
+        jm1 = j;
+        j = rn * j;
+      }
+      const cdd ji = j * isr;
+      stc(f + n * kRadD + 8, j);
+      stc(f + n * kRadD + 12, jm1 - ji * (double)n);
+      stc(f + n * kRadD + 16, ji);
     }
   }
 }
 
-// The eight surface integrals of one (job, i, k): J[out][a][b] with out 0 regular (j_n(r)),
-// 1 outgoing (h_n(r)), a, b in {M, N}, summed over the job's nodes in order (ebcm.py:145-186).
+// Normalized d_{mn}(theta), pi = m d / sin, tau = dd/dtheta, n = 0..N, m >= 0 (ebcm.py:68-100).
+__global__ void __launch_bounds__(128) tm_angular_kernel(TmArgs a) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.n_ang_total) return;
+  const int ji = owner(a.n_jobs, t, [&](int i) { return a.jobs[i].ang_node0; });
+  const TmJob jb = a.jobs[ji];
+  const TmGeom g = a.geoms[jb.geom];
+  const int q = (int)(t - jb.ang_node0), N = g.N, m = jb.m;
+  const double* ns = a.node + (g.node0 + q) * kNodeD;
+  const dd ct = ld(ns + 12), stt = ld(ns + 14);
+  const dd ist = mkdd(1.0) / stt;
+  double* f = a.ang + jb.ang0 + (int64_t)q * (N + 1) * kAngD;
+  dd am = mkdd(1.0);
+  for (int k = 1; k <= m; ++k) am = am * ddm::dd_sqrt(mkdd((double)(2 * k - 1)) / (double)(2 * k));
+  dd sp = mkdd(1.0);
+  for (int k = 0; k < m; ++k) sp = sp * stt;
+  dd dprev = mkdd(0.0), dcur = mkdd(0.0);
+  for (int n = 0; n <= N; ++n) {
+    dd dn;
+    if (n < m) dn = mkdd(0.0);
+    else if (n == m) dn = am * sp;
+    else if (n == m + 1) dn = ddm::dd_sqrt((double)(2 * m + 1)) * ct * dcur;
+    else
+      dn = ((ct * dcur) * (double)(2 * n - 1) -
+            ddm::dd_sqrt((double)(n - 1) * (n - 1) - (double)m * m) * dprev) /
+           ddm::dd_sqrt((double)n * n - (double)m * m);
+    dd tau = mkdd(0.0), pi = mkdd(0.0);
+    if (n >= (m > 1 ? m : 1)) {
+      const dd prev = n - 1 >= m ? dcur : mkdd(0.0);
+      tau = ((ct * dn) * (double)n - ddm::dd_sqrt((double)n * n - (double)m * m) * prev) * ist;
+      pi = (dn * (double)m) * ist;
+    }
+    st(f + n * kAngD + 0, dn);
+    st(f + n * kAngD + 2, pi);
+    st(f + n * kAngD + 4, tau);
+    dprev = dcur;
+    dcur = dn;
+  }
+}
+
+// The eight surface integrals of one (mode, i, k), out 0 regular (z = j_i(r)), 1 outgoing
+// (z = h_i(r) = j + i y), a, b in {M, N}. With zeta = z or [r z]'/r and the inner w, w' at s r,
+// the triple products n . (A_i x B_k) reduce to (ebcm.py:103-186, pi -> -pi for the outgoing
+// functions' phi-factor convention, g_i g_k taken out of the sum):
+//   MM = i z w (pi_i tau_k + tau_i pi_k)
+//   MN = z w' (pi_i pi_k + tau_i tau_k) - nu k(k+1) z w/(s r) tau_i d_k
+//   NM = -z' w (tau_i tau_k + pi_i pi_k) + nu i(i+1) (z/r) w d_i tau_k
+//   NN = i [z' w' (tau_i pi_k + pi_i tau_k) - nu (k(k+1) z' w/(s r) pi_i d_k
+//                                                + i(i+1) (z/r) w' d_i pi_k)]
 __global__ void __launch_bounds__(128) tm_surface_kernel(TmArgs a) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= a.n_pair_total) return;
-  int lo = 0, hi = a.n_jobs - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) / 2;
-    if (a.jobs[mid].pair0 <= t) lo = mid; else hi = mid - 1;
-  }
-  const TmJob jb = a.jobs[lo];
-  const int N = jb.N, m = jb.m, n0 = m > 1 ? m : 1, K = N - n0 + 1;
+  const int ji = owner(a.n_jobs, t, [&](int i) { return a.jobs[i].pair0; });
+  const TmJob jb = a.jobs[ji];
+  const TmGeom g = a.geoms[jb.geom];
+  const int N = g.N, m = jb.m, n0 = m > 1 ? m : 1, K = jb.K;
   const int pr = (int)(t - jb.pair0), i = n0 + pr / K, k = n0 + pr % K;
-  const double gi = sqrt((double)(2 * i + 1) / (4.0 * kPi * i * (i + 1)));
-  const double gk = sqrt((double)(2 * k + 1) / (4.0 * kPi * k * (k + 1)));
-  cplx J[2][2][2];
+  cdd J[8];
 #pragma unroll
-  for (int o = 0; o < 2; ++o)
-#pragma unroll
-    for (int p = 0; p < 2; ++p)
-#pragma unroll
-      for (int b = 0; b < 2; ++b) J[o][p][b] = rl(0.0);
-  const int nq = 2 * jb.n_theta;
+  for (int c = 0; c < 8; ++c) J[c] = mkc(0.0);
+  const double cki = (double)i * (i + 1), ckk = (double)k * (k + 1);
+  const int nq = 2 * g.n_theta;
   for (int q = 0; q < nq; ++q) {
-    const double* ns = a.node + (jb.node0 + q) * kNode;
-    const double r = ns[0], nut = ns[1], fac = ns[2];
-    const cplx sr = mk(ns[3], ns[4]);
-    const double* fi = a.fun + jb.fun0 + ((int64_t)q * (N + 1) + i) * kFun;
-    const double* fk = a.fun + jb.fun0 + ((int64_t)q * (N + 1) + k) * kFun;
-    // Inner functions of order k at s r: M = (0, i g w pi, -g w tau),
-    // N = (g k(k+1) w / (s r) d, g w' tau, i g w' pi).
-    const cplx w = mk(fk[9], fk[10]), wd = mk(fk[11], fk[12]);
-    const double dk = fk[0], pk = fk[1], tk = fk[2];
-    const cplx BM[3] = {rl(0.0), cti(scl(w, gk * pk)), scl(w, -gk * tk)};
-    const cplx BN[3] = {scl(w * cinv(sr), gk * k * (k + 1) * dk), scl(wd, gk * tk),
-                        cti(scl(wd, gk * pk))};
-    const double di = fi[0], pi = -fi[1], ti = fi[2];  // outgoing: pi -> -pi
+    const double* ns = a.node + (g.node0 + q) * kNodeD;
+    const dd ir = ld(ns + 2), nu = ld(ns + 4), fac = ld(ns + 6);
+    const double* ri = a.rad + g.rad0 + ((int64_t)q * (N + 1) + i) * kRadD;
+    const double* rk = a.rad + g.rad0 + ((int64_t)q * (N + 1) + k) * kRadD;
+    const double* ai = a.ang + jb.ang0 + ((int64_t)q * (N + 1) + i) * kAngD;
+    const double* ak = a.ang + jb.ang0 + ((int64_t)q * (N + 1) + k) * kAngD;
+    const dd di = ld(ai), pii = ld(ai + 2), ti = ld(ai + 4);
+    const dd dk = ld(ak), pik = ld(ak + 2), tk = ld(ak + 4);
+    const dd A1 = pii * tk + ti * pik, A2 = pii * pik + ti * tk;
+    const dd A3 = ti * dk, A4 = di * tk, A5 = pii * dk, A6 = di * pik;
+    const cdd w = ldc(rk + 8), wd = ldc(rk + 12), u = ldc(rk + 16);
+    const dd jr = ld(ri), jdr = ld(ri + 2), yr = ld(ri + 4), ydr = ld(ri + 6);
+#pragma unroll
     for (int o = 0; o < 2; ++o) {
-      const cplx z = o ? mk(fi[3], fi[4]) : rl(fi[7]);
-      const cplx zd = o ? mk(fi[5], fi[6]) : rl(fi[8]);
-      const cplx AM[3] = {rl(0.0), cti(scl(z, gi * pi)), scl(z, -gi * ti)};
-      const cplx AN[3] = {scl(z, gi * i * (i + 1) * di / r), scl(zd, gi * ti),
-                          cti(scl(zd, gi * pi))};
-      for (int p = 0; p < 2; ++p) {
-        const cplx* A = p ? AN : AM;
-        for (int b = 0; b < 2; ++b) {
-          const cplx* B = b ? BN : BM;
-          const cplx trip = (A[1] * B[2] - A[2] * B[1]) + scl(A[2] * B[0] - A[0] * B[2], nut);
-          J[o][p][b] = J[o][p][b] + scl(trip, fac);
-        }
-      }
+      const cdd z = o ? cdd{jr, yr} : cdd{jr, mkdd(0.0)};
+      const cdd zd = o ? cdd{jdr, ydr} : cdd{jdr, mkdd(0.0)};
+      const cdd zr = z * ir;
+      const cdd mm = ddm::times_i((z * w) * A1);
+      const cdd mn = (z * wd) * A2 - ((z * u) * A3) * (nu * ckk);
+      const cdd nm = ((zr * w) * A4) * (nu * cki) - (zd * w) * A2;
+      const cdd nn = ddm::times_i((zd * wd) * A1 -
+                                  (((zd * u) * A5) * ckk + ((zr * wd) * A6) * cki) * nu);
+      J[o * 4 + 0] = J[o * 4 + 0] + mm * fac;
+      J[o * 4 + 1] = J[o * 4 + 1] + mn * fac;
+      J[o * 4 + 2] = J[o * 4 + 2] + nm * fac;
+      J[o * 4 + 3] = J[o * 4 + 3] + nn * fac;
     }
   }
-  double2* out = reinterpret_cast<double2*>(a.J) + jb.J0;
+  // g_i g_k = sqrt((2i+1)(2k+1) / (16 pi^2 i(i+1) k(k+1))).
+  const dd pi2 = dd{kPiHi, kPiLo} * dd{kPiHi, kPiLo};
+  const dd gg = ddm::dd_sqrt((mkdd((double)(2 * i + 1) * (2 * k + 1)) / (pi2 * 16.0)) /
+                             (cki * ckk));
+  double* out = a.J + 4 * jb.J0;
   const int64_t KK = (int64_t)K * K, e = (int64_t)(i - n0) * K + (k - n0);
 #pragma unroll
-  for (int o = 0; o < 2; ++o)
-#pragma unroll
-    for (int p = 0; p < 2; ++p)
-#pragma unroll
-      for (int b = 0; b < 2; ++b)
-        out[((o * 2 + p) * 2 + b) * KK + e] = make_double2(J[o][p][b].re, J[o][p][b].im);
+  for (int c = 0; c < 8; ++c) stc(out + 4 * (c * KK + e), J[c] * gg);
 }
 
-// One job per block of 256 threads: Q^T (into the workspace as A) and the right-hand sides
-// -RgQ^T (as B), Q^T X = B by LU with partial pivoting (largest modulus, the first on ties)
-// applied to B as it goes, back substitution per column, T = X^T; and the mode's sums.
+namespace {
+
+struct Cd {  // complex double
+  double re, im;
+};
+__device__ __forceinline__ Cd cmul(Cd a, Cd b) {
+  return Cd{a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+}
+__device__ __forceinline__ Cd csub(Cd a, Cd b) { return Cd{a.re - b.re, a.im - b.im}; }
+__device__ __forceinline__ Cd cdiv(Cd a, Cd b) {
+  const double s = fmax(fabs(b.re), fabs(b.im));
+  const Cd bs{b.re / s, b.im / s};
+  const double d = bs.re * bs.re + bs.im * bs.im;
+  const Cd as{a.re / s, a.im / s};
+  return Cd{(as.re * bs.re + as.im * bs.im) / d, (as.im * bs.re - as.re * bs.im) / d};
+}
+
+// Block-wide max of v (blockDim.x = 256) through red; every thread gets the result.
+__device__ double block_max(double v, double* red) {
+  const int t = threadIdx.x;
+  red[t] = v;
+  __syncthreads();
+  for (int off = 128; off > 0; off >>= 1) {
+    if (t < off) red[t] = fmax(red[t], red[t + off]);
+    __syncthreads();
+  }
+  const double r = red[0];
+  __syncthreads();
+  return r;
+}
+
+// Applies the LU factors (row swaps piv in order, unit L, U) to column c of X (row-major n2 x n2
+// complex doubles), one column per thread.
+__device__ void lu_apply(const Cd* A, const int* piv, Cd* X, int n2, int c) {
+  for (int k = 0; k < n2; ++k) {
+    const int p = piv[k];
+    if (p != k) {
+      const Cd x = X[(int64_t)k * n2 + c];
+      X[(int64_t)k * n2 + c] = X[(int64_t)p * n2 + c];
+      X[(int64_t)p * n2 + c] = x;
+    }
+  }
+  for (int i = 1; i < n2; ++i) {
+    Cd v = X[(int64_t)i * n2 + c];
+    for (int j = 0; j < i; ++j) v = csub(v, cmul(A[(int64_t)i * n2 + j], X[(int64_t)j * n2 + c]));
+    X[(int64_t)i * n2 + c] = v;
+  }
+  for (int i = n2 - 1; i >= 0; --i) {
+    Cd v = X[(int64_t)i * n2 + c];
+    for (int j = i + 1; j < n2; ++j)
+      v = csub(v, cmul(A[(int64_t)i * n2 + j], X[(int64_t)j * n2 + c]));
+    X[(int64_t)i * n2 + c] = cdiv(v, A[(int64_t)i * n2 + i]);
+  }
+}
+
+}  // namespace
+
+// One mode per block of 256 threads. Workspace (doubles): Q^T and -P^T as complex double-double
+// (4 (2K)^2 each), the LU factors, X and the residual as complex doubles (2 (2K)^2 each).
 __global__ void __launch_bounds__(256) tm_solve_kernel(TmArgs a) {
   __shared__ double red_v[256];
   __shared__ int red_i[256];
   __shared__ double sums[2][256];
   const TmJob jb = a.jobs[blockIdx.x];
+  const TmGeom g = a.geoms[jb.geom];
   const int t = threadIdx.x;
-  const int N = jb.N, m = jb.m, n0 = m > 1 ? m : 1, K = N - n0 + 1, n2 = 2 * K;
-  const int64_t KK = (int64_t)K * K;
-  const double2* J = reinterpret_cast<const double2*>(a.J) + jb.J0;
-  double2* A = reinterpret_cast<double2*>(a.work) + jb.W0;
-  double2* B = A + (int64_t)n2 * n2;
-  const cplx s = mk(jb.s_re, jb.s_im);
-  const cplx mis = scl(cti(s), -1.0), mi = mk(0.0, -1.0);
-  auto Jv = [&](int o, int p, int b, int e) {
-    const double2 v = J[((o * 2 + p) * 2 + b) * KK + e];
-    return mk(v.x, v.y);
-  };
+  const int K = jb.K, n2 = 2 * K;
+  const int64_t KK = (int64_t)K * K, NN = (int64_t)n2 * n2;
+  const double* J = a.J + 4 * jb.J0;
+  double* Qd = a.work + jb.W0;  // Q^T, dd complex
+  double* Bd = Qd + 4 * NN;     // -P^T, dd complex
+  Cd* A = reinterpret_cast<Cd*>(Bd + 4 * NN);
+  Cd* X = A + NN;
+  Cd* R = X + NN;
+  int* piv = a.piv + jb.piv0;
+  const cdd s = mkc(g.s_re, g.s_im);
+  const cdd mis = -ddm::times_i(s), mi = mkc(0.0, -1.0);
+  auto Jv = [&](int o, int p, int b, int64_t e) { return ldc(J + 4 * (((o * 2 + p) * 2 + b) * KK + e)); };
   // Q11 = -i s J12 - i J21, Q12 = -i s J11 - i J22, Q21 = -i s J22 - i J11,
-  // Q22 = -i s J21 - i J12 (ebcm.py:189-195); A = Q^T (outgoing), B = -RgQ^T (regular).
-  for (int idx = t; idx < n2 * n2; idx += blockDim.x) {
-    const int row = idx / n2, col = idx % n2;  // element (row, col) of Q
+  // Q22 = -i s J21 - i J12 (ebcm.py:189-195); element (row, col) of Q goes to (col, row).
+  for (int64_t idx = t; idx < NN; idx += blockDim.x) {
+    const int row = (int)(idx / n2), col = (int)(idx % n2);
     const int bi = row >= K, bk = col >= K;
-    const int e = (row - bi * K) * K + (col - bk * K);
-    cplx q[2];
+    const int64_t e = (int64_t)(row - bi * K) * K + (col - bk * K);
+    cdd q[2];
     for (int o = 0; o < 2; ++o) {
-      cplx v;
-      if (!bi && !bk) v = mis * Jv(o, 0, 1, e) + mi * Jv(o, 1, 0, e);
-      else if (!bi && bk) v = mis * Jv(o, 0, 0, e) + mi * Jv(o, 1, 1, e);
-      else if (bi && !bk) v = mis * Jv(o, 1, 1, e) + mi * Jv(o, 0, 0, e);
-      else v = mis * Jv(o, 1, 0, e) + mi * Jv(o, 0, 1, e);
-      q[o] = v;
+      if (!bi && !bk) q[o] = mis * Jv(o, 0, 1, e) + mi * Jv(o, 1, 0, e);
+      else if (!bi && bk) q[o] = mis * Jv(o, 0, 0, e) + mi * Jv(o, 1, 1, e);
+      else if (bi && !bk) q[o] = mis * Jv(o, 1, 1, e) + mi * Jv(o, 0, 0, e);
+      else q[o] = mis * Jv(o, 1, 0, e) + mi * Jv(o, 0, 1, e);
     }
-    A[(int64_t)col * n2 + row] = make_double2(q[1].re, q[1].im);
-    B[(int64_t)col * n2 + row] = make_double2(-q[0].re, -q[0].im);
+    const int64_t tr = (int64_t)col * n2 + row;
+    stc(Qd + 4 * tr, q[1]);
+    stc(Bd + 4 * tr, -q[0]);
+    A[tr] = Cd{q[1].re.hi + q[1].re.lo, q[1].im.hi + q[1].im.lo};
+    X[tr] = Cd{-(q[0].re.hi + q[0].re.lo), -(q[0].im.hi + q[0].im.lo)};
   }
   __syncthreads();
-  auto at = [&](double2* M, int r, int c) -> double2& { return M[(int64_t)r * n2 + c]; };
+  // LU of A with partial pivoting (the largest modulus, the first row on ties).
   for (int kk = 0; kk < n2; ++kk) {
-    // Pivot: the largest |A[r][kk]|, r >= kk, the first row on ties.
     double best = -1.0;
     int bi = kk;
     for (int r = kk + t; r < n2; r += blockDim.x) {
-      const double2 v = at(A, r, kk);
-      const double mag = hypot(v.x, v.y);
+      const Cd v = A[(int64_t)r * n2 + kk];
+      const double mag = hypot(v.re, v.im);
       if (mag > best) {
         best = mag;
         bi = r;
@@ -275,73 +389,77 @@ __global__ void __launch_bounds__(256) tm_solve_kernel(TmArgs a) {
       __syncthreads();
     }
     const int p = red_i[0];
-    if (red_v[0] == 0.0) {
-      if (t == 0) atomicExch(a.err, 1u);  // singular Q
+    const bool singular = !(red_v[0] > 0.0);
+    __syncthreads();
+    if (singular) {
+      if (t == 0) atomicExch(a.err, 1u);
       return;
     }
-    if (p != kk) {
+    if (t == 0) piv[kk] = p;
+    if (p != kk)
       for (int c = t; c < n2; c += blockDim.x) {
-        const double2 x = at(A, kk, c);
-        at(A, kk, c) = at(A, p, c);
-        at(A, p, c) = x;
-        const double2 y = at(B, kk, c);
-        at(B, kk, c) = at(B, p, c);
-        at(B, p, c) = y;
+        const Cd x = A[(int64_t)kk * n2 + c];
+        A[(int64_t)kk * n2 + c] = A[(int64_t)p * n2 + c];
+        A[(int64_t)p * n2 + c] = x;
       }
-    }
     __syncthreads();
-    const double2 pv = at(A, kk, kk);
-    const cplx ipv = cinv(mk(pv.x, pv.y));
-    // Multipliers, then the trailing update of A and of every column of B.
-    for (int r = kk + 1 + t; r < n2; r += blockDim.x) {
-      const double2 v = at(A, r, kk);
-      const cplx fct = mk(v.x, v.y) * ipv;
-      at(A, r, kk) = make_double2(fct.re, fct.im);
-    }
+    const Cd pv = A[(int64_t)kk * n2 + kk];
+    for (int r = kk + 1 + t; r < n2; r += blockDim.x)
+      A[(int64_t)r * n2 + kk] = cdiv(A[(int64_t)r * n2 + kk], pv);
     __syncthreads();
-    const int rows = n2 - kk - 1, cols = (n2 - kk - 1) + n2;
-    for (int idx = t; idx < rows * cols; idx += blockDim.x) {
-      const int r = kk + 1 + idx / cols, c = idx % cols;
-      const double2 fv = at(A, r, kk);
-      const cplx fct = mk(fv.x, fv.y);
-      if (c < n2 - kk - 1) {
-        const int cc = kk + 1 + c;
-        const double2 u = at(A, kk, cc), x = at(A, r, cc);
-        const cplx y = mk(x.x, x.y) - fct * mk(u.x, u.y);
-        at(A, r, cc) = make_double2(y.re, y.im);
-      } else {
-        const int cc = c - (n2 - kk - 1);
-        const double2 u = at(B, kk, cc), x = at(B, r, cc);
-        const cplx y = mk(x.x, x.y) - fct * mk(u.x, u.y);
-        at(B, r, cc) = make_double2(y.re, y.im);
-      }
+    const int w = n2 - kk - 1;
+    for (int idx = t; idx < w * w; idx += blockDim.x) {
+      const int r = kk + 1 + idx / w, c = kk + 1 + idx % w;
+      A[(int64_t)r * n2 + c] =
+          csub(A[(int64_t)r * n2 + c], cmul(A[(int64_t)r * n2 + kk], A[(int64_t)kk * n2 + c]));
     }
     __syncthreads();
   }
-  // Back substitution, one column per thread.
-  for (int c = t; c < n2; c += blockDim.x) {
-    for (int i = n2 - 1; i >= 0; --i) {
-      const double2 bv = at(B, i, c);
-      cplx x = mk(bv.x, bv.y);
-      for (int j = i + 1; j < n2; ++j) {
-        const double2 u = at(A, i, j), v = at(B, j, c);
-        x = x - mk(u.x, u.y) * mk(v.x, v.y);
-      }
-      const double2 d = at(A, i, i);
-      x = x * cinv(mk(d.x, d.y));
-      at(B, i, c) = make_double2(x.re, x.im);
-    }
-  }
+  for (int c = t; c < n2; c += blockDim.x) lu_apply(A, piv, X, n2, c);
   __syncthreads();
-  // T[i][k] = X[k][i]: T's rows are B's columns.
+  // Residual sweeps: R = -P^T - Q^T X with the products and sums in double-double.
+  double rel = 0.0;
+  for (int sweep = 0; sweep < a.max_sweeps; ++sweep) {
+    double xm = 0.0, rm = 0.0;
+    for (int64_t idx = t; idx < NN; idx += blockDim.x) {
+      const int i = (int)(idx / n2), c = (int)(idx % n2);
+      cdd acc = ldc(Bd + 4 * idx);
+      const double* qrow = Qd + 4 * (int64_t)i * n2;
+      for (int j = 0; j < n2; ++j) {
+        const cdd qv = ldc(qrow + 4 * j);
+        const Cd x = X[(int64_t)j * n2 + c];
+        acc = acc - cdd{qv.re * x.re - qv.im * x.im, qv.re * x.im + qv.im * x.re};
+      }
+      const Cd rv{acc.re.hi + acc.re.lo, acc.im.hi + acc.im.lo};
+      R[idx] = rv;
+      const Cd xv = X[idx];
+      xm = fmax(xm, fmax(fabs(xv.re), fabs(xv.im)));
+    }
+    __syncthreads();
+    for (int c = t; c < n2; c += blockDim.x) lu_apply(A, piv, R, n2, c);
+    __syncthreads();
+    for (int64_t idx = t; idx < NN; idx += blockDim.x) {
+      const Cd d = R[idx];
+      rm = fmax(rm, fmax(fabs(d.re), fabs(d.im)));
+      X[idx] = Cd{X[idx].re + d.re, X[idx].im + d.im};
+    }
+    xm = block_max(xm, red_v);
+    rm = block_max(rm, red_v);
+    rel = xm > 0.0 ? rm / xm : 0.0;
+    if (!(rel > 0x1p-54)) break;
+  }
+  // T[i][k] = X[k][i].
   double ext = 0.0, sca = 0.0;
-  double2* T = a.T ? reinterpret_cast<double2*>(a.T) + jb.T0 : nullptr;
-  for (int idx = t; idx < n2 * n2; idx += blockDim.x) {
-    const int i = idx / n2, k = idx % n2;
-    const double2 v = at(B, k, i);
-    if (T) T[idx] = v;
-    if (i == k) ext -= v.x;
-    sca += v.x * v.x + v.y * v.y;
+  double* T = a.T ? a.T + 2 * jb.T0 : nullptr;
+  for (int64_t idx = t; idx < NN; idx += blockDim.x) {
+    const int i = (int)(idx / n2), k = (int)(idx % n2);
+    const Cd v = X[(int64_t)k * n2 + i];
+    if (T) {
+      T[2 * idx] = v.re;
+      T[2 * idx + 1] = v.im;
+    }
+    if (i == k) ext -= v.re;
+    sca += v.re * v.re + v.im * v.im;
   }
   sums[0][t] = ext;
   sums[1][t] = sca;
@@ -354,14 +472,16 @@ __global__ void __launch_bounds__(256) tm_solve_kernel(TmArgs a) {
     __syncthreads();
   }
   if (t == 0) {
-    a.sums[2 * blockIdx.x] = sums[0][0];
-    a.sums[2 * blockIdx.x + 1] = sums[1][0];
+    a.sums[3 * blockIdx.x] = sums[0][0];
+    a.sums[3 * blockIdx.x + 1] = sums[1][0];
+    a.sums[3 * blockIdx.x + 2] = rel;
   }
 }
 
 void launch_tmatrix(const TmArgs& a, cudaStream_t s) {
   if (a.n_jobs <= 0) return;
-  tm_functions_kernel<<<(unsigned)((a.n_node_total + 127) / 128), 128, 0, s>>>(a);
+  tm_geom_kernel<<<(unsigned)((a.n_node_total + 127) / 128), 128, 0, s>>>(a);
+  tm_angular_kernel<<<(unsigned)((a.n_ang_total + 127) / 128), 128, 0, s>>>(a);
   tm_surface_kernel<<<(unsigned)((a.n_pair_total + 127) / 128), 128, 0, s>>>(a);
   tm_solve_kernel<<<a.n_jobs, 256, 0, s>>>(a);
 }

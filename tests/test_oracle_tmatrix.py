@@ -100,3 +100,26 @@ def test_a_sphere_gives_the_mie_coefficients():
             assert abs(T[k + i, k + i] + mie["a"][n0 + i - 1]) <= 1e-13
         off = T - np.diag(np.diag(T))
         assert np.abs(off).max() <= 1e-13
+
+
+@pytest.mark.parametrize("r", FIXED, ids=[r["case"] for r in FIXED])
+def test_quadruple_precision_oracle_matches_every_record(r):
+    """The quadruple-precision EBCM (oracle/oracle_tmatrix_q.cpp) reproduces every record,
+    the elongated and flattened shapes included, to the records' double rounding: 1e-14 of
+    the largest element of the record's modes, Q within 1e-14."""
+    x, eps, s, N, nt = r["x"], r["eps"], complex(*r["m"]), r["n_terms"], r["n_theta"]
+    modes = _modes(r)
+    Ts = {mm: O.tmatrix_mode(x, eps, s, mm, N, nt, quad=True) for mm in modes}
+    big = max(np.abs(T).max() for T in Ts.values())
+    for mm, T in Ts.items():
+        k = T.shape[0] // 2
+        got = {"diag11": [T[i, i] for i in range(k)], "diag22": [T[k + i, k + i] for i in range(k)],
+               "col": [T[i, 0] for i in range(2 * k)] + [T[i, k] for i in range(2 * k)]}
+        for stem, g in got.items():
+            for i, gv in enumerate(g):
+                ref = complex(val(r[f"t{mm}_{stem}_re"], i), val(r[f"t{mm}_{stem}_im"], i))
+                assert abs(gv - ref) <= 1e-14 * big, (mm, stem, i)
+    if r["n_terms"] <= 14:
+        qe, qs = O.spheroid_q(x, eps, s, N, nt, quad=True)
+        assert abs(qe - val(r["q_ext"], 0)) <= 1e-14 * val(r["q_ext"], 0)
+        assert abs(qs - val(r["q_sca"], 0)) <= 1e-14 * val(r["q_sca"], 0)
