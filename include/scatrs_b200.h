@@ -216,6 +216,29 @@ int scatrs_spheroid_efficiencies(int64_t n, const double* x, const double* aspec
                                  const double* m, double rtol, double* q, int32_t* n_terms,
                                  int32_t* n_theta, char* err, size_t err_len);
 
+/*
+ * Randomly oriented spheroids (TMatrix::compute and its solution's efficiencies() and greek(),
+ * tmatrix/mod.rs:221-362, 437-491; the orientation average random.rs:85-335): n spheroids in one
+ * batch. n_terms / n_theta > 0 fix N / n_theta (TMatrixOptions::n_terms, n_theta), 0 converges
+ * them to rtol. eff[5 n]: Q_ext, Q_sca, Q_abs, Q_back, g (Q_back and g from the averaged Greek
+ * expansion, exact to 2N). greek[6 n (greek_order + 1)] (alpha1..alpha4, beta1, beta2, each
+ * zero above 2N), normalized (alpha1_0 = 1) or unnormalized (times Q_sca); greek_order -1 for
+ * none. n_terms, n_theta, error_estimate (the largest relative correction of the last refinement
+ * sweep over the modes) may be NULL. N is limited to 120 here.
+ */
+typedef struct scatrs_spheroid_options {
+  double rtol;
+  int32_t n_terms;
+  int32_t n_theta;
+  int32_t greek_order;
+  int32_t normalized;
+} scatrs_spheroid_options;
+
+int scatrs_spheroid_compute(int64_t n, const double* x, const double* aspect_ratio,
+                            const double* m, const scatrs_spheroid_options* options, double* eff,
+                            double* greek, int32_t* n_terms, int32_t* n_theta,
+                            double* error_estimate, char* err, size_t err_len);
+
 /* Layered spheres (scatrs/src/layered/mod.rs; Particle::LayeredSphere,
  * scatrs/src/ensemble/mod.rs:58-65): n_layers layers, the core first; per distribution the
  * n_layers - 1 outer radii of layers 0..L-2 as fractions of the particle's radius (nondecreasing

@@ -412,3 +412,37 @@ def spheroid_converged(x: float, eps: float, s: complex, rtol: float = 1e-8):
     if st != 0:
         raise OracleError(st, "spheroid_converged")
     return q, n.value, nth.value
+
+
+def tmatrix_modes(x: float, eps: float, s: complex, n: int, n_theta: int, quad: bool = False):
+    """Every mode's T-matrix (m = 0..n) of a spheroid."""
+    return [tmatrix_mode(x, eps, s, m, n, n_theta, quad) for m in range(n + 1)]
+
+
+def _flat_modes(modes) -> np.ndarray:
+    return np.ascontiguousarray(np.concatenate([np.ascontiguousarray(t).reshape(-1)
+                                                for t in modes])).view(np.float64)
+
+
+def random_orientation(modes, mu) -> np.ndarray:
+    """The orientation-averaged phase matrix (6, n_mu): F11, F12, F22, F33, F34, F44 in 1/k^2
+    per steradian, of the T-matrix modes 0..N."""
+    n = len(modes) - 1
+    mu = np.ascontiguousarray(mu, dtype=np.float64)
+    f = np.zeros(6 * mu.size)
+    fn = lib().orc_random_orientation
+    fn.argtypes = [ctypes.c_int, _PD, _PD, ctypes.c_int, _PD]
+    fn(n, _p(_flat_modes(modes)), _p(mu), mu.size, _p(f))
+    return f.reshape(6, mu.size)
+
+
+def random_greek(modes, order: int) -> np.ndarray:
+    """The unnormalized Greek coefficients (6, L + 1), L = min(order, 2N): alpha1..alpha4,
+    beta1, beta2 of the average."""
+    n = len(modes) - 1
+    L = min(order, 2 * n)
+    out = np.zeros(6 * (L + 1))
+    fn = lib().orc_random_greek
+    fn.argtypes = [ctypes.c_int, _PD, ctypes.c_int, _PD]
+    fn(n, _p(_flat_modes(modes)), order, _p(out))
+    return out.reshape(6, L + 1)

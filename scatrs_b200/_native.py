@@ -45,6 +45,11 @@ class Component(ctypes.Structure):
                 ("weight", _D), ("m", _PD)]
 
 
+class SpheroidOptions(ctypes.Structure):
+    _fields_ = [("rtol", _D), ("n_terms", _I32), ("n_theta", _I32), ("greek_order", _I32),
+                ("normalized", _I32)]
+
+
 class FixedOptions(ctypes.Structure):
     _fields_ = [("n_nodes", _I32), ("greek_order", _I32), ("normalized", _I32),
                 ("allow_unvalidated", _I32)]
@@ -76,6 +81,8 @@ SYMBOLS = {
     "scatrs_spheroid_tmatrix": (ctypes.c_int, [_D, _D, _PD, _I32, _I32, _I32, _PD, _CP, _SZ]),
     "scatrs_spheroid_efficiencies": (ctypes.c_int, [_I64, _PD, _PD, _PD, _D, _PD, _VP, _VP, _CP,
                                                     _SZ]),
+    "scatrs_spheroid_compute": (ctypes.c_int, [_I64, _PD, _PD, _PD, ctypes.POINTER(SpheroidOptions),
+                                               _PD, _PD, _VP, _VP, _PD, _CP, _SZ]),
     "scatrs_check_errors": (ctypes.c_int, [_VP, _CP, _SZ]),
     "scatrs_mie": (ctypes.c_int, [_PD, _PD, _I64, _I32, _PI64, _PI64, _PD, _PD, _CP, _SZ]),
     "scatrs_mie_static": (ctypes.c_int, [_VP, _VP, _I64, _I32, _I64, _VP, _VP, _VP, _VP, _VP,
@@ -394,6 +401,29 @@ def spheroid_efficiencies(x, aspect_ratio, m, rtol: float = 1e-8):
                                                float(rtol), _p(q), n_terms.ctypes.data,
                                                n_theta.ctypes.data, err, 1024), err)
     return q, n_terms, n_theta
+
+
+def spheroid_compute(x, aspect_ratio, m, rtol: float = 1e-8, n_terms: int = 0, n_theta: int = 0,
+                     greek_order: int = -1, normalized: bool = True) -> dict:
+    """Randomly oriented spheroids: efficiencies (n, 5) = Q_ext, Q_sca, Q_abs, Q_back, g; Greek
+    coefficients (n, 6, order + 1) if greek_order >= 0; the N and n_theta used and the
+    refinement's error estimate."""
+    require_device()
+    x = np.ascontiguousarray(np.atleast_1d(x), dtype=np.float64)
+    eps = np.ascontiguousarray(np.broadcast_to(np.asarray(aspect_ratio, dtype=np.float64), x.shape))
+    mm = np.ascontiguousarray(np.broadcast_to(np.asarray(m, dtype=np.complex128), x.shape))
+    eff = np.zeros((x.size, 5))
+    greek = np.zeros((x.size, 6, greek_order + 1)) if greek_order >= 0 else None
+    nt = np.zeros(x.size, dtype=np.int32)
+    nth = np.zeros(x.size, dtype=np.int32)
+    est = np.zeros(x.size)
+    o = SpheroidOptions(rtol, n_terms, n_theta, greek_order, int(normalized))
+    err = ctypes.create_string_buffer(1024)
+    _check(load().scatrs_spheroid_compute(x.size, _p(x), _p(eps), _p(mm.view(np.float64)),
+                                          ctypes.byref(o), _p(eff), _p(greek), nt.ctypes.data,
+                                          nth.ctypes.data, _p(est), err, 1024), err)
+    return {"efficiencies": eff, "greek": greek, "n_terms": nt, "n_theta": nth,
+            "error_estimate": est}
 
 
 def check_errors(stream: int = 0) -> None:

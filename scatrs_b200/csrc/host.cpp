@@ -159,6 +159,7 @@ struct Context {
   // Spheroid T-matrices.
   DevBuf tm_geoms, tm_jobs, tm_rules, tm_node, tm_rad, tm_ang, tm_J, tm_work, tm_piv, tm_T, tm_sums,
       tm_err;
+  DevBuf ro_sph, ro_rank, ro_w, ro_part, ro_f, ro_greek, ro_mu, ro_proj;
   std::map<int64_t, std::vector<double>> dd_rules;  // n -> per node x (hi, lo), w (hi, lo)
   std::vector<int> chunk_n_host;
   int* pinned_chunk_n = nullptr;
@@ -1473,11 +1474,18 @@ const std::vector<double>& dd_rule(Context& c, int64_t n) {
 // spheroid at the same N and n_theta share one geometry (nodes and radial functions). Per
 // spec j: sums[3 j] = -Re tr T, sums[3 j + 1] = sum |T|^2, sums[3 j + 2] = the refinement's
 // last relative correction; each T (row-major (2K)^2 complex) into t_out if given.
+//
+// With greek_out, every spheroid's specs must be its modes 0..N in order: its orientation
+// average (random.cu) then runs on the device-resident T, and greek_out gets, per spheroid in
+// order, the unnormalized Greek coefficients [6][2N + 1] (alpha1_0 = C_sca / (4 pi), 1/k^2).
 void run_tmatrices(Context& c, const std::vector<TmSpec>& specs, std::vector<double>& sums,
-                   std::vector<std::vector<double>>* t_out, cudaStream_t s) {
+                   std::vector<std::vector<double>>* t_out, cudaStream_t s,
+                   std::vector<std::vector<double>>* greek_out = nullptr) {
   sums.assign(3 * specs.size(), 0.0);
   if (t_out) t_out->assign(specs.size(), {});
+  if (greek_out) greek_out->clear();
   constexpr double kBudget = 8.0e9;  // bytes of device workspace per batch
+  const bool ro = greek_out != nullptr;
   auto same_geom = [](const TmSpec& p, const TmSpec& q) {
     return p.x == q.x && p.eps == q.eps && p.s_re == q.s_re && p.s_im == q.s_im && p.N == q.N &&
            p.n_theta == q.n_theta;
@@ -1494,12 +1502,23 @@ void run_tmatrices(Context& c, const std::vector<TmSpec>& specs, std::vector<dou
     for (; j1 < specs.size(); ++j1) {
       const TmSpec& t = specs[j1];
       check_tm_spec(t);
-      const bool new_geom = j1 == j0 || !same_geom(specs[j1 - 1], t);
+      const bool new_geom = j1 == j0 || t.m == 0 || !same_geom(specs[j1 - 1], t);
       const int K = t.N - std::max(t.m, 1) + 1, n2 = 2 * K, nq = 2 * t.n_theta;
       double b = 8.0 * ((double)nq * (t.N + 1) * 6 + 32.0 * K * K + 14.0 * n2 * n2 +
-                        (t_out ? 2.0 * n2 * n2 : 0.0)) + 4.0 * n2;
+                        (t_out || ro ? 2.0 * n2 * n2 : 0.0)) + 4.0 * n2;
       if (new_geom) b += 8.0 * ((double)nq * 16 + (double)nq * (t.N + 1) * 20);
-      if (j1 > j0 && bytes + b > kBudget) break;
+      if (ro && new_geom) {
+        if (t.m != 0 || t.N > kRoMaxN)
+          throw Failure{SCATRS_INVALID_INPUT,
+                        "the orientation average needs the modes 0..N in order and N <= " +
+                            std::to_string(kRoMaxN)};
+        const double n1 = t.N + 1, S = 2 * t.N + 1, Q = 2 * t.N + 3, q = 2 * t.N + 1;
+        b += 16.0 * (4 * n1 * n1 * S + Q * 4 * S * n1 + Q * 16 * q) + 8.0 * 12 * q;
+      }
+      if (ro && !new_geom && t.m != specs[j1 - 1].m + 1)
+        throw Failure{SCATRS_INVALID_INPUT, "the orientation average needs the modes 0..N in order"};
+      // Batches break between spheroids when their modes must stay together.
+      if (j1 > j0 && bytes + b > kBudget && (!ro || new_geom)) break;
       bytes += b;
       if (new_geom) {
         if (!rule_at.count(nq)) {
@@ -1557,7 +1576,7 @@ void run_tmatrices(Context& c, const std::vector<TmSpec>& specs, std::vector<dou
     a.J = c.tm_J.as<double>(4 * (size_t)J);
     a.work = c.tm_work.as<double>((size_t)W);
     a.piv = c.tm_piv.as<int>((size_t)P);
-    a.T = t_out ? c.tm_T.as<double>(2 * (size_t)T) : nullptr;
+    a.T = t_out || ro ? c.tm_T.as<double>(2 * (size_t)T) : nullptr;
     a.sums = c.tm_sums.as<double>(3 * jobs.size());
     a.err = c.tm_err.as<unsigned>(1);
     a.max_sweeps = 4;
@@ -1569,6 +1588,71 @@ void run_tmatrices(Context& c, const std::vector<TmSpec>& specs, std::vector<dou
     SB_CUDA(cudaMemsetAsync(a.err, 0, sizeof(unsigned), s));
     timed_launch(K_UNITS, s, [&] { launch_tmatrix(a, s); });
     SB_CUDA(cudaGetLastError());
+    std::vector<double> greek_all;
+    std::vector<RoSph> sph;
+    if (ro) {
+      RoArgs r{};
+      std::vector<double> mus;
+      std::vector<const double*> projs;
+      int64_t rank = 0, w = 0, part = 0, f = 0, g = 0;
+      for (size_t k = 0; k < jobs.size(); ++k) {
+        if (jobs[k].m != 0) continue;
+        const TmGeom& gm = geoms[jobs[k].geom];
+        RoSph e{};
+        e.N = gm.N;
+        e.L = 2 * gm.N;
+        e.nq = gm.N + (e.L + 2) / 2;
+        e.job0 = (int)k;
+        const int64_t n1 = e.N + 1, S = 2 * e.N + 1, Q = 2 * e.N + 3;
+        e.rank0 = rank;
+        e.w0 = w;
+        e.part0 = part;
+        e.f0 = f;
+        e.g0 = g;
+        e.mu0 = (int64_t)mus.size();
+        e.t_rank = r.n_rank;
+        e.t_w = r.n_w;
+        e.t_phi = r.n_phi;
+        e.t_f = r.n_f;
+        e.t_g = r.n_g;
+        rank += 2 * 4 * n1 * n1 * S;
+        w += 2 * Q * 4 * S * n1;
+        part += 2 * Q * 16 * e.nq;
+        f += 6 * e.nq;
+        g += 6 * (e.L + 1);
+        r.n_rank += (int64_t)e.N * e.N;
+        r.n_w += Q * 2 * e.N;
+        r.n_phi += Q * e.nq;
+        r.n_f += e.nq;
+        r.n_g += e.L + 1;
+        const auto& rl = rule(c, e.nq);
+        mus.insert(mus.end(), rl.first.begin(), rl.first.end());
+        projs.push_back(projector(c, e.nq, e.L, s).d.as<double>(0));
+        sph.push_back(e);
+      }
+      r.sph = c.ro_sph.as<RoSph>(sph.size());
+      r.n_sph = (int)sph.size();
+      r.jobs = a.jobs;
+      r.T = a.T;
+      r.rank = c.ro_rank.as<double>((size_t)rank);
+      r.w = c.ro_w.as<double>((size_t)w);
+      r.part = c.ro_part.as<double>((size_t)part);
+      r.f = c.ro_f.as<double>((size_t)f);
+      r.greek = c.ro_greek.as<double>((size_t)g);
+      double* mu_d = c.ro_mu.as<double>(mus.size());
+      const double** proj_d = c.ro_proj.as<const double*>(projs.size());
+      r.mu = mu_d;
+      r.proj = proj_d;
+      SB_CUDA(cudaMemcpyAsync((void*)r.sph, sph.data(), sph.size() * sizeof(RoSph),
+                              cudaMemcpyHostToDevice, s));
+      SB_CUDA(cudaMemcpyAsync(mu_d, mus.data(), mus.size() * 8, cudaMemcpyHostToDevice, s));
+      SB_CUDA(cudaMemcpyAsync((void*)proj_d, projs.data(), projs.size() * sizeof(double*),
+                              cudaMemcpyHostToDevice, s));
+      timed_launch(K_PROJ, s, [&] { launch_random(r, s); });
+      SB_CUDA(cudaGetLastError());
+      greek_all.resize((size_t)g);
+      SB_CUDA(cudaMemcpyAsync(greek_all.data(), r.greek, (size_t)g * 8, cudaMemcpyDeviceToHost, s));
+    }
     unsigned flag = 0;
     SB_CUDA(cudaMemcpyAsync(sums.data() + 3 * j0, a.sums, 3 * jobs.size() * 8,
                             cudaMemcpyDeviceToHost, s));
@@ -1580,6 +1664,8 @@ void run_tmatrices(Context& c, const std::vector<TmSpec>& specs, std::vector<dou
     }
     SB_CUDA(cudaStreamSynchronize(s));
     if (flag) throw Failure{SCATRS_INVALID_INPUT, "a spheroid's Q matrix is singular"};
+    for (const RoSph& e : sph)
+      greek_out->emplace_back(greek_all.begin() + e.g0, greek_all.begin() + e.g0 + 6 * (e.L + 1));
     if (t_out)
       for (size_t k = 0; k < jobs.size(); ++k) {
         const int n2 = 2 * jobs[k].K;
@@ -1601,6 +1687,142 @@ int tm_theta_of(int n, double eps, double rtol) {
   const int shape =
       h <= 1.0 ? 0 : (int)std::ceil(std::log(1e4 / rtol) / (2.0 * std::log((h + 1.0) / (h - 1.0))));
   return std::max(2 * n, shape);
+}
+
+// One spheroid's converged solution: N, n_theta, the efficiencies (tmatrix/mod.rs:437-462:
+// Q_back = 4 pi F11(180 deg) / (pi x^2) and g = alpha1_1 / (3 alpha1_0) from the Greek
+// expansion, NaN without it), the raw Greek coefficients [6][2N + 1] and the largest last
+// relative correction of the modes' refinement.
+struct SpheroidResult {
+  int n = 0, nth = 0;
+  double q_ext = 0, q_sca = 0, q_abs = 0, q_back = NAN, g = NAN, err_est = 0;
+  std::vector<double> greek;
+};
+
+// The T-matrices of n spheroids converged as driver.rs:343-420 converges them: N grown by
+// max(N/8, 2) on mode 0 until its cross sections settle to rtol, then n_theta by a tenth (each
+// loop skipped when n_fixed / theta_fixed > 0 fixes it), both within their caps; then every mode
+// at the final N and n_theta, with the orientation average if `greek`. All spheroids of a step
+// run as one batch of device work.
+void spheroid_solve(Context& c, int64_t n, const double* x, const double* aspect_ratio,
+                    const double* m, double rtol, int n_fixed, int theta_fixed, bool greek,
+                    std::vector<SpheroidResult>& out, cudaStream_t s) {
+  if (!x || !aspect_ratio || !m)
+    throw Failure{SCATRS_INVALID_INPUT, "x, aspect_ratio and m are required"};
+  if (!(rtol >= 1e-13 && rtol <= 0.1))
+    throw Failure{SCATRS_INVALID_INPUT, "rtol must be in [1e-13, 0.1]"};
+  for (int64_t i = 0; i < n; ++i)
+    check_tm_spec({x[i], aspect_ratio[i], m[2 * i], m[2 * i + 1], 0,
+                   n_fixed > 0 ? n_fixed : 1, theta_fixed > 0 ? theta_fixed : 2});
+  struct St {
+    int n, nth, cap, th_cap, stage;  // stage 0: N, 1: n_theta, 2: done
+    double e, sc;
+  };
+  std::vector<St> st(n);
+  std::vector<TmSpec> specs;
+  auto theta = [&](int64_t i, int nn) {
+    return theta_fixed > 0 ? theta_fixed
+                           : std::min(tm_theta_of(nn, aspect_ratio[i], rtol), st[i].th_cap);
+  };
+  for (int64_t i = 0; i < n; ++i) {
+    const double mag = std::hypot(m[2 * i], m[2 * i + 1]);
+    const int start = tm_wiscombe(tm_x_max(x[i], aspect_ratio[i]));
+    st[i].cap = std::min(2 * tm_wiscombe(tm_x_max(x[i], aspect_ratio[i]) * std::max(mag, 1.0)) + 20,
+                         500);
+    st[i].n = n_fixed > 0 ? n_fixed : std::min(start, st[i].cap);
+    // mod.rs:293-300: n_theta's cap is 4 theta(start) + 40.
+    st[i].th_cap = 4 * tm_theta_of(std::min(start, st[i].cap), aspect_ratio[i], rtol) + 40;
+    st[i].nth = theta(i, st[i].n);
+    st[i].stage = n_fixed > 0 ? (theta_fixed > 0 ? 2 : 1) : 0;
+    if (st[i].stage < 2)
+      specs.push_back({x[i], aspect_ratio[i], m[2 * i], m[2 * i + 1], 0, st[i].n, st[i].nth});
+  }
+  std::vector<double> sums;
+  if (!specs.empty()) {
+    run_tmatrices(c, specs, sums, nullptr, s);
+    int64_t k = 0;
+    for (int64_t i = 0; i < n; ++i)
+      if (st[i].stage < 2) {
+        st[i].e = sums[3 * k];
+        st[i].sc = sums[3 * k + 1];
+        ++k;
+      }
+  }
+  for (;;) {
+    std::vector<int64_t> who;
+    specs.clear();
+    for (int64_t i = 0; i < n; ++i) {
+      St& z = st[i];
+      if (z.stage == 2) continue;
+      if ((z.stage == 0 && z.n >= z.cap) || (z.stage == 1 && z.nth >= z.th_cap)) {
+        char buf[200];
+        snprintf(buf, sizeof buf,
+                 "spheroid %lld: the cross sections did not settle to %g within N = %d, "
+                 "n_theta = %d",
+                 (long long)i, rtol, z.cap, z.th_cap);
+        throw Failure{SCATRS_NOT_CONVERGED, buf};
+      }
+      int nn = z.n, nt = z.nth;
+      if (z.stage == 0) {
+        nn = std::min(z.n + std::max(z.n / 8, 2), z.cap);
+        nt = theta(i, nn);
+      } else {
+        nt = std::min(z.nth + std::max(z.nth / 10, 2), z.th_cap);
+      }
+      specs.push_back({x[i], aspect_ratio[i], m[2 * i], m[2 * i + 1], 0, nn, nt});
+      who.push_back(i);
+    }
+    if (who.empty()) break;
+    run_tmatrices(c, specs, sums, nullptr, s);
+    for (size_t k = 0; k < who.size(); ++k) {
+      St& z = st[who[k]];
+      const double e1 = sums[3 * k], s1 = sums[3 * k + 1];
+      const double ch =
+          std::max(std::fabs(e1 - z.e) / std::fabs(e1), std::fabs(s1 - z.sc) / std::fabs(s1));
+      z.n = specs[k].N;
+      z.nth = specs[k].n_theta;
+      z.e = e1;
+      z.sc = s1;
+      if (ch < rtol) z.stage += 1;
+    }
+  }
+  // Every mode at the final N and n_theta.
+  specs.clear();
+  std::vector<int64_t> owner;
+  for (int64_t i = 0; i < n; ++i)
+    for (int mm = 0; mm <= st[i].n; ++mm) {
+      specs.push_back({x[i], aspect_ratio[i], m[2 * i], m[2 * i + 1], mm, st[i].n, st[i].nth});
+      owner.push_back(i);
+    }
+  std::vector<std::vector<double>> greeks;
+  run_tmatrices(c, specs, sums, nullptr, s, greek ? &greeks : nullptr);
+  out.assign(n, SpheroidResult{});
+  std::vector<double> ext(n, 0.0), sca(n, 0.0);
+  for (size_t k = 0; k < specs.size(); ++k) {
+    const double w = specs[k].m == 0 ? 1.0 : 2.0;
+    ext[owner[k]] += w * sums[3 * k];
+    sca[owner[k]] += w * sums[3 * k + 1];
+    out[owner[k]].err_est = std::max(out[owner[k]].err_est, sums[3 * k + 2]);
+  }
+  const double pi = 3.14159265358979323846;
+  for (int64_t i = 0; i < n; ++i) {
+    SpheroidResult& r = out[i];
+    const double area = pi * x[i] * x[i];
+    r.n = st[i].n;
+    r.nth = st[i].nth;
+    r.q_ext = 2.0 * pi * ext[i] / area;
+    r.q_sca = 2.0 * pi * sca[i] / area;
+    r.q_abs = r.q_ext - r.q_sca;
+    if (greek) {
+      r.greek = std::move(greeks[i]);
+      const int64_t len = 2 * (int64_t)r.n + 1;
+      const double a0 = r.greek[0];
+      r.g = a0 > 0.0 ? (len > 1 ? r.greek[1] : 0.0) / (3.0 * a0) : 0.0;
+      double f11 = 0.0;
+      for (int64_t l = 0; l < len; ++l) f11 += (l % 2 ? -1.0 : 1.0) * r.greek[l];
+      r.q_back = 4.0 * pi * f11 / area;
+    }
+  }
 }
 
 FixedCall g_last_call;  // for scatrs_check_errors
@@ -1854,101 +2076,62 @@ int scatrs_spheroid_efficiencies(int64_t n, const double* x, const double* aspec
                                  int32_t* n_theta, char* err, size_t err_len) {
   return guarded(err, err_len, [&] {
     if (n < 0) throw Failure{SCATRS_INVALID_INPUT, "negative sizes"};
-    if (!(rtol >= 1e-13 && rtol <= 0.1))
-      throw Failure{SCATRS_INVALID_INPUT, "rtol must be in [1e-13, 0.1]"};
     if (n == 0) return;
-    if (!x || !aspect_ratio || !m || !q)
-      throw Failure{SCATRS_INVALID_INPUT, "x, aspect_ratio, m and q are required"};
-    for (int64_t i = 0; i < n; ++i)
-      check_tm_spec({x[i], aspect_ratio[i], m[2 * i], m[2 * i + 1], 0, 1, 2});
+    if (!q) throw Failure{SCATRS_INVALID_INPUT, "q is required"};
     Context& c = context();
     std::lock_guard<std::mutex> lk(c.mtx);
-    cudaStream_t s = 0;
-    // Per spheroid: the loop in N on mode 0, then in n_theta (driver.rs:343-420).
-    struct St {
-      int n, nth, cap, th_cap, stage;  // stage 0: N, 1: n_theta, 2: done
-      double e, sc;
-    };
-    std::vector<St> st(n);
-    std::vector<TmSpec> specs;
-    auto theta = [&](int64_t i, int nn) {
-      return std::min(tm_theta_of(nn, aspect_ratio[i], rtol), st[i].th_cap);
-    };
+    std::vector<SpheroidResult> res;
+    spheroid_solve(c, n, x, aspect_ratio, m, rtol, 0, 0, false, res, 0);
     for (int64_t i = 0; i < n; ++i) {
-      const double mag = std::hypot(m[2 * i], m[2 * i + 1]);
-      st[i].cap = 2 * tm_wiscombe(tm_x_max(x[i], aspect_ratio[i]) * std::max(mag, 1.0)) + 20;
-      st[i].n = std::min(tm_wiscombe(tm_x_max(x[i], aspect_ratio[i])), st[i].cap);
-      // mod.rs:293-300: n_theta's cap is 4 theta(start) + 40.
-      st[i].th_cap = 4 * tm_theta_of(st[i].n, aspect_ratio[i], rtol) + 40;
-      st[i].nth = theta(i, st[i].n);
-      st[i].stage = 0;
-      specs.push_back({x[i], aspect_ratio[i], m[2 * i], m[2 * i + 1], 0, st[i].n, st[i].nth});
+      q[3 * i] = res[i].q_ext;
+      q[3 * i + 1] = res[i].q_sca;
+      q[3 * i + 2] = res[i].q_abs;
+      if (n_terms) n_terms[i] = res[i].n;
+      if (n_theta) n_theta[i] = res[i].nth;
     }
-    std::vector<double> sums;
-    run_tmatrices(c, specs, sums, nullptr, s);
+  });
+}
+
+int scatrs_spheroid_compute(int64_t n, const double* x, const double* aspect_ratio,
+                            const double* m, const scatrs_spheroid_options* options, double* eff,
+                            double* greek, int32_t* n_terms, int32_t* n_theta,
+                            double* error_estimate, char* err, size_t err_len) {
+  return guarded(err, err_len, [&] {
+    if (n < 0) throw Failure{SCATRS_INVALID_INPUT, "negative sizes"};
+    if (!options) throw Failure{SCATRS_INVALID_INPUT, "options are required"};
+    const scatrs_spheroid_options& o = *options;
+    if (o.n_terms < 0 || o.n_theta < 0 || o.greek_order < -1 || o.greek_order > (1 << 20))
+      throw Failure{SCATRS_INVALID_INPUT, "n_terms, n_theta >= 0 and greek_order >= -1 needed"};
+    if (n == 0) return;
+    if (!eff) throw Failure{SCATRS_INVALID_INPUT, "eff is required"};
+    if (o.greek_order >= 0 && !greek)
+      throw Failure{SCATRS_INVALID_INPUT, "greek is required with greek_order >= 0"};
+    Context& c = context();
+    std::lock_guard<std::mutex> lk(c.mtx);
+    std::vector<SpheroidResult> res;
+    spheroid_solve(c, n, x, aspect_ratio, m, o.rtol, o.n_terms, o.n_theta, true, res, 0);
+    const int64_t len = (int64_t)o.greek_order + 1;
     for (int64_t i = 0; i < n; ++i) {
-      st[i].e = sums[3 * i];
-      st[i].sc = sums[3 * i + 1];
-    }
-    for (;;) {
-      std::vector<int64_t> who;
-      specs.clear();
-      for (int64_t i = 0; i < n; ++i) {
-        St& z = st[i];
-        if (z.stage == 2) continue;
-        if ((z.stage == 0 && z.n >= z.cap) || (z.stage == 1 && z.nth >= z.th_cap)) {
-          char buf[200];
-          snprintf(buf, sizeof buf,
-                   "spheroid %lld: the cross sections did not settle to %g within N = %d, "
-                   "n_theta = %d",
-                   (long long)i, rtol, z.cap, z.th_cap);
-          throw Failure{SCATRS_NOT_CONVERGED, buf};
-        }
-        int nn = z.n, nt = z.nth;
-        if (z.stage == 0) {
-          nn = std::min(z.n + std::max(z.n / 8, 2), z.cap);
-          nt = theta(i, nn);
-        } else {
-          nt = std::min(z.nth + std::max(z.nth / 10, 2), z.th_cap);
-        }
-        specs.push_back({x[i], aspect_ratio[i], m[2 * i], m[2 * i + 1], 0, nn, nt});
-        who.push_back(i);
-      }
-      if (who.empty()) break;
-      run_tmatrices(c, specs, sums, nullptr, s);
-      for (size_t k = 0; k < who.size(); ++k) {
-        St& z = st[who[k]];
-        const double e1 = sums[3 * k], s1 = sums[3 * k + 1];
-        const double ch = std::max(std::fabs(e1 - z.e) / std::fabs(e1), std::fabs(s1 - z.sc) / std::fabs(s1));
-        z.n = specs[k].N;
-        z.nth = specs[k].n_theta;
-        z.e = e1;
-        z.sc = s1;
-        if (ch < rtol) z.stage += 1;
-      }
-    }
-    // Every mode at the final N and n_theta.
-    specs.clear();
-    std::vector<int64_t> owner;
-    for (int64_t i = 0; i < n; ++i)
-      for (int mm = 0; mm <= st[i].n; ++mm) {
-        specs.push_back({x[i], aspect_ratio[i], m[2 * i], m[2 * i + 1], mm, st[i].n, st[i].nth});
-        owner.push_back(i);
-      }
-    run_tmatrices(c, specs, sums, nullptr, s);
-    std::vector<double> ext(n, 0.0), sca(n, 0.0);
-    for (size_t k = 0; k < specs.size(); ++k) {
-      const double w = specs[k].m == 0 ? 1.0 : 2.0;
-      ext[owner[k]] += w * sums[3 * k];
-      sca[owner[k]] += w * sums[3 * k + 1];
-    }
-    for (int64_t i = 0; i < n; ++i) {
-      const double area = 3.14159265358979323846 * x[i] * x[i];
-      q[3 * i] = 2.0 * 3.14159265358979323846 * ext[i] / area;
-      q[3 * i + 1] = 2.0 * 3.14159265358979323846 * sca[i] / area;
-      q[3 * i + 2] = q[3 * i] - q[3 * i + 1];
-      if (n_terms) n_terms[i] = st[i].n;
-      if (n_theta) n_theta[i] = st[i].nth;
+      const SpheroidResult& r = res[i];
+      eff[5 * i] = r.q_ext;
+      eff[5 * i + 1] = r.q_sca;
+      eff[5 * i + 2] = r.q_abs;
+      eff[5 * i + 3] = r.q_back;
+      eff[5 * i + 4] = r.g;
+      if (n_terms) n_terms[i] = r.n;
+      if (n_theta) n_theta[i] = r.nth;
+      if (error_estimate) error_estimate[i] = r.err_est;
+      if (o.greek_order < 0) continue;
+      // tmatrix/mod.rs:464-491: truncated or zero-padded to the order; normalized by alpha1_0,
+      // or unnormalized (alpha1_0 = C_sca / (4 pi) in 1/k^2, so times 4 / x^2).
+      const int64_t have = 2 * (int64_t)r.n + 1;
+      const double a0 = r.greek[0];
+      const double scale = o.normalized ? 1.0 / a0 : 4.0 / (x[i] * x[i]);
+      double* out = greek + 6 * len * i;
+      for (int f = 0; f < 6; ++f)
+        for (int64_t l = 0; l < len; ++l)
+          out[f * len + l] = l < have ? scale * r.greek[f * have + l] : 0.0;
+      if (o.normalized) out[0] = 1.0;
     }
   });
 }

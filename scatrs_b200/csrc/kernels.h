@@ -300,6 +300,32 @@ struct TmArgs {
 };
 void launch_tmatrix(const TmArgs& a, cudaStream_t s);
 
+// The orientation average of a spheroid's phase matrix from its T-matrix (random.cu): one
+// entry per spheroid, whose modes 0..N are the consecutive jobs from job0 of a TmArgs batch.
+// Offsets in doubles; thread starts for the five kernels.
+struct RoSph {
+  int N, nq, L, job0;
+  int64_t rank0;  // [4][N+1][N+1][2N+1] complex
+  int64_t w0;     // [2N+3][2][2][2N+1][N+1] complex
+  int64_t part0;  // [2N+3][16][nq] complex
+  int64_t f0;     // [6][nq]
+  int64_t g0;     // [6][L+1]
+  int64_t mu0;    // nq Gauss nodes
+  int64_t t_rank, t_w, t_phi, t_f, t_g;  // first thread of each kernel
+};
+struct RoArgs {
+  const RoSph* sph;
+  int n_sph;
+  int64_t n_rank, n_w, n_phi, n_f, n_g;  // threads of each kernel
+  const TmJob* jobs;
+  const double* T;  // the batch's T-matrices (complex doubles at each job's T0)
+  double *rank, *w, *part, *f, *greek;
+  const double* mu;
+  const double* const* proj;  // per spheroid: [4][nq][L+1] of (2l+1)/2 w_k d_l(mu_k)
+};
+constexpr int kRoMaxN = 120;  // the largest truncation the orientation average takes
+void launch_random(const RoArgs& a, cudaStream_t s);
+
 void launch_greek_fp64(const double* phase, int64_t n_units, int n_q, int len, const double* d,
                        double* greek, cudaStream_t s);
 void launch_mix(const MixArgs& a, cudaStream_t s);
