@@ -239,6 +239,26 @@ int scatrs_spheroid_compute(int64_t n, const double* x, const double* aspect_rat
                             double* greek, int32_t* n_terms, int32_t* n_theta,
                             double* error_estimate, char* err, size_t err_len);
 
+/*
+ * The fixed-grid ensemble of randomly oriented spheroids (Particle::Spheroid; the engine's
+ * direct path, engine.rs:1207-1339, 2192-2216, 2359-2497): each distribution's nodes as
+ * scatrs_ensemble_fixed's, one aspect ratio per distribution (aspect_ratio[n_dist]) and m per
+ * (distribution, wavelength) unit (complex128, distribution-major). Every node's spheroid is
+ * converged to tmatrix_rtol (the reference uses its ensemble rtol / 100 clamped to
+ * [1e-12, 1e-8], engine.rs:87) in one batch of GPU work with its orientation average; the
+ * unit's averages, ratios (the depolarization ratio from Q_back - Q_sca F22(180 deg)) and Greek
+ * coefficients follow, and the phase matrix at mu from the averaged Greek expansion (every order
+ * to 2N). Outputs as scatrs_ensemble_fixed's (values [11][n_units], phase [6][n_units][n_mu],
+ * greek [6][n_units][L+1]); node_terms[n_units][n_nodes][2] (N, n_theta per node) may be NULL.
+ */
+int scatrs_ensemble_fixed_spheroid(const scatrs_distribution* dists, int64_t n_dist,
+                                   const double* wavelengths, int64_t n_wl,
+                                   const double* aspect_ratio, const double* m, const double* mu,
+                                   int64_t n_mu, const scatrs_fixed_options* options,
+                                   double tmatrix_rtol, double* values, double* phase,
+                                   double* greek, int32_t* node_terms, char* err,
+                                   size_t err_len);
+
 /* Layered spheres (scatrs/src/layered/mod.rs; Particle::LayeredSphere,
  * scatrs/src/ensemble/mod.rs:58-65): n_layers layers, the core first; per distribution the
  * n_layers - 1 outer radii of layers 0..L-2 as fractions of the particle's radius (nondecreasing

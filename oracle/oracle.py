@@ -446,3 +446,83 @@ def random_greek(modes, order: int) -> np.ndarray:
     fn.argtypes = [ctypes.c_int, _PD, ctypes.c_int, _PD]
     fn(n, _p(_flat_modes(modes)), order, _p(out))
     return out.reshape(6, L + 1)
+
+
+def ensemble_fixed_spheroid(dists: np.ndarray, wavelengths, eps, m, n_nodes: int, node_terms,
+                            mu=None, greek_order: int | None = None, normalized: bool = True,
+                            quad: bool = False) -> dict:
+    """The fixed-grid spheroid ensemble, restated over the oracle's per-node solutions: each
+    node's T-matrix at the given (N, n_theta) (node_terms (n_units, n_nodes, 2)), its orientation
+    average (random_greek), the per-particle quantities and direct segment of
+    scatrs/src/ensemble/engine.rs:1207-1339 and particle.rs:276-285, the averages on the grid's
+    weights w u(r) r, and the outputs of engine.rs:2359-2497 (the phase matrix from the averaged
+    Greek expansion). Units distribution-major."""
+    dists = np.ascontiguousarray(dists, dtype=DIST_DTYPE)
+    wl = np.ascontiguousarray(wavelengths, dtype=np.float64).reshape(-1)
+    eps = np.broadcast_to(np.asarray(eps, dtype=np.float64), (dists.size,))
+    m = np.broadcast_to(np.asarray(m, dtype=np.complex128), (dists.size, wl.size))
+    mu = np.zeros(0) if mu is None else np.asarray(mu, dtype=np.float64).reshape(-1)
+    xi, om = gauss_legendre(n_nodes)
+    n_units = dists.size * wl.size
+    L = -1 if greek_order is None else int(greek_order)
+    values = np.zeros((11, n_units))
+    phase = np.zeros((6, n_units, mu.size))
+    greek = np.zeros((6, n_units, max(L, 0) + 1))
+    for d in range(dists.size):
+        a, b = np.log(dists["r_lo"][d]), np.log(dists["r_hi"][d])
+        c, h = 0.5 * (a + b), 0.5 * (b - a)
+        r = np.exp(c + h * xi)
+        params = list(dists["p"][d])
+        W = np.array([h * om[j] * (density(int(dists["kind"][d]), params, r[j])[0] * r[j])
+                      for j in range(n_nodes)])
+        for w in range(wl.size):
+            u = d * wl.size + w
+            rows = []
+            for j in range(n_nodes):
+                x = 2 * np.pi * r[j] / wl[w]
+                N, nth = (int(v) for v in node_terms[u, j])
+                modes = tmatrix_modes(x, eps[d], complex(m[d, w]), N, nth, quad)
+                ext = sum((1 if k == 0 else 2) * -np.trace(t).real for k, t in enumerate(modes))
+                sca = sum((1 if k == 0 else 2) * (abs(t) ** 2).sum() for k, t in enumerate(modes))
+                raw = random_greek(modes, 2 * N)
+                area_x = np.pi * x * x
+                q_ext, q_sca = 2 * np.pi * ext / area_x, 2 * np.pi * sca / area_x
+                g = raw[0, 1] / (3 * raw[0, 0])
+                sgn = (-1.0) ** np.arange(2 * N + 1)
+                q_back = 4 * np.pi * np.dot(sgn, raw[0]) / area_x
+                un = raw * 4 / (x * x)
+                depol = np.dot(sgn, un[0] - 0.5 * (un[1] - un[2]))
+                area = np.pi * r[j] ** 2
+                rows.append((W[j], area, r[j], q_ext, q_sca, g, q_back, depol, un))
+            Z = sum(row[0] for row in rows)
+            top = max(row[8].shape[1] for row in rows)
+            G = np.zeros((6, max(top, L + 1)))
+            acc = np.zeros(9)
+            for (Wj, area, rj, qe, qs, g, qb, dep, un) in rows:
+                acc += Wj * np.array([area * qe, area * qs, area * qs * g, area * (qe - qs),
+                                      area * qb, rj * rj, rj ** 3, area * dep, 0.0])
+                G[:, : un.shape[1]] += Wj * area * un
+            ext, sca, scag, ab, back, r2, r3, dep, _ = acc / Z
+            G /= Z
+            values[:, u] = [ext, sca, ab, back, sca / ext, scag / sca, 4 * np.pi * ext / back,
+                            dep / (2 * back - dep), r3 / r2, np.pi * r2, 4 * np.pi / 3 * r3]
+            if L >= 0:
+                gg = G[:, : L + 1] / (G[0, 0] if normalized else 1.0)
+                if normalized:
+                    gg[0, 0] = 1.0
+                greek[:, u, :] = gg
+            for j, c0 in enumerate(mu):
+                dd = [wigner_d(p, q, c0, top - 1) for p, q in ((0, 0), (2, 2), (2, -2), (0, 2))]
+                plus, minus = 0.5 * (dd[1] + dd[2]), 0.5 * (dd[1] - dd[2])
+                Gt = G[:, :top]
+                f = [np.dot(Gt[0], dd[0]), np.dot(Gt[4], dd[3]),
+                     np.dot(Gt[1], plus) + np.dot(Gt[2], minus),
+                     np.dot(Gt[1], minus) + np.dot(Gt[2], plus), np.dot(Gt[5], dd[3]),
+                     np.dot(Gt[3], dd[0])]
+                phase[:, u, j] = np.array(f) / (sca if normalized else 1.0)
+    out = {"values": values}
+    if mu.size:
+        out["phase"] = phase
+    if L >= 0:
+        out["greek"] = greek
+    return out

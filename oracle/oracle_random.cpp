@@ -28,10 +28,15 @@ namespace {
 
 typedef __float128 Q;
 
+// n! for n <= 600 (the table built once).
 Q fact(int n) {
-  Q f = 1;
-  for (int k = 2; k <= n; ++k) f *= k;
-  return f;
+  static std::vector<Q> t = [] {
+    std::vector<Q> v(601);
+    v[0] = 1;
+    for (int k = 1; k <= 600; ++k) v[k] = v[k - 1] * k;
+    return v;
+  }();
+  return t[n];
 }
 
 // C^{J M}_{j1 m1; j2 m2} by Racah's formula (Condon-Shortley phases).

@@ -61,6 +61,9 @@ SYMBOLS = {
     "scatrs_ensemble_fixed": (ctypes.c_int, [_VP, _I64, _PD, _I64, _PD, _PD, _I64,
                                              ctypes.POINTER(FixedOptions), _PD, _PD, _PD, _CP,
                                              _SZ]),
+    "scatrs_ensemble_fixed_spheroid": (ctypes.c_int, [_VP, _I64, _PD, _I64, _PD, _PD, _PD, _I64,
+                                                      ctypes.POINTER(FixedOptions), _D, _PD, _PD,
+                                                      _PD, _VP, _CP, _SZ]),
     "scatrs_ensemble_fixed_d": (ctypes.c_int, [_VP, _I64, _PD, _I64, _PD, _PD, _I64,
                                                ctypes.POINTER(FixedOptions), _PD, _PD, _PD, _PD,
                                                _PD, _PD, _CP, _SZ]),
@@ -205,6 +208,36 @@ def ensemble_fixed(dists: np.ndarray, wavelengths, m, mu, n_nodes: int, greek_or
                                       1024)
     _check(st, err)
     return values, phase, greek
+
+
+def ensemble_fixed_spheroid(dists: np.ndarray, wavelengths, aspect_ratio, m, mu, n_nodes: int,
+                            greek_order: int = -1, normalized: bool = True,
+                            tmatrix_rtol: float = 1e-8):
+    """The fixed-grid ensemble of randomly oriented spheroids (one aspect ratio per
+    distribution); returns (values, phase or None, greek or None, node_terms) with node_terms
+    (n, n_nodes, 2) the N and n_theta of each node."""
+    require_device()
+    dists = np.ascontiguousarray(dists, dtype=DIST_DTYPE)
+    wl = np.ascontiguousarray(wavelengths, dtype=np.float64).reshape(-1)
+    eps = np.ascontiguousarray(np.broadcast_to(np.asarray(aspect_ratio, dtype=np.float64),
+                                               (dists.size,)))
+    m = np.ascontiguousarray(np.broadcast_to(np.asarray(m, dtype=np.complex128),
+                                             (dists.size, wl.size)))
+    mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
+    n = dists.size * wl.size
+    opts = FixedOptions(int(n_nodes), int(greek_order), int(normalized), 0)
+    values = np.zeros((11, n))
+    phase = np.zeros((6, n, mu.size)) if mu.size else None
+    greek = np.zeros((6, n, greek_order + 1)) if greek_order >= 0 else None
+    terms = np.zeros((n, int(n_nodes), 2), dtype=np.int32)
+    err = ctypes.create_string_buffer(1024)
+    st = load().scatrs_ensemble_fixed_spheroid(dists.ctypes.data, dists.size, _p(wl), wl.size,
+                                               _p(eps), _p(m.view(np.float64)), _p(mu), mu.size,
+                                               ctypes.byref(opts), float(tmatrix_rtol),
+                                               _p(values), _p(phase), _p(greek),
+                                               terms.ctypes.data, err, 1024)
+    _check(st, err)
+    return values, phase, greek, terms
 
 
 def ensemble_fixed_d(dists: np.ndarray, wavelengths, m, mu, n_nodes: int, greek_order: int = -1,

@@ -2136,6 +2136,148 @@ int scatrs_spheroid_compute(int64_t n, const double* x, const double* aspect_rat
   });
 }
 
+int scatrs_ensemble_fixed_spheroid(const scatrs_distribution* dists, int64_t n_dist,
+                                   const double* wavelengths, int64_t n_wl,
+                                   const double* aspect_ratio, const double* m, const double* mu,
+                                   int64_t n_mu, const scatrs_fixed_options* options,
+                                   double tmatrix_rtol, double* values, double* phase,
+                                   double* greek, int32_t* node_terms, char* err,
+                                   size_t err_len) {
+  return guarded(err, err_len, [&] {
+    if (n_dist < 0 || n_wl < 0) throw Failure{SCATRS_INVALID_INPUT, "negative sizes"};
+    for (int64_t i = 0; i < n_wl; ++i)
+      if (!(std::isfinite(wavelengths[i]) && wavelengths[i] > 0.0))
+        throw Failure{SCATRS_INVALID_INPUT, "wavelengths must be finite and > 0"};
+    const int64_t n_units = n_dist * n_wl;
+    check_options(options, n_units, n_mu, mu);
+    if (n_units == 0) return;
+    if (!aspect_ratio || !m || !values)
+      throw Failure{SCATRS_INVALID_INPUT, "aspect_ratio, m and values are required"};
+    const int64_t n_nodes = options->n_nodes;
+    const int L = options->greek_order;
+    Context& c = context();
+    std::lock_guard<std::mutex> lk(c.mtx);
+    // The nodes of each distribution, as the sphere grid's: Gauss-Legendre in ln r over
+    // [r_lo, r_hi], weights w u(r) r (engine.rs:1636-1651).
+    const auto& gl = rule(c, n_nodes);
+    std::vector<double> radius(n_dist * n_nodes), weight(n_dist * n_nodes);
+    for (int64_t d = 0; d < n_dist; ++d) {
+      std::string msg;
+      if (!validate_distribution(dists[d].kind, dists[d].param, &msg))
+        throw Failure{SCATRS_INVALID_INPUT, "distribution " + std::to_string(d) + ": " + msg};
+      if (!(dists[d].r_lo > 0.0 && dists[d].r_hi > dists[d].r_lo && std::isfinite(dists[d].r_hi)))
+        throw Failure{SCATRS_INVALID_INPUT, "distribution " + std::to_string(d) +
+                                                ": the grid needs 0 < r_lo < r_hi < inf"};
+      const double a = std::log(dists[d].r_lo), b = std::log(dists[d].r_hi);
+      const double ctr = 0.5 * (a + b), h = 0.5 * (b - a);
+      for (int64_t j = 0; j < n_nodes; ++j) {
+        const double r = std::exp(ctr + h * gl.first[j]);
+        radius[d * n_nodes + j] = r;
+        weight[d * n_nodes + j] = h * gl.second[j] * (density(dists[d].kind, dists[d].param, r) * r);
+      }
+    }
+    // Every node of every unit is one spheroid of the batch (particle.rs:317-366).
+    const int64_t n_sph = n_units * n_nodes;
+    std::vector<double> xs(n_sph), es(n_sph), ms(2 * n_sph);
+    const double pi = 3.14159265358979323846;
+    for (int64_t d = 0; d < n_dist; ++d)
+      for (int64_t w = 0; w < n_wl; ++w)
+        for (int64_t j = 0; j < n_nodes; ++j) {
+          const int64_t u = d * n_wl + w, k = u * n_nodes + j;
+          xs[k] = 2.0 * pi * radius[d * n_nodes + j] / wavelengths[w];
+          es[k] = aspect_ratio[d];
+          ms[2 * k] = m[2 * u];
+          ms[2 * k + 1] = m[2 * u + 1];
+        }
+    std::vector<SpheroidResult> res;
+    spheroid_solve(c, n_sph, xs.data(), es.data(), ms.data(), tmatrix_rtol, 0, 0, true, res, 0);
+    // The direct path's per-particle quantities and segment (engine.rs:1207-1339) summed over
+    // each unit's nodes in order, then the averages and the outputs of engine.rs:2396-2497.
+    std::vector<double> d00, d22, d2m2, d02;
+    for (int64_t u = 0; u < n_units; ++u) {
+      const int64_t d = u / n_wl;
+      double Z = 0, ext = 0, sca = 0, scag = 0, ab = 0, back = 0, r2 = 0, r3 = 0, dep = 0;
+      int64_t top = 0;
+      for (int64_t j = 0; j < n_nodes; ++j) top = std::max<int64_t>(top, 2 * res[u * n_nodes + j].n);
+      const int64_t glen = std::max<int64_t>(top, L) + 1;
+      std::vector<double> G(6 * glen, 0.0);
+      for (int64_t j = 0; j < n_nodes; ++j) {
+        const SpheroidResult& v = res[u * n_nodes + j];
+        const double r = radius[d * n_nodes + j], W = weight[d * n_nodes + j];
+        const double x = xs[u * n_nodes + j], area = pi * r * r;
+        const int64_t have = 2 * (int64_t)v.n + 1;
+        // Unnormalized Greek coefficients (alpha1_0 = Q_sca): the raw ones times 4 / x^2.
+        const double un = 4.0 / (x * x);
+        double depol = 0.0;  // Q_back - Q_sca F22(180 deg) (particle.rs:276-285)
+        for (int64_t l = 0; l < have; ++l) {
+          const double t = un * (v.greek[l] - 0.5 * (v.greek[have + l] - v.greek[2 * have + l]));
+          depol += l % 2 ? -t : t;
+        }
+        Z += W;
+        ext += W * (area * v.q_ext);
+        sca += W * (area * v.q_sca);
+        scag += W * (area * (v.q_sca * v.g));
+        ab += W * (area * v.q_abs);
+        back += W * (area * v.q_back);
+        r2 += W * (r * r);
+        r3 += W * (r * r * r);
+        dep += W * (area * depol);
+        for (int f = 0; f < 6; ++f)
+          for (int64_t l = 0; l < have; ++l) G[f * glen + l] += W * (area * (un * v.greek[f * have + l]));
+        if (node_terms) {
+          node_terms[2 * (u * n_nodes + j)] = v.n;
+          node_terms[2 * (u * n_nodes + j) + 1] = v.nth;
+        }
+      }
+      ext /= Z, sca /= Z, scag /= Z, ab /= Z, back /= Z, r2 /= Z, r3 /= Z, dep /= Z;
+      for (double& g : G) g /= Z;
+      if (!(std::isfinite(ext) && ext != 0.0 && std::isfinite(sca) && sca != 0.0 &&
+            std::isfinite(back) && back != 0.0))
+        throw Failure{SCATRS_INVALID_INPUT, "unit " + std::to_string(u) +
+                                                ": <C_ext>, <C_sca> or <C_back> is zero or not "
+                                                "finite, so the ratios are undefined"};
+      const double vals[11] = {ext,        sca,  ab,          back,  sca / ext,     scag / sca,
+                               4 * pi * ext / back, dep / (2 * back - dep), r3 / r2, pi * r2,
+                               4 * pi / 3 * r3};
+      for (int k = 0; k < 11; ++k) values[k * n_units + u] = vals[k];
+      if (L >= 0 && greek) {
+        const double sc = options->normalized ? 1.0 / G[0] : 1.0;
+        for (int f = 0; f < 6; ++f)
+          for (int64_t l = 0; l <= L; ++l)
+            greek[((int64_t)f * n_units + u) * (L + 1) + l] = l <= top ? sc * G[f * glen + l] : 0.0;
+        if (options->normalized) greek[u * (L + 1)] = 1.0;
+      }
+      if (n_mu > 0 && phase) {
+        // The phase matrix from the averaged Greek coefficients, every order to 2N
+        // (engine.rs:2359-2390), normalized by <C_sca>.
+        const int64_t len = top + 1;
+        d00.resize(len);
+        d22.resize(len);
+        d2m2.resize(len);
+        d02.resize(len);
+        const double sc = options->normalized ? 1.0 / sca : 1.0;
+        for (int64_t j = 0; j < n_mu; ++j) {
+          wigner_d(0, 0, mu[j], d00.data(), len);
+          wigner_d(2, 2, mu[j], d22.data(), len);
+          wigner_d(2, -2, mu[j], d2m2.data(), len);
+          wigner_d(0, 2, mu[j], d02.data(), len);
+          double f[6] = {0, 0, 0, 0, 0, 0};
+          for (int64_t l = 0; l < len; ++l) {
+            const double plus = 0.5 * (d22[l] + d2m2[l]), minus = 0.5 * (d22[l] - d2m2[l]);
+            f[0] += G[0 * glen + l] * d00[l];
+            f[1] += G[4 * glen + l] * d02[l];
+            f[2] += G[1 * glen + l] * plus + G[2 * glen + l] * minus;
+            f[3] += G[1 * glen + l] * minus + G[2 * glen + l] * plus;
+            f[4] += G[5 * glen + l] * d02[l];
+            f[5] += G[3 * glen + l] * d00[l];
+          }
+          for (int k = 0; k < 6; ++k) phase[((int64_t)k * n_units + u) * n_mu + j] = sc * f[k];
+        }
+      }
+    }
+  });
+}
+
 int scatrs_ensemble_fixed_layered(const scatrs_distribution* dists, int64_t n_dist,
                                   const double* wavelengths, int64_t n_wl,
                                   const scatrs_layers* layers, const double* mu, int64_t n_mu,
