@@ -226,6 +226,24 @@ int scatrs_spheroid_efficiencies(int64_t n, const double* x, const double* aspec
  * none. n_terms, n_theta, error_estimate (the largest relative correction of the last refinement
  * sweep over the modes) may be NULL. N is limited to 120 here.
  */
+/*
+ * scatrs_ensemble_adaptive for randomly oriented spheroids (Particle::Spheroid on the default
+ * adaptive engine, its direct path): one aspect ratio, m per wavelength, the outputs and batch
+ * semantics of scatrs_ensemble_adaptive. Pass 1 solves every node's T-matrix (to rtol / 100
+ * clamped to [1e-12, 1e-8]) and its orientation average on the GPU in batches; pass 2
+ * integrates those values with their declared errors (4 or 16 times max(rtol_T, the solution's
+ * estimate), tmatrix/domain.rs) without solving again. The phase matrix comes from the averaged
+ * Greek expansion (every order to 2N).
+ */
+int scatrs_ensemble_adaptive_spheroid(const scatrs_distribution* dists, int64_t n_dist,
+                                      int32_t batch, const double* wavelengths, int64_t n_wl,
+                                      double aspect_ratio, const double* m, const double* mu,
+                                      int64_t n_mu, const scatrs_adaptive_options* options,
+                                      double* values, double* errors, double* phase,
+                                      double* phase_err, double* greek, double* greek_err,
+                                      int8_t* converged, int64_t* panels, char* err,
+                                      size_t err_len);
+
 typedef struct scatrs_spheroid_options {
   double rtol;
   int32_t n_terms;
@@ -281,6 +299,20 @@ int scatrs_ensemble_fixed_layered(const scatrs_distribution* dists, int64_t n_di
                                   const scatrs_layers* layers, const double* mu, int64_t n_mu,
                                   const scatrs_fixed_options* options, double* values,
                                   double* phase, double* greek, char* err, size_t err_len);
+
+/*
+ * scatrs_ensemble_adaptive for layered spheres (Particle::LayeredSphere on the default adaptive
+ * engine): the layers as scatrs_ensemble_fixed_layered takes them (per distribution), the
+ * outputs and batch semantics of scatrs_ensemble_adaptive.
+ */
+int scatrs_ensemble_adaptive_layered(const scatrs_distribution* dists, int64_t n_dist,
+                                     int32_t batch, const double* wavelengths, int64_t n_wl,
+                                     const scatrs_layers* layers, const double* mu, int64_t n_mu,
+                                     const scatrs_adaptive_options* options, double* values,
+                                     double* errors, double* phase, double* phase_err,
+                                     double* greek, double* greek_err, int8_t* converged,
+                                     int64_t* panels, char* err, size_t err_len);
+
 
 /*
  * As scatrs_ensemble_fixed, with every array in DEVICE memory of the current device, launched

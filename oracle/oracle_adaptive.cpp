@@ -13,6 +13,7 @@
 //                         project 2310-2355, assemble 2396-2497
 //   ensemble/lin.rs       error propagation through the ratios (Lin)
 #include "oracle_core.hpp"
+#include "oracle_spheroid.hpp"
 
 #include <omp.h>
 
@@ -22,6 +23,7 @@
 #include <cstring>
 #include <functional>
 #include <limits>
+#include <map>
 #include <set>
 #include <string>
 #include <vector>
@@ -224,6 +226,12 @@ enum SupportKind { UNBOUNDED, FINITE, POINT };
 struct Part {
   FixedDist dist;
   const double* m = nullptr;  // complex per wavelength: the part's sphere
+  // A layered sphere: n_layers > 1, fractions [n_layers - 1], m_layers complex [n_layers][n_wl].
+  int n_layers = 1;
+  const double* fractions = nullptr;
+  const double* m_layers = nullptr;
+  int64_t n_wl = 0;
+  double eps = 0.0;  // > 0: a spheroid of this aspect ratio (the direct path)
   double f = 1.0;             // the number fraction in its unit (engine.rs:2131)
   Density den;
   SupportKind support;
@@ -309,14 +317,61 @@ struct Options {
   bool allow_unvalidated, refine_backscatter;
 };
 
-// A solved sphere at radius r, or a Failure with the node's context.
-void solve(double r, double lambda, cplx m, bool allow, MieState& st, int64_t* n_terms) {
+// The particle of a group at one wavelength: a homogeneous sphere (m), or a layered one
+// (layered/kernel.rs; particle.rs:186-195: x_l = f_l x, the outer surface's x last).
+struct Optics {
+  cplx m{0, 0};
+  std::vector<double> fr;  // empty for a homogeneous sphere
+  std::vector<cplx> ml;
+  // A spheroid (eps > 0): its T-matrix tolerance and the wavelength's solved nodes by radius.
+  double eps = 0.0, rtol_t = 0.0;
+  std::map<double, SpheroidNode>* cache = nullptr;
+};
+
+// A spheroid node, solved once (particle.rs:317-366; pass 2 reuses pass 1's values).
+const SpheroidNode& sph_node(double r, double lambda, const Optics& op) {
+  auto it = op.cache->find(r);
+  if (it != op.cache->end()) return it->second;
+  SpheroidNode v;
+  const int st = spheroid_node(size_param(r, lambda), op.eps, op.m, op.rtol_t, &v);
+  if (st != OK)
+    throw Failure{st, at(lambda, r) + (st == NOT_CONVERGED ? "the T-matrix did not converge"
+                                                           : "invalid spheroid")};
+  return op.cache->emplace(r, std::move(v)).first->second;
+}
+
+// The node's number of terms after its input checks, or a Failure with the node's context;
+// the layered sizes into xs.
+int64_t node_terms(double r, double lambda, const Optics& op, bool allow, std::vector<double>& xs) {
+  if (op.eps > 0.0) return sph_node(r, lambda, op).n;
   const double x = size_param(r, lambda);
   std::string msg;
   int64_t n = 0;
-  const int s = check_inputs(x, m.re, m.im, 0, allow, &n, &msg);
+  int s;
+  if (op.fr.empty()) {
+    s = check_inputs(x, op.m.re, op.m.im, 0, allow, &n, &msg);
+  } else {
+    xs.resize(op.ml.size());
+    for (size_t l = 0; l + 1 < op.ml.size(); ++l) xs[l] = op.fr[l] * x;
+    xs.back() = x;
+    s = check_layered(xs, op.ml, allow, &msg);
+    n = default_n_max(x);
+  }
   if (s != OK) throw Failure{s, at(lambda, r) + msg};
-  st.solve(x, m, n, false);
+  return n;
+}
+
+// A solved particle at radius r, or a Failure with the node's context.
+void solve(double r, double lambda, const Optics& op, bool allow, MieState& st,
+           int64_t* n_terms) {
+  std::vector<double> xs;
+  const int64_t n = node_terms(r, lambda, op, allow, xs);
+  if (op.fr.empty()) {
+    st.solve(size_param(r, lambda), op.m, n, false);
+  } else {
+    layered_solve(xs, op.ml, n, st);
+    st.x = xs.back();
+  }
   *n_terms = n;
 }
 
@@ -328,7 +383,7 @@ struct Sums1 {
 
 // quantities1 + panel1 (engine.rs:369-560) for every part of a group.
 std::vector<Sums1> panel1(const std::vector<const Part*>& group, double a, double b,
-                          double lambda, cplx m, const Options& o) {
+                          double lambda, const Optics& m, const Options& o) {
   Node nd[15];
   gk_panel(a, b, nd);
   double q[15][N_BASE];
@@ -336,11 +391,19 @@ std::vector<Sums1> panel1(const std::vector<const Part*>& group, double a, doubl
   MieState st;
   for (int i = 0; i < 15; ++i) {
     const double r = std::exp(nd[i].t);
+    const double area = PI * r * r;
+    if (m.eps > 0.0) {
+      const SpheroidNode& v = sph_node(r, lambda, m);
+      n_max = std::max<int64_t>(n_max, v.n);
+      const double w[N_BASE] = {1.0,           area * v.q_ext,  area * v.q_sca,
+                                area * v.q_sca * v.g, area * v.q_back, area * v.q_abs};
+      for (int j = 0; j < N_BASE; ++j) q[i][j] = w[j];
+      continue;
+    }
     int64_t n;
     solve(r, lambda, m, o.allow_unvalidated, st, &n);
     n_max = std::max(n_max, n);
     const Efficiencies e = efficiencies(st);
-    const double area = PI * r * r;
     const double v[N_BASE] = {1.0,           area * e.q_ext,  area * e.q_sca,
                               area * e.q_sca * e.g, area * e.q_back, area * e.q_abs};
     for (int j = 0; j < N_BASE; ++j) q[i][j] = v[j];
@@ -423,7 +486,8 @@ struct Pass1 {
 };
 
 // engine.rs:724-924.
-Pass1 pass1(const std::vector<const Part*>& group, double lambda, cplx m, const Options& o) {
+Pass1 pass1(const std::vector<const Part*>& group, double lambda, const Optics& m,
+            const Options& o) {
   std::vector<double> breaks;
   for (auto* p : group)
     if (p->support == FINITE) {
@@ -585,18 +649,12 @@ Pass1 pass1(const std::vector<const Part*>& group, double lambda, cplx m, const 
 }
 
 // panel_terms (engine.rs:961-978).
-int64_t panel_terms(double a, double b, double lambda, cplx m, bool allow) {
+int64_t panel_terms(double a, double b, double lambda, const Optics& m, bool allow) {
   Node nd[15];
   gk_panel(a, b, nd);
   int64_t most = 0;
-  for (auto& n : nd) {
-    const double r = std::exp(n.t);
-    std::string msg;
-    int64_t nt = 0;
-    const int s = check_inputs(size_param(r, lambda), m.re, m.im, 0, allow, &nt, &msg);
-    if (s != OK) throw Failure{s, at(lambda, r) + msg};
-    most = std::max(most, nt);
-  }
+  std::vector<double> xs;
+  for (auto& n : nd) most = std::max(most, node_terms(std::exp(n.t), lambda, m, allow, xs));
   return most;
 }
 
@@ -690,6 +748,182 @@ struct UnitOut {
   int64_t panels = 0;
 };
 
+// The direct path's pass 2, averages and outputs for spheroids (engine.rs:1207-1339 direct_node,
+// 1558-1740 the sums with the declared node errors, 1782-1836 averages, 1896-1961 a single
+// radius, 2121-2176 mixing, 2359-2497 assembly: the depolarization ratio, the Greek
+// coefficients from the direct segment and the phase matrix from their expansion).
+std::vector<UnitOut> direct_outputs(const std::vector<Part>& parts,
+                                    const std::vector<std::vector<int>>& groups,
+                                    const std::vector<std::vector<int>>& units,
+                                    const std::vector<Pass1>& firsts,
+                                    const std::vector<int>& group_of, const std::vector<int>& place,
+                                    double lambda, const Optics& op, const double* mu,
+                                    int64_t n_mu, int64_t order, bool normalized,
+                                    const Options& o) {
+  const bool keep = order >= 0 || n_mu > 0;
+  int64_t n_direct = 0;
+  for (auto& kv : *op.cache) n_direct = std::max<int64_t>(n_direct, kv.second.n);
+  const int64_t ld = !keep ? -1 : n_mu == 0 ? std::min<int64_t>(order, 2 * n_direct) : 2 * n_direct;
+  const int64_t glen = ld + 1, NS = 9, len = NS + 6 * glen;
+  auto node = [&](double r, std::vector<double>& g, std::vector<double>& ge) {
+    const SpheroidNode& v = sph_node(r, lambda, op);
+    const double area = PI * r * r, tau = op.rtol_t;  // max(rtol, estimate): the estimate is below
+    const double c4 = 4.0 * tau, c16 = 16.0 * tau;
+    const double sv[9] = {1.0,           area * v.q_ext, area * v.q_sca, area * v.q_sca * v.g,
+                          area * v.q_abs, area * v.q_back, r * r,         r * r * r,
+                          area * v.depol};
+    const double back = area * std::max(std::fabs(v.q_back), std::fabs(v.q_sca));
+    const double se[9] = {0.0, c4 * std::fabs(sv[1]), c4 * std::fabs(sv[2]),
+                          c4 * std::fabs(sv[2]) * (1.0 + std::fabs(v.g)), c16 * std::fabs(sv[1]),
+                          c16 * back, 0.0, 0.0, 2.0 * c16 * back};
+    g.assign(len, 0.0);
+    ge.assign(len, 0.0);
+    for (int k = 0; k < 9; ++k) {
+      g[k] = sv[k];
+      ge[k] = se[k];
+    }
+    if (glen > 0) {
+      const int64_t have = 2 * (int64_t)v.n + 1;
+      double big = 0.0;
+      for (int64_t l = 0; l < have; ++l) big = std::max(big, std::fabs(v.greek[l]));
+      for (int f = 0; f < 6; ++f)
+        for (int64_t l = 0; l < glen; ++l) {
+          g[NS + f * glen + l] = l < have ? area * v.greek[f * have + l] : 0.0;
+          ge[NS + f * glen + l] = c16 * area * big;
+        }
+    }
+  };
+  std::vector<std::vector<double>> av(parts.size()), ae(parts.size());
+  std::vector<double> g, ge;
+  for (size_t gi = 0; gi < groups.size(); ++gi) {
+    const auto& grp = groups[gi];
+    if (parts[grp[0]].support == POINT) {
+      node(parts[grp[0]].s_a, g, ge);
+      av[grp[0]] = g;
+      ae[grp[0]] = ge;
+      continue;
+    }
+    for (size_t p = 0; p < grp.size(); ++p) {
+      const Part& part = parts[grp[p]];
+      std::vector<double> S(len, 0.0), E(len, 0.0);
+      for (auto& ab : firsts[gi].panels) {
+        Node nd[15];
+        gk_panel(ab.first, ab.second, nd);
+        for (int64_t j = 0; j < len; ++j) {
+          double K = 0.0, G = 0.0, NE = 0.0;
+          for (int i = 0; i < 15; ++i) {
+            const double r = std::exp(nd[i].t);
+            const double ur = density_eval(part.den, r, nullptr) * r;
+            node(r, g, ge);
+            K += nd[i].wk * ur * g[j];
+            G += nd[i].wg * ur * g[j];
+            NE += std::fabs(nd[i].wk * ur) * ge[j];
+          }
+          S[j] += K;
+          E[j] += std::fabs(K - G) + NE;
+        }
+      }
+      const double trunc = part.support == UNBOUNDED ? 0.2 * o.rtol : 0.0;
+      const double z = part.mom.z, ez = part.mom.ez;
+      std::vector<double> v(len), er(len);
+      for (int64_t j = 0; j < len; ++j) {
+        v[j] = S[j] / z;
+        er[j] = (E[j] + std::fabs(v[j]) * ez) / z + trunc * std::fabs(v[j]);
+      }
+      for (int k = 0; k < 2; ++k) {
+        v[6 + k] = part.mom.v[k];
+        er[6 + k] = part.mom.e[k];
+      }
+      av[grp[p]] = std::move(v);
+      ae[grp[p]] = std::move(er);
+    }
+  }
+  std::vector<UnitOut> out;
+  std::vector<double> d00, d22, d2m2, d02;
+  for (auto& un : units) {
+    std::vector<double> v(len, 0.0), e(len, 0.0);
+    for (int p : un)
+      for (int64_t j = 0; j < len; ++j) {
+        v[j] += parts[p].f * av[p][j];
+        e[j] += parts[p].f * ae[p][j];
+      }
+    UnitOut u;
+    auto lin = [&](int64_t j) { return Lin{v[j], e[j]}; };
+    Lin ext = lin(1), sca = lin(2), scag = lin(3), ab = lin(4), back = lin(5), r2 = lin(6),
+        r3 = lin(7), num = lin(8);
+    for (Lin* l : {&ext, &sca, &back})
+      if (!(std::isfinite(l->v) && l->v != 0.0))
+        throw Failure{INVALID_INPUT,
+                      "a ratio's denominator (<C_ext>, <C_sca> or <C_back>) is 0 or not finite"};
+    const Lin den{2.0 * back.v - num.v, 2.0 * back.e + num.e};
+    const Lin sc[11] = {ext, sca, ab, back, ldiv(sca, ext), ldiv(scag, sca),
+                        lscale(ldiv(ext, back), 4.0 * PI), ldiv(num, den), ldiv(r3, r2),
+                        lscale(r2, PI), lscale(r3, 4.0 * PI / 3.0)};
+    for (int k = 0; k < 11; ++k) {
+      u.values[k] = sc[k].v;
+      u.errors[k] = sc[k].e;
+    }
+    auto G = [&](int f, int64_t l) { return lin(NS + f * glen + l); };
+    if (order >= 0) {
+      u.greek.assign(6 * (order + 1), 0.0);
+      u.greek_err.assign(6 * (order + 1), 0.0);
+      const Lin a0 = G(0, 0);
+      for (int f = 0; f < 6; ++f)
+        for (int64_t l = 0; l <= order && l < glen; ++l) {
+          Lin x = G(f, l);
+          if (normalized) x = (f == 0 && l == 0) ? Lin{1.0, 0.0} : ldiv(x, a0);
+          u.greek[f * (order + 1) + l] = x.v;
+          u.greek_err[f * (order + 1) + l] = x.e;
+        }
+      if (normalized) u.greek[0] = 1.0;
+    }
+    if (n_mu > 0) {
+      u.phase.assign(6 * n_mu, 0.0);
+      u.phase_err.assign(6 * n_mu, 0.0);
+      d00.resize(glen);
+      d22.resize(glen);
+      d2m2.resize(glen);
+      d02.resize(glen);
+      for (int64_t j = 0; j < n_mu; ++j) {
+        wigner_d(0, 0, mu[j], d00.data(), glen);
+        wigner_d(2, 2, mu[j], d22.data(), glen);
+        wigner_d(2, -2, mu[j], d2m2.data(), glen);
+        wigner_d(0, 2, mu[j], d02.data(), glen);
+        Lin f[6] = {};
+        auto acc = [](Lin& t, double w, const Lin& x) {
+          t.v += w * x.v;
+          t.e += std::fabs(w) * x.e;
+        };
+        for (int64_t l = 0; l < glen; ++l) {
+          const double pl = 0.5 * (d22[l] + d2m2[l]), mn = 0.5 * (d22[l] - d2m2[l]);
+          acc(f[0], d00[l], G(0, l));
+          acc(f[1], d02[l], G(4, l));
+          acc(f[2], pl, G(1, l));
+          acc(f[2], mn, G(2, l));
+          acc(f[3], mn, G(1, l));
+          acc(f[3], pl, G(2, l));
+          acc(f[4], d02[l], G(5, l));
+          acc(f[5], d00[l], G(3, l));
+        }
+        for (int k = 0; k < 6; ++k) {
+          const Lin x = normalized ? ldiv(f[k], sca) : f[k];
+          u.phase[k * n_mu + j] = x.v;
+          u.phase_err[k * n_mu + j] = x.e;
+        }
+      }
+    }
+    std::set<int> ug;
+    for (int p : un) {
+      if (parts[p].support == POINT) continue;
+      u.converged = u.converged && firsts[group_of[p]].converged[place[p]];
+      ug.insert(group_of[p]);
+    }
+    for (int gi : ug) u.panels += (int64_t)firsts[gi].panels.size();
+    out.push_back(std::move(u));
+  }
+  return out;
+}
+
 // One wavelength (engine.rs:1964-2250): pass 1 per group, bands, pass 2, averages, a unit per
 // entry of `units` (each a list of parts with weight 1), the projection and the assembly.
 std::vector<UnitOut> wavelength(const std::vector<Part>& parts,
@@ -697,23 +931,38 @@ std::vector<UnitOut> wavelength(const std::vector<Part>& parts,
                                 const std::vector<std::vector<int>>& units, double lambda,
                                 int64_t wi, const double* mu, int64_t n_mu, int64_t order,
                                 bool normalized, const Options& o) {
-  auto m_of = [&](int p) { return C(parts[p].m[2 * wi], parts[p].m[2 * wi + 1]); };
+  const int64_t n_wl_all = parts.empty() ? 0 : parts[0].n_wl;
+  std::map<double, SpheroidNode> cache;
+  auto m_of = [&](int p) {
+    Optics op;
+    const Part& q = parts[p];
+    if (q.eps > 0.0) {
+      op.m = C(q.m[2 * wi], q.m[2 * wi + 1]);
+      op.eps = q.eps;
+      op.rtol_t = std::min(std::max(o.rtol / 100.0, 1e-12), 1e-8);  // engine.rs:87
+      op.cache = &cache;
+      return op;
+    }
+    if (q.n_layers <= 1) {
+      op.m = C(q.m[2 * wi], q.m[2 * wi + 1]);
+    } else {
+      op.fr.assign(q.fractions, q.fractions + q.n_layers - 1);
+      for (int l = 0; l < q.n_layers; ++l)
+        op.ml.push_back(C(q.m_layers[2 * (l * n_wl_all + wi)], q.m_layers[2 * (l * n_wl_all + wi) + 1]));
+    }
+    return op;
+  };
   std::vector<Pass1> firsts;
   int64_t n_max = 0;
   for (auto& g : groups) {
     std::vector<const Part*> mem;
     for (int p : g) mem.push_back(&parts[p]);
-    const cplx m = m_of(g[0]);  // a group shares its particle
+    const Optics m = m_of(g[0]);  // a group shares its particle
     Pass1 p1;
     if (mem[0]->support == POINT) {
-      const double r = mem[0]->s_a;
-      std::string msg;
-      int64_t nt = 0;
-      const int s = check_inputs(size_param(r, lambda), m.re, m.im, 0, o.allow_unvalidated,
-                                 &nt, &msg);
-      if (s != OK) throw Failure{s, at(lambda, r) + msg};
+      std::vector<double> xs;
       p1.converged = {true};
-      p1.n_terms = nt;
+      p1.n_terms = node_terms(mem[0]->s_a, lambda, m, o.allow_unvalidated, xs);
     } else {
       p1 = pass1(mem, lambda, m, o);
     }
@@ -726,13 +975,19 @@ std::vector<UnitOut> wavelength(const std::vector<Part>& parts,
       group_of[groups[gi][k]] = (int)gi;
       place[groups[gi][k]] = (int)k;
     }
+  if (!parts.empty() && parts[0].eps > 0.0) {
+    // Spheroids: pass 2 and the outputs on the direct path, from the solved nodes.
+    const Optics op = m_of(groups[0][0]);
+    return direct_outputs(parts, groups, units, firsts, group_of, place, lambda, op, mu, n_mu,
+                          order, normalized, o);
+  }
   Layout L;
   L.n_mu = n_mu;
   L.len = SCALARS + 4 * n_mu;
   if (order >= 0) {
     std::set<int64_t> uppers;
     for (size_t gi = 0; gi < groups.size(); ++gi) {
-      const cplx m = m_of(groups[gi][0]);
+      const Optics m = m_of(groups[gi][0]);
       if (parts[groups[gi][0]].support == POINT) {
         uppers.insert(bucket(firsts[gi].n_terms));
         continue;
@@ -753,7 +1008,7 @@ std::vector<UnitOut> wavelength(const std::vector<Part>& parts,
   MieState st;
   for (size_t gi = 0; gi < groups.size(); ++gi) {
     const auto& grp = groups[gi];
-    const cplx m = m_of(grp[0]);
+    const Optics m = m_of(grp[0]);
     if (parts[grp[0]].support == POINT) {
       const double r = parts[grp[0]].s_a;
       int64_t n;
@@ -937,13 +1192,14 @@ extern "C" {
 // all (shared panels per wavelength). Outputs distribution-major (unit = d * n_wl + i): values
 // and errors (11, n), phase and phase_err (6, n, n_mu), greek and greek_err (6, n, L + 1),
 // converged (n) as bytes, panels (n). Returns a status, the first error in wavelength order.
-int orc_ensemble_adaptive(const FixedDist* dists, int64_t n_dist, int batch, const double* wl,
-                          int64_t n_wl, const double* m, const double* mu, int64_t n_mu,
-                          int64_t greek_order, int normalized, double rtol, int64_t max_panels,
-                          int allow_unvalidated, int refine_backscatter, int n_threads,
-                          double* values, double* errors, double* phase, double* phase_err,
-                          double* greek, double* greek_err, int8_t* converged, int64_t* panels,
-                          char* err, int64_t err_len) {
+static int adaptive_impl(const FixedDist* dists, int64_t n_dist, int batch, const double* wl,
+                         int64_t n_wl, const double* m, int n_layers, const double* fractions,
+                         const double* m_layers, const double* mu, int64_t n_mu,
+                         int64_t greek_order, int normalized, double rtol, int64_t max_panels,
+                         int allow_unvalidated, int refine_backscatter, int n_threads,
+                         double* values, double* errors, double* phase, double* phase_err,
+                         double* greek, double* greek_err, int8_t* converged, int64_t* panels,
+                         char* err, int64_t err_len, double eps = 0.0) {
   const int64_t n_units = n_dist * n_wl;
   Options o{rtol, (size_t)max_panels, allow_unvalidated != 0, refine_backscatter != 0};
   auto fail = [&](const Failure& f) {
@@ -957,6 +1213,13 @@ int orc_ensemble_adaptive(const FixedDist* dists, int64_t n_dist, int batch, con
     for (int64_t d = 0; d < n_dist; ++d) {
       parts.push_back(make_part(dists[d], rtol));
       parts.back().m = m;
+      parts.back().n_wl = n_wl;
+      parts.back().eps = eps;
+      if (n_layers > 1) {
+        parts.back().n_layers = n_layers;
+        parts.back().fractions = fractions + d * (n_layers - 1);
+        parts.back().m_layers = m_layers + 2 * d * n_layers * n_wl;
+      }
     }
   } catch (const Failure& f) {
     return fail(f);
@@ -1027,6 +1290,54 @@ int orc_ensemble_adaptive(const FixedDist* dists, int64_t n_dist, int batch, con
   return OK;
 }
 
+int orc_ensemble_adaptive(const FixedDist* dists, int64_t n_dist, int batch, const double* wl,
+                          int64_t n_wl, const double* m, const double* mu, int64_t n_mu,
+                          int64_t greek_order, int normalized, double rtol, int64_t max_panels,
+                          int allow_unvalidated, int refine_backscatter, int n_threads,
+                          double* values, double* errors, double* phase, double* phase_err,
+                          double* greek, double* greek_err, int8_t* converged, int64_t* panels,
+                          char* err, int64_t err_len) {
+  return adaptive_impl(dists, n_dist, batch, wl, n_wl, m, 1, nullptr, nullptr, mu, n_mu,
+                       greek_order, normalized, rtol, max_panels, allow_unvalidated,
+                       refine_backscatter, n_threads, values, errors, phase, phase_err, greek,
+                       greek_err, converged, panels, err, err_len);
+}
+
+// orc_ensemble_adaptive for layered spheres: n_layers layers, fractions [n_dist][n_layers - 1],
+// m_layers complex [n_dist][n_layers][n_wl] (layered/kernel.rs per node; particle.rs:186-195).
+int orc_ensemble_adaptive_layered(const FixedDist* dists, int64_t n_dist, int batch,
+                                  const double* wl, int64_t n_wl, int n_layers,
+                                  const double* fractions, const double* m_layers,
+                                  const double* mu, int64_t n_mu, int64_t greek_order,
+                                  int normalized, double rtol, int64_t max_panels,
+                                  int allow_unvalidated, int refine_backscatter, int n_threads,
+                                  double* values, double* errors, double* phase,
+                                  double* phase_err, double* greek, double* greek_err,
+                                  int8_t* converged, int64_t* panels, char* err,
+                                  int64_t err_len) {
+  return adaptive_impl(dists, n_dist, batch, wl, n_wl, m_layers, n_layers, fractions, m_layers,
+                       mu, n_mu, greek_order, normalized, rtol, max_panels, allow_unvalidated,
+                       refine_backscatter, n_threads, values, errors, phase, phase_err, greek,
+                       greek_err, converged, panels, err, err_len);
+}
+
+// orc_ensemble_adaptive for randomly oriented spheroids of aspect ratio eps (m per wavelength):
+// every node solved by the oracle's EBCM and orientation average, pass 2 on the direct path.
+int orc_ensemble_adaptive_spheroid(const FixedDist* dists, int64_t n_dist, int batch,
+                                   const double* wl, int64_t n_wl, double eps, const double* m,
+                                   const double* mu, int64_t n_mu, int64_t greek_order,
+                                   int normalized, double rtol, int64_t max_panels,
+                                   int allow_unvalidated, int refine_backscatter, int n_threads,
+                                   double* values, double* errors, double* phase,
+                                   double* phase_err, double* greek, double* greek_err,
+                                   int8_t* converged, int64_t* panels, char* err,
+                                   int64_t err_len) {
+  return adaptive_impl(dists, n_dist, batch, wl, n_wl, m, 1, nullptr, nullptr, mu, n_mu,
+                       greek_order, normalized, rtol, max_panels, allow_unvalidated,
+                       refine_backscatter, n_threads, values, errors, phase, phase_err, greek,
+                       greek_err, converged, panels, err, err_len, eps);
+}
+
 // The adaptive ensemble of a mixture (compute_mixture, ensemble/mod.rs:609-625): n_comp
 // components, component c with n_modes[c] modes (its distributions, consecutive in `modes`,
 // with weights mode_w, ignored for one mode), weight w[c] and m of its own (complex per
@@ -1058,6 +1369,7 @@ int orc_ensemble_mixture(const FixedDist* modes, const double* mode_w, const int
         const double v = n_modes[c] > 1 ? mode_w[k + j] : 1.0;
         parts.push_back(make_part(modes[k + j], rtol));
         parts.back().m = m + 2 * n_wl * c;
+        parts.back().n_wl = n_wl;
         parts.back().f = w[c] / w_total * v / v_total;
         unit.push_back((int)parts.size() - 1);
       }

@@ -166,40 +166,6 @@ int64_t orc_bucket(int64_t n) { return bucket(n); }
 // ascending radius; a chunk's largest number of terms chooses its projector band, as a panel's
 // does in the reference. Units are distribution-major: unit = d * n_wl + i.
 // ---------------------------------------------------------------------------------------
-// Layered::check_inputs (layered/mod.rs:233-305) with the default truncation.
-static int check_layered(const std::vector<double>& x, const std::vector<cplx>& m,
-                         bool allow_unvalidated, std::string* msg) {
-  const size_t L = x.size();
-  for (size_t l = 0; l < L; ++l)
-    if (!std::isfinite(x[l]) || (l > 0 && x[l] < x[l - 1])) {
-      *msg = "the size parameters must be finite and nondecreasing from the core out";
-      return INVALID_INPUT;
-    }
-  const double outer = x[L - 1];
-  if (x[0] < MIN_SIZE_PARAMETER || outer > MAX_SIZE_PARAMETER) {
-    *msg = "the size parameters must be in [1e-30, 1e6]";
-    return INVALID_INPUT;
-  }
-  for (auto& v : m) {
-    if (!(std::isfinite(v.re) && std::isfinite(v.im)) || v.re < 0.0 || v.im < 0.0 ||
-        !(cnorm(v) >= MIN_REFRACTIVE_INDEX && cnorm(v) <= MAX_REFRACTIVE_INDEX)) {
-      *msg = "invalid refractive index of a layer";
-      return INVALID_INPUT;
-    }
-  }
-  if (!allow_unvalidated) {
-    bool in = L <= 16 && outer >= 1e-6 && outer <= 1e4;
-    for (auto& v : m)
-      in = in && cnorm(v) * outer <= 3e4 && v.re > 0.0 && v.re <= 10.0 && v.im >= 0.0 &&
-           v.im <= 10.0 && cnorm(v) >= 0.1;
-    if (!in) {
-      *msg = "outside the validated domain of layered spheres";
-      return OUTSIDE_VALIDATED_DOMAIN;
-    }
-  }
-  return OK;
-}
-
 static int ensemble_impl(const FixedDist* dists, int64_t n_dist, const double* wl, int64_t n_wl,
                          const double* m, int n_layers, const double* fractions,
                          const double* m_layers, int64_t n_nodes, const double* mu,

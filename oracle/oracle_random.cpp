@@ -18,6 +18,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
+#include <unordered_map>
 #include <vector>
 
 #include "oracle_core.hpp"
@@ -39,8 +41,23 @@ Q fact(int n) {
   return t[n];
 }
 
-// C^{J M}_{j1 m1; j2 m2} by Racah's formula (Condon-Shortley phases).
+double cg_racah(int j1, int m1, int j2, int m2, int J);
+
+// C^{J M}_{j1 m1; j2 m2}, memoized per thread (the values depend on the indices alone).
 double cg(int j1, int m1, int j2, int m2, int J) {
+  thread_local std::unordered_map<uint64_t, double> memo;
+  // Five 12-bit fields (every index below 2048 in magnitude here).
+  const uint64_t key = ((uint64_t)j1 << 48) | ((uint64_t)(m1 + 2048) << 36) |
+                       ((uint64_t)j2 << 24) | ((uint64_t)(m2 + 2048) << 12) | (uint64_t)J;
+  auto it = memo.find(key);
+  if (it != memo.end()) return it->second;
+  const double v = cg_racah(j1, m1, j2, m2, J);
+  memo.emplace(key, v);
+  return v;
+}
+
+// C^{J M}_{j1 m1; j2 m2} by Racah's formula (Condon-Shortley phases).
+double cg_racah(int j1, int m1, int j2, int m2, int J) {
   const int M = m1 + m2;
   if (J < std::abs(j1 - j2) || J > j1 + j2 || std::abs(m1) > j1 || std::abs(m2) > j2 ||
       std::abs(M) > J)

@@ -8,6 +8,7 @@
 // Conventions (ebcm.py:8-11): e^{-i w t}; relative index s; k = 1, lengths are size parameters
 // and x is the equal-volume sphere's; aspect ratio eps = a/c, > 1 oblate.
 #include "oracle_core.hpp"
+#include "oracle_spheroid.hpp"
 
 #include <array>
 #include <cmath>
@@ -251,16 +252,10 @@ int shape_theta(double eps, double rtol) {
 }
 int theta_of(int n, double eps, double rtol) { return std::max(2 * n, shape_theta(eps, rtol)); }
 
-}  // namespace
-
-extern "C" {
-
-// Orientation-averaged Q_ext, Q_sca, Q_abs with N and n_theta grown until the cross sections of
-// mode 0 settle to rtol (driver.rs:343-420: N by max(N/8, 2), then n_theta by a tenth), then
-// every mode at the final N and n_theta. out: q[3], n_terms, n_theta. Returns 0, 1 (invalid or
-// singular) or 2 (not converged within the cap).
-int orc_spheroid_converged(double x, double eps, double s_re, double s_im, double rtol,
-                           double* q, int* n_out, int* nth_out) {
+// The N and n_theta loops of driver.rs:343-420 on mode 0 (double precision): returns 0, 1
+// (invalid or singular) or 2 (not converged within the caps).
+int converge(double x, double eps, double s_re, double s_im, double rtol, int* n_out,
+             int* nth_out) {
   const cplx s = C(s_re, s_im);
   const int cap = 2 * wiscombe(x_max(x, eps) * std::max(cnorm(s), 1.0)) + 20;
   const int start = std::min(wiscombe(x_max(x, eps)), cap);
@@ -299,6 +294,26 @@ int orc_spheroid_converged(double x, double eps, double s_re, double s_im, doubl
     s0 = s1;
     if (c < rtol) break;
   }
+  *n_out = n;
+  *nth_out = nth;
+  return OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Orientation-averaged Q_ext, Q_sca, Q_abs with N and n_theta grown until the cross sections of
+// mode 0 settle to rtol (driver.rs:343-420: N by max(N/8, 2), then n_theta by a tenth), then
+// every mode at the final N and n_theta. out: q[3], n_terms, n_theta. Returns 0, 1 (invalid or
+// singular) or 2 (not converged within the cap).
+int orc_spheroid_converged(double x, double eps, double s_re, double s_im, double rtol,
+                           double* q, int* n_out, int* nth_out) {
+  const cplx s = C(s_re, s_im);
+  int n = 0, nth = 0;
+  const int st = converge(x, eps, s_re, s_im, rtol, &n, &nth);
+  if (st != OK) return st;
+  std::vector<cplx> T;
   double ext = 0.0, sca = 0.0;
   for (int m = 0; m <= n; ++m) {
     if (!mode_tmatrix(x, eps, s, m, n, nth, T)) return INVALID_INPUT;
@@ -354,3 +369,51 @@ int orc_spheroid_q(double x, double eps, double s_re, double s_im, int N, int n_
 }
 
 }  // extern "C"
+
+extern "C" int orc_random_greek(int N, const double* t_all, int order, double* out);
+
+namespace orc {
+
+int spheroid_node(double x, double eps, cplx s, double rtol, SpheroidNode* out) {
+  int n = 0, nth = 0;
+  const int st = converge(x, eps, s.re, s.im, rtol, &n, &nth);
+  if (st != OK) return st;
+  std::vector<double> t_all;
+  double ext = 0.0, sca = 0.0;
+  for (int m = 0; m <= n; ++m) {
+    std::vector<cplx> T;
+    if (!mode_tmatrix(x, eps, s, m, n, nth, T)) return INVALID_INPUT;
+    double e, sc;
+    mode_sums(T, &e, &sc);
+    const double w = m == 0 ? 1.0 : 2.0;
+    ext += w * e;
+    sca += w * sc;
+    for (const cplx& v : T) {
+      t_all.push_back(v.re);
+      t_all.push_back(v.im);
+    }
+  }
+  const int len = 2 * n + 1;
+  std::vector<double> raw(6 * len);
+  orc_random_greek(n, t_all.data(), 2 * n, raw.data());
+  const double area = PI * x * x, un = 4.0 / (x * x);
+  out->n = n;
+  out->nth = nth;
+  out->q_ext = 2.0 * PI * ext / area;
+  out->q_sca = 2.0 * PI * sca / area;
+  out->q_abs = out->q_ext - out->q_sca;
+  out->g = raw[0] > 0.0 ? raw[1] / (3.0 * raw[0]) : 0.0;
+  double f11 = 0.0, dep = 0.0;
+  for (int l = 0; l < len; ++l) {
+    const double sg = l % 2 ? -1.0 : 1.0;
+    f11 += sg * raw[l];
+    dep += sg * un * (raw[l] - 0.5 * (raw[len + l] - raw[2 * len + l]));
+  }
+  out->q_back = 4.0 * PI * f11 / area;
+  out->depol = dep;
+  out->greek.resize(6 * len);
+  for (int k = 0; k < 6 * len; ++k) out->greek[k] = un * raw[k];
+  return OK;
+}
+
+}  // namespace orc

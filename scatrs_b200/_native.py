@@ -76,6 +76,15 @@ SYMBOLS = {
     "scatrs_ensemble_adaptive": (ctypes.c_int, [_VP, _I64, _I32, _PD, _I64, _PD, _PD, _I64,
                                                 ctypes.POINTER(AdaptiveOptions), _PD, _PD, _PD,
                                                 _PD, _PD, _PD, _VP, _VP, _CP, _SZ]),
+    "scatrs_ensemble_adaptive_layered": (ctypes.c_int, [_VP, _I64, _I32, _PD, _I64,
+                                                        ctypes.POINTER(Layers), _PD, _I64,
+                                                        ctypes.POINTER(AdaptiveOptions), _PD, _PD,
+                                                        _PD, _PD, _PD, _PD, _VP, _VP, _CP, _SZ]),
+    "scatrs_ensemble_adaptive_spheroid": (ctypes.c_int, [_VP, _I64, _I32, _PD, _I64, _D, _PD,
+                                                         _PD, _I64,
+                                                         ctypes.POINTER(AdaptiveOptions), _PD,
+                                                         _PD, _PD, _PD, _PD, _PD, _VP, _VP, _CP,
+                                                         _SZ]),
     "scatrs_ensemble_mixture": (ctypes.c_int, [ctypes.POINTER(Component), _I64, _PD, _I64, _PD,
                                                _I64, ctypes.POINTER(AdaptiveOptions), _PD, _PD,
                                                _PD, _PD, _PD, _PD, _VP, _VP, _CP, _SZ]),
@@ -300,6 +309,85 @@ def ensemble_adaptive(dists: np.ndarray, wavelengths, m, mu=None, greek_order: i
                                          _p(out["errors"]), _p(ph), _p(pe), _p(g), _p(ge),
                                          out["converged"].ctypes.data, out["panels"].ctypes.data,
                                          err, 1024)
+    _check(st, err)
+    out["converged"] = out["converged"].astype(bool)
+    if ph is not None:
+        out["phase"], out["phase_err"] = ph, pe
+    if g is not None:
+        out["greek"], out["greek_err"] = g, ge
+    return out
+
+
+def ensemble_adaptive_layered(dists: np.ndarray, wavelengths, fractions, m_layers, mu=None,
+                               greek_order: int = -1, normalized: bool = True,
+                               rtol: float = 1e-6, max_panels: int = 4096,
+                               allow_unvalidated: bool = False, refine_backscatter: bool = False,
+                               batch: bool = False) -> dict:
+    """ensemble_adaptive for layered spheres: fractions (n_dist, L - 1), m_layers complex
+    (n_dist, L, n_wl); the same outputs."""
+    require_device()
+    dists = np.ascontiguousarray(dists, dtype=DIST_DTYPE)
+    wl = np.ascontiguousarray(wavelengths, dtype=np.float64).reshape(-1)
+    ml = np.ascontiguousarray(np.asarray(m_layers, dtype=np.complex128))
+    nl = ml.shape[1]
+    fr = np.ascontiguousarray(np.asarray(fractions, dtype=np.float64).reshape(dists.size,
+                                                                              max(nl - 1, 0)))
+    mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
+    n = dists.size * wl.size
+    L = int(greek_order)
+    opts = AdaptiveOptions(float(rtol), int(max_panels), L, int(normalized),
+                           int(allow_unvalidated), int(refine_backscatter))
+    lay = Layers(nl, 0, _p(fr), _p(ml.view(np.float64)))
+    out = {"values": np.zeros((11, n)), "errors": np.zeros((11, n)),
+           "converged": np.zeros(n, dtype=np.int8), "panels": np.zeros(n, dtype=np.int64)}
+    ph = pe = g = ge = None
+    if mu.size:
+        ph, pe = np.zeros((6, n, mu.size)), np.zeros((6, n, mu.size))
+    if L >= 0:
+        g, ge = np.zeros((6, n, L + 1)), np.zeros((6, n, L + 1))
+    err = ctypes.create_string_buffer(1024)
+    st = load().scatrs_ensemble_adaptive_layered(
+        dists.ctypes.data, dists.size, int(batch), _p(wl), wl.size, ctypes.byref(lay), _p(mu),
+        mu.size, ctypes.byref(opts), _p(out["values"]), _p(out["errors"]), _p(ph), _p(pe),
+        _p(g), _p(ge), out["converged"].ctypes.data, out["panels"].ctypes.data, err, 1024)
+    _check(st, err)
+    out["converged"] = out["converged"].astype(bool)
+    if ph is not None:
+        out["phase"], out["phase_err"] = ph, pe
+    if g is not None:
+        out["greek"], out["greek_err"] = g, ge
+    return out
+
+
+def ensemble_adaptive_spheroid(dists: np.ndarray, wavelengths, aspect_ratio: float, m, mu=None,
+                                greek_order: int = -1, normalized: bool = True,
+                                rtol: float = 1e-6, max_panels: int = 4096,
+                                allow_unvalidated: bool = False,
+                                refine_backscatter: bool = False, batch: bool = False) -> dict:
+    """ensemble_adaptive for randomly oriented spheroids (one aspect ratio, m per wavelength);
+    the same outputs."""
+    require_device()
+    dists = np.ascontiguousarray(dists, dtype=DIST_DTYPE)
+    wl = np.ascontiguousarray(wavelengths, dtype=np.float64).reshape(-1)
+    m = np.ascontiguousarray(np.broadcast_to(np.asarray(m, dtype=np.complex128), wl.shape))
+    mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
+    n = dists.size * wl.size
+    L = int(greek_order)
+    opts = AdaptiveOptions(float(rtol), int(max_panels), L, int(normalized),
+                           int(allow_unvalidated), int(refine_backscatter))
+    out = {"values": np.zeros((11, n)), "errors": np.zeros((11, n)),
+           "converged": np.zeros(n, dtype=np.int8), "panels": np.zeros(n, dtype=np.int64)}
+    ph = pe = g = ge = None
+    if mu.size:
+        ph, pe = np.zeros((6, n, mu.size)), np.zeros((6, n, mu.size))
+    if L >= 0:
+        g, ge = np.zeros((6, n, L + 1)), np.zeros((6, n, L + 1))
+    err = ctypes.create_string_buffer(1024)
+    st = load().scatrs_ensemble_adaptive_spheroid(
+        dists.ctypes.data, dists.size, int(batch), _p(wl), wl.size, float(aspect_ratio),
+        _p(m.view(np.float64)), _p(mu), mu.size, ctypes.byref(opts), _p(out["values"]),
+        _p(out["errors"]), _p(ph), _p(pe), _p(g), _p(ge), out["converged"].ctypes.data,
+        out["panels"].ctypes.data, err, 1024)
     _check(st, err)
     out["converged"] = out["converged"].astype(bool)
     if ph is not None:

@@ -139,13 +139,31 @@ def _adaptive_dict(out: dict, mu_size: int, k: int) -> dict:
     return raw
 
 
+def _layers(particle_spec, n_wl: int):
+    """(fractions (L - 1), m (L, n_wl)) of a ('layered', fractions, m) spec
+    (scatrs-py/src/ensemble.rs:80-135)."""
+    fr = np.ascontiguousarray(np.asarray(particle_spec[1], dtype=np.float64).reshape(-1))
+    ml = np.ascontiguousarray(np.asarray(particle_spec[2], dtype=np.complex128))
+    if ml.ndim != 2 or ml.shape[1] != n_wl or ml.shape[0] != fr.size + 1:
+        raise InvalidInputError(f"layered m must be ({fr.size + 1}, {n_wl}), got {ml.shape}")
+    return fr, ml
+
+
+def _spheroid(particle_spec, n_wl: int):
+    """(aspect ratio, m (n_wl)) of a ('spheroid', aspect_ratio, m) spec."""
+    m = np.ascontiguousarray(np.asarray(particle_spec[2], dtype=np.complex128).reshape(-1))
+    if m.size != n_wl:
+        raise InvalidInputError(f"{m.size} refractive indices for {n_wl} wavelengths")
+    return float(particle_spec[1]), m
+
+
 def _sphere_m(particle_spec, n_wl: int) -> np.ndarray:
     if not isinstance(particle_spec, tuple):
         raise TypeError("a particle spec must be a tuple")
     if particle_spec[0] != "sphere":
         if particle_spec[0] in ("layered", "spheroid"):
             raise InvalidInputError(
-                f"{particle_spec[0]} particles are not on the adaptive GPU path")
+                f"{particle_spec[0]} particles are not on this GPU path here (mixtures)")
         raise TypeError(f"unknown particle kind {particle_spec[0]!r}")
     m = np.asarray(particle_spec[1], dtype=np.complex128).reshape(-1)
     if m.size != n_wl:
@@ -179,12 +197,34 @@ def ensemble_compute(items, wavelengths, mixture, greek, all_orders, mu, normali
     if all_orders:
         raise InvalidInputError("greek='all' is not on the GPU path: give an order")
     wl = np.ascontiguousarray(wavelengths, dtype=np.float64).reshape(-1)
+    mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
+    L = -1 if greek is None else int(greek)
+    kinds = {p[0] if isinstance(p, tuple) and p else None for _, p, _ in items}
+    if "spheroid" in kinds:
+        if len(items) != 1 or (isinstance(items[0][0], tuple) and items[0][0][0] == "multimodal"):
+            raise InvalidInputError("spheroids take one distribution on the GPU path")
+        spec, particle, _ = items[0]
+        eps, m = _spheroid(particle, wl.size)
+        out = _native.ensemble_adaptive_spheroid(
+            _adaptive_dists([spec]), wl, eps, m, mu, L, bool(normalized), float(rtol),
+            int(max_panels), bool(allow_unvalidated), bool(refine_backscatter))
+        return _adaptive_dict(out, mu.size, 0)
+    if "layered" in kinds:
+        # One layered component, one distribution (mixtures of layered spheres are not on the
+        # GPU path).
+        if len(items) != 1 or (isinstance(items[0][0], tuple) and items[0][0][0] == "multimodal"):
+            raise InvalidInputError("layered spheres take one distribution on the GPU path")
+        spec, particle, _ = items[0]
+        fr, ml = _layers(particle, wl.size)
+        out = _native.ensemble_adaptive_layered(
+            _adaptive_dists([spec]), wl, fr[None], ml[None], mu, L, bool(normalized),
+            float(rtol), int(max_panels), bool(allow_unvalidated), bool(refine_backscatter))
+        return _adaptive_dict(out, mu.size, 0)
     comps = []
     for spec, particle, weight in items:
         dists, mode_w = _modes(spec)
         comps.append((dists, mode_w, float(weight), _sphere_m(particle, wl.size)))
-    mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
-    out = _native.ensemble_mixture(comps, wl, mu, -1 if greek is None else int(greek),
+    out = _native.ensemble_mixture(comps, wl, mu, L,
                                    bool(normalized), float(rtol), int(max_panels),
                                    bool(allow_unvalidated), bool(refine_backscatter))
     return _adaptive_dict(out, mu.size, 0)
@@ -199,8 +239,24 @@ def ensemble_compute_batch(specs, particle_spec, wavelengths, greek, all_orders,
     if all_orders:
         raise InvalidInputError("greek='all' is not on the GPU path: give an order")
     wl = np.ascontiguousarray(wavelengths, dtype=np.float64).reshape(-1)
-    m = _sphere_m(particle_spec, wl.size)
     mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
+    if isinstance(particle_spec, tuple) and particle_spec and particle_spec[0] == "spheroid":
+        eps, m = _spheroid(particle_spec, wl.size)
+        out = _native.ensemble_adaptive_spheroid(
+            _adaptive_dists(list(specs)), wl, eps, m, mu, -1 if greek is None else int(greek),
+            bool(normalized), float(rtol), int(max_panels), bool(allow_unvalidated),
+            bool(refine_backscatter), batch=True)
+        return _adaptive_dict(out, mu.size, 0)
+    if isinstance(particle_spec, tuple) and particle_spec and particle_spec[0] == "layered":
+        fr, ml = _layers(particle_spec, wl.size)
+        n = len(specs)
+        out = _native.ensemble_adaptive_layered(
+            _adaptive_dists(list(specs)), wl, np.broadcast_to(fr, (n,) + fr.shape),
+            np.broadcast_to(ml, (n,) + ml.shape), mu, -1 if greek is None else int(greek),
+            bool(normalized), float(rtol), int(max_panels), bool(allow_unvalidated),
+            bool(refine_backscatter), batch=True)
+        return _adaptive_dict(out, mu.size, 0)
+    m = _sphere_m(particle_spec, wl.size)
     out = _native.ensemble_adaptive(_adaptive_dists(list(specs)), wl, m, mu,
                                     -1 if greek is None else int(greek), bool(normalized),
                                     float(rtol), int(max_panels), bool(allow_unvalidated),
@@ -210,12 +266,15 @@ def ensemble_compute_batch(specs, particle_spec, wavelengths, greek, all_orders,
 
 def ensemble_compute_fixed(specs, particle_spec, wavelengths, greek, all_orders, mu, normalized,
                            n_nodes: int = 256, spread: float = 5.0, allow_unvalidated=False,
-                           ranges=None, derivatives=()) -> dict:
+                           ranges=None, derivatives=(), tmatrix_rtol: float = 1e-8) -> dict:
     """The batch dict on a fixed grid. ``derivatives`` selects parameters by their index in
     ``ensemble_parameters([(specs[0], particle_spec, 1.0)], False)`` (the reference's
-    ``deriv_idx``); they need homogeneous spheres and every distribution of one kind."""
-    if not isinstance(particle_spec, tuple) or particle_spec[0] not in ("sphere", "layered"):
-        raise TypeError("the fixed-grid ensemble takes ('sphere', m) or ('layered', fractions, m)")
+    ``deriv_idx``); they need homogeneous spheres and every distribution of one kind. Spheroids
+    (``('spheroid', aspect_ratio, m)``) converge every node's T-matrix to ``tmatrix_rtol``."""
+    if not isinstance(particle_spec, tuple) or particle_spec[0] not in ("sphere", "layered",
+                                                                         "spheroid"):
+        raise TypeError("the fixed-grid ensemble takes ('sphere', m), ('layered', fractions, m) "
+                        "or ('spheroid', aspect_ratio, m)")
     if all_orders:
         raise InvalidInputError("the fixed-grid ensemble needs a finite Greek order")
     wl = np.ascontiguousarray(wavelengths, dtype=np.float64).reshape(-1)
@@ -224,7 +283,16 @@ def ensemble_compute_fixed(specs, particle_spec, wavelengths, greek, all_orders,
     L = -1 if greek is None else int(greek)
     derivatives = [int(k) for k in derivatives]
     d = dp = dg = None
-    if particle_spec[0] == "layered":
+    if particle_spec[0] == "spheroid":
+        if derivatives:
+            raise InvalidInputError("derivatives of spheroids are not on the fixed grid")
+        m = np.asarray(particle_spec[2], dtype=np.complex128)
+        if m.ndim == 1:
+            m = np.broadcast_to(m, (dists.size, wl.size))
+        values, phase, g, _ = _native.ensemble_fixed_spheroid(
+            dists, wl, float(particle_spec[1]), m, mu, n_nodes, L, bool(normalized),
+            tmatrix_rtol=tmatrix_rtol)
+    elif particle_spec[0] == "layered":
         if derivatives:
             raise InvalidInputError("derivatives of layered spheres are not on the fixed grid")
         fr = np.asarray(particle_spec[1], dtype=np.float64).reshape(-1)

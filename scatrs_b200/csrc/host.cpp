@@ -160,6 +160,7 @@ struct Context {
   DevBuf tm_geoms, tm_jobs, tm_rules, tm_node, tm_rad, tm_ang, tm_J, tm_work, tm_piv, tm_T, tm_sums,
       tm_err;
   DevBuf ro_sph, ro_rank, ro_w, ro_part, ro_f, ro_greek, ro_mu, ro_proj;
+  DevBuf p1_fr, p1_ml;  // layered parts of an adaptive call
   std::map<int64_t, std::vector<double>> dd_rules;  // n -> per node x (hi, lo), w (hi, lo)
   std::vector<int> chunk_n_host;
   int* pinned_chunk_n = nullptr;
@@ -1022,9 +1023,12 @@ struct AdOutputs {
 // own panels, or (batch) every part with a range on one shared group per wavelength; pass 2 on
 // the final panels; each part's averages; the mixing and the outputs per (output unit,
 // wavelength), unit-major.
+// With layers (n_layers > 1), every part p is a layered sphere with the fractions
+// layers->fractions[p][L - 1] and indices layers->m[p][L][n_wl] (the parts' m unused).
 void adaptive_call(const std::vector<AdPart>& in, int n_out, bool batch, const double* wavelengths,
                    int64_t n_wl, const double* mu, int64_t n_mu,
-                   const scatrs_adaptive_options* options, const AdOutputs& res) {
+                   const scatrs_adaptive_options* options, const AdOutputs& res,
+                   const scatrs_layers* layers = nullptr) {
   if (!options) throw Failure{SCATRS_INVALID_INPUT, "options must not be NULL"};
   if (n_wl < 0) throw Failure{SCATRS_INVALID_INPUT, "negative sizes"};
   const adaptive::Options o{options->rtol, options->max_panels, options->allow_unvalidated != 0,
@@ -1060,14 +1064,38 @@ void adaptive_call(const std::vector<AdPart>& in, int n_out, bool batch, const d
   double* wl_d = c.wl.as<double>(n_wl);
   SB_CUDA(cudaMemcpyAsync(wl_d, wavelengths, n_wl * 8, cudaMemcpyHostToDevice, s));
   // Each pipeline unit's m, and a distinct index per (part, wavelength) for pass 1.
-  std::vector<double> m_unit(2 * n_units);
-  for (int64_t u = 0; u < n_units; ++u) {
-    const int64_t p = u / n_wl, i = u % n_wl;
-    m_unit[2 * u] = in[p].m[2 * i];
-    m_unit[2 * u + 1] = in[p].m[2 * i + 1];
-  }
+  const int L = layers && layers->n_layers > 1 ? layers->n_layers : 1;
+  if (L > 16) throw Failure{SCATRS_INVALID_INPUT, "the GPU path takes 1 to 16 layers"};
+  if (L > 1 && (!layers->fractions || !layers->m))
+    throw Failure{SCATRS_INVALID_INPUT, "layers must give fractions and m"};
+  std::vector<double> m_unit(2 * n_units, 0.0);
+  if (L == 1)
+    for (int64_t u = 0; u < n_units; ++u) {
+      const int64_t p = u / n_wl, i = u % n_wl;
+      m_unit[2 * u] = in[p].m[2 * i];
+      m_unit[2 * u + 1] = in[p].m[2 * i + 1];
+    }
   double* m_d = c.m.as<double>(2 * n_units);
   SB_CUDA(cudaMemcpyAsync(m_d, m_unit.data(), 2 * n_units * 8, cudaMemcpyHostToDevice, s));
+  // Layered parts: the fractions and layer indices on the device for pass 1 and pass 2.
+  double* fr_d = nullptr;
+  double* ml_d = nullptr;
+  if (L > 1) {
+    for (int64_t p = 0; p < n_parts; ++p)
+      for (int l = 0; l < L - 1; ++l) {
+        const double f = layers->fractions[p * (L - 1) + l];
+        const double prev = l > 0 ? layers->fractions[p * (L - 1) + l - 1] : 0.0;
+        if (!(f > 0.0 && f <= 1.0 && f >= prev))
+          throw Failure{SCATRS_INVALID_INPUT,
+                        in[p].who + "radius fractions must be nondecreasing in (0, 1]"};
+      }
+    fr_d = c.p1_fr.as<double>((size_t)n_parts * (L - 1));
+    ml_d = c.p1_ml.as<double>((size_t)2 * n_parts * L * n_wl);
+    SB_CUDA(cudaMemcpyAsync(fr_d, layers->fractions, (size_t)n_parts * (L - 1) * 8,
+                            cudaMemcpyHostToDevice, s));
+    SB_CUDA(cudaMemcpyAsync(ml_d, layers->m, (size_t)2 * n_parts * L * n_wl * 8,
+                            cudaMemcpyHostToDevice, s));
+  }
   // Node evaluations on the device (queries carry the pipeline unit in `wl`), in batches of at
   // most kRows scratch rows.
   constexpr int64_t kRows = int64_t(1) << 26;
@@ -1104,7 +1132,7 @@ void adaptive_call(const std::vector<AdPart>& in, int n_out, bool batch, const d
       a.radius = c.p1_radius.as<double>(n);
       a.wl_index = c.p1_wl.as<int>(n);
       a.scratch = c.p1_scratch.as<int64_t>(n + 1);
-      a.uz = c.p1_uz.as<double2>(rows);
+      a.uz = c.p1_uz.as<double2>((size_t)rows * (2 * L - 1));
       a.ux = c.p1_ux.as<double>(rows);
       a.q = c.p1_q.as<double>(6 * n);
       a.n_terms = c.p1_n.as<int64_t>(n);
@@ -1113,6 +1141,10 @@ void adaptive_call(const std::vector<AdPart>& in, int n_out, bool batch, const d
       a.m = reinterpret_cast<const double2*>(m_d);
       a.n = n;
       a.allow_unvalidated = o.allow_unvalidated ? 1 : 0;
+      a.n_layers = L;
+      a.n_wl = (int)n_wl;
+      a.fractions = fr_d;
+      a.m_layers = reinterpret_cast<const double2*>(ml_d);
       SB_CUDA(cudaMemcpyAsync((void*)a.radius, r.data(), n * 8, cudaMemcpyHostToDevice, s));
       SB_CUDA(cudaMemcpyAsync((void*)a.wl_index, wi.data(), n * 4, cudaMemcpyHostToDevice, s));
       SB_CUDA(cudaMemcpyAsync((void*)a.scratch, off.data(), (n + 1) * 8, cudaMemcpyHostToDevice,
@@ -1275,8 +1307,14 @@ void adaptive_call(const std::vector<AdPart>& in, int n_out, bool batch, const d
   call.n_wl = n_wl;
   call.n_nodes = n_nodes;
   std::vector<scatrs_distribution> dummy(n_parts);
+  LayerInput li;
+  if (L > 1) {
+    li.n_layers = L;
+    li.fractions = layers->fractions;
+    li.m_dev = ml_d;
+  }
   run_fixed(c, dummy.data(), n_parts, wl_d, n_wl, m_d, mu, n_mu, &fo, nullptr, nullptr, nullptr,
-            s, &call, LayerInput(), DerivOutput(), ad);
+            s, &call, li, DerivOutput(), ad);
   // Mixing and outputs.
   const int64_t n_outs = (int64_t)n_out * n_wl;
   int64_t vl, pl, gl;
@@ -1825,6 +1863,311 @@ void spheroid_solve(Context& c, int64_t n, const double* x, const double* aspect
   }
 }
 
+// A value and its error bound, propagated to first order through the ratios (lin.rs:7-68,
+// without derivatives).
+struct LinE {
+  double v = 0.0, e = 0.0;
+};
+LinE lin_div(const LinE& a, const LinE& b) {
+  const double v = a.v / b.v;
+  return {v, (a.e + std::fabs(v) * b.e) / std::fabs(b.v)};
+}
+LinE lin_scale(const LinE& a, double c) { return {c * a.v, std::fabs(c) * a.e}; }
+
+// The adaptive ensemble of randomly oriented spheroids (Particle::Spheroid on the engine's
+// direct path, engine.rs:369-449 for pass 1, 1207-1339 and 1558-1740 for pass 2, 1782-1836
+// for the averages, 2396-2497 for the outputs). Pass 1's node evaluations are spheroid batches
+// on the GPU (T-matrix converged to the ensemble's rtol / 100 clamped to [1e-12, 1e-8],
+// engine.rs:87, with the orientation average when Greek coefficients or phase are asked for),
+// kept for pass 2, which integrates them without solving again. One particle per call: every
+// distribution is an output unit of its own (batch: panels shared per wavelength).
+void adaptive_spheroid_call(const scatrs_distribution* dists, int64_t n_dist, bool batch,
+                            const double* wavelengths, int64_t n_wl, double eps,
+                            const double* m, const double* mu, int64_t n_mu,
+                            const scatrs_adaptive_options* options, const AdOutputs& res) {
+  if (!options) throw Failure{SCATRS_INVALID_INPUT, "options must not be NULL"};
+  if (n_dist < 0 || n_wl < 0) throw Failure{SCATRS_INVALID_INPUT, "negative sizes"};
+  const adaptive::Options o{options->rtol, options->max_panels, options->allow_unvalidated != 0,
+                            options->refine_backscatter != 0};
+  if (!(o.rtol >= 1e-13 && o.rtol <= 0.1)) {
+    char buf[80];
+    snprintf(buf, sizeof buf, "rtol must be in [1e-13, 0.1], got %g", o.rtol);
+    throw Failure{SCATRS_INVALID_INPUT, buf};
+  }
+  if (o.max_panels < 1) throw Failure{SCATRS_INVALID_INPUT, "max_panels must be at least 1"};
+  for (int64_t i = 0; i < n_wl; ++i)
+    if (!(std::isfinite(wavelengths[i]) && wavelengths[i] > 0.0))
+      throw Failure{SCATRS_INVALID_INPUT,
+                    "wavelength " + std::to_string(i) + " must be finite and > 0"};
+  if (!(std::isfinite(eps) && eps > 0.0))
+    throw Failure{SCATRS_INVALID_INPUT, "the aspect ratio must be finite and > 0"};
+  scatrs_fixed_options fo{32, options->greek_order, options->normalized,
+                          options->allow_unvalidated};
+  const int64_t n_units = n_dist * n_wl;
+  check_options(&fo, n_units, n_mu, mu);
+  if (n_units == 0) return;
+  std::vector<adaptive::Part> parts;
+  for (int64_t d = 0; d < n_dist; ++d) {
+    try {
+      parts.push_back(adaptive::make_part(dists[d].kind, dists[d].param, o.rtol));
+    } catch (const adaptive::Error& e) {
+      throw Failure{e.status, "distribution " + std::to_string(d) + ": " + e.msg};
+    }
+  }
+  const double rtol_t = std::min(std::max(o.rtol / 100.0, 1e-12), 1e-8);
+  const bool keep_greek = options->greek_order >= 0 || n_mu > 0;
+  const double pi = 3.14159265358979323846;
+  Context& c = context();
+  std::lock_guard<std::mutex> lk(c.mtx);
+  cudaStream_t s = 0;
+  // Solved nodes by (wavelength, radius bits).
+  std::map<std::pair<int64_t, uint64_t>, SpheroidResult> cache;
+  auto key_of = [](int64_t i, double r) {
+    uint64_t b;
+    memcpy(&b, &r, 8);
+    return std::make_pair(i, b);
+  };
+  auto eval = [&](const std::vector<adaptive::Query>& qs, std::vector<adaptive::NodeResult>& out) {
+    std::vector<double> xs, es, ms;
+    std::vector<size_t> which;
+    for (size_t k = 0; k < qs.size(); ++k) {
+      const int64_t i = qs[k].wl % n_wl;
+      if (cache.count(key_of(i, qs[k].r))) continue;
+      xs.push_back(2.0 * pi * qs[k].r / wavelengths[i]);
+      es.push_back(eps);
+      ms.push_back(m[2 * i]);
+      ms.push_back(m[2 * i + 1]);
+      which.push_back(k);
+    }
+    if (!which.empty()) {
+      std::vector<SpheroidResult> r;
+      // The orientation average always: Q_back, g and the depolarization numerator come
+      // from it (particle.rs:334-343).
+      spheroid_solve(c, (int64_t)which.size(), xs.data(), es.data(), ms.data(), rtol_t, 0, 0,
+                     true, r, s);
+      for (size_t k = 0; k < which.size(); ++k) {
+        const adaptive::Query& q = qs[which[k]];
+        cache[key_of(q.wl % n_wl, q.r)] = std::move(r[k]);
+      }
+    }
+    for (size_t k = 0; k < qs.size(); ++k) {
+      const SpheroidResult& v = cache.at(key_of(qs[k].wl % n_wl, qs[k].r));
+      const double area = pi * qs[k].r * qs[k].r;
+      adaptive::NodeResult& x = out[k];
+      const double q[6] = {1.0, area * v.q_ext, area * v.q_sca, area * v.q_sca * v.g,
+                           area * v.q_back, area * v.q_abs};
+      for (int j = 0; j < 6; ++j) x.q[j] = q[j];
+      x.n = v.n;
+      x.status = 0;
+    }
+  };
+  // Pass 1 per (group, wavelength): every distribution on its own, or one batch.
+  std::vector<adaptive::Job> jobs;
+  std::vector<int> job_of(n_units, -1), place(n_units, 0);
+  for (int64_t i = 0; i < n_wl; ++i) {
+    adaptive::Job shared;
+    for (int64_t p = 0; p < n_dist; ++p) {
+      if (parts[p].support == adaptive::POINT) continue;
+      const int64_t u = p * n_wl + i;
+      if (batch) {
+        if (shared.parts.empty()) shared.wl = (int)u;
+        place[u] = (int)shared.parts.size();
+        job_of[u] = -2;  // fixed below
+        shared.parts.push_back((int)p);
+      } else {
+        job_of[u] = (int)jobs.size();
+        adaptive::Job jb;
+        jb.wl = (int)u;
+        jb.parts = {(int)p};
+        jobs.push_back(jb);
+      }
+    }
+    if (batch && !shared.parts.empty()) {
+      for (int p : shared.parts) job_of[p * n_wl + i] = (int)jobs.size();
+      jobs.push_back(shared);
+    }
+  }
+  std::vector<double> wl_units(n_units);
+  for (int64_t u = 0; u < n_units; ++u) wl_units[u] = wavelengths[u % n_wl];
+  std::vector<adaptive::Query> points;
+  for (int64_t p = 0; p < n_dist; ++p)
+    if (parts[p].support == adaptive::POINT)
+      for (int64_t i = 0; i < n_wl; ++i) points.push_back({parts[p].lo, (int)(p * n_wl + i)});
+  std::vector<adaptive::NodeResult> point_res(points.size());
+  if (!points.empty()) eval(points, point_res);
+  adaptive::pass1(jobs, parts, wl_units.data(), o, eval);
+  for (const adaptive::Job& jb : jobs)
+    if (jb.status != 0) throw Failure{jb.status, jb.msg};
+  // The direct order per wavelength: every order to 2N for the phase matrix, else to the
+  // requested one (engine.rs:2073-2086).
+  const int L = options->greek_order;
+  std::vector<int64_t> n_direct(n_wl, 0);
+  for (const auto& kv : cache) n_direct[kv.first.first] = std::max<int64_t>(n_direct[kv.first.first], kv.second.n);
+  constexpr int kS = 9;  // ONE, EXT, SCA, SCAG, ABS, BACK, R2, R3, DEPOL
+  for (int64_t u = 0; u < n_units; ++u) {
+    const int64_t p = u / n_wl, i = u % n_wl;
+    const double lambda = wavelengths[i];
+    const adaptive::Part& part = parts[p];
+    const int64_t ld = !keep_greek ? -1 : n_mu == 0 ? std::min<int64_t>(L, 2 * n_direct[i])
+                                                      : 2 * n_direct[i];
+    const int64_t glen = ld + 1;  // 0 without a direct segment
+    const int64_t len = kS + 6 * glen;
+    // One node's direct quantities and declared errors (direct_scalars, direct_node).
+    std::vector<double> g(len), ge(len);
+    auto direct_node = [&](double r) {
+      const SpheroidResult& v = cache.at(key_of(i, r));
+      const double area = pi * r * r;
+      const double tau = std::max(rtol_t, v.err_est);
+      const double c4 = 4.0 * tau, c16 = 16.0 * tau;
+      const int64_t have = 2 * (int64_t)v.n + 1;
+      const double x = 2.0 * pi * r / lambda, un = 4.0 / (x * x);
+      double depol = 0.0;
+      for (int64_t l = 0; l < have; ++l) {
+        const double t = un * (v.greek[l] - 0.5 * (v.greek[have + l] - v.greek[2 * have + l]));
+        depol += l % 2 ? -t : t;
+      }
+      const double sv[kS] = {1.0,         area * v.q_ext, area * v.q_sca, area * v.q_sca * v.g,
+                             area * v.q_abs, area * v.q_back, r * r, r * r * r, area * depol};
+      const double back = area * std::max(std::fabs(v.q_back), std::fabs(v.q_sca));
+      const double se[kS] = {0.0,
+                             c4 * std::fabs(sv[1]),
+                             c4 * std::fabs(sv[2]),
+                             c4 * std::fabs(sv[2]) * (1.0 + std::fabs(v.g)),
+                             c16 * std::fabs(sv[1]),
+                             c16 * back,
+                             0.0,
+                             0.0,
+                             2.0 * c16 * back};
+      for (int k = 0; k < kS; ++k) {
+        g[k] = sv[k];
+        ge[k] = se[k];
+      }
+      if (glen > 0) {
+        double big = 0.0;
+        for (int64_t l = 0; l < have; ++l) big = std::max(big, std::fabs(un * v.greek[l]));
+        const double ce = c16 * area * big;
+        for (int f = 0; f < 6; ++f)
+          for (int64_t l = 0; l < glen; ++l) {
+            g[kS + f * glen + l] = l < have ? area * un * v.greek[f * have + l] : 0.0;
+            ge[kS + f * glen + l] = ce;
+          }
+      }
+    };
+    std::vector<double> av(len, 0.0), ae(len, 0.0);
+    bool conv = true;
+    int64_t panels = 0;
+    if (part.support == adaptive::POINT) {
+      // monodisperse_direct (engine.rs:1896-1961): the particle itself.
+      direct_node(part.lo);
+      av = g;
+      ae = ge;
+    } else {
+      const adaptive::Job& jb = jobs[job_of[u]];
+      conv = jb.converged[place[u]];
+      panels = (int64_t)jb.panels.size();
+      std::vector<double> S(len, 0.0), E(len, 0.0);
+      for (const auto& ab : jb.panels) {
+        adaptive::Node nd[15];
+        adaptive::gk15(ab.first, ab.second, nd);
+        std::vector<double> ks(len, 0.0), gs(len, 0.0), ne(len, 0.0);
+        for (int k = 0; k < 15; ++k) {
+          const double r = std::exp(nd[k].t), ur = part.u(r) * r;
+          direct_node(r);
+          for (int64_t j = 0; j < len; ++j) {
+            ks[j] += nd[k].wk * ur * g[j];
+            gs[j] += nd[k].wg * ur * g[j];
+            ne[j] += std::fabs(nd[k].wk * ur) * ge[j];
+          }
+        }
+        for (int64_t j = 0; j < len; ++j) {
+          S[j] += ks[j];
+          E[j] += std::fabs(ks[j] - gs[j]) + ne[j];
+        }
+      }
+      // averages (engine.rs:1782-1836).
+      const double z = part.mom.z, ez = part.mom.ez;
+      const double trunc = part.support == adaptive::UNBOUNDED ? 0.2 * o.rtol : 0.0;
+      for (int64_t j = 0; j < len; ++j) {
+        av[j] = S[j] / z;
+        ae[j] = (E[j] + std::fabs(av[j]) * ez) / z + trunc * std::fabs(av[j]);
+      }
+      av[6] = part.mom.v[0];
+      ae[6] = part.mom.e[0];
+      av[7] = part.mom.v[1];
+      ae[7] = part.mom.e[1];
+    }
+    // assemble (engine.rs:2396-2497).
+    auto lin = [&](int64_t j) { return LinE{av[j], ae[j]}; };
+    const LinE ext = lin(1), sca = lin(2), scag = lin(3), abs_ = lin(4), back = lin(5),
+               r2 = lin(6), r3 = lin(7), num = lin(8);
+    for (const auto& w : {std::make_pair("<C_ext>", ext), std::make_pair("<C_sca>", sca),
+                          std::make_pair("<C_back>", back)})
+      if (!(std::isfinite(w.second.v) && w.second.v != 0.0))
+        throw Failure{SCATRS_INVALID_INPUT,
+                      std::string("the ensemble's ") + w.first +
+                          " is zero or not finite, so its ratios are undefined (does m = 1?)"};
+    const LinE den{2.0 * back.v - num.v, 2.0 * back.e + num.e};
+    const LinE outs[11] = {ext,
+                           sca,
+                           abs_,
+                           back,
+                           lin_div(sca, ext),
+                           lin_div(scag, sca),
+                           lin_scale(lin_div(ext, back), 4.0 * pi),
+                           lin_div(num, den),
+                           lin_div(r3, r2),
+                           lin_scale(r2, pi),
+                           lin_scale(r3, 4.0 * pi / 3.0)};
+    for (int k = 0; k < 11; ++k) {
+      res.values[k * n_units + u] = outs[k].v;
+      if (res.errors) res.errors[k * n_units + u] = outs[k].e;
+    }
+    const bool norm = options->normalized != 0;
+    auto G = [&](int f, int64_t l) { return LinE{av[kS + f * glen + l], ae[kS + f * glen + l]}; };
+    if (L >= 0 && res.greek) {
+      const LinE a0 = G(0, 0);
+      for (int f = 0; f < 6; ++f)
+        for (int64_t l = 0; l <= L; ++l) {
+          LinE x = l < glen ? G(f, l) : LinE{};
+          if (norm) x = (f == 0 && l == 0) ? LinE{1.0, 0.0} : lin_div(x, a0);
+          res.greek[((int64_t)f * n_units + u) * (L + 1) + l] = x.v;
+          if (res.greek_err) res.greek_err[((int64_t)f * n_units + u) * (L + 1) + l] = x.e;
+        }
+    }
+    if (n_mu > 0 && res.phase) {
+      // greek_phase (engine.rs:2359-2390): combinations with exact weights, errors as bounds.
+      std::vector<double> d00(glen), d22(glen), d2m2(glen), d02(glen);
+      for (int64_t j = 0; j < n_mu; ++j) {
+        wigner_d(0, 0, mu[j], d00.data(), glen);
+        wigner_d(2, 2, mu[j], d22.data(), glen);
+        wigner_d(2, -2, mu[j], d2m2.data(), glen);
+        wigner_d(0, 2, mu[j], d02.data(), glen);
+        LinE f[6];
+        for (int64_t l = 0; l < glen; ++l) {
+          const double plus = 0.5 * (d22[l] + d2m2[l]), minus = 0.5 * (d22[l] - d2m2[l]);
+          const double w[6][2] = {{d00[l], 0}, {d02[l], 0}, {plus, minus},
+                                  {minus, plus}, {d02[l], 0}, {d00[l], 0}};
+          const int src[6][2] = {{0, -1}, {4, -1}, {1, 2}, {1, 2}, {5, -1}, {3, -1}};
+          for (int k = 0; k < 6; ++k)
+            for (int t = 0; t < 2; ++t) {
+              if (src[k][t] < 0) continue;
+              const LinE x = G(src[k][t], l);
+              f[k].v += w[k][t] * x.v;
+              f[k].e += std::fabs(w[k][t]) * x.e;
+            }
+        }
+        for (int k = 0; k < 6; ++k) {
+          const LinE x = norm ? lin_div(f[k], sca) : f[k];
+          res.phase[((int64_t)k * n_units + u) * n_mu + j] = x.v;
+          if (res.phase_err) res.phase_err[((int64_t)k * n_units + u) * n_mu + j] = x.e;
+        }
+      }
+    }
+    if (res.converged) res.converged[u] = conv ? 1 : 0;
+    if (res.panels) res.panels[u] = panels;
+  }
+}
+
 FixedCall g_last_call;  // for scatrs_check_errors
 
 template <class F>
@@ -1957,6 +2300,47 @@ int scatrs_ensemble_adaptive(const scatrs_distribution* dists, int64_t n_dist, i
                              m, 1.0, (int)d, "distribution " + std::to_string(d) + ": "});
     AdOutputs out{values, errors, phase, phase_err, greek, greek_err, converged, panels};
     adaptive_call(parts, (int)n_dist, batch != 0, wavelengths, n_wl, mu, n_mu, options, out);
+  });
+}
+
+int scatrs_ensemble_adaptive_layered(const scatrs_distribution* dists, int64_t n_dist,
+                                     int32_t batch, const double* wavelengths, int64_t n_wl,
+                                     const scatrs_layers* layers, const double* mu, int64_t n_mu,
+                                     const scatrs_adaptive_options* options, double* values,
+                                     double* errors, double* phase, double* phase_err,
+                                     double* greek, double* greek_err, int8_t* converged,
+                                     int64_t* panels, char* err, size_t err_len) {
+  return guarded(err, err_len, [&] {
+    if (n_dist < 0) throw Failure{SCATRS_INVALID_INPUT, "negative sizes"};
+    if (!layers || layers->n_layers < 1 || !layers->m ||
+        (layers->n_layers > 1 && !layers->fractions))
+      throw Failure{SCATRS_INVALID_INPUT, "layers must give n_layers >= 1, fractions and m"};
+    // One layer: a homogeneous sphere with m = layers->m[d][0][n_wl].
+    std::vector<AdPart> parts;
+    for (int64_t d = 0; d < n_dist; ++d)
+      parts.push_back(AdPart{dists[d].kind, {dists[d].param[0], dists[d].param[1],
+                                             dists[d].param[2]},
+                             layers->m + 2 * d * layers->n_layers * n_wl, 1.0, (int)d,
+                             "distribution " + std::to_string(d) + ": "});
+    AdOutputs out{values, errors, phase, phase_err, greek, greek_err, converged, panels};
+    adaptive_call(parts, (int)n_dist, batch != 0, wavelengths, n_wl, mu, n_mu, options, out,
+                  layers);
+  });
+}
+
+int scatrs_ensemble_adaptive_spheroid(const scatrs_distribution* dists, int64_t n_dist,
+                                      int32_t batch, const double* wavelengths, int64_t n_wl,
+                                      double aspect_ratio, const double* m, const double* mu,
+                                      int64_t n_mu, const scatrs_adaptive_options* options,
+                                      double* values, double* errors, double* phase,
+                                      double* phase_err, double* greek, double* greek_err,
+                                      int8_t* converged, int64_t* panels, char* err,
+                                      size_t err_len) {
+  return guarded(err, err_len, [&] {
+    if (!values || !m) throw Failure{SCATRS_INVALID_INPUT, "values and m are required"};
+    AdOutputs out{values, errors, phase, phase_err, greek, greek_err, converged, panels};
+    adaptive_spheroid_call(dists, n_dist, batch != 0, wavelengths, n_wl, aspect_ratio, m, mu,
+                           n_mu, options, out);
   });
 }
 

@@ -229,6 +229,13 @@ struct Pass1Args {
   int64_t* n_terms;
   int* status;
   int allow_unvalidated;
+  // Layered spheres (n_layers > 1): wl_index is the pipeline unit part * n_wl + i; the part's
+  // fractions [part][n_layers - 1] and indices [(part * n_layers + l) * n_wl + i]; the scratch
+  // rows then hold 2 n_layers - 1 arrays of scratch[t + 1] - scratch[t] rows each.
+  int n_layers;
+  int n_wl;
+  const double* fractions;
+  const double2* m_layers;
 };
 
 void launch_plan_chunks(const PlanArgs& a, cudaStream_t s);

@@ -270,6 +270,11 @@ __global__ void __launch_bounds__(128) mie_layered_kernel(MieFixedArgs a) {
   mie_chunk<true, false>(a);
 }
 
+// Layered spheres on adaptive panels.
+__global__ void __launch_bounds__(128) mie_layered_adaptive_kernel(MieFixedArgs a) {
+  mie_chunk<true, true>(a);
+}
+
 // Independent spheres, one per thread (the batched Mie::compute): coefficients a_1..a_N then
 // b_1..b_N per sphere, and the efficiencies.
 __global__ void __launch_bounds__(128) mie_nodes_kernel(MieNodesArgs a) {
@@ -318,9 +323,26 @@ __global__ void __launch_bounds__(128) pass1_kernel(Pass1Args a) {
   const double r = a.radius[t];
   const int wi = a.wl_index[t];
   const double x = 2.0 * kPi * r / a.wl[wi];
-  const cplx m = mk(a.m[wi].x, a.m[wi].y);
   int64_t n = default_n_max(x);
-  int st = check_node(x, m, n, a.allow_unvalidated != 0);
+  const int L = a.n_layers > 1 ? a.n_layers : 1;
+  double xs[kMaxLayers];
+  cplx ms[kMaxLayers];
+  bool lossless = true;
+  int st;
+  if (L == 1) {
+    ms[0] = mk(a.m[wi].x, a.m[wi].y);
+    st = check_node(x, ms[0], n, a.allow_unvalidated != 0);
+  } else {
+    // x_l = f_l x, the outer surface's x last (ensemble/particle.rs:186-195).
+    const int p = wi / a.n_wl, i = wi % a.n_wl;
+    for (int l = 0; l < L; ++l) {
+      xs[l] = l < L - 1 ? a.fractions[p * (L - 1) + l] * x : x;
+      const double2 mv = a.m_layers[(p * L + l) * a.n_wl + i];
+      ms[l] = mk(mv.x, mv.y);
+      lossless = lossless && mv.y == 0.0;
+    }
+    st = check_layered(xs, ms, L, n, a.allow_unvalidated != 0);
+  }
   const int64_t off = a.scratch[t], cap = a.scratch[t + 1] - off;
   if (st == 0 && n + 2 > cap) st = 1;
   a.status[t] = st;
@@ -331,12 +353,27 @@ __global__ void __launch_bounds__(128) pass1_kernel(Pass1Args a) {
     return;
   }
   Scratch s;
-  s.uz = a.uz + off;
+  s.uz = a.uz + off * (2 * L - 1);
   s.ux = a.ux + off;
   s.stride = 1;
-  mie_prepare(x, m, n, s);
+  mie_prepare(x, ms[L - 1], n, s);
   ValueSums vs;
-  const double asum = mie_finish(x, m, n, s, vs, [](int64_t, cplx, cplx) {});
+  double asum;
+  if (L == 1) {
+    asum = mie_finish(x, ms[0], n, s, vs, [](int64_t, cplx, cplx) {});
+  } else {
+    Layered lay;
+    lay.layers = L;
+    lay.x = xs;
+    lay.m = ms;
+    lay.arr.base = s.uz;
+    lay.arr.astride = cap;
+    lay.arr.stride = 1;
+    lay.prepare(n);
+    asum = mie_finish(x, ms[L - 1], n, s, vs, [](int64_t, cplx, cplx) {}, lay);
+    // A lossless particle absorbs nothing (layered/kernel.rs:455-464).
+    if (lossless) asum = 0.0;
+  }
   const Eff e = efficiencies_from(x, asum, vs);
   const double area = kPi * r * r;
   q[0] = 1.0;
@@ -364,6 +401,8 @@ void launch_mie_fixed(const MieFixedArgs& a, cudaStream_t s) {
   int blocks = (a.n_chunks * 32 + threads - 1) / threads;
   if (a.deriv)
     mie_deriv_kernel<<<blocks, threads, 0, s>>>(a);
+  else if (a.n_layers > 1 && a.wdiff)
+    mie_layered_adaptive_kernel<<<blocks, threads, 0, s>>>(a);
   else if (a.n_layers > 1)
     mie_layered_kernel<<<blocks, threads, 0, s>>>(a);
   else if (a.wdiff)
