@@ -46,6 +46,8 @@ def parse():
     p.add_argument("--scale", type=float, default=1.0, help="fraction of the batch (tests)")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-spheroids", action="store_true",
+                   help="skip the spheroid ensemble leg")
     p.add_argument("--no-projection", action="store_true",
                    help="skip the tensor-core Greek projection measurement")
     return p.parse_args()
@@ -328,6 +330,80 @@ def projection_c3(torch, steps: int = 3, scale: float = 1.0):
             "max_err_vs_fp64": err}
 
 
+# FP64 operations (DADD + DMUL + 2 DFMA) per (pair, node) of tm_surface_kernel, from the ncu
+# instruction counts of one launch divided by its pairs x nodes
+# (profiles/tm_surface_kernel_spheroids_small.md).
+TM_SURFACE_FLOP_PER_PAIR_NODE = 1799.5
+
+
+def spheroid_leg(torch, fp64_peak: float, scale: float = 1.0, cpu_seconds: float = 10.0):
+    """The fixed-grid ensemble of randomly oriented spheroids on a sample of the spheroid
+    workload (16 aspect ratios over 0.4-3.0 x 2 lognormals x 4 of its 32 wavelengths x 64
+    nodes, size parameters to 15): every node's T-matrix converged (double-double EBCM) with
+    its orientation average. Timed after one identical warm-up call; nodes per second, the
+    kernels' shares, and the surface-integral kernel's FP64 rate against the FP64 peak
+    measured in this run. The CPU baseline is the oracle's double-precision node solve on a
+    random sample of the same nodes, one thread."""
+    from scatrs_b200 import _native
+    from scatrs_b200 import workloads as W
+
+    w = W.spheroids(scale=max(1 / 32, scale / 8), x_max=15.0)
+    call = lambda: _native.ensemble_fixed_spheroid(w.dists, w.wavelengths, w.aspect_ratio, w.m,
+                                                   w.mu, w.n_nodes, w.greek_order,
+                                                   tmatrix_rtol=1e-8)
+    call()
+    torch.cuda.synchronize()
+    _native.set_profiling(True)
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    _, _, _, terms = call()
+    e.record()
+    torch.cuda.synchronize()
+    kt = _native.kernel_times()
+    work = _native.spheroid_work()
+    _native.set_profiling(False)
+    ms = s.elapsed_time(e)
+    names = ("tm_tables_kernels", "tm_surface_kernel", "tm_solve_kernel", "ro_kernels")
+    kms = {k: kt[k][0] for k in names}
+    out = {"workload": f"{w.n_nodes_total} spheroid nodes ({w.name}): 16 aspect ratios x 2 "
+                       f"lognormals x {w.wavelengths.size} wavelengths x 64 nodes, "
+                       "T-matrix rtol 1e-8, Greek order 64, 180 cosines",
+           "value": w.n_nodes_total / (ms * 1e-3), "unit": "nodes/s", "ms": ms,
+           "n_terms_max": int(terms[:, :, 0].max()), "n_terms_mean": float(terms[:, :, 0].mean()),
+           "kernels_ms": kms, "kernel_share": {k: v / ms for k, v in kms.items()}}
+    if TM_SURFACE_FLOP_PER_PAIR_NODE and kms["tm_surface_kernel"] > 0:
+        achieved = TM_SURFACE_FLOP_PER_PAIR_NODE * float(work.sum()) / (
+            kms["tm_surface_kernel"] * 1e-3) / 1e12
+        out["roofline"] = {"bound": "fp64", "kernel": "tm_surface_kernel (double-double)",
+                           "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                           "frac": achieved / fp64_peak,
+                           "peak_source": "cuBLAS DGEMM 8192^3 measured in this run"}
+    # CPU: the oracle's double-precision solve of random nodes of the same workload.
+    from oracle import oracle as O
+    rng = np.random.default_rng(1)
+    xi, _ = O.gauss_legendre(w.n_nodes)
+    done, failed, t0 = 0, 0, time.time()
+    while time.time() - t0 < cpu_seconds:
+        d = int(rng.integers(w.dists.size))
+        i = int(rng.integers(w.wavelengths.size))
+        j = int(rng.integers(w.n_nodes))
+        a, b = np.log(w.dists["r_lo"][d]), np.log(w.dists["r_hi"][d])
+        r = np.exp(0.5 * (a + b) + 0.5 * (b - a) * xi[j])
+        try:
+            O.spheroid_node(2 * np.pi * r / w.wavelengths[i], float(w.aspect_ratio[d]),
+                            complex(w.m[d, i]), 1e-8)
+        except O.OracleError:
+            failed += 1  # plain double does not converge there; its time is still spent
+        done += 1
+    dt = time.time() - t0
+    out["cpu_baseline"] = {"value": done / dt, "unit": "nodes/s", "cores": 1, "kind": "port",
+                           "sample": f"{done} random nodes of the same workload in {dt:.1f} s "
+                                     f"({failed} of them not converging in double): the "
+                                     "oracle's double-precision EBCM (converged) and "
+                                     "orientation average, one thread"}
+    return out
+
+
 def ours(args):
     import torch
 
@@ -469,6 +545,8 @@ def ours(args):
     line["clocks"] = clk.summary()
     if world == 1 and not args.no_projection:
         line["projection_tc"] = projection_c3(torch, scale=args.scale)
+    if world == 1 and not args.no_spheroids:
+        line["spheroids"] = spheroid_leg(torch, line["roofline"]["peak"], scale=args.scale)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_sample(w, args.cpu_seconds)
     print(json.dumps(line), flush=True)

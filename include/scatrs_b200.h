@@ -381,6 +381,11 @@ int64_t scatrs_launch_count(void);
  * kernels. */
 void scatrs_set_profiling(int32_t on);
 int scatrs_kernel_times(double* ms, int64_t* launches, int32_t n);
+/* While profiling: the work of each tm_surface_kernel launch (the sum over its modes of K^2
+ * pairs times 2 n_theta nodes) into per_launch[cap]; returns the number of launches. Kernel ids
+ * 6-9 of scatrs_kernel_times are the T-matrix tables, surface integrals, solve and the
+ * orientation average. */
+int64_t scatrs_spheroid_work(int64_t* per_launch, int64_t cap);
 
 /* Gauss-Legendre rule of n points on [-1, 1] (ascending nodes), as the host tables use it
  * (scatrs/src/special/gauss_legendre.rs:188-260). */

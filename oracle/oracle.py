@@ -610,3 +610,16 @@ def ensemble_fixed_spheroid(dists: np.ndarray, wavelengths, eps, m, n_nodes: int
     if L >= 0:
         out["greek"] = greek
     return out
+
+
+def spheroid_node(x: float, eps: float, s: complex, rtol: float = 1e-8):
+    """One spheroid node of the ensemble's direct path in double precision: (Q_ext, Q_sca,
+    Q_abs, Q_back, g), N, n_theta."""
+    q = np.zeros(5)
+    n = np.zeros(2, dtype=np.int32)
+    f = lib().orc_spheroid_node
+    f.argtypes = [_D, _D, _D, _D, _D, _PD, ctypes.c_void_p]
+    st = f(x, eps, s.real, s.imag, rtol, _p(q), n.ctypes.data)
+    if st != 0:
+        raise OracleError(st, "spheroid_node")
+    return q, int(n[0]), int(n[1])

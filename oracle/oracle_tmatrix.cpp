@@ -417,3 +417,24 @@ int spheroid_node(double x, double eps, cplx s, double rtol, SpheroidNode* out) 
 }
 
 }  // namespace orc
+
+extern "C" {
+
+// One spheroid node of the ensemble's direct path (oracle_spheroid.hpp): q[5] = Q_ext, Q_sca,
+// Q_abs, Q_back, g; n[2] = N, n_theta. Returns the status.
+int orc_spheroid_node(double x, double eps, double s_re, double s_im, double rtol, double* q,
+                      int* n) {
+  orc::SpheroidNode v;
+  const int st = orc::spheroid_node(x, eps, C(s_re, s_im), rtol, &v);
+  if (st != OK) return st;
+  q[0] = v.q_ext;
+  q[1] = v.q_sca;
+  q[2] = v.q_abs;
+  q[3] = v.q_back;
+  q[4] = v.g;
+  n[0] = v.n;
+  n[1] = v.nth;
+  return OK;
+}
+
+}  // extern "C"

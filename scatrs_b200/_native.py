@@ -95,6 +95,7 @@ SYMBOLS = {
                                                     _SZ]),
     "scatrs_spheroid_compute": (ctypes.c_int, [_I64, _PD, _PD, _PD, ctypes.POINTER(SpheroidOptions),
                                                _PD, _PD, _VP, _VP, _PD, _CP, _SZ]),
+    "scatrs_spheroid_work": (ctypes.c_int64, [_VP, _I64]),
     "scatrs_check_errors": (ctypes.c_int, [_VP, _CP, _SZ]),
     "scatrs_mie": (ctypes.c_int, [_PD, _PD, _I64, _I32, _PI64, _PI64, _PD, _PD, _CP, _SZ]),
     "scatrs_mie_static": (ctypes.c_int, [_VP, _VP, _I64, _I32, _I64, _VP, _VP, _VP, _VP, _VP,
@@ -108,7 +109,8 @@ SYMBOLS = {
 }
 
 KERNEL_NAMES = ("plan_chunks_kernel", "mie_fixed_kernel", "unit_kernel", "mie_nodes_kernel",
-                "final_kernel", "proj_kernel")
+                "final_kernel", "proj_kernel", "tm_tables_kernels", "tm_surface_kernel",
+                "tm_solve_kernel", "ro_kernels")
 # The kernels each id covers: K-a also as mie_layered_kernel / mie_deriv_kernel, the unit kernel
 # as unit_deriv_kernel, the final kernel as final_deriv_kernel.
 
@@ -161,10 +163,18 @@ def set_profiling(on: bool) -> None:
 
 def kernel_times() -> dict:
     """{kernel: (total ms, launches)} since set_profiling (synchronizes)."""
-    ms = np.zeros(8)
-    n = np.zeros(8, dtype=np.int64)
-    k = load().scatrs_kernel_times(_p(ms), n.ctypes.data_as(_PI64), 8)
+    ms = np.zeros(len(KERNEL_NAMES))
+    n = np.zeros(len(KERNEL_NAMES), dtype=np.int64)
+    k = load().scatrs_kernel_times(_p(ms), n.ctypes.data_as(_PI64), len(KERNEL_NAMES))
     return {KERNEL_NAMES[i]: (float(ms[i]), int(n[i])) for i in range(k)}
+
+
+def spheroid_work() -> np.ndarray:
+    """While profiling: each tm_surface_kernel launch's (pair, node) count."""
+    n = int(load().scatrs_spheroid_work(None, 0))
+    out = np.zeros(n, dtype=np.int64)
+    load().scatrs_spheroid_work(out.ctypes.data, n)
+    return out
 
 
 def mie(x, m, allow_unvalidated: bool = False):

@@ -54,15 +54,28 @@ DD_FN dd operator+(dd x, double y) {
   return fast_two_sum(s.hi, s.lo);
 }
 DD_FN dd operator-(dd x, double y) { return x + (-y); }
+// Products: the exact error of hi * hi from one fma, the cross terms folded into it by two
+// more.
 DD_FN dd operator*(dd x, dd y) {
-  dd p = two_prod(x.hi, y.hi);
-  p.lo += x.hi * y.lo + x.lo * y.hi;
-  return fast_two_sum(p.hi, p.lo);
+  const double p = x.hi * y.hi;
+  double e = fma(x.hi, y.hi, -p);
+  e = fma(x.hi, y.lo, e);
+  e = fma(x.lo, y.hi, e);
+  return fast_two_sum(p, e);
 }
 DD_FN dd operator*(dd x, double y) {
-  dd p = two_prod(x.hi, y);
-  p.lo += x.lo * y;
-  return fast_two_sum(p.hi, p.lo);
+  const double p = x.hi * y;
+  double e = fma(x.hi, y, -p);
+  e = fma(x.lo, y, e);
+  return fast_two_sum(p, e);
+}
+// x + y with one two-sum (the low parts added in double): its error is about 2^-106 of
+// max(|x|, |y|) rather than of |x + y|, which sums whose accuracy is measured against the
+// size of their terms can afford.
+DD_FN dd add_terms(dd x, dd y) {
+  dd s = two_sum(x.hi, y.hi);
+  s.lo += x.lo + y.lo;
+  return fast_two_sum(s.hi, s.lo);
 }
 DD_FN dd operator/(dd x, double y) {
   const double q1 = x.hi / y;
@@ -170,6 +183,12 @@ DD_FN cdd operator*(cdd a, cdd b) {
 DD_FN cdd operator*(cdd a, dd s) { return cdd{a.re * s, a.im * s}; }
 DD_FN cdd operator*(cdd a, double s) { return cdd{a.re * s, a.im * s}; }
 DD_FN cdd times_i(cdd a) { return cdd{-a.im, a.re}; }
+// Complex operations with add_terms.
+DD_FN cdd add_terms(cdd a, cdd b) { return cdd{add_terms(a.re, b.re), add_terms(a.im, b.im)}; }
+DD_FN cdd sub_terms(cdd a, cdd b) { return cdd{add_terms(a.re, -b.re), add_terms(a.im, -b.im)}; }
+DD_FN cdd mul_terms(cdd a, cdd b) {
+  return cdd{add_terms(a.re * b.re, -(a.im * b.im)), add_terms(a.re * b.im, a.im * b.re)};
+}
 DD_FN dd norm2(cdd a) { return a.re * a.re + a.im * a.im; }
 // 1 / a, scaled by a power of two first so that |a|^2 neither overflows nor underflows.
 DD_FN cdd inv(cdd a) {

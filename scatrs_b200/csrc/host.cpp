@@ -35,8 +35,23 @@ static std::atomic<int64_t> g_launches{0};
 
 // Optional per-kernel timing: CUDA events recorded around each launch on its stream, read back
 // by scatrs_kernel_times (which synchronizes). Off unless scatrs_set_profiling(1).
-enum KernelId { K_PLAN = 0, K_MIE = 1, K_UNITS = 2, K_NODES = 3, K_FINAL = 4, K_PROJ = 5, K_COUNT = 6 };
+enum KernelId {
+  K_PLAN = 0,
+  K_MIE = 1,
+  K_UNITS = 2,
+  K_NODES = 3,
+  K_FINAL = 4,
+  K_PROJ = 5,
+  K_TM_TABLES = 6,   // tm_geom_kernel + tm_angular_kernel
+  K_TM_SURFACE = 7,  // tm_surface_kernel
+  K_TM_SOLVE = 8,    // tm_solve_kernel
+  K_RANDOM = 9,      // the orientation average's five kernels
+  K_COUNT = 10
+};
 static bool g_profiling = false;
+// The spheroid surface integrals' work per tm_surface_kernel launch while profiling: the sum
+// over the launch's modes of K^2 (i, k) pairs times the 2 n_theta nodes.
+static std::vector<int64_t> g_tm_pair_nodes;
 struct Timed {
   int id;
   cudaEvent_t a, b;
@@ -1624,7 +1639,14 @@ void run_tmatrices(Context& c, const std::vector<TmSpec>& specs, std::vector<dou
                             cudaMemcpyHostToDevice, s));
     SB_CUDA(cudaMemcpyAsync(rl, rules.data(), rules.size() * 8, cudaMemcpyHostToDevice, s));
     SB_CUDA(cudaMemsetAsync(a.err, 0, sizeof(unsigned), s));
-    timed_launch(K_UNITS, s, [&] { launch_tmatrix(a, s); });
+    if (g_profiling) {
+      int64_t pn = 0;
+      for (const TmJob& jb : jobs) pn += (int64_t)jb.K * jb.K * 2 * geoms[jb.geom].n_theta;
+      g_tm_pair_nodes.push_back(pn);
+    }
+    timed_launch(K_TM_TABLES, s, [&] { launch_tm_tables(a, s); });
+    timed_launch(K_TM_SURFACE, s, [&] { launch_tm_surface(a, s); });
+    timed_launch(K_TM_SOLVE, s, [&] { launch_tm_solve(a, s); });
     SB_CUDA(cudaGetLastError());
     std::vector<double> greek_all;
     std::vector<RoSph> sph;
@@ -1686,7 +1708,7 @@ void run_tmatrices(Context& c, const std::vector<TmSpec>& specs, std::vector<dou
       SB_CUDA(cudaMemcpyAsync(mu_d, mus.data(), mus.size() * 8, cudaMemcpyHostToDevice, s));
       SB_CUDA(cudaMemcpyAsync((void*)proj_d, projs.data(), projs.size() * sizeof(double*),
                               cudaMemcpyHostToDevice, s));
-      timed_launch(K_PROJ, s, [&] { launch_random(r, s); });
+      timed_launch(K_RANDOM, s, [&] { launch_random(r, s); });
       SB_CUDA(cudaGetLastError());
       greek_all.resize((size_t)g);
       SB_CUDA(cudaMemcpyAsync(greek_all.data(), r.greek, (size_t)g * 8, cudaMemcpyDeviceToHost, s));
@@ -2839,6 +2861,13 @@ void scatrs_set_profiling(int32_t on) {
     sb::g_kernel_ms[k] = 0.0;
     sb::g_kernel_launches[k] = 0;
   }
+  sb::g_tm_pair_nodes.clear();
+}
+
+int64_t scatrs_spheroid_work(int64_t* per_launch, int64_t cap) {
+  for (int64_t k = 0; k < cap && k < (int64_t)sb::g_tm_pair_nodes.size(); ++k)
+    per_launch[k] = sb::g_tm_pair_nodes[k];
+  return (int64_t)sb::g_tm_pair_nodes.size();
 }
 
 int scatrs_kernel_times(double* ms, int64_t* launches, int32_t n) {

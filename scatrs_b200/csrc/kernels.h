@@ -306,6 +306,9 @@ struct TmArgs {
   int max_sweeps;
 };
 void launch_tmatrix(const TmArgs& a, cudaStream_t s);
+void launch_tm_tables(const TmArgs& a, cudaStream_t s);
+void launch_tm_surface(const TmArgs& a, cudaStream_t s);
+void launch_tm_solve(const TmArgs& a, cudaStream_t s);
 
 // The orientation average of a spheroid's phase matrix from its T-matrix (random.cu): one
 // entry per spheroid, whose modes 0..N are the consecutive jobs from job0 of a TmArgs batch.

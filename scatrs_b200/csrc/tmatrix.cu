@@ -234,24 +234,36 @@ __global__ void __launch_bounds__(128) tm_surface_kernel(TmArgs a) {
     const double* ak = a.ang + jb.ang0 + ((int64_t)q * (N + 1) + k) * kAngD;
     const dd di = ld(ai), pii = ld(ai + 2), ti = ld(ai + 4);
     const dd dk = ld(ak), pik = ld(ak + 2), tk = ld(ak + 4);
-    const dd A1 = pii * tk + ti * pik, A2 = pii * pik + ti * tk;
+    // The sums below are measured against their terms (add_terms): the surface integrals'
+    // accuracy is about 2^-106 of the largest term, which is what the cancellation needs.
+    const dd A1 = ddm::add_terms(pii * tk, ti * pik), A2 = ddm::add_terms(pii * pik, ti * tk);
     const dd A3 = ti * dk, A4 = di * tk, A5 = pii * dk, A6 = di * pik;
     const cdd w = ldc(rk + 8), wd = ldc(rk + 12), u = ldc(rk + 16);
     const dd jr = ld(ri), jdr = ld(ri + 2), yr = ld(ri + 4), ydr = ld(ri + 6);
+    const dd nk = nu * ckk, ni = nu * cki;
 #pragma unroll
     for (int o = 0; o < 2; ++o) {
+      // z = j (real) for the regular functions, j + i y for the outgoing ones.
       const cdd z = o ? cdd{jr, yr} : cdd{jr, mkdd(0.0)};
       const cdd zd = o ? cdd{jdr, ydr} : cdd{jdr, mkdd(0.0)};
       const cdd zr = z * ir;
-      const cdd mm = ddm::times_i((z * w) * A1);
-      const cdd mn = (z * wd) * A2 - ((z * u) * A3) * (nu * ckk);
-      const cdd nm = ((zr * w) * A4) * (nu * cki) - (zd * w) * A2;
-      const cdd nn = ddm::times_i((zd * wd) * A1 -
-                                  (((zd * u) * A5) * ckk + ((zr * wd) * A6) * cki) * nu);
-      J[o * 4 + 0] = J[o * 4 + 0] + mm * fac;
-      J[o * 4 + 1] = J[o * 4 + 1] + mn * fac;
-      J[o * 4 + 2] = J[o * 4 + 2] + nm * fac;
-      J[o * 4 + 3] = J[o * 4 + 3] + nn * fac;
+      const cdd zw = o ? ddm::mul_terms(z, w) : w * jr;
+      const cdd zwd = o ? ddm::mul_terms(z, wd) : wd * jr;
+      const cdd zu = o ? ddm::mul_terms(z, u) : u * jr;
+      const cdd zdw = o ? ddm::mul_terms(zd, w) : w * jdr;
+      const cdd zdwd = o ? ddm::mul_terms(zd, wd) : wd * jdr;
+      const cdd zdu = o ? ddm::mul_terms(zd, u) : u * jdr;
+      const cdd zrw = o ? ddm::mul_terms(zr, w) : w * zr.re;
+      const cdd zrwd = o ? ddm::mul_terms(zr, wd) : wd * zr.re;
+      const cdd mm = ddm::times_i(zw * A1);
+      const cdd mn = ddm::sub_terms(zwd * A2, (zu * A3) * nk);
+      const cdd nm = ddm::sub_terms((zrw * A4) * ni, zdw * A2);
+      const cdd nn = ddm::times_i(ddm::sub_terms(
+          zdwd * A1, ddm::add_terms((zdu * A5) * ckk, (zrwd * A6) * cki) * nu));
+      J[o * 4 + 0] = ddm::add_terms(J[o * 4 + 0], mm * fac);
+      J[o * 4 + 1] = ddm::add_terms(J[o * 4 + 1], mn * fac);
+      J[o * 4 + 2] = ddm::add_terms(J[o * 4 + 2], nm * fac);
+      J[o * 4 + 3] = ddm::add_terms(J[o * 4 + 3], nn * fac);
     }
   }
   // g_i g_k = sqrt((2i+1)(2k+1) / (16 pi^2 i(i+1) k(k+1))).
@@ -428,7 +440,10 @@ __global__ void __launch_bounds__(256) tm_solve_kernel(TmArgs a) {
       for (int j = 0; j < n2; ++j) {
         const cdd qv = ldc(qrow + 4 * j);
         const Cd x = X[(int64_t)j * n2 + c];
-        acc = acc - cdd{qv.re * x.re - qv.im * x.im, qv.re * x.im + qv.im * x.re};
+        // The residual's accuracy is measured against its terms (2^-106 of |Q^T| |X|), as
+        // mixed-precision refinement needs.
+        acc = ddm::sub_terms(acc, cdd{ddm::add_terms(qv.re * x.re, -(qv.im * x.im)),
+                                      ddm::add_terms(qv.re * x.im, qv.im * x.re)});
       }
       const Cd rv{acc.re.hi + acc.re.lo, acc.im.hi + acc.im.lo};
       R[idx] = rv;
@@ -478,12 +493,23 @@ __global__ void __launch_bounds__(256) tm_solve_kernel(TmArgs a) {
   }
 }
 
-void launch_tmatrix(const TmArgs& a, cudaStream_t s) {
+void launch_tm_tables(const TmArgs& a, cudaStream_t s) {
   if (a.n_jobs <= 0) return;
   tm_geom_kernel<<<(unsigned)((a.n_node_total + 127) / 128), 128, 0, s>>>(a);
   tm_angular_kernel<<<(unsigned)((a.n_ang_total + 127) / 128), 128, 0, s>>>(a);
+}
+void launch_tm_surface(const TmArgs& a, cudaStream_t s) {
+  if (a.n_jobs <= 0) return;
   tm_surface_kernel<<<(unsigned)((a.n_pair_total + 127) / 128), 128, 0, s>>>(a);
+}
+void launch_tm_solve(const TmArgs& a, cudaStream_t s) {
+  if (a.n_jobs <= 0) return;
   tm_solve_kernel<<<a.n_jobs, 256, 0, s>>>(a);
+}
+void launch_tmatrix(const TmArgs& a, cudaStream_t s) {
+  launch_tm_tables(a, s);
+  launch_tm_surface(a, s);
+  launch_tm_solve(a, s);
 }
 
 }  // namespace sb

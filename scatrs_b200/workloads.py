@@ -157,3 +157,54 @@ def config4(seed: int = 0, scale: float = 1.0, mu: np.ndarray | None = None) -> 
     mu = gauss_legendre(180) if mu is None else mu
     return LayeredWorkload(f"config4(seed={seed},scale={scale})", lognormals(med, wid, 4), wl, f,
                            ml, mu, 256, 32)
+
+
+@dataclass
+class SpheroidWorkload:
+    name: str
+    dists: np.ndarray       # DIST_DTYPE, (n_dist,)
+    wavelengths: np.ndarray
+    aspect_ratio: np.ndarray  # (n_dist,)
+    m: np.ndarray             # complex128 (n_dist, n_wl)
+    mu: np.ndarray
+    n_nodes: int
+    greek_order: int
+
+    @property
+    def n_units(self) -> int:
+        return self.dists.size * self.wavelengths.size
+
+    @property
+    def n_nodes_total(self) -> int:
+        return self.n_units * self.n_nodes
+
+
+def spheroids(seed: int = 0, scale: float = 1.0, per_ratio: int = 2, x_max: float = 25.0,
+              mu: np.ndarray | None = None) -> SpheroidWorkload:
+    """Randomly oriented spheroids: 16 aspect ratios log-spaced over 0.4-3.0, `per_ratio`
+    lognormal volume-equivalent size distributions each (median uniform 0.2-1.5, width uniform
+    1.5-2.0), m = 1.53 + k i with k log-uniform 1e-4-1e-1 per distribution, 32 wavelengths
+    log-spaced over 0.35-1.0, 64 Gauss nodes in ln r over median width^(+-2) with the upper end
+    capped where the size parameter at the shortest wavelength reaches `x_max` (the workload's
+    sizes reach about 25); Greek order 64, 180 Gauss cosines."""
+    rng = np.random.default_rng(seed)
+    eps = np.repeat(np.geomspace(0.4, 3.0, 16), per_ratio)
+    n_dist, n_wl = eps.size, 32
+    wl = np.geomspace(0.35, 1.0, n_wl)
+    med = rng.uniform(0.2, 1.5, n_dist)
+    wid = rng.uniform(1.5, 2.0, n_dist)
+    k = np.exp(rng.uniform(np.log(1e-4), np.log(1e-1), n_dist))
+    m = np.repeat((1.53 + 1j * k)[:, None], n_wl, axis=1)
+    d = np.zeros(n_dist, dtype=DIST_DTYPE)
+    d["kind"] = KINDS["lognormal"]
+    d["param"][:, 0] = med
+    d["param"][:, 1] = wid
+    r_cap = x_max * wl.min() / (2 * np.pi)
+    d["r_hi"] = np.minimum(med * wid ** 2, r_cap)
+    d["r_lo"] = np.minimum(med * wid ** -2, d["r_hi"] / 4)
+    if scale < 1.0:
+        kw = max(1, int(round(n_wl * scale)))
+        wl, m = wl[:kw], m[:, :kw]
+    mu = gauss_legendre(180) if mu is None else mu
+    return SpheroidWorkload(f"spheroids(seed={seed},scale={scale},x_max={x_max})", d, wl, eps, m,
+                            mu, 64, 64)
