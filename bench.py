@@ -78,7 +78,7 @@ def total_nodes(world: int, nodes_per_rank: int) -> int:
 
 
 def workload_config(w, args):
-    return {"workload": "config2: 1024 wavelengths x 64 lognormal distributions x 512 ln-r Gauss "
+    return {"workload": "batched_spheres: 1024 wavelengths x 64 lognormal distributions x 512 ln-r Gauss "
                         "nodes, m per (distribution, wavelength), 360 Gauss cosines, Greek L=64",
             "n_dist": int(w.dists.size), "n_wl": int(w.wavelengths.size),
             "n_nodes": int(w.n_nodes), "n_mu": int(w.mu.size), "greek_order": int(w.greek_order),
@@ -126,7 +126,7 @@ def reference_arm(args):
         return
     from scatrs_b200 import workloads as W
 
-    w = W.config2(seed=0, scale=args.scale, mu=None)
+    w = W.batched_spheres(seed=0, scale=args.scale, mu=None)
     vals = []
     base = None
     for s in range(args.warmup + args.steps):
@@ -273,7 +273,7 @@ def tf32_peak_tflops(torch):
     return 2.0 * n ** 3 / (best * 1e-3) / 1e12
 
 
-def projection_c3(torch, steps: int = 3, scale: float = 1.0):
+def projection_large_droplets(torch, steps: int = 3, scale: float = 1.0):
     """The Greek projection of the large-droplet configuration's shape (128 distributions x
     256 wavelengths = 32,768 tables at 4096 Gauss cosines, order 1024) on the tensor cores
     (3xTF32, FP32 accumulation) against the FP64 projection of the same tables: throughput of
@@ -418,7 +418,7 @@ def ours(args):
     from scatrs_b200 import workloads as W
 
     _native.require_device()
-    w = W.config2(seed=rank, scale=args.scale)
+    w = W.batched_spheres(seed=rank, scale=args.scale)
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream(dev)
     wl_d = torch.tensor(w.wavelengths, dtype=torch.float64, device=dev)
@@ -535,7 +535,7 @@ def ours(args):
                      "traffic": UNIT_DRAM_BYTES_PER_NODE * w.n_nodes_total / max(unit_n, 1),
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
                                        "launch on the 0.1-scale workload, scaled by nodes per "
-                                       "launch (profiles/unit_kernel_config2_scale0.1.md)",
+                                       "launch (profiles/unit_kernel_batched_scale0.1.md)",
                      "launches": unit_n, "avg_launch_ms": unit_ms / max(unit_n, 1),
                      "algorithmic_flop_per_step": flops},
         "kernels_ms_per_step": {k: v[0] for k, v in kt.items()},
@@ -544,7 +544,7 @@ def ours(args):
     }
     line["clocks"] = clk.summary()
     if world == 1 and not args.no_projection:
-        line["projection_tc"] = projection_c3(torch, scale=args.scale)
+        line["projection_tc"] = projection_large_droplets(torch, scale=args.scale)
     if world == 1 and not args.no_spheroids:
         line["spheroids"] = spheroid_leg(torch, line["roofline"]["peak"], scale=args.scale)
     if world == 1 and not args.no_cpu_baseline:

@@ -1,9 +1,9 @@
 """Seeded synthetic inputs of the benchmark configurations (no dataset is involved: every
 input is drawn from numpy's default_rng with a recorded seed).
 
-* ``config1``: spheres m = 1.43 + 1e-8 i; lognormal r_g = 0.08, sigma_g = 1.6; wavelengths
+* ``small_spheres``: spheres m = 1.43 + 1e-8 i; lognormal r_g = 0.08, sigma_g = 1.6; wavelengths
   0.35, 0.55, 1.0; 256 Gauss nodes in ln r over r_g sigma_g^(+-5); 180 Gauss cosines; L = 32.
-* ``config2``: 1024 wavelengths log-spaced over 0.3-2.5; 64 lognormals (median log-uniform
+* ``batched_spheres``: 1024 wavelengths log-spaced over 0.3-2.5; 64 lognormals (median log-uniform
   0.05-5, width uniform 1.2-2.2); m per (distribution, wavelength) with Re uniform 1.33-1.60 and
   Im log-uniform 1e-8-1e-1; 512 Gauss nodes over median width^(+-4); 360 Gauss cosines; L = 64.
   ``scale`` keeps the first fraction of the wavelengths and distributions for smaller cases of
@@ -73,15 +73,15 @@ def lognormals(median, width, spread) -> np.ndarray:
     return d
 
 
-def config1(mu: np.ndarray | None = None) -> Workload:
+def small_spheres(mu: np.ndarray | None = None) -> Workload:
     wl = np.array([0.35, 0.55, 1.0])
     d = lognormals(0.08, 1.6, 5)
     m = np.full((1, wl.size), 1.43 + 1e-8j)
     mu = gauss_legendre(180) if mu is None else mu
-    return Workload("config1", d, wl, m, mu, 256, 32)
+    return Workload("small_spheres", d, wl, m, mu, 256, 32)
 
 
-def config2(seed: int = 0, scale: float = 1.0, mu: np.ndarray | None = None) -> Workload:
+def batched_spheres(seed: int = 0, scale: float = 1.0, mu: np.ndarray | None = None) -> Workload:
     rng = np.random.default_rng(seed)
     n_dist, n_wl = 64, 1024
     wl = np.geomspace(0.3, 2.5, n_wl)
@@ -96,7 +96,7 @@ def config2(seed: int = 0, scale: float = 1.0, mu: np.ndarray | None = None) -> 
         med, wid, m = med[:kd], wid[:kd], m[:kd, :kw]
         wl = wl[:kw]
     mu = gauss_legendre(360) if mu is None else mu
-    return Workload(f"config2(seed={seed},scale={scale})", lognormals(med, wid, 4), wl, m, mu,
+    return Workload(f"batched_spheres(seed={seed},scale={scale})", lognormals(med, wid, 4), wl, m, mu,
                     512, 64)
 
 
@@ -114,7 +114,7 @@ def gammas(r_eff, v_eff) -> np.ndarray:
     return d
 
 
-def config3(seed: int = 0, scale: float = 1.0, n_q: int = 4096) -> Workload:
+def large_droplets(seed: int = 0, scale: float = 1.0, n_q: int = 4096) -> Workload:
     """Large droplets: 128 gamma distributions (effective radius uniform 5-20, effective
     variance uniform 0.05-0.2) x 256 wavelengths log-spaced over 0.4-2.2, m = 1.33 + k i with k
     log-uniform 1e-9-1e-3 per (distribution, wavelength), 256 nodes in ln r, the phase matrix at
@@ -131,11 +131,11 @@ def config3(seed: int = 0, scale: float = 1.0, n_q: int = 4096) -> Workload:
         kd = max(1, int(round(n_dist * scale)))
         kw = max(1, int(round(n_wl * scale)))
         a, b, m, wl = a[:kd], b[:kd], m[:kd, :kw], wl[:kw]
-    return Workload(f"config3(seed={seed},scale={scale})", gammas(a, b), wl, m,
+    return Workload(f"large_droplets(seed={seed},scale={scale})", gammas(a, b), wl, m,
                     gauss_legendre(n_q), 256, 1024)
 
 
-def config4(seed: int = 0, scale: float = 1.0, mu: np.ndarray | None = None) -> LayeredWorkload:
+def layered_spheres(seed: int = 0, scale: float = 1.0, mu: np.ndarray | None = None) -> LayeredWorkload:
     """Three-layer spheres (a core and two shells): core fraction uniform 0.3-0.9, inner shell
     boundary uniform 0.9-0.99; each layer's index Re uniform 1.3-2.0, Im log-uniform 1e-6-0.5
     (per distribution and layer, the same at every wavelength); lognormal median uniform
@@ -155,7 +155,7 @@ def config4(seed: int = 0, scale: float = 1.0, mu: np.ndarray | None = None) -> 
         kw = max(1, int(round(n_wl * scale)))
         med, wid, f, ml, wl = med[:kd], wid[:kd], f[:kd], ml[:kd, :, :kw], wl[:kw]
     mu = gauss_legendre(180) if mu is None else mu
-    return LayeredWorkload(f"config4(seed={seed},scale={scale})", lognormals(med, wid, 4), wl, f,
+    return LayeredWorkload(f"layered_spheres(seed={seed},scale={scale})", lognormals(med, wid, 4), wl, f,
                            ml, mu, 256, 32)
 
 

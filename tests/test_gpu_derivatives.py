@@ -63,7 +63,7 @@ def _compare(got, ref, tol=1e-9):
 
 @pytest.mark.parametrize("normalized", [True, False])
 def test_lognormal_matches_oracle(gpu, normalized):
-    w = W.config2(seed=5, scale=0.03)  # 2 distributions x 31 wavelengths
+    w = W.batched_spheres(seed=5, scale=0.03)  # 2 distributions x 31 wavelengths
     w.n_nodes = 96
     got = gpu.ensemble_fixed_d(w.dists, w.wavelengths, w.m, MU, w.n_nodes, 24,
                                normalized=normalized)
@@ -88,7 +88,7 @@ def test_other_kinds_match_oracle(gpu, kind, params, lo, hi):
 
 
 def test_values_match_the_plain_path(gpu):
-    w = W.config1()
+    w = W.small_spheres()
     got = gpu.ensemble_fixed_d(w.dists, w.wavelengths, w.m, w.mu, w.n_nodes, w.greek_order)
     plain = gpu.ensemble_fixed(w.dists, w.wavelengths, w.m, w.mu, w.n_nodes, w.greek_order)
     for a, b in zip(got[:3], plain):
@@ -100,7 +100,7 @@ def test_values_match_the_plain_path(gpu):
 def test_no_outputs_and_errors(gpu):
     from scatrs_b200.errors import InvalidInputError
 
-    w = W.config1()
+    w = W.small_spheres()
     got = gpu.ensemble_fixed_d(w.dists, w.wavelengths, w.m, None, w.n_nodes, -1)
     assert got[1] is None and got[2] is None and got[4] is None and got[5] is None
     ref = O.ensemble_fixed_d(_odists(w.dists), w.wavelengths, w.m, w.n_nodes)

@@ -52,16 +52,16 @@ def _compare(got, ref, tol=TOL):
         assert e.max() <= tol, (np.unravel_index(e.argmax(), e.shape), e.max())
 
 
-def test_config1_matches_oracle(gpu):
-    w = W.config1()
+def test_small_spheres_matches_oracle(gpu):
+    w = W.small_spheres()
     got = gpu.ensemble_fixed(w.dists, w.wavelengths, w.m, w.mu, w.n_nodes, w.greek_order)
     _compare(got, _oracle(w))
     v, ph, g = got
     assert np.all(g[0, :, 0] == 1.0)
 
 
-def test_config2_shape_small_matches_oracle(gpu):
-    w = W.config2(seed=3, scale=0.04)  # 3 distributions x 41 wavelengths, x up to ~1000
+def test_batched_shape_small_matches_oracle(gpu):
+    w = W.batched_spheres(seed=3, scale=0.04)  # 3 distributions x 41 wavelengths, x up to ~1000
     w.mu = W.gauss_legendre(64)
     got = gpu.ensemble_fixed(w.dists, w.wavelengths, w.m, w.mu, w.n_nodes, w.greek_order)
     _compare(got, _oracle(w))
@@ -69,7 +69,7 @@ def test_config2_shape_small_matches_oracle(gpu):
 
 @pytest.mark.parametrize("n_nodes", [1, 7, 33, 100])
 def test_ragged_chunks(gpu, n_nodes):
-    w = W.config1()
+    w = W.small_spheres()
     w.n_nodes = n_nodes
     w.mu = np.array([1.0, 0.3, -0.3, 0.0, -1.0, 0.77])  # unpaired and paired cosines
     got = gpu.ensemble_fixed(w.dists, w.wavelengths, w.m, w.mu, w.n_nodes, 12)
@@ -77,7 +77,7 @@ def test_ragged_chunks(gpu, n_nodes):
 
 
 def test_real_index_unnormalized_no_outputs(gpu):
-    w = W.config1()
+    w = W.small_spheres()
     w.m = np.full_like(w.m, 1.5 + 0j)
     got = gpu.ensemble_fixed(w.dists, w.wavelengths, w.m, None, w.n_nodes, -1, normalized=False)
     assert got[1] is None and got[2] is None
@@ -90,7 +90,7 @@ def test_real_index_unnormalized_no_outputs(gpu):
 
 def test_phase_normalization_and_greek_consistency(gpu):
     """Normalized: 1/2 sum w F11 = 1 on a Gauss grid that integrates exactly, and alpha1_1 = 3g."""
-    w = W.config1()
+    w = W.small_spheres()
     mu, wt = gpu.gauss_legendre(200)
     v, ph, g = gpu.ensemble_fixed(w.dists, w.wavelengths, w.m, mu, w.n_nodes, 32)
     norm = 0.5 * (ph[0] * wt[None]).sum(axis=1)
@@ -101,7 +101,7 @@ def test_phase_normalization_and_greek_consistency(gpu):
 def test_errors(gpu):
     from scatrs_b200.errors import InvalidInputError, OutsideValidatedDomainError
 
-    w = W.config1()
+    w = W.small_spheres()
     with pytest.raises(OutsideValidatedDomainError, match="at wavelength"):
         gpu.ensemble_fixed(w.dists, w.wavelengths, np.full_like(w.m, 1.5 + 11j), w.mu,
                            w.n_nodes, 8)
@@ -121,7 +121,7 @@ def test_errors(gpu):
 
 
 def test_deterministic_and_empty(gpu):
-    w = W.config2(seed=1, scale=0.02)
+    w = W.batched_spheres(seed=1, scale=0.02)
     w.mu = W.gauss_legendre(32)
     a = gpu.ensemble_fixed(w.dists, w.wavelengths, w.m, w.mu, w.n_nodes, 16)
     b = gpu.ensemble_fixed(w.dists, w.wavelengths, w.m, w.mu, w.n_nodes, 16)
@@ -140,7 +140,7 @@ def _oracle_layered(w, **kw):
 
 
 def test_layered_matches_oracle(gpu):
-    w = W.config4(seed=2, scale=0.03)  # 8 distributions x 4 wavelengths of three-layer spheres
+    w = W.layered_spheres(seed=2, scale=0.03)  # 8 distributions x 4 wavelengths of three-layer spheres
     got = gpu.ensemble_fixed_layered(w.dists, w.wavelengths, w.fractions, w.m_layers, w.mu,
                                      w.n_nodes, w.greek_order)
     _compare(got, _oracle_layered(w), tol=1e-11)
@@ -149,7 +149,7 @@ def test_layered_matches_oracle(gpu):
 def test_layered_with_equal_indices_is_the_sphere(gpu):
     """One index in every layer: the sphere's results bit for bit (tests/ensemble_layered.rs:
     62-116 of the reference)."""
-    w = W.config1()
+    w = W.small_spheres()
     ml = np.repeat(w.m[:, None, :], 3, axis=1)
     fr = np.array([[0.4, 0.8]])
     got = gpu.ensemble_fixed_layered(w.dists, w.wavelengths, fr, ml, w.mu, w.n_nodes, 16)

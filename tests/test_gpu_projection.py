@@ -47,7 +47,7 @@ def test_fp64_projection_matches_the_bands(gpu, n_q, L):
 
 
 def test_tensor_core_projection_matches_fp64(gpu):
-    w = W.config3(seed=1, scale=0.02, n_q=1024)  # 3 distributions x 5 wavelengths
+    w = W.large_droplets(seed=1, scale=0.02, n_q=1024)  # 3 distributions x 5 wavelengths
     w.wavelengths = w.wavelengths * 4.0            # smaller size parameters: N < 1024 - L / 2
     L = 300
     phase, _ = _ensemble_on_device(w, w.mu, -1)

@@ -41,13 +41,13 @@ def test_distribution_specs_and_ranges():
 
 
 def test_workloads_are_seeded_and_shaped():
-    a, b = W.config2(seed=5), W.config2(seed=5)
+    a, b = W.batched_spheres(seed=5), W.batched_spheres(seed=5)
     assert np.array_equal(a.m, b.m) and np.array_equal(a.dists, b.dists)
     assert a.n_nodes_total == 33554432 and a.mu.size == 360 and a.greek_order == 64
-    assert not np.array_equal(W.config2(seed=6).m, a.m)
+    assert not np.array_equal(W.batched_spheres(seed=6).m, a.m)
     assert 1.33 <= a.m.real.min() and a.m.real.max() <= 1.60
     assert 1e-8 <= a.m.imag.min() and a.m.imag.max() <= 1e-1
-    c = W.config1()
+    c = W.small_spheres()
     assert c.n_nodes_total == 768 and c.greek_order == 32
 
 
@@ -80,7 +80,7 @@ def test_narrow_distribution_is_the_single_sphere():
 
 
 def test_normalized_phase_integrates_to_one_and_alpha1_is_3g():
-    w = W.config1()
+    w = W.small_spheres()
     mu, wt = O.gauss_legendre(200)
     w.mu = mu
     out = _fixed(w)
@@ -100,7 +100,7 @@ def test_rayleigh_limit():
 
 
 def test_errors_are_the_reference_classes():
-    w = W.config1()
+    w = W.small_spheres()
     w.m = np.full_like(w.m, 1.5 + 11j)
     with pytest.raises(O.OracleError) as e:
         _fixed(w)

@@ -28,7 +28,7 @@ def _rank(rank, world, port, out):
     import bench
     from scatrs_b200 import workloads as W
 
-    w = W.config2(seed=rank, scale=0.01)
+    w = W.batched_spheres(seed=rank, scale=0.01)
     ms = bench.max_over_ranks(10.0 + rank, device="cpu")
     nodes = bench.total_nodes(world, w.n_nodes_total)
     dist.barrier()
