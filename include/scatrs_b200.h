@@ -301,6 +301,23 @@ int scatrs_ensemble_fixed_layered(const scatrs_distribution* dists, int64_t n_di
                                   double* phase, double* greek, char* err, size_t err_len);
 
 /*
+ * scatrs_ensemble_fixed_layered with the derivatives (forward mode, as scatrs_ensemble_fixed_d)
+ * along the distribution's parameters, then Re m_l and Im m_l of every layer l (each unit's
+ * own index at its wavelength), then the radius fractions f_1..f_{L-1} (n_layers >= 2; every
+ * distribution of one kind): P = n_theta + 3 L - 1 blocks, d_values [P][11][n], d_phase
+ * [P][6][n][n_mu], d_greek [P][6][n][L+1]. The layered recursion carries its derivatives
+ * (layered/kernel.rs's solve and its derivatives); one pass of the derivative pipeline per
+ * layer index and per fraction.
+ */
+int scatrs_ensemble_fixed_layered_d(const scatrs_distribution* dists, int64_t n_dist,
+                                    const double* wavelengths, int64_t n_wl,
+                                    const scatrs_layers* layers, const double* mu, int64_t n_mu,
+                                    const scatrs_fixed_options* options, double* values,
+                                    double* phase, double* greek, double* d_values,
+                                    double* d_phase, double* d_greek, char* err,
+                                    size_t err_len);
+
+/*
  * scatrs_ensemble_adaptive for layered spheres (Particle::LayeredSphere on the default adaptive
  * engine): the layers as scatrs_ensemble_fixed_layered takes them (per distribution), the
  * outputs and batch semantics of scatrs_ensemble_adaptive.

@@ -76,6 +76,9 @@ SYMBOLS = {
     "scatrs_ensemble_adaptive": (ctypes.c_int, [_VP, _I64, _I32, _PD, _I64, _PD, _PD, _I64,
                                                 ctypes.POINTER(AdaptiveOptions), _PD, _PD, _PD,
                                                 _PD, _PD, _PD, _VP, _VP, _CP, _SZ]),
+    "scatrs_ensemble_fixed_layered_d": (ctypes.c_int, [_VP, _I64, _PD, _I64, ctypes.POINTER(Layers),
+                                                       _PD, _I64, ctypes.POINTER(FixedOptions),
+                                                       _PD, _PD, _PD, _PD, _PD, _PD, _CP, _SZ]),
     "scatrs_ensemble_adaptive_layered": (ctypes.c_int, [_VP, _I64, _I32, _PD, _I64,
                                                         ctypes.POINTER(Layers), _PD, _I64,
                                                         ctypes.POINTER(AdaptiveOptions), _PD, _PD,
@@ -476,6 +479,40 @@ def ensemble_fixed_layered(dists: np.ndarray, wavelengths, fractions, m_layers, 
                                               _p(greek), err, 1024)
     _check(st, err)
     return values, phase, greek
+
+
+def ensemble_fixed_layered_d(dists: np.ndarray, wavelengths, fractions, m_layers, mu,
+                             n_nodes: int, greek_order: int = -1, normalized: bool = True,
+                             allow_unvalidated: bool = False):
+    """ensemble_fixed_layered with the derivatives along the distribution's parameters, then
+    Re m_l and Im m_l of every layer, then the fractions (P blocks); returns (values, phase,
+    greek, d_values, d_phase, d_greek), the derivative arrays shaped (P,) + the value array's
+    shape."""
+    require_device()
+    dists = np.ascontiguousarray(dists, dtype=DIST_DTYPE)
+    wl = np.ascontiguousarray(wavelengths, dtype=np.float64).reshape(-1)
+    ml = np.ascontiguousarray(m_layers, dtype=np.complex128)
+    nl = ml.shape[1]
+    fr = np.ascontiguousarray(fractions, dtype=np.float64).reshape(dists.size, nl - 1)
+    mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
+    n = dists.size * wl.size
+    kind = int(dists["kind"][0]) if dists.size else KINDS["lognormal"]
+    P = {3: 3, 4: 1}.get(kind, 2) + 3 * nl - 1
+    lay = Layers(nl, 0, _p(fr), _p(ml.view(np.float64).reshape(-1)))
+    opts = FixedOptions(int(n_nodes), int(greek_order), int(normalized), int(allow_unvalidated))
+    values, d_values = np.zeros((11, n)), np.zeros((P, 11, n))
+    phase = np.zeros((6, n, mu.size)) if mu.size else None
+    d_phase = np.zeros((P, 6, n, mu.size)) if mu.size else None
+    greek = np.zeros((6, n, greek_order + 1)) if greek_order >= 0 else None
+    d_greek = np.zeros((P, 6, n, greek_order + 1)) if greek_order >= 0 else None
+    err = ctypes.create_string_buffer(1024)
+    st = load().scatrs_ensemble_fixed_layered_d(dists.ctypes.data, dists.size, _p(wl), wl.size,
+                                                ctypes.byref(lay), _p(mu), mu.size,
+                                                ctypes.byref(opts), _p(values), _p(phase),
+                                                _p(greek), _p(d_values), _p(d_phase),
+                                                _p(d_greek), err, 1024)
+    _check(st, err)
+    return values, phase, greek, d_values, d_phase, d_greek
 
 
 def ensemble_fixed_device(dists: np.ndarray, wl_ptr: int, n_wl: int, m_ptr: int, mu, n_nodes: int,

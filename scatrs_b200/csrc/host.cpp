@@ -419,6 +419,7 @@ struct LayerInput {
 struct DerivOutput {
   bool on = false;
   int n_theta = 0;
+  int dir = 0;  // layered spheres: the direction of the pass (MieFixedArgs::deriv_dir)
   double* d_values = nullptr;
   double* d_phase = nullptr;
   double* d_greek = nullptr;
@@ -455,8 +456,6 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
   std::vector<double> radius(n_dist * n_nodes), weight(n_dist * n_nodes);
   std::vector<double> wtheta(dv.on ? n_dist * n_nodes * 3 : 0);
   if (dv.on) {
-    if (layers.n_layers > 1)
-      throw Failure{SCATRS_INVALID_INPUT, "derivatives are for homogeneous spheres"};
     for (int64_t d = 0; d < n_dist; ++d)
       if (parameter_count(dists[d].kind) != dv.n_theta)
         throw Failure{SCATRS_INVALID_INPUT,
@@ -711,7 +710,10 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
   WorkItem* items_d = c.items.as<WorkItem>(std::max<int64_t>(n_items_all, 1));
   double* X = c.X.as<double>((size_t)arena * 128);
   const int n_arr = L_layers > 1 ? 2 * L_layers - 1 : 1;
-  double2* uz = c.uz.as<double2>((size_t)(arena + 2 * kMaxSlabChunks) * 32 * n_arr);
+  // Layered derivatives keep each ratio array's derivative beside it.
+  const int arr_factor = dv.on && L_layers > 1 ? 2 : 1;
+  double2* uz =
+      c.uz.as<double2>((size_t)(arena + 2 * kMaxSlabChunks) * 32 * n_arr * arr_factor);
   double* ux = c.ux.as<double>((size_t)(arena + 2 * kMaxSlabChunks) * 32);
   double* chunk_sums = c.chunk_sums.as<double>((size_t)kMaxSlabChunks * 8 * n_blk);
   double* acc = c.acc.as<double>((size_t)acc_max);
@@ -743,6 +745,7 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
   ka.allow_unvalidated = opt->allow_unvalidated;
   if (dv.on) {
     ka.deriv = 1;
+    ka.deriv_dir = dv.dir;
     ka.n_theta = dv.n_theta;
     ka.wtheta = c.wtheta.as<double>(0);
   }
@@ -2732,6 +2735,92 @@ int scatrs_ensemble_fixed_layered(const scatrs_distribution* dists, int64_t n_di
     if (pl > 0 && phase) SB_CUDA(cudaMemcpyAsync(phase, p_d, pl * 8, cudaMemcpyDeviceToHost, s));
     if (gl > 0 && greek) SB_CUDA(cudaMemcpyAsync(greek, g_d, gl * 8, cudaMemcpyDeviceToHost, s));
     SB_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+int scatrs_ensemble_fixed_layered_d(const scatrs_distribution* dists, int64_t n_dist,
+                                    const double* wavelengths, int64_t n_wl,
+                                    const scatrs_layers* layers, const double* mu, int64_t n_mu,
+                                    const scatrs_fixed_options* options, double* values,
+                                    double* phase, double* greek, double* d_values,
+                                    double* d_phase, double* d_greek, char* err,
+                                    size_t err_len) {
+  return guarded(err, err_len, [&] {
+    if (n_dist < 0 || n_wl < 0) throw Failure{SCATRS_INVALID_INPUT, "negative sizes"};
+    if (!layers || layers->n_layers < 2 || !layers->fractions || !layers->m)
+      throw Failure{SCATRS_INVALID_INPUT,
+                    "layers must give n_layers >= 2, fractions and m (one layer: use "
+                    "scatrs_ensemble_fixed_d)"};
+    for (int64_t i = 0; i < n_wl; ++i)
+      if (!(std::isfinite(wavelengths[i]) && wavelengths[i] > 0.0))
+        throw Failure{SCATRS_INVALID_INPUT, "wavelengths must be finite and > 0"};
+    const int L = layers->n_layers;
+    if (L > 16) throw Failure{SCATRS_INVALID_INPUT, "the GPU path takes 1 to 16 layers"};
+    const int P_th = n_dist > 0 ? parameter_count(dists[0].kind) : 2;
+    const int P = P_th + 2 * L + (L - 1);
+    Context& c = context();
+    std::lock_guard<std::mutex> lk(c.mtx);
+    cudaStream_t s = 0;
+    const int64_t n_units = n_dist * n_wl;
+    check_options(options, n_units, n_mu, mu, P);
+    if (n_units == 0) return;
+    double* wl_d = c.wl.as<double>(n_wl);
+    SB_CUDA(cudaMemcpyAsync(wl_d, wavelengths, n_wl * 8, cudaMemcpyHostToDevice, s));
+    LayerInput li;
+    li.n_layers = L;
+    li.fractions = layers->fractions;
+    double* m_d = c.m.as<double>(2 * n_dist * L * n_wl);
+    SB_CUDA(cudaMemcpyAsync(m_d, layers->m, 2 * n_dist * L * n_wl * 8, cudaMemcpyHostToDevice, s));
+    li.m_dev = m_d;
+    int64_t vl, pl, gl;
+    scatrs_ensemble_fixed_sizes(n_units, n_mu, options->greek_order, &vl, &pl, &gl);
+    const int Pp = P_th + 2;  // blocks of one pass: the parameters, then the direction and i x it
+    double* v_d = c.values.as<double>(vl * (1 + Pp));
+    double* p_d = pl > 0 ? c.phase.as<double>(pl * (1 + Pp)) : nullptr;
+    double* g_d = gl > 0 ? c.greek.as<double>(gl * (1 + Pp)) : nullptr;
+    // One pass per direction group: layer l's index (its Re and Im blocks), then each fraction
+    // (its block; the pass's second block is discarded). Blocks out: the distribution's
+    // parameters, Re m_l and Im m_l per layer, then f_1..f_{L-1}.
+    for (int g = 0; g < 2 * L - 1; ++g) {
+      DerivOutput dv;
+      dv.on = true;
+      dv.n_theta = P_th;
+      dv.dir = g;
+      dv.d_values = v_d + vl;
+      dv.d_phase = p_d ? p_d + pl : nullptr;
+      dv.d_greek = g_d ? g_d + gl : nullptr;
+      FixedCall call;
+      call.wl_host.assign(wavelengths, wavelengths + n_wl);
+      run_fixed(c, dists, n_dist, wl_d, n_wl, m_d, mu, n_mu, options, v_d, p_d, g_d, s, &call, li,
+                dv);
+      check_device_errors(c, s, &call);
+      auto take = [&](int from, int to) {
+        if (d_values)
+          SB_CUDA(cudaMemcpyAsync(d_values + to * vl, dv.d_values + from * vl, vl * 8,
+                                  cudaMemcpyDeviceToHost, s));
+        if (pl > 0 && d_phase)
+          SB_CUDA(cudaMemcpyAsync(d_phase + to * pl, dv.d_phase + from * pl, pl * 8,
+                                  cudaMemcpyDeviceToHost, s));
+        if (gl > 0 && d_greek)
+          SB_CUDA(cudaMemcpyAsync(d_greek + to * gl, dv.d_greek + from * gl, gl * 8,
+                                  cudaMemcpyDeviceToHost, s));
+      };
+      if (g == 0) {
+        for (int p = 0; p < P_th; ++p) take(p, p);
+        SB_CUDA(cudaMemcpyAsync(values, v_d, vl * 8, cudaMemcpyDeviceToHost, s));
+        if (pl > 0 && phase)
+          SB_CUDA(cudaMemcpyAsync(phase, p_d, pl * 8, cudaMemcpyDeviceToHost, s));
+        if (gl > 0 && greek)
+          SB_CUDA(cudaMemcpyAsync(greek, g_d, gl * 8, cudaMemcpyDeviceToHost, s));
+      }
+      if (g < L) {
+        take(P_th, P_th + 2 * g);
+        take(P_th + 1, P_th + 2 * g + 1);
+      } else {
+        take(P_th, P_th + 2 * L + (g - L));
+      }
+      SB_CUDA(cudaStreamSynchronize(s));
+    }
   });
 }
 

@@ -5,6 +5,7 @@
 // 4 per lane: u.re, u.im, v.re, v.im with (u, v) = (a_n, b_n) for odd n and (b_n, a_n) for even
 // n (scatrs/src/ensemble/fast.rs:95-137), zero above the node's own N.
 #include "kernels.h"
+#include "layered_deriv.cuh"
 #include "mie_device.cuh"
 
 namespace sb {
@@ -265,6 +266,125 @@ __global__ void __launch_bounds__(128) mie_adaptive_kernel(MieFixedArgs a) {
 // Homogeneous spheres with derivatives.
 __global__ void __launch_bounds__(128) mie_deriv_kernel(MieFixedArgs a) { mie_chunk_deriv(a); }
 
+// Layered spheres with derivatives along one parameter direction (a.deriv_dir: 0..L-1 the
+// complex derivative along layer l's index, then L..2L-2 along the fraction f_{l-L}): the same
+// row layout and chunk sums as mie_chunk_deriv, the blocks "Re" and "Im" being the derivative
+// along the direction and along i times it (meaningful for the index directions only).
+// Scratch per chunk: 2 (2L - 1) arrays (the ratios and their derivatives) of nc + 2 rows.
+__global__ void __launch_bounds__(128) mie_layered_deriv_kernel(MieFixedArgs a) {
+  int wslot = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (wslot >= a.n_chunks) return;
+  int chunk = wslot;
+  int64_t unit = a.units[chunk / a.cpu];
+  int c = chunk % a.cpu;
+  int64_t d = unit / a.n_wl, i = unit % a.n_wl;
+  int j = c * 32 + lane;
+  int nc = a.chunk_n[chunk];
+  int64_t row0 = a.chunk_row[chunk];
+  double* X = a.X + (row0 + (int64_t)(lane >> 4) * nc) * 128 + (lane & 15) * 4;
+  const int L = a.n_layers, n_arr = 2 * L - 1;
+  Scratch s;
+  s.uz = a.uz + (row0 + 2 * (int64_t)chunk) * (2 * n_arr) * 32 + lane;
+  s.ux = a.ux + (row0 + 2 * (int64_t)chunk) * 32 + lane;
+  s.stride = 32;
+  const int P = a.n_theta;
+  const int B = 3 + P;
+  double q[6][8];
+#pragma unroll
+  for (int b = 0; b < 6; ++b)
+#pragma unroll
+    for (int k = 0; k < 8; ++k) q[b][k] = 0.0;
+  int64_t n = 0;
+  if (j < a.n_nodes) {
+    const double r = a.radius[d * a.n_nodes + j];
+    const double w = a.weight[d * a.n_nodes + j];
+    const double x = 2.0 * kPi * r / a.wl[i];
+    n = default_n_max(x);
+    double xs[kMaxLayers];
+    cplx ms[kMaxLayers];
+    lder::DR xd[kMaxLayers];
+    lder::DC md[kMaxLayers];
+    bool lossless = true;
+    const int dir = a.deriv_dir;
+    for (int l = 0; l < L; ++l) {
+      xs[l] = l < L - 1 ? a.fractions[d * (L - 1) + l] * x : x;
+      const double2 mv = a.m_layers[(d * L + l) * a.n_wl + i];
+      ms[l] = mk(mv.x, mv.y);
+      lossless = lossless && mv.y == 0.0;
+      xd[l] = lder::DR{xs[l], dir >= L && l == dir - L ? x : 0.0};
+      md[l] = lder::DC{ms[l], rl(dir == l ? 1.0 : 0.0)};
+    }
+    const int st = check_layered(xs, ms, L, n, a.allow_unvalidated != 0);
+    double asum = 0.0, abs_d[2] = {0.0, 0.0};
+    ValueSums vs;
+    DerivSums ds;
+    if (st == 0 && n <= nc) {
+      mie_prepare(x, ms[L - 1], n, s);  // u_k(x); array 0 is redone with its derivatives
+      lder::LayeredD lay;
+      lay.layers = L;
+      lay.x = xd;
+      lay.m = md;
+      lay.arr.arr.base = s.uz;
+      lay.arr.arr.astride = (int64_t)(nc + 2) * 32;
+      lay.arr.arr.stride = 32;
+      lay.arr.n_val = n_arr;
+      lay.prepare(n, lder::DR{x, 0.0});
+      auto emit = [&](int64_t k, cplx an, cplx bn, cplx dan, cplx dbn) {
+        const bool odd = (k & 1) != 0;
+        const cplx u = odd ? an : bn, v = odd ? bn : an;
+        const cplx du = odd ? dan : dbn, dv = odd ? dbn : dan;
+        *reinterpret_cast<double4*>(X + (k - 1) * 128) = make_double4(u.re, u.im, v.re, v.im);
+        *reinterpret_cast<double4*>(X + (k - 1) * 128 + 64) =
+            make_double4(du.re, du.im, dv.re, dv.im);
+        ds.add(k, an, bn, dan, dbn);
+      };
+      asum = lder::layered_finish_d(x, md[L - 1], n, s, vs, emit, lay, abs_d);
+      ds.close(n);
+      // A lossless particle absorbs nothing (layered/kernel.rs:455-464); its derivatives stand.
+      if (lossless) asum = 0.0;
+    }
+    if (st != 0 || n > nc) {
+      record_error(a.err, i, d, j, a.n_dist, a.n_nodes, st != 0 ? st : 1);
+      n = 0;
+    } else {
+      const Eff e = efficiencies_from(x, asum, vs);
+      const double area = kPi * r * r;
+      const double qv[8] = {1.0,           area * e.q_ext, area * e.q_sca, area * e.q_sca * e.g,
+                            area * e.q_abs, area * e.q_back, r * r,         r * r * r};
+      for (int k = 0; k < 8; ++k) q[0][k] = w * qv[k];
+      for (int p = 0; p < P; ++p) {
+        const double wt = a.wtheta[(d * a.n_nodes + j) * 3 + p];
+        for (int k = 0; k < 8; ++k) q[1 + p][k] = wt * qv[k];
+      }
+      for (int p = 0; p < 2; ++p) {
+        const Eff de = efficiency_derivs(x, vs, e, ds, p, abs_d[p]);
+        const double qd[8] = {0.0,
+                              area * de.q_ext,
+                              area * de.q_sca,
+                              area * (de.q_sca * e.g + e.q_sca * de.g),
+                              area * de.q_abs,
+                              area * de.q_back,
+                              0.0,
+                              0.0};
+        for (int k = 0; k < 8; ++k) q[1 + P + p][k] = w * qd[k];
+      }
+    }
+  }
+  for (int64_t k = n + 1; k <= nc; ++k) {
+    *reinterpret_cast<double4*>(X + (k - 1) * 128) = make_double4(0.0, 0.0, 0.0, 0.0);
+    *reinterpret_cast<double4*>(X + (k - 1) * 128 + 64) = make_double4(0.0, 0.0, 0.0, 0.0);
+  }
+  for (int b = 0; b < 6; ++b) {
+    if (b >= B) break;
+    for (int k = 0; k < 8; ++k) {
+      double v = q[b][k];
+      for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+      if (lane == 0) a.chunk_sums[((int64_t)chunk * B + b) * 8 + k] = v;
+    }
+  }
+}
+
 // Layered spheres (their per-layer state lives in local memory).
 __global__ void __launch_bounds__(128) mie_layered_kernel(MieFixedArgs a) {
   mie_chunk<true, false>(a);
@@ -399,7 +519,9 @@ void launch_plan_chunks(const PlanArgs& a, cudaStream_t s) {
 void launch_mie_fixed(const MieFixedArgs& a, cudaStream_t s) {
   int threads = 128;
   int blocks = (a.n_chunks * 32 + threads - 1) / threads;
-  if (a.deriv)
+  if (a.deriv && a.n_layers > 1)
+    mie_layered_deriv_kernel<<<blocks, threads, 0, s>>>(a);
+  else if (a.deriv)
     mie_deriv_kernel<<<blocks, threads, 0, s>>>(a);
   else if (a.n_layers > 1 && a.wdiff)
     mie_layered_adaptive_kernel<<<blocks, threads, 0, s>>>(a);
