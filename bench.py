@@ -46,6 +46,8 @@ def parse():
     p.add_argument("--scale", type=float, default=1.0, help="fraction of the batch (tests)")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-layered", action="store_true",
+                   help="skip the layered-sphere derivatives leg")
     p.add_argument("--no-spheroids", action="store_true",
                    help="skip the spheroid ensemble leg")
     p.add_argument("--no-projection", action="store_true",
@@ -404,6 +406,54 @@ def spheroid_leg(torch, fp64_peak: float, scale: float = 1.0, cpu_seconds: float
     return out
 
 
+def layered_adjoint_leg(torch, scale: float = 1.0, cpu_seconds: float = 8.0):
+    """The layered-sphere ensemble with its derivatives (the layered adjoint workload: three
+    layers, 256 distributions x 128 wavelengths x 256 nodes, Greek order 32) on its first
+    quarter of distributions and wavelengths (the full size at scale 4): values and the 10
+    forward-mode derivative blocks (median, width, each layer's n and k, both fractions), timed
+    after one identical warm-up call. The CPU baseline is the oracle's layered forward ensemble
+    (values only) on the same workload's units, all host threads."""
+    from scatrs_b200 import _native
+    from scatrs_b200 import workloads as W
+
+    w = W.layered_spheres(seed=0, scale=min(1.0, 0.25 * scale))
+    call = lambda: _native.ensemble_fixed_layered_d(w.dists, w.wavelengths, w.fractions,
+                                                    w.m_layers, None, w.n_nodes, w.greek_order)
+    call()
+    torch.cuda.synchronize()
+    _native.set_profiling(True)
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    out = call()
+    e.record()
+    torch.cuda.synchronize()
+    kt = _native.kernel_times()
+    _native.set_profiling(False)
+    ms = s.elapsed_time(e)
+    nodes = w.n_units * w.n_nodes
+    res = {"workload": f"{nodes} layered nodes ({w.name}): 3 layers, Greek order 32, values and "
+                       f"{out[3].shape[0]} derivative blocks",
+           "value": nodes / (ms * 1e-3), "unit": "nodes/s (values and every derivative block)",
+           "ms": ms, "passes": 2 * w.m_layers.shape[1] - 1,
+           "kernels_ms": {k: v[0] for k, v in kt.items() if v[1] > 0}}
+    from oracle import oracle as O
+    od = w.dists.view(O.DIST_DTYPE)
+    done, t0 = 0, time.time()
+    k = 0
+    while time.time() - t0 < cpu_seconds and k < w.dists.size:
+        O.ensemble_fixed_layered(od[k:k + 1], w.wavelengths, w.fractions[k:k + 1],
+                                 w.m_layers[k:k + 1], w.n_nodes, greek_order=w.greek_order)
+        done += w.wavelengths.size * w.n_nodes
+        k += 1
+    dt = time.time() - t0
+    res["cpu_baseline"] = {"value": done / dt, "unit": "nodes/s (values only)",
+                           "cores": os.cpu_count(), "kind": "port",
+                           "sample": f"{k} distributions x {w.wavelengths.size} wavelengths x "
+                                     f"{w.n_nodes} nodes in {dt:.1f} s: the oracle's layered "
+                                     "forward ensemble, OpenMP over units"}
+    return res
+
+
 def ours(args):
     import torch
 
@@ -545,6 +595,8 @@ def ours(args):
     line["clocks"] = clk.summary()
     if world == 1 and not args.no_projection:
         line["projection_tc"] = projection_large_droplets(torch, scale=args.scale)
+    if world == 1 and not args.no_layered:
+        line["layered_adjoint"] = layered_adjoint_leg(torch, scale=args.scale)
     if world == 1 and not args.no_spheroids:
         line["spheroids"] = spheroid_leg(torch, line["roofline"]["peak"], scale=args.scale)
     if world == 1 and not args.no_cpu_baseline:

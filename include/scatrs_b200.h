@@ -39,17 +39,24 @@ enum scatrs_distribution_kind {
   SCATRS_LOGNORMAL = 1,
   SCATRS_GAMMA = 2,
   SCATRS_MODIFIED_GAMMA = 3,
-  SCATRS_POWER_LAW = 4
+  SCATRS_POWER_LAW = 4,
+  /* n(r) linear between table_len points (radii increasing and > 0, densities >= 0 and not all
+   * 0), 0 outside them: table = [radii..., densities...] (distribution.rs:55-62, 406-417);
+   * no parameters. */
+  SCATRS_TABULATED = 6
 };
 
 /* One size distribution on a fixed grid: n_nodes Gauss-Legendre nodes in t = ln r over
- * [ln r_lo, ln r_hi] (the radius of a sphere). */
+ * [ln r_lo, ln r_hi] (the radius of a sphere). table / table_len: SCATRS_TABULATED only (NULL,
+ * 0 otherwise). */
 typedef struct scatrs_distribution {
   int32_t kind;
   int32_t reserved;
   double param[3];
   double r_lo;
   double r_hi;
+  const double* table;
+  int64_t table_len;
 } scatrs_distribution;
 
 /* Options of the fixed-grid ensemble. The reference's EnsembleOptions

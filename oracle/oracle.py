@@ -146,7 +146,9 @@ def default_n_max(x: float) -> int:
 
 
 DIST_DTYPE = np.dtype([("kind", np.int32), ("pad", np.int32), ("p", np.float64, 3),
-                       ("r_lo", np.float64), ("r_hi", np.float64)])
+                       ("r_lo", np.float64), ("r_hi", np.float64), ("table", np.uint64),
+                       ("table_len", np.int64)])
+TABULATED = 6
 
 
 def ensemble_fixed(dists: np.ndarray, wavelengths, m, n_nodes: int, mu=None,
@@ -243,7 +245,7 @@ def ensemble_fixed_d(dists: np.ndarray, wavelengths, m, n_nodes: int, mu=None,
                                              (dists.size, wl.size)))
     mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
     kinds = set(int(k) for k in dists["kind"])
-    P = 2 + ({3: 3, 4: 1}.get(kinds.pop(), 2) if len(kinds) == 1 else 2)
+    P = 2 + ({3: 3, 4: 1, TABULATED: 0}.get(kinds.pop(), 2) if len(kinds) == 1 else 2)
     n_units = dists.size * wl.size
     L = -1 if greek_order is None else int(greek_order)
     values = np.zeros((11, n_units))
@@ -403,6 +405,39 @@ def dist(kind: int, *params) -> np.ndarray:
     d = np.zeros(1, dtype=DIST_DTYPE)
     d["kind"] = kind
     d["p"][0, :len(params)] = params
+    return d
+
+
+class TableRecords(np.ndarray):
+    """DIST_DTYPE records that own the tables their TABULATED entries point at."""
+
+    def __array_finalize__(self, obj):
+        self.tables = getattr(obj, "tables", [])
+
+
+def table_dist(radii, densities) -> np.ndarray:
+    """One TABULATED record: n(r) linear through (radii, densities), 0 outside them
+    (scatrs/src/ensemble/distribution.rs:55-62); the record owns the table. Concatenate such
+    records with ``join`` to keep the tables alive."""
+    r = np.asarray(radii, dtype=np.float64).reshape(-1)
+    n = np.asarray(densities, dtype=np.float64).reshape(-1)
+    if r.size != n.size:
+        raise ValueError("as many densities as radii")
+    tab = np.ascontiguousarray(np.concatenate([r, n]))
+    d = np.zeros(1, dtype=DIST_DTYPE).view(TableRecords)
+    d.tables = [tab]
+    d["kind"] = TABULATED
+    d["table"] = tab.ctypes.data
+    d["table_len"] = r.size
+    if r.size:
+        d["r_lo"], d["r_hi"] = r[0], r[-1]
+    return d
+
+
+def join(*records) -> np.ndarray:
+    """Concatenate distribution records, keeping every table alive."""
+    d = np.concatenate([np.asarray(r) for r in records]).view(TableRecords)
+    d.tables = [t for r in records for t in getattr(r, "tables", [])]
     return d
 
 

@@ -143,14 +143,25 @@ struct Moments {
 
 // moments.rs:62-167 (no derivative parameters).
 Moments moments(const Density& d, std::pair<double, double> range, double rtol,
-                double truncation) {
+                double truncation, const std::vector<double>& breaks = {}) {
   const double step = max_step(d, STEP);
   const double t_lo = std::log(range.first), t_hi = std::log(range.second);
   std::vector<std::pair<double, double>> panels;
   {
-    const size_t n = (size_t)std::max(1.0, std::ceil((t_hi - t_lo) / step));
-    const double h = (t_hi - t_lo) / (double)n;
-    for (size_t i = 0; i < n; ++i) panels.push_back({t_lo + i * h, t_lo + (i + 1) * h});
+    // moments.rs:71-86: the breaks inside the range are panel edges, each interval in equal
+    // panels of at most the step.
+    std::vector<double> edges{t_lo};
+    for (double r : breaks) {
+      const double t = std::log(r);
+      if (t > t_lo && t < t_hi) edges.push_back(t);
+    }
+    edges.push_back(t_hi);
+    for (size_t w = 0; w + 1 < edges.size(); ++w) {
+      const double a = edges[w], b = edges[w + 1];
+      const size_t n = (size_t)std::max(1.0, std::ceil((b - a) / step));
+      const double h = (b - a) / (double)n;
+      for (size_t i = 0; i < n; ++i) panels.push_back({a + i * h, a + (i + 1) * h});
+    }
   }
   auto finish = [&](const std::vector<std::array<double, 6>>& sums) {
     double s[3] = {0, 0, 0}, e[3] = {0, 0, 0};
@@ -248,6 +259,20 @@ Part make_part(const FixedDist& d, double rtol) {
     p.support = POINT;
     p.s_a = d.p[0];
     p.cut = {d.p[0], d.p[0]};
+    return p;
+  }
+  if (d.kind == TABULATED) {
+    // distribution.rs:285-287 and engine.rs:181-185: finite support between the first and
+    // last radii, the table's radii as edges of the moment panels.
+    std::string msg;
+    if (!table_valid(d.table, d.table_len, &msg)) throw Failure{INVALID_INPUT, msg};
+    p.den = prepare(d);
+    p.support = FINITE;
+    p.s_a = d.table[0];
+    p.s_b = d.table[d.table_len - 1];
+    p.mom = moments(p.den, {p.s_a, p.s_b}, rtol, 0.0,
+                    std::vector<double>(d.table, d.table + d.table_len));
+    p.cut = {p.s_a, p.s_b};
     return p;
   }
   p.den = prepare(d.kind, d.p[0], d.p[1], d.p[2]);
@@ -489,11 +514,15 @@ struct Pass1 {
 Pass1 pass1(const std::vector<const Part*>& group, double lambda, const Optics& m,
             const Options& o) {
   std::vector<double> breaks;
-  for (auto* p : group)
+  for (auto* p : group) {
     if (p->support == FINITE) {
       breaks.push_back(p->s_a);
       breaks.push_back(p->s_b);
     }
+    // engine.rs:740-752: a table's radii are panel edges too.
+    if (p->dist.kind == TABULATED)
+      breaks.insert(breaks.end(), p->dist.table, p->dist.table + p->dist.table_len);
+  }
   std::sort(breaks.begin(), breaks.end());
   breaks.erase(std::unique(breaks.begin(), breaks.end()), breaks.end());
   double lo = INF, hi = 0.0;

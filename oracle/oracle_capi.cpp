@@ -226,7 +226,9 @@ static void element_derivs(cplx s1, cplx s2, cplx d1, cplx d2, double out[4]) {
   out[3] = p.im;
 }
 
-static int theta_count(int kind) { return kind == MODIFIED_GAMMA ? 3 : kind == POWER_LAW ? 1 : 2; }
+static int theta_count(int kind) {
+  return kind == MODIFIED_GAMMA ? 3 : kind == POWER_LAW ? 1 : kind == TABULATED ? 0 : 2;
+}
 
 static int ensemble_impl(const FixedDist* dists, int64_t n_dist, const double* wl, int64_t n_wl,
                          const double* m, int n_layers, const double* fractions,
@@ -257,7 +259,14 @@ static int ensemble_impl(const FixedDist* dists, int64_t n_dist, const double* w
   std::vector<double> radius(n_dist * n_nodes), weight(n_dist * n_nodes);
   std::vector<double> wth(n_dist * n_nodes * 3, 0.0);
   for (int64_t d = 0; d < n_dist; ++d) {
-    Density den = prepare(dists[d].kind, dists[d].p[0], dists[d].p[1], dists[d].p[2]);
+    if (dists[d].kind == TABULATED) {
+      std::string msg;
+      if (!table_valid(dists[d].table, dists[d].table_len, &msg)) {
+        if (err && err_len > 0) snprintf(err, err_len, "%s", msg.c_str());
+        return INVALID_INPUT;
+      }
+    }
+    Density den = prepare(dists[d]);
     double a = std::log(dists[d].r_lo), b = std::log(dists[d].r_hi);
     double c = 0.5 * (a + b), h = 0.5 * (b - a);
     for (int64_t j = 0; j < n_nodes; ++j) {

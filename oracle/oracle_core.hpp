@@ -900,14 +900,53 @@ inline Greek project(const double* nodes, const double* weights, int64_t n_q, in
 // ---------------------------------------------------------------------------------------
 // Size distributions (scatrs/src/ensemble/distribution.rs:15-468).
 // ---------------------------------------------------------------------------------------
-enum DistKind { LOGNORMAL = 1, GAMMA = 2, MODIFIED_GAMMA = 3, POWER_LAW = 4 };
+enum DistKind { LOGNORMAL = 1, GAMMA = 2, MODIFIED_GAMMA = 3, POWER_LAW = 4, TABULATED = 6 };
 
 struct Density {
   int kind;
   double p0, p1, p2;
   double reference;
   double log_width;
+  // TABULATED: table_len radii (increasing) followed by their table_len densities.
+  const double* table = nullptr;
+  int64_t table_len = 0;
 };
+
+// interpolate (distribution.rs:458-468): linear through the points, 0 outside them.
+inline double table_interpolate(const double* r_tab, const double* n_tab, int64_t n, double r) {
+  if (r < r_tab[0] || r > r_tab[n - 1]) return 0.0;
+  int64_t i = std::upper_bound(r_tab, r_tab + n, r) - r_tab;  // first radius above r
+  i = std::min<int64_t>(std::max<int64_t>(i, 1), n - 1);
+  const double t = (r - r_tab[i - 1]) / (r_tab[i] - r_tab[i - 1]);
+  return n_tab[i - 1] + t * (n_tab[i] - n_tab[i - 1]);
+}
+
+// SizeDistribution::validate for Tabulated (distribution.rs:149-172).
+inline bool table_valid(const double* table, int64_t n, std::string* msg) {
+  if (table == nullptr || n < 2) {
+    *msg = "a tabulated distribution needs at least 2 points and as many densities as radii";
+    return false;
+  }
+  const double* dens = table + n;
+  bool any = false;
+  for (int64_t i = 0; i < n; ++i) {
+    if (!(std::isfinite(table[i]) && table[i] > 0.0)) {
+      *msg = "radius must be finite and > 0";
+      return false;
+    }
+    if (i > 0 && !(table[i - 1] < table[i])) {
+      *msg = "tabulated radii must increase";
+      return false;
+    }
+    if (!(std::isfinite(dens[i]) && dens[i] >= 0.0)) {
+      *msg = "tabulated densities must be finite and >= 0";
+      return false;
+    }
+    any = any || dens[i] != 0.0;
+  }
+  if (!any) *msg = "tabulated densities must not all be 0";
+  return any;
+}
 
 // SizeDistribution::prepare (distribution.rs:296-355).
 inline Density prepare(int kind, double p0, double p1, double p2) {
@@ -934,6 +973,14 @@ inline Density prepare(int kind, double p0, double p1, double p2) {
       d.reference = p0 >= 0.0 ? p1 : p2;
       break;
   }
+  return d;
+}
+
+// A tabulated density: reference radius 1, no width limit on the steps.
+inline Density prepare_table(const double* table, int64_t n) {
+  Density d = prepare(TABULATED, 0.0, 0.0, 0.0);
+  d.table = table;
+  d.table_len = n;
   return d;
 }
 
@@ -970,6 +1017,10 @@ inline double density_eval(const Density& d, double r, double* grad) {
       dln[1] = -(rg - r0g);
       dln[2] = -b * (rg * std::log(r) - r0g * std::log(r0));
       break;
+    }
+    case TABULATED: {
+      if (grad) grad[0] = grad[1] = grad[2] = 0.0;
+      return table_interpolate(d.table, d.table + d.table_len, d.table_len, r);
     }
     case POWER_LAW: {
       double ex = d.p0, lo = d.p1, hi = d.p2;
@@ -1042,7 +1093,14 @@ struct FixedDist {
   int32_t pad;
   double p[3];
   double r_lo, r_hi;
+  const double* table;  // TABULATED: radii then densities, table_len of each
+  int64_t table_len;
 };
+
+inline Density prepare(const FixedDist& d) {
+  return d.kind == TABULATED ? prepare_table(d.table, d.table_len)
+                             : prepare(d.kind, d.p[0], d.p[1], d.p[2]);
+}
 
 constexpr int NODES_PER_CHUNK = 32;
 

@@ -11,7 +11,7 @@ import os
 
 import numpy as np
 
-from .errors import DeviceError, raise_for
+from .errors import DeviceError, InvalidInputError, raise_for
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libscatrs_b200.so")
@@ -26,7 +26,40 @@ _CP = ctypes.c_char_p
 _SZ = ctypes.c_size_t
 
 DIST_DTYPE = np.dtype([("kind", np.int32), ("reserved", np.int32), ("param", np.float64, 3),
-                       ("r_lo", np.float64), ("r_hi", np.float64)])
+                       ("r_lo", np.float64), ("r_hi", np.float64), ("table", np.uint64),
+                       ("table_len", np.int64)])
+TABULATED = 6  # table = address of [radii..., densities...], table_len points
+
+
+class DistArray(np.ndarray):
+    """A DIST_DTYPE array that owns the tables its tabulated records point at."""
+
+    def __array_finalize__(self, obj):
+        self.tables = getattr(obj, "tables", [])
+
+
+def dist_records(n: int) -> DistArray:
+    """n zeroed distribution records."""
+    d = np.zeros(n, dtype=DIST_DTYPE).view(DistArray)
+    d.tables = []
+    return d
+
+
+def set_table(d: DistArray, k: int, radii, densities) -> None:
+    """Make record k the tabulated n(r) through (radii, densities), linear between the points
+    and 0 outside them (scatrs/src/ensemble/distribution.rs:55-62); d keeps the table alive."""
+    r = np.asarray(radii, dtype=np.float64).reshape(-1)
+    n = np.asarray(densities, dtype=np.float64).reshape(-1)
+    if r.size < 2 or r.size != n.size:
+        raise InvalidInputError(
+            "a tabulated distribution needs at least 2 points and as many densities as radii, "
+            f"got {r.size} radii and {n.size} densities")
+    tab = np.ascontiguousarray(np.concatenate([r, n]))
+    d.tables.append(tab)
+    d[k]["kind"] = TABULATED
+    d[k]["table"] = tab.ctypes.data
+    d[k]["table_len"] = r.size
+    d[k]["r_lo"], d[k]["r_hi"] = r[0], r[-1]
 KINDS = {"lognormal": 1, "gamma": 2, "modified_gamma": 3, "power_law": 4}
 MONODISPERSE = 5  # adaptive calls only: param[0] the radius
 
@@ -275,7 +308,7 @@ def ensemble_fixed_d(dists: np.ndarray, wavelengths, m, mu, n_nodes: int, greek_
     mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
     n = dists.size * wl.size
     kind = int(dists["kind"][0]) if dists.size else KINDS["lognormal"]
-    P = {3: 3, 4: 1}.get(kind, 2) + 2
+    P = {3: 3, 4: 1, TABULATED: 0}.get(kind, 2) + 2
     opts = FixedOptions(int(n_nodes), int(greek_order), int(normalized), int(allow_unvalidated))
     values, d_values = np.zeros((11, n)), np.zeros((P, 11, n))
     phase = np.zeros((6, n, mu.size)) if mu.size else None
@@ -497,7 +530,7 @@ def ensemble_fixed_layered_d(dists: np.ndarray, wavelengths, fractions, m_layers
     mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
     n = dists.size * wl.size
     kind = int(dists["kind"][0]) if dists.size else KINDS["lognormal"]
-    P = {3: 3, 4: 1}.get(kind, 2) + 3 * nl - 1
+    P = {3: 3, 4: 1, TABULATED: 0}.get(kind, 2) + 3 * nl - 1
     lay = Layers(nl, 0, _p(fr), _p(ml.view(np.float64).reshape(-1)))
     opts = FixedOptions(int(n_nodes), int(greek_order), int(normalized), int(allow_unvalidated))
     values, d_values = np.zeros((11, n)), np.zeros((P, 11, n))

@@ -80,11 +80,17 @@ def ensemble_parameters(items, mixture: bool) -> list[str]:
 
 
 def _dist_array(specs, spread: float, ranges=None) -> np.ndarray:
-    d = np.zeros(len(specs), dtype=_native.DIST_DTYPE)
+    d = _native.dist_records(len(specs))
     for k, spec in enumerate(specs):
         if not isinstance(spec, tuple):
             raise TypeError("a distribution spec must be a tuple")
         kind = spec[0]
+        if kind == "tabulated":
+            # The grid spans the table unless a range is given.
+            _native.set_table(d, k, spec[1], spec[2])
+            if ranges is not None:
+                d[k]["r_lo"], d[k]["r_hi"] = ranges[k]
+            continue
         if kind not in _native.KINDS:
             raise TypeError(f"unknown distribution kind {kind!r}")
         p = [float(v) for v in spec[1:]]
@@ -103,18 +109,20 @@ def _dist_array(specs, spread: float, ranges=None) -> np.ndarray:
 
 
 def _adaptive_dists(specs) -> np.ndarray:
-    d = np.zeros(len(specs), dtype=_native.DIST_DTYPE)
+    d = _native.dist_records(len(specs))
     for k, spec in enumerate(specs):
         if not isinstance(spec, tuple):
             raise TypeError("a distribution spec must be a tuple")
         kind = spec[0]
+        if kind == "tabulated":
+            # ("tabulated", radii, densities) (scatrs-py/src/ensemble.rs:58-61).
+            _native.set_table(d, k, spec[1], spec[2])
+            continue
         p = [float(v) for v in spec[1:]]
         if kind == "monodisperse":
             d[k]["kind"] = _native.MONODISPERSE
         elif kind in _native.KINDS:
             d[k]["kind"] = _native.KINDS[kind]
-        elif kind == "tabulated":
-            raise InvalidInputError("tabulated distributions are not on the GPU path")
         elif kind == "multimodal":
             raise InvalidInputError("a multimodal distribution is not one distribution here")
         else:

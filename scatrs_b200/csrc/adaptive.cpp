@@ -91,14 +91,26 @@ std::pair<double, double> cutoffs(const Part& p, double center, double eps,
 
 // moments.rs:62-167 without derivative parameters: GK15 panels of at most max_step, split
 // where their |Kronrod - Gauss| is above their share, until Z, <r^2 u>, <r^3 u> meet rtol.
-Moments moments(const Part& p, double lo, double hi, double rtol, double truncation) {
+Moments moments(const Part& p, double lo, double hi, double rtol, double truncation,
+                const std::vector<double>& breaks = {}) {
   const double step = max_step(p, kStep);
   const double t_lo = std::log(lo), t_hi = std::log(hi);
   std::vector<std::pair<double, double>> panels;
   {
-    const size_t n = (size_t)std::max(1.0, std::ceil((t_hi - t_lo) / step));
-    const double h = (t_hi - t_lo) / (double)n;
-    for (size_t i = 0; i < n; ++i) panels.push_back({t_lo + i * h, t_lo + (i + 1) * h});
+    // The breaks inside the range are panel edges; each interval in equal panels of at most
+    // the step (moments.rs:72-86).
+    std::vector<double> edges{t_lo};
+    for (double r : breaks) {
+      const double t = std::log(r);
+      if (t > t_lo && t < t_hi) edges.push_back(t);
+    }
+    edges.push_back(t_hi);
+    for (size_t w = 0; w + 1 < edges.size(); ++w) {
+      const double a = edges[w], b = edges[w + 1];
+      const size_t n = (size_t)std::max(1.0, std::ceil((b - a) / step));
+      const double h = (b - a) / (double)n;
+      for (size_t i = 0; i < n; ++i) panels.push_back({a + i * h, a + (i + 1) * h});
+    }
   }
   std::vector<double> sums;  // per panel: K0, K2, K3, |K-G| x 3
   auto result = [&]() {
@@ -283,7 +295,19 @@ struct State {
 
 double Part::u(double r) const {
   if (support == POINT) return 0.0;
+  if (kind == kTabulated) return table_density(table.data(), (int64_t)table.size() / 2, r);
   return density(kind, p, r);
+}
+
+std::vector<double> Part::breaks() const {
+  std::vector<double> out;
+  if (support == FINITE) {
+    out.push_back(lo);
+    out.push_back(hi);
+  }
+  if (kind == kTabulated)
+    out.insert(out.end(), table.begin(), table.begin() + (int64_t)table.size() / 2);
+  return out;
 }
 
 void gk15(double a, double b, Node out[15]) {
@@ -318,10 +342,24 @@ void gk15(double a, double b, Node out[15]) {
   out[7] = {c, h * kw[7], h * gw[3]};
 }
 
-Part make_part(int kind, const double* p, double rtol) {
+Part make_part(int kind, const double* p, double rtol, const double* table, int64_t table_len) {
   Part part;
   part.kind = kind;
   for (int k = 0; k < 3; ++k) part.p[k] = p[k];
+  if (kind == kTabulated) {
+    // Finite support between the table's first and last radii (distribution.rs:285-287),
+    // reference radius 1, no width limit; the moments with the table's radii as edges.
+    std::string msg;
+    if (!validate_table(table, table_len, &msg)) throw Error{1, msg};
+    part.table.assign(table, table + 2 * table_len);
+    part.reference = 1.0;
+    part.log_width = kInf;  // the steps are not limited by a width
+    part.support = FINITE;
+    part.lo = table[0];
+    part.hi = table[table_len - 1];
+    part.mom = moments(part, part.lo, part.hi, rtol, 0.0, part.breaks());
+    return part;
+  }
   if (kind == kMonodisperse) {
     if (!(std::isfinite(p[0]) && p[0] > 0.0)) throw Error{1, "radius must be finite and > 0"};
     part.support = POINT;
@@ -367,10 +405,8 @@ void pass1(std::vector<Job>& jobs, const std::vector<Part>& parts, const double*
     double lo = kInf, hi = 0.0;
     for (int pi : job.parts) {
       const Part& p = parts[pi];
-      if (p.support == FINITE) {
-        breaks.push_back(p.lo);
-        breaks.push_back(p.hi);
-      }
+      const std::vector<double> pb = p.breaks();
+      breaks.insert(breaks.end(), pb.begin(), pb.end());
       lo = std::min(lo, p.lo);
       hi = std::max(hi, p.hi);
       st.exts.push_back(std::min(kStep, p.log_width));

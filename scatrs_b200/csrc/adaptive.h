@@ -38,12 +38,17 @@ struct Part {
   Support support = UNBOUNDED;
   double lo = 0.0, hi = 0.0;  // the Mie range before extensions (a point: r, r)
   Moments mom;
+  std::vector<double> table;  // a tabulated distribution's [radii..., densities...]
   double u(double r) const;  // the unnormalized density
+  // The radii that are panel edges (engine.rs:181-184, 738-751): a finite support's ends and a
+  // table's points.
+  std::vector<double> breaks() const;
 };
 
 // Parses and prepares a part: validation, support, cut-offs (range.rs) and moments
-// (moments.rs). Throws Error.
-Part make_part(int kind, const double* p, double rtol);
+// (moments.rs). A tabulated distribution (kind 6) brings its table. Throws Error.
+Part make_part(int kind, const double* p, double rtol, const double* table = nullptr,
+               int64_t table_len = 0);
 
 struct Options {
   double rtol = 1e-6;

@@ -367,6 +367,12 @@ BandTables& ensure_bands(Context& c, int L, int last_band, cudaStream_t s) {
   return bt;
 }
 
+// A distribution's density at r: its closed form, or a tabulated one's interpolation.
+double node_density(const scatrs_distribution& d, double r) {
+  return d.kind == kTabulated ? table_density(d.table, d.table_len, r)
+                              : density(d.kind, d.param, r);
+}
+
 void check_options(const scatrs_fixed_options* o, int64_t n_units, int64_t n_mu,
                    const double* mu, int n_derivs = 0) {
   if (!o) throw Failure{SCATRS_INVALID_INPUT, "options must not be NULL"};
@@ -464,7 +470,9 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
   }
   for (int64_t d = 0; d < n_dist && !ad.on; ++d) {
     std::string msg;
-    if (!validate_distribution(dists[d].kind, dists[d].param, &msg))
+    if (!(dists[d].kind == kTabulated
+              ? validate_table(dists[d].table, dists[d].table_len, &msg)
+              : validate_distribution(dists[d].kind, dists[d].param, &msg)))
       throw Failure{SCATRS_INVALID_INPUT, "distribution " + std::to_string(d) + ": " + msg};
     if (!(dists[d].r_lo > 0.0 && dists[d].r_hi > dists[d].r_lo && std::isfinite(dists[d].r_hi)))
       throw Failure{SCATRS_INVALID_INPUT, "distribution " + std::to_string(d) +
@@ -478,10 +486,15 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
       double u;
       if (dv.on) {
         double g[3];
-        u = density_gradient(dists[d].kind, dists[d].param, r, g);
+        if (dists[d].kind == kTabulated) {
+          u = node_density(dists[d], r);
+          g[0] = g[1] = g[2] = 0.0;
+        } else {
+          u = density_gradient(dists[d].kind, dists[d].param, r, g);
+        }
         for (int p = 0; p < 3; ++p) wtheta[(d * n_nodes + j) * 3 + p] = w * (g[p] * r);
       } else {
-        u = density(dists[d].kind, dists[d].param, r);
+        u = node_density(dists[d], r);
       }
       radius[d * n_nodes + j] = r;
       weight[d * n_nodes + j] = w * (u * r);
@@ -1028,6 +1041,8 @@ struct AdPart {
   double f;
   int out;
   std::string who;
+  const double* table = nullptr;  // a tabulated distribution's table
+  int64_t table_len = 0;
 };
 
 struct AdOutputs {
@@ -1071,7 +1086,7 @@ void adaptive_call(const std::vector<AdPart>& in, int n_out, bool batch, const d
   std::vector<adaptive::Part> parts;
   for (const AdPart& p : in) {
     try {
-      parts.push_back(adaptive::make_part(p.kind, p.p, o.rtol));
+      parts.push_back(adaptive::make_part(p.kind, p.p, o.rtol, p.table, p.table_len));
     } catch (const adaptive::Error& e) {
       throw Failure{e.status, p.who + e.msg};
     }
@@ -1934,7 +1949,8 @@ void adaptive_spheroid_call(const scatrs_distribution* dists, int64_t n_dist, bo
   std::vector<adaptive::Part> parts;
   for (int64_t d = 0; d < n_dist; ++d) {
     try {
-      parts.push_back(adaptive::make_part(dists[d].kind, dists[d].param, o.rtol));
+      parts.push_back(adaptive::make_part(dists[d].kind, dists[d].param, o.rtol, dists[d].table,
+                                          dists[d].table_len));
     } catch (const adaptive::Error& e) {
       throw Failure{e.status, "distribution " + std::to_string(d) + ": " + e.msg};
     }
@@ -2322,7 +2338,8 @@ int scatrs_ensemble_adaptive(const scatrs_distribution* dists, int64_t n_dist, i
     for (int64_t d = 0; d < n_dist; ++d)
       parts.push_back(AdPart{dists[d].kind, {dists[d].param[0], dists[d].param[1],
                                              dists[d].param[2]},
-                             m, 1.0, (int)d, "distribution " + std::to_string(d) + ": "});
+                             m, 1.0, (int)d, "distribution " + std::to_string(d) + ": ",
+                             dists[d].table, dists[d].table_len});
     AdOutputs out{values, errors, phase, phase_err, greek, greek_err, converged, panels};
     adaptive_call(parts, (int)n_dist, batch != 0, wavelengths, n_wl, mu, n_mu, options, out);
   });
@@ -2346,7 +2363,8 @@ int scatrs_ensemble_adaptive_layered(const scatrs_distribution* dists, int64_t n
       parts.push_back(AdPart{dists[d].kind, {dists[d].param[0], dists[d].param[1],
                                              dists[d].param[2]},
                              layers->m + 2 * d * layers->n_layers * n_wl, 1.0, (int)d,
-                             "distribution " + std::to_string(d) + ": "});
+                             "distribution " + std::to_string(d) + ": ", dists[d].table,
+                             dists[d].table_len});
     AdOutputs out{values, errors, phase, phase_err, greek, greek_err, converged, panels};
     adaptive_call(parts, (int)n_dist, batch != 0, wavelengths, n_wl, mu, n_mu, options, out,
                   layers);
@@ -2409,7 +2427,7 @@ int scatrs_ensemble_mixture(const scatrs_component* components, int64_t n_comp,
         // The number fraction of engine.rs:2131: w / w_total * v / v_total.
         parts.push_back(AdPart{d.kind, {d.param[0], d.param[1], d.param[2]}, k.m,
                                k.weight / total * v / v_total, 0,
-                               "component " + std::to_string(c) + ": "});
+                               "component " + std::to_string(c) + ": ", d.table, d.table_len});
       }
     }
     AdOutputs out{values, errors, phase, phase_err, greek, greek_err, converged, panels};
@@ -2572,7 +2590,9 @@ int scatrs_ensemble_fixed_spheroid(const scatrs_distribution* dists, int64_t n_d
     std::vector<double> radius(n_dist * n_nodes), weight(n_dist * n_nodes);
     for (int64_t d = 0; d < n_dist; ++d) {
       std::string msg;
-      if (!validate_distribution(dists[d].kind, dists[d].param, &msg))
+      if (!(dists[d].kind == kTabulated
+                ? validate_table(dists[d].table, dists[d].table_len, &msg)
+                : validate_distribution(dists[d].kind, dists[d].param, &msg)))
         throw Failure{SCATRS_INVALID_INPUT, "distribution " + std::to_string(d) + ": " + msg};
       if (!(dists[d].r_lo > 0.0 && dists[d].r_hi > dists[d].r_lo && std::isfinite(dists[d].r_hi)))
         throw Failure{SCATRS_INVALID_INPUT, "distribution " + std::to_string(d) +
@@ -2582,7 +2602,7 @@ int scatrs_ensemble_fixed_spheroid(const scatrs_distribution* dists, int64_t n_d
       for (int64_t j = 0; j < n_nodes; ++j) {
         const double r = std::exp(ctr + h * gl.first[j]);
         radius[d * n_nodes + j] = r;
-        weight[d * n_nodes + j] = h * gl.second[j] * (density(dists[d].kind, dists[d].param, r) * r);
+        weight[d * n_nodes + j] = h * gl.second[j] * (node_density(dists[d], r) * r);
       }
     }
     // Every node of every unit is one spheroid of the batch (particle.rs:317-366).

@@ -148,15 +148,17 @@ __device__ __forceinline__ SideD layer_side_d(DC mi, DC mo, SideD prev, DC h, DC
 }
 
 // Layered (mie_device.cuh) with derivatives: interface sizes x[l] and indices m[l] with their
-// derivatives along the parameter.
+// derivatives along the parameter, for at most kCap layers (the per-shell state sized at
+// compile time, so that a few layers stay out of local memory).
+template <int kCap>
 struct LayeredD {
   int layers;
   const DR* x;
   const DC* m;
   ArraysD arr;
-  LArgD inner[kMaxLayers - 1], outer[kMaxLayers - 1], core;
-  DC p[kMaxLayers - 1], lead[kMaxLayers - 1];
-  bool chi[kMaxLayers - 1];
+  LArgD inner[kCap - 1], outer[kCap - 1], core;
+  DC p[kCap - 1], lead[kCap - 1];
+  bool chi[kCap - 1];
 
   __device__ __forceinline__ int a_outer(int l) const { return l == layers - 1 ? 0 : 2 * l + 1; }
   __device__ __forceinline__ int a_inner(int l) const { return 2 * l; }
@@ -240,9 +242,9 @@ struct LayeredD {
 // the particle's size parameter (fixed), m its outer index (with its derivative). emit(k, a_k,
 // b_k, da_k, db_k); the absorption sum's derivatives along the parameter (abs_d[0]) and, for a
 // complex-derivative direction, along i times it (abs_d[1]). Returns the absorption sum.
-template <class Emit>
+template <class Emit, class Lay>
 __device__ double layered_finish_d(double x, DC m, int64_t n, const Scratch& s, ValueSums& vs,
-                                   Emit emit, LayeredD& layers, double abs_d[2]) {
+                                   Emit emit, Lay& layers, double abs_d[2]) {
   const double one = 1.0;
   const DC z = dscl(m, x);
   const int64_t n_s = upward_orders(x, n);

@@ -271,7 +271,8 @@ __global__ void __launch_bounds__(128) mie_deriv_kernel(MieFixedArgs a) { mie_ch
 // row layout and chunk sums as mie_chunk_deriv, the blocks "Re" and "Im" being the derivative
 // along the direction and along i times it (meaningful for the index directions only).
 // Scratch per chunk: 2 (2L - 1) arrays (the ratios and their derivatives) of nc + 2 rows.
-__global__ void __launch_bounds__(128) mie_layered_deriv_kernel(MieFixedArgs a) {
+template <int kCap>
+__device__ __forceinline__ void layered_deriv_chunk(const MieFixedArgs& a) {
   int wslot = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   int lane = threadIdx.x & 31;
   if (wslot >= a.n_chunks) return;
@@ -301,10 +302,10 @@ __global__ void __launch_bounds__(128) mie_layered_deriv_kernel(MieFixedArgs a) 
     const double w = a.weight[d * a.n_nodes + j];
     const double x = 2.0 * kPi * r / a.wl[i];
     n = default_n_max(x);
-    double xs[kMaxLayers];
-    cplx ms[kMaxLayers];
-    lder::DR xd[kMaxLayers];
-    lder::DC md[kMaxLayers];
+    double xs[kCap];
+    cplx ms[kCap];
+    lder::DR xd[kCap];
+    lder::DC md[kCap];
     bool lossless = true;
     const int dir = a.deriv_dir;
     for (int l = 0; l < L; ++l) {
@@ -321,7 +322,7 @@ __global__ void __launch_bounds__(128) mie_layered_deriv_kernel(MieFixedArgs a) 
     DerivSums ds;
     if (st == 0 && n <= nc) {
       mie_prepare(x, ms[L - 1], n, s);  // u_k(x); array 0 is redone with its derivatives
-      lder::LayeredD lay;
+      lder::LayeredD<kCap> lay;
       lay.layers = L;
       lay.x = xd;
       lay.m = md;
@@ -383,6 +384,14 @@ __global__ void __launch_bounds__(128) mie_layered_deriv_kernel(MieFixedArgs a) 
       if (lane == 0) a.chunk_sums[((int64_t)chunk * B + b) * 8 + k] = v;
     }
   }
+}
+
+// Up to 4 layers with the per-shell state sized for them; more through the general form.
+__global__ void __launch_bounds__(128) mie_layered_deriv_kernel(MieFixedArgs a) {
+  layered_deriv_chunk<4>(a);
+}
+__global__ void __launch_bounds__(128) mie_layered_deriv16_kernel(MieFixedArgs a) {
+  layered_deriv_chunk<kMaxLayers>(a);
 }
 
 // Layered spheres (their per-layer state lives in local memory).
@@ -519,7 +528,9 @@ void launch_plan_chunks(const PlanArgs& a, cudaStream_t s) {
 void launch_mie_fixed(const MieFixedArgs& a, cudaStream_t s) {
   int threads = 128;
   int blocks = (a.n_chunks * 32 + threads - 1) / threads;
-  if (a.deriv && a.n_layers > 1)
+  if (a.deriv && a.n_layers > 4)
+    mie_layered_deriv16_kernel<<<blocks, threads, 0, s>>>(a);
+  else if (a.deriv && a.n_layers > 1)
     mie_layered_deriv_kernel<<<blocks, threads, 0, s>>>(a);
   else if (a.deriv)
     mie_deriv_kernel<<<blocks, threads, 0, s>>>(a);

@@ -281,7 +281,42 @@ double density(int kind, const double* p, double r) {
   return std::exp(ln_u);
 }
 
-int parameter_count(int kind) { return kind == 3 ? 3 : kind == 4 ? 1 : 2; }
+int parameter_count(int kind) { return kind == 3 ? 3 : kind == 4 ? 1 : kind == kTabulated ? 0 : 2; }
+
+double table_density(const double* t, int64_t n, double r) {
+  const double* xs = t;
+  const double* ys = t + n;
+  if (r < xs[0] || r > xs[n - 1]) return 0.0;
+  // The first point above r (partition_point of v <= r), kept in 1..n-1.
+  int64_t lo = 0, hi = n;
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) / 2;
+    if (xs[mid] <= r) lo = mid + 1; else hi = mid;
+  }
+  const int64_t i = std::min<int64_t>(std::max<int64_t>(lo, 1), n - 1);
+  const double w = (r - xs[i - 1]) / (xs[i] - xs[i - 1]);
+  return ys[i - 1] + w * (ys[i] - ys[i - 1]);
+}
+
+bool validate_table(const double* t, int64_t n, std::string* msg) {
+  if (!t || n < 2) {
+    *msg = "a tabulated distribution needs at least 2 points and as many densities as radii";
+    return false;
+  }
+  for (int64_t k = 0; k < n; ++k)
+    if (!(std::isfinite(t[k]) && t[k] > 0.0)) return *msg = "radius must be finite and > 0", false;
+  for (int64_t k = 1; k < n; ++k)
+    if (!(t[k - 1] < t[k])) return *msg = "tabulated radii must increase", false;
+  bool any = false;
+  for (int64_t k = 0; k < n; ++k) {
+    const double u = t[n + k];
+    if (!(std::isfinite(u) && u >= 0.0))
+      return *msg = "tabulated densities must be finite and >= 0", false;
+    any = any || u != 0.0;
+  }
+  if (!any) return *msg = "tabulated densities must not all be 0", false;
+  return true;
+}
 
 double density_gradient(int kind, const double* p, double r, double grad[3]) {
   const double u = density(kind, p, r);

@@ -32,6 +32,12 @@ int64_t band_upper(int index);
 // density u(r).
 bool validate_distribution(int kind, const double* p, std::string* msg);
 double density(int kind, const double* p, double r);
+// Tabulated distributions (kind 6): table = [r_0..r_{n-1}, u_0..u_{n-1}], n(r) linear between
+// the points and 0 outside them (distribution.rs:406-417); their checks
+// (distribution.rs:149-171).
+constexpr int kTabulated = 6;
+double table_density(const double* table, int64_t n, double r);
+bool validate_table(const double* table, int64_t n, std::string* msg);
 
 // The number of a distribution kind's parameters (ensemble/mod.rs:254-337) and the gradient of
 // u(r) along them at a fixed reference radius (distribution.rs:370-441); the reference radius'

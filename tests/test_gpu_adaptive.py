@@ -16,8 +16,11 @@ MU = np.array([1.0, 0.7, 0.0, -0.4, -1.0])
 
 
 def _odist(d):
+    """The oracle's records of d (tables are shared: d must outlive the oracle call)."""
     o = np.zeros(d.size, dtype=O.DIST_DTYPE)
     o["kind"], o["p"] = d["kind"], d["param"]
+    o["r_lo"], o["r_hi"] = d["r_lo"], d["r_hi"]
+    o["table"], o["table_len"] = d["table"], d["table_len"]
     return o
 
 

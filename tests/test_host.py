@@ -2,11 +2,15 @@
 workloads, and ensemble identities of the reference's tests (scatrs/tests/ensemble.rs) on the
 oracle's fixed-grid restatement."""
 
+import ctypes
+import os
+import subprocess
+
 import numpy as np
 import pytest
 
 from oracle import oracle as O
-from scatrs_b200 import _scatrs, workloads as W
+from scatrs_b200 import _native, _scatrs, workloads as W
 from scatrs_b200.errors import InvalidInputError
 
 
@@ -38,6 +42,43 @@ def test_distribution_specs_and_ranges():
         _scatrs._dist_array([("gamma", 1.0, 0.1)], 4.0)
     with pytest.raises(TypeError):
         _scatrs._dist_array([("bogus", 1.0)], 4.0)
+
+
+def test_tabulated_specs_point_at_their_tables():
+    """("tabulated", radii, densities) (scatrs-py/src/ensemble.rs:58-61): kind 6, the table as
+    radii then densities, kept alive by the records; the grid spans the table."""
+    d = _scatrs._adaptive_dists([("lognormal", 0.2, 1.5), ("tabulated", [0.1, 0.3, 0.9],
+                                                            [0.0, 2.0, 1.0])])
+    assert d["kind"].tolist() == [1, _native.TABULATED] and d["table_len"].tolist() == [0, 3]
+    tab = np.ctypeslib.as_array(
+        ctypes.cast(int(d["table"][1]), ctypes.POINTER(ctypes.c_double)), shape=(6,))
+    assert tab.tolist() == [0.1, 0.3, 0.9, 0.0, 2.0, 1.0]
+    assert len(d.tables) == 1 and d.tables[0].ctypes.data == int(d["table"][1])
+    f = _scatrs._dist_array([("tabulated", [0.1, 0.9], [1.0, 1.0])], 4.0)
+    assert (f["r_lo"][0], f["r_hi"][0]) == (0.1, 0.9)
+    with pytest.raises(InvalidInputError, match="at least 2 points"):
+        _scatrs._adaptive_dists([("tabulated", [0.1, 0.2, 0.3], [1.0, 1.0])])
+
+
+def test_distribution_records_match_the_c_struct(tmp_path):
+    """The numpy record is scatrs_distribution byte for byte (size and field offsets)."""
+    src = tmp_path / "layout.c"
+    src.write_text(
+        '#include <stddef.h>\n#include <stdio.h>\n#include "scatrs_b200.h"\n'
+        "int main(void) { printf(\"%zu %zu %zu %zu %zu %zu %zu\", sizeof(scatrs_distribution), "
+        "offsetof(scatrs_distribution, param), offsetof(scatrs_distribution, r_lo), "
+        "offsetof(scatrs_distribution, r_hi), offsetof(scatrs_distribution, table), "
+        "offsetof(scatrs_distribution, table_len), offsetof(scatrs_distribution, kind)); "
+        "return 0; }\n")
+    exe = tmp_path / "layout"
+    inc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
+    subprocess.run(["gcc", "-I", inc, str(src), "-o", str(exe)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True,
+                                          check=True).stdout.split()]
+    t = _native.DIST_DTYPE
+    want = [t.itemsize] + [t.fields[k][1] for k in ("param", "r_lo", "r_hi", "table",
+                                                     "table_len", "kind")]
+    assert got == want
 
 
 def test_workloads_are_seeded_and_shaped():
