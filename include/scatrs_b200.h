@@ -180,6 +180,50 @@ int scatrs_ensemble_mixture(const scatrs_component* components, int64_t n_comp,
                             double* greek_err, int8_t* converged, int64_t* panels, char* err,
                             size_t err_len);
 
+/* A parameter to differentiate the outputs with respect to (scatrs::ensemble::EnsembleParam,
+ * ensemble/mod.rs:180-215): the mixture component (0 for a single distribution), the mode of a
+ * multimodal distribution (-1 when the component's distribution is not multimodal, or for its
+ * refractive index and its weight), the kind, and for a distribution parameter its index in the
+ * distribution's parameter list (SizeDistribution::parameter_names: lognormal median_radius,
+ * width; gamma effective_radius, effective_variance; modified gamma alpha, b, gamma; power law
+ * exponent). */
+enum {
+  SCATRS_PARAM_DISTRIBUTION = 0, /* ParamKind::Distribution(name) */
+  SCATRS_PARAM_REFR_REAL = 1,    /* ParamKind::RefrReal */
+  SCATRS_PARAM_REFR_IMAG = 2,    /* ParamKind::RefrImag */
+  SCATRS_PARAM_WEIGHT = 3        /* ParamKind::Weight: a component's (mode -1) or a mode's */
+};
+typedef struct scatrs_param {
+  int32_t component;
+  int32_t mode;
+  int32_t kind;
+  int32_t index;
+} scatrs_param;
+
+/*
+ * scatrs_ensemble_mixture with the derivatives of every output along `params`
+ * (EnsembleOptions::derivatives; the adaptive engine's derivative blocks, engine.rs:1370-1380,
+ * 1782-1836, 2121-2176): each pass refines and integrates the requested distribution parameters'
+ * blocks (weights du/dtheta r) and the derivatives along Re m and Im m, the averages follow
+ * the quotient rule against the moments' dZ, the mixing adds the weight derivatives, and the
+ * ratios carry the derivatives with first-order error estimates (ensemble/lin.rs). A component
+ * is multimodal when its mode_weights are given. Spheres only; not for a single radius's
+ * radius. d_values, d_errors (P, 11, n_wl); d_phase, d_phase_err (P, 6, n_wl, n_mu); d_greek,
+ * d_greek_err (P, 6, n_wl, L + 1), P = n_params, in the order of `params`. Invalid or
+ * repeated parameters: SCATRS_INVALID_INPUT naming the parameter.
+ * Replaces: the derivative path of Mixture::compute / Ensemble.compute(derivatives=...)
+ * (scatrs/src/ensemble/mod.rs:548-625; scatrs-py/src/ensemble.rs:295-349 deriv_idx).
+ */
+int scatrs_ensemble_mixture_d(const scatrs_component* components, int64_t n_comp,
+                              const double* wavelengths, int64_t n_wl, const double* mu,
+                              int64_t n_mu, const scatrs_adaptive_options* options,
+                              const scatrs_param* params, int64_t n_params, double* values,
+                              double* errors, double* d_values, double* d_errors, double* phase,
+                              double* phase_err, double* d_phase, double* d_phase_err,
+                              double* greek, double* greek_err, double* d_greek,
+                              double* d_greek_err, int8_t* converged, int64_t* panels, char* err,
+                              size_t err_len);
+
 /*
  * The Greek coefficients of phase matrices tabulated at the n_q Gauss-Legendre cosines
  * (ascending, the rule of scatrs_gauss_legendre), projected with the reference's projector

@@ -494,6 +494,62 @@ def ensemble_mixture(components, wavelengths, mu=None, greek_order=None, normali
     return out
 
 
+PARAM_DTYPE = np.dtype([("component", np.int32), ("mode", np.int32), ("kind", np.int32),
+                        ("index", np.int32)])
+PK_DIST, PK_REFR_REAL, PK_REFR_IMAG, PK_WEIGHT = 0, 1, 2, 3
+
+
+def params(*specs) -> np.ndarray:
+    """Parameter records from (component, mode or -1, kind, index) tuples."""
+    return np.array([tuple(p) for p in specs], dtype=PARAM_DTYPE)
+
+
+def ensemble_mixture_d(components, wavelengths, derivs, mu=None, greek_order=None,
+                       normalized=True, rtol=1e-6, max_panels=4096, allow_unvalidated=False,
+                       refine_backscatter=False) -> dict:
+    """ensemble_mixture with the derivatives along `derivs` (PARAM_DTYPE records): adds d, d_err
+    (P, 11, n), phase_d, phase_d_err (P, 6, n, n_mu), greek_d, greek_d_err (P, 6, n, L + 1).
+    A component whose mode weights are given is multimodal (its parameters carry a mode)."""
+    wl = np.ascontiguousarray(wavelengths, dtype=np.float64).reshape(-1)
+    modes, mw, nm, w, ms = _mixture_arrays(components, wl.size)
+    mm = np.array([1 if mwc is not None else 0 for _d, mwc, _w, _m in components], dtype=np.int32)
+    pr = np.ascontiguousarray(np.atleast_1d(np.asarray(derivs, dtype=PARAM_DTYPE)))
+    P = pr.size
+    mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
+    n = wl.size
+    L = -1 if greek_order is None else int(greek_order)
+    out = {"values": np.zeros((11, n)), "errors": np.zeros((11, n)),
+           "d": np.zeros((P, 11, n)), "d_err": np.zeros((P, 11, n)),
+           "converged": np.zeros(n, dtype=np.int8), "panels": np.zeros(n, dtype=np.int64)}
+    ph = pe = g = ge = dph = dpe = dg = dge = None
+    if mu.size:
+        ph, pe = np.zeros((6, n, mu.size)), np.zeros((6, n, mu.size))
+        dph, dpe = np.zeros((P, 6, n, mu.size)), np.zeros((P, 6, n, mu.size))
+    if L >= 0:
+        g, ge = np.zeros((6, n, L + 1)), np.zeros((6, n, L + 1))
+        dg, dge = np.zeros((P, 6, n, L + 1)), np.zeros((P, 6, n, L + 1))
+    err = ctypes.create_string_buffer(512)
+    f = lib().orc_ensemble_mixture_d
+    f.argtypes = [ctypes.c_void_p, _PD, ctypes.c_void_p, ctypes.c_void_p, _PD, _PD, _I64, _PD,
+                  _I64, _PD, _I64, _I64, ctypes.c_int, _D, _I64, ctypes.c_int, ctypes.c_int,
+                  ctypes.c_void_p, _I64] + [_PD] * 12 + [ctypes.c_void_p, ctypes.c_void_p,
+                                                         ctypes.c_char_p, _I64]
+    st = f(modes.ctypes.data, _p(mw), nm.ctypes.data, mm.ctypes.data, _p(w),
+           _p(ms.view(np.float64)), nm.size, _p(wl), wl.size, _p(mu), mu.size, L,
+           int(normalized), rtol, max_panels, int(allow_unvalidated), int(refine_backscatter),
+           pr.ctypes.data if P else None, P, _p(out["values"]), _p(out["errors"]), _p(ph),
+           _p(pe), _p(g), _p(ge), _p(out["d"]), _p(out["d_err"]), _p(dph), _p(dpe), _p(dg),
+           _p(dge), out["converged"].ctypes.data, out["panels"].ctypes.data, err, 512)
+    if st != 0:
+        raise OracleError(st, err.value.decode())
+    out["converged"] = out["converged"].astype(bool)
+    if ph is not None:
+        out["phase"], out["phase_err"], out["phase_d"], out["phase_d_err"] = ph, pe, dph, dpe
+    if g is not None:
+        out["greek"], out["greek_err"], out["greek_d"], out["greek_d_err"] = g, ge, dg, dge
+    return out
+
+
 def tmatrix_mode(x: float, eps: float, s: complex, m: int, n: int, n_theta: int,
                  quad: bool = False) -> np.ndarray:
     """One azimuthal mode's T-matrix of a spheroid (2K x 2K complex, K = n - max(m, 1) + 1); in

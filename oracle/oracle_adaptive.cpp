@@ -137,15 +137,25 @@ std::pair<double, double> cutoffs(const Density& d, double center, double eps,
   throw Failure{INVALID_INPUT, "the size distribution is too broad: its tails do not decay"};
 }
 
+// moments.rs:15-26: <r^2>, <r^3> and Z with their error estimates, and their derivatives along
+// the requested distribution parameters with theirs.
 struct Moments {
   double v[2], e[2], z, ez;
+  std::vector<std::array<double, 2>> d, de;
+  std::vector<double> dz, dez;
 };
 
-// moments.rs:62-167 (no derivative parameters).
+// moments.rs:62-167: GK15 panels of at most the step (the breaks inside the range as edges),
+// split where |Kronrod - Gauss| of any of the 3 (1 + nt) sums is above its share, until each
+// meets rtol (of |sum| for the values, of the Kronrod sum of the absolute integrand for the
+// derivatives); the averages by the quotient rule with first-order error propagation. `grads`
+// are the requested parameters' indices into the density's gradient.
 Moments moments(const Density& d, std::pair<double, double> range, double rtol,
-                double truncation, const std::vector<double>& breaks = {}) {
+                double truncation, const std::vector<double>& breaks = {},
+                const std::vector<int>& grads = {}) {
   const double step = max_step(d, STEP);
   const double t_lo = std::log(range.first), t_hi = std::log(range.second);
+  const int nt = (int)grads.size(), nq = 3 * (1 + nt);
   std::vector<std::pair<double, double>> panels;
   {
     // moments.rs:71-86: the breaks inside the range are panel edges, each interval in equal
@@ -163,16 +173,15 @@ Moments moments(const Density& d, std::pair<double, double> range, double rtol,
       for (size_t i = 0; i < n; ++i) panels.push_back({a + i * h, a + (i + 1) * h});
     }
   }
-  auto finish = [&](const std::vector<std::array<double, 6>>& sums) {
-    double s[3] = {0, 0, 0}, e[3] = {0, 0, 0};
-    for (int j = 0; j < 3; ++j)
-      for (auto& p : sums) {
-        s[j] += p[j];
-        e[j] += p[3 + j];
-      }
+  // moments.rs:171-212 (averages).
+  auto finish = [&](const std::vector<double>& s, const std::vector<double>& e) {
     const double z = s[0], ez = e[0];
-    if (!(std::isfinite(z) && z > 0.0))
-      throw Failure{INVALID_INPUT, "the size distribution has no finite positive mass on its range"};
+    if (!(std::isfinite(z) && z > 0.0)) {
+      char buf[128];
+      snprintf(buf, sizeof buf,
+               "the size distribution has no finite positive mass on its range (got %e)", z);
+      throw Failure{INVALID_INPUT, buf};
+    }
     Moments m;
     m.z = z;
     m.ez = ez;
@@ -180,44 +189,73 @@ Moments moments(const Density& d, std::pair<double, double> range, double rtol,
       m.v[k] = s[1 + k] / z;
       m.e[k] = (e[1 + k] + std::fabs(m.v[k]) * ez) / z + truncation * std::fabs(m.v[k]);
     }
+    for (int b = 0; b < nt; ++b) {
+      const int o = 3 * (1 + b);
+      const double dz = s[o];
+      std::array<double, 2> dv, dev;
+      for (int k = 0; k < 2; ++k) dv[k] = (s[o + 1 + k] - m.v[k] * dz) / z;
+      for (int k = 0; k < 2; ++k)
+        dev[k] = (e[o + 1 + k] + std::fabs(m.v[k]) * e[o] + std::fabs(dv[k]) * ez +
+                  m.e[k] * std::fabs(dz)) / z +
+                 truncation * std::fabs(dv[k]);
+      m.d.push_back(dv);
+      m.de.push_back(dev);
+      m.dz.push_back(dz);
+      m.dez.push_back(e[o]);
+    }
     return m;
   };
+  std::vector<double> grad(3);
   for (;;) {
-    std::vector<std::array<double, 6>> sums;  // Kronrod sums of 1, r^2, r^3, then |K - G|
-    for (auto& p : panels) {
+    // Per panel: Kronrod sums, |K - G| and Kronrod sums of the absolute integrands
+    // (moments.rs:31-53).
+    const size_t n = panels.size();
+    std::vector<double> K(n * nq, 0.0), E(n * nq, 0.0), A(n * nq, 0.0);
+    for (size_t i = 0; i < n; ++i) {
       Node nd[15];
-      gk_panel(p.first, p.second, nd);
-      double k[3] = {0, 0, 0}, g[3] = {0, 0, 0};
-      for (auto& n : nd) {
-        const double r = std::exp(n.t);
-        const double u = density_eval(d, r, nullptr);
+      gk_panel(panels[i].first, panels[i].second, nd);
+      std::vector<double> g(nq, 0.0);
+      for (auto& x : nd) {
+        const double r = std::exp(x.t);
+        const double u = density_eval(d, r, grad.data());
         const double q[3] = {1.0, r * r, r * r * r};
         for (int j = 0; j < 3; ++j) {
-          k[j] += n.wk * u * r * q[j];
-          g[j] += n.wg * u * r * q[j];
+          K[i * nq + j] += x.wk * u * r * q[j];
+          g[j] += x.wg * u * r * q[j];
+          for (int b = 0; b < nt; ++b) {
+            const int o = 3 * (1 + b) + j;
+            const double y = grad[grads[b]] * r * q[j];
+            K[i * nq + o] += x.wk * y;
+            g[o] += x.wg * y;
+            A[i * nq + o] += x.wk * std::fabs(y);
+          }
         }
       }
-      sums.push_back({k[0], k[1], k[2], std::fabs(k[0] - g[0]), std::fabs(k[1] - g[1]),
-                      std::fabs(k[2] - g[2])});
+      for (int j = 0; j < nq; ++j) E[i * nq + j] = std::fabs(K[i * nq + j] - g[j]);
     }
-    double total[3] = {0, 0, 0}, terr[3] = {0, 0, 0}, target[3];
-    for (auto& s : sums)
-      for (int j = 0; j < 3; ++j) {
-        total[j] += s[j];
-        terr[j] += s[3 + j];
+    std::vector<double> total(nq, 0.0), terr(nq, 0.0), target(nq, 0.0);
+    for (size_t i = 0; i < n; ++i)
+      for (int j = 0; j < nq; ++j) {
+        total[j] += K[i * nq + j];
+        terr[j] += E[i * nq + j];
       }
-    bool met = true;
-    for (int j = 0; j < 3; ++j) {
-      target[j] = rtol * std::fabs(total[j]);
-      met = met && terr[j] <= target[j];
+    for (int j = 0; j < nq; ++j) {
+      if (j < 3) {
+        target[j] = rtol * std::fabs(total[j]);
+      } else {
+        double abs = 0.0;
+        for (size_t i = 0; i < n; ++i) abs += A[i * nq + j];
+        target[j] = rtol * abs;
+      }
     }
-    const size_t n = panels.size();
-    if (met || n >= MOMENT_MAX_PANELS) return finish(sums);
+    bool met = true;
+    for (int j = 0; j < nq; ++j) met = met && terr[j] <= target[j];
+    if (met || n >= MOMENT_MAX_PANELS) return finish(total, terr);
     std::vector<std::pair<double, double>> next;
     for (size_t i = 0; i < n; ++i) {
       bool bad = false;
-      for (int j = 0; j < 3; ++j)
-        bad = bad || (sums[i][3 + j] * (double)n > target[j] && terr[j] > target[j]);
+      for (int j = 0; j < nq; ++j)
+        bad = bad || (E[i * nq + j] * (double)n > target[j] && terr[j] > target[j]);
       const auto& p = panels[i];
       if (bad && p.second - p.first > 1e-10) {
         const double mid = 0.5 * (p.first + p.second);
@@ -227,7 +265,7 @@ Moments moments(const Density& d, std::pair<double, double> range, double rtol,
         next.push_back(p);
       }
     }
-    if (next.size() == n) return finish(sums);
+    if (next.size() == n) return finish(total, terr);
     panels.swap(next);
   }
 }
@@ -244,6 +282,15 @@ struct Part {
   int64_t n_wl = 0;
   double eps = 0.0;  // > 0: a spheroid of this aspect ratio (the direct path)
   double f = 1.0;             // the number fraction in its unit (engine.rs:2131)
+  // engine.rs:95-115: the component and mode, the component's weight w and the mode's weight
+  // v with the component's sum of mode weights (1, 1 without modes); the requested
+  // distribution parameters (result column, index into the gradient) and the result columns
+  // of the derivatives along Re m and Im m (-1: not requested).
+  int component = 0, mode = -1;
+  double w = 1.0, v = 1.0, v_total = 1.0;
+  std::vector<std::pair<int, int>> theta;
+  int dir_col[2] = {-1, -1};
+  bool dir_derivatives() const { return dir_col[0] >= 0 || dir_col[1] >= 0; }
   Density den;
   SupportKind support;
   double s_a = 0, s_b = 0;  // center (unbounded), [lo, hi] (finite), radius (point)
@@ -251,7 +298,9 @@ struct Part {
   Moments mom{};
 };
 
-Part make_part(const FixedDist& d, double rtol) {
+// parts (engine.rs:141-223) for one distribution: its support, cut-offs and moments, the
+// moments with the derivatives along `grads` (indices into the density's gradient).
+Part make_part(const FixedDist& d, double rtol, const std::vector<int>& grads = {}) {
   Part p;
   p.dist = d;
   if (d.kind == MONODISPERSE) {
@@ -271,7 +320,7 @@ Part make_part(const FixedDist& d, double rtol) {
     p.s_a = d.table[0];
     p.s_b = d.table[d.table_len - 1];
     p.mom = moments(p.den, {p.s_a, p.s_b}, rtol, 0.0,
-                    std::vector<double>(d.table, d.table + d.table_len));
+                    std::vector<double>(d.table, d.table + d.table_len), grads);
     p.cut = {p.s_a, p.s_b};
     return p;
   }
@@ -280,7 +329,7 @@ Part make_part(const FixedDist& d, double rtol) {
     p.support = FINITE;
     p.s_a = d.p[1];
     p.s_b = d.p[2];
-    p.mom = moments(p.den, {p.s_a, p.s_b}, rtol, 0.0);
+    p.mom = moments(p.den, {p.s_a, p.s_b}, rtol, 0.0, {}, grads);
     p.cut = {p.s_a, p.s_b};
     return p;
   }
@@ -291,7 +340,7 @@ Part make_part(const FixedDist& d, double rtol) {
   p.cut = cutoffs(p.den, p.s_a, rtol / 10.0, {2});
   const double eps = std::max(1e-3 * rtol, 1e-16);
   auto wide = cutoffs(p.den, p.s_a, eps, {0, 2, 3});
-  p.mom = moments(p.den, wide, rtol, 0.2 * rtol);
+  p.mom = moments(p.den, wide, rtol, 0.2 * rtol, {}, grads);
   return p;
 }
 
@@ -386,13 +435,14 @@ int64_t node_terms(double r, double lambda, const Optics& op, bool allow, std::v
   return n;
 }
 
-// A solved particle at radius r, or a Failure with the node's context.
+// A solved particle at radius r (with the derivatives along m if asked: spheres only), or a
+// Failure with the node's context.
 void solve(double r, double lambda, const Optics& op, bool allow, MieState& st,
-           int64_t* n_terms) {
+           int64_t* n_terms, bool derivs = false) {
   std::vector<double> xs;
   const int64_t n = node_terms(r, lambda, op, allow, xs);
   if (op.fr.empty()) {
-    st.solve(size_param(r, lambda), op.m, n, false);
+    st.solve(size_param(r, lambda), op.m, n, derivs);
   } else {
     layered_solve(xs, op.ml, n, st);
     st.x = xs.back();
@@ -400,18 +450,35 @@ void solve(double r, double lambda, const Optics& op, bool allow, MieState& st,
   *n_terms = n;
 }
 
+// engine.rs:358-373: per part, the Kronrod sums of each refined quantity and then of each
+// theta-weighted one (a block of n_refined per requested parameter), |Kronrod - Gauss| of the
+// same, the Kronrod sums of |du/dtheta| r |q| (the theta blocks' scales) and of u r |q| (the
+// scales of the derivatives along m), the largest number of terms, and the integrands per unit
+// ln r at the panel's first and last nodes.
 struct Sums1 {
-  double k[N_BASE], err[N_BASE], absv[N_BASE];
-  int64_t n_terms;
-  double edge[2][N_BASE];
+  std::vector<double> k, err, abs, absv;
+  int64_t n_terms = 0;
+  std::vector<double> edge[2];
 };
 
-// quantities1 + panel1 (engine.rs:369-560) for every part of a group.
+// The pass-1 quantities (engine.rs:50-55, 464-471): 1, C_ext, C_sca, C_sca g, C_back, C_abs,
+// then M_GROUP derivatives per requested direction along m.
+constexpr int M_GROUP = 5;
+int n_refined(const Part& p) {
+  return N_BASE + M_GROUP * ((p.dir_col[0] >= 0) + (p.dir_col[1] >= 0));
+}
+
+// quantities1 + panel1 (engine.rs:369-560) for every part of a group: each node's quantities
+// (the derivatives of C_ext, C_sca, C_sca g, C_back and C_abs along each direction that the
+// group's first part asks for), weighted by each part's u r and du/dtheta r.
 std::vector<Sums1> panel1(const std::vector<const Part*>& group, double a, double b,
                           double lambda, const Optics& m, const Options& o) {
   Node nd[15];
   gk_panel(a, b, nd);
-  double q[15][N_BASE];
+  const Part& first = *group.front();
+  const int nr = n_refined(first);
+  const bool derivs = first.dir_derivatives();
+  std::vector<std::vector<double>> q(15, std::vector<double>(nr, 0.0));
   int64_t n_max = 0;
   MieState st;
   for (int i = 0; i < 15; ++i) {
@@ -426,45 +493,76 @@ std::vector<Sums1> panel1(const std::vector<const Part*>& group, double a, doubl
       continue;
     }
     int64_t n;
-    solve(r, lambda, m, o.allow_unvalidated, st, &n);
+    solve(r, lambda, m, o.allow_unvalidated, st, &n, derivs);
     n_max = std::max(n_max, n);
     const Efficiencies e = efficiencies(st);
     const double v[N_BASE] = {1.0,           area * e.q_ext,  area * e.q_sca,
                               area * e.q_sca * e.g, area * e.q_back, area * e.q_abs};
     for (int j = 0; j < N_BASE; ++j) q[i][j] = v[j];
+    int at = N_BASE;
+    for (int dir = 0; dir < 2; ++dir) {
+      if (first.dir_col[dir] < 0) continue;
+      const Efficiencies d = efficiency_dir(st, dir, e);
+      const double dq[M_GROUP] = {area * d.q_ext, area * d.q_sca,
+                                  area * (d.q_sca * e.g + e.q_sca * d.g), area * d.q_back,
+                                  area * d.q_abs};
+      for (int j = 0; j < M_GROUP; ++j) q[i][at + j] = dq[j];
+      at += M_GROUP;
+    }
   }
   std::vector<Sums1> out;
+  double grad[3];
   for (const Part* p : group) {
-    Sums1 s{};
-    double g[N_BASE] = {};
+    const int nt = (int)p->theta.size(), nb = (1 + nt) * nr;
+    Sums1 s;
+    s.k.assign(nb, 0.0);
+    s.err.assign(nb, 0.0);
+    s.abs.assign(nt * nr, 0.0);
+    s.absv.assign(nr, 0.0);
+    s.edge[0].assign(nb, 0.0);
+    s.edge[1].assign(nb, 0.0);
+    std::vector<double> g(nb, 0.0);
     for (int i = 0; i < 15; ++i) {
       const double r = std::exp(nd[i].t);
-      const double u = density_eval(p->den, r, nullptr);
+      const double u = density_eval(p->den, r, grad);
       const double base = u * r;
-      for (int j = 0; j < N_BASE; ++j) {
-        s.k[j] += nd[i].wk * base * q[i][j];
-        g[j] += nd[i].wg * base * q[i][j];
-        s.absv[j] += nd[i].wk * std::fabs(base * q[i][j]);
-        if (i == 0) s.edge[0][j] = base * q[i][j];
-        if (i == 14) s.edge[1][j] = base * q[i][j];
+      const int end = i == 0 ? 0 : (i == 14 ? 1 : -1);
+      for (int j = 0; j < nr; ++j) {
+        const double qj = q[i][j];
+        s.k[j] += nd[i].wk * base * qj;
+        g[j] += nd[i].wg * base * qj;
+        s.absv[j] += nd[i].wk * std::fabs(base * qj);
+        if (end >= 0) s.edge[end][j] = base * qj;
+        for (int bi = 0; bi < nt; ++bi) {
+          const double dw = grad[p->theta[bi].second] * r;
+          const int o2 = (1 + bi) * nr + j;
+          s.k[o2] += nd[i].wk * dw * qj;
+          g[o2] += nd[i].wg * dw * qj;
+          s.abs[bi * nr + j] += nd[i].wk * std::fabs(dw * qj);
+          if (end >= 0) s.edge[end][o2] = dw * qj;
+        }
       }
     }
-    for (int j = 0; j < N_BASE; ++j) s.err[j] = std::fabs(s.k[j] - g[j]);
+    for (int j = 0; j < nb; ++j) s.err[j] = std::fabs(s.k[j] - g[j]);
     s.n_terms = n_max;
-    out.push_back(s);
+    out.push_back(std::move(s));
   }
   return out;
 }
 
 struct Status {
-  double target[N_BASE], errors[N_BASE];
+  std::vector<double> target, errors;
   bool met;
   bool small[2];
 };
 
-// engine.rs:620-720 (no Greek refinement, no derivatives).
-Status status(const std::vector<const Sums1*>& sums, const Options& o, double ext) {
+// engine.rs:620-720 (no Greek refinement): the targets, errors and ends of one part.
+Status status(const Part& part, const std::vector<const Sums1*>& sums, const Options& o,
+              double ext) {
+  const int nr = n_refined(part), nt = (int)part.theta.size(), nb = (1 + nt) * nr;
+  const int n_greek = N_BASE;
   Status s;
+  s.target.assign(nb, 0.0);
   auto total = [&](int j) {
     double t = 0.0;
     for (auto* x : sums) t += x->k[j];
@@ -475,28 +573,59 @@ Status status(const std::vector<const Sums1*>& sums, const Options& o, double ex
     for (auto* x : sums) t += x->err[j];
     return t;
   };
-  auto scale_of = [](int j) { return j == P1_ABS ? P1_EXT : j; };
+  auto abs_of = [&](int k) {
+    double t = 0.0;
+    for (auto* x : sums) t += x->abs[k];
+    return t;
+  };
+  // C_abs and each direction's derivative of C_abs are refined to rtol of C_ext's.
+  auto scale_of = [&](int j) {
+    if (j == P1_ABS) return P1_EXT;
+    if (j >= n_greek && (j - n_greek) % M_GROUP == M_GROUP - 1) return j + 1 - M_GROUP;
+    return j;
+  };
   const double c_sca = std::fabs(total(P1_SCA));
-  for (int j = 0; j < N_BASE; ++j) {
+  for (int j = 0; j < nr; ++j) {
     double scale;
-    if (j == P1_SCAG)
+    if (j == P1_SCAG) {
       scale = c_sca;
-    else if (j == P1_BACK)
+    } else if (j == P1_BACK) {
       scale = std::max(std::fabs(total(P1_BACK)), c_sca);
-    else
+    } else if (j >= n_greek) {
+      scale = 0.0;
+      for (auto* x : sums) scale += x->absv[scale_of(j)];
+    } else {
       scale = std::fabs(total(scale_of(j)));
+    }
     s.target[j] = o.rtol * scale;
+    for (int b = 0; b < nt; ++b) s.target[(1 + b) * nr + j] = o.rtol * abs_of(b * nr + scale_of(j));
   }
-  s.target[P1_ONE] = INF;
-  if (!o.refine_backscatter) s.target[P1_BACK] = INF;
+  for (int b = 0; b <= nt; ++b) s.target[b * nr + P1_ONE] = INF;
+  for (int b = 1; b <= nt; ++b)
+    for (int j = n_greek; j < nr; ++j) s.target[b * nr + j] = INF;
+  if (!o.refine_backscatter)
+    for (int b = 0; b <= nt; ++b) {
+      s.target[b * nr + P1_BACK] = INF;
+      for (int j = n_greek + 3; j < nr; j += M_GROUP) s.target[b * nr + j] = INF;
+    }
+  s.errors.assign(nb, 0.0);
   s.met = true;
-  for (int j = 0; j < N_BASE; ++j) {
+  for (int j = 0; j < nb; ++j) {
     s.errors[j] = err(j);
     s.met = s.met && s.errors[j] <= s.target[j];
   }
-  auto small = [&](const double* density) {
-    for (int j = 0; j < N_BASE; ++j)
-      if (!(std::fabs(density[j]) * (ext / STEP) <= 0.1 * s.target[j])) return false;
+  std::vector<double> end_target(nb);
+  for (int o2 = 0; o2 < nb; ++o2) {
+    if (o2 < nr || std::isinf(s.target[o2])) {
+      end_target[o2] = s.target[o2];
+    } else {
+      const int b = o2 / nr - 1, j = o2 % nr;
+      end_target[o2] = o.rtol * std::max(std::fabs(total(o2)), 1e-3 * abs_of(b * nr + scale_of(j)));
+    }
+  }
+  auto small = [&](const std::vector<double>& density) {
+    for (int j = 0; j < nb; ++j)
+      if (!(std::fabs(density[j]) * (ext / STEP) <= 0.1 * end_target[j])) return false;
     return true;
   };
   s.small[0] = small(sums.front()->edge[0]);
@@ -584,7 +713,7 @@ Pass1 pass1(const std::vector<const Part*>& group, double lambda, const Optics& 
     for (size_t p = 0; p < np; ++p) {
       std::vector<const Sums1*> sums;
       for (auto& pn : panels) sums.push_back(&pn.sums[p]);
-      statuses.push_back(status(sums, o, exts[p]));
+      statuses.push_back(status(*group[p], sums, o, exts[p]));
     }
     auto finish = [&]() {
       Pass1 r;
@@ -648,7 +777,7 @@ Pass1 pass1(const std::vector<const Part*>& group, double lambda, const Optics& 
       if (!(panels[i].ab.second - panels[i].ab.first > MIN_WIDTH)) continue;
       double bad = 0.0;
       for (size_t p = 0; p < np; ++p)
-        for (int j = 0; j < N_BASE; ++j) {
+        for (size_t j = 0; j < statuses[p].target.size(); ++j) {
           if (!(statuses[p].errors[j] > statuses[p].target[j])) continue;
           const double t = std::max(statuses[p].target[j], std::numeric_limits<double>::min());
           bad = std::max(bad, panels[i].sums[p].err[j] * (double)n / t);
@@ -700,27 +829,59 @@ struct Layout {
   }
 };
 
-// quantities2 (engine.rs:1025-1202) without derivatives: the scalars, the requested cosines'
-// tables (times the area) and the band's tables (fast.rs:95-205) of one solved sphere.
+// quantities2 (engine.rs:1025-1202): the scalars, the requested cosines' tables (times the
+// area) and the band's tables (fast.rs:95-205) of one solved sphere into g; with dm (a sphere
+// solved with derivatives), their derivatives along Re m and Im m into dm[0..len) and
+// dm[len..2 len) (the amplitudes' derivatives dS/dm and i dS/dm; phase.rs:289-341).
 void quantities2(const MieState& st, int64_t n, double r, double lambda, const Layout& L,
-                 const double* mu, int band, int64_t band_terms, double* g) {
+                 const double* mu, int band, int64_t band_terms, double* g,
+                 double* dm = nullptr) {
   const double x = size_param(r, lambda);
   const Efficiencies q = efficiencies(st);
   const double area = PI * r * r;
+  const int64_t len = L.len;
   const double sc[SCALARS] = {1.0,           area * q.q_ext, area * q.q_sca, area * q.q_sca * q.g,
                               area * q.q_abs, area * q.q_back, r * r,         r * r * r,
                               0.0};
   for (int k = 0; k < SCALARS; ++k) g[k] = sc[k];
+  if (dm) {
+    for (int dir = 0; dir < 2; ++dir) {
+      const Efficiencies e = efficiency_dir(st, dir, q);
+      const double sd[SCALARS] = {0.0,
+                                  area * e.q_ext,
+                                  area * e.q_sca,
+                                  area * (e.q_sca * q.g + q.q_sca * e.g),
+                                  area * e.q_abs,
+                                  area * e.q_back,
+                                  0.0,
+                                  0.0,
+                                  0.0};
+      for (int k = 0; k < SCALARS; ++k) dm[dir * len + k] = sd[k];
+    }
+  }
   const double cph = 4.0 / (x * x);
   for (int64_t j = 0; j < L.n_mu; ++j) {
-    cplx s1 = real(0.0), s2 = real(0.0);
+    cplx s1 = real(0.0), s2 = real(0.0), d1 = real(0.0), d2 = real(0.0);
     for_each_order(mu[j], n, [&](int64_t k, double pi, double tau) {
       s1 = s1 + scale(st.a[k - 1], pi) + scale(st.b[k - 1], tau);
       s2 = s2 + scale(st.a[k - 1], tau) + scale(st.b[k - 1], pi);
+      if (dm) {
+        d1 = d1 + scale(st.da_dm[k - 1], pi) + scale(st.db_dm[k - 1], tau);
+        d2 = d2 + scale(st.da_dm[k - 1], tau) + scale(st.db_dm[k - 1], pi);
+      }
     });
     double e[4];
     elements(s1, s2, e);
     for (int t = 0; t < 4; ++t) g[SCALARS + t * L.n_mu + j] = cph * e[t] * area;
+    if (dm) {
+      double fr[4], fi[4];
+      element_derivs(s1, s2, d1, d2, fr);
+      element_derivs(s1, s2, times_i(d1), times_i(d2), fi);
+      for (int t = 0; t < 4; ++t) {
+        dm[SCALARS + t * L.n_mu + j] = area * (cph * fr[t]);
+        dm[len + SCALARS + t * L.n_mu + j] = area * (cph * fi[t]);
+      }
+    }
   }
   if (band < 0) return;
   const BandData& B = L.bands[band];
@@ -729,9 +890,11 @@ void quantities2(const MieState& st, int64_t n, double r, double lambda, const L
   const int64_t terms = std::min(band_terms, B.upper);
   const double scl = 4.0 / (x * x) * (PI * r * r);
   for (int64_t ii = 0; ii < h; ++ii) {
-    double ce[4] = {0, 0, 0, 0}, co[4] = {0, 0, 0, 0};
+    // ce = G_E X and co = G_O X over the sphere's 4 columns and, with derivatives, its 4
+    // derivative columns (fast.rs:98-145).
+    double ce[8] = {0, 0, 0, 0, 0, 0, 0, 0}, co[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     for (int64_t k = 0; k < terms; ++k) {
-      double xr[4] = {0, 0, 0, 0};
+      double xr[8] = {0, 0, 0, 0, 0, 0, 0, 0};
       if (k < n) {
         const cplx uu = (k % 2 == 0) ? st.a[k] : st.b[k];
         const cplx vv = (k % 2 == 0) ? st.b[k] : st.a[k];
@@ -739,20 +902,41 @@ void quantities2(const MieState& st, int64_t n, double r, double lambda, const L
         xr[1] = uu.im;
         xr[2] = vv.re;
         xr[3] = vv.im;
+        if (dm) {
+          const cplx du = (k % 2 == 0) ? st.da_dm[k] : st.db_dm[k];
+          const cplx dv = (k % 2 == 0) ? st.db_dm[k] : st.da_dm[k];
+          xr[4] = du.re;
+          xr[5] = du.im;
+          xr[6] = dv.re;
+          xr[7] = dv.im;
+        }
       }
       const double ge = B.ge[ii * B.upper + k], go = B.go[ii * B.upper + k];
-      for (int t = 0; t < 4; ++t) {
+      for (int t = 0; t < 8; ++t) {
         ce[t] += ge * xr[t];
         co[t] += go * xr[t];
       }
     }
     const cplx eu = C(ce[0], ce[1]), ev = C(ce[2], ce[3]);
     const cplx ou = C(co[0], co[1]), ov = C(co[2], co[3]);
+    const cplx deu = C(ce[4], ce[5]), dev = C(ce[6], ce[7]);
+    const cplx dou = C(co[4], co[5]), dov = C(co[6], co[7]);
     const int64_t jn = lo + ii;
     auto write = [&](int64_t node, double sign) {
+      const cplx s1 = eu + scale(ov, sign), s2 = ev + scale(ou, sign);
       double e[4];
-      elements(eu + scale(ov, sign), ev + scale(ou, sign), e);
+      elements(s1, s2, e);
       for (int t = 0; t < 4; ++t) out[t * qn + node] = scl * e[t];
+      if (dm) {
+        const cplx d1 = deu + scale(dov, sign), d2 = dev + scale(dou, sign);
+        double fr[4], fi[4];
+        element_derivs(s1, s2, d1, d2, fr);
+        element_derivs(s1, s2, times_i(d1), times_i(d2), fi);
+        for (int t = 0; t < 4; ++t) {
+          dm[L.start[band] + t * qn + node] = scl * fr[t];
+          dm[len + L.start[band] + t * qn + node] = scl * fi[t];
+        }
+      }
     };
     write(jn, 1.0);
     const int64_t mirror = qn - 1 - jn;
@@ -773,8 +957,56 @@ struct UnitOut {
   double values[11], errors[11];
   std::vector<double> phase, phase_err;  // 6 x n_mu
   std::vector<double> greek, greek_err;  // 6 x (L + 1)
+  // The derivatives and their error estimates, a block per requested parameter:
+  // [P][11], [P][6 n_mu], [P][6 (L + 1)].
+  std::vector<double> d_values, d_errors, d_phase, d_phase_err, d_greek, d_greek_err;
   bool converged = true;
   int64_t panels = 0;
+};
+
+// A requested parameter (EnsembleParam, ensemble/mod.rs:180-215): its component, its mode (-1:
+// none), its kind and, for a distribution parameter, its index into the distribution's
+// gradient.
+enum ParamKindId { PK_DIST = 0, PK_REFR_REAL = 1, PK_REFR_IMAG = 2, PK_WEIGHT = 3 };
+struct Param {
+  int32_t component, mode, kind, index;
+};
+
+// Lin (lin.rs:7-68): a value, its error estimate, its derivatives and their error estimates.
+struct LinD {
+  double v = 0.0, e = 0.0;
+  std::vector<double> d, de;
+  static LinD constant(double v, size_t n) {
+    LinD x;
+    x.v = v;
+    x.d.assign(n, 0.0);
+    x.de.assign(n, 0.0);
+    return x;
+  }
+  LinD div(const LinD& b) const {
+    LinD o;
+    o.v = v / b.v;
+    o.e = (e + std::fabs(o.v) * b.e) / std::fabs(b.v);
+    const size_t n = d.size();
+    o.d.resize(n);
+    o.de.resize(n);
+    for (size_t k = 0; k < n; ++k) o.d[k] = (d[k] - o.v * b.d[k]) / b.v;
+    for (size_t k = 0; k < n; ++k)
+      o.de[k] = (de[k] + std::fabs(o.v) * b.de[k] + std::fabs(o.d[k]) * b.e +
+                 o.e * std::fabs(b.d[k])) /
+                std::fabs(b.v);
+    return o;
+  }
+  LinD scale(double c) const {
+    LinD o = *this;
+    o.v = c * v;
+    o.e = std::fabs(c) * e;
+    for (size_t k = 0; k < d.size(); ++k) {
+      o.d[k] = c * d[k];
+      o.de[k] = std::fabs(c) * de[k];
+    }
+    return o;
+  }
 };
 
 // The direct path's pass 2, averages and outputs for spheroids (engine.rs:1207-1339 direct_node,
@@ -959,7 +1191,8 @@ std::vector<UnitOut> wavelength(const std::vector<Part>& parts,
                                 const std::vector<std::vector<int>>& groups,
                                 const std::vector<std::vector<int>>& units, double lambda,
                                 int64_t wi, const double* mu, int64_t n_mu, int64_t order,
-                                bool normalized, const Options& o) {
+                                bool normalized, const Options& o,
+                                const std::vector<Param>& params = {}) {
   const int64_t n_wl_all = parts.empty() ? 0 : parts[0].n_wl;
   std::map<double, SpheroidNode> cache;
   auto m_of = [&](int p) {
@@ -1031,27 +1264,58 @@ std::vector<UnitOut> wavelength(const std::vector<Part>& parts,
     }
   }
   const int64_t len = L.len;
-  // Pass 2 and the averages of every part.
-  std::vector<std::vector<double>> av(parts.size()), ae(parts.size());
-  std::vector<double> g(len);
+  // Pass 2 and the averages of every part (engine.rs:1423-1766, 1782-1836): blocks of sums,
+  // the values (weights u r), each requested distribution parameter (du/dtheta r) and, when
+  // the part asks for any derivative along m, Re m and Im m (u r on the nodes' derivatives).
+  const size_t n_cols = params.size();
+  struct Avg {
+    std::vector<double> v, e;
+    std::vector<std::pair<int, std::vector<double>>> d, de;  // (column, array)
+  };
+  std::vector<Avg> avg(parts.size());
+  std::vector<double> g(len), dmv(2 * len);
   MieState st;
+  double grad[3];
   for (size_t gi = 0; gi < groups.size(); ++gi) {
     const auto& grp = groups[gi];
     const Optics m = m_of(grp[0]);
+    bool derivs = false;
+    for (int p : grp) derivs = derivs || parts[p].dir_derivatives();
     if (parts[grp[0]].support == POINT) {
-      const double r = parts[grp[0]].s_a;
+      // monodisperse (engine.rs:1838-1890): the particle itself, exact.
+      const Part& part = parts[grp[0]];
+      if (!part.theta.empty())
+        throw Failure{INVALID_INPUT,
+                      "the derivative along a single radius is not on this path"};
+      const double r = part.s_a;
       int64_t n;
-      solve(r, lambda, m, o.allow_unvalidated, st, &n);
+      solve(r, lambda, m, o.allow_unvalidated, st, &n, derivs);
       std::fill(g.begin(), g.end(), 0.0);
+      std::fill(dmv.begin(), dmv.end(), 0.0);
       const int band = order >= 0 ? L.band_of(n) : -1;
-      quantities2(st, n, r, lambda, L, mu, band, n, g.data());
-      av[grp[0]] = g;
-      ae[grp[0]].assign(len, 0.0);
+      quantities2(st, n, r, lambda, L, mu, band, n, g.data(), derivs ? dmv.data() : nullptr);
+      Avg& a = avg[grp[0]];
+      a.v = g;
+      a.e.assign(len, 0.0);
+      for (int dir = 0; dir < 2; ++dir)
+        if (part.dir_col[dir] >= 0) {
+          a.d.push_back({part.dir_col[dir],
+                         std::vector<double>(dmv.begin() + dir * len,
+                                             dmv.begin() + (dir + 1) * len)});
+          a.de.push_back({part.dir_col[dir], std::vector<double>(len, 0.0)});
+        }
       continue;
     }
     const size_t np = grp.size();
-    std::vector<std::vector<double>> s(np, std::vector<double>(len, 0.0)),
-        e(np, std::vector<double>(len, 0.0));
+    // s[p][blk * len + i], e[p][blk * len + i].
+    std::vector<int> nblk(np);
+    std::vector<std::vector<double>> s(np), e(np);
+    for (size_t p = 0; p < np; ++p) {
+      const Part& part = parts[grp[p]];
+      nblk[p] = 1 + (int)part.theta.size() + (part.dir_derivatives() ? 2 : 0);
+      s[p].assign(nblk[p] * len, 0.0);
+      e[p].assign(nblk[p] * len, 0.0);
+    }
     for (auto& ab : firsts[gi].panels) {
       const int64_t bt = order >= 0 ? panel_terms(ab.first, ab.second, lambda, m,
                                                   o.allow_unvalidated)
@@ -1060,11 +1324,13 @@ std::vector<UnitOut> wavelength(const std::vector<Part>& parts,
       Node nd[15];
       gk_panel(ab.first, ab.second, nd);
       std::vector<std::vector<double>> vals(15, std::vector<double>(len, 0.0));
+      std::vector<std::vector<double>> dvals(derivs ? 15 : 0, std::vector<double>(2 * len, 0.0));
       for (int i = 0; i < 15; ++i) {
         const double r = std::exp(nd[i].t);
         int64_t n;
-        solve(r, lambda, m, o.allow_unvalidated, st, &n);
-        quantities2(st, n, r, lambda, L, mu, band, bt, vals[i].data());
+        solve(r, lambda, m, o.allow_unvalidated, st, &n, derivs);
+        quantities2(st, n, r, lambda, L, mu, band, bt, vals[i].data(),
+                    derivs ? dvals[i].data() : nullptr);
       }
       // The ranges the panel touches: the common part and its band's tables.
       const int64_t common = SCALARS + 4 * n_mu;
@@ -1072,22 +1338,34 @@ std::vector<UnitOut> wavelength(const std::vector<Part>& parts,
       const int64_t b_hi = band >= 0 ? b_lo + 4 * L.bands[band].n_q : 0;
       for (size_t p = 0; p < np; ++p) {
         const Part& part = parts[grp[p]];
-        double wk[15], wg[15];
+        const int nt = (int)part.theta.size();
+        // Kronrod and Gauss weights of each block's rows at the panel's nodes.
+        std::vector<double> wk((1 + nt) * 15), wg((1 + nt) * 15);
         for (int i = 0; i < 15; ++i) {
           const double r = std::exp(nd[i].t);
-          const double u = density_eval(part.den, r, nullptr);
+          const double u = density_eval(part.den, r, grad);
           wk[i] = nd[i].wk * (u * r);
           wg[i] = nd[i].wg * (u * r);
+          for (int b = 0; b < nt; ++b) {
+            const double dw = grad[part.theta[b].second] * r;
+            wk[(1 + b) * 15 + i] = nd[i].wk * dw;
+            wg[(1 + b) * 15 + i] = nd[i].wg * dw;
+          }
         }
         auto add = [&](int64_t a, int64_t b) {
-          for (int64_t idx = a; idx < b; ++idx) {
-            double K = 0.0, G = 0.0;
-            for (int i = 0; i < 15; ++i) {
-              K += wk[i] * vals[i][idx];
-              G += wg[i] * vals[i][idx];
+          for (int blk = 0; blk < nblk[p]; ++blk) {
+            const int row = blk <= nt ? blk : 0;  // the m blocks take the values' weights
+            const int dir = blk - 1 - nt;
+            for (int64_t idx = a; idx < b; ++idx) {
+              double K = 0.0, G = 0.0;
+              for (int i = 0; i < 15; ++i) {
+                const double q = blk <= nt ? vals[i][idx] : dvals[i][dir * len + idx];
+                K += wk[row * 15 + i] * q;
+                G += wg[row * 15 + i] * q;
+              }
+              s[p][blk * len + idx] += K;
+              e[p][blk * len + idx] += std::fabs(K - G);
             }
-            s[p][idx] += K;
-            e[p][idx] += std::fabs(K - G);
           }
         };
         add(0, common);
@@ -1096,109 +1374,232 @@ std::vector<UnitOut> wavelength(const std::vector<Part>& parts,
     }
     for (size_t p = 0; p < np; ++p) {
       const Part& part = parts[grp[p]];
+      const int nt = (int)part.theta.size();
       const double trunc = part.support == UNBOUNDED ? 0.2 * o.rtol : 0.0;
       const double z = part.mom.z, ez = part.mom.ez;
-      std::vector<double> v(len), er(len);
+      Avg& a = avg[grp[p]];
+      a.v.resize(len);
+      a.e.resize(len);
       for (int64_t i = 0; i < len; ++i) {
-        v[i] = s[p][i] / z;
-        er[i] = (e[p][i] + std::fabs(v[i]) * ez) / z + trunc * std::fabs(v[i]);
+        a.v[i] = s[p][i] / z;
+        a.e[i] = (e[p][i] + std::fabs(a.v[i]) * ez) / z + trunc * std::fabs(a.v[i]);
       }
+      for (int b = 0; b < nt; ++b) {
+        const double dz = part.mom.dz[b], edz = part.mom.dez[b];
+        std::vector<double> dv(len), de(len);
+        for (int64_t i = 0; i < len; ++i) {
+          const double sb = s[p][(1 + b) * len + i], eb = e[p][(1 + b) * len + i];
+          dv[i] = (sb - a.v[i] * dz) / z;
+          de[i] = (eb + std::fabs(a.v[i]) * edz + std::fabs(dv[i]) * ez + a.e[i] * std::fabs(dz)) /
+                      z +
+                  trunc * std::fabs(dv[i]);
+        }
+        a.d.push_back({part.theta[b].first, std::move(dv)});
+        a.de.push_back({part.theta[b].first, std::move(de)});
+      }
+      for (int dir = 0; dir < 2; ++dir) {
+        if (part.dir_col[dir] < 0) continue;
+        const int blk = 1 + nt + dir;
+        std::vector<double> dv(len), de(len);
+        for (int64_t i = 0; i < len; ++i) {
+          dv[i] = s[p][blk * len + i] / z;
+          de[i] = (e[p][blk * len + i] + std::fabs(dv[i]) * ez) / z + trunc * std::fabs(dv[i]);
+        }
+        a.d.push_back({part.dir_col[dir], std::move(dv)});
+        a.de.push_back({part.dir_col[dir], std::move(de)});
+      }
+      // <r^2>, <r^3> and their derivatives from the moments (0 along m).
       for (int k = 0; k < 2; ++k) {
-        v[S_R2 + k] = part.mom.v[k];
-        er[S_R2 + k] = part.mom.e[k];
+        a.v[S_R2 + k] = part.mom.v[k];
+        a.e[S_R2 + k] = part.mom.e[k];
+        for (size_t c = 0; c < a.d.size(); ++c) {
+          int b = -1;
+          for (int t = 0; t < nt; ++t)
+            if (part.theta[t].first == a.d[c].first) b = t;
+          a.d[c].second[S_R2 + k] = b >= 0 ? part.mom.d[b][k] : 0.0;
+          a.de[c].second[S_R2 + k] = b >= 0 ? part.mom.de[b][k] : 0.0;
+        }
       }
-      av[grp[p]] = std::move(v);
-      ae[grp[p]] = std::move(er);
     }
   }
-  // Units: the mixture of their parts with their number fractions (engine.rs:2121-2176).
+  // Units: the mixture of their parts with their number fractions and the weight derivatives
+  // (engine.rs:2121-2176).
   std::vector<UnitOut> out;
   for (auto& un : units) {
+    double w_total = 0.0;
+    {
+      std::set<int> comps;
+      for (int p : un)
+        if (comps.insert(parts[p].component).second) w_total += parts[p].w;
+    }
     std::vector<double> v(len, 0.0), e(len, 0.0);
+    std::vector<std::vector<double>> d(n_cols, std::vector<double>(len, 0.0)),
+        de(n_cols, std::vector<double>(len, 0.0));
     for (int p : un) {
       const double f = parts[p].f;
       for (int64_t i = 0; i < len; ++i) {
-        v[i] += f * av[p][i];
-        e[i] += f * ae[p][i];
+        v[i] += f * avg[p].v[i];
+        e[i] += f * avg[p].e[i];
+      }
+      for (size_t c = 0; c < avg[p].d.size(); ++c) {
+        const int col = avg[p].d[c].first;
+        for (int64_t i = 0; i < len; ++i) {
+          d[col][i] += f * avg[p].d[c].second[i];
+          de[col][i] += f * avg[p].de[c].second[i];
+        }
+      }
+    }
+    for (size_t col = 0; col < n_cols; ++col) {
+      const Param& pr = params[col];
+      if (pr.kind != PK_WEIGHT) continue;
+      for (int q : un) {
+        const Part& part = parts[q];
+        const double f = part.w / w_total * part.v / part.v_total;
+        double df;
+        if (pr.mode < 0) {
+          const double own = part.component == pr.component ? part.v / part.v_total : 0.0;
+          df = (own - f) / w_total;
+        } else if (part.component != pr.component) {
+          df = 0.0;
+        } else {
+          const double own = part.mode == pr.mode ? 1.0 : 0.0;
+          df = part.w / w_total * (own - part.v / part.v_total) / part.v_total;
+        }
+        for (int64_t i = 0; i < len; ++i) {
+          d[col][i] += df * avg[q].v[i];
+          de[col][i] += std::fabs(df) * avg[q].e[i];
+        }
       }
     }
     UnitOut u;
-    auto lin = [&](int i) { return Lin{v[i], e[i]}; };
-    Lin ext = lin(S_EXT), sca = lin(S_SCA), scag = lin(S_SCAG), ab = lin(S_ABS),
-        back = lin(S_BACK), r2 = lin(S_R2), r3 = lin(S_R3);
-    for (Lin* l : {&ext, &sca, &back})
+    auto lin = [&](int64_t i) {
+      LinD x;
+      x.v = v[i];
+      x.e = e[i];
+      x.d.resize(n_cols);
+      x.de.resize(n_cols);
+      for (size_t c = 0; c < n_cols; ++c) {
+        x.d[c] = d[c][i];
+        x.de[c] = de[c][i];
+      }
+      return x;
+    };
+    const LinD ext = lin(S_EXT), sca = lin(S_SCA), scag = lin(S_SCAG), ab = lin(S_ABS),
+               back = lin(S_BACK), r2 = lin(S_R2), r3 = lin(S_R3);
+    for (const LinD* l : {&ext, &sca, &back})
       if (!(std::isfinite(l->v) && l->v != 0.0))
         throw Failure{INVALID_INPUT,
                       "a ratio's denominator (<C_ext>, <C_sca> or <C_back>) is 0 or not finite"};
-    const Lin sc[11] = {ext, sca, ab, back, ldiv(sca, ext), ldiv(scag, sca),
-                        lscale(ldiv(ext, back), 4.0 * PI), Lin{0.0, 0.0}, ldiv(r3, r2),
-                        lscale(r2, PI), lscale(r3, 4.0 * PI / 3.0)};
+    const LinD sc[11] = {ext,
+                         sca,
+                         ab,
+                         back,
+                         sca.div(ext),
+                         scag.div(sca),
+                         ext.div(back).scale(4.0 * PI),
+                         LinD::constant(0.0, n_cols),
+                         r3.div(r2),
+                         r2.scale(PI),
+                         r3.scale(4.0 * PI / 3.0)};
+    u.d_values.assign(n_cols * 11, 0.0);
+    u.d_errors.assign(n_cols * 11, 0.0);
     for (int k = 0; k < 11; ++k) {
       u.values[k] = sc[k].v;
       u.errors[k] = sc[k].e;
+      for (size_t c = 0; c < n_cols; ++c) {
+        u.d_values[c * 11 + k] = sc[k].d[c];
+        u.d_errors[c * 11 + k] = sc[k].de[c];
+      }
     }
     if (n_mu > 0) {
       u.phase.assign(6 * n_mu, 0.0);
       u.phase_err.assign(6 * n_mu, 0.0);
+      u.d_phase.assign(n_cols * 6 * n_mu, 0.0);
+      u.d_phase_err.assign(n_cols * 6 * n_mu, 0.0);
       const int src[6] = {0, 1, 0, 2, 3, 2};
       for (int el = 0; el < 6; ++el)
         for (int64_t j = 0; j < n_mu; ++j) {
-          Lin f = lin((int)(SCALARS + src[el] * n_mu + j));
-          if (normalized) f = ldiv(f, sca);
+          LinD f = lin(SCALARS + src[el] * n_mu + j);
+          if (normalized) f = f.div(sca);
           u.phase[el * n_mu + j] = f.v;
           u.phase_err[el * n_mu + j] = f.e;
+          for (size_t c = 0; c < n_cols; ++c) {
+            u.d_phase[(c * 6 + el) * n_mu + j] = f.d[c];
+            u.d_phase_err[(c * 6 + el) * n_mu + j] = f.de[c];
+          }
         }
     }
     if (order >= 0) {
       int64_t top = 0;
       for (auto& B : L.bands) top = std::max(top, std::min(order, 2 * B.upper));
-      std::vector<Lin> gk(6 * (top + 1), Lin{0.0, 0.0});
+      std::vector<LinD> gk(6 * (top + 1), LinD::constant(0.0, n_cols));
+      // project (engine.rs:2310-2355): values and derivatives projected, errors as bounds.
+      auto project = [&](const double* f, const double* fe, const BandData& B, int64_t qn,
+                         int64_t l, double c[6], double cerr[6]) {
+        const int64_t blen = B.order + 1;
+        double pp = 0, mi = 0, ce[4] = {0, 0, 0, 0}, bp = 0, bm = 0;
+        for (int t = 0; t < 6; ++t) c[t] = 0.0;
+        for (int64_t k = 0; k < qn; ++k) {
+          const double d00 = B.dmat[0][k * blen + l], d22 = B.dmat[1][k * blen + l];
+          const double d2m2 = B.dmat[2][k * blen + l], d02 = B.dmat[3][k * blen + l];
+          c[0] += f[k] * d00;
+          c[3] += f[2 * qn + k] * d00;
+          pp += (f[k] + f[2 * qn + k]) * d22;
+          mi += (f[k] - f[2 * qn + k]) * d2m2;
+          c[4] += f[qn + k] * d02;
+          c[5] += f[3 * qn + k] * d02;
+          const double es = fe[k] + fe[2 * qn + k];
+          ce[0] += fe[k] * std::fabs(d00);
+          ce[1] += fe[2 * qn + k] * std::fabs(d00);
+          ce[2] += fe[qn + k] * std::fabs(d02);
+          ce[3] += fe[3 * qn + k] * std::fabs(d02);
+          bp += es * std::fabs(d22);
+          bm += es * std::fabs(d2m2);
+        }
+        c[1] = (pp + mi) * 0.5;
+        c[2] = (pp - mi) * 0.5;
+        const double both = (bp + bm) * 0.5;
+        const double cr[6] = {ce[0], both, both, ce[1], ce[2], ce[3]};
+        for (int t = 0; t < 6; ++t) cerr[t] = cr[t];
+      };
       for (size_t b = 0; b < L.bands.size(); ++b) {
         const BandData& B = L.bands[b];
         const int64_t qn = B.n_q, blen = B.order + 1;
-        const double* f = v.data() + L.start[b];
-        const double* fe = e.data() + L.start[b];
         for (int64_t l = 0; l < blen; ++l) {
-          double c[6] = {0, 0, 0, 0, 0, 0}, pp = 0, mi = 0;
-          double ce[4] = {0, 0, 0, 0}, bp = 0, bm = 0;
-          for (int64_t k = 0; k < qn; ++k) {
-            const double d00 = B.dmat[0][k * blen + l], d22 = B.dmat[1][k * blen + l];
-            const double d2m2 = B.dmat[2][k * blen + l], d02 = B.dmat[3][k * blen + l];
-            c[0] += f[k] * d00;
-            c[3] += f[2 * qn + k] * d00;
-            pp += (f[k] + f[2 * qn + k]) * d22;
-            mi += (f[k] - f[2 * qn + k]) * d2m2;
-            c[4] += f[qn + k] * d02;
-            c[5] += f[3 * qn + k] * d02;
-            const double es = fe[k] + fe[2 * qn + k];
-            ce[0] += fe[k] * std::fabs(d00);
-            ce[1] += fe[2 * qn + k] * std::fabs(d00);
-            ce[2] += fe[qn + k] * std::fabs(d02);
-            ce[3] += fe[3 * qn + k] * std::fabs(d02);
-            bp += es * std::fabs(d22);
-            bm += es * std::fabs(d2m2);
-          }
-          c[1] = (pp + mi) * 0.5;
-          c[2] = (pp - mi) * 0.5;
-          const double both = (bp + bm) * 0.5;
-          const double cerr[6] = {ce[0], both, both, ce[1], ce[2], ce[3]};
+          double c[6], cerr[6];
+          project(v.data() + L.start[b], e.data() + L.start[b], B, qn, l, c, cerr);
           for (int el = 0; el < 6; ++el) {
             gk[el * (top + 1) + l].v += c[el];
             gk[el * (top + 1) + l].e += cerr[el];
           }
+          for (size_t col = 0; col < n_cols; ++col) {
+            project(d[col].data() + L.start[b], de[col].data() + L.start[b], B, qn, l, c, cerr);
+            for (int el = 0; el < 6; ++el) {
+              gk[el * (top + 1) + l].d[col] += c[el];
+              gk[el * (top + 1) + l].de[col] += cerr[el];
+            }
+          }
         }
       }
       if (normalized) {
-        const Lin a0 = gk[0];
-        for (auto& x : gk) x = ldiv(x, a0);
-        gk[0] = Lin{1.0, 0.0};
+        const LinD a0 = gk[0];
+        for (auto& x : gk) x = x.div(a0);
+        gk[0] = LinD::constant(1.0, n_cols);
       }
-      u.greek.assign(6 * (order + 1), 0.0);
-      u.greek_err.assign(6 * (order + 1), 0.0);
+      const int64_t glen = order + 1;
+      u.greek.assign(6 * glen, 0.0);
+      u.greek_err.assign(6 * glen, 0.0);
+      u.d_greek.assign(n_cols * 6 * glen, 0.0);
+      u.d_greek_err.assign(n_cols * 6 * glen, 0.0);
       for (int el = 0; el < 6; ++el)
         for (int64_t l = 0; l <= std::min(top, order); ++l) {
-          u.greek[el * (order + 1) + l] = gk[el * (top + 1) + l].v;
-          u.greek_err[el * (order + 1) + l] = gk[el * (top + 1) + l].e;
+          const LinD& x = gk[el * (top + 1) + l];
+          u.greek[el * glen + l] = x.v;
+          u.greek_err[el * glen + l] = x.e;
+          for (size_t c = 0; c < n_cols; ++c) {
+            u.d_greek[(c * 6 + el) * glen + l] = x.d[c];
+            u.d_greek_err[(c * 6 + el) * glen + l] = x.de[c];
+          }
         }
     }
     std::set<int> ug;
@@ -1365,6 +1766,137 @@ int orc_ensemble_adaptive_spheroid(const FixedDist* dists, int64_t n_dist, int b
                        greek_order, normalized, rtol, max_panels, allow_unvalidated,
                        refine_backscatter, n_threads, values, errors, phase, phase_err, greek,
                        greek_err, converged, panels, err, err_len, eps);
+}
+
+// The adaptive ensemble of a mixture with the derivatives along `params` (n_params of them,
+// each {component, mode (-1 none), kind (0 distribution parameter by gradient index, 1 Re m,
+// 2 Im m, 3 weight), index}): compute_mixture (ensemble/mod.rs:609-625) with
+// EnsembleOptions::derivatives. Components as orc_ensemble_mixture, multimodal[c] != 0 when
+// component c is a multimodal distribution (its parameters then carry a mode). Outputs per
+// wavelength as orc_ensemble_mixture, and d_values, d_errors (P, 11, n_wl), d_phase,
+// d_phase_err (P, 6, n_wl, n_mu), d_greek, d_greek_err (P, 6, n_wl, L + 1).
+int orc_ensemble_mixture_d(const FixedDist* modes, const double* mode_w, const int32_t* n_modes,
+                           const int32_t* multimodal, const double* w, const double* m,
+                           int64_t n_comp, const double* wl, int64_t n_wl, const double* mu,
+                           int64_t n_mu, int64_t greek_order, int normalized, double rtol,
+                           int64_t max_panels, int allow_unvalidated, int refine_backscatter,
+                           const Param* params, int64_t n_params, double* values,
+                           double* errors, double* phase, double* phase_err, double* greek,
+                           double* greek_err, double* d_values, double* d_errors,
+                           double* d_phase, double* d_phase_err, double* d_greek,
+                           double* d_greek_err, int8_t* converged, int64_t* panels, char* err,
+                           int64_t err_len) {
+  Options o{rtol, (size_t)max_panels, allow_unvalidated != 0, refine_backscatter != 0};
+  auto fail = [&](const Failure& f) {
+    if (err && err_len > 0) snprintf(err, err_len, "%s", f.msg.c_str());
+    return f.status;
+  };
+  if (!(rtol >= 1e-13 && rtol <= 0.1)) return fail({INVALID_INPUT, "rtol must be in [1e-13, 0.1]"});
+  std::vector<Param> ps(params, params + n_params);
+  for (int64_t k = 0; k < n_params; ++k)
+    for (int64_t j = 0; j < k; ++j)
+      if (ps[j].component == ps[k].component && ps[j].mode == ps[k].mode &&
+          ps[j].kind == ps[k].kind && ps[j].index == ps[k].index)
+        return fail({INVALID_INPUT, "a parameter is requested twice"});
+  double w_total = 0.0;
+  for (int64_t c = 0; c < n_comp; ++c) w_total += w[c];
+  std::vector<Part> parts;
+  std::vector<int> unit;
+  try {
+    int64_t k = 0;
+    for (int64_t c = 0; c < n_comp; ++c) {
+      double v_total = 0.0;
+      for (int j = 0; j < n_modes[c]; ++j) v_total += multimodal[c] ? mode_w[k + j] : 1.0;
+      for (int j = 0; j < n_modes[c]; ++j) {
+        const int mode = multimodal[c] ? j : -1;
+        // engine.rs:153-176: the part's parameters.
+        std::vector<std::pair<int, int>> theta;
+        int dir_col[2] = {-1, -1};
+        std::vector<int> grads;
+        for (int64_t col = 0; col < n_params; ++col) {
+          const Param& pr = ps[col];
+          if (pr.component != c) continue;
+          if (pr.kind == PK_DIST && pr.mode == mode) {
+            theta.push_back({(int)col, pr.index});
+            grads.push_back(pr.index);
+          } else if (pr.kind == PK_REFR_REAL) {
+            dir_col[0] = (int)col;
+          } else if (pr.kind == PK_REFR_IMAG) {
+            dir_col[1] = (int)col;
+          }
+        }
+        const double v = multimodal[c] ? mode_w[k + j] : 1.0;
+        parts.push_back(make_part(modes[k + j], rtol, grads));
+        Part& pt = parts.back();
+        pt.m = m + 2 * n_wl * c;
+        pt.n_wl = n_wl;
+        pt.f = w[c] / w_total * v / v_total;
+        pt.component = (int)c;
+        pt.mode = mode;
+        pt.w = w[c];
+        pt.v = v;
+        pt.v_total = v_total;
+        pt.theta = theta;
+        pt.dir_col[0] = dir_col[0];
+        pt.dir_col[1] = dir_col[1];
+        unit.push_back((int)parts.size() - 1);
+      }
+      k += n_modes[c];
+    }
+  } catch (const Failure& f) {
+    return fail(f);
+  }
+  std::vector<std::vector<int>> groups;
+  for (size_t p = 0; p < parts.size(); ++p) groups.push_back({(int)p});
+  std::vector<std::vector<int>> units{unit};
+  const int64_t glen = greek_order >= 0 ? greek_order + 1 : 0;
+  const int64_t P = n_params;
+  std::vector<Failure> fails(n_wl, Failure{OK, ""});
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int64_t i = 0; i < n_wl; ++i) {
+    try {
+      auto res = wavelength(parts, groups, units, wl[i], i, mu, n_mu, greek_order,
+                            normalized != 0, o, ps);
+      const UnitOut& u = res[0];
+      for (int q = 0; q < 11; ++q) {
+        values[q * n_wl + i] = u.values[q];
+        errors[q * n_wl + i] = u.errors[q];
+        for (int64_t c = 0; c < P; ++c) {
+          d_values[(c * 11 + q) * n_wl + i] = u.d_values[c * 11 + q];
+          d_errors[(c * 11 + q) * n_wl + i] = u.d_errors[c * 11 + q];
+        }
+      }
+      if (phase && n_mu > 0)
+        for (int el = 0; el < 6; ++el)
+          for (int64_t j = 0; j < n_mu; ++j) {
+            phase[(el * n_wl + i) * n_mu + j] = u.phase[el * n_mu + j];
+            phase_err[(el * n_wl + i) * n_mu + j] = u.phase_err[el * n_mu + j];
+            for (int64_t c = 0; c < P; ++c) {
+              d_phase[((c * 6 + el) * n_wl + i) * n_mu + j] = u.d_phase[(c * 6 + el) * n_mu + j];
+              d_phase_err[((c * 6 + el) * n_wl + i) * n_mu + j] =
+                  u.d_phase_err[(c * 6 + el) * n_mu + j];
+            }
+          }
+      if (greek && glen > 0)
+        for (int el = 0; el < 6; ++el)
+          for (int64_t l = 0; l < glen; ++l) {
+            greek[(el * n_wl + i) * glen + l] = u.greek[el * glen + l];
+            greek_err[(el * n_wl + i) * glen + l] = u.greek_err[el * glen + l];
+            for (int64_t c = 0; c < P; ++c) {
+              d_greek[((c * 6 + el) * n_wl + i) * glen + l] = u.d_greek[(c * 6 + el) * glen + l];
+              d_greek_err[((c * 6 + el) * n_wl + i) * glen + l] =
+                  u.d_greek_err[(c * 6 + el) * glen + l];
+            }
+          }
+      converged[i] = u.converged ? 1 : 0;
+      panels[i] = u.panels;
+    } catch (const Failure& f) {
+      fails[i] = f;
+    }
+  }
+  for (int64_t i = 0; i < n_wl; ++i)
+    if (fails[i].status != OK) return fail(fails[i]);
+  return OK;
 }
 
 // The adaptive ensemble of a mixture (compute_mixture, ensemble/mod.rs:609-625): n_comp

@@ -216,16 +216,6 @@ static LinV lin_scale(const LinV& a, double c) {
 }
 
 // element_derivatives (mie/phase.rs:62-73).
-static void element_derivs(cplx s1, cplx s2, cplx d1, cplx d2, double out[4]) {
-  double r1 = (conj(s1) * d1).re;
-  double r2 = (conj(s2) * d2).re;
-  cplx p = d2 * conj(s1) + s2 * conj(d1);
-  out[0] = r1 + r2;
-  out[1] = r2 - r1;
-  out[2] = p.re;
-  out[3] = p.im;
-}
-
 static int theta_count(int kind) {
   return kind == MODIFIED_GAMMA ? 3 : kind == POWER_LAW ? 1 : kind == TABULATED ? 0 : 2;
 }
@@ -372,35 +362,11 @@ static int ensemble_impl(const FixedDist* dists, int64_t n_dist, const double* w
         if (derivs) {
           // derivative_sums (efficiencies.rs:89-146) along Re m and Im m, and
           // efficiencies_jacobian (192-230) for those directions.
-          Sums vs = value_sums(st.a.data(), st.b.data(), n);
           for (int p = 0; p < 2; ++p) {
-            double sca = 0.0, g = 0.0;
-            cplx back = real(0.0);
-            auto dA = [&](int64_t i2) { return p == 0 ? st.da_dm[i2] : times_i(st.da_dm[i2]); };
-            auto dB = [&](int64_t i2) { return p == 0 ? st.db_dm[i2] : times_i(st.db_dm[i2]); };
-            for (int64_t k = 1; k <= n; ++k) {
-              cplx ak = st.a[k - 1], bk = st.b[k - 1], dak = dA(k - 1), dbk = dB(k - 1);
-              double w = (double)(2 * k + 1), kf = (double)k;
-              double pair = kf * (kf + 2.0) / (kf + 1.0);
-              double own = w / (kf * (kf + 1.0));
-              sca += w * 2.0 * (re_mul_conj(dak, ak) + re_mul_conj(dbk, bk));
-              cplx t = scale(dak - dbk, w);
-              back = (k % 2 == 0) ? back + t : back - t;
-              if (k < n) {
-                cplx a1 = st.a[k], b1 = st.b[k], da1 = dA(k), db1 = dB(k);
-                g += pair * (re_mul_conj(dak, a1) + re_mul_conj(ak, da1) + re_mul_conj(dbk, b1) +
-                             re_mul_conj(bk, db1));
-              }
-              g += own * (re_mul_conj(dak, bk) + re_mul_conj(ak, dbk));
-            }
-            double inv_x = 1.0 / x, inv_x2 = inv_x * inv_x, two_x2 = 2.0 * inv_x2;
-            double dsca = two_x2 * sca;
-            double dabs = two_x2 * st.abs_sum_jacobian[1 + p];
-            double dback = 2.0 * re_mul_conj(back, vs.back) * inv_x2;
-            double dg = vs.sca == 0.0 ? 0.0 : (2.0 * g - q.g * sca) / vs.sca;
-            double dext = dsca + dabs;
-            double qd[8] = {0.0,          area * dext, area * dsca, area * (dsca * q.g + q.q_sca * dg),
-                            area * dabs, area * dback, 0.0,        0.0};
+            const Efficiencies de = efficiency_dir(st, p, q);
+            double qd[8] = {0.0,          area * de.q_ext, area * de.q_sca,
+                            area * (de.q_sca * q.g + q.q_sca * de.g),
+                            area * de.q_abs, area * de.q_back, 0.0,        0.0};
             for (int k = 0; k < 8; ++k) qb[1 + P_th + p][k] = qd[k];
           }
         }

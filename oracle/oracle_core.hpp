@@ -608,6 +608,39 @@ inline Efficiencies efficiencies(const MieState& st) {
   return efficiencies_from(st.x, st.abs_sum, value_sums(st.a.data(), st.b.data(), st.a.size()));
 }
 
+// The efficiencies' derivatives along direction p (0: Re m, 1: Im m, with d/d(Im m) = i d/dm)
+// of a sphere solved with derivatives: derivative_sums (efficiencies.rs:89-146) and
+// efficiencies_jacobian (192-230). q are the sphere's efficiencies.
+inline Efficiencies efficiency_dir(const MieState& st, int p, const Efficiencies& q) {
+  const int64_t n = (int64_t)st.a.size();
+  const Sums vs = value_sums(st.a.data(), st.b.data(), n);
+  double sca = 0.0, g = 0.0;
+  cplx back = real(0.0);
+  auto dA = [&](int64_t i) { return p == 0 ? st.da_dm[i] : times_i(st.da_dm[i]); };
+  auto dB = [&](int64_t i) { return p == 0 ? st.db_dm[i] : times_i(st.db_dm[i]); };
+  for (int64_t k = 1; k <= n; ++k) {
+    const cplx ak = st.a[k - 1], bk = st.b[k - 1], dak = dA(k - 1), dbk = dB(k - 1);
+    const double w = (double)(2 * k + 1), kf = (double)k;
+    const double pair = kf * (kf + 2.0) / (kf + 1.0);
+    const double own = w / (kf * (kf + 1.0));
+    sca += w * 2.0 * (re_mul_conj(dak, ak) + re_mul_conj(dbk, bk));
+    const cplx t = scale(dak - dbk, w);
+    back = (k % 2 == 0) ? back + t : back - t;
+    if (k < n) {
+      const cplx a1 = st.a[k], b1 = st.b[k], da1 = dA(k), db1 = dB(k);
+      g += pair * (re_mul_conj(dak, a1) + re_mul_conj(ak, da1) + re_mul_conj(dbk, b1) +
+                   re_mul_conj(bk, db1));
+    }
+    g += own * (re_mul_conj(dak, bk) + re_mul_conj(ak, dbk));
+  }
+  const double inv_x = 1.0 / st.x, inv_x2 = inv_x * inv_x, two_x2 = 2.0 * inv_x2;
+  const double dsca = two_x2 * sca;
+  const double dabs = two_x2 * st.abs_sum_jacobian[1 + p];
+  const double dback = 2.0 * re_mul_conj(back, vs.back) * inv_x2;
+  const double dg = vs.sca == 0.0 ? 0.0 : (2.0 * g - q.g * sca) / vs.sca;
+  return {dsca + dabs, dsca, dabs, dback, dg};
+}
+
 // ---------------------------------------------------------------------------------------
 // Angular functions, amplitudes and the phase matrix (mie/amplitudes.rs:52-65, 328-344;
 // mie/phase.rs:54-59, 151-158, 204-219).
@@ -645,6 +678,18 @@ inline void elements(cplx s1, cplx s2, double out[4]) {
   cplx p = s2 * conj(s1);
   out[0] = 0.5 * (n1 + n2);
   out[1] = 0.5 * (n2 - n1);
+  out[2] = p.re;
+  out[3] = p.im;
+}
+
+// element_derivatives (phase.rs:62-73): the elements' derivatives for amplitude derivatives
+// (d1, d2).
+inline void element_derivs(cplx s1, cplx s2, cplx d1, cplx d2, double out[4]) {
+  double r1 = (conj(s1) * d1).re;
+  double r2 = (conj(s2) * d2).re;
+  cplx p = d2 * conj(s1) + s2 * conj(d1);
+  out[0] = r1 + r2;
+  out[1] = r2 - r1;
   out[2] = p.re;
   out[3] = p.im;
 }

@@ -124,6 +124,9 @@ SYMBOLS = {
     "scatrs_ensemble_mixture": (ctypes.c_int, [ctypes.POINTER(Component), _I64, _PD, _I64, _PD,
                                                _I64, ctypes.POINTER(AdaptiveOptions), _PD, _PD,
                                                _PD, _PD, _PD, _PD, _VP, _VP, _CP, _SZ]),
+    "scatrs_ensemble_mixture_d": (ctypes.c_int, [ctypes.POINTER(Component), _I64, _PD, _I64, _PD,
+                                                 _I64, ctypes.POINTER(AdaptiveOptions), _VP, _I64]
+                                  + [_PD] * 12 + [_VP, _VP, _CP, _SZ]),
     "scatrs_project_greek_device": (ctypes.c_int, [_VP, _I64, _I64, _I32, _I32, _VP, _VP, _CP,
                                                    _SZ]),
     "scatrs_spheroid_tmatrix": (ctypes.c_int, [_D, _D, _PD, _I32, _I32, _I32, _PD, _CP, _SZ]),
@@ -484,6 +487,62 @@ def ensemble_mixture(components, wavelengths, mu=None, greek_order: int = -1,
         out["phase"], out["phase_err"] = ph, pe
     if g is not None:
         out["greek"], out["greek_err"] = g, ge
+    return out
+
+
+# scatrs_param: (component, mode or -1, kind, index); kinds as SCATRS_PARAM_*.
+PARAM_DTYPE = np.dtype([("component", np.int32), ("mode", np.int32), ("kind", np.int32),
+                        ("index", np.int32)])
+PARAM_DISTRIBUTION, PARAM_REFR_REAL, PARAM_REFR_IMAG, PARAM_WEIGHT = 0, 1, 2, 3
+
+
+def ensemble_mixture_d(components, wavelengths, params, mu=None, greek_order: int = -1,
+                       normalized: bool = True, rtol: float = 1e-6, max_panels: int = 4096,
+                       allow_unvalidated: bool = False, refine_backscatter: bool = False) -> dict:
+    """ensemble_mixture with the derivatives along `params` (PARAM_DTYPE records); a component
+    whose mode weights are given is multimodal. Adds d, d_err (P, 11, n), and with phase or
+    Greek coefficients phase_d, phase_d_err (P, 6, n, n_mu), greek_d, greek_d_err
+    (P, 6, n, L + 1)."""
+    require_device()
+    wl = np.ascontiguousarray(wavelengths, dtype=np.float64).reshape(-1)
+    keep = []
+    comps = (Component * max(len(components), 1))()
+    for k, (dists, mode_w, weight, m) in enumerate(components):
+        d = np.ascontiguousarray(np.atleast_1d(dists), dtype=DIST_DTYPE)
+        mw = None if mode_w is None else np.ascontiguousarray(mode_w, dtype=np.float64)
+        mm = np.ascontiguousarray(np.broadcast_to(np.asarray(m, dtype=np.complex128), wl.shape))
+        keep += [d, mw, mm]
+        comps[k] = Component(d.ctypes.data, _p(mw), d.size, 0, float(weight),
+                             _p(mm.view(np.float64)))
+    pr = np.ascontiguousarray(np.atleast_1d(np.asarray(params, dtype=PARAM_DTYPE)))
+    P = pr.size
+    mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
+    n = wl.size
+    L = int(greek_order)
+    opts = AdaptiveOptions(float(rtol), int(max_panels), L, int(normalized),
+                           int(allow_unvalidated), int(refine_backscatter))
+    out = {"values": np.zeros((11, n)), "errors": np.zeros((11, n)),
+           "d": np.zeros((P, 11, n)), "d_err": np.zeros((P, 11, n)),
+           "converged": np.zeros(n, dtype=np.int8), "panels": np.zeros(n, dtype=np.int64)}
+    ph = pe = g = ge = dph = dpe = dg = dge = None
+    if mu.size:
+        ph, pe = np.zeros((6, n, mu.size)), np.zeros((6, n, mu.size))
+        dph, dpe = np.zeros((P, 6, n, mu.size)), np.zeros((P, 6, n, mu.size))
+    if L >= 0:
+        g, ge = np.zeros((6, n, L + 1)), np.zeros((6, n, L + 1))
+        dg, dge = np.zeros((P, 6, n, L + 1)), np.zeros((P, 6, n, L + 1))
+    err = ctypes.create_string_buffer(1024)
+    st = load().scatrs_ensemble_mixture_d(
+        comps, len(components), _p(wl), wl.size, _p(mu), mu.size, ctypes.byref(opts),
+        pr.ctypes.data if P else None, P, _p(out["values"]), _p(out["errors"]), _p(out["d"]),
+        _p(out["d_err"]), _p(ph), _p(pe), _p(dph), _p(dpe), _p(g), _p(ge), _p(dg), _p(dge),
+        out["converged"].ctypes.data, out["panels"].ctypes.data, err, 1024)
+    _check(st, err)
+    out["converged"] = out["converged"].astype(bool)
+    if ph is not None:
+        out["phase"], out["phase_err"], out["phase_d"], out["phase_d_err"] = ph, pe, dph, dpe
+    if g is not None:
+        out["greek"], out["greek_err"], out["greek_d"], out["greek_d_err"] = g, ge, dg, dge
     return out
 
 

@@ -79,6 +79,32 @@ def ensemble_parameters(items, mixture: bool) -> list[str]:
     return out
 
 
+def _parameter_records(items, mixture: bool) -> list:
+    """The (component, mode, kind, index) of every name of ensemble_parameters, in its order
+    (scatrs/src/ensemble/mod.rs:254-337); kind None marks a parameter of a layered sphere or a
+    spheroid, which this path does not differentiate."""
+    out = []
+    for ci, (spec, particle, _w) in enumerate(items):
+        kind = spec[0]
+        if kind == "multimodal":
+            for j, (_v, mode) in enumerate(spec[1]):
+                out += [(ci, j, _native.PARAM_DISTRIBUTION, k) for k in range(len(_PARAMS[mode[0]]))]
+                out.append((ci, j, _native.PARAM_WEIGHT, 0))
+        else:
+            out += [(ci, -1, _native.PARAM_DISTRIBUTION, k) for k in range(len(_PARAMS[kind]))]
+        pk = particle[0]
+        if pk == "sphere":
+            out += [(ci, -1, _native.PARAM_REFR_REAL, 0), (ci, -1, _native.PARAM_REFR_IMAG, 0)]
+        elif pk == "spheroid":
+            out += [(ci, -1, None, k) for k in range(3)]
+        else:
+            layers = np.asarray(particle[2]).shape[0]
+            out += [(ci, -1, None, k) for k in range(3 * layers - 1)]
+        if mixture:
+            out.append((ci, -1, _native.PARAM_WEIGHT, 0))
+    return out
+
+
 def _dist_array(specs, spread: float, ranges=None) -> np.ndarray:
     d = _native.dist_records(len(specs))
     for k, spec in enumerate(specs):
@@ -199,9 +225,11 @@ def ensemble_compute(items, wavelengths, mixture, greek, all_orders, mu, normali
     (a mixture), each a distribution or a multimodal one, one output per wavelength."""
     if not items:
         raise InvalidInputError("a mixture needs a component")
-    if list(derivatives):
-        raise InvalidInputError(
-            "derivatives of the adaptive ensemble are not on the GPU path: use the fixed grid")
+    derivatives = [int(i) for i in derivatives]
+    if derivatives:
+        return _compute_with_derivatives(items, wavelengths, mixture, greek, all_orders, mu,
+                                         normalized, derivatives, rtol, max_panels,
+                                         allow_unvalidated, refine_backscatter)
     if all_orders:
         raise InvalidInputError("greek='all' is not on the GPU path: give an order")
     wl = np.ascontiguousarray(wavelengths, dtype=np.float64).reshape(-1)
@@ -236,6 +264,52 @@ def ensemble_compute(items, wavelengths, mixture, greek, all_orders, mu, normali
                                    bool(normalized), float(rtol), int(max_panels),
                                    bool(allow_unvalidated), bool(refine_backscatter))
     return _adaptive_dict(out, mu.size, 0)
+
+
+def _compute_with_derivatives(items, wavelengths, mixture, greek, all_orders, mu, normalized,
+                              derivatives, rtol, max_panels, allow_unvalidated,
+                              refine_backscatter) -> dict:
+    """ensemble_compute with derivatives (scatrs-py/src/ensemble.rs:318-349): the parameters by
+    their index in ensemble_parameters, every one once; spheres, through
+    scatrs_ensemble_mixture_d (compute_mixture with EnsembleOptions::derivatives)."""
+    names = ensemble_parameters(items, mixture)
+    records = _parameter_records(items, mixture)
+    chosen = []
+    for i in derivatives:
+        if not 0 <= i < len(records):
+            raise InvalidInputError(f"no parameter {i}")
+        if i in chosen:
+            raise InvalidInputError(f"parameter {names[i]} requested twice")
+        chosen.append(i)
+    for i in chosen:
+        if records[i][2] is None:
+            raise InvalidInputError(
+                f"the derivative along {names[i]} (a layered sphere's or a spheroid's) is not "
+                "on the adaptive GPU path: use the fixed grid")
+    if all_orders:
+        raise InvalidInputError("greek='all' is not on the GPU path: give an order")
+    wl = np.ascontiguousarray(wavelengths, dtype=np.float64).reshape(-1)
+    mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
+    L = -1 if greek is None else int(greek)
+    comps = []
+    for spec, particle, weight in items:
+        dists, mode_w = _modes(spec)
+        comps.append((dists, mode_w, float(weight), _sphere_m(particle, wl.size)))
+    params = np.array([records[i] for i in chosen], dtype=_native.PARAM_DTYPE)
+    out = _native.ensemble_mixture_d(comps, wl, params, mu, L, bool(normalized), float(rtol),
+                                     int(max_panels), bool(allow_unvalidated),
+                                     bool(refine_backscatter))
+    raw = {"values": out["values"], "errors": out["errors"], "d": out["d"],
+           "d_errors": out["d_err"]}
+    for prefix in ("greek", "phase"):
+        if prefix in out:
+            raw[prefix] = out[prefix]
+            raw[f"{prefix}_errors"] = out[f"{prefix}_err"]
+            raw[f"{prefix}_d"] = out[f"{prefix}_d"]
+            raw[f"{prefix}_d_errors"] = out[f"{prefix}_d_err"]
+    raw["converged"] = out["converged"]
+    raw["panels"] = out["panels"].astype(np.uint64)
+    return raw
 
 
 def ensemble_compute_batch(specs, particle_spec, wavelengths, greek, all_orders, mu, normalized,

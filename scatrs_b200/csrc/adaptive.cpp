@@ -89,12 +89,16 @@ std::pair<double, double> cutoffs(const Part& p, double center, double eps,
   throw Error{1, buf};
 }
 
-// moments.rs:62-167 without derivative parameters: GK15 panels of at most max_step, split
-// where their |Kronrod - Gauss| is above their share, until Z, <r^2 u>, <r^3 u> meet rtol.
+// moments.rs:62-167: GK15 panels of at most max_step (the breaks inside the range as edges),
+// split where a sum's |Kronrod - Gauss| is above its share, until Z, <r^2 u>, <r^3 u> and,
+// along each requested parameter, their derivatives meet rtol (the derivatives of their
+// absolute integrands' Kronrod sums); then the quotient rule with first-order error
+// propagation (moments.rs:171-212).
 Moments moments(const Part& p, double lo, double hi, double rtol, double truncation,
                 const std::vector<double>& breaks = {}) {
   const double step = max_step(p, kStep);
   const double t_lo = std::log(lo), t_hi = std::log(hi);
+  const int nt = (int)p.grads.size(), nq = 3 * (1 + nt);
   std::vector<std::pair<double, double>> panels;
   {
     // The breaks inside the range are panel edges; each interval in equal panels of at most
@@ -112,14 +116,7 @@ Moments moments(const Part& p, double lo, double hi, double rtol, double truncat
       for (size_t i = 0; i < n; ++i) panels.push_back({a + i * h, a + (i + 1) * h});
     }
   }
-  std::vector<double> sums;  // per panel: K0, K2, K3, |K-G| x 3
-  auto result = [&]() {
-    double s[3] = {0, 0, 0}, e[3] = {0, 0, 0};
-    for (int j = 0; j < 3; ++j)
-      for (size_t i = 0; i < panels.size(); ++i) {
-        s[j] += sums[6 * i + j];
-        e[j] += sums[6 * i + 3 + j];
-      }
+  auto result = [&](const std::vector<double>& s, const std::vector<double>& e) {
     if (!(std::isfinite(s[0]) && s[0] > 0.0)) {
       char buf[128];
       snprintf(buf, sizeof buf,
@@ -133,45 +130,72 @@ Moments moments(const Part& p, double lo, double hi, double rtol, double truncat
       m.v[k] = s[1 + k] / m.z;
       m.e[k] = (e[1 + k] + std::fabs(m.v[k]) * m.ez) / m.z + truncation * std::fabs(m.v[k]);
     }
+    for (int b = 0; b < nt; ++b) {
+      const int o = 3 * (1 + b);
+      const double dz = s[o];
+      std::array<double, 2> dv, dev;
+      for (int k = 0; k < 2; ++k) dv[k] = (s[o + 1 + k] - m.v[k] * dz) / m.z;
+      for (int k = 0; k < 2; ++k)
+        dev[k] = (e[o + 1 + k] + std::fabs(m.v[k]) * e[o] + std::fabs(dv[k]) * m.ez +
+                  m.e[k] * std::fabs(dz)) / m.z +
+                 truncation * std::fabs(dv[k]);
+      m.d.push_back(dv);
+      m.de.push_back(dev);
+      m.dz.push_back(dz);
+      m.dez.push_back(e[o]);
+    }
     return m;
   };
+  double grad[3];
   for (;;) {
-    sums.assign(6 * panels.size(), 0.0);
-    for (size_t i = 0; i < panels.size(); ++i) {
+    // Per panel (moments.rs:31-53): Kronrod sums, |K - G| and the Kronrod sums of the
+    // absolute derivative integrands.
+    const size_t n = panels.size();
+    std::vector<double> K(n * nq, 0.0), E(n * nq, 0.0), A(n * nq, 0.0), g(nq);
+    for (size_t i = 0; i < n; ++i) {
       Node nd[15];
       gk15(panels[i].first, panels[i].second, nd);
-      double k[3] = {0, 0, 0}, g[3] = {0, 0, 0};
-      for (const Node& n : nd) {
-        const double r = std::exp(n.t), u = p.u(r);
+      std::fill(g.begin(), g.end(), 0.0);
+      for (const Node& x : nd) {
+        const double r = std::exp(x.t), u = nt > 0 ? p.u(r, grad) : p.u(r);
         const double q[3] = {1.0, r * r, r * r * r};
         for (int j = 0; j < 3; ++j) {
-          k[j] += n.wk * u * r * q[j];
-          g[j] += n.wg * u * r * q[j];
+          K[i * nq + j] += x.wk * u * r * q[j];
+          g[j] += x.wg * u * r * q[j];
+          for (int b = 0; b < nt; ++b) {
+            const int o = 3 * (1 + b) + j;
+            const double y = grad[p.grads[b]] * r * q[j];
+            K[i * nq + o] += x.wk * y;
+            g[o] += x.wg * y;
+            A[i * nq + o] += x.wk * std::fabs(y);
+          }
         }
       }
-      for (int j = 0; j < 3; ++j) {
-        sums[6 * i + j] = k[j];
-        sums[6 * i + 3 + j] = std::fabs(k[j] - g[j]);
+      for (int j = 0; j < nq; ++j) E[i * nq + j] = std::fabs(K[i * nq + j] - g[j]);
+    }
+    std::vector<double> total(nq, 0.0), terr(nq, 0.0), target(nq, 0.0);
+    for (size_t i = 0; i < n; ++i)
+      for (int j = 0; j < nq; ++j) {
+        total[j] += K[i * nq + j];
+        terr[j] += E[i * nq + j];
+      }
+    for (int j = 0; j < nq; ++j) {
+      if (j < 3) {
+        target[j] = rtol * std::fabs(total[j]);
+      } else {
+        double abs = 0.0;
+        for (size_t i = 0; i < n; ++i) abs += A[i * nq + j];
+        target[j] = rtol * abs;
       }
     }
-    double total[3] = {0, 0, 0}, terr[3] = {0, 0, 0}, target[3];
-    for (size_t i = 0; i < panels.size(); ++i)
-      for (int j = 0; j < 3; ++j) {
-        total[j] += sums[6 * i + j];
-        terr[j] += sums[6 * i + 3 + j];
-      }
     bool met = true;
-    for (int j = 0; j < 3; ++j) {
-      target[j] = rtol * std::fabs(total[j]);
-      met = met && terr[j] <= target[j];
-    }
-    const size_t n = panels.size();
-    if (met || n >= kMomentPanels) return result();
+    for (int j = 0; j < nq; ++j) met = met && terr[j] <= target[j];
+    if (met || n >= kMomentPanels) return result(total, terr);
     std::vector<std::pair<double, double>> next;
     for (size_t i = 0; i < n; ++i) {
       bool bad = false;
-      for (int j = 0; j < 3; ++j)
-        bad = bad || (sums[6 * i + 3 + j] * (double)n > target[j] && terr[j] > target[j]);
+      for (int j = 0; j < nq; ++j)
+        bad = bad || (E[i * nq + j] * (double)n > target[j] && terr[j] > target[j]);
       if (bad && panels[i].second - panels[i].first > 1e-10) {
         const double mid = 0.5 * (panels[i].first + panels[i].second);
         next.push_back({panels[i].first, mid});
@@ -180,7 +204,7 @@ Moments moments(const Part& p, double lo, double hi, double rtol, double truncat
         next.push_back(panels[i]);
       }
     }
-    if (next.size() == n) return result();
+    if (next.size() == n) return result(total, terr);
     panels.swap(next);
   }
 }
@@ -226,48 +250,91 @@ std::vector<std::pair<double, double>> initial_panels(double t_lo, double t_hi, 
   return equal;
 }
 
-// One panel's pass-1 sums for one part (engine.rs:482-549).
+// One panel's pass-1 sums for one part (engine.rs:358-373, 482-549): the Kronrod sums of each
+// refined quantity, then of each theta-weighted one (a block of n_refined per requested
+// parameter), |Kronrod - Gauss| of the same, the Kronrod sums of |du/dtheta| r |q| and of
+// u r |q| (the scales of the parameter blocks and of the derivatives along m), and the
+// integrands per unit ln r at the first and last nodes.
 struct Sums1 {
-  double k[kPass1], err[kPass1], edge[2][kPass1];
+  std::vector<double> k, err, abs, absv, edge[2];
 };
 
-// The targets, errors and ends of a part (engine.rs:620-720, no Greek refinement, no
-// derivatives).
+// The targets, errors and ends of a part (engine.rs:620-720, no Greek refinement).
 struct Status {
-  double target[kPass1], errors[kPass1];
+  std::vector<double> target, errors;
   bool met, small[2];
 };
 
-Status status_of(const std::vector<const Sums1*>& s, const Options& o, double ext) {
+Status status_of(const Part& part, const std::vector<const Sums1*>& s, const Options& o,
+                 double ext) {
+  const int nr = part.n_refined(), nt = (int)part.grads.size(), nb = (1 + nt) * nr;
+  const int n_greek = kPass1;
   Status st;
+  st.target.assign(nb, 0.0);
   auto total = [&](int j) {
     double t = 0.0;
     for (auto* x : s) t += x->k[j];
     return t;
   };
+  auto abs_of = [&](int k) {
+    double t = 0.0;
+    for (auto* x : s) t += x->abs[k];
+    return t;
+  };
+  // C_abs and each direction's derivative of it are refined to rtol of C_ext's.
+  auto scale_of = [&](int j) {
+    if (j == ABS) return EXT;
+    if (j >= n_greek && (j - n_greek) % kGroup == kGroup - 1) return j + 1 - kGroup;
+    return j;
+  };
   const double c_sca = std::fabs(total(SCA));
-  for (int j = 0; j < kPass1; ++j) {
+  for (int j = 0; j < nr; ++j) {
     double scale;
-    if (j == SCAG)
+    if (j == SCAG) {
       scale = c_sca;
-    else if (j == BACK)
+    } else if (j == BACK) {
       scale = std::max(std::fabs(total(BACK)), c_sca);
-    else
-      scale = std::fabs(total(j == ABS ? EXT : j));  // C_abs to rtol of C_ext
+    } else if (j >= n_greek) {
+      // The derivatives along m can cancel: their absolute integrands.
+      scale = 0.0;
+      for (auto* x : s) scale += x->absv[scale_of(j)];
+    } else {
+      scale = std::fabs(total(scale_of(j)));
+    }
     st.target[j] = o.rtol * scale;
+    for (int b = 0; b < nt; ++b) st.target[(1 + b) * nr + j] = o.rtol * abs_of(b * nr + scale_of(j));
   }
-  st.target[ONE] = kInf;
-  if (!o.refine_backscatter) st.target[BACK] = kInf;
+  // Z comes from the moments; the theta blocks of the derivatives along m are no outputs.
+  for (int b = 0; b <= nt; ++b) st.target[b * nr + ONE] = kInf;
+  for (int b = 1; b <= nt; ++b)
+    for (int j = n_greek; j < nr; ++j) st.target[b * nr + j] = kInf;
+  if (!o.refine_backscatter)
+    for (int b = 0; b <= nt; ++b) {
+      st.target[b * nr + BACK] = kInf;
+      for (int j = n_greek + 3; j < nr; j += kGroup) st.target[b * nr + j] = kInf;
+    }
+  st.errors.assign(nb, 0.0);
   st.met = true;
-  for (int j = 0; j < kPass1; ++j) {
+  for (int j = 0; j < nb; ++j) {
     double e = 0.0;
     for (auto* x : s) e += x->err[j];
     st.errors[j] = e;
     st.met = st.met && e <= st.target[j];
   }
-  auto small = [&](const double* d) {
-    for (int j = 0; j < kPass1; ++j)
-      if (!(std::fabs(d[j]) * (ext / kStep) <= 0.1 * st.target[j])) return false;
+  // The ends: a tenth of the target per ext/STEP units of ln r; the parameter blocks against
+  // their own size, floored at 1e-3 of the absolute integral.
+  std::vector<double> end_target(nb);
+  for (int x = 0; x < nb; ++x) {
+    if (x < nr || std::isinf(st.target[x])) {
+      end_target[x] = st.target[x];
+    } else {
+      const int b = x / nr - 1, j = x % nr;
+      end_target[x] = o.rtol * std::max(std::fabs(total(x)), 1e-3 * abs_of(b * nr + scale_of(j)));
+    }
+  }
+  auto small = [&](const std::vector<double>& d) {
+    for (int j = 0; j < nb; ++j)
+      if (!(std::fabs(d[j]) * (ext / kStep) <= 0.1 * end_target[j])) return false;
     return true;
   };
   st.small[0] = small(s.front()->edge[0]);
@@ -297,6 +364,13 @@ double Part::u(double r) const {
   if (support == POINT) return 0.0;
   if (kind == kTabulated) return table_density(table.data(), (int64_t)table.size() / 2, r);
   return density(kind, p, r);
+}
+
+double Part::u(double r, double grad[3]) const {
+  grad[0] = grad[1] = grad[2] = 0.0;
+  if (support == POINT) return 0.0;
+  if (kind == kTabulated) return table_density(table.data(), (int64_t)table.size() / 2, r);
+  return density_gradient(kind, p, r, grad);
 }
 
 std::vector<double> Part::breaks() const {
@@ -342,10 +416,12 @@ void gk15(double a, double b, Node out[15]) {
   out[7] = {c, h * kw[7], h * gw[3]};
 }
 
-Part make_part(int kind, const double* p, double rtol, const double* table, int64_t table_len) {
+Part make_part(int kind, const double* p, double rtol, const double* table, int64_t table_len,
+               const std::vector<int>& grads) {
   Part part;
   part.kind = kind;
   for (int k = 0; k < 3; ++k) part.p[k] = p[k];
+  part.grads = grads;
   if (kind == kTabulated) {
     // Finite support between the table's first and last radii (distribution.rs:285-287),
     // reference radius 1, no width limit; the moments with the table's radii as edges.
@@ -483,23 +559,52 @@ void pass1(std::vector<Job>& jobs, const std::vector<Part>& parts, const double*
       pn.n_terms = 0;
       for (int i = 0; i < 15; ++i) pn.n_terms = std::max(pn.n_terms, res[15 * k + i].n);
       pn.sums.assign(jobs[ji].parts.size(), Sums1{});
+      // The quantities of the group's first part's directions (engine.rs:491-506).
+      const Part& first = parts[jobs[ji].parts[0]];
+      const int nr = first.n_refined();
+      int qi[kNodeQ];
+      for (int j = 0; j < kPass1; ++j) qi[j] = j;
+      {
+        int at = kPass1;
+        for (int dir = 0; dir < 2; ++dir)
+          if (first.dirs[dir])
+            for (int j = 0; j < kGroup; ++j) qi[at++] = kPass1 + kGroup * dir + j;
+      }
+      double grad[3];
       for (size_t p = 0; p < jobs[ji].parts.size(); ++p) {
         const Part& part = parts[jobs[ji].parts[p]];
+        const int nt = (int)part.grads.size(), nb = (1 + nt) * nr;
         Sums1& s = pn.sums[p];
-        double g[kPass1] = {0, 0, 0, 0, 0, 0};
-        for (int j = 0; j < kPass1; ++j) s.k[j] = 0.0;
+        s.k.assign(nb, 0.0);
+        s.err.assign(nb, 0.0);
+        s.abs.assign(nt * nr, 0.0);
+        s.absv.assign(nr, 0.0);
+        s.edge[0].assign(nb, 0.0);
+        s.edge[1].assign(nb, 0.0);
+        std::vector<double> g(nb, 0.0);
         for (int i = 0; i < 15; ++i) {
           const double r = qs[15 * k + i].r;
-          const double base = part.u(r) * r;
+          const double base = (nt > 0 ? part.u(r, grad) : part.u(r)) * r;
           const double* q = res[15 * k + i].q;
-          for (int j = 0; j < kPass1; ++j) {
-            s.k[j] += nd[i].wk * base * q[j];
-            g[j] += nd[i].wg * base * q[j];
-            if (i == 0) s.edge[0][j] = base * q[j];
-            if (i == 14) s.edge[1][j] = base * q[j];
+          for (int j = 0; j < nr; ++j) {
+            const double qj = q[qi[j]];
+            s.k[j] += nd[i].wk * base * qj;
+            g[j] += nd[i].wg * base * qj;
+            s.absv[j] += nd[i].wk * std::fabs(base * qj);
+            if (i == 0) s.edge[0][j] = base * qj;
+            if (i == 14) s.edge[1][j] = base * qj;
+            for (int b = 0; b < nt; ++b) {
+              const double dw = grad[part.grads[b]] * r;
+              const int x = (1 + b) * nr + j;
+              s.k[x] += nd[i].wk * dw * qj;
+              g[x] += nd[i].wg * dw * qj;
+              s.abs[b * nr + j] += nd[i].wk * std::fabs(dw * qj);
+              if (i == 0) s.edge[0][x] = dw * qj;
+              if (i == 14) s.edge[1][x] = dw * qj;
+            }
           }
         }
-        for (int j = 0; j < kPass1; ++j) s.err[j] = std::fabs(s.k[j] - g[j]);
+        for (int j = 0; j < nb; ++j) s.err[j] = std::fabs(s.k[j] - g[j]);
       }
     }
     for (size_t ji = 0; ji < jobs.size(); ++ji) {
@@ -516,7 +621,7 @@ void pass1(std::vector<Job>& jobs, const std::vector<Part>& parts, const double*
       for (size_t p = 0; p < np; ++p) {
         std::vector<const Sums1*> s;
         for (auto& pn : st.panels) s.push_back(&pn.sums[p]);
-        stat.push_back(status_of(s, o, st.exts[p]));
+        stat.push_back(status_of(parts[job.parts[p]], s, o, st.exts[p]));
       }
       auto finish = [&]() {
         job.panels.clear();
@@ -589,7 +694,7 @@ void pass1(std::vector<Job>& jobs, const std::vector<Part>& parts, const double*
         if (!(st.panels[i].b - st.panels[i].a > kMinWidth)) continue;
         double bad = 0.0;
         for (size_t p = 0; p < np; ++p)
-          for (int j = 0; j < kPass1; ++j) {
+          for (size_t j = 0; j < stat[p].target.size(); ++j) {
             if (!(stat[p].errors[j] > stat[p].target[j])) continue;
             const double t = std::max(stat[p].target[j], std::numeric_limits<double>::min());
             bad = std::max(bad, st.panels[i].sums[p].err[j] * (double)n / t);

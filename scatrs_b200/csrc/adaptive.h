@@ -17,6 +17,8 @@ namespace adaptive {
 
 constexpr int kMonodisperse = 5;  // a single radius (param[0])
 constexpr int kPass1 = 6;         // 1, C_ext, C_sca, C_sca g, C_back, C_abs (engine.rs:43-54)
+constexpr int kGroup = 5;         // per direction along m: d of C_ext, C_sca, C_sca g, C_back, C_abs
+constexpr int kNodeQ = kPass1 + 2 * kGroup;  // a node's quantities with both directions
 
 struct Error {
   int status;
@@ -28,27 +30,41 @@ enum Support { UNBOUNDED, FINITE, POINT };
 struct Moments {
   double v[2] = {0, 0}, e[2] = {0, 0};  // <r^2>, <r^3> and their error estimates
   double z = 1.0, ez = 0.0;             // the normalization Z = integral of u dr
+  // Along each requested distribution parameter (moments.rs:15-26): d<r^2>, d<r^3> and their
+  // error estimates, dZ and its error estimate.
+  std::vector<std::array<double, 2>> d, de;
+  std::vector<double> dz, dez;
 };
 
-// One distribution of a call (engine.rs:78-112 Part, without modes or derivatives).
+// One distribution of a call (engine.rs:95-115 Part; the mixing weights live with the caller).
 struct Part {
   int kind = 0;
   double p[3] = {0, 0, 0};
+  // The requested distribution parameters (indices into the density's gradient, in the order
+  // of their result columns) and the requested derivatives along Re m and Im m.
+  std::vector<int> grads;
+  bool dirs[2] = {false, false};
+  bool dir_derivatives() const { return dirs[0] || dirs[1]; }
+  // The pass-1 quantities (engine.rs:464-471): the base ones, then kGroup per requested
+  // direction.
+  int n_refined() const { return kPass1 + kGroup * ((int)dirs[0] + (int)dirs[1]); }
   double reference = 1.0, log_width = 0.0;  // distribution.rs:292-336
   Support support = UNBOUNDED;
   double lo = 0.0, hi = 0.0;  // the Mie range before extensions (a point: r, r)
   Moments mom;
   std::vector<double> table;  // a tabulated distribution's [radii..., densities...]
   double u(double r) const;  // the unnormalized density
+  double u(double r, double grad[3]) const;  // and its gradient along the parameters
   // The radii that are panel edges (engine.rs:181-184, 738-751): a finite support's ends and a
   // table's points.
   std::vector<double> breaks() const;
 };
 
 // Parses and prepares a part: validation, support, cut-offs (range.rs) and moments
-// (moments.rs). A tabulated distribution (kind 6) brings its table. Throws Error.
+// (moments.rs), the moments with their derivatives along `grads` (indices into the density's
+// gradient). A tabulated distribution (kind 6) brings its table. Throws Error.
 Part make_part(int kind, const double* p, double rtol, const double* table = nullptr,
-               int64_t table_len = 0);
+               int64_t table_len = 0, const std::vector<int>& grads = {});
 
 struct Options {
   double rtol = 1e-6;
@@ -64,7 +80,7 @@ struct Query {
   int wl;
 };
 struct NodeResult {
-  double q[kPass1];
+  double q[kNodeQ];  // the kPass1 quantities, then kGroup derivatives along Re m and along Im m
   int64_t n;
   int status;
 };

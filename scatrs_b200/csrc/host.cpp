@@ -83,6 +83,7 @@ constexpr int64_t kMaxGreekOrder = 1 << 21;        // MAX_GREEK_ORDER (mie/greek
 constexpr int64_t kMaxMieValues = 1 << 27;         // scatrs-py/src/mie.rs:30
 constexpr int64_t kArenaRows = 1 << 22;            // coefficient rows per slab (1 KiB each)
 constexpr int64_t kMaxSlabChunks = 1 << 18;        // chunks per slab
+constexpr double kPi = 3.14159265358979323846264338327950288;
 
 struct Failure {
   int status;
@@ -158,7 +159,7 @@ struct Context {
   UserTables user;
   std::map<int, BandTables> bands;  // by Greek order
   std::map<int64_t, std::pair<std::vector<double>, std::vector<double>>> rules;
-  DevBuf radius, weight, wtheta, wdiff, unit_norm, wl, m, fractions, chunk_n, chunk_n_slab, chunk_row, chunk_acc, plan_units,
+  DevBuf radius, weight, wtheta, wthdiff, wdiff, unit_norm, wl, m, fractions, chunk_n, chunk_n_slab, chunk_row, chunk_acc, plan_units,
       unit_acc, unit_slots, slots, items, proj_items, slot_index, slot_greek, X, uz, ux,
       chunk_sums, err, acc, counter, values, phase, greek;
   // Pass 1 of the adaptive ensemble.
@@ -441,6 +442,12 @@ struct AdaptiveInput {
   const double* wdiff = nullptr;
   const double* unit_norm = nullptr;
   double* avg = nullptr;  // the units' averages, mixed and assembled by mix_assemble_kernel
+  // With derivatives (and DerivOutput::on with n_theta parameters): per unit and node the
+  // parameters' Kronrod weights w_K (du/dtheta) r and error weights (w_K - w_G) (du/dtheta) r
+  // ([n_units][n_nodes][3]); unit_norm then holds kNormStrideD doubles per unit and avg the
+  // per-block averages of final_adaptive_d_kernel.
+  const double* wtheta = nullptr;
+  const double* wthdiff = nullptr;
 };
 
 void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, const double* wl_dev,
@@ -461,7 +468,7 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
   const auto& gl = rule(c, n_nodes);
   std::vector<double> radius(n_dist * n_nodes), weight(n_dist * n_nodes);
   std::vector<double> wtheta(dv.on ? n_dist * n_nodes * 3 : 0);
-  if (dv.on) {
+  if (dv.on && !ad.on) {
     for (int64_t d = 0; d < n_dist; ++d)
       if (parameter_count(dists[d].kind) != dv.n_theta)
         throw Failure{SCATRS_INVALID_INPUT,
@@ -522,20 +529,28 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
     SB_CUDA(cudaMemcpyAsync(c.radius.get(cnt * 8), ad.radius, cnt * 8, cudaMemcpyHostToDevice, s));
     SB_CUDA(cudaMemcpyAsync(c.weight.get(cnt * 8), ad.weight, cnt * 8, cudaMemcpyHostToDevice, s));
     SB_CUDA(cudaMemcpyAsync(c.wdiff.get(cnt * 8), ad.wdiff, cnt * 8, cudaMemcpyHostToDevice, s));
-    SB_CUDA(cudaMemcpyAsync(c.unit_norm.get((size_t)n_units * 64), ad.unit_norm,
-                            (size_t)n_units * 64, cudaMemcpyHostToDevice, s));
+    const size_t norm_bytes = (size_t)n_units * (dv.on ? kNormStrideD : 8) * 8;
+    SB_CUDA(cudaMemcpyAsync(c.unit_norm.get(norm_bytes), ad.unit_norm, norm_bytes,
+                            cudaMemcpyHostToDevice, s));
+    if (dv.on) {
+      SB_CUDA(cudaMemcpyAsync(c.wtheta.get(cnt * 24), ad.wtheta, cnt * 24,
+                              cudaMemcpyHostToDevice, s));
+      SB_CUDA(cudaMemcpyAsync(c.wthdiff.get(cnt * 24), ad.wthdiff, cnt * 24,
+                              cudaMemcpyHostToDevice, s));
+    }
   } else {
     SB_CUDA(cudaMemcpyAsync(c.radius.get(radius.size() * 8), radius.data(), radius.size() * 8,
                             cudaMemcpyHostToDevice, s));
     SB_CUDA(cudaMemcpyAsync(c.weight.get(weight.size() * 8), weight.data(), weight.size() * 8,
                             cudaMemcpyHostToDevice, s));
   }
-  if (dv.on)
+  if (dv.on && !ad.on)
     SB_CUDA(cudaMemcpyAsync(c.wtheta.get(wtheta.size() * 8), wtheta.data(), wtheta.size() * 8,
                             cudaMemcpyHostToDevice, s));
   // Blocks of sums per quantity (values, then each derivative) and coefficient rows per term
   // of a chunk (two 16-node halves with derivatives).
-  const int n_blk = dv.on ? 3 + dv.n_theta : (ad.on ? 2 : 1);
+  // Adaptive calls add the error sums of every block (a second set of n_blk / 2).
+  const int n_blk = (dv.on ? 3 + dv.n_theta : 1) * (ad.on ? 2 : 1);
   const int rows_per_term = dv.on ? 2 : 1;  unsigned long long* err = c.err.as<unsigned long long>(2);
   SB_CUDA(cudaMemsetAsync(err, 0xff, 2 * sizeof(unsigned long long), s));
   // 2. Plan: every chunk's largest number of terms.
@@ -765,6 +780,7 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
   if (ad.on) {
     ka.per_unit = 1;
     ka.wdiff = c.wdiff.as<double>(0);
+    if (dv.on) ka.wthdiff = c.wthdiff.as<double>(0);
   }
   UnitArgs ua{};
   ua.radius = ka.radius;
@@ -794,14 +810,19 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
   ua.wtheta = ka.wtheta;
   ua.per_unit = ka.per_unit;
   ua.wdiff = ka.wdiff;
+  ua.wthdiff = ka.wthdiff;
   ProjArgs pj{};
   pj.cpu = cpu;
   pj.greek_order = L;
   pj.acc = acc;
   pj.chunk_sums = chunk_sums;
   pj.slot_greek = slot_greek;
-  pj.raw = dv.on ? 1 : 0;
+  pj.raw = dv.on && !ad.on ? 1 : 0;
   if (ad.on) pj.unit_norm = c.unit_norm.as<double>(0);
+  if (ad.on && dv.on) {
+    pj.ad_blocks = 3 + dv.n_theta;
+    pj.n_theta = dv.n_theta;
+  }
   if (bt) {
     pj.bands = bt->desc_d.as<BandDesc>(0);
     pj.band_d = bt->d_d.as<double>(0);
@@ -831,6 +852,13 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
   if (ad.on) {
     fa.unit_norm = c.unit_norm.as<double>(0);
     fa.avg = ad.avg;
+    if (dv.on) {
+      fa.ad_blocks = 3 + dv.n_theta;
+      fa.n_theta = dv.n_theta;
+      fa.d_values = nullptr;
+      fa.d_phase = nullptr;
+      fa.d_greek = nullptr;
+    }
   }
   std::vector<std::pair<double, int64_t>> order;  // work items by cost
   std::vector<int> per_band;
@@ -880,8 +908,9 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
               P_slots[nslot].band = b;
               P_slots[nslot].unit = (int)lu;
               P_slots[nslot].off = band_acc;
-              P_slots[nslot].kind = ad.on ? blk : 0;
-              P_slots[nslot].pad = 0;
+              // Adaptive: the value slots, then the error slots; pad is the block.
+              P_slots[nslot].kind = ad.on ? (2 * blk >= n_blk ? 1 : 0) : 0;
+              P_slots[nslot].pad = ad.on ? blk % (n_blk / 2) : 0;
               band_acc += 4 * (int64_t)band_nq[b];
               ++nslot;
             }
@@ -1043,6 +1072,63 @@ struct AdPart {
   std::string who;
   const double* table = nullptr;  // a tabulated distribution's table
   int64_t table_len = 0;
+  // Derivatives (engine.rs:95-115, 153-176): the requested distribution parameters (indices
+  // into the density's gradient) and their result columns, the columns along Re m and Im m
+  // (-1: not requested), and the part's component, mode (-1: none) and weights w (the
+  // component's), v (the mode's) and v_total (the component's mode weights' sum).
+  std::vector<int> grads, theta_cols;
+  int dir_cols[2] = {-1, -1};
+  int component = 0, mode = -1;
+  double w = 1.0, v = 1.0, v_total = 1.0;
+};
+
+// The derivative outputs of an adaptive call: the requested parameters and the arrays
+// d_values, d_errors [P][11][n], d_phase, d_phase_err [P][6][n][n_mu], d_greek, d_greek_err
+// [P][6][n][L + 1].
+struct AdDerivs {
+  const scatrs_param* params = nullptr;
+  int64_t n = 0;
+  double *d_values = nullptr, *d_errors = nullptr, *d_phase = nullptr, *d_phase_err = nullptr,
+         *d_greek = nullptr, *d_greek_err = nullptr;
+};
+
+// Lin (ensemble/lin.rs:7-68): a value with its error estimate, its derivatives along the
+// requested parameters and theirs, through the ratios with the quotient rule and first-order
+// bounds.
+struct LinD {
+  double v = 0.0, e = 0.0;
+  std::vector<double> d, de;
+  static LinD constant(double v, size_t n) {
+    LinD x;
+    x.v = v;
+    x.d.assign(n, 0.0);
+    x.de.assign(n, 0.0);
+    return x;
+  }
+  LinD div(const LinD& b) const {
+    LinD o;
+    o.v = v / b.v;
+    o.e = (e + std::fabs(o.v) * b.e) / std::fabs(b.v);
+    const size_t n = d.size();
+    o.d.resize(n);
+    o.de.resize(n);
+    for (size_t k = 0; k < n; ++k) o.d[k] = (d[k] - o.v * b.d[k]) / b.v;
+    for (size_t k = 0; k < n; ++k)
+      o.de[k] = (de[k] + std::fabs(o.v) * b.de[k] + std::fabs(o.d[k]) * b.e +
+                 o.e * std::fabs(b.d[k])) /
+                std::fabs(b.v);
+    return o;
+  }
+  LinD scale(double c) const {
+    LinD o = *this;
+    o.v = c * v;
+    o.e = std::fabs(c) * e;
+    for (size_t k = 0; k < d.size(); ++k) {
+      o.d[k] = c * d[k];
+      o.de[k] = std::fabs(c) * de[k];
+    }
+    return o;
+  }
 };
 
 struct AdOutputs {
@@ -1058,10 +1144,199 @@ struct AdOutputs {
 // wavelength), unit-major.
 // With layers (n_layers > 1), every part p is a layered sphere with the fractions
 // layers->fractions[p][L - 1] and indices layers->m[p][L][n_wl] (the parts' m unused).
+// converged: every part of the output unit; panels: the sum over its distinct groups
+// (engine.rs:2228-2236).
+void adaptive_flags(const std::vector<AdPart>& in, const std::vector<adaptive::Job>& jobs,
+                    const std::vector<int>& job_of, const std::vector<char>& unit_converged,
+                    const std::vector<int64_t>& unit_panels, int n_out, int64_t n_wl,
+                    const AdOutputs& res) {
+  (void)jobs;
+  for (int ou = 0; ou < n_out; ++ou)
+    for (int64_t i = 0; i < n_wl; ++i) {
+      bool conv = true;
+      int64_t pan = 0;
+      std::vector<int> seen;
+      for (size_t p = 0; p < in.size(); ++p) {
+        if (in[p].out != ou) continue;
+        const int64_t u = (int64_t)p * n_wl + i;
+        conv = conv && unit_converged[u];
+        const int g = job_of[u];
+        if (g >= 0 && std::find(seen.begin(), seen.end(), g) == seen.end()) {
+          seen.push_back(g);
+          pan += unit_panels[u];
+        }
+      }
+      if (res.converged) res.converged[ou * n_wl + i] = conv ? 1 : 0;
+      if (res.panels) res.panels[ou * n_wl + i] = pan;
+    }
+}
+
+// The mixing and outputs of an adaptive call with derivatives, on the host from the parts'
+// per-block averages (final_adaptive_d_kernel's rows): per output unit and wavelength, the
+// number fractions f (engine.rs:2121-2140) on the values, errors and each block's column, the
+// weight derivatives df (2141-2176: of w/w_total for a component's weight, of v/v_total for a
+// mode's), then the ratios, normalizations and bounds with the derivatives (lin.rs,
+// engine.rs:2396-2497) and the Greek coefficients normalized by the mixture's alpha1_0.
+void mix_derivatives(const std::vector<AdPart>& in, const std::vector<adaptive::Part>& parts,
+                     int n_out, int64_t n_wl, int64_t n_mu, int greek_order, bool normalized,
+                     int n_theta, const std::vector<double>& hav, const AdDerivs& dd,
+                     const AdOutputs& res) {
+  (void)parts;
+  const int B = 3 + n_theta;
+  const int64_t glen = greek_order >= 0 ? greek_order + 1 : 0;
+  const int64_t row = 8 + 4 * n_mu + 6 * glen, stride = 2 * B * row;
+  const size_t P = (size_t)dd.n;
+  const int64_t n_outs = (int64_t)n_out * n_wl;
+  // The result column of block b of part p (-1: none).
+  auto column = [&](const AdPart& a, int b) {
+    if (b >= 1 && b <= n_theta) return b - 1 < (int)a.theta_cols.size() ? a.theta_cols[b - 1] : -1;
+    if (b == n_theta + 1) return a.dir_cols[0];
+    if (b == n_theta + 2) return a.dir_cols[1];
+    return -1;
+  };
+  std::vector<double> v(row), e(row), d(P * row), de(P * row);
+  for (int ou = 0; ou < n_out; ++ou) {
+    double w_total = 0.0;
+    {
+      std::vector<int> comps;
+      for (const AdPart& a : in)
+        if (a.out == ou && std::find(comps.begin(), comps.end(), a.component) == comps.end()) {
+          comps.push_back(a.component);
+          w_total += a.w;
+        }
+    }
+    for (int64_t i = 0; i < n_wl; ++i) {
+      std::fill(v.begin(), v.end(), 0.0);
+      std::fill(e.begin(), e.end(), 0.0);
+      std::fill(d.begin(), d.end(), 0.0);
+      std::fill(de.begin(), de.end(), 0.0);
+      for (size_t p = 0; p < in.size(); ++p) {
+        const AdPart& a = in[p];
+        if (a.out != ou) continue;
+        const double* av = hav.data() + ((int64_t)p * n_wl + i) * stride;
+        for (int64_t k = 0; k < row; ++k) {
+          v[k] += a.f * av[k];
+          e[k] += a.f * av[row + k];
+        }
+        for (int b = 1; b < B; ++b) {
+          const int col = column(a, b);
+          if (col < 0) continue;
+          for (int64_t k = 0; k < row; ++k) {
+            d[col * row + k] += a.f * av[2 * b * row + k];
+            de[col * row + k] += a.f * av[(2 * b + 1) * row + k];
+          }
+        }
+      }
+      for (size_t col = 0; col < P; ++col) {
+        const scatrs_param& pr = dd.params[col];
+        if (pr.kind != SCATRS_PARAM_WEIGHT) continue;
+        for (size_t p = 0; p < in.size(); ++p) {
+          const AdPart& a = in[p];
+          if (a.out != ou) continue;
+          const double f = a.w / w_total * a.v / a.v_total;
+          double df;
+          if (pr.mode < 0) {
+            const double own = a.component == pr.component ? a.v / a.v_total : 0.0;
+            df = (own - f) / w_total;
+          } else if (a.component != pr.component) {
+            df = 0.0;
+          } else {
+            const double own = a.mode == pr.mode ? 1.0 : 0.0;
+            df = a.w / w_total * (own - a.v / a.v_total) / a.v_total;
+          }
+          const double* av = hav.data() + ((int64_t)p * n_wl + i) * stride;
+          for (int64_t k = 0; k < row; ++k) {
+            d[col * row + k] += df * av[k];
+            de[col * row + k] += std::fabs(df) * av[row + k];
+          }
+        }
+      }
+      auto lin = [&](int64_t k) {
+        LinD x;
+        x.v = v[k];
+        x.e = e[k];
+        x.d.resize(P);
+        x.de.resize(P);
+        for (size_t c = 0; c < P; ++c) {
+          x.d[c] = d[c * row + k];
+          x.de[c] = de[c * row + k];
+        }
+        return x;
+      };
+      const LinD ext = lin(1), sca = lin(2), scag = lin(3), ab = lin(4), back = lin(5),
+                 r2 = lin(6), r3 = lin(7);
+      const LinD* dens[3] = {&ext, &sca, &back};
+      const char* names[3] = {"<C_ext>", "<C_sca>", "<C_back>"};
+      for (int k = 0; k < 3; ++k)
+        if (!(std::isfinite(dens[k]->v) && dens[k]->v != 0.0))
+          throw Failure{SCATRS_INVALID_INPUT,
+                        std::string("the ensemble's ") + names[k] +
+                            " is 0 or not finite, so its ratios (albedo, asymmetry parameter, "
+                            "lidar ratio) are undefined (does m = 1?)"};
+      const LinD sc[11] = {ext,
+                           sca,
+                           ab,
+                           back,
+                           sca.div(ext),
+                           scag.div(sca),
+                           ext.div(back).scale(4.0 * kPi),
+                           LinD::constant(0.0, P),
+                           r3.div(r2),
+                           r2.scale(kPi),
+                           r3.scale(4.0 * kPi / 3.0)};
+      const int64_t ox = ou * n_wl + i;
+      for (int k = 0; k < 11; ++k) {
+        res.values[k * n_outs + ox] = sc[k].v;
+        if (res.errors) res.errors[k * n_outs + ox] = sc[k].e;
+        for (size_t c = 0; c < P; ++c) {
+          if (dd.d_values) dd.d_values[(c * 11 + k) * n_outs + ox] = sc[k].d[c];
+          if (dd.d_errors) dd.d_errors[(c * 11 + k) * n_outs + ox] = sc[k].de[c];
+        }
+      }
+      if (n_mu > 0) {
+        const int src[6] = {0, 1, 0, 2, 3, 2};
+        for (int el = 0; el < 6; ++el)
+          for (int64_t j = 0; j < n_mu; ++j) {
+            LinD f = lin(8 + src[el] * n_mu + j);
+            if (normalized) f = f.div(sca);
+            const int64_t at = (el * n_outs + ox) * n_mu + j;
+            if (res.phase) res.phase[at] = f.v;
+            if (res.phase_err) res.phase_err[at] = f.e;
+            for (size_t c = 0; c < P; ++c) {
+              const int64_t atd = (((int64_t)c * 6 + el) * n_outs + ox) * n_mu + j;
+              if (dd.d_phase) dd.d_phase[atd] = f.d[c];
+              if (dd.d_phase_err) dd.d_phase_err[atd] = f.de[c];
+            }
+          }
+      }
+      if (glen > 0) {
+        const int64_t g0 = 8 + 4 * n_mu;
+        const LinD a0 = lin(g0);
+        for (int el = 0; el < 6; ++el)
+          for (int64_t l = 0; l < glen; ++l) {
+            LinD x = lin(g0 + el * glen + l);
+            if (normalized) x = (el == 0 && l == 0) ? LinD::constant(1.0, P) : x.div(a0);
+            const int64_t at = (el * n_outs + ox) * glen + l;
+            if (res.greek) res.greek[at] = x.v;
+            if (res.greek_err) res.greek_err[at] = x.e;
+            for (size_t c = 0; c < P; ++c) {
+              const int64_t atd = (((int64_t)c * 6 + el) * n_outs + ox) * glen + l;
+              if (dd.d_greek) dd.d_greek[atd] = x.d[c];
+              if (dd.d_greek_err) dd.d_greek_err[atd] = x.de[c];
+            }
+          }
+      }
+    }
+  }
+}
+
+// With dd (derivatives), pass 1 refines the requested parameters' blocks too, pass 2 runs the
+// derivative blocks of every part, and the mixing (with the weight derivatives) and the
+// outputs are assembled on the host from the parts' per-block averages.
 void adaptive_call(const std::vector<AdPart>& in, int n_out, bool batch, const double* wavelengths,
                    int64_t n_wl, const double* mu, int64_t n_mu,
                    const scatrs_adaptive_options* options, const AdOutputs& res,
-                   const scatrs_layers* layers = nullptr) {
+                   const scatrs_layers* layers = nullptr, const AdDerivs* dd = nullptr) {
   if (!options) throw Failure{SCATRS_INVALID_INPUT, "options must not be NULL"};
   if (n_wl < 0) throw Failure{SCATRS_INVALID_INPUT, "negative sizes"};
   const adaptive::Options o{options->rtol, options->max_panels, options->allow_unvalidated != 0,
@@ -1083,13 +1358,23 @@ void adaptive_call(const std::vector<AdPart>& in, int n_out, bool batch, const d
   const int64_t n_units = n_parts * n_wl;  // pipeline units: (part, wavelength)
   check_options(&fo, (int64_t)n_out * n_wl, n_mu, mu);
   if (n_units == 0 || n_out == 0) return;
+  const bool deriv = dd && dd->n > 0;
   std::vector<adaptive::Part> parts;
+  int n_theta = 0;  // the most requested distribution parameters of a part
+  bool any_dirs = false;
   for (const AdPart& p : in) {
     try {
-      parts.push_back(adaptive::make_part(p.kind, p.p, o.rtol, p.table, p.table_len));
+      parts.push_back(adaptive::make_part(p.kind, p.p, o.rtol, p.table, p.table_len, p.grads));
     } catch (const adaptive::Error& e) {
       throw Failure{e.status, p.who + e.msg};
     }
+    parts.back().dirs[0] = p.dir_cols[0] >= 0;
+    parts.back().dirs[1] = p.dir_cols[1] >= 0;
+    n_theta = std::max(n_theta, (int)p.grads.size());
+    any_dirs = any_dirs || parts.back().dir_derivatives();
+    if (!p.grads.empty() && parts.back().support == adaptive::POINT)
+      throw Failure{SCATRS_INVALID_INPUT,
+                    p.who + "the derivative along a single radius is not on the GPU path"};
   }
   Context& c = context();
   std::lock_guard<std::mutex> lk(c.mtx);
@@ -1101,6 +1386,9 @@ void adaptive_call(const std::vector<AdPart>& in, int n_out, bool batch, const d
   if (L > 16) throw Failure{SCATRS_INVALID_INPUT, "the GPU path takes 1 to 16 layers"};
   if (L > 1 && (!layers->fractions || !layers->m))
     throw Failure{SCATRS_INVALID_INPUT, "layers must give fractions and m"};
+  if (L > 1 && deriv)
+    throw Failure{SCATRS_INVALID_INPUT,
+                  "derivatives of layered spheres on the adaptive path are not on the GPU path"};
   std::vector<double> m_unit(2 * n_units, 0.0);
   if (L == 1)
     for (int64_t u = 0; u < n_units; ++u) {
@@ -1167,7 +1455,9 @@ void adaptive_call(const std::vector<AdPart>& in, int n_out, bool batch, const d
       a.scratch = c.p1_scratch.as<int64_t>(n + 1);
       a.uz = c.p1_uz.as<double2>((size_t)rows * (2 * L - 1));
       a.ux = c.p1_ux.as<double>(rows);
-      a.q = c.p1_q.as<double>(6 * n);
+      const int nq = any_dirs ? adaptive::kNodeQ : adaptive::kPass1;
+      a.deriv = any_dirs ? 1 : 0;
+      a.q = c.p1_q.as<double>(nq * n);
       a.n_terms = c.p1_n.as<int64_t>(n);
       a.status = c.p1_status.as<int>(n);
       a.wl = wl_unit_d;
@@ -1184,16 +1474,16 @@ void adaptive_call(const std::vector<AdPart>& in, int n_out, bool batch, const d
                               s));
       timed_launch(K_NODES, s, [&] { launch_pass1(a, s); });
       SB_CUDA(cudaGetLastError());
-      std::vector<double> q(6 * n);
+      std::vector<double> q(nq * n);
       std::vector<int64_t> nt(n);
       std::vector<int> st(n);
-      SB_CUDA(cudaMemcpyAsync(q.data(), a.q, 6 * n * 8, cudaMemcpyDeviceToHost, s));
+      SB_CUDA(cudaMemcpyAsync(q.data(), a.q, nq * n * 8, cudaMemcpyDeviceToHost, s));
       SB_CUDA(cudaMemcpyAsync(nt.data(), a.n_terms, n * 8, cudaMemcpyDeviceToHost, s));
       SB_CUDA(cudaMemcpyAsync(st.data(), a.status, n * 4, cudaMemcpyDeviceToHost, s));
       SB_CUDA(cudaStreamSynchronize(s));
       for (int64_t k = 0; k < n; ++k) {
         adaptive::NodeResult& x = out[k0 + k];
-        for (int j = 0; j < 6; ++j) x.q[j] = q[6 * k + j];
+        for (int j = 0; j < adaptive::kNodeQ; ++j) x.q[j] = j < nq ? q[nq * k + j] : 0.0;
         x.n = nt[k];
         x.status = st[k];
       }
@@ -1282,8 +1572,10 @@ void adaptive_call(const std::vector<AdPart>& in, int n_out, bool batch, const d
   }
   if ((double)n_units * (double)n_nodes > 4e9)
     throw Failure{SCATRS_INVALID_INPUT, "too many (unit, node) pairs for one call"};
+  const int ns = deriv ? kNormStrideD : 8;  // unit_norm doubles per unit
   std::vector<double> radius((size_t)n_units * n_nodes, 0.0), weight(radius.size(), 0.0),
-      wdiff(radius.size(), 0.0), norm((size_t)n_units * 8, 0.0);
+      wdiff(radius.size(), 0.0), norm((size_t)n_units * ns, 0.0);
+  std::vector<double> wth(deriv ? 3 * radius.size() : 0, 0.0), wthd(wth.size(), 0.0);
   std::vector<char> unit_converged(n_units, 1);
   std::vector<int64_t> unit_panels(n_units, 0);
   for (int64_t u = 0; u < n_units; ++u) {
@@ -1292,7 +1584,7 @@ void adaptive_call(const std::vector<AdPart>& in, int n_out, bool batch, const d
     double* nr = &radius[(size_t)u * n_nodes];
     double* nw = &weight[(size_t)u * n_nodes];
     double* nd = &wdiff[(size_t)u * n_nodes];
-    double* un = &norm[(size_t)u * 8];
+    double* un = &norm[(size_t)u * ns];
     if (part.support == adaptive::POINT) {
       nr[0] = part.lo;
       nw[0] = 1.0;
@@ -1306,10 +1598,19 @@ void adaptive_call(const std::vector<AdPart>& in, int n_out, bool batch, const d
       adaptive::gk15(jb.panels[pi].first, jb.panels[pi].second, g);
       const size_t base = (size_t)slot_of[job_of[u]][pi];
       for (int k = 0; k < 15; ++k) {
-        const double r = std::exp(g[k].t), ur = part.u(r) * r;
+        const double r = std::exp(g[k].t);
+        double grad[3];
+        const double ur = (part.grads.empty() ? part.u(r) : part.u(r, grad)) * r;
         nr[base + k] = r;
         nw[base + k] = g[k].wk * ur;
         nd[base + k] = g[k].wk * ur - g[k].wg * ur;
+        // Each requested parameter's weights w (du/dtheta) r (engine.rs:1637-1644).
+        for (size_t b = 0; b < part.grads.size(); ++b) {
+          const double dw = grad[part.grads[b]] * r;
+          const size_t at = ((size_t)u * n_nodes + base + k) * 3 + b;
+          wth[at] = g[k].wk * dw;
+          wthd[at] = g[k].wk * dw - g[k].wg * dw;
+        }
       }
     }
     un[0] = part.mom.z;
@@ -1319,12 +1620,24 @@ void adaptive_call(const std::vector<AdPart>& in, int n_out, bool batch, const d
     un[5] = part.mom.e[0];
     un[6] = part.mom.v[1];
     un[7] = part.mom.e[1];
+    for (size_t b = 0; deriv && b < part.grads.size(); ++b) {
+      un[8 + b] = part.mom.dz[b];
+      un[11 + b] = part.mom.dez[b];
+      un[14 + 4 * b] = part.mom.d[b][0];
+      un[15 + 4 * b] = part.mom.de[b][0];
+      un[16 + 4 * b] = part.mom.d[b][1];
+      un[17 + 4 * b] = part.mom.de[b][1];
+    }
     unit_converged[u] = jb.converged[place[u]] ? 1 : 0;
     unit_panels[u] = (int64_t)jb.panels.size();
   }
   fo.n_nodes = (int32_t)n_nodes;
   const int glen = options->greek_order >= 0 ? options->greek_order + 1 : 0;
-  const int64_t stride = 16 + 8 * n_mu + 12 * (int64_t)glen;
+  // The parts' averages: values and errors, or per block of a call with derivatives (values,
+  // n_theta parameters, Re m, Im m).
+  const int n_blocks = 3 + n_theta;
+  const int64_t row = 8 + 4 * n_mu + 6 * (int64_t)glen;
+  const int64_t stride = deriv ? 2 * n_blocks * row : 16 + 8 * n_mu + 12 * (int64_t)glen;
   double* avg = c.avg.as<double>((size_t)n_units * stride);
   AdaptiveInput ad;
   ad.on = true;
@@ -1333,6 +1646,13 @@ void adaptive_call(const std::vector<AdPart>& in, int n_out, bool batch, const d
   ad.wdiff = wdiff.data();
   ad.unit_norm = norm.data();
   ad.avg = avg;
+  DerivOutput dvo;
+  if (deriv) {
+    ad.wtheta = wth.data();
+    ad.wthdiff = wthd.data();
+    dvo.on = true;
+    dvo.n_theta = n_theta;
+  }
   FixedCall call;
   call.wl_host.assign(wavelengths, wavelengths + n_wl);
   call.per_unit = true;
@@ -1347,7 +1667,18 @@ void adaptive_call(const std::vector<AdPart>& in, int n_out, bool batch, const d
     li.m_dev = ml_d;
   }
   run_fixed(c, dummy.data(), n_parts, wl_d, n_wl, m_d, mu, n_mu, &fo, nullptr, nullptr, nullptr,
-            s, &call, li, DerivOutput(), ad);
+            s, &call, li, dvo, ad);
+  if (deriv) {
+    call.radius = std::move(radius);
+    check_device_errors(c, s, &call);
+    std::vector<double> hav((size_t)n_units * stride);
+    SB_CUDA(cudaMemcpyAsync(hav.data(), avg, hav.size() * 8, cudaMemcpyDeviceToHost, s));
+    SB_CUDA(cudaStreamSynchronize(s));
+    mix_derivatives(in, parts, n_out, n_wl, n_mu, options->greek_order, options->normalized != 0,
+                    n_theta, hav, *dd, res);
+    adaptive_flags(in, jobs, job_of, unit_converged, unit_panels, n_out, n_wl, res);
+    return;
+  }
   // Mixing and outputs.
   const int64_t n_outs = (int64_t)n_out * n_wl;
   int64_t vl, pl, gl;
@@ -1403,25 +1734,7 @@ void adaptive_call(const std::vector<AdPart>& in, int n_out, bool batch, const d
   if (gl > 0 && res.greek_err)
     SB_CUDA(cudaMemcpyAsync(res.greek_err, g_d + gl, gl * 8, cudaMemcpyDeviceToHost, s));
   SB_CUDA(cudaStreamSynchronize(s));
-  // converged: every part of the output unit; panels: the sum over its distinct groups
-  // (engine.rs:2228-2236).
-  for (int ou = 0; ou < n_out; ++ou)
-    for (int64_t i = 0; i < n_wl; ++i) {
-      bool conv = true;
-      int64_t pan = 0;
-      std::vector<int> seen;
-      for (int k = first[ou]; k < first[ou + 1]; ++k) {
-        const int64_t u = (int64_t)member[k] * n_wl + i;
-        conv = conv && unit_converged[u];
-        const int g = job_of[u];
-        if (g >= 0 && std::find(seen.begin(), seen.end(), g) == seen.end()) {
-          seen.push_back(g);
-          pan += unit_panels[u];
-        }
-      }
-      if (res.converged) res.converged[ou * n_wl + i] = conv ? 1 : 0;
-      if (res.panels) res.panels[ou * n_wl + i] = pan;
-    }
+  adaptive_flags(in, jobs, job_of, unit_converged, unit_panels, n_out, n_wl, res);
 }
 
 // The driver's tensor-map encoder, found once through the runtime.
@@ -2225,6 +2538,52 @@ int guarded(char* err, size_t err_len, F f) {
   }
 }
 
+// The parts of a mixture (ensemble/mod.rs:609-625, 688-780 validation; engine.rs:141-223): each
+// mode of each component with its number fraction w / w_total * v / v_total (engine.rs:2131).
+std::vector<AdPart> mixture_parts(const scatrs_component* components, int64_t n_comp) {
+  if (n_comp < 1) throw Failure{SCATRS_INVALID_INPUT, "a mixture needs a component"};
+  double total = 0.0;
+  for (int64_t c = 0; c < n_comp; ++c) {
+    const scatrs_component& k = components[c];
+    const std::string who = "component " + std::to_string(c);
+    if (!(std::isfinite(k.weight) && k.weight >= 0.0))
+      throw Failure{SCATRS_INVALID_INPUT, "the weight of " + who + " must be finite and >= 0"};
+    if (k.n_modes < 1 || !k.modes || !k.m)
+      throw Failure{SCATRS_INVALID_INPUT, who + ": needs a distribution and m"};
+    if (k.n_modes > 1) {
+      if (!k.mode_weights) throw Failure{SCATRS_INVALID_INPUT, who + ": needs mode weights"};
+      double sum = 0.0;
+      for (int j = 0; j < k.n_modes; ++j) sum += k.mode_weights[j];
+      if (!std::isfinite(sum))
+        throw Failure{SCATRS_INVALID_INPUT, who + ": the mode weights must have a finite sum"};
+    }
+    total += k.weight;
+  }
+  if (!(std::isfinite(total) && total > 0.0))
+    throw Failure{SCATRS_INVALID_INPUT,
+                  "the mixture weights must have a finite, positive sum"};
+  std::vector<AdPart> parts;
+  for (int64_t c = 0; c < n_comp; ++c) {
+    const scatrs_component& k = components[c];
+    double v_total = 0.0;
+    for (int j = 0; j < k.n_modes; ++j) v_total += k.n_modes > 1 ? k.mode_weights[j] : 1.0;
+    for (int j = 0; j < k.n_modes; ++j) {
+      const double v = k.n_modes > 1 ? k.mode_weights[j] : 1.0;
+      const scatrs_distribution& d = k.modes[j];
+      parts.push_back(AdPart{d.kind, {d.param[0], d.param[1], d.param[2]}, k.m,
+                             k.weight / total * v / v_total, 0,
+                             "component " + std::to_string(c) + ": ", d.table, d.table_len});
+      AdPart& a = parts.back();
+      a.component = (int)c;
+      a.mode = k.mode_weights ? j : -1;
+      a.w = k.weight;
+      a.v = v;
+      a.v_total = v_total;
+    }
+  }
+  return parts;
+}
+
 }  // namespace
 }  // namespace sb
 
@@ -2387,6 +2746,109 @@ int scatrs_ensemble_adaptive_spheroid(const scatrs_distribution* dists, int64_t 
   });
 }
 
+int scatrs_ensemble_mixture_d(const scatrs_component* components, int64_t n_comp,
+                              const double* wavelengths, int64_t n_wl, const double* mu,
+                              int64_t n_mu, const scatrs_adaptive_options* options,
+                              const scatrs_param* params, int64_t n_params, double* values,
+                              double* errors, double* d_values, double* d_errors, double* phase,
+                              double* phase_err, double* d_phase, double* d_phase_err,
+                              double* greek, double* greek_err, double* d_greek,
+                              double* d_greek_err, int8_t* converged, int64_t* panels, char* err,
+                              size_t err_len) {
+  return guarded(err, err_len, [&] {
+    if (n_params < 0 || (n_params > 0 && !params))
+      throw Failure{SCATRS_INVALID_INPUT, "params must hold n_params parameters"};
+    std::vector<AdPart> parts = mixture_parts(components, n_comp);
+    // ensemble/mod.rs:781-799: every parameter once and among the mixture's (mod.rs:254-337).
+    bool mixture = n_comp > 1;
+    for (int64_t k = 0; k < n_params; ++k)
+      mixture = mixture || (params[k].kind == SCATRS_PARAM_WEIGHT && params[k].mode < 0);
+    auto name = [&](const scatrs_param& q) {
+      static const char* dist_names[7][3] = {{"", "", ""},
+                                             {"median_radius", "width", ""},
+                                             {"effective_radius", "effective_variance", ""},
+                                             {"alpha", "b", "gamma"},
+                                             {"exponent", "", ""},
+                                             {"radius", "", ""},
+                                             {"", "", ""}};
+      std::string out = mixture ? "c" + std::to_string(q.component) + "." : "";
+      if (q.mode >= 0) out += "mode" + std::to_string(q.mode) + ".";
+      switch (q.kind) {
+        case SCATRS_PARAM_DISTRIBUTION: {
+          const bool ok = q.component >= 0 && q.component < n_comp && q.mode >= -1 &&
+                          q.mode < components[q.component].n_modes;
+          const int kind = ok ? components[q.component].modes[q.mode < 0 ? 0 : q.mode].kind : 0;
+          out += kind >= 0 && kind < 7 && q.index >= 0 && q.index < 3 && dist_names[kind][q.index][0]
+                     ? dist_names[kind][q.index]
+                     : "parameter" + std::to_string(q.index);
+          break;
+        }
+        case SCATRS_PARAM_REFR_REAL: out += "m_real"; break;
+        case SCATRS_PARAM_REFR_IMAG: out += "m_imag"; break;
+        case SCATRS_PARAM_WEIGHT: out += "weight"; break;
+        default: out += "kind" + std::to_string(q.kind);
+      }
+      return out;
+    };
+    for (int64_t k = 0; k < n_params; ++k) {
+      const scatrs_param& q = params[k];
+      for (int64_t j = 0; j < k; ++j)
+        if (params[j].component == q.component && params[j].mode == q.mode &&
+            params[j].kind == q.kind && params[j].index == q.index)
+          throw Failure{SCATRS_INVALID_INPUT, "parameter " + name(q) + " requested twice"};
+      bool allowed = q.component >= 0 && q.component < n_comp;
+      if (allowed) {
+        const scatrs_component& cp = components[q.component];
+        const bool multi = cp.mode_weights != nullptr;
+        switch (q.kind) {
+          case SCATRS_PARAM_DISTRIBUTION: {
+            const bool mode_ok = multi ? (q.mode >= 0 && q.mode < cp.n_modes) : q.mode == -1;
+            const int kind = mode_ok ? cp.modes[q.mode < 0 ? 0 : q.mode].kind : 0;
+            const int np = kind == adaptive::kMonodisperse ? 1 : parameter_count(kind);
+            allowed = mode_ok && q.index >= 0 && q.index < np;
+            break;
+          }
+          case SCATRS_PARAM_REFR_REAL:
+          case SCATRS_PARAM_REFR_IMAG: allowed = q.mode == -1; break;
+          case SCATRS_PARAM_WEIGHT:
+            allowed = q.mode == -1 || (multi && q.mode >= 0 && q.mode < cp.n_modes);
+            break;
+          default: allowed = false;
+        }
+      }
+      if (!allowed) throw Failure{SCATRS_INVALID_INPUT, "no parameter " + name(q) + " here"};
+    }
+    // engine.rs:153-176: each part's parameters and their columns.
+    for (AdPart& a : parts)
+      for (int64_t k = 0; k < n_params; ++k) {
+        const scatrs_param& q = params[k];
+        if (q.component != a.component) continue;
+        if (q.kind == SCATRS_PARAM_DISTRIBUTION && q.mode == a.mode) {
+          a.grads.push_back(q.index);
+          a.theta_cols.push_back((int)k);
+        } else if (q.kind == SCATRS_PARAM_REFR_REAL) {
+          a.dir_cols[0] = (int)k;
+        } else if (q.kind == SCATRS_PARAM_REFR_IMAG) {
+          a.dir_cols[1] = (int)k;
+        }
+      }
+    AdOutputs out{values, errors, phase, phase_err, greek, greek_err, converged, panels};
+    AdDerivs dd;
+    dd.params = params;
+    dd.n = n_params;
+    dd.d_values = d_values;
+    dd.d_errors = d_errors;
+    dd.d_phase = d_phase;
+    dd.d_phase_err = d_phase_err;
+    dd.d_greek = d_greek;
+    dd.d_greek_err = d_greek_err;
+    if (n_params > 0 && !d_values)
+      throw Failure{SCATRS_INVALID_INPUT, "d_values is required with parameters"};
+    adaptive_call(parts, 1, false, wavelengths, n_wl, mu, n_mu, options, out, nullptr,
+                  n_params > 0 ? &dd : nullptr);
+  });
+}
+
 int scatrs_ensemble_mixture(const scatrs_component* components, int64_t n_comp,
                             const double* wavelengths, int64_t n_wl, const double* mu,
                             int64_t n_mu, const scatrs_adaptive_options* options, double* values,
@@ -2394,46 +2856,12 @@ int scatrs_ensemble_mixture(const scatrs_component* components, int64_t n_comp,
                             double* greek_err, int8_t* converged, int64_t* panels, char* err,
                             size_t err_len) {
   return guarded(err, err_len, [&] {
-    // ensemble/mod.rs:609-625, 688-780: the components' weights and modes.
-    if (n_comp < 1) throw Failure{SCATRS_INVALID_INPUT, "a mixture needs a component"};
-    double total = 0.0;
-    for (int64_t c = 0; c < n_comp; ++c) {
-      const scatrs_component& k = components[c];
-      const std::string who = "component " + std::to_string(c);
-      if (!(std::isfinite(k.weight) && k.weight >= 0.0))
-        throw Failure{SCATRS_INVALID_INPUT, "the weight of " + who + " must be finite and >= 0"};
-      if (k.n_modes < 1 || !k.modes || !k.m)
-        throw Failure{SCATRS_INVALID_INPUT, who + ": needs a distribution and m"};
-      if (k.n_modes > 1) {
-        if (!k.mode_weights) throw Failure{SCATRS_INVALID_INPUT, who + ": needs mode weights"};
-        double sum = 0.0;
-        for (int j = 0; j < k.n_modes; ++j) sum += k.mode_weights[j];
-        if (!std::isfinite(sum))
-          throw Failure{SCATRS_INVALID_INPUT, who + ": the mode weights must have a finite sum"};
-      }
-      total += k.weight;
-    }
-    if (!(std::isfinite(total) && total > 0.0))
-      throw Failure{SCATRS_INVALID_INPUT,
-                    "the mixture weights must have a finite, positive sum"};
-    std::vector<AdPart> parts;
-    for (int64_t c = 0; c < n_comp; ++c) {
-      const scatrs_component& k = components[c];
-      double v_total = 0.0;
-      for (int j = 0; j < k.n_modes; ++j) v_total += k.n_modes > 1 ? k.mode_weights[j] : 1.0;
-      for (int j = 0; j < k.n_modes; ++j) {
-        const double v = k.n_modes > 1 ? k.mode_weights[j] : 1.0;
-        const scatrs_distribution& d = k.modes[j];
-        // The number fraction of engine.rs:2131: w / w_total * v / v_total.
-        parts.push_back(AdPart{d.kind, {d.param[0], d.param[1], d.param[2]}, k.m,
-                               k.weight / total * v / v_total, 0,
-                               "component " + std::to_string(c) + ": ", d.table, d.table_len});
-      }
-    }
+    std::vector<AdPart> parts = mixture_parts(components, n_comp);
     AdOutputs out{values, errors, phase, phase_err, greek, greek_err, converged, panels};
     adaptive_call(parts, 1, false, wavelengths, n_wl, mu, n_mu, options, out);
   });
 }
+
 
 int scatrs_project_greek_device(const double* phase_dev, int64_t n_units, int64_t n_q,
                                 int32_t order, int32_t precision, double* greek_dev,
@@ -3003,7 +3431,7 @@ void scatrs_release(void) {
   std::lock_guard<std::mutex> lk(g_ctx_mtx);
   if (dev < (int)g_ctx.size() && g_ctx[dev]) {
     Context& c = *g_ctx[dev];
-    for (DevBuf* b : {&c.radius, &c.weight, &c.wtheta, &c.wdiff, &c.unit_norm, &c.wl, &c.m, &c.fractions, &c.chunk_n, &c.chunk_n_slab,
+    for (DevBuf* b : {&c.radius, &c.weight, &c.wtheta, &c.wthdiff, &c.wdiff, &c.unit_norm, &c.wl, &c.m, &c.fractions, &c.chunk_n, &c.chunk_n_slab,
                       &c.chunk_row, &c.chunk_acc, &c.plan_units, &c.unit_acc, &c.unit_slots,
                       &c.slots, &c.items, &c.proj_items, &c.slot_index, &c.slot_greek,
                       &c.X, &c.uz, &c.ux, &c.chunk_sums, &c.err, &c.acc,

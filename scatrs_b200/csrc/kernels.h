@@ -50,6 +50,10 @@ struct MieFixedArgs {
   // chunk_sums [n_chunks][2][8]: the Kronrod sums, then the sums of |Kronrod - Gauss| per panel.
   int per_unit;
   const double* wdiff;
+  // Adaptive panels with derivatives (deriv and per_unit): the parameters' error weights
+  // (w_K - w_G) (du/dtheta_p) r ([n_units][n_nodes][3]); chunk_sums [n_chunks][2 (3 + n_theta)]
+  // [8]: each block's Kronrod sums, then each block's sums of |Kronrod - Gauss| per panel.
+  const double* wthdiff;
 };
 
 struct MieNodesArgs {
@@ -129,7 +133,19 @@ struct ProjArgs {
   // sums as (e + |s/z| ez) / z + truncation |s/z| (engine.rs:1782-1800), then bounded with |d|.
   const double* unit_norm;
   const int* units;  // slab-local unit -> unit
+  // Adaptive panels with derivatives (ad_blocks = B = 3 + n_theta > 0): a unit's slots per band
+  // are B value slots then B error slots (BandSlot::pad the block); unit_norm holds
+  // kNormStrideD doubles per unit (see FinalArgs). Value slots project the part's averages
+  // along their block, v = S_0/Z, dv = (S_p - v Z_p)/Z or S_m/Z; error slots bound their
+  // first-order error estimates (engine.rs:1782-1836) with |d|.
+  int ad_blocks;
+  int n_theta;
 };
+
+// unit_norm per unit of an adaptive call with derivatives: the 8 doubles of FinalArgs, then
+// per distribution parameter p < 3 its Z_p at 8 + p, the error of Z_p at 11 + p, and
+// d<r^2>/dp, its error, d<r^3>/dp, its error at 14 + 4 p.
+constexpr int kNormStrideD = 32;
 
 // K-b and K-c over one slab: the work items write the per-unit accumulators (zeroed before).
 struct UnitArgs {
@@ -164,6 +180,9 @@ struct UnitArgs {
   int deriv;
   int n_theta;
   const double* wtheta;
+  // Adaptive panels with derivatives (deriv and wdiff): the parameters' error weights; the
+  // accumulators hold each block's sums, then each block's error sums (2 (3 + n_theta) blocks).
+  const double* wthdiff;
 };
 
 // K-d and the outputs over one slab: averages, band projections, assembly.
@@ -196,6 +215,10 @@ struct FinalArgs {
   // error); the averages go to avg (per unit 16 + 8 n_mu + 12 (L + 1) doubles) for the mixing.
   const double* unit_norm;
   double* avg;
+  // Adaptive panels with derivatives (ad_blocks = B > 0): avg per unit holds, block after block,
+  // the part's averages (8 scalars, 4 n_mu cosine values, 6 (L + 1) Greek coefficients) and
+  // then their error estimates, 2 B (8 + 4 n_mu + 6 (L + 1)) doubles.
+  int ad_blocks;
 };
 
 // The mixing and the outputs of adaptive calls: output unit (o, wavelength i) is
@@ -237,6 +260,10 @@ struct Pass1Args {
   int n_wl;
   const double* fractions;
   const double2* m_layers;
+  // Homogeneous spheres with deriv != 0: q is [n][16], the 6 quantities followed by the
+  // derivatives of pi r^2 (Q_ext, Q_sca, Q_sca g, Q_back, Q_abs) along Re m, then along Im m
+  // (engine.rs:447-461).
+  int deriv;
 };
 
 void launch_plan_chunks(const PlanArgs& a, cudaStream_t s);

@@ -179,15 +179,16 @@ __device__ __forceinline__ void mie_chunk_deriv(const MieFixedArgs& a) {
   s.stride = 32;
   const int P = a.n_theta;
   const int B = 3 + P;
-  double q[6][8];
-#pragma unroll
-  for (int b = 0; b < 6; ++b)
-#pragma unroll
-    for (int k = 0; k < 8; ++k) q[b][k] = 0.0;
+  // The node's quantities, their derivatives along Re m and Im m, and the blocks' weights
+  // (adaptive: and their error weights (w_K - w_G) ...).
+  double qv[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  double qd[2][8] = {{0, 0, 0, 0, 0, 0, 0, 0}, {0, 0, 0, 0, 0, 0, 0, 0}};
+  double wb[4] = {0, 0, 0, 0}, wbd[4] = {0, 0, 0, 0};  // values, then each parameter
+  const bool adaptive = a.wdiff != nullptr;
   int64_t n = 0;
-  if (j < a.n_nodes) {
-    const double r = a.radius[d * a.n_nodes + j];
-    const double w = a.weight[d * a.n_nodes + j];
+  const int64_t node = (a.per_unit ? unit : d) * a.n_nodes + j;
+  if (j < a.n_nodes && a.radius[node] > 0.0) {
+    const double r = a.radius[node];
     const double x = 2.0 * kPi * r / a.wl[i];
     n = default_n_max(x);
     ValueSums vs;
@@ -218,16 +219,12 @@ __device__ __forceinline__ void mie_chunk_deriv(const MieFixedArgs& a) {
     } else {
       const Eff e = efficiencies_from(x, asum, vs);
       const double area = kPi * r * r;
-      const double qv[8] = {1.0,           area * e.q_ext, area * e.q_sca, area * e.q_sca * e.g,
+      const double q0[8] = {1.0,           area * e.q_ext, area * e.q_sca, area * e.q_sca * e.g,
                             area * e.q_abs, area * e.q_back, r * r,         r * r * r};
-      for (int k = 0; k < 8; ++k) q[0][k] = w * qv[k];
-      for (int p = 0; p < P; ++p) {
-        const double wt = a.wtheta[(d * a.n_nodes + j) * 3 + p];
-        for (int k = 0; k < 8; ++k) q[1 + p][k] = wt * qv[k];
-      }
+      for (int k = 0; k < 8; ++k) qv[k] = q0[k];
       for (int p = 0; p < 2; ++p) {
         const Eff de = efficiency_derivs(x, vs, e, ds, p, p == 0 ? md.abs_re : md.abs_im);
-        const double qd[8] = {0.0,
+        const double q1[8] = {0.0,
                               area * de.q_ext,
                               area * de.q_sca,
                               area * (de.q_sca * e.g + e.q_sca * de.g),
@@ -235,7 +232,13 @@ __device__ __forceinline__ void mie_chunk_deriv(const MieFixedArgs& a) {
                               area * de.q_back,
                               0.0,
                               0.0};
-        for (int k = 0; k < 8; ++k) q[1 + P + p][k] = w * qd[k];
+        for (int k = 0; k < 8; ++k) qd[p][k] = q1[k];
+      }
+      wb[0] = a.weight[node];
+      for (int p = 0; p < P; ++p) wb[1 + p] = a.wtheta[node * 3 + p];
+      if (adaptive) {
+        wbd[0] = a.wdiff[node];
+        for (int p = 0; p < P; ++p) wbd[1 + p] = a.wthdiff[node * 3 + p];
       }
     }
   }
@@ -243,12 +246,25 @@ __device__ __forceinline__ void mie_chunk_deriv(const MieFixedArgs& a) {
     *reinterpret_cast<double4*>(X + (k - 1) * 128) = make_double4(0.0, 0.0, 0.0, 0.0);
     *reinterpret_cast<double4*>(X + (k - 1) * 128 + 64) = make_double4(0.0, 0.0, 0.0, 0.0);
   }
-  for (int b = 0; b < 6; ++b) {
-    if (b >= B) break;
+  // Per block: the values and each parameter weight the node's quantities, Re m and Im m
+  // weight its derivatives with the values' weight. The chunk's sums in a fixed tree order;
+  // adaptive: then |Kronrod - Gauss| of each of the chunk's two panels (lanes 0-15, 16-31),
+  // added.
+  const int stride = adaptive ? 2 * B : B;
+  for (int b = 0; b < B; ++b) {
+    const int wi = b <= P ? b : 0;
     for (int k = 0; k < 8; ++k) {
-      double v = q[b][k];
+      const double qk = b <= P ? qv[k] : qd[b - 1 - P][k];
+      double v = wb[wi] * qk;
       for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-      if (lane == 0) a.chunk_sums[((int64_t)chunk * B + b) * 8 + k] = v;
+      if (lane == 0) a.chunk_sums[((int64_t)chunk * stride + b) * 8 + k] = v;
+      if (adaptive) {
+        double e = wbd[wi] * qk;
+        for (int off = 8; off > 0; off >>= 1) e += __shfl_xor_sync(0xffffffffu, e, off);
+        const double other = __shfl_sync(0xffffffffu, e, 16);
+        if (lane == 0)
+          a.chunk_sums[((int64_t)chunk * stride + B + b) * 8 + k] = fabs(e) + fabs(other);
+      }
     }
   }
 }
@@ -476,9 +492,10 @@ __global__ void __launch_bounds__(128) pass1_kernel(Pass1Args a) {
   if (st == 0 && n + 2 > cap) st = 1;
   a.status[t] = st;
   a.n_terms[t] = st == 0 ? n : 0;
-  double* q = a.q + 6 * t;
+  const int nq = a.deriv ? 16 : 6;
+  double* q = a.q + nq * t;
   if (st != 0) {
-    for (int k = 0; k < 6; ++k) q[k] = 0.0;
+    for (int k = 0; k < nq; ++k) q[k] = 0.0;
     return;
   }
   Scratch s;
@@ -488,7 +505,28 @@ __global__ void __launch_bounds__(128) pass1_kernel(Pass1Args a) {
   mie_prepare(x, ms[L - 1], n, s);
   ValueSums vs;
   double asum;
-  if (L == 1) {
+  if (L == 1 && a.deriv) {
+    // The derivatives of the pass-1 quantities along Re m and Im m (engine.rs:447-461).
+    DerivSums ds;
+    MDeriv md;
+    NoLayers none;
+    asum = mie_finish(
+        x, ms[0], n, s, vs,
+        [&](int64_t k, cplx an, cplx bn, cplx dan, cplx dbn) { ds.add(k, an, bn, dan, dbn); },
+        none, &md);
+    ds.close(n);
+    const Eff e = efficiencies_from(x, asum, vs);
+    const double area = kPi * r * r;
+    for (int p = 0; p < 2; ++p) {
+      const Eff d = efficiency_derivs(x, vs, e, ds, p, p == 0 ? md.abs_re : md.abs_im);
+      double* o = q + 6 + 5 * p;
+      o[0] = area * d.q_ext;
+      o[1] = area * d.q_sca;
+      o[2] = area * (d.q_sca * e.g + e.q_sca * d.g);
+      o[3] = area * d.q_back;
+      o[4] = area * d.q_abs;
+    }
+  } else if (L == 1) {
     asum = mie_finish(x, ms[0], n, s, vs, [](int64_t, cplx, cplx) {});
   } else {
     Layered lay;

@@ -61,6 +61,7 @@ struct Smem {
   double xs[2][KB][128];   // [stage][order][4 columns x 32 nodes]
   double w[32], cu[32], area[32], sc[32];
   double wth[3][32];  // the distribution parameters' weights (derivatives only)
+  double wd[32], wthd[3][32];  // adaptive derivatives: the error weights (w_K - w_G) ...
   double S[8];
   int slot;
 };
@@ -354,14 +355,16 @@ __device__ __forceinline__ void chunk_elements(const Smem& sm, const double accE
 // block blk: values (weight w), the distribution's parameters (their weights), Re m and Im m
 // (weight w, the element derivatives along dS/dm and i dS/dm; phase.rs:322-335), reduced over
 // the 16 spheres as chunk_elements does.
-template <bool kUser>
+// kDiff: with the error weights (w_K - w_G) ... instead.
+template <bool kUser, bool kDiff = false>
 __device__ __forceinline__ void chunk_elements_d(const Smem& sm, const double accE[4][8],
                                                  const double accO[4][8], int half, int blk,
                                                  int n_theta, double v[2]) {
   const int ng = threadIdx.x & 15;
   const int node = 16 * half + ng;
   const int kind = blk == 0 ? 0 : (blk <= n_theta ? 0 : blk - n_theta);  // 0 f, 1 Re m, 2 Im m
-  const double wt = (blk >= 1 && blk <= n_theta) ? sm.wth[blk - 1][node] : sm.w[node];
+  const double wt = kDiff ? ((blk >= 1 && blk <= n_theta) ? sm.wthd[blk - 1][node] : sm.wd[node])
+                          : ((blk >= 1 && blk <= n_theta) ? sm.wth[blk - 1][node] : sm.w[node]);
   const double cu = sm.cu[node], ar = sm.area[node], sc = sm.sc[node];
   double p[32];
 #pragma unroll
@@ -433,10 +436,13 @@ __device__ __forceinline__ void chunk_errors(const Smem& sm, const double accE[4
   v[1] = out[1];
 }
 
-// kMode 0: values; 1: with the derivative blocks; 2: adaptive panels (values and errors).
+// kMode 0: values; 1: with the derivative blocks; 2: adaptive panels (values and errors);
+// 3: adaptive panels with the derivative blocks (each block's sums, then its error sums: every
+// 16-node half of a chunk is one panel).
 template <int kMode>
 __device__ __forceinline__ void unit_body(const UnitArgs& a) {
-  constexpr bool kDeriv = kMode == 1;
+  constexpr bool kDeriv = kMode == 1 || kMode == 3;
+  constexpr bool kAdD = kMode == 3;
   extern __shared__ __align__(16) unsigned char unit_raw[];
   Smem& sm = *reinterpret_cast<Smem*>(unit_raw);
   const int t = threadIdx.x, rg = t >> 4, ng = t & 15;
@@ -446,7 +452,7 @@ __device__ __forceinline__ void unit_body(const UnitArgs& a) {
   // Blocks of sums: the values, then (with derivatives) each distribution parameter, Re m and
   // Im m; halves: a chunk's coefficient rows are one 32-node tile, or two of 16 nodes with
   // their derivative columns.
-  const int n_blk = kDeriv ? 3 + a.n_theta : (kMode == 2 ? 2 : 1);
+  const int n_blk = kDeriv ? 3 + a.n_theta : (kMode == 2 ? 2 : 1);  // blocks of sums computed
   constexpr int kHalves = kDeriv ? 2 : 1;
   for (;;) {
     if (t == 0) sm.slot = atomicAdd(a.work_counter, 1);
@@ -469,8 +475,8 @@ __device__ __forceinline__ void unit_body(const UnitArgs& a) {
       if (it.group >= t_user + t_band) continue;
       if (t < 32) {
         const int j = c * 32 + t;
-        double w = 0.0, cu = 0.0, ar = 0.0, sc = 0.0;
-        double wth[3] = {0.0, 0.0, 0.0};
+        double w = 0.0, cu = 0.0, ar = 0.0, sc = 0.0, wd = 0.0;
+        double wth[3] = {0.0, 0.0, 0.0}, wthd[3] = {0.0, 0.0, 0.0};
         const int64_t node = (a.per_unit ? unit : d) * a.n_nodes + j;
         if (j < a.n_nodes && a.radius[node] > 0.0) {
           const double r = a.radius[node];
@@ -482,6 +488,10 @@ __device__ __forceinline__ void unit_body(const UnitArgs& a) {
           if (kDeriv)
             for (int p = 0; p < a.n_theta; ++p) wth[p] = a.wtheta[node * 3 + p];
           if (kMode == 2) wth[0] = a.wdiff[node];
+          if (kAdD) {
+            wd = a.wdiff[node];
+            for (int p = 0; p < a.n_theta; ++p) wthd[p] = a.wthdiff[node * 3 + p];
+          }
         }
         sm.w[t] = w;
         sm.cu[t] = cu;
@@ -489,6 +499,10 @@ __device__ __forceinline__ void unit_body(const UnitArgs& a) {
         sm.sc[t] = sc;
         if (kDeriv || kMode == 2)
           for (int p = 0; p < 3; ++p) sm.wth[p][t] = wth[p];
+        if (kAdD) {
+          sm.wd[t] = wd;
+          for (int p = 0; p < 3; ++p) sm.wthd[p][t] = wthd[p];
+        }
       }
       __syncthreads();
       for (int half = 0; half < kHalves; ++half) {
@@ -554,6 +568,19 @@ __device__ __forceinline__ void unit_body(const UnitArgs& a) {
                 ab[o_e0 * len + j] += v[0];
                 ab[(o_e0 + 1) * len + j] += v[1];
               }
+              if constexpr (kAdD) {
+                // The panel's |Kronrod - Gauss| into the block's error sums.
+                double ve[2];
+                if (user)
+                  chunk_elements_d<true, true>(sm, accE, accO, half, blk, a.n_theta, ve);
+                else
+                  chunk_elements_d<false, true>(sm, accE, accO, half, blk, a.n_theta, ve);
+                if (j >= 0) {
+                  double* ab = base + (int64_t)(n_blk + blk) * 4 * len;
+                  ab[o_e0 * len + j] += fabs(ve[0]);
+                  ab[(o_e0 + 1) * len + j] += fabs(ve[1]);
+                }
+              }
             }
           }
         }
@@ -577,6 +604,9 @@ __global__ void __launch_bounds__(NT) unit_deriv_kernel(UnitArgs a) { unit_body<
 // Adaptive panels: per tile the values' sums and the sums of |Kronrod - Gauss| per panel.
 __global__ void __launch_bounds__(NT) unit_adaptive_kernel(UnitArgs a) { unit_body<2>(a); }
 
+// Adaptive panels with the derivative blocks: per tile every block's sums and error sums.
+__global__ void __launch_bounds__(NT) unit_adaptive_deriv_kernel(UnitArgs a) { unit_body<3>(a); }
+
 // K-d: the Greek coefficients of each band slot, (2l+1)/2 sum_k w_k F(mu_k) d_l(mu_k) with F
 // the slot's averaged tables (fast.rs:238-253): a contraction over the band's n_q nodes shared
 // by a tile of up to 32 slots. Lane s of each warp holds slot s; warp w the orders
@@ -590,9 +620,40 @@ struct ProjSmem {
   double ds[4][PQ][PL];  // d00, d22, d2-2, d02 (scaled) per node and order
   double rz[32];         // 1/Z per slot
   double z[32], ez[32], tr[32];  // adaptive: Z, its error, the truncation term
+  double dz[32], edz[32];        // adaptive derivatives: the slot's Z_p and its error
+  int blk[32];                   // adaptive derivatives: the slot's block
   int64_t offs[32];
 };
 }  // namespace
+
+// An adaptive call's table element o of slot s along its block b (engine.rs:1782-1836): the
+// part's average (values) or its first-order error estimate (bounds), from the block's sums
+// and error sums and the values' (a unit's slots per band: B value slots, then B error slots,
+// 4 n_q doubles each). v = S_0/Z, e = (E_0 + |v| e_Z)/Z + t |v|; a parameter p:
+// dv = (S_p - v Z_p)/Z, (E_p + |v| e_Zp + |dv| e_Z + e |Z_p|)/Z + t |dv|; along m: dv = S_m/Z,
+// (E_m + |dv| e_Z)/Z + t |dv|.
+__device__ __forceinline__ double ad_table(const ProjArgs& a, const ProjSmem& sm, int s,
+                                           int64_t o, int q, bool bounds) {
+  const int b = sm.blk[s], B = a.ad_blocks;
+  const int64_t q4 = 4 * (int64_t)q;
+  const double z = sm.z[s], ez = sm.ez[s], tr = sm.tr[s], dz = sm.dz[s], edz = sm.edz[s];
+  if (!bounds) {
+    const double v0 = a.acc[o - b * q4] / z;
+    if (b == 0) return v0;
+    if (b <= a.n_theta) return (a.acc[o] - v0 * dz) / z;
+    return a.acc[o] / z;
+  }
+  const double v0 = a.acc[o - (B + b) * q4] / z, av0 = fabs(v0);
+  const double e0 = (a.acc[o - b * q4] + av0 * ez) / z + tr * av0;
+  if (b == 0) return e0;
+  const double sb = a.acc[o - B * q4], eb = a.acc[o];
+  if (b <= a.n_theta) {
+    const double dv = (sb - v0 * dz) / z;
+    return (eb + av0 * edz + fabs(dv) * ez + e0 * fabs(dz)) / z + tr * fabs(dv);
+  }
+  const double dv = sb / z;
+  return (eb + fabs(dv) * ez) / z + tr * fabs(dv);
+}
 
 __global__ void __launch_bounds__(PT) proj_kernel(ProjArgs a) {
   extern __shared__ __align__(16) unsigned char proj_raw[];
@@ -610,10 +671,17 @@ __global__ void __launch_bounds__(PT) proj_kernel(ProjArgs a) {
       if (t < it.count) {
         const BandSlot bs = a.slots[a.slot_index[it.first + t]];
         if (a.unit_norm) {
-          const double* un = a.unit_norm + 8 * (int64_t)a.units[bs.unit];
+          const int stride = a.ad_blocks > 0 ? kNormStrideD : 8;
+          const double* un = a.unit_norm + stride * (int64_t)a.units[bs.unit];
           sm.z[t] = un[0];
           sm.ez[t] = un[1];
           sm.tr[t] = un[2];
+          if (a.ad_blocks > 0) {
+            const int b = bs.pad, p = b - 1;
+            sm.blk[t] = b;
+            sm.dz[t] = (b >= 1 && b <= a.n_theta) ? un[8 + p] : 0.0;
+            sm.edz[t] = (b >= 1 && b <= a.n_theta) ? un[11 + p] : 0.0;
+          }
         } else if (a.raw) {
           rz = 1.0;
         } else {
@@ -644,7 +712,9 @@ __global__ void __launch_bounds__(PT) proj_kernel(ProjArgs a) {
           const int64_t off = sm.offs[s];
           if (kk < kn && off >= 0) {
             const int64_t o = off + (int64_t)e * q + k0 + kk;
-            if (!a.unit_norm) {
+            if (a.ad_blocks > 0) {
+              v = ad_table(a, sm, s, o, q, bounds);
+            } else if (!a.unit_norm) {
               v = a.acc[o] * sm.rz[s];
             } else if (!bounds) {
               v = a.acc[o] / sm.z[s];
@@ -1002,6 +1072,105 @@ __global__ void __launch_bounds__(NT) final_adaptive_kernel(FinalArgs a) {
   }
 }
 
+// Stage 1 of an adaptive call with derivatives: each (part, wavelength) unit's averages along
+// every block b < B (values, each distribution parameter, Re m, Im m) with their error
+// estimates into `avg`, block after block: 8 scalars, 4 n_mu cosine values, 6 (L + 1) Greek
+// coefficients, then the same for the errors (engine.rs:1782-1836 with the quotient rule of
+// the parameter blocks). <r^2> and <r^3> and their parameter derivatives come from the moments
+// (a single radius keeps its own; 0 along m). The Greek sums are already averaged per slot.
+__global__ void __launch_bounds__(NT) final_adaptive_d_kernel(FinalArgs a) {
+  __shared__ double S[12][8];
+  const int t = threadIdx.x;
+  const int L = a.greek_order;
+  const int glen = L >= 0 ? L + 1 : 0;
+  const int B = a.ad_blocks, nth = a.n_theta;
+  const int64_t row = 8 + 4 * (int64_t)a.n_mu + 6 * (int64_t)glen;
+  for (int ul = blockIdx.x; ul < a.n_units; ul += gridDim.x) {
+    const int64_t unit = a.units[ul];
+    if (t < 16 * B) {
+      const int b = t / 8, k = t % 8;
+      double s = 0.0;
+      for (int c = 0; c < a.cpu; ++c)
+        s += a.chunk_sums[(((int64_t)ul * a.cpu + c) * 2 * B + b) * 8 + k];
+      S[b][k] = s;
+    }
+    __syncthreads();
+    const double* un = a.unit_norm + kNormStrideD * unit;
+    const double z = un[0], ez = un[1], tr = un[2];
+    const bool point = un[3] != 0.0;
+    // One element's average and error along block b from its sums (s0, e0: the values';
+    // sb, eb: the block's).
+    auto avg = [&](int b, double s0, double e0, double sb, double eb, double* v, double* e) {
+      const double v0 = s0 / z, av0 = fabs(v0);
+      const double er0 = (e0 + av0 * ez) / z + tr * av0;
+      if (b == 0) {
+        *v = v0;
+        *e = er0;
+      } else if (b <= nth) {
+        const double dz = un[8 + b - 1], edz = un[11 + b - 1];
+        const double dv = (sb - v0 * dz) / z;
+        *v = dv;
+        *e = (eb + av0 * edz + fabs(dv) * ez + er0 * fabs(dz)) / z + tr * fabs(dv);
+      } else {
+        const double dv = sb / z;
+        *v = dv;
+        *e = (eb + fabs(dv) * ez) / z + tr * fabs(dv);
+      }
+    };
+    double* out = a.avg + 2 * B * row * unit;
+    for (int idx = t; idx < 8 * B; idx += NT) {
+      const int b = idx / 8, k = idx % 8;
+      double v, e;
+      avg(b, S[0][k], S[B][k], S[b][k], S[B + b][k], &v, &e);
+      if (!point && k >= 6) {
+        const int m = k - 6;
+        if (b == 0) {
+          v = un[4 + 2 * m];
+          e = un[5 + 2 * m];
+        } else if (b <= nth) {
+          v = un[14 + 4 * (b - 1) + 2 * m];
+          e = un[15 + 4 * (b - 1) + 2 * m];
+        } else {
+          v = 0.0;
+          e = 0.0;
+        }
+      }
+      out[2 * b * row + k] = v;
+      out[(2 * b + 1) * row + k] = e;
+    }
+    const double* acc_user = a.acc + a.unit_acc[ul];
+    const int64_t tl = 4 * (int64_t)a.n_mu;
+    for (int64_t idx = t; idx < tl * B; idx += NT) {
+      const int b = (int)(idx / tl);
+      const int64_t j = idx % tl;
+      double v, e;
+      avg(b, acc_user[j], acc_user[B * tl + j], acc_user[b * tl + j], acc_user[(B + b) * tl + j],
+          &v, &e);
+      out[2 * b * row + 8 + j] = v;
+      out[(2 * b + 1) * row + 8 + j] = e;
+    }
+    if (glen > 0) {
+      // The unit's slots per band: B value slots, then B error slots.
+      const int2 sl = a.unit_slots[ul];
+      for (int64_t idx = t; idx < 6 * (int64_t)glen * B; idx += NT) {
+        const int b = (int)(idx / (6 * glen));
+        const int g = (int)(idx % (6 * glen)), e = g / glen, l = g % glen;
+        double gv = 0.0, ge = 0.0;
+        for (int k = 0; k + 2 * B <= sl.y; k += 2 * B) {
+          const BandSlot bs = a.slots[sl.x + k];
+          if (l <= a.bands[bs.band].order) {
+            gv += a.slot_greek[(int64_t)(sl.x + k + b) * 6 * glen + (int64_t)e * glen + l];
+            ge += a.slot_greek[(int64_t)(sl.x + k + B + b) * 6 * glen + (int64_t)e * glen + l];
+          }
+        }
+        out[2 * b * row + 8 + tl + g] = gv;
+        out[(2 * b + 1) * row + 8 + tl + g] = ge;
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // Stage 2: each output unit (o, wavelength i) mixes its parts' averages with their number
 // fractions f (engine.rs:2121-2176: values and errors alike, in part order) and assembles the
 // outputs: ratios, normalizations and bounds of ensemble/lin.rs, Greek normalized by the
@@ -1096,7 +1265,7 @@ static void configure_units() {
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev >= 0 && dev < 64 && !configured[dev]) {
-    for (auto f : {unit_kernel, unit_deriv_kernel, unit_adaptive_kernel})
+    for (auto f : {unit_kernel, unit_deriv_kernel, unit_adaptive_kernel, unit_adaptive_deriv_kernel})
       cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Smem));
     configured[dev] = true;
   }
@@ -1111,7 +1280,9 @@ int unit_kernel_blocks_per_sm() {
 
 void launch_units(const UnitArgs& a, int grid, cudaStream_t s) {
   configure_units();
-  if (a.deriv)
+  if (a.deriv && a.wdiff)
+    unit_adaptive_deriv_kernel<<<grid, NT, sizeof(Smem), s>>>(a);
+  else if (a.deriv)
     unit_deriv_kernel<<<grid, NT, sizeof(Smem), s>>>(a);
   else if (a.wdiff)
     unit_adaptive_kernel<<<grid, NT, sizeof(Smem), s>>>(a);
@@ -1135,7 +1306,9 @@ void launch_proj(const ProjArgs& a, cudaStream_t s) {
 
 void launch_final(const FinalArgs& a, cudaStream_t s) {
   int grid = a.n_units < 4096 ? a.n_units : 4096;
-  if (a.d_values)
+  if (a.ad_blocks > 0)
+    final_adaptive_d_kernel<<<grid, NT, 0, s>>>(a);
+  else if (a.d_values)
     final_deriv_kernel<<<grid, NT, 0, s>>>(a);
   else if (a.unit_norm)
     final_adaptive_kernel<<<grid, NT, 0, s>>>(a);
