@@ -126,11 +126,21 @@ int scatrs_ensemble_fixed_d(const scatrs_distribution* dists, int64_t n_dist,
 typedef struct scatrs_adaptive_options {
   double rtol;                /* relative tolerance of the size integration, in [1e-13, 0.1] */
   int64_t max_panels;         /* panels per part and wavelength, >= 1 */
-  int32_t greek_order;        /* highest Greek order L, or -1 for none */
+  int32_t greek_order;        /* highest Greek order L, -1 for none, or SCATRS_GREEK_ALL */
   int32_t normalized;         /* 1: normalized phase matrix and Greek coefficients */
   int32_t allow_unvalidated;  /* 1: compute outside the Mie validated domain */
   int32_t refine_backscatter; /* 1: also refine on <C_back> */
 } scatrs_adaptive_options;
+
+/* greek_order = SCATRS_GREEK_ALL (GreekOrder::All, ensemble/mod.rs:163-170): every order up to
+ * 2 N_max at each wavelength (N_max the largest number of terms there), spheres and layered
+ * spheres. The call then leaves its greek arrays unwritten; the coefficients of the calling
+ * thread's last such call come from scatrs_greek_all_take, (6, n, W) and with derivatives
+ * (P, 6, n, W) as the call's other outputs, W = scatrs_greek_all_width() the longest plus one,
+ * zero above each wavelength's order (scatrs-py/src/ensemble.rs:419-429). */
+#define SCATRS_GREEK_ALL (-2)
+int64_t scatrs_greek_all_width(void);
+int scatrs_greek_all_take(double* greek, double* greek_err, double* d_greek, double* d_greek_err);
 
 /*
  * The adaptive ensemble of spheres, the reference's default integration: per distribution

@@ -275,6 +275,21 @@ def ensemble_fixed_d(dists: np.ndarray, wavelengths, m, n_nodes: int, mu=None,
 MONODISPERSE = 5
 
 
+def _take_all_orders(out: dict, n: int, P: int = 0) -> None:
+    """The Greek coefficients of the last greek_order="all" call, zero-padded to the longest."""
+    f = lib().orc_greek_all_width
+    f.restype = _I64
+    w = int(f())
+    g, ge = np.zeros((6, n, w)), np.zeros((6, n, w))
+    dg, dge = np.zeros((P, 6, n, w)), np.zeros((P, 6, n, w))
+    t = lib().orc_greek_all_take
+    t.argtypes = [_PD, _PD, _PD, _PD]
+    t(_p(g), _p(ge), _p(dg) if P else None, _p(dge) if P else None)
+    out["greek"], out["greek_err"] = g, ge
+    if P:
+        out["greek_d"], out["greek_d_err"] = dg, dge
+
+
 def ensemble_adaptive(dists: np.ndarray, wavelengths, m, mu=None, greek_order=None,
                       normalized: bool = True, rtol: float = 1e-6, max_panels: int = 4096,
                       allow_unvalidated: bool = False, refine_backscatter: bool = False,
@@ -288,7 +303,7 @@ def ensemble_adaptive(dists: np.ndarray, wavelengths, m, mu=None, greek_order=No
     m = np.ascontiguousarray(np.broadcast_to(np.asarray(m, dtype=np.complex128), wl.shape))
     mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
     n = dists.size * wl.size
-    L = -1 if greek_order is None else int(greek_order)
+    L = -1 if greek_order is None else (-2 if greek_order == "all" else int(greek_order))
     out = {"values": np.zeros((11, n)), "errors": np.zeros((11, n)),
            "converged": np.zeros(n, dtype=np.int8), "panels": np.zeros(n, dtype=np.int64)}
     ph = pe = g = ge = None
@@ -313,6 +328,8 @@ def ensemble_adaptive(dists: np.ndarray, wavelengths, m, mu=None, greek_order=No
         out["phase"], out["phase_err"] = ph, pe
     if g is not None:
         out["greek"], out["greek_err"] = g, ge
+    if L == -2:
+        _take_all_orders(out, n)
     return out
 
 
@@ -517,7 +534,7 @@ def ensemble_mixture_d(components, wavelengths, derivs, mu=None, greek_order=Non
     P = pr.size
     mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
     n = wl.size
-    L = -1 if greek_order is None else int(greek_order)
+    L = -1 if greek_order is None else (-2 if greek_order == "all" else int(greek_order))
     out = {"values": np.zeros((11, n)), "errors": np.zeros((11, n)),
            "d": np.zeros((P, 11, n)), "d_err": np.zeros((P, 11, n)),
            "converged": np.zeros(n, dtype=np.int8), "panels": np.zeros(n, dtype=np.int64)}
@@ -547,6 +564,8 @@ def ensemble_mixture_d(components, wavelengths, derivs, mu=None, greek_order=Non
         out["phase"], out["phase_err"], out["phase_d"], out["phase_d_err"] = ph, pe, dph, dpe
     if g is not None:
         out["greek"], out["greek_err"], out["greek_d"], out["greek_d_err"] = g, ge, dg, dge
+    if L == -2:
+        _take_all_orders(out, n, P)
     return out
 
 

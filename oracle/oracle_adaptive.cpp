@@ -39,6 +39,24 @@ constexpr double MIN_WIDTH = 1e-10;
 constexpr double MAX_DX = 20.0;
 constexpr size_t MOMENT_MAX_PANELS = 100000;
 constexpr int MONODISPERSE = 5;
+constexpr int64_t GREEK_ALL = -2;  // every order up to 2 N_max at each wavelength
+
+// The Greek coefficients of the last call with GREEK_ALL, per output unit (its own length),
+// and with derivatives per parameter.
+struct AllOrders {
+  std::vector<std::vector<double>> g, ge, dg, dge;
+  size_t P = 0;
+};
+AllOrders g_all_orders;
+void keep_all_orders(std::vector<std::vector<double>>& g, std::vector<std::vector<double>>& ge,
+                     std::vector<std::vector<double>>& dg, std::vector<std::vector<double>>& dge,
+                     size_t P) {
+  g_all_orders.g.swap(g);
+  g_all_orders.ge.swap(ge);
+  g_all_orders.dg.swap(dg);
+  g_all_orders.dge.swap(dge);
+  g_all_orders.P = P;
+}
 constexpr double INF = std::numeric_limits<double>::infinity();
 
 // Pass-1 quantities (engine.rs:43-54): 1, C_ext, C_sca, C_sca g, C_back, C_abs.
@@ -1231,6 +1249,7 @@ std::vector<UnitOut> wavelength(const std::vector<Part>& parts,
     n_max = std::max(n_max, p1.n_terms);
     firsts.push_back(std::move(p1));
   }
+  if (order == GREEK_ALL) order = 2 * n_max;  // GreekOrder::All (engine.rs:2016-2020)
   std::vector<int> group_of(parts.size()), place(parts.size());
   for (size_t gi = 0; gi < groups.size(); ++gi)
     for (size_t k = 0; k < groups[gi].size(); ++k) {
@@ -1678,6 +1697,8 @@ static int adaptive_impl(const FixedDist* dists, int64_t n_dist, int batch, cons
   }
   const int64_t n_calls = (int64_t)groups_of.size();
   const int64_t glen = greek_order >= 0 ? greek_order + 1 : 0;
+  const bool all = greek_order == GREEK_ALL;
+  std::vector<std::vector<double>> all_g(all ? n_units : 0), all_ge(all_g.size()), none;
   std::vector<Failure> fails(n_calls * n_wl, Failure{OK, ""});
   if (n_threads > 0) omp_set_num_threads(n_threads);
 #pragma omp parallel for schedule(dynamic, 1)
@@ -1706,6 +1727,10 @@ static int adaptive_impl(const FixedDist* dists, int64_t n_dist, int batch, cons
               greek[(el * n_units + unit) * glen + l] = u.greek[el * glen + l];
               greek_err[(el * n_units + unit) * glen + l] = u.greek_err[el * glen + l];
             }
+        if (all) {
+          all_g[unit] = u.greek;
+          all_ge[unit] = u.greek_err;
+        }
         converged[unit] = u.converged ? 1 : 0;
         panels[unit] = u.panels;
       }
@@ -1713,11 +1738,38 @@ static int adaptive_impl(const FixedDist* dists, int64_t n_dist, int batch, cons
       fails[job] = f;
     }
   }
+  if (all) keep_all_orders(all_g, all_ge, none, none, 0);
   // The first error in (wavelength, call) order, as the reference reports the first in order.
   for (int64_t i = 0; i < n_wl; ++i)
     for (int64_t c = 0; c < n_calls; ++c)
       if (fails[c * n_wl + i].status != OK) return fail(fails[c * n_wl + i]);
   return OK;
+}
+
+// The last GREEK_ALL call's Greek coefficients: the width (the longest order plus one), and the
+// arrays (6, n, width) and (P, 6, n, width), zero above each unit's order.
+int64_t orc_greek_all_width() {
+  size_t w = 1;
+  for (auto& g : g_all_orders.g) w = std::max(w, g.size() / 6);
+  return (int64_t)w;
+}
+
+void orc_greek_all_take(double* greek, double* greek_err, double* d_greek, double* d_greek_err) {
+  const AllOrders& a = g_all_orders;
+  const int64_t n = (int64_t)a.g.size(), w = orc_greek_all_width(), P = (int64_t)a.P;
+  for (int64_t u = 0; u < n; ++u) {
+    const int64_t len = (int64_t)a.g[u].size() / 6;
+    for (int el = 0; el < 6; ++el)
+      for (int64_t l = 0; l < w; ++l) {
+        const bool in = l < len;
+        greek[(el * n + u) * w + l] = in ? a.g[u][el * len + l] : 0.0;
+        greek_err[(el * n + u) * w + l] = in ? a.ge[u][el * len + l] : 0.0;
+        for (int64_t c = 0; c < P && d_greek; ++c) {
+          d_greek[((c * 6 + el) * n + u) * w + l] = in ? a.dg[u][(c * 6 + el) * len + l] : 0.0;
+          d_greek_err[((c * 6 + el) * n + u) * w + l] = in ? a.dge[u][(c * 6 + el) * len + l] : 0.0;
+        }
+      }
+  }
 }
 
 int orc_ensemble_adaptive(const FixedDist* dists, int64_t n_dist, int batch, const double* wl,
@@ -1851,6 +1903,9 @@ int orc_ensemble_mixture_d(const FixedDist* modes, const double* mode_w, const i
   std::vector<std::vector<int>> units{unit};
   const int64_t glen = greek_order >= 0 ? greek_order + 1 : 0;
   const int64_t P = n_params;
+  const bool all = greek_order == GREEK_ALL;
+  std::vector<std::vector<double>> all_g(all ? n_wl : 0), all_ge(all_g.size()),
+      all_dg(all_g.size()), all_dge(all_g.size());
   std::vector<Failure> fails(n_wl, Failure{OK, ""});
 #pragma omp parallel for schedule(dynamic, 1)
   for (int64_t i = 0; i < n_wl; ++i) {
@@ -1888,12 +1943,19 @@ int orc_ensemble_mixture_d(const FixedDist* modes, const double* mode_w, const i
                   u.d_greek_err[(c * 6 + el) * glen + l];
             }
           }
+      if (all) {
+        all_g[i] = u.greek;
+        all_ge[i] = u.greek_err;
+        all_dg[i] = u.d_greek;
+        all_dge[i] = u.d_greek_err;
+      }
       converged[i] = u.converged ? 1 : 0;
       panels[i] = u.panels;
     } catch (const Failure& f) {
       fails[i] = f;
     }
   }
+  if (all) keep_all_orders(all_g, all_ge, all_dg, all_dge, (size_t)P);
   for (int64_t i = 0; i < n_wl; ++i)
     if (fails[i].status != OK) return fail(fails[i]);
   return OK;

@@ -124,6 +124,8 @@ SYMBOLS = {
     "scatrs_ensemble_mixture": (ctypes.c_int, [ctypes.POINTER(Component), _I64, _PD, _I64, _PD,
                                                _I64, ctypes.POINTER(AdaptiveOptions), _PD, _PD,
                                                _PD, _PD, _PD, _PD, _VP, _VP, _CP, _SZ]),
+    "scatrs_greek_all_width": (_I64, []),
+    "scatrs_greek_all_take": (ctypes.c_int, [_PD, _PD, _PD, _PD]),
     "scatrs_ensemble_mixture_d": (ctypes.c_int, [ctypes.POINTER(Component), _I64, _PD, _I64, _PD,
                                                  _I64, ctypes.POINTER(AdaptiveOptions), _VP, _I64]
                                   + [_PD] * 12 + [_VP, _VP, _CP, _SZ]),
@@ -364,6 +366,8 @@ def ensemble_adaptive(dists: np.ndarray, wavelengths, m, mu=None, greek_order: i
         out["phase"], out["phase_err"] = ph, pe
     if g is not None:
         out["greek"], out["greek_err"] = g, ge
+    if L == GREEK_ALL:
+        _take_all_orders(out, n)
     return out
 
 
@@ -405,6 +409,8 @@ def ensemble_adaptive_layered(dists: np.ndarray, wavelengths, fractions, m_layer
         out["phase"], out["phase_err"] = ph, pe
     if g is not None:
         out["greek"], out["greek_err"] = g, ge
+    if L == GREEK_ALL:
+        _take_all_orders(out, n)
     return out
 
 
@@ -487,7 +493,24 @@ def ensemble_mixture(components, wavelengths, mu=None, greek_order: int = -1,
         out["phase"], out["phase_err"] = ph, pe
     if g is not None:
         out["greek"], out["greek_err"] = g, ge
+    if L == GREEK_ALL:
+        _take_all_orders(out, n)
     return out
+
+
+GREEK_ALL = -2  # every order up to 2 N_max per wavelength (adaptive calls)
+
+
+def _take_all_orders(out: dict, n: int, P: int = 0) -> None:
+    """The Greek coefficients of this thread's last GREEK_ALL call into out, (6, n, W) and
+    with derivatives (P, 6, n, W)."""
+    w = int(load().scatrs_greek_all_width())
+    g, ge = np.zeros((6, n, w)), np.zeros((6, n, w))
+    dg, dge = np.zeros((P, 6, n, w)), np.zeros((P, 6, n, w))
+    load().scatrs_greek_all_take(_p(g), _p(ge), _p(dg) if P else None, _p(dge) if P else None)
+    out["greek"], out["greek_err"] = g, ge
+    if P:
+        out["greek_d"], out["greek_d_err"] = dg, dge
 
 
 # scatrs_param: (component, mode or -1, kind, index); kinds as SCATRS_PARAM_*.
@@ -543,6 +566,8 @@ def ensemble_mixture_d(components, wavelengths, params, mu=None, greek_order: in
         out["phase"], out["phase_err"], out["phase_d"], out["phase_d_err"] = ph, pe, dph, dpe
     if g is not None:
         out["greek"], out["greek_err"], out["greek_d"], out["greek_d_err"] = g, ge, dg, dge
+    if L == GREEK_ALL:
+        _take_all_orders(out, n, P)
     return out
 
 

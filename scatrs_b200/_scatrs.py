@@ -219,6 +219,14 @@ def _modes(spec):
     return _adaptive_dists([spec]), None
 
 
+def _greek_order(greek, all_orders) -> int:
+    """The C ABI's Greek order: -1 none, GREEK_ALL for greek='all' (every order up to 2 N_max
+    per wavelength, GreekOrder::All), else the order."""
+    if all_orders:
+        return _native.GREEK_ALL
+    return -1 if greek is None else int(greek)
+
+
 def ensemble_compute(items, wavelengths, mixture, greek, all_orders, mu, normalized, derivatives,
                      rtol, max_panels, allow_unvalidated, refine_backscatter) -> dict:
     """The reference's ``_scatrs.ensemble_compute`` on the GPU: one or more sphere components
@@ -230,11 +238,9 @@ def ensemble_compute(items, wavelengths, mixture, greek, all_orders, mu, normali
         return _compute_with_derivatives(items, wavelengths, mixture, greek, all_orders, mu,
                                          normalized, derivatives, rtol, max_panels,
                                          allow_unvalidated, refine_backscatter)
-    if all_orders:
-        raise InvalidInputError("greek='all' is not on the GPU path: give an order")
     wl = np.ascontiguousarray(wavelengths, dtype=np.float64).reshape(-1)
     mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
-    L = -1 if greek is None else int(greek)
+    L = _greek_order(greek, all_orders)
     kinds = {p[0] if isinstance(p, tuple) and p else None for _, p, _ in items}
     if "spheroid" in kinds:
         if len(items) != 1 or (isinstance(items[0][0], tuple) and items[0][0][0] == "multimodal"):
@@ -286,11 +292,9 @@ def _compute_with_derivatives(items, wavelengths, mixture, greek, all_orders, mu
             raise InvalidInputError(
                 f"the derivative along {names[i]} (a layered sphere's or a spheroid's) is not "
                 "on the adaptive GPU path: use the fixed grid")
-    if all_orders:
-        raise InvalidInputError("greek='all' is not on the GPU path: give an order")
     wl = np.ascontiguousarray(wavelengths, dtype=np.float64).reshape(-1)
     mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
-    L = -1 if greek is None else int(greek)
+    L = _greek_order(greek, all_orders)
     comps = []
     for spec, particle, weight in items:
         dists, mode_w = _modes(spec)
@@ -318,9 +322,9 @@ def ensemble_compute_batch(specs, particle_spec, wavelengths, greek, all_orders,
     one sphere material on shared panels per wavelength, rows distribution-major."""
     if not specs:
         raise InvalidInputError("a batch needs a distribution")
-    if all_orders:
-        raise InvalidInputError("greek='all' is not on the GPU path: give an order")
     wl = np.ascontiguousarray(wavelengths, dtype=np.float64).reshape(-1)
+    greek = _greek_order(greek, all_orders)
+    greek = None if greek == -1 else greek
     mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
     if isinstance(particle_spec, tuple) and particle_spec and particle_spec[0] == "spheroid":
         eps, m = _spheroid(particle_spec, wl.size)

@@ -1333,10 +1333,13 @@ void mix_derivatives(const std::vector<AdPart>& in, const std::vector<adaptive::
 // With dd (derivatives), pass 1 refines the requested parameters' blocks too, pass 2 runs the
 // derivative blocks of every part, and the mixing (with the weight derivatives) and the
 // outputs are assembled on the host from the parts' per-block averages.
-void adaptive_call(const std::vector<AdPart>& in, int n_out, bool batch, const double* wavelengths,
-                   int64_t n_wl, const double* mu, int64_t n_mu,
-                   const scatrs_adaptive_options* options, const AdOutputs& res,
-                   const scatrs_layers* layers = nullptr, const AdDerivs* dd = nullptr) {
+// With n_max_out, only pass 1 runs (and its errors are reported): n_max_out receives each
+// (part, wavelength) unit's largest number of terms, its group's (engine.rs:1987-2030).
+void adaptive_call_order(const std::vector<AdPart>& in, int n_out, bool batch,
+                         const double* wavelengths, int64_t n_wl, const double* mu, int64_t n_mu,
+                         const scatrs_adaptive_options* options, const AdOutputs& res,
+                         const scatrs_layers* layers = nullptr, const AdDerivs* dd = nullptr,
+                         std::vector<int64_t>* n_max_out = nullptr) {
   if (!options) throw Failure{SCATRS_INVALID_INPUT, "options must not be NULL"};
   if (n_wl < 0) throw Failure{SCATRS_INVALID_INPUT, "negative sizes"};
   const adaptive::Options o{options->rtol, options->max_panels, options->allow_unvalidated != 0,
@@ -1555,6 +1558,14 @@ void adaptive_call(const std::vector<AdPart>& in, int n_out, bool batch, const d
     }
     if (status != 0) throw Failure{status, msg};
   }
+  if (n_max_out) {
+    // Per (part, wavelength) unit: its group's largest number of terms (a point's own).
+    n_max_out->assign(n_units, 0);
+    for (int64_t u = 0; u < n_units; ++u)
+      if (job_of[u] >= 0) (*n_max_out)[u] = jobs[job_of[u]].n_terms;
+    for (size_t k = 0; k < points.size(); ++k) (*n_max_out)[point_unit[k]] = point_res[k].n;
+    return;
+  }
   // Pass 2: every unit's nodes, up to two panels per chunk of 32 (nodes 0-14 and 16-30), two
   // only when their projector bands agree, so that each panel's tables go to its own band
   // (engine.rs:1530-1543).
@@ -1735,6 +1746,171 @@ void adaptive_call(const std::vector<AdPart>& in, int n_out, bool batch, const d
     SB_CUDA(cudaMemcpyAsync(res.greek_err, g_d + gl, gl * 8, cudaMemcpyDeviceToHost, s));
   SB_CUDA(cudaStreamSynchronize(s));
   adaptive_flags(in, jobs, job_of, unit_converged, unit_panels, n_out, n_wl, res);
+}
+
+// The Greek coefficients of the thread's last greek="all" call, (6, n, width) and with
+// derivatives (P, 6, n, width), zero above each wavelength's order.
+struct GreekAll {
+  int64_t width = 0, n = 0, p = 0;
+  std::vector<double> g, ge, dg, dge;
+};
+thread_local GreekAll t_greek_all;
+
+// adaptive_call_order, and greek="all" (GreekOrder::All, engine.rs:2016-2020: every order up to
+// 2 N_max, N_max the largest number of terms of the call at that wavelength: every part of a
+// batch, else the output unit's own parts; ensemble.rs:419-429 pads the arrays to the longest):
+// pass 1 finds the N_max, then the wavelengths of one order run together at that order (all
+// output units of a batch, else each unit alone), so that each band projects to
+// min(2 N_max, 2 N_band) as the reference's. The coefficients go to t_greek_all.
+void adaptive_call(const std::vector<AdPart>& in, int n_out, bool batch, const double* wavelengths,
+                   int64_t n_wl, const double* mu, int64_t n_mu,
+                   const scatrs_adaptive_options* options, const AdOutputs& res,
+                   const scatrs_layers* layers = nullptr, const AdDerivs* dd = nullptr) {
+  if (!options || options->greek_order != SCATRS_GREEK_ALL) {
+    adaptive_call_order(in, n_out, batch, wavelengths, n_wl, mu, n_mu, options, res, layers, dd);
+    return;
+  }
+  scatrs_adaptive_options o1 = *options;
+  o1.greek_order = -1;
+  std::vector<int64_t> n_max;
+  adaptive_call_order(in, n_out, batch, wavelengths, n_wl, mu, n_mu, &o1, AdOutputs{}, layers,
+                      dd, &n_max);
+  const int64_t n_parts = (int64_t)in.size();
+  // Each output unit's order at each wavelength: 2 N_max over the parts of its call (a batch is
+  // one call over every part; otherwise each output unit is a call of its own).
+  std::vector<int64_t> order((size_t)n_out * n_wl, 0);
+  for (int64_t p = 0; p < n_parts && !n_max.empty(); ++p)
+    for (int64_t i = 0; i < n_wl; ++i)
+      for (int o = 0; o < n_out; ++o)
+        if (batch || in[p].out == o)
+          order[o * n_wl + i] = std::max(order[o * n_wl + i], 2 * n_max[p * n_wl + i]);
+  int64_t width = 1;
+  for (int64_t x : order) width = std::max(width, x + 1);
+  const int64_t n_outs = (int64_t)n_out * n_wl, P = dd ? dd->n : 0;
+  GreekAll& ga = t_greek_all;
+  ga.width = width;
+  ga.n = n_outs;
+  ga.p = P;
+  ga.g.assign(6 * n_outs * width, 0.0);
+  ga.ge.assign(ga.g.size(), 0.0);
+  ga.dg.assign(P * ga.g.size(), 0.0);
+  ga.dge.assign(ga.dg.size(), 0.0);
+  const int nl = layers && layers->n_layers > 1 ? layers->n_layers : 1;
+  // One call per set of output units run together (all of a batch, else each alone) and order.
+  std::vector<std::vector<int>> sets;
+  if (batch) {
+    sets.push_back({});
+    for (int o = 0; o < n_out; ++o) sets[0].push_back(o);
+  } else {
+    for (int o = 0; o < n_out; ++o) sets.push_back({o});
+  }
+  for (const std::vector<int>& outs : sets) {
+    std::map<int64_t, std::vector<int64_t>> by_order;
+    for (int64_t i = 0; i < n_wl; ++i) by_order[order[outs[0] * n_wl + i]].push_back(i);
+    // The set's parts, their output units renumbered.
+    std::vector<int64_t> ps;
+    for (int64_t p = 0; p < n_parts; ++p)
+      if (std::find(outs.begin(), outs.end(), in[p].out) != outs.end()) ps.push_back(p);
+    const int no = (int)outs.size(), np = (int)ps.size();
+    for (const auto& kv : by_order) {
+      const int64_t L = kv.first;
+      const std::vector<int64_t>& ws = kv.second;
+      const int64_t nw = (int64_t)ws.size(), ns = (int64_t)no * nw, glen = L + 1;
+      std::vector<double> wl_s(nw);
+      for (int64_t k = 0; k < nw; ++k) wl_s[k] = wavelengths[ws[k]];
+      std::vector<AdPart> in_s;
+      std::vector<std::vector<double>> m_s(np);
+      for (int q = 0; q < np; ++q) {
+        AdPart a = in[ps[q]];
+        a.out = (int)(std::find(outs.begin(), outs.end(), a.out) - outs.begin());
+        if (a.m) {
+          m_s[q].resize(2 * nw);
+          for (int64_t k = 0; k < nw; ++k) {
+            m_s[q][2 * k] = a.m[2 * ws[k]];
+            m_s[q][2 * k + 1] = a.m[2 * ws[k] + 1];
+          }
+          a.m = m_s[q].data();
+        }
+        in_s.push_back(a);
+      }
+      scatrs_layers lay_s{};
+      std::vector<double> ml_s, fr_s;
+      if (nl > 1) {
+        lay_s = *layers;
+        ml_s.resize(2 * (size_t)np * nl * nw);
+        fr_s.resize((size_t)np * (nl - 1));
+        for (int q = 0; q < np; ++q) {
+          for (int l = 0; l + 1 < nl; ++l) fr_s[q * (nl - 1) + l] = layers->fractions[ps[q] * (nl - 1) + l];
+          for (int l = 0; l < nl; ++l)
+            for (int64_t k = 0; k < nw; ++k)
+              for (int c = 0; c < 2; ++c)
+                ml_s[2 * ((q * nl + l) * nw + k) + c] =
+                    layers->m[2 * ((ps[q] * nl + l) * n_wl + ws[k]) + c];
+        }
+        lay_s.m = ml_s.data();
+        lay_s.fractions = fr_s.data();
+      }
+      std::vector<double> v(11 * ns), e(11 * ns), ph(6 * ns * n_mu), phe(ph.size()),
+          g(6 * ns * glen), ge(g.size()), dv(P * v.size()), de(dv.size()), dph(P * ph.size()),
+          dphe(dph.size()), dg(P * g.size()), dge(dg.size());
+      std::vector<int8_t> conv(ns);
+      std::vector<int64_t> pan(ns);
+      AdOutputs out_s{v.data(), e.data(), ph.data(), phe.data(), g.data(), ge.data(),
+                      conv.data(), pan.data()};
+      AdDerivs dd_s;
+      if (dd) {
+        dd_s = *dd;
+        dd_s.d_values = dv.data();
+        dd_s.d_errors = de.data();
+        dd_s.d_phase = dph.data();
+        dd_s.d_phase_err = dphe.data();
+        dd_s.d_greek = dg.data();
+        dd_s.d_greek_err = dge.data();
+      }
+      scatrs_adaptive_options o2 = *options;
+      o2.greek_order = (int32_t)L;
+      adaptive_call_order(in_s, no, batch, wl_s.data(), nw, mu, n_mu, &o2, out_s,
+                          nl > 1 ? &lay_s : nullptr, dd ? &dd_s : nullptr);
+      // Back to the call's output units and wavelengths.
+      for (int q = 0; q < no; ++q)
+        for (int64_t k = 0; k < nw; ++k) {
+          const int64_t x = q * nw + k, y = outs[q] * n_wl + ws[k];
+          for (int c2 = 0; c2 < 11; ++c2) {
+            res.values[c2 * n_outs + y] = v[c2 * ns + x];
+            if (res.errors) res.errors[c2 * n_outs + y] = e[c2 * ns + x];
+            for (int64_t c = 0; c < P; ++c) {
+              if (dd->d_values) dd->d_values[(c * 11 + c2) * n_outs + y] = dv[(c * 11 + c2) * ns + x];
+              if (dd->d_errors) dd->d_errors[(c * 11 + c2) * n_outs + y] = de[(c * 11 + c2) * ns + x];
+            }
+          }
+          for (int el = 0; el < 6; ++el) {
+            for (int64_t j = 0; j < n_mu; ++j) {
+              const int64_t a = (el * n_outs + y) * n_mu + j, b = (el * ns + x) * n_mu + j;
+              if (res.phase) res.phase[a] = ph[b];
+              if (res.phase_err) res.phase_err[a] = phe[b];
+              for (int64_t c = 0; c < P; ++c) {
+                const int64_t ad = ((c * 6 + el) * n_outs + y) * n_mu + j;
+                const int64_t bd = ((c * 6 + el) * ns + x) * n_mu + j;
+                if (dd->d_phase) dd->d_phase[ad] = dph[bd];
+                if (dd->d_phase_err) dd->d_phase_err[ad] = dphe[bd];
+              }
+            }
+            for (int64_t l = 0; l < glen; ++l) {
+              ga.g[(el * n_outs + y) * width + l] = g[(el * ns + x) * glen + l];
+              ga.ge[(el * n_outs + y) * width + l] = ge[(el * ns + x) * glen + l];
+              for (int64_t c = 0; c < P; ++c) {
+                ga.dg[((c * 6 + el) * n_outs + y) * width + l] =
+                    dg[((c * 6 + el) * ns + x) * glen + l];
+                ga.dge[((c * 6 + el) * n_outs + y) * width + l] =
+                    dge[((c * 6 + el) * ns + x) * glen + l];
+              }
+            }
+          }
+          if (res.converged) res.converged[y] = conv[x];
+          if (res.panels) res.panels[y] = pan[x];
+        }
+    }
+  }
 }
 
 // The driver's tensor-map encoder, found once through the runtime.
@@ -2240,6 +2416,8 @@ void adaptive_spheroid_call(const scatrs_distribution* dists, int64_t n_dist, bo
                             const scatrs_adaptive_options* options, const AdOutputs& res) {
   if (!options) throw Failure{SCATRS_INVALID_INPUT, "options must not be NULL"};
   if (n_dist < 0 || n_wl < 0) throw Failure{SCATRS_INVALID_INPUT, "negative sizes"};
+  if (options->greek_order == SCATRS_GREEK_ALL)
+    throw Failure{SCATRS_INVALID_INPUT, "greek='all' for spheroids is not on the GPU path"};
   const adaptive::Options o{options->rtol, options->max_panels, options->allow_unvalidated != 0,
                             options->refine_backscatter != 0};
   if (!(o.rtol >= 1e-13 && o.rtol <= 0.1)) {
@@ -3373,6 +3551,17 @@ int scatrs_mie(const double* x, const double* m, int64_t n, int32_t allow_unvali
     if (eff) SB_CUDA(cudaMemcpyAsync(eff, a.eff, 5 * n * 8, cudaMemcpyDeviceToHost, s));
     SB_CUDA(cudaStreamSynchronize(s));
   });
+}
+
+int64_t scatrs_greek_all_width(void) { return t_greek_all.width; }
+
+int scatrs_greek_all_take(double* greek, double* greek_err, double* d_greek, double* d_greek_err) {
+  const GreekAll& ga = t_greek_all;
+  if (greek) std::copy(ga.g.begin(), ga.g.end(), greek);
+  if (greek_err) std::copy(ga.ge.begin(), ga.ge.end(), greek_err);
+  if (d_greek) std::copy(ga.dg.begin(), ga.dg.end(), d_greek);
+  if (d_greek_err) std::copy(ga.dge.begin(), ga.dge.end(), d_greek_err);
+  return SCATRS_OK;
 }
 
 int scatrs_device_count(void) {

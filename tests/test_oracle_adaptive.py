@@ -153,3 +153,23 @@ def test_mixtures_average_with_the_number_weights():
                               greek_order=10)
     assert np.array_equal(bi["values"], both["values"])
     assert bi["panels"][0] == both["panels"][0]
+
+
+def test_all_orders_are_each_wavelengths_2n_max():
+    """GreekOrder::All (engine.rs:2016-2020): each wavelength projects to 2 N_max, its largest
+    number of terms, the arrays padded with zeros to the longest (scatrs-py ensemble.rs:419-429):
+    the same as that explicit order at that wavelength."""
+    d = O.dist(1, 0.3, 1.4)
+    wl = [0.4, 1.6]
+    mu = np.array([0.5, -0.5])
+    a = O.ensemble_adaptive(d, wl, 1.45 + 0.01j, mu=mu, greek_order="all")
+    w = a["greek"].shape[-1]
+    for i, lam in enumerate(wl):
+        g = a["greek"][0, i]
+        order = int(np.flatnonzero(g)[-1])  # the last nonzero alpha1: 2 N_max
+        assert order % 2 == 0 and np.all(a["greek"][:, i, order + 1:] == 0.0)
+        b = O.ensemble_adaptive(d, [lam], 1.45 + 0.01j, mu=mu, greek_order=order)
+        assert np.array_equal(a["greek"][:, i, :order + 1], b["greek"][:, 0])
+        assert np.array_equal(a["greek_err"][:, i, :order + 1], b["greek_err"][:, 0])
+        assert np.array_equal(a["values"][:, i], b["values"][:, 0])
+    assert w == order + 1 or w > order + 1
