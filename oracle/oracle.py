@@ -528,7 +528,30 @@ def ensemble_mixture_d(components, wavelengths, derivs, mu=None, greek_order=Non
     (P, 11, n), phase_d, phase_d_err (P, 6, n, n_mu), greek_d, greek_d_err (P, 6, n, L + 1).
     A component whose mode weights are given is multimodal (its parameters carry a mode)."""
     wl = np.ascontiguousarray(wavelengths, dtype=np.float64).reshape(-1)
-    modes, mw, nm, w, ms = _mixture_arrays(components, wl.size)
+    # A component's m may be a particle: ("sphere", m), ("layered", fractions, m [L][n_wl]) or
+    # ("spheroid", aspect_ratio, m).
+    nls, frs, eps, mlist, plain = [], [], [], [], []
+    for dists, mode_w, weight, m in components:
+        if isinstance(m, tuple) and m[0] == "layered":
+            ml = np.asarray(m[2], dtype=np.complex128).reshape(-1, wl.size)
+            nls.append(ml.shape[0])
+            frs += [float(f) for f in np.asarray(m[1]).reshape(-1)]
+            eps.append(0.0)
+            mlist.append(ml.reshape(-1))
+        elif isinstance(m, tuple):
+            nls.append(1)
+            eps.append(float(m[1]) if m[0] == "spheroid" else 0.0)
+            mlist.append(np.broadcast_to(np.asarray(m[-1], dtype=np.complex128), wl.shape))
+        else:
+            nls.append(1)
+            eps.append(0.0)
+            mlist.append(np.broadcast_to(np.asarray(m, dtype=np.complex128), wl.shape))
+        plain.append((dists, mode_w, weight, np.zeros(wl.size, dtype=np.complex128)))
+    modes, mw, nm, w, _ = _mixture_arrays(plain, wl.size)
+    ms = np.ascontiguousarray(np.concatenate(mlist))
+    nls = np.array(nls, dtype=np.int32)
+    frs = np.array(frs + [0.0], dtype=np.float64)
+    eps = np.array(eps, dtype=np.float64)
     mm = np.array([1 if mwc is not None else 0 for _d, mwc, _w, _m in components], dtype=np.int32)
     pr = np.ascontiguousarray(np.atleast_1d(np.asarray(derivs, dtype=PARAM_DTYPE)))
     P = pr.size
@@ -547,12 +570,13 @@ def ensemble_mixture_d(components, wavelengths, derivs, mu=None, greek_order=Non
         dg, dge = np.zeros((P, 6, n, L + 1)), np.zeros((P, 6, n, L + 1))
     err = ctypes.create_string_buffer(512)
     f = lib().orc_ensemble_mixture_d
-    f.argtypes = [ctypes.c_void_p, _PD, ctypes.c_void_p, ctypes.c_void_p, _PD, _PD, _I64, _PD,
+    f.argtypes = [ctypes.c_void_p, _PD, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _PD,
+                  _PD, _PD, _PD, _I64, _PD,
                   _I64, _PD, _I64, _I64, ctypes.c_int, _D, _I64, ctypes.c_int, ctypes.c_int,
                   ctypes.c_void_p, _I64] + [_PD] * 12 + [ctypes.c_void_p, ctypes.c_void_p,
                                                          ctypes.c_char_p, _I64]
-    st = f(modes.ctypes.data, _p(mw), nm.ctypes.data, mm.ctypes.data, _p(w),
-           _p(ms.view(np.float64)), nm.size, _p(wl), wl.size, _p(mu), mu.size, L,
+    st = f(modes.ctypes.data, _p(mw), nm.ctypes.data, mm.ctypes.data, nls.ctypes.data, _p(frs),
+           _p(eps), _p(w), _p(ms.view(np.float64)), nm.size, _p(wl), wl.size, _p(mu), mu.size, L,
            int(normalized), rtol, max_panels, int(allow_unvalidated), int(refine_backscatter),
            pr.ctypes.data if P else None, P, _p(out["values"]), _p(out["errors"]), _p(ph),
            _p(pe), _p(g), _p(ge), _p(out["d"]), _p(out["d_err"]), _p(dph), _p(dpe), _p(dg),

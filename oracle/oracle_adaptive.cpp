@@ -1027,6 +1027,37 @@ struct LinD {
   }
 };
 
+// direct_node (engine.rs:1281-1339) of a solved spheroid node at radius r: the scalars (ONE ...
+// DEPOL) into g[0..9) with their declared errors into ge, and its Greek coefficients times the
+// area into the direct segment g[dstart + f glen + l] (zero beyond its 2N), each with the
+// declared error relative to its largest alpha1; tau the node's T-matrix tolerance.
+void fill_direct(const SpheroidNode& v, double r, double tau, double* g, double* ge,
+                 int64_t dstart, int64_t glen) {
+  const double area = PI * r * r;
+  const double c4 = 4.0 * tau, c16 = 16.0 * tau;
+  const double sv[9] = {1.0,           area * v.q_ext, area * v.q_sca, area * v.q_sca * v.g,
+                        area * v.q_abs, area * v.q_back, r * r,         r * r * r,
+                        area * v.depol};
+  const double back = area * std::max(std::fabs(v.q_back), std::fabs(v.q_sca));
+  const double se[9] = {0.0, c4 * std::fabs(sv[1]), c4 * std::fabs(sv[2]),
+                        c4 * std::fabs(sv[2]) * (1.0 + std::fabs(v.g)), c16 * std::fabs(sv[1]),
+                        c16 * back, 0.0, 0.0, 2.0 * c16 * back};
+  for (int k = 0; k < 9; ++k) {
+    g[k] = sv[k];
+    ge[k] = se[k];
+  }
+  if (glen > 0) {
+    const int64_t have = 2 * (int64_t)v.n + 1;
+    double big = 0.0;
+    for (int64_t l = 0; l < have; ++l) big = std::max(big, std::fabs(v.greek[l]));
+    for (int f = 0; f < 6; ++f)
+      for (int64_t l = 0; l < glen; ++l) {
+        g[dstart + f * glen + l] = l < have ? area * v.greek[f * have + l] : 0.0;
+        ge[dstart + f * glen + l] = c16 * area * big;
+      }
+  }
+}
+
 // The direct path's pass 2, averages and outputs for spheroids (engine.rs:1207-1339 direct_node,
 // 1558-1740 the sums with the declared node errors, 1782-1836 averages, 1896-1961 a single
 // radius, 2121-2176 mixing, 2359-2497 assembly: the depolarization ratio, the Greek
@@ -1045,32 +1076,10 @@ std::vector<UnitOut> direct_outputs(const std::vector<Part>& parts,
   const int64_t ld = !keep ? -1 : n_mu == 0 ? std::min<int64_t>(order, 2 * n_direct) : 2 * n_direct;
   const int64_t glen = ld + 1, NS = 9, len = NS + 6 * glen;
   auto node = [&](double r, std::vector<double>& g, std::vector<double>& ge) {
-    const SpheroidNode& v = sph_node(r, lambda, op);
-    const double area = PI * r * r, tau = op.rtol_t;  // max(rtol, estimate): the estimate is below
-    const double c4 = 4.0 * tau, c16 = 16.0 * tau;
-    const double sv[9] = {1.0,           area * v.q_ext, area * v.q_sca, area * v.q_sca * v.g,
-                          area * v.q_abs, area * v.q_back, r * r,         r * r * r,
-                          area * v.depol};
-    const double back = area * std::max(std::fabs(v.q_back), std::fabs(v.q_sca));
-    const double se[9] = {0.0, c4 * std::fabs(sv[1]), c4 * std::fabs(sv[2]),
-                          c4 * std::fabs(sv[2]) * (1.0 + std::fabs(v.g)), c16 * std::fabs(sv[1]),
-                          c16 * back, 0.0, 0.0, 2.0 * c16 * back};
+    // max(rtol, estimate) as the declared tolerance: the estimate is below rtol.
     g.assign(len, 0.0);
     ge.assign(len, 0.0);
-    for (int k = 0; k < 9; ++k) {
-      g[k] = sv[k];
-      ge[k] = se[k];
-    }
-    if (glen > 0) {
-      const int64_t have = 2 * (int64_t)v.n + 1;
-      double big = 0.0;
-      for (int64_t l = 0; l < have; ++l) big = std::max(big, std::fabs(v.greek[l]));
-      for (int f = 0; f < 6; ++f)
-        for (int64_t l = 0; l < glen; ++l) {
-          g[NS + f * glen + l] = l < have ? area * v.greek[f * have + l] : 0.0;
-          ge[NS + f * glen + l] = c16 * area * big;
-        }
-    }
+    fill_direct(sph_node(r, lambda, op), r, op.rtol_t, g.data(), ge.data(), NS, glen);
   };
   std::vector<std::vector<double>> av(parts.size()), ae(parts.size());
   std::vector<double> g, ge;
@@ -1212,7 +1221,8 @@ std::vector<UnitOut> wavelength(const std::vector<Part>& parts,
                                 bool normalized, const Options& o,
                                 const std::vector<Param>& params = {}) {
   const int64_t n_wl_all = parts.empty() ? 0 : parts[0].n_wl;
-  std::map<double, SpheroidNode> cache;
+  // Solved spheroid nodes per particle (aspect ratio, indices): a batch's parts share one.
+  std::map<std::pair<double, const double*>, std::map<double, SpheroidNode>> caches;
   auto m_of = [&](int p) {
     Optics op;
     const Part& q = parts[p];
@@ -1220,7 +1230,7 @@ std::vector<UnitOut> wavelength(const std::vector<Part>& parts,
       op.m = C(q.m[2 * wi], q.m[2 * wi + 1]);
       op.eps = q.eps;
       op.rtol_t = std::min(std::max(o.rtol / 100.0, 1e-12), 1e-8);  // engine.rs:87
-      op.cache = &cache;
+      op.cache = &caches[{q.eps, q.m}];
       return op;
     }
     if (q.n_layers <= 1) {
@@ -1256,8 +1266,17 @@ std::vector<UnitOut> wavelength(const std::vector<Part>& parts,
       group_of[groups[gi][k]] = (int)gi;
       place[groups[gi][k]] = (int)k;
     }
-  if (!parts.empty() && parts[0].eps > 0.0) {
-    // Spheroids: pass 2 and the outputs on the direct path, from the solved nodes.
+  // The groups on the direct path (spheroids, engine.rs:1975-2000).
+  std::vector<char> direct(groups.size(), 0);
+  bool all_direct = !groups.empty();
+  int64_t n_direct = 0;
+  for (size_t gi = 0; gi < groups.size(); ++gi) {
+    direct[gi] = parts[groups[gi][0]].eps > 0.0;
+    all_direct = all_direct && direct[gi];
+    if (direct[gi]) n_direct = std::max(n_direct, firsts[gi].n_terms);
+  }
+  if (all_direct) {
+    // Spheroids alone: pass 2 and the outputs on the direct path, from the solved nodes.
     const Optics op = m_of(groups[0][0]);
     return direct_outputs(parts, groups, units, firsts, group_of, place, lambda, op, mu, n_mu,
                           order, normalized, o);
@@ -1268,6 +1287,7 @@ std::vector<UnitOut> wavelength(const std::vector<Part>& parts,
   if (order >= 0) {
     std::set<int64_t> uppers;
     for (size_t gi = 0; gi < groups.size(); ++gi) {
+      if (direct[gi]) continue;
       const Optics m = m_of(groups[gi][0]);
       if (parts[groups[gi][0]].support == POINT) {
         uppers.insert(bucket(firsts[gi].n_terms));
@@ -1281,6 +1301,14 @@ std::vector<UnitOut> wavelength(const std::vector<Part>& parts,
       L.start.push_back(L.len);
       L.len += 4 * L.bands.back().n_q;
     }
+  }
+  // The spheroids' direct segment (engine.rs:2073-2086): every order to 2 N for the phase
+  // matrix, else to the requested one.
+  const bool keep = order >= 0 || n_mu > 0;
+  int64_t ld = -1, d_start = L.len;
+  if (n_direct > 0 && keep) {
+    ld = n_mu == 0 ? std::min<int64_t>(order, 2 * n_direct) : 2 * n_direct;
+    L.len += 6 * (ld + 1);
   }
   const int64_t len = L.len;
   // Pass 2 and the averages of every part (engine.rs:1423-1766, 1782-1836): blocks of sums,
@@ -1298,6 +1326,62 @@ std::vector<UnitOut> wavelength(const std::vector<Part>& parts,
   for (size_t gi = 0; gi < groups.size(); ++gi) {
     const auto& grp = groups[gi];
     const Optics m = m_of(grp[0]);
+    if (direct[gi]) {
+      // A spheroid group (engine.rs:1558-1606 with direct_node, 1896-1961 for one radius): the
+      // solved nodes' rows with their declared errors, summed with |w| on the errors.
+      std::vector<double> row(len), rowe(len);
+      auto node_row = [&](double r) {
+        std::fill(row.begin(), row.end(), 0.0);
+        std::fill(rowe.begin(), rowe.end(), 0.0);
+        fill_direct(sph_node(r, lambda, m), r, m.rtol_t, row.data(), rowe.data(), d_start,
+                    ld + 1);
+      };
+      for (int p : grp) {
+        const Part& part = parts[p];
+        if (!part.theta.empty() || part.dir_derivatives())
+          throw Failure{INVALID_INPUT, "derivatives of spheroids are not on this path"};
+        Avg& a = avg[p];
+        if (part.support == POINT) {
+          node_row(part.s_a);
+          a.v = row;
+          a.e = rowe;
+          continue;
+        }
+        std::vector<double> S(len, 0.0), E(len, 0.0);
+        for (auto& ab : firsts[gi].panels) {
+          Node nd[15];
+          gk_panel(ab.first, ab.second, nd);
+          std::vector<double> K(len, 0.0), G(len, 0.0), NE(len, 0.0);
+          for (int i = 0; i < 15; ++i) {
+            const double r = std::exp(nd[i].t);
+            const double ur = density_eval(part.den, r, nullptr) * r;
+            node_row(r);
+            for (int64_t j = 0; j < len; ++j) {
+              K[j] += nd[i].wk * ur * row[j];
+              G[j] += nd[i].wg * ur * row[j];
+              NE[j] += std::fabs(nd[i].wk * ur) * rowe[j];
+            }
+          }
+          for (int64_t j = 0; j < len; ++j) {
+            S[j] += K[j];
+            E[j] += std::fabs(K[j] - G[j]) + NE[j];
+          }
+        }
+        const double trunc = part.support == UNBOUNDED ? 0.2 * o.rtol : 0.0;
+        const double z = part.mom.z, ez = part.mom.ez;
+        a.v.resize(len);
+        a.e.resize(len);
+        for (int64_t j = 0; j < len; ++j) {
+          a.v[j] = S[j] / z;
+          a.e[j] = (E[j] + std::fabs(a.v[j]) * ez) / z + trunc * std::fabs(a.v[j]);
+        }
+        for (int k = 0; k < 2; ++k) {
+          a.v[S_R2 + k] = part.mom.v[k];
+          a.e[S_R2 + k] = part.mom.e[k];
+        }
+      }
+      continue;
+    }
     bool derivs = false;
     for (int p : grp) derivs = derivs || parts[p].dir_derivatives();
     if (parts[grp[0]].support == POINT) {
@@ -1509,6 +1593,22 @@ std::vector<UnitOut> wavelength(const std::vector<Part>& parts,
       if (!(std::isfinite(l->v) && l->v != 0.0))
         throw Failure{INVALID_INPUT,
                       "a ratio's denominator (<C_ext>, <C_sca> or <C_back>) is 0 or not finite"};
+    // (F11 - F22)/(F11 + F22) at 180 degrees for units with spheroids: the numerator over
+    // 2 C_back minus it (engine.rs:2432-2438).
+    bool has_direct = false;
+    for (int p : un) has_direct = has_direct || parts[p].eps > 0.0;
+    LinD depol = LinD::constant(0.0, n_cols);
+    if (has_direct) {
+      const LinD num = lin(SCALARS - 1);
+      LinD den = num;
+      den.v = 2.0 * back.v - num.v;
+      den.e = 2.0 * back.e + num.e;
+      for (size_t c = 0; c < n_cols; ++c) {
+        den.d[c] = 2.0 * back.d[c] - num.d[c];
+        den.de[c] = 2.0 * back.de[c] + num.de[c];
+      }
+      depol = num.div(den);
+    }
     const LinD sc[11] = {ext,
                          sca,
                          ab,
@@ -1516,10 +1616,20 @@ std::vector<UnitOut> wavelength(const std::vector<Part>& parts,
                          sca.div(ext),
                          scag.div(sca),
                          ext.div(back).scale(4.0 * PI),
-                         LinD::constant(0.0, n_cols),
+                         depol,
                          r3.div(r2),
                          r2.scale(PI),
                          r3.scale(4.0 * PI / 3.0)};
+    // Adds c x to t as Lin::combine does (errors as bounds).
+    auto add_to = [&](LinD& t, double c, const LinD& x) {
+      t.v += c * x.v;
+      t.e += std::fabs(c) * x.e;
+      for (size_t k = 0; k < n_cols; ++k) {
+        t.d[k] += c * x.d[k];
+        t.de[k] += std::fabs(c) * x.de[k];
+      }
+    };
+    auto direct_g = [&](int f, int64_t l) { return lin(d_start + f * (ld + 1) + l); };
     u.d_values.assign(n_cols * 11, 0.0);
     u.d_errors.assign(n_cols * 11, 0.0);
     for (int k = 0; k < 11; ++k) {
@@ -1536,9 +1646,33 @@ std::vector<UnitOut> wavelength(const std::vector<Part>& parts,
       u.d_phase.assign(n_cols * 6 * n_mu, 0.0);
       u.d_phase_err.assign(n_cols * 6 * n_mu, 0.0);
       const int src[6] = {0, 1, 0, 2, 3, 2};
+      // greek_phase (engine.rs:2363-2390) of the spheroids' averaged direct coefficients.
+      std::vector<std::vector<LinD>> fd(n_mu);
+      if (has_direct && ld >= 0) {
+        std::vector<double> d00(ld + 1), d22(ld + 1), d2m2(ld + 1), d02(ld + 1);
+        for (int64_t j = 0; j < n_mu; ++j) {
+          wigner_d(0, 0, mu[j], d00.data(), ld + 1);
+          wigner_d(2, 2, mu[j], d22.data(), ld + 1);
+          wigner_d(2, -2, mu[j], d2m2.data(), ld + 1);
+          wigner_d(0, 2, mu[j], d02.data(), ld + 1);
+          fd[j].assign(6, LinD::constant(0.0, n_cols));
+          for (int64_t l = 0; l <= ld; ++l) {
+            const double pl = 0.5 * (d22[l] + d2m2[l]), mn = 0.5 * (d22[l] - d2m2[l]);
+            add_to(fd[j][0], d00[l], direct_g(0, l));
+            add_to(fd[j][1], d02[l], direct_g(4, l));
+            add_to(fd[j][2], pl, direct_g(1, l));
+            add_to(fd[j][2], mn, direct_g(2, l));
+            add_to(fd[j][3], mn, direct_g(1, l));
+            add_to(fd[j][3], pl, direct_g(2, l));
+            add_to(fd[j][4], d02[l], direct_g(5, l));
+            add_to(fd[j][5], d00[l], direct_g(3, l));
+          }
+        }
+      }
       for (int el = 0; el < 6; ++el)
         for (int64_t j = 0; j < n_mu; ++j) {
           LinD f = lin(SCALARS + src[el] * n_mu + j);
+          if (!fd[j].empty()) add_to(f, 1.0, fd[j][el]);
           if (normalized) f = f.div(sca);
           u.phase[el * n_mu + j] = f.v;
           u.phase_err[el * n_mu + j] = f.e;
@@ -1599,6 +1733,19 @@ std::vector<UnitOut> wavelength(const std::vector<Part>& parts,
             }
           }
         }
+      }
+      if (has_direct && ld >= 0) {
+        // The spheroids' coefficients added to the spheres' (engine.rs:2196-2216).
+        const int64_t top_d = std::min<int64_t>(ld, order);
+        if (top_d > top) {
+          std::vector<LinD> wider(6 * (top_d + 1), LinD::constant(0.0, n_cols));
+          for (int el = 0; el < 6; ++el)
+            for (int64_t l = 0; l <= top; ++l) wider[el * (top_d + 1) + l] = gk[el * (top + 1) + l];
+          gk.swap(wider);
+          top = top_d;
+        }
+        for (int el = 0; el < 6; ++el)
+          for (int64_t l = 0; l <= top_d; ++l) add_to(gk[el * (top + 1) + l], 1.0, direct_g(el, l));
       }
       if (normalized) {
         const LinD a0 = gk[0];
@@ -1828,7 +1975,9 @@ int orc_ensemble_adaptive_spheroid(const FixedDist* dists, int64_t n_dist, int b
 // wavelength as orc_ensemble_mixture, and d_values, d_errors (P, 11, n_wl), d_phase,
 // d_phase_err (P, 6, n_wl, n_mu), d_greek, d_greek_err (P, 6, n_wl, L + 1).
 int orc_ensemble_mixture_d(const FixedDist* modes, const double* mode_w, const int32_t* n_modes,
-                           const int32_t* multimodal, const double* w, const double* m,
+                           const int32_t* multimodal, const int32_t* n_layers,
+                           const double* fractions, const double* eps, const double* w,
+                           const double* m,
                            int64_t n_comp, const double* wl, int64_t n_wl, const double* mu,
                            int64_t n_mu, int64_t greek_order, int normalized, double rtol,
                            int64_t max_panels, int allow_unvalidated, int refine_backscatter,
@@ -1855,8 +2004,15 @@ int orc_ensemble_mixture_d(const FixedDist* modes, const double* mode_w, const i
   std::vector<Part> parts;
   std::vector<int> unit;
   try {
-    int64_t k = 0;
+    int64_t k = 0, m_off = 0, fr_off = 0;
     for (int64_t c = 0; c < n_comp; ++c) {
+      // The component's particle (engine.rs:95-115; particle.rs): a sphere, a layered sphere
+      // (its fractions, indices [n_layers][n_wl]) or a spheroid of aspect ratio eps.
+      const int nl = n_layers ? std::max(1, n_layers[c]) : 1;
+      const double* mc = m + 2 * m_off;
+      const double* fc = nl > 1 ? fractions + fr_off : nullptr;
+      m_off += (int64_t)nl * n_wl;
+      fr_off += nl - 1;
       double v_total = 0.0;
       for (int j = 0; j < n_modes[c]; ++j) v_total += multimodal[c] ? mode_w[k + j] : 1.0;
       for (int j = 0; j < n_modes[c]; ++j) {
@@ -1880,8 +2036,17 @@ int orc_ensemble_mixture_d(const FixedDist* modes, const double* mode_w, const i
         const double v = multimodal[c] ? mode_w[k + j] : 1.0;
         parts.push_back(make_part(modes[k + j], rtol, grads));
         Part& pt = parts.back();
-        pt.m = m + 2 * n_wl * c;
+        pt.m = mc;
         pt.n_wl = n_wl;
+        if (nl > 1) {
+          pt.n_layers = nl;
+          pt.fractions = fc;
+          pt.m_layers = mc;
+        }
+        if (eps && eps[c] > 0.0) pt.eps = eps[c];
+        if ((nl > 1 || pt.eps > 0.0) && (!theta.empty() || dir_col[0] >= 0 || dir_col[1] >= 0))
+          throw Failure{INVALID_INPUT,
+                        "derivatives of layered spheres and spheroids are not on this path"};
         pt.f = w[c] / w_total * v / v_total;
         pt.component = (int)c;
         pt.mode = mode;
