@@ -164,15 +164,19 @@ int scatrs_ensemble_adaptive(const scatrs_distribution* dists, int64_t n_dist, i
 
 /* One component of a mixture (scatrs::ensemble::Component, ensemble/mod.rs:136-160): its
  * distribution, or the modes of a multimodal one (SizeDistribution::MultiModal,
- * distribution.rs:60-66) with their weights, its weight w in the mixture, and its sphere's
- * index per wavelength. */
+ * distribution.rs:60-66) with their weights, its weight w in the mixture, and its particle
+ * (Particle, ensemble/particle.rs): a homogeneous sphere (n_layers 0 or 1, aspect_ratio 0), a
+ * layered sphere (n_layers > 1, its radius fractions) or a randomly oriented spheroid
+ * (aspect_ratio > 0). */
 typedef struct scatrs_component {
   const scatrs_distribution* modes; /* n_modes distributions (one for a plain distribution) */
   const double* mode_weights;       /* n_modes weights v_j of a multimodal one, or NULL */
   int32_t n_modes;
-  int32_t reserved;
+  int32_t n_layers;                 /* > 1: a layered sphere of n_layers layers */
   double weight;                    /* w */
-  const double* m;                  /* complex128 per wavelength */
+  const double* m;                  /* complex128 per wavelength; layered: [n_layers][n_wl] */
+  const double* fractions;          /* layered: the n_layers - 1 radius fractions, else NULL */
+  double aspect_ratio;              /* > 0: a spheroid of this aspect ratio, else 0 */
 } scatrs_component;
 
 /*
@@ -182,6 +186,12 @@ typedef struct scatrs_component {
  * with the number fractions (w / sum w) (v_j / sum v) (engine.rs:2121-2176) before the ratios,
  * normalizations and the Greek projection. Outputs per wavelength as scatrs_ensemble_adaptive
  * with n_units = n_wl; converged when every part converged, panels summed over the parts.
+ * Components of different particles (spheres, layered spheres, spheroids) are integrated by
+ * their own engines and mixed on one layout (engine.rs:1964-2250): the spheres' tables and
+ * projected Greek coefficients, the spheroids' direct Greek segment (to the largest 2 N of the
+ * mixture's spheroids at each wavelength), the depolarization ratio from the spheroids, and the
+ * phase matrix from the spheres' tables plus the spheroids' averaged expansion. Such mixtures
+ * take no derivatives and no SCATRS_GREEK_ALL.
  */
 int scatrs_ensemble_mixture(const scatrs_component* components, int64_t n_comp,
                             const double* wavelengths, int64_t n_wl, const double* mu,

@@ -74,8 +74,8 @@ class AdaptiveOptions(ctypes.Structure):
 
 
 class Component(ctypes.Structure):
-    _fields_ = [("modes", _VP), ("mode_weights", _PD), ("n_modes", _I32), ("reserved", _I32),
-                ("weight", _D), ("m", _PD)]
+    _fields_ = [("modes", _VP), ("mode_weights", _PD), ("n_modes", _I32), ("n_layers", _I32),
+                ("weight", _D), ("m", _PD), ("fractions", _PD), ("aspect_ratio", _D)]
 
 
 class SpheroidOptions(ctypes.Structure):
@@ -463,12 +463,7 @@ def ensemble_mixture(components, wavelengths, mu=None, greek_order: int = -1,
     keep = []
     comps = (Component * max(len(components), 1))()
     for k, (dists, mode_w, weight, m) in enumerate(components):
-        d = np.ascontiguousarray(np.atleast_1d(dists), dtype=DIST_DTYPE)
-        mw = None if mode_w is None else np.ascontiguousarray(mode_w, dtype=np.float64)
-        mm = np.ascontiguousarray(np.broadcast_to(np.asarray(m, dtype=np.complex128), wl.shape))
-        keep += [d, mw, mm]
-        comps[k] = Component(d.ctypes.data, _p(mw), d.size, 0, float(weight),
-                             _p(mm.view(np.float64)))
+        comps[k] = _component(dists, mode_w, weight, m, wl.size, keep)
     mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
     n = wl.size
     L = int(greek_order)
@@ -513,6 +508,27 @@ def _take_all_orders(out: dict, n: int, P: int = 0) -> None:
         out["greek_d"], out["greek_d_err"] = dg, dge
 
 
+def _component(dists, mode_w, weight, m, n_wl: int, keep: list) -> Component:
+    """A mixture component: its distribution records, mode weights (or None) and weight, and
+    its particle: m per wavelength (a sphere), or ("sphere", m), ("layered", fractions,
+    m (L, n_wl)), ("spheroid", aspect_ratio, m). The arrays go to keep."""
+    d = np.ascontiguousarray(np.atleast_1d(dists), dtype=DIST_DTYPE)
+    mw = None if mode_w is None else np.ascontiguousarray(mode_w, dtype=np.float64)
+    n_layers, fr, eps = 0, None, 0.0
+    if isinstance(m, tuple) and m[0] == "layered":
+        fr = np.ascontiguousarray(np.asarray(m[1], dtype=np.float64).reshape(-1))
+        mm = np.ascontiguousarray(np.asarray(m[2], dtype=np.complex128).reshape(-1, n_wl))
+        n_layers = mm.shape[0]
+    else:
+        if isinstance(m, tuple):
+            eps = float(m[1]) if m[0] == "spheroid" else 0.0
+            m = m[-1]
+        mm = np.ascontiguousarray(np.broadcast_to(np.asarray(m, dtype=np.complex128), (n_wl,)))
+    keep += [d, mw, mm, fr]
+    return Component(d.ctypes.data, _p(mw), d.size, n_layers, float(weight),
+                     _p(mm.view(np.float64).reshape(-1)), _p(fr), eps)
+
+
 # scatrs_param: (component, mode or -1, kind, index); kinds as SCATRS_PARAM_*.
 PARAM_DTYPE = np.dtype([("component", np.int32), ("mode", np.int32), ("kind", np.int32),
                         ("index", np.int32)])
@@ -531,12 +547,7 @@ def ensemble_mixture_d(components, wavelengths, params, mu=None, greek_order: in
     keep = []
     comps = (Component * max(len(components), 1))()
     for k, (dists, mode_w, weight, m) in enumerate(components):
-        d = np.ascontiguousarray(np.atleast_1d(dists), dtype=DIST_DTYPE)
-        mw = None if mode_w is None else np.ascontiguousarray(mode_w, dtype=np.float64)
-        mm = np.ascontiguousarray(np.broadcast_to(np.asarray(m, dtype=np.complex128), wl.shape))
-        keep += [d, mw, mm]
-        comps[k] = Component(d.ctypes.data, _p(mw), d.size, 0, float(weight),
-                             _p(mm.view(np.float64)))
+        comps[k] = _component(dists, mode_w, weight, m, wl.size, keep)
     pr = np.ascontiguousarray(np.atleast_1d(np.asarray(params, dtype=PARAM_DTYPE)))
     P = pr.size
     mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)

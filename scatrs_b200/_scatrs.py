@@ -205,6 +205,20 @@ def _sphere_m(particle_spec, n_wl: int) -> np.ndarray:
     return m
 
 
+def _particle(particle_spec, n_wl: int):
+    """A mixture component's particle for _native: m (a sphere) or the checked layered or
+    spheroid spec."""
+    if not isinstance(particle_spec, tuple) or not particle_spec:
+        raise TypeError("a particle spec must be a tuple")
+    if particle_spec[0] == "layered":
+        fr, ml = _layers(particle_spec, n_wl)
+        return ("layered", fr, ml)
+    if particle_spec[0] == "spheroid":
+        eps, m = _spheroid(particle_spec, n_wl)
+        return ("spheroid", eps, m)
+    return _sphere_m(particle_spec, n_wl)
+
+
 def _modes(spec):
     """(DIST_DTYPE modes, mode weights or None) of a spec; multimodal specs list (v, spec)."""
     if isinstance(spec, tuple) and spec and spec[0] == "multimodal":
@@ -229,8 +243,9 @@ def _greek_order(greek, all_orders) -> int:
 
 def ensemble_compute(items, wavelengths, mixture, greek, all_orders, mu, normalized, derivatives,
                      rtol, max_panels, allow_unvalidated, refine_backscatter) -> dict:
-    """The reference's ``_scatrs.ensemble_compute`` on the GPU: one or more sphere components
-    (a mixture), each a distribution or a multimodal one, one output per wavelength."""
+    """The reference's ``_scatrs.ensemble_compute`` on the GPU: one or more components (a
+    mixture) of spheres, layered spheres or spheroids, each a distribution or a multimodal
+    one, one output per wavelength."""
     if not items:
         raise InvalidInputError("a mixture needs a component")
     derivatives = [int(i) for i in derivatives]
@@ -242,9 +257,19 @@ def ensemble_compute(items, wavelengths, mixture, greek, all_orders, mu, normali
     mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
     L = _greek_order(greek, all_orders)
     kinds = {p[0] if isinstance(p, tuple) and p else None for _, p, _ in items}
+    single = len(items) == 1 and not (isinstance(items[0][0], tuple)
+                                      and items[0][0][0] == "multimodal")
+    if kinds - {"sphere"} and not single:
+        # Components of different particles, or multimodal ones: the mixture path.
+        comps = []
+        for spec, particle, weight in items:
+            dists, mode_w = _modes(spec)
+            comps.append((dists, mode_w, float(weight), _particle(particle, wl.size)))
+        out = _native.ensemble_mixture(comps, wl, mu, L, bool(normalized), float(rtol),
+                                       int(max_panels), bool(allow_unvalidated),
+                                       bool(refine_backscatter))
+        return _adaptive_dict(out, mu.size, 0)
     if "spheroid" in kinds:
-        if len(items) != 1 or (isinstance(items[0][0], tuple) and items[0][0][0] == "multimodal"):
-            raise InvalidInputError("spheroids take one distribution on the GPU path")
         spec, particle, _ = items[0]
         eps, m = _spheroid(particle, wl.size)
         out = _native.ensemble_adaptive_spheroid(
@@ -252,10 +277,6 @@ def ensemble_compute(items, wavelengths, mixture, greek, all_orders, mu, normali
             int(max_panels), bool(allow_unvalidated), bool(refine_backscatter))
         return _adaptive_dict(out, mu.size, 0)
     if "layered" in kinds:
-        # One layered component, one distribution (mixtures of layered spheres are not on the
-        # GPU path).
-        if len(items) != 1 or (isinstance(items[0][0], tuple) and items[0][0][0] == "multimodal"):
-            raise InvalidInputError("layered spheres take one distribution on the GPU path")
         spec, particle, _ = items[0]
         fr, ml = _layers(particle, wl.size)
         out = _native.ensemble_adaptive_layered(

@@ -17,6 +17,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <tuple>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -1333,13 +1334,25 @@ void mix_derivatives(const std::vector<AdPart>& in, const std::vector<adaptive::
 // With dd (derivatives), pass 1 refines the requested parameters' blocks too, pass 2 runs the
 // derivative blocks of every part, and the mixing (with the weight derivatives) and the
 // outputs are assembled on the host from the parts' per-block averages.
+// The parts' averages of an adaptive call (final_adaptive_kernel's rows, per (part, wavelength)
+// unit: 8 scalars, 4 n_mu cosine values, 6 (L + 1) Greek coefficients, then their errors), with
+// each unit's converged flag and panel count, for a mixture's host assembly.
+struct PartRows {
+  std::vector<double> rows;
+  int64_t stride = 0;
+  std::vector<char> converged;
+  std::vector<int64_t> panels;
+};
+
 // With n_max_out, only pass 1 runs (and its errors are reported): n_max_out receives each
-// (part, wavelength) unit's largest number of terms, its group's (engine.rs:1987-2030).
+// (part, wavelength) unit's largest number of terms, its group's (engine.rs:1987-2030). With
+// rows_out (no derivatives), the parts' averages go there instead of the outputs.
 void adaptive_call_order(const std::vector<AdPart>& in, int n_out, bool batch,
                          const double* wavelengths, int64_t n_wl, const double* mu, int64_t n_mu,
                          const scatrs_adaptive_options* options, const AdOutputs& res,
                          const scatrs_layers* layers = nullptr, const AdDerivs* dd = nullptr,
-                         std::vector<int64_t>* n_max_out = nullptr) {
+                         std::vector<int64_t>* n_max_out = nullptr,
+                         PartRows* rows_out = nullptr) {
   if (!options) throw Failure{SCATRS_INVALID_INPUT, "options must not be NULL"};
   if (n_wl < 0) throw Failure{SCATRS_INVALID_INPUT, "negative sizes"};
   const adaptive::Options o{options->rtol, options->max_panels, options->allow_unvalidated != 0,
@@ -1688,6 +1701,18 @@ void adaptive_call_order(const std::vector<AdPart>& in, int n_out, bool batch,
     mix_derivatives(in, parts, n_out, n_wl, n_mu, options->greek_order, options->normalized != 0,
                     n_theta, hav, *dd, res);
     adaptive_flags(in, jobs, job_of, unit_converged, unit_panels, n_out, n_wl, res);
+    return;
+  }
+  if (rows_out) {
+    call.radius = std::move(radius);
+    check_device_errors(c, s, &call);
+    rows_out->stride = stride;
+    rows_out->rows.resize((size_t)n_units * stride);
+    SB_CUDA(cudaMemcpyAsync(rows_out->rows.data(), avg, rows_out->rows.size() * 8,
+                            cudaMemcpyDeviceToHost, s));
+    SB_CUDA(cudaStreamSynchronize(s));
+    rows_out->converged = unit_converged;
+    rows_out->panels = unit_panels;
     return;
   }
   // Mixing and outputs.
@@ -2408,14 +2433,33 @@ LinE lin_scale(const LinE& a, double c) { return {c * a.v, std::fabs(c) * a.e}; 
 // for the averages, 2396-2497 for the outputs). Pass 1's node evaluations are spheroid batches
 // on the GPU (T-matrix converged to the ensemble's rtol / 100 clamped to [1e-12, 1e-8],
 // engine.rs:87, with the orientation average when Greek coefficients or phase are asked for),
-// kept for pass 2, which integrates them without solving again. One particle per call: every
-// distribution is an output unit of its own (batch: panels shared per wavelength).
-void adaptive_spheroid_call(const scatrs_distribution* dists, int64_t n_dist, bool batch,
-                            const double* wavelengths, int64_t n_wl, double eps,
-                            const double* m, const double* mu, int64_t n_mu,
-                            const scatrs_adaptive_options* options, const AdOutputs& res) {
+// kept for pass 2, which integrates them without solving again. Every distribution of every
+// particle is an output unit of its own (batch, one particle: panels shared per wavelength);
+// the direct order at a wavelength follows the largest N of all the call's spheroids there
+// (engine.rs:2073-2086). With rows, the parts' averages go there instead of the outputs (a
+// mixture's host assembly).
+struct SphParticle {
+  const scatrs_distribution* dists;
+  int64_t n_dist;
+  double eps;
+  const double* m;  // complex per wavelength
+};
+struct SphRows {
+  std::vector<std::vector<double>> av, ae;  // per (part, wavelength): 9 + 6 (ld + 1) doubles
+  std::vector<int64_t> ld;                  // per wavelength: the direct order, or -1
+  std::vector<char> converged;
+  std::vector<int64_t> panels;
+};
+
+void spheroid_call(const std::vector<SphParticle>& ps, bool batch, const double* wavelengths,
+                   int64_t n_wl, const double* mu, int64_t n_mu,
+                   const scatrs_adaptive_options* options, const AdOutputs& res,
+                   SphRows* rows = nullptr) {
   if (!options) throw Failure{SCATRS_INVALID_INPUT, "options must not be NULL"};
+  int64_t n_dist = 0;
+  for (const SphParticle& q : ps) n_dist += q.n_dist;
   if (n_dist < 0 || n_wl < 0) throw Failure{SCATRS_INVALID_INPUT, "negative sizes"};
+  if (batch && ps.size() > 1) throw Failure{SCATRS_INVALID_INPUT, "a batch has one particle"};
   if (options->greek_order == SCATRS_GREEK_ALL)
     throw Failure{SCATRS_INVALID_INPUT, "greek='all' for spheroids is not on the GPU path"};
   const adaptive::Options o{options->rtol, options->max_panels, options->allow_unvalidated != 0,
@@ -2430,45 +2474,51 @@ void adaptive_spheroid_call(const scatrs_distribution* dists, int64_t n_dist, bo
     if (!(std::isfinite(wavelengths[i]) && wavelengths[i] > 0.0))
       throw Failure{SCATRS_INVALID_INPUT,
                     "wavelength " + std::to_string(i) + " must be finite and > 0"};
-  if (!(std::isfinite(eps) && eps > 0.0))
-    throw Failure{SCATRS_INVALID_INPUT, "the aspect ratio must be finite and > 0"};
+  for (const SphParticle& q : ps)
+    if (!(std::isfinite(q.eps) && q.eps > 0.0))
+      throw Failure{SCATRS_INVALID_INPUT, "the aspect ratio must be finite and > 0"};
   scatrs_fixed_options fo{32, options->greek_order, options->normalized,
                           options->allow_unvalidated};
   const int64_t n_units = n_dist * n_wl;
   check_options(&fo, n_units, n_mu, mu);
   if (n_units == 0) return;
   std::vector<adaptive::Part> parts;
-  for (int64_t d = 0; d < n_dist; ++d) {
-    try {
-      parts.push_back(adaptive::make_part(dists[d].kind, dists[d].param, o.rtol, dists[d].table,
-                                          dists[d].table_len));
-    } catch (const adaptive::Error& e) {
-      throw Failure{e.status, "distribution " + std::to_string(d) + ": " + e.msg};
+  std::vector<int> particle_of;  // per part
+  for (size_t q = 0; q < ps.size(); ++q)
+    for (int64_t d = 0; d < ps[q].n_dist; ++d) {
+      const scatrs_distribution& dd = ps[q].dists[d];
+      try {
+        parts.push_back(
+            adaptive::make_part(dd.kind, dd.param, o.rtol, dd.table, dd.table_len));
+      } catch (const adaptive::Error& e) {
+        throw Failure{e.status, "distribution " + std::to_string(d) + ": " + e.msg};
+      }
+      particle_of.push_back((int)q);
     }
-  }
   const double rtol_t = std::min(std::max(o.rtol / 100.0, 1e-12), 1e-8);
   const bool keep_greek = options->greek_order >= 0 || n_mu > 0;
   const double pi = 3.14159265358979323846;
   Context& c = context();
   std::lock_guard<std::mutex> lk(c.mtx);
   cudaStream_t s = 0;
-  // Solved nodes by (wavelength, radius bits).
-  std::map<std::pair<int64_t, uint64_t>, SpheroidResult> cache;
-  auto key_of = [](int64_t i, double r) {
+  // Solved nodes by (particle, wavelength, radius bits).
+  std::map<std::tuple<int, int64_t, uint64_t>, SpheroidResult> cache;
+  auto key_of = [](int q, int64_t i, double r) {
     uint64_t b;
     memcpy(&b, &r, 8);
-    return std::make_pair(i, b);
+    return std::make_tuple(q, i, b);
   };
   auto eval = [&](const std::vector<adaptive::Query>& qs, std::vector<adaptive::NodeResult>& out) {
     std::vector<double> xs, es, ms;
     std::vector<size_t> which;
     for (size_t k = 0; k < qs.size(); ++k) {
       const int64_t i = qs[k].wl % n_wl;
-      if (cache.count(key_of(i, qs[k].r))) continue;
+      const int q = particle_of[qs[k].wl / n_wl];
+      if (cache.count(key_of(q, i, qs[k].r))) continue;
       xs.push_back(2.0 * pi * qs[k].r / wavelengths[i]);
-      es.push_back(eps);
-      ms.push_back(m[2 * i]);
-      ms.push_back(m[2 * i + 1]);
+      es.push_back(ps[q].eps);
+      ms.push_back(ps[q].m[2 * i]);
+      ms.push_back(ps[q].m[2 * i + 1]);
       which.push_back(k);
     }
     if (!which.empty()) {
@@ -2479,11 +2529,12 @@ void adaptive_spheroid_call(const scatrs_distribution* dists, int64_t n_dist, bo
                      true, r, s);
       for (size_t k = 0; k < which.size(); ++k) {
         const adaptive::Query& q = qs[which[k]];
-        cache[key_of(q.wl % n_wl, q.r)] = std::move(r[k]);
+        cache[key_of(particle_of[q.wl / n_wl], q.wl % n_wl, q.r)] = std::move(r[k]);
       }
     }
     for (size_t k = 0; k < qs.size(); ++k) {
-      const SpheroidResult& v = cache.at(key_of(qs[k].wl % n_wl, qs[k].r));
+      const SpheroidResult& v =
+          cache.at(key_of(particle_of[qs[k].wl / n_wl], qs[k].wl % n_wl, qs[k].r));
       const double area = pi * qs[k].r * qs[k].r;
       adaptive::NodeResult& x = out[k];
       const double q[6] = {1.0, area * v.q_ext, area * v.q_sca, area * v.q_sca * v.g,
@@ -2534,7 +2585,17 @@ void adaptive_spheroid_call(const scatrs_distribution* dists, int64_t n_dist, bo
   // requested one (engine.rs:2073-2086).
   const int L = options->greek_order;
   std::vector<int64_t> n_direct(n_wl, 0);
-  for (const auto& kv : cache) n_direct[kv.first.first] = std::max<int64_t>(n_direct[kv.first.first], kv.second.n);
+  for (const auto& kv : cache) {
+    const int64_t i = std::get<1>(kv.first);
+    n_direct[i] = std::max<int64_t>(n_direct[i], kv.second.n);
+  }
+  if (rows) {
+    rows->av.assign(n_units, {});
+    rows->ae.assign(n_units, {});
+    rows->ld.assign(n_wl, -1);
+    rows->converged.assign(n_units, 1);
+    rows->panels.assign(n_units, 0);
+  }
   constexpr int kS = 9;  // ONE, EXT, SCA, SCAG, ABS, BACK, R2, R3, DEPOL
   for (int64_t u = 0; u < n_units; ++u) {
     const int64_t p = u / n_wl, i = u % n_wl;
@@ -2547,7 +2608,7 @@ void adaptive_spheroid_call(const scatrs_distribution* dists, int64_t n_dist, bo
     // One node's direct quantities and declared errors (direct_scalars, direct_node).
     std::vector<double> g(len), ge(len);
     auto direct_node = [&](double r) {
-      const SpheroidResult& v = cache.at(key_of(i, r));
+      const SpheroidResult& v = cache.at(key_of(particle_of[p], i, r));
       const double area = pi * r * r;
       const double tau = std::max(rtol_t, v.err_est);
       const double c4 = 4.0 * tau, c16 = 16.0 * tau;
@@ -2627,6 +2688,14 @@ void adaptive_spheroid_call(const scatrs_distribution* dists, int64_t n_dist, bo
       ae[6] = part.mom.e[0];
       av[7] = part.mom.v[1];
       ae[7] = part.mom.e[1];
+    }
+    if (rows) {
+      rows->av[u] = std::move(av);
+      rows->ae[u] = std::move(ae);
+      rows->ld[i] = ld;
+      rows->converged[u] = conv ? 1 : 0;
+      rows->panels[u] = panels;
+      continue;
     }
     // assemble (engine.rs:2396-2497).
     auto lin = [&](int64_t j) { return LinE{av[j], ae[j]}; };
@@ -2716,6 +2785,13 @@ int guarded(char* err, size_t err_len, F f) {
   }
 }
 
+// Whether a mixture has components other than homogeneous spheres.
+bool heterogeneous(const scatrs_component* components, int64_t n_comp) {
+  for (int64_t c = 0; c < n_comp && components; ++c)
+    if (components[c].n_layers > 1 || components[c].aspect_ratio != 0.0) return true;
+  return false;
+}
+
 // The parts of a mixture (ensemble/mod.rs:609-625, 688-780 validation; engine.rs:141-223): each
 // mode of each component with its number fraction w / w_total * v / v_total (engine.rs:2131).
 std::vector<AdPart> mixture_parts(const scatrs_component* components, int64_t n_comp) {
@@ -2760,6 +2836,250 @@ std::vector<AdPart> mixture_parts(const scatrs_component* components, int64_t n_
     }
   }
   return parts;
+}
+
+// A mixture whose components are not all homogeneous spheres (engine.rs:1964-2250 over
+// components of different particles): the spheres in one adaptive call, the layered spheres in
+// one per number of layers, the spheroids in one spheroid call (one direct order per
+// wavelength over all of them), each returning its parts' averages; then per wavelength the
+// number-fraction mixing on one layout (scalars with the depolarization numerator, the spheres'
+// cosine tables and projected Greek coefficients, the spheroids' direct segment) and the
+// assembly: ratios and bounds (lin.rs), the depolarization ratio, the Greek coefficients of the
+// spheres plus the spheroids', the phase matrix of the spheres' tables plus the spheroids'
+// averaged expansion (greek_phase, engine.rs:2363-2390), normalized by alpha1_0 and <C_sca>.
+void mixture_hetero(const scatrs_component* components, int64_t n_comp,
+                    const double* wavelengths, int64_t n_wl, const double* mu, int64_t n_mu,
+                    const scatrs_adaptive_options* options, const AdOutputs& res) {
+  if (!options) throw Failure{SCATRS_INVALID_INPUT, "options must not be NULL"};
+  if (options->greek_order == SCATRS_GREEK_ALL)
+    throw Failure{SCATRS_INVALID_INPUT,
+                  "greek='all' for mixtures with layered spheres or spheroids is not on the GPU "
+                  "path"};
+  const std::vector<AdPart> parts = mixture_parts(components, n_comp);
+  const int64_t np = (int64_t)parts.size();
+  for (int64_t c = 0; c < n_comp; ++c) {
+    const scatrs_component& k = components[c];
+    const std::string who = "component " + std::to_string(c) + ": ";
+    if (!(std::isfinite(k.aspect_ratio) && k.aspect_ratio >= 0.0))
+      throw Failure{SCATRS_INVALID_INPUT, who + "the aspect ratio must be finite and > 0"};
+    if (k.aspect_ratio > 0.0 && k.n_layers > 1)
+      throw Failure{SCATRS_INVALID_INPUT, who + "a particle is layered or a spheroid, not both"};
+    if (k.n_layers > 16) throw Failure{SCATRS_INVALID_INPUT, who + "at most 16 layers"};
+    if (k.n_layers > 1 && !k.fractions)
+      throw Failure{SCATRS_INVALID_INPUT, who + "a layered sphere needs its fractions"};
+  }
+  const int L = options->greek_order;
+  const int64_t glen = L >= 0 ? L + 1 : 0;
+  // Each part's averages at each wavelength: 9 scalars (the last the depolarization
+  // numerator), 4 n_mu cosine values, 6 glen Greek coefficients, each with its error, and the
+  // spheroids' direct segment.
+  struct Avg {
+    std::vector<double> v, e, dv, de;  // v, e: 9 + 4 n_mu + 6 glen; dv, de: 6 (ld + 1)
+    bool converged = true;
+    int64_t panels = 0;
+  };
+  const int64_t row = 9 + 4 * n_mu + 6 * glen;
+  std::vector<Avg> avg((size_t)np * n_wl);
+  // Spheres, and layered spheres by their number of layers.
+  std::map<int, std::vector<int64_t>> by_layers;
+  for (int64_t p = 0; p < np; ++p) {
+    const scatrs_component& k = components[parts[p].component];
+    if (k.aspect_ratio == 0.0) by_layers[k.n_layers > 1 ? k.n_layers : 1].push_back(p);
+  }
+  for (const auto& kv : by_layers) {
+    const int nl = kv.first;
+    const std::vector<int64_t>& ps = kv.second;
+    std::vector<AdPart> sub;
+    std::vector<double> fr, ml;
+    for (int64_t p : ps) {
+      AdPart a = parts[p];
+      a.out = 0;
+      sub.push_back(a);
+      if (nl > 1) {
+        const scatrs_component& k = components[parts[p].component];
+        fr.insert(fr.end(), k.fractions, k.fractions + nl - 1);
+        ml.insert(ml.end(), k.m, k.m + 2 * (size_t)nl * n_wl);
+      }
+    }
+    scatrs_layers lay{nl, 0, fr.data(), ml.data()};
+    PartRows rows;
+    adaptive_call_order(sub, 1, false, wavelengths, n_wl, mu, n_mu, options, AdOutputs{},
+                        nl > 1 ? &lay : nullptr, nullptr, nullptr, &rows);
+    const int64_t n2 = 4 * n_mu, base_t = 16, base_g = 16 + 8 * n_mu;
+    for (size_t q = 0; q < ps.size(); ++q)
+      for (int64_t i = 0; i < n_wl; ++i) {
+        const double* r = rows.rows.data() + ((int64_t)q * n_wl + i) * rows.stride;
+        Avg& a = avg[ps[q] * n_wl + i];
+        a.v.assign(row, 0.0);
+        a.e.assign(row, 0.0);
+        for (int k = 0; k < 8; ++k) {
+          a.v[k] = r[k];
+          a.e[k] = r[8 + k];
+        }
+        for (int64_t j = 0; j < n2; ++j) {
+          a.v[9 + j] = r[base_t + j];
+          a.e[9 + j] = r[base_t + n2 + j];
+        }
+        for (int64_t j = 0; j < 6 * glen; ++j) {
+          a.v[9 + n2 + j] = r[base_g + j];
+          a.e[9 + n2 + j] = r[base_g + 6 * glen + j];
+        }
+        a.converged = rows.converged[q * n_wl + i] != 0;
+        a.panels = rows.panels[q * n_wl + i];
+      }
+  }
+  // Spheroids: one particle per component, its modes its distributions.
+  std::vector<SphParticle> sph;
+  std::vector<int64_t> sph_parts;  // the parts in the order of the spheroid call's
+  for (int64_t c = 0; c < n_comp; ++c) {
+    const scatrs_component& k = components[c];
+    if (k.aspect_ratio == 0.0) continue;
+    sph.push_back(SphParticle{k.modes, k.n_modes, k.aspect_ratio, k.m});
+    for (int64_t p = 0; p < np; ++p)
+      if (parts[p].component == c) sph_parts.push_back(p);
+  }
+  std::vector<int64_t> ld(n_wl, -1);
+  if (!sph.empty()) {
+    SphRows rows;
+    spheroid_call(sph, false, wavelengths, n_wl, mu, n_mu, options, AdOutputs{}, &rows);
+    ld = rows.ld;
+    for (size_t q = 0; q < sph_parts.size(); ++q)
+      for (int64_t i = 0; i < n_wl; ++i) {
+        const std::vector<double>& sv = rows.av[q * n_wl + i];
+        const std::vector<double>& se = rows.ae[q * n_wl + i];
+        Avg& a = avg[sph_parts[q] * n_wl + i];
+        a.v.assign(row, 0.0);
+        a.e.assign(row, 0.0);
+        for (int k = 0; k < 9; ++k) {
+          a.v[k] = sv[k];
+          a.e[k] = se[k];
+        }
+        a.dv.assign(sv.begin() + 9, sv.end());
+        a.de.assign(se.begin() + 9, se.end());
+        a.converged = rows.converged[q * n_wl + i] != 0;
+        a.panels = rows.panels[q * n_wl + i];
+      }
+  }
+  // Mixing and assembly per wavelength.
+  const bool norm = options->normalized != 0;
+  for (int64_t i = 0; i < n_wl; ++i) {
+    const int64_t ldi = ld[i], dlen = ldi >= 0 ? 6 * (ldi + 1) : 0;
+    std::vector<double> v(row, 0.0), e(row, 0.0), dv(dlen, 0.0), de(dlen, 0.0);
+    bool has_direct = false, conv = true;
+    int64_t panels = 0;
+    for (int64_t p = 0; p < np; ++p) {
+      const Avg& a = avg[p * n_wl + i];
+      const double f = parts[p].f;
+      for (int64_t k = 0; k < row; ++k) {
+        v[k] += f * a.v[k];
+        e[k] += f * a.e[k];
+      }
+      if (components[parts[p].component].aspect_ratio > 0.0) {
+        has_direct = true;
+        for (int64_t k = 0; k < dlen; ++k) {
+          dv[k] += f * a.dv[k];
+          de[k] += f * a.de[k];
+        }
+      }
+      conv = conv && a.converged;
+      panels += a.panels;
+    }
+    auto lin = [&](int64_t k) { return LinE{v[k], e[k]}; };
+    const LinE ext = lin(1), sca = lin(2), scag = lin(3), abs_ = lin(4), back = lin(5),
+               r2 = lin(6), r3 = lin(7), num = lin(8);
+    for (const auto& w : {std::make_pair("<C_ext>", ext), std::make_pair("<C_sca>", sca),
+                          std::make_pair("<C_back>", back)})
+      if (!(std::isfinite(w.second.v) && w.second.v != 0.0))
+        throw Failure{SCATRS_INVALID_INPUT,
+                      std::string("the ensemble's ") + w.first +
+                          " is 0 or not finite, so its ratios (albedo, asymmetry parameter, "
+                          "lidar ratio) are undefined (does m = 1?)"};
+    const LinE depol = has_direct ? lin_div(num, LinE{2.0 * back.v - num.v, 2.0 * back.e + num.e})
+                                  : LinE{0.0, 0.0};
+    const LinE outs[11] = {ext,
+                           sca,
+                           abs_,
+                           back,
+                           lin_div(sca, ext),
+                           lin_div(scag, sca),
+                           lin_scale(lin_div(ext, back), 4.0 * kPi),
+                           depol,
+                           lin_div(r3, r2),
+                           lin_scale(r2, kPi),
+                           lin_scale(r3, 4.0 * kPi / 3.0)};
+    for (int k = 0; k < 11; ++k) {
+      res.values[k * n_wl + i] = outs[k].v;
+      if (res.errors) res.errors[k * n_wl + i] = outs[k].e;
+    }
+    auto D = [&](int f, int64_t l) {
+      return LinE{dv[f * (ldi + 1) + l], de[f * (ldi + 1) + l]};
+    };
+    const int64_t g0 = 9 + 4 * n_mu;
+    if (glen > 0 && res.greek) {
+      // The spheres' coefficients plus the spheroids' (engine.rs:2196-2216).
+      auto G = [&](int f, int64_t l) {
+        LinE x = lin(g0 + f * glen + l);
+        if (has_direct && l <= ldi) {
+          const LinE y = D(f, l);
+          x.v += y.v;
+          x.e += y.e;
+        }
+        return x;
+      };
+      const LinE a0 = G(0, 0);
+      for (int f = 0; f < 6; ++f)
+        for (int64_t l = 0; l < glen; ++l) {
+          LinE x = G(f, l);
+          if (norm) x = (f == 0 && l == 0) ? LinE{1.0, 0.0} : lin_div(x, a0);
+          res.greek[(f * n_wl + i) * glen + l] = x.v;
+          if (res.greek_err) res.greek_err[(f * n_wl + i) * glen + l] = x.e;
+        }
+    }
+    if (n_mu > 0 && res.phase) {
+      const int src[6] = {0, 1, 0, 2, 3, 2};
+      std::vector<double> d00, d22, d2m2, d02;
+      if (has_direct && ldi >= 0) {
+        d00.resize(ldi + 1);
+        d22.resize(ldi + 1);
+        d2m2.resize(ldi + 1);
+        d02.resize(ldi + 1);
+      }
+      for (int64_t j = 0; j < n_mu; ++j) {
+        LinE fd[6];
+        if (has_direct && ldi >= 0) {
+          wigner_d(0, 0, mu[j], d00.data(), ldi + 1);
+          wigner_d(2, 2, mu[j], d22.data(), ldi + 1);
+          wigner_d(2, -2, mu[j], d2m2.data(), ldi + 1);
+          wigner_d(0, 2, mu[j], d02.data(), ldi + 1);
+          auto acc = [](LinE& t, double w, const LinE& x) {
+            t.v += w * x.v;
+            t.e += std::fabs(w) * x.e;
+          };
+          for (int64_t l = 0; l <= ldi; ++l) {
+            const double pl = 0.5 * (d22[l] + d2m2[l]), mn = 0.5 * (d22[l] - d2m2[l]);
+            acc(fd[0], d00[l], D(0, l));
+            acc(fd[1], d02[l], D(4, l));
+            acc(fd[2], pl, D(1, l));
+            acc(fd[2], mn, D(2, l));
+            acc(fd[3], mn, D(1, l));
+            acc(fd[3], pl, D(2, l));
+            acc(fd[4], d02[l], D(5, l));
+            acc(fd[5], d00[l], D(3, l));
+          }
+        }
+        for (int el = 0; el < 6; ++el) {
+          LinE x = lin(9 + src[el] * n_mu + j);
+          x.v += fd[el].v;
+          x.e += fd[el].e;
+          if (norm) x = lin_div(x, sca);
+          res.phase[(el * n_wl + i) * n_mu + j] = x.v;
+          if (res.phase_err) res.phase_err[(el * n_wl + i) * n_mu + j] = x.e;
+        }
+      }
+    }
+    if (res.converged) res.converged[i] = conv ? 1 : 0;
+    if (res.panels) res.panels[i] = panels;
+  }
 }
 
 }  // namespace
@@ -2919,8 +3239,8 @@ int scatrs_ensemble_adaptive_spheroid(const scatrs_distribution* dists, int64_t 
   return guarded(err, err_len, [&] {
     if (!values || !m) throw Failure{SCATRS_INVALID_INPUT, "values and m are required"};
     AdOutputs out{values, errors, phase, phase_err, greek, greek_err, converged, panels};
-    adaptive_spheroid_call(dists, n_dist, batch != 0, wavelengths, n_wl, aspect_ratio, m, mu,
-                           n_mu, options, out);
+    spheroid_call({SphParticle{dists, n_dist, aspect_ratio, m}}, batch != 0, wavelengths, n_wl,
+                  mu, n_mu, options, out);
   });
 }
 
@@ -2936,6 +3256,15 @@ int scatrs_ensemble_mixture_d(const scatrs_component* components, int64_t n_comp
   return guarded(err, err_len, [&] {
     if (n_params < 0 || (n_params > 0 && !params))
       throw Failure{SCATRS_INVALID_INPUT, "params must hold n_params parameters"};
+    if (heterogeneous(components, n_comp)) {
+      if (n_params > 0)
+        throw Failure{SCATRS_INVALID_INPUT,
+                      "derivatives of mixtures with layered spheres or spheroids are not on the "
+                      "GPU path"};
+      AdOutputs out{values, errors, phase, phase_err, greek, greek_err, converged, panels};
+      mixture_hetero(components, n_comp, wavelengths, n_wl, mu, n_mu, options, out);
+      return;
+    }
     std::vector<AdPart> parts = mixture_parts(components, n_comp);
     // ensemble/mod.rs:781-799: every parameter once and among the mixture's (mod.rs:254-337).
     bool mixture = n_comp > 1;
@@ -3034,8 +3363,12 @@ int scatrs_ensemble_mixture(const scatrs_component* components, int64_t n_comp,
                             double* greek_err, int8_t* converged, int64_t* panels, char* err,
                             size_t err_len) {
   return guarded(err, err_len, [&] {
-    std::vector<AdPart> parts = mixture_parts(components, n_comp);
     AdOutputs out{values, errors, phase, phase_err, greek, greek_err, converged, panels};
+    if (heterogeneous(components, n_comp)) {
+      mixture_hetero(components, n_comp, wavelengths, n_wl, mu, n_mu, options, out);
+      return;
+    }
+    std::vector<AdPart> parts = mixture_parts(components, n_comp);
     adaptive_call(parts, 1, false, wavelengths, n_wl, mu, n_mu, options, out);
   });
 }
