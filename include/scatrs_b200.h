@@ -133,8 +133,8 @@ typedef struct scatrs_adaptive_options {
 } scatrs_adaptive_options;
 
 /* greek_order = SCATRS_GREEK_ALL (GreekOrder::All, ensemble/mod.rs:163-170): every order up to
- * 2 N_max at each wavelength (N_max the largest number of terms there), spheres and layered
- * spheres. The call then leaves its greek arrays unwritten; the coefficients of the calling
+ * 2 N_max at each wavelength (N_max the largest number of terms there), spheres, layered
+ * spheres and spheroids (not mixtures of different particles). The call then leaves its greek arrays unwritten; the coefficients of the calling
  * thread's last such call come from scatrs_greek_all_take, (6, n, W) and with derivatives
  * (P, 6, n, W) as the call's other outputs, W = scatrs_greek_all_width() the longest plus one,
  * zero above each wavelength's order (scatrs-py/src/ensemble.rs:419-429). */

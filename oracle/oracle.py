@@ -348,7 +348,7 @@ def ensemble_adaptive_layered(dists: np.ndarray, wavelengths, fractions, m_layer
                                                                               max(nl - 1, 0)))
     mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
     n = dists.size * wl.size
-    L = -1 if greek_order is None else int(greek_order)
+    L = -1 if greek_order is None else (-2 if greek_order == "all" else int(greek_order))
     out = {"values": np.zeros((11, n)), "errors": np.zeros((11, n)),
            "converged": np.zeros(n, dtype=np.int8), "panels": np.zeros(n, dtype=np.int64)}
     ph = pe = g = ge = None
@@ -374,6 +374,8 @@ def ensemble_adaptive_layered(dists: np.ndarray, wavelengths, fractions, m_layer
         out["phase"], out["phase_err"] = ph, pe
     if g is not None:
         out["greek"], out["greek_err"] = g, ge
+    if L == -2:
+        _take_all_orders(out, n)
     return out
 
 
@@ -389,7 +391,7 @@ def ensemble_adaptive_spheroid(dists: np.ndarray, wavelengths, eps: float, m, mu
     m = np.ascontiguousarray(np.broadcast_to(np.asarray(m, dtype=np.complex128), wl.shape))
     mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
     n = dists.size * wl.size
-    L = -1 if greek_order is None else int(greek_order)
+    L = -1 if greek_order is None else (-2 if greek_order == "all" else int(greek_order))
     out = {"values": np.zeros((11, n)), "errors": np.zeros((11, n)),
            "converged": np.zeros(n, dtype=np.int8), "panels": np.zeros(n, dtype=np.int64)}
     ph = pe = g = ge = None
@@ -414,6 +416,8 @@ def ensemble_adaptive_spheroid(dists: np.ndarray, wavelengths, eps: float, m, mu
         out["phase"], out["phase_err"] = ph, pe
     if g is not None:
         out["greek"], out["greek_err"] = g, ge
+    if L == -2:
+        _take_all_orders(out, n)
     return out
 
 

@@ -1071,8 +1071,9 @@ std::vector<UnitOut> direct_outputs(const std::vector<Part>& parts,
                                     int64_t n_mu, int64_t order, bool normalized,
                                     const Options& o) {
   const bool keep = order >= 0 || n_mu > 0;
+  // N_max over the call's groups, each its final panels' (engine.rs:1987-2030, p1.n_terms).
   int64_t n_direct = 0;
-  for (auto& kv : *op.cache) n_direct = std::max<int64_t>(n_direct, kv.second.n);
+  for (const Pass1& p1 : firsts) n_direct = std::max<int64_t>(n_direct, p1.n_terms);
   const int64_t ld = !keep ? -1 : n_mu == 0 ? std::min<int64_t>(order, 2 * n_direct) : 2 * n_direct;
   const int64_t glen = ld + 1, NS = 9, len = NS + 6 * glen;
   auto node = [&](double r, std::vector<double>& g, std::vector<double>& ge) {

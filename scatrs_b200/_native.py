@@ -449,6 +449,8 @@ def ensemble_adaptive_spheroid(dists: np.ndarray, wavelengths, aspect_ratio: flo
         out["phase"], out["phase_err"] = ph, pe
     if g is not None:
         out["greek"], out["greek_err"] = g, ge
+    if L == GREEK_ALL:
+        _take_all_orders(out, n)
     return out
 
 

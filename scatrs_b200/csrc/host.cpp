@@ -2460,8 +2460,9 @@ void spheroid_call(const std::vector<SphParticle>& ps, bool batch, const double*
   for (const SphParticle& q : ps) n_dist += q.n_dist;
   if (n_dist < 0 || n_wl < 0) throw Failure{SCATRS_INVALID_INPUT, "negative sizes"};
   if (batch && ps.size() > 1) throw Failure{SCATRS_INVALID_INPUT, "a batch has one particle"};
-  if (options->greek_order == SCATRS_GREEK_ALL)
-    throw Failure{SCATRS_INVALID_INPUT, "greek='all' for spheroids is not on the GPU path"};
+  const bool all_orders = options->greek_order == SCATRS_GREEK_ALL;
+  if (all_orders && rows)
+    throw Failure{SCATRS_INVALID_INPUT, "greek='all' is not on the GPU path for mixtures"};
   const adaptive::Options o{options->rtol, options->max_panels, options->allow_unvalidated != 0,
                             options->refine_backscatter != 0};
   if (!(o.rtol >= 1e-13 && o.rtol <= 0.1)) {
@@ -2477,7 +2478,7 @@ void spheroid_call(const std::vector<SphParticle>& ps, bool batch, const double*
   for (const SphParticle& q : ps)
     if (!(std::isfinite(q.eps) && q.eps > 0.0))
       throw Failure{SCATRS_INVALID_INPUT, "the aspect ratio must be finite and > 0"};
-  scatrs_fixed_options fo{32, options->greek_order, options->normalized,
+  scatrs_fixed_options fo{32, all_orders ? -1 : options->greek_order, options->normalized,
                           options->allow_unvalidated};
   const int64_t n_units = n_dist * n_wl;
   check_options(&fo, n_units, n_mu, mu);
@@ -2496,7 +2497,7 @@ void spheroid_call(const std::vector<SphParticle>& ps, bool batch, const double*
       particle_of.push_back((int)q);
     }
   const double rtol_t = std::min(std::max(o.rtol / 100.0, 1e-12), 1e-8);
-  const bool keep_greek = options->greek_order >= 0 || n_mu > 0;
+  const bool keep_greek = options->greek_order >= 0 || all_orders || n_mu > 0;
   const double pi = 3.14159265358979323846;
   Context& c = context();
   std::lock_guard<std::mutex> lk(c.mtx);
@@ -2583,11 +2584,29 @@ void spheroid_call(const std::vector<SphParticle>& ps, bool batch, const double*
     if (jb.status != 0) throw Failure{jb.status, jb.msg};
   // The direct order per wavelength: every order to 2N for the phase matrix, else to the
   // requested one (engine.rs:2073-2086).
-  const int L = options->greek_order;
-  std::vector<int64_t> n_direct(n_wl, 0);
-  for (const auto& kv : cache) {
-    const int64_t i = std::get<1>(kv.first);
-    n_direct[i] = std::max<int64_t>(n_direct[i], kv.second.n);
+  // N_max of each unit's call at its wavelength (engine.rs:1987-2030, p1.n_terms over the
+  // final panels): the unit's own part, or every part of a batch or a mixture.
+  std::vector<int64_t> n_own(n_units, 0), n_direct(n_units, 0), n_at(n_wl, 0);
+  for (int64_t u = 0; u < n_units; ++u) {
+    const int64_t p = u / n_wl, i = u % n_wl;
+    n_own[u] = parts[p].support == adaptive::POINT
+                   ? cache.at(key_of(particle_of[p], i, parts[p].lo)).n
+                   : jobs[job_of[u]].n_terms;
+    n_at[i] = std::max(n_at[i], n_own[u]);
+  }
+  for (int64_t u = 0; u < n_units; ++u) n_direct[u] = batch || rows ? n_at[u % n_wl] : n_own[u];
+  // greek='all': every order to 2 N_max (GreekOrder::All), padded to the longest.
+  int64_t width = 0;
+  if (all_orders) {
+    for (int64_t u = 0; u < n_units; ++u) width = std::max(width, 2 * n_direct[u] + 1);
+    GreekAll& ga = t_greek_all;
+    ga.width = width;
+    ga.n = n_units;
+    ga.p = 0;
+    ga.g.assign(6 * n_units * width, 0.0);
+    ga.ge.assign(ga.g.size(), 0.0);
+    ga.dg.clear();
+    ga.dge.clear();
   }
   if (rows) {
     rows->av.assign(n_units, {});
@@ -2601,8 +2620,9 @@ void spheroid_call(const std::vector<SphParticle>& ps, bool batch, const double*
     const int64_t p = u / n_wl, i = u % n_wl;
     const double lambda = wavelengths[i];
     const adaptive::Part& part = parts[p];
-    const int64_t ld = !keep_greek ? -1 : n_mu == 0 ? std::min<int64_t>(L, 2 * n_direct[i])
-                                                      : 2 * n_direct[i];
+    const int L = all_orders ? (int)(2 * n_direct[u]) : options->greek_order;
+    const int64_t ld = !keep_greek ? -1 : n_mu == 0 ? std::min<int64_t>(L, 2 * n_direct[u])
+                                                      : 2 * n_direct[u];
     const int64_t glen = ld + 1;  // 0 without a direct segment
     const int64_t len = kS + 6 * glen;
     // One node's direct quantities and declared errors (direct_scalars, direct_node).
@@ -2725,14 +2745,17 @@ void spheroid_call(const std::vector<SphParticle>& ps, bool batch, const double*
     }
     const bool norm = options->normalized != 0;
     auto G = [&](int f, int64_t l) { return LinE{av[kS + f * glen + l], ae[kS + f * glen + l]}; };
-    if (L >= 0 && res.greek) {
+    if (L >= 0 && (res.greek || all_orders)) {
       const LinE a0 = G(0, 0);
+      double* gv = all_orders ? t_greek_all.g.data() : res.greek;
+      double* ge_out = all_orders ? t_greek_all.ge.data() : res.greek_err;
+      const int64_t w = all_orders ? width : L + 1;
       for (int f = 0; f < 6; ++f)
         for (int64_t l = 0; l <= L; ++l) {
           LinE x = l < glen ? G(f, l) : LinE{};
           if (norm) x = (f == 0 && l == 0) ? LinE{1.0, 0.0} : lin_div(x, a0);
-          res.greek[((int64_t)f * n_units + u) * (L + 1) + l] = x.v;
-          if (res.greek_err) res.greek_err[((int64_t)f * n_units + u) * (L + 1) + l] = x.e;
+          gv[((int64_t)f * n_units + u) * w + l] = x.v;
+          if (ge_out) ge_out[((int64_t)f * n_units + u) * w + l] = x.e;
         }
     }
     if (n_mu > 0 && res.phase) {

@@ -52,3 +52,28 @@ def test_drop_in_spec(gpu):
                                        np.array([1.5 + 0.02j]), None, 4, rtol=1e-3)
     assert np.allclose(raw["values"], ref["values"], rtol=1e-9, atol=0)
     assert raw["greek"].shape == (6, 1, 5)
+
+
+def test_each_distribution_has_its_own_direct_order(gpu):
+    """Every distribution of a call is a call of its own (engine.rs:1987-2030): its direct order,
+    to which the phase matrix's expansion and its error bounds run, follows its own N_max over
+    its final panels."""
+    d = _dists((1, 0.03, 1.3), (1, 0.2, 1.4))
+    wl = np.array([0.6])
+    m = np.array([1.5 + 0.01j])
+    got = gpu.ensemble_adaptive_spheroid(d, wl, 1.4, m, MU, 4, rtol=1e-4)
+    ref = O.ensemble_adaptive_spheroid(_odist(d), wl, 1.4, m, MU, 4, rtol=1e-4)
+    _compare(got, ref)
+
+
+def test_all_orders(gpu):
+    """greek='all': every order to 2 N_max of each distribution, padded to the longest."""
+    from scatrs_b200 import _native
+
+    d = _dists((1, 0.05, 1.4), (1, 0.15, 1.3))
+    wl = np.array([0.5, 0.9])
+    m = np.array([1.5 + 0.01j, 1.45 + 0.001j])
+    got = gpu.ensemble_adaptive_spheroid(d, wl, 0.8, m, MU, _native.GREEK_ALL, rtol=1e-4)
+    ref = O.ensemble_adaptive_spheroid(_odist(d), wl, 0.8, m, MU, "all", rtol=1e-4)
+    assert got["greek"].shape == ref["greek"].shape
+    _compare(got, ref)

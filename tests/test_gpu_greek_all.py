@@ -1,7 +1,8 @@
 """greek='all' (GreekOrder::All) on the GPU: every order up to 2 N_max at each wavelength, the
 arrays padded with zeros to the longest, against the oracle (same widths, same zeros, values and
 error estimates as the adaptive path's tolerances), alone, batched, in a mixture with
-derivatives, and through the reference-facing call; spheroids refuse it."""
+derivatives, and through the reference-facing call (spheroids too); mixtures of different
+particles refuse it."""
 
 import numpy as np
 import pytest
@@ -50,7 +51,11 @@ def test_the_reference_call(gpu):
     ref = gpu.ensemble_adaptive(_dists((1, 0.2, 1.5)), wl, m, MU, _native.GREEK_ALL)
     assert np.array_equal(raw["greek"], ref["greek"])
     assert raw["greek"].shape[-1] > 1 and np.all(raw["greek"][0, :, 0] == 1.0)
-    spheroid = [(("lognormal", 0.2, 1.5), ("spheroid", 1.5, m), 1.0)]
-    with pytest.raises(InvalidInputError, match="spheroids"):
-        _scatrs.ensemble_compute(spheroid, wl, False, None, True, None, True, [], 1e-6, 4096,
-                                 False, False)
+    spheroid = [(("lognormal", 0.05, 1.3), ("spheroid", 1.5, m), 1.0)]
+    sph = _scatrs.ensemble_compute(spheroid, wl, False, None, True, None, True, [], 1e-4, 4096,
+                                   False, False)
+    assert sph["greek"].shape[-1] > 1 and np.all(sph["greek"][0, :, 0] == 1.0)
+    mixed = spheroid + [(("lognormal", 0.2, 1.5), ("sphere", m), 1.0)]
+    with pytest.raises(InvalidInputError, match="mixtures"):
+        _scatrs.ensemble_compute(mixed, wl, True, None, True, None, True, [], 1e-4, 4096, False,
+                                 False)
