@@ -2214,7 +2214,8 @@ void run_tmatrices(Context& c, const std::vector<TmSpec>& specs, std::vector<dou
         g += 6 * (e.L + 1);
         r.n_rank += (int64_t)e.N * e.N;
         r.n_w += Q * 2 * e.N;
-        r.n_phi += Q * e.nq;
+        r.n_phi += Q * ((e.nq + 31) / 32);  // blocks: a tile of 32 cosines per q
+        r.max_n = std::max(r.max_n, e.N);
         r.n_f += e.nq;
         r.n_g += e.L + 1;
         const auto& rl = rule(c, e.nq);

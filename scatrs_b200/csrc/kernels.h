@@ -349,12 +349,13 @@ struct RoSph {
   int64_t f0;     // [6][nq]
   int64_t g0;     // [6][L+1]
   int64_t mu0;    // nq Gauss nodes
-  int64_t t_rank, t_w, t_phi, t_f, t_g;  // first thread of each kernel
+  int64_t t_rank, t_w, t_phi, t_f, t_g;  // first thread of each kernel (ro_phi: first block)
 };
 struct RoArgs {
   const RoSph* sph;
   int n_sph;
-  int64_t n_rank, n_w, n_phi, n_f, n_g;  // threads of each kernel
+  int64_t n_rank, n_w, n_phi, n_f, n_g;  // threads of each kernel (ro_phi: blocks)
+  int max_n;                              // the batch's largest N
   const TmJob* jobs;
   const double* T;  // the batch's T-matrices (complex doubles at each job's T0)
   double *rank, *w, *part, *f, *greek;

@@ -3,15 +3,19 @@
 // and its Greek coefficients (greek_raw, random.rs:283-292), batched over spheroids in five
 // kernels:
 //
-//   ro_rank_kernel   one thread per (spheroid, n, n'): the helicity blocks
+//   ro_rank_kernel   one thread per (spheroid, n, n'), the modes u and -u together: the helicity
+//                    blocks
 //                    T^{p sigma}_mu(n, n') = (T11 + sigma T12 + p T21 + p sigma T22)/2 of every
 //                    mode mu (T^{p sigma}_{-m} = T^{-p,-sigma}_m) and their rank components
 //                    t^(s)(n, n') = sum_mu (-1)^(n'-mu) C^{s 0}_{n mu; n' -mu} T^{p sigma}_mu(n, n');
 //   ro_w_kernel      one thread per (spheroid, q, sigma, n): w_n = sum_n' inc_n' (-1)^(n'-sigma)
-//                    C^{s q}_{n, q+sigma; n', -sigma} t^(s)(n, n') for both scattered helicities;
-//   ro_phi_kernel    one thread per (spheroid, q, cosine): Phi_{sq} = sum_n far_n w_n with
-//                    far_n(m, p) = gamma_n (-i)^n (pi_mn + p tau_mn), and the q-th share of
-//                    <A_a A_b*> = sum_s Phi_a Phi_b* / (2s + 1) for the 16 helicity pairs;
+//                    C^{s q}_{n, q+sigma; n', -sigma} t^(s)(n, n') for both scattered helicities,
+//                    times the cosine-independent part gamma_n (-i)^n of the far field;
+//   ro_phi_kernel    one block per (spheroid, q, tile of 32 cosines), one thread per (cosine,
+//                    helicity key): Phi_{sq} = sum_n w_n (pi_mn + p tau_mn) (the far field's
+//                    angular part, in shared memory for the tile), and the q-th share of
+//                    <A_a A_b*> = sum_s Phi_a Phi_b* / (2s + 1) for the 16 helicity pairs, the
+//                    four keys of a cosine exchanged between adjacent lanes;
 //   ro_f_kernel      one thread per (spheroid, cosine): the shares summed over q in order, and
 //                    the Mueller form F11, F12, F22, F33, F34, F44 (S = U A U^{-1});
 //   ro_greek_kernel  one thread per (spheroid, l): the six projections on the
@@ -147,10 +151,12 @@ __global__ void __launch_bounds__(128) ro_rank_kernel(RoArgs a) {
   }
   double cgv[kS], scratch[kS];
   const int umax = min(n, np);
-  for (int u = -umax; u <= umax; ++u) {
-    const int m = abs(u), n0 = max(m, 1);
+  // Modes u and -u together: T^{p sigma}_{-u} = T^{-p,-sigma}_u and
+  // C^{s 0}_{n,-u; n',u} = (-1)^{n+n'-s} C^{s 0}_{n,u; n',-u}, with the same (-1)^{n'-u}.
+  for (int u = 0; u <= umax; ++u) {
+    const int n0 = max(u, 1);
     if (n < n0 || np < n0) continue;
-    const TmJob& jb = a.jobs[sp.job0 + m];
+    const TmJob& jb = a.jobs[sp.job0 + u];
     const int K = jb.K;
     const C2* T = reinterpret_cast<const C2*>(a.T) + jb.T0;
     const int r = n - n0, c = np - n0;
@@ -159,16 +165,21 @@ __global__ void __launch_bounds__(128) ro_rank_kernel(RoArgs a) {
     const int j0 = cg_vector(n, u, np, -u, cgv, scratch);
     if (j0 < 0) continue;
     const double ph = sgn(np - u);
+    C2 h[2][2];
     for (int pi = 0; pi < 2; ++pi)
       for (int sg = 0; sg < 2; ++sg) {
-        double p = pi ? -1.0 : 1.0, s = sg ? -1.0 : 1.0;
-        if (u < 0) {
-          p = -p;
-          s = -s;
-        }
-        const C2 h = c_scale(c_add(c_add(t11, c_scale(t12, s)), c_add(c_scale(t21, p), c_scale(t22, p * s))), 0.5);
+        const double p = pi ? -1.0 : 1.0, s = sg ? -1.0 : 1.0;
+        h[pi][sg] = c_scale(c_add(c_add(t11, c_scale(t12, s)), c_add(c_scale(t21, p), c_scale(t22, p * s))), 0.5);
+      }
+    for (int pi = 0; pi < 2; ++pi)
+      for (int sg = 0; sg < 2; ++sg) {
         C2* dst = acc[pi * 2 + sg];
-        for (int q = 0; q + j0 <= n + np; ++q) dst[j0 + q - smin] = c_add(dst[j0 + q - smin], c_scale(h, ph * cgv[q]));
+        const C2 hp = h[pi][sg], hm = h[1 - pi][1 - sg];
+        for (int q = 0; q + j0 <= n + np; ++q) {
+          const int J = j0 + q;
+          const C2 hh = u == 0 ? hp : c_add(hp, c_scale(hm, sgn(n + np - J)));
+          dst[J - smin] = c_add(dst[J - smin], c_scale(hh, ph * cgv[q]));
+        }
       }
   }
 }
@@ -204,68 +215,78 @@ __global__ void __launch_bounds__(128) ro_w_kernel(RoArgs a) {
       }
     }
   }
+  // The far field's cosine-independent factor gamma_n (-i)^n (functions.rs:192-239).
+  const C2 fn = c_scale(ipow(-n), sqrt((2.0 * n + 1) / (kPi * 4.0 * n * (n + 1))));
+  for (int p = 0; p < 2; ++p)
+    for (int s = 0; s < S; ++s) at(p, s) = c_mul(at(p, s), fn);
 }
 
 __global__ void __launch_bounds__(128) ro_phi_kernel(RoArgs a) {
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= a.n_phi) return;
-  const int si = owner(a.n_sph, t, [&](int i) { return a.sph[i].t_phi; });
+  extern __shared__ double ro_pt[];  // [2 sigma][N + 1][32 cosines][2]: pi_mn, tau_mn
+  const int b = blockIdx.x, t = threadIdx.x;
+  const int si = owner(a.n_sph, b, [&](int i) { return a.sph[i].t_phi; });
   const RoSph sp = a.sph[si];
-  const int N = sp.N, n1 = N + 1, S = 2 * N + 1, nq = sp.nq;
-  const int idx = (int)(t - sp.t_phi), qi = idx / nq, j = idx % nq, q = qi - N - 1;
-  const double ct = a.mu[sp.mu0 + j], st = sqrt(1.0 - ct * ct);
-  // far[sg][p][n] = gamma_n (-i)^n (pi' + p tau') at this cosine, for m = q + sigma.
-  C2 far[2][2][kRoMaxN + 1];
-  bool on[2];
-  double d[kRoMaxN + 1];
-  for (int sg = 0; sg < 2; ++sg) {
+  const int N = sp.N, n1 = N + 1, S = 2 * N + 1, nq = sp.nq, tiles = (nq + 31) / 32;
+  const int idx = b - (int)sp.t_phi, qi = idx / tiles, q = qi - N - 1;
+  const int key = t & 3, p = key >> 1, sg = key & 1, jl = t >> 2, j = (idx % tiles) * 32 + jl;
+  const bool valid = j < nq;
+  // The angular parts at this thread's cosine for both sigma (threads of key 0 and 1):
+  // normalized d_{|m| n}, pi and tau (functions.rs:192-239), m = q + sigma, zero where |m| > N.
+  if (p == 0) {
+    double* pt = ro_pt + (int64_t)sg * n1 * 64;
+    for (int k = 0; k <= N; ++k) {
+      pt[(k * 32 + jl) * 2] = 0.0;
+      pt[(k * 32 + jl) * 2 + 1] = 0.0;
+    }
     const int m = q + (sg ? -1 : 1), am = abs(m);
-    on[sg] = am <= N;
-    for (int k = 0; k <= N; ++k) far[sg][0][k] = far[sg][1][k] = C2{0, 0};
-    if (!on[sg]) continue;
-    // Normalized d_{am n}, pi, tau (functions.rs:192-239).
-    double am_ = 1.0;
-    for (int k = 1; k <= am; ++k) am_ *= sqrt((double)(2 * k - 1) / (2 * k));
-    for (int k = 0; k <= N; ++k) d[k] = 0.0;
-    double sp_ = 1.0;
-    for (int k = 0; k < am; ++k) sp_ *= st;
-    d[am] = am_ * sp_;
-    if (am < N) d[am + 1] = sqrt(2.0 * am + 1) * ct * d[am];
-    for (int k = am + 1; k < N; ++k)
-      d[k + 1] = ((2 * k + 1) * ct * d[k] - sqrt((double)k * k - (double)am * am) * d[k - 1]) /
-                 sqrt((double)(k + 1) * (k + 1) - (double)am * am);
-    const double flip = m < 0 ? sgn(am) : 1.0;
-    for (int k = max(am, 1); k <= N; ++k) {
-      const double prev = k > am ? d[k - 1] : 0.0;
-      const double tau = (k * ct * d[k] - sqrt((double)k * k - (double)am * am) * prev) / st;
-      const double pi = am * d[k] / st;
-      const double tk = tau * flip, pk = m < 0 ? -(pi * flip) : pi;
-      const double g = sqrt((2.0 * k + 1) / (kPi * 4.0 * k * (k + 1)));
-      const C2 f = c_scale(ipow(-k), g);
-      far[sg][0][k] = c_scale(f, pk + tk);
-      far[sg][1][k] = c_scale(f, pk - tk);
-    }
-  }
-  const C2* w = reinterpret_cast<const C2*>(a.w + sp.w0);
-  C2 prod[16];
-  for (int k = 0; k < 16; ++k) prod[k] = C2{0, 0};
-  for (int s = 0; s < S; ++s) {
-    C2 phi[4];
-    for (int key = 0; key < 4; ++key) {
-      const int p = key / 2, sg = key % 2;
-      C2 v{0, 0};
-      if (on[sg]) {
-        const C2* wr = w + (((int64_t)(qi * 2 + sg) * 2 + p) * S + s) * n1;
-        for (int n = 1; n <= N; ++n) v = c_add(v, c_mul(wr[n], far[sg][p][n]));
+    if (valid && am <= N) {
+      const double ct = a.mu[sp.mu0 + j], st = sqrt(1.0 - ct * ct);
+      double am_ = 1.0;
+      for (int k = 1; k <= am; ++k) am_ *= sqrt((double)(2 * k - 1) / (2 * k));
+      double sp_ = 1.0;
+      for (int k = 0; k < am; ++k) sp_ *= st;
+      const double flip = m < 0 ? sgn(am) : 1.0;
+      double dprev = 0.0, dk = am_ * sp_;  // d_{am - 1} = 0, d_{am}
+      for (int k = am; k <= N; ++k) {
+        if (k >= 1) {
+          const double tau = (k * ct * dk - sqrt((double)k * k - (double)am * am) * dprev) / st;
+          const double pi = am * dk / st;
+          pt[(k * 32 + jl) * 2] = m < 0 ? -(pi * flip) : pi;
+          pt[(k * 32 + jl) * 2 + 1] = tau * flip;
+        }
+        double dnext;
+        if (k == am)
+          dnext = sqrt(2.0 * am + 1) * ct * dk;
+        else
+          dnext = ((2 * k + 1) * ct * dk - sqrt((double)k * k - (double)am * am) * dprev) /
+                  sqrt((double)(k + 1) * (k + 1) - (double)am * am);
+        dprev = dk;
+        dk = dnext;
       }
-      phi[key] = v;
     }
-    const double inv = 1.0 / (2 * s + 1);
-    for (int x = 0; x < 4; ++x)
-      for (int y = 0; y < 4; ++y) prod[x * 4 + y] = c_add(prod[x * 4 + y], c_scale(c_mul(phi[x], c_conj(phi[y])), inv));
   }
-  C2* part = reinterpret_cast<C2*>(a.part + sp.part0);
-  for (int k = 0; k < 16; ++k) part[((int64_t)qi * 16 + k) * nq + j] = prod[k];
+  __syncthreads();
+  // Phi over s for this key; the 16 products with the other keys of the same cosine.
+  const C2* wr = reinterpret_cast<const C2*>(a.w + sp.w0) + ((int64_t)(qi * 2 + sg) * 2 + p) * S * n1;
+  const double* pt = ro_pt + (int64_t)sg * n1 * 64 + jl * 2;
+  const double sign = p ? -1.0 : 1.0;
+  C2 prod[4] = {C2{0, 0}, C2{0, 0}, C2{0, 0}, C2{0, 0}};
+  for (int s = 0; s < S; ++s) {
+    C2 v{0, 0};
+    const C2* ws = wr + (int64_t)s * n1;
+    for (int n = 1; n <= N; ++n) v = c_add(v, c_scale(ws[n], pt[n * 64] + sign * pt[n * 64 + 1]));
+    const double inv = 1.0 / (2 * s + 1);
+    C2 other[4];
+    for (int y = 0; y < 4; ++y) {
+      other[y].re = __shfl_sync(0xffffffffu, v.re, y, 4);
+      other[y].im = __shfl_sync(0xffffffffu, v.im, y, 4);
+    }
+    for (int y = 0; y < 4; ++y) prod[y] = c_add(prod[y], c_scale(c_mul(v, c_conj(other[y])), inv));
+  }
+  if (valid) {
+    C2* part = reinterpret_cast<C2*>(a.part + sp.part0);
+    for (int y = 0; y < 4; ++y) part[((int64_t)qi * 16 + key * 4 + y) * nq + j] = prod[y];
+  }
 }
 
 __global__ void __launch_bounds__(128) ro_f_kernel(RoArgs a) {
@@ -339,7 +360,17 @@ void launch_random(const RoArgs& a, cudaStream_t s) {
   auto grid = [](int64_t n) { return (unsigned)((n + 127) / 128); };
   ro_rank_kernel<<<grid(a.n_rank), 128, 0, s>>>(a);
   ro_w_kernel<<<grid(a.n_w), 128, 0, s>>>(a);
-  ro_phi_kernel<<<grid(a.n_phi), 128, 0, s>>>(a);
+  // Shared memory: pi and tau of both sigma at a tile of 32 cosines for the batch's largest N.
+  const size_t pt_bytes = (size_t)2 * (a.max_n + 1) * 32 * 2 * sizeof(double);
+  static bool configured[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev >= 0 && dev < 64 && !configured[dev]) {
+    cudaFuncSetAttribute(ro_phi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)((size_t)2 * (kRoMaxN + 1) * 32 * 2 * sizeof(double)));
+    configured[dev] = true;
+  }
+  ro_phi_kernel<<<(unsigned)a.n_phi, 128, pt_bytes, s>>>(a);
   ro_f_kernel<<<grid(a.n_f), 128, 0, s>>>(a);
   ro_greek_kernel<<<grid(a.n_g), 128, 0, s>>>(a);
 }
