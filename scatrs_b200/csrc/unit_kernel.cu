@@ -62,6 +62,7 @@ struct Smem {
   double w[32], cu[32], area[32], sc[32];
   double wth[3][32];  // the distribution parameters' weights (derivatives only)
   double wd[32], wthd[3][32];  // adaptive derivatives: the error weights (w_K - w_G) ...
+  int nn[32];  // each node's number of terms plus one (an upper bound of K-a's), 0 for padding
   double S[8];
   int slot;
 };
@@ -149,6 +150,11 @@ __device__ __forceinline__ void gemm_tile_mma(Smem& sm, const double* __restrict
       cE[mt][nt][0] = cE[mt][nt][1] = 0.0;
       cO[mt][nt][0] = cO[mt][nt][1] = 0.0;
     }
+  // This warp's nodes (8 w .. 8 w + 7) have no coefficients above their largest number of
+  // terms (K-a writes zero rows up to the chunk's): its MMAs stop there.
+  int wmax = 0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) wmax = max(wmax, sm.nn[8 * w + i]);
   load_stage_z(sm, 0, ge, go, ldr, r0, 0, nc, xc);
   int st = 0;
   for (int k0 = 0; k0 < nc; k0 += KB, st ^= 1) {
@@ -158,7 +164,7 @@ __device__ __forceinline__ void gemm_tile_mma(Smem& sm, const double* __restrict
     const int kend = nc - k0 < KB ? nc - k0 : KB;
 #pragma unroll
     for (int k4 = 0; k4 < KB; k4 += 4) {
-      if (k4 < kend) {
+      if (k4 < kend && k0 + k4 < wmax) {
         const int kk = k4 + q;
         double aE[4], aO[4], b[4];
 #pragma unroll
@@ -476,11 +482,14 @@ __device__ __forceinline__ void unit_body(const UnitArgs& a) {
       if (t < 32) {
         const int j = c * 32 + t;
         double w = 0.0, cu = 0.0, ar = 0.0, sc = 0.0, wd = 0.0;
+        int nn = 0;
         double wth[3] = {0.0, 0.0, 0.0}, wthd[3] = {0.0, 0.0, 0.0};
         const int64_t node = (a.per_unit ? unit : d) * a.n_nodes + j;
         if (j < a.n_nodes && a.radius[node] > 0.0) {
           const double r = a.radius[node];
           const double x = 2.0 * kPi * r / lam;
+          // ceil(x + 6 x^(1/3) + 3), the truncation, plus one for a contraction's rounding.
+          nn = (int)ceil(x + 6.0 * cbrt(x) + 3.0) + 1;
           w = a.weight[node];  // w_j u(r_j) r_j
           cu = 4.0 / (x * x);
           ar = kPi * r * r;
@@ -497,6 +506,7 @@ __device__ __forceinline__ void unit_body(const UnitArgs& a) {
         sm.cu[t] = cu;
         sm.area[t] = ar;
         sm.sc[t] = sc;
+        sm.nn[t] = nn;
         if (kDeriv || kMode == 2)
           for (int p = 0; p < 3; ++p) sm.wth[p][t] = wth[p];
         if (kAdD) {
