@@ -227,8 +227,8 @@ typedef struct scatrs_param {
  * blocks (weights du/dtheta r) and the derivatives along Re m and Im m, the averages follow
  * the quotient rule against the moments' dZ, the mixing adds the weight derivatives, and the
  * ratios carry the derivatives with first-order error estimates (ensemble/lin.rs). A component
- * is multimodal when its mode_weights are given. Spheres only; not for a single radius's
- * radius. d_values, d_errors (P, 11, n_wl); d_phase, d_phase_err (P, 6, n_wl, n_mu); d_greek,
+ * is multimodal when its mode_weights are given. Spheres only; a single radius's radius is
+ * exact (engine.rs:1158-1170), with zero error estimates. d_values, d_errors (P, 11, n_wl); d_phase, d_phase_err (P, 6, n_wl, n_mu); d_greek,
  * d_greek_err (P, 6, n_wl, L + 1), P = n_params, in the order of `params`. Invalid or
  * repeated parameters: SCATRS_INVALID_INPUT naming the parameter.
  * Replaces: the derivative path of Mixture::compute / Ensemble.compute(derivatives=...)

@@ -851,9 +851,12 @@ struct Layout {
 // area) and the band's tables (fast.rs:95-205) of one solved sphere into g; with dm (a sphere
 // solved with derivatives), their derivatives along Re m and Im m into dm[0..len) and
 // dm[len..2 len) (the amplitudes' derivatives dS/dm and i dS/dm; phase.rs:289-341).
+// With dr, the derivatives with respect to r at fixed m go there (engine.rs:1158-1170):
+// 2 pi r Q + pi r^2 (2 pi / lambda) dQ/dx for the scalars, 2 r and 3 r^2 for r^2 and r^3, and
+// 2 pi r F + pi r^2 (2 pi / lambda) dF/dx for the unnormalized phase tables F.
 void quantities2(const MieState& st, int64_t n, double r, double lambda, const Layout& L,
                  const double* mu, int band, int64_t band_terms, double* g,
-                 double* dm = nullptr) {
+                 double* dm = nullptr, double* dr = nullptr) {
   const double x = size_param(r, lambda);
   const Efficiencies q = efficiencies(st);
   const double area = PI * r * r;
@@ -862,6 +865,18 @@ void quantities2(const MieState& st, int64_t n, double r, double lambda, const L
                               area * q.q_abs, area * q.q_back, r * r,         r * r * r,
                               0.0};
   for (int k = 0; k < SCALARS; ++k) g[k] = sc[k];
+  const double kw = 2.0 * PI / lambda;
+  if (dr) {
+    const Efficiencies e = efficiency_x(st, q);
+    const double values[6] = {0.0, q.q_ext, q.q_sca, q.q_sca * q.g, q.q_abs, q.q_back};
+    const double dx[6] = {0.0, area * e.q_ext, area * e.q_sca,
+                          area * (e.q_sca * q.g + q.q_sca * e.g), area * e.q_abs, area * e.q_back};
+    for (int j = 1; j < 6; ++j) dr[j] = 2.0 * PI * r * values[j] + kw * dx[j];
+    dr[S_ONE] = 0.0;
+    dr[S_R2] = 2.0 * r;
+    dr[S_R3] = 3.0 * r * r;
+    dr[SCALARS - 1] = 0.0;
+  }
   if (dm) {
     for (int dir = 0; dir < 2; ++dir) {
       const Efficiencies e = efficiency_dir(st, dir, q);
@@ -878,8 +893,17 @@ void quantities2(const MieState& st, int64_t n, double r, double lambda, const L
     }
   }
   const double cph = 4.0 / (x * x);
+  // d(cph F)/dx of the unnormalized tables, cph = 4/x^2.
+  auto table_dr = [&](cplx s1, cplx s2, cplx x1, cplx x2, double c, double* out, int64_t stride) {
+    double e[4], de[4];
+    elements(s1, s2, e);
+    element_derivs(s1, s2, x1, x2, de);
+    for (int t = 0; t < 4; ++t)
+      out[t * stride] = 2.0 * PI * r * (c * e[t]) + area * kw * (c * de[t] - 2.0 / x * (c * e[t]));
+  };
   for (int64_t j = 0; j < L.n_mu; ++j) {
     cplx s1 = real(0.0), s2 = real(0.0), d1 = real(0.0), d2 = real(0.0);
+    cplx x1 = real(0.0), x2 = real(0.0);
     for_each_order(mu[j], n, [&](int64_t k, double pi, double tau) {
       s1 = s1 + scale(st.a[k - 1], pi) + scale(st.b[k - 1], tau);
       s2 = s2 + scale(st.a[k - 1], tau) + scale(st.b[k - 1], pi);
@@ -887,7 +911,12 @@ void quantities2(const MieState& st, int64_t n, double r, double lambda, const L
         d1 = d1 + scale(st.da_dm[k - 1], pi) + scale(st.db_dm[k - 1], tau);
         d2 = d2 + scale(st.da_dm[k - 1], tau) + scale(st.db_dm[k - 1], pi);
       }
+      if (dr) {
+        x1 = x1 + scale(st.da_dx[k - 1], pi) + scale(st.db_dx[k - 1], tau);
+        x2 = x2 + scale(st.da_dx[k - 1], tau) + scale(st.db_dx[k - 1], pi);
+      }
     });
+    if (dr) table_dr(s1, s2, x1, x2, cph, dr + SCALARS + j, L.n_mu);
     double e[4];
     elements(s1, s2, e);
     for (int t = 0; t < 4; ++t) g[SCALARS + t * L.n_mu + j] = cph * e[t] * area;
@@ -911,8 +940,9 @@ void quantities2(const MieState& st, int64_t n, double r, double lambda, const L
     // ce = G_E X and co = G_O X over the sphere's 4 columns and, with derivatives, its 4
     // derivative columns (fast.rs:98-145).
     double ce[8] = {0, 0, 0, 0, 0, 0, 0, 0}, co[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    double cx[4] = {0, 0, 0, 0}, cy[4] = {0, 0, 0, 0};  // the x derivative columns
     for (int64_t k = 0; k < terms; ++k) {
-      double xr[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      double xr[8] = {0, 0, 0, 0, 0, 0, 0, 0}, xx[4] = {0, 0, 0, 0};
       if (k < n) {
         const cplx uu = (k % 2 == 0) ? st.a[k] : st.b[k];
         const cplx vv = (k % 2 == 0) ? st.b[k] : st.a[k];
@@ -928,11 +958,23 @@ void quantities2(const MieState& st, int64_t n, double r, double lambda, const L
           xr[6] = dv.re;
           xr[7] = dv.im;
         }
+        if (dr) {
+          const cplx du = (k % 2 == 0) ? st.da_dx[k] : st.db_dx[k];
+          const cplx dv = (k % 2 == 0) ? st.db_dx[k] : st.da_dx[k];
+          xx[0] = du.re;
+          xx[1] = du.im;
+          xx[2] = dv.re;
+          xx[3] = dv.im;
+        }
       }
       const double ge = B.ge[ii * B.upper + k], go = B.go[ii * B.upper + k];
       for (int t = 0; t < 8; ++t) {
         ce[t] += ge * xr[t];
         co[t] += go * xr[t];
+      }
+      for (int t = 0; t < 4; ++t) {
+        cx[t] += ge * xx[t];
+        cy[t] += go * xx[t];
       }
     }
     const cplx eu = C(ce[0], ce[1]), ev = C(ce[2], ce[3]);
@@ -940,11 +982,16 @@ void quantities2(const MieState& st, int64_t n, double r, double lambda, const L
     const cplx deu = C(ce[4], ce[5]), dev = C(ce[6], ce[7]);
     const cplx dou = C(co[4], co[5]), dov = C(co[6], co[7]);
     const int64_t jn = lo + ii;
+    const cplx xeu = C(cx[0], cx[1]), xev = C(cx[2], cx[3]);
+    const cplx xou = C(cy[0], cy[1]), xov = C(cy[2], cy[3]);
     auto write = [&](int64_t node, double sign) {
       const cplx s1 = eu + scale(ov, sign), s2 = ev + scale(ou, sign);
       double e[4];
       elements(s1, s2, e);
       for (int t = 0; t < 4; ++t) out[t * qn + node] = scl * e[t];
+      if (dr)
+        table_dr(s1, s2, xeu + scale(xov, sign), xev + scale(xou, sign), 4.0 / (x * x),
+                 dr + L.start[band] + node, qn);
       if (dm) {
         const cplx d1 = deu + scale(dov, sign), d2 = dev + scale(dou, sign);
         double fr[4], fi[4];
@@ -1388,19 +1435,25 @@ std::vector<UnitOut> wavelength(const std::vector<Part>& parts,
     if (parts[grp[0]].support == POINT) {
       // monodisperse (engine.rs:1838-1890): the particle itself, exact.
       const Part& part = parts[grp[0]];
-      if (!part.theta.empty())
-        throw Failure{INVALID_INPUT,
-                      "the derivative along a single radius is not on this path"};
+      const bool radius = !part.theta.empty();  // monodisperse: radius, its one parameter
+      if (radius && !m.fr.empty())
+        throw Failure{INVALID_INPUT, "the radius derivative of a layered sphere is not here"};
       const double r = part.s_a;
       int64_t n;
-      solve(r, lambda, m, o.allow_unvalidated, st, &n, derivs);
+      solve(r, lambda, m, o.allow_unvalidated, st, &n, derivs || radius);
       std::fill(g.begin(), g.end(), 0.0);
       std::fill(dmv.begin(), dmv.end(), 0.0);
+      std::vector<double> drv(radius ? len : 0, 0.0);
       const int band = order >= 0 ? L.band_of(n) : -1;
-      quantities2(st, n, r, lambda, L, mu, band, n, g.data(), derivs ? dmv.data() : nullptr);
+      quantities2(st, n, r, lambda, L, mu, band, n, g.data(), derivs ? dmv.data() : nullptr,
+                  radius ? drv.data() : nullptr);
       Avg& a = avg[grp[0]];
       a.v = g;
       a.e.assign(len, 0.0);
+      if (radius) {
+        a.d.push_back({part.theta[0].first, drv});
+        a.de.push_back({part.theta[0].first, std::vector<double>(len, 0.0)});
+      }
       for (int dir = 0; dir < 2; ++dir)
         if (part.dir_col[dir] >= 0) {
           a.d.push_back({part.dir_col[dir],

@@ -608,6 +608,37 @@ inline Efficiencies efficiencies(const MieState& st) {
   return efficiencies_from(st.x, st.abs_sum, value_sums(st.a.data(), st.b.data(), st.a.size()));
 }
 
+// The efficiencies' derivatives along the size parameter x at fixed m of a sphere solved with
+// derivatives: derivative_sums along da/dx, db/dx and efficiencies_jacobian's x column with its
+// -(2/x) Q term (efficiencies.rs:89-146, 192-230).
+inline Efficiencies efficiency_x(const MieState& st, const Efficiencies& q) {
+  const int64_t n = (int64_t)st.a.size();
+  const Sums vs = value_sums(st.a.data(), st.b.data(), n);
+  double sca = 0.0, g = 0.0;
+  cplx back = real(0.0);
+  for (int64_t k = 1; k <= n; ++k) {
+    const cplx ak = st.a[k - 1], bk = st.b[k - 1], dak = st.da_dx[k - 1], dbk = st.db_dx[k - 1];
+    const double w = (double)(2 * k + 1), kf = (double)k;
+    const double pair = kf * (kf + 2.0) / (kf + 1.0);
+    const double own = w / (kf * (kf + 1.0));
+    sca += w * 2.0 * (re_mul_conj(dak, ak) + re_mul_conj(dbk, bk));
+    const cplx t = scale(dak - dbk, w);
+    back = (k % 2 == 0) ? back + t : back - t;
+    if (k < n) {
+      const cplx a1 = st.a[k], b1 = st.b[k], da1 = st.da_dx[k], db1 = st.db_dx[k];
+      g += pair * (re_mul_conj(dak, a1) + re_mul_conj(ak, da1) + re_mul_conj(dbk, b1) +
+                   re_mul_conj(bk, db1));
+    }
+    g += own * (re_mul_conj(dak, bk) + re_mul_conj(ak, dbk));
+  }
+  const double inv_x = 1.0 / st.x, inv_x2 = inv_x * inv_x, two_x2 = 2.0 * inv_x2;
+  const double dsca = two_x2 * sca - 2.0 * inv_x * q.q_sca;
+  const double dabs = two_x2 * st.abs_sum_jacobian[0] - 2.0 * inv_x * q.q_abs;
+  const double dback = 2.0 * re_mul_conj(back, vs.back) * inv_x2 - 2.0 * inv_x * q.q_back;
+  const double dg = vs.sca == 0.0 ? 0.0 : (2.0 * g - q.g * sca) / vs.sca;
+  return {dsca + dabs, dsca, dabs, dback, dg};
+}
+
 // The efficiencies' derivatives along direction p (0: Re m, 1: Im m, with d/d(Im m) = i d/dm)
 // of a sphere solved with derivatives: derivative_sums (efficiencies.rs:89-146) and
 // efficiencies_jacobian (192-230). q are the sphere's efficiencies.

@@ -1178,11 +1178,15 @@ void adaptive_flags(const std::vector<AdPart>& in, const std::vector<adaptive::J
 // weight derivatives df (2141-2176: of w/w_total for a component's weight, of v/v_total for a
 // mode's), then the ratios, normalizations and bounds with the derivatives (lin.rs,
 // engine.rs:2396-2497) and the Greek coefficients normalized by the mixture's alpha1_0.
+// hav_x: with single radii whose radius is asked for, the rows of the pass along x, whose Re m
+// block is d/dx of every slot at fixed m; d/dr = (2 pi / lambda) d/dx there (pi r^2 (2/x^2) is
+// constant: the 2 pi r Q term of engine.rs:1158-1170 cancels the -2/x Q of dQ/dx), with 2 r and
+// 3 r^2 for <r^2> and <r^3>.
 void mix_derivatives(const std::vector<AdPart>& in, const std::vector<adaptive::Part>& parts,
                      int n_out, int64_t n_wl, int64_t n_mu, int greek_order, bool normalized,
                      int n_theta, const std::vector<double>& hav, const AdDerivs& dd,
-                     const AdOutputs& res) {
-  (void)parts;
+                     const AdOutputs& res, const double* wavelengths,
+                     const std::vector<double>& hav_x) {
   const int B = 3 + n_theta;
   const int64_t glen = greek_order >= 0 ? greek_order + 1 : 0;
   const int64_t row = 8 + 4 * n_mu + 6 * glen, stride = 2 * B * row;
@@ -1226,6 +1230,15 @@ void mix_derivatives(const std::vector<AdPart>& in, const std::vector<adaptive::
             d[col * row + k] += a.f * av[2 * b * row + k];
             de[col * row + k] += a.f * av[(2 * b + 1) * row + k];
           }
+        }
+        if (parts[p].support == adaptive::POINT && !a.grads.empty() && !hav_x.empty()) {
+          // monodisperse (engine.rs:1857-1883): exact, no error estimate.
+          const int col = a.theta_cols[0];
+          const double r = parts[p].lo, kw = 2.0 * kPi / wavelengths[i];
+          const double* ax = hav_x.data() + ((int64_t)p * n_wl + i) * stride +
+                             2 * (n_theta + 1) * row;
+          for (int64_t k = 1; k < row; ++k)
+            d[col * row + k] += a.f * (k == 6 ? 2.0 * r : k == 7 ? 3.0 * r * r : kw * ax[k]);
         }
       }
       for (size_t col = 0; col < P; ++col) {
@@ -1376,6 +1389,7 @@ void adaptive_call_order(const std::vector<AdPart>& in, int n_out, bool batch,
   if (n_units == 0 || n_out == 0) return;
   const bool deriv = dd && dd->n > 0;
   std::vector<adaptive::Part> parts;
+  bool radius_x = false;  // a single radius's radius: a pass along x
   int n_theta = 0;  // the most requested distribution parameters of a part
   bool any_dirs = false;
   for (const AdPart& p : in) {
@@ -1388,9 +1402,7 @@ void adaptive_call_order(const std::vector<AdPart>& in, int n_out, bool batch,
     parts.back().dirs[1] = p.dir_cols[1] >= 0;
     n_theta = std::max(n_theta, (int)p.grads.size());
     any_dirs = any_dirs || parts.back().dir_derivatives();
-    if (!p.grads.empty() && parts.back().support == adaptive::POINT)
-      throw Failure{SCATRS_INVALID_INPUT,
-                    p.who + "the derivative along a single radius is not on the GPU path"};
+    if (!p.grads.empty() && parts.back().support == adaptive::POINT) radius_x = true;
   }
   Context& c = context();
   std::lock_guard<std::mutex> lk(c.mtx);
@@ -1695,11 +1707,23 @@ void adaptive_call_order(const std::vector<AdPart>& in, int n_out, bool batch,
   if (deriv) {
     call.radius = std::move(radius);
     check_device_errors(c, s, &call);
-    std::vector<double> hav((size_t)n_units * stride);
+    std::vector<double> hav((size_t)n_units * stride), hav_x;
     SB_CUDA(cudaMemcpyAsync(hav.data(), avg, hav.size() * 8, cudaMemcpyDeviceToHost, s));
     SB_CUDA(cudaStreamSynchronize(s));
+    if (radius_x) {
+      // The single radii's derivatives along x (engine.rs:1158-1170, 1857-1883): the pipeline
+      // again with K-a's x direction in place of Re m.
+      DerivOutput dvx = dvo;
+      dvx.dir = 1;
+      run_fixed(c, dummy.data(), n_parts, wl_d, n_wl, m_d, mu, n_mu, &fo, nullptr, nullptr,
+                nullptr, s, &call, li, dvx, ad);
+      check_device_errors(c, s, &call);
+      hav_x.resize(hav.size());
+      SB_CUDA(cudaMemcpyAsync(hav_x.data(), avg, hav_x.size() * 8, cudaMemcpyDeviceToHost, s));
+      SB_CUDA(cudaStreamSynchronize(s));
+    }
     mix_derivatives(in, parts, n_out, n_wl, n_mu, options->greek_order, options->normalized != 0,
-                    n_theta, hav, *dd, res);
+                    n_theta, hav, *dd, res, wavelengths, hav_x);
     adaptive_flags(in, jobs, job_of, unit_converged, unit_panels, n_out, n_wl, res);
     return;
   }

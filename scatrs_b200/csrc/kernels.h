@@ -42,7 +42,9 @@ struct MieFixedArgs {
   // Derivatives (homogeneous spheres): chunk rows of two 16-node halves, chunk_sums
   // [n_chunks][3 + n_theta][8], and the parameter weights w_j (du/dtheta_p)(r_j) r_j.
   int deriv;
-  int deriv_dir;  // layered spheres: 0..L-1 along layer l's index, L..2L-2 along f_{l-L}
+  int deriv_dir;  // layered spheres: 0..L-1 along layer l's index, L..2L-2 along f_{l-L};
+                  // homogeneous spheres: 0 along m, 1 along x at fixed m (the Re m block, with
+                  // the efficiencies' derivatives without their -2/x Q term)
   int n_theta;
   const double* wtheta;  // [n_dist][n_nodes][3]
   // Adaptive panels: nodes per unit ([n_units][n_nodes], radius 0 for padding), two GK15 panels

@@ -293,9 +293,13 @@ struct NoDeriv {
 // The derivatives along the refractive index of a homogeneous sphere (kernel.rs:486-532):
 // da/dm, db/dm per order go to emit(k, a_k, b_k, da_k/dm, db_k/dm), and the absorption sum's
 // derivatives along Re m and Im m (d/d(Im m) = i d/dm) accumulate here.
+// With along_x, emit receives the derivatives along the size parameter x at fixed m instead,
+// and abs_x the absorption sum's (kernel.rs:501-518, 509-516).
 struct MDeriv {
   static constexpr bool kOn = true;
   double abs_re = 0.0, abs_im = 0.0;
+  bool along_x = false;
+  double abs_x = 0.0;
 };
 
 // State::finish (kernel.rs:324-559): calls emit(k, a_k, b_k) for k = 1..n and returns the
@@ -346,7 +350,7 @@ __device__ __forceinline__ double mie_finish(double x, cplx m, int64_t n, const 
     cplx md = hh_b * m;
     cplx big_a = d_m + rl(k_x);
     cplx big_b = md + rl(k_x);
-    cplx an, bn, inv_da, inv_db, g_a, g_b;
+    cplx an, bn, inv_da, inv_db, g_a, g_b, h_a, h_b;
     if (k <= n_s) {
       double c = (double)(2 * k - 1) * inv_x;
       double psi_next = c * psi - psi_prev;
@@ -376,6 +380,8 @@ __device__ __forceinline__ double mie_finish(double x, cplx m, int64_t n, const 
       if (Deriv::kOn) {
         g_a = xi * inv_da;
         g_b = xi * inv_db;
+        h_a = xi_prev * inv_da;
+        h_b = xi_prev * inv_db;
       }
       if (k == n_s) {
         inv_xi = cinv(xi);
@@ -403,6 +409,10 @@ __device__ __forceinline__ double mie_finish(double x, cplx m, int64_t n, const 
       inv_db = inv_xi * ib;
       g_a = ia;
       g_b = ib;
+      if (Deriv::kOn) {
+        h_a = r * ia;
+        h_b = r * ib;
+      }
     }
     vs.add(k, an, bn);
     double na = nsq(inv_da);
@@ -418,6 +428,24 @@ __device__ __forceinline__ double mie_finish(double x, cplx m, int64_t n, const 
       cplx d_minus = scl(d, two) - d_plus;
       cplx ida2 = inv_da * inv_da;
       cplx idb2 = inv_db * inv_db;
+      if (deriv->along_x) {
+        // da/dx and db/dx at fixed m (kernel.rs:501-504); D' = n(n+1)/z^2 - 1 - D^2 in terms
+        // of u, and the absorption sum's x term (kernel.rs:509-516).
+        const double kk1 = kf * (double)(k + 1);
+        cplx dan = cti(m2_minus_1) * (d * d + rl(kk1 * inv_x * inv_x)) * inv_m2 * ida2;
+        cplx dbn = cti(m2_minus_1) * idb2;
+        emit(k, an, bn, dan, dbn);
+        cplx dp = scl(scl(u_z1, two) * inv_z - inv_z * inv_z, (double)(k + 1)) - one_u2;
+        const cplx m2 = m * m;
+        const double k_x2 = k_x * inv_x;
+        cplx la_x = g_a * (dp - rl(k_x2) - scl(big_a, k_x) + rl(one)) + h_a * d_m;
+        cplx lb_x = g_b * (m2 * dp - rl(k_x2) - scl(big_b, k_x) + rl(one)) + h_b * md;
+        auto term = [&](cplx f, cplx df, cplx l, double n2) {
+          return -((df.im - two * f.im * l.re) * n2);
+        };
+        deriv->abs_x += weight * (term(d_m, dp, la_x, na) + term(md, m2 * dp, lb_x, nb));
+        continue;
+      }
       cplx dan = cti(d_minus) * inv_m2 * ida2;
       cplx dbn = -(cti(d_plus) * idb2);
       emit(k, an, bn, dan, dbn);

@@ -194,6 +194,7 @@ __device__ __forceinline__ void mie_chunk_deriv(const MieFixedArgs& a) {
     ValueSums vs;
     DerivSums ds;
     MDeriv md;
+    md.along_x = a.deriv_dir == 1;  // the x pass: derivatives along x at fixed m
     const double2 mv = a.m[unit];
     const cplx m = mk(mv.x, mv.y);
     const int st = check_node(x, m, n, a.allow_unvalidated != 0);
@@ -223,7 +224,8 @@ __device__ __forceinline__ void mie_chunk_deriv(const MieFixedArgs& a) {
                             area * e.q_abs, area * e.q_back, r * r,         r * r * r};
       for (int k = 0; k < 8; ++k) qv[k] = q0[k];
       for (int p = 0; p < 2; ++p) {
-        const Eff de = efficiency_derivs(x, vs, e, ds, p, p == 0 ? md.abs_re : md.abs_im);
+        const Eff de = efficiency_derivs(x, vs, e, ds, p,
+                                         p == 0 ? (md.along_x ? md.abs_x : md.abs_re) : md.abs_im);
         const double q1[8] = {0.0,
                               area * de.q_ext,
                               area * de.q_sca,

@@ -62,11 +62,31 @@ def test_a_lognormal_matches_the_oracle(gpu):
     ((3, 2.0, 15.0, 0.5), [(0, -1, IM, 0), (0, -1, PD, 2)]),  # Im m and gamma
     ((4, 3.0, 0.02, 1.0), [(0, -1, PD, 0), (0, -1, RE, 0)]),  # finite support
     ((5, 0.3), [(0, -1, IM, 0), (0, -1, RE, 0)]),             # a single radius along m
+    ((5, 0.3), [(0, -1, PD, 0)]),                             # its radius (engine.rs:1158-1170)
 ])
 def test_other_kinds_match_the_oracle(gpu, dist, params):
     wl = np.array([0.55, 0.9])
     m = np.array([1.45 + 0.02j, 1.44 + 0.01j])
     got, ref = _both([(_dist(*dist), None, 1.0, m)], params, wl, L=10, refine_backscatter=True)
+    _check(got, ref)
+
+
+@pytest.mark.parametrize("radius,m", [(2.1, 1.33 + 1e-8j), (0.05, 1.6 + 0.3j), (6.0, 1.5 + 0.1j)])
+def test_a_single_radius_along_its_radius_and_m(gpu, radius, m):
+    """The single radius's derivative along r (the Mie pass along x at fixed m) beside those
+    along Re m and Im m, from x = 0.3 to x = 75, nearly real to strongly absorbing m."""
+    wl = np.array([0.5, 1.0])
+    got, ref = _both([(_dist(5, radius), None, 1.0, np.array([m, m]))],
+                     [(0, -1, RE, 0), (0, -1, PD, 0), (0, -1, IM, 0)], wl, L=10)
+    _check(got, ref)
+    assert np.all(got["d_err"] == 0.0)
+
+
+def test_a_single_radius_in_a_mixture(gpu):
+    """A monodisperse component's radius, the other component's width and the weights."""
+    comps = [(_dist(5, 0.4), None, 0.3, np.array([1.5 + 0.01j])),
+             (_dist(1, 0.2, 1.5), None, 1.0, np.array([1.45 + 0.001j]))]
+    got, ref = _both(comps, [(0, -1, PD, 0), (1, -1, PD, 1), (0, -1, W, 0)], np.array([0.6]))
     _check(got, ref)
 
 
@@ -116,9 +136,12 @@ def test_the_reference_call(gpu):
     with pytest.raises(InvalidInputError, match="adaptive GPU path"):
         _scatrs.ensemble_compute(layered, wl, False, None, False, None, True, [2], 1e-6, 4096,
                                  False, False)
-    with pytest.raises(InvalidInputError, match="single radius"):
-        _scatrs.ensemble_compute([(("monodisperse", 0.3), ("sphere", m), 1.0)], wl, False, None,
-                                 False, None, True, [0], 1e-6, 4096, False, False)
+    mono = _scatrs.ensemble_compute([(("monodisperse", 0.3), ("sphere", m), 1.0)], wl, False,
+                                    None, False, None, True, [0], 1e-6, 4096, False, False)
+    ref = _native.ensemble_mixture_d([(_dist(5, 0.3), None, 1.0, m)], wl,
+                                     np.array([(0, -1, PD, 0)], dtype=_native.PARAM_DTYPE), None,
+                                     -1)
+    assert np.array_equal(mono["d"], ref["d"]) and not mono["d_errors"].any()
 
 
 def test_invalid_parameters_are_rejected(gpu):

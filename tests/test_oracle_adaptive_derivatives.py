@@ -5,7 +5,7 @@ every kind of parameter's Jacobian against central differences of the values at 
 1e-5 of max(|fd|, F11/|p|)); the error estimates of the derivatives bound their true errors
 against a tighter run (469-647, a factor 2 for the unrefined outputs); derivatives that cannot
 be resolved within the panel budget are flagged (666-680). A single radius's radius
-derivative is not on this path (the GPU's Mie kernels carry no x-derivative) and is rejected."""
+derivative (engine.rs:1158-1170) is checked the same way (ensemble.rs's "radius" case)."""
 
 import numpy as np
 import pytest
@@ -24,10 +24,10 @@ def _tight(comps, derivs=()):
                                 max_panels=50_000)
 
 
-def _check(make, param, value, what):
-    """check_derivative (ensemble.rs:263-320)."""
+def _check(make, param, value, what, step=1e-4):
+    """check_derivative (ensemble.rs:263-320); `step` relative to the value."""
     r = _tight(make(value), [param])
-    h = 1e-4 * max(abs(value), 1e-3)
+    h = step * max(abs(value), 1e-3)
     plus, minus = _tight(make(value + h)), _tight(make(value - h))
     d, v = r["d"][0, :, 0], r["values"][:, 0]
     fd = (plus["values"][:, 0] - minus["values"][:, 0]) / (2 * h)
@@ -115,7 +115,7 @@ def test_unresolvable_derivatives_are_flagged():
         "converged"][0]
 
 
-def test_a_single_radius_has_its_m_derivatives_but_not_its_radius():
+def test_a_single_radius_has_its_m_derivatives_and_its_radius():
     r = O.ensemble_mixture_d(_one(O.dist(O.MONODISPERSE, 0.3)), [LAMBDA],
                              O.params((0, -1, RE, 0)), mu=MU, greek_order=6)
     h = 1e-6
@@ -126,6 +126,11 @@ def test_a_single_radius_has_its_m_derivatives_but_not_its_radius():
     fd = (p["values"] - q["values"]) / (2 * h)
     assert np.allclose(r["d"][0], fd, rtol=1e-6, atol=1e-9 * np.abs(r["values"]).max())
     assert np.all(r["d_err"] == 0.0)
-    with pytest.raises(O.OracleError, match="single radius"):
-        O.ensemble_mixture_d(_one(O.dist(O.MONODISPERSE, 0.3)), [LAMBDA],
-                             O.params((0, -1, PD, 0)))
+    _check(lambda v: _one(O.dist(O.MONODISPERSE, v)), (0, -1, PD, 0), 0.3, "radius")
+    # x = 24 with a nearly real m: ripple resonances make the 1e-4 step's truncation error
+    # about 5e-4 relative, so the step is 5e-6 relative here.
+    _check(lambda v: _one(O.dist(O.MONODISPERSE, v), 1.33 + 1e-8j), (0, -1, PD, 0), 2.1,
+           "radius, nearly real m", step=5e-6)
+    r = O.ensemble_mixture_d(_one(O.dist(O.MONODISPERSE, 0.3)), [LAMBDA],
+                             O.params((0, -1, PD, 0)), mu=MU, greek_order=6)
+    assert np.all(r["d_err"] == 0.0) and r["converged"][0]
