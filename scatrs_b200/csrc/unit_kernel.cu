@@ -21,6 +21,11 @@ constexpr double kPi = 3.14159265358979323846264338327950288;
 constexpr int KB = 8;     // orders per GEMM stage
 constexpr int TR = 32;    // table rows per tile
 constexpr int NT = 128;   // threads: 8 row groups of 4 rows x 16 node groups of 2 nodes
+// The stage rows' strides in shared memory: 4 doubles past 32 and 128, so that the FP64 MMA's
+// operand loads (lane = 4 g + q reads order k4 + q, row or column g) of a half-warp fall in 16
+// distinct 8-byte banks.
+constexpr int TRP = TR + 4;
+constexpr int XP = 128 + 4;
 
 __device__ __forceinline__ void elements4(double s1r, double s1i, double s2r, double s2i,
                                           double e[4]) {
@@ -57,12 +62,13 @@ __device__ __forceinline__ int band_of(int n) {
 }
 
 struct Smem {
-  double a[2][2][KB][TR];  // [stage][G_E, G_O][order][row]
-  double xs[2][KB][128];   // [stage][order][4 columns x 32 nodes]
+  double a[2][2][KB][TRP];  // [stage][G_E, G_O][order][row] (rows 32 .. 35 unused)
+  double xs[2][KB][XP];    // [stage][order][4 columns x 32 nodes] (128 .. 131 unused)
   double w[32], cu[32], area[32], sc[32];
   double wth[3][32];  // the distribution parameters' weights (derivatives only)
   double wd[32], wthd[3][32];  // adaptive derivatives: the error weights (w_K - w_G) ...
   int nn[32];  // each node's number of terms plus one (an upper bound of K-a's), 0 for padding
+  double red[4 * 256];  // the MMA tile's per-warp partial sums (the stages stay in flight)
   double S[8];
   int slot;
 };
@@ -135,13 +141,26 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
                : "d"(a), "d"(b));
 }
 
+// A row tile's table source: G_E, G_O (order-major, ldr doubles per order) from row r0.
+struct TileSrc {
+  const double* ge;
+  const double* go;
+  int ldr, r0;
+};
+
 // The tile C_E = G_E X, C_O = G_O X (32 rows x 128 columns) on the FP64 tensor path: warp w
 // computes columns 32w .. 32w + 31 of all 32 rows as 4 x 4 MMA tiles of 8 x 8 each for E and O;
 // cE[mt][nt] is D of rows 8 mt .., columns 32 w + 8 nt ...
-__device__ __forceinline__ void gemm_tile_mma(Smem& sm, const double* __restrict__ ge,
-                                              const double* __restrict__ go, int ldr, int r0,
-                                              int nc, const double* __restrict__ xc,
-                                              double cE[4][4][2], double cO[4][4][2]) {
+// The tile's first stage is already in flight in buffer st0; with nx, the next tile's first stage
+// (same chunk, same coefficient rows) is issued during this tile's last stage, so that the
+// pipeline does not drain between tiles, and st0 returns the buffer it went to.
+__device__ __forceinline__ void gemm_tile_mma(Smem& sm, const TileSrc& src, int nc,
+                                              const double* __restrict__ xc,
+                                              double cE[4][4][2], double cO[4][4][2], int& st0,
+                                              const TileSrc* nx) {
+  const double* __restrict__ ge = src.ge;
+  const double* __restrict__ go = src.go;
+  const int ldr = src.ldr, r0 = src.r0;
   const int t = threadIdx.x, w = t >> 5, lane = t & 31, q = lane & 3, g = lane >> 2;
 #pragma unroll
   for (int mt = 0; mt < 4; ++mt)
@@ -155,12 +174,14 @@ __device__ __forceinline__ void gemm_tile_mma(Smem& sm, const double* __restrict
   int wmax = 0;
 #pragma unroll
   for (int i = 0; i < 8; ++i) wmax = max(wmax, sm.nn[8 * w + i]);
-  load_stage_z(sm, 0, ge, go, ldr, r0, 0, nc, xc);
-  int st = 0;
+  int st = st0;
   for (int k0 = 0; k0 < nc; k0 += KB, st ^= 1) {
     cp_wait_all();
     __syncthreads();
-    if (k0 + KB < nc) load_stage_z(sm, st ^ 1, ge, go, ldr, r0, k0 + KB, nc, xc);
+    if (k0 + KB < nc)
+      load_stage_z(sm, st ^ 1, ge, go, ldr, r0, k0 + KB, nc, xc);
+    else if (nx)
+      load_stage_z(sm, st ^ 1, nx->ge, nx->go, nx->ldr, nx->r0, 0, nc, xc);
     const int kend = nc - k0 < KB ? nc - k0 : KB;
 #pragma unroll
     for (int k4 = 0; k4 < KB; k4 += 4) {
@@ -184,7 +205,10 @@ __device__ __forceinline__ void gemm_tile_mma(Smem& sm, const double* __restrict
       }
     }
   }
-  __syncthreads();  // the stage buffers are free for the reduction and the next tile
+  // The next tile's first stage went to buffer st; the next tile's second stage reuses this
+  // tile's last buffer only after the next tile's first barrier, which every warp reaches after
+  // its MMAs here.
+  st0 = st;
 }
 
 // The elements of an MMA tile, scaled, weighted and summed over the chunk's 32 spheres. Lane
@@ -231,7 +255,7 @@ __device__ __forceinline__ void chunk_elements_mma(Smem& sm, const double cE[4][
   for (int mt = 0; mt < 4; ++mt)
 #pragma unroll
     for (int k = 0; k < 4; ++k) p[mt][k] += __shfl_xor_sync(0xffffffffu, p[mt][k], 2);
-  double* red = &sm.xs[0][0][0];  // 4 warps x 256 partial sums
+  double* red = sm.red;  // 4 warps x 256 partial sums
   if (q < 2) {
 #pragma unroll
     for (int mt = 0; mt < 4; ++mt)
@@ -522,6 +546,18 @@ __device__ __forceinline__ void unit_body(const UnitArgs& a) {
         const int o_row = kMode == 0 ? (t >> 2) : rg * 4 + rr;
         const int o_side = kMode == 0 ? ((t >> 1) & 1) : side;
         const int o_e0 = kMode == 0 ? 2 * (t & 1) : e0;
+        // A tile's table rows: the user cosines', then the band's.
+        auto source = [&](int tl) {
+          const bool u = tl < t_user;
+          const BandDesc Bd = u ? BandDesc{} : a.bands[b];
+          return TileSrc{u ? a.ge_u : a.band_ge + Bd.g_off, u ? a.go_u : a.band_go + Bd.g_off,
+                         u ? a.h_u_pad : Bd.h_pad, (u ? tl : tl - t_user) * TR};
+        };
+        int st0 = 0;  // the stage buffer of the next MMA tile's first stage (kMode 0)
+        if constexpr (kMode == 0) {
+          const TileSrc s0 = source(it.group);
+          load_stage_z(sm, 0, s0.ge, s0.go, s0.ldr, s0.r0, 0, nc, xc);
+        }
         for (int tile = it.group; tile < t_user + t_band; tile += it.n_groups) {
           const bool user = tile < t_user;
           const BandDesc B = user ? BandDesc{} : a.bands[b];
@@ -545,7 +581,10 @@ __device__ __forceinline__ void unit_body(const UnitArgs& a) {
           double* base = user ? acc_user : a.acc + a.chunk_acc[ci];
           if constexpr (kMode == 0) {
             double cE[4][4][2], cO[4][4][2];
-            gemm_tile_mma(sm, ge, go, ldr, r0, nc, xc, cE, cO);
+            const int tn = tile + it.n_groups;
+            const TileSrc nx = source(tn < t_user + t_band ? tn : tile);
+            gemm_tile_mma(sm, TileSrc{ge, go, ldr, r0}, nc, xc, cE, cO, st0,
+                          tn < t_user + t_band ? &nx : nullptr);
             if (user)
               chunk_elements_mma<true>(sm, cE, cO, v);
             else
