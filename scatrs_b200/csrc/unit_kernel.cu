@@ -68,7 +68,6 @@ struct Smem {
   double wth[3][32];  // the distribution parameters' weights (derivatives only)
   double wd[32], wthd[3][32];  // adaptive derivatives: the error weights (w_K - w_G) ...
   int nn[32];  // each node's number of terms plus one (an upper bound of K-a's), 0 for padding
-  double red[4 * 256];  // the MMA tile's per-warp partial sums (the stages stay in flight)
   double S[8];
   int slot;
 };
@@ -149,31 +148,29 @@ struct TileSrc {
 };
 
 // The tile C_E = G_E X, C_O = G_O X (32 rows x 128 columns) on the FP64 tensor path: warp w
-// computes columns 32w .. 32w + 31 of all 32 rows as 4 x 4 MMA tiles of 8 x 8 each for E and O;
-// cE[mt][nt] is D of rows 8 mt .., columns 32 w + 8 nt ...
+// computes rows 8w .. 8w + 7 of all 128 columns as 16 MMA tiles of 8 columns (2 nodes) each for E
+// and O; cE[nt] is D of columns 8 nt ... Every warp does the same work, the MMAs of a group of 4
+// tiles (8 nodes) stopping above the group's largest number of terms (K-a writes zero rows up to
+// the chunk's), so that no warp, and no SM sub-partition, carries the chunk's largest spheres
+// alone.
 // The tile's first stage is already in flight in buffer st0; with nx, the next tile's first stage
 // (same chunk, same coefficient rows) is issued during this tile's last stage, so that the
 // pipeline does not drain between tiles, and st0 returns the buffer it went to.
 __device__ __forceinline__ void gemm_tile_mma(Smem& sm, const TileSrc& src, int nc,
-                                              const double* __restrict__ xc,
-                                              double cE[4][4][2], double cO[4][4][2], int& st0,
-                                              const TileSrc* nx) {
+                                              const double* __restrict__ xc, double cE[16][2],
+                                              double cO[16][2], int& st0, const TileSrc* nx) {
   const double* __restrict__ ge = src.ge;
   const double* __restrict__ go = src.go;
   const int ldr = src.ldr, r0 = src.r0;
   const int t = threadIdx.x, w = t >> 5, lane = t & 31, q = lane & 3, g = lane >> 2;
 #pragma unroll
-  for (int mt = 0; mt < 4; ++mt)
+  for (int nt = 0; nt < 16; ++nt) {
+    cE[nt][0] = cE[nt][1] = 0.0;
+    cO[nt][0] = cO[nt][1] = 0.0;
+  }
+  int gmax[4] = {0, 0, 0, 0};
 #pragma unroll
-    for (int nt = 0; nt < 4; ++nt) {
-      cE[mt][nt][0] = cE[mt][nt][1] = 0.0;
-      cO[mt][nt][0] = cO[mt][nt][1] = 0.0;
-    }
-  // This warp's nodes (8 w .. 8 w + 7) have no coefficients above their largest number of
-  // terms (K-a writes zero rows up to the chunk's): its MMAs stop there.
-  int wmax = 0;
-#pragma unroll
-  for (int i = 0; i < 8; ++i) wmax = max(wmax, sm.nn[8 * w + i]);
+  for (int i = 0; i < 32; ++i) gmax[i >> 3] = max(gmax[i >> 3], sm.nn[i]);
   int st = st0;
   for (int k0 = 0; k0 < nc; k0 += KB, st ^= 1) {
     cp_wait_all();
@@ -185,23 +182,23 @@ __device__ __forceinline__ void gemm_tile_mma(Smem& sm, const TileSrc& src, int 
     const int kend = nc - k0 < KB ? nc - k0 : KB;
 #pragma unroll
     for (int k4 = 0; k4 < KB; k4 += 4) {
-      if (k4 < kend && k0 + k4 < wmax) {
+      if (k4 < kend) {
         const int kk = k4 + q;
-        double aE[4], aO[4], b[4];
+        const double aE = sm.a[st][0][kk][8 * w + g];
+        const double aO = sm.a[st][1][kk][8 * w + g];
 #pragma unroll
-        for (int mt = 0; mt < 4; ++mt) {
-          aE[mt] = sm.a[st][0][kk][8 * mt + g];
-          aO[mt] = sm.a[st][1][kk][8 * mt + g];
-        }
+        for (int gr = 0; gr < 4; ++gr) {
+          if (k0 + k4 < gmax[gr]) {
+            double b[4];
 #pragma unroll
-        for (int nt = 0; nt < 4; ++nt) b[nt] = sm.xs[st][kk][32 * w + 8 * nt + g];
+            for (int j = 0; j < 4; ++j) b[j] = sm.xs[st][kk][32 * gr + 8 * j + g];
 #pragma unroll
-        for (int mt = 0; mt < 4; ++mt)
-#pragma unroll
-          for (int nt = 0; nt < 4; ++nt) {
-            dmma(cE[mt][nt][0], cE[mt][nt][1], aE[mt], b[nt]);
-            dmma(cO[mt][nt][0], cO[mt][nt][1], aO[mt], b[nt]);
+            for (int j = 0; j < 4; ++j) {
+              dmma(cE[4 * gr + j][0], cE[4 * gr + j][1], aE, b[j]);
+              dmma(cO[4 * gr + j][0], cO[4 * gr + j][1], aO, b[j]);
+            }
           }
+        }
       }
     }
   }
@@ -213,64 +210,42 @@ __device__ __forceinline__ void gemm_tile_mma(Smem& sm, const TileSrc& src, int 
 
 // The elements of an MMA tile, scaled, weighted and summed over the chunk's 32 spheres. Lane
 // pairs (q, q ^ 1) hold a node's (u) and (v) columns; after exchanging them the even lane forms
-// the elements at +mu and the odd lane those at -mu, of its 4 rows (8 mt + g) and of its 4 nodes
-// (8 w + 2 nt + q / 2); the 4 nodes add in the thread, node pairs across lanes q, q ^ 2, and the
-// 4 warps in a fixed order through shared memory. Thread t ends with v[0], v[1] of row t / 4,
-// side (t / 2) & 1 and elements 2 (t & 1), 2 (t & 1) + 1.
+// the elements at +mu and the odd lane those at -mu of its row (8 w + g) for its node of each
+// tile (2 nt + q / 2); the 16 nodes add in the thread, then node pairs across lanes q, q ^ 2.
+// Thread t ends with v[0], v[1]: row t / 4, side t & 1, elements 2 ((t / 2) & 1) + {0, 1}.
 template <bool kUser>
-__device__ __forceinline__ void chunk_elements_mma(Smem& sm, const double cE[4][4][2],
-                                                   const double cO[4][4][2], double v[2]) {
-  const int t = threadIdx.x, w = t >> 5, lane = t & 31, q = lane & 3, g = lane >> 2;
+__device__ __forceinline__ void chunk_elements_mma(Smem& sm, const double cE[16][2],
+                                                   const double cO[16][2], double v[2]) {
+  const int lane = threadIdx.x & 31, q = lane & 3;
   const int side = q & 1;
   const double sg = side ? -1.0 : 1.0;
-  double p[4][4];
+  double p[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-  for (int mt = 0; mt < 4; ++mt)
-#pragma unroll
-    for (int k = 0; k < 4; ++k) p[mt][k] = 0.0;
-#pragma unroll
-  for (int nt = 0; nt < 4; ++nt) {
-    const int node = 8 * w + 2 * nt + (q >> 1);
+  for (int nt = 0; nt < 16; ++nt) {
+    const int node = 2 * nt + (q >> 1);
     const double wt = sm.w[node], cu = sm.cu[node], ar = sm.area[node], sc = sm.sc[node];
+    const double e0 = cE[nt][0], e1 = cE[nt][1];
+    const double o0 = cO[nt][0], o1 = cO[nt][1];
+    const double pe0 = __shfl_xor_sync(0xffffffffu, e0, 1);
+    const double pe1 = __shfl_xor_sync(0xffffffffu, e1, 1);
+    const double po0 = __shfl_xor_sync(0xffffffffu, o0, 1);
+    const double po1 = __shfl_xor_sync(0xffffffffu, o1, 1);
+    // The even lane of a pair holds u (re, im), the odd one v.
+    const double eur = side ? pe0 : e0, eui = side ? pe1 : e1;
+    const double evr = side ? e0 : pe0, evi = side ? e1 : pe1;
+    const double our = side ? po0 : o0, oui = side ? po1 : o1;
+    const double ovr = side ? o0 : po0, ovi = side ? o1 : po1;
+    double e[4];
+    elements4(eur + sg * ovr, eui + sg * ovi, evr + sg * our, evi + sg * oui, e);
 #pragma unroll
-    for (int mt = 0; mt < 4; ++mt) {
-      const double e0 = cE[mt][nt][0], e1 = cE[mt][nt][1];
-      const double o0 = cO[mt][nt][0], o1 = cO[mt][nt][1];
-      const double pe0 = __shfl_xor_sync(0xffffffffu, e0, 1);
-      const double pe1 = __shfl_xor_sync(0xffffffffu, e1, 1);
-      const double po0 = __shfl_xor_sync(0xffffffffu, o0, 1);
-      const double po1 = __shfl_xor_sync(0xffffffffu, o1, 1);
-      // The even lane of a pair holds u (re, im), the odd one v.
-      const double eur = side ? pe0 : e0, eui = side ? pe1 : e1;
-      const double evr = side ? e0 : pe0, evi = side ? e1 : pe1;
-      const double our = side ? po0 : o0, oui = side ? po1 : o1;
-      const double ovr = side ? o0 : po0, ovi = side ? o1 : po1;
-      double e[4];
-      elements4(eur + sg * ovr, eui + sg * ovi, evr + sg * our, evi + sg * oui, e);
-#pragma unroll
-      for (int k = 0; k < 4; ++k) p[mt][k] += kUser ? wt * ((cu * e[k]) * ar) : wt * (sc * e[k]);
-    }
+    for (int k = 0; k < 4; ++k) p[k] += kUser ? wt * ((cu * e[k]) * ar) : wt * (sc * e[k]);
   }
 #pragma unroll
-  for (int mt = 0; mt < 4; ++mt)
-#pragma unroll
-    for (int k = 0; k < 4; ++k) p[mt][k] += __shfl_xor_sync(0xffffffffu, p[mt][k], 2);
-  double* red = sm.red;  // 4 warps x 256 partial sums
-  if (q < 2) {
-#pragma unroll
-    for (int mt = 0; mt < 4; ++mt)
-#pragma unroll
-      for (int k = 0; k < 4; ++k) red[w * 256 + ((8 * mt + g) * 2 + side) * 4 + k] = p[mt][k];
-  }
-  __syncthreads();
-#pragma unroll
-  for (int j = 0; j < 2; ++j) {
-    const int o = 2 * t + j;
-    v[j] = ((red[o] + red[256 + o]) + red[512 + o]) + red[768 + o];
-  }
-  __syncthreads();
+  for (int k = 0; k < 4; ++k) p[k] += __shfl_xor_sync(0xffffffffu, p[k], 2);
+  const int e2 = 2 * (q >> 1);
+  v[0] = e2 ? p[2] : p[0];
+  v[1] = e2 ? p[3] : p[1];
 }
-
 // accE/accO[r][c] = sum_k G[r0 + 4 rg + r][k] X[k][4 ng + c (+ 64 for c >= 4)] for k < nc.
 __device__ __forceinline__ void gemm_tile(Smem& sm, const double* __restrict__ ge,
                                           const double* __restrict__ go, int ldr, int r0, int nc,
@@ -544,8 +519,8 @@ __device__ __forceinline__ void unit_body(const UnitArgs& a) {
         double v[2];
         // This thread's output of a reduced tile (kMode 0, the MMA tile, owns row t / 4).
         const int o_row = kMode == 0 ? (t >> 2) : rg * 4 + rr;
-        const int o_side = kMode == 0 ? ((t >> 1) & 1) : side;
-        const int o_e0 = kMode == 0 ? 2 * (t & 1) : e0;
+        const int o_side = kMode == 0 ? (t & 1) : side;
+        const int o_e0 = kMode == 0 ? 2 * ((t >> 1) & 1) : e0;
         // A tile's table rows: the user cosines', then the band's.
         auto source = [&](int tl) {
           const bool u = tl < t_user;
@@ -580,7 +555,7 @@ __device__ __forceinline__ void unit_body(const UnitArgs& a) {
           const int64_t len = user ? a.n_mu : B.n_q;
           double* base = user ? acc_user : a.acc + a.chunk_acc[ci];
           if constexpr (kMode == 0) {
-            double cE[4][4][2], cO[4][4][2];
+            double cE[16][2], cO[16][2];
             const int tn = tile + it.n_groups;
             const TileSrc nx = source(tn < t_user + t_band ? tn : tile);
             gemm_tile_mma(sm, TileSrc{ge, go, ldr, r0}, nc, xc, cE, cO, st0,
