@@ -31,7 +31,7 @@ sys.path.insert(0, ROOT)
 
 # DRAM bytes per node of the unit kernel: (805.47 MB read + 27.56 MB written) / 313,344 nodes in
 # one ncu capture of the 0.1-scale batched workload (the traffic grows with the nodes).
-UNIT_DRAM_BYTES_PER_NODE = (805.469952e6 + 27.562752e6) / 313344
+UNIT_DRAM_BYTES_PER_NODE = (720.229632e6 + 27.529984e6) / 313344
 
 METRIC = "Mie ensemble nodes/s on 1 B200, batched vs plain FP64, at 1e-10 rel err vs FP64"
 UNIT = "nodes/s"
