@@ -133,8 +133,9 @@ typedef struct scatrs_adaptive_options {
 } scatrs_adaptive_options;
 
 /* greek_order = SCATRS_GREEK_ALL (GreekOrder::All, ensemble/mod.rs:163-170): every order up to
- * 2 N_max at each wavelength (N_max the largest number of terms there), spheres, layered
- * spheres and spheroids (not mixtures of different particles). The call then leaves its greek arrays unwritten; the coefficients of the calling
+ * 2 N_max at each wavelength (N_max the largest number of terms there, over every part of the
+ * call: spheres, layered spheres and spheroids, alone or mixed). The call then leaves its greek
+ * arrays unwritten; the coefficients of the calling
  * thread's last such call come from scatrs_greek_all_take, (6, n, W) and with derivatives
  * (P, 6, n, W) as the call's other outputs, W = scatrs_greek_all_width() the longest plus one,
  * zero above each wavelength's order (scatrs-py/src/ensemble.rs:419-429). */
@@ -191,7 +192,7 @@ typedef struct scatrs_component {
  * projected Greek coefficients, the spheroids' direct Greek segment (to the largest 2 N of the
  * mixture's spheroids at each wavelength), the depolarization ratio from the spheroids, and the
  * phase matrix from the spheres' tables plus the spheroids' averaged expansion. Such mixtures
- * take no derivatives and no SCATRS_GREEK_ALL.
+ * take no derivatives; with SCATRS_GREEK_ALL each wavelength's order is 2 N_max over every part.
  */
 int scatrs_ensemble_mixture(const scatrs_component* components, int64_t n_comp,
                             const double* wavelengths, int64_t n_wl, const double* mu,

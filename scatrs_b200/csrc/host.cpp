@@ -2486,8 +2486,6 @@ void spheroid_call(const std::vector<SphParticle>& ps, bool batch, const double*
   if (n_dist < 0 || n_wl < 0) throw Failure{SCATRS_INVALID_INPUT, "negative sizes"};
   if (batch && ps.size() > 1) throw Failure{SCATRS_INVALID_INPUT, "a batch has one particle"};
   const bool all_orders = options->greek_order == SCATRS_GREEK_ALL;
-  if (all_orders && rows)
-    throw Failure{SCATRS_INVALID_INPUT, "greek='all' is not on the GPU path for mixtures"};
   const adaptive::Options o{options->rtol, options->max_panels, options->allow_unvalidated != 0,
                             options->refine_backscatter != 0};
   if (!(o.rtol >= 1e-13 && o.rtol <= 0.1)) {
@@ -2622,7 +2620,7 @@ void spheroid_call(const std::vector<SphParticle>& ps, bool batch, const double*
   for (int64_t u = 0; u < n_units; ++u) n_direct[u] = batch || rows ? n_at[u % n_wl] : n_own[u];
   // greek='all': every order to 2 N_max (GreekOrder::All), padded to the longest.
   int64_t width = 0;
-  if (all_orders) {
+  if (all_orders && !rows) {  // a mixture's rows: the mixture sets its own coefficients
     for (int64_t u = 0; u < n_units; ++u) width = std::max(width, 2 * n_direct[u] + 1);
     GreekAll& ga = t_greek_all;
     ga.width = width;
@@ -2899,10 +2897,7 @@ void mixture_hetero(const scatrs_component* components, int64_t n_comp,
                     const double* wavelengths, int64_t n_wl, const double* mu, int64_t n_mu,
                     const scatrs_adaptive_options* options, const AdOutputs& res) {
   if (!options) throw Failure{SCATRS_INVALID_INPUT, "options must not be NULL"};
-  if (options->greek_order == SCATRS_GREEK_ALL)
-    throw Failure{SCATRS_INVALID_INPUT,
-                  "greek='all' for mixtures with layered spheres or spheroids is not on the GPU "
-                  "path"};
+  const bool all_orders = options->greek_order == SCATRS_GREEK_ALL;
   const std::vector<AdPart> parts = mixture_parts(components, n_comp);
   const int64_t np = (int64_t)parts.size();
   for (int64_t c = 0; c < n_comp; ++c) {
@@ -2916,67 +2911,8 @@ void mixture_hetero(const scatrs_component* components, int64_t n_comp,
     if (k.n_layers > 1 && !k.fractions)
       throw Failure{SCATRS_INVALID_INPUT, who + "a layered sphere needs its fractions"};
   }
-  const int L = options->greek_order;
-  const int64_t glen = L >= 0 ? L + 1 : 0;
-  // Each part's averages at each wavelength: 9 scalars (the last the depolarization
-  // numerator), 4 n_mu cosine values, 6 glen Greek coefficients, each with its error, and the
-  // spheroids' direct segment.
-  struct Avg {
-    std::vector<double> v, e, dv, de;  // v, e: 9 + 4 n_mu + 6 glen; dv, de: 6 (ld + 1)
-    bool converged = true;
-    int64_t panels = 0;
-  };
-  const int64_t row = 9 + 4 * n_mu + 6 * glen;
-  std::vector<Avg> avg((size_t)np * n_wl);
-  // Spheres, and layered spheres by their number of layers.
-  std::map<int, std::vector<int64_t>> by_layers;
-  for (int64_t p = 0; p < np; ++p) {
-    const scatrs_component& k = components[parts[p].component];
-    if (k.aspect_ratio == 0.0) by_layers[k.n_layers > 1 ? k.n_layers : 1].push_back(p);
-  }
-  for (const auto& kv : by_layers) {
-    const int nl = kv.first;
-    const std::vector<int64_t>& ps = kv.second;
-    std::vector<AdPart> sub;
-    std::vector<double> fr, ml;
-    for (int64_t p : ps) {
-      AdPart a = parts[p];
-      a.out = 0;
-      sub.push_back(a);
-      if (nl > 1) {
-        const scatrs_component& k = components[parts[p].component];
-        fr.insert(fr.end(), k.fractions, k.fractions + nl - 1);
-        ml.insert(ml.end(), k.m, k.m + 2 * (size_t)nl * n_wl);
-      }
-    }
-    scatrs_layers lay{nl, 0, fr.data(), ml.data()};
-    PartRows rows;
-    adaptive_call_order(sub, 1, false, wavelengths, n_wl, mu, n_mu, options, AdOutputs{},
-                        nl > 1 ? &lay : nullptr, nullptr, nullptr, &rows);
-    const int64_t n2 = 4 * n_mu, base_t = 16, base_g = 16 + 8 * n_mu;
-    for (size_t q = 0; q < ps.size(); ++q)
-      for (int64_t i = 0; i < n_wl; ++i) {
-        const double* r = rows.rows.data() + ((int64_t)q * n_wl + i) * rows.stride;
-        Avg& a = avg[ps[q] * n_wl + i];
-        a.v.assign(row, 0.0);
-        a.e.assign(row, 0.0);
-        for (int k = 0; k < 8; ++k) {
-          a.v[k] = r[k];
-          a.e[k] = r[8 + k];
-        }
-        for (int64_t j = 0; j < n2; ++j) {
-          a.v[9 + j] = r[base_t + j];
-          a.e[9 + j] = r[base_t + n2 + j];
-        }
-        for (int64_t j = 0; j < 6 * glen; ++j) {
-          a.v[9 + n2 + j] = r[base_g + j];
-          a.e[9 + n2 + j] = r[base_g + 6 * glen + j];
-        }
-        a.converged = rows.converged[q * n_wl + i] != 0;
-        a.panels = rows.panels[q * n_wl + i];
-      }
-  }
-  // Spheroids: one particle per component, its modes its distributions.
+  // Spheroids: one particle per component, its modes its distributions. They run first: with
+  // greek='all' their N at each wavelength (ld = 2 N) enters the mixture's order.
   std::vector<SphParticle> sph;
   std::vector<int64_t> sph_parts;  // the parts in the order of the spheroid call's
   for (int64_t c = 0; c < n_comp; ++c) {
@@ -2987,26 +2923,158 @@ void mixture_hetero(const scatrs_component* components, int64_t n_comp,
       if (parts[p].component == c) sph_parts.push_back(p);
   }
   std::vector<int64_t> ld(n_wl, -1);
+  SphRows srows;
   if (!sph.empty()) {
-    SphRows rows;
-    spheroid_call(sph, false, wavelengths, n_wl, mu, n_mu, options, AdOutputs{}, &rows);
-    ld = rows.ld;
-    for (size_t q = 0; q < sph_parts.size(); ++q)
-      for (int64_t i = 0; i < n_wl; ++i) {
-        const std::vector<double>& sv = rows.av[q * n_wl + i];
-        const std::vector<double>& se = rows.ae[q * n_wl + i];
-        Avg& a = avg[sph_parts[q] * n_wl + i];
-        a.v.assign(row, 0.0);
-        a.e.assign(row, 0.0);
-        for (int k = 0; k < 9; ++k) {
-          a.v[k] = sv[k];
-          a.e[k] = se[k];
-        }
-        a.dv.assign(sv.begin() + 9, sv.end());
-        a.de.assign(se.begin() + 9, se.end());
-        a.converged = rows.converged[q * n_wl + i] != 0;
-        a.panels = rows.panels[q * n_wl + i];
+    spheroid_call(sph, false, wavelengths, n_wl, mu, n_mu, options, AdOutputs{}, &srows);
+    ld = srows.ld;
+  }
+  // Spheres, and layered spheres by their number of layers.
+  std::map<int, std::vector<int64_t>> by_layers;
+  for (int64_t p = 0; p < np; ++p) {
+    const scatrs_component& k = components[parts[p].component];
+    if (k.aspect_ratio == 0.0) by_layers[k.n_layers > 1 ? k.n_layers : 1].push_back(p);
+  }
+  // A class's parts (output unit 0) with their layers' fractions and indices.
+  struct Cls {
+    std::vector<AdPart> sub;
+    std::vector<double> fr, ml;
+    int nl;
+  };
+  auto make_cls = [&](int nl, const std::vector<int64_t>& ps) {
+    Cls k{{}, {}, {}, nl};
+    for (int64_t p : ps) {
+      AdPart a = parts[p];
+      a.out = 0;
+      k.sub.push_back(a);
+      if (nl > 1) {
+        const scatrs_component& c = components[parts[p].component];
+        k.fr.insert(k.fr.end(), c.fractions, c.fractions + nl - 1);
+        k.ml.insert(k.ml.end(), c.m, c.m + 2 * (size_t)nl * n_wl);
       }
+    }
+    return k;
+  };
+  // The Greek order at each wavelength: the requested one, or with greek='all' 2 N_max over
+  // every part of the mixture (GreekOrder::All, engine.rs:2016-2036: spheres, layered spheres
+  // and spheroids alike), the sphere classes' N_max from their pass 1.
+  std::vector<int64_t> order(n_wl, options->greek_order);
+  if (all_orders) {
+    std::fill(order.begin(), order.end(), 0);
+    for (int64_t i = 0; i < n_wl; ++i)
+      if (ld[i] >= 0) order[i] = ld[i];
+    scatrs_adaptive_options o1 = *options;
+    o1.greek_order = -1;
+    for (const auto& kv : by_layers) {
+      Cls k = make_cls(kv.first, kv.second);
+      scatrs_layers lay{k.nl, 0, k.fr.data(), k.ml.data()};
+      std::vector<int64_t> n_max;
+      adaptive_call_order(k.sub, 1, false, wavelengths, n_wl, mu, n_mu, &o1, AdOutputs{},
+                          k.nl > 1 ? &lay : nullptr, nullptr, &n_max);
+      for (size_t q = 0; q < k.sub.size() && !n_max.empty(); ++q)
+        for (int64_t i = 0; i < n_wl; ++i)
+          order[i] = std::max(order[i], 2 * n_max[q * n_wl + i]);
+    }
+  }
+  // The Greek coefficients' width in the rows: the order plus one (the longest with 'all').
+  int64_t gw = 0;
+  for (int64_t i = 0; i < n_wl; ++i) gw = std::max(gw, order[i] + 1);
+  // Each part's averages at each wavelength: 9 scalars (the last the depolarization
+  // numerator), 4 n_mu cosine values, 6 gw Greek coefficients (zero above the wavelength's
+  // order), each with its error, and the spheroids' direct segment.
+  struct Avg {
+    std::vector<double> v, e, dv, de;  // v, e: 9 + 4 n_mu + 6 gw; dv, de: 6 (ld + 1)
+    bool converged = true;
+    int64_t panels = 0;
+  };
+  const int64_t row = 9 + 4 * n_mu + 6 * gw;
+  std::vector<Avg> avg((size_t)np * n_wl);
+  for (const auto& kv : by_layers) {
+    const std::vector<int64_t>& ps = kv.second;
+    const Cls k = make_cls(kv.first, ps);
+    // The wavelengths of one order run together (all of them without 'all').
+    std::map<int64_t, std::vector<int64_t>> by_order;
+    for (int64_t i = 0; i < n_wl; ++i) by_order[order[i]].push_back(i);
+    for (const auto& ko : by_order) {
+      const int64_t L = ko.first, glen = L >= 0 ? L + 1 : 0;
+      const std::vector<int64_t>& ws = ko.second;
+      const int64_t nw = (int64_t)ws.size();
+      std::vector<double> wl_s(nw);
+      for (int64_t j = 0; j < nw; ++j) wl_s[j] = wavelengths[ws[j]];
+      std::vector<AdPart> sub = k.sub;
+      std::vector<std::vector<double>> m_s(sub.size());
+      std::vector<double> ml_s(k.ml.size() / std::max<int64_t>(n_wl, 1) * nw);
+      for (size_t q = 0; q < sub.size(); ++q) {
+        if (sub[q].m) {
+          m_s[q].resize(2 * nw);
+          for (int64_t j = 0; j < nw; ++j) {
+            m_s[q][2 * j] = sub[q].m[2 * ws[j]];
+            m_s[q][2 * j + 1] = sub[q].m[2 * ws[j] + 1];
+          }
+          sub[q].m = m_s[q].data();
+        }
+        for (int l = 0; k.nl > 1 && l < k.nl; ++l)
+          for (int64_t j = 0; j < nw; ++j)
+            for (int c = 0; c < 2; ++c)
+              ml_s[2 * ((q * k.nl + l) * nw + j) + c] =
+                  k.ml[2 * ((q * k.nl + l) * n_wl + ws[j]) + c];
+      }
+      scatrs_layers lay{k.nl, 0, k.fr.data(), ml_s.data()};
+      scatrs_adaptive_options oL = *options;
+      oL.greek_order = (int)L;
+      PartRows rows;
+      adaptive_call_order(sub, 1, false, wl_s.data(), nw, mu, n_mu, &oL, AdOutputs{},
+                          k.nl > 1 ? &lay : nullptr, nullptr, nullptr, &rows);
+      const int64_t n2 = 4 * n_mu, base_t = 16, base_g = 16 + 8 * n_mu;
+      for (size_t q = 0; q < ps.size(); ++q)
+        for (int64_t j = 0; j < nw; ++j) {
+          const int64_t i = ws[j];
+          const double* r = rows.rows.data() + ((int64_t)q * nw + j) * rows.stride;
+          Avg& a = avg[ps[q] * n_wl + i];
+          a.v.assign(row, 0.0);
+          a.e.assign(row, 0.0);
+          for (int c = 0; c < 8; ++c) {
+            a.v[c] = r[c];
+            a.e[c] = r[8 + c];
+          }
+          for (int64_t t = 0; t < n2; ++t) {
+            a.v[9 + t] = r[base_t + t];
+            a.e[9 + t] = r[base_t + n2 + t];
+          }
+          for (int f = 0; f < 6; ++f)
+            for (int64_t l = 0; l < glen; ++l) {
+              a.v[9 + n2 + f * gw + l] = r[base_g + f * glen + l];
+              a.e[9 + n2 + f * gw + l] = r[base_g + 6 * glen + f * glen + l];
+            }
+          a.converged = rows.converged[q * nw + j] != 0;
+          a.panels = rows.panels[q * nw + j];
+        }
+    }
+  }
+  for (size_t q = 0; q < sph_parts.size(); ++q)
+    for (int64_t i = 0; i < n_wl; ++i) {
+      const std::vector<double>& sv = srows.av[q * n_wl + i];
+      const std::vector<double>& se = srows.ae[q * n_wl + i];
+      Avg& a = avg[sph_parts[q] * n_wl + i];
+      a.v.assign(row, 0.0);
+      a.e.assign(row, 0.0);
+      for (int k = 0; k < 9; ++k) {
+        a.v[k] = sv[k];
+        a.e[k] = se[k];
+      }
+      a.dv.assign(sv.begin() + 9, sv.end());
+      a.de.assign(se.begin() + 9, se.end());
+      a.converged = srows.converged[q * n_wl + i] != 0;
+      a.panels = srows.panels[q * n_wl + i];
+    }
+  if (all_orders) {
+    GreekAll& ga = t_greek_all;
+    ga.width = gw;
+    ga.n = n_wl;
+    ga.p = 0;
+    ga.g.assign(6 * n_wl * gw, 0.0);
+    ga.ge.assign(ga.g.size(), 0.0);
+    ga.dg.clear();
+    ga.dge.clear();
   }
   // Mixing and assembly per wavelength.
   const bool norm = options->normalized != 0;
@@ -3062,11 +3130,13 @@ void mixture_hetero(const scatrs_component* components, int64_t n_comp,
     auto D = [&](int f, int64_t l) {
       return LinE{dv[f * (ldi + 1) + l], de[f * (ldi + 1) + l]};
     };
-    const int64_t g0 = 9 + 4 * n_mu;
-    if (glen > 0 && res.greek) {
+    const int64_t g0 = 9 + 4 * n_mu, glen = order[i] + 1;
+    double* g_out = all_orders ? t_greek_all.g.data() : res.greek;
+    double* ge_out = all_orders ? t_greek_all.ge.data() : res.greek_err;
+    if (glen > 0 && g_out) {
       // The spheres' coefficients plus the spheroids' (engine.rs:2196-2216).
       auto G = [&](int f, int64_t l) {
-        LinE x = lin(g0 + f * glen + l);
+        LinE x = lin(g0 + f * gw + l);
         if (has_direct && l <= ldi) {
           const LinE y = D(f, l);
           x.v += y.v;
@@ -3079,8 +3149,8 @@ void mixture_hetero(const scatrs_component* components, int64_t n_comp,
         for (int64_t l = 0; l < glen; ++l) {
           LinE x = G(f, l);
           if (norm) x = (f == 0 && l == 0) ? LinE{1.0, 0.0} : lin_div(x, a0);
-          res.greek[(f * n_wl + i) * glen + l] = x.v;
-          if (res.greek_err) res.greek_err[(f * n_wl + i) * glen + l] = x.e;
+          g_out[(f * n_wl + i) * gw + l] = x.v;
+          if (ge_out) ge_out[(f * n_wl + i) * gw + l] = x.e;
         }
     }
     if (n_mu > 0 && res.phase) {

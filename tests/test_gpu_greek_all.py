@@ -1,8 +1,8 @@
 """greek='all' (GreekOrder::All) on the GPU: every order up to 2 N_max at each wavelength, the
 arrays padded with zeros to the longest, against the oracle (same widths, same zeros, values and
 error estimates as the adaptive path's tolerances), alone, batched, in a mixture with
-derivatives, and through the reference-facing call (spheroids too); mixtures of different
-particles refuse it."""
+derivatives, and through the reference-facing call (spheroids, and mixtures of different
+particles, too)."""
 
 import numpy as np
 import pytest
@@ -56,6 +56,9 @@ def test_the_reference_call(gpu):
                                    False, False)
     assert sph["greek"].shape[-1] > 1 and np.all(sph["greek"][0, :, 0] == 1.0)
     mixed = spheroid + [(("lognormal", 0.2, 1.5), ("sphere", m), 1.0)]
-    with pytest.raises(InvalidInputError, match="mixtures"):
-        _scatrs.ensemble_compute(mixed, wl, True, None, True, None, True, [], 1e-4, 4096, False,
-                                 False)
+    mix = _scatrs.ensemble_compute(mixed, wl, True, None, True, None, True, [], 1e-4, 4096,
+                                   False, False)
+    ref = _native.ensemble_mixture([(_dists((1, 0.05, 1.3)), None, 1.0, ("spheroid", 1.5, m)),
+                                    (_dists((1, 0.2, 1.5)), None, 1.0, m)], wl, None,
+                                   _native.GREEK_ALL, rtol=1e-4)
+    assert np.array_equal(mix["greek"], ref["greek"]) and np.all(mix["greek"][0, :, 0] == 1.0)

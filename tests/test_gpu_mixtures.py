@@ -66,6 +66,42 @@ def test_spheres_and_spheroids(gpu, normalized):
     assert np.all(got["values"][7] > 0.0)
 
 
+def _orders(greek):
+    """The order of each wavelength's coefficients: the last nonzero alpha1."""
+    return np.array([np.flatnonzero(g)[-1] for g in greek[0]])
+
+
+def test_all_orders_with_layered_spheres(gpu):
+    """greek='all': each wavelength's order is 2 N_max over every part (engine.rs:2016-2036),
+    the layered class's pass 1 included."""
+    wl = np.array([0.45, 0.8])
+    core = np.array([1.95 + 0.79j, 1.9 + 0.7j])
+    shell = np.array([1.43 + 0.01j, 1.42 + 0.01j])
+    comps = [(_dists((1, 0.1, 1.5)), None, 2.0, np.array([1.45 + 0j, 1.44 + 1e-5j])),
+             (_dists((1, 0.12, 1.4)), None, 0.5, ("layered", [0.5], np.stack([core, shell])))]
+    got = _native.ensemble_mixture(comps, wl, MU, _native.GREEK_ALL)
+    ref = O.ensemble_mixture_d([(_odist(d), mw, w, m) for d, mw, w, m in comps], wl, NONE,
+                               mu=MU, greek_order="all")
+    assert got["greek"].shape == ref["greek"].shape
+    assert np.array_equal(_orders(got["greek"]), _orders(ref["greek"]))
+    _compare(got, ref, 1e-11, 1e-9)
+
+
+def test_all_orders_with_spheroids(gpu):
+    """The spheroids' N enters the order; the spheres' bands project to min(2 N_max, 2 N_band)
+    and the spheroids' direct segment to 2 N of their own."""
+    wl = np.array([0.8, 1.0])
+    dust = np.array([1.53 + 0.008j, 1.52 + 0.01j])
+    comps = [(_dists((1, 0.03, 1.5)), None, 2.0, np.array([1.45 + 0j, 1.44 + 0j])),
+             (_dists((1, 0.08, 1.4)), None, 0.5, ("spheroid", 1.5, dust))]
+    got = _native.ensemble_mixture(comps, wl, MU, _native.GREEK_ALL, rtol=1e-4)
+    ref = O.ensemble_mixture_d([(_odist(d), mw, w, m) for d, mw, w, m in comps], wl, NONE,
+                               mu=MU, greek_order="all", rtol=1e-4)
+    assert got["greek"].shape == ref["greek"].shape
+    assert np.array_equal(_orders(got["greek"]), _orders(ref["greek"]))
+    _compare(got, ref, 1e-9, 1e-6)
+
+
 def test_the_reference_call(gpu):
     wl = np.array([0.6])
     m = np.array([1.5 + 0.02j])
