@@ -187,6 +187,15 @@ struct Context {
   size_t staging_cap = 0;  // bytes per half
   cudaEvent_t staged[2] = {nullptr, nullptr};
   bool staged_pending[2] = {false, false};
+  // The outputs' copies to pinned host arrays, slab by slab, beside the next slabs' kernels: a
+  // non-blocking stream (the kernels run on the legacy default stream) ordered by slab_done.
+  cudaStream_t copies = nullptr;
+  cudaEvent_t slab_done = nullptr;
+  void ensure_copies() {
+    if (copies) return;
+    SB_CUDA(cudaStreamCreateWithFlags(&copies, cudaStreamNonBlocking));
+    SB_CUDA(cudaEventCreateWithFlags(&slab_done, cudaEventDisableTiming));
+  }
 
   void ensure_staging(size_t bytes) {
     if (!staged[0]) {
@@ -410,6 +419,11 @@ struct FixedCall {
   std::vector<double> wl_host;
   int64_t n_dist = 0, n_wl = 0, n_nodes = 0;
   bool per_unit = false;
+  // Pinned host outputs (values, and phase and greek when they have a length): each slab's units
+  // are copied there on the copy stream once its final kernel is done (Context::copies).
+  double* h_values = nullptr;
+  double* h_phase = nullptr;
+  double* h_greek = nullptr;
 };
 
 // The device pipeline; wl_dev and m_dev are device arrays, outputs device arrays.
@@ -643,24 +657,30 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
   std::sort(by_cost.begin(), by_cost.end(), [&](int x, int y) {
     return ucost[x] != ucost[y] ? ucost[x] > ucost[y] : x < y;
   });
-  // Deal the units, largest first, in snake order over n_slabs slabs: every slab gets the same
-  // mix of large and small units. More slabs while one overflows the arena.
+  // Cut the units, in order, into slabs of consecutive units (so that a slab's outputs are a few
+  // contiguous ranges, copied out while the next slabs run) of about equal work, each within the
+  // arena and the chunk limit.
   int64_t n_slabs = std::max<int64_t>(1, (total_rows + arena - 1) / arena);
   n_slabs = std::max<int64_t>(n_slabs, (n_chunks + kMaxSlabChunks - 1) / kMaxSlabChunks);
   std::vector<int> slab_of(n_units);
-  for (;;) {
-    std::vector<int64_t> rows(n_slabs, 0), chunks(n_slabs, 0);
-    bool fits = true;
-    for (int64_t k = 0; k < n_units; ++k) {
-      const int64_t round = k / n_slabs, pos = k % n_slabs;
-      const int64_t sl = (round & 1) ? n_slabs - 1 - pos : pos;
-      slab_of[by_cost[k]] = (int)sl;
-      rows[sl] += urows[by_cost[k]];
-      chunks[sl] += cpu;
-      if (rows[sl] > arena || chunks[sl] > kMaxSlabChunks) fits = false;
+  std::vector<int64_t> slab_lo;  // the first unit of each slab
+  {
+    const double target = total_cost / (double)n_slabs;
+    int64_t rows = 0, chunks = 0;
+    double cost = 0.0;
+    for (int64_t u = 0; u < n_units; ++u) {
+      if (u == 0 || rows + urows[u] > arena || chunks + cpu > kMaxSlabChunks ||
+          cost >= target) {
+        slab_lo.push_back(u);
+        rows = chunks = 0;
+        cost = 0.0;
+      }
+      slab_of[u] = (int)slab_lo.size() - 1;
+      rows += urows[u];
+      chunks += cpu;
+      cost += ucost[u];
     }
-    if (fits) break;
-    ++n_slabs;
+    n_slabs = (int64_t)slab_lo.size();
   }
   // A large unit's row tiles split into work items of about item_target work each.
   const int grid_max = c.sms * c.unit_bps;
@@ -1022,6 +1042,24 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
     fa.slots = slots_d + S.sl0;
     timed_launch(K_FINAL, s, [&] { launch_final(fa, s); });
     SB_CUDA(cudaGetLastError());
+    if (call && call->h_values && !ad.on && !dv.on) {
+      // This slab's units are [lo, hi): copy their outputs out beside the next slabs.
+      const int64_t lo = slab_lo[sl], hi = sl + 1 < n_slabs ? slab_lo[sl + 1] : n_units;
+      const int64_t nu = hi - lo, glen = opt->greek_order + 1;
+      SB_CUDA(cudaEventRecord(c.slab_done, s));
+      SB_CUDA(cudaStreamWaitEvent(c.copies, c.slab_done, 0));
+      for (int k = 0; k < 11; ++k)
+        SB_CUDA(cudaMemcpyAsync(call->h_values + k * n_units + lo, values + k * n_units + lo,
+                                nu * 8, cudaMemcpyDeviceToHost, c.copies));
+      for (int e = 0; e < 6 && call->h_phase && n_mu > 0; ++e)
+        SB_CUDA(cudaMemcpyAsync(call->h_phase + (e * n_units + lo) * n_mu,
+                                phase + (e * n_units + lo) * n_mu, nu * n_mu * 8,
+                                cudaMemcpyDeviceToHost, c.copies));
+      for (int e = 0; e < 6 && call->h_greek && glen > 0; ++e)
+        SB_CUDA(cudaMemcpyAsync(call->h_greek + (e * n_units + lo) * glen,
+                                greek + (e * n_units + lo) * glen, nu * glen * 8,
+                                cudaMemcpyDeviceToHost, c.copies));
+    }
   }
   if (call && !ad.on) {
     call->radius = std::move(radius);
@@ -3241,7 +3279,30 @@ int scatrs_ensemble_fixed(const scatrs_distribution* dists, int64_t n_dist,
     double* g_d = gl > 0 ? c.greek.as<double>(gl) : nullptr;
     FixedCall call;
     call.wl_host.assign(wavelengths, wavelengths + n_wl);
+    // Pinned outputs are copied slab by slab beside the computation; others at the end.
+    auto pinned = [](const void* p) {
+      cudaPointerAttributes at{};
+      if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+      }
+      return at.type == cudaMemoryTypeHost;
+    };
+    const bool overlap = pinned(values) && (pl == 0 || !phase || pinned(phase)) &&
+                         (gl == 0 || !greek || pinned(greek));
+    if (overlap) {
+      c.ensure_copies();
+      call.h_values = values;
+      call.h_phase = pl > 0 ? phase : nullptr;
+      call.h_greek = gl > 0 ? greek : nullptr;
+    }
     run_fixed(c, dists, n_dist, wl_d, n_wl, m_d, mu, n_mu, options, v_d, p_d, g_d, s, &call);
+    if (overlap) {
+      const cudaError_t e = cudaStreamSynchronize(c.copies);
+      check_device_errors(c, s, &call);
+      SB_CUDA(e);
+      return;
+    }
     check_device_errors(c, s, &call);
     SB_CUDA(cudaMemcpyAsync(values, v_d, vl * 8, cudaMemcpyDeviceToHost, s));
     if (pl > 0 && phase) SB_CUDA(cudaMemcpyAsync(phase, p_d, pl * 8, cudaMemcpyDeviceToHost, s));
