@@ -279,8 +279,10 @@ __global__ void __launch_bounds__(128, 4) mie_fixed_kernel(MieFixedArgs a) {
   mie_chunk<false, false>(a);
 }
 
-// Homogeneous spheres on adaptive panels (with the chunk's |Kronrod - Gauss| sums).
-__global__ void __launch_bounds__(128) mie_adaptive_kernel(MieFixedArgs a) {
+// Homogeneous spheres on adaptive panels (with the chunk's |Kronrod - Gauss| sums). 4 CTAs per
+// SM as mie_fixed_kernel (178 -> 128 registers): 7.8 -> 5.1 ms on a batch of 16 lognormals x 256
+// wavelengths (3 CTAs: 6.0 ms).
+__global__ void __launch_bounds__(128, 4) mie_adaptive_kernel(MieFixedArgs a) {
   mie_chunk<false, true>(a);
 }
 
