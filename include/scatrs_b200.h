@@ -448,9 +448,13 @@ int scatrs_mie(const double* x, const double* m, int64_t n, int32_t allow_unvali
  * n_terms[n], coeffs[4 * total_terms] (laid out as in scatrs_mie), eff[5 * n] or NULL;
  * total_terms is the sum of the N_s. The recurrences' scratch is a fixed 12 MiB array compiled
  * into the library (every GPU that loads it holds the array until exit): calls needing more than
- * its 524288 rows (total_terms + 2 n) are rejected with SCATRS_INVALID_INPUT. The first call on a
- * device resolves the array's address with that device current, so make it before any stream
- * capture. All calls on a device share the array: calls that overlap on the GPU race on it.
+ * its 524288 rows (total_terms + 2 n) are rejected with SCATRS_INVALID_INPUT. A sphere whose N_s
+ * terms (the device's own count) start below 0, reach the next sphere's offset or pass
+ * total_terms is rejected with SCATRS_INVALID_INPUT before it writes anything; on any error the
+ * outputs' contents are unspecified, but nothing is written outside [0, total_terms) terms. The
+ * first call on a device (and the first after its current CUDA context changed) resolves the
+ * array's address with that device current, so make it before any stream capture. All calls
+ * on a device share the array: calls that overlap on the GPU race on it.
  * Runs on `stream` (a cudaStream_t, or NULL) and synchronizes it before returning.
  */
 int scatrs_mie_static(const double* x, const double* m, int64_t n, int32_t allow_unvalidated,

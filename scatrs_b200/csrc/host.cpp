@@ -3290,14 +3290,24 @@ int scatrs_ensemble_fixed(const scatrs_distribution* dists, int64_t n_dist,
     };
     const bool overlap = pinned(values) && (pl == 0 || !phase || pinned(phase)) &&
                          (gl == 0 || !greek || pinned(greek));
+    // Waits for the slab copies into the caller's pinned arrays on every exit, the error
+    // exits included, so that no copy outlives the call.
+    struct CopyWait {
+      cudaStream_t st = nullptr;
+      ~CopyWait() {
+        if (st && cudaStreamSynchronize(st) != cudaSuccess) cudaGetLastError();
+      }
+    } copy_wait;
     if (overlap) {
       c.ensure_copies();
+      copy_wait.st = c.copies;
       call.h_values = values;
       call.h_phase = pl > 0 ? phase : nullptr;
       call.h_greek = gl > 0 ? greek : nullptr;
     }
     run_fixed(c, dists, n_dist, wl_d, n_wl, m_d, mu, n_mu, options, v_d, p_d, g_d, s, &call);
     if (overlap) {
+      copy_wait.st = nullptr;
       const cudaError_t e = cudaStreamSynchronize(c.copies);
       check_device_errors(c, s, &call);
       SB_CUDA(e);

@@ -12,7 +12,8 @@
 // calls on a device share it and it keeps the last call's contents: two calls that overlap on the
 // GPU (on different streams, or from different host threads) race on it and must not be issued.
 // The first call on each device resolves the array's device address (cudaGetSymbolAddress) with
-// that device current; make that first call before any stream capture.
+// that device current, and again whenever the device's current CUDA context has changed (a
+// symbol's address belongs to a context); make that first call before any stream capture.
 //
 // Compiled with -fmad=false, like the allocating entry point (scatrs_mie), whose results this
 // one reproduces bit for bit.
@@ -38,17 +39,50 @@ static __device__ __align__(256) double g_scratch[3 * kStaticRows];
 // call before its launch.
 static __device__ __align__(256) unsigned long long g_status;
 
+// The arrays' device addresses, resolved per device and per CUDA context: a symbol's address
+// belongs to the context that loaded the module, so a new primary context (after
+// cudaDeviceReset) or a caller's own context on the same device resolves them again.
+struct Resolved {
+  void* ctx = nullptr;
+  double* scratch = nullptr;
+  unsigned long long* status = nullptr;
+};
 std::mutex g_mtx;
-double* g_scratch_dev[kMaxDevices];
-unsigned long long* g_status_dev[kMaxDevices];
+Resolved g_resolved[kMaxDevices];
 
-// The batched Mie solve with its scratch in the static array: sphere t uses rows
-// [coeff_offset[t] + 2t, coeff_offset[t] + 2t + N_t + 2), checked against the array's size.
+// The current context's handle (the driver's cuCtxGetCurrent, reached through the runtime so
+// that the library needs no link to libcuda); nullptr when it cannot be read.
+void* current_context() {
+  using GetCurrent = int (*)(void**);
+  static GetCurrent fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      return GetCurrent(nullptr);
+    }
+    return reinterpret_cast<GetCurrent>(p);
+  }();
+  void* ctx = nullptr;
+  if (!fn || fn(&ctx) != 0) return nullptr;
+  return ctx;
+}
+
+// The batched Mie solve with its scratch in the static array: sphere t writes coefficient
+// terms [coeff_offset[t], coeff_offset[t] + N_t) and uses scratch rows
+// [coeff_offset[t] + 2t, coeff_offset[t] + 2t + N_t + 2). Before any write, a sphere whose terms
+// start below 0, pass total_terms or reach the next sphere's offset is rejected (status 2): the
+// device's own N_t decides, so a caller whose N_t differs (a host cbrt that rounds the other way
+// at an integer boundary) gets an error, never a write outside its buffers. With every sphere
+// accepted the ranges are disjoint and inside [0, total_terms), and since the host checked
+// total_terms + 2n <= kStaticRows, the scratch rows stay inside the array too.
 __global__ void __launch_bounds__(128)
     mie_nodes_static_kernel(const double* __restrict__ x_in, const double2* __restrict__ m_in,
-                            int64_t n, int allow_unvalidated, int64_t* n_terms,
-                            const int64_t* __restrict__ coeff_offset, double* coeffs,
-                            double* eff, double* scratch, unsigned long long* status) {
+                            int64_t n, int allow_unvalidated, int64_t total_terms,
+                            int64_t* n_terms, const int64_t* __restrict__ coeff_offset,
+                            double* coeffs, double* eff, double* scratch,
+                            unsigned long long* status) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   const double x = x_in[t];
@@ -56,7 +90,10 @@ __global__ void __launch_bounds__(128)
   const int64_t nt = default_n_max(x);
   int st = check_node(x, m, nt, allow_unvalidated != 0);
   const int64_t off = coeff_offset[t];
-  if (st == 0 && (off < 0 || off + 2 * t + nt + 2 > kStaticRows)) st = 2;  // scratch exceeded
+  const int64_t end = t + 1 < n ? coeff_offset[t + 1] : total_terms;
+  if (st == 0 && (off < 0 || off + nt > end || end > total_terms ||
+                  off + 2 * t + nt + 2 > kStaticRows))
+    st = 2;  // the caller's layout does not hold this sphere's terms
   if (st != 0) {
     atomicMin(status, ((unsigned long long)t << 2) | (unsigned long long)st);
     return;
@@ -123,20 +160,26 @@ extern "C" int scatrs_mie_static(const double* x, const double* m, int64_t n,
   unsigned long long* status;
   {
     std::lock_guard<std::mutex> lk(g_mtx);
-    if (!g_scratch_dev[dev]) {
+    // No context yet (the runtime creates the primary context lazily) reads as nullptr and
+    // resolves; resolving creates it, and its handle is recorded after.
+    void* ctx = current_context();
+    Resolved& r = g_resolved[dev];
+    if (!r.scratch || !ctx || r.ctx != ctx) {
       void* p = nullptr;
       void* q = nullptr;
       rc = cudaGetSymbolAddress(&p, g_scratch);
       if (rc == cudaSuccess) rc = cudaGetSymbolAddress(&q, g_status);
       if (rc != cudaSuccess) {
+        r = Resolved{};
         put(err, err_len, cudaGetErrorString(rc));
         return SCATRS_CUDA;
       }
-      g_scratch_dev[dev] = static_cast<double*>(p);
-      g_status_dev[dev] = static_cast<unsigned long long*>(q);
+      r.ctx = current_context();
+      r.scratch = static_cast<double*>(p);
+      r.status = static_cast<unsigned long long*>(q);
     }
-    scratch = g_scratch_dev[dev];
-    status = g_status_dev[dev];
+    scratch = r.scratch;
+    status = r.status;
   }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   rc = cudaMemsetAsync(status, 0xff, sizeof(unsigned long long), s);
@@ -144,8 +187,8 @@ extern "C" int scatrs_mie_static(const double* x, const double* m, int64_t n,
     const int threads = 128;
     const int blocks = (int)((n + threads - 1) / threads);
     mie_nodes_static_kernel<<<blocks, threads, 0, s>>>(
-        x, reinterpret_cast<const double2*>(m), n, allow_unvalidated, n_terms, coeff_offset,
-        coeffs, eff, scratch, status);
+        x, reinterpret_cast<const double2*>(m), n, allow_unvalidated, total_terms, n_terms,
+        coeff_offset, coeffs, eff, scratch, status);
     rc = cudaGetLastError();
   }
   unsigned long long h = ~0ull;
@@ -157,11 +200,12 @@ extern "C" int scatrs_mie_static(const double* x, const double* m, int64_t n,
   }
   if (h != ~0ull) {
     const int st = (int)(h & 3);
-    char buf[200];
+    char buf[320];
     snprintf(buf, sizeof buf, "sphere %lld: %s", (long long)(h >> 2),
              st == 3   ? "outside the validated domain"
-             : st == 2 ? "its scratch rows pass the end of the static array (coeff_offset is "
-                         "not the prefix sum of the terms, or total_terms is too small)"
+             : st == 2 ? "its N terms do not fit the caller's layout (coeff_offset is not the "
+                         "exclusive prefix sum of N = ceil(x + 6 x^(1/3) + 3), or total_terms "
+                         "is too small); nothing was written for it"
                        : "invalid input");
     put(err, err_len, buf);
     return st == 3 ? SCATRS_OUTSIDE_VALIDATED_DOMAIN : SCATRS_INVALID_INPUT;

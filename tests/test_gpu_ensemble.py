@@ -190,3 +190,44 @@ def test_pinned_outputs_are_copied_per_slab(gpu):
     assert np.array_equal(pv.numpy().reshape(values.shape), values)
     assert np.array_equal(pp.numpy().reshape(phase.shape), phase)
     assert np.array_equal(pg.numpy().reshape(greek.shape), greek)
+
+
+def _sub(w, dist_idx, wl_idx):
+    """The units (dist_idx x wl_idx) of a workload, at its own shape (nodes, cosines, order)."""
+    dist_idx, wl_idx = np.atleast_1d(dist_idx), np.atleast_1d(wl_idx)
+    return W.Workload(w.name + "[sub]", w.dists[dist_idx], w.wavelengths[wl_idx],
+                      w.m[np.ix_(dist_idx, wl_idx)], w.mu, w.n_nodes, w.greek_order)
+
+
+def test_batched_full_shape_largest_n_units(gpu):
+    """The batched workload at its real shape (512 nodes, 360 Gauss cosines, order 64) on its
+    units of largest N (the widest lognormal at the shortest wavelengths: N up to 2198) and on
+    units of a middle and a small distribution."""
+    w = W.batched_spheres(seed=0)
+    assert w.mu.size == 360 and w.n_nodes == 512 and w.greek_order == 64
+    top = int(np.argmax(w.dists["r_hi"]))
+    sub = _sub(w, top, [0, 1, 2, 3, 700, 1023])
+    x = 2 * np.pi * sub.dists["r_hi"][0] / sub.wavelengths[0]
+    assert np.ceil(x + 6 * np.cbrt(x) + 3) >= 2190
+    got = gpu.ensemble_fixed(sub.dists, sub.wavelengths, sub.m, sub.mu, sub.n_nodes,
+                             sub.greek_order)
+    _compare(got, _oracle(sub, threads=0))
+    order = np.argsort(w.dists["r_hi"])
+    sub = _sub(w, [int(order[0]), int(order[w.dists.size // 2])], [0, 333, 1023])
+    got = gpu.ensemble_fixed(sub.dists, sub.wavelengths, sub.m, sub.mu, sub.n_nodes,
+                             sub.greek_order)
+    _compare(got, _oracle(sub, threads=0))
+
+
+def test_layered_full_shape_units(gpu):
+    """The layered workload at its real shape (three layers, 256 nodes, order 32) on full-size
+    units: its two widest distributions at its shortest and longest wavelengths."""
+    w = W.layered_spheres(seed=0)
+    top = np.argsort(w.dists["r_hi"])[-2:]
+    wl_idx = np.array([0, w.wavelengths.size - 1])
+    sub = W.LayeredWorkload(w.name + "[sub]", w.dists[top], w.wavelengths[wl_idx],
+                            w.fractions[top], w.m_layers[np.ix_(top, np.arange(3), wl_idx)],
+                            w.mu, w.n_nodes, w.greek_order)
+    got = gpu.ensemble_fixed_layered(sub.dists, sub.wavelengths, sub.fractions, sub.m_layers,
+                                     sub.mu, sub.n_nodes, sub.greek_order)
+    _compare(got, _oracle_layered(sub), tol=1e-11)
