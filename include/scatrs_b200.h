@@ -461,6 +461,42 @@ int scatrs_mie_static(const double* x, const double* m, int64_t n, int32_t allow
                       int64_t total_terms, int64_t* n_terms, const int64_t* coeff_offset,
                       double* coeffs, double* eff, void* stream, char* err, size_t err_len);
 
+/* The accuracy reached and the accuracy requested of the last call on this thread that failed
+ * with SCATRS_NOT_CONVERGED (scatrs::Error::NotConverged { achieved, requested },
+ * scatrs/src/error.rs:22-28, which the reference's binding passes to NotConvergedError,
+ * scatrs-py/src/errors.rs:24-31): returns 1 and writes both when the last call on this thread
+ * returned SCATRS_NOT_CONVERGED, else returns 0 and writes NaN. */
+int scatrs_not_converged_detail(double* achieved, double* requested);
+
+/* Test hooks, not part of the API (the reference's scatrs._scatrs._testing,
+ * scatrs-py/src/testing.rs:29-57):
+ * scatrs_testing_raise fails with `status` (1-5), `message` and, for SCATRS_NOT_CONVERGED,
+ *   `achieved`/`requested`, through the same error path as every entry point (the status, the
+ *   message buffer and scatrs_not_converged_detail); status 0 returns SCATRS_OK.
+ * scatrs_testing_fail_allocation(k): the k-th device buffer growth from now fails as an
+ *   out-of-memory cudaMalloc would (SCATRS_CUDA); 0 disarms it.
+ * scatrs_testing_force_node_error(key, status): the next fixed-grid call's device error word
+ *   also holds a node error `status` (1 invalid input, 3 outside the validated domain) at
+ *   key = (wavelength * n_dist + distribution) * n_nodes + node, merged as the kernels merge
+ *   theirs (the first in order wins); a negative key disarms it. */
+int scatrs_testing_raise(int32_t status, const char* message, double achieved, double requested,
+                         char* err, size_t err_len);
+void scatrs_testing_fail_allocation(int64_t k);
+void scatrs_testing_force_node_error(int64_t key, int32_t status);
+
+/* The library's limits, which it enforces, as the reference module exports them
+ * (scatrs-py/src/lib.rs:17-50); -1 for an unknown `which`. */
+enum scatrs_limit_kind {
+  SCATRS_LIMIT_MIE_ORDER = 0,             /* terms of one sphere (mie/mod.rs:101) */
+  SCATRS_LIMIT_MIE_VALUES = 1,            /* real values of one output array / 2 */
+  SCATRS_LIMIT_GREEK_ORDER = 2,           /* Greek order (mie/greek.rs:344) */
+  SCATRS_LIMIT_LAYERS = 3,                /* layers of a layered sphere on the GPU (16) */
+  SCATRS_LIMIT_TMATRIX_ORDER = 4,         /* spheroid truncation N (tmatrix/mod.rs:180) */
+  SCATRS_LIMIT_GAUSS_LEGENDRE_POINTS = 5, /* points of a Gauss-Legendre rule */
+  SCATRS_LIMIT_WIGNER_D_VALUES = 6        /* Wigner values of one projection table */
+};
+int64_t scatrs_limit(int32_t which);
+
 /* The CUDA device count, or -1 when the runtime is unusable. */
 int scatrs_device_count(void);
 
@@ -481,7 +517,8 @@ int scatrs_kernel_times(double* ms, int64_t* launches, int32_t n);
 int64_t scatrs_spheroid_work(int64_t* per_launch, int64_t cap);
 
 /* Gauss-Legendre rule of n points on [-1, 1] (ascending nodes), as the host tables use it
- * (scatrs/src/special/gauss_legendre.rs:188-260). */
+ * (scatrs/src/special/gauss_legendre.rs:188-260); writes nothing unless
+ * 1 <= n <= SCATRS_LIMIT_GAUSS_LEGENDRE_POINTS. */
 void scatrs_gauss_legendre(int64_t n, double* nodes, double* weights);
 
 /* Frees the cached tables and buffers of the current device. */

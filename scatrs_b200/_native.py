@@ -11,7 +11,7 @@ import os
 
 import numpy as np
 
-from .errors import DeviceError, InvalidInputError, raise_for
+from .errors import DeviceError, InvalidInputError, classes, raise_for
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libscatrs_b200.so")
@@ -141,6 +141,11 @@ SYMBOLS = {
     "scatrs_mie": (ctypes.c_int, [_PD, _PD, _I64, _I32, _PI64, _PI64, _PD, _PD, _CP, _SZ]),
     "scatrs_mie_static": (ctypes.c_int, [_VP, _VP, _I64, _I32, _I64, _VP, _VP, _VP, _VP, _VP,
                                          _CP, _SZ]),
+    "scatrs_not_converged_detail": (ctypes.c_int, [_PD, _PD]),
+    "scatrs_testing_raise": (ctypes.c_int, [_I32, _CP, _D, _D, _CP, _SZ]),
+    "scatrs_testing_fail_allocation": (None, [_I64]),
+    "scatrs_testing_force_node_error": (None, [_I64, _I32]),
+    "scatrs_limit": (_I64, [_I32]),
     "scatrs_device_count": (ctypes.c_int, []),
     "scatrs_launch_count": (_I64, []),
     "scatrs_gauss_legendre": (None, [_I64, _PD, _PD]),
@@ -176,7 +181,7 @@ def load() -> ctypes.CDLL:
 def require_device() -> None:
     n = load().scatrs_device_count()
     if n <= 0:
-        raise DeviceError("no usable CUDA device: the ensemble path runs on the GPU only")
+        raise classes()[3]("no usable CUDA device: the ensemble path runs on the GPU only")
 
 
 def _p(a):
@@ -184,10 +189,27 @@ def _p(a):
 
 
 def _check(status: int, buf) -> None:
-    raise_for(status, buf.value.decode(errors="replace"))
+    achieved = requested = None
+    if status == 2:
+        a, r = _D(), _D()
+        if load().scatrs_not_converged_detail(ctypes.byref(a), ctypes.byref(r)):
+            achieved, requested = a.value, r.value
+    raise_for(status, buf.value.decode(errors="replace"), achieved, requested)
+
+
+_LIMITS = {"MIE_ORDER": 0, "MIE_VALUES": 1, "GREEK_ORDER": 2, "LAYERS": 3, "TMATRIX_ORDER": 4,
+           "GAUSS_LEGENDRE_POINTS": 5, "WIGNER_D_VALUES": 6}
+
+
+def limit(name: str) -> int:
+    """One of the library's limits (scatrs_limit), by its SCATRS_LIMIT_ name."""
+    return int(load().scatrs_limit(_LIMITS[name]))
 
 
 def gauss_legendre(n: int):
+    if not 1 <= n <= limit("GAUSS_LEGENDRE_POINTS"):
+        raise InvalidInputError(
+            f"a Gauss-Legendre rule needs 1 <= n <= MAX_GAUSS_LEGENDRE_POINTS, got {n}")
     x = np.zeros(n)
     w = np.zeros(n)
     load().scatrs_gauss_legendre(n, _p(x), _p(w))

@@ -21,7 +21,13 @@ the GPU library.
   mixture), each a lognormal, gamma, modified gamma, power law, monodisperse or multimodal
   distribution; values and error estimates.
 
-Errors are those of the reference's Python package (scatrs_b200.errors).
+Errors are those of the reference's Python package: the classes of ``scatrs.errors`` when this
+module serves that package as its extension (``scatrs._scatrs``), else the same hierarchy from
+``scatrs_b200.errors``; NotConvergedError carries ``achieved`` and ``requested``.
+
+Module attributes read by the reference package at import (scatrs-py/src/lib.rs:17-50):
+``__version__`` (the reference workspace version this module stands in for) and the ``MAX_*``
+limits, read from the library, which enforces them.
 """
 
 from __future__ import annotations
@@ -30,6 +36,17 @@ import numpy as np
 
 from . import _native
 from .errors import InvalidInputError
+
+# The reference's workspace version (Cargo.toml:6) that this binding surface follows.
+__version__ = "0.3.0"
+
+MAX_MIE_ORDER: int = _native.limit("MIE_ORDER")
+MAX_MIE_VALUES: int = _native.limit("MIE_VALUES")
+MAX_GREEK_ORDER: int = _native.limit("GREEK_ORDER")
+MAX_LAYERS: int = _native.limit("LAYERS")
+MAX_TMATRIX_ORDER: int = _native.limit("TMATRIX_ORDER")
+MAX_GAUSS_LEGENDRE_POINTS: int = _native.limit("GAUSS_LEGENDRE_POINTS")
+MAX_WIGNER_D_VALUES: int = _native.limit("WIGNER_D_VALUES")
 
 _PARAMS = {
     "lognormal": ("median_radius", "width"),
@@ -439,3 +456,30 @@ def ensemble_compute_fixed(specs, particle_spec, wavelengths, greek, all_orders,
     out["converged"] = np.ones(n, dtype=bool)
     out["panels"] = np.zeros(n, dtype=np.uint64)
     return out
+
+
+class _Testing:
+    """Hooks for tests, not part of the API (the reference's ``scatrs._scatrs._testing``,
+    scatrs-py/src/testing.rs:29-57): ``raise_core_error`` raises what a failed library call with
+    that error raises, through the library's own error path."""
+
+    _STATUS = {"InvalidInput": 1, "NotConverged": 2, "OutsideValidatedDomain": 3}
+
+    @staticmethod
+    def raise_core_error(variant: str, message: str = "", achieved: float = 0.0,
+                         requested: float = 0.0) -> None:
+        import ctypes
+
+        if variant not in _Testing._STATUS:
+            raise ValueError(f"unknown scatrs::Error variant {variant!r}")
+        # The reference's Display texts (scatrs/src/error.rs:18-31).
+        text = {"InvalidInput": f"invalid input: {message}",
+                "NotConverged": f"not converged: achieved {achieved:e}, requested {requested:e}",
+                "OutsideValidatedDomain": f"outside validated domain: {message}"}[variant]
+        err = ctypes.create_string_buffer(1024)
+        st = _native.load().scatrs_testing_raise(_Testing._STATUS[variant], text.encode(),
+                                                 achieved, requested, err, 1024)
+        _native._check(st, err)
+
+
+_testing = _Testing()

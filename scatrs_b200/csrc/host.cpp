@@ -82,14 +82,28 @@ namespace {
 
 constexpr int64_t kMaxGreekOrder = 1 << 21;        // MAX_GREEK_ORDER (mie/greek.rs:344)
 constexpr int64_t kMaxMieValues = 1 << 27;         // scatrs-py/src/mie.rs:30
+constexpr int64_t kMaxMieOrder = 1 << 20;          // MAX_MIE_ORDER (mie/mod.rs:101), check_node
+constexpr int64_t kMaxLayersAbi = 16;              // layers the layered kernels carry
+constexpr int64_t kMaxTmatrixOrder = 500;          // MAX_TMATRIX_ORDER (tmatrix/mod.rs:180)
+constexpr int64_t kMaxGaussPoints = 1 << 17;       // special/gauss_legendre.rs:43
+constexpr int64_t kMaxWignerValues = 1 << 28;      // scatrs-py/src/special.rs:24
 constexpr int64_t kArenaRows = 1 << 22;            // coefficient rows per slab (1 KiB each)
 constexpr int64_t kMaxSlabChunks = 1 << 18;        // chunks per slab
 constexpr double kPi = 3.14159265358979323846264338327950288;
 
+// A failed call: its status, its message and, for SCATRS_NOT_CONVERGED, the accuracy reached
+// and the accuracy requested (scatrs::Error::NotConverged, scatrs/src/error.rs:22-28).
 struct Failure {
   int status;
   std::string msg;
+  double achieved = NAN;
+  double requested = NAN;
 };
+
+// The last failed call's accuracies on this thread (NaN unless it was SCATRS_NOT_CONVERGED).
+thread_local int g_last_status = SCATRS_OK;
+thread_local double g_last_achieved = NAN;
+thread_local double g_last_requested = NAN;
 
 void set_err(char* err, size_t len, const std::string& msg) {
   if (err && len > 0) {
@@ -108,6 +122,12 @@ void set_err(char* err, size_t len, const std::string& msg) {
 
 int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
 
+// Test hooks (scatrs_testing_*): the device allocation that fails as an out-of-memory
+// cudaMalloc would (0: none; k: the k-th growth from now), and a node error merged into the
+// next fixed-grid call's device error word (~0: none).
+std::atomic<int64_t> g_fail_allocation{0};
+std::atomic<unsigned long long> g_forced_node_error{~0ull};
+
 // A grow-only device buffer.
 struct DevBuf {
   void* p = nullptr;
@@ -118,6 +138,9 @@ struct DevBuf {
       p = nullptr;
       cap = 0;
       size_t want = std::max<size_t>(bytes, 256);
+      if (g_fail_allocation.load() > 0 && g_fail_allocation.fetch_sub(1) == 1)
+        throw Failure{SCATRS_CUDA, std::string("cudaMalloc(&p, want): ") +
+                                       cudaGetErrorString(cudaErrorMemoryAllocation)};
       SB_CUDA(cudaMalloc(&p, want));
       cap = want;
     }
@@ -523,7 +546,7 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
     }
   }
   const int L_layers = layers.n_layers;
-  if (L_layers < 1 || L_layers > 16)
+  if (L_layers < 1 || L_layers > kMaxLayersAbi)
     throw Failure{SCATRS_INVALID_INPUT, "the GPU path takes 1 to 16 layers"};
   if (L_layers > 1) {
     for (int64_t d = 0; d < n_dist; ++d)
@@ -1074,6 +1097,8 @@ void check_device_errors(Context& c, cudaStream_t s, const FixedCall* call) {
   unsigned long long h[2];
   SB_CUDA(cudaMemcpyAsync(h, c.err.as<unsigned long long>(2), sizeof h, cudaMemcpyDeviceToHost, s));
   SB_CUDA(cudaStreamSynchronize(s));
+  // A forced node error (test hook) merges as a kernel's atomicMin would: the first in order.
+  h[0] = std::min(h[0], g_forced_node_error.exchange(~0ull));
   if (h[0] != ~0ull) {
     int status = (int)(h[0] & 3);
     unsigned long long key = h[0] >> 2;
@@ -1449,7 +1474,7 @@ void adaptive_call_order(const std::vector<AdPart>& in, int n_out, bool batch,
   SB_CUDA(cudaMemcpyAsync(wl_d, wavelengths, n_wl * 8, cudaMemcpyHostToDevice, s));
   // Each pipeline unit's m, and a distinct index per (part, wavelength) for pass 1.
   const int L = layers && layers->n_layers > 1 ? layers->n_layers : 1;
-  if (L > 16) throw Failure{SCATRS_INVALID_INPUT, "the GPU path takes 1 to 16 layers"};
+  if (L > kMaxLayersAbi) throw Failure{SCATRS_INVALID_INPUT, "the GPU path takes 1 to 16 layers"};
   if (L > 1 && (!layers->fractions || !layers->m))
     throw Failure{SCATRS_INVALID_INPUT, "layers must give fractions and m"};
   if (L > 1 && deriv)
@@ -2372,6 +2397,7 @@ void spheroid_solve(Context& c, int64_t n, const double* x, const double* aspect
   struct St {
     int n, nth, cap, th_cap, stage;  // stage 0: N, 1: n_theta, 2: done
     double e, sc;
+    double change = INFINITY;  // the last step's relative change of the cross sections
   };
   std::vector<St> st(n);
   std::vector<TmSpec> specs;
@@ -2410,12 +2436,13 @@ void spheroid_solve(Context& c, int64_t n, const double* x, const double* aspect
       St& z = st[i];
       if (z.stage == 2) continue;
       if ((z.stage == 0 && z.n >= z.cap) || (z.stage == 1 && z.nth >= z.th_cap)) {
-        char buf[200];
+        // driver.rs:356-359: achieved is the last relative change, requested the rtol.
+        char buf[240];
         snprintf(buf, sizeof buf,
-                 "spheroid %lld: the cross sections did not settle to %g within N = %d, "
-                 "n_theta = %d",
-                 (long long)i, rtol, z.cap, z.th_cap);
-        throw Failure{SCATRS_NOT_CONVERGED, buf};
+                 "not converged: achieved %e, requested %e (spheroid %lld: the cross sections "
+                 "did not settle within N = %d, n_theta = %d)",
+                 z.change, rtol, (long long)i, z.cap, z.th_cap);
+        throw Failure{SCATRS_NOT_CONVERGED, buf, z.change, rtol};
       }
       int nn = z.n, nt = z.nth;
       if (z.stage == 0) {
@@ -2438,6 +2465,7 @@ void spheroid_solve(Context& c, int64_t n, const double* x, const double* aspect
       z.nth = specs[k].n_theta;
       z.e = e1;
       z.sc = s1;
+      z.change = ch;
       if (ch < rtol) z.stage += 1;
     }
   }
@@ -2857,14 +2885,20 @@ FixedCall g_last_call;  // for scatrs_check_errors
 
 template <class F>
 int guarded(char* err, size_t err_len, F f) {
+  g_last_status = SCATRS_OK;
+  g_last_achieved = g_last_requested = NAN;
   try {
     f();
     return SCATRS_OK;
   } catch (const Failure& e) {
     set_err(err, err_len, e.msg);
+    g_last_status = e.status;
+    g_last_achieved = e.achieved;
+    g_last_requested = e.requested;
     return e.status;
   } catch (const std::bad_alloc&) {
     set_err(err, err_len, "host allocation failed");
+    g_last_status = SCATRS_INVALID_INPUT;
     return SCATRS_INVALID_INPUT;
   }
 }
@@ -2945,7 +2979,7 @@ void mixture_hetero(const scatrs_component* components, int64_t n_comp,
       throw Failure{SCATRS_INVALID_INPUT, who + "the aspect ratio must be finite and > 0"};
     if (k.aspect_ratio > 0.0 && k.n_layers > 1)
       throw Failure{SCATRS_INVALID_INPUT, who + "a particle is layered or a spheroid, not both"};
-    if (k.n_layers > 16) throw Failure{SCATRS_INVALID_INPUT, who + "at most 16 layers"};
+    if (k.n_layers > kMaxLayersAbi) throw Failure{SCATRS_INVALID_INPUT, who + "at most 16 layers"};
     if (k.n_layers > 1 && !k.fractions)
       throw Failure{SCATRS_INVALID_INPUT, who + "a layered sphere needs its fractions"};
   }
@@ -3567,8 +3601,12 @@ int scatrs_project_greek_device(const double* phase_dev, int64_t n_units, int64_
                                 int32_t order, int32_t precision, double* greek_dev,
                                 void* stream, char* err, size_t err_len) {
   return guarded(err, err_len, [&] {
-    if (n_units < 0 || n_q < 1 || order < 0 || order > (1 << 21))
+    if (n_units < 0 || n_q < 1 || order < 0 || order > kMaxGreekOrder)
       throw Failure{SCATRS_INVALID_INPUT, "needs n_units >= 0, n_q >= 1 and 0 <= order"};
+    if (n_q > kMaxGaussPoints || (double)n_q * ((double)order + 1.0) > (double)kMaxWignerValues)
+      throw Failure{SCATRS_INVALID_INPUT,
+                    "the projection tables would exceed MAX_GAUSS_LEGENDRE_POINTS cosines or "
+                    "MAX_WIGNER_D_VALUES Wigner values"};
     if (precision != 0 && precision != 1)
       throw Failure{SCATRS_INVALID_INPUT, "precision must be 0 (FP64) or 1 (3xTF32)"};
     if (n_units == 0) return;
@@ -3903,7 +3941,7 @@ int scatrs_ensemble_fixed_layered_d(const scatrs_distribution* dists, int64_t n_
       if (!(std::isfinite(wavelengths[i]) && wavelengths[i] > 0.0))
         throw Failure{SCATRS_INVALID_INPUT, "wavelengths must be finite and > 0"};
     const int L = layers->n_layers;
-    if (L > 16) throw Failure{SCATRS_INVALID_INPUT, "the GPU path takes 1 to 16 layers"};
+    if (L > kMaxLayersAbi) throw Failure{SCATRS_INVALID_INPUT, "the GPU path takes 1 to 16 layers"};
     const int P_th = n_dist > 0 ? parameter_count(dists[0].kind) : 2;
     const int P = P_th + 2 * L + (L - 1);
     Context& c = context();
@@ -4095,7 +4133,43 @@ int scatrs_device_count(void) {
 int64_t scatrs_launch_count(void) { return g_launches.load(); }
 
 void scatrs_gauss_legendre(int64_t n, double* nodes, double* weights) {
+  if (n < 1 || n > sb::kMaxGaussPoints || !nodes || !weights) return;
   sb::gauss_legendre(n, nodes, weights);
+}
+
+int scatrs_testing_raise(int32_t status, const char* message, double achieved,
+                        double requested, char* err, size_t err_len) {
+  return sb::guarded(err, err_len, [&] {
+    if (status < SCATRS_INVALID_INPUT || status > SCATRS_NO_DEVICE) return;
+    throw sb::Failure{status, message ? message : "", achieved, requested};
+  });
+}
+
+void scatrs_testing_fail_allocation(int64_t after) { sb::g_fail_allocation = after; }
+
+void scatrs_testing_force_node_error(int64_t unit_key, int32_t status) {
+  sb::g_forced_node_error = unit_key < 0 ? ~0ull
+                                         : ((unsigned long long)unit_key << 2) |
+                                               (unsigned long long)(status & 3);
+}
+
+int scatrs_not_converged_detail(double* achieved, double* requested) {
+  if (achieved) *achieved = sb::g_last_achieved;
+  if (requested) *requested = sb::g_last_requested;
+  return sb::g_last_status == SCATRS_NOT_CONVERGED ? 1 : 0;
+}
+
+int64_t scatrs_limit(int32_t which) {
+  switch (which) {
+    case SCATRS_LIMIT_MIE_ORDER: return sb::kMaxMieOrder;
+    case SCATRS_LIMIT_MIE_VALUES: return sb::kMaxMieValues;
+    case SCATRS_LIMIT_GREEK_ORDER: return sb::kMaxGreekOrder;
+    case SCATRS_LIMIT_LAYERS: return sb::kMaxLayersAbi;
+    case SCATRS_LIMIT_TMATRIX_ORDER: return sb::kMaxTmatrixOrder;
+    case SCATRS_LIMIT_GAUSS_LEGENDRE_POINTS: return sb::kMaxGaussPoints;
+    case SCATRS_LIMIT_WIGNER_D_VALUES: return sb::kMaxWignerValues;
+    default: return -1;
+  }
 }
 
 void scatrs_set_profiling(int32_t on) {
