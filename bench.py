@@ -1,11 +1,15 @@
 """Benchmark of the fixed-grid Mie ensemble (the batched configuration: 1024 wavelengths x 64
 lognormal distributions x 512 radius nodes, 360 Gauss cosines, Greek order 64, FP64).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--i8-above T]
 
-A step is one pass of the hot path over the whole batch (33,554,432 size nodes). ``value`` is
-node throughput with the inputs resident in HBM, timed with CUDA events on the launching
-stream, L2 flushed between steps (a 512 MiB write outside the timed events), max over ranks.
+A step is one pass of the hot path over the whole batch (33,554,432 size nodes). Two forms run
+on the same inputs: the plain FP64 path and the mixed form (the angle GEMMs of every chunk with
+more than T terms as exact int8 digit products on the tensor cores). ``value`` is node
+throughput with the inputs resident in HBM, timed with CUDA events on the launching stream, L2
+flushed between steps (a 512 MiB write outside the timed events), max over ranks, of the mixed
+form when its outputs are within 1e-10 of the oracle on the sampled units (``parity_mixed``),
+else of the plain form (``headline_form`` says which); ``forms`` holds both and their ratio.
 ``e2e`` is the same metric through the C ABI with host buffers (pinned), the host-device copies
 of the inputs and outputs inside the timed region. For N > 1 every rank runs its own batch
 (seed = rank): weak scaling, no collective on the data path.
@@ -52,6 +56,11 @@ def parse():
                    help="skip the spheroid ensemble leg")
     p.add_argument("--no-projection", action="store_true",
                    help="skip the tensor-core Greek projection measurement")
+    p.add_argument("--i8-above", type=int, default=64,
+                   help="the mixed form: chunks with more terms than this take the int8 path "
+                        "(0: plain FP64 only)")
+    p.add_argument("--i8-levels", type=int, default=0,
+                   help="the mixed form's product levels kept: 5, 6, or 0 for the default")
     return p.parse_args()
 
 
@@ -311,10 +320,82 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def algorithmic_flops(w, user_rows: int):
+def chunk_shape(w, user_rows: int):
+    """Per wavelength: each node's N, each chunk's N_c and its band's table rows h_b."""
+    from scatrs_b200 import _native
+
+    r = np.empty((w.dists.size, w.n_nodes))
+    xi, _ = _native.gauss_legendre(w.n_nodes)
+    for d in range(w.dists.size):
+        a, b = np.log(w.dists["r_lo"][d]), np.log(w.dists["r_hi"][d])
+        r[d] = np.exp(0.5 * (a + b) + 0.5 * (b - a) * xi)
+    L = w.greek_order
+    cpu = (w.n_nodes + 31) // 32
+    pad = cpu * 32 - w.n_nodes
+    for lam in w.wavelengths:
+        x = 2.0 * np.pi * r / lam
+        n = np.ceil(x + 6.0 * np.cbrt(x) + 3.0)
+        npad = np.pad(n, ((0, 0), (0, pad)))
+        nc = npad.reshape(w.dists.size, cpu, 32).max(axis=2)
+        hb = np.zeros_like(nc)
+        if L >= 0:
+            u = np.ones_like(nc)
+            while np.any(u < nc):
+                u = np.where(u < nc, np.ceil(u * 1.25), u)
+            order = np.minimum(L, 2 * u)
+            nq = u + np.floor((order + 2) / 2)
+            hb = nq - np.floor(nq / 2)
+        yield n, nc, hb
+
+
+def algorithmic_i8_ops(w, user_rows: int, above: int, levels: int = 5):
+    """The mixed form's int8 work per step: per chunk with above < N_c <= 4096, the digit
+    products (15 for 5 levels, 19 for 6) of its two GEMMs [2 (h_u + h_b) rows x N_c orders] x
+    [N_c x 128 columns], 2 ops per multiply-add, at the real (unpadded) sizes."""
+    prods = 19 if levels == 6 else 15
+    total = 0.0
+    for _, nc, hb in chunk_shape(w, user_rows):
+        sel = (nc > above) & (nc <= 4096)
+        total += float(np.sum(np.where(sel, prods * 2.0 * 2 * (user_rows + hb) * 128 * nc,
+                                       0.0)))
+    return total
+
+
+def int8_peak_tops(torch):
+    """cuBLASLt int8 GEMM throughput (torch._int_mm, int32 results), best of 5, TOP/s."""
+    n = 8192
+    try:
+        a = torch.randint(-128, 127, (n, n), dtype=torch.int8, device="cuda")
+        b = torch.randint(-128, 127, (n, n), dtype=torch.int8, device="cuda")
+        for _ in range(2):
+            torch._int_mm(a, b)
+        best = 1e30
+        for _ in range(5):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            torch._int_mm(a, b)
+            e.record()
+            torch.cuda.synchronize()
+            best = min(best, s.elapsed_time(e))
+        del a, b
+        return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+    except (RuntimeError, AttributeError):
+        return None
+
+
+def algorithmic_flops(w, user_rows: int, at_most: int | None = None):
     """FP64 flops of K-b per step: 16 N_j (h_u + h_b) for node j (2 GEMMs x 4 real columns x 2
     flops per order and table row; h_u the requested cosines' table rows, h_b the rows of the
-    band of the node's chunk) -- the per-node figure of the angle sums."""
+    band of the node's chunk) -- the per-node figure of the angle sums. at_most: only the nodes
+    of chunks with N_c <= at_most (or above 4096), those the mixed form leaves in FP64."""
+    if at_most is not None:
+        total = 0.0
+        for n, nc, hb in chunk_shape(w, user_rows):
+            keep = (nc <= at_most) | (nc > 4096)
+            nrow = np.repeat(np.where(keep, 1.0, 0.0), 32, axis=1)[:, : w.n_nodes]
+            hrow = np.repeat(hb, 32, axis=1)[:, : w.n_nodes]
+            total += float(np.sum(nrow * 16.0 * n * (user_rows + hrow)))
+        return total
     r = np.empty((w.dists.size, w.n_nodes))
     from scatrs_b200 import _native
 
@@ -588,18 +669,151 @@ def ours(args):
     greek_d = torch.empty(6 * n * (w.greek_order + 1), dtype=torch.float64, device=dev)
     flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)
 
-    def step():
-        _native.ensemble_fixed_device(w.dists, wl_d.data_ptr(), w.wavelengths.size,
-                                      m_d.data_ptr(), w.mu, w.n_nodes, w.greek_order, True,
-                                      values_d.data_ptr(), phase_d.data_ptr(),
-                                      greek_d.data_ptr(), stream.cuda_stream)
-
     def barrier():
         if world > 1:
             import torch.distributed as dist
 
             dist.barrier()
         torch.cuda.synchronize()
+
+    # Both forms on the same inputs: the plain FP64 path, then the mixed form (the int8 angle
+    # GEMMs of the chunks with more than i8_above terms).
+    plain = run_form(args, w, 0, (values_d, phase_d, greek_d), wl_d, m_d, stream, flush,
+                     barrier, world, dev, local)
+    bufs_m = tuple(torch.empty_like(b) for b in (values_d, phase_d, greek_d))
+    mixed = None
+    if args.i8_above > 0:
+        mixed = run_form(args, w, args.i8_above, bufs_m, wl_d, m_d, stream, flush, barrier,
+                         world, dev, local)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    fp64 = fp64_peak_tflops(torch)
+    user_rows = int(np.unique(np.abs(w.mu)).size)
+    flops = algorithmic_flops(w, user_rows)
+    kt = plain["kt"]
+    unit_ms, unit_n = kt["unit_kernel"]
+    achieved = flops / (unit_ms * 1e-3) / 1e12
+    roof_fp64 = {"bound": "fp64", "kernel": "unit_kernel (K-b/c)", "achieved": achieved,
+                 "peak": fp64, "unit": "TFLOP/s", "frac": achieved / fp64,
+                 "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (the measured peaks "
+                                "file has no FP64 entry)",
+                 "traffic": UNIT_DRAM_BYTES_PER_NODE * w.n_nodes_total / max(unit_n, 1),
+                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
+                                   "launch on the 0.1-scale workload, scaled by nodes per "
+                                   "launch",
+                 "launches": unit_n, "avg_launch_ms": unit_ms / max(unit_n, 1),
+                 "algorithmic_flop_per_step": flops}
+    forms = {"fp64": form_summary(plain, w)}
+    head, roof = plain, roof_fp64
+    if mixed is not None:
+        forms["mixed"] = form_summary(mixed, w)
+        forms["mixed"]["i8_above"] = args.i8_above
+        forms["mixed"]["levels"] = args.i8_levels or 5
+        ops = algorithmic_i8_ops(w, user_rows, args.i8_above, args.i8_levels or 5)
+        ktm = mixed["kt"]
+        i8_ms, i8_n = ktm.get("unit_i8_kernel", (0.0, 0))
+        i8_peak = int8_peak_tops(torch)
+        ach8 = ops / (i8_ms * 1e-3) / 1e12 if i8_ms > 0 else 0.0
+        forms["mixed"]["roofline_i8"] = {
+            "bound": "tensor", "kernel": "unit_i8_kernel (int8 digit products, tcgen05)",
+            "achieved": ach8, "peak": i8_peak, "unit": "TOP/s (int8)",
+            "frac": ach8 / i8_peak if i8_peak else None,
+            "peak_source": "cuBLASLt int8 GEMM (torch._int_mm) 8192^3 measured in this run",
+            "launches": i8_n, "avg_launch_ms": i8_ms / max(i8_n, 1),
+            "algorithmic_ops_per_step": ops}
+        # The mixed form's FP64 share (the chunks at or below i8_above) on the FP64 roofline.
+        fp_flops = algorithmic_flops(w, user_rows, at_most=args.i8_above)
+        u_ms, u_n = ktm["unit_kernel"]
+        forms["mixed"]["roofline_fp64_part"] = {
+            "kernel": "unit_kernel (chunks with at most i8_above terms)",
+            "achieved": fp_flops / (u_ms * 1e-3) / 1e12 if u_ms > 0 else 0.0, "peak": fp64,
+            "unit": "TFLOP/s", "launches": u_n}
+        forms["speedup_mixed_vs_fp64"] = mixed["value"] / plain["value"]
+        forms["e2e_speedup_mixed_vs_fp64"] = mixed["e2e_value"] / plain["e2e_value"]
+    line = {
+        "metric": METRIC, "value": None, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": workload_config(w, args),
+        "hbm_peak_gbs": peaks.get("hbm_gbs"),
+        "forms": forms,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        ow = oracle_view(w)
+        forced, n_max = largest_units(ow, 8)
+        base, kept = cpu_sample(ow, args.cpu_seconds, forced=forced, keep=True)
+        line["cpu_baseline"] = base
+        line["parity"] = parity_leg(kept, values_d, phase_d, greek_d, n, w, forced, n_max)
+        if mixed is not None:
+            line["parity_mixed"] = parity_leg(kept, *bufs_m, n, w, forced, n_max, tol=1e-10)
+    # The headline: the mixed form where its parity is measured and within 1e-10 of the
+    # oracle, else the plain FP64 path.
+    use_mixed = (mixed is not None and line.get("parity_mixed", {}).get("within_tol", False))
+    if use_mixed:
+        head = mixed
+        i8 = forms["mixed"]["roofline_i8"]
+        roof = dict(i8)
+        roof["traffic"] = None
+    line["headline_form"] = "mixed" if use_mixed else "fp64"
+    line["value"] = head["value"]
+    line["ms_per_step"] = head["ms"] / args.steps
+    line["dtype"] = "f64 with int8 digit products (mixed)" if use_mixed else "f64"
+    line["e2e"] = {"value": head["e2e_value"], "unit": UNIT, "h2d_bytes_per_step": head["h2d"],
+                   "d2h_bytes_per_step": head["d2h"]}
+    line["gpu_launches"] = int(head["launches"])
+    line["roofline"] = roof
+    line["roofline_fp64_path"] = roof_fp64
+    line["kernels_ms_per_step"] = {k: v[0] for k, v in head["kt"].items() if v[1] > 0}
+    total_k = sum(v for v in line["kernels_ms_per_step"].values())
+    line["kernel_share"] = {k: v / total_k for k, v in line["kernels_ms_per_step"].items()}
+    line["clocks"] = head["clocks"]
+    if world == 1 and not args.no_projection:
+        line["projection_tc"] = projection_large_droplets(torch, scale=args.scale)
+    if world == 1 and not args.no_layered:
+        line["layered_adjoint"] = layered_adjoint_leg(torch, scale=args.scale)
+    if world == 1 and not args.no_spheroids:
+        line["spheroids"] = spheroid_leg(torch, roof_fp64["peak"], scale=args.scale)
+    print(json.dumps(line), flush=True)
+
+
+def form_summary(f, w):
+    return {"value": f["value"], "ms_per_step": f["ms"] / max(f["steps"], 1),
+            "e2e": f["e2e_value"], "gpu_launches": int(f["launches"]),
+            "kernels_ms_per_step": {k: v[0] for k, v in f["kt"].items() if v[1] > 0},
+            "clocks": f["clocks"]}
+
+
+def run_form(args, w, i8_above, bufs, wl_d, m_d, stream, flush, barrier, world, dev, local):
+    """One form of the hot path (plain FP64: i8_above 0; mixed): W warm-up steps, K steps on
+    device-resident inputs timed with CUDA events on the launching stream (L2 flushed before
+    each), K e2e steps through the host entry point with pinned buffers, and the kernel times of
+    one profiled step."""
+    import ctypes
+
+    import torch
+
+    from scatrs_b200 import _native
+
+    values_d, phase_d, greek_d = bufs
+    n = w.n_units
+
+    def step():
+        _native.ensemble_fixed_device(w.dists, wl_d.data_ptr(), w.wavelengths.size,
+                                      m_d.data_ptr(), w.mu, w.n_nodes, w.greek_order, True,
+                                      values_d.data_ptr(), phase_d.data_ptr(),
+                                      greek_d.data_ptr(), stream.cuda_stream,
+                                      i8_above=i8_above, levels=args.i8_levels)
 
     for _ in range(args.warmup):
         step()
@@ -629,17 +843,24 @@ def ours(args):
     v_h = torch.empty(11 * n, dtype=torch.float64).pin_memory()
     p_h = torch.empty(6 * n * w.mu.size, dtype=torch.float64).pin_memory()
     g_h = torch.empty(6 * n * (w.greek_order + 1), dtype=torch.float64).pin_memory()
-    import ctypes
-
     opts = _native.FixedOptions(w.n_nodes, w.greek_order, 1, 0)
     err = ctypes.create_string_buffer(1024)
     mu = np.ascontiguousarray(w.mu)
     pd = lambda t: ctypes.cast(t.data_ptr(), _native._PD)  # noqa: E731
+    lib = _native.load()
+    mixed_opts = _native.MixedOptions(int(i8_above), int(args.i8_levels))
 
     def e2e_step():
-        st = _native.load().scatrs_ensemble_fixed(
-            w.dists.ctypes.data, w.dists.size, pd(wl_h), w.wavelengths.size, pd(m_h),
-            _native._p(mu), mu.size, ctypes.byref(opts), pd(v_h), pd(p_h), pd(g_h), err, 1024)
+        if i8_above > 0:
+            st = lib.scatrs_ensemble_fixed_mixed(
+                w.dists.ctypes.data, w.dists.size, pd(wl_h), w.wavelengths.size, pd(m_h),
+                _native._p(mu), mu.size, ctypes.byref(opts), ctypes.byref(mixed_opts), pd(v_h),
+                pd(p_h), pd(g_h), err, 1024)
+        else:
+            st = lib.scatrs_ensemble_fixed(
+                w.dists.ctypes.data, w.dists.size, pd(wl_h), w.wavelengths.size, pd(m_h),
+                _native._p(mu), mu.size, ctypes.byref(opts), pd(v_h), pd(p_h), pd(g_h), err,
+                1024)
         _native._check(st, err)
 
     e2e_step()
@@ -653,68 +874,15 @@ def ours(args):
     h2d = 8 * w.wavelengths.size + 16 * n + 16 * w.dists.size * w.n_nodes
     d2h = 8 * (11 * n + 6 * n * w.mu.size + 6 * n * (w.greek_order + 1)) + 4 * n * (
         (w.n_nodes + 31) // 32)
-
+    del v_h, p_h, g_h
     # Kernel times of one profiled step (events around each launch on its stream).
     _native.set_profiling(True)
     step()
     kt = _native.kernel_times()
     _native.set_profiling(False)
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.barrier()
-        dist.destroy_process_group()
-    if rank != 0:
-        return
-    peaks = {}
-    try:
-        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
-            peaks = json.load(f)
-    except OSError:
-        pass
-    fp64 = fp64_peak_tflops(torch)
-    user_rows = int(np.unique(np.abs(w.mu)).size)
-    flops = algorithmic_flops(w, user_rows)
-    unit_ms, unit_n = kt["unit_kernel"]
-    mie_ms, mie_n = kt["mie_fixed_kernel"]
-    achieved = flops / (unit_ms * 1e-3) / 1e12
-    total_k = sum(v[0] for v in kt.values())
-    line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-        "config": workload_config(w, args),
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(d2h)},
-        "gpu_launches": int(launches),
-        "roofline": {"bound": "fp64", "kernel": "unit_kernel (K-b/c/d)", "achieved": achieved,
-                     "peak": fp64, "unit": "TFLOP/s", "frac": achieved / fp64,
-                     "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (the measured "
-                                    "peaks file has no FP64 entry)",
-                     "traffic": UNIT_DRAM_BYTES_PER_NODE * w.n_nodes_total / max(unit_n, 1),
-                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
-                                       "launch on the 0.1-scale workload, scaled by nodes per "
-                                       "launch",
-                     "launches": unit_n, "avg_launch_ms": unit_ms / max(unit_n, 1),
-                     "algorithmic_flop_per_step": flops},
-        "kernels_ms_per_step": {k: v[0] for k, v in kt.items()},
-        "kernel_share": {k: (v[0] / total_k if total_k else None) for k, v in kt.items()},
-        "hbm_peak_gbs": peaks.get("hbm_gbs"),
-    }
-    line["clocks"] = clk.summary()
-    if world == 1 and not args.no_projection:
-        line["projection_tc"] = projection_large_droplets(torch, scale=args.scale)
-    if world == 1 and not args.no_layered:
-        line["layered_adjoint"] = layered_adjoint_leg(torch, scale=args.scale)
-    if world == 1 and not args.no_spheroids:
-        line["spheroids"] = spheroid_leg(torch, line["roofline"]["peak"], scale=args.scale)
-    if world == 1 and not args.no_cpu_baseline:
-        ow = oracle_view(w)
-        forced, n_max = largest_units(ow, 8)
-        base, kept = cpu_sample(ow, args.cpu_seconds, forced=forced, keep=True)
-        line["cpu_baseline"] = base
-        line["parity"] = parity_leg(kept, values_d, phase_d, greek_d, n, w, forced, n_max)
-    print(json.dumps(line), flush=True)
+    return {"value": value, "ms": ms, "steps": args.steps, "e2e_value": e2e_value,
+            "h2d": int(h2d), "d2h": int(d2h), "launches": launches, "kt": kt,
+            "clocks": clk.summary()}
 
 
 def parity_leg(kept, values_d, phase_d, greek_d, n, w, forced, n_max, tol=1e-12):

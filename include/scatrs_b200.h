@@ -417,6 +417,43 @@ int scatrs_ensemble_fixed_device(const scatrs_distribution* dists_host, int64_t 
                                  double* phase_dev, double* greek_dev, void* stream, char* err,
                                  size_t err_len);
 
+/* Options of the mixed form: chunks with i8_above < N_c <= 4096 take the int8 path (i8_above
+ * <= 0: none); levels, the product levels kept (i + j < levels): 5 (15 digit products), 6 (19),
+ * or 0 for 5. */
+typedef struct scatrs_mixed_options {
+  int32_t i8_above;
+  int32_t levels;
+} scatrs_mixed_options;
+
+/*
+ * The mixed form of scatrs_ensemble_fixed / scatrs_ensemble_fixed_device (values; homogeneous
+ * spheres): the angle GEMMs that replace the reference's FP64 band products
+ * (PanelProducts::multiply, scatrs/src/ensemble/fast.rs:141-145) run, for every chunk of 32
+ * nodes whose largest number of terms N_c satisfies i8_above < N_c <= 4096, as exact integer
+ * products on the tensor cores: each table row and each coefficient column is a 40-bit
+ * fixed-point integer with its own power-of-two scale, split into five balanced signed bytes,
+ * and the digit products of the leading levels (i + j < levels) are summed exactly in INT32
+ * (tcgen05.mma kind::i8); every product term keeps about 2^-38 (5 levels) of its row's largest
+ * |table| value times its column's largest |coefficient|, the dropped terms centred on zero.
+ * The Mie coefficients, the elements, the weighted sums, the projection and the outputs are
+ * FP64 as in the plain form; chunks at or below i8_above run the plain FP64 path. mixed NULL or
+ * i8_above <= 0 is the plain form exactly. This form has no counterpart in the reference, whose
+ * band products are FP64 GEMMs.
+ */
+int scatrs_ensemble_fixed_mixed(const scatrs_distribution* dists, int64_t n_dist,
+                                const double* wavelengths, int64_t n_wl, const double* m,
+                                const double* mu, int64_t n_mu,
+                                const scatrs_fixed_options* options,
+                                const scatrs_mixed_options* mixed, double* values,
+                                double* phase, double* greek, char* err, size_t err_len);
+int scatrs_ensemble_fixed_mixed_device(const scatrs_distribution* dists_host, int64_t n_dist,
+                                       const double* wavelengths_dev, int64_t n_wl,
+                                       const double* m_dev, const double* mu_host, int64_t n_mu,
+                                       const scatrs_fixed_options* options,
+                                       const scatrs_mixed_options* mixed, double* values_dev,
+                                       double* phase_dev, double* greek_dev, void* stream,
+                                       char* err, size_t err_len);
+
 /* Synchronizes `stream` and returns the first device-side input error of the last
  * scatrs_ensemble_fixed_device call on it (in wavelength, distribution, radius order). */
 int scatrs_check_errors(void* stream, char* err, size_t err_len);

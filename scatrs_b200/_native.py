@@ -88,6 +88,10 @@ class FixedOptions(ctypes.Structure):
                 ("allow_unvalidated", _I32)]
 
 
+class MixedOptions(ctypes.Structure):
+    _fields_ = [("i8_above", _I32), ("levels", _I32)]
+
+
 # Every symbol the header declares, with (restype, argtypes).
 SYMBOLS = {
     "scatrs_ensemble_fixed_sizes": (None, [_I64, _I64, _I32, _PI64, _PI64, _PI64]),
@@ -106,6 +110,14 @@ SYMBOLS = {
     "scatrs_ensemble_fixed_device": (ctypes.c_int, [_VP, _I64, _VP, _I64, _VP, _PD, _I64,
                                                     ctypes.POINTER(FixedOptions), _VP, _VP, _VP,
                                                     _VP, _CP, _SZ]),
+    "scatrs_ensemble_fixed_mixed": (ctypes.c_int, [_VP, _I64, _PD, _I64, _PD, _PD, _I64,
+                                                   ctypes.POINTER(FixedOptions),
+                                                   ctypes.POINTER(MixedOptions), _PD, _PD, _PD,
+                                                   _CP, _SZ]),
+    "scatrs_ensemble_fixed_mixed_device": (ctypes.c_int, [_VP, _I64, _VP, _I64, _VP, _PD, _I64,
+                                                          ctypes.POINTER(FixedOptions),
+                                                          ctypes.POINTER(MixedOptions), _VP, _VP,
+                                                          _VP, _VP, _CP, _SZ]),
     "scatrs_ensemble_adaptive": (ctypes.c_int, [_VP, _I64, _I32, _PD, _I64, _PD, _PD, _I64,
                                                 ctypes.POINTER(AdaptiveOptions), _PD, _PD, _PD,
                                                 _PD, _PD, _PD, _VP, _VP, _CP, _SZ]),
@@ -156,7 +168,7 @@ SYMBOLS = {
 
 KERNEL_NAMES = ("plan_chunks_kernel", "mie_fixed_kernel", "unit_kernel", "mie_nodes_kernel",
                 "final_kernel", "proj_kernel", "tm_tables_kernels", "tm_surface_kernel",
-                "tm_solve_kernel", "ro_kernels")
+                "tm_solve_kernel", "ro_kernels", "unit_i8_kernel", "x_split_kernel")
 # The kernels each id covers: K-a also as mie_layered_kernel / mie_deriv_kernel, the unit kernel
 # as unit_deriv_kernel, the final kernel as final_deriv_kernel.
 
@@ -269,9 +281,13 @@ def mie(x, m, allow_unvalidated: bool = False):
 
 
 def ensemble_fixed(dists: np.ndarray, wavelengths, m, mu, n_nodes: int, greek_order: int = -1,
-                   normalized: bool = True, allow_unvalidated: bool = False):
+                   normalized: bool = True, allow_unvalidated: bool = False, i8_above: int = 0,
+                   levels: int = 0):
     """The fixed-grid ensemble from host arrays; returns (values, phase or None, greek or None)
-    shaped (11, n), (6, n, n_mu), (6, n, L + 1) with n = n_dist * n_wl, distribution-major."""
+    shaped (11, n), (6, n, n_mu), (6, n, L + 1) with n = n_dist * n_wl, distribution-major.
+    i8_above > 0: the mixed form (scatrs_ensemble_fixed_mixed), the angle GEMMs of the chunks
+    with more terms than i8_above as exact int8 digit products on the tensor cores, keeping
+    `levels` product levels (0: the library's default)."""
     require_device()
     dists = np.ascontiguousarray(dists, dtype=DIST_DTYPE)
     wl = np.ascontiguousarray(wavelengths, dtype=np.float64).reshape(-1)
@@ -284,10 +300,18 @@ def ensemble_fixed(dists: np.ndarray, wavelengths, m, mu, n_nodes: int, greek_or
     phase = np.zeros((6, n, mu.size)) if mu.size else None
     greek = np.zeros((6, n, greek_order + 1)) if greek_order >= 0 else None
     err = ctypes.create_string_buffer(1024)
-    st = load().scatrs_ensemble_fixed(dists.ctypes.data, dists.size, _p(wl), wl.size,
-                                      _p(m.view(np.float64)), _p(mu), mu.size,
-                                      ctypes.byref(opts), _p(values), _p(phase), _p(greek), err,
-                                      1024)
+    if i8_above > 0:
+        st = load().scatrs_ensemble_fixed_mixed(dists.ctypes.data, dists.size, _p(wl), wl.size,
+                                                _p(m.view(np.float64)), _p(mu), mu.size,
+                                                ctypes.byref(opts),
+                                                ctypes.byref(MixedOptions(int(i8_above),
+                                                                          int(levels))),
+                                                _p(values), _p(phase), _p(greek), err, 1024)
+    else:
+        st = load().scatrs_ensemble_fixed(dists.ctypes.data, dists.size, _p(wl), wl.size,
+                                          _p(m.view(np.float64)), _p(mu), mu.size,
+                                          ctypes.byref(opts), _p(values), _p(phase), _p(greek),
+                                          err, 1024)
     _check(st, err)
     return values, phase, greek
 
@@ -669,17 +693,25 @@ def ensemble_fixed_layered_d(dists: np.ndarray, wavelengths, fractions, m_layers
 
 def ensemble_fixed_device(dists: np.ndarray, wl_ptr: int, n_wl: int, m_ptr: int, mu, n_nodes: int,
                           greek_order: int, normalized: bool, values_ptr: int, phase_ptr: int,
-                          greek_ptr: int, stream: int = 0, allow_unvalidated: bool = False):
+                          greek_ptr: int, stream: int = 0, allow_unvalidated: bool = False,
+                          i8_above: int = 0, levels: int = 0):
     """The fixed-grid ensemble on device arrays (raw pointers, e.g. torch's data_ptr()),
-    enqueued on `stream`; device-side input errors surface in check_errors(stream)."""
+    enqueued on `stream`; device-side input errors surface in check_errors(stream).
+    i8_above > 0: the mixed form (scatrs_ensemble_fixed_mixed_device)."""
     dists = np.ascontiguousarray(dists, dtype=DIST_DTYPE)
     mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
     opts = FixedOptions(int(n_nodes), int(greek_order), int(normalized), int(allow_unvalidated))
     err = ctypes.create_string_buffer(1024)
-    st = load().scatrs_ensemble_fixed_device(dists.ctypes.data, dists.size, wl_ptr, n_wl, m_ptr,
-                                             _p(mu), mu.size, ctypes.byref(opts), values_ptr,
-                                             phase_ptr or None, greek_ptr or None, stream or None,
-                                             err, 1024)
+    if i8_above > 0:
+        st = load().scatrs_ensemble_fixed_mixed_device(
+            dists.ctypes.data, dists.size, wl_ptr, n_wl, m_ptr, _p(mu), mu.size,
+            ctypes.byref(opts), ctypes.byref(MixedOptions(int(i8_above), int(levels))),
+            values_ptr, phase_ptr or None, greek_ptr or None, stream or None, err, 1024)
+    else:
+        st = load().scatrs_ensemble_fixed_device(dists.ctypes.data, dists.size, wl_ptr, n_wl,
+                                                 m_ptr, _p(mu), mu.size, ctypes.byref(opts),
+                                                 values_ptr, phase_ptr or None,
+                                                 greek_ptr or None, stream or None, err, 1024)
     _check(st, err)
 
 

@@ -328,8 +328,9 @@ def _compute_with_derivatives(items, wavelengths, mixture, greek, all_orders, mu
     for i in chosen:
         if records[i][2] is None:
             raise InvalidInputError(
-                f"the derivative along {names[i]} (a layered sphere's or a spheroid's) is not "
-                "on the adaptive GPU path: use the fixed grid")
+                f"the derivative along {names[i]} is not on the adaptive GPU path: a layered "
+                "sphere's derivatives are on the fixed grid (ensemble_compute_fixed), a "
+                "spheroid's are not built")
     wl = np.ascontiguousarray(wavelengths, dtype=np.float64).reshape(-1)
     mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
     L = _greek_order(greek, all_orders)
@@ -393,8 +394,9 @@ def ensemble_compute_fixed(specs, particle_spec, wavelengths, greek, all_orders,
                            ranges=None, derivatives=(), tmatrix_rtol: float = 1e-8) -> dict:
     """The batch dict on a fixed grid. ``derivatives`` selects parameters by their index in
     ``ensemble_parameters([(specs[0], particle_spec, 1.0)], False)`` (the reference's
-    ``deriv_idx``); they need homogeneous spheres and every distribution of one kind. Spheroids
-    (``('spheroid', aspect_ratio, m)``) converge every node's T-matrix to ``tmatrix_rtol``."""
+    ``deriv_idx``): homogeneous or layered spheres, every distribution of one kind. Spheroids
+    (``('spheroid', aspect_ratio, m)``) converge every node's T-matrix to ``tmatrix_rtol``; their
+    derivatives are not built."""
     if not isinstance(particle_spec, tuple) or particle_spec[0] not in ("sphere", "layered",
                                                                          "spheroid"):
         raise TypeError("the fixed-grid ensemble takes ('sphere', m), ('layered', fractions, m) "
@@ -409,7 +411,7 @@ def ensemble_compute_fixed(specs, particle_spec, wavelengths, greek, all_orders,
     d = dp = dg = None
     if particle_spec[0] == "spheroid":
         if derivatives:
-            raise InvalidInputError("derivatives of spheroids are not on the fixed grid")
+            raise InvalidInputError("a spheroid's derivatives are not built on the GPU path")
         m = np.asarray(particle_spec[2], dtype=np.complex128)
         if m.ndim == 1:
             m = np.broadcast_to(m, (dists.size, wl.size))
@@ -417,16 +419,29 @@ def ensemble_compute_fixed(specs, particle_spec, wavelengths, greek, all_orders,
             dists, wl, float(particle_spec[1]), m, mu, n_nodes, L, bool(normalized),
             tmatrix_rtol=tmatrix_rtol)
     elif particle_spec[0] == "layered":
-        if derivatives:
-            raise InvalidInputError("derivatives of layered spheres are not on the fixed grid")
-        fr = np.asarray(particle_spec[1], dtype=np.float64).reshape(-1)
         ml = np.asarray(particle_spec[2], dtype=np.complex128)
+        fr = np.asarray(particle_spec[1], dtype=np.float64)
         if ml.ndim == 2:  # (L, n_wl): the same particle for every distribution
+            fr = fr.reshape(-1)
             ml = np.broadcast_to(ml, (dists.size,) + ml.shape)
             fr = np.broadcast_to(fr, (dists.size, fr.size))
-        values, phase, g = _native.ensemble_fixed_layered(dists, wl, fr, ml, mu, n_nodes, L,
-                                                          bool(normalized),
-                                                          bool(allow_unvalidated))
+        else:
+            fr = fr.reshape(dists.size, -1)
+        if derivatives:
+            # The derivative blocks come in ensemble_parameters' order: the distribution's
+            # parameters, each layer's Re m and Im m, each radius fraction.
+            names = ensemble_parameters([(specs[0], ("layered", fr[0], ml[0]), 1.0)], False)
+            for k in derivatives:
+                if not 0 <= k < len(names):
+                    raise InvalidInputError(f"derivative index {k} out of range of {names}")
+            values, phase, g, d, dp, dg = _native.ensemble_fixed_layered_d(
+                dists, wl, fr, ml, mu, n_nodes, L, bool(normalized), bool(allow_unvalidated))
+            d, dp, dg = (None if a is None else np.ascontiguousarray(a[derivatives])
+                         for a in (d, dp, dg))
+        else:
+            values, phase, g = _native.ensemble_fixed_layered(dists, wl, fr, ml, mu, n_nodes, L,
+                                                              bool(normalized),
+                                                              bool(allow_unvalidated))
     else:
         m = np.asarray(particle_spec[1], dtype=np.complex128)
         if m.ndim == 1:

@@ -47,7 +47,9 @@ enum KernelId {
   K_TM_SURFACE = 7,  // tm_surface_kernel
   K_TM_SOLVE = 8,    // tm_solve_kernel
   K_RANDOM = 9,      // the orientation average's five kernels
-  K_COUNT = 10
+  K_UNITS_I8 = 10,   // unit_i8_kernel (the mixed form's int8 angle GEMMs)
+  K_X_SPLIT = 11,    // x_split_kernel (the int8 chunks' digits)
+  K_COUNT = 12
 };
 static bool g_profiling = false;
 // The spheroid surface integrals' work per tm_surface_kernel launch while profiling: the sum
@@ -161,6 +163,7 @@ struct DevBuf {
 // orders 1..ld.
 struct UserTables {
   std::vector<double> mu;
+  std::vector<double> rows;  // each table row's cosine (a cosine, or a pair c, -c)
   int64_t n_orders = 0;
   int h = 0, h_pad = 0, ld = 0;
   DevBuf ge, go, map;
@@ -196,6 +199,16 @@ struct Context {
   };
   std::map<std::pair<int64_t, int>, Projector> projectors;
   DevBuf tc_a_hi, tc_a_lo, tc_prod, tc_err;
+  // The mixed form: digit tables (I8Tables) and the slabs' chunk digits.
+  struct I8Tables {
+    std::vector<double> mu;
+    int64_t user_orders = 0;
+    int order = -2;
+    int n_bands = 0;
+    std::vector<I8Table> user, band;
+    DevBuf dig, scale, user_d, band_d;
+  } i8;
+  DevBuf xdig, xscale, chunk_xoff, chunk_xidx, i8_list, i8_err;
   // Spheroid T-matrices.
   DevBuf tm_geoms, tm_jobs, tm_rules, tm_node, tm_rad, tm_ang, tm_J, tm_work, tm_piv, tm_T, tm_sums,
       tm_err;
@@ -319,6 +332,7 @@ void ensure_user(Context& c, const double* mu, int64_t n_mu, int64_t n_orders, c
     map.push_back(make_int2(j, partner));
   }
   u.h = (int)cosines.size();
+  u.rows = cosines;
   u.h_pad = (int)round_up(std::max(u.h, 1), 32);
   u.ld = (int)u.n_orders;
   // Order-major (transposed) tables: element (row, order k) at k * h_pad + row, so that one
@@ -401,6 +415,120 @@ BandTables& ensure_bands(Context& c, int L, int last_band, cudaStream_t s) {
   return bt;
 }
 
+// The digits of one table of the mixed form (kernels.h): pairs [0, h) whose E and O rows over
+// orders 0 .. n_orders - 1 row(pair, e, o) writes (zero beyond), in M tiles of kI8Pairs pairs
+// (E rows, then the same pairs' O rows) and n_kb K blocks; each MMA row's power of two 2^e puts
+// its largest |value| below 127 2^-e (in [63.5, 127) 2^-e), and F = rint(value 2^(e + 32))
+// goes out as its five balanced digits (each in [-128, 127]: the low ones the sign-extended low
+// byte of what is left) into the 64-byte swizzle (16-byte chunk q of row r at chunk
+// q ^ ((r >> 1) & 3)). The scale written per row is 2^-e (0 for a zero row).
+template <class Row>
+I8Table i8_table(int h, int64_t n_orders, int n_kb, Row row, std::vector<unsigned char>& dig,
+                 std::vector<double>& scale) {
+  I8Table t;
+  t.off = (int64_t)dig.size();
+  t.scale_off = (int64_t)scale.size();
+  t.n_kb = n_kb;
+  t.n_tiles = (h + kI8Pairs - 1) / kI8Pairs;
+  const int64_t K = (int64_t)n_kb * kI8KB;
+  dig.resize(dig.size() + (size_t)t.n_tiles * n_kb * kI8TileBytes, 0);
+  scale.resize(scale.size() + (size_t)t.n_tiles * 128, 0.0);
+  std::vector<double> e_row(K), o_row(K);
+  for (int tile = 0; tile < t.n_tiles; ++tile) {
+    for (int pp = 0; pp < kI8Pairs; ++pp) {
+      const int pair = tile * kI8Pairs + pp;
+      if (pair >= h) break;
+      std::fill(e_row.begin(), e_row.end(), 0.0);
+      std::fill(o_row.begin(), o_row.end(), 0.0);
+      row(pair, std::min<int64_t>(n_orders, K), e_row.data(), o_row.data());
+      for (int side = 0; side < 2; ++side) {
+        const std::vector<double>& v = side ? o_row : e_row;
+        const int r = side * kI8Pairs + pp;
+        double m = 0.0;
+        for (int64_t k = 0; k < K; ++k) m = std::max(m, std::fabs(v[k]));
+        if (!(m > 0.0)) continue;
+        int ex = 0;
+        std::frexp(m, &ex);
+        int e = 7 - ex;
+        if (std::ldexp(m, e) >= 127.0) --e;
+        scale[t.scale_off + (size_t)tile * 128 + r] = std::ldexp(1.0, -e);
+        for (int64_t k = 0; k < K; ++k) {
+          long long f = std::llrint(std::ldexp(v[k], e + 32));
+          const int kb = (int)(k / kI8KB), kk = (int)(k % kI8KB);
+          const int q = kk / 16, b = kk % 16, qs = q ^ ((r >> 1) & 3);
+          const size_t at = (size_t)t.off + ((size_t)(tile * n_kb + kb) * kI8Levels) * 8192 +
+                            (size_t)r * kI8KB + qs * 16 + b;
+          int d[kI8Levels];
+          for (int s2 = kI8Levels - 1; s2 > 0; --s2) {
+            d[s2] = (int)(signed char)(f & 0xff);
+            f = (f - d[s2]) >> 8;
+          }
+          d[0] = (int)f;
+          for (int s2 = 0; s2 < kI8Levels; ++s2)
+            dig[at + (size_t)s2 * 8192] = (unsigned char)(d[s2] & 0xff);
+        }
+      }
+    }
+  }
+  return t;
+}
+
+// The mixed form's digit tables for the requested cosines (versions v = 0, 1, ... covering
+// orders < 64 2^v up to n_max, each row scaled over its version's orders, so that a chunk's
+// rows keep their bits relative to the orders it uses) and for bands 0 .. n_bands - 1 of Greek
+// order L (L < 0: none); cached per context until the cosines, the order or the reach change.
+void ensure_i8(Context& c, int64_t n_max, const BandTables* bt, cudaStream_t s) {
+  Context::I8Tables& T = c.i8;
+  const int L = bt ? bt->order : -1;
+  const int nb = bt ? bt->n_bands : 0;
+  int n_ver = 1;
+  while (((int64_t)kI8KB << (n_ver - 1)) < std::min<int64_t>(n_max, kI8MaxTerms)) ++n_ver;
+  if (T.mu == c.user.mu && T.user_orders >= ((int64_t)kI8KB << (n_ver - 1)) && T.order == L &&
+      T.n_bands >= nb)
+    return;
+  std::vector<unsigned char> dig;
+  std::vector<double> scale;
+  T.user.clear();
+  T.band.clear();
+  const int h_u = c.user.h;
+  const std::vector<double>& cosines = c.user.rows;
+  for (int v = 0; v < n_ver; ++v) {
+    const int n_kb = 1 << v;
+    const int64_t K = (int64_t)n_kb * kI8KB;
+    T.user.push_back(i8_table(
+        h_u, K, n_kb,
+        [&](int pair, int64_t n, double* e, double* o) { pi_tau_row(cosines[pair], n, e, o); },
+        dig, scale));
+  }
+  for (int b = 0; b < nb; ++b) {
+    const BandDesc& d = bt->desc[b];
+    const int n_kb = (d.upper + kI8KB - 1) / kI8KB;
+    T.band.push_back(i8_table(
+        d.h, d.upper, n_kb,
+        [&](int pair, int64_t n, double* e, double* o) {
+          for (int64_t k = 0; k < n; ++k) {
+            e[k] = bt->ge[d.g_off + (size_t)k * d.h_pad + pair];
+            o[k] = bt->go[d.g_off + (size_t)k * d.h_pad + pair];
+          }
+        },
+        dig, scale));
+  }
+  if (T.band.empty()) T.band.push_back(I8Table{});
+  SB_CUDA(cudaMemcpyAsync(T.dig.get(std::max<size_t>(dig.size(), 16)), dig.data(), dig.size(),
+                          cudaMemcpyHostToDevice, s));
+  SB_CUDA(cudaMemcpyAsync(T.scale.get(std::max<size_t>(scale.size(), 1) * 8), scale.data(),
+                          scale.size() * 8, cudaMemcpyHostToDevice, s));
+  SB_CUDA(cudaMemcpyAsync(T.user_d.get(T.user.size() * sizeof(I8Table)), T.user.data(),
+                          T.user.size() * sizeof(I8Table), cudaMemcpyHostToDevice, s));
+  SB_CUDA(cudaMemcpyAsync(T.band_d.get(T.band.size() * sizeof(I8Table)), T.band.data(),
+                          T.band.size() * sizeof(I8Table), cudaMemcpyHostToDevice, s));
+  SB_CUDA(cudaStreamSynchronize(s));
+  T.mu = c.user.mu;
+  T.user_orders = (int64_t)kI8KB << (n_ver - 1);
+  T.order = L;
+  T.n_bands = nb;
+}
+
 // A distribution's density at r: its closed form, or a tabulated one's interpolation.
 double node_density(const scatrs_distribution& d, double r) {
   return d.kind == kTabulated ? table_density(d.table, d.table_len, r)
@@ -447,6 +575,11 @@ struct FixedCall {
   double* h_values = nullptr;
   double* h_phase = nullptr;
   double* h_greek = nullptr;
+  // The mixed form (values of homogeneous spheres): chunks with i8_above < N_c <=
+  // kI8MaxTerms run their angle GEMMs on int8 digits (unit_i8_kernel); 0 for plain FP64.
+  int i8_above = 0;
+  int i8_levels = 5;           // product levels kept (5 or 6)
+  unsigned* i8_err = nullptr;  // the int8 kernel's timeout flag, checked with the errors
 };
 
 // The device pipeline; wl_dev and m_dev are device arrays, outputs device arrays.
@@ -623,6 +756,16 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
   ensure_user(c, mu, n_mu, n_max, s);
   BandTables* bt = nullptr;
   if (L >= 0) bt = &ensure_bands(c, L, band_index(n_max), s);
+  // The mixed form: values of the fixed grid only.
+  const int i8_above = (call && !ad.on && !dv.on) ? call->i8_above : 0;
+  auto on_i8 = [&](int nc) { return i8_above > 0 && nc > i8_above && nc <= kI8MaxTerms; };
+  unsigned* i8_err = nullptr;
+  if (i8_above > 0) {
+    ensure_i8(c, n_max, bt, s);
+    i8_err = c.i8_err.as<unsigned>(1);
+    SB_CUDA(cudaMemsetAsync(i8_err, 0, sizeof(unsigned), s));
+    call->i8_err = i8_err;
+  }
   // 3. Slabs. Each unit's work: its chunks' rows times the table rows they meet.
   const int nb = bt ? bt->n_bands : 0;
   std::vector<int> band_of_n(n_max + 1, -1), band_tiles(nb), band_nq(nb);
@@ -639,7 +782,7 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
   }
   const int t_user = (c.user.h + 31) / 32;
   const int64_t acc_head = 4 * n_mu * n_blk;
-  std::vector<int64_t> urows(n_units), uacc(n_units);
+  std::vector<int64_t> urows(n_units), uacc(n_units), ui8(n_units, 0), ui8n(n_units, 0);
   std::vector<int> uslots(n_units), utiles(n_units);
   std::vector<double> ucost(n_units);
   int64_t total_rows = 0;
@@ -652,6 +795,10 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
     for (int k = 0; k < cpu; ++k) {
       const int nc = cu[k];
       rows += (int64_t)rows_per_term * nc;
+      if (on_i8(nc)) {
+        ui8[u] += 2 * (int64_t)((nc + kI8KB - 1) / kI8KB) * kI8HalfBytes;
+        ui8n[u] += 1;
+      }
       int tiles = t_user;
       if (bt && nc > 0) {
         const int b = band_of_n[nc];
@@ -719,6 +866,7 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
     int64_t it0 = 0, n_items = 0;
     int64_t acc_len = 0;
     int64_t n_proj = 0;
+    int64_t i8_bytes = 0, i8_chunks = 0;  // the mixed form's chunk digits
   };
   std::vector<Slab> slabs(n_slabs);
   std::vector<int> members(n_units);
@@ -730,6 +878,8 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
       S.n_slots += uslots[u];
       S.n_items += ugroups[u];
       S.acc_len += uacc[u];
+      S.i8_bytes += ui8[u];
+      S.i8_chunks += ui8n[u];
     }
     int64_t u0 = 0, sl0 = 0, pi0 = 0, it0 = 0;
     for (int64_t sl = 0; sl < n_slabs; ++sl) {
@@ -754,12 +904,13 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
     }
   }
   int64_t acc_max = 1, slots_max = 1, stage_max = 0, n_slots_all = 0, n_proj_all = 0,
-          n_items_all = 0;
+          n_items_all = 0, i8_bytes_max = 16, i8_chunks_max = 1;
   auto stage_bytes = [&](const Slab& S) {
     return S.nu * (int64_t)(sizeof(int) + 8 + sizeof(int2)) +
            S.nu * cpu * (int64_t)(sizeof(int) + 16) +
            S.n_slots * (int64_t)(sizeof(BandSlot) + sizeof(int)) +
-           S.pi_cap * (int64_t)sizeof(ProjItem) + S.n_items * (int64_t)sizeof(WorkItem) + 256;
+           S.pi_cap * (int64_t)sizeof(ProjItem) + S.n_items * (int64_t)sizeof(WorkItem) +
+           (i8_above > 0 ? S.nu * cpu * (int64_t)(8 + 2 * sizeof(int)) + 64 : 0) + 256;
   };
   for (const Slab& S : slabs) {
     acc_max = std::max(acc_max, S.acc_len);
@@ -768,6 +919,8 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
     n_slots_all += S.n_slots;
     n_proj_all += S.pi_cap;
     n_items_all += S.n_items;
+    i8_bytes_max = std::max(i8_bytes_max, S.i8_bytes);
+    i8_chunks_max = std::max(i8_chunks_max, S.i8_chunks);
   }
   // Device buffers: the plan's flat arrays (every slab its own segment), arena, scratch, sums.
   int* units_d = c.plan_units.as<int>(n_units);
@@ -792,6 +945,18 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
   double* slot_greek =
       L >= 0 ? c.slot_greek.as<double>((size_t)slots_max * 6 * (L + 1)) : nullptr;
   int* counter = c.counter.as<int>(64);
+  int64_t* chunk_xoff_d = nullptr;
+  int* chunk_xidx_d = nullptr;
+  int* i8_list_d = nullptr;
+  unsigned char* xdig = nullptr;
+  double* xscale = nullptr;
+  if (i8_above > 0) {
+    chunk_xoff_d = c.chunk_xoff.as<int64_t>(n_chunks);
+    chunk_xidx_d = c.chunk_xidx.as<int>(n_chunks);
+    i8_list_d = c.i8_list.as<int>(n_chunks);
+    xdig = c.xdig.as<unsigned char>((size_t)i8_bytes_max);
+    xscale = c.xscale.as<double>((size_t)i8_chunks_max * 128);
+  }
   c.ensure_staging((size_t)stage_max);
   // 4. Per slab: build its plan into pinned staging, upload it, launch its kernels. The host
   // builds the next slab while the device runs this one.
@@ -855,6 +1020,7 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
   ua.per_unit = ka.per_unit;
   ua.wdiff = ka.wdiff;
   ua.wthdiff = ka.wthdiff;
+  ua.i8_above = i8_above;
   ProjArgs pj{};
   pj.cpu = cpu;
   pj.greek_order = L;
@@ -927,6 +1093,11 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
     int* P_sidx = (int*)take(S.n_slots * sizeof(int));
     ProjItem* P_proj = (ProjItem*)take(S.pi_cap * sizeof(ProjItem));
     WorkItem* P_items = (WorkItem*)take(S.n_items * sizeof(WorkItem));
+    int64_t* P_xoff = i8_above > 0 ? (int64_t*)take(nch * 8) : nullptr;
+    int* P_xidx = i8_above > 0 ? (int*)take(nch * sizeof(int)) : nullptr;
+    int* P_list = i8_above > 0 ? (int*)take(nch * sizeof(int)) : nullptr;
+    int64_t xoff = 0;
+    int n_i8 = 0;
     const size_t used = (size_t)(base - c.staging_half(sl & 1));
     int64_t row = 0, accpos = 0, nslot = 0;
     order.clear();
@@ -942,6 +1113,16 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
         const int nc = cn[(int64_t)u * cpu + k];
         P_cn[ci] = nc;
         P_row[ci] = row;
+        if (P_xoff) {
+          P_xoff[ci] = -1;
+          P_xidx[ci] = 0;
+          if (on_i8(nc)) {
+            P_xoff[ci] = xoff;
+            P_xidx[ci] = n_i8;
+            P_list[n_i8++] = (int)ci;
+            xoff += 2 * (int64_t)((nc + kI8KB - 1) / kI8KB) * kI8HalfBytes;
+          }
+        }
         row += (int64_t)rows_per_term * nc;
         P_cacc[ci] = -1;
         if (bt && nc > 0) {
@@ -1029,6 +1210,14 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
                               cudaMemcpyHostToDevice, s));
     SB_CUDA(cudaMemcpyAsync(items_d + S.it0, P_items, S.n_items * sizeof(WorkItem),
                             cudaMemcpyHostToDevice, s));
+    if (i8_above > 0) {
+      SB_CUDA(cudaMemcpyAsync(chunk_xoff_d + ch0, P_xoff, nch * 8, cudaMemcpyHostToDevice, s));
+      SB_CUDA(cudaMemcpyAsync(chunk_xidx_d + ch0, P_xidx, nch * sizeof(int),
+                              cudaMemcpyHostToDevice, s));
+      if (n_i8 > 0)
+        SB_CUDA(cudaMemcpyAsync(i8_list_d + ch0, P_list, n_i8 * sizeof(int),
+                                cudaMemcpyHostToDevice, s));
+    }
     c.staging_uploaded(sl & 1, s);
     // Launches.
     ka.units = units_d + S.u0;
@@ -1049,6 +1238,56 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
     const int grid = (int)std::min<int64_t>(grid_max, S.n_items);
     timed_launch(K_UNITS, s, [&] { launch_units(ua, grid, s); });
     SB_CUDA(cudaGetLastError());
+    if (i8_above > 0 && n_i8 > 0) {
+      // The mixed form: the int8 chunks' digits, then their angle GEMMs on the tensor cores.
+      XSplitArgs xa{};
+      xa.X = X;
+      xa.chunk_row = ua.chunk_row;
+      xa.chunk_n = ua.chunk_n;
+      xa.list = i8_list_d + ch0;
+      xa.n = n_i8;
+      xa.chunk_xoff = chunk_xoff_d + ch0;
+      xa.chunk_xidx = chunk_xidx_d + ch0;
+      xa.xdig = xdig;
+      xa.xscale = xscale;
+      timed_launch(K_X_SPLIT, s, [&] { launch_x_split(xa, s); });
+      SB_CUDA(cudaGetLastError());
+      UnitI8Args ia{};
+      ia.radius = ua.radius;
+      ia.weight = ua.weight;
+      ia.wl = wl_dev;
+      ia.n_dist = (int)n_dist;
+      ia.n_wl = (int)n_wl;
+      ia.n_nodes = (int)n_nodes;
+      ia.cpu = cpu;
+      ia.units = ua.units;
+      ia.n_items = ua.n_items;
+      ia.items = ua.items;
+      ia.chunk_n = ua.chunk_n;
+      ia.chunk_acc = ua.chunk_acc;
+      ia.unit_acc = ua.unit_acc;
+      ia.n_mu = (int)n_mu;
+      ia.h_u = c.user.h;
+      ia.user_map = ua.user_map;
+      ia.greek_order = L;
+      ia.bands = ua.bands;
+      ia.acc = acc;
+      ia.chunk_xoff = xa.chunk_xoff;
+      ia.chunk_xidx = xa.chunk_xidx;
+      ia.xdig = xdig;
+      ia.xscale = xscale;
+      ia.tdig = c.i8.dig.as<unsigned char>(0);
+      ia.tscale = c.i8.scale.as<double>(0);
+      ia.user_tabs = c.i8.user_d.as<I8Table>(0);
+      ia.n_user_tabs = (int)c.i8.user.size();
+      ia.band_tabs = c.i8.band_d.as<I8Table>(0);
+      ia.levels = call->i8_levels;
+      ia.err = i8_err;
+      const int grid8 = (int)std::min<int64_t>(c.sms, S.n_items);
+      cudaError_t le = cudaSuccess;
+      timed_launch(K_UNITS_I8, s, [&] { le = launch_units_i8(ia, grid8, s); });
+      SB_CUDA(le);
+    }
     if (bt && S.n_proj > 0) {
       pj.items = proj_d + S.pi0;
       pj.n_items = (int)S.n_proj;
@@ -1099,6 +1338,14 @@ void check_device_errors(Context& c, cudaStream_t s, const FixedCall* call) {
   SB_CUDA(cudaStreamSynchronize(s));
   // A forced node error (test hook) merges as a kernel's atomicMin would: the first in order.
   h[0] = std::min(h[0], g_forced_node_error.exchange(~0ull));
+  if (call && call->i8_err) {
+    unsigned f = 0;
+    SB_CUDA(cudaMemcpy(&f, call->i8_err, sizeof f, cudaMemcpyDeviceToHost));
+    if (f)
+      throw Failure{SCATRS_CUDA,
+                    "the int8 angle GEMMs gave up waiting on the tensor cores or the copies "
+                    "(bounded wait)"};
+  }
   if (h[0] != ~0ull) {
     int status = (int)(h[0] & 3);
     unsigned long long key = h[0] >> 2;
@@ -3286,11 +3533,23 @@ void scatrs_ensemble_fixed_sizes(int64_t n_units, int64_t n_mu, int32_t greek_or
   if (greek_len) *greek_len = greek_order >= 0 ? 6 * n_units * ((int64_t)greek_order + 1) : 0;
 }
 
-int scatrs_ensemble_fixed(const scatrs_distribution* dists, int64_t n_dist,
-                          const double* wavelengths, int64_t n_wl, const double* m,
-                          const double* mu, int64_t n_mu, const scatrs_fixed_options* options,
-                          double* values, double* phase, double* greek, char* err,
-                          size_t err_len) {
+}  // extern "C"
+
+namespace sb {
+namespace {
+// The mixed form's options into a call (NULL or i8_above <= 0: the plain form).
+void set_mixed(FixedCall& call, const scatrs_mixed_options* mixed) {
+  if (!mixed || mixed->i8_above <= 0) return;
+  if (mixed->levels != 0 && mixed->levels != 5 && mixed->levels != 6)
+    throw Failure{SCATRS_INVALID_INPUT, "the mixed form keeps 5 or 6 product levels (0: 5)"};
+  call.i8_above = mixed->i8_above;
+  call.i8_levels = mixed->levels == 0 ? 5 : mixed->levels;
+}
+// scatrs_ensemble_fixed and its mixed form.
+int fixed_host(const scatrs_distribution* dists, int64_t n_dist, const double* wavelengths,
+               int64_t n_wl, const double* m, const double* mu, int64_t n_mu,
+               const scatrs_fixed_options* options, double* values, double* phase,
+               double* greek, const scatrs_mixed_options* mixed, char* err, size_t err_len) {
   return guarded(err, err_len, [&] {
     if (n_dist < 0 || n_wl < 0) throw Failure{SCATRS_INVALID_INPUT, "negative sizes"};
     for (int64_t i = 0; i < n_wl; ++i)
@@ -3313,6 +3572,7 @@ int scatrs_ensemble_fixed(const scatrs_distribution* dists, int64_t n_dist,
     double* g_d = gl > 0 ? c.greek.as<double>(gl) : nullptr;
     FixedCall call;
     call.wl_host.assign(wavelengths, wavelengths + n_wl);
+    set_mixed(call, mixed);
     // Pinned outputs are copied slab by slab beside the computation; others at the end.
     auto pinned = [](const void* p) {
       cudaPointerAttributes at{};
@@ -3353,6 +3613,63 @@ int scatrs_ensemble_fixed(const scatrs_distribution* dists, int64_t n_dist,
     if (gl > 0 && greek) SB_CUDA(cudaMemcpyAsync(greek, g_d, gl * 8, cudaMemcpyDeviceToHost, s));
     SB_CUDA(cudaStreamSynchronize(s));
   });
+}
+
+// scatrs_ensemble_fixed_device and its mixed form.
+int fixed_device(const scatrs_distribution* dists_host, int64_t n_dist,
+                 const double* wavelengths_dev, int64_t n_wl, const double* m_dev,
+                 const double* mu_host, int64_t n_mu, const scatrs_fixed_options* options,
+                 double* values_dev, double* phase_dev, double* greek_dev, void* stream,
+                 const scatrs_mixed_options* mixed, char* err, size_t err_len) {
+  return guarded(err, err_len, [&] {
+    if (n_dist < 0 || n_wl < 0) throw Failure{SCATRS_INVALID_INPUT, "negative sizes"};
+    Context& c = context();
+    std::lock_guard<std::mutex> lk(c.mtx);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    FixedCall call;
+    set_mixed(call, mixed);
+    call.wl_host.resize(n_wl);
+    if (n_wl > 0)
+      SB_CUDA(cudaMemcpyAsync(call.wl_host.data(), wavelengths_dev, n_wl * 8,
+                              cudaMemcpyDeviceToHost, s));
+    run_fixed(c, dists_host, n_dist, wavelengths_dev, n_wl, m_dev, mu_host, n_mu, options,
+              values_dev, phase_dev, greek_dev, s, &call);
+    g_last_call = std::move(call);
+  });
+}
+}  // namespace
+}  // namespace sb
+
+extern "C" {
+
+int scatrs_ensemble_fixed(const scatrs_distribution* dists, int64_t n_dist,
+                          const double* wavelengths, int64_t n_wl, const double* m,
+                          const double* mu, int64_t n_mu, const scatrs_fixed_options* options,
+                          double* values, double* phase, double* greek, char* err,
+                          size_t err_len) {
+  return fixed_host(dists, n_dist, wavelengths, n_wl, m, mu, n_mu, options, values, phase,
+                    greek, nullptr, err, err_len);
+}
+
+int scatrs_ensemble_fixed_mixed(const scatrs_distribution* dists, int64_t n_dist,
+                                const double* wavelengths, int64_t n_wl, const double* m,
+                                const double* mu, int64_t n_mu,
+                                const scatrs_fixed_options* options,
+                                const scatrs_mixed_options* mixed, double* values,
+                                double* phase, double* greek, char* err, size_t err_len) {
+  return fixed_host(dists, n_dist, wavelengths, n_wl, m, mu, n_mu, options, values, phase,
+                    greek, mixed, err, err_len);
+}
+
+int scatrs_ensemble_fixed_mixed_device(const scatrs_distribution* dists_host, int64_t n_dist,
+                                       const double* wavelengths_dev, int64_t n_wl,
+                                       const double* m_dev, const double* mu_host, int64_t n_mu,
+                                       const scatrs_fixed_options* options,
+                                       const scatrs_mixed_options* mixed, double* values_dev,
+                                       double* phase_dev, double* greek_dev, void* stream,
+                                       char* err, size_t err_len) {
+  return fixed_device(dists_host, n_dist, wavelengths_dev, n_wl, m_dev, mu_host, n_mu, options,
+                      values_dev, phase_dev, greek_dev, stream, mixed, err, err_len);
 }
 
 int scatrs_ensemble_fixed_d(const scatrs_distribution* dists, int64_t n_dist,
@@ -4016,20 +4333,8 @@ int scatrs_ensemble_fixed_device(const scatrs_distribution* dists_host, int64_t 
                                  const scatrs_fixed_options* options, double* values_dev,
                                  double* phase_dev, double* greek_dev, void* stream, char* err,
                                  size_t err_len) {
-  return guarded(err, err_len, [&] {
-    if (n_dist < 0 || n_wl < 0) throw Failure{SCATRS_INVALID_INPUT, "negative sizes"};
-    Context& c = context();
-    std::lock_guard<std::mutex> lk(c.mtx);
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
-    FixedCall call;
-    call.wl_host.resize(n_wl);
-    if (n_wl > 0)
-      SB_CUDA(cudaMemcpyAsync(call.wl_host.data(), wavelengths_dev, n_wl * 8,
-                              cudaMemcpyDeviceToHost, s));
-    run_fixed(c, dists_host, n_dist, wavelengths_dev, n_wl, m_dev, mu_host, n_mu, options,
-              values_dev, phase_dev, greek_dev, s, &call);
-    g_last_call = std::move(call);
-  });
+  return fixed_device(dists_host, n_dist, wavelengths_dev, n_wl, m_dev, mu_host, n_mu, options,
+                      values_dev, phase_dev, greek_dev, stream, nullptr, err, err_len);
 }
 
 int scatrs_check_errors(void* stream, char* err, size_t err_len) {
@@ -4221,8 +4526,12 @@ void scatrs_release(void) {
                       &c.slots, &c.items, &c.proj_items, &c.slot_index, &c.slot_greek,
                       &c.X, &c.uz, &c.ux, &c.chunk_sums, &c.err, &c.acc,
                       &c.counter, &c.values, &c.phase, &c.greek, &c.user.ge, &c.user.go,
-                      &c.user.map})
+                      &c.user.map, &c.tc_a_hi, &c.tc_a_lo, &c.tc_prod, &c.tc_err, &c.xdig,
+                      &c.xscale, &c.chunk_xoff, &c.chunk_xidx, &c.i8_list, &c.i8_err,
+                      &c.i8.dig, &c.i8.scale, &c.i8.user_d, &c.i8.band_d})
       b->release();
+    for (auto& kv : c.projectors)
+      for (DevBuf* b : {&kv.second.d, &kv.second.d_hi, &kv.second.d_lo}) b->release();
     for (auto& kv : c.bands)
       for (DevBuf* b : {&kv.second.ge_d, &kv.second.go_d, &kv.second.d_d, &kv.second.desc_d})
         b->release();

@@ -144,6 +144,84 @@ struct ProjArgs {
   int n_theta;
 };
 
+// The angle GEMMs of a chunk in exact integer arithmetic on the tensor cores (the mixed form):
+// every value v of a table row (or of a coefficient column) is the fixed-point integer
+// F = rint(v 2^(e + 32)) with 2^e the row's (column's) power of two that puts its largest |v|
+// below 127 (in [63.5, 127)), F split into kI8Levels balanced signed digits,
+// F = d0 2^32 + d1 2^24 + d2 2^16 + d3 2^8 + d4 with every d in [-128, 127]. A product's digit
+// pairs (i, j) with i + j = s < kI8Levels sum exactly in the INT32 accumulator of level s
+// (tcgen05.mma kind::i8, signed); sum_s L_s 2^(-8 s) 2^(-e_row - e_col) is the product to about
+// 2^-38 of the largest |G| |X| per term, the dropped levels' terms centred on zero.
+constexpr int kI8Levels = 5;         // digits per value
+constexpr int kI8MaxLevels = 6;      // product levels kept at most (i + j < 6: 19 products)
+constexpr int kI8KB = 64;            // orders per K block (a row of the 64-byte swizzle)
+constexpr int kI8Pairs = 64;         // angle pairs per M tile: 128 MMA rows, E rows then O rows
+constexpr int kI8MaxTerms = 4096;    // the INT32 level sums stay exact up to this many orders
+constexpr int kI8TileBytes = kI8Levels * 128 * kI8KB;  // one (M tile, K block): 40 KiB
+constexpr int kI8HalfBytes = kI8Levels * 64 * kI8KB;   // one (16-node half, K block): 20 KiB
+
+// Where one table's digits live: M tile t, K block kb, digit s, row r at
+// off + ((t * n_kb + kb) * kI8Levels + s) * 8192 + r * 64 (64-byte swizzle inside the row), its
+// rows' scales 2^-e at scale_off + t * 128 + r.
+struct I8Table {
+  int64_t off;
+  int64_t scale_off;
+  int n_kb;
+  int n_tiles;
+};
+
+// The mixed form of K-b and K-c over one slab (values of the fixed grid): the chunks with
+// above < nc <= kI8MaxTerms, the others left to unit_kernel.
+struct UnitI8Args {
+  const double* radius;
+  const double* weight;
+  const double* wl;
+  int n_dist, n_wl, n_nodes, cpu;
+  const int* units;
+  int n_items;
+  const WorkItem* items;
+  const int* chunk_n;
+  const int64_t* chunk_acc;
+  const int64_t* unit_acc;
+  int n_mu, h_u;
+  const int2* user_map;
+  int greek_order;
+  const BandDesc* bands;
+  double* acc;
+  // Chunk digits: per slab-local chunk the byte offset of its digits ((half, K block) blocks of
+  // kI8HalfBytes) or -1 when it is not on this path, and the index of its 128 column scales.
+  const int64_t* chunk_xoff;
+  const int* chunk_xidx;
+  const unsigned char* xdig;
+  const double* xscale;
+  // Table digits: the requested cosines' tables in versions v (orders < 64 2^v, their rows'
+  // scales over those orders), then one table per band.
+  const unsigned char* tdig;
+  const double* tscale;
+  const I8Table* user_tabs;
+  int n_user_tabs;
+  const I8Table* band_tabs;
+  int levels;     // product levels kept: 5 (15 products) or 6 (19)
+  unsigned* err;  // set when a bounded wait gave up
+};
+
+// The digits of the int8 chunks' coefficient rows (one CTA per listed chunk).
+struct XSplitArgs {
+  const double* X;
+  const int64_t* chunk_row;
+  const int* chunk_n;
+  const int* list;  // slab-local chunks on the int8 path
+  int n;
+  const int64_t* chunk_xoff;
+  const int* chunk_xidx;
+  unsigned char* xdig;
+  double* xscale;
+};
+
+void launch_x_split(const XSplitArgs& a, cudaStream_t s);
+cudaError_t launch_units_i8(const UnitI8Args& a, int grid, cudaStream_t s);
+size_t units_i8_smem();
+
 // unit_norm per unit of an adaptive call with derivatives: the 8 doubles of FinalArgs, then
 // per distribution parameter p < 3 its Z_p at 8 + p, the error of Z_p at 11 + p, and
 // d<r^2>/dp, its error, d<r^3>/dp, its error at 14 + 4 p.
@@ -185,6 +263,9 @@ struct UnitArgs {
   // Adaptive panels with derivatives (deriv and wdiff): the parameters' error weights; the
   // accumulators hold each block's sums, then each block's error sums (2 (3 + n_theta) blocks).
   const double* wthdiff;
+  // The mixed form (i8_above > 0): chunks with i8_above < nc <= kI8MaxTerms are left to
+  // unit_i8_kernel.
+  int i8_above;
 };
 
 // K-d and the outputs over one slab: averages, band projections, assembly.

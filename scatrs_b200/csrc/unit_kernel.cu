@@ -475,6 +475,7 @@ __device__ __forceinline__ void unit_body(const UnitArgs& a) {
       const int64_t ci = (int64_t)ul * a.cpu + c;
       const int nc = a.chunk_n[ci];
       if (nc == 0) continue;
+      if (a.i8_above > 0 && nc > a.i8_above && nc <= kI8MaxTerms) continue;  // the int8 path's
       const int b = a.greek_order >= 0 ? band_of(nc) : -1;
       const int t_band = b >= 0 ? (a.bands[b].h + TR - 1) / TR : 0;
       if (it.group >= t_user + t_band) continue;

@@ -3,10 +3,11 @@
 The reference (usask-arg/scatrs) ships certified or high-precision values computed with Arb
 ball arithmetic in ``reference/data/*.jsonl`` (each value as hi + lo + lo2 plus an error bound).
 This script keeps the records on the ensemble path (homogeneous spheres, their Greek
-coefficients, Gauss-Legendre rules, the Wigner d functions the projection uses, layered
-spheres, spheroids' T-matrices) as hi + lo pairs in compact JSON, so that the tests run without the reference tree.
+coefficients, the derivatives of their coefficients and efficiencies, Gauss-Legendre rules, the
+Wigner d functions the projection uses, layered spheres and their derivatives, spheroids'
+T-matrices) as hi + lo pairs in compact JSON, so that the tests run without the reference tree.
 
-Run from the repository root:  python tests/golden/make_fixtures.py [path/to/reference]
+Run from the repository root:  python tests/golden/make_fixtures.py path/to/reference
 """
 
 from __future__ import annotations
@@ -85,6 +86,24 @@ def main(ref: str) -> None:
          **{k: pairs(r["outputs"][k]) for k in r["outputs"] if k.startswith("q_") or k == "g"}}
         for r in layered if r["case"].endswith(",series")
     ]
+    md = load(ref, "mie_derivatives.jsonl")
+    out["mie_coefficient_derivatives"] = [
+        {"case": r["case"], "x": r["inputs"]["x"], "m": [r["inputs"]["m_re"], r["inputs"]["m_im"]],
+         "orders": r["inputs"]["orders"], **{k: pairs(v) for k, v in r["outputs"].items()}}
+        for r in md if r["case"].endswith(",coefficients")
+    ]
+    out["mie_jacobian"] = [
+        {"case": r["case"], "x": r["inputs"]["x"], "m": [r["inputs"]["m_re"], r["inputs"]["m_im"]],
+         **{k: pairs(v) for k, v in r["outputs"].items() if k.startswith(("q_", "g_"))}}
+        for r in md if r["case"].endswith(",series")
+    ]
+    ld = load(ref, "layered_derivatives.jsonl")
+    out["layered_derivatives"] = [
+        {"case": r["case"], "x": r["inputs"]["x"], "m_re": r["inputs"]["m_re"],
+         "m_im": r["inputs"]["m_im"], "orders": r["inputs"]["orders"],
+         **{k: pairs(v) for k, v in r["outputs"].items()}}
+        for r in ld
+    ]
     sph = load(ref, "spheroid.jsonl")
     out["spheroid"] = [
         {"case": r["case"], "x": r["inputs"]["x"], "eps": r["inputs"]["aspect_ratio"],
@@ -100,4 +119,6 @@ def main(ref: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_fixtures.py path/to/reference")
+    main(sys.argv[1])

@@ -1,9 +1,11 @@
 """Derivatives of the layered-sphere ensemble on the GPU (scatrs_ensemble_fixed_layered_d: the
 layered recursion carried in forward mode, one derivative pass per layer index and per radius
-fraction) against central finite differences of the oracle's layered ensemble (an independent
-double-precision restatement), step 1e-5 relative: the scalars, phase matrix and Greek
-coefficients along the distribution's parameters, Re m_l and Im m_l of every layer and the
-fractions, within 2e-6 of each output row's scale. Values equal the plain layered ensemble."""
+fraction) against Richardson-extrapolated central differences of the oracle's layered ensemble
+(an independent double-precision restatement; steps 1e-3 and 5e-4 relative, so the differences'
+truncation error is O(h^4)): the scalars, phase matrix and Greek coefficients along the
+distribution's parameters, Re m_l and Im m_l of every layer and the fractions, within 1e-6 of
+each output row's scale. Values equal the plain layered ensemble. The derivatives themselves are
+pinned to the reference's Arb records in test_gpu_derivative_pins.py."""
 
 import numpy as np
 import pytest
@@ -55,33 +57,37 @@ def test_matches_finite_differences(gpu):
     assert dv.shape[0] == 10
     for blk, kind, k in blocks:
         for dist in range(2):
-            def perturbed(sign):
+            def perturbed(sign, rel):
                 dd, ff, mm = d.copy(), fr.copy(), ml.copy()
                 if kind == "param":
-                    h = 1e-5 * dd["param"][dist, k]
+                    h = rel * dd["param"][dist, k]
                     dd["param"][dist, k] += sign * h
                 elif kind == "re":
-                    h = 1e-5 * abs(mm[dist, k, 0])
+                    h = rel * abs(mm[dist, k, 0])
                     mm[dist, k, :] += sign * h
                 elif kind == "im":
-                    h = 1e-5 * abs(mm[dist, k, 0])
+                    h = rel * abs(mm[dist, k, 0])
                     mm[dist, k, :] += sign * 1j * h
                 else:
-                    h = 1e-5 * ff[dist, k]
+                    h = rel * ff[dist, k]
                     ff[dist, k] += sign * h
                 return _oracle(dd, wl, ff, mm), h
-            (vp, php, gp), h = perturbed(+1)
-            (vm, phm, gm), _ = perturbed(-1)
+
+            def central(rel):
+                (vp, php, gp), h = perturbed(+1, rel)
+                (vm, phm, gm), _ = perturbed(-1, rel)
+                return [(p_ - m_) / (2 * h) for p_, m_ in ((vp, vm), (php, phm), (gp, gm))]
+
+            coarse, fine = central(1e-3), central(5e-4)
             sl = slice(dist * n_wl, (dist + 1) * n_wl)
-            for got, plus, minus in ((dv[blk], vp, vm), (dph[blk], php, phm),
-                                     (dg[blk], gp, gm)):
-                fd = (plus - minus) / (2 * h)
+            for got, dc, df in zip((dv[blk], dph[blk], dg[blk]), coarse, fine):
+                fd = (4.0 * df - dc) / 3.0  # Richardson: the h^2 terms cancel
                 g_, f_ = got[:, sl], fd[:, sl]
                 # Each output row (a scalar, a phase element, a Greek array) against its own
                 # largest derivative in the unit slice.
                 scale = np.abs(f_).reshape(f_.shape[0], -1).max(axis=1)
                 err = np.abs(g_ - f_).reshape(f_.shape[0], -1).max(axis=1)
-                assert np.all(err <= 2e-6 * np.maximum(scale, 1e-300)), (blk, kind, k, dist,
+                assert np.all(err <= 1e-6 * np.maximum(scale, 1e-300)), (blk, kind, k, dist,
                                                                          err / scale)
 
 
@@ -89,7 +95,8 @@ def test_autograd_gradient_of_a_loss(gpu):
     """A loss of the layered-adjoint shape (weighted squared differences of c_ext, ssa, g and
     alpha1[0:16] from targets) differentiated by torch through scatrs_ensemble_fixed_layered_d:
     the gradient along the medians, widths, fractions and every layer's n and k (the same at
-    every wavelength) against central differences of the loss, 1e-5 relative."""
+    every wavelength) against Richardson-extrapolated central differences of the loss (steps
+    1e-4 and 5e-5 relative), 1e-6 relative."""
     import torch
     from scatrs_b200 import autograd
 
@@ -119,13 +126,44 @@ def test_autograd_gradient_of_a_loss(gpu):
     for which, p in enumerate(params):
         flat = p.grad.reshape(-1)
         for idx in range(flat.numel()):
-            h = 1e-6 * max(abs(float(base[which].reshape(-1)[idx])), 1e-3)
-            vals = []
-            for sign in (1, -1):
-                args = [b.clone() for b in base]
-                args[which].view(-1)[idx] += sign * h
-                with torch.no_grad():
-                    vals.append(float(loss_of(*args)))
-            fd = (vals[0] - vals[1]) / (2 * h)
-            assert abs(float(flat[idx]) - fd) <= 1e-5 * max(abs(fd), 1e-3 * abs(loss.item())), (
+            x0 = max(abs(float(base[which].reshape(-1)[idx])), 1e-3)
+
+            def central(h):
+                vals = []
+                for sign in (1, -1):
+                    args = [b.clone() for b in base]
+                    args[which].view(-1)[idx] += sign * h
+                    with torch.no_grad():
+                        vals.append(float(loss_of(*args)))
+                return (vals[0] - vals[1]) / (2 * h)
+
+            fd = (4.0 * central(5e-5 * x0) - central(1e-4 * x0)) / 3.0
+            assert abs(float(flat[idx]) - fd) <= 1e-6 * max(abs(fd), 1e-3 * abs(loss.item())), (
                 which, idx, float(flat[idx]), fd)
+
+
+def test_fixed_binding_selects_the_layered_blocks(gpu):
+    """_scatrs.ensemble_compute_fixed with derivatives of a layered sphere: the blocks of
+    scatrs_ensemble_fixed_layered_d in ensemble_parameters' order, selected by index."""
+    from scatrs_b200 import _scatrs
+
+    wl = np.array([0.5, 0.8])
+    fr = np.array([0.6, 0.9])
+    ml = np.array([[1.8 + 0.1j, 1.8 + 0.1j], [1.5 + 0.01j, 1.5 + 0.01j],
+                   [1.34 + 1e-4j, 1.33 + 1e-4j]])
+    spec = ("lognormal", 0.15, 1.5)
+    names = _scatrs.ensemble_parameters([(spec, ("layered", fr, ml), 1.0)], False)
+    assert names[:4] == ["median_radius", "width", "layer0.m_real", "layer0.m_imag"]
+    assert names[-2:] == ["layer0.radius_fraction", "layer1.radius_fraction"]
+    pick = [1, names.index("layer1.m_imag"), names.index("layer1.radius_fraction")]
+    out = _scatrs.ensemble_compute_fixed([spec], ("layered", fr, ml), wl, 8, False, MU, True,
+                                         n_nodes=48, spread=3.0, derivatives=pick)
+    d = np.zeros(1, dtype=_native.DIST_DTYPE)
+    d["kind"] = 1
+    d["param"][0, :2] = (0.15, 1.5)
+    d["r_lo"], d["r_hi"] = 0.15 * 1.5 ** -3, 0.15 * 1.5 ** 3
+    ref = gpu.ensemble_fixed_layered_d(d, wl, fr[None], ml[None], MU, 48, 8)
+    assert np.array_equal(out["values"], ref[0])
+    assert np.array_equal(out["d"], ref[3][pick])
+    assert np.array_equal(out["greek_d"], ref[5][pick])
+    assert np.array_equal(out["phase_d"], ref[4][pick])

@@ -208,3 +208,85 @@ def test_layered_within_declared_tolerance():
                 scale = max(abs(ref), 1e-3 * s["q_ext"])
             tol = 16.0 * (kappa_layered(x[-1], ms) + cond_num[i] / scale) * EPS * 4
             assert abs(q[i] - ref) / scale <= tol, (r["case"], k, q[i], ref)
+
+
+def test_coefficient_derivatives_within_declared_tolerance():
+    """da/dx, da/dm, db/dx, db/dm against the Arb records (reference/data/mie_derivatives.jsonl)
+    within 512 (1 + max(1, |m|) x + cond) 2^-52 of the largest |value| of each array
+    (scatrs/src/mie/domain.rs:150-199, CoefficientDerivatives), cond from central differences
+    of the oracle's own derivatives (x |d/dx| + |m| |d/dm|, relative)."""
+    worst = 0.0
+    for r in load("mie_coefficient_derivatives"):
+        x, m = r["x"], complex(*r["m"])
+        orders = np.array(r["orders"])
+        n_max = max(O.default_n_max(x), int(orders.max()))
+        s = O.mie(x, m, n_max=n_max, derivatives=True)
+        h = 1e-5
+        sp = O.mie(x * (1 + h), m, n_max=n_max, derivatives=True)
+        sm = O.mie(x * (1 - h), m, n_max=n_max, derivatives=True)
+        mp = O.mie(x, m * (1 + h), n_max=n_max, derivatives=True)
+        mm = O.mie(x, m * (1 - h), n_max=n_max, derivatives=True)
+        for key in ("da_dx", "da_dm", "db_dx", "db_dm"):
+            ref = np.array([complex(val(r[key + "_re"], i), val(r[key + "_im"], i))
+                            for i in range(orders.size)])
+            got = s[key][orders - 1]
+            scale = np.abs(ref).max()
+            if scale == 0.0:
+                continue
+            ddx = (sp[key][orders - 1] - sm[key][orders - 1]) / (2 * h)   # x d/dx
+            ddm = (mp[key][orders - 1] - mm[key][orders - 1]) / (2 * h)   # m d/dm
+            cond = (np.abs(ddx).max() + np.abs(ddm).max()) / scale
+            tol = 512.0 * (1.0 + max(abs(m), 1.0) * x + cond) * EPS
+            err = np.abs(got - ref).max() / scale
+            worst = max(worst, err / tol)
+            assert err <= tol, (r["case"], key, err, tol)
+    assert worst > 0.0
+
+
+def single_node(x, lam=1.0):
+    """A fixed grid whose one node is a sphere of size parameter x at wavelength lam: a
+    lognormal on [r / 1.5, 1.5 r], whose one Gauss node is the midpoint in ln r."""
+    r = x * lam / (2.0 * np.pi)
+    d = np.zeros(1, dtype=O.DIST_DTYPE)
+    d["kind"] = 1
+    d["p"][0, :2] = (r, 1.5)
+    d["r_lo"], d["r_hi"] = r / 1.5, r * 1.5
+    return d, r
+
+
+JAC_NAMES = ("q_ext", "q_sca", "q_abs", "q_back")
+
+
+def jacobian_errors(r, q, dq):
+    """Errors of dQ/dRe m, dQ/dIm m (dq[p][k], p = 0 Re, 1 Im) against a record, relative to
+    max(|dQ|, |Q|) (Q_back against max(Q_back, Q_sca)), and their bounds
+    256 (kappa max(1, |m|/|m-1|)) 2^-52 (scatrs/src/mie/domain.rs:150-199, EfficiencyJacobian)."""
+    x, m = r["x"], complex(*r["m"])
+    near = max(abs(m) / abs(m - 1), 1.0) if m != 1 else np.inf
+    tol = 256.0 * kappa(x, m) * near * EPS
+    out = []
+    for p, key in enumerate(("dm_re", "dm_im")):
+        for k, name in enumerate(JAC_NAMES):
+            ref = val(r[f"{name}_{key}"], 0)
+            qs = max(abs(q[k]), abs(q[1])) if name == "q_back" else abs(q[k])
+            scale = max(abs(ref), qs, 1e-300)
+            out.append((name + "_" + key, abs(dq[p][k] - ref) / scale, tol))
+    return out
+
+
+def test_efficiency_jacobian_of_the_oracle_within_declared_tolerance():
+    """The oracle's dQ/dRe m and dQ/dIm m through its one-node fixed-grid ensemble with
+    derivatives (d c / dm = pi r^2 dQ/dm) against the Arb records' efficiency Jacobian."""
+    worst = 0.0
+    for r in load("mie_jacobian"):
+        x, m = r["x"], complex(*r["m"])
+        d, rad = single_node(x)
+        out = O.ensemble_fixed_d(d, np.array([1.0]), np.array([[m]]), 1, None, -1,
+                                 allow_unvalidated=True)
+        area = np.pi * rad * rad
+        q = out["values"][:4, 0] / area
+        dq = out["d_values"][2:4, :4, 0] / area
+        for name, err, tol in jacobian_errors(r, q, dq):
+            worst = max(worst, err / tol)
+            assert err <= tol, (r["case"], name, err, tol)
+    assert worst > 0.0
