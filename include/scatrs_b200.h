@@ -454,6 +454,70 @@ int scatrs_ensemble_fixed_mixed_device(const scatrs_distribution* dists_host, in
                                        double* phase_dev, double* greek_dev, void* stream,
                                        char* err, size_t err_len);
 
+/*
+ * scatrs_ensemble_fixed_d and scatrs_ensemble_fixed_layered_d with DEVICE arrays for the index
+ * (m_dev: complex [n_dist][n_wl]; layers->m: complex [n_dist][L][n_wl] in device memory, the
+ * fractions on the host), the wavelengths and every output (laid out as the host entries';
+ * phase and greek arrays required when n_mu > 0 and L >= 0), run on `stream` (a cudaStream_t or
+ * NULL), which they synchronize before returning, device-side input errors included. For
+ * callers whose inputs and outputs live on the GPU (the torch autograd layer): only the
+ * distributions, the cosines and the fractions cross from the host.
+ */
+int scatrs_ensemble_fixed_d_device(const scatrs_distribution* dists_host, int64_t n_dist,
+                                   const double* wavelengths_dev, int64_t n_wl,
+                                   const double* m_dev, const double* mu_host, int64_t n_mu,
+                                   const scatrs_fixed_options* options, double* values_dev,
+                                   double* phase_dev, double* greek_dev, double* d_values_dev,
+                                   double* d_phase_dev, double* d_greek_dev, void* stream,
+                                   char* err, size_t err_len);
+int scatrs_ensemble_fixed_layered_d_device(const scatrs_distribution* dists_host,
+                                           int64_t n_dist, const double* wavelengths_dev,
+                                           int64_t n_wl, const scatrs_layers* layers,
+                                           const double* mu_host, int64_t n_mu,
+                                           const scatrs_fixed_options* options,
+                                           double* values_dev, double* phase_dev,
+                                           double* greek_dev, double* d_values_dev,
+                                           double* d_phase_dev, double* d_greek_dev,
+                                           void* stream, char* err, size_t err_len);
+
+/* Refractive-index models m(lambda) (python/scatrs/refractive.py:168-354), evaluated on the
+ * device:
+ *   SCATRS_M_CONSTANT      m = p[0] + i p[1]; parameters n, k
+ *   SCATRS_M_TABLE         n points: table = wavelengths[n] then m as (re, im) pairs[n],
+ *                          interpolated linearly in lambda (np.interp); no parameters
+ *   SCATRS_M_TABLE_LOG_K   the same with ln Im m interpolated (Im m > 0 at every point)
+ *   SCATRS_M_CAUCHY        n = p[0] + p[1] / lambda^2 + p[2] / lambda^4, Im m = p[3];
+ *                          parameters A, B, C, k
+ *   SCATRS_M_SELLMEIER     n^2 = 1 + sum_i B_i lambda^2 / (lambda^2 - C_i), Im m = p[3], n terms:
+ *                          table = B[n] then C[n]; parameters B_0.., C_0.., k
+ * A model given as a Python function (refractive.py:357-368) is evaluated by the caller. */
+enum scatrs_refractive_kind {
+  SCATRS_M_CONSTANT = 0,
+  SCATRS_M_TABLE = 1,
+  SCATRS_M_TABLE_LOG_K = 2,
+  SCATRS_M_CAUCHY = 3,
+  SCATRS_M_SELLMEIER = 4
+};
+typedef struct scatrs_refractive_model {
+  int32_t kind;
+  int32_t n;
+  double p[4];
+  const double* table; /* host memory, as above */
+} scatrs_refractive_model;
+
+/* The number of parameters of a model (-1 for an unknown kind). */
+int scatrs_refractive_parameter_count(const scatrs_refractive_model* model);
+
+/* m of every model at every wavelength into m_dev (complex [n_models][n_wl], device) and, when
+ * dm_dev is not NULL, dm/dtheta into dm_dev (complex [n_models][p_max][n_wl], zero past each
+ * model's own parameters), with the checks and messages of refractive.py (a wavelength outside a
+ * table's range, Sellmeier's n^2 not positive, the first failure in (model, wavelength) order).
+ * Runs on `stream` and synchronizes it. */
+int scatrs_refractive_index_device(const scatrs_refractive_model* models, int64_t n_models,
+                                   const double* wavelengths_dev, int64_t n_wl, double* m_dev,
+                                   double* dm_dev, int32_t p_max, void* stream, char* err,
+                                   size_t err_len);
+
 /* Synchronizes `stream` and returns the first device-side input error of the last
  * scatrs_ensemble_fixed_device call on it (in wavelength, distribution, radius order). */
 int scatrs_check_errors(void* stream, char* err, size_t err_len);

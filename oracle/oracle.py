@@ -761,3 +761,57 @@ def spheroid_node(x: float, eps: float, s: complex, rtol: float = 1e-8):
     if st != 0:
         raise OracleError(st, "spheroid_node")
     return q, int(n[0]), int(n[1])
+
+
+# ---------------------------------------------------------------------------------------------
+# Refractive-index models (python/scatrs/refractive.py:168-354), restated with numpy in the
+# reference's order of operations: m at the wavelengths and dm/dtheta for each parameter.
+# ---------------------------------------------------------------------------------------------
+def refractive_index(spec, wavelength):
+    """m of a model spec at `wavelength` (1-D), and dm (P, n): ("constant", m) (refractive.py:
+    190-197), ("table", wl, m) / ("table_log_k", wl, m) (246-262, np.interp), ("cauchy", A, B,
+    C, k) (283-294), ("sellmeier", B, C, k) (326-354). Raises ValueError where the reference
+    raises InvalidInputError (a wavelength outside a table, Sellmeier's n^2 <= 0)."""
+    lam = np.asarray(wavelength, dtype=np.float64).reshape(-1)
+    kind = spec[0]
+    if kind == "constant":
+        m = complex(spec[1])
+        dm = np.empty((2, lam.size), dtype=complex)
+        dm[0], dm[1] = 1.0, 1j
+        return np.full(lam.shape, m), dm
+    if kind in ("table", "table_log_k"):
+        wl = np.asarray(spec[1], dtype=np.float64)
+        nodes = np.asarray(spec[2], dtype=np.complex128)
+        if np.any(~((lam >= wl[0]) & (lam <= wl[-1]))):
+            raise ValueError("a wavelength is outside the Table's range")
+        n = np.interp(lam, wl, nodes.real)
+        if kind == "table":
+            k = np.interp(lam, wl, nodes.imag)
+        else:
+            k = np.exp(np.interp(lam, wl, np.log(nodes.imag)))
+        return n + 1j * k, np.zeros((0, lam.size), dtype=complex)
+    if kind == "cauchy":
+        A, B, C, k = (float(v) for v in spec[1:5])
+        s = lam ** -2.0
+        dm = np.empty((4, lam.size), dtype=complex)
+        dm[0], dm[1], dm[2], dm[3] = 1.0, s, s * s, 1j
+        return A + B * s + C * s * s + 1j * k, dm
+    if kind == "sellmeier":
+        b = np.asarray(spec[1], dtype=np.float64).reshape(-1)
+        c = np.asarray(spec[2], dtype=np.float64).reshape(-1)
+        k = float(spec[3])
+        l2 = lam * lam
+        n2 = np.ones_like(l2)
+        for bi, ci in zip(b, c):
+            n2 += bi * l2 / (l2 - ci)
+        if np.any(~(n2 > 0) | ~np.isfinite(n2)):
+            raise ValueError("Sellmeier gives n^2 <= 0")
+        n = np.sqrt(n2)
+        t = b.size
+        dm = np.empty((2 * t + 1, lam.size), dtype=complex)
+        for i, (bi, ci) in enumerate(zip(b, c)):
+            dm[i] = l2 / (l2 - ci) / (2 * n)
+            dm[t + i] = bi * l2 / (l2 - ci) ** 2 / (2 * n)
+        dm[-1] = 1j
+        return n + 1j * k, dm
+    raise TypeError(f"unknown refractive-index model {kind!r}")

@@ -92,6 +92,13 @@ class MixedOptions(ctypes.Structure):
     _fields_ = [("i8_above", _I32), ("levels", _I32)]
 
 
+class RefractiveModel(ctypes.Structure):
+    _fields_ = [("kind", _I32), ("n", _I32), ("p", _D * 4), ("table", _PD)]
+
+
+REFRACTIVE_KINDS = {"constant": 0, "table": 1, "table_log_k": 2, "cauchy": 3, "sellmeier": 4}
+
+
 # Every symbol the header declares, with (restype, argtypes).
 SYMBOLS = {
     "scatrs_ensemble_fixed_sizes": (None, [_I64, _I64, _I32, _PI64, _PI64, _PI64]),
@@ -154,6 +161,18 @@ SYMBOLS = {
     "scatrs_mie_static": (ctypes.c_int, [_VP, _VP, _I64, _I32, _I64, _VP, _VP, _VP, _VP, _VP,
                                          _CP, _SZ]),
     "scatrs_not_converged_detail": (ctypes.c_int, [_PD, _PD]),
+    "scatrs_ensemble_fixed_d_device": (ctypes.c_int, [_VP, _I64, _VP, _I64, _VP, _PD, _I64,
+                                                      ctypes.POINTER(FixedOptions), _VP, _VP,
+                                                      _VP, _VP, _VP, _VP, _VP, _CP, _SZ]),
+    "scatrs_ensemble_fixed_layered_d_device": (ctypes.c_int, [_VP, _I64, _VP, _I64,
+                                                              ctypes.POINTER(Layers), _PD, _I64,
+                                                              ctypes.POINTER(FixedOptions), _VP,
+                                                              _VP, _VP, _VP, _VP, _VP, _VP, _CP,
+                                                              _SZ]),
+    "scatrs_refractive_parameter_count": (ctypes.c_int, [ctypes.POINTER(RefractiveModel)]),
+    "scatrs_refractive_index_device": (ctypes.c_int, [ctypes.POINTER(RefractiveModel), _I64,
+                                                      _VP, _I64, _VP, _VP, _I32, _VP, _CP,
+                                                      _SZ]),
     "scatrs_testing_raise": (ctypes.c_int, [_I32, _CP, _D, _D, _CP, _SZ]),
     "scatrs_testing_fail_allocation": (None, [_I64]),
     "scatrs_testing_force_node_error": (None, [_I64, _I32]),
@@ -781,3 +800,92 @@ def spheroid_compute(x, aspect_ratio, m, rtol: float = 1e-8, n_terms: int = 0, n
 def check_errors(stream: int = 0) -> None:
     err = ctypes.create_string_buffer(1024)
     _check(load().scatrs_check_errors(stream or None, err, 1024), err)
+
+
+def ensemble_fixed_d_device(dists: np.ndarray, wl_ptr: int, n_wl: int, m_ptr: int, mu,
+                            n_nodes: int, greek_order: int, normalized: bool, out_ptrs,
+                            stream: int = 0, allow_unvalidated: bool = False) -> None:
+    """scatrs_ensemble_fixed_d_device: device arrays (raw pointers) for the wavelengths, m and the
+    six outputs out_ptrs = (values, phase, greek, d_values, d_phase, d_greek); synchronizes."""
+    dists = np.ascontiguousarray(dists, dtype=DIST_DTYPE)
+    mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
+    opts = FixedOptions(int(n_nodes), int(greek_order), int(normalized), int(allow_unvalidated))
+    err = ctypes.create_string_buffer(1024)
+    st = load().scatrs_ensemble_fixed_d_device(dists.ctypes.data, dists.size, wl_ptr, n_wl, m_ptr,
+                                               _p(mu), mu.size, ctypes.byref(opts),
+                                               *[p or None for p in out_ptrs], stream or None,
+                                               err, 1024)
+    _check(st, err)
+
+
+def ensemble_fixed_layered_d_device(dists: np.ndarray, wl_ptr: int, n_wl: int, fractions,
+                                    n_layers: int, m_ptr: int, mu, n_nodes: int,
+                                    greek_order: int, normalized: bool, out_ptrs,
+                                    stream: int = 0, allow_unvalidated: bool = False) -> None:
+    """scatrs_ensemble_fixed_layered_d_device: the layers' m (complex [n_dist][L][n_wl]) and the
+    outputs on the device, the fractions (n_dist, L - 1) on the host; synchronizes."""
+    dists = np.ascontiguousarray(dists, dtype=DIST_DTYPE)
+    fr = np.ascontiguousarray(fractions, dtype=np.float64).reshape(dists.size, n_layers - 1)
+    mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
+    lay = Layers(int(n_layers), 0, _p(fr), ctypes.cast(m_ptr, _PD))
+    opts = FixedOptions(int(n_nodes), int(greek_order), int(normalized), int(allow_unvalidated))
+    err = ctypes.create_string_buffer(1024)
+    st = load().scatrs_ensemble_fixed_layered_d_device(
+        dists.ctypes.data, dists.size, wl_ptr, n_wl, ctypes.byref(lay), _p(mu), mu.size,
+        ctypes.byref(opts), *[p or None for p in out_ptrs], stream or None, err, 1024)
+    _check(st, err)
+
+
+def refractive_models(specs):
+    """scatrs_refractive_model records (and the arrays they point at) from specs: ("constant", m),
+    ("cauchy", A, B, C, k), ("sellmeier", B, C, k), ("table", wavelengths, m) or
+    ("table_log_k", wavelengths, m)."""
+    recs = (RefractiveModel * max(len(specs), 1))()
+    keep = []
+    for i, spec in enumerate(specs):
+        kind = spec[0]
+        if kind not in REFRACTIVE_KINDS:
+            raise TypeError(f"unknown refractive-index model {kind!r}")
+        r = recs[i]
+        r.kind = REFRACTIVE_KINDS[kind]
+        if kind == "constant":
+            m = complex(spec[1])
+            r.p[0], r.p[1] = m.real, m.imag
+        elif kind == "cauchy":
+            for j in range(4):
+                r.p[j] = float(spec[1 + j])
+        elif kind == "sellmeier":
+            b = np.asarray(spec[1], dtype=np.float64).reshape(-1)
+            c = np.asarray(spec[2], dtype=np.float64).reshape(-1)
+            if b.size != c.size:
+                raise InvalidInputError("invalid input: Sellmeier: B and C must have the same "
+                                        f"length, got {b.size} and {c.size}")
+            tab = np.ascontiguousarray(np.concatenate([b, c]))
+            keep.append(tab)
+            r.n, r.p[3], r.table = b.size, float(spec[3]), _p(tab)
+        else:
+            wl = np.asarray(spec[1], dtype=np.float64).reshape(-1)
+            m = np.asarray(spec[2], dtype=np.complex128).reshape(-1)
+            if m.size != wl.size:
+                raise InvalidInputError("invalid input: a Table needs as many m as wavelengths")
+            tab = np.ascontiguousarray(np.concatenate([wl, m.view(np.float64)]))
+            keep.append(tab)
+            r.n, r.table = wl.size, _p(tab)
+    return recs, keep
+
+
+def refractive_parameter_count(spec) -> int:
+    recs, _keep = refractive_models([spec])
+    return int(load().scatrs_refractive_parameter_count(ctypes.byref(recs[0])))
+
+
+def refractive_index_device(specs, wl_ptr: int, n_wl: int, m_ptr: int, dm_ptr: int = 0,
+                            p_max: int = 0, stream: int = 0) -> None:
+    """m (complex [n_models][n_wl]) of every model at every wavelength into device memory, and
+    dm/dtheta (complex [n_models][p_max][n_wl]) when dm_ptr is given; synchronizes."""
+    recs, _keep = refractive_models(specs)
+    err = ctypes.create_string_buffer(1024)
+    st = load().scatrs_refractive_index_device(recs, len(specs), wl_ptr, n_wl, m_ptr,
+                                               dm_ptr or None, int(p_max), stream or None, err,
+                                               1024)
+    _check(st, err)

@@ -3672,53 +3672,102 @@ int scatrs_ensemble_fixed_mixed_device(const scatrs_distribution* dists_host, in
                       values_dev, phase_dev, greek_dev, stream, mixed, err, err_len);
 }
 
+}  // extern "C"
+
+namespace sb {
+namespace {
+// The wavelengths on the host for checks and messages: a copy of device ones.
+std::vector<double> host_wavelengths(const double* wl, int64_t n_wl, bool device, cudaStream_t s) {
+  std::vector<double> h(std::max<int64_t>(n_wl, 0));
+  if (n_wl <= 0) return h;
+  if (device) {
+    SB_CUDA(cudaMemcpyAsync(h.data(), wl, n_wl * 8, cudaMemcpyDeviceToHost, s));
+    SB_CUDA(cudaStreamSynchronize(s));
+  } else {
+    h.assign(wl, wl + n_wl);
+  }
+  for (int64_t i = 0; i < n_wl; ++i)
+    if (!(std::isfinite(h[i]) && h[i] > 0.0))
+      throw Failure{SCATRS_INVALID_INPUT, "wavelengths must be finite and > 0"};
+  return h;
+}
+
+// scatrs_ensemble_fixed_d with host (device = false) or device arrays.
+void fixed_d_impl(const scatrs_distribution* dists, int64_t n_dist, const double* wavelengths,
+                  int64_t n_wl, const double* m, const double* mu, int64_t n_mu,
+                  const scatrs_fixed_options* options, double* values, double* phase,
+                  double* greek, double* d_values, double* d_phase, double* d_greek, bool device,
+                  cudaStream_t s) {
+  if (n_dist < 0 || n_wl < 0) throw Failure{SCATRS_INVALID_INPUT, "negative sizes"};
+  DerivOutput dv;
+  dv.on = true;
+  dv.n_theta = n_dist > 0 ? parameter_count(dists[0].kind) : 2;
+  const int P = dv.n_theta + 2;
+  Context& c = context();
+  std::lock_guard<std::mutex> lk(c.mtx);
+  const std::vector<double> wl_host = host_wavelengths(wavelengths, n_wl, device, s);
+  const int64_t n_units = n_dist * n_wl;
+  check_options(options, n_units, n_mu, mu, P);
+  if (n_units == 0) return;
+  const cudaMemcpyKind in = device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  const cudaMemcpyKind out = device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  double* wl_d = c.wl.as<double>(n_wl);
+  double* m_d = c.m.as<double>(2 * n_units);
+  SB_CUDA(cudaMemcpyAsync(wl_d, wavelengths, n_wl * 8, in, s));
+  SB_CUDA(cudaMemcpyAsync(m_d, m, 2 * n_units * 8, in, s));
+  int64_t vl, pl, gl;
+  scatrs_ensemble_fixed_sizes(n_units, n_mu, options->greek_order, &vl, &pl, &gl);
+  if (device && ((pl > 0 && (!phase || !d_phase)) || (gl > 0 && (!greek || !d_greek)) ||
+                 !values || !d_values))
+    throw Failure{SCATRS_INVALID_INPUT,
+                  "the device entry needs every output array the options call for"};
+  // One allocation per output kind: the values, then the P derivative blocks.
+  double* v_d = c.values.as<double>(vl * (1 + P));
+  double* p_d = pl > 0 ? c.phase.as<double>(pl * (1 + P)) : nullptr;
+  double* g_d = gl > 0 ? c.greek.as<double>(gl * (1 + P)) : nullptr;
+  dv.d_values = v_d + vl;
+  dv.d_phase = p_d ? p_d + pl : nullptr;
+  dv.d_greek = g_d ? g_d + gl : nullptr;
+  FixedCall call;
+  call.wl_host = wl_host;
+  run_fixed(c, dists, n_dist, wl_d, n_wl, m_d, mu, n_mu, options, v_d, p_d, g_d, s, &call,
+            LayerInput(), dv);
+  check_device_errors(c, s, &call);
+  SB_CUDA(cudaMemcpyAsync(values, v_d, vl * 8, out, s));
+  if (d_values) SB_CUDA(cudaMemcpyAsync(d_values, dv.d_values, P * vl * 8, out, s));
+  if (pl > 0 && phase) SB_CUDA(cudaMemcpyAsync(phase, p_d, pl * 8, out, s));
+  if (pl > 0 && d_phase) SB_CUDA(cudaMemcpyAsync(d_phase, dv.d_phase, P * pl * 8, out, s));
+  if (gl > 0 && greek) SB_CUDA(cudaMemcpyAsync(greek, g_d, gl * 8, out, s));
+  if (gl > 0 && d_greek) SB_CUDA(cudaMemcpyAsync(d_greek, dv.d_greek, P * gl * 8, out, s));
+  SB_CUDA(cudaStreamSynchronize(s));
+}
+}  // namespace
+}  // namespace sb
+
+extern "C" {
+
 int scatrs_ensemble_fixed_d(const scatrs_distribution* dists, int64_t n_dist,
                             const double* wavelengths, int64_t n_wl, const double* m,
                             const double* mu, int64_t n_mu, const scatrs_fixed_options* options,
                             double* values, double* phase, double* greek, double* d_values,
                             double* d_phase, double* d_greek, char* err, size_t err_len) {
   return guarded(err, err_len, [&] {
-    if (n_dist < 0 || n_wl < 0) throw Failure{SCATRS_INVALID_INPUT, "negative sizes"};
-    for (int64_t i = 0; i < n_wl; ++i)
-      if (!(std::isfinite(wavelengths[i]) && wavelengths[i] > 0.0))
-        throw Failure{SCATRS_INVALID_INPUT, "wavelengths must be finite and > 0"};
-    DerivOutput dv;
-    dv.on = true;
-    dv.n_theta = n_dist > 0 ? parameter_count(dists[0].kind) : 2;
-    const int P = dv.n_theta + 2;
-    Context& c = context();
-    std::lock_guard<std::mutex> lk(c.mtx);
-    cudaStream_t s = 0;
-    const int64_t n_units = n_dist * n_wl;
-    check_options(options, n_units, n_mu, mu, P);
-    if (n_units == 0) return;
-    double* wl_d = c.wl.as<double>(n_wl);
-    double* m_d = c.m.as<double>(2 * n_units);
-    SB_CUDA(cudaMemcpyAsync(wl_d, wavelengths, n_wl * 8, cudaMemcpyHostToDevice, s));
-    SB_CUDA(cudaMemcpyAsync(m_d, m, 2 * n_units * 8, cudaMemcpyHostToDevice, s));
-    int64_t vl, pl, gl;
-    scatrs_ensemble_fixed_sizes(n_units, n_mu, options->greek_order, &vl, &pl, &gl);
-    // One allocation per output kind: the values, then the P derivative blocks.
-    double* v_d = c.values.as<double>(vl * (1 + P));
-    double* p_d = pl > 0 ? c.phase.as<double>(pl * (1 + P)) : nullptr;
-    double* g_d = gl > 0 ? c.greek.as<double>(gl * (1 + P)) : nullptr;
-    dv.d_values = v_d + vl;
-    dv.d_phase = p_d ? p_d + pl : nullptr;
-    dv.d_greek = g_d ? g_d + gl : nullptr;
-    FixedCall call;
-    call.wl_host.assign(wavelengths, wavelengths + n_wl);
-    run_fixed(c, dists, n_dist, wl_d, n_wl, m_d, mu, n_mu, options, v_d, p_d, g_d, s, &call,
-              LayerInput(), dv);
-    check_device_errors(c, s, &call);
-    SB_CUDA(cudaMemcpyAsync(values, v_d, vl * 8, cudaMemcpyDeviceToHost, s));
-    if (d_values) SB_CUDA(cudaMemcpyAsync(d_values, dv.d_values, P * vl * 8, cudaMemcpyDeviceToHost, s));
-    if (pl > 0 && phase) SB_CUDA(cudaMemcpyAsync(phase, p_d, pl * 8, cudaMemcpyDeviceToHost, s));
-    if (pl > 0 && d_phase)
-      SB_CUDA(cudaMemcpyAsync(d_phase, dv.d_phase, P * pl * 8, cudaMemcpyDeviceToHost, s));
-    if (gl > 0 && greek) SB_CUDA(cudaMemcpyAsync(greek, g_d, gl * 8, cudaMemcpyDeviceToHost, s));
-    if (gl > 0 && d_greek)
-      SB_CUDA(cudaMemcpyAsync(d_greek, dv.d_greek, P * gl * 8, cudaMemcpyDeviceToHost, s));
-    SB_CUDA(cudaStreamSynchronize(s));
+    fixed_d_impl(dists, n_dist, wavelengths, n_wl, m, mu, n_mu, options, values, phase, greek,
+                 d_values, d_phase, d_greek, false, 0);
+  });
+}
+
+int scatrs_ensemble_fixed_d_device(const scatrs_distribution* dists_host, int64_t n_dist,
+                                   const double* wavelengths_dev, int64_t n_wl,
+                                   const double* m_dev, const double* mu_host, int64_t n_mu,
+                                   const scatrs_fixed_options* options, double* values_dev,
+                                   double* phase_dev, double* greek_dev, double* d_values_dev,
+                                   double* d_phase_dev, double* d_greek_dev, void* stream,
+                                   char* err, size_t err_len) {
+  return guarded(err, err_len, [&] {
+    fixed_d_impl(dists_host, n_dist, wavelengths_dev, n_wl, m_dev, mu_host, n_mu, options,
+                 values_dev, phase_dev, greek_dev, d_values_dev, d_phase_dev, d_greek_dev, true,
+                 static_cast<cudaStream_t>(stream));
   });
 }
 
@@ -4241,42 +4290,49 @@ int scatrs_ensemble_fixed_layered(const scatrs_distribution* dists, int64_t n_di
   });
 }
 
-int scatrs_ensemble_fixed_layered_d(const scatrs_distribution* dists, int64_t n_dist,
-                                    const double* wavelengths, int64_t n_wl,
-                                    const scatrs_layers* layers, const double* mu, int64_t n_mu,
-                                    const scatrs_fixed_options* options, double* values,
-                                    double* phase, double* greek, double* d_values,
-                                    double* d_phase, double* d_greek, char* err,
-                                    size_t err_len) {
-  return guarded(err, err_len, [&] {
+}  // extern "C"
+
+namespace sb {
+namespace {
+// scatrs_ensemble_fixed_layered_d with host (device = false) or device arrays (the layers' m,
+// the wavelengths and the outputs).
+void fixed_layered_d_impl(const scatrs_distribution* dists, int64_t n_dist,
+                          const double* wavelengths, int64_t n_wl, const scatrs_layers* layers,
+                          const double* mu, int64_t n_mu, const scatrs_fixed_options* options,
+                          double* values, double* phase, double* greek, double* d_values,
+                          double* d_phase, double* d_greek, bool device, cudaStream_t s) {
+  {
     if (n_dist < 0 || n_wl < 0) throw Failure{SCATRS_INVALID_INPUT, "negative sizes"};
     if (!layers || layers->n_layers < 2 || !layers->fractions || !layers->m)
       throw Failure{SCATRS_INVALID_INPUT,
                     "layers must give n_layers >= 2, fractions and m (one layer: use "
                     "scatrs_ensemble_fixed_d)"};
-    for (int64_t i = 0; i < n_wl; ++i)
-      if (!(std::isfinite(wavelengths[i]) && wavelengths[i] > 0.0))
-        throw Failure{SCATRS_INVALID_INPUT, "wavelengths must be finite and > 0"};
     const int L = layers->n_layers;
     if (L > kMaxLayersAbi) throw Failure{SCATRS_INVALID_INPUT, "the GPU path takes 1 to 16 layers"};
     const int P_th = n_dist > 0 ? parameter_count(dists[0].kind) : 2;
     const int P = P_th + 2 * L + (L - 1);
     Context& c = context();
     std::lock_guard<std::mutex> lk(c.mtx);
-    cudaStream_t s = 0;
+    const std::vector<double> wl_host = host_wavelengths(wavelengths, n_wl, device, s);
+    const cudaMemcpyKind in = device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    const cudaMemcpyKind out = device ? cudaMemcpyDeviceToDevice : out;
     const int64_t n_units = n_dist * n_wl;
     check_options(options, n_units, n_mu, mu, P);
     if (n_units == 0) return;
     double* wl_d = c.wl.as<double>(n_wl);
-    SB_CUDA(cudaMemcpyAsync(wl_d, wavelengths, n_wl * 8, cudaMemcpyHostToDevice, s));
+    SB_CUDA(cudaMemcpyAsync(wl_d, wavelengths, n_wl * 8, in, s));
     LayerInput li;
     li.n_layers = L;
     li.fractions = layers->fractions;
     double* m_d = c.m.as<double>(2 * n_dist * L * n_wl);
-    SB_CUDA(cudaMemcpyAsync(m_d, layers->m, 2 * n_dist * L * n_wl * 8, cudaMemcpyHostToDevice, s));
+    SB_CUDA(cudaMemcpyAsync(m_d, layers->m, 2 * n_dist * L * n_wl * 8, in, s));
     li.m_dev = m_d;
     int64_t vl, pl, gl;
     scatrs_ensemble_fixed_sizes(n_units, n_mu, options->greek_order, &vl, &pl, &gl);
+    if (device && ((pl > 0 && (!phase || !d_phase)) || (gl > 0 && (!greek || !d_greek)) ||
+                   !values || !d_values))
+      throw Failure{SCATRS_INVALID_INPUT,
+                    "the device entry needs every output array the options call for"};
     const int Pp = P_th + 2;  // blocks of one pass: the parameters, then the direction and i x it
     double* v_d = c.values.as<double>(vl * (1 + Pp));
     double* p_d = pl > 0 ? c.phase.as<double>(pl * (1 + Pp)) : nullptr;
@@ -4293,28 +4349,28 @@ int scatrs_ensemble_fixed_layered_d(const scatrs_distribution* dists, int64_t n_
       dv.d_phase = p_d ? p_d + pl : nullptr;
       dv.d_greek = g_d ? g_d + gl : nullptr;
       FixedCall call;
-      call.wl_host.assign(wavelengths, wavelengths + n_wl);
+      call.wl_host = wl_host;
       run_fixed(c, dists, n_dist, wl_d, n_wl, m_d, mu, n_mu, options, v_d, p_d, g_d, s, &call, li,
                 dv);
       check_device_errors(c, s, &call);
       auto take = [&](int from, int to) {
         if (d_values)
           SB_CUDA(cudaMemcpyAsync(d_values + to * vl, dv.d_values + from * vl, vl * 8,
-                                  cudaMemcpyDeviceToHost, s));
+                                  out, s));
         if (pl > 0 && d_phase)
           SB_CUDA(cudaMemcpyAsync(d_phase + to * pl, dv.d_phase + from * pl, pl * 8,
-                                  cudaMemcpyDeviceToHost, s));
+                                  out, s));
         if (gl > 0 && d_greek)
           SB_CUDA(cudaMemcpyAsync(d_greek + to * gl, dv.d_greek + from * gl, gl * 8,
-                                  cudaMemcpyDeviceToHost, s));
+                                  out, s));
       };
       if (g == 0) {
         for (int p = 0; p < P_th; ++p) take(p, p);
-        SB_CUDA(cudaMemcpyAsync(values, v_d, vl * 8, cudaMemcpyDeviceToHost, s));
+        SB_CUDA(cudaMemcpyAsync(values, v_d, vl * 8, out, s));
         if (pl > 0 && phase)
-          SB_CUDA(cudaMemcpyAsync(phase, p_d, pl * 8, cudaMemcpyDeviceToHost, s));
+          SB_CUDA(cudaMemcpyAsync(phase, p_d, pl * 8, out, s));
         if (gl > 0 && greek)
-          SB_CUDA(cudaMemcpyAsync(greek, g_d, gl * 8, cudaMemcpyDeviceToHost, s));
+          SB_CUDA(cudaMemcpyAsync(greek, g_d, gl * 8, out, s));
       }
       if (g < L) {
         take(P_th, P_th + 2 * g);
@@ -4324,6 +4380,39 @@ int scatrs_ensemble_fixed_layered_d(const scatrs_distribution* dists, int64_t n_
       }
       SB_CUDA(cudaStreamSynchronize(s));
     }
+  }
+}
+}  // namespace
+}  // namespace sb
+
+extern "C" {
+
+int scatrs_ensemble_fixed_layered_d(const scatrs_distribution* dists, int64_t n_dist,
+                                    const double* wavelengths, int64_t n_wl,
+                                    const scatrs_layers* layers, const double* mu, int64_t n_mu,
+                                    const scatrs_fixed_options* options, double* values,
+                                    double* phase, double* greek, double* d_values,
+                                    double* d_phase, double* d_greek, char* err,
+                                    size_t err_len) {
+  return guarded(err, err_len, [&] {
+    fixed_layered_d_impl(dists, n_dist, wavelengths, n_wl, layers, mu, n_mu, options, values,
+                         phase, greek, d_values, d_phase, d_greek, false, 0);
+  });
+}
+
+int scatrs_ensemble_fixed_layered_d_device(const scatrs_distribution* dists_host,
+                                           int64_t n_dist, const double* wavelengths_dev,
+                                           int64_t n_wl, const scatrs_layers* layers,
+                                           const double* mu_host, int64_t n_mu,
+                                           const scatrs_fixed_options* options,
+                                           double* values_dev, double* phase_dev,
+                                           double* greek_dev, double* d_values_dev,
+                                           double* d_phase_dev, double* d_greek_dev,
+                                           void* stream, char* err, size_t err_len) {
+  return guarded(err, err_len, [&] {
+    fixed_layered_d_impl(dists_host, n_dist, wavelengths_dev, n_wl, layers, mu_host, n_mu,
+                         options, values_dev, phase_dev, greek_dev, d_values_dev, d_phase_dev,
+                         d_greek_dev, true, static_cast<cudaStream_t>(stream));
   });
 }
 
