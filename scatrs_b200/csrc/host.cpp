@@ -115,11 +115,15 @@ void set_err(char* err, size_t len, const std::string& msg) {
   }
 }
 
+// A failed runtime call becomes a SCATRS_CUDA failure; its error is also cleared from the
+// runtime's last-error state, so that the next call does not report it again.
 #define SB_CUDA(call)                                                                        \
   do {                                                                                       \
     cudaError_t e_ = (call);                                                                 \
-    if (e_ != cudaSuccess)                                                                   \
+    if (e_ != cudaSuccess) {                                                                 \
+      cudaGetLastError();                                                                    \
       throw Failure{SCATRS_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)};        \
+    }                                                                                        \
   } while (0)
 
 int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
@@ -417,7 +421,7 @@ BandTables& ensure_bands(Context& c, int L, int last_band, cudaStream_t s) {
 
 // The digits of one table of the mixed form (kernels.h): pairs [0, h) whose E and O rows over
 // orders 0 .. n_orders - 1 row(pair, e, o) writes (zero beyond), in M tiles of kI8Pairs pairs
-// (E rows, then the same pairs' O rows) and n_kb K blocks; each MMA row's power of two 2^e puts
+// (MMA rows 2p and 2p + 1: the E and O rows of the tile's pair p) and n_kb K blocks; each MMA row's power of two 2^e puts
 // its largest |value| below 127 2^-e (in [63.5, 127) 2^-e), and F = rint(value 2^(e + 32))
 // goes out as its five balanced digits (each in [-128, 127]: the low ones the sign-extended low
 // byte of what is left) into the 64-byte swizzle (16-byte chunk q of row r at chunk
@@ -443,7 +447,7 @@ I8Table i8_table(int h, int64_t n_orders, int n_kb, Row row, std::vector<unsigne
       row(pair, std::min<int64_t>(n_orders, K), e_row.data(), o_row.data());
       for (int side = 0; side < 2; ++side) {
         const std::vector<double>& v = side ? o_row : e_row;
-        const int r = side * kI8Pairs + pp;
+        const int r = 2 * pp + side;  // a pair's E and O rows side by side
         double m = 0.0;
         for (int64_t k = 0; k < K; ++k) m = std::max(m, std::fabs(v[k]));
         if (!(m > 0.0)) continue;
@@ -4315,7 +4319,7 @@ void fixed_layered_d_impl(const scatrs_distribution* dists, int64_t n_dist,
     std::lock_guard<std::mutex> lk(c.mtx);
     const std::vector<double> wl_host = host_wavelengths(wavelengths, n_wl, device, s);
     const cudaMemcpyKind in = device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-    const cudaMemcpyKind out = device ? cudaMemcpyDeviceToDevice : out;
+    const cudaMemcpyKind out = device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
     const int64_t n_units = n_dist * n_wl;
     check_options(options, n_units, n_mu, mu, P);
     if (n_units == 0) return;

@@ -155,7 +155,7 @@ struct ProjArgs {
 constexpr int kI8Levels = 5;         // digits per value
 constexpr int kI8MaxLevels = 6;      // product levels kept at most (i + j < 6: 19 products)
 constexpr int kI8KB = 64;            // orders per K block (a row of the 64-byte swizzle)
-constexpr int kI8Pairs = 64;         // angle pairs per M tile: 128 MMA rows, E rows then O rows
+constexpr int kI8Pairs = 64;         // angle pairs per M tile: 128 MMA rows, E and O per pair
 constexpr int kI8MaxTerms = 4096;    // the INT32 level sums stay exact up to this many orders
 constexpr int kI8TileBytes = kI8Levels * 128 * kI8KB;  // one (M tile, K block): 40 KiB
 constexpr int kI8HalfBytes = kI8Levels * 64 * kI8KB;   // one (16-node half, K block): 20 KiB

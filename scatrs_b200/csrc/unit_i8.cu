@@ -16,11 +16,12 @@
 // is 64 angle pairs: 64 rows of G_E, then the same pairs' 64 rows of G_O. Warp 0 streams each
 // job's K blocks (64 orders: the table's 5 digit slices of 128 rows and the chunk half's 5 slices
 // of 64 columns, 60 KiB laid out in the 64-byte swizzle by the digit builders) with bulk copies
-// into three stages; warp 1 issues the 15 products of every 32-order K step; warps 2-5 read the
-// five level accumulators of their 32 lanes back, free the tensor memory for the next job's
-// MMAs, and form the phase-matrix elements at +mu (E rows' threads) and -mu (O rows' threads)
-// after exchanging the E and O sums of each pair through shared memory. Every output sum has
-// one owner thread and runs over the chunks in order. Every wait is bounded: on a timeout the
+// into three stages; warp 1 issues the 15 products of every 32-order K step; warps 2-9 (two
+// warpgroups, each half of the job's columns) read the level accumulators of their 32 lanes
+// back, free the tensor memory for the next job's MMAs, and form the phase-matrix elements at
+// +mu (E rows' threads) and -mu (O rows' threads), the pair's E and O rows being neighbouring
+// lanes (an M tile's rows 2p, 2p + 1). Every output sum has one owner thread and runs over the
+// chunks in order. Every wait is bounded: on a timeout the
 // kernel sets *err, every role stops, and the tensor memory is freed.
 #include <cuda_runtime.h>
 
@@ -33,7 +34,7 @@ namespace sb {
 namespace {
 
 constexpr double kPi = 3.14159265358979323846264338327950288;
-constexpr int kThreads = 192;
+constexpr int kThreads = 320;  // warp 0 copies, warp 1 MMAs, warps 2-9 the epilogue
 constexpr int kStages = 3;
 constexpr int kASlice = 128 * kI8KB;                                // 8 KiB
 constexpr int kBSlice = 64 * kI8KB;                                 // 4 KiB
@@ -42,7 +43,7 @@ constexpr uint32_t kTmemCols = 512;
 constexpr long long kSpinCycles = 4000000000LL;  // about 2 s at the B200's clocks
 
 struct I8Smem {
-  double xbuf[128][17];  // one group's 16 sums per row, exchanged between a pair's E and O rows
+  double red[2][128][4];  // warpgroup 1's sums per row, handed to warpgroup 0
   double w[32], cu[32], area[32], sc[32];
   double cs[128];        // the chunk's column scales
   unsigned long long full[kStages], empty[kStages], tmem_full, tmem_empty, drained;
@@ -160,7 +161,7 @@ __device__ __forceinline__ void balanced_digits(long long f, int d[kI8Levels]) {
   }
   d[0] = (int)f;
 }
-__device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 1, 128;\n" ::: "memory"); }
+__device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 1, 256;\n" ::: "memory"); }
 
 __device__ __forceinline__ void elements4(double s1r, double s1i, double s2r, double s2i,
                                           double e[4]) {
@@ -224,6 +225,7 @@ __device__ __forceinline__ const I8Table& job_table(const UnitI8Args& a, const J
 
 }  // namespace
 
+template <int LEV>
 __global__ void __launch_bounds__(kThreads, 1) unit_i8_kernel(UnitI8Args a) {
   extern __shared__ __align__(1024) unsigned char i8_raw[];
   unsigned char* stages =
@@ -236,7 +238,7 @@ __global__ void __launch_bounds__(kThreads, 1) unit_i8_kernel(UnitI8Args a) {
       mbar_init(&sm.empty[i], 1);
     }
     mbar_init(&sm.tmem_full, 1);
-    mbar_init(&sm.tmem_empty, 128);
+    mbar_init(&sm.tmem_empty, 256);
     mbar_init(&sm.drained, 1);
     sm.abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
@@ -284,7 +286,7 @@ __global__ void __launch_bounds__(kThreads, 1) unit_i8_kernel(UnitI8Args a) {
     if (lane == 0) {
       int it = 0, job = 0;
       const uint32_t idesc = idesc_i8();
-      const int n_lev = a.levels;
+      constexpr int n_lev = LEV;
       for_each_job(a, [&](const Job& j) {
         if (job > 0 && !mbar_wait(&sm.tmem_empty, (job - 1) & 1, sm, a.err)) return false;
         asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
@@ -322,11 +324,15 @@ __global__ void __launch_bounds__(kThreads, 1) unit_i8_kernel(UnitI8Args a) {
       mbar_wait_drain(&sm.drained, 0, a.err);
     }
   } else {
-    // Epilogue: warps 2-5; lane quarter (w & 3) of the accumulators, row r.
+    // Epilogue: warps 2-9, two warpgroups; warp w reads lane quarter (w & 3) of the
+    // accumulators (row r) and the columns of its warpgroup e: nodes 8 e .. 8 e + 7 of the job's
+    // 16-node half. Row r is pair r >> 1's E row (r even) or O row (r odd), so that a pair's two
+    // rows are neighbouring lanes.
     const int r = 32 * (w & 3) + lane;
-    const int side = r >= 64 ? 1 : 0;  // 0: E row, elements at +mu; 1: O row, at -mu
-    const int p = r & 63;              // the angle pair within the tile
-    const int e_thread = t - 64;       // 0 .. 127
+    const int e = (w - 2) >> 2;
+    const int side = r & 1;            // 0: E row, elements at +mu; 1: O row, at -mu
+    const int p = r >> 1;              // the angle pair within the tile
+    const int e_thread = t - 64;       // 0 .. 255
     const int t_user = (a.h_u + kI8Pairs - 1) / kI8Pairs;
     int job = 0;
     int64_t cur = -1;
@@ -352,8 +358,9 @@ __global__ void __launch_bounds__(kThreads, 1) unit_i8_kernel(UnitI8Args a) {
           sm.cu[e_thread] = cu;
           sm.area[e_thread] = ar;
           sm.sc[e_thread] = sc;
+        } else if (e_thread < 160) {
+          sm.cs[e_thread - 32] = a.xscale[(int64_t)a.chunk_xidx[j.ci] * 128 + e_thread - 32];
         }
-        sm.cs[e_thread] = a.xscale[(int64_t)a.chunk_xidx[j.ci] * 128 + e_thread];
         epi_sync();
         cur = j.ci;
       }
@@ -365,35 +372,33 @@ __global__ void __launch_bounds__(kThreads, 1) unit_i8_kernel(UnitI8Args a) {
       epi_sync();
       if (sm.stop) return false;
       asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-      // The five levels of this row's 64 columns, recombined in FP64.
-      double v[64];
-      const uint32_t lane_base = tmem + ((uint32_t)(32 * (w & 3)) << 16);
-      const int n_lev = a.levels;
+      // The kept levels of this row's 32 columns, recombined in FP64.
+      double v[32];
+      const uint32_t lane_base = tmem + ((uint32_t)(32 * (w & 3)) << 16) + (uint32_t)(32 * e);
 #pragma unroll
-      for (int g = 0; g < 4; ++g) {
+      for (int g = 0; g < 2; ++g) {
+        uint32_t q[LEV][16];
 #pragma unroll
-        for (int s = kI8MaxLevels - 1; s >= 0; --s) {
-          if (s >= n_lev) continue;
-          uint32_t q[16];
+        for (int s = 0; s < LEV; ++s) {
           asm volatile(
               "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, "
               "%10, %11, %12, %13, %14, %15}, [%16];\n"
-              : "=r"(q[0]), "=r"(q[1]), "=r"(q[2]), "=r"(q[3]), "=r"(q[4]), "=r"(q[5]),
-                "=r"(q[6]), "=r"(q[7]), "=r"(q[8]), "=r"(q[9]), "=r"(q[10]), "=r"(q[11]),
-                "=r"(q[12]), "=r"(q[13]), "=r"(q[14]), "=r"(q[15])
+              : "=r"(q[s][0]), "=r"(q[s][1]), "=r"(q[s][2]), "=r"(q[s][3]), "=r"(q[s][4]),
+                "=r"(q[s][5]), "=r"(q[s][6]), "=r"(q[s][7]), "=r"(q[s][8]), "=r"(q[s][9]),
+                "=r"(q[s][10]), "=r"(q[s][11]), "=r"(q[s][12]), "=r"(q[s][13]), "=r"(q[s][14]),
+                "=r"(q[s][15])
               : "r"(lane_base + (uint32_t)(s * 64 + g * 16)));
-          asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-          const double f = s == 0   ? 1.0
-                           : s == 1 ? 0x1p-8
-                           : s == 2 ? 0x1p-16
-                           : s == 3 ? 0x1p-24
-                           : s == 4 ? 0x1p-32
-                                    : 0x1p-40;
+        }
+        asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 #pragma unroll
-          for (int k = 0; k < 16; ++k) {
-            const double dv = i32_to_f64(q[k]);
-            v[g * 16 + k] = s == n_lev - 1 ? dv * f : fma(dv, f, v[g * 16 + k]);
-          }
+        for (int k = 0; k < 16; ++k) {
+          double acc = 0.0;
+          if constexpr (LEV == 6) acc = i32_to_f64(q[5][k]) * 0x1p-40;
+          acc = fma(i32_to_f64(q[4][k]), 0x1p-32, acc);
+          acc = fma(i32_to_f64(q[3][k]), 0x1p-24, acc);
+          acc = fma(i32_to_f64(q[2][k]), 0x1p-16, acc);
+          acc = fma(i32_to_f64(q[1][k]), 0x1p-8, acc);
+          v[g * 16 + k] = i32_to_f64(q[0][k]) + acc;
         }
       }
       // The accumulators are free for the next job's MMAs.
@@ -403,60 +408,63 @@ __global__ void __launch_bounds__(kThreads, 1) unit_i8_kernel(UnitI8Args a) {
       const I8Table& tab = job_table(a, j, tl);
       const double rs = a.tscale[tab.scale_off + (int64_t)tl * 128 + r];
       const bool user = j.tile < t_user;
+      const double sg = side ? -1.0 : 1.0;
 #pragma unroll
-      for (int g = 0; g < 4; ++g) {
-        epi_sync();  // the previous group's readers are done with xbuf
+      for (int nd = 0; nd < 8; ++nd) {
+        // Columns u.re, u.im, v.re, v.im of node 8 e + nd of the half; the pair's other row from
+        // the neighbouring lane. S1 = E_u +- O_v, S2 = E_v +- O_u (fast.rs:151-204).
+        double mine[4], other[4], E[4], O[4];
 #pragma unroll
-        for (int k = 0; k < 16; ++k) {
-          v[g * 16 + k] *= rs * sm.cs[j.half * 64 + g * 16 + k];
-          sm.xbuf[r][k] = v[g * 16 + k];
+        for (int k = 0; k < 4; ++k) {
+          mine[k] = v[4 * nd + k] * (rs * sm.cs[j.half * 64 + 32 * e + 4 * nd + k]);
+          other[k] = __shfl_xor_sync(0xffffffffu, mine[k], 1);
+          E[k] = side ? other[k] : mine[k];
+          O[k] = side ? mine[k] : other[k];
         }
-        epi_sync();
-        const double sg = side ? -1.0 : 1.0;
+        double el[4];
+        elements4(E[0] + sg * O[2], E[1] + sg * O[3], E[2] + sg * O[0], E[3] + sg * O[1], el);
+        const int node = j.half * 16 + 8 * e + nd;
+        const double wt = sm.w[node], cu = sm.cu[node], ar = sm.area[node], sc = sm.sc[node];
 #pragma unroll
-        for (int nd = 0; nd < 4; ++nd) {
-          const int node = j.half * 16 + g * 4 + nd;
-          double E[4], O[4];
-#pragma unroll
-          for (int k = 0; k < 4; ++k) {
-            const double mine = v[g * 16 + 4 * nd + k], other = sm.xbuf[r ^ 64][4 * nd + k];
-            E[k] = side ? other : mine;
-            O[k] = side ? mine : other;
-          }
-          // Columns: u.re, u.im, v.re, v.im; S1 = E_u +- O_v, S2 = E_v +- O_u (fast.rs:151-204).
-          double e[4];
-          elements4(E[0] + sg * O[2], E[1] + sg * O[3], E[2] + sg * O[0], E[3] + sg * O[1], e);
-          const double wt = sm.w[node], cu = sm.cu[node], ar = sm.area[node], sc = sm.sc[node];
-#pragma unroll
-          for (int k = 0; k < 4; ++k) out[k] += user ? wt * ((cu * e[k]) * ar) : wt * (sc * e[k]);
-        }
+        for (int k = 0; k < 4; ++k) out[k] += user ? wt * ((cu * el[k]) * ar) : wt * (sc * el[k]);
       }
       if (j.half == 1) {
-        // The job pair's sums into this row's (pair, side) accumulators.
-        int jo = -1;
-        int64_t len;
-        double* base;
-        if (user) {
-          const int row = j.tile * kI8Pairs + p;
-          if (row < a.h_u) {
-            const int2 mp = a.user_map[row];
-            jo = side ? mp.y : mp.x;
-          }
-          len = a.n_mu;
-          base = a.acc + a.unit_acc[j.ul];
-        } else {
-          const BandDesc B = a.bands[j.b];
-          const int row = (j.tile - t_user) * kI8Pairs + p;
-          if (row < B.h) {
-            const int q = B.n_q, jn = q / 2 + row, mirror = q - 1 - jn;
-            if (side == 0 || mirror != jn) jo = side ? mirror : jn;
-          }
-          len = B.n_q;
-          base = a.acc + a.chunk_acc[j.ci];
-        }
-        if (jo >= 0)
+        // The job pair's sums into this row's (pair, side) accumulators: warpgroup 1 hands its
+        // sums to warpgroup 0 through shared memory (two buffers, one per parity of the pair).
+        const int buf = (job >> 1) & 1;
+        if (e == 1) {
 #pragma unroll
-          for (int k = 0; k < 4; ++k) base[k * len + jo] += out[k];
+          for (int k = 0; k < 4; ++k) sm.red[buf][r][k] = out[k];
+        }
+        epi_sync();
+        if (e == 0) {
+#pragma unroll
+          for (int k = 0; k < 4; ++k) out[k] += sm.red[buf][r][k];
+          int jo = -1;
+          int64_t len;
+          double* base;
+          if (user) {
+            const int row = j.tile * kI8Pairs + p;
+            if (row < a.h_u) {
+              const int2 mp = a.user_map[row];
+              jo = side ? mp.y : mp.x;
+            }
+            len = a.n_mu;
+            base = a.acc + a.unit_acc[j.ul];
+          } else {
+            const BandDesc B = a.bands[j.b];
+            const int row = (j.tile - t_user) * kI8Pairs + p;
+            if (row < B.h) {
+              const int qn = B.n_q, jn = qn / 2 + row, mirror = qn - 1 - jn;
+              if (side == 0 || mirror != jn) jo = side ? mirror : jn;
+            }
+            len = B.n_q;
+            base = a.acc + a.chunk_acc[j.ci];
+          }
+          if (jo >= 0)
+#pragma unroll
+            for (int k = 0; k < 4; ++k) base[k * len + jo] += out[k];
+        }
 #pragma unroll
         for (int k = 0; k < 4; ++k) out[k] = 0.0;
       }
@@ -532,12 +540,19 @@ cudaError_t launch_units_i8(const UnitI8Args& a, int grid, cudaStream_t s) {
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev >= 0 && dev < 64 && !configured[dev]) {
-    cudaError_t e = cudaFuncSetAttribute(unit_i8_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)units_i8_smem());
-    if (e != cudaSuccess) return e;
+    for (auto f : {unit_i8_kernel<5>, unit_i8_kernel<6>}) {
+      cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)units_i8_smem());
+      if (e != cudaSuccess) return e;
+    }
     configured[dev] = true;
   }
-  if (grid > 0) unit_i8_kernel<<<grid, kThreads, units_i8_smem(), s>>>(a);
+  if (grid > 0) {
+    if (a.levels == 6)
+      unit_i8_kernel<6><<<grid, kThreads, units_i8_smem(), s>>>(a);
+    else
+      unit_i8_kernel<5><<<grid, kThreads, units_i8_smem(), s>>>(a);
+  }
   return cudaGetLastError();
 }
 

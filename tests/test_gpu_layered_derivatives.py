@@ -1,8 +1,8 @@
 """Derivatives of the layered-sphere ensemble on the GPU (scatrs_ensemble_fixed_layered_d: the
 layered recursion carried in forward mode, one derivative pass per layer index and per radius
 fraction) against Richardson-extrapolated central differences of the oracle's layered ensemble
-(an independent double-precision restatement; steps 1e-3 and 5e-4 relative, so the differences'
-truncation error is O(h^4)): the scalars, phase matrix and Greek coefficients along the
+(an independent double-precision restatement; steps 2e-5 and 1e-5 relative, so the differences'
+truncation error is O(h^4); larger steps cross the layered recursion's switches between forms): the scalars, phase matrix and Greek coefficients along the
 distribution's parameters, Re m_l and Im m_l of every layer and the fractions, within 1e-6 of
 each output row's scale. Values equal the plain layered ensemble. The derivatives themselves are
 pinned to the reference's Arb records in test_gpu_derivative_pins.py."""
@@ -78,7 +78,7 @@ def test_matches_finite_differences(gpu):
                 (vm, phm, gm), _ = perturbed(-1, rel)
                 return [(p_ - m_) / (2 * h) for p_, m_ in ((vp, vm), (php, phm), (gp, gm))]
 
-            coarse, fine = central(1e-3), central(5e-4)
+            coarse, fine = central(2e-5), central(1e-5)
             sl = slice(dist * n_wl, (dist + 1) * n_wl)
             for got, dc, df in zip((dv[blk], dph[blk], dg[blk]), coarse, fine):
                 fd = (4.0 * df - dc) / 3.0  # Richardson: the h^2 terms cancel

@@ -57,3 +57,21 @@ def test_tensor_core_projection_matches_fp64(gpu):
     err = np.abs(tc - ref) / size
     assert err.max() <= 2e-5, err.max()
     assert err.max() > 0.0  # the tensor-core form ran (it differs from FP64 by rounding)
+
+
+def test_tensor_core_projection_at_the_large_droplet_shape(gpu):
+    """The large-droplet configuration's own shape: 4096 Gauss cosines, order 1024, on the
+    ensemble's own phase tables (gamma distributions of effective radius 5-20 um, x up to about
+    300), the 3xTF32 form against the FP64 form. The stated tolerance is 2e-5 of each table's
+    largest coefficient (TF32 heads and tails, the tensor cores' FP32 accumulation over 4096
+    cosines)."""
+    w = W.large_droplets(seed=0, scale=0.02, n_q=4096)  # 3 distributions x 5 wavelengths
+    L = 1024
+    phase, _ = _ensemble_on_device(w, w.mu, -1)
+    ref = _project(phase, w.n_units, w.mu.size, L, 0)
+    tc = _project(phase, w.n_units, w.mu.size, L, 1)
+    size = np.abs(ref).max(axis=(0, 2), keepdims=True)
+    err = np.abs(tc - ref) / size
+    print(f"3xTF32 at n_q = 4096, L = 1024: max error {err.max():.3e} of the largest "
+          "coefficient")
+    assert err.max() <= 2e-5, err.max()
