@@ -212,7 +212,7 @@ struct Context {
     std::vector<I8Table> user, band;
     DevBuf dig, scale, user_d, band_d;
   } i8;
-  DevBuf xdig, xscale, chunk_xoff, chunk_xidx, i8_list, i8_err;
+  DevBuf xdig, xside, chunk_xoff, chunk_xidx, i8_list, i8_err;
   // Spheroid T-matrices.
   DevBuf tm_geoms, tm_jobs, tm_rules, tm_node, tm_rad, tm_ang, tm_J, tm_work, tm_piv, tm_T, tm_sums,
       tm_err;
@@ -953,13 +953,13 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
   int* chunk_xidx_d = nullptr;
   int* i8_list_d = nullptr;
   unsigned char* xdig = nullptr;
-  double* xscale = nullptr;
+  double* xside = nullptr;
   if (i8_above > 0) {
     chunk_xoff_d = c.chunk_xoff.as<int64_t>(n_chunks);
     chunk_xidx_d = c.chunk_xidx.as<int>(n_chunks);
     i8_list_d = c.i8_list.as<int>(n_chunks);
     xdig = c.xdig.as<unsigned char>((size_t)i8_bytes_max);
-    xscale = c.xscale.as<double>((size_t)i8_chunks_max * 128);
+    xside = c.xside.as<double>((size_t)i8_chunks_max * kI8Side);
   }
   c.ensure_staging((size_t)stage_max);
   // 4. Per slab: build its plan into pinned staging, upload it, launch its kernels. The host
@@ -1253,7 +1253,14 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
       xa.chunk_xoff = chunk_xoff_d + ch0;
       xa.chunk_xidx = chunk_xidx_d + ch0;
       xa.xdig = xdig;
-      xa.xscale = xscale;
+      xa.xside = xside;
+      xa.radius = ua.radius;
+      xa.weight = ua.weight;
+      xa.wl = wl_dev;
+      xa.units = ua.units;
+      xa.n_wl = (int)n_wl;
+      xa.n_nodes = (int)n_nodes;
+      xa.cpu = cpu;
       timed_launch(K_X_SPLIT, s, [&] { launch_x_split(xa, s); });
       SB_CUDA(cudaGetLastError());
       UnitI8Args ia{};
@@ -1279,7 +1286,7 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
       ia.chunk_xoff = xa.chunk_xoff;
       ia.chunk_xidx = xa.chunk_xidx;
       ia.xdig = xdig;
-      ia.xscale = xscale;
+      ia.xside = xside;
       ia.tdig = c.i8.dig.as<unsigned char>(0);
       ia.tscale = c.i8.scale.as<double>(0);
       ia.user_tabs = c.i8.user_d.as<I8Table>(0);
@@ -4620,7 +4627,7 @@ void scatrs_release(void) {
                       &c.X, &c.uz, &c.ux, &c.chunk_sums, &c.err, &c.acc,
                       &c.counter, &c.values, &c.phase, &c.greek, &c.user.ge, &c.user.go,
                       &c.user.map, &c.tc_a_hi, &c.tc_a_lo, &c.tc_prod, &c.tc_err, &c.xdig,
-                      &c.xscale, &c.chunk_xoff, &c.chunk_xidx, &c.i8_list, &c.i8_err,
+                      &c.xside, &c.chunk_xoff, &c.chunk_xidx, &c.i8_list, &c.i8_err,
                       &c.i8.dig, &c.i8.scale, &c.i8.user_d, &c.i8.band_d})
       b->release();
     for (auto& kv : c.projectors)

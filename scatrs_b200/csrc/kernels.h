@@ -159,6 +159,7 @@ constexpr int kI8Pairs = 64;         // angle pairs per M tile: 128 MMA rows, E 
 constexpr int kI8MaxTerms = 4096;    // the INT32 level sums stay exact up to this many orders
 constexpr int kI8TileBytes = kI8Levels * 128 * kI8KB;  // one (M tile, K block): 40 KiB
 constexpr int kI8HalfBytes = kI8Levels * 64 * kI8KB;   // one (16-node half, K block): 20 KiB
+constexpr int kI8Side = 160;  // per int8 chunk: its 128 column scales, then 32 node factors
 
 // Where one table's digits live: M tile t, K block kb, digit s, row r at
 // off + ((t * n_kb + kb) * kI8Levels + s) * 8192 + r * 64 (64-byte swizzle inside the row), its
@@ -189,11 +190,12 @@ struct UnitI8Args {
   const BandDesc* bands;
   double* acc;
   // Chunk digits: per slab-local chunk the byte offset of its digits ((half, K block) blocks of
-  // kI8HalfBytes) or -1 when it is not on this path, and the index of its 128 column scales.
+  // kI8HalfBytes) or -1 when it is not on this path, and the index of its side record (kI8Side
+  // doubles: the 128 column scales, then the nodes' factors w 4 pi r^2 / x^2).
   const int64_t* chunk_xoff;
   const int* chunk_xidx;
   const unsigned char* xdig;
-  const double* xscale;
+  const double* xside;
   // Table digits: the requested cosines' tables in versions v (orders < 64 2^v, their rows'
   // scales over those orders), then one table per band.
   const unsigned char* tdig;
@@ -215,7 +217,13 @@ struct XSplitArgs {
   const int64_t* chunk_xoff;
   const int* chunk_xidx;
   unsigned char* xdig;
-  double* xscale;
+  double* xside;
+  // The nodes, for the side record's node factors.
+  const double* radius;
+  const double* weight;
+  const double* wl;
+  const int* units;
+  int n_wl, n_nodes, cpu;
 };
 
 void launch_x_split(const XSplitArgs& a, cudaStream_t s);

@@ -43,10 +43,10 @@ constexpr uint32_t kTmemCols = 512;
 constexpr long long kSpinCycles = 4000000000LL;  // about 2 s at the B200's clocks
 
 struct I8Smem {
+  alignas(16) double side[2][kI8Side];  // two chunks' side records (column scales, node factors)
   double red[2][128][4];  // warpgroup 1's sums per row, handed to warpgroup 0
-  double w[32], cu[32], area[32], sc[32];
-  double cs[128];        // the chunk's column scales
-  unsigned long long full[kStages], empty[kStages], tmem_full, tmem_empty, drained;
+  unsigned long long full[kStages], empty[kStages], side_full[2], side_empty[2], tmem_full,
+      tmem_empty, drained;
   uint32_t tmem_base;
   int abort;
   int stop;  // the epilogue warps' common decision to stop
@@ -65,6 +65,11 @@ __device__ __forceinline__ void mbar_expect_tx(unsigned long long* b, uint32_t b
 }
 __device__ __forceinline__ void mbar_arrive(unsigned long long* b) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(b)) : "memory");
+}
+// One arrival for the calling warp, after all its lanes got here.
+__device__ __forceinline__ void warp_arrive(unsigned long long* b) {
+  __syncwarp();
+  if ((threadIdx.x & 31) == 0) mbar_arrive(b);
 }
 // A bounded wait on phase `parity`: false if it gave up (then *err and sm.abort are set) or if
 // another role gave up first.
@@ -173,6 +178,32 @@ __device__ __forceinline__ void elements4(double s1r, double s1i, double s2r, do
   e[3] = s2i * s1r - s2r * s1i;
 }
 
+// 16 consecutive columns of the warp's 32 lanes of tensor memory (one 32-bit value each).
+__device__ __forceinline__ void tmem_ld16(uint32_t (&q)[16], uint32_t addr) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+      "%12, %13, %14, %15}, [%16];\n"
+      : "=r"(q[0]), "=r"(q[1]), "=r"(q[2]), "=r"(q[3]), "=r"(q[4]), "=r"(q[5]), "=r"(q[6]),
+        "=r"(q[7]), "=r"(q[8]), "=r"(q[9]), "=r"(q[10]), "=r"(q[11]), "=r"(q[12]), "=r"(q[13]),
+        "=r"(q[14]), "=r"(q[15])
+      : "r"(addr));
+}
+// The level sums of 16 columns as the values sum_s q[s] 2^(-8 s), in units of the level-0 digit
+// product (each level's sum is exact; the FP64 sum rounds once per level).
+template <int LEV>
+__device__ __forceinline__ void recombine(const uint32_t (&q)[LEV][16], double* v) {
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    double acc = 0.0;
+    if constexpr (LEV == 6) acc = i32_to_f64(q[5][k]) * 0x1p-40;
+    acc = fma(i32_to_f64(q[4][k]), 0x1p-32, acc);
+    acc = fma(i32_to_f64(q[3][k]), 0x1p-24, acc);
+    acc = fma(i32_to_f64(q[2][k]), 0x1p-16, acc);
+    acc = fma(i32_to_f64(q[1][k]), 0x1p-8, acc);
+    v[k] = i32_to_f64(q[0][k]) + acc;
+  }
+}
+
 __device__ __forceinline__ int band_of(int n) {
   int u = 1, idx = 0;
   while (u < n) {
@@ -237,8 +268,12 @@ __global__ void __launch_bounds__(kThreads, 1) unit_i8_kernel(UnitI8Args a) {
       mbar_init(&sm.full[i], 1);
       mbar_init(&sm.empty[i], 1);
     }
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(&sm.side_full[i], 1);
+      mbar_init(&sm.side_empty[i], 8);  // one arrival per epilogue warp
+    }
     mbar_init(&sm.tmem_full, 1);
-    mbar_init(&sm.tmem_empty, 256);
+    mbar_init(&sm.tmem_empty, 8);
     mbar_init(&sm.drained, 1);
     sm.abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
@@ -255,10 +290,22 @@ __global__ void __launch_bounds__(kThreads, 1) unit_i8_kernel(UnitI8Args a) {
   const uint32_t tmem = sm.tmem_base;
 
   if (w == 0) {
-    // Copies: every job's K blocks into the stages.
+    // Copies: every chunk's side record into one of two slots, every job's K blocks into the
+    // stages.
     if (lane == 0) {
-      int it = 0;
+      int it = 0, q = -1;
+      int64_t cur = -1;
       for_each_job(a, [&](const Job& j) {
+        if (j.ci != cur) {
+          cur = j.ci;
+          ++q;
+          const int sl = q & 1;
+          if (q >= 2 && !mbar_wait(&sm.side_empty[sl], ((q >> 1) - 1) & 1, sm, a.err))
+            return false;
+          mbar_expect_tx(&sm.side_full[sl], kI8Side * 8);
+          bulk_load(sm.side[sl], a.xside + (int64_t)a.chunk_xidx[j.ci] * kI8Side, kI8Side * 8,
+                    &sm.side_full[sl]);
+        }
         int tl;
         const I8Table& tab = job_table(a, j, tl);
         const int n_kb = (j.nc + kI8KB - 1) / kI8KB;
@@ -276,10 +323,12 @@ __global__ void __launch_bounds__(kThreads, 1) unit_i8_kernel(UnitI8Args a) {
         }
         return true;
       });
-      // The last stages' copies have landed before the CTA can exit (they are the only ones
-      // that may still be in flight when a role stopped early).
+      // The last copies have landed before the CTA can exit (they are the only ones that may
+      // still be in flight when a role stopped early).
       for (int i = it > kStages ? it - kStages : 0; i < it; ++i)
         mbar_wait_drain(&sm.full[i % kStages], (i / kStages) & 1, a.err);
+      for (int i = q > 1 ? q - 1 : 0; i <= q; ++i)
+        mbar_wait_drain(&sm.side_full[i & 1], (i >> 1) & 1, a.err);
     }
   } else if (w == 1) {
     // MMAs: per job, per K block, per 32-order step the 15 digit products into their levels.
@@ -334,35 +383,20 @@ __global__ void __launch_bounds__(kThreads, 1) unit_i8_kernel(UnitI8Args a) {
     const int p = r >> 1;              // the angle pair within the tile
     const int e_thread = t - 64;       // 0 .. 255
     const int t_user = (a.h_u + kI8Pairs - 1) / kI8Pairs;
-    int job = 0;
+    int job = 0, q = -1;
     int64_t cur = -1;
     double out[4] = {0.0, 0.0, 0.0, 0.0};
     for_each_job(a, [&](const Job& j) {
+      // The row's scale, read before the waits so that its latency hides behind them.
+      int tl;
+      const I8Table& tab = job_table(a, j, tl);
+      const double rs = a.tscale[tab.scale_off + (int64_t)tl * 128 + r];
       if (j.ci != cur) {
-        // The chunk's node weights and column scales.
-        epi_sync();
-        if (e_thread < 32) {
-          const int64_t unit = a.units[j.ul];
-          const int64_t d = unit / a.n_wl, i = unit % a.n_wl;
-          const int jn = j.c * 32 + e_thread;
-          double wt = 0.0, cu = 0.0, ar = 0.0, sc = 0.0;
-          if (jn < a.n_nodes && a.radius[d * a.n_nodes + jn] > 0.0) {
-            const double rad = a.radius[d * a.n_nodes + jn];
-            const double x = 2.0 * kPi * rad / a.wl[i];
-            wt = a.weight[d * a.n_nodes + jn];
-            cu = 4.0 / (x * x);
-            ar = kPi * rad * rad;
-            sc = 4.0 / (x * x) * (kPi * rad * rad);
-          }
-          sm.w[e_thread] = wt;
-          sm.cu[e_thread] = cu;
-          sm.area[e_thread] = ar;
-          sm.sc[e_thread] = sc;
-        } else if (e_thread < 160) {
-          sm.cs[e_thread - 32] = a.xscale[(int64_t)a.chunk_xidx[j.ci] * 128 + e_thread - 32];
-        }
-        epi_sync();
+        // The previous chunk's side record is free; this chunk's has landed.
+        if (q >= 0) warp_arrive(&sm.side_empty[q & 1]);
+        ++q;
         cur = j.ci;
+        mbar_wait(&sm.side_full[q & 1], (q >> 1) & 1, sm, a.err);
       }
       // Every epilogue thread takes the same decision: one reads the abort flag between two
       // barriers that all of them reach.
@@ -372,42 +406,32 @@ __global__ void __launch_bounds__(kThreads, 1) unit_i8_kernel(UnitI8Args a) {
       epi_sync();
       if (sm.stop) return false;
       asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-      // The kept levels of this row's 32 columns, recombined in FP64.
+      // The kept levels of this row's 32 columns: read back, the tensor memory freed for the
+      // next job's MMAs, then recombined in FP64. With 5 levels all 160 sums are read before
+      // the release; with 6, the first group is recombined before the second group's are read.
       double v[32];
       const uint32_t lane_base = tmem + ((uint32_t)(32 * (w & 3)) << 16) + (uint32_t)(32 * e);
+      constexpr int kHeld = LEV == 5 ? 2 : 1;  // column groups held as sums across the release
+      uint32_t sums[kHeld][LEV][16];
+      if constexpr (LEV != 5) {
 #pragma unroll
-      for (int g = 0; g < 2; ++g) {
-        uint32_t q[LEV][16];
-#pragma unroll
-        for (int s = 0; s < LEV; ++s) {
-          asm volatile(
-              "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, "
-              "%10, %11, %12, %13, %14, %15}, [%16];\n"
-              : "=r"(q[s][0]), "=r"(q[s][1]), "=r"(q[s][2]), "=r"(q[s][3]), "=r"(q[s][4]),
-                "=r"(q[s][5]), "=r"(q[s][6]), "=r"(q[s][7]), "=r"(q[s][8]), "=r"(q[s][9]),
-                "=r"(q[s][10]), "=r"(q[s][11]), "=r"(q[s][12]), "=r"(q[s][13]), "=r"(q[s][14]),
-                "=r"(q[s][15])
-              : "r"(lane_base + (uint32_t)(s * 64 + g * 16)));
-        }
+        for (int s = 0; s < LEV; ++s) tmem_ld16(sums[0][s], lane_base + (uint32_t)(s * 64));
         asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-#pragma unroll
-        for (int k = 0; k < 16; ++k) {
-          double acc = 0.0;
-          if constexpr (LEV == 6) acc = i32_to_f64(q[5][k]) * 0x1p-40;
-          acc = fma(i32_to_f64(q[4][k]), 0x1p-32, acc);
-          acc = fma(i32_to_f64(q[3][k]), 0x1p-24, acc);
-          acc = fma(i32_to_f64(q[2][k]), 0x1p-16, acc);
-          acc = fma(i32_to_f64(q[1][k]), 0x1p-8, acc);
-          v[g * 16 + k] = i32_to_f64(q[0][k]) + acc;
-        }
+        recombine<LEV>(sums[0], v);
       }
-      // The accumulators are free for the next job's MMAs.
+#pragma unroll
+      for (int g = 2 - kHeld; g < 2; ++g)
+#pragma unroll
+        for (int s = 0; s < LEV; ++s)
+          tmem_ld16(sums[g - (2 - kHeld)][s], lane_base + (uint32_t)(s * 64 + g * 16));
+      asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
       asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-      mbar_arrive(&sm.tmem_empty);
-      int tl;
-      const I8Table& tab = job_table(a, j, tl);
-      const double rs = a.tscale[tab.scale_off + (int64_t)tl * 128 + r];
+      warp_arrive(&sm.tmem_empty);
+#pragma unroll
+      for (int g = 2 - kHeld; g < 2; ++g) recombine<LEV>(sums[g - (2 - kHeld)], v + 16 * g);
       const bool user = j.tile < t_user;
+      const double* cs = sm.side[q & 1];
+      const double* nf = sm.side[q & 1] + 128;
       const double sg = side ? -1.0 : 1.0;
 #pragma unroll
       for (int nd = 0; nd < 8; ++nd) {
@@ -416,17 +440,16 @@ __global__ void __launch_bounds__(kThreads, 1) unit_i8_kernel(UnitI8Args a) {
         double mine[4], other[4], E[4], O[4];
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-          mine[k] = v[4 * nd + k] * (rs * sm.cs[j.half * 64 + 32 * e + 4 * nd + k]);
+          mine[k] = v[4 * nd + k] * (rs * cs[j.half * 64 + 32 * e + 4 * nd + k]);
           other[k] = __shfl_xor_sync(0xffffffffu, mine[k], 1);
           E[k] = side ? other[k] : mine[k];
           O[k] = side ? mine[k] : other[k];
         }
         double el[4];
         elements4(E[0] + sg * O[2], E[1] + sg * O[3], E[2] + sg * O[0], E[3] + sg * O[1], el);
-        const int node = j.half * 16 + 8 * e + nd;
-        const double wt = sm.w[node], cu = sm.cu[node], ar = sm.area[node], sc = sm.sc[node];
+        const double f = nf[j.half * 16 + 8 * e + nd];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) out[k] += user ? wt * ((cu * el[k]) * ar) : wt * (sc * el[k]);
+        for (int k = 0; k < 4; ++k) out[k] = fma(f, el[k], out[k]);
       }
       if (j.half == 1) {
         // The job pair's sums into this row's (pair, side) accumulators: warpgroup 1 hands its
@@ -461,9 +484,11 @@ __global__ void __launch_bounds__(kThreads, 1) unit_i8_kernel(UnitI8Args a) {
             len = B.n_q;
             base = a.acc + a.chunk_acc[j.ci];
           }
+          // Reductions without a reply: this thread's adds to one sum stay in its program order,
+          // and no other thread adds to it while the kernel runs.
           if (jo >= 0)
 #pragma unroll
-            for (int k = 0; k < 4; ++k) base[k * len + jo] += out[k];
+            for (int k = 0; k < 4; ++k) atomicAdd(base + k * len + jo, out[k]);
         }
 #pragma unroll
         for (int k = 0; k < 4; ++k) out[k] = 0.0;
@@ -495,7 +520,22 @@ __global__ void __launch_bounds__(128) x_split_kernel(XSplitArgs a) {
   frexp(m, &ex);
   int e = 7 - ex;  // m 2^e in [64, 128)
   if (ldexp(m, e) >= 127.0) --e;
-  a.xscale[(int64_t)a.chunk_xidx[ci] * 128 + c] = m > 0.0 ? ldexp(1.0, -e) : 0.0;
+  double* side = a.xside + (int64_t)a.chunk_xidx[ci] * kI8Side;
+  side[c] = m > 0.0 ? ldexp(1.0, -e) : 0.0;
+  if (c < 32) {
+    // The node factor w 4 pi r^2 / x^2 (the phase-matrix normalisation times the area); padding
+    // nodes and nodes of zero radius weigh nothing.
+    const int64_t unit = a.units[ci / a.cpu];
+    const int64_t d = unit / a.n_wl, i = unit % a.n_wl;
+    const int jn = (ci % a.cpu) * 32 + c;
+    double f = 0.0;
+    if (jn < a.n_nodes && a.radius[d * a.n_nodes + jn] > 0.0) {
+      const double rad = a.radius[d * a.n_nodes + jn];
+      const double x = 2.0 * kPi * rad / a.wl[i];
+      f = a.weight[d * a.n_nodes + jn] * (4.0 / (x * x) * (kPi * rad * rad));
+    }
+    side[128 + c] = f;
+  }
   const int half = c >> 6, row = c & 63;
   const int n_kb = (nc + kI8KB - 1) / kI8KB;
   unsigned char* base = a.xdig + a.chunk_xoff[ci];
