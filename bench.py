@@ -56,9 +56,12 @@ def parse():
                    help="skip the spheroid ensemble leg")
     p.add_argument("--no-projection", action="store_true",
                    help="skip the tensor-core Greek projection measurement")
-    p.add_argument("--i8-above", type=int, default=64,
+    p.add_argument("--i8-above", type=int, default=None,
                    help="the mixed form: chunks with more terms than this take the int8 path "
-                        "(0: plain FP64 only)")
+                        "(0: plain FP64 only; default: the autotuner's choice, else 32)")
+    p.add_argument("--no-tune", action="store_true",
+                   help="skip the autotuner (work split and threshold timed on a sample of the "
+                        "batch's wavelengths before the timed steps)")
     p.add_argument("--i8-levels", type=int, default=0,
                    help="the mixed form's product levels kept: 5, 6, or 0 for the default")
     return p.parse_args()
@@ -676,6 +679,20 @@ def ours(args):
             dist.barrier()
         torch.cuda.synchronize()
 
+    # The autotuner (outside the timed steps): the work split, and the mixed form's threshold
+    # unless one was given, timed on 64 of the batch's wavelengths.
+    tuned = None
+    if not args.no_tune:
+        from scatrs_b200 import tune
+
+        thresholds = (16, 24, 32, 48, 64) if args.i8_above is None else (args.i8_above,)
+        tuned = tune.autotune_fixed(w.dists, w.wavelengths, w.m, w.mu, w.n_nodes, w.greek_order,
+                                    sample_wl=64, thresholds=(0,) + tuple(
+                                        t for t in thresholds if t > 0), levels=args.i8_levels)
+        if args.i8_above is None:
+            args.i8_above = tuned.i8_above if tuned.i8_above > 0 else 32
+    elif args.i8_above is None:
+        args.i8_above = 32
     # Both forms on the same inputs: the plain FP64 path, then the mixed form (the int8 angle
     # GEMMs of the chunks with more than i8_above terms).
     plain = run_form(args, w, 0, (values_d, phase_d, greek_d), wl_d, m_d, stream, flush,
@@ -720,6 +737,11 @@ def ours(args):
         forms["mixed"] = form_summary(mixed, w)
         forms["mixed"]["i8_above"] = args.i8_above
         forms["mixed"]["levels"] = args.i8_levels or 5
+    if tuned is not None:
+        forms["tuning"] = {"split": tuned.split, "arena_rows": tuned.arena_rows,
+                           "i8_above": tuned.i8_above, "sample_units": tuned.sample_units,
+                           "ms_per_candidate": {k: round(v, 3) for k, v in tuned.ms.items()},
+                           "errors": tuned.errors}
         ops = algorithmic_i8_ops(w, user_rows, args.i8_above, args.i8_levels or 5)
         ktm = mixed["kt"]
         i8_ms, i8_n = ktm.get("unit_i8_kernel", (0.0, 0))

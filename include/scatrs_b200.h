@@ -598,6 +598,23 @@ enum scatrs_limit_kind {
 };
 int64_t scatrs_limit(int32_t which);
 
+/*
+ * Work-division settings of the fixed-grid entries, process-wide; they change how the work is cut
+ * and scheduled, never a result (every output sum runs over its chunks in the same order whatever
+ * the settings). split: a unit's table-row tiles are cut into work items of about
+ * (work per slab) / (split x resident CTAs) each, 1..64 (0: the default, 4); arena_rows: the
+ * coefficient rows (1 KiB each) a slab's arena holds, 2^16..2^24 (0: the default, 2^22). The
+ * reference has no counterpart (its batch runs on host threads); the tuner in
+ * scatrs_b200.tune picks them, and the mixed form's i8_above, by timing a sample of a workload.
+ */
+typedef struct scatrs_tuning {
+  int32_t split;
+  int32_t reserved; /* 0 */
+  int64_t arena_rows;
+} scatrs_tuning;
+int scatrs_set_tuning(const scatrs_tuning* tuning, char* err, size_t err_len);
+int scatrs_get_tuning(scatrs_tuning* tuning);
+
 /* The CUDA device count, or -1 when the runtime is unusable. */
 int scatrs_device_count(void);
 

@@ -92,6 +92,10 @@ class MixedOptions(ctypes.Structure):
     _fields_ = [("i8_above", _I32), ("levels", _I32)]
 
 
+class Tuning(ctypes.Structure):
+    _fields_ = [("split", _I32), ("reserved", _I32), ("arena_rows", _I64)]
+
+
 class RefractiveModel(ctypes.Structure):
     _fields_ = [("kind", _I32), ("n", _I32), ("p", _D * 4), ("table", _PD)]
 
@@ -177,6 +181,8 @@ SYMBOLS = {
     "scatrs_testing_fail_allocation": (None, [_I64]),
     "scatrs_testing_force_node_error": (None, [_I64, _I32]),
     "scatrs_limit": (_I64, [_I32]),
+    "scatrs_set_tuning": (ctypes.c_int, [ctypes.POINTER(Tuning), _CP, _SZ]),
+    "scatrs_get_tuning": (ctypes.c_int, [ctypes.POINTER(Tuning)]),
     "scatrs_device_count": (ctypes.c_int, []),
     "scatrs_launch_count": (_I64, []),
     "scatrs_gauss_legendre": (None, [_I64, _PD, _PD]),
@@ -235,6 +241,21 @@ _LIMITS = {"MIE_ORDER": 0, "MIE_VALUES": 1, "GREEK_ORDER": 2, "LAYERS": 3, "TMAT
 def limit(name: str) -> int:
     """One of the library's limits (scatrs_limit), by its SCATRS_LIMIT_ name."""
     return int(load().scatrs_limit(_LIMITS[name]))
+
+
+def set_tuning(split: int = 0, arena_rows: int = 0) -> None:
+    """The fixed-grid entries' work division (scatrs_set_tuning; 0 = the default)."""
+    t = Tuning(int(split), 0, int(arena_rows))
+    buf = ctypes.create_string_buffer(512)
+    st = load().scatrs_set_tuning(ctypes.byref(t), buf, 512)
+    if st != 0:
+        _check(st, buf)
+
+
+def get_tuning() -> dict:
+    t = Tuning()
+    load().scatrs_get_tuning(ctypes.byref(t))
+    return {"split": int(t.split), "arena_rows": int(t.arena_rows)}
 
 
 def gauss_legendre(n: int):

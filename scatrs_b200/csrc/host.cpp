@@ -90,6 +90,10 @@ constexpr int64_t kMaxTmatrixOrder = 500;          // MAX_TMATRIX_ORDER (tmatrix
 constexpr int64_t kMaxGaussPoints = 1 << 17;       // special/gauss_legendre.rs:43
 constexpr int64_t kMaxWignerValues = 1 << 28;      // scatrs-py/src/special.rs:24
 constexpr int64_t kArenaRows = 1 << 22;            // coefficient rows per slab (1 KiB each)
+constexpr int kDefaultSplit = 4;                     // work items per resident CTA and slab
+// The work-division settings (scatrs_set_tuning): read once per call.
+std::atomic<int> g_split{kDefaultSplit};
+std::atomic<int64_t> g_arena_rows{kArenaRows};
 constexpr int64_t kMaxSlabChunks = 1 << 18;        // chunks per slab
 constexpr double kPi = 3.14159265358979323846264338327950288;
 
@@ -212,7 +216,7 @@ struct Context {
     std::vector<I8Table> user, band;
     DevBuf dig, scale, user_d, band_d;
   } i8;
-  DevBuf xdig, xside, chunk_xoff, chunk_xidx, i8_list, i8_err;
+  DevBuf xdig, xside, colmax, chunk_xoff, chunk_xidx, i8_list, i8_err;
   // Spheroid T-matrices.
   DevBuf tm_geoms, tm_jobs, tm_rules, tm_node, tm_rad, tm_ang, tm_J, tm_work, tm_piv, tm_T, tm_sums,
       tm_err;
@@ -825,7 +829,7 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
     total_cost += cost;
   }
   const int64_t max_urows = *std::max_element(urows.begin(), urows.end());
-  const int64_t arena = std::max<int64_t>(kArenaRows, 2 * max_urows);
+  const int64_t arena = std::max<int64_t>(g_arena_rows.load(), 2 * max_urows);
   std::vector<int> by_cost(n_units);
   for (int64_t u = 0; u < n_units; ++u) by_cost[u] = (int)u;
   std::sort(by_cost.begin(), by_cost.end(), [&](int x, int y) {
@@ -858,7 +862,8 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
   }
   // A large unit's row tiles split into work items of about item_target work each.
   const int grid_max = c.sms * c.unit_bps;
-  const double item_target = std::max(1.0, total_cost / (double)n_slabs / (4.0 * grid_max));
+  const double item_target =
+      std::max(1.0, total_cost / (double)n_slabs / ((double)g_split.load() * grid_max));
   std::vector<int> ugroups(n_units);
   for (int64_t u = 0; u < n_units; ++u)
     ugroups[u] = (int)std::min<double>(std::max(1.0, std::ceil(ucost[u] / item_target)),
@@ -954,12 +959,14 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
   int* i8_list_d = nullptr;
   unsigned char* xdig = nullptr;
   double* xside = nullptr;
+  double* colmax = nullptr;
   if (i8_above > 0) {
     chunk_xoff_d = c.chunk_xoff.as<int64_t>(n_chunks);
     chunk_xidx_d = c.chunk_xidx.as<int>(n_chunks);
     i8_list_d = c.i8_list.as<int>(n_chunks);
     xdig = c.xdig.as<unsigned char>((size_t)i8_bytes_max);
     xside = c.xside.as<double>((size_t)i8_chunks_max * kI8Side);
+    colmax = c.colmax.as<double>((size_t)kMaxSlabChunks * 128);
   }
   c.ensure_staging((size_t)stage_max);
   // 4. Per slab: build its plan into pinned staging, upload it, launch its kernels. The host
@@ -979,6 +986,7 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
     ka.m_layers = reinterpret_cast<const double2*>(layers.m_dev);
   }
   ka.X = X;
+  ka.colmax = colmax;  // the mixed form's digit scales; null otherwise
   ka.uz = uz;
   ka.ux = ux;
   ka.chunk_sums = chunk_sums;
@@ -1246,6 +1254,7 @@ void run_fixed(Context& c, const scatrs_distribution* dists, int64_t n_dist, con
       // The mixed form: the int8 chunks' digits, then their angle GEMMs on the tensor cores.
       XSplitArgs xa{};
       xa.X = X;
+      xa.colmax = colmax;
       xa.chunk_row = ua.chunk_row;
       xa.chunk_n = ua.chunk_n;
       xa.list = i8_list_d + ch0;
@@ -4564,6 +4573,28 @@ int scatrs_not_converged_detail(double* achieved, double* requested) {
   return sb::g_last_status == SCATRS_NOT_CONVERGED ? 1 : 0;
 }
 
+int scatrs_set_tuning(const scatrs_tuning* t, char* err, size_t err_len) {
+  return guarded(err, err_len, [&] {
+    if (!t) throw Failure{SCATRS_INVALID_INPUT, "tuning: null settings"};
+    const int split = t->split == 0 ? kDefaultSplit : t->split;
+    const int64_t rows = t->arena_rows == 0 ? kArenaRows : t->arena_rows;
+    if (split < 1 || split > 64)
+      throw Failure{SCATRS_INVALID_INPUT, "tuning: split must be in 1..64 (0: 4)"};
+    if (rows < (1 << 16) || rows > (1 << 24))
+      throw Failure{SCATRS_INVALID_INPUT, "tuning: arena_rows must be in 2^16..2^24 (0: 2^22)"};
+    g_split.store(split);
+    g_arena_rows.store(rows);
+  });
+}
+
+int scatrs_get_tuning(scatrs_tuning* t) {
+  if (!t) return SCATRS_INVALID_INPUT;
+  t->split = g_split.load();
+  t->reserved = 0;
+  t->arena_rows = g_arena_rows.load();
+  return SCATRS_OK;
+}
+
 int64_t scatrs_limit(int32_t which) {
   switch (which) {
     case SCATRS_LIMIT_MIE_ORDER: return sb::kMaxMieOrder;
@@ -4627,7 +4658,7 @@ void scatrs_release(void) {
                       &c.X, &c.uz, &c.ux, &c.chunk_sums, &c.err, &c.acc,
                       &c.counter, &c.values, &c.phase, &c.greek, &c.user.ge, &c.user.go,
                       &c.user.map, &c.tc_a_hi, &c.tc_a_lo, &c.tc_prod, &c.tc_err, &c.xdig,
-                      &c.xside, &c.chunk_xoff, &c.chunk_xidx, &c.i8_list, &c.i8_err,
+                      &c.xside, &c.colmax, &c.chunk_xoff, &c.chunk_xidx, &c.i8_list, &c.i8_err,
                       &c.i8.dig, &c.i8.scale, &c.i8.user_d, &c.i8.band_d})
       b->release();
     for (auto& kv : c.projectors)

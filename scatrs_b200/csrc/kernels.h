@@ -34,6 +34,7 @@ struct MieFixedArgs {
   const int* chunk_n;       // slab-local: each chunk's largest number of terms
   const int64_t* chunk_row; // slab-local: first coefficient row of each chunk
   double* X;                // coefficient rows, 128 doubles each
+  double* colmax;           // or null; per chunk, each of its 128 columns' largest |X|
   double2* uz;              // scratch rows of u_k(mx), 32 lanes each
   double* ux;               // scratch rows of u_k(x)
   double* chunk_sums;       // [n_chunks][8] weighted per-particle quantities
@@ -210,6 +211,7 @@ struct UnitI8Args {
 // The digits of the int8 chunks' coefficient rows (one CTA per listed chunk).
 struct XSplitArgs {
   const double* X;
+  const double* colmax;  // per slab-local chunk, its columns' largest |X| (written by K-a)
   const int64_t* chunk_row;
   const int* chunk_n;
   const int* list;  // slab-local chunks on the int8 path

@@ -67,6 +67,7 @@ __device__ __forceinline__ void mie_chunk(const MieFixedArgs& a) {
   s.stride = 32;
   double q[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   double qe[kAdaptive ? 8 : 1] = {};  // adaptive: weighted by w_K - w_G
+  double cm[4] = {0.0, 0.0, 0.0, 0.0};  // the largest |X| of this lane's four columns
   int64_t n = 0;
   const int64_t node = (a.per_unit ? unit : d) * a.n_nodes + j;
   if (j < a.n_nodes && a.radius[node] > 0.0) {
@@ -78,6 +79,10 @@ __device__ __forceinline__ void mie_chunk(const MieFixedArgs& a) {
       const bool odd = (k & 1) != 0;
       const cplx u = odd ? an : bn, v = odd ? bn : an;
       *reinterpret_cast<double4*>(X + (k - 1) * 128) = make_double4(u.re, u.im, v.re, v.im);
+      cm[0] = fmax(cm[0], fabs(u.re));
+      cm[1] = fmax(cm[1], fabs(u.im));
+      cm[2] = fmax(cm[2], fabs(v.re));
+      cm[3] = fmax(cm[3], fabs(v.im));
     };
     ValueSums vs;
     double asum = 0.0;
@@ -137,6 +142,9 @@ __device__ __forceinline__ void mie_chunk(const MieFixedArgs& a) {
   // Orders above the node's own N are zero up to the chunk's.
   for (int64_t k = n + 1; k <= nc; ++k)
     *reinterpret_cast<double4*>(X + (k - 1) * 128) = make_double4(0.0, 0.0, 0.0, 0.0);
+  if (a.colmax != nullptr)
+    *reinterpret_cast<double4*>(a.colmax + (int64_t)chunk * 128 + lane * 4) =
+        make_double4(cm[0], cm[1], cm[2], cm[3]);
   // The chunk's weighted sums, in a fixed tree order.
   const int stride = kAdaptive ? 16 : 8;
   for (int k = 0; k < 8; ++k) {

@@ -188,19 +188,30 @@ __device__ __forceinline__ void tmem_ld16(uint32_t (&q)[16], uint32_t addr) {
         "=r"(q[14]), "=r"(q[15])
       : "r"(addr));
 }
-// The level sums of 16 columns as the values sum_s q[s] 2^(-8 s), in units of the level-0 digit
-// product (each level's sum is exact; the FP64 sum rounds once per level).
+// The level sums of 16 columns as values. With 5 levels: w = sum_s q[s] 2^(32 - 8 s) exactly
+// in 64-bit integers (|q[s]| < 2^28.4, so |w| < 2^61), then w as a double, rounded once (the
+// caller scales by 2^-32). With 6: sum_s q[s] 2^(-8 s) in FP64, rounding once per level.
 template <int LEV>
 __device__ __forceinline__ void recombine(const uint32_t (&q)[LEV][16], double* v) {
 #pragma unroll
   for (int k = 0; k < 16; ++k) {
-    double acc = 0.0;
-    if constexpr (LEV == 6) acc = i32_to_f64(q[5][k]) * 0x1p-40;
-    acc = fma(i32_to_f64(q[4][k]), 0x1p-32, acc);
-    acc = fma(i32_to_f64(q[3][k]), 0x1p-24, acc);
-    acc = fma(i32_to_f64(q[2][k]), 0x1p-16, acc);
-    acc = fma(i32_to_f64(q[1][k]), 0x1p-8, acc);
-    v[k] = i32_to_f64(q[0][k]) + acc;
+    if constexpr (LEV == 5) {
+      long long w = (long long)(int)q[0][k] * 4294967296LL;
+      w += (long long)(int)q[1][k] * 16777216LL;
+      w += (long long)(int)q[2][k] * 65536LL;
+      w += (long long)(int)q[3][k] * 256LL;
+      w += (long long)(int)q[4][k];
+      const double hi = i32_to_f64((uint32_t)(w >> 32));
+      const double lo = __hiloint2double(0x43300000, (int)(uint32_t)w) - 4503599627370496.0;
+      v[k] = fma(hi, 4294967296.0, lo);
+    } else {
+      double acc = i32_to_f64(q[5][k]) * 0x1p-40;
+      acc = fma(i32_to_f64(q[4][k]), 0x1p-32, acc);
+      acc = fma(i32_to_f64(q[3][k]), 0x1p-24, acc);
+      acc = fma(i32_to_f64(q[2][k]), 0x1p-16, acc);
+      acc = fma(i32_to_f64(q[1][k]), 0x1p-8, acc);
+      v[k] = i32_to_f64(q[0][k]) + acc;
+    }
   }
 }
 
@@ -390,7 +401,8 @@ __global__ void __launch_bounds__(kThreads, 1) unit_i8_kernel(UnitI8Args a) {
       // The row's scale, read before the waits so that its latency hides behind them.
       int tl;
       const I8Table& tab = job_table(a, j, tl);
-      const double rs = a.tscale[tab.scale_off + (int64_t)tl * 128 + r];
+      // (times 2^-32 with 5 levels: the recombined values are in units of the lowest level)
+      const double rs = a.tscale[tab.scale_off + (int64_t)tl * 128 + r] * (LEV == 5 ? 0x1p-32 : 1.0);
       if (j.ci != cur) {
         // The previous chunk's side record is free; this chunk's has landed.
         if (q >= 0) warp_arrive(&sm.side_empty[q & 1]);
@@ -505,17 +517,16 @@ __global__ void __launch_bounds__(kThreads, 1) unit_i8_kernel(UnitI8Args a) {
 }
 
 // The digits of one int8 chunk's coefficient rows: thread c owns column c (node c / 4,
-// component c % 4); its scale 2^-e puts the column's largest |X| below 127 2^-e (in [63.5, 127)
-// 2^-e), and each value's F = rint(X 2^(e + 32)) is written as its 5 balanced digits, 16
-// orders at a time, into the (half, K block, digit) slices in the 64-byte swizzle (16-byte
-// chunk q of row r at chunk q ^ ((r >> 1) & 3)).
+// component c % 4); its scale 2^-e puts the column's largest |X| (recorded by K-a) below
+// 127 2^-e (in [63.5, 127) 2^-e), and each value's F = rint(X 2^(e + 32)) is written as its 5
+// balanced digits, 16 orders at a time, into the (half, K block, digit) slices in the 64-byte
+// swizzle (16-byte chunk q of row r at chunk q ^ ((r >> 1) & 3)).
 __global__ void __launch_bounds__(128) x_split_kernel(XSplitArgs a) {
   const int ci = a.list[blockIdx.x];
   const int nc = a.chunk_n[ci];
   const double* X = a.X + a.chunk_row[ci] * 128;
   const int c = threadIdx.x;
-  double m = 0.0;
-  for (int k = 0; k < nc; ++k) m = fmax(m, fabs(X[(int64_t)k * 128 + c]));
+  const double m = a.colmax[(int64_t)ci * 128 + c];
   int ex = 0;
   frexp(m, &ex);
   int e = 7 - ex;  // m 2^e in [64, 128)
