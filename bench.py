@@ -54,6 +54,8 @@ def parse():
                    help="skip the layered-sphere derivatives leg")
     p.add_argument("--no-spheroids", action="store_true",
                    help="skip the spheroid ensemble leg")
+    p.add_argument("--no-small", action="store_true",
+                   help="skip the small plain configuration (768 nodes, one call per step)")
     p.add_argument("--no-projection", action="store_true",
                    help="skip the tensor-core Greek projection measurement")
     p.add_argument("--i8-above", type=int, default=None,
@@ -470,28 +472,29 @@ def tf32_peak_tflops(torch):
 
 
 def projection_large_droplets(torch, steps: int = 3, scale: float = 1.0):
-    """The Greek projection of the large-droplet configuration's shape (128 distributions x
-    256 wavelengths = 32,768 tables at 4096 Gauss cosines, order 1024) on the tensor cores
-    (3xTF32, FP32 accumulation) against the FP64 projection of the same tables: throughput of
-    the tcgen05 GEMM against the cuBLAS TF32 rate measured here, and the error. The tables are
-    seeded synthetic phase matrices (smooth in the cosine, positive F11)."""
+    """The Greek projection of the large-droplet configuration (128 distributions x 256
+    wavelengths = 32,768 tables at 4096 Gauss cosines, order 1024) on the tensor cores (3xTF32,
+    FP32 accumulation) against the FP64 projection of the same tables: throughput of the tcgen05
+    GEMM against the cuBLAS TF32 rate measured here, and the error. The tables are the
+    configuration's own phase matrices: the fixed-grid ensemble (FP64) of its first 3
+    distributions x 5 wavelengths (x up to about 300) at the 4096 cosines, repeated to the
+    configuration's number of tables (the GEMM's cost does not depend on the values)."""
     from scatrs_b200 import _native
     from scatrs_b200 import workloads as W
 
-    n_units, n_q, L = max(1, round(128 * 256 * min(scale, 1.0))), 4096, 1024
-    g = torch.Generator(device="cuda").manual_seed(3)
-    mu = torch.tensor(W.gauss_legendre(n_q), device="cuda")
-    # F = sum of a few Legendre-like smooth lobes per table.
-    c = torch.rand(n_units, 4, generator=g, device="cuda", dtype=torch.float64)
-    lobes = torch.stack([torch.exp(3.0 * (mu - 1.0)), (1 + mu) ** 2 / 4, 1 - mu * mu, mu]).T
-    f11 = (c @ lobes.T).clamp_min(0) + 0.01
-    phase = torch.empty(6, n_units, n_q, dtype=torch.float64, device="cuda")
-    phase[0] = f11
-    phase[1] = -0.3 * f11 * (1 - mu * mu)
-    phase[2] = f11
-    phase[3] = f11 * mu
-    phase[4] = 0.1 * f11 * torch.sqrt(1 - mu * mu)
-    phase[5] = phase[3]
+    n_units, L = max(1, round(128 * 256 * min(scale, 1.0))), 1024
+    w = W.large_droplets(seed=0, scale=0.02, n_q=4096)
+    n_q, n_real = w.mu.size, w.n_units
+    wl = torch.tensor(w.wavelengths, device="cuda")
+    m = torch.tensor(np.ascontiguousarray(w.m).view(np.float64).reshape(-1), device="cuda")
+    values = torch.empty(11 * n_real, dtype=torch.float64, device="cuda")
+    real = torch.empty(6, n_real, n_q, dtype=torch.float64, device="cuda")
+    _native.ensemble_fixed_device(w.dists, wl.data_ptr(), w.wavelengths.size, m.data_ptr(), w.mu,
+                                  w.n_nodes, -1, True, values.data_ptr(), real.data_ptr(), 0)
+    _native.check_errors()
+    reps = (n_units + n_real - 1) // n_real
+    phase = real.repeat(1, reps, 1)[:, :n_units].contiguous()
+    del real, values
     out_tc = torch.empty(6, n_units, L + 1, dtype=torch.float64, device="cuda")
     out_64 = torch.empty_like(out_tc)
     _native.project_greek_device(phase.data_ptr(), n_units, n_q, L, 0, out_64.data_ptr())
@@ -516,7 +519,8 @@ def projection_large_droplets(torch, steps: int = 3, scale: float = 1.0):
     del phase, out_tc, out_64
     torch.cuda.empty_cache()
     return {"workload": f"{n_units} tables x 4096 Gauss cosines -> Greek order 1024 "
-                        "(large-droplet shape, seeded synthetic tables)",
+                        f"(large droplets: the ensemble's own tables of {n_real} units, "
+                        "repeated)",
             "kernel": "greek_tc_kernel (tcgen05.mma kind::tf32, 3 products)",
             "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
             "frac": achieved / peak,
@@ -600,16 +604,17 @@ def spheroid_leg(torch, fp64_peak: float, scale: float = 1.0, cpu_seconds: float
 
 
 def layered_adjoint_leg(torch, scale: float = 1.0, cpu_seconds: float = 8.0):
-    """The layered-sphere ensemble with its derivatives (the layered adjoint workload: three
-    layers, 256 distributions x 128 wavelengths x 256 nodes, Greek order 32) on its first
-    quarter of distributions and wavelengths (the full size at scale 4): values and the 10
-    forward-mode derivative blocks (median, width, each layer's n and k, both fractions), timed
-    after one identical warm-up call. The CPU baseline is the oracle's layered forward ensemble
-    (values only) on the same workload's units, all host threads."""
+    """The layered-sphere ensemble with its derivatives (the layered adjoint workload at full
+    size: three layers, 256 distributions x 128 wavelengths x 256 nodes, Greek order 32): values
+    and the 10 forward-mode derivative blocks (median, width, each layer's n and k, both
+    fractions) through the host-buffer entry point, timed after one identical warm-up call. The
+    CPU baseline produces the same outputs the way the oracle can: its layered forward ensemble
+    (all host threads) 21 times per unit, the values and a central difference for each of the 10
+    directions; the rate of one forward pass is reported beside it."""
     from scatrs_b200 import _native
     from scatrs_b200 import workloads as W
 
-    w = W.layered_spheres(seed=0, scale=min(1.0, 0.25 * scale))
+    w = W.layered_spheres(seed=0, scale=min(1.0, scale))
     call = lambda: _native.ensemble_fixed_layered_d(w.dists, w.wavelengths, w.fractions,
                                                     w.m_layers, None, w.n_nodes, w.greek_order)
     call()
@@ -639,11 +644,55 @@ def layered_adjoint_leg(torch, scale: float = 1.0, cpu_seconds: float = 8.0):
         done += w.wavelengths.size * w.n_nodes
         k += 1
     dt = time.time() - t0
-    res["cpu_baseline"] = {"value": done / dt, "unit": "nodes/s (values only)",
+    blocks = int(out[3].shape[0])
+    res["cpu_baseline"] = {"value": done / dt / (2 * blocks + 1),
+                           "unit": "nodes/s (values and every derivative block)",
                            "cores": os.cpu_count(), "kind": "port",
+                           "forward_only": done / dt,
                            "sample": f"{k} distributions x {w.wavelengths.size} wavelengths x "
                                      f"{w.n_nodes} nodes in {dt:.1f} s: the oracle's layered "
-                                     "forward ensemble, OpenMP over units"}
+                                     f"forward ensemble, OpenMP over units; {2 * blocks + 1} "
+                                     "forward passes per unit give the values and the "
+                                     f"{blocks} blocks by central differences"}
+    return res
+
+
+def small_plain_leg(torch, calls: int = 50, cpu_seconds: float = 5.0):
+    """The small plain configuration (one lognormal, median 0.08 um, width 1.6, 256 nodes over
+    median width^(+-5), m = 1.43 + 1e-8 i, wavelengths 0.35, 0.55, 1.0 um, 180 Gauss cosines,
+    Greek order 32): the host-buffer entry point, one call per step (a latency-bound case of
+    768 nodes), and the oracle on one host thread for the same call."""
+    from scatrs_b200 import _native
+    from scatrs_b200 import workloads as W
+
+    w = W.small_spheres()
+    call = lambda: _native.ensemble_fixed(w.dists, w.wavelengths, w.m, w.mu, w.n_nodes,
+                                          w.greek_order, True)
+    for _ in range(3):
+        call()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(calls):
+        call()
+    torch.cuda.synchronize()
+    dt = (time.perf_counter() - t0) / calls
+    nodes = w.dists.size * w.wavelengths.size * w.n_nodes
+    res = {"workload": f"{nodes} nodes ({w.name}): 1 lognormal x 3 wavelengths x 256 nodes, "
+                       "180 cosines, Greek order 32, FP64",
+           "value": nodes / dt, "unit": "nodes/s", "ms_per_call": dt * 1e3,
+           "timing": "wall clock around the host-buffer call (copies included), mean of "
+                     f"{calls} calls"}
+    from oracle import oracle as O
+    od = w.dists.view(O.DIST_DTYPE)
+    n, t0 = 0, time.time()
+    while time.time() - t0 < cpu_seconds:
+        O.ensemble_fixed(od, w.wavelengths, w.m, w.n_nodes, w.mu, w.greek_order, True,
+                         threads=1)
+        n += 1
+    dt_cpu = (time.time() - t0) / n
+    res["cpu_baseline"] = {"value": nodes / dt_cpu, "unit": "nodes/s", "cores": 1,
+                           "kind": "port", "ms_per_call": dt_cpu * 1e3,
+                           "sample": f"the same call {n} times on one host thread (the oracle)"}
     return res
 
 
@@ -806,6 +855,8 @@ def ours(args):
         line["layered_adjoint"] = layered_adjoint_leg(torch, scale=args.scale)
     if world == 1 and not args.no_spheroids:
         line["spheroids"] = spheroid_leg(torch, roof_fp64["peak"], scale=args.scale)
+    if world == 1 and not args.no_small:
+        line["small_plain"] = small_plain_leg(torch)
     print(json.dumps(line), flush=True)
 
 
