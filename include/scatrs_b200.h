@@ -330,6 +330,25 @@ int scatrs_spheroid_compute(int64_t n, const double* x, const double* aspect_rat
                             double* error_estimate, char* err, size_t err_len);
 
 /*
+ * scatrs_spheroid_compute with the derivatives of every output along x, the aspect ratio, Re m
+ * and Im m (TMatrix::compute_with_derivatives, tmatrix/mod.rs:231-245, with the efficiencies'
+ * Jacobian and greek_with_derivatives, mod.rs:695-760): the derivatives of the solution at each
+ * spheroid's converged N and n_theta, as the reference takes them. They come from the outputs
+ * solved at perturbed parameters at the same (N, n_theta), in one batch with the values: central
+ * differences at steps h and h/2 (h = 1e-4 of the parameter, of |m| for m), Richardson-
+ * extrapolated, and a one-sided fourth-order stencil along Im m when Im m < 4h (Im m cannot go
+ * below zero); accurate to about 1e-9 of each output's scale (the reference's dual numbers are
+ * exact to rounding). eff, greek as scatrs_spheroid_compute's (their values at that N and
+ * n_theta); d_eff[4][n][5] and d_greek[4][n][6 (greek_order + 1)], direction-major in the order
+ * x, aspect ratio, Re m, Im m. Seventeen solutions of every mode per spheroid.
+ */
+int scatrs_spheroid_compute_d(int64_t n, const double* x, const double* aspect_ratio,
+                              const double* m, const scatrs_spheroid_options* options,
+                              double* eff, double* greek, double* d_eff, double* d_greek,
+                              int32_t* n_terms, int32_t* n_theta, double* error_estimate,
+                              char* err, size_t err_len);
+
+/*
  * The fixed-grid ensemble of randomly oriented spheroids (Particle::Spheroid; the engine's
  * direct path, engine.rs:1207-1339, 2192-2216, 2359-2497): each distribution's nodes as
  * scatrs_ensemble_fixed's, one aspect ratio per distribution (aspect_ratio[n_dist]) and m per
@@ -348,6 +367,27 @@ int scatrs_ensemble_fixed_spheroid(const scatrs_distribution* dists, int64_t n_d
                                    double tmatrix_rtol, double* values, double* phase,
                                    double* greek, int32_t* node_terms, char* err,
                                    size_t err_len);
+
+/*
+ * scatrs_ensemble_fixed_spheroid with the derivatives of every output (the directions of a
+ * spheroid's solution, ensemble/particle.rs:142-237 with tmatrix/mod.rs:231-245, through the
+ * averages and the ratios of engine.rs:1782-1836, 2396-2497): P = n_theta + 3 directions, the
+ * distribution's parameters (every distribution of one kind; the size grid held fixed), then the
+ * aspect ratio of the unit's distribution, Re m and Im m of the unit's index. Each node's
+ * derivatives along the aspect ratio and m are those of its solution at its converged N and
+ * n_theta (scatrs_spheroid_compute_d), the weights' along the parameters are exact, and the
+ * averages, the ratios, the Greek coefficients and the phase matrix carry them in forward mode.
+ * The values equal scatrs_ensemble_fixed_spheroid's. d_values[P][11][n_units], d_phase
+ * [P][6][n_units][n_mu] and d_greek[P][6][n_units][L + 1], required beside their value arrays.
+ */
+int scatrs_ensemble_fixed_spheroid_d(const scatrs_distribution* dists, int64_t n_dist,
+                                     const double* wavelengths, int64_t n_wl,
+                                     const double* aspect_ratio, const double* m,
+                                     const double* mu, int64_t n_mu,
+                                     const scatrs_fixed_options* options, double tmatrix_rtol,
+                                     double* values, double* phase, double* greek,
+                                     double* d_values, double* d_phase, double* d_greek,
+                                     int32_t* node_terms, char* err, size_t err_len);
 
 /* Layered spheres (scatrs/src/layered/mod.rs; Particle::LayeredSphere,
  * scatrs/src/ensemble/mod.rs:58-65): n_layers layers, the core first; per distribution the

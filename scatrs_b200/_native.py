@@ -112,6 +112,10 @@ SYMBOLS = {
     "scatrs_ensemble_fixed_spheroid": (ctypes.c_int, [_VP, _I64, _PD, _I64, _PD, _PD, _PD, _I64,
                                                       ctypes.POINTER(FixedOptions), _D, _PD, _PD,
                                                       _PD, _VP, _CP, _SZ]),
+    "scatrs_ensemble_fixed_spheroid_d": (ctypes.c_int, [_VP, _I64, _PD, _I64, _PD, _PD, _PD,
+                                                        _I64, ctypes.POINTER(FixedOptions), _D,
+                                                        _PD, _PD, _PD, _PD, _PD, _PD, _VP, _CP,
+                                                        _SZ]),
     "scatrs_ensemble_fixed_d": (ctypes.c_int, [_VP, _I64, _PD, _I64, _PD, _PD, _I64,
                                                ctypes.POINTER(FixedOptions), _PD, _PD, _PD, _PD,
                                                _PD, _PD, _CP, _SZ]),
@@ -159,6 +163,9 @@ SYMBOLS = {
                                                     _SZ]),
     "scatrs_spheroid_compute": (ctypes.c_int, [_I64, _PD, _PD, _PD, ctypes.POINTER(SpheroidOptions),
                                                _PD, _PD, _VP, _VP, _PD, _CP, _SZ]),
+    "scatrs_spheroid_compute_d": (ctypes.c_int, [_I64, _PD, _PD, _PD,
+                                                 ctypes.POINTER(SpheroidOptions), _PD, _PD, _PD,
+                                                 _PD, _VP, _VP, _PD, _CP, _SZ]),
     "scatrs_spheroid_work": (ctypes.c_int64, [_VP, _I64]),
     "scatrs_check_errors": (ctypes.c_int, [_VP, _CP, _SZ]),
     "scatrs_mie": (ctypes.c_int, [_PD, _PD, _I64, _I32, _PI64, _PI64, _PD, _PD, _CP, _SZ]),
@@ -384,6 +391,40 @@ def ensemble_fixed_spheroid(dists: np.ndarray, wavelengths, aspect_ratio, m, mu,
                                                terms.ctypes.data, err, 1024)
     _check(st, err)
     return values, phase, greek, terms
+
+
+def ensemble_fixed_spheroid_d(dists: np.ndarray, wavelengths, aspect_ratio, m, mu,
+                              n_nodes: int, greek_order: int = -1, normalized: bool = True,
+                              tmatrix_rtol: float = 1e-8):
+    """ensemble_fixed_spheroid with the derivatives along the distribution's parameters, the
+    aspect ratio, Re m and Im m (P of them): returns (values, phase, greek, d_values, d_phase,
+    d_greek, node_terms), the derivative arrays shaped (P,) + the value array's shape."""
+    require_device()
+    dists = np.ascontiguousarray(dists, dtype=DIST_DTYPE)
+    wl = np.ascontiguousarray(wavelengths, dtype=np.float64).reshape(-1)
+    eps = np.ascontiguousarray(np.broadcast_to(np.asarray(aspect_ratio, dtype=np.float64),
+                                               (dists.size,)))
+    m = np.ascontiguousarray(np.broadcast_to(np.asarray(m, dtype=np.complex128),
+                                             (dists.size, wl.size)))
+    mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
+    n = dists.size * wl.size
+    kind = int(dists["kind"][0]) if dists.size else 1
+    P = {3: 3, 4: 1, TABULATED: 0}.get(kind, 2) + 3
+    opts = FixedOptions(int(n_nodes), int(greek_order), int(normalized), 0)
+    values = np.zeros((11, n))
+    d_values = np.zeros((P, 11, n))
+    phase = np.zeros((6, n, mu.size)) if mu.size else None
+    d_phase = np.zeros((P, 6, n, mu.size)) if mu.size else None
+    greek = np.zeros((6, n, greek_order + 1)) if greek_order >= 0 else None
+    d_greek = np.zeros((P, 6, n, greek_order + 1)) if greek_order >= 0 else None
+    terms = np.zeros((n, int(n_nodes), 2), dtype=np.int32)
+    err = ctypes.create_string_buffer(1024)
+    st = load().scatrs_ensemble_fixed_spheroid_d(
+        dists.ctypes.data, dists.size, _p(wl), wl.size, _p(eps), _p(m.view(np.float64)), _p(mu),
+        mu.size, ctypes.byref(opts), float(tmatrix_rtol), _p(values), _p(phase), _p(greek),
+        _p(d_values), _p(d_phase), _p(d_greek), terms.ctypes.data, err, 1024)
+    _check(st, err)
+    return values, phase, greek, d_values, d_phase, d_greek, terms
 
 
 def ensemble_fixed_d(dists: np.ndarray, wavelengths, m, mu, n_nodes: int, greek_order: int = -1,
@@ -816,6 +857,36 @@ def spheroid_compute(x, aspect_ratio, m, rtol: float = 1e-8, n_terms: int = 0, n
                                           nth.ctypes.data, _p(est), err, 1024), err)
     return {"efficiencies": eff, "greek": greek, "n_terms": nt, "n_theta": nth,
             "error_estimate": est}
+
+
+SPHEROID_DIRECTIONS = ("x", "aspect_ratio", "m_re", "m_im")
+
+
+def spheroid_compute_d(x, aspect_ratio, m, rtol: float = 1e-8, n_terms: int = 0,
+                       n_theta: int = 0, greek_order: int = -1, normalized: bool = True) -> dict:
+    """spheroid_compute with the derivatives of the efficiencies and Greek coefficients along
+    x, the aspect ratio, Re m and Im m (scatrs_spheroid_compute_d): d_efficiencies (4, n, 5),
+    d_greek (4, n, 6, order + 1), in the order of SPHEROID_DIRECTIONS."""
+    require_device()
+    x = np.ascontiguousarray(np.atleast_1d(x), dtype=np.float64)
+    eps = np.ascontiguousarray(np.broadcast_to(np.asarray(aspect_ratio, dtype=np.float64), x.shape))
+    mm = np.ascontiguousarray(np.broadcast_to(np.asarray(m, dtype=np.complex128), x.shape))
+    n = x.size
+    eff = np.zeros((n, 5))
+    d_eff = np.zeros((4, n, 5))
+    greek = np.zeros((n, 6, greek_order + 1)) if greek_order >= 0 else None
+    d_greek = np.zeros((4, n, 6, greek_order + 1)) if greek_order >= 0 else None
+    nt = np.zeros(n, dtype=np.int32)
+    nth = np.zeros(n, dtype=np.int32)
+    est = np.zeros(n)
+    o = SpheroidOptions(rtol, n_terms, n_theta, greek_order, int(normalized))
+    err = ctypes.create_string_buffer(1024)
+    _check(load().scatrs_spheroid_compute_d(n, _p(x), _p(eps), _p(mm.view(np.float64)),
+                                            ctypes.byref(o), _p(eff), _p(greek), _p(d_eff),
+                                            _p(d_greek), nt.ctypes.data, nth.ctypes.data,
+                                            _p(est), err, 1024), err)
+    return {"efficiencies": eff, "greek": greek, "d_efficiencies": d_eff, "d_greek": d_greek,
+            "n_terms": nt, "n_theta": nth, "error_estimate": est}
 
 
 def check_errors(stream: int = 0) -> None:

@@ -145,6 +145,58 @@ def ensemble_fixed(theta: torch.Tensor, m_re: torch.Tensor, m_im: torch.Tensor, 
     return _FixedEnsemble.apply(theta, m_re, m_im, spec)
 
 
+class _SpheroidEnsemble(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, theta, aspect_ratio, m_re, m_im, spec):
+        dists, wl, mu, n_nodes, greek_order, normalized, rtol = spec
+        d = dists.copy()
+        n_th = _theta_count(d)
+        d["param"][:, :n_th] = theta.detach().to("cpu", torch.float64).numpy()
+        dev = m_re.device
+        m = (m_re.detach().to("cpu", torch.float64).numpy()
+             + 1j * m_im.detach().to("cpu", torch.float64).numpy())
+        eps = aspect_ratio.detach().to("cpu", torch.float64).numpy()
+        res = _native.ensemble_fixed_spheroid_d(d, wl, eps, m, mu, n_nodes, greek_order,
+                                                normalized, rtol)
+        empty = torch.zeros(0, dtype=torch.float64, device=dev)
+        v, ph, g = (torch.from_numpy(a).to(dev) if a is not None else empty for a in res[:3])
+        ctx.jac = tuple(torch.from_numpy(a).to(dev) if a is not None else None
+                        for a in res[3:6])
+        ctx.n_dist, ctx.n_wl, ctx.n_th = d.size, wl.size, n_th
+        return v, ph, g
+
+    @staticmethod
+    def backward(ctx, gv, gph, gg):
+        total = _contract((gv, gph, gg), ctx.jac)
+        if total is None:
+            return None, None, None, None, None
+        n_th = ctx.n_th
+        per_unit = total.reshape(total.shape[0], ctx.n_dist, ctx.n_wl)
+        g_theta = per_unit[:n_th].sum(dim=2).transpose(0, 1)   # (n_dist, n_th)
+        g_eps = per_unit[n_th].sum(dim=1)                      # (n_dist,)
+        g_re, g_im = per_unit[n_th + 1], per_unit[n_th + 2]     # (n_dist, n_wl)
+        return g_theta, g_eps, g_re, g_im, None
+
+
+def ensemble_fixed_spheroid(theta: torch.Tensor, aspect_ratio: torch.Tensor, m_re: torch.Tensor,
+                            m_im: torch.Tensor, *, kind: str, ranges, wavelengths, mu=None,
+                            n_nodes: int = 64, greek_order: int = -1, normalized: bool = True,
+                            tmatrix_rtol: float = 1e-8):
+    """Differentiable fixed-grid ensemble of randomly oriented spheroids.
+
+    ``theta`` (n_dist, P) the distributions' parameters (as ensemble_fixed's), ``aspect_ratio``
+    (n_dist,) each distribution's spheroid aspect ratio, ``m_re``, ``m_im`` (n_dist, n_wl) the
+    index, ``ranges`` (n_dist, 2) the fixed grid of volume-equivalent radii. Returns (values,
+    phase, greek) as ensemble_fixed does; gradients flow to theta, aspect_ratio, m_re and m_im
+    (scatrs_ensemble_fixed_spheroid_d: each node's solution differentiated at its converged N
+    and n_theta, the averages and ratios in forward mode)."""
+    d = _grid(kind, ranges)
+    wl = np.ascontiguousarray(wavelengths, dtype=np.float64).reshape(-1)
+    mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
+    spec = (d, wl, mu, int(n_nodes), int(greek_order), bool(normalized), float(tmatrix_rtol))
+    return _SpheroidEnsemble.apply(theta, aspect_ratio, m_re, m_im, spec)
+
+
 class _LayeredEnsemble(torch.autograd.Function):
     @staticmethod
     def forward(ctx, theta, fractions, m_re, m_im, spec):

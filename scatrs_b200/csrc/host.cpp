@@ -2775,6 +2775,125 @@ void spheroid_solve(Context& c, int64_t n, const double* x, const double* aspect
   }
 }
 
+// The outputs of spheroids at a given truncation N and node count n_theta each (no convergence
+// loop): every mode at that discretization, the orientation average, and per spheroid the
+// efficiencies (Q_ext, Q_sca, Q_abs, Q_back, g) followed by the Greek coefficients [6][L + 1]
+// (normalized by alpha1_0, or unnormalized: times 4 / x^2; zero above 2N), as
+// scatrs_spheroid_compute reports them.
+struct SphEval {
+  double x, eps, m_re, m_im;
+  int N, nth;
+};
+void spheroid_fixed_outputs(Context& c, const std::vector<SphEval>& ev, int order,
+                            bool normalized, std::vector<std::vector<double>>& out,
+                            cudaStream_t s) {
+  std::vector<TmSpec> specs;
+  std::vector<int64_t> owner;
+  for (size_t i = 0; i < ev.size(); ++i)
+    for (int mm = 0; mm <= ev[i].N; ++mm) {
+      specs.push_back({ev[i].x, ev[i].eps, ev[i].m_re, ev[i].m_im, mm, ev[i].N, ev[i].nth});
+      owner.push_back((int64_t)i);
+    }
+  std::vector<double> sums;
+  std::vector<std::vector<double>> greeks;
+  run_tmatrices(c, specs, sums, nullptr, s, &greeks);
+  std::vector<double> ext(ev.size(), 0.0), sca(ev.size(), 0.0);
+  for (size_t k = 0; k < specs.size(); ++k) {
+    const double w = specs[k].m == 0 ? 1.0 : 2.0;
+    ext[owner[k]] += w * sums[3 * k];
+    sca[owner[k]] += w * sums[3 * k + 1];
+  }
+  const double pi = 3.14159265358979323846;
+  const int64_t len = (int64_t)order + 1;
+  out.assign(ev.size(), {});
+  for (size_t i = 0; i < ev.size(); ++i) {
+    const double x = ev[i].x, area = pi * x * x;
+    const std::vector<double>& gr = greeks[i];
+    const int64_t have = 2 * (int64_t)ev[i].N + 1;
+    const double a0 = gr[0];
+    double f11 = 0.0;
+    for (int64_t l = 0; l < have; ++l) f11 += (l % 2 ? -1.0 : 1.0) * gr[l];
+    std::vector<double>& o = out[i];
+    o.assign(5 + (order >= 0 ? 6 * len : 0), 0.0);
+    o[0] = 2.0 * pi * ext[i] / area;
+    o[1] = 2.0 * pi * sca[i] / area;
+    o[2] = o[0] - o[1];
+    o[3] = 4.0 * pi * f11 / area;
+    o[4] = a0 > 0.0 ? (have > 1 ? gr[1] : 0.0) / (3.0 * a0) : 0.0;
+    if (order < 0) continue;
+    const double scale = normalized ? 1.0 / a0 : 4.0 / (x * x);
+    for (int f = 0; f < 6; ++f)
+      for (int64_t l = 0; l < len; ++l)
+        o[5 + f * len + l] = l < have ? scale * gr[f * have + l] : 0.0;
+    if (normalized) o[5] = 1.0;
+  }
+}
+
+// The derivatives of those outputs along x, the aspect ratio, Re m and Im m at each spheroid's
+// converged (N, n_theta) -- the derivatives of the discretized solution, as the reference's
+// compute_with_derivatives takes them (tmatrix/mod.rs:231-245). They are formed from the
+// outputs at perturbed parameters, solved at the same (N, n_theta) in one batch: per direction
+// the central differences at steps h and h/2 (h = 1e-4 of x, of the aspect ratio, of |m|),
+// Richardson-extrapolated (truncation O(h^4)); along Im m, whose values cannot go below zero,
+// the one-sided fourth-order stencil on the steps h, 2h, 3h, 4h when Im m < 4h. d[dir][i] holds
+// spheroid i's output vector's derivative.
+void spheroid_fixed_derivs(Context& c, const std::vector<SphEval>& base, int order,
+                           bool normalized, std::vector<std::vector<double>> d[4],
+                           cudaStream_t s, unsigned dir_mask = 0xF) {
+  std::vector<SphEval> ev;
+  struct Plan {
+    double h;
+    bool forward;
+  };
+  std::vector<Plan> plan(4 * base.size());
+  for (size_t i = 0; i < base.size(); ++i) {
+    const SphEval& b = base[i];
+    const double mag = std::hypot(b.m_re, b.m_im);
+    const double hs[4] = {1e-4 * b.x, 1e-4 * b.eps, 1e-4 * mag, 1e-4 * mag};
+    for (int dir = 0; dir < 4; ++dir) {
+      Plan& p = plan[4 * i + dir];
+      p.h = hs[dir];
+      if (!(dir_mask >> dir & 1u)) continue;
+      p.forward = dir == 3 && b.m_im < 4.0 * p.h;
+      const double steps_c[4] = {p.h, -p.h, 0.5 * p.h, -0.5 * p.h};
+      const double steps_f[4] = {p.h, 2.0 * p.h, 3.0 * p.h, 4.0 * p.h};
+      for (int k = 0; k < 4; ++k) {
+        const double st = p.forward ? steps_f[k] : steps_c[k];
+        SphEval e = b;
+        if (dir == 0) e.x += st;
+        if (dir == 1) e.eps += st;
+        if (dir == 2) e.m_re += st;
+        if (dir == 3) e.m_im += st;
+        ev.push_back(e);
+      }
+    }
+  }
+  std::vector<std::vector<double>> val, at;
+  spheroid_fixed_outputs(c, base, order, normalized, val, s);
+  spheroid_fixed_outputs(c, ev, order, normalized, at, s);
+  const int n_dirs = __builtin_popcount(dir_mask & 0xFu);
+  for (int dir = 0; dir < 4; ++dir) d[dir].assign(base.size(), {});
+  for (size_t i = 0; i < base.size(); ++i)
+    for (int dir = 0, slot = 0; dir < 4; ++dir) {
+      if (!(dir_mask >> dir & 1u)) continue;
+      const Plan& p = plan[4 * i + dir];
+      const size_t k0 = 4 * (n_dirs * i + slot++);
+      const std::vector<double>& f0 = val[i];
+      std::vector<double>& o = d[dir][i];
+      o.assign(f0.size(), 0.0);
+      for (size_t q = 0; q < f0.size(); ++q) {
+        const double a = at[k0][q], b = at[k0 + 1][q], a2 = at[k0 + 2][q], b2 = at[k0 + 3][q];
+        if (p.forward) {
+          // f'(0) = (-25 f0 + 48 f1 - 36 f2 + 16 f3 - 3 f4) / (12 h)
+          o[q] = (-25.0 * f0[q] + 48.0 * a - 36.0 * b + 16.0 * a2 - 3.0 * b2) / (12.0 * p.h);
+        } else {
+          const double dh = (a - b) / (2.0 * p.h), dh2 = (a2 - b2) / p.h;
+          o[q] = (4.0 * dh2 - dh) / 3.0;
+        }
+      }
+    }
+}
+
 // A value and its error bound, propagated to first order through the ratios (lin.rs:7-68,
 // without derivatives).
 struct LinE {
@@ -4115,6 +4234,50 @@ int scatrs_spheroid_compute(int64_t n, const double* x, const double* aspect_rat
   });
 }
 
+int scatrs_spheroid_compute_d(int64_t n, const double* x, const double* aspect_ratio,
+                              const double* m, const scatrs_spheroid_options* options,
+                              double* eff, double* greek, double* d_eff, double* d_greek,
+                              int32_t* n_terms, int32_t* n_theta, double* error_estimate,
+                              char* err, size_t err_len) {
+  return guarded(err, err_len, [&] {
+    if (n < 0) throw Failure{SCATRS_INVALID_INPUT, "negative sizes"};
+    if (!options) throw Failure{SCATRS_INVALID_INPUT, "options are required"};
+    const scatrs_spheroid_options& o = *options;
+    if (o.n_terms < 0 || o.n_theta < 0 || o.greek_order < -1 || o.greek_order > (1 << 20))
+      throw Failure{SCATRS_INVALID_INPUT, "n_terms, n_theta >= 0 and greek_order >= -1 needed"};
+    if (n == 0) return;
+    if (!eff || !d_eff) throw Failure{SCATRS_INVALID_INPUT, "eff and d_eff are required"};
+    if (o.greek_order >= 0 && (!greek || !d_greek))
+      throw Failure{SCATRS_INVALID_INPUT, "greek and d_greek are required with greek_order >= 0"};
+    Context& c = context();
+    std::lock_guard<std::mutex> lk(c.mtx);
+    std::vector<SpheroidResult> res;
+    spheroid_solve(c, n, x, aspect_ratio, m, o.rtol, o.n_terms, o.n_theta, false, res, 0);
+    std::vector<SphEval> base(n);
+    for (int64_t i = 0; i < n; ++i) {
+      base[i] = {x[i], aspect_ratio[i], m[2 * i], m[2 * i + 1], res[i].n, res[i].nth};
+      if (n_terms) n_terms[i] = res[i].n;
+      if (n_theta) n_theta[i] = res[i].nth;
+      if (error_estimate) error_estimate[i] = res[i].err_est;
+    }
+    std::vector<std::vector<double>> val, d[4];
+    spheroid_fixed_outputs(c, base, o.greek_order, o.normalized != 0, val, 0);
+    spheroid_fixed_derivs(c, base, o.greek_order, o.normalized != 0, d, 0);
+    const int64_t len = (int64_t)o.greek_order + 1;
+    for (int64_t i = 0; i < n; ++i) {
+      for (int q = 0; q < 5; ++q) eff[5 * i + q] = val[i][q];
+      for (int dir = 0; dir < 4; ++dir)
+        for (int q = 0; q < 5; ++q) d_eff[(dir * n + i) * 5 + q] = d[dir][i][q];
+      if (o.greek_order < 0) continue;
+      for (int64_t q = 0; q < 6 * len; ++q) {
+        greek[6 * len * i + q] = val[i][5 + q];
+        for (int dir = 0; dir < 4; ++dir)
+          d_greek[(dir * n + i) * 6 * len + q] = d[dir][i][5 + q];
+      }
+    }
+  });
+}
+
 int scatrs_ensemble_fixed_spheroid(const scatrs_distribution* dists, int64_t n_dist,
                                    const double* wavelengths, int64_t n_wl,
                                    const double* aspect_ratio, const double* m, const double* mu,
@@ -4253,6 +4416,245 @@ int scatrs_ensemble_fixed_spheroid(const scatrs_distribution* dists, int64_t n_d
             f[5] += G[3 * glen + l] * d00[l];
           }
           for (int k = 0; k < 6; ++k) phase[((int64_t)k * n_units + u) * n_mu + j] = sc * f[k];
+        }
+      }
+    }
+  });
+}
+
+}  // extern "C"
+
+namespace {
+// A value with its derivatives along up to 8 directions (forward mode), for the host assembly of
+// the spheroid ensemble's derivative blocks.
+struct DualP {
+  double v = 0.0;
+  double d[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  static int P;
+};
+int DualP::P = 0;
+DualP operator+(const DualP& a, const DualP& b) {
+  DualP o;
+  o.v = a.v + b.v;
+  for (int k = 0; k < DualP::P; ++k) o.d[k] = a.d[k] + b.d[k];
+  return o;
+}
+DualP operator-(const DualP& a, const DualP& b) {
+  DualP o;
+  o.v = a.v - b.v;
+  for (int k = 0; k < DualP::P; ++k) o.d[k] = a.d[k] - b.d[k];
+  return o;
+}
+DualP operator*(const DualP& a, const DualP& b) {
+  DualP o;
+  o.v = a.v * b.v;
+  for (int k = 0; k < DualP::P; ++k) o.d[k] = a.d[k] * b.v + a.v * b.d[k];
+  return o;
+}
+DualP operator*(double a, const DualP& b) {
+  DualP o;
+  o.v = a * b.v;
+  for (int k = 0; k < DualP::P; ++k) o.d[k] = a * b.d[k];
+  return o;
+}
+DualP operator/(const DualP& a, const DualP& b) {
+  DualP o;
+  o.v = a.v / b.v;
+  for (int k = 0; k < DualP::P; ++k) o.d[k] = (a.d[k] - o.v * b.d[k]) / b.v;
+  return o;
+}
+}  // namespace
+
+extern "C" {
+
+int scatrs_ensemble_fixed_spheroid_d(const scatrs_distribution* dists, int64_t n_dist,
+                                     const double* wavelengths, int64_t n_wl,
+                                     const double* aspect_ratio, const double* m,
+                                     const double* mu, int64_t n_mu,
+                                     const scatrs_fixed_options* options, double tmatrix_rtol,
+                                     double* values, double* phase, double* greek,
+                                     double* d_values, double* d_phase, double* d_greek,
+                                     int32_t* node_terms, char* err, size_t err_len) {
+  return guarded(err, err_len, [&] {
+    if (n_dist < 0 || n_wl < 0) throw Failure{SCATRS_INVALID_INPUT, "negative sizes"};
+    for (int64_t i = 0; i < n_wl; ++i)
+      if (!(std::isfinite(wavelengths[i]) && wavelengths[i] > 0.0))
+        throw Failure{SCATRS_INVALID_INPUT, "wavelengths must be finite and > 0"};
+    const int n_theta = n_dist > 0 ? parameter_count(dists[0].kind) : 2;
+    const int P = n_theta + 3;
+    const int64_t n_units = n_dist * n_wl;
+    check_options(options, n_units, n_mu, mu);
+    if (n_units == 0) return;
+    if (!aspect_ratio || !m || !values || !d_values)
+      throw Failure{SCATRS_INVALID_INPUT, "aspect_ratio, m, values and d_values are required"};
+    for (int64_t d = 0; d < n_dist; ++d)
+      if (dists[d].kind != dists[0].kind)
+        throw Failure{SCATRS_INVALID_INPUT, "derivatives need every distribution of one kind"};
+    const int64_t n_nodes = options->n_nodes;
+    const int L = options->greek_order;
+    if ((L >= 0 && greek && !d_greek) || (n_mu > 0 && phase && !d_phase))
+      throw Failure{SCATRS_INVALID_INPUT, "each output array needs its derivative array"};
+    Context& c = context();
+    std::lock_guard<std::mutex> lk(c.mtx);
+    // The nodes and weights as scatrs_ensemble_fixed_spheroid's, with the weights' derivatives
+    // along the distribution's parameters (the grid [r_lo, r_hi] held fixed).
+    const auto& gl = rule(c, n_nodes);
+    std::vector<double> radius(n_dist * n_nodes);
+    std::vector<DualP> weight(n_dist * n_nodes);
+    DualP::P = P;
+    for (int64_t d = 0; d < n_dist; ++d) {
+      std::string msg;
+      if (!(dists[d].kind == kTabulated
+                ? validate_table(dists[d].table, dists[d].table_len, &msg)
+                : validate_distribution(dists[d].kind, dists[d].param, &msg)))
+        throw Failure{SCATRS_INVALID_INPUT, "distribution " + std::to_string(d) + ": " + msg};
+      if (!(dists[d].r_lo > 0.0 && dists[d].r_hi > dists[d].r_lo && std::isfinite(dists[d].r_hi)))
+        throw Failure{SCATRS_INVALID_INPUT, "distribution " + std::to_string(d) +
+                                                ": the grid needs 0 < r_lo < r_hi < inf"};
+      const double a = std::log(dists[d].r_lo), b = std::log(dists[d].r_hi);
+      const double ctr = 0.5 * (a + b), h = 0.5 * (b - a);
+      for (int64_t j = 0; j < n_nodes; ++j) {
+        const double r = std::exp(ctr + h * gl.first[j]);
+        radius[d * n_nodes + j] = r;
+        double g[3] = {0.0, 0.0, 0.0};
+        const double u = dists[d].kind == kTabulated
+                             ? node_density(dists[d], r)
+                             : density_gradient(dists[d].kind, dists[d].param, r, g);
+        DualP& W = weight[d * n_nodes + j];
+        W.v = h * gl.second[j] * (u * r);
+        for (int k = 0; k < n_theta; ++k) W.d[k] = h * gl.second[j] * (g[k] * r);
+      }
+    }
+    const int64_t n_sph = n_units * n_nodes;
+    std::vector<double> xs(n_sph), es(n_sph), ms(2 * n_sph);
+    const double pi = 3.14159265358979323846;
+    for (int64_t d = 0; d < n_dist; ++d)
+      for (int64_t w = 0; w < n_wl; ++w)
+        for (int64_t j = 0; j < n_nodes; ++j) {
+          const int64_t u = d * n_wl + w, k = u * n_nodes + j;
+          xs[k] = 2.0 * pi * radius[d * n_nodes + j] / wavelengths[w];
+          es[k] = aspect_ratio[d];
+          ms[2 * k] = m[2 * u];
+          ms[2 * k + 1] = m[2 * u + 1];
+        }
+    // Every node converged as the value entry converges it, then its outputs and their
+    // derivatives along the aspect ratio, Re m and Im m at that (N, n_theta).
+    std::vector<SpheroidResult> res;
+    spheroid_solve(c, n_sph, xs.data(), es.data(), ms.data(), tmatrix_rtol, 0, 0, false, res, 0);
+    std::vector<SphEval> base(n_sph);
+    int top_all = 0;
+    for (int64_t k = 0; k < n_sph; ++k) {
+      base[k] = {xs[k], es[k], ms[2 * k], ms[2 * k + 1], res[k].n, res[k].nth};
+      top_all = std::max(top_all, 2 * res[k].n);
+      if (node_terms) {
+        node_terms[2 * k] = res[k].n;
+        node_terms[2 * k + 1] = res[k].nth;
+      }
+    }
+    std::vector<std::vector<double>> val, dd4[4];
+    spheroid_fixed_outputs(c, base, top_all, false, val, 0);
+    spheroid_fixed_derivs(c, base, top_all, false, dd4, 0, 0xEu);
+    const int64_t gl_all = (int64_t)top_all + 1;
+    // Node k's output q as a dual: its derivatives along the aspect ratio, Re m and Im m in
+    // directions n_theta .. n_theta + 2.
+    auto node_out = [&](int64_t k, int64_t q) {
+      DualP o;
+      o.v = val[k][q];
+      for (int dir = 1; dir < 4; ++dir) o.d[n_theta + dir - 1] = dd4[dir][k][q];
+      return o;
+    };
+    std::vector<double> d00, d22, d2m2, d02;
+    auto put = [&](double* v, double* dv, int64_t idx, int64_t block, const DualP& x) {
+      v[idx] = x.v;
+      for (int k = 0; k < P; ++k) dv[k * block + idx] = x.d[k];
+    };
+    for (int64_t u = 0; u < n_units; ++u) {
+      const int64_t d = u / n_wl;
+      DualP Z, ext, sca, scag, ab, back, r2, r3, dep;
+      int64_t top = 0;
+      for (int64_t j = 0; j < n_nodes; ++j) top = std::max<int64_t>(top, 2 * res[u * n_nodes + j].n);
+      const int64_t glen = std::max<int64_t>(top, L) + 1;
+      std::vector<DualP> G(6 * glen);
+      for (int64_t j = 0; j < n_nodes; ++j) {
+        const int64_t k = u * n_nodes + j;
+        const double r = radius[d * n_nodes + j], area = pi * r * r;
+        const DualP& W = weight[d * n_nodes + j];
+        const int64_t have = 2 * (int64_t)res[k].n + 1;
+        const DualP q_ext = node_out(k, 0), q_sca = node_out(k, 1), q_abs = node_out(k, 2);
+        const DualP q_back = node_out(k, 3), g = node_out(k, 4);
+        DualP depol;  // Q_back - Q_sca F22(180 deg) (particle.rs:276-285)
+        for (int64_t l = 0; l < have; ++l) {
+          const DualP t = node_out(k, 5 + l) -
+                          0.5 * (node_out(k, 5 + gl_all + l) - node_out(k, 5 + 2 * gl_all + l));
+          depol = l % 2 ? depol - t : depol + t;
+        }
+        Z = Z + W;
+        ext = ext + W * (area * q_ext);
+        sca = sca + W * (area * q_sca);
+        scag = scag + W * (area * (q_sca * g));
+        ab = ab + W * (area * q_abs);
+        back = back + W * (area * q_back);
+        DualP rr;
+        rr.v = r * r;
+        r2 = r2 + W * rr;
+        rr.v = r * r * r;
+        r3 = r3 + W * rr;
+        dep = dep + W * (area * depol);
+        for (int f = 0; f < 6; ++f)
+          for (int64_t l = 0; l < have; ++l)
+            G[f * glen + l] = G[f * glen + l] + W * (area * node_out(k, 5 + f * gl_all + l));
+      }
+      ext = ext / Z, sca = sca / Z, scag = scag / Z, ab = ab / Z, back = back / Z;
+      r2 = r2 / Z, r3 = r3 / Z, dep = dep / Z;
+      for (DualP& gg : G) gg = gg / Z;
+      if (!(std::isfinite(ext.v) && ext.v != 0.0 && std::isfinite(sca.v) && sca.v != 0.0 &&
+            std::isfinite(back.v) && back.v != 0.0))
+        throw Failure{SCATRS_INVALID_INPUT, "unit " + std::to_string(u) +
+                                                ": <C_ext>, <C_sca> or <C_back> is zero or not "
+                                                "finite, so the ratios are undefined"};
+      const DualP vals[11] = {ext,  sca, ab, back, sca / ext, scag / sca,
+                              (4 * pi) * ext / back, dep / (2.0 * back - dep), r3 / r2,
+                              pi * r2, (4 * pi / 3) * r3};
+      for (int k = 0; k < 11; ++k) put(values, d_values, k * n_units + u, 11 * n_units, vals[k]);
+      if (L >= 0 && greek) {
+        DualP one;
+        one.v = 1.0;
+        const DualP sc = options->normalized ? one / G[0] : one;
+        const int64_t block = 6 * n_units * ((int64_t)L + 1);
+        for (int f = 0; f < 6; ++f)
+          for (int64_t l = 0; l <= L; ++l) {
+            const DualP gv = l <= top ? sc * G[f * glen + l] : DualP{};
+            put(greek, d_greek, ((int64_t)f * n_units + u) * (L + 1) + l, block, gv);
+          }
+        if (options->normalized) put(greek, d_greek, u * (L + 1), block, one);
+      }
+      if (n_mu > 0 && phase) {
+        const int64_t len = top + 1;
+        d00.resize(len);
+        d22.resize(len);
+        d2m2.resize(len);
+        d02.resize(len);
+        DualP one;
+        one.v = 1.0;
+        const DualP sc = options->normalized ? one / sca : one;
+        const int64_t block = 6 * n_units * n_mu;
+        for (int64_t j = 0; j < n_mu; ++j) {
+          wigner_d(0, 0, mu[j], d00.data(), len);
+          wigner_d(2, 2, mu[j], d22.data(), len);
+          wigner_d(2, -2, mu[j], d2m2.data(), len);
+          wigner_d(0, 2, mu[j], d02.data(), len);
+          DualP f[6];
+          for (int64_t l = 0; l < len; ++l) {
+            const double plus = 0.5 * (d22[l] + d2m2[l]), minus = 0.5 * (d22[l] - d2m2[l]);
+            f[0] = f[0] + d00[l] * G[0 * glen + l];
+            f[1] = f[1] + d02[l] * G[4 * glen + l];
+            f[2] = f[2] + plus * G[1 * glen + l] + minus * G[2 * glen + l];
+            f[3] = f[3] + minus * G[1 * glen + l] + plus * G[2 * glen + l];
+            f[4] = f[4] + d02[l] * G[5 * glen + l];
+            f[5] = f[5] + d00[l] * G[3 * glen + l];
+          }
+          for (int k = 0; k < 6; ++k)
+            put(phase, d_phase, ((int64_t)k * n_units + u) * n_mu + j, block, sc * f[k]);
         }
       }
     }
