@@ -255,8 +255,27 @@ std::vector<std::pair<double, double>> initial_panels(double t_lo, double t_hi, 
 // parameter), |Kronrod - Gauss| of the same, the Kronrod sums of |du/dtheta| r |q| and of
 // u r |q| (the scales of the parameter blocks and of the derivatives along m), and the
 // integrands per unit ln r at the first and last nodes.
+// One panel's pass-1 sums for one part, in one buffer (a panel of a job of many parts holds one
+// per part): the Kronrod sums k[nb] and their |Kronrod - Gauss| errors err[nb], the parameter
+// blocks' absolute integrals abs[nt nr], the absolute value integrals absv[nr], and the
+// integrands at the panel's two ends edge(0)[nb], edge(1)[nb].
 struct Sums1 {
-  std::vector<double> k, err, abs, absv, edge[2];
+  std::vector<double> buf;
+  int nb = 0, nab = 0, nr = 0;
+  void init(int nb_, int nab_, int nr_) {
+    nb = nb_, nab = nab_, nr = nr_;
+    buf.assign((size_t)4 * nb + nab + nr, 0.0);
+  }
+  double* k() { return buf.data(); }
+  double* err() { return buf.data() + nb; }
+  double* abs() { return buf.data() + 2 * nb; }
+  double* absv() { return buf.data() + 2 * nb + nab; }
+  double* edge(int e) { return buf.data() + 2 * nb + nab + nr + e * nb; }
+  const double* k() const { return buf.data(); }
+  const double* err() const { return buf.data() + nb; }
+  const double* abs() const { return buf.data() + 2 * nb; }
+  const double* absv() const { return buf.data() + 2 * nb + nab; }
+  const double* edge(int e) const { return buf.data() + 2 * nb + nab + nr + e * nb; }
 };
 
 // The targets, errors and ends of a part (engine.rs:620-720, no Greek refinement).
@@ -273,12 +292,12 @@ Status status_of(const Part& part, const std::vector<const Sums1*>& s, const Opt
   st.target.assign(nb, 0.0);
   auto total = [&](int j) {
     double t = 0.0;
-    for (auto* x : s) t += x->k[j];
+    for (auto* x : s) t += x->k()[j];
     return t;
   };
   auto abs_of = [&](int k) {
     double t = 0.0;
-    for (auto* x : s) t += x->abs[k];
+    for (auto* x : s) t += x->abs()[k];
     return t;
   };
   // C_abs and each direction's derivative of it are refined to rtol of C_ext's.
@@ -297,7 +316,7 @@ Status status_of(const Part& part, const std::vector<const Sums1*>& s, const Opt
     } else if (j >= n_greek) {
       // The derivatives along m can cancel: their absolute integrands.
       scale = 0.0;
-      for (auto* x : s) scale += x->absv[scale_of(j)];
+      for (auto* x : s) scale += x->absv()[scale_of(j)];
     } else {
       scale = std::fabs(total(scale_of(j)));
     }
@@ -317,7 +336,7 @@ Status status_of(const Part& part, const std::vector<const Sums1*>& s, const Opt
   st.met = true;
   for (int j = 0; j < nb; ++j) {
     double e = 0.0;
-    for (auto* x : s) e += x->err[j];
+    for (auto* x : s) e += x->err()[j];
     st.errors[j] = e;
     st.met = st.met && e <= st.target[j];
   }
@@ -332,13 +351,13 @@ Status status_of(const Part& part, const std::vector<const Sums1*>& s, const Opt
       end_target[x] = o.rtol * std::max(std::fabs(total(x)), 1e-3 * abs_of(b * nr + scale_of(j)));
     }
   }
-  auto small = [&](const std::vector<double>& d) {
+  auto small = [&](const double* d) {
     for (int j = 0; j < nb; ++j)
       if (!(std::fabs(d[j]) * (ext / kStep) <= 0.1 * end_target[j])) return false;
     return true;
   };
-  st.small[0] = small(s.front()->edge[0]);
-  st.small[1] = small(s.back()->edge[1]);
+  st.small[0] = small(s.front()->edge(0));
+  st.small[1] = small(s.back()->edge(1));
   return st;
 }
 
@@ -512,31 +531,35 @@ void pass1(std::vector<Job>& jobs, const std::vector<Part>& parts, const double*
     for (auto& ab : initial_panels(st.t_lo, st.t_hi, lambda, breaks, step_of, budget_max))
       st.panels.push_back({ab.first, ab.second});
   }
+  // The rounds' node lists and results, kept across rounds (their memory touched once).
+  std::vector<Query> qs;
+  std::vector<NodeResult> res;
   for (;;) {
-    // Gather this round's nodes.
-    std::vector<Query> qs;
+    // Gather this round's nodes: the open panels in (job, panel) order, then their 15 nodes each
+    // (filled on the host's threads; the order, and so every sum, does not depend on them).
     std::vector<std::pair<size_t, size_t>> owner;  // (job, panel) per 15 nodes
     for (size_t ji = 0; ji < jobs.size(); ++ji) {
       if (states[ji].finished) continue;
-      for (size_t pi = 0; pi < states[ji].panels.size(); ++pi) {
-        Panel& pn = states[ji].panels[pi];
-        if (pn.done) continue;
-        Node nd[15];
-        gk15(pn.a, pn.b, nd);
-        for (const Node& n : nd) qs.push_back({std::exp(n.t), jobs[ji].wl});
-        owner.push_back({ji, pi});
-      }
+      for (size_t pi = 0; pi < states[ji].panels.size(); ++pi)
+        if (!states[ji].panels[pi].done) owner.push_back({ji, pi});
     }
     if (owner.empty()) break;
-    std::vector<NodeResult> res(qs.size());
-    eval(qs, res);
-    // Panel sums, and each job's first failing node in panel order.
-    std::vector<int> first_fail(jobs.size(), -1);
-    for (size_t k = 0; k < owner.size(); ++k) {
-      const size_t ji = owner[k].first, pi = owner[k].second;
-      Panel& pn = states[ji].panels[pi];
+    qs.resize(15 * owner.size());
+#pragma omp parallel for schedule(static)
+    for (int64_t k = 0; k < (int64_t)owner.size(); ++k) {
+      const Panel& pn = states[owner[k].first].panels[owner[k].second];
       Node nd[15];
       gk15(pn.a, pn.b, nd);
+      for (int i = 0; i < 15; ++i) qs[15 * k + i] = {std::exp(nd[i].t), jobs[owner[k].first].wl};
+    }
+    res.resize(qs.size());
+    eval(qs, res);
+    // Each job's first failing node in panel order (in order, on one thread), then the panel
+    // sums of the panels whose nodes all succeeded (each panel on its own, on the host's threads).
+    std::vector<int> first_fail(jobs.size(), -1);
+    std::vector<char> node_ok(owner.size(), 1);
+    for (size_t k = 0; k < owner.size(); ++k) {
+      const size_t ji = owner[k].first, pi = owner[k].second;
       bool ok = true;
       for (int i = 0; i < 15 && ok; ++i)
         if (res[15 * k + i].status != 0) {
@@ -554,7 +577,15 @@ void pass1(std::vector<Job>& jobs, const std::vector<Part>& parts, const double*
                                   "[1e-6, 1e3]");
           }
         }
-      if (!ok) continue;
+      node_ok[k] = ok ? 1 : 0;
+    }
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int64_t k = 0; k < (int64_t)owner.size(); ++k) {
+      if (!node_ok[k]) continue;
+      const size_t ji = owner[k].first, pi = owner[k].second;
+      Panel& pn = states[ji].panels[pi];
+      Node nd[15];
+      gk15(pn.a, pn.b, nd);
       pn.done = true;
       pn.n_terms = 0;
       for (int i = 0; i < 15; ++i) pn.n_terms = std::max(pn.n_terms, res[15 * k + i].n);
@@ -575,12 +606,9 @@ void pass1(std::vector<Job>& jobs, const std::vector<Part>& parts, const double*
         const Part& part = parts[jobs[ji].parts[p]];
         const int nt = (int)part.grads.size(), nb = (1 + nt) * nr;
         Sums1& s = pn.sums[p];
-        s.k.assign(nb, 0.0);
-        s.err.assign(nb, 0.0);
-        s.abs.assign(nt * nr, 0.0);
-        s.absv.assign(nr, 0.0);
-        s.edge[0].assign(nb, 0.0);
-        s.edge[1].assign(nb, 0.0);
+        s.init(nb, nt * nr, nr);
+        double *sk = s.k(), *serr = s.err(), *sabs = s.abs(), *sabsv = s.absv();
+        double *e0 = s.edge(0), *e1 = s.edge(1);
         std::vector<double> g(nb, 0.0);
         for (int i = 0; i < 15; ++i) {
           const double r = qs[15 * k + i].r;
@@ -588,26 +616,28 @@ void pass1(std::vector<Job>& jobs, const std::vector<Part>& parts, const double*
           const double* q = res[15 * k + i].q;
           for (int j = 0; j < nr; ++j) {
             const double qj = q[qi[j]];
-            s.k[j] += nd[i].wk * base * qj;
+            sk[j] += nd[i].wk * base * qj;
             g[j] += nd[i].wg * base * qj;
-            s.absv[j] += nd[i].wk * std::fabs(base * qj);
-            if (i == 0) s.edge[0][j] = base * qj;
-            if (i == 14) s.edge[1][j] = base * qj;
+            sabsv[j] += nd[i].wk * std::fabs(base * qj);
+            if (i == 0) e0[j] = base * qj;
+            if (i == 14) e1[j] = base * qj;
             for (int b = 0; b < nt; ++b) {
               const double dw = grad[part.grads[b]] * r;
               const int x = (1 + b) * nr + j;
-              s.k[x] += nd[i].wk * dw * qj;
+              sk[x] += nd[i].wk * dw * qj;
               g[x] += nd[i].wg * dw * qj;
-              s.abs[b * nr + j] += nd[i].wk * std::fabs(dw * qj);
-              if (i == 0) s.edge[0][x] = dw * qj;
-              if (i == 14) s.edge[1][x] = dw * qj;
+              sabs[b * nr + j] += nd[i].wk * std::fabs(dw * qj);
+              if (i == 0) e0[x] = dw * qj;
+              if (i == 14) e1[x] = dw * qj;
             }
           }
         }
-        for (int j = 0; j < nb; ++j) s.err[j] = std::fabs(s.k[j] - g[j]);
+        for (int j = 0; j < nb; ++j) serr[j] = std::fabs(sk[j] - g[j]);
       }
     }
-    for (size_t ji = 0; ji < jobs.size(); ++ji) {
+    // Each job's targets, extensions and splits (jobs are independent of one another).
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t ji = 0; ji < (int64_t)jobs.size(); ++ji) {
       State& st = states[ji];
       Job& job = jobs[ji];
       if (st.finished) continue;
@@ -697,7 +727,7 @@ void pass1(std::vector<Job>& jobs, const std::vector<Part>& parts, const double*
           for (size_t j = 0; j < stat[p].target.size(); ++j) {
             if (!(stat[p].errors[j] > stat[p].target[j])) continue;
             const double t = std::max(stat[p].target[j], std::numeric_limits<double>::min());
-            bad = std::max(bad, st.panels[i].sums[p].err[j] * (double)n / t);
+            bad = std::max(bad, st.panels[i].sums[p].err()[j] * (double)n / t);
           }
         if (bad > 1.0) cand.push_back({bad, i});
       }
