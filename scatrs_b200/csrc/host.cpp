@@ -1944,6 +1944,8 @@ void adaptive_call_order(const std::vector<AdPart>& in, int n_out, bool batch,
   std::vector<double> wth(deriv ? 3 * radius.size() : 0, 0.0), wthd(wth.size(), 0.0);
   std::vector<char> unit_converged(n_units, 1);
   std::vector<int64_t> unit_panels(n_units, 0);
+  // Every unit's nodes and weights on its own (the host's threads; each unit writes its rows).
+#pragma omp parallel for schedule(dynamic, 4)
   for (int64_t u = 0; u < n_units; ++u) {
     const int64_t p = u / n_wl;
     const adaptive::Part& part = parts[p];
