@@ -196,48 +196,29 @@ __global__ void __launch_bounds__(128) ro_w_kernel(RoArgs a) {
   C2* w = reinterpret_cast<C2*>(a.w + sp.w0);
   // w[qi][sg][p][s][n]
   auto at = [&](int p, int s) -> C2& { return w[(((int64_t)(qi * 2 + sg) * 2 + p) * S + s) * n1 + n]; };
-  if (abs(m) > N || n < max(abs(m), 1)) {
-    for (int p = 0; p < 2; ++p)
-      for (int s = 0; s < S; ++s) at(p, s) = C2{0, 0};
-    return;
-  }
+  for (int p = 0; p < 2; ++p)
+    for (int s = 0; s < S; ++s) at(p, s) = C2{0, 0};
+  if (abs(m) > N || n < max(abs(m), 1)) return;
   double cgv[kS], scratch[kS];
   const C2* rank = reinterpret_cast<const C2*>(a.rank + sp.rank0);
-  // The far field's cosine-independent factor gamma_n (-i)^n (functions.rs:192-239).
-  const C2 fn = c_scale(ipow(-n), sqrt((2.0 * n + 1) / (kPi * 4.0 * n * (n + 1))));
-  // The sums of a window of kWin orders s at a time in registers, each over n' in order (the
-  // Clebsch-Gordan vector of n' recomputed per window it reaches), then written once.
-  constexpr int kWin = 16;
-  for (int s0 = 0; s0 < S; s0 += kWin) {
-    C2 acc[2][kWin];
-#pragma unroll
-    for (int p = 0; p < 2; ++p)
-#pragma unroll
-      for (int k = 0; k < kWin; ++k) acc[p][k] = C2{0, 0};
-    for (int np = 1; np <= N; ++np) {
-      const int smin = abs(n - np), smax = n + np;
-      if (smax < s0 || smin >= s0 + kWin) continue;
-      const int j0 = cg_vector(n, m, np, -sigma, cgv, scratch);
-      if (j0 < 0) continue;
-      const C2 pre = c_scale(ipow(np - 1), 2.0 * sqrt(kPi * (2 * np + 1)) * sgn(np - sigma));
-      const int lo = max(max(j0, smin), s0);
-#pragma unroll
-      for (int p = 0; p < 2; ++p) {
-        const C2* tr = rank + ((int64_t)((p * 2 + sg) * n1 + n) * n1 + np) * S;
-#pragma unroll
-        for (int k = 0; k < kWin; ++k) {
-          const int s = s0 + k;
-          if (s < lo || s > smax) continue;
-          acc[p][k] = c_add(acc[p][k], c_mul(pre, c_scale(tr[s - smin], cgv[s - j0])));
-        }
+  for (int np = 1; np <= N; ++np) {
+    const int j0 = cg_vector(n, m, np, -sigma, cgv, scratch);
+    if (j0 < 0) continue;
+    const int smin = abs(n - np);
+    const C2 pre = c_scale(ipow(np - 1), 2.0 * sqrt(kPi * (2 * np + 1)) * sgn(np - sigma));
+    for (int p = 0; p < 2; ++p) {
+      const C2* tr = rank + ((int64_t)((p * 2 + sg) * n1 + n) * n1 + np) * S;
+      for (int k = 0; j0 + k <= n + np; ++k) {
+        const int s = j0 + k;
+        if (s < smin) continue;
+        at(p, s) = c_add(at(p, s), c_mul(pre, c_scale(tr[s - smin], cgv[k])));
       }
     }
-#pragma unroll
-    for (int p = 0; p < 2; ++p)
-#pragma unroll
-      for (int k = 0; k < kWin; ++k)
-        if (s0 + k < S) at(p, s0 + k) = c_mul(acc[p][k], fn);
   }
+  // The far field's cosine-independent factor gamma_n (-i)^n (functions.rs:192-239).
+  const C2 fn = c_scale(ipow(-n), sqrt((2.0 * n + 1) / (kPi * 4.0 * n * (n + 1))));
+  for (int p = 0; p < 2; ++p)
+    for (int s = 0; s < S; ++s) at(p, s) = c_mul(at(p, s), fn);
 }
 
 __global__ void __launch_bounds__(128) ro_phi_kernel(RoArgs a) {

@@ -7,8 +7,8 @@
 // (its own power-of-two scale) split into five balanced signed bytes (kernels.h).
 // tcgen05.mma kind::i8 (M 128 x N 64 x K 32, operands in shared memory, INT32 accumulators in
 // tensor memory) multiplies the digit pairs (i, j) with i + j < 5, each into the accumulator of
-// its level i + j, where the sums are exact; the epilogue recombines the levels in FP64 and
-// applies the row and column scales. Each product term keeps about 38 bits of the largest
+// its level i + j, where the sums are exact; the epilogue recombines the levels exactly in 64-bit
+// integers, rounds once to FP64 and applies the row and column scales. Each product term keeps about 38 bits of the largest
 // |G| |X| of its row and column, and the terms the truncation drops are centred on zero.
 //
 // A CTA (one per SM, persistent) takes work items (a unit and a share of its row tiles, the
@@ -551,30 +551,39 @@ __global__ void __launch_bounds__(128) x_split_kernel(XSplitArgs a) {
   const int n_kb = (nc + kI8KB - 1) / kI8KB;
   unsigned char* base = a.xdig + a.chunk_xoff[ci];
   for (int kb = 0; kb < n_kb; ++kb) {
-    for (int q = 0; q < kI8KB / 16; ++q) {
-      uint32_t dg[kI8Levels][4];
+    for (int q2 = 0; q2 < kI8KB / 32; ++q2) {
+      // 32 orders' values loaded before any is split, so that their loads are in flight together.
+      double xv[32];
 #pragma unroll
-      for (int s = 0; s < kI8Levels; ++s)
-#pragma unroll
-        for (int u = 0; u < 4; ++u) dg[s][u] = 0;
-#pragma unroll
-      for (int b = 0; b < 16; ++b) {
-        const int k = kb * kI8KB + q * 16 + b;
-        const double x = (k < nc && m > 0.0) ? X[(int64_t)k * 128 + c] : 0.0;
-        long long f = __double2ll_rn(ldexp(x, e + 32));
-        const int sh = 8 * (b & 3);
-        int d[kI8Levels];
-        balanced_digits(f, d);
-#pragma unroll
-        for (int s = 0; s < kI8Levels; ++s) dg[s][b >> 2] |= (uint32_t)(d[s] & 0xff) << sh;
+      for (int b = 0; b < 32; ++b) {
+        const int k = kb * kI8KB + q2 * 32 + b;
+        xv[b] = (k < nc && m > 0.0) ? X[(int64_t)k * 128 + c] : 0.0;
       }
-      const int qs = q ^ ((row >> 1) & 3);
 #pragma unroll
-      for (int s = 0; s < kI8Levels; ++s) {
-        uint4* dst = reinterpret_cast<uint4*>(
-            base + ((int64_t)(half * n_kb + kb) * kI8Levels + s) * (64 * kI8KB) + row * kI8KB +
-            qs * 16);
-        *dst = make_uint4(dg[s][0], dg[s][1], dg[s][2], dg[s][3]);
+      for (int h = 0; h < 2; ++h) {
+        const int q = 2 * q2 + h;
+        uint32_t dg[kI8Levels][4];
+#pragma unroll
+        for (int s = 0; s < kI8Levels; ++s)
+#pragma unroll
+          for (int u = 0; u < 4; ++u) dg[s][u] = 0;
+#pragma unroll
+        for (int b = 0; b < 16; ++b) {
+          long long f = __double2ll_rn(ldexp(xv[16 * h + b], e + 32));
+          const int sh = 8 * (b & 3);
+          int d[kI8Levels];
+          balanced_digits(f, d);
+#pragma unroll
+          for (int s = 0; s < kI8Levels; ++s) dg[s][b >> 2] |= (uint32_t)(d[s] & 0xff) << sh;
+        }
+        const int qs = q ^ ((row >> 1) & 3);
+#pragma unroll
+        for (int s = 0; s < kI8Levels; ++s) {
+          uint4* dst = reinterpret_cast<uint4*>(
+              base + ((int64_t)(half * n_kb + kb) * kI8Levels + s) * (64 * kI8KB) + row * kI8KB +
+              qs * 16);
+          *dst = make_uint4(dg[s][0], dg[s][1], dg[s][2], dg[s][3]);
+        }
       }
     }
   }
