@@ -40,3 +40,26 @@ def test_sample_wavelengths_spans_the_range():
     assert idx[0] == 0 and idx[-1] == 1023 and 60 <= idx.size <= 64
     assert np.all(np.diff(idx) > 0)
     assert np.array_equal(tune.sample_wavelengths(10, 64), np.arange(10))
+
+
+def test_tuning_settings_are_validated_and_restored():
+    """scatrs_set_tuning through the C ABI (no GPU needed): accepted ranges, 0 for the
+    defaults, refusals with the library's messages."""
+    import pytest
+
+    from scatrs_b200 import _native
+    from scatrs_b200.errors import InvalidInputError
+
+    before = _native.get_tuning()
+    try:
+        _native.set_tuning(8, 1 << 20)
+        assert _native.get_tuning() == {"split": 8, "arena_rows": 1 << 20}
+        _native.set_tuning(0, 0)
+        assert _native.get_tuning() == {"split": 4, "arena_rows": 1 << 22}
+        with pytest.raises(InvalidInputError, match="split"):
+            _native.set_tuning(65, 0)
+        with pytest.raises(InvalidInputError, match="arena_rows"):
+            _native.set_tuning(4, 1 << 30)
+        assert _native.get_tuning() == {"split": 4, "arena_rows": 1 << 22}
+    finally:
+        _native.set_tuning(before["split"], before["arena_rows"])
