@@ -15,6 +15,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <tuple>
@@ -53,7 +54,7 @@ enum KernelId {
 };
 static bool g_profiling = false;
 // The spheroid surface integrals' work per tm_surface_kernel launch while profiling: the sum
-// over the launch's modes of K^2 (i, k) pairs times the 2 n_theta nodes.
+// over the launch's modes of K^2 (i, k) pairs times the n_theta nodes of half the surface.
 static std::vector<int64_t> g_tm_pair_nodes;
 struct Timed {
   int id;
@@ -218,8 +219,8 @@ struct Context {
   } i8;
   DevBuf xdig, xside, colmax, chunk_xoff, chunk_xidx, i8_list, i8_err;
   // Spheroid T-matrices.
-  DevBuf tm_geoms, tm_jobs, tm_rules, tm_node, tm_rad, tm_ang, tm_J, tm_work, tm_piv, tm_T, tm_sums,
-      tm_err;
+  DevBuf tm_geoms, tm_jobs, tm_rules, tm_node, tm_rad, tm_ang, tm_ser, tm_J, tm_work, tm_piv, tm_T,
+      tm_sums, tm_err;
   DevBuf ro_sph, ro_rank, ro_w, ro_part, ro_f, ro_greek, ro_mu, ro_proj;
   DevBuf p1_fr, p1_ml;  // layered parts of an adaptive call
   std::map<int64_t, std::vector<double>> dd_rules;  // n -> per node x (hi, lo), w (hi, lo)
@@ -2411,6 +2412,16 @@ const std::vector<double>& dd_rule(Context& c, int64_t n) {
   return c.dd_rules.emplace(n, std::move(out)).first->second;
 }
 
+// The form each element of Q is assembled in: -1 (the cleanest of the three exact ones, the
+// default) or, for diagnostics, the environment's SCATRS_TMATRIX_FORM: 0 plain, 1 without the
+// y-part's terms of power < 0, 2 without those of power <= 0 (each where it applies).
+int tm_form_override() {
+  const char* v = std::getenv("SCATRS_TMATRIX_FORM");
+  if (!v || !*v) return -1;
+  const int f = std::atoi(v);
+  return f >= 0 && f <= 2 ? f : -1;
+}
+
 // Runs the T-matrices of specs in batches of bounded memory. Consecutive specs of the same
 // spheroid at the same N and n_theta share one geometry (nodes and radial functions). Per
 // spec j: sums[3 j] = -Re tr T, sums[3 j + 1] = sum |T|^2, sums[3 j + 2] = the refinement's
@@ -2438,6 +2449,7 @@ void run_tmatrices(Context& c, const std::vector<TmSpec>& specs, std::vector<dou
     std::map<int64_t, int64_t> rule_at;
     std::vector<double> rules;
     int64_t nodes = 0, rad = 0, ang_nodes = 0, ang = 0, pairs = 0, J = 0, W = 0, P = 0, T = 0;
+    int64_t ser = 0, ser_threads = 0;
     double bytes = 0.0;
     size_t j1 = j0;
     for (; j1 < specs.size(); ++j1) {
@@ -2447,7 +2459,9 @@ void run_tmatrices(Context& c, const std::vector<TmSpec>& specs, std::vector<dou
       const int K = t.N - std::max(t.m, 1) + 1, n2 = 2 * K, nq = 2 * t.n_theta;
       double b = 8.0 * ((double)nq * (t.N + 1) * 6 + 32.0 * K * K + 14.0 * n2 * n2 +
                         (t_out || ro ? 2.0 * n2 * n2 : 0.0)) + 4.0 * n2;
-      if (new_geom) b += 8.0 * ((double)nq * 16 + (double)nq * (t.N + 1) * 20);
+      if (new_geom)
+        b += 8.0 * ((double)nq * 16 + (double)nq * (t.N + 1) * 20 +
+                    (double)t.n_theta * (t.N + 1) * tm_series_slot(t.N));
       if (ro && new_geom) {
         if (t.m != 0 || t.N > kRoMaxN)
           throw Failure{SCATRS_INVALID_INPUT,
@@ -2477,8 +2491,12 @@ void run_tmatrices(Context& c, const std::vector<TmSpec>& specs, std::vector<dou
         g.node0 = nodes;
         g.rule = rule_at[nq];
         g.rad0 = rad;
+        g.ser0 = ser;
+        g.sth0 = ser_threads;
         nodes += nq;
         rad += (int64_t)nq * (t.N + 1) * 20;
+        ser += (int64_t)t.n_theta * (t.N + 1) * tm_series_slot(t.N);
+        ser_threads += (int64_t)t.n_theta * t.N;
         geoms.push_back(g);
       }
       TmJob jb{};
@@ -2514,6 +2532,9 @@ void run_tmatrices(Context& c, const std::vector<TmSpec>& specs, std::vector<dou
     a.node = c.tm_node.as<double>(16 * (size_t)nodes);
     a.rad = c.tm_rad.as<double>((size_t)rad);
     a.ang = c.tm_ang.as<double>((size_t)ang);
+    a.ser = c.tm_ser.as<double>((size_t)ser);
+    a.n_ser_total = ser_threads;
+    a.form = tm_form_override();
     a.J = c.tm_J.as<double>(4 * (size_t)J);
     a.work = c.tm_work.as<double>((size_t)W);
     a.piv = c.tm_piv.as<int>((size_t)P);
@@ -2529,7 +2550,7 @@ void run_tmatrices(Context& c, const std::vector<TmSpec>& specs, std::vector<dou
     SB_CUDA(cudaMemsetAsync(a.err, 0, sizeof(unsigned), s));
     if (g_profiling) {
       int64_t pn = 0;
-      for (const TmJob& jb : jobs) pn += (int64_t)jb.K * jb.K * 2 * geoms[jb.geom].n_theta;
+      for (const TmJob& jb : jobs) pn += (int64_t)jb.K * jb.K * geoms[jb.geom].n_theta;
       g_tm_pair_nodes.push_back(pn);
     }
     timed_launch(K_TM_TABLES, s, [&] { launch_tm_tables(a, s); });
@@ -2612,6 +2633,9 @@ void run_tmatrices(Context& c, const std::vector<TmSpec>& specs, std::vector<dou
       SB_CUDA(cudaMemcpyAsync(all.data(), a.T, all.size() * 8, cudaMemcpyDeviceToHost, s));
     }
     SB_CUDA(cudaStreamSynchronize(s));
+    if (flag & 2u)
+      throw Failure{SCATRS_INVALID_INPUT,
+                    "a spheroid's radial series needs more than 4000 terms (size too large)"};
     if (flag) throw Failure{SCATRS_INVALID_INPUT, "a spheroid's Q matrix is singular"};
     for (const RoSph& e : sph)
       greek_out->emplace_back(greek_all.begin() + e.g0, greek_all.begin() + e.g0 + 6 * (e.L + 1));

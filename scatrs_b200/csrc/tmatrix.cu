@@ -8,9 +8,12 @@
 //                      theta-component, the weight factor, s r, and the radial functions
 //                      j_n(r), y_n(r), j_n(s r) with their [z z_n]'/z, orders 0..N;
 //   tm_angular_kernel  one thread per (mode, node): the normalized d, pi, tau, orders 0..N;
-//   tm_surface_kernel  one thread per (mode, i, k): the eight surface integrals
-//                      J[out][a][b]_{ik} = sum_nodes w r^2 2 pi n . (A_i x B_k) of the outgoing
-//                      (j or h) and inner vector spherical wave functions;
+//   tm_series_kernel   one thread per (spheroid, node, order): the power series of y_n(r) and
+//                      j_n(s r) with their partial sums (regular.rs);
+//   tm_surface_kernel  one thread per (mode, i, k): the surface integrals
+//                      J[a][b]_{ik} = sum_nodes w r^2 2 pi n . (A_i x B_k) of the regular
+//                      and inner vector spherical wave functions, and the y-part of the outgoing
+//                      ones in the cleanest of three exact forms per element of Q;
 //   tm_solve_kernel    one block per mode: Q^T and -P^T from J, an FP64 LU factorization of Q^T
 //                      with partial pivoting, the solve, and residual sweeps X += LU^{-1}
 //                      (-P^T - Q^T X) with the residual in double-double; then the mode's
@@ -20,11 +23,14 @@
 // cancel exactly in their singular (electrostatic) terms, by up to 1e16 and more at the sizes
 // and aspect ratios of the spheroid workloads (research/tmatrix/README.md, findings 1-3), and
 // any pointwise error of the sampled functions or the rule is amplified by that factor.
-// Carrying the functions, the Gauss-Legendre rule and the sums in about 106 bits leaves the
-// elements accurate to about 1e-32 times the cancellation; the residual refinement then
-// removes the FP64 factorization's floor (Skeel(Q) 2^-53, finding 4), which is what the
-// reference's refinement (solve.rs:249-385) does with its own cancellation-free integrands.
-// The formulation of the integrands is the classical one from the definition (Mishchenko,
+// The y-part's singular terms are removed as the reference removes them (regular.rs:1-24,
+// kernel.rs:468-490): the terms of power <= 0 (or < 0) of each radial product's Laurent series
+// integrate to zero over an element, so each element keeps the form without them whose
+// magnitude sum is the smallest. Carrying the functions, the Gauss-Legendre rule and the sums
+// in about 106 bits leaves the elements accurate to about 1e-32 times what cancellation
+// remains; the residual refinement then removes the FP64 factorization's floor (Skeel(Q)
+// 2^-53, finding 4), which is what the reference's refinement (solve.rs:249-385) does. The
+// vector products of the integrands are the classical ones from the definition (Mishchenko,
 // Travis & Lacis 2002, section 5.8; research/tmatrix/ebcm.py).
 #include <cuda_runtime.h>
 
@@ -203,15 +209,240 @@ __global__ void __launch_bounds__(128) tm_angular_kernel(TmArgs a) {
   }
 }
 
-// The eight surface integrals of one (mode, i, k), out 0 regular (z = j_i(r)), 1 outgoing
-// (z = h_i(r) = j + i y), a, b in {M, N}. With zeta = z or [r z]'/r and the inner w, w' at s r,
-// the triple products n . (A_i x B_k) reduce to (ebcm.py:103-186, pi -> -pi for the outgoing
-// functions' phi-factor convention, g_i g_k taken out of the sum):
+namespace {
+
+constexpr int kMaxSeriesTerms = 4000;
+constexpr double kSeriesTol = 0x1p-112;  // a term negligible against the largest at r_max
+
+// The series table's slot of (node n_theta + h, order n) and its parts (tm_series_slot).
+struct SerSlot {
+  const double* p;
+  int G;
+  __device__ int ly() const { return (int)p[0]; }
+  __device__ int lj() const { return (int)p[1]; }
+  __device__ const double* yk(int c) const { return p + 2 + c * (5 * G + 3); }
+  __device__ const double* jk(int c) const { return p + 2 + 3 * (5 * G + 3) + c * (10 * G + 5); }
+};
+
+// The number of terms of a series with term ratios x^2 / den(l), l >= 1, until the terms at
+// r_max are past their peak (after l_min) and below kSeriesTol of it (regular.rs:97-124, 140-150).
+template <class Den>
+__device__ int series_length(double x2max, int l_min, Den den) {
+  double at = 1.0, peak = 1.0;
+  for (int l = 1; l < kMaxSeriesTerms; ++l) {
+    const double ratio = x2max / fabs(den(l));
+    at *= ratio;
+    peak = fmax(peak, at);
+    if (l > l_min && ratio < 0.5 && at < kSeriesTol * peak) return l + 1;
+  }
+  return -1;
+}
+
+}  // namespace
+
+// The power series of the radial factors at the nodes of one half of the surface (the
+// integrands of the nonzero elements are even in cos theta), one thread per (spheroid, node,
+// order n >= 1) (regular.rs:1-31, 155-211, in the unscaled functions of tm_geom_kernel):
+//   y_n(r) = sum_l Y_l,      Y_l = a_l r^(2l - n - 1), a_0 = -(2n - 1)!!, a_l = -a_{l-1} / (2l (2l - 2n - 1));
+//   j_n(s r) = sum_i t_i,    t_i = b_i (s r)^(n + 2i), b_0 = 1 / (2n + 1)!!, b_i = -b_{i-1} / (2i (2i + 2n + 1));
+// with [r y]'/r = sum (2l - n) Y_l / r, y / r = sum Y_l / r, [z j]'/z = sum (n + 2i + 1) t_i / z and
+// j / z = sum t_i / z (z = s r). Kept: the y terms l < G with their suffix sums (and the sums of
+// their magnitudes) l <= G, the j prefix sums i < G and suffix sums i <= G, G = N/2 + 2, which
+// is every index the surface kernel's forms reach. Each suffix sum is accumulated from the
+// series' far end (its terms by the backward recurrence), so that it is accurate against its
+// own terms.
+__global__ void __launch_bounds__(128) tm_series_kernel(TmArgs a) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.n_ser_total) return;
+  const int gi = owner(a.n_geoms, t, [&](int i) { return a.geoms[i].sth0; });
+  const TmGeom g = a.geoms[gi];
+  const int N = g.N, G = N / 2 + 2;
+  const int64_t local = t - g.sth0;
+  const int h = (int)(local / N), n = 1 + (int)(local % N);
+  const int64_t S = tm_series_slot(N);
+  double* p = a.ser + g.ser0 + ((int64_t)h * (N + 1) + n) * S;
+  for (int64_t j = 0; j < S; ++j) p[j] = 0.0;
+  const double* ns = a.node + (g.node0 + g.n_theta + h) * kNodeD;
+  const dd r = ld(ns), ir = ld(ns + 2);
+  const cdd sr = ldc(ns + 8);
+  const double xmax = fmax(g.a, g.c), smag2 = g.s_re * g.s_re + g.s_im * g.s_im;
+  const int Ly = series_length(xmax * xmax, n, [&](int l) { return 2.0 * l * (2.0 * l - 2.0 * n - 1.0); });
+  const int Lj = series_length(xmax * xmax * smag2, 0, [&](int i) { return 2.0 * i * (2.0 * i + 2.0 * n + 1.0); });
+  if (Ly < 0 || Lj < 0) {
+    atomicOr(a.err, 2u);
+    return;
+  }
+  p[0] = Ly;
+  p[1] = Lj;
+  double* yb[3];
+  double* jb[3];
+  for (int c = 0; c < 3; ++c) {
+    yb[c] = p + 2 + c * (5 * G + 3);
+    jb[c] = p + 2 + 3 * (5 * G + 3) + c * (10 * G + 5);
+  }
+  // y: the first term, forward to the last, then back with the suffix sums.
+  {
+    const dd r2 = r * r, ir2 = ir * ir;
+    dd v = -ir;
+    for (int i = 1; i <= n; ++i) v = (v * (double)(2 * i - 1)) * ir;
+    for (int l = 1; l < Ly; ++l) v = -(v * r2) / (2.0 * l * (2.0 * l - 2.0 * n - 1.0));
+    dd sum[3] = {mkdd(0.0), mkdd(0.0), mkdd(0.0)};
+    double mag[3] = {0.0, 0.0, 0.0};
+    for (int l = Ly - 1; l >= 0; --l) {
+      const dd over = v * ir;
+      const dd term[3] = {v, over * (double)(2 * l - n), over};
+      for (int c = 0; c < 3; ++c) {
+        sum[c] = sum[c] + term[c];
+        mag[c] += fabs(term[c].hi);
+        if (l < G) st(yb[c] + 2 * l, term[c]);
+        if (l <= G) {
+          st(yb[c] + 2 * G + 2 * l, sum[c]);
+          yb[c][4 * G + 2 + l] = mag[c];
+        }
+      }
+      if (l > 0) v = -(v * (2.0 * l * (2.0 * l - 2.0 * n - 1.0))) * ir2;
+    }
+  }
+  // j(s r): the first term, forward with the prefix sums, then back with the suffix sums.
+  {
+    const cdd sr2 = sr * sr, isr = ddm::inv(sr), isr2 = isr * isr;
+    cdd v = mkc(1.0);
+    for (int i = 1; i <= n; ++i) {
+      v = v * sr;
+      v = cdd{v.re / (double)(2 * i + 1), v.im / (double)(2 * i + 1)};
+    }
+    cdd sum[3] = {mkc(0.0), mkc(0.0), mkc(0.0)};
+    double mag[3] = {0.0, 0.0, 0.0};
+    for (int i = 0; i < Lj; ++i) {
+      if (i > 0) {
+        const double den = 2.0 * i * (2.0 * i + 2.0 * n + 1.0);
+        v = -(v * sr2);
+        v = cdd{v.re / den, v.im / den};
+      }
+      if (i < G) {
+        const cdd over = v * isr;
+        const cdd term[3] = {v, over * (double)(n + 2 * i + 1), over};
+        for (int c = 0; c < 3; ++c) {
+          sum[c] = sum[c] + term[c];
+          mag[c] += fabs(term[c].re.hi) + fabs(term[c].im.hi);
+          stc(jb[c] + 4 * i, sum[c]);
+          jb[c][4 * G + i] = mag[c];
+        }
+      }
+    }
+    for (int c = 0; c < 3; ++c) {
+      sum[c] = mkc(0.0);
+      mag[c] = 0.0;
+    }
+    for (int i = Lj - 1; i >= 0; --i) {
+      const cdd over = v * isr;
+      const cdd term[3] = {v, over * (double)(n + 2 * i + 1), over};
+      for (int c = 0; c < 3; ++c) {
+        sum[c] = sum[c] + term[c];
+        mag[c] += fabs(term[c].re.hi) + fabs(term[c].im.hi);
+        if (i <= G) {
+          stc(jb[c] + 5 * G + 4 * i, sum[c]);
+          jb[c][9 * G + 4 + i] = mag[c];
+        }
+      }
+      if (i > 0) v = -((v * isr2) * (2.0 * i * (2.0 * i + 2.0 * n + 1.0)));
+    }
+  }
+}
+
+namespace {
+
+// R+ of one radial product R_t = r^e Y_t(r) J_t(s r) of the y-part at one node: R minus the
+// terms of its Laurent series in r of power <= cut, by the series of its higher powers or as
+// R minus the lower ones, whichever adds less in magnitude (regular.rs:255-311). yk, jk: the
+// kinds of the y_n and j_k factors (0 f, 1 [z f]'/z, 2 f/z); full = R_t at the node, xe = r^e.
+__device__ __forceinline__ void reg_form(const SerSlot& si, const SerSlot& sk, int yk, int jk,
+                                         int e, int n, int k, int cut, dd xe, cdd full,
+                                         cdd* out, double* out_abs) {
+  const double* yb = si.yk(yk);
+  const double* jb = sk.jk(jk);
+  const int G = si.G, Ly = si.ly(), Lj = sk.lj();
+  const int base0 = (-n - 1 - (yk > 0)) + (k - (jk > 0)) + e;
+  int l_end = cut >= base0 ? (cut - base0) / 2 + 1 : 0;
+  l_end = min(min(l_end, Ly), G - 1);
+  cdd neg = mkc(0.0), pos = mkc(0.0);
+  double neg_abs = 0.0, pos_abs = 0.0;
+  for (int l = 0; l < l_end; ++l) {
+    const int i_max = (cut - base0 - 2 * l) / 2;
+    const dd yv = ld(yb + 2 * l) * xe;
+    const double ya = fabs(yv.hi);
+    const int ii = max(min(min(i_max, Lj - 1), G - 1), 0);
+    neg = ddm::add_terms(neg, ldc(jb + 4 * ii) * yv);
+    neg_abs += jb[4 * G + ii] * ya;
+    const int from = min(min(i_max + 1, Lj), G);
+    pos = ddm::add_terms(pos, ldc(jb + 5 * G + 4 * from) * yv);
+    pos_abs += jb[9 * G + 4 + from] * ya;
+  }
+  const dd ysum = ld(yb + 2 * G + 2 * l_end) * xe;
+  pos = ddm::add_terms(pos, ldc(jb + 5 * G) * ysum);
+  pos_abs += jb[9 * G + 4] * yb[4 * G + 2 + l_end] * fabs(xe.hi);
+  const double sub_abs = fabs(full.re.hi) + fabs(full.im.hi) + neg_abs;
+  if (pos_abs <= sub_abs) {
+    *out = pos;
+    *out_abs = pos_abs;
+  } else {
+    *out = ddm::sub_terms(full, neg);
+    *out_abs = sub_abs;
+  }
+}
+
+// One term c R_t of a y-part integrand (c = alpha or i alpha, im) in the three forms: plain,
+// minus the powers < 0 (|n - k| >= 3) and minus the powers <= 0 (n != k), each with the sum of
+// the magnitudes it adds (kernel.rs:418-442).
+struct Forms3 {
+  cdd v[3];
+  double a[3];
+};
+__device__ __forceinline__ void add_type(Forms3& f, const SerSlot& si, const SerSlot& sk, int yk,
+                                         int jk, int e, int n, int k, dd xe, cdd full, dd alpha,
+                                         bool im, dd W) {
+  const dd cw = alpha * W;
+  const double ca = fabs(cw.hi);
+  auto acc = [&](int form, cdd v, double va) {
+    cdd x = v * cw;
+    if (im) x = ddm::times_i(x);
+    f.v[form] = ddm::add_terms(f.v[form], x);
+    f.a[form] += ca * va;
+  };
+  acc(0, full, fabs(full.re.hi) + fabs(full.im.hi));
+  if (n == k) return;
+  cdd v;
+  double va;
+  if (abs(n - k) >= 3) {
+    reg_form(si, sk, yk, jk, e, n, k, -1, xe, full, &v, &va);
+    acc(1, v, va);
+  }
+  reg_form(si, sk, yk, jk, e, n, k, 0, xe, full, &v, &va);
+  acc(2, v, va);
+}
+
+}  // namespace
+
+// The surface integrals of one (mode, i, k) (ebcm.py:103-186, pi -> -pi for the outgoing
+// functions' phi-factor convention, g_i g_k taken out of the sum). With z = j_i(r) or
+// i y_i(r), zeta = z or [r z]'/r, and the inner w, w' = [s r w]'/(s r), u = w/(s r) at s r, the
+// triple products n . (A_i x B_k) are
 //   MM = i z w (pi_i tau_k + tau_i pi_k)
-//   MN = z w' (pi_i pi_k + tau_i tau_k) - nu k(k+1) z w/(s r) tau_i d_k
+//   MN = z w' (pi_i pi_k + tau_i tau_k) - nu k(k+1) z u tau_i d_k
 //   NM = -z' w (tau_i tau_k + pi_i pi_k) + nu i(i+1) (z/r) w d_i tau_k
-//   NN = i [z' w' (tau_i pi_k + pi_i tau_k) - nu (k(k+1) z' w/(s r) pi_i d_k
-//                                                + i(i+1) (z/r) w' d_i pi_k)]
+//   NN = i [z' w' (tau_i pi_k + pi_i tau_k) - nu (k(k+1) z' u pi_i d_k + i(i+1) (z/r) w' d_i pi_k)]
+// where nu = -r'/r = nu' r^2, nu' = -beta sin cos (1/r^2 = alpha + beta cos^2). MN and NM are even
+// in cos theta when i + k is even and odd otherwise, MM and NN the reverse: each (i, k) has two
+// nonzero integrals, taken over the half cos theta > 0 of the rule and doubled; the other two
+// are exactly zero.
+//
+// Out: J[0..3] = the regular (z = j) MM, MN, NM, NN; J[4 + 2 bi + bk] = the y-part (z = i y) of
+// the element (bi, bk) of Q, -i s J_a - i J_b (tm_solve_kernel's pairs), in the cleanest of its
+// three exact forms (kernel.rs:468-490): per type t the radial product R_t = r^e Y_t J_t has
+// powers of r whose terms <= 0 integrate, over the element's four types together, to zero when
+// i != k, and those < 0 when |i - k| >= 3 (the spheroid's 1/r^2 is a polynomial in cos theta);
+// removing them removes the catastrophic cancellation of the plain integrals. The form whose
+// magnitude sum is the smallest is kept.
 __global__ void __launch_bounds__(128) tm_surface_kernel(TmArgs a) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= a.n_pair_total) return;
@@ -220,62 +451,107 @@ __global__ void __launch_bounds__(128) tm_surface_kernel(TmArgs a) {
   const TmGeom g = a.geoms[jb.geom];
   const int N = g.N, m = jb.m, n0 = m > 1 ? m : 1, K = jb.K;
   const int pr = (int)(t - jb.pair0), i = n0 + pr / K, k = n0 + pr % K;
-  cdd J[8];
+  const bool even = ((i + k) & 1) == 0;
+  const int G = N / 2 + 2;
+  const int64_t S = tm_series_slot(N);
+  cdd R0 = mkc(0.0), R1 = mkc(0.0);  // regular: MN, NM (even) or MM, NN (odd)
+  Forms3 Y0, Y1;                     // y-part: the same two
 #pragma unroll
-  for (int c = 0; c < 8; ++c) J[c] = mkc(0.0);
+  for (int c = 0; c < 3; ++c) {
+    Y0.v[c] = Y1.v[c] = mkc(0.0);
+    Y0.a[c] = Y1.a[c] = 0.0;
+  }
   const double cki = (double)i * (i + 1), ckk = (double)k * (k + 1);
-  const int nq = 2 * g.n_theta;
-  for (int q = 0; q < nq; ++q) {
+  const int nh = g.n_theta;
+  for (int h = 0; h < nh; ++h) {
+    const int q = nh + h;
     const double* ns = a.node + (g.node0 + q) * kNodeD;
-    const dd ir = ld(ns + 2), nu = ld(ns + 4), fac = ld(ns + 6);
+    const dd ir = ld(ns + 2), nu = ld(ns + 4), fac = ld(ns + 6) * 2.0;
+    const dd r = ld(ns), r2 = r * r, r4 = r2 * r2, ir2 = ir * ir;
+    const dd W = fac * ir2, nup = nu * ir2;
     const double* ri = a.rad + g.rad0 + ((int64_t)q * (N + 1) + i) * kRadD;
     const double* rk = a.rad + g.rad0 + ((int64_t)q * (N + 1) + k) * kRadD;
     const double* ai = a.ang + jb.ang0 + ((int64_t)q * (N + 1) + i) * kAngD;
     const double* ak = a.ang + jb.ang0 + ((int64_t)q * (N + 1) + k) * kAngD;
     const dd di = ld(ai), pii = ld(ai + 2), ti = ld(ai + 4);
     const dd dk = ld(ak), pik = ld(ak + 2), tk = ld(ak + 4);
-    // The sums below are measured against their terms (add_terms): the surface integrals'
-    // accuracy is about 2^-106 of the largest term, which is what the cancellation needs.
-    const dd A1 = ddm::add_terms(pii * tk, ti * pik), A2 = ddm::add_terms(pii * pik, ti * tk);
-    const dd A3 = ti * dk, A4 = di * tk, A5 = pii * dk, A6 = di * pik;
     const cdd w = ldc(rk + 8), wd = ldc(rk + 12), u = ldc(rk + 16);
     const dd jr = ld(ri), jdr = ld(ri + 2), yr = ld(ri + 4), ydr = ld(ri + 6);
-    const dd nk = nu * ckk, ni = nu * cki;
-#pragma unroll
-    for (int o = 0; o < 2; ++o) {
-      // z = j (real) for the regular functions, j + i y for the outgoing ones.
-      const cdd z = o ? cdd{jr, yr} : cdd{jr, mkdd(0.0)};
-      const cdd zd = o ? cdd{jdr, ydr} : cdd{jdr, mkdd(0.0)};
-      const cdd zr = z * ir;
-      const cdd zw = o ? ddm::mul_terms(z, w) : w * jr;
-      const cdd zwd = o ? ddm::mul_terms(z, wd) : wd * jr;
-      const cdd zu = o ? ddm::mul_terms(z, u) : u * jr;
-      const cdd zdw = o ? ddm::mul_terms(zd, w) : w * jdr;
-      const cdd zdwd = o ? ddm::mul_terms(zd, wd) : wd * jdr;
-      const cdd zdu = o ? ddm::mul_terms(zd, u) : u * jdr;
-      const cdd zrw = o ? ddm::mul_terms(zr, w) : w * zr.re;
-      const cdd zrwd = o ? ddm::mul_terms(zr, wd) : wd * zr.re;
-      const cdd mm = ddm::times_i(zw * A1);
-      const cdd mn = ddm::sub_terms(zwd * A2, (zu * A3) * nk);
-      const cdd nm = ddm::sub_terms((zrw * A4) * ni, zdw * A2);
+    const dd yo = yr * ir;  // y / r
+    const SerSlot si{a.ser + g.ser0 + ((int64_t)h * (N + 1) + i) * S, G};
+    const SerSlot sk{a.ser + g.ser0 + ((int64_t)h * (N + 1) + k) * S, G};
+    if (even) {
+      const dd A2 = ddm::add_terms(pii * pik, ti * tk), A3 = ti * dk, A4 = di * tk;
+      // Regular: MN = j w' A2 - nu k(k+1) j u A3, NM = nu i(i+1) (j/r) w A4 - j' w A2.
+      const cdd mn = ddm::sub_terms(wd * (jr * A2), u * ((jr * A3) * (nu * ckk)));
+      const cdd nm = ddm::sub_terms(w * (((jr * ir) * A4) * (nu * cki)), w * (jdr * A2));
+      R0 = ddm::add_terms(R0, mn * fac);
+      R1 = ddm::add_terms(R1, nm * fac);
+      // y-part: MN = i A2 R_1 - i k(k+1) A3 nu' R_4, NM = i i(i+1) A4 nu' R_6 - i A2 R_2.
+      add_type(Y0, si, sk, 0, 1, 2, i, k, r2, wd * (yr * r2), A2, true, W);
+      add_type(Y0, si, sk, 0, 2, 4, i, k, r4, u * (yr * r4), -((A3 * nup) * ckk), true, W);
+      add_type(Y1, si, sk, 2, 0, 4, i, k, r4, w * (yo * r4), (A4 * nup) * cki, true, W);
+      add_type(Y1, si, sk, 1, 0, 2, i, k, r2, w * (ydr * r2), -A2, true, W);
+    } else {
+      const dd A1 = ddm::add_terms(pii * tk, ti * pik), A5 = pii * dk, A6 = di * pik;
+      // Regular: MM = i j w A1, NN = i [j' w' A1 - nu (k(k+1) j' u A5 + i(i+1) (j/r) w' A6)].
+      const cdd mm = ddm::times_i(w * (jr * A1));
       const cdd nn = ddm::times_i(ddm::sub_terms(
-          zdwd * A1, ddm::add_terms((zdu * A5) * ckk, (zrwd * A6) * cki) * nu));
-      J[o * 4 + 0] = ddm::add_terms(J[o * 4 + 0], mm * fac);
-      J[o * 4 + 1] = ddm::add_terms(J[o * 4 + 1], mn * fac);
-      J[o * 4 + 2] = ddm::add_terms(J[o * 4 + 2], nm * fac);
-      J[o * 4 + 3] = ddm::add_terms(J[o * 4 + 3], nn * fac);
+          wd * (jdr * A1),
+          ddm::add_terms(u * ((jdr * A5) * ckk), wd * (((jr * ir) * A6) * cki)) * nu));
+      R0 = ddm::add_terms(R0, mm * fac);
+      R1 = ddm::add_terms(R1, nn * fac);
+      // y-part: MM = -A1 R_0, NN = -A1 R_3 + k(k+1) A5 nu' R_5 + i(i+1) A6 nu' R_7.
+      add_type(Y0, si, sk, 0, 0, 2, i, k, r2, w * (yr * r2), -A1, false, W);
+      add_type(Y1, si, sk, 1, 1, 2, i, k, r2, wd * (ydr * r2), -A1, false, W);
+      add_type(Y1, si, sk, 1, 2, 4, i, k, r4, u * (ydr * r4), (A5 * nup) * ckk, false, W);
+      add_type(Y1, si, sk, 2, 1, 4, i, k, r4, wd * (yo * r4), (A6 * nup) * cki, false, W);
     }
   }
   // g_i g_k = sqrt((2i+1)(2k+1) / (16 pi^2 i(i+1) k(k+1))).
   const dd pi2 = dd{kPiHi, kPiLo} * dd{kPiHi, kPiLo};
   const dd gg = ddm::dd_sqrt((mkdd((double)(2 * i + 1) * (2 * k + 1)) / (pi2 * 16.0)) /
                              (cki * ckk));
-  double* out = a.J + 4 * jb.J0;
+  // The two elements of Q this (i, k) feeds, with s on the first of their pair:
+  // even: (0, 0) = -i s MN - i NM, (1, 1) = -i s NM - i MN; odd: (0, 1) = -i s MM - i NN,
+  // (1, 0) = -i s NN - i MM.
+  const cdd s = mkc(g.s_re, g.s_im), mis = -ddm::times_i(s);
+  const double sa = fabs(g.s_re) + fabs(g.s_im);
+  auto element = [&](const Forms3& first, const Forms3& second) {
+    int best = 0;
+    if (a.form >= 0) {
+      if (a.form == 2 && i != k) best = 2;
+      if (a.form == 1 && abs(i - k) >= 3) best = 1;
+    } else if (i != k) {
+      const double m2 = sa * first.a[2] + second.a[2];
+      double mb = sa * first.a[0] + second.a[0];
+      if (m2 < mb) {
+        best = 2;
+        mb = m2;
+      }
+      if (abs(i - k) >= 3 && sa * first.a[1] + second.a[1] < mb) best = 1;
+    }
+    return ddm::add_terms(mis * first.v[best], ddm::times_i(second.v[best]) * -1.0) * gg;
+  };
+  cdd out[8];
+#pragma unroll
+  for (int c = 0; c < 8; ++c) out[c] = mkc(0.0);
+  if (even) {
+    out[1] = R0 * gg;
+    out[2] = R1 * gg;
+    out[4 + 0] = element(Y0, Y1);
+    out[4 + 3] = element(Y1, Y0);
+  } else {
+    out[0] = R0 * gg;
+    out[3] = R1 * gg;
+    out[4 + 1] = element(Y0, Y1);
+    out[4 + 2] = element(Y1, Y0);
+  }
+  double* o = a.J + 4 * jb.J0;
   const int64_t KK = (int64_t)K * K, e = (int64_t)(i - n0) * K + (k - n0);
 #pragma unroll
-  for (int c = 0; c < 8; ++c) stc(out + 4 * (c * KK + e), J[c] * gg);
+  for (int c = 0; c < 8; ++c) stc(o + 4 * (c * KK + e), out[c]);
 }
-
 namespace {
 
 struct Cd {  // complex double
@@ -354,19 +630,19 @@ __global__ void __launch_bounds__(256) tm_solve_kernel(TmArgs a) {
   const cdd s = mkc(g.s_re, g.s_im);
   const cdd mis = -ddm::times_i(s), mi = mkc(0.0, -1.0);
   auto Jv = [&](int o, int p, int b, int64_t e) { return ldc(J + 4 * (((o * 2 + p) * 2 + b) * KK + e)); };
-  // Q11 = -i s J12 - i J21, Q12 = -i s J11 - i J22, Q21 = -i s J22 - i J11,
-  // Q22 = -i s J21 - i J12 (ebcm.py:189-195); element (row, col) of Q goes to (col, row).
+  // RgQ11 = -i s J12 - i J21, RgQ12 = -i s J11 - i J22, RgQ21 = -i s J22 - i J11,
+  // RgQ22 = -i s J21 - i J12 (ebcm.py:189-195) of the regular J, and Q = RgQ + its y-part
+  // (tm_surface_kernel); element (row, col) of Q goes to (col, row).
   for (int64_t idx = t; idx < NN; idx += blockDim.x) {
     const int row = (int)(idx / n2), col = (int)(idx % n2);
     const int bi = row >= K, bk = col >= K;
     const int64_t e = (int64_t)(row - bi * K) * K + (col - bk * K);
     cdd q[2];
-    for (int o = 0; o < 2; ++o) {
-      if (!bi && !bk) q[o] = mis * Jv(o, 0, 1, e) + mi * Jv(o, 1, 0, e);
-      else if (!bi && bk) q[o] = mis * Jv(o, 0, 0, e) + mi * Jv(o, 1, 1, e);
-      else if (bi && !bk) q[o] = mis * Jv(o, 1, 1, e) + mi * Jv(o, 0, 0, e);
-      else q[o] = mis * Jv(o, 1, 0, e) + mi * Jv(o, 0, 1, e);
-    }
+    if (!bi && !bk) q[0] = mis * Jv(0, 0, 1, e) + mi * Jv(0, 1, 0, e);
+    else if (!bi && bk) q[0] = mis * Jv(0, 0, 0, e) + mi * Jv(0, 1, 1, e);
+    else if (bi && !bk) q[0] = mis * Jv(0, 1, 1, e) + mi * Jv(0, 0, 0, e);
+    else q[0] = mis * Jv(0, 1, 0, e) + mi * Jv(0, 0, 1, e);
+    q[1] = q[0] + Jv(1, bi, bk, e);
     const int64_t tr = (int64_t)col * n2 + row;
     stc(Qd + 4 * tr, q[1]);
     stc(Bd + 4 * tr, -q[0]);
@@ -497,6 +773,8 @@ void launch_tm_tables(const TmArgs& a, cudaStream_t s) {
   if (a.n_jobs <= 0) return;
   tm_geom_kernel<<<(unsigned)((a.n_node_total + 127) / 128), 128, 0, s>>>(a);
   tm_angular_kernel<<<(unsigned)((a.n_ang_total + 127) / 128), 128, 0, s>>>(a);
+  if (a.n_ser_total > 0)
+    tm_series_kernel<<<(unsigned)((a.n_ser_total + 127) / 128), 128, 0, s>>>(a);
 }
 void launch_tm_surface(const TmArgs& a, cudaStream_t s) {
   if (a.n_jobs <= 0) return;
