@@ -538,7 +538,9 @@ TM_SURFACE_FLOP_PER_PAIR_NODE = 1799.5
 def spheroid_leg(torch, fp64_peak: float, scale: float = 1.0, cpu_seconds: float = 10.0):
     """The fixed-grid ensemble of randomly oriented spheroids on a sample of the spheroid
     workload (16 aspect ratios over 0.4-3.0 x 2 lognormals x 4 of its 32 wavelengths x 64
-    nodes, size parameters to 15): every node's T-matrix converged (double-double EBCM) with
+    nodes, size parameters to 21, the largest at which every aspect ratio of the workload
+    stays inside the validated domain, |m| x_max <= 60): every node's T-matrix converged
+    (double-double EBCM, regularized y-part) with
     its orientation average. Timed after one identical warm-up call; nodes per second, the
     kernels' shares, and the surface-integral kernel's FP64 rate against the FP64 peak
     measured in this run. The CPU baseline is the oracle's double-precision node solve on a
@@ -546,7 +548,7 @@ def spheroid_leg(torch, fp64_peak: float, scale: float = 1.0, cpu_seconds: float
     from scatrs_b200 import _native
     from scatrs_b200 import workloads as W
 
-    w = W.spheroids(scale=max(1 / 32, scale / 8), x_max=15.0)
+    w = W.spheroids(scale=max(1 / 32, scale / 8), x_max=21.0)
     call = lambda: _native.ensemble_fixed_spheroid(w.dists, w.wavelengths, w.aspect_ratio, w.m,
                                                    w.mu, w.n_nodes, w.greek_order,
                                                    tmatrix_rtol=1e-8)
@@ -791,6 +793,7 @@ def ours(args):
                            "i8_above": tuned.i8_above, "sample_units": tuned.sample_units,
                            "ms_per_candidate": {k: round(v, 3) for k, v in tuned.ms.items()},
                            "errors": tuned.errors}
+    if mixed is not None:
         ops = algorithmic_i8_ops(w, user_rows, args.i8_above, args.i8_levels or 5)
         ktm = mixed["kt"]
         i8_ms, i8_n = ktm.get("unit_i8_kernel", (0.0, 0))

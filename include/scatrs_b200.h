@@ -322,6 +322,10 @@ typedef struct scatrs_spheroid_options {
   int32_t n_theta;
   int32_t greek_order;
   int32_t normalized;
+  /* 1: compute outside the spheroids' validated domain (tmatrix/domain.rs:45-79: aspect ratio
+   * 0.2-5, x >= 1e-6, |m| x_max <= 60, 1.3 <= Re m <= 3, Im m <= 0.5, rtol >= 1e-12); else such
+   * a spheroid returns SCATRS_OUTSIDE_VALIDATED_DOMAIN (TMatrix::compute, tmatrix/mod.rs:280-292) */
+  int32_t allow_unvalidated;
 } scatrs_spheroid_options;
 
 int scatrs_spheroid_compute(int64_t n, const double* x, const double* aspect_ratio,

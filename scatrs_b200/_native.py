@@ -80,7 +80,7 @@ class Component(ctypes.Structure):
 
 class SpheroidOptions(ctypes.Structure):
     _fields_ = [("rtol", _D), ("n_terms", _I32), ("n_theta", _I32), ("greek_order", _I32),
-                ("normalized", _I32)]
+                ("normalized", _I32), ("allow_unvalidated", _I32)]
 
 
 class FixedOptions(ctypes.Structure):
@@ -365,7 +365,7 @@ def ensemble_fixed(dists: np.ndarray, wavelengths, m, mu, n_nodes: int, greek_or
 
 def ensemble_fixed_spheroid(dists: np.ndarray, wavelengths, aspect_ratio, m, mu, n_nodes: int,
                             greek_order: int = -1, normalized: bool = True,
-                            tmatrix_rtol: float = 1e-8):
+                            tmatrix_rtol: float = 1e-8, allow_unvalidated: bool = False):
     """The fixed-grid ensemble of randomly oriented spheroids (one aspect ratio per
     distribution); returns (values, phase or None, greek or None, node_terms) with node_terms
     (n, n_nodes, 2) the N and n_theta of each node."""
@@ -378,7 +378,7 @@ def ensemble_fixed_spheroid(dists: np.ndarray, wavelengths, aspect_ratio, m, mu,
                                              (dists.size, wl.size)))
     mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
     n = dists.size * wl.size
-    opts = FixedOptions(int(n_nodes), int(greek_order), int(normalized), 0)
+    opts = FixedOptions(int(n_nodes), int(greek_order), int(normalized), int(allow_unvalidated))
     values = np.zeros((11, n))
     phase = np.zeros((6, n, mu.size)) if mu.size else None
     greek = np.zeros((6, n, greek_order + 1)) if greek_order >= 0 else None
@@ -395,7 +395,7 @@ def ensemble_fixed_spheroid(dists: np.ndarray, wavelengths, aspect_ratio, m, mu,
 
 def ensemble_fixed_spheroid_d(dists: np.ndarray, wavelengths, aspect_ratio, m, mu,
                               n_nodes: int, greek_order: int = -1, normalized: bool = True,
-                              tmatrix_rtol: float = 1e-8):
+                              tmatrix_rtol: float = 1e-8, allow_unvalidated: bool = False):
     """ensemble_fixed_spheroid with the derivatives along the distribution's parameters, the
     aspect ratio, Re m and Im m (P of them): returns (values, phase, greek, d_values, d_phase,
     d_greek, node_terms), the derivative arrays shaped (P,) + the value array's shape."""
@@ -410,7 +410,7 @@ def ensemble_fixed_spheroid_d(dists: np.ndarray, wavelengths, aspect_ratio, m, m
     n = dists.size * wl.size
     kind = int(dists["kind"][0]) if dists.size else 1
     P = {3: 3, 4: 1, TABULATED: 0}.get(kind, 2) + 3
-    opts = FixedOptions(int(n_nodes), int(greek_order), int(normalized), 0)
+    opts = FixedOptions(int(n_nodes), int(greek_order), int(normalized), int(allow_unvalidated))
     values = np.zeros((11, n))
     d_values = np.zeros((P, 11, n))
     phase = np.zeros((6, n, mu.size)) if mu.size else None
@@ -837,7 +837,8 @@ def spheroid_efficiencies(x, aspect_ratio, m, rtol: float = 1e-8):
 
 
 def spheroid_compute(x, aspect_ratio, m, rtol: float = 1e-8, n_terms: int = 0, n_theta: int = 0,
-                     greek_order: int = -1, normalized: bool = True) -> dict:
+                     greek_order: int = -1, normalized: bool = True,
+                     allow_unvalidated: bool = False) -> dict:
     """Randomly oriented spheroids: efficiencies (n, 5) = Q_ext, Q_sca, Q_abs, Q_back, g; Greek
     coefficients (n, 6, order + 1) if greek_order >= 0; the N and n_theta used and the
     refinement's error estimate."""
@@ -850,7 +851,8 @@ def spheroid_compute(x, aspect_ratio, m, rtol: float = 1e-8, n_terms: int = 0, n
     nt = np.zeros(x.size, dtype=np.int32)
     nth = np.zeros(x.size, dtype=np.int32)
     est = np.zeros(x.size)
-    o = SpheroidOptions(rtol, n_terms, n_theta, greek_order, int(normalized))
+    o = SpheroidOptions(rtol, n_terms, n_theta, greek_order, int(normalized),
+                        int(allow_unvalidated))
     err = ctypes.create_string_buffer(1024)
     _check(load().scatrs_spheroid_compute(x.size, _p(x), _p(eps), _p(mm.view(np.float64)),
                                           ctypes.byref(o), _p(eff), _p(greek), nt.ctypes.data,
@@ -863,7 +865,8 @@ SPHEROID_DIRECTIONS = ("x", "aspect_ratio", "m_re", "m_im")
 
 
 def spheroid_compute_d(x, aspect_ratio, m, rtol: float = 1e-8, n_terms: int = 0,
-                       n_theta: int = 0, greek_order: int = -1, normalized: bool = True) -> dict:
+                       n_theta: int = 0, greek_order: int = -1, normalized: bool = True,
+                       allow_unvalidated: bool = False) -> dict:
     """spheroid_compute with the derivatives of the efficiencies and Greek coefficients along
     x, the aspect ratio, Re m and Im m (scatrs_spheroid_compute_d): d_efficiencies (4, n, 5),
     d_greek (4, n, 6, order + 1), in the order of SPHEROID_DIRECTIONS."""
@@ -879,7 +882,8 @@ def spheroid_compute_d(x, aspect_ratio, m, rtol: float = 1e-8, n_terms: int = 0,
     nt = np.zeros(n, dtype=np.int32)
     nth = np.zeros(n, dtype=np.int32)
     est = np.zeros(n)
-    o = SpheroidOptions(rtol, n_terms, n_theta, greek_order, int(normalized))
+    o = SpheroidOptions(rtol, n_terms, n_theta, greek_order, int(normalized),
+                        int(allow_unvalidated))
     err = ctypes.create_string_buffer(1024)
     _check(load().scatrs_spheroid_compute_d(n, _p(x), _p(eps), _p(mm.view(np.float64)),
                                             ctypes.byref(o), _p(eff), _p(greek), _p(d_eff),

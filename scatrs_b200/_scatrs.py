@@ -417,7 +417,7 @@ def ensemble_compute_fixed(specs, particle_spec, wavelengths, greek, all_orders,
             m = np.broadcast_to(m, (dists.size, wl.size))
         values, phase, g, _ = _native.ensemble_fixed_spheroid(
             dists, wl, float(particle_spec[1]), m, mu, n_nodes, L, bool(normalized),
-            tmatrix_rtol=tmatrix_rtol)
+            tmatrix_rtol=tmatrix_rtol, allow_unvalidated=bool(allow_unvalidated))
     elif particle_spec[0] == "layered":
         ml = np.asarray(particle_spec[2], dtype=np.complex128)
         fr = np.asarray(particle_spec[1], dtype=np.float64)

@@ -2449,7 +2449,7 @@ void run_tmatrices(Context& c, const std::vector<TmSpec>& specs, std::vector<dou
     std::map<int64_t, int64_t> rule_at;
     std::vector<double> rules;
     int64_t nodes = 0, rad = 0, ang_nodes = 0, ang = 0, pairs = 0, J = 0, W = 0, P = 0, T = 0;
-    int64_t ser = 0, ser_threads = 0;
+    int64_t ser = 0, ser_threads = 0, forms_threads = 0;
     double bytes = 0.0;
     size_t j1 = j0;
     for (; j1 < specs.size(); ++j1) {
@@ -2493,10 +2493,12 @@ void run_tmatrices(Context& c, const std::vector<TmSpec>& specs, std::vector<dou
         g.rad0 = rad;
         g.ser0 = ser;
         g.sth0 = ser_threads;
+        g.fth0 = forms_threads;
         nodes += nq;
         rad += (int64_t)nq * (t.N + 1) * 20;
         ser += (int64_t)t.n_theta * (t.N + 1) * tm_series_slot(t.N);
         ser_threads += (int64_t)t.n_theta * t.N;
+        forms_threads += (int64_t)t.n_theta * t.N * t.N;
         geoms.push_back(g);
       }
       TmJob jb{};
@@ -2534,6 +2536,7 @@ void run_tmatrices(Context& c, const std::vector<TmSpec>& specs, std::vector<dou
     a.ang = c.tm_ang.as<double>((size_t)ang);
     a.ser = c.tm_ser.as<double>((size_t)ser);
     a.n_ser_total = ser_threads;
+    a.n_forms_total = forms_threads;
     a.form = tm_form_override();
     a.J = c.tm_J.as<double>(4 * (size_t)J);
     a.work = c.tm_work.as<double>((size_t)W);
@@ -2654,6 +2657,14 @@ double tm_x_max(double x, double eps) {
   const double a = x * std::cbrt(eps);
   return std::max(a, a / eps);
 }
+// The validated domain of spheroids (tmatrix/domain.rs:45-79): aspect ratios 0.2 to 5,
+// equal-volume x >= 1e-6, |m| x_max <= 60 (x_max of the longest semi-axis), 1.3 <= Re m <= 3,
+// 0 <= Im m <= 0.5, rtol >= 1e-12.
+constexpr double kTmDomainRtolMin = 1e-12;
+bool tm_in_domain(double x, double eps, double mr, double mi) {
+  return eps >= 0.2 && eps <= 5.0 && x >= 1e-6 && std::hypot(mr, mi) * tm_x_max(x, eps) <= 60.0 &&
+         mr >= 1.3 && mr <= 3.0 && mi >= 0.0 && mi <= 0.5;
+}
 int tm_wiscombe(double xm) { return std::max((int)std::ceil(xm + 4.0 * std::cbrt(xm)) + 2, 4); }
 int tm_theta_of(int n, double eps, double rtol) {
   const double h = std::max(eps, 1.0 / eps);
@@ -2679,7 +2690,7 @@ struct SpheroidResult {
 // run as one batch of device work.
 void spheroid_solve(Context& c, int64_t n, const double* x, const double* aspect_ratio,
                     const double* m, double rtol, int n_fixed, int theta_fixed, bool greek,
-                    std::vector<SpheroidResult>& out, cudaStream_t s) {
+                    std::vector<SpheroidResult>& out, cudaStream_t s, bool allow_unvalidated) {
   if (!x || !aspect_ratio || !m)
     throw Failure{SCATRS_INVALID_INPUT, "x, aspect_ratio and m are required"};
   if (!(rtol >= 1e-13 && rtol <= 0.1))
@@ -2687,6 +2698,23 @@ void spheroid_solve(Context& c, int64_t n, const double* x, const double* aspect
   for (int64_t i = 0; i < n; ++i)
     check_tm_spec({x[i], aspect_ratio[i], m[2 * i], m[2 * i + 1], 0,
                    n_fixed > 0 ? n_fixed : 1, theta_fixed > 0 ? theta_fixed : 2});
+  if (!allow_unvalidated) {
+    // mod.rs:280-292: outside the validated domain only when asked for.
+    if (rtol < kTmDomainRtolMin) {
+      char buf[120];
+      snprintf(buf, sizeof buf, "outside the validated domain: rtol %e is below %e", rtol,
+               kTmDomainRtolMin);
+      throw Failure{SCATRS_OUTSIDE_VALIDATED_DOMAIN, buf};
+    }
+    for (int64_t i = 0; i < n; ++i)
+      if (!tm_in_domain(x[i], aspect_ratio[i], m[2 * i], m[2 * i + 1])) {
+        char buf[200];
+        snprintf(buf, sizeof buf,
+                 "outside the validated domain: aspect ratio %g, x = %g, m = %g%+gi (spheroid %lld)",
+                 aspect_ratio[i], x[i], m[2 * i], m[2 * i + 1], (long long)i);
+        throw Failure{SCATRS_OUTSIDE_VALIDATED_DOMAIN, buf};
+      }
+  }
   struct St {
     int n, nth, cap, th_cap, stage;  // stage 0: N, 1: n_theta, 2: done
     double e, sc;
@@ -3028,7 +3056,7 @@ void spheroid_call(const std::vector<SphParticle>& ps, bool batch, const double*
       // The orientation average always: Q_back, g and the depolarization numerator come
       // from it (particle.rs:334-343).
       spheroid_solve(c, (int64_t)which.size(), xs.data(), es.data(), ms.data(), rtol_t, 0, 0,
-                     true, r, s);
+                     true, r, s, o.allow_unvalidated);
       for (size_t k = 0; k < which.size(); ++k) {
         const adaptive::Query& q = qs[which[k]];
         cache[key_of(particle_of[q.wl / n_wl], q.wl % n_wl, q.r)] = std::move(r[k]);
@@ -4205,7 +4233,7 @@ int scatrs_spheroid_efficiencies(int64_t n, const double* x, const double* aspec
     Context& c = context();
     std::lock_guard<std::mutex> lk(c.mtx);
     std::vector<SpheroidResult> res;
-    spheroid_solve(c, n, x, aspect_ratio, m, rtol, 0, 0, false, res, 0);
+    spheroid_solve(c, n, x, aspect_ratio, m, rtol, 0, 0, false, res, 0, true);
     for (int64_t i = 0; i < n; ++i) {
       q[3 * i] = res[i].q_ext;
       q[3 * i + 1] = res[i].q_sca;
@@ -4233,7 +4261,8 @@ int scatrs_spheroid_compute(int64_t n, const double* x, const double* aspect_rat
     Context& c = context();
     std::lock_guard<std::mutex> lk(c.mtx);
     std::vector<SpheroidResult> res;
-    spheroid_solve(c, n, x, aspect_ratio, m, o.rtol, o.n_terms, o.n_theta, true, res, 0);
+    spheroid_solve(c, n, x, aspect_ratio, m, o.rtol, o.n_terms, o.n_theta, true, res, 0,
+                   o.allow_unvalidated != 0);
     const int64_t len = (int64_t)o.greek_order + 1;
     for (int64_t i = 0; i < n; ++i) {
       const SpheroidResult& r = res[i];
@@ -4278,7 +4307,8 @@ int scatrs_spheroid_compute_d(int64_t n, const double* x, const double* aspect_r
     Context& c = context();
     std::lock_guard<std::mutex> lk(c.mtx);
     std::vector<SpheroidResult> res;
-    spheroid_solve(c, n, x, aspect_ratio, m, o.rtol, o.n_terms, o.n_theta, false, res, 0);
+    spheroid_solve(c, n, x, aspect_ratio, m, o.rtol, o.n_terms, o.n_theta, false, res, 0,
+                   o.allow_unvalidated != 0);
     std::vector<SphEval> base(n);
     for (int64_t i = 0; i < n; ++i) {
       base[i] = {x[i], aspect_ratio[i], m[2 * i], m[2 * i + 1], res[i].n, res[i].nth};
@@ -4360,7 +4390,8 @@ int scatrs_ensemble_fixed_spheroid(const scatrs_distribution* dists, int64_t n_d
           ms[2 * k + 1] = m[2 * u + 1];
         }
     std::vector<SpheroidResult> res;
-    spheroid_solve(c, n_sph, xs.data(), es.data(), ms.data(), tmatrix_rtol, 0, 0, true, res, 0);
+    spheroid_solve(c, n_sph, xs.data(), es.data(), ms.data(), tmatrix_rtol, 0, 0, true, res, 0,
+                   options->allow_unvalidated != 0);
     // The direct path's per-particle quantities and segment (engine.rs:1207-1339) summed over
     // each unit's nodes in order, then the averages and the outputs of engine.rs:2396-2497.
     std::vector<double> d00, d22, d2m2, d02;
@@ -4566,7 +4597,8 @@ int scatrs_ensemble_fixed_spheroid_d(const scatrs_distribution* dists, int64_t n
     // Every node converged as the value entry converges it, then its outputs and their
     // derivatives along the aspect ratio, Re m and Im m at that (N, n_theta).
     std::vector<SpheroidResult> res;
-    spheroid_solve(c, n_sph, xs.data(), es.data(), ms.data(), tmatrix_rtol, 0, 0, false, res, 0);
+    spheroid_solve(c, n_sph, xs.data(), es.data(), ms.data(), tmatrix_rtol, 0, 0, false, res, 0,
+                   options->allow_unvalidated != 0);
     std::vector<SphEval> base(n_sph);
     int top_all = 0;
     for (int64_t k = 0; k < n_sph; ++k) {

@@ -397,16 +397,20 @@ struct TmGeom {
   int64_t node0;  // first node (of 2 n_theta) in the node table
   int64_t rule;   // first node of its Gauss-Legendre rule in the rule table
   int64_t rad0;   // radial table [node][order 0..N][20]
-  int64_t ser0;   // series table [node n_theta + h, h < n_theta][order 0..N][tm_series_slot(N)]
+  int64_t ser0;   // series table of nodes n_theta + h, h < n_theta (tm_series_slot)
   int64_t sth0;   // first (node, order) thread of the series kernel
+  int64_t fth0;   // first (node, order pair) thread of the forms kernel
 };
-// Doubles per (node, order) of the series table: the lengths of the two series, then per kind
-// (f, [z f]'/z, f/z) the y_n terms, suffix sums and their magnitudes up to G = N/2 + 2, and the
-// j_k(s r) prefix sums, suffix sums and their magnitudes up to G.
+// Doubles per (node, order) of the series table: a j-slot (the lengths of the two series, then
+// per kind (f, [z f]'/z, f/z) the j_k(s r) prefix sums, suffix sums and their magnitudes up to
+// G = N/2 + 2: 30 G + 17), the order's entries of the y-table (per kind and index l <= G the
+// y_n term, suffix sum and magnitude sum: 15 (G + 1)) and of the forms table (per column order,
+// four radial products, the two regularized forms with their magnitude sums: 40 (N + 1)); the
+// y-table and the forms table are laid out row-order-fastest.
 #ifdef __CUDACC__
 __host__ __device__
 #endif
-inline int64_t tm_series_slot(int N) { return 45 * (int64_t)(N / 2 + 2) + 26; }
+inline int64_t tm_series_slot(int N) { return 45 * (int64_t)(N / 2 + 2) + 32 + 40 * (int64_t)(N + 1); }
 struct TmJob {
   int geom, m, K, pad;
   int64_t ang_node0;  // first (job, node) index of the angular table
@@ -434,8 +438,8 @@ struct TmArgs {
   double* sums;   // per job: -Re tr T, sum |T|^2, the refinement's last relative correction
   unsigned* err;  // 1: a singular Q, 2: a series longer than its cap
   int max_sweeps;
-  double* ser;    // series table (tm_series_kernel)
-  int64_t n_ser_total;
+  double* ser;    // series and forms tables (tm_series_kernel, tm_forms_kernel)
+  int64_t n_ser_total, n_forms_total;
   int form;       // -1: each element's cleanest form; 0: plain; 1, 2: that form where it applies
 };
 void launch_tmatrix(const TmArgs& a, cudaStream_t s);

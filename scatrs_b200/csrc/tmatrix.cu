@@ -212,17 +212,51 @@ __global__ void __launch_bounds__(128) tm_angular_kernel(TmArgs a) {
 namespace {
 
 constexpr int kMaxSeriesTerms = 4000;
+// The plain form is kept only when its magnitude sum is below 2^-20 of the regularized forms':
+// its integrand comes from the radial functions' recurrences, whose accumulated rounding its
+// magnitude sum does not see, while the regularized forms within 2^20 of it still hold about 86
+// bits against it. (At x = 25, aspect ratio 0.4 the unbiased choice left the mode-0 T-matrix's
+// unitarity at 1e-3 to 1e-2, the biased one at 1e-5; at x = 21 and x = 25, aspect ratio 3,
+// 5e-9 became 5e-11 and 1e-10 became 2e-12.)
+constexpr double kPlainBias = 0x1p20;
 constexpr double kSeriesTol = 0x1p-112;  // a term negligible against the largest at r_max
 
-// The series table's slot of (node n_theta + h, order n) and its parts (tm_series_slot).
-struct SerSlot {
+// The series table of one spheroid (tm_series_slot): j-slots of JS = 30 G + 17 doubles per
+// (node h, order n), then the y-table, per (node h, kind c, index l <= G) five fields (the term
+// hi, lo, the suffix sum hi, lo, the suffix magnitude sum), each over the orders 0..N.
+__device__ __forceinline__ int64_t j_slot_size(int G) { return 30 * (int64_t)G + 17; }
+struct JSlot {
   const double* p;
   int G;
-  __device__ int ly() const { return (int)p[0]; }
-  __device__ int lj() const { return (int)p[1]; }
-  __device__ const double* yk(int c) const { return p + 2 + c * (5 * G + 3); }
-  __device__ const double* jk(int c) const { return p + 2 + 3 * (5 * G + 3) + c * (10 * G + 5); }
+  __device__ const double* jk(int c) const { return p + 2 + c * (10 * G + 5); }
 };
+struct YTab {  // the y-table of one (node, kind)
+  const double* p;
+  int n1;
+  __device__ dd term(int l, int n) const {
+    const double* q = p + (int64_t)l * 5 * n1 + n;
+    return dd{q[0], q[n1]};
+  }
+  __device__ dd sum(int l, int n) const {
+    const double* q = p + ((int64_t)l * 5 + 2) * n1 + n;
+    return dd{q[0], q[n1]};
+  }
+  __device__ double mag(int l, int n) const { return p[((int64_t)l * 5 + 4) * n1 + n]; }
+};
+__device__ __forceinline__ const double* y_table(const double* ser0, int n_theta, int N, int G,
+                                                 int h, int c) {
+  const int n1 = N + 1;
+  return ser0 + (int64_t)n_theta * n1 * j_slot_size(G) + (int64_t)(h * 3 + c) * (G + 1) * 5 * n1;
+}
+// The forms table after the y-table: per (node h, column order k, product slot ts < 4) ten
+// fields over the row orders 0..N: the form without the powers <= 0 (re hi, lo, im hi, lo), its
+// magnitude sum, the form without the powers < 0 (the same five).
+__device__ __forceinline__ double* forms_slot(const double* ser0, int n_theta, int N, int G, int h,
+                                              int k, int ts) {
+  const int64_t n1 = N + 1;
+  return const_cast<double*>(ser0) + (int64_t)n_theta * n1 * (j_slot_size(G) + 15 * (int64_t)(G + 1)) +
+         (((int64_t)h * n1 + k) * 4 + ts) * 10 * n1;
+}
 
 // The number of terms of a series with term ratios x^2 / den(l), l >= 1, until the terms at
 // r_max are past their peak (after l_min) and below kSeriesTol of it (regular.rs:97-124, 140-150).
@@ -259,9 +293,14 @@ __global__ void __launch_bounds__(128) tm_series_kernel(TmArgs a) {
   const int N = g.N, G = N / 2 + 2;
   const int64_t local = t - g.sth0;
   const int h = (int)(local / N), n = 1 + (int)(local % N);
-  const int64_t S = tm_series_slot(N);
-  double* p = a.ser + g.ser0 + ((int64_t)h * (N + 1) + n) * S;
-  for (int64_t j = 0; j < S; ++j) p[j] = 0.0;
+  const int64_t JS = j_slot_size(G), n1 = N + 1;
+  double* p = a.ser + g.ser0 + ((int64_t)h * n1 + n) * JS;
+  for (int64_t j = 0; j < JS; ++j) p[j] = 0.0;
+  double* yb[3];
+  for (int c = 0; c < 3; ++c) {
+    yb[c] = const_cast<double*>(y_table(a.ser + g.ser0, g.n_theta, N, G, h, c)) + n;
+    for (int64_t j = 0; j < 5 * (int64_t)(G + 1); ++j) yb[c][j * n1] = 0.0;
+  }
   const double* ns = a.node + (g.node0 + g.n_theta + h) * kNodeD;
   const dd r = ld(ns), ir = ld(ns + 2);
   const cdd sr = ldc(ns + 8);
@@ -274,12 +313,8 @@ __global__ void __launch_bounds__(128) tm_series_kernel(TmArgs a) {
   }
   p[0] = Ly;
   p[1] = Lj;
-  double* yb[3];
   double* jb[3];
-  for (int c = 0; c < 3; ++c) {
-    yb[c] = p + 2 + c * (5 * G + 3);
-    jb[c] = p + 2 + 3 * (5 * G + 3) + c * (10 * G + 5);
-  }
+  for (int c = 0; c < 3; ++c) jb[c] = p + 2 + c * (10 * G + 5);
   // y: the first term, forward to the last, then back with the suffix sums.
   {
     const dd r2 = r * r, ir2 = ir * ir;
@@ -294,10 +329,15 @@ __global__ void __launch_bounds__(128) tm_series_kernel(TmArgs a) {
       for (int c = 0; c < 3; ++c) {
         sum[c] = sum[c] + term[c];
         mag[c] += fabs(term[c].hi);
-        if (l < G) st(yb[c] + 2 * l, term[c]);
         if (l <= G) {
-          st(yb[c] + 2 * G + 2 * l, sum[c]);
-          yb[c][4 * G + 2 + l] = mag[c];
+          double* e = yb[c] + (int64_t)l * 5 * n1;
+          if (l < G) {
+            e[0] = term[c].hi;
+            e[n1] = term[c].lo;
+          }
+          e[2 * n1] = sum[c].hi;
+          e[3 * n1] = sum[c].lo;
+          e[4 * n1] = mag[c];
         }
       }
       if (l > 0) v = -(v * (2.0 * l * (2.0 * l - 2.0 * n - 1.0))) * ir2;
@@ -356,12 +396,11 @@ namespace {
 // terms of its Laurent series in r of power <= cut, by the series of its higher powers or as
 // R minus the lower ones, whichever adds less in magnitude (regular.rs:255-311). yk, jk: the
 // kinds of the y_n and j_k factors (0 f, 1 [z f]'/z, 2 f/z); full = R_t at the node, xe = r^e.
-__device__ __forceinline__ void reg_form(const SerSlot& si, const SerSlot& sk, int yk, int jk,
-                                         int e, int n, int k, int cut, dd xe, cdd full,
+__device__ __forceinline__ void reg_form(const YTab& yt, int Ly, const JSlot& sk, int Lj, int yk,
+                                         int jk, int e, int n, int k, int cut, dd xe, cdd full,
                                          cdd* out, double* out_abs) {
-  const double* yb = si.yk(yk);
   const double* jb = sk.jk(jk);
-  const int G = si.G, Ly = si.ly(), Lj = sk.lj();
+  const int G = sk.G;
   const int base0 = (-n - 1 - (yk > 0)) + (k - (jk > 0)) + e;
   int l_end = cut >= base0 ? (cut - base0) / 2 + 1 : 0;
   l_end = min(min(l_end, Ly), G - 1);
@@ -369,7 +408,7 @@ __device__ __forceinline__ void reg_form(const SerSlot& si, const SerSlot& sk, i
   double neg_abs = 0.0, pos_abs = 0.0;
   for (int l = 0; l < l_end; ++l) {
     const int i_max = (cut - base0 - 2 * l) / 2;
-    const dd yv = ld(yb + 2 * l) * xe;
+    const dd yv = yt.term(l, n) * xe;
     const double ya = fabs(yv.hi);
     const int ii = max(min(min(i_max, Lj - 1), G - 1), 0);
     neg = ddm::add_terms(neg, ldc(jb + 4 * ii) * yv);
@@ -378,9 +417,9 @@ __device__ __forceinline__ void reg_form(const SerSlot& si, const SerSlot& sk, i
     pos = ddm::add_terms(pos, ldc(jb + 5 * G + 4 * from) * yv);
     pos_abs += jb[9 * G + 4 + from] * ya;
   }
-  const dd ysum = ld(yb + 2 * G + 2 * l_end) * xe;
+  const dd ysum = yt.sum(l_end, n) * xe;
   pos = ddm::add_terms(pos, ldc(jb + 5 * G) * ysum);
-  pos_abs += jb[9 * G + 4] * yb[4 * G + 2 + l_end] * fabs(xe.hi);
+  pos_abs += jb[9 * G + 4] * yt.mag(l_end, n) * fabs(xe.hi);
   const double sub_abs = fabs(full.re.hi) + fabs(full.im.hi) + neg_abs;
   if (pos_abs <= sub_abs) {
     *out = pos;
@@ -395,33 +434,112 @@ __device__ __forceinline__ void reg_form(const SerSlot& si, const SerSlot& sk, i
 // minus the powers < 0 (|n - k| >= 3) and minus the powers <= 0 (n != k), each with the sum of
 // the magnitudes it adds (kernel.rs:418-442).
 struct Forms3 {
-  cdd v[3];
-  double a[3];
+  cdd v0, v1, v2;
+  double a0, a1, a2;
 };
-__device__ __forceinline__ void add_type(Forms3& f, const SerSlot& si, const SerSlot& sk, int yk,
-                                         int jk, int e, int n, int k, dd xe, cdd full, dd alpha,
-                                         bool im, dd W) {
+// The series' view at one node for a row order n and a column order k.
+struct SerView {
+  YTab yt[3];  // y-table of the node per kind
+  JSlot sk;    // j-slot of (node, k)
+  int Ly, Lj;
+};
+
+// The radial products of an (n, k) pair's nonzero elements, by the parity of n + k, as (y kind,
+// j kind, e): even (MN, NM): R_1, R_4, R_6, R_2; odd (MM, NN): R_0, R_3, R_5, R_7.
+__device__ __forceinline__ void product_kind(bool even, int ts, int* yk, int* jk, int* e) {
+  constexpr int kEven[4][3] = {{0, 1, 2}, {0, 2, 4}, {2, 0, 4}, {1, 0, 2}};
+  constexpr int kOdd[4][3] = {{0, 0, 2}, {1, 1, 2}, {1, 2, 4}, {2, 1, 4}};
+  const int* v = even ? kEven[ts] : kOdd[ts];
+  *yk = v[0];
+  *jk = v[1];
+  *e = v[2];
+}
+
+// One term c R_t of a y-part integrand (c = alpha or i alpha, im) in the three forms: plain,
+// minus the powers < 0 (|n - k| >= 3) and minus the powers <= 0 (n != k), each with the sum of
+// the magnitudes it adds (kernel.rs:418-442); the regularized forms from the forms table
+// (fs: the pair's slot at the node, row n at offset 0).
+__device__ __forceinline__ void add_type(Forms3& f, const double* fs, int n1, int n, int k,
+                                         cdd full, dd alpha, bool im, dd W) {
   const dd cw = alpha * W;
   const double ca = fabs(cw.hi);
-  auto acc = [&](int form, cdd v, double va) {
-    cdd x = v * cw;
-    if (im) x = ddm::times_i(x);
-    f.v[form] = ddm::add_terms(f.v[form], x);
-    f.a[form] += ca * va;
+  auto scaled = [&](cdd v) {
+    const cdd x = v * cw;
+    return im ? ddm::times_i(x) : x;
   };
-  acc(0, full, fabs(full.re.hi) + fabs(full.im.hi));
+  f.v0 = ddm::add_terms(f.v0, scaled(full));
+  f.a0 += ca * (fabs(full.re.hi) + fabs(full.im.hi));
   if (n == k) return;
-  cdd v;
-  double va;
+  auto field = [&](int j) { return fs[(int64_t)j * n1]; };
+  f.v2 = ddm::add_terms(f.v2, scaled(cdd{dd{field(0), field(1)}, dd{field(2), field(3)}}));
+  f.a2 += ca * field(4);
   if (abs(n - k) >= 3) {
-    reg_form(si, sk, yk, jk, e, n, k, -1, xe, full, &v, &va);
-    acc(1, v, va);
+    f.v1 = ddm::add_terms(f.v1, scaled(cdd{dd{field(5), field(6)}, dd{field(7), field(8)}}));
+    f.a1 += ca * field(9);
   }
-  reg_form(si, sk, yk, jk, e, n, k, 0, xe, full, &v, &va);
-  acc(2, v, va);
 }
 
 }  // namespace
+
+// The regularized forms of the radial products of the y-part, which do not depend on the
+// azimuthal mode: one thread per (spheroid, node of the half surface, column order k, row order
+// n != k), rows fastest (the reference computes them once per node before its mode loop,
+// kernel.rs:327-342). Per product of the pair's nonzero elements the forms without the powers
+// <= 0 and (|n - k| >= 3) without those < 0, with their magnitude sums, into the forms table.
+__global__ void __launch_bounds__(128) tm_forms_kernel(TmArgs a) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.n_forms_total) return;
+  const int gi = owner(a.n_geoms, t, [&](int i) { return a.geoms[i].fth0; });
+  const TmGeom g = a.geoms[gi];
+  const int N = g.N, G = N / 2 + 2, nh = g.n_theta;
+  const int64_t local = t - g.fth0, NN = (int64_t)N * N;
+  const int h = (int)(local / NN), rem = (int)(local % NN);
+  const int k = 1 + rem / N, n = 1 + rem % N;
+  if (n == k) return;
+  const int q = nh + h;
+  const double* ser = a.ser + g.ser0;
+  const int64_t JS = j_slot_size(G);
+  SerView sv;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) sv.yt[c] = YTab{y_table(ser, nh, N, G, h, c), N + 1};
+  sv.sk = JSlot{ser + ((int64_t)h * (N + 1) + k) * JS, G};
+  sv.Ly = (int)ser[(int64_t)n * JS];
+  sv.Lj = (int)ser[(int64_t)k * JS + 1];
+  const double* ns = a.node + (g.node0 + q) * kNodeD;
+  const dd r = ld(ns), ir = ld(ns + 2), r2 = r * r, r4 = r2 * r2;
+  const double* ri = a.rad + g.rad0 + ((int64_t)q * (N + 1) + n) * kRadD;
+  const double* rk = a.rad + g.rad0 + ((int64_t)q * (N + 1) + k) * kRadD;
+  const dd yr = ld(ri + 4), ydr = ld(ri + 6), yo = yr * ir;
+  const cdd w = ldc(rk + 8), wd = ldc(rk + 12), u = ldc(rk + 16);
+  const bool even = ((n + k) & 1) == 0;
+  const int n1 = N + 1;
+#pragma unroll
+  for (int ts = 0; ts < 4; ++ts) {
+    int yk, jk, e;
+    product_kind(even, ts, &yk, &jk, &e);
+    const dd yv = yk == 0 ? yr : (yk == 1 ? ydr : yo);
+    const cdd jv = jk == 0 ? w : (jk == 1 ? wd : u);
+    const dd xe = e == 2 ? r2 : r4;
+    const cdd full = jv * (yv * xe);
+    double* fs = forms_slot(ser, nh, N, G, h, k, ts) + n;
+    cdd v;
+    double va;
+    reg_form(sv.yt[yk], sv.Ly, sv.sk, sv.Lj, yk, jk, e, n, k, 0, xe, full, &v, &va);
+    fs[0] = v.re.hi;
+    fs[n1] = v.re.lo;
+    fs[2 * n1] = v.im.hi;
+    fs[3 * n1] = v.im.lo;
+    fs[4 * n1] = va;
+    if (abs(n - k) >= 3) {
+      reg_form(sv.yt[yk], sv.Ly, sv.sk, sv.Lj, yk, jk, e, n, k, -1, xe, full, &v, &va);
+      fs[5 * n1] = v.re.hi;
+      fs[6 * n1] = v.re.lo;
+      fs[7 * n1] = v.im.hi;
+      fs[8 * n1] = v.im.lo;
+      fs[9 * n1] = va;
+    }
+  }
+}
 
 // The surface integrals of one (mode, i, k) (ebcm.py:103-186, pi -> -pi for the outgoing
 // functions' phi-factor convention, g_i g_k taken out of the sum). With z = j_i(r) or
@@ -450,17 +568,17 @@ __global__ void __launch_bounds__(128) tm_surface_kernel(TmArgs a) {
   const TmJob jb = a.jobs[ji];
   const TmGeom g = a.geoms[jb.geom];
   const int N = g.N, m = jb.m, n0 = m > 1 ? m : 1, K = jb.K;
-  const int pr = (int)(t - jb.pair0), i = n0 + pr / K, k = n0 + pr % K;
+  // Rows fastest: a warp's threads share the column order k, so its j-slot, and read the
+  // y-table's consecutive orders.
+  const int pr = (int)(t - jb.pair0), i = n0 + pr % K, k = n0 + pr / K;
   const bool even = ((i + k) & 1) == 0;
   const int G = N / 2 + 2;
-  const int64_t S = tm_series_slot(N);
+  const double* ser = a.ser + g.ser0;
   cdd R0 = mkc(0.0), R1 = mkc(0.0);  // regular: MN, NM (even) or MM, NN (odd)
   Forms3 Y0, Y1;                     // y-part: the same two
-#pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    Y0.v[c] = Y1.v[c] = mkc(0.0);
-    Y0.a[c] = Y1.a[c] = 0.0;
-  }
+  Y0.v0 = Y0.v1 = Y0.v2 = Y1.v0 = Y1.v1 = Y1.v2 = mkc(0.0);
+  Y0.a0 = Y0.a1 = Y0.a2 = Y1.a0 = Y1.a1 = Y1.a2 = 0.0;
+
   const double cki = (double)i * (i + 1), ckk = (double)k * (k + 1);
   const int nh = g.n_theta;
   for (int h = 0; h < nh; ++h) {
@@ -478,8 +596,8 @@ __global__ void __launch_bounds__(128) tm_surface_kernel(TmArgs a) {
     const cdd w = ldc(rk + 8), wd = ldc(rk + 12), u = ldc(rk + 16);
     const dd jr = ld(ri), jdr = ld(ri + 2), yr = ld(ri + 4), ydr = ld(ri + 6);
     const dd yo = yr * ir;  // y / r
-    const SerSlot si{a.ser + g.ser0 + ((int64_t)h * (N + 1) + i) * S, G};
-    const SerSlot sk{a.ser + g.ser0 + ((int64_t)h * (N + 1) + k) * S, G};
+    const int n1 = N + 1;
+    const double* fs = forms_slot(ser, nh, N, G, h, k, 0) + i;  // product slot ts at ts 10 n1
     if (even) {
       const dd A2 = ddm::add_terms(pii * pik, ti * tk), A3 = ti * dk, A4 = di * tk;
       // Regular: MN = j w' A2 - nu k(k+1) j u A3, NM = nu i(i+1) (j/r) w A4 - j' w A2.
@@ -488,10 +606,10 @@ __global__ void __launch_bounds__(128) tm_surface_kernel(TmArgs a) {
       R0 = ddm::add_terms(R0, mn * fac);
       R1 = ddm::add_terms(R1, nm * fac);
       // y-part: MN = i A2 R_1 - i k(k+1) A3 nu' R_4, NM = i i(i+1) A4 nu' R_6 - i A2 R_2.
-      add_type(Y0, si, sk, 0, 1, 2, i, k, r2, wd * (yr * r2), A2, true, W);
-      add_type(Y0, si, sk, 0, 2, 4, i, k, r4, u * (yr * r4), -((A3 * nup) * ckk), true, W);
-      add_type(Y1, si, sk, 2, 0, 4, i, k, r4, w * (yo * r4), (A4 * nup) * cki, true, W);
-      add_type(Y1, si, sk, 1, 0, 2, i, k, r2, w * (ydr * r2), -A2, true, W);
+      add_type(Y0, fs, n1, i, k, wd * (yr * r2), A2, true, W);
+      add_type(Y0, fs + 10 * n1, n1, i, k, u * (yr * r4), -((A3 * nup) * ckk), true, W);
+      add_type(Y1, fs + 20 * n1, n1, i, k, w * (yo * r4), (A4 * nup) * cki, true, W);
+      add_type(Y1, fs + 30 * n1, n1, i, k, w * (ydr * r2), -A2, true, W);
     } else {
       const dd A1 = ddm::add_terms(pii * tk, ti * pik), A5 = pii * dk, A6 = di * pik;
       // Regular: MM = i j w A1, NN = i [j' w' A1 - nu (k(k+1) j' u A5 + i(i+1) (j/r) w' A6)].
@@ -502,10 +620,10 @@ __global__ void __launch_bounds__(128) tm_surface_kernel(TmArgs a) {
       R0 = ddm::add_terms(R0, mm * fac);
       R1 = ddm::add_terms(R1, nn * fac);
       // y-part: MM = -A1 R_0, NN = -A1 R_3 + k(k+1) A5 nu' R_5 + i(i+1) A6 nu' R_7.
-      add_type(Y0, si, sk, 0, 0, 2, i, k, r2, w * (yr * r2), -A1, false, W);
-      add_type(Y1, si, sk, 1, 1, 2, i, k, r2, wd * (ydr * r2), -A1, false, W);
-      add_type(Y1, si, sk, 1, 2, 4, i, k, r4, u * (ydr * r4), (A5 * nup) * ckk, false, W);
-      add_type(Y1, si, sk, 2, 1, 4, i, k, r4, wd * (yo * r4), (A6 * nup) * cki, false, W);
+      add_type(Y0, fs, n1, i, k, w * (yr * r2), -A1, false, W);
+      add_type(Y1, fs + 10 * n1, n1, i, k, wd * (ydr * r2), -A1, false, W);
+      add_type(Y1, fs + 20 * n1, n1, i, k, u * (ydr * r4), (A5 * nup) * ckk, false, W);
+      add_type(Y1, fs + 30 * n1, n1, i, k, wd * (yo * r4), (A6 * nup) * cki, false, W);
     }
   }
   // g_i g_k = sqrt((2i+1)(2k+1) / (16 pi^2 i(i+1) k(k+1))).
@@ -523,15 +641,17 @@ __global__ void __launch_bounds__(128) tm_surface_kernel(TmArgs a) {
       if (a.form == 2 && i != k) best = 2;
       if (a.form == 1 && abs(i - k) >= 3) best = 1;
     } else if (i != k) {
-      const double m2 = sa * first.a[2] + second.a[2];
-      double mb = sa * first.a[0] + second.a[0];
+      const double m2 = sa * first.a2 + second.a2;
+      double mb = kPlainBias * (sa * first.a0 + second.a0);
       if (m2 < mb) {
         best = 2;
         mb = m2;
       }
-      if (abs(i - k) >= 3 && sa * first.a[1] + second.a[1] < mb) best = 1;
+      if (abs(i - k) >= 3 && sa * first.a1 + second.a1 < mb) best = 1;
     }
-    return ddm::add_terms(mis * first.v[best], ddm::times_i(second.v[best]) * -1.0) * gg;
+    const cdd fv = best == 0 ? first.v0 : (best == 1 ? first.v1 : first.v2);
+    const cdd sv = best == 0 ? second.v0 : (best == 1 ? second.v1 : second.v2);
+    return ddm::add_terms(mis * fv, ddm::times_i(sv) * -1.0) * gg;
   };
   cdd out[8];
 #pragma unroll
@@ -648,6 +768,28 @@ __global__ void __launch_bounds__(256) tm_solve_kernel(TmArgs a) {
     stc(Bd + 4 * tr, -q[0]);
     A[tr] = Cd{q[1].re.hi + q[1].re.lo, q[1].im.hi + q[1].im.lo};
     X[tr] = Cd{-(q[0].re.hi + q[0].re.lo), -(q[0].im.hi + q[0].im.lo)};
+  }
+  __syncthreads();
+  // Each equation scaled by the power of two that brings its largest coefficient to [1, 2):
+  // the unscaled radial functions give the rows magnitudes over hundreds of decades, and
+  // partial pivoting is only as good as the rows' balance. Exact, and the solution is unchanged.
+  for (int r = t; r < n2; r += blockDim.x) {
+    double mx = 0.0;
+    for (int c = 0; c < n2; ++c) {
+      const Cd v = A[(int64_t)r * n2 + c];
+      mx = fmax(mx, fmax(fabs(v.re), fabs(v.im)));
+    }
+    if (!(mx > 0.0) || !isfinite(mx)) continue;
+    const int e = -ilogb(mx);
+    for (int c = 0; c < n2; ++c) {
+      const int64_t idx = (int64_t)r * n2 + c;
+      A[idx] = Cd{ldexp(A[idx].re, e), ldexp(A[idx].im, e)};
+      X[idx] = Cd{ldexp(X[idx].re, e), ldexp(X[idx].im, e)};
+      for (int p = 0; p < 4; ++p) {
+        Qd[4 * idx + p] = ldexp(Qd[4 * idx + p], e);
+        Bd[4 * idx + p] = ldexp(Bd[4 * idx + p], e);
+      }
+    }
   }
   __syncthreads();
   // LU of A with partial pivoting (the largest modulus, the first row on ties).
@@ -775,6 +917,8 @@ void launch_tm_tables(const TmArgs& a, cudaStream_t s) {
   tm_angular_kernel<<<(unsigned)((a.n_ang_total + 127) / 128), 128, 0, s>>>(a);
   if (a.n_ser_total > 0)
     tm_series_kernel<<<(unsigned)((a.n_ser_total + 127) / 128), 128, 0, s>>>(a);
+  if (a.n_forms_total > 0)
+    tm_forms_kernel<<<(unsigned)((a.n_forms_total + 127) / 128), 128, 0, s>>>(a);
 }
 void launch_tm_surface(const TmArgs& a, cudaStream_t s) {
   if (a.n_jobs <= 0) return;
