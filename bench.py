@@ -571,7 +571,8 @@ def spheroid_leg(torch, fp64_peak: float, scale: float = 1.0, cpu_seconds: float
                        "T-matrix rtol 1e-8, Greek order 64, 180 cosines",
            "value": w.n_nodes_total / (ms * 1e-3), "unit": "nodes/s", "ms": ms,
            "n_terms_max": int(terms[:, :, 0].max()), "n_terms_mean": float(terms[:, :, 0].mean()),
-           "kernels_ms": kms, "kernel_share": {k: v / ms for k, v in kms.items()}}
+           "kernels_ms": kms, "kernel_share": {k: v / ms for k, v in kms.items()},
+           "surface_pair_nodes_per_launch": [int(v) for v in work]}
     if TM_SURFACE_FLOP_PER_PAIR_NODE and kms["tm_surface_kernel"] > 0:
         achieved = TM_SURFACE_FLOP_PER_PAIR_NODE * float(work.sum()) / (
             kms["tm_surface_kernel"] * 1e-3) / 1e12
