@@ -530,9 +530,10 @@ def projection_large_droplets(torch, steps: int = 3, scale: float = 1.0):
             "max_err_vs_fp64": err}
 
 
-# FP64 operations (DADD + DMUL + 2 DFMA) per (pair, node) of tm_surface_kernel: the ncu
-# instruction counts of one launch on a small spheroid case divided by its pairs x nodes.
-TM_SURFACE_FLOP_PER_PAIR_NODE = 1799.5
+# FP64 operations (DADD + DMUL + 2 DFMA) per (pair, node of the half surface) of
+# tm_surface_kernel: the ncu instruction counts of its first three launches on the spheroid
+# leg's smallest case divided by their pairs x nodes.
+TM_SURFACE_FLOP_PER_PAIR_NODE = 1115.8
 
 
 def spheroid_leg(torch, fp64_peak: float, scale: float = 1.0, cpu_seconds: float = 10.0):
