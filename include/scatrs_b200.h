@@ -212,7 +212,8 @@ enum {
   SCATRS_PARAM_DISTRIBUTION = 0, /* ParamKind::Distribution(name) */
   SCATRS_PARAM_REFR_REAL = 1,    /* ParamKind::RefrReal */
   SCATRS_PARAM_REFR_IMAG = 2,    /* ParamKind::RefrImag */
-  SCATRS_PARAM_WEIGHT = 3        /* ParamKind::Weight: a component's (mode -1) or a mode's */
+  SCATRS_PARAM_WEIGHT = 3,       /* ParamKind::Weight: a component's (mode -1) or a mode's */
+  SCATRS_PARAM_ASPECT_RATIO = 4  /* ParamKind::AspectRatio: a spheroid component's */
 };
 typedef struct scatrs_param {
   int32_t component;
@@ -228,8 +229,12 @@ typedef struct scatrs_param {
  * blocks (weights du/dtheta r) and the derivatives along Re m and Im m, the averages follow
  * the quotient rule against the moments' dZ, the mixing adds the weight derivatives, and the
  * ratios carry the derivatives with first-order error estimates (ensemble/lin.rs). A component
- * is multimodal when its mode_weights are given. Spheres only; a single radius's radius is
- * exact (engine.rs:1158-1170), with zero error estimates. d_values, d_errors (P, 11, n_wl); d_phase, d_phase_err (P, 6, n_wl, n_mu); d_greek,
+ * is multimodal when its mode_weights are given. Spheres; or one spheroid component of one
+ * distribution, along its distribution's parameters, Re m, Im m and the aspect ratio
+ * (SCATRS_PARAM_ASPECT_RATIO), each node's derivatives those of its solution at its converged N
+ * and n_theta (engine.rs:379-471, 1281-1340 direct path). A single sphere radius's radius is
+ * exact (engine.rs:1158-1170), with zero error estimates; a single spheroid's follows
+ * monodisperse_direct (engine.rs:1896-1961). d_values, d_errors (P, 11, n_wl); d_phase, d_phase_err (P, 6, n_wl, n_mu); d_greek,
  * d_greek_err (P, 6, n_wl, L + 1), P = n_params, in the order of `params`. Invalid or
  * repeated parameters: SCATRS_INVALID_INPUT naming the parameter.
  * Replaces: the derivative path of Mixture::compute / Ensemble.compute(derivatives=...)

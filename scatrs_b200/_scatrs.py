@@ -98,8 +98,8 @@ def ensemble_parameters(items, mixture: bool) -> list[str]:
 
 def _parameter_records(items, mixture: bool) -> list:
     """The (component, mode, kind, index) of every name of ensemble_parameters, in its order
-    (scatrs/src/ensemble/mod.rs:254-337); kind None marks a parameter of a layered sphere or a
-    spheroid, which this path does not differentiate."""
+    (scatrs/src/ensemble/mod.rs:254-337); kind None marks a parameter of a layered sphere,
+    which this path does not differentiate."""
     out = []
     for ci, (spec, particle, _w) in enumerate(items):
         kind = spec[0]
@@ -113,7 +113,8 @@ def _parameter_records(items, mixture: bool) -> list:
         if pk == "sphere":
             out += [(ci, -1, _native.PARAM_REFR_REAL, 0), (ci, -1, _native.PARAM_REFR_IMAG, 0)]
         elif pk == "spheroid":
-            out += [(ci, -1, None, k) for k in range(3)]
+            out += [(ci, -1, _native.PARAM_REFR_REAL, 0), (ci, -1, _native.PARAM_REFR_IMAG, 0),
+                    (ci, -1, _native.PARAM_ASPECT_RATIO, 0)]
         else:
             layers = np.asarray(particle[2]).shape[0]
             out += [(ci, -1, None, k) for k in range(3 * layers - 1)]
@@ -329,15 +330,17 @@ def _compute_with_derivatives(items, wavelengths, mixture, greek, all_orders, mu
         if records[i][2] is None:
             raise InvalidInputError(
                 f"the derivative along {names[i]} is not on the adaptive GPU path: a layered "
-                "sphere's derivatives are on the fixed grid (ensemble_compute_fixed), a "
-                "spheroid's are not built")
+                "sphere's derivatives are on the fixed grid (ensemble_compute_fixed)")
     wl = np.ascontiguousarray(wavelengths, dtype=np.float64).reshape(-1)
     mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
     L = _greek_order(greek, all_orders)
     comps = []
     for spec, particle, weight in items:
         dists, mode_w = _modes(spec)
-        comps.append((dists, mode_w, float(weight), _sphere_m(particle, wl.size)))
+        # A spheroid (one component of one distribution) goes as its checked spec.
+        part = (_particle(particle, wl.size) if isinstance(particle, tuple) and particle
+                and particle[0] == "spheroid" else _sphere_m(particle, wl.size))
+        comps.append((dists, mode_w, float(weight), part))
     params = np.array([records[i] for i in chosen], dtype=_native.PARAM_DTYPE)
     out = _native.ensemble_mixture_d(comps, wl, params, mu, L, bool(normalized), float(rtol),
                                      int(max_panels), bool(allow_unvalidated),

@@ -597,7 +597,7 @@ void pass1(std::vector<Job>& jobs, const std::vector<Part>& parts, const double*
       for (int j = 0; j < kPass1; ++j) qi[j] = j;
       {
         int at = kPass1;
-        for (int dir = 0; dir < 2; ++dir)
+        for (int dir = 0; dir < kMaxDirs; ++dir)
           if (first.dirs[dir])
             for (int j = 0; j < kGroup; ++j) qi[at++] = kPass1 + kGroup * dir + j;
       }

@@ -17,8 +17,11 @@ namespace adaptive {
 
 constexpr int kMonodisperse = 5;  // a single radius (param[0])
 constexpr int kPass1 = 6;         // 1, C_ext, C_sca, C_sca g, C_back, C_abs (engine.rs:43-54)
-constexpr int kGroup = 5;         // per direction along m: d of C_ext, C_sca, C_sca g, C_back, C_abs
-constexpr int kNodeQ = kPass1 + 2 * kGroup;  // a node's quantities with both directions
+constexpr int kGroup = 5;         // per direction: d of C_ext, C_sca, C_sca g, C_back, C_abs
+// The particle's directions (particle.rs:119-145): Re m and Im m, and a spheroid's aspect ratio.
+constexpr int kMaxDirs = 3;
+constexpr int kSphereQ = kPass1 + 2 * kGroup;       // a sphere node's quantities with Re m, Im m
+constexpr int kNodeQ = kPass1 + kMaxDirs * kGroup;  // a node's quantities with every direction
 
 struct Error {
   int status;
@@ -41,13 +44,16 @@ struct Part {
   int kind = 0;
   double p[3] = {0, 0, 0};
   // The requested distribution parameters (indices into the density's gradient, in the order
-  // of their result columns) and the requested derivatives along Re m and Im m.
+  // of their result columns) and the requested derivatives along Re m, Im m and (a spheroid)
+  // the aspect ratio.
   std::vector<int> grads;
-  bool dirs[2] = {false, false};
-  bool dir_derivatives() const { return dirs[0] || dirs[1]; }
+  bool dirs[kMaxDirs] = {false, false, false};
+  bool dir_derivatives() const { return dirs[0] || dirs[1] || dirs[2]; }
   // The pass-1 quantities (engine.rs:464-471): the base ones, then kGroup per requested
   // direction.
-  int n_refined() const { return kPass1 + kGroup * ((int)dirs[0] + (int)dirs[1]); }
+  int n_refined() const {
+    return kPass1 + kGroup * ((int)dirs[0] + (int)dirs[1] + (int)dirs[2]);
+  }
   double reference = 1.0, log_width = 0.0;  // distribution.rs:292-336
   Support support = UNBOUNDED;
   double lo = 0.0, hi = 0.0;  // the Mie range before extensions (a point: r, r)
@@ -80,7 +86,7 @@ struct Query {
   int wl;
 };
 struct NodeResult {
-  double q[kNodeQ];  // the kPass1 quantities, then kGroup derivatives along Re m and along Im m
+  double q[kNodeQ];  // the kPass1 quantities, then kGroup derivatives along each direction
   int64_t n;
   int status;
 };

@@ -1814,7 +1814,7 @@ void adaptive_call_order(const std::vector<AdPart>& in, int n_out, bool batch,
       a.scratch = c.p1_scratch.as<int64_t>(n + 1);
       a.uz = c.p1_uz.as<double2>((size_t)rows * (2 * L - 1));
       a.ux = c.p1_ux.as<double>(rows);
-      const int nq = any_dirs ? adaptive::kNodeQ : adaptive::kPass1;
+      const int nq = any_dirs ? adaptive::kSphereQ : adaptive::kPass1;
       a.deriv = any_dirs ? 1 : 0;
       a.q = c.p1_q.as<double>(nq * n);
       a.n_terms = c.p1_n.as<int64_t>(n);
@@ -3321,6 +3321,538 @@ void spheroid_call(const std::vector<SphParticle>& ps, bool batch, const double*
   }
 }
 
+// The adaptive ensemble of one spheroid distribution with derivatives (EnsembleOptions::
+// derivatives on the engine's direct path): pass 1 refines the requested distribution
+// parameters' blocks and the derivatives of C_ext, C_sca, C_sca g, C_back and C_abs along each
+// requested direction of the particle (Re m, Im m, the aspect ratio; engine.rs:379-471,
+// 620-720); pass 2 integrates the stored node values and their derivatives with their declared
+// errors (direct_node, engine.rs:1281-1340; the node errors summed with the absolute weights,
+// 1682-1740); the averages follow the quotient rule against the moments' dZ (averages,
+// engine.rs:1782-1836; a single radius: monodisperse_direct, 1896-1961, with the radius
+// derivative 2/r g + (2 pi / lambda) dg/dx); the outputs carry the derivatives through the
+// ratios (assemble, engine.rs:2396-2497; lin.rs). A node's derivatives are those of its
+// discretized solution at its converged N and n_theta (spheroid_fixed_derivs), where the
+// reference carries dual numbers through its T-matrix (tmatrix/mod.rs:231-245).
+struct SphDerivReq {
+  std::vector<int> grads, theta_cols;  // distribution parameters and their result columns
+  int dir_cols[3] = {-1, -1, -1};      // result columns along Re m, Im m, the aspect ratio
+};
+
+void spheroid_call_d(const SphParticle& sp, const SphDerivReq& req, const double* wavelengths,
+                     int64_t n_wl, const double* mu, int64_t n_mu,
+                     const scatrs_adaptive_options* options, const AdOutputs& res,
+                     const AdDerivs& dd) {
+  if (!options) throw Failure{SCATRS_INVALID_INPUT, "options must not be NULL"};
+  if (sp.n_dist != 1) throw Failure{SCATRS_INVALID_INPUT, "one distribution"};
+  if (n_wl < 0) throw Failure{SCATRS_INVALID_INPUT, "negative sizes"};
+  const bool all_orders = options->greek_order == SCATRS_GREEK_ALL;
+  const adaptive::Options o{options->rtol, options->max_panels, options->allow_unvalidated != 0,
+                            options->refine_backscatter != 0};
+  if (!(o.rtol >= 1e-13 && o.rtol <= 0.1)) {
+    char buf[80];
+    snprintf(buf, sizeof buf, "rtol must be in [1e-13, 0.1], got %g", o.rtol);
+    throw Failure{SCATRS_INVALID_INPUT, buf};
+  }
+  if (o.max_panels < 1) throw Failure{SCATRS_INVALID_INPUT, "max_panels must be at least 1"};
+  for (int64_t i = 0; i < n_wl; ++i)
+    if (!(std::isfinite(wavelengths[i]) && wavelengths[i] > 0.0))
+      throw Failure{SCATRS_INVALID_INPUT,
+                    "wavelength " + std::to_string(i) + " must be finite and > 0"};
+  if (!(std::isfinite(sp.eps) && sp.eps > 0.0))
+    throw Failure{SCATRS_INVALID_INPUT, "the aspect ratio must be finite and > 0"};
+  scatrs_fixed_options fo{32, all_orders ? -1 : options->greek_order, options->normalized,
+                          options->allow_unvalidated};
+  const int64_t n_units = n_wl;
+  check_options(&fo, n_units, n_mu, mu);
+  if (n_units == 0) return;
+  const scatrs_distribution& dist = sp.dists[0];
+  adaptive::Part part;
+  try {
+    part = adaptive::make_part(dist.kind, dist.param, o.rtol, dist.table, dist.table_len,
+                               req.grads);
+  } catch (const adaptive::Error& e) {
+    throw Failure{e.status, "distribution 0: " + e.msg};
+  }
+  for (int k = 0; k < 3; ++k) part.dirs[k] = req.dir_cols[k] >= 0;
+  const bool point = part.support == adaptive::POINT;
+  const int nt = (int)req.grads.size();
+  // The directions solved at each node: every one of the particle's when any is asked for
+  // (engine.rs:1438-1440), and x for a single radius's radius. spheroid_fixed_derivs orders
+  // them x, aspect ratio, Re m, Im m; here the directions are Re m, Im m, aspect ratio, x.
+  const bool any_dir = part.dir_derivatives();
+  const bool along_x = point && nt > 0;
+  const unsigned mask = (any_dir ? 0xEu : 0u) | (along_x ? 0x1u : 0u);
+  const int sfd_of[4] = {2, 3, 1, 0};
+  const double rtol_t = std::min(std::max(o.rtol / 100.0, 1e-12), 1e-8);
+  const double pi = 3.14159265358979323846;
+  Context& c = context();
+  std::lock_guard<std::mutex> lk(c.mtx);
+  cudaStream_t s = 0;
+  // Solved nodes by (wavelength, radius bits): the values, and per direction the derivatives
+  // of (Q_ext, Q_sca, Q_abs, Q_back, g, then the six unnormalized Greek arrays to 2N).
+  struct Node {
+    SpheroidResult v;
+    std::vector<double> d[4];
+  };
+  std::map<std::pair<int64_t, uint64_t>, Node> cache;
+  auto key_of = [](int64_t i, double r) {
+    uint64_t b;
+    memcpy(&b, &r, 8);
+    return std::make_pair(i, b);
+  };
+  auto solve = [&](const std::vector<adaptive::Query>& qs) {
+    std::vector<double> xs, es, ms;
+    std::vector<std::pair<int64_t, double>> which;
+    for (const adaptive::Query& q : qs) {
+      const int64_t i = q.wl;
+      if (cache.count(key_of(i, q.r))) continue;
+      xs.push_back(2.0 * pi * q.r / wavelengths[i]);
+      es.push_back(sp.eps);
+      ms.push_back(sp.m[2 * i]);
+      ms.push_back(sp.m[2 * i + 1]);
+      which.push_back({i, q.r});
+    }
+    if (which.empty()) return;
+    std::vector<SpheroidResult> r;
+    spheroid_solve(c, (int64_t)which.size(), xs.data(), es.data(), ms.data(), rtol_t, 0, 0, true,
+                   r, s, o.allow_unvalidated);
+    std::vector<SphEval> ev(which.size());
+    int order = 0;
+    for (size_t k = 0; k < which.size(); ++k) {
+      ev[k] = {xs[k], sp.eps, ms[2 * k], ms[2 * k + 1], r[k].n, r[k].nth};
+      order = std::max(order, 2 * r[k].n);
+    }
+    std::vector<std::vector<double>> d[4];
+    if (mask) spheroid_fixed_derivs(c, ev, order, false, d, s, mask);
+    const int64_t len = (int64_t)order + 1;
+    for (size_t k = 0; k < which.size(); ++k) {
+      Node nd;
+      const int64_t have = 2 * (int64_t)r[k].n + 1;
+      for (int dir = 0; dir < 4; ++dir) {
+        if (!(mask >> sfd_of[dir] & 1u)) continue;
+        const std::vector<double>& src = d[sfd_of[dir]][k];
+        std::vector<double>& dst = nd.d[dir];
+        dst.assign(5 + 6 * have, 0.0);
+        for (int j = 0; j < 5; ++j) dst[j] = src[j];
+        for (int f = 0; f < 6; ++f)
+          for (int64_t l = 0; l < have; ++l) dst[5 + f * have + l] = src[5 + f * len + l];
+      }
+      nd.v = std::move(r[k]);
+      cache[key_of(which[k].first, which[k].second)] = std::move(nd);
+    }
+  };
+  // The pass-1 quantities (quantities1, engine.rs:379-417): the values, then per direction
+  // d C_ext, d C_sca, d(C_sca g), d C_back, d C_abs.
+  auto eval = [&](const std::vector<adaptive::Query>& qs, std::vector<adaptive::NodeResult>& out) {
+    solve(qs);
+    for (size_t k = 0; k < qs.size(); ++k) {
+      const Node& nd = cache.at(key_of(qs[k].wl, qs[k].r));
+      const SpheroidResult& v = nd.v;
+      const double area = pi * qs[k].r * qs[k].r;
+      adaptive::NodeResult& x = out[k];
+      const double q[6] = {1.0, area * v.q_ext, area * v.q_sca, area * v.q_sca * v.g,
+                           area * v.q_back, area * v.q_abs};
+      for (int j = 0; j < adaptive::kNodeQ; ++j) x.q[j] = 0.0;
+      for (int j = 0; j < 6; ++j) x.q[j] = q[j];
+      for (int dir = 0; dir < 3 && any_dir; ++dir) {
+        const std::vector<double>& dq = nd.d[dir];
+        double* o5 = x.q + adaptive::kPass1 + adaptive::kGroup * dir;
+        o5[0] = area * dq[0];
+        o5[1] = area * dq[1];
+        o5[2] = area * (dq[1] * v.g + v.q_sca * dq[4]);
+        o5[3] = area * dq[3];
+        o5[4] = area * dq[2];
+      }
+      x.n = v.n;
+      x.status = 0;
+    }
+  };
+  // Pass 1 per wavelength (the part on its own panels), or the single radius itself.
+  std::vector<adaptive::Part> parts{part};
+  std::vector<adaptive::Job> jobs;
+  std::vector<adaptive::NodeResult> point_res;
+  if (point) {
+    std::vector<adaptive::Query> points;
+    for (int64_t i = 0; i < n_wl; ++i) points.push_back({part.lo, (int)i});
+    point_res.resize(points.size());
+    eval(points, point_res);
+  } else {
+    for (int64_t i = 0; i < n_wl; ++i) {
+      adaptive::Job jb;
+      jb.wl = (int)i;
+      jb.parts = {0};
+      jobs.push_back(jb);
+    }
+    adaptive::pass1(jobs, parts, wavelengths, o, eval);
+    for (const adaptive::Job& jb : jobs)
+      if (jb.status != 0) throw Failure{jb.status, jb.msg};
+  }
+  std::vector<int64_t> n_direct(n_units);
+  int64_t width = 0;
+  for (int64_t u = 0; u < n_units; ++u) {
+    n_direct[u] = point ? cache.at(key_of(u, part.lo)).v.n : jobs[u].n_terms;
+    width = std::max(width, 2 * n_direct[u] + 1);
+  }
+  const int64_t P = dd.n;
+  if (all_orders) {
+    GreekAll& ga = t_greek_all;
+    ga.width = width;
+    ga.n = n_units;
+    ga.p = P;
+    ga.g.assign(6 * n_units * width, 0.0);
+    ga.ge.assign(ga.g.size(), 0.0);
+    ga.dg.assign(P * ga.g.size(), 0.0);
+    ga.dge.assign(ga.dg.size(), 0.0);
+  }
+  const bool keep_greek = options->greek_order >= 0 || all_orders || n_mu > 0;
+  constexpr int kS = 9;  // ONE, EXT, SCA, SCAG, ABS, BACK, R2, R3, DEPOL
+  for (int64_t u = 0; u < n_units; ++u) {
+    const int64_t i = u;
+    const double lambda = wavelengths[i];
+    const int L = all_orders ? (int)(2 * n_direct[u]) : options->greek_order;
+    const int64_t ld = !keep_greek ? -1 : n_mu == 0 ? std::min<int64_t>(L, 2 * n_direct[u])
+                                                      : 2 * n_direct[u];
+    const int64_t glen = ld + 1;  // 0 without a direct segment
+    const int64_t len = kS + 6 * glen;
+    // A node's rows (direct_node, direct_scalars): the values and their declared errors, and
+    // per direction (Re m, Im m, aspect ratio, x) the derivatives and theirs, relative to the
+    // derivatives themselves.
+    std::vector<double> g(len), ge(len), dg(4 * len), dge(4 * len);
+    auto rows_at = [&](double r) {
+      const Node& nd = cache.at(key_of(i, r));
+      const SpheroidResult& v = nd.v;
+      const double area = pi * r * r;
+      const double tau = std::max(rtol_t, v.err_est);
+      const double c4 = 4.0 * tau, c16 = 16.0 * tau;
+      const int64_t have = 2 * (int64_t)v.n + 1;
+      const double x = 2.0 * pi * r / lambda, un = 4.0 / (x * x);
+      double depol = 0.0;
+      for (int64_t l = 0; l < have; ++l) {
+        const double t = un * (v.greek[l] - 0.5 * (v.greek[have + l] - v.greek[2 * have + l]));
+        depol += l % 2 ? -t : t;
+      }
+      const double sv[kS] = {1.0,         area * v.q_ext, area * v.q_sca, area * v.q_sca * v.g,
+                             area * v.q_abs, area * v.q_back, r * r, r * r * r, area * depol};
+      const double back = area * std::max(std::fabs(v.q_back), std::fabs(v.q_sca));
+      const double se[kS] = {0.0,
+                             c4 * std::fabs(sv[1]),
+                             c4 * std::fabs(sv[2]),
+                             c4 * std::fabs(sv[2]) * (1.0 + std::fabs(v.g)),
+                             c16 * std::fabs(sv[1]),
+                             c16 * back,
+                             0.0,
+                             0.0,
+                             2.0 * c16 * back};
+      for (int k = 0; k < kS; ++k) {
+        g[k] = sv[k];
+        ge[k] = se[k];
+      }
+      if (glen > 0) {
+        double big = 0.0;
+        for (int64_t l = 0; l < have; ++l) big = std::max(big, std::fabs(un * v.greek[l]));
+        const double ce = c16 * area * big;
+        for (int f = 0; f < 6; ++f)
+          for (int64_t l = 0; l < glen; ++l) {
+            g[kS + f * glen + l] = l < have ? area * un * v.greek[f * have + l] : 0.0;
+            ge[kS + f * glen + l] = ce;
+          }
+      }
+      for (int dir = 0; dir < 4; ++dir) {
+        double* d = dg.data() + dir * len;
+        double* de = dge.data() + dir * len;
+        if (nd.d[dir].empty()) {
+          std::fill(d, d + len, 0.0);
+          std::fill(de, de + len, 0.0);
+          continue;
+        }
+        // The unnormalized Greek arrays' derivatives (4/x^2 times the coefficients').
+        const double* dq = nd.d[dir].data();
+        const double* gr = dq + 5;
+        double ddepol = 0.0;
+        for (int64_t l = 0; l < have; ++l) {
+          const double t = gr[l] - 0.5 * (gr[have + l] - gr[2 * have + l]);
+          ddepol += l % 2 ? -t : t;
+        }
+        const double sd[kS] = {0.0,
+                               area * dq[0],
+                               area * dq[1],
+                               area * (dq[1] * v.g + v.q_sca * dq[4]),
+                               area * dq[2],
+                               area * dq[3],
+                               0.0,
+                               0.0,
+                               area * ddepol};
+        const double cd[kS] = {0.0, c4, c4, c4, c16, c16, 0.0, 0.0, c16};
+        for (int k = 0; k < kS; ++k) {
+          d[k] = sd[k];
+          de[k] = cd[k] * std::fabs(sd[k]);
+        }
+        for (int f = 0; f < 6; ++f)
+          for (int64_t l = 0; l < glen; ++l) {
+            const double y = l < have ? area * gr[f * have + l] : 0.0;
+            d[kS + f * glen + l] = y;
+            de[kS + f * glen + l] = c16 * std::fabs(y);
+          }
+      }
+    };
+    std::vector<double> av(len, 0.0), ae(len, 0.0), dv(P * len, 0.0), de(P * len, 0.0);
+    bool conv = true;
+    int64_t panels = 0;
+    if (point) {
+      // monodisperse_direct (engine.rs:1896-1961): the particle itself; its radius
+      // d/dr = 2/r g + (2 pi / lambda) dg/dx, errors likewise, exact r^2 and r^3.
+      const double r = part.lo;
+      rows_at(r);
+      av = g;
+      ae = ge;
+      if (nt > 0) {
+        const int col = req.theta_cols[0];
+        const double k = 2.0 * pi / lambda;
+        const double* gx = dg.data() + 3 * len;
+        const double* ex = dge.data() + 3 * len;
+        for (int64_t j = 0; j < len; ++j) {
+          dv[col * len + j] = 2.0 / r * g[j] + k * gx[j];
+          de[col * len + j] = 2.0 / r * ge[j] + k * ex[j];
+        }
+        dv[col * len + 0] = 0.0;
+        dv[col * len + 6] = 2.0 * r;
+        dv[col * len + 7] = 3.0 * r * r;
+        de[col * len + 0] = de[col * len + 6] = de[col * len + 7] = 0.0;
+      }
+      for (int dir = 0; dir < 3; ++dir) {
+        const int col = req.dir_cols[dir];
+        if (col < 0) continue;
+        for (int64_t j = 0; j < len; ++j) {
+          dv[col * len + j] = dg[dir * len + j];
+          de[col * len + j] = dge[dir * len + j];
+        }
+      }
+    } else {
+      const adaptive::Job& jb = jobs[u];
+      conv = jb.converged[0];
+      panels = (int64_t)jb.panels.size();
+      // Blocks: the values (weights u r), each parameter's (weights du/dtheta r on the values),
+      // each requested direction's (weights u r on its derivative rows).
+      std::vector<int> dirs;
+      for (int dir = 0; dir < 3; ++dir)
+        if (req.dir_cols[dir] >= 0) dirs.push_back(dir);
+      const int nb = 1 + nt + (int)dirs.size();
+      std::vector<double> S(nb * len, 0.0), E(nb * len, 0.0);
+      std::vector<double> ks(nb * len), gs(nb * len), ne(nb * len);
+      double grad[3] = {0.0, 0.0, 0.0};
+      for (const auto& ab : jb.panels) {
+        adaptive::Node nd[15];
+        adaptive::gk15(ab.first, ab.second, nd);
+        std::fill(ks.begin(), ks.end(), 0.0);
+        std::fill(gs.begin(), gs.end(), 0.0);
+        std::fill(ne.begin(), ne.end(), 0.0);
+        for (int k = 0; k < 15; ++k) {
+          const double r = std::exp(nd[k].t);
+          const double ur = (nt > 0 ? part.u(r, grad) : part.u(r)) * r;
+          rows_at(r);
+          for (int b = 0; b < nb; ++b) {
+            double w;
+            const double *row, *err;
+            if (b == 0) {
+              w = ur;
+              row = g.data();
+              err = ge.data();
+            } else if (b <= nt) {
+              w = grad[req.grads[b - 1]] * r;
+              row = g.data();
+              err = ge.data();
+            } else {
+              w = ur;
+              row = dg.data() + dirs[b - 1 - nt] * len;
+              err = dge.data() + dirs[b - 1 - nt] * len;
+            }
+            double* kb = ks.data() + b * len;
+            double* gb = gs.data() + b * len;
+            double* nb_ = ne.data() + b * len;
+            const double wk = nd[k].wk * w, wg = nd[k].wg * w, wa = std::fabs(wk);
+            for (int64_t j = 0; j < len; ++j) {
+              kb[j] += wk * row[j];
+              gb[j] += wg * row[j];
+              nb_[j] += wa * err[j];
+            }
+          }
+        }
+        for (int64_t j = 0; j < nb * len; ++j) {
+          S[j] += ks[j];
+          E[j] += std::fabs(ks[j] - gs[j]) + ne[j];
+        }
+      }
+      // averages (engine.rs:1782-1836).
+      const adaptive::Moments& mom = part.mom;
+      const double z = mom.z, ez = mom.ez;
+      const double trunc = part.support == adaptive::UNBOUNDED ? 0.2 * o.rtol : 0.0;
+      for (int64_t j = 0; j < len; ++j) {
+        av[j] = S[j] / z;
+        ae[j] = (E[j] + std::fabs(av[j]) * ez) / z + trunc * std::fabs(av[j]);
+      }
+      for (int b = 0; b < nt; ++b) {
+        const int col = req.theta_cols[b];
+        const double dz = mom.dz[b], edz = mom.dez[b];
+        const double* sb = S.data() + (1 + b) * len;
+        const double* eb = E.data() + (1 + b) * len;
+        for (int64_t j = 0; j < len; ++j) {
+          const double x = (sb[j] - av[j] * dz) / z;
+          dv[col * len + j] = x;
+          de[col * len + j] = (eb[j] + std::fabs(av[j]) * edz + std::fabs(x) * ez +
+                               ae[j] * std::fabs(dz)) /
+                                  z +
+                              trunc * std::fabs(x);
+        }
+      }
+      for (size_t c2 = 0; c2 < dirs.size(); ++c2) {
+        const int col = req.dir_cols[dirs[c2]];
+        const double* sb = S.data() + (1 + nt + c2) * len;
+        const double* eb = E.data() + (1 + nt + c2) * len;
+        for (int64_t j = 0; j < len; ++j) {
+          const double x = sb[j] / z;
+          dv[col * len + j] = x;
+          de[col * len + j] = (eb[j] + std::fabs(x) * ez) / z + trunc * std::fabs(x);
+        }
+      }
+      // <r^2>, <r^3> from the moments, with their parameter derivatives.
+      for (int k = 0; k < 2; ++k) {
+        av[6 + k] = mom.v[k];
+        ae[6 + k] = mom.e[k];
+        for (int64_t col = 0; col < P; ++col) {
+          dv[col * len + 6 + k] = 0.0;
+          de[col * len + 6 + k] = 0.0;
+        }
+        for (int b = 0; b < nt; ++b) {
+          dv[req.theta_cols[b] * len + 6 + k] = mom.d[b][k];
+          de[req.theta_cols[b] * len + 6 + k] = mom.de[b][k];
+        }
+      }
+    }
+    // assemble (engine.rs:2396-2497) with the derivatives (lin.rs).
+    auto lin = [&](int64_t j) {
+      LinD x;
+      x.v = av[j];
+      x.e = ae[j];
+      x.d.resize(P);
+      x.de.resize(P);
+      for (int64_t col = 0; col < P; ++col) {
+        x.d[col] = dv[col * len + j];
+        x.de[col] = de[col * len + j];
+      }
+      return x;
+    };
+    // sum of c_k terms_k for exact constants (Lin::combine).
+    auto combine = [&](std::initializer_list<std::pair<double, const LinD*>> terms) {
+      LinD out = LinD::constant(0.0, (size_t)P);
+      for (const auto& t : terms) {
+        const double cw = t.first;
+        const LinD& x = *t.second;
+        out.v += cw * x.v;
+        out.e += std::fabs(cw) * x.e;
+        for (int64_t k = 0; k < P; ++k) {
+          out.d[k] += cw * x.d[k];
+          out.de[k] += std::fabs(cw) * x.de[k];
+        }
+      }
+      return out;
+    };
+    const LinD ext = lin(1), sca = lin(2), scag = lin(3), abs_ = lin(4), back = lin(5),
+               r2 = lin(6), r3 = lin(7), num = lin(8);
+    for (const auto& w : {std::make_pair("<C_ext>", &ext), std::make_pair("<C_sca>", &sca),
+                          std::make_pair("<C_back>", &back)})
+      if (!(std::isfinite(w.second->v) && w.second->v != 0.0))
+        throw Failure{SCATRS_INVALID_INPUT,
+                      std::string("the ensemble's ") + w.first +
+                          " is zero or not finite, so its ratios are undefined (does m = 1?)"};
+    const LinD outs[11] = {ext,
+                           sca,
+                           abs_,
+                           back,
+                           sca.div(ext),
+                           scag.div(sca),
+                           ext.div(back).scale(4.0 * pi),
+                           num.div(combine({{2.0, &back}, {-1.0, &num}})),
+                           r3.div(r2),
+                           r2.scale(pi),
+                           r3.scale(4.0 * pi / 3.0)};
+    for (int k = 0; k < 11; ++k) {
+      res.values[k * n_units + u] = outs[k].v;
+      if (res.errors) res.errors[k * n_units + u] = outs[k].e;
+      for (int64_t col = 0; col < P; ++col) {
+        if (dd.d_values) dd.d_values[(col * 11 + k) * n_units + u] = outs[k].d[col];
+        if (dd.d_errors) dd.d_errors[(col * 11 + k) * n_units + u] = outs[k].de[col];
+      }
+    }
+    const bool norm = options->normalized != 0;
+    auto G = [&](int f, int64_t l) { return lin(kS + f * glen + l); };
+    if (L >= 0 && (res.greek || all_orders)) {
+      const LinD a0 = glen > 0 ? G(0, 0) : LinD::constant(0.0, (size_t)P);
+      const int64_t w = all_orders ? width : L + 1;
+      GreekAll& ga = t_greek_all;
+      for (int f = 0; f < 6; ++f)
+        for (int64_t l = 0; l <= L; ++l) {
+          LinD x = l < glen ? G(f, l) : LinD::constant(0.0, (size_t)P);
+          if (norm) x = (f == 0 && l == 0) ? LinD::constant(1.0, (size_t)P) : x.div(a0);
+          const int64_t at = ((int64_t)f * n_units + u) * w + l;
+          if (all_orders) {
+            ga.g[at] = x.v;
+            ga.ge[at] = x.e;
+          } else {
+            res.greek[at] = x.v;
+            if (res.greek_err) res.greek_err[at] = x.e;
+          }
+          for (int64_t col = 0; col < P; ++col) {
+            const int64_t atd = ((col * 6 + f) * n_units + u) * w + l;
+            if (all_orders) {
+              ga.dg[atd] = x.d[col];
+              ga.dge[atd] = x.de[col];
+            } else {
+              if (dd.d_greek) dd.d_greek[atd] = x.d[col];
+              if (dd.d_greek_err) dd.d_greek_err[atd] = x.de[col];
+            }
+          }
+        }
+    }
+    if (n_mu > 0 && res.phase) {
+      // greek_phase (engine.rs:2359-2390): combinations with exact weights, errors as bounds.
+      std::vector<double> d00(glen), d22(glen), d2m2(glen), d02(glen);
+      for (int64_t j = 0; j < n_mu; ++j) {
+        wigner_d(0, 0, mu[j], d00.data(), glen);
+        wigner_d(2, 2, mu[j], d22.data(), glen);
+        wigner_d(2, -2, mu[j], d2m2.data(), glen);
+        wigner_d(0, 2, mu[j], d02.data(), glen);
+        LinD f[6];
+        for (int k = 0; k < 6; ++k) f[k] = LinD::constant(0.0, (size_t)P);
+        for (int64_t l = 0; l < glen; ++l) {
+          const double plus = 0.5 * (d22[l] + d2m2[l]), minus = 0.5 * (d22[l] - d2m2[l]);
+          const double wt[6][2] = {{d00[l], 0}, {d02[l], 0}, {plus, minus},
+                                   {minus, plus}, {d02[l], 0}, {d00[l], 0}};
+          const int src[6][2] = {{0, -1}, {4, -1}, {1, 2}, {1, 2}, {5, -1}, {3, -1}};
+          for (int k = 0; k < 6; ++k)
+            for (int t = 0; t < 2; ++t) {
+              if (src[k][t] < 0) continue;
+              const LinD x = G(src[k][t], l);
+              f[k] = combine({{1.0, &f[k]}, {wt[k][t], &x}});
+            }
+        }
+        for (int k = 0; k < 6; ++k) {
+          const LinD x = norm ? f[k].div(sca) : f[k];
+          const int64_t at = ((int64_t)k * n_units + u) * n_mu + j;
+          res.phase[at] = x.v;
+          if (res.phase_err) res.phase_err[at] = x.e;
+          for (int64_t col = 0; col < P; ++col) {
+            const int64_t atd = ((col * 6 + k) * n_units + u) * n_mu + j;
+            if (dd.d_phase) dd.d_phase[atd] = x.d[col];
+            if (dd.d_phase_err) dd.d_phase_err[atd] = x.de[col];
+          }
+        }
+      }
+    }
+    if (res.converged) res.converged[u] = conv ? 1 : 0;
+    if (res.panels) res.panels[u] = panels;
+  }
+}
+
 FixedCall g_last_call;  // for scatrs_check_errors
 
 template <class F>
@@ -4038,11 +4570,15 @@ int scatrs_ensemble_mixture_d(const scatrs_component* components, int64_t n_comp
   return guarded(err, err_len, [&] {
     if (n_params < 0 || (n_params > 0 && !params))
       throw Failure{SCATRS_INVALID_INPUT, "params must hold n_params parameters"};
-    if (heterogeneous(components, n_comp)) {
+    // One spheroid distribution takes its derivatives on the direct path (spheroid_call_d).
+    const bool spheroid_alone = n_comp == 1 && components && components[0].aspect_ratio > 0.0 &&
+                                components[0].n_layers <= 1 && components[0].n_modes == 1 &&
+                                !components[0].mode_weights;
+    if (heterogeneous(components, n_comp) && !(n_params > 0 && spheroid_alone)) {
       if (n_params > 0)
         throw Failure{SCATRS_INVALID_INPUT,
-                      "derivatives of mixtures with layered spheres or spheroids are not on the "
-                      "GPU path"};
+                      "derivatives of layered spheres, and of spheroids beside other components "
+                      "or in multimodal distributions, are not on the adaptive GPU path"};
       AdOutputs out{values, errors, phase, phase_err, greek, greek_err, converged, panels};
       mixture_hetero(components, n_comp, wavelengths, n_wl, mu, n_mu, options, out);
       return;
@@ -4075,6 +4611,7 @@ int scatrs_ensemble_mixture_d(const scatrs_component* components, int64_t n_comp
         case SCATRS_PARAM_REFR_REAL: out += "m_real"; break;
         case SCATRS_PARAM_REFR_IMAG: out += "m_imag"; break;
         case SCATRS_PARAM_WEIGHT: out += "weight"; break;
+        case SCATRS_PARAM_ASPECT_RATIO: out += "aspect_ratio"; break;
         default: out += "kind" + std::to_string(q.kind);
       }
       return out;
@@ -4099,6 +4636,7 @@ int scatrs_ensemble_mixture_d(const scatrs_component* components, int64_t n_comp
           }
           case SCATRS_PARAM_REFR_REAL:
           case SCATRS_PARAM_REFR_IMAG: allowed = q.mode == -1; break;
+          case SCATRS_PARAM_ASPECT_RATIO: allowed = q.mode == -1 && cp.aspect_ratio > 0.0; break;
           case SCATRS_PARAM_WEIGHT:
             allowed = q.mode == -1 || (multi && q.mode >= 0 && q.mode < cp.n_modes);
             break;
@@ -4106,6 +4644,40 @@ int scatrs_ensemble_mixture_d(const scatrs_component* components, int64_t n_comp
         }
       }
       if (!allowed) throw Failure{SCATRS_INVALID_INPUT, "no parameter " + name(q) + " here"};
+    }
+    if (spheroid_alone) {
+      if (n_params > 0 && !d_values)
+        throw Failure{SCATRS_INVALID_INPUT, "d_values is required with parameters"};
+      SphDerivReq req;
+      for (int64_t k = 0; k < n_params; ++k) {
+        const scatrs_param& q = params[k];
+        if (q.kind == SCATRS_PARAM_DISTRIBUTION) {
+          req.grads.push_back(q.index);
+          req.theta_cols.push_back((int)k);
+        } else if (q.kind == SCATRS_PARAM_REFR_REAL) {
+          req.dir_cols[0] = (int)k;
+        } else if (q.kind == SCATRS_PARAM_REFR_IMAG) {
+          req.dir_cols[1] = (int)k;
+        } else if (q.kind == SCATRS_PARAM_ASPECT_RATIO) {
+          req.dir_cols[2] = (int)k;
+        }  // a single component's weight: its number fraction is 1 whatever it is
+      }
+      AdOutputs out{values, errors, phase, phase_err, greek, greek_err, converged, panels};
+      AdDerivs dd;
+      dd.params = params;
+      dd.n = n_params;
+      dd.d_values = d_values;
+      dd.d_errors = d_errors;
+      dd.d_phase = d_phase;
+      dd.d_phase_err = d_phase_err;
+      dd.d_greek = d_greek;
+      dd.d_greek_err = d_greek_err;
+      for (int64_t k = 0; k < n_params * 11 * n_wl && d_values; ++k) d_values[k] = 0.0;
+      for (int64_t k = 0; k < n_params * 11 * n_wl && d_errors; ++k) d_errors[k] = 0.0;
+      const scatrs_component& cp = components[0];
+      spheroid_call_d(SphParticle{cp.modes, 1, cp.aspect_ratio, cp.m}, req, wavelengths, n_wl, mu,
+                      n_mu, options, out, dd);
+      return;
     }
     // engine.rs:153-176: each part's parameters and their columns.
     for (AdPart& a : parts)
