@@ -213,7 +213,10 @@ enum {
   SCATRS_PARAM_REFR_REAL = 1,    /* ParamKind::RefrReal */
   SCATRS_PARAM_REFR_IMAG = 2,    /* ParamKind::RefrImag */
   SCATRS_PARAM_WEIGHT = 3,       /* ParamKind::Weight: a component's (mode -1) or a mode's */
-  SCATRS_PARAM_ASPECT_RATIO = 4  /* ParamKind::AspectRatio: a spheroid component's */
+  SCATRS_PARAM_ASPECT_RATIO = 4,     /* ParamKind::AspectRatio: a spheroid component's */
+  SCATRS_PARAM_LAYER_REFR_REAL = 5,  /* ParamKind::LayerRefrReal(index): layer index's Re m */
+  SCATRS_PARAM_LAYER_REFR_IMAG = 6,  /* ParamKind::LayerRefrImag(index) */
+  SCATRS_PARAM_RADIUS_FRACTION = 7   /* ParamKind::RadiusFraction(index), index < n_layers - 1 */
 };
 typedef struct scatrs_param {
   int32_t component;

@@ -662,7 +662,7 @@ def _component(dists, mode_w, weight, m, n_wl: int, keep: list) -> Component:
 PARAM_DTYPE = np.dtype([("component", np.int32), ("mode", np.int32), ("kind", np.int32),
                         ("index", np.int32)])
 PARAM_DISTRIBUTION, PARAM_REFR_REAL, PARAM_REFR_IMAG, PARAM_WEIGHT = 0, 1, 2, 3
-PARAM_ASPECT_RATIO = 4
+PARAM_ASPECT_RATIO, PARAM_LAYER_REFR_REAL, PARAM_LAYER_REFR_IMAG, PARAM_RADIUS_FRACTION = 4, 5, 6, 7
 
 
 def ensemble_mixture_d(components, wavelengths, params, mu=None, greek_order: int = -1,

@@ -98,8 +98,8 @@ def ensemble_parameters(items, mixture: bool) -> list[str]:
 
 def _parameter_records(items, mixture: bool) -> list:
     """The (component, mode, kind, index) of every name of ensemble_parameters, in its order
-    (scatrs/src/ensemble/mod.rs:254-337); kind None marks a parameter of a layered sphere,
-    which this path does not differentiate."""
+    (scatrs/src/ensemble/mod.rs:254-337); a layered sphere's are LayerRefrReal(l),
+    LayerRefrImag(l) per layer, then RadiusFraction(l) (the record's index the layer)."""
     out = []
     for ci, (spec, particle, _w) in enumerate(items):
         kind = spec[0]
@@ -117,7 +117,11 @@ def _parameter_records(items, mixture: bool) -> list:
                     (ci, -1, _native.PARAM_ASPECT_RATIO, 0)]
         else:
             layers = np.asarray(particle[2]).shape[0]
-            out += [(ci, -1, None, k) for k in range(3 * layers - 1)]
+            for layer in range(layers):
+                out += [(ci, -1, _native.PARAM_LAYER_REFR_REAL, layer),
+                        (ci, -1, _native.PARAM_LAYER_REFR_IMAG, layer)]
+            out += [(ci, -1, _native.PARAM_RADIUS_FRACTION, layer)
+                    for layer in range(layers - 1)]
         if mixture:
             out.append((ci, -1, _native.PARAM_WEIGHT, 0))
     return out
@@ -315,8 +319,9 @@ def _compute_with_derivatives(items, wavelengths, mixture, greek, all_orders, mu
                               derivatives, rtol, max_panels, allow_unvalidated,
                               refine_backscatter) -> dict:
     """ensemble_compute with derivatives (scatrs-py/src/ensemble.rs:318-349): the parameters by
-    their index in ensemble_parameters, every one once; spheres, through
-    scatrs_ensemble_mixture_d (compute_mixture with EnsembleOptions::derivatives)."""
+    their index in ensemble_parameters, every one once, through scatrs_ensemble_mixture_d
+    (compute_mixture with EnsembleOptions::derivatives): spheres, or one spheroid or layered
+    sphere component."""
     names = ensemble_parameters(items, mixture)
     records = _parameter_records(items, mixture)
     chosen = []
@@ -326,20 +331,15 @@ def _compute_with_derivatives(items, wavelengths, mixture, greek, all_orders, mu
         if i in chosen:
             raise InvalidInputError(f"parameter {names[i]} requested twice")
         chosen.append(i)
-    for i in chosen:
-        if records[i][2] is None:
-            raise InvalidInputError(
-                f"the derivative along {names[i]} is not on the adaptive GPU path: a layered "
-                "sphere's derivatives are on the fixed grid (ensemble_compute_fixed)")
     wl = np.ascontiguousarray(wavelengths, dtype=np.float64).reshape(-1)
     mu = np.zeros(0) if mu is None else np.ascontiguousarray(mu, dtype=np.float64).reshape(-1)
     L = _greek_order(greek, all_orders)
     comps = []
     for spec, particle, weight in items:
         dists, mode_w = _modes(spec)
-        # A spheroid (one component of one distribution) goes as its checked spec.
+        # A spheroid or a layered sphere (one component) goes as its checked spec.
         part = (_particle(particle, wl.size) if isinstance(particle, tuple) and particle
-                and particle[0] == "spheroid" else _sphere_m(particle, wl.size))
+                and particle[0] in ("spheroid", "layered") else _sphere_m(particle, wl.size))
         comps.append((dists, mode_w, float(weight), part))
     params = np.array([records[i] for i in chosen], dtype=_native.PARAM_DTYPE)
     out = _native.ensemble_mixture_d(comps, wl, params, mu, L, bool(normalized), float(rtol),

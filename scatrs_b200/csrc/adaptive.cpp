@@ -568,7 +568,8 @@ void pass1(std::vector<Job>& jobs, const std::vector<Part>& parts, const double*
             first_fail[ji] = (int)pi;
             jobs[ji].status = res[15 * k + i].status;
             jobs[ji].msg = at(wavelengths[jobs[ji].wl], qs[15 * k + i].r) +
-                           (jobs[ji].status == 3
+                           (res[15 * k + i].msg ? std::string(res[15 * k + i].msg)
+                            : jobs[ji].status == 3
                                 ? "the size parameter and refractive index are outside the "
                                   "validated domain x in [1e-06, 2e4], 0 < Re m <= 10, "
                                   "0 <= Im m <= 10, |m| >= 0.1"
@@ -593,11 +594,11 @@ void pass1(std::vector<Job>& jobs, const std::vector<Part>& parts, const double*
       // The quantities of the group's first part's directions (engine.rs:491-506).
       const Part& first = parts[jobs[ji].parts[0]];
       const int nr = first.n_refined();
-      int qi[kNodeQ];
+      std::vector<int> qi(nr);
       for (int j = 0; j < kPass1; ++j) qi[j] = j;
       {
         int at = kPass1;
-        for (int dir = 0; dir < kMaxDirs; ++dir)
+        for (int dir = 0; dir < (int)first.dirs.size(); ++dir)
           if (first.dirs[dir])
             for (int j = 0; j < kGroup; ++j) qi[at++] = kPass1 + kGroup * dir + j;
       }
@@ -614,8 +615,9 @@ void pass1(std::vector<Job>& jobs, const std::vector<Part>& parts, const double*
           const double r = qs[15 * k + i].r;
           const double base = (nt > 0 ? part.u(r, grad) : part.u(r)) * r;
           const double* q = res[15 * k + i].q;
+          const double* dq = res[15 * k + i].dq;
           for (int j = 0; j < nr; ++j) {
-            const double qj = q[qi[j]];
+            const double qj = dq && qi[j] >= kPass1 ? dq[qi[j] - kPass1] : q[qi[j]];
             sk[j] += nd[i].wk * base * qj;
             g[j] += nd[i].wg * base * qj;
             sabsv[j] += nd[i].wk * std::fabs(base * qj);

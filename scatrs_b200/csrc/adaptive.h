@@ -47,12 +47,20 @@ struct Part {
   // of their result columns) and the requested derivatives along Re m, Im m and (a spheroid)
   // the aspect ratio.
   std::vector<int> grads;
-  bool dirs[kMaxDirs] = {false, false, false};
-  bool dir_derivatives() const { return dirs[0] || dirs[1] || dirs[2]; }
+  // A layered sphere has 3 L - 1 directions (each layer's Re m and Im m, then each radius
+  // fraction, particle.rs:119-145).
+  std::vector<char> dirs = std::vector<char>(kMaxDirs, 0);
+  bool dir_derivatives() const {
+    for (char d : dirs)
+      if (d) return true;
+    return false;
+  }
   // The pass-1 quantities (engine.rs:464-471): the base ones, then kGroup per requested
   // direction.
   int n_refined() const {
-    return kPass1 + kGroup * ((int)dirs[0] + (int)dirs[1] + (int)dirs[2]);
+    int k = 0;
+    for (char d : dirs) k += d ? 1 : 0;
+    return kPass1 + kGroup * k;
   }
   double reference = 1.0, log_width = 0.0;  // distribution.rs:292-336
   Support support = UNBOUNDED;
@@ -87,8 +95,12 @@ struct Query {
 };
 struct NodeResult {
   double q[kNodeQ];  // the kPass1 quantities, then kGroup derivatives along each direction
+  // If set, the kGroup derivatives of every direction of the particle, in order, in place of
+  // q's (a layered sphere's, more than kMaxDirs); owned by the evaluator until its next call.
+  const double* dq = nullptr;
   int64_t n;
   int status;
+  const char* msg = nullptr;  // with a status: the reason, if not the node's domain
 };
 using Evaluate = std::function<void(const std::vector<Query>&, std::vector<NodeResult>&)>;
 

@@ -1405,11 +1405,13 @@ struct AdPart {
   const double* table = nullptr;  // a tabulated distribution's table
   int64_t table_len = 0;
   // Derivatives (engine.rs:95-115, 153-176): the requested distribution parameters (indices
-  // into the density's gradient) and their result columns, the columns along Re m and Im m
-  // (-1: not requested), and the part's component, mode (-1: none) and weights w (the
-  // component's), v (the mode's) and v_total (the component's mode weights' sum).
+  // into the density's gradient) and their result columns, the columns along the particle's
+  // directions (-1: not requested; a sphere's Re m and Im m, a layered sphere's Re m_l and
+  // Im m_l per layer and then each radius fraction), and the part's component, mode (-1:
+  // none) and weights w (the component's), v (the mode's) and v_total (the component's mode
+  // weights' sum).
   std::vector<int> grads, theta_cols;
-  int dir_cols[2] = {-1, -1};
+  std::vector<int> dir_cols = std::vector<int>(2, -1);
   int component = 0, mode = -1;
   double w = 1.0, v = 1.0, v_total = 1.0;
 };
@@ -1518,7 +1520,9 @@ void mix_derivatives(const std::vector<AdPart>& in, const std::vector<adaptive::
                      int n_theta, const std::vector<double>& hav, const AdDerivs& dd,
                      const AdOutputs& res, const double* wavelengths,
                      const std::vector<double>& hav_x) {
-  const int B = 3 + n_theta;
+  // Blocks per part: the values, n_theta parameters, then every direction of the particle.
+  const int n_dirs = in.empty() ? 2 : (int)in[0].dir_cols.size();
+  const int B = 1 + n_theta + n_dirs;
   const int64_t glen = greek_order >= 0 ? greek_order + 1 : 0;
   const int64_t row = 8 + 4 * n_mu + 6 * glen, stride = 2 * B * row;
   const size_t P = (size_t)dd.n;
@@ -1526,8 +1530,8 @@ void mix_derivatives(const std::vector<AdPart>& in, const std::vector<adaptive::
   // The result column of block b of part p (-1: none).
   auto column = [&](const AdPart& a, int b) {
     if (b >= 1 && b <= n_theta) return b - 1 < (int)a.theta_cols.size() ? a.theta_cols[b - 1] : -1;
-    if (b == n_theta + 1) return a.dir_cols[0];
-    if (b == n_theta + 2) return a.dir_cols[1];
+    const int k = b - n_theta - 1;
+    if (k >= 0 && k < (int)a.dir_cols.size()) return a.dir_cols[k];
     return -1;
   };
   std::vector<double> v(row), e(row), d(P * row), de(P * row);
@@ -1729,8 +1733,8 @@ void adaptive_call_order(const std::vector<AdPart>& in, int n_out, bool batch,
     } catch (const adaptive::Error& e) {
       throw Failure{e.status, p.who + e.msg};
     }
-    parts.back().dirs[0] = p.dir_cols[0] >= 0;
-    parts.back().dirs[1] = p.dir_cols[1] >= 0;
+    parts.back().dirs.assign(p.dir_cols.size(), 0);
+    for (size_t k = 0; k < p.dir_cols.size(); ++k) parts.back().dirs[k] = p.dir_cols[k] >= 0;
     n_theta = std::max(n_theta, (int)p.grads.size());
     any_dirs = any_dirs || parts.back().dir_derivatives();
     if (!p.grads.empty() && parts.back().support == adaptive::POINT) radius_x = true;
@@ -1745,9 +1749,27 @@ void adaptive_call_order(const std::vector<AdPart>& in, int n_out, bool batch,
   if (L > kMaxLayersAbi) throw Failure{SCATRS_INVALID_INPUT, "the GPU path takes 1 to 16 layers"};
   if (L > 1 && (!layers->fractions || !layers->m))
     throw Failure{SCATRS_INVALID_INPUT, "layers must give fractions and m"};
-  if (L > 1 && deriv)
+  if (L > 1 && radius_x)
     throw Failure{SCATRS_INVALID_INPUT,
-                  "derivatives of layered spheres on the adaptive path are not on the GPU path"};
+                  "the radius derivative of a single layered sphere is not on the GPU path"};
+  // A layered sphere's direction groups with a requested direction (any part's): group l < L is
+  // layer l's index (directions 2 l, 2 l + 1), group L + f the radius fraction f (direction
+  // 2 L + f).
+  std::vector<int> groups;
+  const int n_dirs_all = L > 1 ? 3 * L - 1 : 2;
+  if (L > 1 && any_dirs)
+    for (int g = 0; g < 2 * L - 1; ++g) {
+      bool want = false;
+      for (const AdPart& p : in) {
+        if ((int)p.dir_cols.size() != n_dirs_all)
+          throw Failure{SCATRS_INVALID_INPUT, "a layered part's directions must number 3 L - 1"};
+        if (g < L)
+          want = want || p.dir_cols[2 * g] >= 0 || p.dir_cols[2 * g + 1] >= 0;
+        else
+          want = want || p.dir_cols[2 * L + (g - L)] >= 0;
+      }
+      if (want) groups.push_back(g);
+    }
   std::vector<double> m_unit(2 * n_units, 0.0);
   if (L == 1)
     for (int64_t u = 0; u < n_units; ++u) {
@@ -1785,11 +1807,19 @@ void adaptive_call_order(const std::vector<AdPart>& in, int n_out, bool batch,
     for (int64_t u = 0; u < n_units; ++u) wlu[u] = wavelengths[u % n_wl];
     SB_CUDA(cudaMemcpyAsync(wl_unit_d, wlu.data(), n_units * 8, cudaMemcpyHostToDevice, s));
   }
+  // A layered sphere's derivatives: each node's kGroup quantities per direction (all
+  // 3 L - 1), filled by one pass per requested group, read by pass 1 through NodeResult::dq.
+  const bool layered_dirs = L > 1 && any_dirs;
+  std::vector<double> dq_store;
+  const int64_t row_cap =
+      layered_dirs ? std::max<int64_t>(int64_t(1) << 20, kRows / (2 * (2 * L - 1))) : kRows;
   auto eval = [&](const std::vector<adaptive::Query>& qs, std::vector<adaptive::NodeResult>& out) {
     size_t k0 = 0;
     std::vector<double> r;
     std::vector<int> wi;
     std::vector<int64_t> off;
+    const int64_t dstride = (int64_t)n_dirs_all * adaptive::kGroup;
+    if (layered_dirs) dq_store.assign(qs.size() * (size_t)dstride, 0.0);
     while (k0 < qs.size()) {
       r.clear();
       wi.clear();
@@ -1801,7 +1831,7 @@ void adaptive_call_order(const std::vector<AdPart>& in, int n_out, bool batch,
         const int64_t cap = (std::isfinite(x) && x > 0.0 && x <= 1e6)
                                 ? (int64_t)std::ceil(x + 6.0 * std::cbrt(x) + 3.0) + 4
                                 : 0;
-        if (k1 > k0 && off.back() + cap > kRows) break;
+        if (k1 > k0 && off.back() + cap > row_cap) break;
         r.push_back(qs[k1].r);
         wi.push_back(qs[k1].wl);
         off.push_back(off.back() + cap);
@@ -1814,8 +1844,10 @@ void adaptive_call_order(const std::vector<AdPart>& in, int n_out, bool batch,
       a.scratch = c.p1_scratch.as<int64_t>(n + 1);
       a.uz = c.p1_uz.as<double2>((size_t)rows * (2 * L - 1));
       a.ux = c.p1_ux.as<double>(rows);
-      const int nq = any_dirs ? adaptive::kSphereQ : adaptive::kPass1;
-      a.deriv = any_dirs ? 1 : 0;
+      // A sphere's directions come with its values; a layered sphere's in the group passes.
+      const bool sphere_dirs = any_dirs && L == 1;
+      const int nq = sphere_dirs ? adaptive::kSphereQ : adaptive::kPass1;
+      a.deriv = sphere_dirs ? 1 : 0;
       a.q = c.p1_q.as<double>(nq * n);
       a.n_terms = c.p1_n.as<int64_t>(n);
       a.status = c.p1_status.as<int>(n);
@@ -1845,6 +1877,41 @@ void adaptive_call_order(const std::vector<AdPart>& in, int n_out, bool batch,
         for (int j = 0; j < adaptive::kNodeQ; ++j) x.q[j] = j < nq ? q[nq * k + j] : 0.0;
         x.n = nt[k];
         x.status = st[k];
+        x.dq = layered_dirs ? dq_store.data() + (k0 + k) * dstride : nullptr;
+        x.msg = nullptr;
+      }
+      // A layered sphere's requested direction groups, one pass each (nodes that failed above
+      // fail the same way there and keep zeros).
+      for (int g : groups) {
+        Pass1Args b = a;
+        b.deriv = 1;
+        b.deriv_dir = g;
+        b.uz = c.p1_uz.as<double2>((size_t)rows * 2 * (2 * L - 1));
+        b.q = c.p1_q.as<double>(16 * n);
+        timed_launch(K_NODES, s, [&] { launch_pass1_layered_deriv(b, s); });
+        SB_CUDA(cudaGetLastError());
+        std::vector<double> qd(16 * n);
+        std::vector<int> sd(n);
+        SB_CUDA(cudaMemcpyAsync(qd.data(), b.q, 16 * n * 8, cudaMemcpyDeviceToHost, s));
+        SB_CUDA(cudaMemcpyAsync(sd.data(), b.status, n * 4, cudaMemcpyDeviceToHost, s));
+        SB_CUDA(cudaStreamSynchronize(s));
+        for (int64_t k = 0; k < n; ++k) {
+          adaptive::NodeResult& x = out[k0 + k];
+          if (x.status == 0 && sd[k] != 0) {
+            x.status = sd[k];
+            if (sd[k] == 3)
+              x.msg = "the layered sphere's derivatives are outside their validated domain "
+                      "x_L <= 1000";
+          }
+          double* o = dq_store.data() + (k0 + k) * dstride;
+          if (g < L) {
+            for (int j = 0; j < 2 * adaptive::kGroup; ++j)
+              o[2 * g * adaptive::kGroup + j] = qd[16 * k + 6 + j];
+          } else {
+            for (int j = 0; j < adaptive::kGroup; ++j)
+              o[(2 * L + (g - L)) * adaptive::kGroup + j] = qd[16 * k + 6 + j];
+          }
+        }
       }
       k0 = k1;
     }
@@ -2034,6 +2101,47 @@ void adaptive_call_order(const std::vector<AdPart>& in, int n_out, bool batch,
     li.n_layers = L;
     li.fractions = layers->fractions;
     li.m_dev = ml_d;
+  }
+  if (L > 1 && deriv) {
+    // A layered sphere: the derivative pipeline once per requested direction group (K-a along
+    // the group's direction, engine.rs:1047-1109 with Solved::direction), each pass's values and
+    // parameter blocks alike; the direction blocks gathered into one row per unit of the values,
+    // the n_theta parameters and all 3 L - 1 directions for the mixing.
+    const std::vector<int> passes = groups.empty() ? std::vector<int>{0} : groups;
+    const int n_all = 1 + n_theta + n_dirs_all;
+    const int64_t cstride = 2 * (int64_t)n_all * row;
+    std::vector<double> hav((size_t)n_units * cstride, 0.0), one((size_t)n_units * stride);
+    call.radius = radius;
+    for (size_t pi = 0; pi < passes.size(); ++pi) {
+      const int g = passes[pi];
+      DerivOutput dvg = dvo;
+      dvg.dir = g;
+      run_fixed(c, dummy.data(), n_parts, wl_d, n_wl, m_d, mu, n_mu, &fo, nullptr, nullptr,
+                nullptr, s, &call, li, dvg, ad);
+      check_device_errors(c, s, &call);
+      SB_CUDA(cudaMemcpyAsync(one.data(), avg, one.size() * 8, cudaMemcpyDeviceToHost, s));
+      SB_CUDA(cudaStreamSynchronize(s));
+      auto copy_block = [&](const double* src, double* dst, int from, int to) {
+        std::copy(src + 2 * from * row, src + (2 * from + 2) * row, dst + 2 * to * row);
+      };
+      for (int64_t u = 0; u < n_units; ++u) {
+        const double* src = one.data() + u * stride;
+        double* dst = hav.data() + u * cstride;
+        if (pi == 0)
+          for (int b = 0; b <= n_theta; ++b) copy_block(src, dst, b, b);
+        if (groups.empty()) continue;
+        if (g < L) {
+          copy_block(src, dst, n_theta + 1, 1 + n_theta + 2 * g);
+          copy_block(src, dst, n_theta + 2, 2 + n_theta + 2 * g);
+        } else {
+          copy_block(src, dst, n_theta + 1, 1 + n_theta + 2 * L + (g - L));
+        }
+      }
+    }
+    mix_derivatives(in, parts, n_out, n_wl, n_mu, options->greek_order, options->normalized != 0,
+                    n_theta, hav, *dd, res, wavelengths, {});
+    adaptive_flags(in, jobs, job_of, unit_converged, unit_panels, n_out, n_wl, res);
+    return;
   }
   run_fixed(c, dummy.data(), n_parts, wl_d, n_wl, m_d, mu, n_mu, &fo, nullptr, nullptr, nullptr,
             s, &call, li, dvo, ad);
@@ -4574,11 +4682,17 @@ int scatrs_ensemble_mixture_d(const scatrs_component* components, int64_t n_comp
     const bool spheroid_alone = n_comp == 1 && components && components[0].aspect_ratio > 0.0 &&
                                 components[0].n_layers <= 1 && components[0].n_modes == 1 &&
                                 !components[0].mode_weights;
-    if (heterogeneous(components, n_comp) && !(n_params > 0 && spheroid_alone)) {
+    // One layered component (plain or multimodal) takes them on the adaptive pipeline with
+    // its layers.
+    const bool layered_alone = n_comp == 1 && components && components[0].n_layers > 1 &&
+                               components[0].aspect_ratio == 0.0;
+    if (heterogeneous(components, n_comp) &&
+        !(n_params > 0 && (spheroid_alone || layered_alone))) {
       if (n_params > 0)
         throw Failure{SCATRS_INVALID_INPUT,
-                      "derivatives of layered spheres, and of spheroids beside other components "
-                      "or in multimodal distributions, are not on the adaptive GPU path"};
+                      "derivatives of layered spheres or spheroids beside other components, or "
+                      "of spheroids in multimodal distributions, are not on the adaptive GPU "
+                      "path"};
       AdOutputs out{values, errors, phase, phase_err, greek, greek_err, converged, panels};
       mixture_hetero(components, n_comp, wavelengths, n_wl, mu, n_mu, options, out);
       return;
@@ -4612,6 +4726,11 @@ int scatrs_ensemble_mixture_d(const scatrs_component* components, int64_t n_comp
         case SCATRS_PARAM_REFR_IMAG: out += "m_imag"; break;
         case SCATRS_PARAM_WEIGHT: out += "weight"; break;
         case SCATRS_PARAM_ASPECT_RATIO: out += "aspect_ratio"; break;
+        case SCATRS_PARAM_LAYER_REFR_REAL: out += "layer" + std::to_string(q.index) + ".m_real"; break;
+        case SCATRS_PARAM_LAYER_REFR_IMAG: out += "layer" + std::to_string(q.index) + ".m_imag"; break;
+        case SCATRS_PARAM_RADIUS_FRACTION:
+          out += "layer" + std::to_string(q.index) + ".radius_fraction";
+          break;
         default: out += "kind" + std::to_string(q.kind);
       }
       return out;
@@ -4635,8 +4754,16 @@ int scatrs_ensemble_mixture_d(const scatrs_component* components, int64_t n_comp
             break;
           }
           case SCATRS_PARAM_REFR_REAL:
-          case SCATRS_PARAM_REFR_IMAG: allowed = q.mode == -1; break;
+          case SCATRS_PARAM_REFR_IMAG: allowed = q.mode == -1 && cp.n_layers <= 1; break;
           case SCATRS_PARAM_ASPECT_RATIO: allowed = q.mode == -1 && cp.aspect_ratio > 0.0; break;
+          case SCATRS_PARAM_LAYER_REFR_REAL:
+          case SCATRS_PARAM_LAYER_REFR_IMAG:
+            allowed = q.mode == -1 && cp.n_layers > 1 && q.index >= 0 && q.index < cp.n_layers;
+            break;
+          case SCATRS_PARAM_RADIUS_FRACTION:
+            allowed = q.mode == -1 && cp.n_layers > 1 && q.index >= 0 &&
+                      q.index < cp.n_layers - 1;
+            break;
           case SCATRS_PARAM_WEIGHT:
             allowed = q.mode == -1 || (multi && q.mode >= 0 && q.mode < cp.n_modes);
             break;
@@ -4677,6 +4804,50 @@ int scatrs_ensemble_mixture_d(const scatrs_component* components, int64_t n_comp
       const scatrs_component& cp = components[0];
       spheroid_call_d(SphParticle{cp.modes, 1, cp.aspect_ratio, cp.m}, req, wavelengths, n_wl, mu,
                       n_mu, options, out, dd);
+      return;
+    }
+    if (layered_alone) {
+      // Each mode a part with the component's layers; the directions each layer's Re m and
+      // Im m, then each radius fraction (particle.rs:119-145).
+      const scatrs_component& cp = components[0];
+      const int L = cp.n_layers;
+      if (!cp.fractions || !cp.m)
+        throw Failure{SCATRS_INVALID_INPUT, "component 0: a layered sphere needs fractions and m"};
+      const int64_t np = (int64_t)parts.size();
+      std::vector<double> fr((size_t)np * (L - 1)), ml((size_t)np * 2 * L * n_wl);
+      for (int64_t p = 0; p < np; ++p) {
+        std::copy(cp.fractions, cp.fractions + (L - 1), fr.begin() + p * (L - 1));
+        std::copy(cp.m, cp.m + 2 * L * n_wl, ml.begin() + p * 2 * L * n_wl);
+      }
+      for (AdPart& a : parts) {
+        a.dir_cols.assign(3 * L - 1, -1);
+        for (int64_t k = 0; k < n_params; ++k) {
+          const scatrs_param& q = params[k];
+          if (q.kind == SCATRS_PARAM_DISTRIBUTION && q.mode == a.mode) {
+            a.grads.push_back(q.index);
+            a.theta_cols.push_back((int)k);
+          } else if (q.kind == SCATRS_PARAM_LAYER_REFR_REAL) {
+            a.dir_cols[2 * q.index] = (int)k;
+          } else if (q.kind == SCATRS_PARAM_LAYER_REFR_IMAG) {
+            a.dir_cols[2 * q.index + 1] = (int)k;
+          } else if (q.kind == SCATRS_PARAM_RADIUS_FRACTION) {
+            a.dir_cols[2 * L + q.index] = (int)k;
+          }
+        }
+      }
+      scatrs_layers lay{L, 0, fr.data(), ml.data()};
+      AdOutputs out{values, errors, phase, phase_err, greek, greek_err, converged, panels};
+      AdDerivs dd;
+      dd.params = params;
+      dd.n = n_params;
+      dd.d_values = d_values;
+      dd.d_errors = d_errors;
+      dd.d_phase = d_phase;
+      dd.d_phase_err = d_phase_err;
+      dd.d_greek = d_greek;
+      dd.d_greek_err = d_greek_err;
+      if (!d_values) throw Failure{SCATRS_INVALID_INPUT, "d_values is required with parameters"};
+      adaptive_call(parts, 1, false, wavelengths, n_wl, mu, n_mu, options, out, &lay, &dd);
       return;
     }
     // engine.rs:153-176: each part's parameters and their columns.

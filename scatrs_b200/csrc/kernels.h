@@ -355,10 +355,16 @@ struct Pass1Args {
   const double2* m_layers;
   // Homogeneous spheres with deriv != 0: q is [n][16], the 6 quantities followed by the
   // derivatives of pi r^2 (Q_ext, Q_sca, Q_sca g, Q_back, Q_abs) along Re m, then along Im m
-  // (engine.rs:447-461).
+  // (engine.rs:447-461). Layered spheres with deriv != 0 (launch_pass1_layered_deriv): the
+  // same [n][16] along direction deriv_dir (0..L-1: layer l's index, the complex derivative
+  // and i times it; L..2L-2: the radius fraction f_{dir-L}, x_L d/dx_l, its second group
+  // unused), and the scratch rows hold 2 (2 n_layers - 1) arrays (each ratio array's
+  // derivative beside it).
   int deriv;
+  int deriv_dir;
 };
 
+void launch_pass1_layered_deriv(const Pass1Args& a, cudaStream_t s);
 void launch_plan_chunks(const PlanArgs& a, cudaStream_t s);
 void launch_mie_fixed(const MieFixedArgs& a, cudaStream_t s);
 void launch_mie_nodes(const MieNodesArgs& a, cudaStream_t s);

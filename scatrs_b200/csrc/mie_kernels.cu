@@ -322,15 +322,16 @@ __device__ __forceinline__ void layered_deriv_chunk(const MieFixedArgs& a) {
   s.stride = 32;
   const int P = a.n_theta;
   const int B = 3 + P;
-  double q[6][8];
-#pragma unroll
-  for (int b = 0; b < 6; ++b)
-#pragma unroll
-    for (int k = 0; k < 8; ++k) q[b][k] = 0.0;
+  // The node's quantities, their derivatives along the direction and along i times it, and
+  // the blocks' weights (adaptive panels: and their error weights, as mie_chunk_deriv's).
+  double qv[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  double qd[2][8] = {{0, 0, 0, 0, 0, 0, 0, 0}, {0, 0, 0, 0, 0, 0, 0, 0}};
+  double wb[4] = {0, 0, 0, 0}, wbd[4] = {0, 0, 0, 0};
+  const bool adaptive = a.wdiff != nullptr;
   int64_t n = 0;
-  if (j < a.n_nodes) {
-    const double r = a.radius[d * a.n_nodes + j];
-    const double w = a.weight[d * a.n_nodes + j];
+  const int64_t node = (a.per_unit ? unit : d) * a.n_nodes + j;
+  if (j < a.n_nodes && a.radius[node] > 0.0) {
+    const double r = a.radius[node];
     const double x = 2.0 * kPi * r / a.wl[i];
     n = default_n_max(x);
     double xs[kCap];
@@ -382,16 +383,12 @@ __device__ __forceinline__ void layered_deriv_chunk(const MieFixedArgs& a) {
     } else {
       const Eff e = efficiencies_from(x, asum, vs);
       const double area = kPi * r * r;
-      const double qv[8] = {1.0,           area * e.q_ext, area * e.q_sca, area * e.q_sca * e.g,
+      const double q0[8] = {1.0,           area * e.q_ext, area * e.q_sca, area * e.q_sca * e.g,
                             area * e.q_abs, area * e.q_back, r * r,         r * r * r};
-      for (int k = 0; k < 8; ++k) q[0][k] = w * qv[k];
-      for (int p = 0; p < P; ++p) {
-        const double wt = a.wtheta[(d * a.n_nodes + j) * 3 + p];
-        for (int k = 0; k < 8; ++k) q[1 + p][k] = wt * qv[k];
-      }
+      for (int k = 0; k < 8; ++k) qv[k] = q0[k];
       for (int p = 0; p < 2; ++p) {
         const Eff de = efficiency_derivs(x, vs, e, ds, p, abs_d[p]);
-        const double qd[8] = {0.0,
+        const double q1[8] = {0.0,
                               area * de.q_ext,
                               area * de.q_sca,
                               area * (de.q_sca * e.g + e.q_sca * de.g),
@@ -399,7 +396,13 @@ __device__ __forceinline__ void layered_deriv_chunk(const MieFixedArgs& a) {
                               area * de.q_back,
                               0.0,
                               0.0};
-        for (int k = 0; k < 8; ++k) q[1 + P + p][k] = w * qd[k];
+        for (int k = 0; k < 8; ++k) qd[p][k] = q1[k];
+      }
+      wb[0] = a.weight[node];
+      for (int p = 0; p < P; ++p) wb[1 + p] = a.wtheta[node * 3 + p];
+      if (adaptive) {
+        wbd[0] = a.wdiff[node];
+        for (int p = 0; p < P; ++p) wbd[1 + p] = a.wthdiff[node * 3 + p];
       }
     }
   }
@@ -407,12 +410,24 @@ __device__ __forceinline__ void layered_deriv_chunk(const MieFixedArgs& a) {
     *reinterpret_cast<double4*>(X + (k - 1) * 128) = make_double4(0.0, 0.0, 0.0, 0.0);
     *reinterpret_cast<double4*>(X + (k - 1) * 128 + 64) = make_double4(0.0, 0.0, 0.0, 0.0);
   }
-  for (int b = 0; b < 6; ++b) {
-    if (b >= B) break;
+  // The chunk's sums per block (values and each parameter on the values' quantities, the
+  // direction's blocks on the derivatives with the values' weight) in a fixed tree order;
+  // adaptive: then |Kronrod - Gauss| of each of the chunk's two panels, added.
+  const int stride = adaptive ? 2 * B : B;
+  for (int b = 0; b < B; ++b) {
+    const int wi = b <= P ? b : 0;
     for (int k = 0; k < 8; ++k) {
-      double v = q[b][k];
+      const double qk = b <= P ? qv[k] : qd[b - 1 - P][k];
+      double v = wb[wi] * qk;
       for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-      if (lane == 0) a.chunk_sums[((int64_t)chunk * B + b) * 8 + k] = v;
+      if (lane == 0) a.chunk_sums[((int64_t)chunk * stride + b) * 8 + k] = v;
+      if (adaptive) {
+        double e = wbd[wi] * qk;
+        for (int off = 8; off > 0; off >>= 1) e += __shfl_xor_sync(0xffffffffu, e, off);
+        const double other = __shfl_sync(0xffffffffu, e, 16);
+        if (lane == 0)
+          a.chunk_sums[((int64_t)chunk * stride + B + b) * 8 + k] = fabs(e) + fabs(other);
+      }
     }
   }
 }
@@ -564,6 +579,97 @@ __global__ void __launch_bounds__(128) pass1_kernel(Pass1Args a) {
   q[3] = area * e.q_sca * e.g;
   q[4] = area * e.q_back;
   q[5] = area * e.q_abs;
+}
+
+// Pass 1 of a layered sphere's derivatives along one direction (engine.rs:447-461 with
+// Solved::direction, particle.rs:206-219): one thread per node, the layered recursion in
+// forward mode (layered_deriv.cuh) along a.deriv_dir; q[t] gets the node's 6 quantities and
+// the derivatives of pi r^2 (Q_ext, Q_sca, Q_sca g, Q_back, Q_abs) along the direction, then
+// along i times it (meaningful for an index direction only).
+__global__ void __launch_bounds__(128) pass1_layered_deriv_kernel(Pass1Args a) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.n) return;
+  const double r = a.radius[t];
+  const int wi = a.wl_index[t];
+  const double x = 2.0 * kPi * r / a.wl[wi];
+  int64_t n = default_n_max(x);
+  const int L = a.n_layers;
+  double xs[kMaxLayers];
+  cplx ms[kMaxLayers];
+  bool lossless = true;
+  const int p = wi / a.n_wl, i = wi % a.n_wl;
+  for (int l = 0; l < L; ++l) {
+    xs[l] = l < L - 1 ? a.fractions[p * (L - 1) + l] * x : x;
+    const double2 mv = a.m_layers[(p * L + l) * a.n_wl + i];
+    ms[l] = mk(mv.x, mv.y);
+    lossless = lossless && mv.y == 0.0;
+  }
+  int st = check_layered(xs, ms, L, n, a.allow_unvalidated != 0);
+  // The derivatives are validated up to x_L = 1000 (layered/domain.rs:39-70).
+  if (st == 0 && a.allow_unvalidated == 0 && xs[L - 1] > 1e3) st = 3;
+  const int64_t off = a.scratch[t], cap = a.scratch[t + 1] - off;
+  if (st == 0 && n + 2 > cap) st = 1;
+  a.status[t] = st;
+  a.n_terms[t] = st == 0 ? n : 0;
+  double* q = a.q + 16 * t;
+  if (st != 0) {
+    for (int k = 0; k < 16; ++k) q[k] = 0.0;
+    return;
+  }
+  const int n_arr = 2 * L - 1, dir = a.deriv_dir;
+  Scratch s;
+  s.uz = a.uz + off * (2 * n_arr);
+  s.ux = a.ux + off;
+  s.stride = 1;
+  lder::DR xd[kMaxLayers];
+  lder::DC md[kMaxLayers];
+  for (int l = 0; l < L; ++l) {
+    xd[l] = lder::DR{xs[l], dir >= L && l == dir - L ? x : 0.0};
+    md[l] = lder::DC{ms[l], rl(dir == l ? 1.0 : 0.0)};
+  }
+  mie_prepare(x, ms[L - 1], n, s);  // u_k(x); array 0 is redone with its derivatives
+  lder::LayeredD<kMaxLayers> lay;
+  lay.layers = L;
+  lay.x = xd;
+  lay.m = md;
+  lay.arr.arr.base = s.uz;
+  lay.arr.arr.astride = cap;
+  lay.arr.arr.stride = 1;
+  lay.arr.n_val = n_arr;
+  lay.prepare(n, lder::DR{x, 0.0});
+  ValueSums vs;
+  DerivSums ds;
+  double abs_d[2];
+  double asum = lder::layered_finish_d(
+      x, md[L - 1], n, s, vs,
+      [&](int64_t k, cplx an, cplx bn, cplx dan, cplx dbn) { ds.add(k, an, bn, dan, dbn); }, lay,
+      abs_d);
+  ds.close(n);
+  // A lossless particle absorbs nothing (layered/kernel.rs:455-464); its derivatives stand.
+  if (lossless) asum = 0.0;
+  const Eff e = efficiencies_from(x, asum, vs);
+  const double area = kPi * r * r;
+  q[0] = 1.0;
+  q[1] = area * e.q_ext;
+  q[2] = area * e.q_sca;
+  q[3] = area * e.q_sca * e.g;
+  q[4] = area * e.q_back;
+  q[5] = area * e.q_abs;
+  for (int c = 0; c < 2; ++c) {
+    const Eff d = efficiency_derivs(x, vs, e, ds, c, abs_d[c]);
+    double* o = q + 6 + 5 * c;
+    o[0] = area * d.q_ext;
+    o[1] = area * d.q_sca;
+    o[2] = area * (d.q_sca * e.g + e.q_sca * d.g);
+    o[3] = area * d.q_back;
+    o[4] = area * d.q_abs;
+  }
+}
+
+void launch_pass1_layered_deriv(const Pass1Args& a, cudaStream_t s) {
+  const int threads = 128;
+  const int64_t blocks = (a.n + threads - 1) / threads;
+  if (blocks > 0) pass1_layered_deriv_kernel<<<(unsigned)blocks, threads, 0, s>>>(a);
 }
 
 void launch_pass1(const Pass1Args& a, cudaStream_t s) {

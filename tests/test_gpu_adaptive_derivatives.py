@@ -132,10 +132,12 @@ def test_the_reference_call(gpu):
     with pytest.raises(InvalidInputError, match="width requested twice"):
         _scatrs.ensemble_compute(items, wl, False, None, False, None, True, [1, 1], 1e-6, 4096,
                                  False, False)
+    # A layered sphere's directions (its checks against differences are in
+    # test_gpu_adaptive_layered_derivatives.py).
     layered = [(("lognormal", 0.2, 1.5), ("layered", [0.5], np.stack([m, m])), 1.0)]
-    with pytest.raises(InvalidInputError, match="adaptive GPU path"):
-        _scatrs.ensemble_compute(layered, wl, False, None, False, None, True, [2], 1e-6, 4096,
-                                 False, False)
+    lay = _scatrs.ensemble_compute(layered, wl, False, None, False, None, True, [2], 1e-6, 4096,
+                                   False, False)
+    assert lay["d"].shape == (1, 11, wl.size) and np.all(np.isfinite(lay["d"]))
     mono = _scatrs.ensemble_compute([(("monodisperse", 0.3), ("sphere", m), 1.0)], wl, False,
                                     None, False, None, True, [0], 1e-6, 4096, False, False)
     ref = _native.ensemble_mixture_d([(_dist(5, 0.3), None, 1.0, m)], wl,
