@@ -235,7 +235,10 @@ typedef struct scatrs_param {
  * is multimodal when its mode_weights are given. Spheres; or one spheroid component of one
  * distribution, along its distribution's parameters, Re m, Im m and the aspect ratio
  * (SCATRS_PARAM_ASPECT_RATIO), each node's derivatives those of its solution at its converged N
- * and n_theta (engine.rs:379-471, 1281-1340 direct path). A single sphere radius's radius is
+ * and n_theta (engine.rs:379-471, 1281-1340 direct path); or one layered component, along its
+ * distribution's parameters, each layer's Re m and Im m and each radius fraction
+ * (SCATRS_PARAM_LAYER_REFR_REAL/_IMAG, SCATRS_PARAM_RADIUS_FRACTION; validated up to
+ * x_L = 1000, layered/domain.rs:39-70). A single sphere radius's radius is
  * exact (engine.rs:1158-1170), with zero error estimates; a single spheroid's follows
  * monodisperse_direct (engine.rs:1896-1961). d_values, d_errors (P, 11, n_wl); d_phase, d_phase_err (P, 6, n_wl, n_mu); d_greek,
  * d_greek_err (P, 6, n_wl, L + 1), P = n_params, in the order of `params`. Invalid or
