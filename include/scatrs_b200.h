@@ -192,7 +192,8 @@ typedef struct scatrs_component {
  * projected Greek coefficients, the spheroids' direct Greek segment (to the largest 2 N of the
  * mixture's spheroids at each wavelength), the depolarization ratio from the spheroids, and the
  * phase matrix from the spheres' tables plus the spheroids' averaged expansion. Such mixtures
- * take no derivatives; with SCATRS_GREEK_ALL each wavelength's order is 2 N_max over every part.
+ * take their derivatives through scatrs_ensemble_mixture_d; with SCATRS_GREEK_ALL each
+ * wavelength's order is 2 N_max over every part.
  */
 int scatrs_ensemble_mixture(const scatrs_component* components, int64_t n_comp,
                             const double* wavelengths, int64_t n_wl, const double* mu,
@@ -238,7 +239,9 @@ typedef struct scatrs_param {
  * and n_theta (engine.rs:379-471, 1281-1340 direct path); or one layered component, along its
  * distribution's parameters, each layer's Re m and Im m and each radius fraction
  * (SCATRS_PARAM_LAYER_REFR_REAL/_IMAG, SCATRS_PARAM_RADIUS_FRACTION; validated up to
- * x_L = 1000, layered/domain.rs:39-70). A single sphere radius's radius is
+ * x_L = 1000, layered/domain.rs:39-70); or a mixture of different particles along any of
+ * its components' parameters and weights (each part on its own engine, mixed and assembled on
+ * the host; not with SCATRS_GREEK_ALL). A single sphere radius's radius is
  * exact (engine.rs:1158-1170), with zero error estimates; a single spheroid's follows
  * monodisperse_direct (engine.rs:1896-1961). d_values, d_errors (P, 11, n_wl); d_phase, d_phase_err (P, 6, n_wl, n_mu); d_greek,
  * d_greek_err (P, 6, n_wl, L + 1), P = n_params, in the order of `params`. Invalid or

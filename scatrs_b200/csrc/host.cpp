@@ -18,6 +18,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <set>
 #include <tuple>
 #include <memory>
 #include <mutex>
@@ -1694,7 +1695,10 @@ struct PartRows {
 
 // With n_max_out, only pass 1 runs (and its errors are reported): n_max_out receives each
 // (part, wavelength) unit's largest number of terms, its group's (engine.rs:1987-2030). With
-// rows_out (no derivatives), the parts' averages go there instead of the outputs.
+// rows_out, the parts' averages go there instead of the outputs: without derivatives as
+// PartRows describes, with them final_adaptive_d_kernel's rows (per block, values then
+// errors, 8 + 4 n_mu + 6 (L + 1) each; blocks the values, n_theta parameters and every
+// direction of the particle).
 void adaptive_call_order(const std::vector<AdPart>& in, int n_out, bool batch,
                          const double* wavelengths, int64_t n_wl, const double* mu, int64_t n_mu,
                          const scatrs_adaptive_options* options, const AdOutputs& res,
@@ -2138,6 +2142,13 @@ void adaptive_call_order(const std::vector<AdPart>& in, int n_out, bool batch,
         }
       }
     }
+    if (rows_out) {  // a mixture's host assembly: the per-block rows by unit
+      rows_out->stride = cstride;
+      rows_out->rows = std::move(hav);
+      rows_out->converged = unit_converged;
+      rows_out->panels = unit_panels;
+      return;
+    }
     mix_derivatives(in, parts, n_out, n_wl, n_mu, options->greek_order, options->normalized != 0,
                     n_theta, hav, *dd, res, wavelengths, {});
     adaptive_flags(in, jobs, job_of, unit_converged, unit_panels, n_out, n_wl, res);
@@ -2151,6 +2162,17 @@ void adaptive_call_order(const std::vector<AdPart>& in, int n_out, bool batch,
     std::vector<double> hav((size_t)n_units * stride), hav_x;
     SB_CUDA(cudaMemcpyAsync(hav.data(), avg, hav.size() * 8, cudaMemcpyDeviceToHost, s));
     SB_CUDA(cudaStreamSynchronize(s));
+    if (rows_out) {  // a mixture's host assembly: the per-block rows by unit
+      if (radius_x)
+        throw Failure{SCATRS_INVALID_INPUT,
+                      "the radius derivative of a single radius in a mixture of different "
+                      "particles is not on the GPU path"};
+      rows_out->stride = stride;
+      rows_out->rows = std::move(hav);
+      rows_out->converged = unit_converged;
+      rows_out->panels = unit_panels;
+      return;
+    }
     if (radius_x) {
       // The single radii's derivatives along x (engine.rs:1158-1170, 1857-1883): the pipeline
       // again with K-a's x direction in place of Re m.
@@ -3429,7 +3451,7 @@ void spheroid_call(const std::vector<SphParticle>& ps, bool batch, const double*
   }
 }
 
-// The adaptive ensemble of one spheroid distribution with derivatives (EnsembleOptions::
+// The adaptive ensemble of spheroid distributions with derivatives (EnsembleOptions::
 // derivatives on the engine's direct path): pass 1 refines the requested distribution
 // parameters' blocks and the derivatives of C_ext, C_sca, C_sca g, C_back and C_abs along each
 // requested direction of the particle (Re m, Im m, the aspect ratio; engine.rs:379-471,
@@ -3440,18 +3462,34 @@ void spheroid_call(const std::vector<SphParticle>& ps, bool batch, const double*
 // derivative 2/r g + (2 pi / lambda) dg/dx); the outputs carry the derivatives through the
 // ratios (assemble, engine.rs:2396-2497; lin.rs). A node's derivatives are those of its
 // discretized solution at its converged N and n_theta (spheroid_fixed_derivs), where the
-// reference carries dual numbers through its T-matrix (tmatrix/mod.rs:231-245).
+// reference carries dual numbers through its T-matrix (tmatrix/mod.rs:231-245). Every
+// distribution of every particle is a part on its own panels; reqs holds each part's request
+// (particle-major). Alone (one part) the call writes the outputs; with rows (a mixture's host
+// assembly) each (part, wavelength) unit's averages go there, the direct order at a wavelength
+// following the largest N of all its spheroids (engine.rs:2073-2086).
 struct SphDerivReq {
   std::vector<int> grads, theta_cols;  // distribution parameters and their result columns
   int dir_cols[3] = {-1, -1, -1};      // result columns along Re m, Im m, the aspect ratio
 };
+// Per (part, wavelength) unit: the 9 scalars and the direct segment (9 + 6 (ld + 1)) with their
+// errors, and per result column (P of them, column-major) their derivatives and errors.
+struct SphRowsD {
+  std::vector<std::vector<double>> av, ae, dv, de;
+  std::vector<int64_t> ld;  // per wavelength, or -1
+  std::vector<char> converged;
+  std::vector<int64_t> panels;
+};
 
-void spheroid_call_d(const SphParticle& sp, const SphDerivReq& req, const double* wavelengths,
-                     int64_t n_wl, const double* mu, int64_t n_mu,
+void spheroid_call_d(const std::vector<SphParticle>& ps, const std::vector<SphDerivReq>& reqs,
+                     const double* wavelengths, int64_t n_wl, const double* mu, int64_t n_mu,
                      const scatrs_adaptive_options* options, const AdOutputs& res,
-                     const AdDerivs& dd) {
+                     const AdDerivs& dd, SphRowsD* rows = nullptr) {
   if (!options) throw Failure{SCATRS_INVALID_INPUT, "options must not be NULL"};
-  if (sp.n_dist != 1) throw Failure{SCATRS_INVALID_INPUT, "one distribution"};
+  int64_t n_parts = 0;
+  for (const SphParticle& q : ps) n_parts += q.n_dist;
+  if ((int64_t)reqs.size() != n_parts)
+    throw Failure{SCATRS_INVALID_INPUT, "one derivative request per distribution"};
+  if (!rows && n_parts != 1) throw Failure{SCATRS_INVALID_INPUT, "one distribution"};
   if (n_wl < 0) throw Failure{SCATRS_INVALID_INPUT, "negative sizes"};
   const bool all_orders = options->greek_order == SCATRS_GREEK_ALL;
   const adaptive::Options o{options->rtol, options->max_panels, options->allow_unvalidated != 0,
@@ -3466,29 +3504,39 @@ void spheroid_call_d(const SphParticle& sp, const SphDerivReq& req, const double
     if (!(std::isfinite(wavelengths[i]) && wavelengths[i] > 0.0))
       throw Failure{SCATRS_INVALID_INPUT,
                     "wavelength " + std::to_string(i) + " must be finite and > 0"};
-  if (!(std::isfinite(sp.eps) && sp.eps > 0.0))
-    throw Failure{SCATRS_INVALID_INPUT, "the aspect ratio must be finite and > 0"};
+  for (const SphParticle& q : ps)
+    if (!(std::isfinite(q.eps) && q.eps > 0.0))
+      throw Failure{SCATRS_INVALID_INPUT, "the aspect ratio must be finite and > 0"};
+  if (rows && all_orders)
+    throw Failure{SCATRS_INVALID_INPUT,
+                  "greek='all' with derivatives of a mixture of different particles is not on "
+                  "the GPU path"};
   scatrs_fixed_options fo{32, all_orders ? -1 : options->greek_order, options->normalized,
                           options->allow_unvalidated};
-  const int64_t n_units = n_wl;
+  const int64_t n_units = n_parts * n_wl;
   check_options(&fo, n_units, n_mu, mu);
   if (n_units == 0) return;
-  const scatrs_distribution& dist = sp.dists[0];
-  adaptive::Part part;
-  try {
-    part = adaptive::make_part(dist.kind, dist.param, o.rtol, dist.table, dist.table_len,
-                               req.grads);
-  } catch (const adaptive::Error& e) {
-    throw Failure{e.status, "distribution 0: " + e.msg};
-  }
-  for (int k = 0; k < 3; ++k) part.dirs[k] = req.dir_cols[k] >= 0;
-  const bool point = part.support == adaptive::POINT;
-  const int nt = (int)req.grads.size();
+  std::vector<adaptive::Part> parts;
+  std::vector<int> particle_of;
+  bool any_dir = false, along_x = false;
+  for (size_t q = 0; q < ps.size(); ++q)
+    for (int64_t d = 0; d < ps[q].n_dist; ++d) {
+      const scatrs_distribution& dist = ps[q].dists[d];
+      const SphDerivReq& rq = reqs[parts.size()];
+      try {
+        parts.push_back(adaptive::make_part(dist.kind, dist.param, o.rtol, dist.table,
+                                            dist.table_len, rq.grads));
+      } catch (const adaptive::Error& e) {
+        throw Failure{e.status, "distribution " + std::to_string(d) + ": " + e.msg};
+      }
+      for (int k = 0; k < 3; ++k) parts.back().dirs[k] = rq.dir_cols[k] >= 0;
+      any_dir = any_dir || parts.back().dir_derivatives();
+      along_x = along_x || (parts.back().support == adaptive::POINT && !rq.grads.empty());
+      particle_of.push_back((int)q);
+    }
   // The directions solved at each node: every one of the particle's when any is asked for
   // (engine.rs:1438-1440), and x for a single radius's radius. spheroid_fixed_derivs orders
   // them x, aspect ratio, Re m, Im m; here the directions are Re m, Im m, aspect ratio, x.
-  const bool any_dir = part.dir_derivatives();
-  const bool along_x = point && nt > 0;
   const unsigned mask = (any_dir ? 0xEu : 0u) | (along_x ? 0x1u : 0u);
   const int sfd_of[4] = {2, 3, 1, 0};
   const double rtol_t = std::min(std::max(o.rtol / 100.0, 1e-12), 1e-8);
@@ -3496,29 +3544,33 @@ void spheroid_call_d(const SphParticle& sp, const SphDerivReq& req, const double
   Context& c = context();
   std::lock_guard<std::mutex> lk(c.mtx);
   cudaStream_t s = 0;
-  // Solved nodes by (wavelength, radius bits): the values, and per direction the derivatives
-  // of (Q_ext, Q_sca, Q_abs, Q_back, g, then the six unnormalized Greek arrays to 2N).
+  // Solved nodes by (particle, wavelength, radius bits): the values, and per direction the
+  // derivatives of (Q_ext, Q_sca, Q_abs, Q_back, g, then the six unnormalized Greek arrays to
+  // 2N). A query's `wl` is its unit, part * n_wl + wavelength.
   struct Node {
     SpheroidResult v;
     std::vector<double> d[4];
   };
-  std::map<std::pair<int64_t, uint64_t>, Node> cache;
-  auto key_of = [](int64_t i, double r) {
+  std::map<std::tuple<int, int64_t, uint64_t>, Node> cache;
+  auto key_of = [](int q, int64_t i, double r) {
     uint64_t b;
     memcpy(&b, &r, 8);
-    return std::make_pair(i, b);
+    return std::make_tuple(q, i, b);
   };
+  auto key_u = [&](int64_t u, double r) { return key_of(particle_of[u / n_wl], u % n_wl, r); };
   auto solve = [&](const std::vector<adaptive::Query>& qs) {
     std::vector<double> xs, es, ms;
     std::vector<std::pair<int64_t, double>> which;
+    std::set<std::tuple<int, int64_t, uint64_t>> batch;  // parts of one particle may share nodes
     for (const adaptive::Query& q : qs) {
-      const int64_t i = q.wl;
-      if (cache.count(key_of(i, q.r))) continue;
+      const int64_t i = q.wl % n_wl;
+      const SphParticle& sp = ps[particle_of[q.wl / n_wl]];
+      if (cache.count(key_u(q.wl, q.r)) || !batch.insert(key_u(q.wl, q.r)).second) continue;
       xs.push_back(2.0 * pi * q.r / wavelengths[i]);
       es.push_back(sp.eps);
       ms.push_back(sp.m[2 * i]);
       ms.push_back(sp.m[2 * i + 1]);
-      which.push_back({i, q.r});
+      which.push_back({q.wl, q.r});
     }
     if (which.empty()) return;
     std::vector<SpheroidResult> r;
@@ -3527,7 +3579,7 @@ void spheroid_call_d(const SphParticle& sp, const SphDerivReq& req, const double
     std::vector<SphEval> ev(which.size());
     int order = 0;
     for (size_t k = 0; k < which.size(); ++k) {
-      ev[k] = {xs[k], sp.eps, ms[2 * k], ms[2 * k + 1], r[k].n, r[k].nth};
+      ev[k] = {xs[k], es[k], ms[2 * k], ms[2 * k + 1], r[k].n, r[k].nth};
       order = std::max(order, 2 * r[k].n);
     }
     std::vector<std::vector<double>> d[4];
@@ -3546,7 +3598,7 @@ void spheroid_call_d(const SphParticle& sp, const SphDerivReq& req, const double
           for (int64_t l = 0; l < have; ++l) dst[5 + f * have + l] = src[5 + f * len + l];
       }
       nd.v = std::move(r[k]);
-      cache[key_of(which[k].first, which[k].second)] = std::move(nd);
+      cache[key_u(which[k].first, which[k].second)] = std::move(nd);
     }
   };
   // The pass-1 quantities (quantities1, engine.rs:379-417): the values, then per direction
@@ -3554,7 +3606,7 @@ void spheroid_call_d(const SphParticle& sp, const SphDerivReq& req, const double
   auto eval = [&](const std::vector<adaptive::Query>& qs, std::vector<adaptive::NodeResult>& out) {
     solve(qs);
     for (size_t k = 0; k < qs.size(); ++k) {
-      const Node& nd = cache.at(key_of(qs[k].wl, qs[k].r));
+      const Node& nd = cache.at(key_u(qs[k].wl, qs[k].r));
       const SpheroidResult& v = nd.v;
       const double area = pi * qs[k].r * qs[k].r;
       adaptive::NodeResult& x = out[k];
@@ -3575,31 +3627,50 @@ void spheroid_call_d(const SphParticle& sp, const SphDerivReq& req, const double
       x.status = 0;
     }
   };
-  // Pass 1 per wavelength (the part on its own panels), or the single radius itself.
-  std::vector<adaptive::Part> parts{part};
+  // Pass 1 per (part, wavelength) unit, each part on its own panels; single radii themselves.
   std::vector<adaptive::Job> jobs;
-  std::vector<adaptive::NodeResult> point_res;
-  if (point) {
-    std::vector<adaptive::Query> points;
-    for (int64_t i = 0; i < n_wl; ++i) points.push_back({part.lo, (int)i});
-    point_res.resize(points.size());
-    eval(points, point_res);
-  } else {
-    for (int64_t i = 0; i < n_wl; ++i) {
-      adaptive::Job jb;
-      jb.wl = (int)i;
-      jb.parts = {0};
-      jobs.push_back(jb);
+  std::vector<int> job_of(n_units, -1);
+  std::vector<adaptive::Query> points;
+  for (int64_t u = 0; u < n_units; ++u) {
+    const adaptive::Part& pt = parts[u / n_wl];
+    if (pt.support == adaptive::POINT) {
+      points.push_back({pt.lo, (int)u});
+      continue;
     }
-    adaptive::pass1(jobs, parts, wavelengths, o, eval);
-    for (const adaptive::Job& jb : jobs)
-      if (jb.status != 0) throw Failure{jb.status, jb.msg};
+    job_of[u] = (int)jobs.size();
+    adaptive::Job jb;
+    jb.wl = (int)u;
+    jb.parts = {(int)(u / n_wl)};
+    jobs.push_back(jb);
   }
-  std::vector<int64_t> n_direct(n_units);
+  std::vector<double> wl_units(n_units);
+  for (int64_t u = 0; u < n_units; ++u) wl_units[u] = wavelengths[u % n_wl];
+  std::vector<adaptive::NodeResult> point_res(points.size());
+  if (!points.empty()) eval(points, point_res);
+  adaptive::pass1(jobs, parts, wl_units.data(), o, eval);
+  for (const adaptive::Job& jb : jobs)
+    if (jb.status != 0) throw Failure{jb.status, jb.msg};
+  // The direct order: each unit's own N_max, or in a mixture the largest at its wavelength.
+  std::vector<int64_t> n_direct(n_units), n_at(n_wl, 0);
   int64_t width = 0;
   for (int64_t u = 0; u < n_units; ++u) {
-    n_direct[u] = point ? cache.at(key_of(u, part.lo)).v.n : jobs[u].n_terms;
+    const adaptive::Part& pt = parts[u / n_wl];
+    n_direct[u] = pt.support == adaptive::POINT ? cache.at(key_u(u, pt.lo)).v.n
+                                                : jobs[job_of[u]].n_terms;
+    n_at[u % n_wl] = std::max(n_at[u % n_wl], n_direct[u]);
+  }
+  for (int64_t u = 0; u < n_units; ++u) {
+    if (rows) n_direct[u] = n_at[u % n_wl];
     width = std::max(width, 2 * n_direct[u] + 1);
+  }
+  if (rows) {
+    rows->av.assign(n_units, {});
+    rows->ae.assign(n_units, {});
+    rows->dv.assign(n_units, {});
+    rows->de.assign(n_units, {});
+    rows->ld.assign(n_wl, -1);
+    rows->converged.assign(n_units, 1);
+    rows->panels.assign(n_units, 0);
   }
   const int64_t P = dd.n;
   if (all_orders) {
@@ -3615,7 +3686,11 @@ void spheroid_call_d(const SphParticle& sp, const SphDerivReq& req, const double
   const bool keep_greek = options->greek_order >= 0 || all_orders || n_mu > 0;
   constexpr int kS = 9;  // ONE, EXT, SCA, SCAG, ABS, BACK, R2, R3, DEPOL
   for (int64_t u = 0; u < n_units; ++u) {
-    const int64_t i = u;
+    const int64_t i = u % n_wl;
+    const adaptive::Part& part = parts[u / n_wl];
+    const SphDerivReq& req = reqs[u / n_wl];
+    const bool point = part.support == adaptive::POINT;
+    const int nt = (int)req.grads.size();
     const double lambda = wavelengths[i];
     const int L = all_orders ? (int)(2 * n_direct[u]) : options->greek_order;
     const int64_t ld = !keep_greek ? -1 : n_mu == 0 ? std::min<int64_t>(L, 2 * n_direct[u])
@@ -3627,7 +3702,7 @@ void spheroid_call_d(const SphParticle& sp, const SphDerivReq& req, const double
     // derivatives themselves.
     std::vector<double> g(len), ge(len), dg(4 * len), dge(4 * len);
     auto rows_at = [&](double r) {
-      const Node& nd = cache.at(key_of(i, r));
+      const Node& nd = cache.at(key_u(u, r));
       const SpheroidResult& v = nd.v;
       const double area = pi * r * r;
       const double tau = std::max(rtol_t, v.err_est);
@@ -3736,7 +3811,7 @@ void spheroid_call_d(const SphParticle& sp, const SphDerivReq& req, const double
         }
       }
     } else {
-      const adaptive::Job& jb = jobs[u];
+      const adaptive::Job& jb = jobs[job_of[u]];
       conv = jb.converged[0];
       panels = (int64_t)jb.panels.size();
       // Blocks: the values (weights u r), each parameter's (weights du/dtheta r on the values),
@@ -3835,6 +3910,16 @@ void spheroid_call_d(const SphParticle& sp, const SphDerivReq& req, const double
           de[req.theta_cols[b] * len + 6 + k] = mom.de[b][k];
         }
       }
+    }
+    if (rows) {
+      rows->av[u] = std::move(av);
+      rows->ae[u] = std::move(ae);
+      rows->dv[u] = std::move(dv);
+      rows->de[u] = std::move(de);
+      rows->ld[i] = ld;
+      rows->converged[u] = conv ? 1 : 0;
+      rows->panels[u] = panels;
+      continue;
     }
     // assemble (engine.rs:2396-2497) with the derivatives (lin.rs).
     auto lin = [&](int64_t j) {
@@ -4352,6 +4437,401 @@ void mixture_hetero(const scatrs_component* components, int64_t n_comp,
   }
 }
 
+// mixture_hetero with the derivatives along `dd`'s parameters (engine.rs:1964-2250 with
+// EnsembleOptions::derivatives): each part's averages with its derivative blocks from its own
+// engine (spheres and layered spheres: adaptive_call_order's per-block rows, one call per number
+// of layers; spheroids: spheroid_call_d's rows on the mixture's direct order), placed by result
+// column; then per wavelength the number-fraction mixing with the weight derivatives
+// (engine.rs:2121-2176) and the assembly of mixture_hetero with Lin (lin.rs): ratios, the
+// depolarization ratio, the spheres' Greek coefficients plus the spheroids' direct segment, and
+// the phase matrix of the spheres' tables plus the spheroids' expansion.
+void mixture_hetero_d(const scatrs_component* components, int64_t n_comp,
+                      const double* wavelengths, int64_t n_wl, const double* mu, int64_t n_mu,
+                      const scatrs_adaptive_options* options, const AdOutputs& res,
+                      const AdDerivs& dd) {
+  if (!options) throw Failure{SCATRS_INVALID_INPUT, "options must not be NULL"};
+  if (options->greek_order == SCATRS_GREEK_ALL)
+    throw Failure{SCATRS_INVALID_INPUT,
+                  "greek='all' with derivatives of a mixture of different particles is not on "
+                  "the GPU path"};
+  std::vector<AdPart> parts = mixture_parts(components, n_comp);
+  const int64_t np = (int64_t)parts.size(), P = dd.n;
+  for (int64_t c = 0; c < n_comp; ++c) {
+    const scatrs_component& k = components[c];
+    const std::string who = "component " + std::to_string(c) + ": ";
+    if (!(std::isfinite(k.aspect_ratio) && k.aspect_ratio >= 0.0))
+      throw Failure{SCATRS_INVALID_INPUT, who + "the aspect ratio must be finite and > 0"};
+    if (k.aspect_ratio > 0.0 && k.n_layers > 1)
+      throw Failure{SCATRS_INVALID_INPUT, who + "a particle is layered or a spheroid, not both"};
+    if (k.n_layers > kMaxLayersAbi) throw Failure{SCATRS_INVALID_INPUT, who + "at most 16 layers"};
+    if (k.n_layers > 1 && !k.fractions)
+      throw Failure{SCATRS_INVALID_INPUT, who + "a layered sphere needs its fractions"};
+  }
+  // Each part's parameters and the columns of its particle's directions.
+  for (AdPart& a : parts) {
+    const scatrs_component& k = components[a.component];
+    const int L = k.n_layers > 1 ? k.n_layers : 1;
+    a.dir_cols.assign(k.aspect_ratio > 0.0 ? 3 : L > 1 ? 3 * L - 1 : 2, -1);
+    for (int64_t c = 0; c < P; ++c) {
+      const scatrs_param& q = dd.params[c];
+      if (q.component != a.component) continue;
+      switch (q.kind) {
+        case SCATRS_PARAM_DISTRIBUTION:
+          if (q.mode == a.mode) {
+            a.grads.push_back(q.index);
+            a.theta_cols.push_back((int)c);
+          }
+          break;
+        case SCATRS_PARAM_REFR_REAL: a.dir_cols[0] = (int)c; break;
+        case SCATRS_PARAM_REFR_IMAG: a.dir_cols[1] = (int)c; break;
+        case SCATRS_PARAM_ASPECT_RATIO: a.dir_cols[2] = (int)c; break;
+        case SCATRS_PARAM_LAYER_REFR_REAL: a.dir_cols[2 * q.index] = (int)c; break;
+        case SCATRS_PARAM_LAYER_REFR_IMAG: a.dir_cols[2 * q.index + 1] = (int)c; break;
+        case SCATRS_PARAM_RADIUS_FRACTION: a.dir_cols[2 * L + q.index] = (int)c; break;
+        default: break;  // a weight: the mixing's
+      }
+    }
+  }
+  const int64_t glen = options->greek_order >= 0 ? options->greek_order + 1 : 0;
+  const int64_t gw = glen;
+  const int64_t row = 9 + 4 * n_mu + 6 * gw;
+  // Each (part, wavelength)'s averages on the common layout (9 scalars, the last the
+  // depolarization numerator; 4 n_mu cosine values; 6 gw Greek coefficients) with their errors,
+  // and per column their derivatives (P x row); a spheroid's direct segment likewise.
+  struct PD {
+    std::vector<double> v, e, d, de, sv, se, sd, sde;
+    bool converged = true;
+    int64_t panels = 0;
+  };
+  std::vector<PD> avg((size_t)np * n_wl);
+  for (PD& a : avg) {
+    a.v.assign(row, 0.0);
+    a.e.assign(row, 0.0);
+    a.d.assign((size_t)P * row, 0.0);
+    a.de.assign((size_t)P * row, 0.0);
+  }
+  // Spheroids first: their direct order.
+  std::vector<SphParticle> sph;
+  std::vector<SphDerivReq> sreq;
+  std::vector<int64_t> sph_parts;
+  for (int64_t c = 0; c < n_comp; ++c) {
+    const scatrs_component& k = components[c];
+    if (k.aspect_ratio == 0.0) continue;
+    sph.push_back(SphParticle{k.modes, k.n_modes, k.aspect_ratio, k.m});
+    for (int64_t p = 0; p < np; ++p)
+      if (parts[p].component == c) {
+        sph_parts.push_back(p);
+        SphDerivReq r;
+        r.grads = parts[p].grads;
+        r.theta_cols = parts[p].theta_cols;
+        for (int j = 0; j < 3; ++j) r.dir_cols[j] = parts[p].dir_cols[j];
+        sreq.push_back(r);
+      }
+  }
+  std::vector<int64_t> ld(n_wl, -1);
+  if (!sph.empty()) {
+    SphRowsD srows;
+    spheroid_call_d(sph, sreq, wavelengths, n_wl, mu, n_mu, options, AdOutputs{}, dd, &srows);
+    ld = srows.ld;
+    for (size_t q = 0; q < sph_parts.size(); ++q)
+      for (int64_t i = 0; i < n_wl; ++i) {
+        const int64_t u = (int64_t)q * n_wl + i;
+        const std::vector<double>& sv = srows.av[u];
+        const int64_t len = (int64_t)sv.size(), dlen = len - 9;
+        PD& a = avg[sph_parts[q] * n_wl + i];
+        for (int k = 0; k < 9; ++k) {
+          a.v[k] = sv[k];
+          a.e[k] = srows.ae[u][k];
+        }
+        a.sv.assign(sv.begin() + 9, sv.end());
+        a.se.assign(srows.ae[u].begin() + 9, srows.ae[u].end());
+        a.sd.assign((size_t)P * dlen, 0.0);
+        a.sde.assign((size_t)P * dlen, 0.0);
+        for (int64_t col = 0; col < P; ++col) {
+          for (int k = 0; k < 9; ++k) {
+            a.d[col * row + k] = srows.dv[u][col * len + k];
+            a.de[col * row + k] = srows.de[u][col * len + k];
+          }
+          for (int64_t t = 0; t < dlen; ++t) {
+            a.sd[col * dlen + t] = srows.dv[u][col * len + 9 + t];
+            a.sde[col * dlen + t] = srows.de[u][col * len + 9 + t];
+          }
+        }
+        a.converged = srows.converged[u] != 0;
+        a.panels = srows.panels[u];
+      }
+  }
+  // Spheres, and layered spheres by their number of layers: one adaptive call each, its
+  // per-block rows placed by column.
+  std::map<int, std::vector<int64_t>> by_layers;
+  for (int64_t p = 0; p < np; ++p) {
+    const scatrs_component& k = components[parts[p].component];
+    if (k.aspect_ratio == 0.0) by_layers[k.n_layers > 1 ? k.n_layers : 1].push_back(p);
+  }
+  const int64_t hrow = 8 + 4 * n_mu + 6 * glen;
+  for (const auto& kv : by_layers) {
+    const int nl = kv.first;
+    const std::vector<int64_t>& ps = kv.second;
+    std::vector<AdPart> sub;
+    std::vector<double> fr, ml;
+    int n_theta = 0;
+    for (int64_t p : ps) {
+      AdPart a = parts[p];
+      a.out = 0;
+      n_theta = std::max(n_theta, (int)a.grads.size());
+      sub.push_back(a);
+      if (nl > 1) {
+        const scatrs_component& c = components[parts[p].component];
+        fr.insert(fr.end(), c.fractions, c.fractions + nl - 1);
+        ml.insert(ml.end(), c.m, c.m + 2 * (size_t)nl * n_wl);
+      }
+    }
+    scatrs_layers lay{nl, 0, fr.data(), ml.data()};
+    PartRows rows;
+    adaptive_call_order(sub, 1, false, wavelengths, n_wl, mu, n_mu, options, AdOutputs{},
+                        nl > 1 ? &lay : nullptr, &dd, nullptr, &rows);
+    const int B = 1 + n_theta + (int)sub[0].dir_cols.size();
+    if (rows.stride != 2 * (int64_t)B * hrow)
+      throw Failure{SCATRS_CUDA, "internal: the rows of a mixture's sphere class"};
+    // One row of the per-block layout onto the common one (depolarization numerator 0).
+    auto put = [&](const double* src, double* dst) {
+      for (int c = 0; c < 8; ++c) dst[c] = src[c];
+      dst[8] = 0.0;
+      for (int64_t t = 0; t < 4 * n_mu; ++t) dst[9 + t] = src[8 + t];
+      for (int f = 0; f < 6; ++f)
+        for (int64_t l = 0; l < glen; ++l)
+          dst[9 + 4 * n_mu + f * gw + l] = src[8 + 4 * n_mu + f * glen + l];
+    };
+    for (size_t q = 0; q < ps.size(); ++q) {
+      const AdPart& a = sub[q];
+      for (int64_t i = 0; i < n_wl; ++i) {
+        const double* r = rows.rows.data() + ((int64_t)q * n_wl + i) * rows.stride;
+        PD& x = avg[ps[q] * n_wl + i];
+        put(r, x.v.data());
+        put(r + hrow, x.e.data());
+        for (int b = 1; b < B; ++b) {
+          int col = -1;
+          if (b <= n_theta) {
+            if (b - 1 < (int)a.theta_cols.size()) col = a.theta_cols[b - 1];
+          } else {
+            col = a.dir_cols[b - n_theta - 1];
+          }
+          if (col < 0) continue;
+          put(r + 2 * b * hrow, x.d.data() + col * row);
+          put(r + (2 * b + 1) * hrow, x.de.data() + col * row);
+        }
+        x.converged = rows.converged[q * n_wl + i] != 0;
+        x.panels = rows.panels[q * n_wl + i];
+      }
+    }
+  }
+  // Mixing (with the weight derivatives) and assembly per wavelength.
+  double w_total = 0.0;
+  {
+    std::vector<int> comps;
+    for (const AdPart& a : parts)
+      if (std::find(comps.begin(), comps.end(), a.component) == comps.end()) {
+        comps.push_back(a.component);
+        w_total += a.w;
+      }
+  }
+  const bool norm = options->normalized != 0;
+  for (int64_t i = 0; i < n_wl; ++i) {
+    const int64_t ldi = ld[i], dlen = ldi >= 0 ? 6 * (ldi + 1) : 0;
+    std::vector<double> v(row, 0.0), e(row, 0.0), d((size_t)P * row, 0.0),
+        de((size_t)P * row, 0.0), sv(dlen, 0.0), se(dlen, 0.0), sd((size_t)P * dlen, 0.0),
+        sde((size_t)P * dlen, 0.0);
+    bool has_direct = false, conv = true;
+    int64_t panels = 0;
+    for (int64_t p = 0; p < np; ++p) {
+      const PD& a = avg[p * n_wl + i];
+      const double f = parts[p].f;
+      const bool direct = components[parts[p].component].aspect_ratio > 0.0;
+      for (int64_t k = 0; k < row; ++k) {
+        v[k] += f * a.v[k];
+        e[k] += f * a.e[k];
+      }
+      for (int64_t k = 0; k < P * row; ++k) {
+        d[k] += f * a.d[k];
+        de[k] += f * a.de[k];
+      }
+      if (direct) {
+        has_direct = true;
+        for (int64_t k = 0; k < dlen; ++k) {
+          sv[k] += f * a.sv[k];
+          se[k] += f * a.se[k];
+        }
+        for (int64_t k = 0; k < P * dlen; ++k) {
+          sd[k] += f * a.sd[k];
+          sde[k] += f * a.sde[k];
+        }
+      }
+      conv = conv && a.converged;
+      panels += a.panels;
+    }
+    for (int64_t col = 0; col < P; ++col) {
+      const scatrs_param& pr = dd.params[col];
+      if (pr.kind != SCATRS_PARAM_WEIGHT) continue;
+      for (int64_t p = 0; p < np; ++p) {
+        const AdPart& a = parts[p];
+        const double f = a.w / w_total * a.v / a.v_total;
+        double df;
+        if (pr.mode < 0) {
+          const double own = a.component == pr.component ? a.v / a.v_total : 0.0;
+          df = (own - f) / w_total;
+        } else if (a.component != pr.component) {
+          df = 0.0;
+        } else {
+          const double own = a.mode == pr.mode ? 1.0 : 0.0;
+          df = a.w / w_total * (own - a.v / a.v_total) / a.v_total;
+        }
+        const PD& x = avg[p * n_wl + i];
+        for (int64_t k = 0; k < row; ++k) {
+          d[col * row + k] += df * x.v[k];
+          de[col * row + k] += std::fabs(df) * x.e[k];
+        }
+        if (components[a.component].aspect_ratio > 0.0)
+          for (int64_t k = 0; k < dlen; ++k) {
+            sd[col * dlen + k] += df * x.sv[k];
+            sde[col * dlen + k] += std::fabs(df) * x.se[k];
+          }
+      }
+    }
+    auto lin = [&](int64_t k) {
+      LinD x;
+      x.v = v[k];
+      x.e = e[k];
+      x.d.resize(P);
+      x.de.resize(P);
+      for (int64_t c = 0; c < P; ++c) {
+        x.d[c] = d[c * row + k];
+        x.de[c] = de[c * row + k];
+      }
+      return x;
+    };
+    auto D = [&](int f, int64_t l) {
+      const int64_t k = f * (ldi + 1) + l;
+      LinD x;
+      x.v = sv[k];
+      x.e = se[k];
+      x.d.resize(P);
+      x.de.resize(P);
+      for (int64_t c = 0; c < P; ++c) {
+        x.d[c] = sd[c * dlen + k];
+        x.de[c] = sde[c * dlen + k];
+      }
+      return x;
+    };
+    // x + c y for an exact c (Lin::combine).
+    auto add = [&](LinD x, double c, const LinD& y) {
+      x.v += c * y.v;
+      x.e += std::fabs(c) * y.e;
+      for (int64_t k = 0; k < P; ++k) {
+        x.d[k] += c * y.d[k];
+        x.de[k] += std::fabs(c) * y.de[k];
+      }
+      return x;
+    };
+    const LinD ext = lin(1), sca = lin(2), scag = lin(3), abs_ = lin(4), back = lin(5),
+               r2 = lin(6), r3 = lin(7), num = lin(8);
+    for (const auto& w : {std::make_pair("<C_ext>", &ext), std::make_pair("<C_sca>", &sca),
+                          std::make_pair("<C_back>", &back)})
+      if (!(std::isfinite(w.second->v) && w.second->v != 0.0))
+        throw Failure{SCATRS_INVALID_INPUT,
+                      std::string("the ensemble's ") + w.first +
+                          " is 0 or not finite, so its ratios (albedo, asymmetry parameter, "
+                          "lidar ratio) are undefined (does m = 1?)"};
+    const LinD depol = has_direct ? num.div(add(back.scale(2.0), -1.0, num))
+                                  : LinD::constant(0.0, (size_t)P);
+    const LinD outs[11] = {ext,
+                           sca,
+                           abs_,
+                           back,
+                           sca.div(ext),
+                           scag.div(sca),
+                           ext.div(back).scale(4.0 * kPi),
+                           depol,
+                           r3.div(r2),
+                           r2.scale(kPi),
+                           r3.scale(4.0 * kPi / 3.0)};
+    for (int k = 0; k < 11; ++k) {
+      res.values[k * n_wl + i] = outs[k].v;
+      if (res.errors) res.errors[k * n_wl + i] = outs[k].e;
+      for (int64_t c = 0; c < P; ++c) {
+        if (dd.d_values) dd.d_values[(c * 11 + k) * n_wl + i] = outs[k].d[c];
+        if (dd.d_errors) dd.d_errors[(c * 11 + k) * n_wl + i] = outs[k].de[c];
+      }
+    }
+    const int64_t g0 = 9 + 4 * n_mu;
+    if (glen > 0 && res.greek) {
+      // The spheres' coefficients plus the spheroids' (engine.rs:2196-2216).
+      auto G = [&](int f, int64_t l) {
+        LinD x = lin(g0 + f * gw + l);
+        if (has_direct && l <= ldi) x = add(x, 1.0, D(f, l));
+        return x;
+      };
+      const LinD a0 = G(0, 0);
+      for (int f = 0; f < 6; ++f)
+        for (int64_t l = 0; l < glen; ++l) {
+          LinD x = G(f, l);
+          if (norm) x = (f == 0 && l == 0) ? LinD::constant(1.0, (size_t)P) : x.div(a0);
+          const int64_t at = (f * n_wl + i) * gw + l;
+          res.greek[at] = x.v;
+          if (res.greek_err) res.greek_err[at] = x.e;
+          for (int64_t c = 0; c < P; ++c) {
+            const int64_t atd = ((c * 6 + f) * n_wl + i) * gw + l;
+            if (dd.d_greek) dd.d_greek[atd] = x.d[c];
+            if (dd.d_greek_err) dd.d_greek_err[atd] = x.de[c];
+          }
+        }
+    }
+    if (n_mu > 0 && res.phase) {
+      const int src[6] = {0, 1, 0, 2, 3, 2};
+      std::vector<double> d00, d22, d2m2, d02;
+      if (has_direct && ldi >= 0) {
+        d00.resize(ldi + 1);
+        d22.resize(ldi + 1);
+        d2m2.resize(ldi + 1);
+        d02.resize(ldi + 1);
+      }
+      for (int64_t j = 0; j < n_mu; ++j) {
+        LinD fd[6];
+        for (int k = 0; k < 6; ++k) fd[k] = LinD::constant(0.0, (size_t)P);
+        if (has_direct && ldi >= 0) {
+          wigner_d(0, 0, mu[j], d00.data(), ldi + 1);
+          wigner_d(2, 2, mu[j], d22.data(), ldi + 1);
+          wigner_d(2, -2, mu[j], d2m2.data(), ldi + 1);
+          wigner_d(0, 2, mu[j], d02.data(), ldi + 1);
+          for (int64_t l = 0; l <= ldi; ++l) {
+            const double pl = 0.5 * (d22[l] + d2m2[l]), mn = 0.5 * (d22[l] - d2m2[l]);
+            fd[0] = add(fd[0], d00[l], D(0, l));
+            fd[1] = add(fd[1], d02[l], D(4, l));
+            fd[2] = add(add(fd[2], pl, D(1, l)), mn, D(2, l));
+            fd[3] = add(add(fd[3], mn, D(1, l)), pl, D(2, l));
+            fd[4] = add(fd[4], d02[l], D(5, l));
+            fd[5] = add(fd[5], d00[l], D(3, l));
+          }
+        }
+        for (int el = 0; el < 6; ++el) {
+          LinD x = add(lin(9 + src[el] * n_mu + j), 1.0, fd[el]);
+          if (norm) x = x.div(sca);
+          const int64_t at = (el * n_wl + i) * n_mu + j;
+          res.phase[at] = x.v;
+          if (res.phase_err) res.phase_err[at] = x.e;
+          for (int64_t c = 0; c < P; ++c) {
+            const int64_t atd = ((c * 6 + el) * n_wl + i) * n_mu + j;
+            if (dd.d_phase) dd.d_phase[atd] = x.d[c];
+            if (dd.d_phase_err) dd.d_phase_err[atd] = x.de[c];
+          }
+        }
+      }
+    }
+    if (res.converged) res.converged[i] = conv ? 1 : 0;
+    if (res.panels) res.panels[i] = panels;
+  }
+}
+
+
 }  // namespace
 }  // namespace sb
 
@@ -4686,13 +5166,7 @@ int scatrs_ensemble_mixture_d(const scatrs_component* components, int64_t n_comp
     // its layers.
     const bool layered_alone = n_comp == 1 && components && components[0].n_layers > 1 &&
                                components[0].aspect_ratio == 0.0;
-    if (heterogeneous(components, n_comp) &&
-        !(n_params > 0 && (spheroid_alone || layered_alone))) {
-      if (n_params > 0)
-        throw Failure{SCATRS_INVALID_INPUT,
-                      "derivatives of layered spheres or spheroids beside other components, or "
-                      "of spheroids in multimodal distributions, are not on the adaptive GPU "
-                      "path"};
+    if (heterogeneous(components, n_comp) && n_params == 0) {
       AdOutputs out{values, errors, phase, phase_err, greek, greek_err, converged, panels};
       mixture_hetero(components, n_comp, wavelengths, n_wl, mu, n_mu, options, out);
       return;
@@ -4772,6 +5246,23 @@ int scatrs_ensemble_mixture_d(const scatrs_component* components, int64_t n_comp
       }
       if (!allowed) throw Failure{SCATRS_INVALID_INPUT, "no parameter " + name(q) + " here"};
     }
+    if (heterogeneous(components, n_comp) && !spheroid_alone && !layered_alone) {
+      // Components of different particles (or a multimodal spheroid): every part on its own
+      // engine, mixed and assembled on the host with the derivatives.
+      if (!d_values) throw Failure{SCATRS_INVALID_INPUT, "d_values is required with parameters"};
+      AdOutputs out{values, errors, phase, phase_err, greek, greek_err, converged, panels};
+      AdDerivs dd;
+      dd.params = params;
+      dd.n = n_params;
+      dd.d_values = d_values;
+      dd.d_errors = d_errors;
+      dd.d_phase = d_phase;
+      dd.d_phase_err = d_phase_err;
+      dd.d_greek = d_greek;
+      dd.d_greek_err = d_greek_err;
+      mixture_hetero_d(components, n_comp, wavelengths, n_wl, mu, n_mu, options, out, dd);
+      return;
+    }
     if (spheroid_alone) {
       if (n_params > 0 && !d_values)
         throw Failure{SCATRS_INVALID_INPUT, "d_values is required with parameters"};
@@ -4802,8 +5293,8 @@ int scatrs_ensemble_mixture_d(const scatrs_component* components, int64_t n_comp
       for (int64_t k = 0; k < n_params * 11 * n_wl && d_values; ++k) d_values[k] = 0.0;
       for (int64_t k = 0; k < n_params * 11 * n_wl && d_errors; ++k) d_errors[k] = 0.0;
       const scatrs_component& cp = components[0];
-      spheroid_call_d(SphParticle{cp.modes, 1, cp.aspect_ratio, cp.m}, req, wavelengths, n_wl, mu,
-                      n_mu, options, out, dd);
+      spheroid_call_d({SphParticle{cp.modes, 1, cp.aspect_ratio, cp.m}}, {req}, wavelengths, n_wl,
+                      mu, n_mu, options, out, dd);
       return;
     }
     if (layered_alone) {

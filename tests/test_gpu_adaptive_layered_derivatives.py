@@ -125,8 +125,3 @@ def test_refusals(gpu):
     with pytest.raises(InvalidInputError, match="radius derivative of a single layered"):
         _scatrs.ensemble_compute([(("monodisperse", 0.3), particle, 1.0)], WL, False, None,
                                  False, None, True, [0], 1e-6, 4096, False, False)
-    items = [(("lognormal", 0.1, 1.5), ("sphere", np.array([1.45 + 0j])), 2.0),
-             (("lognormal", 0.3, 1.4), particle, 0.5)]
-    with pytest.raises(InvalidInputError, match="not on the adaptive GPU path"):
-        _scatrs.ensemble_compute(items, WL, True, None, False, None, True, [10], 1e-6, 4096,
-                                 False, False)

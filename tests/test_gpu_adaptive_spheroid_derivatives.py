@@ -91,14 +91,6 @@ def test_every_direction_at_once(gpu):
         assert np.all(np.abs(d_all - d_one) <= 1e-6 * scale), i
 
 
-def test_mixtures_with_spheroids_refuse_derivatives(gpu):
-    items = [(LOGN, ("spheroid", 2.0, np.array([DUST])), 1.0),
-             (("lognormal", 0.05, 1.5), ("sphere", np.array([1.45 + 0j])), 2.0)]
-    with pytest.raises(InvalidInputError, match="not on the adaptive GPU path"):
-        _scatrs.ensemble_compute(items, WL, True, 6, False, MU, True, [4], 1e-6, 4096, False,
-                                 False)
-
-
 def test_a_sphere_has_no_aspect_ratio(gpu):
     d = gpu.dist_records(1)
     d["kind"][0] = gpu.KINDS["lognormal"]
