@@ -241,7 +241,7 @@ typedef struct scatrs_param {
  * (SCATRS_PARAM_LAYER_REFR_REAL/_IMAG, SCATRS_PARAM_RADIUS_FRACTION; validated up to
  * x_L = 1000, layered/domain.rs:39-70); or a mixture of different particles along any of
  * its components' parameters and weights (each part on its own engine, mixed and assembled on
- * the host; not with SCATRS_GREEK_ALL). A single sphere radius's radius is
+ * the host). A single sphere radius's radius is
  * exact (engine.rs:1158-1170), with zero error estimates; a single spheroid's follows
  * monodisperse_direct (engine.rs:1896-1961). d_values, d_errors (P, 11, n_wl); d_phase, d_phase_err (P, 6, n_wl, n_mu); d_greek,
  * d_greek_err (P, 6, n_wl, L + 1), P = n_params, in the order of `params`. Invalid or

@@ -3507,10 +3507,6 @@ void spheroid_call_d(const std::vector<SphParticle>& ps, const std::vector<SphDe
   for (const SphParticle& q : ps)
     if (!(std::isfinite(q.eps) && q.eps > 0.0))
       throw Failure{SCATRS_INVALID_INPUT, "the aspect ratio must be finite and > 0"};
-  if (rows && all_orders)
-    throw Failure{SCATRS_INVALID_INPUT,
-                  "greek='all' with derivatives of a mixture of different particles is not on "
-                  "the GPU path"};
   scatrs_fixed_options fo{32, all_orders ? -1 : options->greek_order, options->normalized,
                           options->allow_unvalidated};
   const int64_t n_units = n_parts * n_wl;
@@ -3673,7 +3669,7 @@ void spheroid_call_d(const std::vector<SphParticle>& ps, const std::vector<SphDe
     rows->panels.assign(n_units, 0);
   }
   const int64_t P = dd.n;
-  if (all_orders) {
+  if (all_orders && !rows) {  // a mixture's rows: the mixture sets its own coefficients
     GreekAll& ga = t_greek_all;
     ga.width = width;
     ga.n = n_units;
@@ -4450,10 +4446,7 @@ void mixture_hetero_d(const scatrs_component* components, int64_t n_comp,
                       const scatrs_adaptive_options* options, const AdOutputs& res,
                       const AdDerivs& dd) {
   if (!options) throw Failure{SCATRS_INVALID_INPUT, "options must not be NULL"};
-  if (options->greek_order == SCATRS_GREEK_ALL)
-    throw Failure{SCATRS_INVALID_INPUT,
-                  "greek='all' with derivatives of a mixture of different particles is not on "
-                  "the GPU path"};
+  const bool all_orders = options->greek_order == SCATRS_GREEK_ALL;
   std::vector<AdPart> parts = mixture_parts(components, n_comp);
   const int64_t np = (int64_t)parts.size(), P = dd.n;
   for (int64_t c = 0; c < n_comp; ++c) {
@@ -4492,24 +4485,18 @@ void mixture_hetero_d(const scatrs_component* components, int64_t n_comp,
       }
     }
   }
-  const int64_t glen = options->greek_order >= 0 ? options->greek_order + 1 : 0;
-  const int64_t gw = glen;
-  const int64_t row = 9 + 4 * n_mu + 6 * gw;
   // Each (part, wavelength)'s averages on the common layout (9 scalars, the last the
   // depolarization numerator; 4 n_mu cosine values; 6 gw Greek coefficients) with their errors,
-  // and per column their derivatives (P x row); a spheroid's direct segment likewise.
+  // and per column their derivatives (P x row); a spheroid's direct segment likewise. The
+  // layout's width gw follows the spheroids' and the sphere classes' orders.
   struct PD {
     std::vector<double> v, e, d, de, sv, se, sd, sde;
     bool converged = true;
     int64_t panels = 0;
   };
   std::vector<PD> avg((size_t)np * n_wl);
-  for (PD& a : avg) {
-    a.v.assign(row, 0.0);
-    a.e.assign(row, 0.0);
-    a.d.assign((size_t)P * row, 0.0);
-    a.de.assign((size_t)P * row, 0.0);
-  }
+  int64_t gw = 0, row = 0;
+  std::vector<int64_t> order(n_wl, options->greek_order);
   // Spheroids first: their direct order.
   std::vector<SphParticle> sph;
   std::vector<SphDerivReq> sreq;
@@ -4529,10 +4516,67 @@ void mixture_hetero_d(const scatrs_component* components, int64_t n_comp,
       }
   }
   std::vector<int64_t> ld(n_wl, -1);
+  SphRowsD srows;
   if (!sph.empty()) {
-    SphRowsD srows;
     spheroid_call_d(sph, sreq, wavelengths, n_wl, mu, n_mu, options, AdOutputs{}, dd, &srows);
     ld = srows.ld;
+  }
+  // Spheres, and layered spheres by their number of layers.
+  std::map<int, std::vector<int64_t>> by_layers;
+  for (int64_t p = 0; p < np; ++p) {
+    const scatrs_component& k = components[parts[p].component];
+    if (k.aspect_ratio == 0.0) by_layers[k.n_layers > 1 ? k.n_layers : 1].push_back(p);
+  }
+  // A class's parts (output unit 0) with their layers' fractions and indices.
+  struct Cls {
+    std::vector<AdPart> sub;
+    std::vector<double> fr, ml;
+    int nl = 1, n_theta = 0;
+  };
+  auto make_cls = [&](int nl, const std::vector<int64_t>& ps) {
+    Cls k;
+    k.nl = nl;
+    for (int64_t p : ps) {
+      AdPart a = parts[p];
+      a.out = 0;
+      k.n_theta = std::max(k.n_theta, (int)a.grads.size());
+      k.sub.push_back(a);
+      if (nl > 1) {
+        const scatrs_component& c = components[parts[p].component];
+        k.fr.insert(k.fr.end(), c.fractions, c.fractions + nl - 1);
+        k.ml.insert(k.ml.end(), c.m, c.m + 2 * (size_t)nl * n_wl);
+      }
+    }
+    return k;
+  };
+  // greek='all': every wavelength's order 2 N_max over every part (engine.rs:2016-2036), the
+  // sphere classes' N_max from their pass 1.
+  if (all_orders) {
+    std::fill(order.begin(), order.end(), 0);
+    for (int64_t i = 0; i < n_wl; ++i)
+      if (ld[i] >= 0) order[i] = ld[i];
+    scatrs_adaptive_options o1 = *options;
+    o1.greek_order = -1;
+    for (const auto& kv : by_layers) {
+      Cls k = make_cls(kv.first, kv.second);
+      scatrs_layers lay{k.nl, 0, k.fr.data(), k.ml.data()};
+      std::vector<int64_t> n_max;
+      adaptive_call_order(k.sub, 1, false, wavelengths, n_wl, mu, n_mu, &o1, AdOutputs{},
+                          k.nl > 1 ? &lay : nullptr, nullptr, &n_max);
+      for (size_t q = 0; q < k.sub.size() && !n_max.empty(); ++q)
+        for (int64_t i = 0; i < n_wl; ++i)
+          order[i] = std::max(order[i], 2 * n_max[q * n_wl + i]);
+    }
+  }
+  for (int64_t i = 0; i < n_wl; ++i) gw = std::max(gw, order[i] + 1);
+  row = 9 + 4 * n_mu + 6 * gw;
+  for (PD& a : avg) {
+    a.v.assign(row, 0.0);
+    a.e.assign(row, 0.0);
+    a.d.assign((size_t)P * row, 0.0);
+    a.de.assign((size_t)P * row, 0.0);
+  }
+  if (!sph.empty()) {
     for (size_t q = 0; q < sph_parts.size(); ++q)
       for (int64_t i = 0; i < n_wl; ++i) {
         const int64_t u = (int64_t)q * n_wl + i;
@@ -4561,69 +4605,91 @@ void mixture_hetero_d(const scatrs_component* components, int64_t n_comp,
         a.panels = srows.panels[u];
       }
   }
-  // Spheres, and layered spheres by their number of layers: one adaptive call each, its
-  // per-block rows placed by column.
-  std::map<int, std::vector<int64_t>> by_layers;
-  for (int64_t p = 0; p < np; ++p) {
-    const scatrs_component& k = components[parts[p].component];
-    if (k.aspect_ratio == 0.0) by_layers[k.n_layers > 1 ? k.n_layers : 1].push_back(p);
-  }
-  const int64_t hrow = 8 + 4 * n_mu + 6 * glen;
+  // The sphere classes: one adaptive call per class and group of wavelengths of one order (all
+  // of them without 'all'), its per-block rows placed by column.
   for (const auto& kv : by_layers) {
-    const int nl = kv.first;
+    const Cls k = make_cls(kv.first, kv.second);
     const std::vector<int64_t>& ps = kv.second;
-    std::vector<AdPart> sub;
-    std::vector<double> fr, ml;
-    int n_theta = 0;
-    for (int64_t p : ps) {
-      AdPart a = parts[p];
-      a.out = 0;
-      n_theta = std::max(n_theta, (int)a.grads.size());
-      sub.push_back(a);
-      if (nl > 1) {
-        const scatrs_component& c = components[parts[p].component];
-        fr.insert(fr.end(), c.fractions, c.fractions + nl - 1);
-        ml.insert(ml.end(), c.m, c.m + 2 * (size_t)nl * n_wl);
-      }
-    }
-    scatrs_layers lay{nl, 0, fr.data(), ml.data()};
-    PartRows rows;
-    adaptive_call_order(sub, 1, false, wavelengths, n_wl, mu, n_mu, options, AdOutputs{},
-                        nl > 1 ? &lay : nullptr, &dd, nullptr, &rows);
-    const int B = 1 + n_theta + (int)sub[0].dir_cols.size();
-    if (rows.stride != 2 * (int64_t)B * hrow)
-      throw Failure{SCATRS_CUDA, "internal: the rows of a mixture's sphere class"};
-    // One row of the per-block layout onto the common one (depolarization numerator 0).
-    auto put = [&](const double* src, double* dst) {
-      for (int c = 0; c < 8; ++c) dst[c] = src[c];
-      dst[8] = 0.0;
-      for (int64_t t = 0; t < 4 * n_mu; ++t) dst[9 + t] = src[8 + t];
-      for (int f = 0; f < 6; ++f)
-        for (int64_t l = 0; l < glen; ++l)
-          dst[9 + 4 * n_mu + f * gw + l] = src[8 + 4 * n_mu + f * glen + l];
-    };
-    for (size_t q = 0; q < ps.size(); ++q) {
-      const AdPart& a = sub[q];
-      for (int64_t i = 0; i < n_wl; ++i) {
-        const double* r = rows.rows.data() + ((int64_t)q * n_wl + i) * rows.stride;
-        PD& x = avg[ps[q] * n_wl + i];
-        put(r, x.v.data());
-        put(r + hrow, x.e.data());
-        for (int b = 1; b < B; ++b) {
-          int col = -1;
-          if (b <= n_theta) {
-            if (b - 1 < (int)a.theta_cols.size()) col = a.theta_cols[b - 1];
-          } else {
-            col = a.dir_cols[b - n_theta - 1];
+    std::map<int64_t, std::vector<int64_t>> by_order;
+    for (int64_t i = 0; i < n_wl; ++i) by_order[order[i]].push_back(i);
+    for (const auto& ko : by_order) {
+      const int64_t glen = ko.first >= 0 ? ko.first + 1 : 0;
+      const std::vector<int64_t>& ws = ko.second;
+      const int64_t nw = (int64_t)ws.size();
+      std::vector<double> wl_s(nw);
+      for (int64_t j = 0; j < nw; ++j) wl_s[j] = wavelengths[ws[j]];
+      std::vector<AdPart> sub = k.sub;
+      std::vector<std::vector<double>> m_s(sub.size());
+      std::vector<double> ml_s(k.ml.size() / std::max<int64_t>(n_wl, 1) * nw);
+      for (size_t q = 0; q < sub.size(); ++q) {
+        if (sub[q].m) {
+          m_s[q].resize(2 * nw);
+          for (int64_t j = 0; j < nw; ++j) {
+            m_s[q][2 * j] = sub[q].m[2 * ws[j]];
+            m_s[q][2 * j + 1] = sub[q].m[2 * ws[j] + 1];
           }
-          if (col < 0) continue;
-          put(r + 2 * b * hrow, x.d.data() + col * row);
-          put(r + (2 * b + 1) * hrow, x.de.data() + col * row);
+          sub[q].m = m_s[q].data();
         }
-        x.converged = rows.converged[q * n_wl + i] != 0;
-        x.panels = rows.panels[q * n_wl + i];
+        for (int l = 0; k.nl > 1 && l < k.nl; ++l)
+          for (int64_t j = 0; j < nw; ++j)
+            for (int c = 0; c < 2; ++c)
+              ml_s[2 * ((q * k.nl + l) * nw + j) + c] =
+                  k.ml[2 * ((q * k.nl + l) * n_wl + ws[j]) + c];
+      }
+      scatrs_layers lay{k.nl, 0, k.fr.data(), ml_s.data()};
+      scatrs_adaptive_options oL = *options;
+      oL.greek_order = (int32_t)ko.first;
+      PartRows rows;
+      adaptive_call_order(sub, 1, false, wl_s.data(), nw, mu, n_mu, &oL, AdOutputs{},
+                          k.nl > 1 ? &lay : nullptr, &dd, nullptr, &rows);
+      const int n_theta = k.n_theta;
+      const int64_t hrow = 8 + 4 * n_mu + 6 * glen;
+      const int B = 1 + n_theta + (int)sub[0].dir_cols.size();
+      if (rows.stride != 2 * (int64_t)B * hrow)
+        throw Failure{SCATRS_CUDA, "internal: the rows of a mixture's sphere class"};
+      // One row of the per-block layout onto the common one (depolarization numerator 0).
+      auto put = [&](const double* src, double* dst) {
+        for (int c = 0; c < 8; ++c) dst[c] = src[c];
+        dst[8] = 0.0;
+        for (int64_t t = 0; t < 4 * n_mu; ++t) dst[9 + t] = src[8 + t];
+        for (int f = 0; f < 6; ++f)
+          for (int64_t l = 0; l < glen; ++l)
+            dst[9 + 4 * n_mu + f * gw + l] = src[8 + 4 * n_mu + f * glen + l];
+      };
+      for (size_t q = 0; q < ps.size(); ++q) {
+        const AdPart& a = sub[q];
+        for (int64_t j = 0; j < nw; ++j) {
+          const int64_t i = ws[j];
+          const double* r = rows.rows.data() + ((int64_t)q * nw + j) * rows.stride;
+          PD& x = avg[ps[q] * n_wl + i];
+          put(r, x.v.data());
+          put(r + hrow, x.e.data());
+          for (int b = 1; b < B; ++b) {
+            int col = -1;
+            if (b <= n_theta) {
+              if (b - 1 < (int)a.theta_cols.size()) col = a.theta_cols[b - 1];
+            } else {
+              col = a.dir_cols[b - n_theta - 1];
+            }
+            if (col < 0) continue;
+            put(r + 2 * b * hrow, x.d.data() + col * row);
+            put(r + (2 * b + 1) * hrow, x.de.data() + col * row);
+          }
+          x.converged = rows.converged[q * nw + j] != 0;
+          x.panels = rows.panels[q * nw + j];
+        }
       }
     }
+  }
+  if (all_orders) {
+    GreekAll& ga = t_greek_all;
+    ga.width = gw;
+    ga.n = n_wl;
+    ga.p = P;
+    ga.g.assign(6 * n_wl * gw, 0.0);
+    ga.ge.assign(ga.g.size(), 0.0);
+    ga.dg.assign(P * ga.g.size(), 0.0);
+    ga.dge.assign(ga.dg.size(), 0.0);
   }
   // Mixing (with the weight derivatives) and assembly per wavelength.
   double w_total = 0.0;
@@ -4762,8 +4828,12 @@ void mixture_hetero_d(const scatrs_component* components, int64_t n_comp,
         if (dd.d_errors) dd.d_errors[(c * 11 + k) * n_wl + i] = outs[k].de[c];
       }
     }
-    const int64_t g0 = 9 + 4 * n_mu;
-    if (glen > 0 && res.greek) {
+    const int64_t g0 = 9 + 4 * n_mu, glen = order[i] + 1;
+    double* g_out = all_orders ? t_greek_all.g.data() : res.greek;
+    double* ge_out = all_orders ? t_greek_all.ge.data() : res.greek_err;
+    double* dg_out = all_orders ? t_greek_all.dg.data() : dd.d_greek;
+    double* dge_out = all_orders ? t_greek_all.dge.data() : dd.d_greek_err;
+    if (glen > 0 && g_out) {
       // The spheres' coefficients plus the spheroids' (engine.rs:2196-2216).
       auto G = [&](int f, int64_t l) {
         LinD x = lin(g0 + f * gw + l);
@@ -4776,12 +4846,12 @@ void mixture_hetero_d(const scatrs_component* components, int64_t n_comp,
           LinD x = G(f, l);
           if (norm) x = (f == 0 && l == 0) ? LinD::constant(1.0, (size_t)P) : x.div(a0);
           const int64_t at = (f * n_wl + i) * gw + l;
-          res.greek[at] = x.v;
-          if (res.greek_err) res.greek_err[at] = x.e;
+          g_out[at] = x.v;
+          if (ge_out) ge_out[at] = x.e;
           for (int64_t c = 0; c < P; ++c) {
             const int64_t atd = ((c * 6 + f) * n_wl + i) * gw + l;
-            if (dd.d_greek) dd.d_greek[atd] = x.d[c];
-            if (dd.d_greek_err) dd.d_greek_err[atd] = x.de[c];
+            if (dg_out) dg_out[atd] = x.d[c];
+            if (dge_out) dge_out[atd] = x.de[c];
           }
         }
     }

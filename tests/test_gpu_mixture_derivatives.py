@@ -98,9 +98,24 @@ def test_multimodal_spheroid_mode_weight(gpu):
     _check(run, k, 0.7, "c1.mode1.weight")
 
 
-def test_greek_all_is_refused(gpu):
-    items = [(("lognormal", 0.05, 1.5), ("sphere", np.array([1.45 + 0j])), 2.0),
-             (("lognormal", 0.03, 1.4), ("spheroid", 0.5, np.array([DUST])), 0.5)]
-    with pytest.raises(InvalidInputError, match="greek='all'"):
-        _scatrs.ensemble_compute(items, np.array([1.0]), True, None, True, None, True, [9],
-                                 1e-6, 4096, False, False)
+def test_greek_all(gpu):
+    """greek='all' (every wavelength's order 2 N_max over every part, engine.rs:2016-2036): at
+    each wavelength the derivatives and coefficients equal a call at that order alone, zero
+    above it (pass 1 does not refine on the Greek coefficients, so the panels are the same)."""
+    items = [(("lognormal", 0.05, 1.5), ("sphere", np.array([1.45 + 0j, 1.45 + 0j])), 2.0),
+             (("lognormal", 0.03, 1.4), ("spheroid", 0.5, np.array([DUST, DUST])), 0.5)]
+    wl = np.array([1.0, 0.5])
+    a = _scatrs.ensemble_compute(items, wl, True, None, True, None, True, [9, 2], 1e-6, 4096,
+                                 False, False)
+    width = a["greek"].shape[-1]
+    for i in range(wl.size):
+        one = [(spec, (p[0],) + p[1:-1] + (p[-1][i:i + 1],), w) for spec, p, w in items]
+        order = int(np.max(np.nonzero(np.any(a["greek"][:, i] != 0, axis=0))[0]))
+        b = _scatrs.ensemble_compute(one, wl[i:i + 1], True, order, False, None, True, [9, 2],
+                                     1e-6, 4096, False, False)
+        np.testing.assert_allclose(a["d"][:, :, i], b["d"][:, :, 0], rtol=1e-12, atol=0)
+        np.testing.assert_allclose(a["greek"][:, i, :order + 1], b["greek"][:, 0], rtol=1e-12,
+                                   atol=1e-300)
+        np.testing.assert_allclose(a["greek_d"][:, :, i, :order + 1], b["greek_d"][:, :, 0],
+                                   rtol=1e-12, atol=1e-300)
+        assert not a["greek_d"][:, :, i, order + 1:].any() and order + 1 <= width
