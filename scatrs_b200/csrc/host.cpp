@@ -2162,17 +2162,6 @@ void adaptive_call_order(const std::vector<AdPart>& in, int n_out, bool batch,
     std::vector<double> hav((size_t)n_units * stride), hav_x;
     SB_CUDA(cudaMemcpyAsync(hav.data(), avg, hav.size() * 8, cudaMemcpyDeviceToHost, s));
     SB_CUDA(cudaStreamSynchronize(s));
-    if (rows_out) {  // a mixture's host assembly: the per-block rows by unit
-      if (radius_x)
-        throw Failure{SCATRS_INVALID_INPUT,
-                      "the radius derivative of a single radius in a mixture of different "
-                      "particles is not on the GPU path"};
-      rows_out->stride = stride;
-      rows_out->rows = std::move(hav);
-      rows_out->converged = unit_converged;
-      rows_out->panels = unit_panels;
-      return;
-    }
     if (radius_x) {
       // The single radii's derivatives along x (engine.rs:1158-1170, 1857-1883): the pipeline
       // again with K-a's x direction in place of Re m.
@@ -2184,6 +2173,30 @@ void adaptive_call_order(const std::vector<AdPart>& in, int n_out, bool batch,
       hav_x.resize(hav.size());
       SB_CUDA(cudaMemcpyAsync(hav_x.data(), avg, hav_x.size() * 8, cudaMemcpyDeviceToHost, s));
       SB_CUDA(cudaStreamSynchronize(s));
+    }
+    if (rows_out) {  // a mixture's host assembly: the per-block rows by unit
+      // A single radius's radius derivative goes into its first parameter block (zero there:
+      // a point has no weight derivatives), as mix_derivatives adds it: d/dr = (2 pi / lambda)
+      // d/dx of every slot, 2 r and 3 r^2 for <r^2> and <r^3>, no error estimate.
+      for (int64_t p = 0; p < n_parts && radius_x; ++p) {
+        if (parts[p].support != adaptive::POINT || in[p].grads.empty()) continue;
+        const double r = parts[p].lo;
+        for (int64_t i = 0; i < n_wl; ++i) {
+          const int64_t u = p * n_wl + i;
+          double* blk = hav.data() + u * stride + 2 * row;
+          const double* ax = hav_x.data() + u * stride + 2 * (n_theta + 1) * row;
+          const double kw = 2.0 * kPi / wavelengths[i];
+          for (int64_t k = 0; k < row; ++k) {
+            blk[k] = k == 0 ? 0.0 : k == 6 ? 2.0 * r : k == 7 ? 3.0 * r * r : kw * ax[k];
+            blk[row + k] = 0.0;
+          }
+        }
+      }
+      rows_out->stride = stride;
+      rows_out->rows = std::move(hav);
+      rows_out->converged = unit_converged;
+      rows_out->panels = unit_panels;
+      return;
     }
     mix_derivatives(in, parts, n_out, n_wl, n_mu, options->greek_order, options->normalized != 0,
                     n_theta, hav, *dd, res, wavelengths, hav_x);

@@ -119,3 +119,15 @@ def test_greek_all(gpu):
         np.testing.assert_allclose(a["greek_d"][:, :, i, :order + 1], b["greek_d"][:, :, 0],
                                    rtol=1e-12, atol=1e-300)
         assert not a["greek_d"][:, :, i, order + 1:].any() and order + 1 <= width
+
+
+def test_single_sphere_radius_in_a_mixture(gpu):
+    """A single sphere radius beside a spheroid: its radius derivative (engine.rs:1158-1170,
+    the x pass placed in the part's parameter block) through the mixture's assembly."""
+    def run(r, derivatives):
+        items = [(("monodisperse", r), ("sphere", np.array([1.45 + 0.01j])), 2.0),
+                 (("lognormal", 0.03, 1.4), ("spheroid", 0.5, np.array([DUST])), 0.5)]
+        return _scatrs.ensemble_compute(items, np.array([1.0]), True, 6, False,
+                                        np.array([0.8, -0.6, -1.0]), True, list(derivatives),
+                                        1e-9, 50_000, False, False)
+    _check(run, 0, 0.2, "c0.radius")
