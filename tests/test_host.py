@@ -33,6 +33,36 @@ def test_parameter_names_follow_the_reference():
         _scatrs.ensemble_parameters([(("weibull", 1.0), ("sphere", m), 1.0)], False)
 
 
+def test_parameter_records_carry_each_name_to_its_kind():
+    """Every name of ensemble_parameters has a (component, mode, kind, index) record in the same
+    order (EnsembleParam, ensemble/mod.rs:180-215): a spheroid's Re m, Im m and aspect ratio, a
+    layered sphere's LayerRefrReal(l), LayerRefrImag(l) per layer then RadiusFraction(l), a
+    multimodal component's modes and mode weights."""
+    m = np.array([1.5 + 0j])
+    items = [(("lognormal", 0.1, 1.5), ("spheroid", 2.0, m), 1.0),
+             (("multimodal", [(1.0, ("lognormal", 0.1, 1.5)), (2.0, ("gamma", 1.0, 0.1))]),
+              ("layered", np.array([0.3, 0.6]), np.ones((3, 1), complex)), 2.0)]
+    names = _scatrs.ensemble_parameters(items, True)
+    records = _scatrs._parameter_records(items, True)
+    assert len(records) == len(names)
+    kind = {_native.PARAM_DISTRIBUTION: "d", _native.PARAM_REFR_REAL: "m_real",
+            _native.PARAM_REFR_IMAG: "m_imag", _native.PARAM_WEIGHT: "weight",
+            _native.PARAM_ASPECT_RATIO: "aspect_ratio",
+            _native.PARAM_LAYER_REFR_REAL: "layer{}.m_real",
+            _native.PARAM_LAYER_REFR_IMAG: "layer{}.m_imag",
+            _native.PARAM_RADIUS_FRACTION: "layer{}.radius_fraction"}
+    for name, (comp, mode, k, index) in zip(names, records):
+        assert name.startswith(f"c{comp}.")
+        if mode >= 0:
+            assert f".mode{mode}." in name
+        if k != _native.PARAM_DISTRIBUTION:
+            assert name.endswith("." + kind[k].format(index)), (name, k, index)
+    assert [r[2] for r in records[:6]] == [0, 0, 1, 2, 4, 3]
+    assert records[-4:-1] == [(1, -1, _native.PARAM_LAYER_REFR_IMAG, 2),
+                              (1, -1, _native.PARAM_RADIUS_FRACTION, 0),
+                              (1, -1, _native.PARAM_RADIUS_FRACTION, 1)]
+
+
 def test_distribution_specs_and_ranges():
     d = _scatrs._dist_array([("lognormal", 0.2, 1.5), ("power_law", 3.0, 0.1, 2.0)], 4.0)
     assert d["kind"].tolist() == [1, 4]
