@@ -224,6 +224,7 @@ struct Context {
       tm_sums, tm_err;
   DevBuf ro_sph, ro_rank, ro_w, ro_part, ro_f, ro_greek, ro_mu, ro_proj;
   DevBuf p1_fr, p1_ml;  // layered parts of an adaptive call
+  DevBuf p1_ml_aug;     // their indices with a vacuum shell (a single radius's radius)
   std::map<int64_t, std::vector<double>> dd_rules;  // n -> per node x (hi, lo), w (hi, lo)
   std::vector<int> chunk_n_host;
   int* pinned_chunk_n = nullptr;
@@ -1693,6 +1694,29 @@ struct PartRows {
   std::vector<int64_t> panels;
 };
 
+// A single radius's radius derivative (engine.rs:1158-1170, 1857-1883) into its first parameter
+// block of an adaptive call's per-block rows (zero there: a point has no weight derivatives), as
+// mix_derivatives adds it: d/dr = (2 pi / lambda) d/dx of every slot from the x rows hav_x,
+// 2 r and 3 r^2 for <r^2> and <r^3>, no error estimate.
+void place_radius_rows(const std::vector<AdPart>& in, const std::vector<adaptive::Part>& parts,
+                       int64_t n_wl, const double* wavelengths, int n_theta, int64_t row,
+                       int64_t stride, const std::vector<double>& hav_x, std::vector<double>& hav) {
+  for (size_t p = 0; p < parts.size(); ++p) {
+    if (parts[p].support != adaptive::POINT || in[p].grads.empty()) continue;
+    const double r = parts[p].lo;
+    for (int64_t i = 0; i < n_wl; ++i) {
+      const int64_t u = (int64_t)p * n_wl + i;
+      double* blk = hav.data() + u * stride + 2 * row;
+      const double* ax = hav_x.data() + u * stride + 2 * (n_theta + 1) * row;
+      const double kw = 2.0 * kPi / wavelengths[i];
+      for (int64_t k = 0; k < row; ++k) {
+        blk[k] = k == 0 ? 0.0 : k == 6 ? 2.0 * r : k == 7 ? 3.0 * r * r : kw * ax[k];
+        blk[row + k] = 0.0;
+      }
+    }
+  }
+}
+
 // With n_max_out, only pass 1 runs (and its errors are reported): n_max_out receives each
 // (part, wavelength) unit's largest number of terms, its group's (engine.rs:1987-2030). With
 // rows_out, the parts' averages go there instead of the outputs: without derivatives as
@@ -1753,9 +1777,9 @@ void adaptive_call_order(const std::vector<AdPart>& in, int n_out, bool batch,
   if (L > kMaxLayersAbi) throw Failure{SCATRS_INVALID_INPUT, "the GPU path takes 1 to 16 layers"};
   if (L > 1 && (!layers->fractions || !layers->m))
     throw Failure{SCATRS_INVALID_INPUT, "layers must give fractions and m"};
-  if (L > 1 && radius_x)
+  if (L > 1 && radius_x && L + 1 > kMaxLayersAbi)
     throw Failure{SCATRS_INVALID_INPUT,
-                  "the radius derivative of a single layered sphere is not on the GPU path"};
+                  "the radius derivative of a single layered sphere takes at most 15 layers"};
   // A layered sphere's direction groups with a requested direction (any part's): group l < L is
   // layer l's index (directions 2 l, 2 l + 1), group L + f the radius fraction f (direction
   // 2 L + f).
@@ -2142,7 +2166,61 @@ void adaptive_call_order(const std::vector<AdPart>& in, int n_out, bool batch,
         }
       }
     }
+    // A single layered radius's radius (particle.rs:221-237 size_derivative: the sum over
+    // the interfaces of f_l d/dx_l and the outer surface's d/dx_L): the particle with a vacuum
+    // shell of zero thickness around it (fractions f_0..f_{L-2}, 1; index 1 outside) has the
+    // same coefficients, and its interface l's direction is x d/dx_l with the outer surface
+    // moving beneath the fixed vacuum radius; so d/dx = (1/x) sum_l f_l (its direction l's
+    // block), f_{L-1} = 1, one pass per interface. The sum goes where mix_derivatives and
+    // place_radius_rows read the x rows of a sphere.
+    std::vector<double> hav_x;
+    if (radius_x) {
+      const int la = L + 1;
+      std::vector<double> fr_aug((size_t)n_parts * L), ml_aug((size_t)2 * n_parts * la * n_wl);
+      for (int64_t p = 0; p < n_parts; ++p) {
+        for (int l = 0; l < L - 1; ++l) fr_aug[p * L + l] = layers->fractions[p * (L - 1) + l];
+        fr_aug[p * L + L - 1] = 1.0;
+        for (int l = 0; l < L; ++l)
+          for (int64_t i = 0; i < n_wl; ++i)
+            for (int k = 0; k < 2; ++k)
+              ml_aug[2 * ((p * la + l) * n_wl + i) + k] =
+                  layers->m[2 * ((p * L + l) * n_wl + i) + k];
+        for (int64_t i = 0; i < n_wl; ++i) {
+          ml_aug[2 * ((p * la + L) * n_wl + i)] = 1.0;
+          ml_aug[2 * ((p * la + L) * n_wl + i) + 1] = 0.0;
+        }
+      }
+      double* mla_d = c.p1_ml_aug.as<double>(ml_aug.size());
+      SB_CUDA(cudaMemcpyAsync(mla_d, ml_aug.data(), ml_aug.size() * 8, cudaMemcpyHostToDevice, s));
+      LayerInput lia;
+      lia.n_layers = la;
+      lia.fractions = fr_aug.data();
+      lia.m_dev = mla_d;
+      hav_x.assign((size_t)n_units * cstride, 0.0);
+      for (int l = 0; l < L; ++l) {
+        DerivOutput dvg = dvo;
+        dvg.dir = la + l;
+        run_fixed(c, dummy.data(), n_parts, wl_d, n_wl, m_d, mu, n_mu, &fo, nullptr, nullptr,
+                  nullptr, s, &call, lia, dvg, ad);
+        check_device_errors(c, s, &call);
+        SB_CUDA(cudaMemcpyAsync(one.data(), avg, one.size() * 8, cudaMemcpyDeviceToHost, s));
+        SB_CUDA(cudaStreamSynchronize(s));
+        for (int64_t p = 0; p < n_parts; ++p) {
+          if (parts[p].support != adaptive::POINT || in[p].grads.empty()) continue;
+          const double f = fr_aug[p * L + l];
+          for (int64_t i = 0; i < n_wl; ++i) {
+            const int64_t u = p * n_wl + i;
+            const double x = 2.0 * kPi * parts[p].lo / wavelengths[i];
+            const double* src = one.data() + u * stride + 2 * (n_theta + 1) * row;
+            double* dst = hav_x.data() + u * cstride + 2 * (n_theta + 1) * row;
+            for (int64_t k = 0; k < row; ++k) dst[k] += f / x * src[k];
+          }
+        }
+      }
+    }
     if (rows_out) {  // a mixture's host assembly: the per-block rows by unit
+      if (radius_x)
+        place_radius_rows(in, parts, n_wl, wavelengths, n_theta, row, cstride, hav_x, hav);
       rows_out->stride = cstride;
       rows_out->rows = std::move(hav);
       rows_out->converged = unit_converged;
@@ -2150,7 +2228,7 @@ void adaptive_call_order(const std::vector<AdPart>& in, int n_out, bool batch,
       return;
     }
     mix_derivatives(in, parts, n_out, n_wl, n_mu, options->greek_order, options->normalized != 0,
-                    n_theta, hav, *dd, res, wavelengths, {});
+                    n_theta, hav, *dd, res, wavelengths, hav_x);
     adaptive_flags(in, jobs, job_of, unit_converged, unit_panels, n_out, n_wl, res);
     return;
   }
@@ -2175,23 +2253,8 @@ void adaptive_call_order(const std::vector<AdPart>& in, int n_out, bool batch,
       SB_CUDA(cudaStreamSynchronize(s));
     }
     if (rows_out) {  // a mixture's host assembly: the per-block rows by unit
-      // A single radius's radius derivative goes into its first parameter block (zero there:
-      // a point has no weight derivatives), as mix_derivatives adds it: d/dr = (2 pi / lambda)
-      // d/dx of every slot, 2 r and 3 r^2 for <r^2> and <r^3>, no error estimate.
-      for (int64_t p = 0; p < n_parts && radius_x; ++p) {
-        if (parts[p].support != adaptive::POINT || in[p].grads.empty()) continue;
-        const double r = parts[p].lo;
-        for (int64_t i = 0; i < n_wl; ++i) {
-          const int64_t u = p * n_wl + i;
-          double* blk = hav.data() + u * stride + 2 * row;
-          const double* ax = hav_x.data() + u * stride + 2 * (n_theta + 1) * row;
-          const double kw = 2.0 * kPi / wavelengths[i];
-          for (int64_t k = 0; k < row; ++k) {
-            blk[k] = k == 0 ? 0.0 : k == 6 ? 2.0 * r : k == 7 ? 3.0 * r * r : kw * ax[k];
-            blk[row + k] = 0.0;
-          }
-        }
-      }
+      if (radius_x)
+        place_radius_rows(in, parts, n_wl, wavelengths, n_theta, row, stride, hav_x, hav);
       rows_out->stride = stride;
       rows_out->rows = std::move(hav);
       rows_out->converged = unit_converged;

@@ -13,7 +13,7 @@ import numpy as np
 import pytest
 
 from scatrs_b200 import _scatrs
-from scatrs_b200.errors import InvalidInputError, OutsideValidatedDomainError
+from scatrs_b200.errors import OutsideValidatedDomainError
 
 pytestmark = pytest.mark.gpu
 
@@ -120,8 +120,12 @@ def test_derivatives_need_the_layered_derivative_domain(gpu):
     assert np.all(np.isfinite(ok["values"]))
 
 
-def test_refusals(gpu):
-    particle = ("layered", [0.6], np.array([[CORE], [SHELL]]))
-    with pytest.raises(InvalidInputError, match="radius derivative of a single layered"):
-        _scatrs.ensemble_compute([(("monodisperse", 0.3), particle, 1.0)], WL, False, None,
-                                 False, None, True, [0], 1e-6, 4096, False, False)
+def test_single_radius(gpu):
+    """A monodisperse ensemble's radius at fixed fractions (particle.rs:221-237, the sum over the
+    interfaces of f_l d/dx_l and the outer surface's d/dx_L; scatrs/tests/ensemble_layered.rs:
+    237-240): the particle with a vacuum shell of zero thickness gives the outer surface's
+    direction."""
+    _check(lambda v, d: _run(("monodisperse", v), [0.6], [CORE, SHELL], d), 0, 0.3, "radius")
+    ms = [1.6 + 0.3j, 2.0 + 0.05j, 1.33 + 1e-6j]
+    _check(lambda v, d: _run(("monodisperse", v), [0.3, 0.7], ms, d), 0, 0.25,
+           "three layers: radius")
