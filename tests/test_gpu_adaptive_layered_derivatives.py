@@ -129,3 +129,40 @@ def test_single_radius(gpu):
     ms = [1.6 + 0.3j, 2.0 + 0.05j, 1.33 + 1e-6j]
     _check(lambda v, d: _run(("monodisperse", v), [0.3, 0.7], ms, d), 0, 0.25,
            "three layers: radius")
+
+
+def test_against_the_oracle_differences(gpu):
+    """Every direction of one call against central differences of the oracle's adaptive layered
+    ensemble (its own panels and values at rtol 1e-11): a pin of the GPU's derivative blocks
+    that does not go through the GPU's values."""
+    from oracle import oracle as O
+
+    def oracle(p):  # p: median radius, width, core Re, Im, shell Re, Im, fraction
+        d = np.zeros(1, dtype=O.DIST_DTYPE)
+        d["kind"] = 1
+        d["p"][0, :2] = p[0], p[1]
+        ml = np.array([[[complex(p[2], p[3])], [complex(p[4], p[5])]]])
+        return O.ensemble_adaptive_layered(d, WL, np.array([[p[6]]]), ml, MU, 6, rtol=1e-11,
+                                           max_panels=50_000)
+
+    base = [0.15, 1.5, CORE.real, CORE.imag, SHELL.real, SHELL.imag, 0.6]
+    got = _run(LOGN, [0.6], [CORE, SHELL], range(7))
+    v = got["values"][:, 0]
+    f11 = got["phase"][0, 0]
+    for k, value in enumerate(base):
+        h = 1e-4 * abs(value)
+        plus, minus = list(base), list(base)
+        plus[k] += h
+        minus[k] -= h
+        op, om = oracle(plus), oracle(minus)
+        for j in range(11):
+            fd = (op["values"][j, 0] - om["values"][j, 0]) / (2 * h)
+            scale = max(abs(fd), abs(v[j]) / abs(value), 1e-300)
+            assert abs(got["d"][k][j, 0] - fd) <= 1e-5 * scale, (k, j, got["d"][k][j, 0], fd)
+        fd = (op["greek"][4, 0] - om["greek"][4, 0]) / (2 * h)
+        gd = got["greek_d"][k][4, 0]
+        assert np.all(np.abs(gd - fd) <= 1e-5 * np.maximum(np.abs(fd), 1e-3)), (k, "beta1")
+        for el in (0, 1):
+            fd = (op["phase"][el, 0] - om["phase"][el, 0]) / (2 * h)
+            scale = np.maximum(np.abs(fd), f11 / abs(value))
+            assert np.all(np.abs(got["phase_d"][k][el, 0] - fd) <= 1e-5 * scale), (k, el)
