@@ -131,3 +131,50 @@ def test_single_sphere_radius_in_a_mixture(gpu):
                                         np.array([0.8, -0.6, -1.0]), True, list(derivatives),
                                         1e-9, 50_000, False, False)
     _check(run, 0, 0.2, "c0.radius")
+
+
+def test_layered_mixture_against_the_oracle_differences(gpu):
+    """A sphere and a coated sphere: the derivatives along the sphere's index, the coating's
+    fraction and index and the coated component's weight against central differences of the
+    oracle's own mixture (its panels and values at rtol 1e-11)."""
+    from oracle import oracle as O
+
+    wl = np.array([0.55])
+    mu = np.array([0.8, -0.6])
+    base = {"m0": 1.45, "f": 0.5, "si": SHELL.imag, "w1": 0.5}
+
+    def items(p):
+        return [(("lognormal", 0.1, 1.5), ("sphere", np.array([complex(p["m0"], 0.0)])), 2.0),
+                (("lognormal", 0.3, 1.4),
+                 ("layered", [p["f"]], np.array([[CORE], [complex(SHELL.real, p["si"])]])),
+                 p["w1"])]
+
+    def oracle(p):
+        comps = []
+        for (kind, *par), particle, w in items(p):
+            d = np.zeros(1, dtype=O.DIST_DTYPE)
+            d["kind"], d["p"][0, :2] = 1, par
+            m = particle[1] if particle[0] == "sphere" else particle
+            comps.append((d, None, w, m))
+        return O.ensemble_mixture_d(comps, wl, np.zeros(0, dtype=O.PARAM_DTYPE), mu, 6,
+                                    rtol=1e-11, max_panels=50_000)
+
+    names = _scatrs.ensemble_parameters(items(base), True)
+    cols = {"m0": names.index("c0.m_real"), "f": names.index("c1.layer0.radius_fraction"),
+            "si": names.index("c1.layer1.m_imag"), "w1": names.index("c1.weight")}
+    got = _scatrs.ensemble_compute(items(base), wl, True, 6, False, mu, True,
+                                   list(cols.values()), 1e-11, 50_000, False, False)
+    v = got["values"][:, 0]
+    for c, (key, value) in enumerate(base.items()):
+        h = 1e-4 * abs(value)
+        op, om = oracle({**base, key: value + h}), oracle({**base, key: value - h})
+        for j in range(11):
+            fd = (op["values"][j, 0] - om["values"][j, 0]) / (2 * h)
+            scale = max(abs(fd), abs(v[j]) / abs(value), 1e-300)
+            assert abs(got["d"][c][j, 0] - fd) <= 1e-5 * scale, (key, j, got["d"][c][j, 0], fd)
+        fd = (op["greek"][0, 0] - om["greek"][0, 0]) / (2 * h)
+        assert np.all(np.abs(got["greek_d"][c][0, 0] - fd)
+                      <= 1e-5 * np.maximum(np.abs(fd), 1e-3)), (key, "alpha1")
+        fd = (op["phase"][:, 0] - om["phase"][:, 0]) / (2 * h)
+        scale = np.maximum(np.abs(fd), got["phase"][0, 0][None, :] / abs(value))
+        assert np.all(np.abs(got["phase_d"][c][:, 0] - fd) <= 1e-5 * scale), (key, "phase")
