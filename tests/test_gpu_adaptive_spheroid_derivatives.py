@@ -99,3 +99,39 @@ def test_a_sphere_has_no_aspect_ratio(gpu):
     bad = np.array([(0, -1, gpu.PARAM_ASPECT_RATIO, 0)], dtype=gpu.PARAM_DTYPE)
     with pytest.raises(InvalidInputError, match="no parameter aspect_ratio"):
         gpu.ensemble_mixture_d(comps, [0.5], bad)
+
+
+def test_against_the_oracle_differences(gpu):
+    """The aspect ratio, Re m, Im m and median radius in one call against central differences
+    of the oracle's own adaptive spheroid ensemble (its panels, its double-precision EBCM and
+    Racah-based orientation average per node, rtol 1e-9): a pin of the GPU's derivative blocks
+    that does not go through the GPU's values."""
+    from oracle import oracle as O
+
+    base = [0.03, 2.0, DUST.real, DUST.imag]  # median radius, aspect ratio, Re m, Im m
+
+    def oracle(p):
+        d = np.zeros(1, dtype=O.DIST_DTYPE)
+        d["kind"] = 1
+        d["p"][0, :2] = p[0], 1.4
+        return O.ensemble_adaptive_spheroid(d, WL, p[1], np.array([complex(p[2], p[3])]), MU, 6,
+                                            rtol=1e-9, max_panels=50_000)
+
+    got = _run(LOGN, 2.0, DUST, [0, 4, 2, 3])
+    v = got["values"][:, 0]
+    for c, value in enumerate(base):
+        h = 1e-4 * abs(value)
+        plus, minus = list(base), list(base)
+        plus[c] += h
+        minus[c] -= h
+        op, om = oracle(plus), oracle(minus)
+        for j in range(11):
+            fd = (op["values"][j, 0] - om["values"][j, 0]) / (2 * h)
+            scale = max(abs(fd), abs(v[j]) / abs(value), 1e-300)
+            assert abs(got["d"][c][j, 0] - fd) <= 1e-5 * scale, (c, j, got["d"][c][j, 0], fd)
+        fd = (op["greek"][0, 0] - om["greek"][0, 0]) / (2 * h)
+        assert np.all(np.abs(got["greek_d"][c][0, 0] - fd)
+                      <= 1e-5 * np.maximum(np.abs(fd), 1e-3)), (c, "alpha1")
+        fd = (op["phase"][:, 0] - om["phase"][:, 0]) / (2 * h)
+        scale = np.maximum(np.abs(fd), got["phase"][0, 0][None, :] / abs(value))
+        assert np.all(np.abs(got["phase_d"][c][:, 0] - fd) <= 1e-5 * scale), (c, "phase")
