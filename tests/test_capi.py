@@ -50,3 +50,19 @@ def test_output_sizes():
 
 def test_device_count_is_an_integer():
     assert isinstance(_native.load().scatrs_device_count(), int)
+
+
+def test_parameter_kinds_match_the_header():
+    """The binding's parameter kinds are the header's SCATRS_PARAM_* values
+    (ParamKind, scatrs/src/ensemble/mod.rs:180-215)."""
+    src = open(os.path.join(ROOT, "include", "scatrs_b200.h")).read()
+    values = {m.group(1): int(m.group(2))
+              for m in re.finditer(r"SCATRS_PARAM_([A-Z_]+)\s*=\s*(\d+)", src)}
+    assert values == {"DISTRIBUTION": _native.PARAM_DISTRIBUTION,
+                      "REFR_REAL": _native.PARAM_REFR_REAL,
+                      "REFR_IMAG": _native.PARAM_REFR_IMAG,
+                      "WEIGHT": _native.PARAM_WEIGHT,
+                      "ASPECT_RATIO": _native.PARAM_ASPECT_RATIO,
+                      "LAYER_REFR_REAL": _native.PARAM_LAYER_REFR_REAL,
+                      "LAYER_REFR_IMAG": _native.PARAM_LAYER_REFR_IMAG,
+                      "RADIUS_FRACTION": _native.PARAM_RADIUS_FRACTION}
