@@ -594,7 +594,7 @@ void pass1(std::vector<Job>& jobs, const std::vector<Part>& parts, const double*
       // The quantities of the group's first part's directions (engine.rs:491-506).
       const Part& first = parts[jobs[ji].parts[0]];
       const int nr = first.n_refined();
-      std::vector<int> qi(nr);
+      int qi[kPass1 + kGroup * kMaxAllDirs];  // make_part's callers keep nr within it
       for (int j = 0; j < kPass1; ++j) qi[j] = j;
       {
         int at = kPass1;

@@ -22,6 +22,7 @@ constexpr int kGroup = 5;         // per direction: d of C_ext, C_sca, C_sca g, 
 constexpr int kMaxDirs = 3;
 constexpr int kSphereQ = kPass1 + 2 * kGroup;       // a sphere node's quantities with Re m, Im m
 constexpr int kNodeQ = kPass1 + kMaxDirs * kGroup;  // a node's quantities with every direction
+constexpr int kMaxAllDirs = 3 * 16 - 1;             // the most directions: a 16-layer sphere's
 
 struct Error {
   int status;

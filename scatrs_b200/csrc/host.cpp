@@ -1761,6 +1761,8 @@ void adaptive_call_order(const std::vector<AdPart>& in, int n_out, bool batch,
     } catch (const adaptive::Error& e) {
       throw Failure{e.status, p.who + e.msg};
     }
+    if ((int)p.dir_cols.size() > adaptive::kMaxAllDirs)
+      throw Failure{SCATRS_INVALID_INPUT, "the GPU path takes 1 to 16 layers"};
     parts.back().dirs.assign(p.dir_cols.size(), 0);
     for (size_t k = 0; k < p.dir_cols.size(); ++k) parts.back().dirs[k] = p.dir_cols[k] >= 0;
     n_theta = std::max(n_theta, (int)p.grads.size());
