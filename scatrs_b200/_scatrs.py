@@ -397,9 +397,9 @@ def ensemble_compute_fixed(specs, particle_spec, wavelengths, greek, all_orders,
                            ranges=None, derivatives=(), tmatrix_rtol: float = 1e-8) -> dict:
     """The batch dict on a fixed grid. ``derivatives`` selects parameters by their index in
     ``ensemble_parameters([(specs[0], particle_spec, 1.0)], False)`` (the reference's
-    ``deriv_idx``): homogeneous or layered spheres, every distribution of one kind. Spheroids
-    (``('spheroid', aspect_ratio, m)``) converge every node's T-matrix to ``tmatrix_rtol``; their
-    derivatives are not built."""
+    ``deriv_idx``): homogeneous or layered spheres or spheroids, every distribution of one kind.
+    Spheroids (``('spheroid', aspect_ratio, m)``) converge every node's T-matrix to
+    ``tmatrix_rtol``."""
     if not isinstance(particle_spec, tuple) or particle_spec[0] not in ("sphere", "layered",
                                                                          "spheroid"):
         raise TypeError("the fixed-grid ensemble takes ('sphere', m), ('layered', fractions, m) "
@@ -413,14 +413,28 @@ def ensemble_compute_fixed(specs, particle_spec, wavelengths, greek, all_orders,
     derivatives = [int(k) for k in derivatives]
     d = dp = dg = None
     if particle_spec[0] == "spheroid":
-        if derivatives:
-            raise InvalidInputError("a spheroid's derivatives are not built on the GPU path")
         m = np.asarray(particle_spec[2], dtype=np.complex128)
         if m.ndim == 1:
             m = np.broadcast_to(m, (dists.size, wl.size))
-        values, phase, g, _ = _native.ensemble_fixed_spheroid(
-            dists, wl, float(particle_spec[1]), m, mu, n_nodes, L, bool(normalized),
-            tmatrix_rtol=tmatrix_rtol, allow_unvalidated=bool(allow_unvalidated))
+        if derivatives:
+            names = ensemble_parameters([(specs[0], particle_spec, 1.0)], False)
+            for k in derivatives:
+                if not 0 <= k < len(names):
+                    raise InvalidInputError(f"derivative index {k} out of range of {names}")
+            values, phase, g, d, dp, dg, _ = _native.ensemble_fixed_spheroid_d(
+                dists, wl, float(particle_spec[1]), m, mu, n_nodes, L, bool(normalized),
+                tmatrix_rtol=tmatrix_rtol, allow_unvalidated=bool(allow_unvalidated))
+            # The library's blocks: the distribution's parameters, the aspect ratio, Re m, Im m;
+            # the names': the distribution's, m_real, m_imag, aspect_ratio.
+            pt = len(names) - 3
+            col = [k if k < pt else {pt: pt + 1, pt + 1: pt + 2, pt + 2: pt}[k]
+                   for k in derivatives]
+            d, dp, dg = (None if a is None else np.ascontiguousarray(a[col])
+                         for a in (d, dp, dg))
+        else:
+            values, phase, g, _ = _native.ensemble_fixed_spheroid(
+                dists, wl, float(particle_spec[1]), m, mu, n_nodes, L, bool(normalized),
+                tmatrix_rtol=tmatrix_rtol, allow_unvalidated=bool(allow_unvalidated))
     elif particle_spec[0] == "layered":
         ml = np.asarray(particle_spec[2], dtype=np.complex128)
         fr = np.asarray(particle_spec[1], dtype=np.float64)

@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 from oracle import oracle as O
-from scatrs_b200 import _native
+from scatrs_b200 import _native, _scatrs
 
 pytestmark = pytest.mark.gpu
 
@@ -178,3 +178,19 @@ def test_spheroid_autograd_aspect_ratio_gradient(gpu):
            m_re.grad[0, 0].item(), m_im.grad[0, 0].item()]
     assert np.allclose(got, expect, rtol=1e-12, atol=1e-15)
     assert abs(got[2]) > 0.0
+
+
+def test_fixed_grid_binding_takes_spheroid_derivatives(gpu):
+    """ensemble_compute_fixed with a spheroid and derivatives: its columns, in
+    ensemble_parameters' order (median_radius, width, m_real, m_imag, aspect_ratio), are the
+    library's blocks (the distribution's, the aspect ratio, Re m, Im m) bit for bit."""
+    d, wl, eps, m, mu = _small_ensemble()
+    spec = ("lognormal", 0.12, 1.5)
+    particle = ("spheroid", eps, m[0])
+    raw = _scatrs.ensemble_compute_fixed([spec], particle, wl, 8, False, mu, True, n_nodes=6,
+                                         ranges=[(d["r_lo"][0], d["r_hi"][0])],
+                                         derivatives=[4, 2, 0], tmatrix_rtol=1e-10)
+    res = _native.ensemble_fixed_spheroid_d(d, wl, eps, m, mu, 6, 8, True, 1e-10)
+    assert np.array_equal(raw["values"], res[0])
+    for got, want in ((raw["d"], res[3]), (raw["phase_d"], res[4]), (raw["greek_d"], res[5])):
+        assert np.array_equal(got, want[[2, 3, 0]])
